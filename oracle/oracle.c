@@ -1,0 +1,698 @@
+/*
+ * oracle.c -- CPU restatement of the reference's bootstrapping hot path.
+ * TEST INFRASTRUCTURE ONLY (see oracle.h): the checker for the CUDA path and the
+ * timed CPU baseline; never linked into or called by the product library.
+ *
+ * Exact integer arithmetic throughout (unsigned __int128).  Batched routines use
+ * OpenMP over independent ciphertexts.
+ */
+#include "oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+typedef unsigned __int128 u128;
+
+int orc_num_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+/* ------------------------------------------------------------------------------------------ */
+/* scalar modular arithmetic                                                                    */
+/* ------------------------------------------------------------------------------------------ */
+
+uint64_t orc_mulmod(uint64_t a, uint64_t b, uint64_t q) { return (uint64_t)(((u128)a * b) % q); }
+
+static inline uint64_t addmod(uint64_t a, uint64_t b, uint64_t q) {
+    uint64_t s = a + b;
+    return (s >= q || s < a) ? s - q : s;
+}
+static inline uint64_t submod(uint64_t a, uint64_t b, uint64_t q) { return a >= b ? a - b : a + q - b; }
+
+uint64_t orc_powmod(uint64_t a, uint64_t e, uint64_t q) {
+    uint64_t r = 1 % q;
+    a %= q;
+    while (e) {
+        if (e & 1) r = orc_mulmod(r, a, q);
+        a = orc_mulmod(a, a, q);
+        e >>= 1;
+    }
+    return r;
+}
+
+uint64_t orc_invmod(uint64_t a, uint64_t q) {
+    /* extended Euclid over signed 128-bit */
+    __int128 t = 0, nt = 1, r = q, nr = a % q;
+    while (nr != 0) {
+        __int128 quo = r / nr, tmp;
+        tmp = t - quo * nt; t = nt; nt = tmp;
+        tmp = r - quo * nr; r = nr; nr = tmp;
+    }
+    if (r != 1) return 0;
+    if (t < 0) t += q;
+    return (uint64_t)t;
+}
+
+/* floor(w * 2^64 / q): the Shoup quotient (src/host/uintarithsmallmod.h compute_shoup) */
+uint64_t orc_shoup(uint64_t w, uint64_t q) { return (uint64_t)(((u128)w << 64) / q); }
+
+/* deterministic Miller-Rabin for 64-bit integers (bases valid for n < 2^64) */
+int orc_is_prime(uint64_t n) {
+    if (n < 2) return 0;
+    static const uint64_t small[] = {2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37};
+    for (size_t i = 0; i < sizeof(small) / sizeof(small[0]); ++i) {
+        if (n == small[i]) return 1;
+        if (n % small[i] == 0) return 0;
+    }
+    uint64_t d = n - 1;
+    int s = 0;
+    while ((d & 1) == 0) { d >>= 1; ++s; }
+    for (size_t i = 0; i < sizeof(small) / sizeof(small[0]); ++i) {
+        uint64_t x = orc_powmod(small[i], d, n);
+        if (x == 1 || x == n - 1) continue;
+        int comp = 1;
+        for (int r = 1; r < s; ++r) {
+            x = orc_mulmod(x, x, n);
+            if (x == n - 1) { comp = 0; break; }
+        }
+        if (comp) return 0;
+    }
+    return 1;
+}
+
+/* src/host/numth.cu:207-233: start at 2^bits - 2N + 1 and step down by 2N */
+int orc_get_primes(uint32_t ntt_size, int bit_size, uint32_t count, uint64_t *out) {
+    const uint64_t factor = 2ull * ntt_size;
+    uint64_t value = (1ull << bit_size) - factor + 1;
+    const uint64_t lower = 1ull << (bit_size - 1);
+    uint32_t found = 0;
+    while (found < count && value > lower) {
+        if (orc_is_prime(value)) out[found++] = value;
+        value -= factor;
+    }
+    return found == count ? 0 : -1;
+}
+
+/* src/host/numth.cu:309-331: the smallest primitive degree-th root of unity. The reference
+ * starts from a random primitive root and scans its odd powers; the minimum over that orbit
+ * does not depend on the starting root, so a deterministic search gives the same value. */
+uint64_t orc_minimal_primitive_root(uint64_t degree, uint64_t q) {
+    if ((q - 1) % degree) return 0;
+    const uint64_t cof = (q - 1) / degree;
+    uint64_t root = 0;
+    for (uint64_t g = 2; g < q; ++g) {
+        uint64_t c = orc_powmod(g, cof, q);
+        if (orc_powmod(c, degree >> 1, q) == q - 1) { root = c; break; }
+    }
+    if (!root) return 0;
+    const uint64_t gsq = orc_mulmod(root, root, q);
+    uint64_t cur = root, best = root;
+    for (uint64_t i = 0; i < degree; ++i) {
+        if (cur < best) best = cur;
+        cur = orc_mulmod(cur, gsq, q);
+    }
+    return best;
+}
+
+/* ------------------------------------------------------------------------------------------ */
+/* Phantom NTT tables and transforms                                                           */
+/* ------------------------------------------------------------------------------------------ */
+
+static inline uint32_t brev(uint32_t x, uint32_t bits) {
+    uint32_t r = 0;
+    for (uint32_t i = 0; i < bits; ++i) { r = (r << 1) | (x & 1); x >>= 1; }
+    return r;
+}
+
+/* src/host/ntt.cu:11-56 */
+int orc_ntt_tables(uint32_t log_n, uint64_t q, uint64_t *rp, uint64_t *rp_sh, uint64_t *irp, uint64_t *irp_sh,
+                   uint64_t *n_inv) {
+    const uint32_t n = 1u << log_n;
+    const uint64_t root = orc_minimal_primitive_root(2ull * n, q);
+    if (!root) return -1;
+    const uint64_t iroot = orc_invmod(root, q);
+    uint64_t pw = root, ipw = iroot;
+    rp[0] = 1;
+    irp[0] = 1;
+    for (uint32_t i = 1; i < n; ++i) {
+        rp[brev(i, log_n)] = pw;
+        irp[brev(i, log_n)] = ipw;
+        pw = orc_mulmod(pw, root, q);
+        ipw = orc_mulmod(ipw, iroot, q);
+    }
+    const uint64_t ninv = orc_invmod(n, q);
+    irp[1] = orc_mulmod(irp[1], ninv, q);
+    for (uint32_t i = 0; i < n; ++i) {
+        if (rp_sh) rp_sh[i] = orc_shoup(rp[i], q);
+        if (irp_sh) irp_sh[i] = orc_shoup(irp[i], q);
+    }
+    n_inv[0] = ninv;
+    n_inv[1] = orc_shoup(ninv, q);
+    return 0;
+}
+
+/* ntt_1d.cu:488-555: Cooley-Tukey, twiddle rp[m+k] for group k of stage m */
+static void ntt_fwd_one(uint64_t *a, uint32_t n, uint64_t q, const uint64_t *rp) {
+    for (uint32_t m = 1; m < n; m <<= 1) {
+        const uint32_t t = n / (2 * m);
+        for (uint32_t k = 0; k < m; ++k) {
+            const uint64_t w = rp[m + k];
+            for (uint32_t j = 2 * k * t; j < 2 * k * t + t; ++j) {
+                const uint64_t u = a[j], v = orc_mulmod(a[j + t], w, q);
+                a[j] = addmod(u, v, q);
+                a[j + t] = submod(u, v, q);
+            }
+        }
+    }
+}
+
+/* ntt_1d.cu:557-617: Gentleman-Sande; the last stage scales x by n^-1 and y through irp[1] */
+static void ntt_inv_one(uint64_t *a, uint32_t n, uint64_t q, const uint64_t *irp, uint64_t n_inv) {
+    for (uint32_t m = n / 2; m >= 1; m >>= 1) {
+        const uint32_t t = n / (2 * m);
+        for (uint32_t k = 0; k < m; ++k) {
+            const uint64_t w = irp[m + k];
+            for (uint32_t j = 2 * k * t; j < 2 * k * t + t; ++j) {
+                const uint64_t u = a[j], v = a[j + t];
+                a[j] = addmod(u, v, q);
+                a[j + t] = orc_mulmod(submod(u, v, q), w, q);
+            }
+        }
+        if (m == 1) break;
+    }
+    for (uint32_t j = 0; j < n / 2; ++j) a[j] = orc_mulmod(a[j], n_inv, q);
+}
+
+void orc_ntt_forward(uint64_t *a, size_t batch, uint32_t n, uint64_t q, const uint64_t *rp) {
+#pragma omp parallel for schedule(static)
+    for (long b = 0; b < (long)batch; ++b) ntt_fwd_one(a + (size_t)b * n, n, q, rp);
+}
+
+void orc_ntt_inverse(uint64_t *a, size_t batch, uint32_t n, uint64_t q, const uint64_t *irp, uint64_t n_inv) {
+#pragma omp parallel for schedule(static)
+    for (long b = 0; b < (long)batch; ++b) ntt_inv_one(a + (size_t)b * n, n, q, irp, n_inv);
+}
+
+void orc_ntt_inverse_permute(uint64_t *out, const uint64_t *in, const uint32_t *map, size_t batch, uint32_t n,
+                             uint64_t q, const uint64_t *irp, uint64_t n_inv) {
+#pragma omp parallel for schedule(static)
+    for (long b = 0; b < (long)batch; ++b) {
+        const uint64_t *src = in + (size_t)b * n;
+        uint64_t *dst = out + (size_t)b * n;
+        for (uint32_t i = 0; i < n; ++i) {
+            uint32_t s = map[i];
+            int neg = 0;
+            if (s >= n) { s -= n; neg = 1; }
+            uint64_t v = src[s];
+            dst[i] = (neg && v) ? q - v : v;
+        }
+        ntt_inv_one(dst, n, q, irp, n_inv);
+    }
+}
+
+void orc_negacyclic_mul(const uint64_t *a, const uint64_t *b, uint64_t *c, uint32_t n, uint64_t q) {
+    u128 *acc = (u128 *)calloc(2 * (size_t)n, sizeof(u128));
+    /* accumulate positive and negative halves separately, reduce at the end */
+    for (uint32_t i = 0; i < n; ++i) {
+        for (uint32_t j = 0; j < n; ++j) {
+            const u128 p = (u128)a[i] * b[j];
+            const uint32_t k = i + j;
+            if (k < n) acc[k] += p % q;
+            else acc[n + (k - n)] += p % q;
+        }
+    }
+    for (uint32_t k = 0; k < n; ++k) c[k] = submod((uint64_t)(acc[k] % q), (uint64_t)(acc[n + k] % q), q);
+    free(acc);
+}
+
+/* kernel.cu:7554-7571 */
+void orc_auto_maps(uint32_t *maps, uint32_t n, uint32_t levels) {
+    uint32_t log_n = 0;
+    while ((1u << log_n) < n) ++log_n;
+    for (uint32_t lv = 0; lv < levels; ++lv) {
+        const uint64_t k = (uint64_t)(n >> lv) + 1;
+        for (uint32_t tid = 0; tid < n; ++tid) {
+            const uint32_t j = brev(tid, log_n);
+            const uint64_t jt = 2ull * j + 1;
+            const uint32_t idx = (uint32_t)(((jt * k) & (2ull * n - 1)) >> 1);
+            maps[(size_t)lv * n + tid] = brev(idx, log_n);
+        }
+    }
+}
+
+/* ------------------------------------------------------------------------------------------ */
+/* gadget decomposition and modulus switching                                                  */
+/* ------------------------------------------------------------------------------------------ */
+
+/* kernel.cu:37-68 (and the identical device_SignedDigitDecompose, kernel.cu:768-798) */
+void orc_signed_decompose(uint64_t x, uint64_t Q, uint32_t base, uint32_t digits, uint64_t *out) {
+    const int gbits = __builtin_ctz(base);
+    const int logq = 64 - __builtin_clzll(Q);
+    int ign = logq - (int)digits * gbits;
+    if (ign < 0) ign = 0;
+    const uint64_t qhalf = Q >> 1;
+    const int64_t qi = (int64_t)Q;
+    int64_t d = x < qhalf ? (int64_t)x : (int64_t)x - qi;
+    int64_t r;
+    if (ign != 0) {
+        r = (int64_t)((uint64_t)d << (64 - ign)) >> (64 - ign);
+        d = (d - r) >> ign;
+    }
+    for (uint32_t i = 0; i < digits; ++i) {
+        r = (int64_t)((uint64_t)d << (64 - gbits)) >> (64 - gbits);
+        d = (d - r) >> gbits;
+        if (r < 0) r += qi;
+        out[i] = (uint64_t)r;
+    }
+}
+
+/* kernel.cu:7316-7326 */
+uint32_t orc_special_ms(uint64_t v, uint32_t two_n, uint64_t q, uint32_t bitwidth) {
+    const uint64_t shift = bitwidth < 63u ? (1ull << bitwidth) : 0ull;
+    if (shift == 0 || two_n == 0 || q == 0) return 0;
+    const double scale = (double)two_n / ((double)q * (double)shift);
+    const double x = (double)v * scale;
+    const uint64_t r = (uint64_t)floor(x + 0.5);
+    return (uint32_t)((r * shift) & ((uint64_t)two_n - 1));
+}
+
+/* ------------------------------------------------------------------------------------------ */
+/* circuit bootstrapping                                                                       */
+/* ------------------------------------------------------------------------------------------ */
+
+/* NTT of the monic polynomial X^e - 1 (e in [0, 2N)), OpenFHE convention (cirbts-init.cu:991-1023) */
+static void monic_ntt(uint64_t *out, uint32_t e, uint32_t N, uint64_t Q, const uint64_t *rp) {
+    memset(out, 0, sizeof(uint64_t) * N);
+    if (e < N) out[e] = addmod(out[e], 1, Q);
+    else out[e - N] = submod(out[e - N], 1, Q);
+    out[0] = submod(out[0], 1, Q);
+    ntt_fwd_one(out, N, Q, rp);
+}
+
+/* X^{-e} * p in the coefficient domain (negacyclic rotation), e in [0, 2N) */
+static void rotate_neg(uint64_t *out, const uint64_t *p, uint32_t e, uint32_t N, uint64_t Q) {
+    for (uint32_t i = 0; i < N; ++i) {
+        /* out[i] = coefficient of X^i in X^{-e} p = p[i+e] with sign */
+        uint32_t s = (i + e) % (2 * N);
+        uint64_t v = s < N ? p[s] : p[s - N];
+        out[i] = (s < N) ? v : (v ? Q - v : 0);
+    }
+}
+
+static void blind_rotate_one(const orc_cbs_params *p, const orc_cbs_keys *k, const uint64_t *a, uint64_t b,
+                             uint64_t *acc, int finalize, uint64_t *work) {
+    const uint32_t N = p->N, l2 = 2 * p->digits_g;
+    const uint64_t Q = p->Q;
+    const uint32_t twoN = 2 * N;
+    const uint32_t bw = (p->num_lut <= 1) ? 0 : (uint32_t)(32 - __builtin_clz(p->num_lut - 1));
+    uint64_t *ct = work;              /* [2][N] */
+    uint64_t *dct = ct + 2 * N;       /* [l2][N] */
+    uint64_t *mono = dct + (size_t)l2 * N;
+    uint64_t dig[64];
+
+    /* acc = (0, LUT * X^{-b~}) : kernel.cu:7328-7358 */
+    const uint32_t bt = orc_special_ms(b, twoN, p->q_lwe, bw);
+    memset(acc, 0, sizeof(uint64_t) * N);
+    rotate_neg(acc + N, k->tv, bt, N, Q);
+    ntt_fwd_one(acc + N, N, Q, k->rp);
+
+    for (uint32_t i = 0; i < p->n; ++i) {
+        /* INTT(acc) -> signed digits -> NTT (kernel.cu:473-559) */
+        memcpy(ct, acc, sizeof(uint64_t) * 2 * N);
+        ntt_inv_one(ct, N, Q, k->irp, k->n_inv);
+        ntt_inv_one(ct + N, N, Q, k->irp, k->n_inv);
+        for (uint32_t poly = 0; poly < 2; ++poly) {
+            for (uint32_t c = 0; c < N; ++c) {
+                orc_signed_decompose(ct[poly * N + c], Q, p->base_g, p->digits_g, dig);
+                for (uint32_t j = 0; j < p->digits_g; ++j) dct[(size_t)(2 * j + poly) * N + c] = dig[j];
+            }
+        }
+        for (uint32_t d = 0; d < l2; ++d) ntt_fwd_one(dct + (size_t)d * N, N, Q, k->rp);
+        /* MAC against BSK_i, times (X^{a~_i} - 1), accumulate (kernel.cu:3008-3055) */
+        const uint32_t at = orc_special_ms(a[i], twoN, p->q_lwe, bw);
+        monic_ntt(mono, at, N, Q, k->rp);
+        const uint64_t *ek = k->bsk + (size_t)i * l2 * 2 * N;
+        for (uint32_t c = 0; c < N; ++c) {
+            uint64_t t0 = 0, t1 = 0;
+            for (uint32_t d = 0; d < l2; ++d) {
+                const uint64_t x = dct[(size_t)d * N + c];
+                t0 = addmod(t0, orc_mulmod(x, ek[(size_t)d * 2 * N + c], Q), Q);
+                t1 = addmod(t1, orc_mulmod(x, ek[(size_t)d * 2 * N + N + c], Q), Q);
+            }
+            acc[c] = addmod(acc[c], orc_mulmod(t0, mono[c], Q), Q);
+            acc[N + c] = addmod(acc[N + c], orc_mulmod(t1, mono[c], Q), Q);
+        }
+    }
+
+    if (finalize) {
+        /* cirbts-batch.cu:2622-2642: x N^-1, INTT, c1[i] += (gpow[i]>>1) N^-1, NTT */
+        const uint64_t ninv = orc_invmod(N, Q);
+        for (uint32_t c = 0; c < 2 * N; ++c) acc[c] = orc_mulmod(acc[c], ninv, Q);
+        ntt_inv_one(acc, N, Q, k->irp, k->n_inv);
+        ntt_inv_one(acc + N, N, Q, k->irp, k->n_inv);
+        for (uint32_t j = 0; j < p->num_lut; ++j)
+            acc[N + j] = addmod(acc[N + j], orc_mulmod(k->gpow[j] >> 1, ninv, Q), Q);
+        ntt_fwd_one(acc, N, Q, k->rp);
+        ntt_fwd_one(acc + N, N, Q, k->rp);
+    }
+}
+
+void orc_blind_rotate(const orc_cbs_params *p, const orc_cbs_keys *k, const uint64_t *a, const uint64_t *b,
+                      uint32_t batch, uint32_t a_stride, uint64_t *acc_out, int finalize) {
+    const size_t wsz = (size_t)(2 + 2 * p->digits_g + 1) * p->N;
+#pragma omp parallel
+    {
+        uint64_t *work = (uint64_t *)malloc(wsz * sizeof(uint64_t));
+#pragma omp for schedule(dynamic, 1)
+        for (long bi = 0; bi < (long)batch; ++bi)
+            blind_rotate_one(p, k, a + (size_t)bi * a_stride, b[bi], acc_out + (size_t)bi * 2 * p->N, finalize, work);
+        free(work);
+    }
+}
+
+/* one HomTrace + SchemeSwitch pipeline for a single MV RLWE (cirbts-batch.cu:1656-1789,
+ * kernel.cu:7832-7888 HT update, kernel.cu:8407-8446 SS update, kernel.cu:7776-7789 layout) */
+static void trace_ss_one(const orc_cbs_params *p, const orc_cbs_keys *k, const uint64_t *ct_in, uint64_t *rgsw,
+                         uint64_t *work) {
+    const uint32_t N = p->N;
+    const uint64_t Q = p->Q;
+    uint64_t *c0 = work, *c1 = c0 + N, *perm = c1 + N, *pc1 = perm + N;
+    const uint32_t maxd = p->digits_ht > p->digits_ss ? p->digits_ht : p->digits_ss;
+    uint64_t *dg = pc1 + N; /* [maxd][N] */
+    uint64_t dig[64];
+    memcpy(c0, ct_in, sizeof(uint64_t) * N);
+    memcpy(c1, ct_in + N, sizeof(uint64_t) * N);
+
+    for (uint32_t r = 0; r < p->trace_rounds; ++r) {
+        const uint32_t *map = k->auto_maps + (size_t)r * N;
+        /* sigma(c0) in the coefficient domain */
+        for (uint32_t i = 0; i < N; ++i) perm[i] = c0[map[i]];
+        ntt_inv_one(perm, N, Q, k->irp, k->n_inv);
+        for (uint32_t c = 0; c < N; ++c) {
+            orc_signed_decompose(perm[c], Q, p->base_ht, p->digits_ht, dig);
+            for (uint32_t j = 0; j < p->digits_ht; ++j) dg[(size_t)j * N + c] = dig[j];
+        }
+        for (uint32_t j = 0; j < p->digits_ht; ++j) ntt_fwd_one(dg + (size_t)j * N, N, Q, k->rp);
+        const uint64_t *key = k->ht_key + (size_t)r * p->digits_ht * 2 * N;
+        for (uint32_t i = 0; i < N; ++i) pc1[i] = c1[map[i]];
+        for (uint32_t c = 0; c < N; ++c) {
+            uint64_t s0 = 0, s1 = 0;
+            for (uint32_t j = 0; j < p->digits_ht; ++j) {
+                const uint64_t x = dg[(size_t)j * N + c];
+                s0 = addmod(s0, orc_mulmod(x, key[(size_t)j * 2 * N + c], Q), Q);
+                s1 = addmod(s1, orc_mulmod(x, key[(size_t)j * 2 * N + N + c], Q), Q);
+            }
+            c0[c] = addmod(c0[c], s0, Q);
+            c1[c] = addmod(addmod(c1[c], s1, Q), pc1[c], Q);
+        }
+    }
+    /* trace result -> RGSW row 2j+1 */
+    memcpy(rgsw + 2 * N, c0, sizeof(uint64_t) * N);
+    memcpy(rgsw + 3 * N, c1, sizeof(uint64_t) * N);
+
+    /* SchemeSwitch: digits(INTT(c0)) x SSkey; row 2j = (c1 + ks0, ks1) */
+    memcpy(perm, c0, sizeof(uint64_t) * N);
+    ntt_inv_one(perm, N, Q, k->irp, k->n_inv);
+    for (uint32_t c = 0; c < N; ++c) {
+        orc_signed_decompose(perm[c], Q, p->base_ss, p->digits_ss, dig);
+        for (uint32_t j = 0; j < p->digits_ss; ++j) dg[(size_t)j * N + c] = dig[j];
+    }
+    for (uint32_t j = 0; j < p->digits_ss; ++j) ntt_fwd_one(dg + (size_t)j * N, N, Q, k->rp);
+    for (uint32_t c = 0; c < N; ++c) {
+        uint64_t s0 = 0, s1 = 0;
+        for (uint32_t j = 0; j < p->digits_ss; ++j) {
+            const uint64_t x = dg[(size_t)j * N + c];
+            s0 = addmod(s0, orc_mulmod(x, k->ss_key[(size_t)j * 2 * N + c], Q), Q);
+            s1 = addmod(s1, orc_mulmod(x, k->ss_key[(size_t)j * 2 * N + N + c], Q), Q);
+        }
+        rgsw[c] = addmod(c1[c], s0, Q);
+        rgsw[N + c] = s1;
+    }
+    (void)maxd;
+}
+
+static size_t trace_work_words(const orc_cbs_params *p) {
+    const uint32_t maxd = p->digits_ht > p->digits_ss ? p->digits_ht : p->digits_ss;
+    return (size_t)(4 + maxd) * p->N;
+}
+
+void orc_trace_schemeswitch(const orc_cbs_params *p, const orc_cbs_keys *k, const uint64_t *ct, uint32_t count,
+                            uint64_t *rgsw_out) {
+    const size_t wsz = trace_work_words(p);
+#pragma omp parallel
+    {
+        uint64_t *work = (uint64_t *)malloc(wsz * sizeof(uint64_t));
+#pragma omp for schedule(dynamic, 1)
+        for (long i = 0; i < (long)count; ++i)
+            trace_ss_one(p, k, ct + (size_t)i * 2 * p->N, rgsw_out + (size_t)i * 4 * p->N, work);
+        free(work);
+    }
+}
+
+void orc_circuit_bootstrap(const orc_cbs_params *p, const orc_cbs_keys *k, const uint64_t *a, const uint64_t *b,
+                           uint32_t batch, uint32_t a_stride, uint64_t *rgsw_out) {
+    const uint32_t N = p->N, L = p->num_lut;
+    const uint64_t Q = p->Q;
+    uint64_t *acc = (uint64_t *)malloc(sizeof(uint64_t) * 2 * N * batch);
+    orc_blind_rotate(p, k, a, b, batch, a_stride, acc, 1);
+    /* kernel.cu:7498-7536: ct_j = acc * X^{-j} (NTT domain) */
+    uint64_t *mv = (uint64_t *)malloc(sizeof(uint64_t) * 2 * N * (size_t)batch * L);
+    uint64_t *mono = (uint64_t *)malloc(sizeof(uint64_t) * N * (L > 1 ? L : 1));
+    for (uint32_t j = 0; j < L; ++j) {
+        uint64_t *m = mono + (size_t)j * N;
+        memset(m, 0, sizeof(uint64_t) * N);
+        if (j == 0) m[0] = 1;
+        else m[N - j] = Q - 1; /* X^{-j} = -X^{N-j} */
+        ntt_fwd_one(m, N, Q, k->rp);
+    }
+    for (uint32_t bi = 0; bi < batch; ++bi)
+        for (uint32_t j = 0; j < L; ++j)
+            for (uint32_t poly = 0; poly < 2; ++poly)
+                for (uint32_t c = 0; c < N; ++c)
+                    mv[(((size_t)bi * L + j) * 2 + poly) * N + c] =
+                        orc_mulmod(acc[((size_t)bi * 2 + poly) * N + c], mono[(size_t)j * N + c], Q);
+    orc_trace_schemeswitch(p, k, mv, batch * L, rgsw_out);
+    free(mono);
+    free(mv);
+    free(acc);
+}
+
+/* ------------------------------------------------------------------------------------------ */
+/* CMux LUT                                                                                    */
+/* ------------------------------------------------------------------------------------------ */
+
+void orc_external_product(const uint64_t *ct_in, const uint64_t *rgsw, uint64_t *out, uint32_t N, uint64_t Q,
+                          const uint64_t *rp, const uint64_t *irp, uint64_t n_inv, uint32_t base, uint32_t digits) {
+    uint64_t *ct = (uint64_t *)malloc(sizeof(uint64_t) * 2 * N);
+    uint64_t *dct = (uint64_t *)malloc(sizeof(uint64_t) * 2 * digits * N);
+    uint64_t dig[64];
+    memcpy(ct, ct_in, sizeof(uint64_t) * 2 * N);
+    ntt_inv_one(ct, N, Q, irp, n_inv);
+    ntt_inv_one(ct + N, N, Q, irp, n_inv);
+    for (uint32_t poly = 0; poly < 2; ++poly)
+        for (uint32_t c = 0; c < N; ++c) {
+            orc_signed_decompose(ct[poly * N + c], Q, base, digits, dig);
+            for (uint32_t j = 0; j < digits; ++j) dct[(size_t)(2 * j + poly) * N + c] = dig[j];
+        }
+    for (uint32_t d = 0; d < 2 * digits; ++d) ntt_fwd_one(dct + (size_t)d * N, N, Q, rp);
+    for (uint32_t c = 0; c < N; ++c) {
+        uint64_t s0 = 0, s1 = 0;
+        for (uint32_t r = 0; r < 2 * digits; ++r) {
+            const uint64_t x = dct[(size_t)r * N + c];
+            s0 = addmod(s0, orc_mulmod(x, rgsw[((size_t)r * 2 + 0) * N + c], Q), Q);
+            s1 = addmod(s1, orc_mulmod(x, rgsw[((size_t)r * 2 + 1) * N + c], Q), Q);
+        }
+        out[c] = s0;
+        out[N + c] = s1;
+    }
+    free(dct);
+    free(ct);
+}
+
+void orc_lut8x32(const uint64_t *table, const uint64_t *const *ctrl, uint64_t *out, uint32_t N, uint64_t Q,
+                 const uint64_t *rp, const uint64_t *irp, uint64_t n_inv, uint32_t base, uint32_t digits) {
+    const size_t ctsz = 2 * (size_t)N;
+    uint64_t *cur = (uint64_t *)malloc(sizeof(uint64_t) * 256 * ctsz);
+    uint64_t *delta = (uint64_t *)malloc(sizeof(uint64_t) * ctsz);
+    uint64_t *prod = (uint64_t *)malloc(sizeof(uint64_t) * ctsz);
+    memcpy(cur, table, sizeof(uint64_t) * 256 * ctsz);
+    uint32_t count = 256;
+    for (uint32_t bit = 0; bit < 8; ++bit) {
+        for (uint32_t i = 0; i < count / 2; ++i) {
+            const uint64_t *c0 = cur + (size_t)(2 * i) * ctsz, *c1 = c0 + ctsz;
+            for (size_t c = 0; c < ctsz; ++c) delta[c] = submod(c1[c], c0[c], Q);
+            orc_external_product(delta, ctrl[bit], prod, N, Q, rp, irp, n_inv, base, digits);
+            uint64_t *dst = cur + (size_t)i * ctsz;
+            for (size_t c = 0; c < ctsz; ++c) dst[c] = addmod(c0[c], prod[c], Q);
+        }
+        count /= 2;
+    }
+    memcpy(out, cur, sizeof(uint64_t) * ctsz);
+    free(prod);
+    free(delta);
+    free(cur);
+}
+
+/* ------------------------------------------------------------------------------------------ */
+/* sample extract + key switch                                                                 */
+/* ------------------------------------------------------------------------------------------ */
+
+/* aes_gpu_ks.cuh:388-394 modswitch_u64_to_pow2_u16 */
+static inline uint32_t ms_pow2(uint64_t v, double q_over_Q, uint32_t mask) {
+    const double x = (double)v * q_over_Q;
+    return ((uint32_t)nearbyint(x)) & mask;
+}
+
+void orc_extract_keyswitch(const uint64_t *words_coef, const uint32_t *info, uint32_t T, uint32_t N, uint64_t Q,
+                           const uint16_t *ksk, uint32_t n, uint32_t base_ks_log2, uint32_t qks, uint64_t q_lwe,
+                           uint64_t *out_a, uint64_t *out_b, uint32_t out_stride) {
+    const double q_over_Q = (double)qks / (double)Q;
+    const uint32_t mask = qks - 1, bmask = (1u << base_ks_log2) - 1;
+    const uint32_t outlen = n + 1, base = 1u << base_ks_log2;
+    const size_t stride_i = (size_t)base * outlen, stride_j = (size_t)N * stride_i;
+    const int divisible = (q_lwe % qks) == 0;
+    const uint64_t scale = divisible ? q_lwe / qks : 0;
+#pragma omp parallel for schedule(dynamic, 4)
+    for (long t = 0; t < (long)T; ++t) {
+        const uint32_t word = info[t] >> 16, idx = info[t] & 0xFFFFu;
+        const uint64_t *a = words_coef + (size_t)word * 2 * N, *bw = a + N;
+        uint32_t *acc = (uint32_t *)calloc(outlen, sizeof(uint32_t));
+        acc[n] = ms_pow2(bw[idx], q_over_Q, mask);
+        for (uint32_t j = 0; j < N; ++j) {
+            uint64_t v;
+            if (j <= idx) v = a[idx - j];
+            else { const uint64_t ak = a[N + idx - j]; v = ak ? Q - ak : 0; }
+            const uint32_t ai = ms_pow2(v, q_over_Q, mask);
+            const uint32_t d0 = ai & bmask, d1 = (ai >> base_ks_log2) & bmask;
+            const uint16_t *k0 = ksk + (size_t)j * stride_i + (size_t)d0 * outlen;
+            const uint16_t *k1 = ksk + stride_j + (size_t)j * stride_i + (size_t)d1 * outlen;
+            for (uint32_t k = 0; k < outlen; ++k) acc[k] -= (uint32_t)k0[k] + (uint32_t)k1[k];
+        }
+        for (uint32_t k = 0; k < outlen; ++k) {
+            const uint64_t v = acc[k] & mask;
+            /* aes_gpu_ks.cuh:431-440 ks_u16_to_lwe (round-half-up division for non-divisible q) */
+            const uint64_t val = divisible ? v * scale : (uint64_t)(((u128)v * q_lwe + (qks >> 1)) / qks);
+            if (k == n) out_b[t] = val;
+            else out_a[(size_t)t * out_stride + k] = val;
+        }
+        free(acc);
+    }
+}
+
+/* ------------------------------------------------------------------------------------------ */
+/* plaintext AES-128 (FIPS-197), restating examples/aes_transcipher/aes128.cuh                 */
+/* ------------------------------------------------------------------------------------------ */
+
+static uint8_t gmul(uint8_t a, uint8_t b) {
+    uint8_t p = 0;
+    while (b) {
+        if (b & 1) p ^= a;
+        a = (uint8_t)((a << 1) ^ ((a & 0x80) ? 0x1b : 0));
+        b >>= 1;
+    }
+    return p;
+}
+
+/* S-box from its definition: multiplicative inverse in GF(2^8) followed by the affine map */
+static void build_sbox(uint8_t sbox[256]) {
+    for (int x = 0; x < 256; ++x) {
+        uint8_t inv = 0;
+        if (x) {
+            for (int y = 1; y < 256; ++y)
+                if (gmul((uint8_t)x, (uint8_t)y) == 1) { inv = (uint8_t)y; break; }
+        }
+        uint8_t s = inv;
+        for (int i = 1; i <= 4; ++i) s ^= (uint8_t)((inv << i) | (inv >> (8 - i)));
+        sbox[x] = (uint8_t)(s ^ 0x63);
+    }
+}
+
+static const uint8_t *get_sbox(void) {
+    static uint8_t sbox[256];
+    static int ready = 0;
+    if (!ready) {
+#pragma omp critical(orc_sbox)
+        {
+            if (!ready) { build_sbox(sbox); ready = 1; }
+        }
+    }
+    return sbox;
+}
+
+/* aes128.cuh:99-121 Aes128KeyExpand; round_keys[r][i] in column-major state order */
+void orc_aes128_key_expand(const uint8_t key[16], uint8_t rk[11][16]) {
+    const uint8_t *sbox = get_sbox();
+    uint8_t w[44][4];
+    static const uint8_t rcon[10] = {0x01, 0x02, 0x04, 0x08, 0x10, 0x20, 0x40, 0x80, 0x1b, 0x36};
+    for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) w[i][j] = key[4 * i + j];
+    for (int i = 4; i < 44; ++i) {
+        uint8_t t[4] = {w[i - 1][0], w[i - 1][1], w[i - 1][2], w[i - 1][3]};
+        if (i % 4 == 0) {
+            const uint8_t t0 = t[0];
+            t[0] = (uint8_t)(sbox[t[1]] ^ rcon[i / 4 - 1]);
+            t[1] = sbox[t[2]];
+            t[2] = sbox[t[3]];
+            t[3] = sbox[t0];
+        }
+        for (int j = 0; j < 4; ++j) w[i][j] = (uint8_t)(w[i - 4][j] ^ t[j]);
+    }
+    for (int r = 0; r < 11; ++r)
+        for (int c = 0; c < 4; ++c)
+            for (int row = 0; row < 4; ++row) rk[r][c * 4 + row] = w[r * 4 + c][row];
+}
+
+/* aes128.cuh:151-165 Aes128EncryptPlain */
+void orc_aes128_encrypt(const uint8_t key[16], const uint8_t in[16], uint8_t out[16]) {
+    const uint8_t *sbox = get_sbox();
+    uint8_t rk[11][16], s[16], t[16];
+    orc_aes128_key_expand(key, rk);
+    for (int i = 0; i < 16; ++i) s[i] = in[i] ^ rk[0][i];
+    for (int r = 1; r <= 10; ++r) {
+        for (int i = 0; i < 16; ++i) s[i] = sbox[s[i]];
+        for (int row = 0; row < 4; ++row)
+            for (int c = 0; c < 4; ++c) t[c * 4 + row] = s[((c + row) & 3) * 4 + row];
+        memcpy(s, t, 16);
+        if (r != 10) {
+            for (int c = 0; c < 4; ++c) {
+                const uint8_t a0 = s[c * 4], a1 = s[c * 4 + 1], a2 = s[c * 4 + 2], a3 = s[c * 4 + 3];
+                s[c * 4 + 0] = (uint8_t)(gmul(a0, 2) ^ gmul(a1, 3) ^ a2 ^ a3);
+                s[c * 4 + 1] = (uint8_t)(a0 ^ gmul(a1, 2) ^ gmul(a2, 3) ^ a3);
+                s[c * 4 + 2] = (uint8_t)(a0 ^ a1 ^ gmul(a2, 2) ^ gmul(a3, 3));
+                s[c * 4 + 3] = (uint8_t)(gmul(a0, 3) ^ a1 ^ a2 ^ gmul(a3, 2));
+            }
+        }
+        for (int i = 0; i < 16; ++i) s[i] ^= rk[r][i];
+    }
+    memcpy(out, s, 16);
+}
+
+static uint32_t pack_be(uint8_t b0, uint8_t b1, uint8_t b2, uint8_t b3) {
+    return ((uint32_t)b0 << 24) | ((uint32_t)b1 << 16) | ((uint32_t)b2 << 8) | b3;
+}
+static uint32_t rotr(uint32_t x, int r) { return (x >> r) | (x << (32 - r)); }
+
+/* aes128.cuh:316-330 BuildAesEncTables */
+void orc_aes_enc_tables(uint32_t te[8][256]) {
+    const uint8_t *sbox = get_sbox();
+    for (int x = 0; x < 256; ++x) {
+        const uint8_t s = sbox[x];
+        const uint32_t t0 = pack_be(gmul(s, 2), s, s, gmul(s, 3));
+        te[0][x] = t0;
+        te[1][x] = rotr(t0, 8);
+        te[2][x] = rotr(t0, 16);
+        te[3][x] = rotr(t0, 24);
+        te[4][x] = pack_be(s, 0, 0, 0);
+        te[5][x] = pack_be(0, s, 0, 0);
+        te[6][x] = pack_be(0, 0, s, 0);
+        te[7][x] = pack_be(0, 0, 0, s);
+    }
+}

@@ -1,0 +1,130 @@
+/*
+ * oracle.h -- CPU restatement of the reference's bootstrapping hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This library is the checker for the CUDA path: only
+ * tests/, __graft_entry__.smoke() and bench.py's cpu_baseline / --impl reference
+ * legs may load it.  The product library never links or calls it.
+ *
+ * Every function cites the reference file:line whose behaviour it restates
+ * (paths relative to the reference project root).  All modular arithmetic is
+ * exact (unsigned __int128); results are fully reduced to [0, q).
+ *
+ * Pinning: the Phantom NTT tables, get_primes and the plaintext AES are checked
+ * against the reference's own host code compiled from its sources (oracle/_ref,
+ * recipe in oracle/Makefile) and against committed golden fixtures generated from
+ * it (tests/golden/make_golden.py), plus the FIPS-197 AES-128 known answer.
+ * The CBS / CMux / extract restatements follow the cited kernels; the keys and
+ * parameter sets they consume come from the OpenFHE fork, which is absent, so
+ * those stages are "parity unpinned" against the reference and are pinned only
+ * end to end (decrypted AES output == plaintext AES-128).
+ */
+#ifndef CBS_ORACLE_H
+#define CBS_ORACLE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------- scalar modular arithmetic (include/uintmodmath.cuh) ---------------- */
+uint64_t orc_mulmod(uint64_t a, uint64_t b, uint64_t q);
+uint64_t orc_powmod(uint64_t a, uint64_t e, uint64_t q);
+uint64_t orc_invmod(uint64_t a, uint64_t q);
+uint64_t orc_shoup(uint64_t w, uint64_t q);
+int orc_is_prime(uint64_t n);
+/* src/host/numth.cu:207-233 get_primes(ntt_size, bit_size, count) */
+int orc_get_primes(uint32_t ntt_size, int bit_size, uint32_t count, uint64_t *out);
+/* src/host/numth.cu:309-331 try_minimal_primitive_root */
+uint64_t orc_minimal_primitive_root(uint64_t degree, uint64_t q);
+
+/* ---------------- Phantom single-modulus NTT (src/host/ntt.cu:11-56, src/ntt/ntt_1d.cu) ---------------- */
+/* rp/rp_sh/irp/irp_sh: N entries each; n_inv[0]=N^-1 mod q, n_inv[1]=its Shoup quotient */
+int orc_ntt_tables(uint32_t log_n, uint64_t q, uint64_t *rp, uint64_t *rp_sh, uint64_t *irp, uint64_t *irp_sh,
+                   uint64_t *n_inv);
+/* ntt_1d.cu:488 inplace_fnwt_radix2_opt_batched: bit-reversed output, fully reduced */
+void orc_ntt_forward(uint64_t *a, size_t batch, uint32_t n, uint64_t q, const uint64_t *rp);
+/* ntt_1d.cu:557 inplace_inwt_radix2_batched (n^-1 fused) */
+void orc_ntt_inverse(uint64_t *a, size_t batch, uint32_t n, uint64_t q, const uint64_t *irp, uint64_t n_inv);
+/* ntt_1d.cu:677 inplace_inwt_radix2_permute_batched: in[map[i]] (negated when map>=n), then INTT */
+void orc_ntt_inverse_permute(uint64_t *out, const uint64_t *in, const uint32_t *map, size_t batch, uint32_t n,
+                             uint64_t q, const uint64_t *irp, uint64_t n_inv);
+/* schoolbook negacyclic product c = a*b mod (X^n+1, q) (for checking the transform) */
+void orc_negacyclic_mul(const uint64_t *a, const uint64_t *b, uint64_t *c, uint32_t n, uint64_t q);
+/* bitwise/src/cirbts/kernel.cu:7554-7571 kernel_GenerateCoefficientAutoMaps (NTT-domain automorphism maps) */
+void orc_auto_maps(uint32_t *maps, uint32_t n, uint32_t levels);
+
+/* ---------------- gadget decomposition / mod switch ---------------- */
+/* bitwise/src/cirbts/kernel.cu:37-68 device_SignedDigitDecompose2: digits in [0,Q) (negatives as Q-|r|) */
+void orc_signed_decompose(uint64_t x, uint64_t Q, uint32_t base, uint32_t digits, uint64_t *out);
+/* bitwise/src/cirbts/kernel.cu:7316-7326 device_SpecialMS_IndexPos */
+uint32_t orc_special_ms(uint64_t v, uint32_t two_n, uint64_t q, uint32_t bitwidth);
+
+/* ---------------- circuit bootstrapping (bitwise/src/cirbts) ---------------- */
+typedef struct {
+    uint32_t N;          /* ring dimension */
+    uint32_t log_n;
+    uint64_t Q;          /* RLWE modulus (NTT prime) */
+    uint32_t n;          /* LWE dimension */
+    uint64_t q_lwe;      /* LWE modulus of the CBS input */
+    uint32_t base_g;     /* blind-rotation gadget base (power of two) */
+    uint32_t digits_g;   /* blind-rotation gadget digits */
+    uint32_t num_lut;    /* = digitsCC, RGSW levels produced */
+    uint32_t base_cc;    /* CMux / RGSW output gadget base */
+    uint32_t base_ht, digits_ht;
+    uint32_t base_ss, digits_ss;
+    uint32_t trace_rounds;
+} orc_cbs_params;
+
+typedef struct {
+    const uint64_t *rp, *irp;   /* Phantom tables for (N, Q) */
+    uint64_t n_inv;
+    const uint32_t *auto_maps;  /* [log_n][N] */
+    const uint64_t *tv;         /* blind-rotation test vector, coefficient domain [N] */
+    const uint64_t *gpow;       /* [num_lut] RGSW gadget powers */
+    const uint64_t *bsk;        /* [n][2*digits_g][2][N] NTT domain */
+    const uint64_t *ht_key;     /* [trace_rounds][digits_ht][2][N] NTT domain */
+    const uint64_t *ss_key;     /* [digits_ss][2][N] NTT domain */
+} orc_cbs_keys;
+
+/* cirbts-batch.cu:3293-4629 (binary GINX EvalAcc) + finalize :2622-2642.
+ * acc_out [batch][2][N] NTT domain. */
+void orc_blind_rotate(const orc_cbs_params *p, const orc_cbs_keys *k, const uint64_t *a, const uint64_t *b,
+                      uint32_t batch, uint32_t a_stride, uint64_t *acc_out, int finalize);
+/* cirbts-batch.cu:1416-1879 full CBS: BR -> MV split -> HomTrace -> SchemeSwitch.
+ * rgsw_out [batch][num_lut][2][2][N] NTT domain, row (2j+0)=scheme-switch row, (2j+1)=trace row. */
+void orc_circuit_bootstrap(const orc_cbs_params *p, const orc_cbs_keys *k, const uint64_t *a, const uint64_t *b,
+                           uint32_t batch, uint32_t a_stride, uint64_t *rgsw_out);
+/* HomTrace + SchemeSwitch alone on MV RLWEs ct [count][2][N] NTT domain -> rgsw [count][2][2][N] */
+void orc_trace_schemeswitch(const orc_cbs_params *p, const orc_cbs_keys *k, const uint64_t *ct, uint32_t count,
+                            uint64_t *rgsw_out);
+
+/* ---------------- CMux LUT (examples/aes_transcipher/rlwe_tables.cuh:52-108, gpu_lut.cuh:521-595) ---------------- */
+/* out = ct_in (x) rgsw, both NTT domain; rgsw [digits][2][2][N] */
+void orc_external_product(const uint64_t *ct_in, const uint64_t *rgsw, uint64_t *out, uint32_t N, uint64_t Q,
+                          const uint64_t *rp, const uint64_t *irp, uint64_t n_inv, uint32_t base, uint32_t digits);
+/* table [256][2][N], ctrl[8] -> pointers to RGSW [digits][2][2][N] (bit 0 = LSB); out [2][N] */
+void orc_lut8x32(const uint64_t *table, const uint64_t *const *ctrl, uint64_t *out, uint32_t N, uint64_t Q,
+                 const uint64_t *rp, const uint64_t *irp, uint64_t n_inv, uint32_t base, uint32_t digits);
+
+/* ---------------- sample extract + LWE key switch (examples/aes_gpu_ks.cuh:341-607) ---------------- */
+/* words [W][2][N] coefficient domain (c0=a, c1=b); info[t] = (word<<16)|coeff; ksk [2][N][base][n+1] u16;
+ * out_a [T][out_stride], out_b [T] mod q_lwe */
+void orc_extract_keyswitch(const uint64_t *words_coef, const uint32_t *info, uint32_t T, uint32_t N, uint64_t Q,
+                           const uint16_t *ksk, uint32_t n, uint32_t base_ks_log2, uint32_t qks, uint64_t q_lwe,
+                           uint64_t *out_a, uint64_t *out_b, uint32_t out_stride);
+
+/* ---------------- plaintext AES-128 (examples/aes_transcipher/aes128.cuh) ---------------- */
+void orc_aes128_key_expand(const uint8_t key[16], uint8_t round_keys[11][16]);
+void orc_aes128_encrypt(const uint8_t key[16], const uint8_t in[16], uint8_t out[16]);
+/* te[8][256]: Te0..Te3 then Te4_0..Te4_3 (aes128.cuh:316-330) */
+void orc_aes_enc_tables(uint32_t te[8][256]);
+
+/* OpenMP thread count used by the batched routines */
+int orc_num_threads(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

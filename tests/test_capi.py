@@ -1,0 +1,66 @@
+"""C-ABI checks that need no GPU: the library loads, exports every declared symbol,
+validates arguments before touching the device, and its host helpers agree with the
+pinned oracle."""
+from __future__ import annotations
+
+import ctypes
+import json
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, oracle_tables
+
+REF = json.loads((GOLDEN / "reference_host.json").read_text())
+
+
+def test_library_exports_every_declared_symbol(pkg, lib):
+    names = pkg.declared_symbols()
+    assert len(names) >= 8
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_abi_version(lib):
+    assert lib.cbs_abi_version() >= 1
+
+
+@pytest.mark.parametrize("case", REF["ntt_tables"], ids=lambda c: f"{c['n']}")
+def test_host_tables_match_oracle(lib, oracle, case):
+    n, q = case["n"], case["q"]
+    mine = [np.zeros(n, np.uint64) for _ in range(4)]
+    ninv = np.zeros(2, np.uint64)
+
+    class DMod(ctypes.Structure):
+        _fields_ = [("value", ctypes.c_uint64), ("const_ratio", ctypes.c_uint64 * 2)]
+
+    dm = DMod()
+    st = lib.cbs_ntt_tables_host(n, q, *(a.ctypes.data for a in mine), ninv.ctypes.data, ctypes.addressof(dm))
+    assert st == 0
+    want = oracle_tables(oracle, n, q)
+    for a, b in zip(mine + [ninv], want):
+        assert (a == b).all()
+    assert dm.value == q
+    assert [dm.const_ratio[0], dm.const_ratio[1]] == case["const_ratio"]
+
+
+@pytest.mark.parametrize("case", REF["primes"], ids=lambda c: f"{c['ntt_size']}-{c['bits']}")
+def test_host_primes_match_reference(lib, case):
+    out = np.zeros(case["count"], np.uint64)
+    assert lib.cbs_get_primes(case["ntt_size"], case["bits"], case["count"], out.ctypes.data) == 0
+    assert [int(x) for x in out] == case["values"]
+
+
+def test_argument_validation_without_device(lib):
+    # invalid dim and null pointers are rejected before any CUDA call
+    assert lib.cbs_fnwt_1d_opt_batched(None, None, None, None, 3000, 4, None) == 1
+    assert b"dim" in lib.cbs_last_error()
+    assert lib.cbs_fnwt_1d_opt_batched(None, None, None, None, 2048, 4, None) == 1
+    assert b"null" in lib.cbs_last_error()
+    assert lib.cbs_inwt_1d_opt_batched(None, None, None, None, None, None, 2048, 0, None) == 0  # empty batch
+    buf = (ctypes.c_uint64 * 4)()
+    p = ctypes.addressof(buf)
+    assert lib.cbs_inwt_1d_opt_permute_batched(p, p, p, p, p, p, p, p, 2048, 1, None) == 1
+    assert b"in-place" in lib.cbs_last_error()
+    # not enough NTT-friendly primes of 13 bits for N=2048
+    assert lib.cbs_get_primes(2048, 13, 5, np.zeros(5, np.uint64).ctypes.data) == 1
