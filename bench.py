@@ -1,0 +1,362 @@
+"""Benchmark: homomorphic AES-128 CTR transciphering throughput (blocks/s) on B200.
+
+Workload (the BASELINE AES-128 configuration): a batch of `--blocks` random 128-bit
+counter blocks per GPU (default 128; the configuration also names 16 and 1024), key =
+128 uniform bits from a seed, full 10-round homomorphic AES via circuit bootstrapping
+(blind rotation + HomTrace + SchemeSwitch), 16 CMux T-table LUTs per block-round and
+sample extract + key switch, every round a captured CUDA graph.  One step = one batch.
+
+value: blocks/s with inputs resident in HBM, CUDA events on the launching stream, max over
+ranks.  e2e: the same metric through the host-buffer C-ABI entry point
+(cbs_aes128_ctr_transcipher: counters in host memory, LWE outputs copied back).  Every
+output block is decrypted and compared with AES-128 from OpenSSL after the timed region.
+
+--impl reference: the CPU restatement of the same path (oracle/, all host threads) on a
+bounded sample of the same workload; rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import importlib.util
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+PKG_DIR = ROOT / "gpu-circuitbootstrapping-aestransciphering_b200"
+METRIC = "AES-128 CTR transciphering blocks/s (1 B200, exact-NTT circuit bootstrapping)"
+UNIT = "blocks/s"
+ROUNDS = 10
+
+
+def load_pkg():
+    spec = importlib.util.spec_from_file_location("cbs_b200", PKG_DIR / "__init__.py")
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["cbs_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def measured_peaks() -> dict:
+    f = ROOT / "MEASURED_PEAKS.json"
+    if f.exists():
+        d = json.loads(f.read_text())
+        return {"hbm_gbs": d.get("hbm_gbs", 6650.0), "src": "measured"}
+    return {"hbm_gbs": 6650.0, "src": "fallback"}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu, self.proc, self.lines = gpu, None, []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def counter_bits(ctrs: np.ndarray) -> np.ndarray:
+    """[blocks][16] bytes -> [blocks*128] bits, bit t = byte*8 + b."""
+    return np.unpackbits(ctrs, axis=1, bitorder="little").reshape(-1).astype(np.uint8)
+
+
+def verify(pkg, ctx, key: bytes, ctrs: np.ndarray, ha: np.ndarray, hb: np.ndarray) -> int:
+    from cryptography.hazmat.primitives.ciphers import Cipher, algorithms, modes
+    n = ctx.params.n
+    blocks = ctrs.shape[0]
+    dec = np.zeros(blocks * 128, np.uint8)
+    pkg.call("cbs_lwe_decrypt_bits", ctx.handle, ha.ctypes.data, hb.ctypes.data, blocks * 128, n, dec.ctypes.data)
+    got = np.packbits(dec.reshape(blocks, 128), axis=1, bitorder="little")
+    enc = Cipher(algorithms.AES(key), modes.ECB()).encryptor()
+    want = np.frombuffer(enc.update(ctrs.tobytes()), np.uint8).reshape(blocks, 16)
+    return int((got == want).all(axis=1).sum())
+
+
+def run_ours(args, rank: int, world: int, local_rank: int) -> None:
+    import torch
+    import torch.distributed as dist
+
+    torch.cuda.set_device(local_rank)
+    pkg = load_pkg()
+    blocks = args.blocks
+    ctx = pkg.Context(max_batch=128 * min(blocks, 256))
+    ctx.keygen(args.seed)
+    key = np.random.default_rng(args.seed).bytes(16)
+    pkg.call("cbs_aes128_setup", ctx.handle, key, args.seed + 1)
+    p = ctx.params
+    rng = np.random.default_rng(args.seed + 100 + rank)
+    ctrs = rng.integers(0, 256, size=(blocks, 16), dtype=np.uint8)
+    d_bits = torch.from_numpy(counter_bits(ctrs)).cuda()
+    out_a = torch.empty((blocks * 128, p.n), dtype=torch.int64, device="cuda")
+    out_b = torch.empty(blocks * 128, dtype=torch.int64, device="cuda")
+    torch.cuda.synchronize()
+    stream = torch.cuda.Stream()  # a real stream: the per-round graphs are captured on it
+    sptr = stream.cuda_stream
+
+    def step():
+        pkg.call("cbs_aes128_ctr_transcipher_device", ctx.handle, d_bits.data_ptr(), blocks, out_a.data_ptr(),
+                 out_b.data_ptr(), 1, sptr)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ms = ev0.elapsed_time(ev1)
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    ms_per_step = ms_max / args.steps
+
+    # correctness of the last step's output
+    ha = out_a.cpu().numpy().view(np.uint64).copy()
+    hb = out_b.cpu().numpy().view(np.uint64).copy()
+    ok = verify(pkg, ctx, key, ctrs, ha, hb)
+
+    # dominant kernel: the fused blind rotation over the whole batch, timed alone
+    T = min(blocks, 256) * 128
+    lwe_a = torch.from_numpy(ha[:T].view(np.int64)).cuda()
+    lwe_b = torch.from_numpy(hb[:T].view(np.int64)).cuda()
+    mv = torch.empty((T, p.num_lut, 2, p.N), dtype=torch.int64, device="cuda")
+    br = lambda: pkg.call("cbs_blind_rotate_batch_device", ctx.handle, lwe_a.data_ptr(), lwe_b.data_ptr(), T, p.n,  # noqa: E731
+                          mv.data_ptr(), sptr)
+    br()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 2
+    e0.record(stream)
+    for _ in range(reps):
+        br()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    br_ms = e0.elapsed_time(e1) / reps
+    N, n, l2, L = p.N, p.n, 2 * p.digits_g, p.num_lut
+    logn = N.bit_length() - 1
+    alg_bytes = n * l2 * 2 * N * 8 + T * ((n + 1) * 8 + L * 2 * N * 8)  # key once + LWE in + MV out
+    modmuls = T * n * (8 * (N // 2) * logn + 2 * l2 * N)  # butterflies + MAC products per launch
+    peaks = measured_peaks()
+    achieved_gbs = alg_bytes / (br_ms * 1e-3) / 1e9
+
+    # e2e through the host-buffer C-ABI entry point
+    out_ha = np.empty((blocks * 128, p.n), np.uint64)
+    out_hb = np.empty(blocks * 128, np.uint64)
+    e2e_steps = max(1, min(args.steps, 2))
+    pkg.call("cbs_aes128_ctr_transcipher", ctx.handle, ctrs.ctypes.data, blocks, out_ha.ctypes.data,
+             out_hb.ctypes.data)
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        pkg.call("cbs_aes128_ctr_transcipher", ctx.handle, ctrs.ctypes.data, blocks, out_ha.ctypes.data,
+                 out_hb.ctypes.data)
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_ok = verify(pkg, ctx, key, ctrs, out_ha, out_hb)
+
+    chunks = -(-blocks // 256)
+    launches_per_step = chunks * (1 + ROUNDS * 13)
+    result = {
+        "metric": METRIC,
+        "value": world * blocks / (ms_per_step * 1e-3),
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_per_step,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "u64 (exact mod-Q NTT arithmetic)",
+        "data": "synthetic (seeded random counters and key)",
+        "config": {"workload": "aes128_ctr_transcipher", "blocks_per_gpu": blocks, "global_blocks": world * blocks,
+                   "params": "N=2048 Q=54-bit n=630 q=2^14 BR 2^12x3 RGSW 2^6x4 HT 2^9x5 SS 2^9x5 KS 2^14/2^7",
+                   "l2": "per-step working set (keys + RGSW + LUT buffers) >> 126 MB L2",
+                   "parallelism": f"replicas x{world} (independent blocks per GPU)"},
+        "us_per_bootstrap": ms_per_step * 1e3 / (blocks * 128 * ROUNDS),
+        "correct_blocks": ok,
+        "gpu_launches": launches_per_step * args.steps,
+        "e2e": {"value": world * blocks / float(te.item()), "unit": UNIT, "h2d_bytes_per_step": blocks * 128,
+                "d2h_bytes_per_step": blocks * 128 * (p.n + 1) * 8, "correct_blocks": e2e_ok},
+        "roofline": {"kernel": "k_blind_rotate (fused GINX blind rotation + finalize + MV split)", "bound": "hbm",
+                     "achieved": achieved_gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": achieved_gbs / peaks["hbm_gbs"], "peak_src": peaks["src"], "traffic": None,
+                     "algorithmic_bytes_per_launch": alg_bytes, "launch_ms": br_ms,
+                     "note": "compute-bound on 64-bit modular multiplies; see modmul_rate"},
+        "modmul_rate": {"kernel": "k_blind_rotate", "modmul_per_launch": modmuls,
+                        "achieved_gmodmul_s": modmuls / (br_ms * 1e-3) / 1e9},
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and args.cpu_baseline:
+        result["cpu_baseline"] = cpu_baseline(args, pkg)
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+    ctx.close()
+
+
+def cpu_sample(args, pkg) -> dict:
+    """Time the CPU oracle on a bounded sample: `threads` circuit bootstraps in parallel, one
+    LUT per thread, 128 extractions; compose per-block time from the per-unit throughputs."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    from cbs_harness import OracleCbs, lwe_encrypt_bits  # noqa: E402
+    from conftest import load_oracle  # noqa: E402
+    from concurrent.futures import ThreadPoolExecutor
+
+    o = load_oracle()
+    threads = int(o.orc_num_threads())
+    p = pkg.default_params()
+    keys = pkg.generate_keys_host(p, args.seed)
+    oc = OracleCbs(o, p, keys)
+    rng = np.random.default_rng(1)
+    nb = threads
+    a, b = lwe_encrypt_bits(rng, keys["s_lwe"], rng.integers(0, 2, nb), p.q_lwe)
+    t0 = time.perf_counter()
+    mv = oc.br_mv(a, b)
+    rg = oc.trace_ss(mv)
+    t_cbs = (time.perf_counter() - t0) / nb
+    rg = rg.reshape(nb, -1)
+    table = rng.integers(0, p.Q, size=(256, 2, p.N), dtype=np.uint64)
+    ctrls = [np.ascontiguousarray(rg[k % nb]) for k in range(8)]
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(threads) as ex:
+        list(ex.map(lambda _: oc.lut(table, ctrls), range(threads)))
+    t_lut = (time.perf_counter() - t0) / threads
+    words = rng.integers(0, p.Q, size=(4, 2, p.N), dtype=np.uint64)
+    info = np.array([((t // 32) << 16) | (t % 32) for t in range(128)], np.uint32)
+    t0 = time.perf_counter()
+    oc.extract(words, info)
+    t_ext = (time.perf_counter() - t0) / 128
+    per_block = ROUNDS * (128 * t_cbs + 16 * t_lut + 128 * t_ext)
+    return {"value": 1.0 / per_block, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{nb} circuit bootstraps (BR n={p.n} + HomTrace + SchemeSwitch) in parallel, {threads} "
+                      f"8->32 CMux LUTs, 128 extract+KS; blocks/s composed as 10 rounds x (128 CBS + 16 LUT + "
+                      f"128 extract) from the per-unit times",
+            "per_unit_s": {"cbs": t_cbs, "lut": t_lut, "extract": t_ext}}
+
+
+def cpu_baseline(args, pkg) -> dict:
+    return cpu_sample(args, pkg)
+
+
+def run_reference(args, rank: int) -> None:
+    if rank != 0:
+        return
+    pkg = load_pkg()
+    vals = []
+    last = None
+    for i in range(args.warmup + args.steps):
+        r = cpu_sample(args, pkg)
+        if i >= args.warmup:
+            vals.append(r["value"])
+            last = r
+    value = statistics.median(vals)
+    last["value"] = value
+    out = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u64 (exact mod-Q arithmetic, CPU)",
+        "data": "synthetic (seeded)",
+        "config": {"workload": "aes128_ctr_transcipher", "blocks_per_gpu": args.blocks,
+                   "note": "the reference's CPU path (OpenFHE fork) is absent; CPU restatement of the same "
+                           "algorithm (oracle/) on all host threads, bounded sample per step"},
+        "cpu_baseline": last,
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--blocks", type=int, default=128)
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -38,6 +38,19 @@ class DModulus(ctypes.Structure):
     _fields_ = [("value", ctypes.c_uint64), ("const_ratio", ctypes.c_uint64 * 2)]
 
 
+class CbsParams(ctypes.Structure):
+    """Mirror of cbs_params (include/cbs_b200.h)."""
+    _fields_ = [("N", ctypes.c_uint32), ("Q", ctypes.c_uint64), ("n", ctypes.c_uint32), ("q_lwe", ctypes.c_uint64),
+                ("base_g", ctypes.c_uint32), ("digits_g", ctypes.c_uint32), ("num_lut", ctypes.c_uint32),
+                ("base_cc", ctypes.c_uint32), ("base_ht", ctypes.c_uint32), ("digits_ht", ctypes.c_uint32),
+                ("base_ss", ctypes.c_uint32), ("digits_ss", ctypes.c_uint32), ("trace_shift", ctypes.c_uint32),
+                ("qks", ctypes.c_uint32), ("base_ks", ctypes.c_uint32), ("sigma_lwe", ctypes.c_double),
+                ("sigma_rlwe", ctypes.c_double)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 def declared_symbols() -> list[str]:
     """Function names declared in include/cbs_b200.h (the C ABI)."""
     text = HEADER_PATH.read_text()
@@ -60,6 +73,24 @@ def _declare(lib: ctypes.CDLL) -> None:
         "cbs_inwt_1d_opt_permute_batched": (st, [c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, sz, sz, c_vp]),
         "cbs_ntt_tables_host": (st, [u32, u64, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
         "cbs_get_primes": (st, [u32, ctypes.c_int, u32, c_vp]),
+        "cbs_params_default": (st, [c_vp]),
+        "cbs_context_create": (st, [c_vp, u32, c_vp]),
+        "cbs_context_destroy": (st, [c_vp]),
+        "cbs_context_stream": (st, [c_vp, c_vp]),
+        "cbs_keygen": (st, [c_vp, u64]),
+        "cbs_export_keys": (st, [c_vp] + [c_vp] * 9),
+        "cbs_generate_keys_host": (st, [c_vp, u64] + [c_vp] * 9),
+        "cbs_context_tables": (st, [c_vp] + [c_vp] * 7),
+        "cbs_blind_rotate_batch_device": (st, [c_vp, c_vp, c_vp, u32, u32, c_vp, c_vp]),
+        "cbs_trace_schemeswitch_device": (st, [c_vp, c_vp, u32, c_vp, c_vp]),
+        "cbs_circuit_bootstrap_batch_device": (st, [c_vp, c_vp, c_vp, u32, u32, c_vp, c_vp]),
+        "cbs_lut8x32_batch_device": (st, [c_vp, c_vp, u32, c_vp, c_vp, u32, u64, c_vp, u32, c_vp, c_vp]),
+        "cbs_extract_keyswitch_device": (st, [c_vp, c_vp, u32, c_vp, u32, c_vp, c_vp, u32, c_vp]),
+        "cbs_aes128_setup": (st, [c_vp, c_vp, u64]),
+        "cbs_aes128_export_material": (st, [c_vp, c_vp, c_vp, c_vp, c_vp]),
+        "cbs_aes128_ctr_transcipher_device": (st, [c_vp, c_vp, u32, c_vp, c_vp, ctypes.c_int, c_vp]),
+        "cbs_aes128_ctr_transcipher": (st, [c_vp, c_vp, u32, c_vp, c_vp]),
+        "cbs_lwe_decrypt_bits": (st, [c_vp, c_vp, c_vp, u32, u32, c_vp]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name, None)
@@ -90,3 +121,65 @@ def check(status: int, where: str) -> None:
 def call(name: str, *args) -> None:
     """Call a C-ABI entry point and raise on a non-OK status."""
     check(getattr(load(), name)(*args), name)
+
+
+def default_params() -> CbsParams:
+    p = CbsParams()
+    call("cbs_params_default", ctypes.byref(p))
+    return p
+
+
+class Context:
+    """Owning handle of a cbs_context (the GPUCirBTSContext counterpart)."""
+
+    def __init__(self, params: CbsParams | None = None, max_batch: int = 128):
+        self.params = params if params is not None else default_params()
+        self.max_batch = max_batch
+        self._h = ctypes.c_void_p()
+        call("cbs_context_create", ctypes.byref(self.params), max_batch, ctypes.byref(self._h))
+
+    @property
+    def handle(self) -> int:
+        return self._h.value
+
+    def keygen(self, seed: int) -> None:
+        call("cbs_keygen", self._h, seed)
+
+    def close(self) -> None:
+        if self._h.value:
+            load().cbs_context_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def export_keys(self):
+        """Host copies (numpy) of secrets and key material in the reference layouts."""
+        out = key_buffers(self.params)
+        call("cbs_export_keys", self._h, *(out[k].ctypes.data for k in KEY_FIELDS))
+        return out
+
+
+KEY_FIELDS = ("s_lwe", "s_rlwe", "bsk", "ht", "ss", "ksk", "tv", "gpow", "maps")
+
+
+def key_buffers(p: CbsParams) -> dict:
+    import numpy as np
+    N, n, L = p.N, p.n, p.num_lut
+    rounds = N.bit_length() - 1 - p.trace_shift
+    return dict(
+        s_lwe=np.zeros(n, np.int32), s_rlwe=np.zeros(N, np.int32),
+        bsk=np.zeros((n, 2 * p.digits_g, 2, N), np.uint64),
+        ht=np.zeros((rounds, p.digits_ht, 2, N), np.uint64), ss=np.zeros((p.digits_ss, 2, N), np.uint64),
+        ksk=np.zeros((2, N, p.base_ks, n + 1), np.uint16), tv=np.zeros(N, np.uint64),
+        gpow=np.zeros(L, np.uint64), maps=np.zeros((rounds, N), np.uint32))
+
+
+def generate_keys_host(p: CbsParams, seed: int) -> dict:
+    """Key generation on the host only (no device needed); same keys as Context.keygen(seed)."""
+    out = key_buffers(p)
+    call("cbs_generate_keys_host", ctypes.byref(p), seed, *(out[k].ctypes.data for k in KEY_FIELDS))
+    return out

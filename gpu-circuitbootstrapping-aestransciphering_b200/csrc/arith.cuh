@@ -61,6 +61,22 @@ __device__ __forceinline__ uint64_t barrett_reduce_128(u128 x, uint64_t q, uint6
     return csub(r, q);
 }
 
+// Montgomery product x * k' * 2^-64 mod q in [0, 2q) for x < q, k' < q (k' = k * 2^64 mod q
+// gives x * k): keys stored in Montgomery form need no Shoup companion, so a MAC reads one
+// word per key coefficient.  qneg_inv = -q^-1 mod 2^64.
+__device__ __forceinline__ uint64_t mont_mul_lazy(uint64_t x, uint64_t kp, uint64_t q, uint64_t qneg_inv) {
+    const uint64_t lo = x * kp;
+    const uint64_t hi = __umul64hi(x, kp);
+    const uint64_t m = lo * qneg_inv;
+    return hi + __umul64hi(m, q) + (lo != 0 ? 1ull : 0ull);
+}
+
+// s mod q for any s < 2^64 using the Shoup quotient of 1 (one_s = floor(2^64 / q))
+__device__ __forceinline__ uint64_t reduce64(uint64_t s, uint64_t q, uint64_t one_s) {
+    const uint64_t hi = __umul64hi(s, one_s);
+    return csub(csub(s - hi * q, q), q);
+}
+
 // Montgomery-free exact product a * b mod q with a 128-bit intermediate (setup paths only).
 __device__ __forceinline__ uint64_t mul_mod_barrett(uint64_t a, uint64_t b, uint64_t q, uint64_t r0, uint64_t r1) {
     return barrett_reduce_128(mul_wide(a, b), q, r0, r1);

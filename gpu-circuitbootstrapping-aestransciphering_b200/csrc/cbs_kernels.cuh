@@ -1,0 +1,73 @@
+// cbs_kernels.cuh -- launch interfaces of the fused circuit-bootstrapping, CMux and
+// extraction kernels (implemented in cbs_kernels.cu, lut_kernels.cu, extract_kernels.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "arith.cuh"
+
+namespace cbs {
+
+struct RingTables {
+    const uint64_t* rp;
+    const uint64_t* rps;
+    const uint64_t* irp;
+    const uint64_t* irps;
+    uint64_t q;
+    uint64_t n_inv, n_inv_s;
+    uint64_t ratio0, ratio1;  // floor(2^128 / q)
+    uint64_t qneg_inv;        // -q^-1 mod 2^64 (Montgomery)
+    uint64_t one_s;           // floor(2^64 / q)
+};
+
+struct BlindRotateArgs {
+    RingTables t;
+    const uint64_t* a;       // [batch][a_stride] LWE masks mod q_lwe
+    const uint64_t* b;       // [batch]
+    uint32_t a_stride;
+    uint32_t n;              // LWE dimension (blind-rotation steps)
+    uint64_t q_lwe;
+    uint32_t bitwidth;       // special mod-switch granularity log2
+    const uint64_t* tv;      // [N] test vector, coefficient domain
+    const uint64_t* bsk;     // [n][2*digits][2][N] NTT domain, Montgomery form
+    Gadget g;                // blind-rotation gadget
+    uint32_t digits;
+    uint32_t num_lut;
+    const uint64_t* gadd;    // [num_lut] (gpow[j] >> 1) * N^-1 mod Q
+    uint64_t* mv_out;        // [batch][num_lut][2][N] NTT domain (MV RLWEs after finalize)
+};
+
+struct TraceArgs {
+    RingTables t;
+    const uint64_t* mv;      // [count][2][N] NTT domain
+    uint64_t* rgsw;          // [count][2][2][N] NTT domain
+    const uint32_t* maps;    // [rounds][N] NTT-domain automorphism permutations
+    uint32_t rounds;
+    const uint64_t* ht_key;  // [rounds][digits_ht][2][N] NTT domain, Montgomery form
+    const uint64_t* ss_key;  // [digits_ss][2][N] NTT domain, Montgomery form
+    Gadget g_ht, g_ss;
+    uint32_t digits_ht, digits_ss;
+};
+
+struct CmuxLevelArgs {
+    RingTables t;
+    const uint64_t* in;           // level input: [sets][in_count][2][N]
+    uint64_t in_lut_stride;       // words between input sets
+    const uint32_t* lut_sel;      // input set of each LUT (level 0: table id); null = the LUT index
+    uint64_t* out;                // [luts][in_count/2][2][N]
+    uint32_t in_count;
+    const uint64_t* rgsw_all;     // CBS output [bits][digits][2][2][N]
+    uint64_t rgsw_stride;         // words per bit
+    const uint32_t* ctrl_bits;    // [luts][8] bit index of the control for each level
+    uint32_t level;
+    Gadget g;
+    uint32_t digits;
+};
+
+cudaError_t launch_blind_rotate(const BlindRotateArgs& a, uint32_t N, uint32_t batch, cudaStream_t s);
+cudaError_t launch_trace_schemeswitch(const TraceArgs& a, uint32_t N, uint32_t count, cudaStream_t s);
+cudaError_t launch_cmux_level(const CmuxLevelArgs& a, uint32_t N, uint32_t luts, cudaStream_t s);
+
+}  // namespace cbs

@@ -1,0 +1,421 @@
+// context.cu -- cbs_context lifecycle, key upload, and the batched CBS / CMux / extraction
+// entry points of the C ABI.
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "common.cuh"
+#include "context.cuh"
+
+namespace cbs {
+
+cudaError_t ntt_forward(uint64_t* out, const uint64_t* in, const uint64_t* tw, const uint64_t* tws,
+                        const cbs_dmodulus* mod, size_t dim, size_t batch, cudaStream_t s);
+cudaError_t ntt_inverse(uint64_t* out, const uint64_t* in, const uint32_t* map, const uint64_t* itw,
+                        const uint64_t* itws, const cbs_dmodulus* mod, const uint64_t* sc, const uint64_t* scs,
+                        size_t dim, size_t batch, cudaStream_t s);
+
+static uint64_t neg_inv64(uint64_t q) {
+    uint64_t inv = q;  // q * q = 1 mod 8 for odd q
+    for (int i = 0; i < 6; ++i) inv *= 2 - q * inv;
+    return ~inv + 1;
+}
+
+static std::vector<uint64_t> to_mont(const std::vector<uint64_t>& v, const FastMod& fm, uint64_t r) {
+    std::vector<uint64_t> out(v.size());
+    for (size_t i = 0; i < v.size(); ++i) out[i] = fm.mul(v[i], r);
+    return out;
+}
+
+cbs_status run_blind_rotate(cbs_context* c, const uint64_t* d_a, const uint64_t* d_b, uint32_t batch,
+                            uint32_t a_stride, uint64_t* d_mv, cudaStream_t s) {
+    BlindRotateArgs a{};
+    a.t = c->ring();
+    a.a = d_a;
+    a.b = d_b;
+    a.a_stride = a_stride;
+    a.n = c->p.n;
+    a.q_lwe = c->p.q_lwe;
+    a.bitwidth = c->bitwidth;
+    a.tv = c->d_tv.p;
+    a.bsk = c->d_bsk.p;
+    a.g = c->g_br;
+    a.digits = c->p.digits_g;
+    a.num_lut = c->p.num_lut;
+    a.gadd = c->d_gadd.p;
+    a.mv_out = d_mv;
+    CBS_CUDA_TRY(launch_blind_rotate(a, c->p.N, batch, s));
+    return CBS_OK;
+}
+
+cbs_status run_trace(cbs_context* c, const uint64_t* d_mv, uint32_t count, uint64_t* d_rgsw, cudaStream_t s) {
+    TraceArgs a{};
+    a.t = c->ring();
+    a.mv = d_mv;
+    a.rgsw = d_rgsw;
+    a.maps = c->d_maps.p;
+    a.rounds = c->rounds;
+    a.ht_key = c->d_ht.p;
+    a.ss_key = c->d_ss.p;
+    a.g_ht = c->g_ht;
+    a.g_ss = c->g_ss;
+    a.digits_ht = c->p.digits_ht;
+    a.digits_ss = c->p.digits_ss;
+    CBS_CUDA_TRY(launch_trace_schemeswitch(a, c->p.N, count, s));
+    return CBS_OK;
+}
+
+cbs_status run_lut_levels(cbs_context* c, const uint64_t* d_tables, uint64_t table_stride, const uint32_t* d_lut_sel,
+                          const uint64_t* d_rgsw_all, uint64_t rgsw_stride, const uint32_t* d_ctrl, uint32_t luts,
+                          uint64_t* d_buf_a, uint64_t* d_buf_b, uint64_t* d_out, cudaStream_t s) {
+    const uint32_t N = c->p.N;
+    const uint64_t* in = d_tables;
+    for (uint32_t level = 0; level < 8; ++level) {
+        CmuxLevelArgs a{};
+        a.t = c->ring();
+        a.in_count = 256u >> level;
+        a.in = in;
+        a.in_lut_stride = (level == 0) ? table_stride : static_cast<uint64_t>(a.in_count) * 2 * N;
+        a.lut_sel = (level == 0) ? d_lut_sel : nullptr;
+        uint64_t* out = (level == 7) ? d_out : ((level & 1) ? d_buf_b : d_buf_a);
+        a.out = out;
+        a.rgsw_all = d_rgsw_all;
+        a.rgsw_stride = rgsw_stride;
+        a.ctrl_bits = d_ctrl;
+        a.level = level;
+        a.g = c->g_cc;
+        a.digits = c->p.num_lut;
+        CBS_CUDA_TRY(launch_cmux_level(a, N, luts, s));
+        in = out;
+    }
+    return CBS_OK;
+}
+
+cbs_status run_extract(cbs_context* c, const uint64_t* d_words_coef, const uint32_t* d_info, uint32_t count,
+                       uint64_t* d_out_a, uint64_t* d_out_b, uint32_t out_stride, cudaStream_t s) {
+    ExtractArgs a{};
+    a.words = d_words_coef;
+    a.info = d_info;
+    a.ksk = c->d_ksk.p;
+    a.out_a = d_out_a;
+    a.out_b = d_out_b;
+    a.out_stride = out_stride;
+    a.N = c->p.N;
+    a.n = c->p.n;
+    a.Q = c->p.Q;
+    a.q_over_Q = static_cast<double>(c->p.qks) / static_cast<double>(c->p.Q);
+    a.qks = c->p.qks;
+    a.mask = c->p.qks - 1;
+    a.base_ks = c->p.base_ks;
+    a.base_log2 = static_cast<uint32_t>(__builtin_ctz(c->p.base_ks));
+    a.q_lwe = c->p.q_lwe;
+    a.scale = (c->p.q_lwe % c->p.qks == 0) ? c->p.q_lwe / c->p.qks : 0;
+    CBS_CUDA_TRY(launch_extract_keyswitch(a, count, s));
+    return CBS_OK;
+}
+
+static bool pow2(uint64_t x) { return x && !(x & (x - 1)); }
+
+static cbs_status validate(const cbs_params& p) {
+    CBS_CHECK_ARG(p.N == 1024 || p.N == 2048 || p.N == 4096, "params: N must be 1024, 2048 or 4096");
+    CBS_CHECK_ARG(p.Q > 2 && p.Q < (1ull << 62) && (p.Q - 1) % (2ull * p.N) == 0, "params: Q must be 1 mod 2N, < 2^62");
+    CBS_CHECK_ARG(host::is_prime(p.Q), "params: Q must be prime");
+    CBS_CHECK_ARG(p.n >= 1 && p.n <= 4096, "params: n out of range");
+    CBS_CHECK_ARG(p.q_lwe >= 2 && p.q_lwe <= (1ull << 32), "params: q_lwe out of range");
+    CBS_CHECK_ARG(pow2(p.base_g) && p.base_g >= 2 && p.digits_g >= 1 && p.digits_g <= 16, "params: bad BR gadget");
+    CBS_CHECK_ARG(p.num_lut >= 1 && p.num_lut <= 8 && pow2(p.base_cc), "params: bad RGSW output gadget");
+    CBS_CHECK_ARG(pow2(p.base_ht) && p.digits_ht >= 1 && p.digits_ht <= 16, "params: bad HomTrace gadget");
+    CBS_CHECK_ARG(pow2(p.base_ss) && p.digits_ss >= 1 && p.digits_ss <= 16, "params: bad SchemeSwitch gadget");
+    CBS_CHECK_ARG(p.trace_shift == 0, "params: only trace_shift = 0 (full HomTrace) is supported");
+    CBS_CHECK_ARG(pow2(p.qks) && p.qks <= 65536 && pow2(p.base_ks), "params: qks/base_ks must be powers of two");
+    CBS_CHECK_ARG(static_cast<uint64_t>(p.base_ks) * p.base_ks >= p.qks && p.base_ks < p.qks,
+                  "params: extraction key switch needs exactly two digits");
+    return CBS_OK;
+}
+
+}  // namespace cbs
+
+using namespace cbs;
+
+extern "C" {
+
+cbs_status cbs_params_default(cbs_params* out) {
+    CBS_CHECK_ARG(out, "params_default: null output");
+    std::vector<uint64_t> q;
+    host::get_primes(2048, 54, 1, q);
+    cbs_params p{};
+    p.N = 2048;
+    p.Q = q[0];
+    p.n = 630;
+    p.q_lwe = 1u << 14;
+    p.base_g = 1u << 12;
+    p.digits_g = 3;
+    p.num_lut = 4;
+    p.base_cc = 1u << 6;
+    p.base_ht = 1u << 9;
+    p.digits_ht = 5;
+    p.base_ss = 1u << 9;
+    p.digits_ss = 5;
+    p.trace_shift = 0;
+    p.qks = 1u << 14;
+    p.base_ks = 1u << 7;
+    p.sigma_lwe = 0.5;
+    p.sigma_rlwe = 3.19;
+    *out = p;
+    return CBS_OK;
+}
+
+cbs_status cbs_context_create(const cbs_params* params, uint32_t max_batch, cbs_context** out) {
+    CBS_CHECK_ARG(params && out, "context_create: null argument");
+    CBS_CHECK_ARG(max_batch >= 1 && max_batch <= (1u << 22), "context_create: max_batch out of range");
+    cbs_status st = validate(*params);
+    if (st != CBS_OK) return st;
+    auto* c = new (std::nothrow) cbs_context();
+    if (!c) {
+        set_error("context_create: host allocation failed");
+        return CBS_ERR_OOM;
+    }
+    std::unique_ptr<cbs_context> guard(c);
+    c->p = *params;
+    c->max_batch = max_batch;
+    CBS_CUDA_TRY(cudaGetDevice(&c->device));
+    if (!host::make_ntt_tables(c->p.N, c->p.Q, c->tab)) {
+        set_error("context_create: NTT tables failed");
+        return CBS_ERR_INVALID_ARG;
+    }
+    c->g_br = make_gadget(c->p.Q, c->p.base_g, c->p.digits_g);
+    c->g_cc = make_gadget(c->p.Q, c->p.base_cc, c->p.num_lut);
+    c->g_ht = make_gadget(c->p.Q, c->p.base_ht, c->p.digits_ht);
+    c->g_ss = make_gadget(c->p.Q, c->p.base_ss, c->p.digits_ss);
+    c->rounds = static_cast<uint32_t>(__builtin_ctz(c->p.N)) - c->p.trace_shift;
+    c->bitwidth = 0;
+    while ((1u << c->bitwidth) < c->p.num_lut) ++c->bitwidth;
+    c->qneg_inv = neg_inv64(c->p.Q);
+    c->one_s = host::shoup(1, c->p.Q);
+    c->mont_r = static_cast<uint64_t>((static_cast<unsigned __int128>(1) << 64) % c->p.Q);
+    CBS_CUDA_TRY(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    const size_t N = c->p.N;
+    cudaStream_t s = c->stream;
+    CBS_CUDA_TRY(c->d_rp.upload(c->tab.rp.data(), N, s));
+    CBS_CUDA_TRY(c->d_rps.upload(c->tab.rp_sh.data(), N, s));
+    CBS_CUDA_TRY(c->d_irp.upload(c->tab.irp.data(), N, s));
+    CBS_CUDA_TRY(c->d_irps.upload(c->tab.irp_sh.data(), N, s));
+    CBS_CUDA_TRY(c->d_ninv.upload(&c->tab.n_inv, 1, s));
+    CBS_CUDA_TRY(c->d_ninv_s.upload(&c->tab.n_inv_sh, 1, s));
+    cbs_dmodulus dm{c->p.Q, {c->tab.ratio0, c->tab.ratio1}};
+    CBS_CUDA_TRY(c->d_mod.upload(&dm, 1, s));
+    // scratch for max_batch inputs
+    const size_t L = c->p.num_lut;
+    CBS_CUDA_TRY(c->d_mv.alloc(static_cast<size_t>(max_batch) * L * 2 * N));
+    CBS_CUDA_TRY(c->d_rgsw.alloc(static_cast<size_t>(max_batch) * L * 4 * N));
+    CBS_CUDA_TRY(cudaStreamSynchronize(s));
+    *out = guard.release();
+    return CBS_OK;
+}
+
+cbs_status cbs_context_destroy(cbs_context* ctx) {
+    if (!ctx) return CBS_OK;
+    for (auto& g : ctx->aes.graphs)
+        if (g) cudaGraphExecDestroy(g);
+    cudaStream_t s = ctx->stream;
+    delete ctx;
+    if (s) cudaStreamDestroy(s);
+    return CBS_OK;
+}
+
+cbs_status cbs_context_stream(const cbs_context* ctx, cbs_stream_t* out) {
+    CBS_CHECK_ARG(ctx && out, "context_stream: null argument");
+    *out = reinterpret_cast<cbs_stream_t>(ctx->stream);
+    return CBS_OK;
+}
+
+cbs_status cbs_keygen(cbs_context* ctx, uint64_t seed) {
+    CBS_CHECK_ARG(ctx, "keygen: null context");
+    cbs_context* c = ctx;
+    try {
+        generate_keys(c->p, c->tab, seed, c->hk);
+    } catch (const std::exception& e) {
+        set_error(std::string("keygen: ") + e.what());
+        return CBS_ERR_OOM;
+    }
+    FastMod fm(c->p.Q);
+    cudaStream_t s = c->stream;
+    const auto bsk_m = to_mont(c->hk.bsk, fm, c->mont_r);
+    const auto ht_m = to_mont(c->hk.ht, fm, c->mont_r);
+    const auto ss_m = to_mont(c->hk.ss, fm, c->mont_r);
+    CBS_CUDA_TRY(c->d_bsk.upload(bsk_m.data(), bsk_m.size(), s));
+    CBS_CUDA_TRY(c->d_ht.upload(ht_m.data(), ht_m.size(), s));
+    CBS_CUDA_TRY(c->d_ss.upload(ss_m.data(), ss_m.size(), s));
+    CBS_CUDA_TRY(c->d_ksk.upload(c->hk.ksk.data(), c->hk.ksk.size(), s));
+    CBS_CUDA_TRY(c->d_tv.upload(c->hk.tv.data(), c->hk.tv.size(), s));
+    CBS_CUDA_TRY(c->d_gadd.upload(c->hk.gadd.data(), c->hk.gadd.size(), s));
+    CBS_CUDA_TRY(c->d_maps.upload(c->hk.maps.data(), c->hk.maps.size(), s));
+    CBS_CUDA_TRY(cudaStreamSynchronize(s));
+    c->keys_ready = true;
+    c->aes.ready = false;
+    return CBS_OK;
+}
+
+cbs_status cbs_generate_keys_host(const cbs_params* params, uint64_t seed, int32_t* s_lwe, int32_t* s_rlwe,
+                                  uint64_t* bsk, uint64_t* ht, uint64_t* ss, uint16_t* ksk, uint64_t* tv, uint64_t* gpow,
+                                  uint32_t* maps) {
+    CBS_CHECK_ARG(params, "generate_keys_host: null params");
+    if (cbs_status st = validate(*params)) return st;
+    host::NttTables t;
+    if (!host::make_ntt_tables(params->N, params->Q, t)) {
+        set_error("generate_keys_host: NTT tables failed");
+        return CBS_ERR_INVALID_ARG;
+    }
+    HostKeys k;
+    try {
+        generate_keys(*params, t, seed, k);
+    } catch (const std::exception& e) {
+        set_error(std::string("generate_keys_host: ") + e.what());
+        return CBS_ERR_OOM;
+    }
+    auto cp = [](auto* dst, const auto& v) {
+        if (dst) std::memcpy(dst, v.data(), v.size() * sizeof(v[0]));
+    };
+    cp(s_lwe, k.s_lwe);
+    cp(s_rlwe, k.s_rlwe);
+    cp(bsk, k.bsk);
+    cp(ht, k.ht);
+    cp(ss, k.ss);
+    cp(ksk, k.ksk);
+    cp(tv, k.tv);
+    cp(gpow, k.gpow);
+    cp(maps, k.maps);
+    return CBS_OK;
+}
+
+cbs_status cbs_export_keys(const cbs_context* ctx, int32_t* s_lwe, int32_t* s_rlwe, uint64_t* bsk, uint64_t* ht,
+                           uint64_t* ss, uint16_t* ksk, uint64_t* tv, uint64_t* gpow, uint32_t* maps) {
+    CBS_CHECK_ARG(ctx, "export_keys: null context");
+    if (!ctx->keys_ready) {
+        set_error("export_keys: no keys (call cbs_keygen first)");
+        return CBS_ERR_NOT_READY;
+    }
+    const HostKeys& k = ctx->hk;
+    auto cp = [](auto* dst, const auto& v) {
+        if (dst) std::memcpy(dst, v.data(), v.size() * sizeof(v[0]));
+    };
+    cp(s_lwe, k.s_lwe);
+    cp(s_rlwe, k.s_rlwe);
+    cp(bsk, k.bsk);
+    cp(ht, k.ht);
+    cp(ss, k.ss);
+    cp(ksk, k.ksk);
+    cp(tv, k.tv);
+    cp(gpow, k.gpow);
+    cp(maps, k.maps);
+    return CBS_OK;
+}
+
+cbs_status cbs_context_tables(const cbs_context* ctx, const cbs_dmodulus** d_modulus, const uint64_t** d_twiddles,
+                              const uint64_t** d_twiddles_shoup, const uint64_t** d_itwiddles,
+                              const uint64_t** d_itwiddles_shoup, const uint64_t** d_n_inv,
+                              const uint64_t** d_n_inv_shoup) {
+    CBS_CHECK_ARG(ctx, "context_tables: null context");
+    if (d_modulus) *d_modulus = ctx->d_mod.p;
+    if (d_twiddles) *d_twiddles = ctx->d_rp.p;
+    if (d_twiddles_shoup) *d_twiddles_shoup = ctx->d_rps.p;
+    if (d_itwiddles) *d_itwiddles = ctx->d_irp.p;
+    if (d_itwiddles_shoup) *d_itwiddles_shoup = ctx->d_irps.p;
+    if (d_n_inv) *d_n_inv = ctx->d_ninv.p;
+    if (d_n_inv_shoup) *d_n_inv_shoup = ctx->d_ninv_s.p;
+    return CBS_OK;
+}
+
+static cbs_status need_keys(const cbs_context* c) {
+    if (!c->keys_ready) {
+        set_error("no key material (call cbs_keygen first)");
+        return CBS_ERR_NOT_READY;
+    }
+    return CBS_OK;
+}
+
+cbs_status cbs_blind_rotate_batch_device(cbs_context* ctx, const uint64_t* d_a, const uint64_t* d_b, uint32_t batch,
+                                         uint32_t a_stride, uint64_t* d_mv, cbs_stream_t stream) {
+    CBS_CHECK_ARG(ctx, "blind_rotate: null context");
+    if (batch == 0) return CBS_OK;
+    CBS_CHECK_ARG(d_a && d_b && d_mv, "blind_rotate: null pointer");
+    CBS_CHECK_ARG(a_stride >= ctx->p.n, "blind_rotate: a_stride < n");
+    if (cbs_status st = need_keys(ctx)) return st;
+    return run_blind_rotate(ctx, d_a, d_b, batch, a_stride, d_mv, reinterpret_cast<cudaStream_t>(stream));
+}
+
+cbs_status cbs_trace_schemeswitch_device(cbs_context* ctx, const uint64_t* d_mv, uint32_t count, uint64_t* d_rgsw,
+                                         cbs_stream_t stream) {
+    CBS_CHECK_ARG(ctx, "trace: null context");
+    if (count == 0) return CBS_OK;
+    CBS_CHECK_ARG(d_mv && d_rgsw, "trace: null pointer");
+    if (cbs_status st = need_keys(ctx)) return st;
+    return run_trace(ctx, d_mv, count, d_rgsw, reinterpret_cast<cudaStream_t>(stream));
+}
+
+cbs_status cbs_circuit_bootstrap_batch_device(cbs_context* ctx, const uint64_t* d_a, const uint64_t* d_b,
+                                              uint32_t batch, uint32_t a_stride, const uint64_t** d_rgsw_view,
+                                              cbs_stream_t stream) {
+    CBS_CHECK_ARG(ctx && d_rgsw_view, "cbs: null argument");
+    *d_rgsw_view = nullptr;
+    if (batch == 0) return CBS_OK;
+    CBS_CHECK_ARG(d_a && d_b, "cbs: null input");
+    CBS_CHECK_ARG(a_stride >= ctx->p.n, "cbs: a_stride < n");
+    if (batch > ctx->max_batch) {
+        set_error("cbs: batch exceeds the context's max_batch (recreate the context)");
+        return CBS_ERR_SHAPE_MISMATCH;
+    }
+    if (cbs_status st = need_keys(ctx)) return st;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    if (cbs_status st = run_blind_rotate(ctx, d_a, d_b, batch, a_stride, ctx->d_mv.p, s)) return st;
+    if (cbs_status st = run_trace(ctx, ctx->d_mv.p, batch * ctx->p.num_lut, ctx->d_rgsw.p, s)) return st;
+    *d_rgsw_view = ctx->d_rgsw.p;
+    return CBS_OK;
+}
+
+cbs_status cbs_lut8x32_batch_device(cbs_context* ctx, const uint64_t* d_tables, uint32_t num_tables,
+                                    const uint32_t* h_table_of_lut, const uint64_t* d_rgsw_all, uint32_t num_bits,
+                                    uint64_t rgsw_stride, const uint32_t* h_ctrl_bits, uint32_t luts, uint64_t* d_out,
+                                    cbs_stream_t stream) {
+    CBS_CHECK_ARG(ctx, "lut: null context");
+    if (luts == 0) return CBS_OK;
+    CBS_CHECK_ARG(d_tables && h_table_of_lut && d_rgsw_all && h_ctrl_bits && d_out, "lut: null pointer");
+    CBS_CHECK_ARG(luts <= 65535, "lut: at most 65535 LUTs per call");
+    CBS_CHECK_ARG(rgsw_stride >= static_cast<uint64_t>(ctx->p.num_lut) * 4 * ctx->p.N, "lut: rgsw_stride too small");
+    for (uint32_t u = 0; u < luts; ++u) {
+        CBS_CHECK_ARG(h_table_of_lut[u] < num_tables, "lut: table index out of range");
+        for (uint32_t k = 0; k < 8; ++k) CBS_CHECK_ARG(h_ctrl_bits[u * 8 + k] < num_bits, "lut: control bit out of range");
+    }
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const size_t N = ctx->p.N;
+    CBS_CUDA_TRY(ctx->d_lut_sel_scratch.alloc(luts));
+    CBS_CUDA_TRY(ctx->d_ctrl_scratch.alloc(static_cast<size_t>(luts) * 8));
+    CBS_CUDA_TRY(ctx->d_lut_a.alloc(static_cast<size_t>(luts) * 128 * 2 * N));
+    CBS_CUDA_TRY(ctx->d_lut_b.alloc(static_cast<size_t>(luts) * 64 * 2 * N));
+    CBS_CUDA_TRY(cudaMemcpyAsync(ctx->d_lut_sel_scratch.p, h_table_of_lut, luts * sizeof(uint32_t),
+                                 cudaMemcpyHostToDevice, s));
+    CBS_CUDA_TRY(cudaMemcpyAsync(ctx->d_ctrl_scratch.p, h_ctrl_bits, static_cast<size_t>(luts) * 8 * sizeof(uint32_t),
+                                 cudaMemcpyHostToDevice, s));
+    return run_lut_levels(ctx, d_tables, 256ull * 2 * N, ctx->d_lut_sel_scratch.p, d_rgsw_all, rgsw_stride,
+                          ctx->d_ctrl_scratch.p, luts, ctx->d_lut_a.p, ctx->d_lut_b.p, d_out, s);
+}
+
+cbs_status cbs_extract_keyswitch_device(cbs_context* ctx, const uint64_t* d_words_coef, uint32_t words,
+                                        const uint32_t* h_info, uint32_t count, uint64_t* d_out_a, uint64_t* d_out_b,
+                                        uint32_t out_stride, cbs_stream_t stream) {
+    CBS_CHECK_ARG(ctx, "extract: null context");
+    if (count == 0) return CBS_OK;
+    CBS_CHECK_ARG(d_words_coef && h_info && d_out_a && d_out_b, "extract: null pointer");
+    CBS_CHECK_ARG(out_stride >= ctx->p.n, "extract: out_stride < n");
+    CBS_CHECK_ARG(count <= 65535u, "extract: at most 65535 outputs per call");
+    for (uint32_t t = 0; t < count; ++t) {
+        CBS_CHECK_ARG((h_info[t] >> 16) < words && (h_info[t] & 0xFFFFu) < ctx->p.N, "extract: info out of range");
+    }
+    if (cbs_status st = need_keys(ctx)) return st;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    CBS_CUDA_TRY(ctx->d_info_scratch.alloc(count));
+    CBS_CUDA_TRY(cudaMemcpyAsync(ctx->d_info_scratch.p, h_info, count * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+    return run_extract(ctx, d_words_coef, ctx->d_info_scratch.p, count, d_out_a, d_out_b, out_stride, s);
+}
+
+}  // extern "C"

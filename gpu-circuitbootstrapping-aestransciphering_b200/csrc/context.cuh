@@ -1,0 +1,123 @@
+// context.cuh -- the cbs_context object behind the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <array>
+#include <cstdint>
+#include <memory>
+#include <vector>
+
+#include "../../include/cbs_b200.h"
+#include "cbs_kernels.cuh"
+#include "extract_kernels.cuh"
+#include "host_math.h"
+#include "keygen.h"
+
+namespace cbs {
+
+// owning device buffer (cudaMalloc / cudaFree)
+template <class T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { reset(); }
+    void reset() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    cudaError_t alloc(size_t count) {
+        if (count <= n && p) return cudaSuccess;
+        reset();
+        if (!count) return cudaSuccess;
+        cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&p), count * sizeof(T));
+        if (e == cudaSuccess) n = count;
+        else p = nullptr;
+        return e;
+    }
+    cudaError_t upload(const T* h, size_t count, cudaStream_t s) {
+        cudaError_t e = alloc(count);
+        if (e != cudaSuccess) return e;
+        return cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, s);
+    }
+};
+
+struct AesState {
+    bool ready = false;
+    uint8_t key[16];
+    uint32_t chunk_blocks = 0;            // blocks per device chunk
+    DevBuf<uint64_t> tables;              // [8][256][2][N]  Te0..3, Te4_0..3
+    DevBuf<uint64_t> rk_words;            // [11][4][2][N]
+    DevBuf<uint64_t> rk0_a, rk0_b;        // [128][n], [128]
+    std::vector<uint64_t> h_tables, h_rk_words, h_rk0_a, h_rk0_b;
+    // per-chunk workspace
+    DevBuf<uint8_t> ctr_bits;             // [chunk*128]
+    DevBuf<uint64_t> st_a, st_b;          // [chunk*128][n], [chunk*128]
+    DevBuf<uint64_t> lut_a, lut_b;        // ping-pong level buffers
+    DevBuf<uint64_t> lut_out;             // [chunk*16][2][N]
+    DevBuf<uint64_t> words;               // [chunk*4][2][N]
+    DevBuf<uint32_t> lut_sel[2];          // table id per LUT (normal rounds, final round)
+    DevBuf<uint32_t> ctrl_bits;           // [chunk*16][8]
+    DevBuf<uint32_t> extract_info;        // [chunk*128]
+    std::array<cudaGraphExec_t, 10> graphs{};
+    uint32_t graph_chunk = 0;
+};
+
+}  // namespace cbs
+
+struct cbs_context {
+    cbs_params p{};
+    uint32_t max_batch = 0;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cbs::host::NttTables tab;
+    cbs::Gadget g_br{}, g_cc{}, g_ht{}, g_ss{};
+    uint32_t rounds = 0, bitwidth = 0;
+    uint64_t qneg_inv = 0, one_s = 0, mont_r = 0;
+    // device tables
+    cbs::DevBuf<uint64_t> d_rp, d_rps, d_irp, d_irps, d_ninv, d_ninv_s;
+    cbs::DevBuf<cbs_dmodulus> d_mod;
+    cbs::DevBuf<uint32_t> d_maps;
+    // keys
+    bool keys_ready = false;
+    cbs::HostKeys hk;
+    cbs::DevBuf<uint64_t> d_tv, d_gadd, d_bsk, d_ht, d_ss;
+    cbs::DevBuf<uint16_t> d_ksk;
+    // scratch
+    cbs::DevBuf<uint64_t> d_mv, d_rgsw;
+    cbs::DevBuf<uint32_t> d_info_scratch, d_lut_sel_scratch, d_ctrl_scratch;
+    cbs::DevBuf<uint64_t> d_lut_a, d_lut_b;
+    cbs::AesState aes;
+
+    cbs::RingTables ring() const {
+        cbs::RingTables t;
+        t.rp = d_rp.p;
+        t.rps = d_rps.p;
+        t.irp = d_irp.p;
+        t.irps = d_irps.p;
+        t.q = p.Q;
+        t.n_inv = tab.n_inv;
+        t.n_inv_s = tab.n_inv_sh;
+        t.ratio0 = tab.ratio0;
+        t.ratio1 = tab.ratio1;
+        t.qneg_inv = qneg_inv;
+        t.one_s = one_s;
+        return t;
+    }
+};
+
+namespace cbs {
+// shared entry used by the AES driver and the C ABI
+cbs_status run_blind_rotate(cbs_context* c, const uint64_t* d_a, const uint64_t* d_b, uint32_t batch,
+                            uint32_t a_stride, uint64_t* d_mv, cudaStream_t s);
+cbs_status run_trace(cbs_context* c, const uint64_t* d_mv, uint32_t count, uint64_t* d_rgsw, cudaStream_t s);
+cbs_status run_lut_levels(cbs_context* c, const uint64_t* d_tables, uint64_t table_stride, const uint32_t* d_lut_sel,
+                          const uint64_t* d_rgsw_all, uint64_t rgsw_stride, const uint32_t* d_ctrl, uint32_t luts,
+                          uint64_t* d_buf_a, uint64_t* d_buf_b, uint64_t* d_out, cudaStream_t s);
+cbs_status run_extract(cbs_context* c, const uint64_t* d_words_coef, const uint32_t* d_info, uint32_t count,
+                       uint64_t* d_out_a, uint64_t* d_out_b, uint32_t out_stride, cudaStream_t s);
+}  // namespace cbs

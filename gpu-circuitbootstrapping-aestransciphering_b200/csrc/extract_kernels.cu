@@ -1,0 +1,148 @@
+// extract_kernels.cu -- sample extraction + LWE key switch, and the AES state glue kernels.
+//
+// k_extract_keyswitch follows the contract of examples/aes_gpu_ks.cuh:538-607
+// (kernel_SampleExtractKeySwitchToLWE): for output bit t, extract coefficient idx of RLWE
+// word w (a'_j = a[idx-j], or -a[N+idx-j]), switch each coefficient Q -> qKS with the same
+// FP64 round-to-nearest expression (aes_gpu_ks.cuh:388-394), key-switch N -> n with two
+// base-2^k digits against the u16 key, and map qKS -> q (exact scale, or round-half-up
+// division when q is not a multiple of qKS, aes_gpu_ks.cuh:431-440).  One CTA per
+// (bit, 256-wide slice of the n+1 outputs); the mod-switched mask is staged through shared
+// memory 256 coefficients at a time; consecutive threads read consecutive key words.
+#include "common.cuh"
+#include "extract_kernels.cuh"
+
+namespace cbs {
+
+__device__ __forceinline__ uint32_t ms_pow2(uint64_t v, double q_over_Q, uint32_t mask) {
+    return static_cast<uint32_t>(__double2uint_rn(static_cast<double>(v) * q_over_Q)) & mask;
+}
+
+__device__ __forceinline__ uint64_t qks_to_q(uint32_t v, uint64_t scale, uint32_t qks, uint64_t q) {
+    if (scale) return static_cast<uint64_t>(v) * scale;
+    const unsigned __int128 x = static_cast<unsigned __int128>(v) * q + (qks >> 1);
+    return static_cast<uint64_t>(x / qks);
+}
+
+__global__ void __launch_bounds__(256) k_extract_keyswitch(const ExtractArgs a) {
+    const uint32_t t = blockIdx.y;
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t outlen = a.n + 1;
+    const uint32_t info = __ldg(a.info + t);
+    const uint32_t word = info >> 16, idx = info & 0xFFFFu;
+    const uint64_t* aw = a.words + static_cast<size_t>(word) * 2 * a.N;
+    const uint64_t* bw = aw + a.N;
+    const bool active = k < outlen;
+    uint32_t acc = 0;
+    if (active && k == a.n) acc = ms_pow2(bw[idx], a.q_over_Q, a.mask);
+
+    const uint32_t bmask = a.base_ks - 1;
+    const size_t stride_i = static_cast<size_t>(a.base_ks) * outlen;
+    const size_t stride_j = static_cast<size_t>(a.N) * stride_i;
+    __shared__ uint16_t s_a[256];
+    for (uint32_t tile = 0; tile < a.N; tile += 256) {
+        const uint32_t c = tile + threadIdx.x;
+        if (c < a.N) {
+            uint64_t v;
+            if (c <= idx) {
+                v = aw[idx - c];
+            } else {
+                const uint64_t x = aw[a.N + idx - c];
+                v = x ? a.Q - x : 0;
+            }
+            s_a[threadIdx.x] = static_cast<uint16_t>(ms_pow2(v, a.q_over_Q, a.mask));
+        }
+        __syncthreads();
+        if (active) {
+            const uint32_t cnt = min(256u, a.N - tile);
+            const uint16_t* k0 = a.ksk + static_cast<size_t>(tile) * stride_i + k;
+            const uint16_t* k1 = k0 + stride_j;
+#pragma unroll 4
+            for (uint32_t j = 0; j < cnt; ++j) {
+                const uint32_t ai = s_a[j];
+                const uint32_t d0 = ai & bmask, d1 = (ai >> a.base_log2) & bmask;
+                acc -= static_cast<uint32_t>(__ldg(k0 + d0 * outlen)) + static_cast<uint32_t>(__ldg(k1 + d1 * outlen));
+                k0 += stride_i;
+                k1 += stride_i;
+            }
+        }
+        __syncthreads();
+    }
+    if (active) {
+        const uint64_t val = qks_to_q(acc & a.mask, a.scale, a.qks, a.q_lwe);
+        if (k == a.n) a.out_b[t] = val;
+        else a.out_a[static_cast<size_t>(t) * a.out_stride + k] = val;
+    }
+}
+
+cudaError_t launch_extract_keyswitch(const ExtractArgs& a, uint32_t count, cudaStream_t s) {
+    if (count == 0) return cudaSuccess;
+    dim3 grid((a.n + 1 + 255) / 256, count);
+    k_extract_keyswitch<<<grid, 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+// state init (gpu_lut.cuh:430 kernel_InitLWEStateFromRoundKey): bit t of block
+// t/128 = Enc(rk0 bit) + public counter bit * q/2
+__global__ void k_init_state(uint64_t* out_a, uint64_t* out_b, const uint64_t* rk_a, const uint64_t* rk_b,
+                             const uint8_t* bits, uint64_t half, uint64_t q, uint32_t n, uint32_t total) {
+    const size_t tid = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const size_t outlen = n + 1;
+    if (tid >= static_cast<size_t>(total) * outlen) return;
+    const uint32_t t = static_cast<uint32_t>(tid / outlen);
+    const uint32_t k = static_cast<uint32_t>(tid - static_cast<size_t>(t) * outlen);
+    const uint32_t bi = t & 127u;
+    if (k == n) {
+        uint64_t v = rk_b[bi];
+        if (bits[t]) {
+            v += half;
+            if (v >= q) v -= q;
+        }
+        out_b[t] = v;
+    } else {
+        out_a[static_cast<size_t>(t) * n + k] = rk_a[static_cast<size_t>(bi) * n + k];
+    }
+}
+
+cudaError_t launch_init_state(uint64_t* out_a, uint64_t* out_b, const uint64_t* rk_a, const uint64_t* rk_b,
+                              const uint8_t* bits, uint64_t half, uint64_t q, uint32_t n, uint32_t total,
+                              cudaStream_t s) {
+    const size_t work = static_cast<size_t>(total) * (n + 1);
+    if (!work) return cudaSuccess;
+    k_init_state<<<static_cast<unsigned>((work + 255) / 256), 256, 0, s>>>(out_a, out_b, rk_a, rk_b, bits, half, q, n,
+                                                                           total);
+    return cudaGetLastError();
+}
+
+// AES word assembly: out column c of block b = sum over rows of the LUT of byte (row, c+row)
+// plus the round-key word (the reference's fused final add, gpu_lut.cuh:1305-1370, and
+// kernel_RLWE_AddWords4Inplace_Blocks, main.cu:1516-1523).  lut_out [blocks][16][2][N] with
+// LUT index row*4 + col; rk [4][2][N]; words [blocks][4][2][N].  NTT domain throughout.
+__global__ void k_assemble_words(uint64_t* words, const uint64_t* lut_out, const uint64_t* rk, uint64_t Q, uint32_t N,
+                                 uint32_t blocks) {
+    const size_t idx = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const size_t per_block = 4ull * 2 * N;
+    if (idx >= per_block * blocks) return;
+    const uint32_t b = static_cast<uint32_t>(idx / per_block);
+    const size_t rem = idx - static_cast<size_t>(b) * per_block;
+    const uint32_t c = static_cast<uint32_t>(rem / (2ull * N));
+    const size_t pc = rem - static_cast<size_t>(c) * 2 * N;  // poly * N + coeff
+    uint64_t acc = rk[static_cast<size_t>(c) * 2 * N + pc];
+#pragma unroll
+    for (uint32_t row = 0; row < 4; ++row) {
+        const uint32_t col = (c + row) & 3u;
+        const uint64_t v = lut_out[((static_cast<size_t>(b) * 16 + row * 4 + col) * 2) * N + pc];
+        acc += v;
+        if (acc >= Q) acc -= Q;
+    }
+    words[idx] = acc;
+}
+
+cudaError_t launch_assemble_words(uint64_t* words, const uint64_t* lut_out, const uint64_t* rk, uint64_t Q, uint32_t N,
+                                  uint32_t blocks, cudaStream_t s) {
+    const size_t work = static_cast<size_t>(blocks) * 8 * N;
+    if (!work) return cudaSuccess;
+    k_assemble_words<<<static_cast<unsigned>((work + 255) / 256), 256, 0, s>>>(words, lut_out, rk, Q, N, blocks);
+    return cudaGetLastError();
+}
+
+}  // namespace cbs

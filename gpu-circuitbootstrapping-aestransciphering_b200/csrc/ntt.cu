@@ -22,7 +22,7 @@ __global__ void __launch_bounds__(NttPlan<LOGN>::T) k_fnwt(uint64_t* __restrict_
     uint64_t* dst = out + (poly << LOGN);
     ntt_forward_cta<LOGN>(
         sm, threadIdx.x, tw, tws, q, [&](uint32_t i) { return src[i]; },
-        [&](uint32_t i, uint64_t v) { dst[i] = v; });
+        [&](int, uint32_t i, uint64_t v) { dst[i] = v; });
 }
 
 template <int LOGN>
@@ -43,13 +43,13 @@ __global__ void __launch_bounds__(NttPlan<LOGN>::T) k_inwt(uint64_t* __restrict_
     uint64_t* dst = out + (poly << LOGN);
     if (map == nullptr) {
         ntt_inverse_cta<LOGN>(
-            sm, threadIdx.x, itw, itws, ninv, ninv_s, q, [&](uint32_t i) { return src[i]; },
+            sm, threadIdx.x, itw, itws, ninv, ninv_s, q, [&](int, uint32_t i) { return src[i]; },
             [&](uint32_t i, uint64_t v) { dst[i] = v; });
     } else {
         // permute variant (ntt_1d.cu:677-757): slot i reads in[map[i]], negated when map[i] >= N
         ntt_inverse_cta<LOGN>(
             sm, threadIdx.x, itw, itws, ninv, ninv_s, q,
-            [&](uint32_t i) {
+            [&](int, uint32_t i) {
                 uint32_t s = __ldg(map + i);
                 const bool neg = s >= N;
                 s -= neg ? N : 0u;

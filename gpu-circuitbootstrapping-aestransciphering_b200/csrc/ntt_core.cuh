@@ -170,87 +170,113 @@ __device__ __forceinline__ void inv_pass(uint64_t (&x)[8], uint32_t m, uint32_t 
 }
 
 // Forward NTT of one polynomial held by the CTA's first NttPlan::T threads.
-// load(i) supplies input coefficient i (< 4q); store(i, v) receives the fully reduced
-// output at bit-reversed slot i.  sm: N words of shared memory.  The caller must
+// load(i) supplies input coefficient i (< 4q); store(j, i, v) receives the fully reduced
+// output at bit-reversed slot i (register slot j of this thread).  sm: N words of shared memory.  The caller must
 // __syncthreads() before reusing sm.
 template <int LOGN, class Load, class Store>
 __device__ __forceinline__ void ntt_forward_cta(uint64_t* sm, uint32_t tid, const uint64_t* __restrict__ tw,
                                                 const uint64_t* __restrict__ tws, uint64_t q, Load load, Store store) {
     using Pl = NttPlan<LOGN>;
+    static_assert(Pl::P >= 2, "ntt_forward_cta needs N >= 64");
     uint64_t x[8];
+    // first radix-8 pass straight from the loader
 #pragma unroll
-    for (int p = 0; p < Pl::P; ++p) {
+    for (int j = 0; j < 8; ++j) x[j] = load(pass_index<LOGN, 3>(1u, tid, j));
+    fwd_pass<LOGN, 3>(x, 1u, tid, tw, tws, q);
+#pragma unroll
+    for (int j = 0; j < 8; ++j) sm[swz(pass_index<LOGN, 3>(1u, tid, j))] = x[j];
+    __syncthreads();
+    // middle radix-8 passes (kept rolled: lower register pressure inside fused kernels)
+#pragma unroll 1
+    for (int p = 1; p < Pl::P - 1; ++p) {
         const uint32_t m = 1u << (3 * p);
-        constexpr int dummy = 0;
-        (void)dummy;
-        if (p == 0) {
 #pragma unroll
-            for (int j = 0; j < 8; ++j) x[j] = load(pass_index<LOGN, (Pl::P == 1 ? Pl::tail_r : 3)>(m, tid, j));
-        } else if (p < Pl::P - 1) {
+        for (int j = 0; j < 8; ++j) x[j] = sm[swz(pass_index<LOGN, 3>(m, tid, j))];
+        fwd_pass<LOGN, 3>(x, m, tid, tw, tws, q);
 #pragma unroll
-            for (int j = 0; j < 8; ++j) x[j] = sm[swz(pass_index<LOGN, 3>(m, tid, j))];
-        } else {
+        for (int j = 0; j < 8; ++j) sm[swz(pass_index<LOGN, 3>(m, tid, j))] = x[j];
+        __syncthreads();
+    }
+    // tail pass to the store
+    {
+        constexpr uint32_t m = 1u << (3 * (Pl::P - 1));
 #pragma unroll
-            for (int j = 0; j < 8; ++j) x[j] = sm[swz(pass_index<LOGN, Pl::tail_r>(m, tid, j))];
-        }
-        if (p < Pl::P - 1) {
-            fwd_pass<LOGN, 3>(x, m, tid, tw, tws, q);
+        for (int j = 0; j < 8; ++j) x[j] = sm[swz(pass_index<LOGN, Pl::tail_r>(m, tid, j))];
+        fwd_pass<LOGN, Pl::tail_r>(x, m, tid, tw, tws, q);
+        const uint64_t q2 = q << 1;
 #pragma unroll
-            for (int j = 0; j < 8; ++j) sm[swz(pass_index<LOGN, 3>(m, tid, j))] = x[j];
-            __syncthreads();
-        } else {
-            fwd_pass<LOGN, Pl::tail_r>(x, m, tid, tw, tws, q);
-            const uint64_t q2 = q << 1;
-#pragma unroll
-            for (int j = 0; j < 8; ++j) store(pass_index<LOGN, Pl::tail_r>(m, tid, j), csub(csub(x[j], q2), q));
-        }
+        for (int j = 0; j < 8; ++j) store(j, pass_index<LOGN, Pl::tail_r>(m, tid, j), csub(csub(x[j], q2), q));
     }
 }
 
-// Inverse NTT (n^-1 included) of one polynomial; load(i) supplies bit-reversed slot i
-// (< 2q); store(i, v) receives coefficient i fully reduced.
+// Inverse NTT (n^-1 included) of one polynomial; load(j, i) supplies bit-reversed slot i
+// (< 2q) for register slot j; store(i, v) receives coefficient i fully reduced.
 template <int LOGN, class Load, class Store>
 __device__ __forceinline__ void ntt_inverse_cta(uint64_t* sm, uint32_t tid, const uint64_t* __restrict__ itw,
                                                 const uint64_t* __restrict__ itws, uint64_t n_inv, uint64_t n_inv_s,
                                                 uint64_t q, Load load, Store store) {
     using Pl = NttPlan<LOGN>;
+    static_assert(Pl::P >= 2, "ntt_inverse_cta needs N >= 64");
     uint64_t x[8];
+    {
+        constexpr uint32_t m = 1u << (3 * (Pl::P - 1));
 #pragma unroll
-    for (int pp = 0; pp < Pl::P; ++pp) {
-        const int p = Pl::P - 1 - pp;  // pass index in forward numbering
-        const uint32_t m = 1u << (3 * p);
-        if (pp == 0) {
+        for (int j = 0; j < 8; ++j) x[j] = load(j, pass_index<LOGN, Pl::tail_r>(m, tid, j));
+        inv_pass<LOGN, Pl::tail_r>(x, m, tid, itw, itws, q);
 #pragma unroll
-            for (int j = 0; j < 8; ++j) x[j] = load(pass_index<LOGN, Pl::tail_r>(m, tid, j));
-            inv_pass<LOGN, Pl::tail_r>(x, m, tid, itw, itws, q);
-            if (Pl::P > 1) {
-#pragma unroll
-                for (int j = 0; j < 8; ++j) sm[swz(pass_index<LOGN, Pl::tail_r>(m, tid, j))] = x[j];
-                __syncthreads();
-            }
-        } else {
-#pragma unroll
-            for (int j = 0; j < 8; ++j) x[j] = sm[swz(pass_index<LOGN, 3>(m, tid, j))];
-            inv_pass<LOGN, 3>(x, m, tid, itw, itws, q);
-            if (p > 0) {
-#pragma unroll
-                for (int j = 0; j < 8; ++j) sm[swz(pass_index<LOGN, 3>(m, tid, j))] = x[j];
-                __syncthreads();
-            }
-        }
-        if (p == 0) {
-            // last stage (m = 1): x-halves (index < N/2) take n^-1 here, y-halves have it folded
-            // into itw[1]
-            constexpr int RL = (Pl::P == 1) ? Pl::tail_r : 3;
-#pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                const uint32_t idx = pass_index<LOGN, RL>(1u, tid, j);
-                uint64_t v = csub(x[j], q);
-                if (idx < (1u << (LOGN - 1))) v = mul_shoup(v, n_inv, n_inv_s, q);
-                store(idx, v);
-            }
-        }
+        for (int j = 0; j < 8; ++j) sm[swz(pass_index<LOGN, Pl::tail_r>(m, tid, j))] = x[j];
+        __syncthreads();
     }
+#pragma unroll 1
+    for (int p = Pl::P - 2; p >= 1; --p) {
+        const uint32_t m = 1u << (3 * p);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) x[j] = sm[swz(pass_index<LOGN, 3>(m, tid, j))];
+        inv_pass<LOGN, 3>(x, m, tid, itw, itws, q);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) sm[swz(pass_index<LOGN, 3>(m, tid, j))] = x[j];
+        __syncthreads();
+    }
+    // last pass (stages 4, 2, 1): x-halves (index < N/2) take n^-1 here, y-halves have it
+    // folded into itw[1]
+#pragma unroll
+    for (int j = 0; j < 8; ++j) x[j] = sm[swz(pass_index<LOGN, 3>(1u, tid, j))];
+    inv_pass<LOGN, 3>(x, 1u, tid, itw, itws, q);
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        const uint32_t idx = pass_index<LOGN, 3>(1u, tid, j);
+        uint64_t v = csub(x[j], q);
+        if (j < 4) v = mul_shoup(v, n_inv, n_inv_s, q);
+        store(idx, v);
+    }
+}
+
+}  // namespace cbs
+
+namespace cbs {
+
+// Register-resident forms used by the fused kernels.  For N = 1024, 2048, 4096 the last
+// forward pass (and the first inverse pass) gives thread tid the eight consecutive
+// bit-reversed slots 8*tid + j, j = 0..7; these helpers expose them in x[j].
+template <int LOGN>
+__device__ __forceinline__ uint32_t owned_slot(uint32_t tid, int j) {
+    return 8u * tid + static_cast<uint32_t>(j);
+}
+
+template <int LOGN, class Load>
+__device__ __forceinline__ void ntt_forward_to_regs(uint64_t* sm, uint32_t tid, const uint64_t* __restrict__ tw,
+                                                    const uint64_t* __restrict__ tws, uint64_t q, Load load,
+                                                    uint64_t (&out)[8]) {
+    ntt_forward_cta<LOGN>(sm, tid, tw, tws, q, load, [&](int j, uint32_t, uint64_t v) { out[j] = v; });
+}
+
+// Inverse NTT starting from the thread's owned slots in x (values < 2q).
+template <int LOGN, class Store>
+__device__ __forceinline__ void ntt_inverse_from_regs(uint64_t* sm, uint32_t tid, const uint64_t* __restrict__ itw,
+                                                      const uint64_t* __restrict__ itws, uint64_t n_inv,
+                                                      uint64_t n_inv_s, uint64_t q, const uint64_t (&x)[8],
+                                                      Store store) {
+    ntt_inverse_cta<LOGN>(sm, tid, itw, itws, n_inv, n_inv_s, q, [&](int j, uint32_t) { return x[j]; }, store);
 }
 
 }  // namespace cbs

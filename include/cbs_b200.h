@@ -88,6 +88,137 @@ cbs_status cbs_ntt_tables_host(uint32_t dim, uint64_t q, uint64_t *h_twiddles, u
 /* Host helper: NTT-friendly primes, Phantom's search (src/host/numth.cu:207 get_primes). */
 cbs_status cbs_get_primes(uint32_t ntt_size, int bit_size, uint32_t count, uint64_t *h_out);
 
+
+/* ------------------------------------------------------------------------------------
+ * Circuit bootstrapping context (replaces GPUCirBTSContext, bitwise/include/cirbts/
+ * cirbts.cuh:31-500, and the OpenFHE CirBTS parameter / key objects it is built from).
+ * ------------------------------------------------------------------------------------ */
+
+typedef struct {
+    uint32_t N;          /* RLWE ring dimension: 1024, 2048 or 4096 */
+    uint64_t Q;          /* RLWE modulus: prime, Q = 1 mod 2N, Q < 2^62 */
+    uint32_t n;          /* LWE dimension (blind-rotation steps) */
+    uint64_t q_lwe;      /* LWE modulus of CBS inputs and key-switch outputs */
+    uint32_t base_g;     /* blind-rotation gadget base (power of two), digitsG */
+    uint32_t digits_g;
+    uint32_t num_lut;    /* digitsCC: RGSW levels produced per bit (multi-value LUT count) */
+    uint32_t base_cc;    /* RGSW / CMux gadget base (power of two) */
+    uint32_t base_ht;    /* HomTrace key-switch gadget */
+    uint32_t digits_ht;
+    uint32_t base_ss;    /* SchemeSwitch gadget */
+    uint32_t digits_ss;
+    uint32_t trace_shift;/* log2 N - trace rounds; 0 = full trace */
+    uint32_t qks;        /* extraction key-switch modulus (power of two, <= 2^16) */
+    uint32_t base_ks;    /* extraction key-switch base (power of two, two digits cover qks) */
+    double sigma_lwe;    /* noise of fresh LWE samples and of the key-switching key */
+    double sigma_rlwe;   /* noise of RLWE / RGSW key material */
+} cbs_params;
+
+typedef struct cbs_context cbs_context;
+
+/* The AES-128 parameter set of this build: N=2048, Q = 54-bit NTT prime, n=630, q=2^14,
+ * BR gadget 2^12 x 3, RGSW out 2^6 x 4 (4 LUT levels), HomTrace 2^9 x 5, SchemeSwitch 2^9 x 5,
+ * extraction KS qKS=2^14, base 2^7 (two digits). */
+cbs_status cbs_params_default(cbs_params *out);
+
+/* replaces GPUCirBTSContext(const CirBTSContext&, uint32_t maxBatchSize) (cirbts.cuh:420)
+ * plus gpu_init_ntt (cirbts-init.cu:867-1302): tables on the current device, scratch for
+ * max_batch LWE inputs. */
+cbs_status cbs_context_create(const cbs_params *params, uint32_t max_batch, cbs_context **out);
+cbs_status cbs_context_destroy(cbs_context *ctx);
+/* the context's compute stream (replaces GPUCirBTSContext::stream(), cirbts.cuh:452) */
+cbs_status cbs_context_stream(const cbs_context *ctx, cbs_stream_t *out);
+
+/* Generate all key material from a seed and upload it (replaces KeyGen, RLWEKeyGen,
+ * CirBTKeyGen, KeySwitchGen at examples/aes_transcipher/main.cu:232-252, and
+ * gpu_init_cirbsk, cirbts-init.cu:200-865). */
+cbs_status cbs_keygen(cbs_context *ctx, uint64_t seed);
+
+/* Export for verification (host buffers, NTT-domain normal form, reference layouts):
+ * any pointer may be NULL.  s_lwe[n], s_rlwe[N]; bsk[n][2*digits_g][2][N];
+ * ht[rounds][digits_ht][2][N]; ss[digits_ss][2][N]; ksk[2][N][base_ks][n+1];
+ * tv[N] (coefficient domain); gpow[num_lut]; maps[rounds][N]. */
+cbs_status cbs_export_keys(const cbs_context *ctx, int32_t *s_lwe, int32_t *s_rlwe, uint64_t *bsk, uint64_t *ht,
+                           uint64_t *ss, uint16_t *ksk, uint64_t *tv, uint64_t *gpow, uint32_t *maps);
+
+/* The same key generation without a device (host buffers as in cbs_export_keys); the keys
+ * of cbs_keygen(ctx, seed) equal those of cbs_generate_keys_host(params, seed). */
+cbs_status cbs_generate_keys_host(const cbs_params *params, uint64_t seed, int32_t *s_lwe, int32_t *s_rlwe,
+                                  uint64_t *bsk, uint64_t *ht, uint64_t *ss, uint16_t *ksk, uint64_t *tv,
+                                  uint64_t *gpow, uint32_t *maps);
+
+/* Device NTT tables of the context (replaces the accessors d_modulus() ... d_n_inv_mod_q_shoup(),
+ * cirbts.cuh:431-455); any pointer may be NULL. */
+cbs_status cbs_context_tables(const cbs_context *ctx, const cbs_dmodulus **d_modulus, const uint64_t **d_twiddles,
+                              const uint64_t **d_twiddles_shoup, const uint64_t **d_itwiddles,
+                              const uint64_t **d_itwiddles_shoup, const uint64_t **d_n_inv,
+                              const uint64_t **d_n_inv_shoup);
+
+/* Blind rotation + finalize + multi-value split for a batch of LWE ciphertexts
+ * (replaces gpu_BootstrapLUT_inplace_batch_device, cirbts-batch.cu:3293-4629, and
+ * kernel_GenMVRLWEs, kernel.cu:7498): d_a [batch][a_stride], d_b [batch] mod q_lwe ->
+ * d_mv [batch][num_lut][2][N] NTT domain. */
+cbs_status cbs_blind_rotate_batch_device(cbs_context *ctx, const uint64_t *d_a, const uint64_t *d_b, uint32_t batch,
+                                         uint32_t a_stride, uint64_t *d_mv, cbs_stream_t stream);
+/* HomTrace + SchemeSwitch for count MV RLWEs (cirbts-batch.cu:1628-1790):
+ * d_mv [count][2][N] -> d_rgsw [count][2][2][N] (row 0 = scheme-switch row, row 1 = trace row). */
+cbs_status cbs_trace_schemeswitch_device(cbs_context *ctx, const uint64_t *d_mv, uint32_t count, uint64_t *d_rgsw,
+                                         cbs_stream_t stream);
+/* Full batched circuit bootstrapping from device LWE (replaces
+ * gpu_CircuitBootstrappingBatchToDeviceFromDeviceLWE, cirbts-batch.cu:1416-1879).
+ * On success *d_rgsw_view points to context-owned [batch][num_lut][2][2][N] (layout
+ * ((row*2+poly)*N + coeff) per bit, rows = 2*num_lut), valid until the next call that
+ * reuses the context scratch (same contract as DeviceRGSWBatchView, cirbts.cuh:406-418). */
+cbs_status cbs_circuit_bootstrap_batch_device(cbs_context *ctx, const uint64_t *d_a, const uint64_t *d_b,
+                                              uint32_t batch, uint32_t a_stride, const uint64_t **d_rgsw_view,
+                                              cbs_stream_t stream);
+
+/* Batched 8->32 CMux LUT (replaces EvalLUT8x32_RLWE_GPU_DeviceCtrl_Batch,
+ * examples/aes_transcipher/gpu_lut.cuh:1783-2214): d_tables [tables][256][2][N] NTT domain,
+ * h_table_of_lut[luts] selects the table, h_ctrl_bits[luts][8] indexes the control bit of
+ * each tree level (bit 0 = LSB) in d_rgsw_all [bits][rgsw_stride]; d_out [luts][2][N]. */
+cbs_status cbs_lut8x32_batch_device(cbs_context *ctx, const uint64_t *d_tables, uint32_t num_tables,
+                                    const uint32_t *h_table_of_lut, const uint64_t *d_rgsw_all, uint32_t num_bits,
+                                    uint64_t rgsw_stride, const uint32_t *h_ctrl_bits, uint32_t luts, uint64_t *d_out,
+                                    cbs_stream_t stream);
+
+/* Sample extract + LWE key switch N->n + modulus switch qKS->q (replaces
+ * ExtractStateBytesToLWEDeviceBatch, examples/aes_transcipher/extract.cuh:283-366, and
+ * kernel_SampleExtractKeySwitchToLWE, aes_gpu_ks.cuh:538-607): d_words [words][2][N]
+ * coefficient domain, h_info[count] = (word << 16) | coefficient; d_out_a [count][out_stride],
+ * d_out_b [count] mod q_lwe. */
+cbs_status cbs_extract_keyswitch_device(cbs_context *ctx, const uint64_t *d_words_coef, uint32_t words,
+                                        const uint32_t *h_info, uint32_t count, uint64_t *d_out_a, uint64_t *d_out_b,
+                                        uint32_t out_stride, cbs_stream_t stream);
+
+/* ------------------------------------------------------------------------------------
+ * Homomorphic AES-128 CTR transciphering (replaces the example's encrypted key material,
+ * BuildEncryptedKeyMaterial key_material.cuh:12-46 + BuildTableRLWE rlwe_tables.cuh:17-24,
+ * and the super-batch driver RunTranscipherBatch, examples/aes_transcipher/main.cu:1318-1619).
+ * Output: per block 128 LWE ciphertexts (mod q_lwe, dimension n) of the AES-128 keystream
+ * bits AES_K(counter), bit t = byte*8 + b (LSB first, byte in FIPS-197 state order).
+ * ------------------------------------------------------------------------------------ */
+
+/* Encrypt the AES material for key[16] under the context's keys (tables Te0..3/Te4_*, the
+ * 11 round-key words, the round-0 key bits). */
+cbs_status cbs_aes128_setup(cbs_context *ctx, const uint8_t *key, uint64_t seed);
+/* Host copies of the encrypted material: tables [8][256][2][N], rk_words [11][4][2][N]
+ * (NTT domain), rk0_a [128][n], rk0_b [128]; any pointer may be NULL. */
+cbs_status cbs_aes128_export_material(const cbs_context *ctx, uint64_t *h_tables, uint64_t *h_rk_words,
+                                      uint64_t *h_rk0_a, uint64_t *h_rk0_b);
+/* Device variant: d_counter_bits [blocks*128] (0/1, bit t = byte*8 + b of each counter
+ * block); d_out_a [blocks*128][n], d_out_b [blocks*128].  use_graphs != 0 replays one
+ * captured CUDA graph per round (captured on the first call for a chunk size). */
+cbs_status cbs_aes128_ctr_transcipher_device(cbs_context *ctx, const uint8_t *d_counter_bits, uint32_t blocks,
+                                             uint64_t *d_out_a, uint64_t *d_out_b, int use_graphs,
+                                             cbs_stream_t stream);
+/* Host-buffer entry point: h_counters [blocks][16] -> h_out_a [blocks*128][n], h_out_b. */
+cbs_status cbs_aes128_ctr_transcipher(cbs_context *ctx, const uint8_t *h_counters, uint32_t blocks,
+                                      uint64_t *h_out_a, uint64_t *h_out_b);
+/* Client-side helper (uses the secret key): decrypt LWE bits (mod q_lwe) to 0/1. */
+cbs_status cbs_lwe_decrypt_bits(const cbs_context *ctx, const uint64_t *h_a, const uint64_t *h_b, uint32_t count,
+                                uint32_t a_stride, uint8_t *h_bits);
+
 #ifdef __cplusplus
 }
 #endif

@@ -457,15 +457,14 @@ void orc_trace_schemeswitch(const orc_cbs_params *p, const orc_cbs_keys *k, cons
     }
 }
 
-void orc_circuit_bootstrap(const orc_cbs_params *p, const orc_cbs_keys *k, const uint64_t *a, const uint64_t *b,
-                           uint32_t batch, uint32_t a_stride, uint64_t *rgsw_out) {
+/* BR + finalize + MV split: kernel.cu:7498-7536 ct_j = acc * X^{-j} (NTT domain) */
+void orc_blind_rotate_mv(const orc_cbs_params *p, const orc_cbs_keys *k, const uint64_t *a, const uint64_t *b,
+                         uint32_t batch, uint32_t a_stride, uint64_t *mv) {
     const uint32_t N = p->N, L = p->num_lut;
     const uint64_t Q = p->Q;
     uint64_t *acc = (uint64_t *)malloc(sizeof(uint64_t) * 2 * N * batch);
     orc_blind_rotate(p, k, a, b, batch, a_stride, acc, 1);
-    /* kernel.cu:7498-7536: ct_j = acc * X^{-j} (NTT domain) */
-    uint64_t *mv = (uint64_t *)malloc(sizeof(uint64_t) * 2 * N * (size_t)batch * L);
-    uint64_t *mono = (uint64_t *)malloc(sizeof(uint64_t) * N * (L > 1 ? L : 1));
+    uint64_t *mono = (uint64_t *)malloc(sizeof(uint64_t) * N * L);
     for (uint32_t j = 0; j < L; ++j) {
         uint64_t *m = mono + (size_t)j * N;
         memset(m, 0, sizeof(uint64_t) * N);
@@ -479,10 +478,16 @@ void orc_circuit_bootstrap(const orc_cbs_params *p, const orc_cbs_keys *k, const
                 for (uint32_t c = 0; c < N; ++c)
                     mv[(((size_t)bi * L + j) * 2 + poly) * N + c] =
                         orc_mulmod(acc[((size_t)bi * 2 + poly) * N + c], mono[(size_t)j * N + c], Q);
-    orc_trace_schemeswitch(p, k, mv, batch * L, rgsw_out);
     free(mono);
-    free(mv);
     free(acc);
+}
+
+void orc_circuit_bootstrap(const orc_cbs_params *p, const orc_cbs_keys *k, const uint64_t *a, const uint64_t *b,
+                           uint32_t batch, uint32_t a_stride, uint64_t *rgsw_out) {
+    uint64_t *mv = (uint64_t *)malloc(sizeof(uint64_t) * 2 * p->N * (size_t)batch * p->num_lut);
+    orc_blind_rotate_mv(p, k, a, b, batch, a_stride, mv);
+    orc_trace_schemeswitch(p, k, mv, batch * p->num_lut, rgsw_out);
+    free(mv);
 }
 
 /* ------------------------------------------------------------------------------------------ */

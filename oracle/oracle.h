@@ -92,6 +92,9 @@ typedef struct {
  * acc_out [batch][2][N] NTT domain. */
 void orc_blind_rotate(const orc_cbs_params *p, const orc_cbs_keys *k, const uint64_t *a, const uint64_t *b,
                       uint32_t batch, uint32_t a_stride, uint64_t *acc_out, int finalize);
+/* BR + finalize + multi-value split (kernel.cu:7498-7536): mv [batch][num_lut][2][N] NTT domain */
+void orc_blind_rotate_mv(const orc_cbs_params *p, const orc_cbs_keys *k, const uint64_t *a, const uint64_t *b,
+                         uint32_t batch, uint32_t a_stride, uint64_t *mv);
 /* cirbts-batch.cu:1416-1879 full CBS: BR -> MV split -> HomTrace -> SchemeSwitch.
  * rgsw_out [batch][num_lut][2][2][N] NTT domain, row (2j+0)=scheme-switch row, (2j+1)=trace row. */
 void orc_circuit_bootstrap(const orc_cbs_params *p, const orc_cbs_keys *k, const uint64_t *a, const uint64_t *b,

@@ -1,0 +1,122 @@
+"""Test-side helpers: oracle structs, encryption/decryption in numpy (test-only, uses the
+secret keys exported by the product) and small utilities shared by the CBS tests."""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from conftest import _U16P, _U32P, _U64P, oracle_tables
+
+
+class OrcParams(ctypes.Structure):
+    _fields_ = [("N", ctypes.c_uint32), ("log_n", ctypes.c_uint32), ("Q", ctypes.c_uint64), ("n", ctypes.c_uint32),
+                ("q_lwe", ctypes.c_uint64), ("base_g", ctypes.c_uint32), ("digits_g", ctypes.c_uint32),
+                ("num_lut", ctypes.c_uint32), ("base_cc", ctypes.c_uint32), ("base_ht", ctypes.c_uint32),
+                ("digits_ht", ctypes.c_uint32), ("base_ss", ctypes.c_uint32), ("digits_ss", ctypes.c_uint32),
+                ("trace_rounds", ctypes.c_uint32)]
+
+
+class OrcKeys(ctypes.Structure):
+    _fields_ = [("rp", ctypes.c_void_p), ("irp", ctypes.c_void_p), ("n_inv", ctypes.c_uint64),
+                ("auto_maps", ctypes.c_void_p), ("tv", ctypes.c_void_p), ("gpow", ctypes.c_void_p),
+                ("bsk", ctypes.c_void_p), ("ht_key", ctypes.c_void_p), ("ss_key", ctypes.c_void_p)]
+
+
+def declare_cbs(oracle) -> None:
+    vp = ctypes.c_void_p
+    u32 = ctypes.c_uint32
+    oracle.orc_blind_rotate.argtypes = [vp, vp, vp, vp, u32, u32, vp, ctypes.c_int]
+    oracle.orc_blind_rotate_mv.argtypes = [vp, vp, vp, vp, u32, u32, vp]
+    oracle.orc_circuit_bootstrap.argtypes = [vp, vp, vp, vp, u32, u32, vp]
+    oracle.orc_trace_schemeswitch.argtypes = [vp, vp, vp, u32, vp]
+    oracle.orc_external_product.argtypes = [vp, vp, vp, u32, ctypes.c_uint64, vp, vp, ctypes.c_uint64, u32, u32]
+    oracle.orc_lut8x32.argtypes = [vp, vp, vp, u32, ctypes.c_uint64, vp, vp, ctypes.c_uint64, u32, u32]
+
+
+class OracleCbs:
+    """Oracle view of one key set (keeps the numpy buffers alive)."""
+
+    def __init__(self, oracle, p, keys: dict):
+        declare_cbs(oracle)
+        self.o, self.p, self.k = oracle, p, keys
+        N = p.N
+        self.rp, self.rps, self.irp, self.irps, self.ninv = oracle_tables(oracle, N, p.Q)
+        self.op = OrcParams(N=N, log_n=N.bit_length() - 1, Q=p.Q, n=p.n, q_lwe=p.q_lwe, base_g=p.base_g,
+                            digits_g=p.digits_g, num_lut=p.num_lut, base_cc=p.base_cc, base_ht=p.base_ht,
+                            digits_ht=p.digits_ht, base_ss=p.base_ss, digits_ss=p.digits_ss,
+                            trace_rounds=N.bit_length() - 1 - p.trace_shift)
+        self.ok = OrcKeys(rp=self.rp.ctypes.data, irp=self.irp.ctypes.data, n_inv=int(self.ninv[0]),
+                          auto_maps=keys["maps"].ctypes.data, tv=keys["tv"].ctypes.data,
+                          gpow=keys["gpow"].ctypes.data, bsk=keys["bsk"].ctypes.data, ht_key=keys["ht"].ctypes.data,
+                          ss_key=keys["ss"].ctypes.data)
+
+    def br_mv(self, a: np.ndarray, b: np.ndarray) -> np.ndarray:
+        batch, stride = a.shape
+        out = np.zeros((batch, self.p.num_lut, 2, self.p.N), np.uint64)
+        self.o.orc_blind_rotate_mv(ctypes.byref(self.op), ctypes.byref(self.ok), a.ctypes.data, b.ctypes.data, batch,
+                                   stride, out.ctypes.data)
+        return out
+
+    def trace_ss(self, mv: np.ndarray) -> np.ndarray:
+        mv = np.ascontiguousarray(mv.reshape(-1, 2, self.p.N))
+        out = np.zeros((mv.shape[0], 2, 2, self.p.N), np.uint64)
+        self.o.orc_trace_schemeswitch(ctypes.byref(self.op), ctypes.byref(self.ok), mv.ctypes.data, mv.shape[0],
+                                      out.ctypes.data)
+        return out
+
+    def lut(self, table: np.ndarray, ctrls: list[np.ndarray]) -> np.ndarray:
+        out = np.zeros((2, self.p.N), np.uint64)
+        ptrs = (ctypes.c_void_p * 8)(*[c.ctypes.data for c in ctrls])
+        self.o.orc_lut8x32(table.ctypes.data, ptrs, out.ctypes.data, self.p.N, self.p.Q, self.rp.ctypes.data,
+                           self.irp.ctypes.data, int(self.ninv[0]), self.p.base_cc, self.p.num_lut)
+        return out
+
+    def extract(self, words_coef: np.ndarray, info: np.ndarray):
+        p = self.p
+        T = len(info)
+        out_a = np.zeros((T, p.n), np.uint64)
+        out_b = np.zeros(T, np.uint64)
+        self.o.orc_extract_keyswitch(np.ascontiguousarray(words_coef, np.uint64), info.astype(np.uint32), T, p.N, p.Q,
+                                     np.ascontiguousarray(self.k["ksk"]), p.n, int(p.base_ks).bit_length() - 1, p.qks,
+                                     p.q_lwe, out_a, out_b, p.n)
+        return out_a, out_b
+
+    # ---- test-only decryption helpers (secret key) ----
+    def phase_coef(self, ct: np.ndarray) -> np.ndarray:
+        """b - a*s of RLWE ct [2][N] (NTT domain) in the coefficient domain, centered."""
+        p = self.p
+        N, Q = p.N, p.Q
+        s = self.k["s_rlwe"].astype(np.int64) % Q
+        s_ntt = s.astype(np.uint64).copy()
+        self.o.orc_ntt_forward(s_ntt, 1, N, Q, self.rp)
+        a = [int(x) for x in ct[0]]
+        b = [int(x) for x in ct[1]]
+        sn = [int(x) for x in s_ntt]
+        ph = np.array([(bb - aa * ss) % Q for aa, bb, ss in zip(a, b, sn)], dtype=np.uint64)
+        self.o.orc_ntt_inverse(ph, 1, N, Q, self.irp, int(self.ninv[0]))
+        v = ph.astype(object)
+        return np.array([int(x) - Q if int(x) > Q // 2 else int(x) for x in v], dtype=object)
+
+    def to_coef(self, poly_ntt: np.ndarray) -> np.ndarray:
+        x = np.ascontiguousarray(poly_ntt, np.uint64).copy()
+        self.o.orc_ntt_inverse(x, 1, self.p.N, self.p.Q, self.irp, int(self.ninv[0]))
+        return x
+
+
+def lwe_encrypt_bits(rng: np.random.Generator, s_lwe: np.ndarray, bits, q: int, sigma: float = 0.5):
+    bits = np.asarray(bits)
+    n = len(s_lwe)
+    a = rng.integers(0, q, size=(len(bits), n), dtype=np.uint64)
+    e = np.rint(rng.normal(0, sigma, size=len(bits))).astype(np.int64)
+    dot = (a.astype(object) * s_lwe.astype(object)).sum(axis=1)
+    b = np.array([(int(d) + int(m) * (q // 2) + int(ee)) % q for d, m, ee in zip(dot, bits, e)], dtype=np.uint64)
+    return a, b
+
+
+def lwe_decrypt_bits(s_lwe: np.ndarray, a: np.ndarray, b: np.ndarray, q: int):
+    dot = (a.astype(object) * s_lwe.astype(object)).sum(axis=1)
+    ph = [(int(bb) - int(d)) % q for bb, d in zip(b, dot)]
+    bits = np.array([((2 * x + q // 2) // q) & 1 for x in ph], dtype=np.uint8)
+    err = [min(abs(x - (q // 2) * int(bt)), q - abs(x - (q // 2) * int(bt))) for x, bt in zip(ph, bits)]
+    return bits, err
