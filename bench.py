@@ -1,6 +1,6 @@
 """Benchmark: homomorphic AES-128 CTR transciphering throughput (blocks/s) on B200.
 
-Workload (the BASELINE AES-128 configuration): a batch of `--blocks` random 128-bit
+Workload (AES-128 transciphering, batches of 16, 128 or 1024 blocks): `--blocks` random 128-bit
 counter blocks per GPU (default 128; the configuration also names 16 and 1024), key =
 128 uniform bits from a seed, full 10-round homomorphic AES via circuit bootstrapping
 (blind rotation + HomTrace + SchemeSwitch), 16 CMux T-table LUTs per block-round and
