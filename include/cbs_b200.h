@@ -219,6 +219,27 @@ cbs_status cbs_aes128_ctr_transcipher(cbs_context *ctx, const uint8_t *h_counter
 cbs_status cbs_lwe_decrypt_bits(const cbs_context *ctx, const uint64_t *h_a, const uint64_t *h_b, uint32_t count,
                                 uint32_t a_stride, uint8_t *h_bits);
 
+/* ------------------------------------------------------------------------------------
+ * Circuit bootstrapping without device allocation.  No counterpart in the reference.
+ * For callers that cannot call cudaMalloc when they bootstrap: code inside a stream-capture
+ * region (an allocation there breaks the capture), latency-bound serving loops (cudaMalloc /
+ * cudaFree may synchronize the device), and components whose device memory belongs to
+ * another allocator.  Same result as cbs_circuit_bootstrap_batch_device, but the caller
+ * passes the output (d_rgsw_out [batch][num_lut][2][2][N]) and the blind-rotation ->
+ * HomTrace hand-off lives in a fixed file-scope device array of
+ * cbs_circuit_bootstrap_noalloc_capacity_words() 64-bit words (4 MiB; every GPU that loads
+ * the library holds it until exit).  Batches with batch * num_lut * 2 * N above that are
+ * rejected with CBS_ERR_SHAPE_MISMATCH (32 bits at N = 2048, num_lut = 4).  The first call
+ * on a device looks up the array's device address (cudaGetSymbolAddress) and caches it:
+ * make that first call before any stream capture.  All calls share the one array and it
+ * keeps the last call's contents, so calls whose work overlaps on the GPU (different
+ * streams or contexts in flight at once) race; serialize them.  The context itself must
+ * already exist with its keys (cbs_context_create / cbs_keygen allocate). */
+size_t cbs_circuit_bootstrap_noalloc_capacity_words(void);
+cbs_status cbs_circuit_bootstrap_batch_device_noalloc(cbs_context *ctx, const uint64_t *d_a, const uint64_t *d_b,
+                                                      uint32_t batch, uint32_t a_stride, uint64_t *d_rgsw_out,
+                                                      cbs_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif
