@@ -32,7 +32,8 @@ import numpy as np
 
 ROOT = Path(__file__).resolve().parent
 PKG_DIR = ROOT / "gpu-circuitbootstrapping-aestransciphering_b200"
-METRIC = "AES-128 CTR transciphering blocks/s (1 B200, exact-NTT circuit bootstrapping)"
+METRICS = {"fft64": "AES-128 CTR transciphering blocks/s (1 B200, FP64-FFT circuit bootstrapping)",
+           "ntt": "AES-128 CTR transciphering blocks/s (1 B200, exact-NTT circuit bootstrapping)"}
 UNIT = "blocks/s"
 ROUNDS = 10
 
@@ -131,6 +132,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     blocks = args.blocks
     ctx = pkg.Context(max_batch=128 * min(blocks, 256))
     ctx.keygen(args.seed)
+    pkg.call("cbs_context_set_br_backend", ctx.handle, pkg.BR_FFT64 if args.backend == "fft64" else pkg.BR_NTT)
     key = np.random.default_rng(args.seed).bytes(16)
     pkg.call("cbs_aes128_setup", ctx.handle, key, args.seed + 1)
     p = ctx.params
@@ -192,9 +194,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     torch.cuda.synchronize()
     br_ms = e0.elapsed_time(e1) / reps
     N, n, l2, L = p.N, p.n, 2 * p.digits_g, p.num_lut
-    logn = N.bit_length() - 1
     alg_bytes = n * l2 * 2 * N * 8 + T * ((n + 1) * 8 + L * 2 * N * 8)  # key once + LWE in + MV out
-    modmuls = T * n * (8 * (N // 2) * logn + 2 * l2 * N)  # butterflies + MAC products per launch
     peaks = measured_peaks()
     achieved_gbs = alg_bytes / (br_ms * 1e-3) / 1e9
 
@@ -219,7 +219,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     chunks = -(-blocks // 256)
     launches_per_step = chunks * (1 + ROUNDS * 13)
     result = {
-        "metric": METRIC,
+        "metric": METRICS[args.backend],
         "value": world * blocks / (ms_per_step * 1e-3),
         "unit": UNIT,
         "n_gpus": world,
@@ -229,7 +229,8 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "u64 (exact mod-Q NTT arithmetic)",
+        "dtype": "f64 (blind-rotation FFT products) + u64 (exact mod-Q NTT elsewhere)" if args.backend == "fft64"
+                 else "u64 (exact mod-Q NTT arithmetic)",
         "data": "synthetic (seeded random counters and key)",
         "config": {"workload": "aes128_ctr_transcipher", "blocks_per_gpu": blocks, "global_blocks": world * blocks,
                    "params": "N=2048 Q=54-bit n=630 q=2^14 BR 2^12x3 RGSW 2^6x4 HT 2^9x5 SS 2^9x5 KS 2^14/2^7",
@@ -240,13 +241,13 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
         "gpu_launches": launches_per_step * args.steps,
         "e2e": {"value": world * blocks / float(te.item()), "unit": UNIT, "h2d_bytes_per_step": blocks * 128,
                 "d2h_bytes_per_step": blocks * 128 * (p.n + 1) * 8, "correct_blocks": e2e_ok},
-        "roofline": {"kernel": "k_blind_rotate (fused GINX blind rotation + finalize + MV split)", "bound": "hbm",
+        "roofline": {"kernel": ("k_blind_rotate_fft" if args.backend == "fft64" else "k_blind_rotate")
+                     + " (fused GINX blind rotation + finalize + MV split)", "bound": "hbm",
                      "achieved": achieved_gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                      "frac": achieved_gbs / peaks["hbm_gbs"], "peak_src": peaks["src"], "traffic": None,
                      "algorithmic_bytes_per_launch": alg_bytes, "launch_ms": br_ms,
-                     "note": "compute-bound on 64-bit modular multiplies; see modmul_rate"},
-        "modmul_rate": {"kernel": "k_blind_rotate", "modmul_per_launch": modmuls,
-                        "achieved_gmodmul_s": modmuls / (br_ms * 1e-3) / 1e9},
+                     "note": "compute-bound (integer multiplies for ntt, FP64 pipe for fft64); see compute_rate"},
+        "compute_rate": compute_rate(args.backend, T, p, br_ms),
         "clocks": clk.summary(),
     }
     if rank == 0 and args.cpu_baseline:
@@ -254,6 +255,190 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     if rank == 0:
         print(json.dumps(result), flush=True)
     ctx.close()
+
+
+def _timed(torch, stream, fn, warmup: int, steps: int) -> float:
+    """Average device milliseconds of fn over `steps` launches on `stream` after `warmup`."""
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def run_blind_rotate(args, rank: int, world: int, local_rank: int) -> None:
+    """Blind rotation alone (the dominant kernel) over `--batch` random LWE ciphertexts: the
+    profiling case for the fused blind-rotation kernel."""
+    import torch
+    torch.cuda.set_device(local_rank)
+    pkg = load_pkg()
+    T = args.batch or 2368
+    ctx = pkg.Context(max_batch=T)
+    ctx.keygen(args.seed)
+    pkg.call("cbs_context_set_br_backend", ctx.handle, pkg.BR_FFT64 if args.backend == "fft64" else pkg.BR_NTT)
+    p = ctx.params
+    rng = np.random.default_rng(args.seed + rank)
+    a = torch.from_numpy(rng.integers(0, p.q_lwe, size=(T, p.n), dtype=np.int64)).cuda()
+    b = torch.from_numpy(rng.integers(0, p.q_lwe, size=T, dtype=np.int64)).cuda()
+    mv = torch.empty((T, p.num_lut, 2, p.N), dtype=torch.int64, device="cuda")
+    stream = torch.cuda.Stream()
+    fn = lambda: pkg.call("cbs_blind_rotate_batch_device", ctx.handle, a.data_ptr(), b.data_ptr(), T, p.n,  # noqa: E731
+                          mv.data_ptr(), stream.cuda_stream)
+    with ClockSampler(local_rank) as clk:
+        ms = _timed(torch, stream, fn, args.warmup, args.steps)
+    N, n, l2, L = p.N, p.n, 2 * p.digits_g, p.num_lut
+    alg_bytes = n * l2 * 2 * N * 8 + T * ((n + 1) * 8 + L * 2 * N * 8)
+    peaks = measured_peaks()
+    gbs = alg_bytes / (ms * 1e-3) / 1e9
+    out = {"metric": f"blind rotations/s ({args.backend}, N={N}, n={n})", "value": world * T / (ms * 1e-3),
+           "unit": "bootstraps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f64" if args.backend == "fft64" else "u64", "data": "synthetic (seeded random LWE)",
+           "config": {"workload": "blind_rotate", "batch": T, "backend": args.backend,
+                      "l2": "BSK read once per launch (124 MB fft64 / 124 MB ntt); no flush between launches"},
+           "us_per_bootstrap": ms * 1e3 / T, "gpu_launches": args.steps,
+           "roofline": {"kernel": "k_blind_rotate_fft" if args.backend == "fft64" else "k_blind_rotate",
+                        "bound": "hbm", "achieved": gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                        "frac": gbs / peaks["hbm_gbs"], "peak_src": peaks["src"], "traffic": None},
+           "compute_rate": compute_rate(args.backend, T, p, ms), "clocks": clk.summary()}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    ctx.close()
+
+
+def rns_chain(pkg, n: int, size_q: int, size_p: int, bits: int = 50):
+    """Phantom-style chain: size_q + size_p NTT primes of `bits` bits (get_primes order)."""
+    out = np.zeros(size_q + size_p, np.uint64)
+    pkg.call("cbs_get_primes", n, bits, size_q + size_p, out.ctypes.data)
+    return out[:size_q].copy(), out[size_q:].copy()
+
+
+def run_keyswitch(args, rank: int, world: int, local_rank: int) -> None:
+    """Phantom RNS core: hybrid key switching of `--batch` ciphertexts (N = 2^16, 24 primes of
+    50 bits + alpha special primes) per step, inputs resident in HBM."""
+    import torch
+    torch.cuda.set_device(local_rank)
+    pkg = load_pkg()
+    n, size_q, alpha = 1 << 16, 24, args.alpha
+    count = args.batch or 32
+    q, p = rns_chain(pkg, n, size_q, alpha)
+    ctx = pkg.RnsContext(n, q, p)
+    chain = np.concatenate([q, p])
+    beta = ctx.beta(size_q)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(args.seed + rank)
+
+    def rand_limbs(lead, mods):
+        t = torch.randint(0, 2 ** 62, lead + (len(mods), n), dtype=torch.int64, device="cuda", generator=g)
+        m = torch.from_numpy(np.asarray(mods).view(np.int64)).cuda().view(*([1] * len(lead)), -1, 1)
+        return torch.remainder(t, m).contiguous()
+
+    c2 = rand_limbs((count,), q)
+    ct = rand_limbs((count, 2), q)
+    evk = [rand_limbs((2,), chain) for _ in range(beta)]
+    ptrs = pkg.RnsContext.evk_array([e.data_ptr() for e in evk])
+    pkg.call("cbs_rns_prepare_level", ctx.handle, size_q)
+    stream = torch.cuda.Stream()
+    fn = lambda: pkg.call("cbs_rns_keyswitch_inplace", ctx.handle, ct.data_ptr(), c2.data_ptr(), ptrs, size_q,  # noqa: E731
+                          count, stream.cuda_stream)
+    with ClockSampler(local_rank) as clk:
+        ms = _timed(torch, stream, fn, args.warmup, args.steps)
+    # e2e: c2 from pinned host memory, the switched ciphertext back to the host
+    h_c2 = c2.cpu().pin_memory()
+    h_ct = torch.empty(ct.shape, dtype=torch.int64).pin_memory()
+
+    def e2e():
+        with torch.cuda.stream(stream):
+            c2.copy_(h_c2, non_blocking=True)
+            fn()
+            h_ct.copy_(ct, non_blocking=True)
+
+    e2e_ms = _timed(torch, stream, e2e, 1, max(1, args.steps))
+    N8 = n * 8
+    qlp = size_q + alpha
+    alg = beta * 2 * qlp * N8 + count * (size_q * N8 + 4 * size_q * N8 + 2 * beta * qlp * N8)
+    peaks = measured_peaks()
+    gbs = alg / (ms * 1e-3) / 1e9
+    out = {"metric": f"CKKS hybrid key switches/s (N=2^16, 24+{alpha} primes, dnum={beta})",
+           "value": world * count / (ms * 1e-3), "unit": "keyswitches/s", "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "u64", "data": "synthetic (seeded uniform residues and keys)",
+           "config": {"workload": "keyswitch", "batch": count, "N": n, "size_q": size_q, "size_p": alpha,
+                      "beta": beta, "l2": "working set (evk + t_mod_up) >> 126 MB L2"},
+           "us_per_keyswitch": ms * 1e3 / count, "gpu_launches": args.steps * 11,
+           "e2e": {"value": world * count / (e2e_ms * 1e-3), "unit": "keyswitches/s",
+                   "h2d_bytes_per_step": count * size_q * N8, "d2h_bytes_per_step": count * 2 * size_q * N8},
+           "roofline": {"kernel": "keyswitch_inplace (modup + inner product + moddown)", "bound": "hbm",
+                        "achieved": gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": gbs / peaks["hbm_gbs"],
+                        "peak_src": peaks["src"], "traffic": None, "algorithmic_bytes_per_step": alg},
+           "clocks": clk.summary()}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    ctx.close()
+
+
+def run_rns_ntt(args, rank: int, world: int, local_rank: int) -> None:
+    """Forward + inverse multi-prime NTT over `--batch` ciphertexts x 2 polys x 24 limbs at
+    N = 2^16 (the Phantom-core transform), in place, inputs resident in HBM."""
+    import torch
+    torch.cuda.set_device(local_rank)
+    pkg = load_pkg()
+    n, size_q = 1 << 16, 24
+    count = args.batch or 32
+    q, p = rns_chain(pkg, n, size_q, 2)
+    ctx = pkg.RnsContext(n, q, p)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(args.seed + rank)
+    t = torch.randint(0, 2 ** 62, (count * 2, size_q, n), dtype=torch.int64, device="cuda", generator=g)
+    x = torch.remainder(t, torch.from_numpy(q.view(np.int64)).cuda().view(1, -1, 1)).contiguous()
+    ref = x.clone()
+    stream = torch.cuda.Stream()
+    polys = count * 2
+
+    def fn():
+        pkg.call("cbs_rns_ntt_batched", ctx.handle, x.data_ptr(), polys, size_q * n, size_q, 0, 0, stream.cuda_stream)
+        pkg.call("cbs_rns_ntt_batched", ctx.handle, x.data_ptr(), polys, size_q * n, size_q, 0, 1, stream.cuda_stream)
+
+    with ClockSampler(local_rank) as clk:
+        ms = _timed(torch, stream, fn, args.warmup, args.steps)
+    ok = bool(torch.equal(x, ref))  # forward then inverse is the identity
+    alg = 2 * 2 * polys * size_q * n * 8  # each transform reads and writes every limb once
+    peaks = measured_peaks()
+    gbs = alg / (ms * 1e-3) / 1e9
+    out = {"metric": "RNS NTT forward+inverse limb-polys/s (N=2^16)", "value": world * polys * size_q / (ms * 1e-3),
+           "unit": "limb-polys/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+           "data": "synthetic (seeded uniform residues)",
+           "config": {"workload": "rns_ntt", "ciphertexts": count, "polys": polys, "limbs": size_q, "N": n,
+                      "l2": f"{polys * size_q * n * 8 / 1e9:.2f} GB per transform >> 126 MB L2"},
+           "roundtrip_identity": ok, "gpu_launches": args.steps * 4,
+           "roofline": {"kernel": "k_rns_fwd/inv cols+rows", "bound": "hbm", "achieved": gbs, "peak": peaks["hbm_gbs"],
+                        "unit": "GB/s", "frac": gbs / peaks["hbm_gbs"], "peak_src": peaks["src"], "traffic": None,
+                        "algorithmic_bytes_per_step": alg, "note": "two HBM round trips per transform (2-D)"},
+           "clocks": clk.summary()}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    ctx.close()
+
+
+def compute_rate(backend: str, T: int, p, br_ms: float) -> dict:
+    """Algorithmic arithmetic of one blind-rotation launch over T ciphertexts."""
+    N, n, l2 = p.N, p.n, 2 * p.digits_g
+    logn = N.bit_length() - 1
+    if backend == "fft64":
+        M = N // 2
+        fft_flop = 5 * M * (logn - 1)  # radix-2 complex FFT flop count
+        flop = T * n * ((l2 + 2) * fft_flop + 2 * l2 * M * 8)
+        return {"kernel": "k_blind_rotate_fft", "fp64_flop_per_launch": flop,
+                "achieved_fp64_tflops": flop / (br_ms * 1e-3) / 1e12}
+    modmuls = T * n * (8 * (N // 2) * logn + 2 * l2 * N)
+    return {"kernel": "k_blind_rotate", "modmul_per_launch": modmuls,
+            "achieved_gmodmul_s": modmuls / (br_ms * 1e-3) / 1e9}
 
 
 def cpu_sample(args, pkg) -> dict:
@@ -314,7 +499,7 @@ def run_reference(args, rank: int) -> None:
     value = statistics.median(vals)
     last["value"] = value
     out = {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "impl": "reference", "metric": METRICS[args.backend], "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u64 (exact mod-Q arithmetic, CPU)",
         "data": "synthetic (seeded)",
@@ -335,7 +520,12 @@ def main() -> None:
     ap.add_argument("--blocks", type=int, default=128)
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--backend", choices=["fft64", "ntt"], default="fft64")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--workload", choices=["aes128", "blind_rotate", "keyswitch", "rns_ntt"], default="aes128",
+                    help="aes128 is the headline; the others time one kernel family")
+    ap.add_argument("--batch", type=int, default=0, help="units per step for the kernel workloads")
+    ap.add_argument("--alpha", type=int, default=2, help="special primes (digit width) for --workload keyswitch")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -350,8 +540,10 @@ def main() -> None:
         import torch.distributed as dist
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    runner = {"aes128": run_ours, "blind_rotate": run_blind_rotate, "keyswitch": run_keyswitch,
+              "rns_ntt": run_rns_ntt}[args.workload]
     try:
-        run_ours(args, rank, world, local_rank)
+        runner(args, rank, world, local_rank)
     finally:
         if world > 1:
             import torch.distributed as dist

@@ -22,6 +22,8 @@ c_u64p = ctypes.POINTER(ctypes.c_uint64)
 c_u32p = ctypes.POINTER(ctypes.c_uint32)
 c_vp = ctypes.c_void_p
 
+BR_NTT, BR_FFT64 = 0, 1
+
 CBS_STATUS = {
     0: "CBS_OK", 1: "CBS_ERR_INVALID_ARG", 2: "CBS_ERR_SHAPE_MISMATCH", 3: "CBS_ERR_OOM",
     4: "CBS_ERR_CUDA", 5: "CBS_ERR_DEVICE_TIMEOUT", 6: "CBS_ERR_UNSUPPORTED", 7: "CBS_ERR_NOT_READY",
@@ -78,6 +80,7 @@ def _declare(lib: ctypes.CDLL) -> None:
         "cbs_context_destroy": (st, [c_vp]),
         "cbs_context_stream": (st, [c_vp, c_vp]),
         "cbs_keygen": (st, [c_vp, u64]),
+        "cbs_context_set_br_backend": (st, [c_vp, ctypes.c_int]),
         "cbs_export_keys": (st, [c_vp] + [c_vp] * 9),
         "cbs_generate_keys_host": (st, [c_vp, u64] + [c_vp] * 9),
         "cbs_context_tables": (st, [c_vp] + [c_vp] * 7),
@@ -93,6 +96,17 @@ def _declare(lib: ctypes.CDLL) -> None:
         "cbs_lwe_decrypt_bits": (st, [c_vp, c_vp, c_vp, u32, u32, c_vp]),
         "cbs_circuit_bootstrap_noalloc_capacity_words": (sz, []),
         "cbs_circuit_bootstrap_batch_device_noalloc": (st, [c_vp, c_vp, c_vp, u32, u32, c_vp, c_vp]),
+        "cbs_rns_context_create": (st, [u32, c_vp, u32, c_vp, u32, c_vp]),
+        "cbs_rns_context_destroy": (st, [c_vp]),
+        "cbs_rns_context_tables": (st, [c_vp, c_vp]),
+        "cbs_rns_prepare_level": (st, [c_vp, u32]),
+        "cbs_nwt_2d_radix8_forward_inplace": (st, [c_vp, c_vp, u32, u32, c_vp]),
+        "cbs_nwt_2d_radix8_backward_inplace": (st, [c_vp, c_vp, u32, u32, c_vp]),
+        "cbs_rns_ntt_batched": (st, [c_vp, c_vp, u32, u64, u32, u32, ctypes.c_int, c_vp]),
+        "cbs_rns_modup": (st, [c_vp, c_vp, c_vp, u32, u32, c_vp]),
+        "cbs_rns_key_switch_inner_prod": (st, [c_vp, c_vp, c_vp, c_vp, u32, u32, c_vp]),
+        "cbs_rns_moddown_from_ntt": (st, [c_vp, c_vp, c_vp, u32, u32, ctypes.c_int, c_vp]),
+        "cbs_rns_keyswitch_inplace": (st, [c_vp, c_vp, c_vp, c_vp, u32, u32, c_vp]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name, None)
@@ -163,6 +177,45 @@ class Context:
         out = key_buffers(self.params)
         call("cbs_export_keys", self._h, *(out[k].ctypes.data for k in KEY_FIELDS))
         return out
+
+
+class RnsContext:
+    """Owning handle of a cbs_rns_context (the PhantomContext counterpart for the NTT and
+    key-switching path).  q / p are the Q-chain and special primes."""
+
+    def __init__(self, poly_degree: int, q, p):
+        import numpy as np
+        self.n = int(poly_degree)
+        self.q = np.ascontiguousarray(q, dtype=np.uint64)
+        self.p = np.ascontiguousarray(p, dtype=np.uint64)
+        self.size_q, self.size_p = len(self.q), len(self.p)
+        self._h = ctypes.c_void_p()
+        call("cbs_rns_context_create", self.n, self.q.ctypes.data, self.size_q, self.p.ctypes.data, self.size_p,
+             ctypes.byref(self._h))
+
+    @property
+    def handle(self) -> int:
+        return self._h.value
+
+    def beta(self, size_ql: int) -> int:
+        return -(-size_ql // self.size_p)
+
+    @staticmethod
+    def evk_array(ptrs):
+        """Host array of device key pointers (one per digit) for the key-switching calls."""
+        arr = (ctypes.c_void_p * len(ptrs))(*ptrs)
+        return arr
+
+    def close(self) -> None:
+        if self._h.value:
+            load().cbs_rns_context_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 KEY_FIELDS = ("s_lwe", "s_rlwe", "bsk", "ht", "ss", "ksk", "tv", "gpow", "maps")

@@ -34,16 +34,6 @@ __device__ __forceinline__ uint64_t digit_mod(uint64_t x, const Gadget& g, uint3
     return signed_to_mod(r, g.q);
 }
 
-// kernel.cu:7316-7326 device_SpecialMS_IndexPos (same FP64 expression and rounding)
-__device__ __forceinline__ uint32_t special_ms(uint64_t v, uint32_t two_n, uint64_t q, uint32_t bitwidth) {
-    const uint64_t shift = (bitwidth < 63u) ? (1ull << bitwidth) : 0ull;
-    if (shift == 0ull || two_n == 0u || q == 0) return 0u;
-    const double scale = static_cast<double>(two_n) / (static_cast<double>(q) * static_cast<double>(shift));
-    const double x = static_cast<double>(v) * scale;
-    const uint64_t r = __double2ull_rd(x + 0.5);
-    return static_cast<uint32_t>((r * shift) & (static_cast<uint64_t>(two_n) - 1ull));
-}
-
 // coefficient i of X^{-e} p (e in [0, 2N))
 template <uint32_t N>
 __device__ __forceinline__ uint64_t rot_neg(const uint64_t* p, uint32_t e, uint32_t i, uint64_t q) {
@@ -79,7 +69,7 @@ __global__ void __launch_bounds__(NttPlan<LOGN>::T, 256 / NttPlan<LOGN>::T + (Nt
 
     // acc = (0, X^{-b~} * TV)   (kernel.cu:7328-7358)
     {
-        const uint32_t bt = special_ms(a.b[ct], TWO_N, a.q_lwe, a.bitwidth);
+        const uint32_t bt = special_ms_f(a.b[ct], TWO_N, a.q_lwe, a.bitwidth);
         for (uint32_t i = tid; i < N; i += T) {
             acc0[i] = 0;
             acc1[i] = rot_neg<N>(a.tv, bt, i, Q);
@@ -90,7 +80,7 @@ __global__ void __launch_bounds__(NttPlan<LOGN>::T, 256 / NttPlan<LOGN>::T + (Nt
     const uint32_t l2 = 2 * a.digits;
     const uint64_t* arow = a.a + static_cast<size_t>(ct) * a.a_stride;
     for (uint32_t step = 0; step < a.n; ++step) {
-        const uint32_t at = special_ms(__ldg(arow + step), TWO_N, a.q_lwe, a.bitwidth);
+        const uint32_t at = special_ms_f(__ldg(arow + step), TWO_N, a.q_lwe, a.bitwidth);
         const uint64_t* ek = a.bsk + static_cast<size_t>(step) * l2 * 2 * N;
         uint64_t s0[8], s1[8];
 #pragma unroll

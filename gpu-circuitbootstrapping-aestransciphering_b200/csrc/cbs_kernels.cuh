@@ -66,6 +66,17 @@ struct CmuxLevelArgs {
     uint32_t digits;
 };
 
+// bitwise/src/cirbts/kernel.cu:7316-7326 device_SpecialMS_IndexPos (same FP64 expression
+// and rounding): round v * 2N / (q * 2^bw) to an integer, times 2^bw, mod 2N
+__device__ __forceinline__ uint32_t special_ms_f(uint64_t v, uint32_t two_n, uint64_t q, uint32_t bitwidth) {
+    const uint64_t shift = (bitwidth < 63u) ? (1ull << bitwidth) : 0ull;
+    if (shift == 0ull || two_n == 0u || q == 0) return 0u;
+    const double scale = static_cast<double>(two_n) / (static_cast<double>(q) * static_cast<double>(shift));
+    const double x = static_cast<double>(v) * scale;
+    const uint64_t r = __double2ull_rd(x + 0.5);
+    return static_cast<uint32_t>((r * shift) & (static_cast<uint64_t>(two_n) - 1ull));
+}
+
 cudaError_t launch_blind_rotate(const BlindRotateArgs& a, uint32_t N, uint32_t batch, cudaStream_t s);
 cudaError_t launch_trace_schemeswitch(const TraceArgs& a, uint32_t N, uint32_t count, cudaStream_t s);
 cudaError_t launch_cmux_level(const CmuxLevelArgs& a, uint32_t N, uint32_t luts, cudaStream_t s);

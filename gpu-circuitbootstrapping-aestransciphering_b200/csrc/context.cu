@@ -27,6 +27,36 @@ static std::vector<uint64_t> to_mont(const std::vector<uint64_t>& v, const FastM
     return out;
 }
 
+// FFT-domain bootstrapping key and FFT tables for the FP64 backend
+static cbs_status prepare_fft(cbs_context* c) {
+    if (c->fft_ready) return CBS_OK;
+    if (!c->keys_ready) {
+        set_error("FFT backend: no key material (call cbs_keygen first)");
+        return CBS_ERR_NOT_READY;
+    }
+    const size_t polys = c->hk.bsk.size() / c->p.N;
+    std::vector<double2> bskf, tw, twist;
+    keys_to_fft_host(c->tab, c->hk.bsk.data(), polys, bskf);
+    fft_tables_host(c->p.N, tw, twist);
+    std::vector<uint64_t> p2(64), p2s(64);
+    FastMod fm(c->p.Q);
+    uint64_t v = 1 % c->p.Q;
+    for (int e = 0; e < 64; ++e) {
+        p2[e] = v;
+        p2s[e] = host::shoup(v, c->p.Q);
+        v = fm.mul(v, 2);
+    }
+    cudaStream_t s = c->stream;
+    CBS_CUDA_TRY(c->d_bskf.upload(bskf.data(), bskf.size(), s));
+    CBS_CUDA_TRY(c->d_fft_tw.upload(tw.data(), tw.size(), s));
+    CBS_CUDA_TRY(c->d_fft_twist.upload(twist.data(), twist.size(), s));
+    CBS_CUDA_TRY(c->d_pow2.upload(p2.data(), p2.size(), s));
+    CBS_CUDA_TRY(c->d_pow2s.upload(p2s.data(), p2s.size(), s));
+    CBS_CUDA_TRY(cudaStreamSynchronize(s));
+    c->fft_ready = true;
+    return CBS_OK;
+}
+
 cbs_status run_blind_rotate(cbs_context* c, const uint64_t* d_a, const uint64_t* d_b, uint32_t batch,
                             uint32_t a_stride, uint64_t* d_mv, cudaStream_t s) {
     BlindRotateArgs a{};
@@ -44,6 +74,21 @@ cbs_status run_blind_rotate(cbs_context* c, const uint64_t* d_a, const uint64_t*
     a.num_lut = c->p.num_lut;
     a.gadd = c->d_gadd.p;
     a.mv_out = d_mv;
+    if (c->br_backend == CBS_BR_FFT64) {
+        if (!c->fft_ready) {
+            set_error("FFT backend selected but its key material is not prepared");
+            return CBS_ERR_NOT_READY;
+        }
+        FftKeyArgs f{};
+        f.bskf = c->d_bskf.p;
+        f.tw = c->d_fft_tw.p;
+        f.twist = c->d_fft_twist.p;
+        f.pow2 = c->d_pow2.p;
+        f.pow2s = c->d_pow2s.p;
+        f.inv_m = 2.0 / static_cast<double>(c->p.N);
+        CBS_CUDA_TRY(launch_blind_rotate_fft(a, f, c->d_mod.p, c->p.N, batch, s));
+        return CBS_OK;
+    }
     CBS_CUDA_TRY(launch_blind_rotate(a, c->p.N, batch, s));
     return CBS_OK;
 }
@@ -253,6 +298,25 @@ cbs_status cbs_keygen(cbs_context* ctx, uint64_t seed) {
     CBS_CUDA_TRY(cudaStreamSynchronize(s));
     c->keys_ready = true;
     c->aes.ready = false;
+    c->fft_ready = false;
+    if (c->br_backend == CBS_BR_FFT64) return prepare_fft(c);
+    return CBS_OK;
+}
+
+cbs_status cbs_context_set_br_backend(cbs_context* ctx, int backend) {
+    CBS_CHECK_ARG(ctx, "set_br_backend: null context");
+    CBS_CHECK_ARG(backend == CBS_BR_NTT || backend == CBS_BR_FFT64, "set_br_backend: unknown backend");
+    if (backend == CBS_BR_FFT64 && ctx->keys_ready) {
+        if (cbs_status st = prepare_fft(ctx)) return st;
+    }
+    ctx->br_backend = backend;
+    // captured AES round graphs bake in the kernel choice
+    for (auto& g : ctx->aes.graphs)
+        if (g) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+    ctx->aes.graph_chunk = 0;
     return CBS_OK;
 }
 

@@ -10,41 +10,13 @@
 
 #include "../../include/cbs_b200.h"
 #include "cbs_kernels.cuh"
+#include "devbuf.cuh"
 #include "extract_kernels.cuh"
+#include "fft_kernels.cuh"
 #include "host_math.h"
 #include "keygen.h"
 
 namespace cbs {
-
-// owning device buffer (cudaMalloc / cudaFree)
-template <class T>
-struct DevBuf {
-    T* p = nullptr;
-    size_t n = 0;
-    DevBuf() = default;
-    DevBuf(const DevBuf&) = delete;
-    DevBuf& operator=(const DevBuf&) = delete;
-    ~DevBuf() { reset(); }
-    void reset() {
-        if (p) cudaFree(p);
-        p = nullptr;
-        n = 0;
-    }
-    cudaError_t alloc(size_t count) {
-        if (count <= n && p) return cudaSuccess;
-        reset();
-        if (!count) return cudaSuccess;
-        cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&p), count * sizeof(T));
-        if (e == cudaSuccess) n = count;
-        else p = nullptr;
-        return e;
-    }
-    cudaError_t upload(const T* h, size_t count, cudaStream_t s) {
-        cudaError_t e = alloc(count);
-        if (e != cudaSuccess) return e;
-        return cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, s);
-    }
-};
 
 struct AesState {
     bool ready = false;
@@ -87,6 +59,11 @@ struct cbs_context {
     cbs::HostKeys hk;
     cbs::DevBuf<uint64_t> d_tv, d_gadd, d_bsk, d_ht, d_ss;
     cbs::DevBuf<uint16_t> d_ksk;
+    // FP64 FFT blind-rotation backend (built on demand from the keys)
+    int br_backend = 0;  // CBS_BR_NTT or CBS_BR_FFT64
+    bool fft_ready = false;
+    cbs::DevBuf<double2> d_bskf, d_fft_tw, d_fft_twist;
+    cbs::DevBuf<uint64_t> d_pow2, d_pow2s;
     // scratch
     cbs::DevBuf<uint64_t> d_mv, d_rgsw;
     cbs::DevBuf<uint32_t> d_info_scratch, d_lut_sel_scratch, d_ctrl_scratch;

@@ -1,0 +1,364 @@
+// ntt_rns.cu -- multi-prime negacyclic NTT for N = 2^13 .. 2^17 (Phantom's 2-D RNS NTT).
+//
+// Same transform as src/ntt/fntt_2d.cu / intt_2d.cu (nwt_2d_radix8_forward_inplace and
+// nwt_2d_radix8_backward_inplace): per limb a Cooley-Tukey negacyclic NTT with Phantom's
+// bit-reversed twiddle table of that limb's prime, bit-reversed output, n^-1 folded into the
+// last inverse stage; outputs fully reduced, bit-identical.
+//
+// Structure: N = 2^L1 * 2^L2 with L2 = 8.  The first L1 forward stages only mix elements
+// congruent mod 2^L2 ("columns"): stage m, group k of the full transform is stage m, group k
+// of a 2^L1-point transform of column c, twiddle index m + k.  The last L2 stages stay inside
+// rows of 2^L2 consecutive elements: for row R, local stage m and group k use twiddle index
+// m*(2^L1 + R) + k of the full table.  Each phase is one kernel of register-blocked
+// sub-transforms (8 coefficients per thread, radix-8 passes through swizzled shared memory),
+// so a limb crosses HBM twice per transform.  Columns: a CTA takes 16 adjacent columns and
+// its threads interleave columns so every global access is a 128-byte run; rows: 16 rows of
+// 256 contiguous words per CTA.  Intermediate values stay lazy (< 4q forward, < 2q
+// inverse); the second kernel reduces fully.
+#include <atomic>
+
+#include "common.cuh"
+#include "ntt_core.cuh"
+#include "ntt_rns.cuh"
+
+namespace cbs {
+
+// forward pass with an explicit twiddle base: i1 = base + k
+template <int LOGS, int R>
+__device__ __forceinline__ void fwd_pass_b(uint64_t (&x)[8], uint32_t m, uint32_t base, uint32_t tid,
+                                           const uint64_t* __restrict__ tw, const uint64_t* __restrict__ tws,
+                                           uint64_t q) {
+    const uint64_t q2 = q << 1;
+    if (R == 3) {
+        const uint32_t i1 = base + pass_group<LOGS, 3>(m, tid, 0);
+        {
+            const uint64_t w = __ldg(tw + i1), ws = __ldg(tws + i1);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) ct_bf(x[j], x[j + 4], w, ws, q2, q);
+        }
+        {
+            const uint64_t w0 = __ldg(tw + 2 * i1), w0s = __ldg(tws + 2 * i1);
+            const uint64_t w1 = __ldg(tw + 2 * i1 + 1), w1s = __ldg(tws + 2 * i1 + 1);
+            ct_bf(x[0], x[2], w0, w0s, q2, q);
+            ct_bf(x[1], x[3], w0, w0s, q2, q);
+            ct_bf(x[4], x[6], w1, w1s, q2, q);
+            ct_bf(x[5], x[7], w1, w1s, q2, q);
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const uint32_t ti = 4 * i1 + j;
+            ct_bf(x[2 * j], x[2 * j + 1], __ldg(tw + ti), __ldg(tws + ti), q2, q);
+        }
+    } else if (R == 2) {
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const uint32_t i1 = base + pass_group<LOGS, 2>(m, tid, h);
+            const uint64_t w = __ldg(tw + i1), ws = __ldg(tws + i1);
+            uint64_t* v = x + 4 * h;
+            ct_bf(v[0], v[2], w, ws, q2, q);
+            ct_bf(v[1], v[3], w, ws, q2, q);
+            ct_bf(v[0], v[1], __ldg(tw + 2 * i1), __ldg(tws + 2 * i1), q2, q);
+            ct_bf(v[2], v[3], __ldg(tw + 2 * i1 + 1), __ldg(tws + 2 * i1 + 1), q2, q);
+        }
+    } else {
+#pragma unroll
+        for (int h = 0; h < 4; ++h) {
+            const uint32_t i1 = base + pass_group<LOGS, 1>(m, tid, h);
+            ct_bf(x[2 * h], x[2 * h + 1], __ldg(tw + i1), __ldg(tws + i1), q2, q);
+        }
+    }
+}
+
+template <int LOGS, int R>
+__device__ __forceinline__ void inv_pass_b(uint64_t (&x)[8], uint32_t m, uint32_t base, uint32_t tid,
+                                           const uint64_t* __restrict__ tw, const uint64_t* __restrict__ tws,
+                                           uint64_t q) {
+    const uint64_t q2 = q << 1;
+    if (R == 3) {
+        const uint32_t i1 = base + pass_group<LOGS, 3>(m, tid, 0);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const uint32_t ti = 4 * i1 + j;
+            gs_bf(x[2 * j], x[2 * j + 1], __ldg(tw + ti), __ldg(tws + ti), q2, q);
+        }
+        {
+            const uint64_t w0 = __ldg(tw + 2 * i1), w0s = __ldg(tws + 2 * i1);
+            const uint64_t w1 = __ldg(tw + 2 * i1 + 1), w1s = __ldg(tws + 2 * i1 + 1);
+            gs_bf(x[0], x[2], w0, w0s, q2, q);
+            gs_bf(x[1], x[3], w0, w0s, q2, q);
+            gs_bf(x[4], x[6], w1, w1s, q2, q);
+            gs_bf(x[5], x[7], w1, w1s, q2, q);
+        }
+        {
+            const uint64_t w = __ldg(tw + i1), ws = __ldg(tws + i1);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) gs_bf(x[j], x[j + 4], w, ws, q2, q);
+        }
+    } else if (R == 2) {
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const uint32_t i1 = base + pass_group<LOGS, 2>(m, tid, h);
+            uint64_t* v = x + 4 * h;
+            gs_bf(v[0], v[1], __ldg(tw + 2 * i1), __ldg(tws + 2 * i1), q2, q);
+            gs_bf(v[2], v[3], __ldg(tw + 2 * i1 + 1), __ldg(tws + 2 * i1 + 1), q2, q);
+            const uint64_t w = __ldg(tw + i1), ws = __ldg(tws + i1);
+            gs_bf(v[0], v[2], w, ws, q2, q);
+            gs_bf(v[1], v[3], w, ws, q2, q);
+        }
+    } else {
+#pragma unroll
+        for (int h = 0; h < 4; ++h) {
+            const uint32_t i1 = base + pass_group<LOGS, 1>(m, tid, h);
+            gs_bf(x[2 * h], x[2 * h + 1], __ldg(tw + i1), __ldg(tws + i1), q2, q);
+        }
+    }
+}
+
+// 2^LOGS-point forward sub-transform of one group; twb(m) gives the twiddle base of local
+// stage m; load(e), store(e, v) address the group's elements (lazy values)
+template <int LOGS, class TwB, class Load, class Store>
+__device__ __forceinline__ void sub_fwd(uint64_t* sm, uint32_t gt, const uint64_t* __restrict__ tw,
+                                        const uint64_t* __restrict__ tws, uint64_t q, TwB twb, Load load,
+                                        Store store) {
+    using Pl = NttPlan<LOGS>;
+    uint64_t x[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) x[j] = load(pass_index<LOGS, 3>(1u, gt, j));
+    fwd_pass_b<LOGS, 3>(x, 1u, twb(1u), gt, tw, tws, q);
+#pragma unroll 1
+    for (int p = 1; p < Pl::P; ++p) {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) sm[swz(pass_index<LOGS, 3>(1u << (3 * (p - 1)), gt, j))] = x[j];
+        __syncthreads();
+        const uint32_t m = 1u << (3 * p);
+        if (p < Pl::P - 1) {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) x[j] = sm[swz(pass_index<LOGS, 3>(m, gt, j))];
+            fwd_pass_b<LOGS, 3>(x, m, twb(m), gt, tw, tws, q);
+        } else {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) x[j] = sm[swz(pass_index<LOGS, Pl::tail_r>(m, gt, j))];
+            fwd_pass_b<LOGS, Pl::tail_r>(x, m, twb(m), gt, tw, tws, q);
+        }
+    }
+    constexpr uint32_t mt = 1u << (3 * (Pl::P - 1));
+#pragma unroll
+    for (int j = 0; j < 8; ++j) store(pass_index<LOGS, Pl::tail_r>(mt, gt, j), x[j]);
+}
+
+template <int LOGS, class TwB, class Load, class Store>
+__device__ __forceinline__ void sub_inv(uint64_t* sm, uint32_t gt, const uint64_t* __restrict__ tw,
+                                        const uint64_t* __restrict__ tws, uint64_t q, TwB twb, Load load,
+                                        Store store) {
+    using Pl = NttPlan<LOGS>;
+    constexpr uint32_t mt = 1u << (3 * (Pl::P - 1));
+    uint64_t x[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) x[j] = load(pass_index<LOGS, Pl::tail_r>(mt, gt, j));
+    inv_pass_b<LOGS, Pl::tail_r>(x, mt, twb(mt), gt, tw, tws, q);
+#pragma unroll
+    for (int j = 0; j < 8; ++j) sm[swz(pass_index<LOGS, Pl::tail_r>(mt, gt, j))] = x[j];
+    __syncthreads();
+#pragma unroll 1
+    for (int p = Pl::P - 2; p >= 0; --p) {
+        const uint32_t m = 1u << (3 * p);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) x[j] = sm[swz(pass_index<LOGS, 3>(m, gt, j))];
+        inv_pass_b<LOGS, 3>(x, m, twb(m), gt, tw, tws, q);
+        if (p > 0) {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) sm[swz(pass_index<LOGS, 3>(m, gt, j))] = x[j];
+            __syncthreads();
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < 8; ++j) store(pass_index<LOGS, 3>(1u, gt, j), x[j], j);
+}
+
+constexpr int kL2 = 8;            // row stages (rows of 256 words)
+constexpr uint32_t kGroups = 16;  // sub-transforms per CTA
+
+// column groups are padded by one word so the 16 interleaved columns of a warp hit 16
+// different banks
+template <int L1>
+constexpr uint32_t col_stride() {
+    return (1u << L1) + 1;
+}
+
+__device__ __forceinline__ uint64_t* limb_ptr(uint64_t* data, const RnsNttArgs& a, uint32_t limb_flat,
+                                              uint32_t log_n) {
+    const uint32_t poly = limb_flat / a.limbs, limb = limb_flat % a.limbs;
+    const uint32_t slot = a.limb_slot ? a.limb_slot[limb] : limb;
+    return data + static_cast<size_t>(poly) * a.poly_stride + (static_cast<size_t>(slot) << log_n);
+}
+
+// source of the first phase: in (out-of-place) or data
+__device__ __forceinline__ const uint64_t* src_ptr(uint64_t* data, const RnsNttArgs& a, uint32_t limb_flat,
+                                                   uint32_t log_n) {
+    if (!a.in) return limb_ptr(data, a, limb_flat, log_n);
+    const uint32_t poly = limb_flat / a.limbs, limb = limb_flat % a.limbs;
+    const uint32_t slot = a.limb_slot ? a.limb_slot[limb] : limb;
+    return a.in + static_cast<size_t>(poly) * a.in_poly_stride + (static_cast<size_t>(slot) << log_n);
+}
+
+// forward phase 1: columns (2^L1 points each, stride 2^L2), lazy output
+template <int L1>
+__global__ void __launch_bounds__(kGroups * (1 << L1) / 8) k_rns_fwd_cols(uint64_t* __restrict__ data,
+                                                                         const RnsNttArgs a) {
+    constexpr uint32_t ROW = 1u << kL2;
+    extern __shared__ uint64_t sm[];
+    const uint32_t tid = threadIdx.x;
+    const uint32_t g = tid % kGroups, gt = tid / kGroups;  // lanes interleave columns
+    const uint32_t colblk = blockIdx.x % (ROW / kGroups);
+    const uint32_t limb_flat = blockIdx.x / (ROW / kGroups);  // poly * limbs + limb
+    const uint32_t prime = a.limb_prime[limb_flat % a.limbs];
+    const size_t N = size_t(1) << (L1 + kL2);
+    const uint64_t* tw = a.tw + prime * N;
+    const uint64_t* tws = a.tws + prime * N;
+    const uint64_t q = a.q[prime];
+    uint64_t* poly = limb_ptr(data, a, limb_flat, L1 + kL2) + colblk * kGroups + g;
+    const uint64_t* src = src_ptr(data, a, limb_flat, L1 + kL2) + colblk * kGroups + g;
+    sub_fwd<L1>(
+        sm + g * col_stride<L1>(), gt, tw, tws, q, [](uint32_t m) { return m; },
+        [&](uint32_t e) { return src[e * ROW]; }, [&](uint32_t e, uint64_t v) { poly[e * ROW] = v; });
+}
+
+// forward phase 2: rows (256 contiguous words), full reduction, optional moddown epilogue
+template <int L1, int EPI>
+__global__ void __launch_bounds__(kGroups * 32) k_rns_fwd_rows(uint64_t* __restrict__ data, const RnsNttArgs a) {
+    constexpr uint32_t ROW = 1u << kL2, ROWS = 1u << L1;
+    extern __shared__ uint64_t sm[];
+    const uint32_t tid = threadIdx.x;
+    const uint32_t g = tid / 32, gt = tid % 32;
+    const uint32_t rowblk = blockIdx.x % (ROWS / kGroups);
+    const uint32_t limb_flat = blockIdx.x / (ROWS / kGroups);
+    const uint32_t prime = a.limb_prime[limb_flat % a.limbs];
+    const size_t N = size_t(1) << (L1 + kL2);
+    const uint64_t* tw = a.tw + prime * N;
+    const uint64_t* tws = a.tws + prime * N;
+    const uint64_t q = a.q[prime], q2 = q << 1;
+    const uint32_t R = rowblk * kGroups + g;
+    uint64_t* row = limb_ptr(data, a, limb_flat, L1 + kL2) + static_cast<size_t>(R) * ROW;
+    if (EPI == 0) {
+        sub_fwd<kL2>(
+            sm + g * ROW, gt, tw, tws, q, [&](uint32_t m) { return m * (ROWS + R); },
+            [&](uint32_t e) { return row[e]; }, [&](uint32_t e, uint64_t v) { row[e] = csub(csub(v, q2), q); });
+    } else {
+        const uint32_t poly = limb_flat / a.limbs, limb = limb_flat % a.limbs;
+        const size_t off = (static_cast<size_t>(limb) << (L1 + kL2)) + static_cast<size_t>(R) * ROW;
+        const uint64_t* cx = a.epi_cx + poly * a.epi_cx_stride + off;
+        uint64_t* dst = a.epi_dst + poly * a.epi_dst_stride + off;
+        const uint64_t f = a.epi_f[limb], fs = a.epi_fs[limb];
+        sub_fwd<kL2>(
+            sm + g * ROW, gt, tw, tws, q, [&](uint32_t m) { return m * (ROWS + R); },
+            [&](uint32_t e) { return row[e]; },
+            [&](uint32_t e, uint64_t v) {
+                v = csub(csub(v, q2), q);
+                uint64_t r = mul_shoup(sub_mod(cx[e], v, q), f, fs, q);
+                if (EPI == 2) r = add_mod(dst[e], r, q);
+                dst[e] = r;
+            });
+    }
+}
+
+// inverse phase A: rows (lazy output < 2q)
+template <int L1>
+__global__ void __launch_bounds__(kGroups * 32) k_rns_inv_rows(uint64_t* __restrict__ data, const RnsNttArgs a) {
+    constexpr uint32_t ROW = 1u << kL2, ROWS = 1u << L1;
+    extern __shared__ uint64_t sm[];
+    const uint32_t tid = threadIdx.x;
+    const uint32_t g = tid / 32, gt = tid % 32;
+    const uint32_t rowblk = blockIdx.x % (ROWS / kGroups);
+    const uint32_t limb_flat = blockIdx.x / (ROWS / kGroups);
+    const uint32_t prime = a.limb_prime[limb_flat % a.limbs];
+    const size_t N = size_t(1) << (L1 + kL2);
+    const uint64_t* itw = a.itw + prime * N;
+    const uint64_t* itws = a.itws + prime * N;
+    const uint64_t q = a.q[prime];
+    const uint32_t R = rowblk * kGroups + g;
+    uint64_t* row = limb_ptr(data, a, limb_flat, L1 + kL2) + static_cast<size_t>(R) * ROW;
+    const uint64_t* src = src_ptr(data, a, limb_flat, L1 + kL2) + static_cast<size_t>(R) * ROW;
+    sub_inv<kL2>(
+        sm + g * ROW, gt, itw, itws, q, [&](uint32_t m) { return m * (ROWS + R); }, [&](uint32_t e) { return src[e]; },
+        [&](uint32_t e, uint64_t v, int) { row[e] = v; });
+}
+
+// inverse phase B: columns, n^-1 on the x-half of the last stage, full reduction
+template <int L1>
+__global__ void __launch_bounds__(kGroups * (1 << L1) / 8) k_rns_inv_cols(uint64_t* __restrict__ data,
+                                                                         const RnsNttArgs a) {
+    constexpr uint32_t ROW = 1u << kL2;
+    extern __shared__ uint64_t sm[];
+    const uint32_t tid = threadIdx.x;
+    const uint32_t g = tid % kGroups, gt = tid / kGroups;
+    const uint32_t colblk = blockIdx.x % (ROW / kGroups);
+    const uint32_t limb_flat = blockIdx.x / (ROW / kGroups);
+    const uint32_t prime = a.limb_prime[limb_flat % a.limbs];
+    const size_t N = size_t(1) << (L1 + kL2);
+    const uint64_t* itw = a.itw + prime * N;
+    const uint64_t* itws = a.itws + prime * N;
+    const uint64_t q = a.q[prime];
+    const uint64_t ninv = a.n_inv[prime], ninvs = a.n_inv_s[prime];
+    const uint64_t sc = a.scale ? a.scale[limb_flat % a.limbs] : 0;
+    const uint64_t scs = a.scale ? a.scale_s[limb_flat % a.limbs] : 0;
+    uint64_t* poly = limb_ptr(data, a, limb_flat, L1 + kL2) + colblk * kGroups + g;
+    sub_inv<L1>(
+        sm + g * col_stride<L1>(), gt, itw, itws, q, [](uint32_t m) { return m; }, [&](uint32_t e) { return poly[e * ROW]; },
+        [&](uint32_t e, uint64_t v, int j) {
+            v = csub(v, q);
+            if (j < 4) v = mul_shoup(v, ninv, ninvs, q);  // x-half of the m = 1 stage
+            if (sc) v = mul_shoup(v, sc, scs, q);
+            poly[e * ROW] = v;
+        });
+}
+
+template <int L1>
+static cudaError_t rns_launch(uint64_t* data, const RnsNttArgs& a, size_t limb_polys, bool inverse, cudaStream_t s) {
+    constexpr uint32_t ROW = 1u << kL2, ROWS = 1u << L1;
+    constexpr size_t col_smem = kGroups * col_stride<L1>() * sizeof(uint64_t);
+    constexpr size_t row_smem = kGroups * ROW * sizeof(uint64_t);
+    static_assert(col_smem <= 227 * 1024 && row_smem <= 227 * 1024, "shared memory");
+    static std::atomic<uint64_t> attr_set{0};  // opt-in above 48 KB, once per device
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (!(attr_set.load() >> dev & 1)) {
+        cudaError_t e = cudaFuncSetAttribute(k_rns_fwd_cols<L1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             static_cast<int>(col_smem));
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_rns_inv_cols<L1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(col_smem));
+        if (e != cudaSuccess) return e;
+        attr_set.fetch_or(uint64_t(1) << dev);
+    }
+    const size_t col_blocks = limb_polys * (ROW / kGroups), row_blocks = limb_polys * (ROWS / kGroups);
+    if (col_blocks > 0x7fffffffu || row_blocks > 0x7fffffffu) return cudaErrorInvalidValue;
+    const uint32_t col_threads = kGroups * (1u << L1) / 8, row_threads = kGroups * 32;
+    if (!inverse) {
+        k_rns_fwd_cols<L1><<<static_cast<unsigned>(col_blocks), col_threads, col_smem, s>>>(data, a);
+        if (a.epi == 0)
+            k_rns_fwd_rows<L1, 0><<<static_cast<unsigned>(row_blocks), row_threads, row_smem, s>>>(data, a);
+        else if (a.epi == 1)
+            k_rns_fwd_rows<L1, 1><<<static_cast<unsigned>(row_blocks), row_threads, row_smem, s>>>(data, a);
+        else
+            k_rns_fwd_rows<L1, 2><<<static_cast<unsigned>(row_blocks), row_threads, row_smem, s>>>(data, a);
+    } else {
+        k_rns_inv_rows<L1><<<static_cast<unsigned>(row_blocks), row_threads, row_smem, s>>>(data, a);
+        k_rns_inv_cols<L1><<<static_cast<unsigned>(col_blocks), col_threads, col_smem, s>>>(data, a);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t rns_ntt(uint64_t* data, const RnsNttArgs& a, uint32_t log_n, size_t polys, bool inverse, cudaStream_t s) {
+    const size_t limb_polys = polys * a.limbs;
+    if (limb_polys == 0) return cudaSuccess;
+    switch (log_n) {
+        case 13: return rns_launch<5>(data, a, limb_polys, inverse, s);
+        case 14: return rns_launch<6>(data, a, limb_polys, inverse, s);
+        case 15: return rns_launch<7>(data, a, limb_polys, inverse, s);
+        case 16: return rns_launch<8>(data, a, limb_polys, inverse, s);
+        case 17: return rns_launch<9>(data, a, limb_polys, inverse, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace cbs

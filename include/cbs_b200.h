@@ -134,6 +134,14 @@ cbs_status cbs_context_stream(const cbs_context *ctx, cbs_stream_t *out);
  * gpu_init_cirbsk, cirbts-init.cu:200-865). */
 cbs_status cbs_keygen(cbs_context *ctx, uint64_t seed);
 
+/* Blind-rotation external-product backend.  CBS_BR_NTT: exact 64-bit NTT arithmetic mod Q
+ * (bit-identical to the reference's kernels).  CBS_BR_FFT64: FP64 FFT products (the
+ * reference's gate-bootstrap / split-FFT form, bitwise/src/fft.cu:3614-3755); the key
+ * spectra are precomputed from the keys, each product carries a bounded FP64 rounding error
+ * that adds to the blind-rotation noise (the test suite states and checks the bound). */
+enum { CBS_BR_NTT = 0, CBS_BR_FFT64 = 1 };
+cbs_status cbs_context_set_br_backend(cbs_context *ctx, int backend);
+
 /* Export for verification (host buffers, NTT-domain normal form, reference layouts):
  * any pointer may be NULL.  s_lwe[n], s_rlwe[N]; bsk[n][2*digits_g][2][N];
  * ht[rounds][digits_ht][2][N]; ss[digits_ss][2][N]; ksk[2][N][base_ks][n+1];
@@ -239,6 +247,76 @@ size_t cbs_circuit_bootstrap_noalloc_capacity_words(void);
 cbs_status cbs_circuit_bootstrap_batch_device_noalloc(cbs_context *ctx, const uint64_t *d_a, const uint64_t *d_b,
                                                       uint32_t batch, uint32_t a_stride, uint64_t *d_rgsw_out,
                                                       cbs_stream_t stream);
+
+/* ------------------------------------------------------------------------------------
+ * RNS (Phantom) core: multi-prime NTT and hybrid key switching, CKKS form.
+ * Key modulus chain = the size_q primes of Q followed by the size_p special primes P
+ * (every one < 2^60, prime, = 1 mod 2N, distinct); alpha = size_p is the digit width and
+ * a level-l ciphertext (size_ql = l limbs of Q) has beta = ceil(l / alpha) digits.
+ * Layouts (uint64 residues, NTT domain, limb-major):
+ *   c2 [count][size_ql][N]; ciphertext polys ct [count][2][size_ql][N];
+ *   t_mod_up [count][beta][size_ql + size_p][N]; cx [count][2][size_ql + size_p][N];
+ *   evk of digit b: [2][size_q + size_p][N] (component 0 then 1, key-chain limbs).
+ * All outputs are fully reduced and equal to the reference's bit for bit.
+ * ------------------------------------------------------------------------------------ */
+typedef struct cbs_rns_context cbs_rns_context;
+
+/* Device tables of the whole chain with the layout of Phantom's DNTTTable
+ * (include/ntt.cuh:100-160): [size][n] power tables, [size] n^-1, [size] moduli. */
+typedef struct {
+    const uint64_t *twiddle, *twiddle_shoup, *itwiddle, *itwiddle_shoup, *n_inv, *n_inv_shoup;
+    const cbs_dmodulus *modulus;
+    uint32_t n, size;
+} cbs_rns_ntt_tables;
+
+/* replaces PhantomContext(const EncryptionParameters&) for the key-switching path
+ * (include/context.cuh:161; src/context.cu): poly_degree 2^13 .. 2^17, 1 <= size_p <= 16,
+ * size_q + size_p <= 256 */
+cbs_status cbs_rns_context_create(uint32_t poly_degree, const uint64_t *h_q, uint32_t size_q, const uint64_t *h_p,
+                                  uint32_t size_p, cbs_rns_context **out);
+cbs_status cbs_rns_context_destroy(cbs_rns_context *ctx);
+/* replaces PhantomContext::gpu_rns_tables() (include/context.cuh) */
+cbs_status cbs_rns_context_tables(const cbs_rns_context *ctx, cbs_rns_ntt_tables *out);
+/* Builds (once) the modup / moddown constants of level size_ql; the other calls build them on
+ * first use with synchronous copies, so call this first when the later calls are captured
+ * into a CUDA graph.  No reference counterpart (the reference builds every level in the
+ * PhantomContext constructor, src/context.cu). */
+cbs_status cbs_rns_prepare_level(cbs_rns_context *ctx, uint32_t size_ql);
+/* replaces nwt_2d_radix8_forward_inplace / nwt_2d_radix8_backward_inplace (include/ntt.cuh:232,
+ * :262; src/ntt/fntt_2d.cu:620, intt_2d.cu:724): limbs start .. start + size - 1 of the chain,
+ * limb i at d_inout + i * N (d_inout is the base of the whole polynomial, as in the reference) */
+cbs_status cbs_nwt_2d_radix8_forward_inplace(cbs_rns_context *ctx, uint64_t *d_inout, uint32_t coeff_modulus_size,
+                                             uint32_t start_modulus_idx, cbs_stream_t stream);
+cbs_status cbs_nwt_2d_radix8_backward_inplace(cbs_rns_context *ctx, uint64_t *d_inout, uint32_t coeff_modulus_size,
+                                              uint32_t start_modulus_idx, cbs_stream_t stream);
+/* Batched form of the two above: polys polynomials poly_stride words apart, each holding
+ * coeff_modulus_size limbs (chain primes start ..) contiguously from its first word.  No
+ * reference counterpart (the reference loops over polynomials). */
+cbs_status cbs_rns_ntt_batched(cbs_rns_context *ctx, uint64_t *d_data, uint32_t polys, uint64_t poly_stride,
+                               uint32_t coeff_modulus_size, uint32_t start_modulus_idx, int inverse,
+                               cbs_stream_t stream);
+/* replaces DRNSTool::modup (include/rns.cuh:156; src/rns_bconv.cu:530-634), CKKS form, for
+ * count ciphertexts at once: d_c2 [count][size_ql][N] -> d_t_mod_up [count][beta][size_ql+size_p][N] */
+cbs_status cbs_rns_modup(cbs_rns_context *ctx, uint64_t *d_t_mod_up, const uint64_t *d_c2, uint32_t size_ql,
+                         uint32_t count, cbs_stream_t stream);
+/* replaces key_switch_inner_prod_c2_and_evk (src/eval_key_switch.cu:13-68): h_evks is a host
+ * array of beta device pointers (PhantomRelinKey::public_keys_ptr(), one key per digit) */
+cbs_status cbs_rns_key_switch_inner_prod(cbs_rns_context *ctx, uint64_t *d_cx, const uint64_t *d_t_mod_up,
+                                         const uint64_t *const *h_evks, uint32_t size_ql, uint32_t count,
+                                         cbs_stream_t stream);
+/* replaces DRNSTool::moddown_from_NTT (include/rns.cuh:162; src/rns_bconv.cu:776-828), CKKS
+ * form, for polys polynomials: d_cx [polys][size_ql+size_p][N] -> d_ct [polys][size_ql][N];
+ * accumulate != 0 adds the result to d_ct (the add_to_ct step of keyswitch_inplace).  The P
+ * limbs of d_cx are overwritten (scratch), as in the reference. */
+cbs_status cbs_rns_moddown_from_ntt(cbs_rns_context *ctx, uint64_t *d_ct, uint64_t *d_cx, uint32_t size_ql,
+                                    uint32_t polys, int accumulate, cbs_stream_t stream);
+/* replaces keyswitch_inplace(const PhantomContext&, PhantomCiphertext&, uint64_t *c2,
+ * const PhantomRelinKey&, bool, const cudaStream_t&) (include/evaluate.cuh:29;
+ * src/eval_key_switch.cu:94-181), CKKS form, for count ciphertexts: d_ct [count][2][size_ql][N]
+ * += keyswitch(d_c2 [count][size_ql][N]).  Scratch is held by the context. */
+cbs_status cbs_rns_keyswitch_inplace(cbs_rns_context *ctx, uint64_t *d_ct, const uint64_t *d_c2,
+                                     const uint64_t *const *h_evks, uint32_t size_ql, uint32_t count,
+                                     cbs_stream_t stream);
 
 #ifdef __cplusplus
 }

@@ -593,6 +593,181 @@ void orc_extract_keyswitch(const uint64_t *words_coef, const uint32_t *info, uin
 }
 
 /* ------------------------------------------------------------------------------------------ */
+/* Phantom RNS NTT and hybrid key switching                                                    */
+/* ------------------------------------------------------------------------------------------ */
+
+typedef struct {
+    uint64_t *rp, *irp;
+    uint64_t ninv;
+} orc_tab;
+
+static void tab_make(orc_tab *t, uint32_t log_n, uint64_t q) {
+    const uint32_t n = 1u << log_n;
+    t->rp = (uint64_t *)malloc(sizeof(uint64_t) * n);
+    t->irp = (uint64_t *)malloc(sizeof(uint64_t) * n);
+    uint64_t ni[2];
+    orc_ntt_tables(log_n, q, t->rp, NULL, t->irp, NULL, ni);
+    t->ninv = ni[0];
+}
+
+static void tab_free(orc_tab *t) {
+    free(t->rp);
+    free(t->irp);
+}
+
+void orc_rns_ntt(uint64_t *data, size_t polys, uint32_t limbs, uint32_t log_n, const uint64_t *q, int inverse) {
+    const uint32_t n = 1u << log_n;
+    orc_tab *tabs = (orc_tab *)malloc(sizeof(orc_tab) * limbs);
+    for (uint32_t l = 0; l < limbs; ++l) tab_make(&tabs[l], log_n, q[l]);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (long i = 0; i < (long)(polys * limbs); ++i) {
+        const uint32_t l = (uint32_t)(i % limbs);
+        uint64_t *a = data + (size_t)i * n;
+        if (inverse) ntt_inv_one(a, n, q[l], tabs[l].irp, tabs[l].ninv);
+        else ntt_fwd_one(a, n, q[l], tabs[l].rp);
+    }
+    for (uint32_t l = 0; l < limbs; ++l) tab_free(&tabs[l]);
+    free(tabs);
+}
+
+/* fast base conversion out_j = sum_i [x_i * qhat_i^-1]_{q_i} * [qhat_i]_{p_j} mod p_j
+ * (src/rns_bconv.cu:109-210), with the products reduced exactly */
+static void bconv(const uint64_t *x, const uint64_t *ib, uint32_t ni, const uint64_t *ob, uint32_t no,
+                  uint64_t *const *out, uint32_t n) {
+    uint64_t *qhat_inv = (uint64_t *)malloc(sizeof(uint64_t) * ni);
+    uint64_t *qhat_mod = (uint64_t *)malloc(sizeof(uint64_t) * ni * no);
+    for (uint32_t i = 0; i < ni; ++i) {
+        uint64_t prod = 1;
+        for (uint32_t k = 0; k < ni; ++k)
+            if (k != i) prod = orc_mulmod(prod, ib[k] % ib[i], ib[i]);
+        qhat_inv[i] = orc_invmod(prod, ib[i]);
+        for (uint32_t j = 0; j < no; ++j) {
+            uint64_t pm = 1 % ob[j];
+            for (uint32_t k = 0; k < ni; ++k)
+                if (k != i) pm = orc_mulmod(pm, ib[k] % ob[j], ob[j]);
+            qhat_mod[(size_t)j * ni + i] = pm;
+        }
+    }
+#pragma omp parallel for schedule(static)
+    for (long c = 0; c < (long)n; ++c) {
+        uint64_t y[64];
+        for (uint32_t i = 0; i < ni; ++i) y[i] = orc_mulmod(x[(size_t)i * n + c], qhat_inv[i], ib[i]);
+        for (uint32_t j = 0; j < no; ++j) {
+            u128 acc = 0;
+            for (uint32_t i = 0; i < ni; ++i) acc += (u128)y[i] * qhat_mod[(size_t)j * ni + i];
+            out[j][c] = (uint64_t)(acc % ob[j]);
+        }
+    }
+    free(qhat_mod);
+    free(qhat_inv);
+}
+
+void orc_modup(const uint64_t *c2, uint64_t *out, uint32_t log_n, const uint64_t *q, uint32_t size_ql,
+               const uint64_t *p, uint32_t size_p) {
+    const uint32_t n = 1u << log_n, alpha = size_p, qlp = size_ql + size_p;
+    const uint32_t beta = (size_ql + alpha - 1) / alpha;
+    uint64_t *coef = (uint64_t *)malloc(sizeof(uint64_t) * size_ql * n);
+    memcpy(coef, c2, sizeof(uint64_t) * size_ql * n);
+    orc_rns_ntt(coef, 1, size_ql, log_n, q, 1);
+    uint64_t *mods = (uint64_t *)malloc(sizeof(uint64_t) * qlp);
+    for (uint32_t i = 0; i < size_ql; ++i) mods[i] = q[i];
+    for (uint32_t j = 0; j < size_p; ++j) mods[size_ql + j] = p[j];
+    for (uint32_t b = 0; b < beta; ++b) {
+        const uint32_t start = alpha * b, cnt = (b == beta - 1) ? size_ql - alpha * (beta - 1) : alpha;
+        uint64_t *blk = out + (size_t)b * qlp * n;
+        /* own limbs: copied from the NTT-domain input */
+        memcpy(blk + (size_t)start * n, c2 + (size_t)start * n, sizeof(uint64_t) * cnt * n);
+        /* complement limbs: base conversion from the part, then NTT */
+        uint32_t no = 0;
+        uint64_t *ob = (uint64_t *)malloc(sizeof(uint64_t) * qlp);
+        uint64_t **dst = (uint64_t **)malloc(sizeof(uint64_t *) * qlp);
+        for (uint32_t l = 0; l < qlp; ++l)
+            if (l < start || l >= start + cnt) {
+                ob[no] = mods[l];
+                dst[no++] = blk + (size_t)l * n;
+            }
+        bconv(coef + (size_t)start * n, q + start, cnt, ob, no, dst, n);
+        for (uint32_t k = 0; k < no; ++k) {
+            orc_tab t;
+            tab_make(&t, log_n, ob[k]);
+            ntt_fwd_one(dst[k], n, ob[k], t.rp);
+            tab_free(&t);
+        }
+        free(dst);
+        free(ob);
+    }
+    free(mods);
+    free(coef);
+}
+
+void orc_ks_inner(const uint64_t *t, const uint64_t *evk, uint64_t *cx, uint32_t n, const uint64_t *q, uint32_t size_ql,
+                  uint32_t size_q, const uint64_t *p, uint32_t size_p) {
+    const uint32_t alpha = size_p, qlp = size_ql + size_p, qp = size_q + size_p;
+    const uint32_t beta = (size_ql + alpha - 1) / alpha;
+#pragma omp parallel for schedule(static)
+    for (long l = 0; l < (long)qlp; ++l) {
+        const uint64_t m = (l < (long)size_ql) ? q[l] : p[l - size_ql];
+        const uint32_t kl = (l < (long)size_ql) ? (uint32_t)l : size_q + (uint32_t)(l - size_ql);
+        for (uint32_t c = 0; c < n; ++c) {
+            u128 a0 = 0, a1 = 0;
+            for (uint32_t b = 0; b < beta; ++b) {
+                const uint64_t x = t[((size_t)b * qlp + l) * n + c];
+                const uint64_t *ek = evk + (size_t)b * 2 * qp * n;
+                a0 += (u128)x * ek[(size_t)kl * n + c];
+                a1 += (u128)x * ek[(size_t)(qp + kl) * n + c];
+            }
+            cx[(size_t)l * n + c] = (uint64_t)(a0 % m);
+            cx[((size_t)qlp + l) * n + c] = (uint64_t)(a1 % m);
+        }
+    }
+}
+
+void orc_moddown(const uint64_t *cx, uint64_t *ct, uint32_t log_n, const uint64_t *q, uint32_t size_ql,
+                 const uint64_t *p, uint32_t size_p) {
+    const uint32_t n = 1u << log_n;
+    uint64_t *cp = (uint64_t *)malloc(sizeof(uint64_t) * size_p * n);
+    memcpy(cp, cx + (size_t)size_ql * n, sizeof(uint64_t) * size_p * n);
+    orc_rns_ntt(cp, 1, size_p, log_n, p, 1);
+    uint64_t *delta = (uint64_t *)malloc(sizeof(uint64_t) * size_ql * n);
+    uint64_t **dst = (uint64_t **)malloc(sizeof(uint64_t *) * size_ql);
+    for (uint32_t i = 0; i < size_ql; ++i) dst[i] = delta + (size_t)i * n;
+    bconv(cp, p, size_p, q, size_ql, dst, n);
+    orc_rns_ntt(delta, 1, size_ql, log_n, q, 0);
+    for (uint32_t i = 0; i < size_ql; ++i) {
+        uint64_t P = 1;
+        for (uint32_t k = 0; k < size_p; ++k) P = orc_mulmod(P, p[k] % q[i], q[i]);
+        const uint64_t pinv = orc_invmod(P, q[i]);
+        for (uint32_t c = 0; c < n; ++c)
+            ct[(size_t)i * n + c] = orc_mulmod(submod(cx[(size_t)i * n + c], delta[(size_t)i * n + c], q[i]), pinv, q[i]);
+    }
+    free(dst);
+    free(delta);
+    free(cp);
+}
+
+void orc_keyswitch(uint64_t *ct, const uint64_t *c2, const uint64_t *evk, uint32_t log_n, const uint64_t *q,
+                   uint32_t size_ql, uint32_t size_q, const uint64_t *p, uint32_t size_p) {
+    const uint32_t n = 1u << log_n, alpha = size_p, qlp = size_ql + size_p;
+    const uint32_t beta = (size_ql + alpha - 1) / alpha;
+    uint64_t *t = (uint64_t *)malloc(sizeof(uint64_t) * beta * qlp * n);
+    uint64_t *cx = (uint64_t *)malloc(sizeof(uint64_t) * 2 * qlp * n);
+    uint64_t *d = (uint64_t *)malloc(sizeof(uint64_t) * size_ql * n);
+    orc_modup(c2, t, log_n, q, size_ql, p, size_p);
+    orc_ks_inner(t, evk, cx, n, q, size_ql, size_q, p, size_p);
+    for (uint32_t k = 0; k < 2; ++k) {
+        orc_moddown(cx + (size_t)k * qlp * n, d, log_n, q, size_ql, p, size_p);
+        for (uint32_t i = 0; i < size_ql; ++i)
+            for (uint32_t c = 0; c < n; ++c) {
+                uint64_t *dst = ct + ((size_t)k * size_ql + i) * n + c;
+                *dst = addmod(*dst, d[(size_t)i * n + c], q[i]);
+            }
+    }
+    free(d);
+    free(cx);
+    free(t);
+}
+
+/* ------------------------------------------------------------------------------------------ */
 /* plaintext AES-128 (FIPS-197), restating examples/aes_transcipher/aes128.cuh                 */
 /* ------------------------------------------------------------------------------------------ */
 

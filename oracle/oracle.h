@@ -118,6 +118,25 @@ void orc_extract_keyswitch(const uint64_t *words_coef, const uint32_t *info, uin
                            const uint16_t *ksk, uint32_t n, uint32_t base_ks_log2, uint32_t qks, uint64_t q_lwe,
                            uint64_t *out_a, uint64_t *out_b, uint32_t out_stride);
 
+/* ---------------- Phantom RNS NTT and hybrid key switching (CKKS path) ---------------- */
+/* data [polys][limbs][2^log_n]; limb l uses prime q[l] with its Phantom tables
+ * (src/ntt/fntt_2d.cu:620 nwt_2d_radix8_forward_inplace, intt_2d.cu:724 backward) */
+void orc_rns_ntt(uint64_t *data, size_t polys, uint32_t limbs, uint32_t log_n, const uint64_t *q, int inverse);
+/* src/rns_bconv.cu:530-634 DRNSTool::modup (CKKS): c2 [Ql][n] NTT -> out [beta][Ql+P][n] NTT,
+ * alpha = size_p digits of Ql per beta */
+void orc_modup(const uint64_t *c2, uint64_t *out, uint32_t log_n, const uint64_t *q, uint32_t size_ql,
+               const uint64_t *p, uint32_t size_p);
+/* src/eval_key_switch.cu:13-68: t [beta][Ql+P][n], evk [beta][2][Q+P][n] (key limbs: Q chain then P)
+ * -> cx [2][Ql+P][n] */
+void orc_ks_inner(const uint64_t *t, const uint64_t *evk, uint64_t *cx, uint32_t n, const uint64_t *q, uint32_t size_ql,
+                  uint32_t size_q, const uint64_t *p, uint32_t size_p);
+/* src/rns_bconv.cu:776-828 DRNSTool::moddown_from_NTT (CKKS): cx [Ql+P][n] NTT -> ct [Ql][n] NTT */
+void orc_moddown(const uint64_t *cx, uint64_t *ct, uint32_t log_n, const uint64_t *q, uint32_t size_ql,
+                 const uint64_t *p, uint32_t size_p);
+/* src/eval_key_switch.cu:94-181 keyswitch_inplace (CKKS): ct [2][Ql][n] += moddown(inner(modup(c2))) */
+void orc_keyswitch(uint64_t *ct, const uint64_t *c2, const uint64_t *evk, uint32_t log_n, const uint64_t *q,
+                   uint32_t size_ql, uint32_t size_q, const uint64_t *p, uint32_t size_p);
+
 /* ---------------- plaintext AES-128 (examples/aes_transcipher/aes128.cuh) ---------------- */
 void orc_aes128_key_expand(const uint8_t key[16], uint8_t round_keys[11][16]);
 void orc_aes128_encrypt(const uint8_t key[16], const uint8_t in[16], uint8_t out[16]);

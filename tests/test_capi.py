@@ -9,7 +9,7 @@ import json
 import numpy as np
 import pytest
 
-from conftest import GOLDEN, oracle_tables
+from conftest import GOLDEN, oracle_primes, oracle_tables
 
 REF = json.loads((GOLDEN / "reference_host.json").read_text())
 
@@ -64,3 +64,23 @@ def test_argument_validation_without_device(lib):
     assert b"in-place" in lib.cbs_last_error()
     # not enough NTT-friendly primes of 13 bits for N=2048
     assert lib.cbs_get_primes(2048, 13, 5, np.zeros(5, np.uint64).ctypes.data) == 1
+
+
+def test_rns_context_validation_without_device(lib, oracle):
+    """cbs_rns_context_create rejects bad chains before any device call."""
+    n = 1 << 13
+    good = np.array(oracle_primes(oracle, n, 50, 3), np.uint64)
+    h = ctypes.c_void_p()
+
+    def create(deg, q, p):
+        q = np.ascontiguousarray(q, np.uint64)
+        p = np.ascontiguousarray(p, np.uint64)
+        return lib.cbs_rns_context_create(deg, q.ctypes.data, len(q), p.ctypes.data, len(p), ctypes.byref(h))
+
+    assert create(n // 2 * 3, good[:2], good[2:]) == 1          # not a power of two
+    assert create(1 << 12, good[:2], good[2:]) == 1             # below 2^13
+    assert create(n, good[:2], np.array([], np.uint64)) == 1    # no special prime
+    assert create(n, np.array([good[0], good[0]]), good[2:]) == 1  # duplicate
+    assert create(n, np.array([good[0] + 2]), good[2:]) == 1   # not prime / not 1 mod 2N
+    assert create(n, good[:1], np.array(oracle_primes(oracle, n, 50, 20)[3:20], np.uint64)) == 1  # alpha > 16
+    assert h.value is None

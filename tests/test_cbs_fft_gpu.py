@@ -1,0 +1,119 @@
+"""FP64 FFT blind-rotation backend: phase error against the exact integer product (the
+oracle's exact NTT blind rotation), RGSW decryption semantics, and AES end to end."""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import pytest
+
+from cbs_harness import OracleCbs, lwe_decrypt_bits, lwe_encrypt_bits
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+# Tolerance on the blind-rotation output: max |phase(FFT) - phase(exact)| over all
+# coefficients of the accumulator (before the N^-1 finalize scaling).  The FP64 products of
+# 54-bit keys by 12-bit digits over N = 2048 carry ~2^18-2^19 rounding error per coefficient
+# and step; over n = 630 steps the accumulator components drift by ~2^23-2^25, and the
+# phase b - a*s multiplies the a-component drift by the ternary secret (|s|_2 ~ 2^5.2), so
+# the phase error reaches ~2^30-2^31 (measured 2^30.3 on B200).  Downstream, the trace keeps
+# only coefficient 0 of this error in the RGSW rows; propagated through the CMux tree it is
+# ~2^46.6 before extraction, i.e. ~100 at qKS = 2^14 against a decision margin of 4096, so
+# the per-bit failure probability stays far below 2^-40.
+FFT_PHASE_TOL_LOG2 = 33.0
+
+
+def _dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a).view(np.int64)).cuda()
+
+
+@pytest.fixture(scope="module")
+def fctx(pkg):
+    c = pkg.Context(max_batch=64)
+    c.keygen(23)
+    pkg.call("cbs_context_set_br_backend", c.handle, pkg.BR_FFT64)
+    yield c
+    c.close()
+
+
+@pytest.fixture(scope="module")
+def fkeys(fctx):
+    return fctx.export_keys()
+
+
+@pytest.fixture(scope="module")
+def foc(oracle, fctx, fkeys):
+    return OracleCbs(oracle, fctx.params, fkeys)
+
+
+def test_fft_blind_rotate_phase_error_bound(pkg, fctx, fkeys, foc):
+    p = fctx.params
+    rng = np.random.default_rng(77)
+    bits = [0, 1, 1]
+    a, b = lwe_encrypt_bits(rng, fkeys["s_lwe"], bits, p.q_lwe)
+    da, db = _dev(a), _dev(b)
+    mv = torch.zeros((len(bits), p.num_lut, 2, p.N), dtype=torch.int64, device="cuda")
+    pkg.call("cbs_blind_rotate_batch_device", fctx.handle, da.data_ptr(), db.data_ptr(), len(bits), p.n,
+             mv.data_ptr(), None)
+    torch.cuda.synchronize()
+    got = mv.cpu().numpy().view(np.uint64).reshape(len(bits), p.num_lut, 2, p.N)
+    want = foc.br_mv(a, b)
+    Q, N = p.Q, p.N
+    worst = 0
+    for i in range(len(bits)):
+        for j in range(p.num_lut):
+            d = foc.phase_coef(got[i, j]) - foc.phase_coef(want[i, j])
+            # undo the N^-1 finalize scaling, then centre
+            e = [((int(x) * N) % Q) for x in d]
+            e = [x - Q if x > Q // 2 else x for x in e]
+            worst = max(worst, max(abs(x) for x in e))
+    log2 = np.log2(worst + 1)
+    print(f"FFT64 blind rotation: max |phase error| = 2^{log2:.1f} (tolerance 2^{FFT_PHASE_TOL_LOG2})")
+    assert log2 < FFT_PHASE_TOL_LOG2
+
+
+def test_fft_cbs_rgsw_semantics(pkg, fctx, fkeys, foc):
+    p = fctx.params
+    rng = np.random.default_rng(78)
+    bits = [1, 0, 1, 1]
+    a, b = lwe_encrypt_bits(rng, fkeys["s_lwe"], bits, p.q_lwe)
+    da, db = _dev(a), _dev(b)
+    out = torch.zeros(len(bits) * p.num_lut * 4 * p.N, dtype=torch.int64, device="cuda")
+    pkg.call("cbs_circuit_bootstrap_batch_device_noalloc", fctx.handle, da.data_ptr(), db.data_ptr(), len(bits), p.n,
+             out.data_ptr(), None)
+    torch.cuda.synchronize()
+    got = out.cpu().numpy().view(np.uint64).reshape(len(bits), p.num_lut, 2, 2, p.N)
+    g = [int(x) for x in fkeys["gpow"]]
+    s = fkeys["s_rlwe"].astype(object)
+    for i, m in enumerate(bits):
+        for j in range(p.num_lut):
+            ph1 = foc.phase_coef(got[i, j, 1])
+            ph1[0] -= m * g[j]
+            ph0 = foc.phase_coef(got[i, j, 0]) + m * g[j] * s
+            assert max(abs(int(x)) for x in ph1) < g[0] // 2
+            assert max(abs(int(x)) for x in ph0) < g[0] * 2
+
+
+def test_fft_aes128_end_to_end(pkg, fctx, fkeys):
+    from cryptography.hazmat.primitives.ciphers import Cipher, algorithms, modes
+    p = fctx.params
+    key = bytes(range(32, 48))
+    pkg.call("cbs_aes128_setup", fctx.handle, key, 5)
+    blocks = 2
+    rng = np.random.default_rng(9)
+    ctrs = [rng.bytes(16) for _ in range(blocks)]
+    h = np.frombuffer(b"".join(ctrs), np.uint8).copy()
+    oa = np.zeros((blocks * 128, p.n), np.uint64)
+    ob = np.zeros(blocks * 128, np.uint64)
+    pkg.call("cbs_aes128_ctr_transcipher", fctx.handle, h.ctypes.data, blocks, oa.ctypes.data, ob.ctypes.data)
+    got_bits, err = lwe_decrypt_bits(fkeys["s_lwe"], oa, ob, p.q_lwe)
+    enc = Cipher(algorithms.AES(key), modes.ECB()).encryptor()
+    for blk in range(blocks):
+        out = bytes(int(sum(int(got_bits[blk * 128 + i * 8 + b]) << b for b in range(8))) for i in range(16))
+        assert out == enc.update(ctrs[blk])
+    assert max(err) < p.q_lwe // 8
+
+
+def test_backend_switch_validates(pkg, fctx):
+    assert pkg.load().cbs_context_set_br_backend(fctx.handle, 7) == 1
