@@ -23,13 +23,6 @@
 
 namespace cbs {
 
-__device__ __forceinline__ int32_t digit_signed(uint64_t x, const Gadget& g, uint32_t d) {
-    int64_t v = gadget_prepare(x, g);
-    int32_t r = 0;
-    for (uint32_t i = 0; i <= d; ++i) r = peel_digit(v, g.gbits);
-    return r;
-}
-
 // round(v) mod Q for |v| < 2^62 * 2^30 (v is the FP64 result of an integer-valued product)
 __device__ __forceinline__ uint64_t double_to_mod(double v, uint64_t Q, const uint64_t* __restrict__ pow2,
                                                   const uint64_t* __restrict__ pow2s) {
@@ -49,37 +42,55 @@ __device__ __forceinline__ uint64_t double_to_mod(double v, uint64_t Q, const ui
     return (neg && r) ? Q - r : r;
 }
 
-template <uint32_t N, uint32_t T>
-__device__ __forceinline__ void rotate_add_f(uint64_t* acc, const uint64_t* t, uint32_t e, uint32_t tid, uint64_t q) {
-#pragma unroll 4
-    for (uint32_t k = 0; k < N / T; ++k) {
-        const uint32_t i = tid + k * T;
-        const uint32_t s = (i + 2 * N - e) & (2 * N - 1);
-        uint64_t v = (s < N) ? t[s] : t[s - N];
-        if (s >= N) v = v ? q - v : 0;
-        acc[i] = add_mod(acc[i], sub_mod(v, t[i], q), q);
-    }
+// Balanced base-2^gbits digits of the prepared value v, all at once: adding
+// O = sum_k 2^(gbits-1) 2^(gbits k) makes every digit field non-negative, so digit k is field
+// k of v + O minus 2^(gbits-1).  This is the unique balanced representation of v modulo
+// 2^(gbits digits) with digits in [-2^(gbits-1), 2^(gbits-1)), i.e. what peel_digit yields
+// with the final carry dropped.
+__device__ __forceinline__ int32_t balanced_digit(int64_t w, int gbits, uint32_t k) {
+    const uint32_t field = static_cast<uint32_t>(static_cast<uint64_t>(w) >> (gbits * k)) & ((1u << gbits) - 1u);
+    return static_cast<int32_t>(field) - (1 << (gbits - 1));
 }
 
-// Two 128-thread halves per CTA (N = 2048): half h owns accumulator polynomial h.  Per step
-// each half forward-transforms the digits of its polynomial and multiplies them against
-// both key columns; the halves then swap partial sums through shared memory so that half 0
-// holds the full spectrum of output 0 and half 1 that of output 1, inverse-transform them
-// side by side, and all threads rotate-add both outputs.
+__device__ __forceinline__ uint32_t pack_digits(int32_t re, int32_t im) {
+    return (static_cast<uint32_t>(re) & 0xffffu) | (static_cast<uint32_t>(im) << 16);
+}
+
 template <int LOGN>
-__global__ void __launch_bounds__((1 << LOGN) / 8, 2) k_blind_rotate_fft(const BlindRotateArgs a,
-                                                                        const FftKeyArgs f) {
+struct BrFftCfg {
+    static constexpr uint32_t T = (1u << LOGN) / 8;
+    static constexpr int MIN_BLOCKS = LOGN <= 10 ? 4 : (LOGN == 11 ? 2 : 1);
+};
+
+// Two halves of M/8 threads per CTA: half h owns accumulator polynomial h.  Per step:
+//  1. all threads decompose the accumulator (coefficient domain, shared memory) into packed
+//     signed digit pairs (a_e, a_(e+M)) of every digit, stored once in shared memory;
+//  2. half h forward-transforms digit d of polynomial h and multiplies the spectrum against
+//     both key columns of key row 2d + h (keys stored in the order the threads consume them,
+//     so each load is one coalesced 512-byte warp access), accumulating two output spectra;
+//  3. the halves swap partial sums through shared memory (swizzled, conflict-free) so half h
+//     holds the full spectrum of output h and inverse-transforms it into registers;
+//  4. each thread owns the same coefficient positions of acc_h and of output h, so the
+//     rotate-add acc_h += (X^a - 1) t_h is done in place in two phases: acc_h[i] -= t_h[i],
+//     barrier, acc_h[i + a] += t_h[i] (negacyclic wrap); each phase writes every position once.
+template <int LOGN>
+__global__ void __launch_bounds__(BrFftCfg<LOGN>::T, BrFftCfg<LOGN>::MIN_BLOCKS)
+    k_blind_rotate_fft(const BlindRotateArgs a, const FftKeyArgs f) {
     constexpr int LOGM = LOGN - 1;
     constexpr uint32_t N = 1u << LOGN, M = N / 2, TH = M / 8, T = 2 * TH, TWO_N = 2 * N;
     extern __shared__ __align__(16) uint64_t smem[];
-    uint64_t* acc = smem;                                      // [2][N]
-    uint64_t* tb = smem + 2 * N;                               // [2][N]
-    double2* fs = reinterpret_cast<double2*>(smem + 4 * N);    // [2][M]
+    uint64_t* acc = smem;                                       // [2][N]
+    uint32_t* dig = reinterpret_cast<uint32_t*>(smem + 2 * N);  // [2][digits <= 4][M] packed pairs
+    double2* fs = reinterpret_cast<double2*>(smem + 4 * N);     // [2][M]
     const uint32_t ct = blockIdx.x, tid = threadIdx.x;
     const uint32_t h = tid / TH, ht = tid % TH;
     uint64_t* my_acc = acc + h * N;
     double2* my_fs = fs + h * M;
     const uint64_t Q = a.t.q;
+    const uint32_t digits = a.digits;
+    const int gbits = a.g.gbits;
+    int64_t offset = 0;
+    for (uint32_t k = 0; k < digits; ++k) offset += static_cast<int64_t>(1) << (gbits * k + gbits - 1);
 
     {
         const uint32_t bt = special_ms_f(a.b[ct], TWO_N, a.q_lwe, a.bitwidth);
@@ -92,60 +103,87 @@ __global__ void __launch_bounds__((1 << LOGN) / 8, 2) k_blind_rotate_fft(const B
     }
     __syncthreads();
 
-    const uint32_t l2 = 2 * a.digits;
+    const uint32_t l2 = 2 * digits;
     const uint64_t* arow = a.a + static_cast<size_t>(ct) * a.a_stride;
     for (uint32_t step = 0; step < a.n; ++step) {
         const uint32_t at = special_ms_f(__ldg(arow + step), TWO_N, a.q_lwe, a.bitwidth);
-        const double2* ek = f.bskf + static_cast<size_t>(step) * l2 * 2 * M;
+        // 1. digits of both polynomials
+        for (uint32_t idx = tid; idx < 2 * M; idx += T) {
+            const uint32_t p = idx / M, e = idx % M;
+            const int64_t wr = gadget_prepare(acc[p * N + e], a.g) + offset;
+            const int64_t wi = gadget_prepare(acc[p * N + e + M], a.g) + offset;
+            uint32_t* dst = dig + p * digits * M + e;
+            for (uint32_t d = 0; d < digits; ++d)
+                dst[d * M] = pack_digits(balanced_digit(wr, gbits, d), balanced_digit(wi, gbits, d));
+        }
+        __syncthreads();
+        // 2. forward transforms and products
+        const double2* ek = f.bskf + static_cast<size_t>(step) * l2 * 2 * M + ht;
         double2 y0[8], y1[8];
 #pragma unroll
         for (int j = 0; j < 8; ++j) y0[j] = y1[j] = make_double2(0.0, 0.0);
-        for (uint32_t d = 0; d < a.digits; ++d) {
-            const uint32_t r = 2 * d + h;  // key row: digit d of polynomial h
+        for (uint32_t d = 0; d < digits; ++d) {
+            const uint32_t* dsrc = dig + (h * digits + d) * M;
             double2 x[8];
             fft_forward_to_regs<LOGM>(
                 my_fs, ht, f.tw,
                 [&](uint32_t e) {
-                    const double re = static_cast<double>(digit_signed(my_acc[e], a.g, d));
-                    const double im = static_cast<double>(digit_signed(my_acc[e + M], a.g, d));
+                    const uint32_t v = dsrc[e];
+                    const double re = static_cast<double>(static_cast<int16_t>(v & 0xffffu));
+                    const double im = static_cast<double>(static_cast<int16_t>(v >> 16));
                     return cmul(make_double2(re, im), __ldg(f.twist + e));
                 },
                 x);
-            const double2* k0 = ek + static_cast<size_t>(r) * 2 * M + 8 * ht;
+            const double2* k0 = ek + static_cast<size_t>(2 * d + h) * 2 * M;  // key row 2d + h, slot-major
             const double2* k1 = k0 + M;
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
-                cfma(y0[j], x[j], __ldg(k0 + j));
-                cfma(y1[j], x[j], __ldg(k1 + j));
+                cfma(y0[j], x[j], __ldg(k0 + j * TH));
+                cfma(y1[j], x[j], __ldg(k1 + j * TH));
             }
             __syncthreads();
         }
-        // swap partial sums: half 0 keeps output 0, half 1 keeps output 1
-        {
-            double2* give = my_fs + 8 * ht;
+        // 3. swap partial sums: half 0 keeps output 0, half 1 keeps output 1
 #pragma unroll
-            for (int j = 0; j < 8; ++j) give[j] = h ? y0[j] : y1[j];
-            __syncthreads();
-            const double2* take = fs + (1 - h) * M + 8 * ht;
+        for (int j = 0; j < 8; ++j) my_fs[cswz(8 * ht + j)] = h ? y0[j] : y1[j];
+        __syncthreads();
+        {
+            const double2* take = fs + (1 - h) * M;
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
-                const double2 t = take[j];
-                if (h) y1[j] = cadd(y1[j], t);
-                else y0[j] = cadd(y0[j], t);
+                const double2 t = take[cswz(8 * ht + j)];
+                y0[j] = cadd(h ? y1[j] : y0[j], t);
             }
-            __syncthreads();
         }
-        uint64_t* my_tb = tb + h * N;
-#pragma unroll
-        for (int j = 0; j < 8; ++j) y0[j] = h ? y1[j] : y0[j];  // register-wise select, no indexing
-        fft_inverse_from_regs<LOGM>(my_fs, ht, f.tw, y0, [&](uint32_t e, double2 v) {
-            const double2 u = cmulc(v, __ldg(f.twist + e));
-            my_tb[e] = double_to_mod(u.x * f.inv_m, Q, f.pow2, f.pow2s);
-            my_tb[e + M] = double_to_mod(u.y * f.inv_m, Q, f.pow2, f.pow2s);
-        });
         __syncthreads();
-        rotate_add_f<N, T>(acc, tb, at, tid, Q);
-        rotate_add_f<N, T>(acc + N, tb + N, at, tid, Q);
+        uint64_t tre[8], tim[8];
+        fft_inverse_from_regs<LOGM>(my_fs, ht, f.tw, y0, [&](int j, uint32_t e, double2 v) {
+            const double2 u = cmulc(v, __ldg(f.twist + e));
+            tre[j] = double_to_mod(u.x * f.inv_m, Q, f.pow2, f.pow2s);
+            tim[j] = double_to_mod(u.y * f.inv_m, Q, f.pow2, f.pow2s);
+        });
+        // 4. in-place rotate-add on the positions e_j = ht + j*TH and e_j + M
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const uint32_t e = ht + j * TH;
+            my_acc[e] = sub_mod(my_acc[e], tre[j], Q);
+            my_acc[e + M] = sub_mod(my_acc[e + M], tim[j], Q);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+#pragma unroll
+            for (int part = 0; part < 2; ++part) {
+                uint32_t tgt = ht + j * TH + part * M + at;
+                uint64_t v = part ? tim[j] : tre[j];
+                tgt &= TWO_N - 1;
+                if (tgt >= N) {
+                    tgt -= N;
+                    v = v ? Q - v : 0;
+                }
+                my_acc[tgt] = add_mod(my_acc[tgt], v, Q);
+            }
+        }
         __syncthreads();
     }
 
@@ -184,7 +222,7 @@ static cudaError_t br_fft_launch(const BlindRotateArgs& a, const FftKeyArgs& f, 
         if (e != cudaSuccess) return e;
         configured = smem;
     }
-    k_blind_rotate_fft<LOGN><<<batch, N / 8, smem, s>>>(a, f);
+    k_blind_rotate_fft<LOGN><<<batch, BrFftCfg<LOGN>::T, smem, s>>>(a, f);
     return cudaGetLastError();
 }
 
@@ -260,8 +298,11 @@ void keys_to_fft_host(const host::NttTables& t, const uint64_t* keys_ntt, size_t
                     z[e] = cld(re, im) * twist[e];
                 }
                 host_dif(z, w);
+                // spectrum slot s is consumed by thread s / 8 of a half as its register j = s % 8:
+                // store it at j * (M / 8) + s / 8 so each warp load is contiguous
                 for (uint32_t e = 0; e < M; ++e)
-                    out[k * M + e] = make_double2(static_cast<double>(z[e].real()), static_cast<double>(z[e].imag()));
+                    out[k * M + (e % 8) * (M / 8) + e / 8] =
+                        make_double2(static_cast<double>(z[e].real()), static_cast<double>(z[e].imag()));
             }
         });
     }

@@ -306,6 +306,10 @@ cbs_status cbs_keygen(cbs_context* ctx, uint64_t seed) {
 cbs_status cbs_context_set_br_backend(cbs_context* ctx, int backend) {
     CBS_CHECK_ARG(ctx, "set_br_backend: null context");
     CBS_CHECK_ARG(backend == CBS_BR_NTT || backend == CBS_BR_FFT64, "set_br_backend: unknown backend");
+    if (backend == CBS_BR_FFT64 && (ctx->p.digits_g > 4 || ctx->p.base_g > (1u << 15))) {
+        set_error("set_br_backend: the FFT64 backend supports at most 4 gadget digits of at most 15 bits");
+        return CBS_ERR_UNSUPPORTED;
+    }
     if (backend == CBS_BR_FFT64 && ctx->keys_ready) {
         if (cbs_status st = prepare_fft(ctx)) return st;
     }

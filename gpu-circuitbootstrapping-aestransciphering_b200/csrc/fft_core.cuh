@@ -139,7 +139,7 @@ __device__ __forceinline__ void fft_forward_to_regs(double2* sm, uint32_t tid, c
 #pragma unroll
     for (int j = 0; j < 8; ++j) x[j] = load(pass_index<LOGM, 3>(1u, tid, j));
     dif_pass<LOGM, 3>(x, 1u, tid, tw);
-#pragma unroll 1
+#pragma unroll
     for (int p = 1; p < Pl::P; ++p) {
 #pragma unroll
         for (int j = 0; j < 8; ++j) sm[cswz(pass_index<LOGM, 3>(1u << (3 * (p - 1)), tid, j))] = x[j];
@@ -158,7 +158,8 @@ __device__ __forceinline__ void fft_forward_to_regs(double2* sm, uint32_t tid, c
 }
 
 // Inverse FFT (without the 1/M factor) from the thread's spectrum slots 8*tid + j in x;
-// store(e, v) receives element e < M in natural order.
+// store(j, e, v) receives element e < M in natural order (register slot j, a compile-time
+// constant after unrolling, so callers can keep per-slot results in registers).
 template <int LOGM, class Store>
 __device__ __forceinline__ void fft_inverse_from_regs(double2* sm, uint32_t tid, const double2* __restrict__ tw,
                                                       double2 (&x)[8], Store store) {
@@ -168,7 +169,7 @@ __device__ __forceinline__ void fft_inverse_from_regs(double2* sm, uint32_t tid,
 #pragma unroll
     for (int j = 0; j < 8; ++j) sm[cswz(pass_index<LOGM, Pl::tail_r>(mt, tid, j))] = x[j];
     __syncthreads();
-#pragma unroll 1
+#pragma unroll
     for (int p = Pl::P - 2; p >= 0; --p) {
         const uint32_t m = 1u << (3 * p);
 #pragma unroll
@@ -182,7 +183,7 @@ __device__ __forceinline__ void fft_inverse_from_regs(double2* sm, uint32_t tid,
         }
     }
 #pragma unroll
-    for (int j = 0; j < 8; ++j) store(pass_index<LOGM, 3>(1u, tid, j), x[j]);
+    for (int j = 0; j < 8; ++j) store(j, pass_index<LOGM, 3>(1u, tid, j), x[j]);
 }
 
 }  // namespace cbs

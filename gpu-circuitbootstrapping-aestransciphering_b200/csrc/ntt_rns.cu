@@ -125,7 +125,7 @@ __device__ __forceinline__ void sub_fwd(uint64_t* sm, uint32_t gt, const uint64_
 #pragma unroll
     for (int j = 0; j < 8; ++j) x[j] = load(pass_index<LOGS, 3>(1u, gt, j));
     fwd_pass_b<LOGS, 3>(x, 1u, twb(1u), gt, tw, tws, q);
-#pragma unroll 1
+#pragma unroll
     for (int p = 1; p < Pl::P; ++p) {
 #pragma unroll
         for (int j = 0; j < 8; ++j) sm[swz(pass_index<LOGS, 3>(1u << (3 * (p - 1)), gt, j))] = x[j];
@@ -159,7 +159,7 @@ __device__ __forceinline__ void sub_inv(uint64_t* sm, uint32_t gt, const uint64_
 #pragma unroll
     for (int j = 0; j < 8; ++j) sm[swz(pass_index<LOGS, Pl::tail_r>(mt, gt, j))] = x[j];
     __syncthreads();
-#pragma unroll 1
+#pragma unroll
     for (int p = Pl::P - 2; p >= 0; --p) {
         const uint32_t m = 1u << (3 * p);
 #pragma unroll
