@@ -56,6 +56,15 @@ __device__ __forceinline__ uint32_t pack_digits(int32_t re, int32_t im) {
     return (static_cast<uint32_t>(re) & 0xffffu) | (static_cast<uint32_t>(im) << 16);
 }
 
+// zeta^e from the half table: register slot j of the first/last pass holds e = tid + j*M/8,
+// so e < M/2 exactly for j < 4; above, zeta^e = i * conj(zeta^(M-e)) = swapped components.
+template <int LOGM>
+__device__ __forceinline__ double2 twist_at(const double2* tws, int j, uint32_t e) {
+    if (j < 4) return tws[e];
+    const double2 t = tws[(1u << LOGM) - e];
+    return make_double2(t.y, t.x);
+}
+
 template <int LOGN>
 struct BrFftCfg {
     static constexpr uint32_t T = (1u << LOGN) / 8;
@@ -78,10 +87,13 @@ __global__ void __launch_bounds__(BrFftCfg<LOGN>::T, BrFftCfg<LOGN>::MIN_BLOCKS)
     k_blind_rotate_fft(const BlindRotateArgs a, const FftKeyArgs f) {
     constexpr int LOGM = LOGN - 1;
     constexpr uint32_t N = 1u << LOGN, M = N / 2, TH = M / 8, T = 2 * TH, TWO_N = 2 * N;
+    using Tb = FftTab<LOGM>;
     extern __shared__ __align__(16) uint64_t smem[];
-    uint64_t* acc = smem;                                       // [2][N]
-    uint32_t* dig = reinterpret_cast<uint32_t*>(smem + 2 * N);  // [2][digits <= 4][M] packed pairs
-    double2* fs = reinterpret_cast<double2*>(smem + 4 * N);     // [2][M]
+    uint64_t* acc = smem;                                           // [2][N]
+    double2* fs = reinterpret_cast<double2*>(smem + 2 * N);         // [2][M]
+    double2* tab = fs + 2 * M;                                      // FftTab<LOGM>
+    uint32_t* dig = reinterpret_cast<uint32_t*>(tab + Tb::size());  // [2][digits][M] packed pairs
+    const double2* tws = tab + Tb::twist_off();
     const uint32_t ct = blockIdx.x, tid = threadIdx.x;
     const uint32_t h = tid / TH, ht = tid % TH;
     uint64_t* my_acc = acc + h * N;
@@ -92,6 +104,7 @@ __global__ void __launch_bounds__(BrFftCfg<LOGN>::T, BrFftCfg<LOGN>::MIN_BLOCKS)
     int64_t offset = 0;
     for (uint32_t k = 0; k < digits; ++k) offset += static_cast<int64_t>(1) << (gbits * k + gbits - 1);
 
+    for (uint32_t i = tid; i < Tb::size(); i += T) tab[i] = f.tab[i];
     {
         const uint32_t bt = special_ms_f(a.b[ct], TWO_N, a.q_lwe, a.bitwidth);
         for (uint32_t i = tid; i < N; i += T) {
@@ -126,12 +139,12 @@ __global__ void __launch_bounds__(BrFftCfg<LOGN>::T, BrFftCfg<LOGN>::MIN_BLOCKS)
             const uint32_t* dsrc = dig + (h * digits + d) * M;
             double2 x[8];
             fft_forward_to_regs<LOGM>(
-                my_fs, ht, f.tw,
-                [&](uint32_t e) {
+                my_fs, ht, tab,
+                [&](int j, uint32_t e) {
                     const uint32_t v = dsrc[e];
                     const double re = static_cast<double>(static_cast<int16_t>(v & 0xffffu));
                     const double im = static_cast<double>(static_cast<int16_t>(v >> 16));
-                    return cmul(make_double2(re, im), __ldg(f.twist + e));
+                    return cmul(make_double2(re, im), twist_at<LOGM>(tws, j, e));
                 },
                 x);
             const double2* k0 = ek + static_cast<size_t>(2 * d + h) * 2 * M;  // key row 2d + h, slot-major
@@ -157,8 +170,8 @@ __global__ void __launch_bounds__(BrFftCfg<LOGN>::T, BrFftCfg<LOGN>::MIN_BLOCKS)
         }
         __syncthreads();
         uint64_t tre[8], tim[8];
-        fft_inverse_from_regs<LOGM>(my_fs, ht, f.tw, y0, [&](int j, uint32_t e, double2 v) {
-            const double2 u = cmulc(v, __ldg(f.twist + e));
+        fft_inverse_from_regs<LOGM>(my_fs, ht, tab, y0, [&](int j, uint32_t e, double2 v) {
+            const double2 u = cmulc(v, twist_at<LOGM>(tws, j, e));
             tre[j] = double_to_mod(u.x * f.inv_m, Q, f.pow2, f.pow2s);
             tim[j] = double_to_mod(u.y * f.inv_m, Q, f.pow2, f.pow2s);
         });
@@ -213,14 +226,18 @@ cudaError_t ntt_forward(uint64_t* out, const uint64_t* in, const uint64_t* tw, c
 
 template <int LOGN>
 static cudaError_t br_fft_launch(const BlindRotateArgs& a, const FftKeyArgs& f, uint32_t batch, cudaStream_t s) {
-    constexpr uint32_t N = 1u << LOGN;
-    const size_t smem = 6ull * N * sizeof(uint64_t);
-    static size_t configured = 0;
-    if (configured < smem) {
+    constexpr uint32_t N = 1u << LOGN, M = N / 2;
+    const size_t smem = 2ull * N * sizeof(uint64_t) + (2ull * M + FftTab<LOGN - 1>::size()) * sizeof(double2) +
+                        2ull * a.digits * M * sizeof(uint32_t);
+    if (f.tab_len != FftTab<LOGN - 1>::size()) return cudaErrorInvalidValue;
+    static size_t configured[64] = {};  // per device
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (configured[dev] < smem) {
         cudaError_t e = cudaFuncSetAttribute(k_blind_rotate_fft<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              static_cast<int>(smem));
         if (e != cudaSuccess) return e;
-        configured = smem;
+        configured[dev] = smem;
     }
     k_blind_rotate_fft<LOGN><<<batch, BrFftCfg<LOGN>::T, smem, s>>>(a, f);
     return cudaGetLastError();
@@ -258,18 +275,52 @@ static void host_dif(std::vector<cld>& a, const std::vector<cld>& w) {
     }
 }
 
-void fft_tables_host(uint32_t N, std::vector<double2>& tw, std::vector<double2>& twist) {
-    const uint32_t M = N / 2;
+template <int LOGM>
+static void fft_tables_for(std::vector<double2>& tab) {
+    using Tb = FftTab<LOGM>;
+    constexpr uint32_t M = 1u << LOGM, N = 2 * M;
+    using Pl = NttPlan<LOGM>;
     const long double pi = 3.141592653589793238462643383279502884L;
-    tw.resize(M / 2);
-    for (uint32_t e = 0; e < M / 2; ++e) {
+    auto tw = [&](uint32_t e) {
         const long double ang = 2.0L * pi * e / M;
-        tw[e] = make_double2(static_cast<double>(cosl(ang)), static_cast<double>(sinl(ang)));
+        return make_double2(static_cast<double>(cosl(ang)), static_cast<double>(sinl(ang)));
+    };
+    tab.assign(Tb::size(), make_double2(0, 0));
+    for (uint32_t e = 0; e < M / 2; ++e) tab[e] = tw(e);
+    for (int p = 1; p < Pl::P; ++p) {
+        const uint32_t m = Tb::pass_m(p), o = Tb::pass_off(p);
+        const int r = Tb::pass_r(p);
+        if (r == 3) {
+            const uint32_t q = M / (8 * m);
+            for (uint32_t j0 = 0; j0 < q; ++j0) {
+                for (uint32_t k = 0; k < 4; ++k) tab[o + k * q + j0] = tw((j0 + k * q) * m);
+                for (uint32_t k = 0; k < 2; ++k) tab[o + 4 * q + k * q + j0] = tw((j0 + k * q) * 2 * m);
+                tab[o + 6 * q + j0] = tw(j0 * 4 * m);
+            }
+        } else if (r == 2) {
+            const uint32_t q = M / (4 * m);
+            for (uint32_t j0 = 0; j0 < q; ++j0) {
+                tab[o + j0] = tw(j0 * m);
+                tab[o + q + j0] = tw((j0 + q) * m);
+                tab[o + 2 * q + j0] = tw(j0 * 2 * m);
+            }
+        } else {
+            const uint32_t h = M / (2 * m);
+            for (uint32_t j0 = 0; j0 < h; ++j0) tab[o + j0] = tw(j0 * m);
+        }
     }
-    twist.resize(M);
-    for (uint32_t e = 0; e < M; ++e) {
+    for (uint32_t e = 0; e <= M / 2; ++e) {
         const long double ang = pi * e / N;
-        twist[e] = make_double2(static_cast<double>(cosl(ang)), static_cast<double>(sinl(ang)));
+        tab[Tb::twist_off() + e] = make_double2(static_cast<double>(cosl(ang)), static_cast<double>(sinl(ang)));
+    }
+}
+
+void fft_tables_host(uint32_t N, std::vector<double2>& tab) {
+    switch (N) {
+        case 1024: fft_tables_for<9>(tab); break;
+        case 2048: fft_tables_for<10>(tab); break;
+        case 4096: fft_tables_for<11>(tab); break;
+        default: tab.clear();
     }
 }
 

@@ -35,9 +35,9 @@ static cbs_status prepare_fft(cbs_context* c) {
         return CBS_ERR_NOT_READY;
     }
     const size_t polys = c->hk.bsk.size() / c->p.N;
-    std::vector<double2> bskf, tw, twist;
+    std::vector<double2> bskf, ftab;
     keys_to_fft_host(c->tab, c->hk.bsk.data(), polys, bskf);
-    fft_tables_host(c->p.N, tw, twist);
+    fft_tables_host(c->p.N, ftab);
     std::vector<uint64_t> p2(64), p2s(64);
     FastMod fm(c->p.Q);
     uint64_t v = 1 % c->p.Q;
@@ -48,8 +48,7 @@ static cbs_status prepare_fft(cbs_context* c) {
     }
     cudaStream_t s = c->stream;
     CBS_CUDA_TRY(c->d_bskf.upload(bskf.data(), bskf.size(), s));
-    CBS_CUDA_TRY(c->d_fft_tw.upload(tw.data(), tw.size(), s));
-    CBS_CUDA_TRY(c->d_fft_twist.upload(twist.data(), twist.size(), s));
+    CBS_CUDA_TRY(c->d_fft_tab.upload(ftab.data(), ftab.size(), s));
     CBS_CUDA_TRY(c->d_pow2.upload(p2.data(), p2.size(), s));
     CBS_CUDA_TRY(c->d_pow2s.upload(p2s.data(), p2s.size(), s));
     CBS_CUDA_TRY(cudaStreamSynchronize(s));
@@ -81,8 +80,8 @@ cbs_status run_blind_rotate(cbs_context* c, const uint64_t* d_a, const uint64_t*
         }
         FftKeyArgs f{};
         f.bskf = c->d_bskf.p;
-        f.tw = c->d_fft_tw.p;
-        f.twist = c->d_fft_twist.p;
+        f.tab = c->d_fft_tab.p;
+        f.tab_len = static_cast<uint32_t>(c->d_fft_tab.n);
         f.pow2 = c->d_pow2.p;
         f.pow2s = c->d_pow2s.p;
         f.inv_m = 2.0 / static_cast<double>(c->p.N);

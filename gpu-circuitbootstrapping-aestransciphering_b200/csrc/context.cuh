@@ -62,7 +62,7 @@ struct cbs_context {
     // FP64 FFT blind-rotation backend (built on demand from the keys)
     int br_backend = 0;  // CBS_BR_NTT or CBS_BR_FFT64
     bool fft_ready = false;
-    cbs::DevBuf<double2> d_bskf, d_fft_tw, d_fft_twist;
+    cbs::DevBuf<double2> d_bskf, d_fft_tab;
     cbs::DevBuf<uint64_t> d_pow2, d_pow2s;
     // scratch
     cbs::DevBuf<uint64_t> d_mv, d_rgsw;

@@ -49,96 +49,249 @@ __device__ __forceinline__ void dit_bf(double2& p, double2& s, double2 w) {
     p = cadd(p, t);
 }
 
-// tw[e] = exp(2*pi*i*e / M), e < M/2
-template <int LOGM, int R>
-__device__ __forceinline__ void dif_pass(double2 (&x)[8], uint32_t m, uint32_t tid, const double2* __restrict__ tw) {
+__device__ __forceinline__ double2 mul_i(double2 v) { return make_double2(-v.y, v.x); }
+__device__ __forceinline__ double2 mul_negi(double2 v) { return make_double2(v.y, -v.x); }
+
+// Twiddle tables of one transform length, kept in shared memory by the kernels:
+//   [0, M/2)            tw[e] = exp(2*pi*i*e/M), read directly by the first pass (its index
+//                       runs over consecutive e);
+//   pass_off(p), p >= 1 the twiddles of pass p laid out [k][j0] (k = the butterfly's place in
+//                       the pass, j0 = the thread's group), so the lanes of a warp read
+//                       consecutive entries;
+//   twist_off()         exp(i*pi*e/N) for e <= M/2 (e > M/2 uses zeta^(M-e) = i conj(zeta^e),
+//                       i.e. the swapped components of entry M - e).
+template <int LOGM>
+struct FftTab {
+    static constexpr uint32_t M = 1u << LOGM;
+    using Pl = NttPlan<LOGM>;
+    static constexpr uint32_t pass_m(int p) { return 1u << (3 * p); }
+    static constexpr int pass_r(int p) { return p < Pl::P - 1 ? 3 : Pl::tail_r; }
+    static constexpr uint32_t pass_size(int p) {
+        return pass_r(p) == 3 ? 7 * (M / (8 * pass_m(p)))
+                              : (pass_r(p) == 2 ? 3 * (M / (4 * pass_m(p))) : M / (2 * pass_m(p)));
+    }
+    static constexpr uint32_t pass_off(int p) {
+        uint32_t o = M / 2;
+        for (int k = 1; k < p; ++k) o += pass_size(k);
+        return o;
+    }
+    static constexpr uint32_t twist_off() { return pass_off(Pl::P); }
+    static constexpr uint32_t size() { return twist_off() + M / 2 + 1; }
+};
+
+// DIF pass over R stages starting at DFT half-size h = M / (2m).  COMPACT: tb is the pass's
+// [k][j0] table; otherwise tb is tw, indexed directly.  Twiddles known to be 1 or i are
+// applied without multiplications.
+template <int LOGM, int R, bool COMPACT>
+__device__ __forceinline__ void dif_pass(double2 (&x)[8], uint32_t m, uint32_t tid, const double2* tb) {
     constexpr uint32_t M = 1u << LOGM;
     const uint32_t h = M / (2 * m);
     if (R == 3) {
         const uint32_t q = h / 4, j0 = tid % q;
+        if (COMPACT && q == 1) {  // h = 4: stage 1 twiddles 1, w8, i, w8^3; stage 2 1, i; stage 3 1
+            {
+                const double2 t = csubd(x[0], x[4]);
+                x[0] = cadd(x[0], x[4]);
+                x[4] = t;
+            }
+            dif_bf(x[1], x[5], tb[1]);
+            {
+                const double2 t = mul_i(csubd(x[2], x[6]));
+                x[2] = cadd(x[2], x[6]);
+                x[6] = t;
+            }
+            dif_bf(x[3], x[7], tb[3]);
+            // stage 2: twiddle 1 on the slot pairs (0,2), (4,6) and i on (1,3), (5,7)
 #pragma unroll
-        for (int r = 0; r < 4; ++r) dif_bf(x[r], x[r + 4], __ldg(tw + (j0 + r * q) * m));
+            for (int g = 0; g < 8; g += 4) {
+                double2 t = csubd(x[g], x[g + 2]);
+                x[g] = cadd(x[g], x[g + 2]);
+                x[g + 2] = t;
+                t = mul_i(csubd(x[g + 1], x[g + 3]));
+                x[g + 1] = cadd(x[g + 1], x[g + 3]);
+                x[g + 3] = t;
+            }
+#pragma unroll
+            for (int r = 0; r < 8; r += 2) {
+                const double2 t = csubd(x[r], x[r + 1]);
+                x[r] = cadd(x[r], x[r + 1]);
+                x[r + 1] = t;
+            }
+            return;
+        }
+#pragma unroll
+        for (int r = 0; r < 4; ++r) dif_bf(x[r], x[r + 4], COMPACT ? tb[r * q + j0] : tb[(j0 + r * q) * m]);
 #pragma unroll
         for (int r = 0; r < 2; ++r) {
-            const double2 w = __ldg(tw + (j0 + r * q) * 2 * m);
+            const double2 w = COMPACT ? tb[4 * q + r * q + j0] : tb[(j0 + r * q) * 2 * m];
             dif_bf(x[r], x[r + 2], w);
             dif_bf(x[r + 4], x[r + 6], w);
         }
-        const double2 w = __ldg(tw + j0 * 4 * m);
+        if (COMPACT && q == 2) {  // h = 8: the last stage's twiddle is i^j0
 #pragma unroll
-        for (int r = 0; r < 8; r += 2) dif_bf(x[r], x[r + 1], w);
+            for (int r = 0; r < 8; r += 2) {
+                const double2 t = csubd(x[r], x[r + 1]);
+                x[r] = cadd(x[r], x[r + 1]);
+                x[r + 1] = j0 ? mul_i(t) : t;
+            }
+        } else {
+            const double2 w = COMPACT ? tb[6 * q + j0] : tb[j0 * 4 * m];
+#pragma unroll
+            for (int r = 0; r < 8; r += 2) dif_bf(x[r], x[r + 1], w);
+        }
     } else if (R == 2) {
         const uint32_t q = h / 2;
 #pragma unroll
         for (int hh = 0; hh < 2; ++hh) {
             const uint32_t j0 = (2 * tid + hh) % q;
             double2* v = x + 4 * hh;
-            dif_bf(v[0], v[2], __ldg(tw + j0 * m));
-            dif_bf(v[1], v[3], __ldg(tw + (j0 + q) * m));
-            const double2 w = __ldg(tw + j0 * 2 * m);
-            dif_bf(v[0], v[1], w);
-            dif_bf(v[2], v[3], w);
+            if (COMPACT && q == 1) {  // twiddles 1, i, 1
+                double2 t = csubd(v[0], v[2]);
+                v[0] = cadd(v[0], v[2]);
+                v[2] = t;
+                t = mul_i(csubd(v[1], v[3]));
+                v[1] = cadd(v[1], v[3]);
+                v[3] = t;
+                t = csubd(v[0], v[1]);
+                v[0] = cadd(v[0], v[1]);
+                v[1] = t;
+                t = csubd(v[2], v[3]);
+                v[2] = cadd(v[2], v[3]);
+                v[3] = t;
+            } else {
+                dif_bf(v[0], v[2], COMPACT ? tb[j0] : tb[j0 * m]);
+                dif_bf(v[1], v[3], COMPACT ? tb[q + j0] : tb[(j0 + q) * m]);
+                const double2 w = COMPACT ? tb[2 * q + j0] : tb[j0 * 2 * m];
+                dif_bf(v[0], v[1], w);
+                dif_bf(v[2], v[3], w);
+            }
         }
     } else {
 #pragma unroll
         for (int hh = 0; hh < 4; ++hh) {
-            const uint32_t j0 = (4 * tid + hh) % h;
-            dif_bf(x[2 * hh], x[2 * hh + 1], __ldg(tw + j0 * m));
+            if (COMPACT && h == 1) {  // twiddle 1
+                const double2 t = csubd(x[2 * hh], x[2 * hh + 1]);
+                x[2 * hh] = cadd(x[2 * hh], x[2 * hh + 1]);
+                x[2 * hh + 1] = t;
+            } else {
+                const uint32_t j0 = (4 * tid + hh) % h;
+                dif_bf(x[2 * hh], x[2 * hh + 1], COMPACT ? tb[j0] : tb[j0 * m]);
+            }
         }
     }
 }
 
-template <int LOGM, int R>
-__device__ __forceinline__ void dit_pass(double2 (&x)[8], uint32_t m, uint32_t tid, const double2* __restrict__ tw) {
+template <int LOGM, int R, bool COMPACT>
+__device__ __forceinline__ void dit_pass(double2 (&x)[8], uint32_t m, uint32_t tid, const double2* tb) {
     constexpr uint32_t M = 1u << LOGM;
     const uint32_t h = M / (2 * m);
     if (R == 3) {
         const uint32_t q = h / 4, j0 = tid % q;
-        {
-            const double2 w = __ldg(tw + j0 * 4 * m);
+        if (COMPACT && q == 1) {
+#pragma unroll
+            for (int r = 0; r < 8; r += 2) {
+                const double2 t = x[r + 1];
+                x[r + 1] = csubd(x[r], t);
+                x[r] = cadd(x[r], t);
+            }
+#pragma unroll
+            for (int g = 0; g < 8; g += 4) {  // twiddle 1 on (0,2), (4,6); i (conjugated) on (1,3), (5,7)
+                double2 t = x[g + 2];
+                x[g + 2] = csubd(x[g], t);
+                x[g] = cadd(x[g], t);
+                t = mul_negi(x[g + 3]);
+                x[g + 3] = csubd(x[g + 1], t);
+                x[g + 1] = cadd(x[g + 1], t);
+            }
+            {
+                const double2 t = x[4];
+                x[4] = csubd(x[0], t);
+                x[0] = cadd(x[0], t);
+            }
+            dit_bf(x[1], x[5], tb[1]);
+            {
+                const double2 t = mul_negi(x[6]);
+                x[6] = csubd(x[2], t);
+                x[2] = cadd(x[2], t);
+            }
+            dit_bf(x[3], x[7], tb[3]);
+            return;
+        }
+        if (COMPACT && q == 2) {
+#pragma unroll
+            for (int r = 0; r < 8; r += 2) {
+                const double2 t = j0 ? mul_negi(x[r + 1]) : x[r + 1];
+                x[r + 1] = csubd(x[r], t);
+                x[r] = cadd(x[r], t);
+            }
+        } else {
+            const double2 w = COMPACT ? tb[6 * q + j0] : tb[j0 * 4 * m];
 #pragma unroll
             for (int r = 0; r < 8; r += 2) dit_bf(x[r], x[r + 1], w);
         }
 #pragma unroll
         for (int r = 0; r < 2; ++r) {
-            const double2 w = __ldg(tw + (j0 + r * q) * 2 * m);
+            const double2 w = COMPACT ? tb[4 * q + r * q + j0] : tb[(j0 + r * q) * 2 * m];
             dit_bf(x[r], x[r + 2], w);
             dit_bf(x[r + 4], x[r + 6], w);
         }
 #pragma unroll
-        for (int r = 0; r < 4; ++r) dit_bf(x[r], x[r + 4], __ldg(tw + (j0 + r * q) * m));
+        for (int r = 0; r < 4; ++r) dit_bf(x[r], x[r + 4], COMPACT ? tb[r * q + j0] : tb[(j0 + r * q) * m]);
     } else if (R == 2) {
         const uint32_t q = h / 2;
 #pragma unroll
         for (int hh = 0; hh < 2; ++hh) {
             const uint32_t j0 = (2 * tid + hh) % q;
             double2* v = x + 4 * hh;
-            const double2 w = __ldg(tw + j0 * 2 * m);
-            dit_bf(v[0], v[1], w);
-            dit_bf(v[2], v[3], w);
-            dit_bf(v[0], v[2], __ldg(tw + j0 * m));
-            dit_bf(v[1], v[3], __ldg(tw + (j0 + q) * m));
+            if (COMPACT && q == 1) {
+                double2 t = v[1];
+                v[1] = csubd(v[0], t);
+                v[0] = cadd(v[0], t);
+                t = v[3];
+                v[3] = csubd(v[2], t);
+                v[2] = cadd(v[2], t);
+                t = v[2];
+                v[2] = csubd(v[0], t);
+                v[0] = cadd(v[0], t);
+                t = mul_negi(v[3]);
+                v[3] = csubd(v[1], t);
+                v[1] = cadd(v[1], t);
+            } else {
+                const double2 w = COMPACT ? tb[2 * q + j0] : tb[j0 * 2 * m];
+                dit_bf(v[0], v[1], w);
+                dit_bf(v[2], v[3], w);
+                dit_bf(v[0], v[2], COMPACT ? tb[j0] : tb[j0 * m]);
+                dit_bf(v[1], v[3], COMPACT ? tb[q + j0] : tb[(j0 + q) * m]);
+            }
         }
     } else {
 #pragma unroll
         for (int hh = 0; hh < 4; ++hh) {
-            const uint32_t j0 = (4 * tid + hh) % h;
-            dit_bf(x[2 * hh], x[2 * hh + 1], __ldg(tw + j0 * m));
+            if (COMPACT && h == 1) {
+                const double2 t = x[2 * hh + 1];
+                x[2 * hh + 1] = csubd(x[2 * hh], t);
+                x[2 * hh] = cadd(x[2 * hh], t);
+            } else {
+                const uint32_t j0 = (4 * tid + hh) % h;
+                dit_bf(x[2 * hh], x[2 * hh + 1], COMPACT ? tb[j0] : tb[j0 * m]);
+            }
         }
     }
 }
 
-// Forward FFT of one folded, twisted polynomial by the first M/8 threads of the CTA.
-// load(e) returns z_e (e < M); on return x[j] holds spectrum slot 8*tid + j.
-// sm: M double2 of shared memory; the caller __syncthreads() before reusing it.
+// Forward FFT of one folded, twisted polynomial by M/8 threads.  tab: the FftTab layout (in
+// shared memory); load(j, e) returns z_e for register slot j (e < M); on return x[j] holds
+// spectrum slot 8*tid + j.  sm: M double2 of shared memory; the caller __syncthreads()
+// before reusing it.
 template <int LOGM, class Load>
-__device__ __forceinline__ void fft_forward_to_regs(double2* sm, uint32_t tid, const double2* __restrict__ tw,
-                                                    Load load, double2 (&x)[8]) {
+__device__ __forceinline__ void fft_forward_to_regs(double2* sm, uint32_t tid, const double2* tab, Load load,
+                                                    double2 (&x)[8]) {
     using Pl = NttPlan<LOGM>;
+    using Tb = FftTab<LOGM>;
     static_assert(Pl::P >= 2, "fft needs M >= 64");
 #pragma unroll
-    for (int j = 0; j < 8; ++j) x[j] = load(pass_index<LOGM, 3>(1u, tid, j));
-    dif_pass<LOGM, 3>(x, 1u, tid, tw);
+    for (int j = 0; j < 8; ++j) x[j] = load(j, pass_index<LOGM, 3>(1u, tid, j));
+    dif_pass<LOGM, 3, false>(x, 1u, tid, tab);
 #pragma unroll
     for (int p = 1; p < Pl::P; ++p) {
 #pragma unroll
@@ -148,11 +301,11 @@ __device__ __forceinline__ void fft_forward_to_regs(double2* sm, uint32_t tid, c
         if (p < Pl::P - 1) {
 #pragma unroll
             for (int j = 0; j < 8; ++j) x[j] = sm[cswz(pass_index<LOGM, 3>(m, tid, j))];
-            dif_pass<LOGM, 3>(x, m, tid, tw);
+            dif_pass<LOGM, 3, true>(x, m, tid, tab + Tb::pass_off(p));
         } else {
 #pragma unroll
             for (int j = 0; j < 8; ++j) x[j] = sm[cswz(pass_index<LOGM, Pl::tail_r>(m, tid, j))];
-            dif_pass<LOGM, Pl::tail_r>(x, m, tid, tw);
+            dif_pass<LOGM, Pl::tail_r, true>(x, m, tid, tab + Tb::pass_off(p));
         }
     }
 }
@@ -161,11 +314,12 @@ __device__ __forceinline__ void fft_forward_to_regs(double2* sm, uint32_t tid, c
 // store(j, e, v) receives element e < M in natural order (register slot j, a compile-time
 // constant after unrolling, so callers can keep per-slot results in registers).
 template <int LOGM, class Store>
-__device__ __forceinline__ void fft_inverse_from_regs(double2* sm, uint32_t tid, const double2* __restrict__ tw,
-                                                      double2 (&x)[8], Store store) {
+__device__ __forceinline__ void fft_inverse_from_regs(double2* sm, uint32_t tid, const double2* tab, double2 (&x)[8],
+                                                      Store store) {
     using Pl = NttPlan<LOGM>;
+    using Tb = FftTab<LOGM>;
     constexpr uint32_t mt = 1u << (3 * (Pl::P - 1));
-    dit_pass<LOGM, Pl::tail_r>(x, mt, tid, tw);
+    dit_pass<LOGM, Pl::tail_r, true>(x, mt, tid, tab + Tb::pass_off(Pl::P - 1));
 #pragma unroll
     for (int j = 0; j < 8; ++j) sm[cswz(pass_index<LOGM, Pl::tail_r>(mt, tid, j))] = x[j];
     __syncthreads();
@@ -174,7 +328,8 @@ __device__ __forceinline__ void fft_inverse_from_regs(double2* sm, uint32_t tid,
         const uint32_t m = 1u << (3 * p);
 #pragma unroll
         for (int j = 0; j < 8; ++j) x[j] = sm[cswz(pass_index<LOGM, 3>(m, tid, j))];
-        dit_pass<LOGM, 3>(x, m, tid, tw);
+        if (p == 0) dit_pass<LOGM, 3, false>(x, m, tid, tab);
+        else dit_pass<LOGM, 3, true>(x, m, tid, tab + Tb::pass_off(p));
         if (p > 0) {
             // each pass reads and writes its own per-thread set, and the sets partition [0, M)
 #pragma unroll

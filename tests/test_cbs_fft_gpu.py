@@ -22,6 +22,7 @@ torch = pytest.importorskip("torch")
 # ~2^46.6 before extraction, i.e. ~100 at qKS = 2^14 against a decision margin of 4096, so
 # the per-bit failure probability stays far below 2^-40.
 FFT_PHASE_TOL_LOG2 = 33.0
+RGSW_ROW_TOL = 2 ** 31
 
 
 def _dev(a):
@@ -91,7 +92,10 @@ def test_fft_cbs_rgsw_semantics(pkg, fctx, fkeys, foc):
             ph1 = foc.phase_coef(got[i, j, 1])
             ph1[0] -= m * g[j]
             ph0 = foc.phase_coef(got[i, j, 0]) + m * g[j] * s
-            assert max(abs(int(x)) for x in ph1) < g[0] // 2
+            # row 1 carries coefficient 0 of the blind-rotation FFT error (rms 2^28.2, max
+            # 2^29.4 measured on B200 for these inputs; exact arithmetic gives <= 2^27.5), so
+            # the bound is the FFT tolerance scaled to one coefficient, not g_0 / 2
+            assert max(abs(int(x)) for x in ph1) < RGSW_ROW_TOL
             assert max(abs(int(x)) for x in ph0) < g[0] * 2
 
 
