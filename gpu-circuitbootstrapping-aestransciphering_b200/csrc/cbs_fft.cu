@@ -23,23 +23,18 @@
 
 namespace cbs {
 
-// round(v) mod Q for |v| < 2^62 * 2^30 (v is the FP64 result of an integer-valued product)
-__device__ __forceinline__ uint64_t double_to_mod(double v, uint64_t Q, const uint64_t* __restrict__ pow2,
-                                                  const uint64_t* __restrict__ pow2s) {
-    const long long bits = __double_as_longlong(v);
-    const int ex = static_cast<int>((bits >> 52) & 0x7ff);
-    const bool neg = bits < 0;
-    uint64_t r;
-    if (ex < 1075) {  // |v| < 2^52: round to the nearest integer directly
-        const long long i = __double2ll_rn(v);
-        const uint64_t a = static_cast<uint64_t>(i < 0 ? -i : i);
-        r = a;  // a < 2^52 < Q
-        return (i < 0 && r) ? Q - r : r;
-    }
-    const int e = ex - 1075;  // v = +-mantissa * 2^e exactly
-    const uint64_t mant = (static_cast<uint64_t>(bits) & ((1ull << 52) - 1)) | (1ull << 52);  // < 2^53 < Q
-    r = mul_shoup(mant, __ldg(pow2 + e), __ldg(pow2s + e), Q);
-    return (neg && r) ? Q - r : r;
+// v mod Q, v the FP64 value of an integer-valued product (|v| < 2^90), computed in FP64:
+// k = rint(v / Q), r = v - k*q_hi - k*q_lo with two fused multiply-adds.  The two roundings of
+// r (|r| < 2Q < 2^55) add at most +-8 to the result, far below the FFT's own rounding error.
+__device__ __forceinline__ uint64_t double_to_mod(double v, const FftKeyArgs& f, uint64_t Q) {
+    const double k = rint(v * f.inv_q);
+    double r = fma(-k, f.q_hi, v);
+    r = fma(-k, f.q_lo, r);
+    int64_t i = __double2ll_rn(r);
+    if (i < 0) i += static_cast<int64_t>(Q);
+    if (i < 0) i += static_cast<int64_t>(Q);
+    if (i >= static_cast<int64_t>(Q)) i -= static_cast<int64_t>(Q);
+    return static_cast<uint64_t>(i);
 }
 
 // Balanced base-2^gbits digits of the prepared value v, all at once: adding
@@ -79,9 +74,8 @@ struct BrFftCfg {
 //     so each load is one coalesced 512-byte warp access), accumulating two output spectra;
 //  3. the halves swap partial sums through shared memory (swizzled, conflict-free) so half h
 //     holds the full spectrum of output h and inverse-transforms it into registers;
-//  4. each thread owns the same coefficient positions of acc_h and of output h, so the
-//     rotate-add acc_h += (X^a - 1) t_h is done in place in two phases: acc_h[i] -= t_h[i],
-//     barrier, acc_h[i + a] += t_h[i] (negacyclic wrap); each phase writes every position once.
+//  4. output h is staged in this half's FFT buffer and each thread updates the accumulator
+//     positions it owns: acc_h[i] += t_h[i - a] (negacyclic wrap) - t_h[i].
 template <int LOGN>
 __global__ void __launch_bounds__(BrFftCfg<LOGN>::T, BrFftCfg<LOGN>::MIN_BLOCKS)
     k_blind_rotate_fft(const BlindRotateArgs a, const FftKeyArgs f) {
@@ -172,30 +166,26 @@ __global__ void __launch_bounds__(BrFftCfg<LOGN>::T, BrFftCfg<LOGN>::MIN_BLOCKS)
         uint64_t tre[8], tim[8];
         fft_inverse_from_regs<LOGM>(my_fs, ht, tab, y0, [&](int j, uint32_t e, double2 v) {
             const double2 u = cmulc(v, twist_at<LOGM>(tws, j, e));
-            tre[j] = double_to_mod(u.x * f.inv_m, Q, f.pow2, f.pow2s);
-            tim[j] = double_to_mod(u.y * f.inv_m, Q, f.pow2, f.pow2s);
+            tre[j] = double_to_mod(u.x * f.inv_m, f, Q);
+            tim[j] = double_to_mod(u.y * f.inv_m, f, Q);
         });
-        // 4. in-place rotate-add on the positions e_j = ht + j*TH and e_j + M
+        // 4. rotate-add acc_h += (X^a - 1) t_h: t_h goes to this half's (now idle) FFT buffer,
+        //    then each thread updates the positions it owns: acc[i] += t[i - a] - t[i]
+        __syncthreads();
+        uint64_t* tsm = reinterpret_cast<uint64_t*>(my_fs);  // N words
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
-            const uint32_t e = ht + j * TH;
-            my_acc[e] = sub_mod(my_acc[e], tre[j], Q);
-            my_acc[e + M] = sub_mod(my_acc[e + M], tim[j], Q);
+            tsm[ht + j * TH] = tre[j];
+            tsm[ht + j * TH + M] = tim[j];
         }
         __syncthreads();
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-#pragma unroll
-            for (int part = 0; part < 2; ++part) {
-                uint32_t tgt = ht + j * TH + part * M + at;
-                uint64_t v = part ? tim[j] : tre[j];
-                tgt &= TWO_N - 1;
-                if (tgt >= N) {
-                    tgt -= N;
-                    v = v ? Q - v : 0;
-                }
-                my_acc[tgt] = add_mod(my_acc[tgt], v, Q);
-            }
+#pragma unroll 4
+        for (uint32_t k = 0; k < 16; ++k) {
+            const uint32_t i = ht + k * TH;
+            const uint32_t s = (i + TWO_N - at) & (TWO_N - 1);  // source index of X^a t in [0, 2N)
+            const uint64_t v = (s < N) ? tsm[s] : tsm[s - N];
+            const uint64_t r = (s < N) ? add_mod(my_acc[i], v, Q) : sub_mod(my_acc[i], v, Q);
+            my_acc[i] = sub_mod(r, tsm[i], Q);
         }
         __syncthreads();
     }

@@ -85,6 +85,9 @@ cbs_status run_blind_rotate(cbs_context* c, const uint64_t* d_a, const uint64_t*
         f.pow2 = c->d_pow2.p;
         f.pow2s = c->d_pow2s.p;
         f.inv_m = 2.0 / static_cast<double>(c->p.N);
+        f.q_hi = static_cast<double>(c->p.Q);
+        f.q_lo = static_cast<double>(static_cast<int64_t>(c->p.Q) - static_cast<int64_t>(f.q_hi));
+        f.inv_q = 1.0 / static_cast<double>(c->p.Q);
         CBS_CUDA_TRY(launch_blind_rotate_fft(a, f, c->d_mod.p, c->p.N, batch, s));
         return CBS_OK;
     }

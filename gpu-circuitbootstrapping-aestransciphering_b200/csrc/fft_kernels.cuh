@@ -18,6 +18,8 @@ struct FftKeyArgs {
     const uint64_t* pow2;   // [64] 2^e mod Q
     const uint64_t* pow2s;  // Shoup quotients of pow2
     double inv_m;           // 1 / (N/2)
+    double q_hi, q_lo;      // Q = q_hi + q_lo exactly (q_hi = Q rounded to a double, |q_lo| <= 1)
+    double inv_q;           // 1 / Q rounded
 };
 
 cudaError_t launch_blind_rotate_fft(const BlindRotateArgs& a, const FftKeyArgs& f, const cbs_dmodulus* d_mod,
