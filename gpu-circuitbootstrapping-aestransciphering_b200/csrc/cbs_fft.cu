@@ -47,6 +47,14 @@ __device__ __forceinline__ int32_t balanced_digit(int64_t w, int gbits, uint32_t
     return static_cast<int32_t>(field) - (1 << (gbits - 1));
 }
 
+// gadget_prepare(x) + offset for x in [0, Q): centre, round away the ign low bits, add the
+// digit offset.  The sum is non-negative because the offset times 2^ign is at least Q / 2.
+__device__ __forceinline__ int64_t prepared_offset(uint64_t x, uint64_t Q, uint64_t qhalf, uint64_t round_c, int ign) {
+    uint64_t t = x + round_c;
+    if (x >= qhalf) t -= Q;
+    return static_cast<int64_t>(t >> ign);
+}
+
 __device__ __forceinline__ uint32_t pack_digits(int32_t re, int32_t im) {
     return (static_cast<uint32_t>(re) & 0xffffu) | (static_cast<uint32_t>(im) << 16);
 }
@@ -97,6 +105,11 @@ __global__ void __launch_bounds__(BrFftCfg<LOGN>::T, BrFftCfg<LOGN>::MIN_BLOCKS)
     const int gbits = a.g.gbits;
     int64_t offset = 0;
     for (uint32_t k = 0; k < digits; ++k) offset += static_cast<int64_t>(1) << (gbits * k + gbits - 1);
+    const int ign = a.g.ign;
+    const uint64_t qhalf = Q >> 1;
+    // (x_centred + 2^(ign-1)) >> ign is the balanced rounding of gadget_prepare; adding the
+    // digit offset before the shift folds both into one constant
+    const uint64_t round_c = (ign ? (uint64_t(1) << (ign - 1)) : 0) + (static_cast<uint64_t>(offset) << ign);
 
     for (uint32_t i = tid; i < Tb::size(); i += T) tab[i] = f.tab[i];
     {
@@ -117,8 +130,8 @@ __global__ void __launch_bounds__(BrFftCfg<LOGN>::T, BrFftCfg<LOGN>::MIN_BLOCKS)
         // 1. digits of both polynomials
         for (uint32_t idx = tid; idx < 2 * M; idx += T) {
             const uint32_t p = idx / M, e = idx % M;
-            const int64_t wr = gadget_prepare(acc[p * N + e], a.g) + offset;
-            const int64_t wi = gadget_prepare(acc[p * N + e + M], a.g) + offset;
+            const int64_t wr = prepared_offset(acc[p * N + e], Q, qhalf, round_c, ign);
+            const int64_t wi = prepared_offset(acc[p * N + e + M], Q, qhalf, round_c, ign);
             uint32_t* dst = dig + p * digits * M + e;
             for (uint32_t d = 0; d < digits; ++d)
                 dst[d * M] = pack_digits(balanced_digit(wr, gbits, d), balanced_digit(wi, gbits, d));
