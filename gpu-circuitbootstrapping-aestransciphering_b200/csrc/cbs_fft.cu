@@ -123,20 +123,27 @@ __global__ void __launch_bounds__(BrFftCfg<LOGN>::T, BrFftCfg<LOGN>::MIN_BLOCKS)
     }
     __syncthreads();
 
+    // barrier over the TH threads of this half (named barrier 1 + h; 0 is __syncthreads)
+    auto half_bar = [h]() {
+        if (h == 0) asm volatile("bar.sync 1, %0;" ::"n"(TH) : "memory");
+        else asm volatile("bar.sync 2, %0;" ::"n"(TH) : "memory");
+    };
     const uint32_t l2 = 2 * digits;
     const uint64_t* arow = a.a + static_cast<size_t>(ct) * a.a_stride;
     for (uint32_t step = 0; step < a.n; ++step) {
         const uint32_t at = special_ms_f(__ldg(arow + step), TWO_N, a.q_lwe, a.bitwidth);
-        // 1. digits of both polynomials
-        for (uint32_t idx = tid; idx < 2 * M; idx += T) {
-            const uint32_t p = idx / M, e = idx % M;
-            const int64_t wr = prepared_offset(acc[p * N + e], Q, qhalf, round_c, ign);
-            const int64_t wi = prepared_offset(acc[p * N + e + M], Q, qhalf, round_c, ign);
-            uint32_t* dst = dig + p * digits * M + e;
+        // 1. digits of this half's polynomial.  Thread ht writes (and its first FFT pass
+        //    reads) exactly the positions ht + j*TH it owns, so no barrier is needed for dig;
+        //    the barrier after this loop orders the previous step's reads of my_fs before
+        //    the first transform writes it.
+        for (uint32_t e = ht; e < M; e += TH) {
+            const int64_t wr = prepared_offset(my_acc[e], Q, qhalf, round_c, ign);
+            const int64_t wi = prepared_offset(my_acc[e + M], Q, qhalf, round_c, ign);
+            uint32_t* dst = dig + h * digits * M + e;
             for (uint32_t d = 0; d < digits; ++d)
                 dst[d * M] = pack_digits(balanced_digit(wr, gbits, d), balanced_digit(wi, gbits, d));
         }
-        __syncthreads();
+        half_bar();
         // 2. forward transforms and products
         const double2* ek = f.bskf + static_cast<size_t>(step) * l2 * 2 * M + ht;
         double2 y0[8], y1[8];
@@ -153,7 +160,7 @@ __global__ void __launch_bounds__(BrFftCfg<LOGN>::T, BrFftCfg<LOGN>::MIN_BLOCKS)
                     const double im = static_cast<double>(static_cast<int16_t>(v >> 16));
                     return cmul(make_double2(re, im), twist_at<LOGM>(tws, j, e));
                 },
-                x);
+                x, half_bar);
             const double2* k0 = ek + static_cast<size_t>(2 * d + h) * 2 * M;  // key row 2d + h, slot-major
             const double2* k1 = k0 + M;
 #pragma unroll
@@ -161,7 +168,7 @@ __global__ void __launch_bounds__(BrFftCfg<LOGN>::T, BrFftCfg<LOGN>::MIN_BLOCKS)
                 cfma(y0[j], x[j], __ldg(k0 + j * TH));
                 cfma(y1[j], x[j], __ldg(k1 + j * TH));
             }
-            __syncthreads();
+            half_bar();  // the last pass's reads of my_fs are done before it is written again
         }
         // 3. swap partial sums: half 0 keeps output 0, half 1 keeps output 1
 #pragma unroll
@@ -177,31 +184,34 @@ __global__ void __launch_bounds__(BrFftCfg<LOGN>::T, BrFftCfg<LOGN>::MIN_BLOCKS)
         }
         __syncthreads();
         uint64_t tre[8], tim[8];
-        fft_inverse_from_regs<LOGM>(my_fs, ht, tab, y0, [&](int j, uint32_t e, double2 v) {
-            const double2 u = cmulc(v, twist_at<LOGM>(tws, j, e));
-            tre[j] = double_to_mod(u.x * f.inv_m, f, Q);
-            tim[j] = double_to_mod(u.y * f.inv_m, f, Q);
-        });
+        fft_inverse_from_regs<LOGM>(
+            my_fs, ht, tab, y0,
+            [&](int j, uint32_t e, double2 v) {
+                const double2 u = cmulc(v, twist_at<LOGM>(tws, j, e));
+                tre[j] = double_to_mod(u.x * f.inv_m, f, Q);
+                tim[j] = double_to_mod(u.y * f.inv_m, f, Q);
+            },
+            half_bar);
         // 4. rotate-add acc_h += (X^a - 1) t_h: t_h goes to this half's (now idle) FFT buffer,
         //    then each thread updates the positions it owns: acc[i] += t[i - a] - t[i]
-        __syncthreads();
+        half_bar();
         uint64_t* tsm = reinterpret_cast<uint64_t*>(my_fs);  // N words
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
             tsm[ht + j * TH] = tre[j];
             tsm[ht + j * TH + M] = tim[j];
         }
-        __syncthreads();
+        half_bar();
 #pragma unroll 4
-        for (uint32_t k = 0; k < 16; ++k) {
+        for (uint32_t k = 0; k < N / TH; ++k) {
             const uint32_t i = ht + k * TH;
             const uint32_t s = (i + TWO_N - at) & (TWO_N - 1);  // source index of X^a t in [0, 2N)
             const uint64_t v = (s < N) ? tsm[s] : tsm[s - N];
             const uint64_t r = (s < N) ? add_mod(my_acc[i], v, Q) : sub_mod(my_acc[i], v, Q);
             my_acc[i] = sub_mod(r, tsm[i], Q);
         }
-        __syncthreads();
     }
+    __syncthreads();
 
     // finalize (cirbts-batch.cu:2622-2642) and the MV split ct_j = acc * X^-j in the
     // coefficient domain; the caller transforms mv_out to the NTT domain

@@ -279,13 +279,30 @@ __device__ __forceinline__ void dit_pass(double2 (&x)[8], uint32_t m, uint32_t t
     }
 }
 
+// Shared-memory exchanges: the elements a thread reads before pass p (forward) lie in one
+// block of the previous pass, written by the (M >> 3(p-1)) / 8 threads of that block; when
+// that group fits in a warp (aligned, consecutive threads) the exchange needs only
+// __syncwarp().  Before inverse pass p the writers are the (M >> 3p) / 8 threads of the
+// reader's own pass-p block.  Other exchanges call the caller's barrier over the M/8
+// threads of this transform.  Every pass writes exactly the set it read, and the sets of a
+// pass partition [0, M), so no write needs a barrier before it.
+template <int LOGM>
+constexpr bool fwd_exchange_in_warp(int p) {
+    return ((1u << LOGM) >> (3 * (p - 1))) / 8 <= 32;
+}
+template <int LOGM>
+constexpr bool inv_exchange_in_warp(int p) {
+    return ((1u << LOGM) >> (3 * p)) / 8 <= 32;
+}
+
 // Forward FFT of one folded, twisted polynomial by M/8 threads.  tab: the FftTab layout (in
 // shared memory); load(j, e) returns z_e for register slot j (e < M); on return x[j] holds
-// spectrum slot 8*tid + j.  sm: M double2 of shared memory; the caller __syncthreads()
-// before reusing it.
-template <int LOGM, class Load>
+// spectrum slot 8*tid + j.  sm: M double2 of shared memory, which the caller must not let
+// other threads of the group still be reading when this is entered; bar() synchronises the
+// M/8 threads of the transform.
+template <int LOGM, class Load, class Bar>
 __device__ __forceinline__ void fft_forward_to_regs(double2* sm, uint32_t tid, const double2* tab, Load load,
-                                                    double2 (&x)[8]) {
+                                                    double2 (&x)[8], Bar bar) {
     using Pl = NttPlan<LOGM>;
     using Tb = FftTab<LOGM>;
     static_assert(Pl::P >= 2, "fft needs M >= 64");
@@ -296,7 +313,8 @@ __device__ __forceinline__ void fft_forward_to_regs(double2* sm, uint32_t tid, c
     for (int p = 1; p < Pl::P; ++p) {
 #pragma unroll
         for (int j = 0; j < 8; ++j) sm[cswz(pass_index<LOGM, 3>(1u << (3 * (p - 1)), tid, j))] = x[j];
-        __syncthreads();
+        if (fwd_exchange_in_warp<LOGM>(p)) __syncwarp();
+        else bar();
         const uint32_t m = 1u << (3 * p);
         if (p < Pl::P - 1) {
 #pragma unroll
@@ -312,17 +330,20 @@ __device__ __forceinline__ void fft_forward_to_regs(double2* sm, uint32_t tid, c
 
 // Inverse FFT (without the 1/M factor) from the thread's spectrum slots 8*tid + j in x;
 // store(j, e, v) receives element e < M in natural order (register slot j, a compile-time
-// constant after unrolling, so callers can keep per-slot results in registers).
-template <int LOGM, class Store>
+// constant after unrolling, so callers can keep per-slot results in registers).  Same
+// shared-memory contract and barrier as the forward transform; on return other threads of
+// the group may still be reading sm.
+template <int LOGM, class Store, class Bar>
 __device__ __forceinline__ void fft_inverse_from_regs(double2* sm, uint32_t tid, const double2* tab, double2 (&x)[8],
-                                                      Store store) {
+                                                      Store store, Bar bar) {
     using Pl = NttPlan<LOGM>;
     using Tb = FftTab<LOGM>;
     constexpr uint32_t mt = 1u << (3 * (Pl::P - 1));
     dit_pass<LOGM, Pl::tail_r, true>(x, mt, tid, tab + Tb::pass_off(Pl::P - 1));
 #pragma unroll
     for (int j = 0; j < 8; ++j) sm[cswz(pass_index<LOGM, Pl::tail_r>(mt, tid, j))] = x[j];
-    __syncthreads();
+    if (inv_exchange_in_warp<LOGM>(Pl::P - 2)) __syncwarp();
+    else bar();
 #pragma unroll
     for (int p = Pl::P - 2; p >= 0; --p) {
         const uint32_t m = 1u << (3 * p);
@@ -331,10 +352,12 @@ __device__ __forceinline__ void fft_inverse_from_regs(double2* sm, uint32_t tid,
         if (p == 0) dit_pass<LOGM, 3, false>(x, m, tid, tab);
         else dit_pass<LOGM, 3, true>(x, m, tid, tab + Tb::pass_off(p));
         if (p > 0) {
-            // each pass reads and writes its own per-thread set, and the sets partition [0, M)
+            // each pass reads and writes its own per-thread set and the sets partition [0, M), so
+            // the write needs no barrier; the read of pass p - 1 does
 #pragma unroll
             for (int j = 0; j < 8; ++j) sm[cswz(pass_index<LOGM, 3>(m, tid, j))] = x[j];
-            __syncthreads();
+            if (inv_exchange_in_warp<LOGM>(p - 1)) __syncwarp();
+            else bar();
         }
     }
 #pragma unroll
