@@ -146,4 +146,49 @@ class GPUCirBTSContext {
     cbs_context* ctx_ = nullptr;
 };
 
+// ---- Phantom RNS core (include/context.cuh:161, include/ntt.cuh:232-262,
+//      src/eval_key_switch.cu:94) ----
+// Owns the modulus chain Q || P and its device tables (PhantomContext's gpu_rns_tables()).
+class RnsContext {
+   public:
+    RnsContext(uint32_t poly_degree, const std::vector<uint64_t>& q, const std::vector<uint64_t>& p)
+        : size_q_(static_cast<uint32_t>(q.size())), size_p_(static_cast<uint32_t>(p.size())) {
+        check(cbs_rns_context_create(poly_degree, q.data(), size_q_, p.data(), size_p_, &ctx_), "RnsContext");
+    }
+    RnsContext(const RnsContext&) = delete;
+    RnsContext& operator=(const RnsContext&) = delete;
+    ~RnsContext() { cbs_rns_context_destroy(ctx_); }
+
+    [[nodiscard]] cbs_rns_ntt_tables gpu_rns_tables() const {
+        cbs_rns_ntt_tables t{};
+        check(cbs_rns_context_tables(ctx_, &t), "gpu_rns_tables");
+        return t;
+    }
+    // nwt_2d_radix8_forward_inplace(inout, tables, coeff_modulus_size, start_modulus_idx, stream)
+    void nwt_2d_radix8_forward_inplace(uint64_t* inout, size_t coeff_modulus_size, size_t start_modulus_idx,
+                                       const cudaStream_t& s) const {
+        check(cbs_nwt_2d_radix8_forward_inplace(ctx_, inout, static_cast<uint32_t>(coeff_modulus_size),
+                                                static_cast<uint32_t>(start_modulus_idx), as_stream(s)),
+              "nwt_2d_radix8_forward_inplace");
+    }
+    void nwt_2d_radix8_backward_inplace(uint64_t* inout, size_t coeff_modulus_size, size_t start_modulus_idx,
+                                        const cudaStream_t& s) const {
+        check(cbs_nwt_2d_radix8_backward_inplace(ctx_, inout, static_cast<uint32_t>(coeff_modulus_size),
+                                                 static_cast<uint32_t>(start_modulus_idx), as_stream(s)),
+              "nwt_2d_radix8_backward_inplace");
+    }
+    // keyswitch_inplace(context, encrypted, c2, relin_keys, is_relin, stream), CKKS form:
+    // ct [count][2][size_ql][N] += keyswitch(c2 [count][size_ql][N]); evks = one key per digit
+    void keyswitch_inplace(uint64_t* ct, const uint64_t* c2, const std::vector<const uint64_t*>& evks,
+                           uint32_t size_ql, uint32_t count, const cudaStream_t& s) const {
+        check(cbs_rns_keyswitch_inplace(ctx_, ct, c2, evks.data(), size_ql, count, as_stream(s)),
+              "keyswitch_inplace");
+    }
+    [[nodiscard]] cbs_rns_context* handle() const { return ctx_; }
+
+   private:
+    uint32_t size_q_, size_p_;
+    cbs_rns_context* ctx_ = nullptr;
+};
+
 }  // namespace cbs_b200

@@ -84,3 +84,25 @@ def test_rns_context_validation_without_device(lib, oracle):
     assert create(n, np.array([good[0] + 2]), good[2:]) == 1   # not prime / not 1 mod 2N
     assert create(n, good[:1], np.array(oracle_primes(oracle, n, 50, 20)[3:20], np.uint64)) == 1  # alpha > 16
     assert h.value is None
+
+
+def test_cpp_facade_compiles(tmp_path):
+    """include/cbs_b200.hpp (the reference-shaped C++ surface) compiles against the C ABI."""
+    import shutil
+    import subprocess
+    from conftest import ROOT
+    gxx = shutil.which("g++")
+    if gxx is None:
+        pytest.skip("no C++ compiler")
+    src = tmp_path / "facade.cpp"
+    src.write_text('#include "cbs_b200.hpp"\n'
+                   'int main() {\n'
+                   '  using namespace cbs_b200;\n'
+                   '  void (*f)(uint64_t*, const uint64_t*, const uint64_t*, const cbs_dmodulus*, size_t, size_t,\n'
+                   '            const cudaStream_t&) = fnwt_1d_opt_batched;\n'
+                   '  (void)f;\n'
+                   '  return sizeof(GPUCirBTSContext) > 0 && sizeof(RnsContext) > 0 ? 0 : 1;\n'
+                   '}\n')
+    r = subprocess.run([gxx, "-std=c++17", "-fsyntax-only", "-I", str(ROOT / "include"), "-I",
+                        "/usr/local/cuda/include", str(src)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
