@@ -426,6 +426,74 @@ def run_rns_ntt(args, rank: int, world: int, local_rank: int) -> None:
     ctx.close()
 
 
+def run_gate(args, rank: int, world: int, local_rank: int) -> None:
+    """Plain gate bootstrapping (torus-32, n=636, N=1024, base 2^7 x 3, FP64 FFT): `--batch`
+    NAND gates per step (default 64, the configuration's batch), inputs resident in HBM."""
+    import torch
+    torch.cuda.set_device(local_rank)
+    pkg = load_pkg()
+    count = args.batch or 64
+    ctx = pkg.GateContext(max_batch=count)
+    ctx.keygen(args.seed)
+    p = ctx.params
+    rng = np.random.default_rng(args.seed + rank)
+    x = rng.integers(0, 2, count).astype(np.uint8)
+    y = rng.integers(0, 2, count).astype(np.uint8)
+    a1, b1 = ctx.encrypt(x, seed=args.seed + 1)
+    a2, b2 = ctx.encrypt(y, seed=args.seed + 2)
+    dev = lambda v: torch.from_numpy(np.ascontiguousarray(v).view(np.int32)).cuda()  # noqa: E731
+    d = [dev(v) for v in (a1, b1, a2, b2)]
+    oa = torch.zeros((count, p.n), dtype=torch.int32, device="cuda")
+    ob = torch.zeros(count, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.Stream()
+    fn = lambda: pkg.call("cbs_gate_eval_batch_device", ctx.handle, pkg.GATE_NAND,  # noqa: E731
+                          *(t.data_ptr() for t in d), count, oa.data_ptr(), ob.data_ptr(), stream.cuda_stream)
+    with ClockSampler(local_rank) as clk:
+        ms = _timed(torch, stream, fn, args.warmup, args.steps)
+    torch.cuda.synchronize()
+    ok = int((ctx.decrypt(oa.cpu().numpy().view(np.uint32), ob.cpu().numpy().view(np.uint32)) == 1 - (x & y)).sum())
+    # e2e: inputs from pinned host memory, outputs back to the host, every step
+    h_in = [t.cpu().pin_memory() for t in d]
+    h_oa = torch.empty(oa.shape, dtype=torch.int32).pin_memory()
+    h_ob = torch.empty(ob.shape, dtype=torch.int32).pin_memory()
+
+    def e2e():
+        with torch.cuda.stream(stream):
+            for t, h in zip(d, h_in):
+                t.copy_(h, non_blocking=True)
+            fn()
+            h_oa.copy_(oa, non_blocking=True)
+            h_ob.copy_(ob, non_blocking=True)
+
+    e2e_ms = _timed(torch, stream, e2e, 1, max(1, args.steps))
+    M = p.N // 2
+    logm = M.bit_length() - 1
+    flop = count * p.n * ((2 * p.levels + 2) * 5 * M * logm + 2 * 2 * p.levels * M * 8)
+    key_bytes = p.n * 2 * p.levels * 2 * M * 16 + p.N * p.ks_levels * ((1 << p.ks_base_bits) - 1) * (p.n + 1) * 4
+    peaks = measured_peaks()
+    gbs = key_bytes / (ms * 1e-3) / 1e9
+    out = {"metric": f"NAND gate bootstraps/s (torus32, n={p.n}, N={p.N}, FP64 FFT)",
+           "value": world * count / (ms * 1e-3), "unit": "gates/s", "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64 (FFT products, exact after rounding) + u32 torus",
+           "data": "synthetic (seeded uniform random input bits)",
+           "config": {"workload": "gate_nand", "batch": count, "n": p.n, "N": p.N,
+                      "gadget": f"2^{p.bg_bits}x{p.levels}", "ks": f"2^{p.ks_base_bits}x{p.ks_levels}",
+                      "l2": "keys (62 MB spectra + 62 MB KSK) stay L2/HBM resident; no flush"},
+           "us_per_gate": ms * 1e3 / count, "correct_gates": ok, "gpu_launches": args.steps * 2,
+           "e2e": {"value": world * count / (e2e_ms * 1e-3), "unit": "gates/s",
+                   "h2d_bytes_per_step": 2 * count * (p.n + 1) * 4, "d2h_bytes_per_step": count * (p.n + 1) * 4},
+           "roofline": {"kernel": "k_gate_blind_rotate + k_gate_keyswitch", "bound": "hbm", "achieved": gbs,
+                        "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": gbs / peaks["hbm_gbs"],
+                        "peak_src": peaks["src"], "traffic": None,
+                        "note": "key bytes once per step; the blind rotation is FP64-bound, see compute_rate"},
+           "compute_rate": {"fp64_flop_per_step": flop, "achieved_fp64_tflops": flop / (ms * 1e-3) / 1e12},
+           "clocks": clk.summary()}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    ctx.close()
+
+
 def compute_rate(backend: str, T: int, p, br_ms: float) -> dict:
     """Algorithmic arithmetic of one blind-rotation launch over T ciphertexts."""
     N, n, l2 = p.N, p.n, 2 * p.digits_g
@@ -522,7 +590,7 @@ def main() -> None:
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--backend", choices=["fft64", "ntt"], default="fft64")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
-    ap.add_argument("--workload", choices=["aes128", "blind_rotate", "keyswitch", "rns_ntt"], default="aes128",
+    ap.add_argument("--workload", choices=["aes128", "blind_rotate", "keyswitch", "rns_ntt", "gate"], default="aes128",
                     help="aes128 is the headline; the others time one kernel family")
     ap.add_argument("--batch", type=int, default=0, help="units per step for the kernel workloads")
     ap.add_argument("--alpha", type=int, default=2, help="special primes (digit width) for --workload keyswitch")
@@ -541,7 +609,7 @@ def main() -> None:
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     runner = {"aes128": run_ours, "blind_rotate": run_blind_rotate, "keyswitch": run_keyswitch,
-              "rns_ntt": run_rns_ntt}[args.workload]
+              "rns_ntt": run_rns_ntt, "gate": run_gate}[args.workload]
     try:
         runner(args, rank, world, local_rank)
     finally:

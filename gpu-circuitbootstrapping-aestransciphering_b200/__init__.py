@@ -96,6 +96,16 @@ def _declare(lib: ctypes.CDLL) -> None:
         "cbs_lwe_decrypt_bits": (st, [c_vp, c_vp, c_vp, u32, u32, c_vp]),
         "cbs_circuit_bootstrap_noalloc_capacity_words": (sz, []),
         "cbs_circuit_bootstrap_batch_device_noalloc": (st, [c_vp, c_vp, c_vp, u32, u32, c_vp, c_vp]),
+        "cbs_gate_params_default": (st, [c_vp]),
+        "cbs_gate_context_create": (st, [c_vp, u32, c_vp]),
+        "cbs_gate_context_destroy": (st, [c_vp]),
+        "cbs_gate_keygen": (st, [c_vp, u64]),
+        "cbs_gate_generate_keys_host": (st, [c_vp, u64, c_vp, c_vp, c_vp, c_vp]),
+        "cbs_gate_export_keys": (st, [c_vp, c_vp, c_vp, c_vp, c_vp]),
+        "cbs_gate_encrypt_bits": (st, [c_vp, c_vp, u32, u64, c_vp, c_vp]),
+        "cbs_gate_decrypt_bits": (st, [c_vp, c_vp, c_vp, u32, c_vp]),
+        "cbs_gate_eval_batch_device": (st, [c_vp, ctypes.c_int, c_vp, c_vp, c_vp, c_vp, u32, c_vp, c_vp, c_vp]),
+        "cbs_gate_bootstrap_batch_device": (st, [c_vp, c_vp, c_vp, u32, c_vp, c_vp, c_vp, c_vp]),
         "cbs_rns_context_create": (st, [u32, c_vp, u32, c_vp, u32, c_vp]),
         "cbs_rns_context_destroy": (st, [c_vp]),
         "cbs_rns_context_tables": (st, [c_vp, c_vp]),
@@ -177,6 +187,88 @@ class Context:
         out = key_buffers(self.params)
         call("cbs_export_keys", self._h, *(out[k].ctypes.data for k in KEY_FIELDS))
         return out
+
+
+GATE_OR, GATE_AND, GATE_NOR, GATE_NAND, GATE_XOR, GATE_XNOR = range(6)
+
+
+class GateParams(ctypes.Structure):
+    """Mirror of cbs_gate_params (include/cbs_b200.h)."""
+    _fields_ = [("n", ctypes.c_uint32), ("N", ctypes.c_uint32), ("bg_bits", ctypes.c_uint32),
+                ("levels", ctypes.c_uint32), ("ks_base_bits", ctypes.c_uint32), ("ks_levels", ctypes.c_uint32),
+                ("sigma_lwe", ctypes.c_double), ("sigma_rlwe", ctypes.c_double)]
+
+
+def gate_default_params() -> GateParams:
+    p = GateParams()
+    call("cbs_gate_params_default", ctypes.byref(p))
+    return p
+
+
+def gate_key_buffers(p: GateParams) -> dict:
+    import numpy as np
+    base = 1 << p.ks_base_bits
+    return dict(s_lwe=np.zeros(p.n, np.int32), z_rlwe=np.zeros(p.N, np.int32),
+                bsk=np.zeros((p.n, 2 * p.levels, 2, p.N), np.uint32),
+                ksk=np.zeros((p.N, p.ks_levels, base - 1, p.n + 1), np.uint32))
+
+
+def gate_generate_keys_host(p: GateParams, seed: int) -> dict:
+    """Gate-bootstrapping keys on the host only; same keys as GateContext.keygen(seed)."""
+    k = gate_key_buffers(p)
+    call("cbs_gate_generate_keys_host", ctypes.byref(p), seed, k["s_lwe"].ctypes.data, k["z_rlwe"].ctypes.data,
+         k["bsk"].ctypes.data, k["ksk"].ctypes.data)
+    return k
+
+
+class GateContext:
+    """Owning handle of a cbs_gate_context (the GPUBinFHEContext counterpart)."""
+
+    def __init__(self, params: GateParams | None = None, max_batch: int = 64):
+        self.params = params if params is not None else gate_default_params()
+        self.max_batch = max_batch
+        self._h = ctypes.c_void_p()
+        call("cbs_gate_context_create", ctypes.byref(self.params), max_batch, ctypes.byref(self._h))
+
+    @property
+    def handle(self) -> int:
+        return self._h.value
+
+    def keygen(self, seed: int) -> None:
+        call("cbs_gate_keygen", self._h, seed)
+
+    def encrypt(self, bits, seed: int):
+        import numpy as np
+        bits = np.ascontiguousarray(bits, dtype=np.uint8)
+        a = np.zeros((len(bits), self.params.n), np.uint32)
+        b = np.zeros(len(bits), np.uint32)
+        call("cbs_gate_encrypt_bits", self._h, bits.ctypes.data, len(bits), seed, a.ctypes.data, b.ctypes.data)
+        return a, b
+
+    def decrypt(self, a, b):
+        import numpy as np
+        a = np.ascontiguousarray(a, dtype=np.uint32)
+        b = np.ascontiguousarray(b, dtype=np.uint32)
+        out = np.zeros(len(b), np.uint8)
+        call("cbs_gate_decrypt_bits", self._h, a.ctypes.data, b.ctypes.data, len(b), out.ctypes.data)
+        return out
+
+    def export_keys(self) -> dict:
+        k = gate_key_buffers(self.params)
+        call("cbs_gate_export_keys", self._h, k["s_lwe"].ctypes.data, k["z_rlwe"].ctypes.data, k["bsk"].ctypes.data,
+             k["ksk"].ctypes.data)
+        return k
+
+    def close(self) -> None:
+        if self._h.value:
+            load().cbs_gate_context_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class RnsContext:

@@ -1,0 +1,599 @@
+// gate.cu -- gate bootstrapping on the 32-bit torus with the FP64 FFT external product.
+//
+// The path of GPUBinFHEContext::BatchGPUEvalBinGate (bitwise/src/binfhe-base-scheme-batch.cu:
+// 82-200): linear gate combination of two LWE ciphertexts, modulus switch to 2N, GINX blind
+// rotation of the test vector 1/8 (binfhe-base-scheme-batch.cu:16-74, bitwise/src/
+// rgsw-acc-batch.cu), sample extract of coefficient 0 and the LWE key switch N -> n
+// (binfhe-base-scheme-batch.cu:119-185).  The reference runs the external product through
+// cuFFTDx in FP64 (bitwise/src/fft.cu:3614-3883); here it is the register-blocked FFT of
+// fft_core.cuh.  Parameters are the torus form of the configuration (32-bit torus, binary
+// secrets), so every residue is a uint32 and every modular reduction is the natural wrap.
+// Products of 7-bit digits by 32-bit keys over N <= 2048 stay below 2^51 in magnitude, so
+// rounding the FFT output recovers the exact integer product: the results equal exact
+// integer arithmetic (checked bit for bit against the oracle).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <complex>
+#include <memory>
+#include <new>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "common.cuh"
+#include "devbuf.cuh"
+#include "fft_core.cuh"
+#include "fft_kernels.cuh"
+#include "keygen.h"
+
+namespace cbs {
+
+struct GateArgs {
+    int gate;              // CBS_GATE_* or -1: bootstrap in1 as is
+    const uint32_t* a1;    // [count][n]
+    const uint32_t* b1;    // [count]
+    const uint32_t* a2;
+    const uint32_t* b2;
+    uint32_t n, levels, bg_bits;
+    const double2* bskf;   // [n][2*levels][2][M] key spectra, slot-major rows
+    const double2* tab;    // FftTab<log2 M>
+    uint32_t* ext;         // [count][N+1] extracted LWE (a then b)
+};
+
+__device__ __forceinline__ uint32_t gate_a(int gate, uint32_t x1, uint32_t x2) {
+    const uint32_t s = x1 + x2;
+    switch (gate) {
+        case 0: case 1: return s;
+        case 2: case 3: return 0u - s;
+        case 4: return 2u * s;
+        case 5: return 0u - 2u * s;
+        default: return x1;
+    }
+}
+
+__device__ __forceinline__ uint32_t gate_b(int gate, uint32_t x1, uint32_t x2) {
+    const uint32_t e8 = 1u << 29, e4 = 1u << 30, s = x1 + x2;
+    switch (gate) {
+        case 0: return e8 + s;
+        case 1: return (0u - e8) + s;
+        case 2: return (0u - e8) - s;
+        case 3: return e8 - s;
+        case 4: return e4 + 2u * s;
+        case 5: return (0u - e4) - 2u * s;
+        default: return x1;
+    }
+}
+
+template <int LOGM>
+__device__ __forceinline__ double2 gate_twist(const double2* tws, int j, uint32_t e) {
+    if (j < 4) return tws[e];
+    const double2 t = tws[(1u << LOGM) - e];
+    return make_double2(t.y, t.x);
+}
+
+template <int LOGN>
+struct GateCfg {
+    static constexpr uint32_t T = (1u << LOGN) / 8;
+    static constexpr int MIN_BLOCKS = LOGN <= 10 ? 4 : 2;
+};
+
+// One CTA of two halves (M/8 threads each) per ciphertext; half h owns accumulator component
+// h (0: a, 1: b), all in shared memory.  Same step structure as k_blind_rotate_fft: digits of
+// the own component, forward FFT + products against both key columns per digit, swap of
+// partial sums, inverse FFT, rounding to the torus, rotate-add acc += (X^a - 1) t in place.
+template <int LOGN>
+__global__ void __launch_bounds__(GateCfg<LOGN>::T, GateCfg<LOGN>::MIN_BLOCKS) k_gate_blind_rotate(const GateArgs a) {
+    constexpr int LOGM = LOGN - 1;
+    constexpr uint32_t N = 1u << LOGN, M = N / 2, TH = M / 8, T = 2 * TH, TWO_N = 2 * N;
+    constexpr uint32_t SH = 32 - (LOGN + 1);  // torus -> Z_2N
+    using Tb = FftTab<LOGM>;
+    extern __shared__ __align__(16) uint64_t smem[];
+    double2* fs = reinterpret_cast<double2*>(smem);                 // [2][M]
+    double2* tab = fs + 2 * M;                                      // FftTab<LOGM>
+    uint32_t* acc = reinterpret_cast<uint32_t*>(tab + Tb::size());  // [2][N]
+    uint32_t* dig = acc + 2 * N;                                    // [2][levels][M] packed pairs
+    const double2* tws = tab + Tb::twist_off();
+    const uint32_t ct = blockIdx.x, tid = threadIdx.x;
+    const uint32_t h = tid / TH, ht = tid % TH;
+    uint32_t* my_acc = acc + h * N;
+    double2* my_fs = fs + h * M;
+    const uint32_t levels = a.levels, bg = a.bg_bits;
+    uint32_t off = 1u << (32 - levels * bg - 1);  // rounding of the dropped bits
+    for (uint32_t k = 0; k < levels; ++k) off += (1u << (bg - 1)) << (32 - (k + 1) * bg);
+    auto half_bar = [h]() {
+        if (h == 0) asm volatile("bar.sync 1, %0;" ::"n"(TH) : "memory");
+        else asm volatile("bar.sync 2, %0;" ::"n"(TH) : "memory");
+    };
+    auto ms = [](uint32_t x) { return ((x + (1u << (SH - 1))) >> SH) & (TWO_N - 1); };
+
+    for (uint32_t i = tid; i < Tb::size(); i += T) tab[i] = a.tab[i];
+    const uint32_t* a1 = a.a1 + static_cast<size_t>(ct) * a.n;
+    const uint32_t* a2 = a.a2 ? a.a2 + static_cast<size_t>(ct) * a.n : a1;
+    {
+        const uint32_t b = gate_b(a.gate, a.b1[ct], a.b2 ? a.b2[ct] : 0u);
+        const uint32_t bt = ms(b);
+        for (uint32_t i = tid; i < N; i += T) {
+            acc[i] = 0;
+            acc[N + i] = (((i + bt) & (TWO_N - 1)) < N) ? (1u << 29) : (0u - (1u << 29));
+        }
+    }
+    __syncthreads();
+
+    const uint32_t l2 = 2 * levels;
+    for (uint32_t step = 0; step < a.n; ++step) {
+        const uint32_t at = ms(gate_a(a.gate, __ldg(a1 + step), __ldg(a2 + step)));
+        if (at == 0) continue;  // X^0 - 1 = 0: the step adds nothing (uniform over the CTA)
+        for (uint32_t e = ht; e < M; e += TH) {
+            const uint32_t wr = my_acc[e] + off, wi = my_acc[e + M] + off;
+            uint32_t* dst = dig + h * levels * M + e;
+            for (uint32_t k = 0; k < levels; ++k) {
+                const uint32_t s = 32 - (k + 1) * bg, mask = (1u << bg) - 1, half = 1u << (bg - 1);
+                const int32_t dr = static_cast<int32_t>((wr >> s) & mask) - static_cast<int32_t>(half);
+                const int32_t di = static_cast<int32_t>((wi >> s) & mask) - static_cast<int32_t>(half);
+                dst[k * M] = (static_cast<uint32_t>(dr) & 0xffffu) | (static_cast<uint32_t>(di) << 16);
+            }
+        }
+        half_bar();
+        const double2* ek = a.bskf + static_cast<size_t>(step) * l2 * 2 * M + ht;
+        double2 y0[8], y1[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) y0[j] = y1[j] = make_double2(0.0, 0.0);
+        for (uint32_t d = 0; d < levels; ++d) {
+            const uint32_t* dsrc = dig + (h * levels + d) * M;
+            double2 x[8];
+            fft_forward_to_regs<LOGM>(
+                my_fs, ht, tab,
+                [&](int j, uint32_t e) {
+                    const uint32_t v = dsrc[e];
+                    const double re = static_cast<double>(static_cast<int16_t>(v & 0xffffu));
+                    const double im = static_cast<double>(static_cast<int16_t>(v >> 16));
+                    return cmul(make_double2(re, im), gate_twist<LOGM>(tws, j, e));
+                },
+                x, half_bar);
+            const double2* k0 = ek + static_cast<size_t>(2 * d + h) * 2 * M;
+            const double2* k1 = k0 + M;
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                cfma(y0[j], x[j], __ldg(k0 + j * TH));
+                cfma(y1[j], x[j], __ldg(k1 + j * TH));
+            }
+            half_bar();
+        }
+#pragma unroll
+        for (int j = 0; j < 8; ++j) my_fs[cswz(8 * ht + j)] = h ? y0[j] : y1[j];
+        __syncthreads();
+        {
+            const double2* take = fs + (1 - h) * M;
+#pragma unroll
+            for (int j = 0; j < 8; ++j) y0[j] = cadd(h ? y1[j] : y0[j], take[cswz(8 * ht + j)]);
+        }
+        __syncthreads();
+        uint32_t tre[8], tim[8];
+        constexpr double inv_m = 1.0 / M;
+        fft_inverse_from_regs<LOGM>(
+            my_fs, ht, tab, y0,
+            [&](int j, uint32_t e, double2 v) {
+                const double2 u = cmulc(v, gate_twist<LOGM>(tws, j, e));
+                tre[j] = static_cast<uint32_t>(static_cast<uint64_t>(__double2ll_rn(u.x * inv_m)));
+                tim[j] = static_cast<uint32_t>(static_cast<uint64_t>(__double2ll_rn(u.y * inv_m)));
+            },
+            half_bar);
+        half_bar();
+        uint32_t* tsm = reinterpret_cast<uint32_t*>(my_fs);  // N words
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            tsm[ht + j * TH] = tre[j];
+            tsm[ht + j * TH + M] = tim[j];
+        }
+        half_bar();
+#pragma unroll 4
+        for (uint32_t k = 0; k < N / TH; ++k) {
+            const uint32_t i = ht + k * TH;
+            const uint32_t s = (i + TWO_N - at) & (TWO_N - 1);
+            const uint32_t v = (s < N) ? tsm[s] : 0u - tsm[s - N];
+            my_acc[i] += v - tsm[i];
+        }
+    }
+    __syncthreads();
+    // sample extract of coefficient 0: a'_0 = a_0, a'_i = -a_(N-i), b' = b_0
+    uint32_t* out = a.ext + static_cast<size_t>(ct) * (N + 1);
+    for (uint32_t i = tid; i <= N; i += T) {
+        uint32_t v;
+        if (i == N) v = acc[N];
+        else if (i == 0) v = acc[0];
+        else v = 0u - acc[N - i];
+        out[i] = v;
+    }
+}
+
+// LWE key switch N -> n of one extracted ciphertext per blockIdx.y; thread j < n + 1 of the
+// grid owns output coefficient j (j = n is b).  The digits of a'_i are the same for every
+// thread, so the inner loop is uniform and each step reads one coalesced key row segment.
+__global__ void __launch_bounds__(256) k_gate_keyswitch(const uint32_t* __restrict__ ext,
+                                                        const uint32_t* __restrict__ ksk, uint32_t n, uint32_t N,
+                                                        uint32_t ks_bits, uint32_t ks_levels,
+                                                        uint32_t* __restrict__ out_a, uint32_t* __restrict__ out_b) {
+    extern __shared__ uint32_t s_ext[];
+    const uint32_t ct = blockIdx.y;
+    const uint32_t* src = ext + static_cast<size_t>(ct) * (N + 1);
+    for (uint32_t i = threadIdx.x; i <= N; i += blockDim.x) s_ext[i] = src[i];
+    __syncthreads();
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j > n) return;
+    const uint32_t base = 1u << ks_bits, round = 1u << (32 - ks_levels * ks_bits - 1);
+    uint32_t accv = (j == n) ? s_ext[N] : 0u;
+    for (uint32_t i = 0; i < N; ++i) {
+        const uint32_t x = s_ext[i] + round;
+        const uint32_t* rows = ksk + static_cast<size_t>(i) * ks_levels * (base - 1) * (n + 1) + j;
+        for (uint32_t l = 0; l < ks_levels; ++l) {
+            const uint32_t v = (x >> (32 - (l + 1) * ks_bits)) & (base - 1);
+            if (v) accv -= __ldg(rows + (static_cast<size_t>(l) * (base - 1) + (v - 1)) * (n + 1));
+        }
+    }
+    if (j < n) out_a[static_cast<size_t>(ct) * n + j] = accv;
+    else out_b[ct] = accv;
+}
+
+template <int LOGN>
+static cudaError_t gate_br_launch(const GateArgs& a, uint32_t count, cudaStream_t s) {
+    constexpr uint32_t N = 1u << LOGN, M = N / 2;
+    const size_t smem = (2ull * M + FftTab<LOGN - 1>::size()) * sizeof(double2) + 2ull * N * sizeof(uint32_t) +
+                        2ull * a.levels * M * sizeof(uint32_t);
+    static size_t configured[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (configured[dev] < smem) {
+        cudaError_t e = cudaFuncSetAttribute(k_gate_blind_rotate<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             static_cast<int>(smem));
+        if (e != cudaSuccess) return e;
+        configured[dev] = smem;
+    }
+    k_gate_blind_rotate<LOGN><<<count, GateCfg<LOGN>::T, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace cbs
+
+// ---------------------------------------------------------------------------------------
+// host side: keys and the C ABI
+// ---------------------------------------------------------------------------------------
+
+using cbs::DevBuf;
+
+struct cbs_gate_context {
+    cbs_gate_params p{};
+    uint32_t max_batch = 0;
+    bool keys_ready = false;
+    std::vector<int32_t> s, z;      // LWE key (n), RLWE key (N), binary
+    std::vector<uint32_t> bsk, ksk;  // coefficient form (exported) / device layout
+    DevBuf<double2> d_bskf, d_tab;
+    DevBuf<uint32_t> d_ksk, d_ext, d_tmp_a, d_tmp_b;
+};
+
+namespace {
+
+using cbs::set_error;
+
+uint32_t torus_from_double(double x) {  // x in torus units (any real), rounded to 2^-32
+    const double f = x - std::floor(x);
+    return static_cast<uint32_t>(static_cast<uint64_t>(std::llround(f * 4294967296.0)));
+}
+
+uint32_t torus_noise(cbs::Rng& rng, double sigma) {
+    return static_cast<uint32_t>(static_cast<int64_t>(std::llround(rng.gaussian() * sigma * 4294967296.0)));
+}
+
+// b += a * z (negacyclic, z binary), mod 2^32
+void mul_binary_acc(const uint32_t* a, const int32_t* z, uint32_t N, uint32_t* b) {
+    for (uint32_t j = 0; j < N; ++j) {
+        if (!z[j]) continue;
+        for (uint32_t i = 0; i < N; ++i) {
+            if (i + j < N) b[i + j] += a[i];
+            else b[i + j - N] -= a[i];
+        }
+    }
+}
+
+template <int LOGM>
+void torus_keys_to_fft(const uint32_t* keys, size_t count, std::vector<double2>& out) {
+    constexpr uint32_t M = 1u << LOGM, N = 2 * M;
+    using cld = std::complex<long double>;
+    const long double pi = 3.141592653589793238462643383279502884L;
+    std::vector<cld> w(M / 2), twist(M);
+    for (uint32_t e = 0; e < M / 2; ++e) w[e] = std::polar(1.0L, 2.0L * pi * e / M);
+    for (uint32_t e = 0; e < M; ++e) twist[e] = std::polar(1.0L, pi * e / N);
+    out.assign(count * M, make_double2(0, 0));
+    const unsigned nth = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    std::vector<std::thread> pool;
+    for (unsigned th = 0; th < nth; ++th) {
+        pool.emplace_back([&, th] {
+            std::vector<cld> zz(M);
+            for (size_t k = th; k < count; k += nth) {
+                const uint32_t* c = keys + k * N;
+                for (uint32_t e = 0; e < M; ++e) {
+                    const long double re = static_cast<long double>(static_cast<int32_t>(c[e]));
+                    const long double im = static_cast<long double>(static_cast<int32_t>(c[e + M]));
+                    zz[e] = cld(re, im) * twist[e];
+                }
+                // decimation-in-frequency, natural order in, bit-reversed out (fft_core.cuh)
+                for (size_t hh = M / 2; hh >= 1; hh /= 2) {
+                    const size_t stride = M / (2 * hh);
+                    for (size_t s0 = 0; s0 < M; s0 += 2 * hh)
+                        for (size_t j = 0; j < hh; ++j) {
+                            const cld u = zz[s0 + j], v = zz[s0 + j + hh];
+                            zz[s0 + j] = u + v;
+                            zz[s0 + j + hh] = (u - v) * w[j * stride];
+                        }
+                    if (hh == 1) break;
+                }
+                for (uint32_t e = 0; e < M; ++e)
+                    out[k * M + (e % 8) * (M / 8) + e / 8] =
+                        make_double2(static_cast<double>(zz[e].real()), static_cast<double>(zz[e].imag()));
+            }
+        });
+    }
+    for (auto& t : pool) t.join();
+}
+
+cbs_status validate_gate(const cbs_gate_params& p) {
+    CBS_CHECK_ARG(p.N == 1024 || p.N == 2048, "gate: N must be 1024 or 2048");
+    CBS_CHECK_ARG(p.n >= 1 && p.n <= 4096, "gate: n out of range");
+    CBS_CHECK_ARG(p.bg_bits >= 1 && p.bg_bits <= 15 && p.levels >= 1 && p.levels <= 4 && p.bg_bits * p.levels <= 30,
+                  "gate: need bg_bits <= 15, levels <= 4, bg_bits * levels <= 30");
+    CBS_CHECK_ARG(p.ks_base_bits >= 1 && p.ks_base_bits <= 8 && p.ks_levels >= 1 &&
+                      p.ks_base_bits * p.ks_levels <= 31,
+                  "gate: key-switch base and levels out of range");
+    CBS_CHECK_ARG(p.sigma_lwe >= 0 && p.sigma_rlwe >= 0 && p.sigma_lwe < 0.01 && p.sigma_rlwe < 0.01,
+                  "gate: noise out of range");
+    // 2^(bg-1) * 2^31 * N * 2*levels must stay below 2^52 for the FFT products to round exactly
+    const double bound = std::ldexp(1.0, static_cast<int>(p.bg_bits) - 1 + 31) * p.N * 2 * p.levels;
+    CBS_CHECK_ARG(bound < std::ldexp(1.0, 52), "gate: parameters exceed the exact FP64 product range");
+    return CBS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+cbs_status cbs_gate_params_default(cbs_gate_params* out) {
+    CBS_CHECK_ARG(out, "gate_params_default: null argument");
+    out->n = 636;
+    out->N = 1024;
+    out->bg_bits = 7;
+    out->levels = 3;
+    out->ks_base_bits = 2;
+    out->ks_levels = 8;
+    out->sigma_lwe = std::ldexp(1.0, -15);
+    out->sigma_rlwe = std::ldexp(1.0, -25);
+    return CBS_OK;
+}
+
+cbs_status cbs_gate_context_create(const cbs_gate_params* params, uint32_t max_batch, cbs_gate_context** out) {
+    CBS_CHECK_ARG(params && out, "gate_context_create: null argument");
+    *out = nullptr;
+    CBS_CHECK_ARG(max_batch >= 1 && max_batch <= (1u << 22), "gate_context_create: max_batch out of range");
+    if (cbs_status st = validate_gate(*params)) return st;
+    auto* c = new (std::nothrow) cbs_gate_context();
+    if (!c) {
+        set_error("gate_context_create: host allocation failed");
+        return CBS_ERR_OOM;
+    }
+    std::unique_ptr<cbs_gate_context> guard(c);
+    c->p = *params;
+    c->max_batch = max_batch;
+    CBS_CUDA_TRY(c->d_ext.alloc(static_cast<size_t>(max_batch) * (params->N + 1)));
+    CBS_CUDA_TRY(c->d_tmp_a.alloc(static_cast<size_t>(max_batch) * params->n));
+    CBS_CUDA_TRY(c->d_tmp_b.alloc(max_batch));
+    *out = guard.release();
+    return CBS_OK;
+}
+
+cbs_status cbs_gate_context_destroy(cbs_gate_context* ctx) {
+    delete ctx;
+    return CBS_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// seeded host key generation (no device): s (n), z (N) binary; BSK rows 2k+c = RLWE_z(0) with
+// s_i * 2^(32-(k+1)*bg_bits) added to component c; KSK rows LWE_s(v * z_i * 2^(32-(l+1)*ks_bits))
+void gate_keys_host(const cbs_gate_params& p, uint64_t seed, std::vector<int32_t>& s_out, std::vector<int32_t>& z_out,
+                    std::vector<uint32_t>& bsk, std::vector<uint32_t>& ksk) {
+    const uint32_t n = p.n, N = p.N, L = p.levels, base = 1u << p.ks_base_bits;
+    cbs::Rng rng(seed ^ 0x6a7e5b07c0ffee11ull);
+    s_out.assign(n, 0);
+    z_out.assign(N, 0);
+    for (auto& v : s_out) v = static_cast<int32_t>(rng.uniform(2));
+    for (auto& v : z_out) v = static_cast<int32_t>(rng.uniform(2));
+    bsk.assign(static_cast<size_t>(n) * 2 * L * 2 * N, 0);
+    for (uint32_t i = 0; i < n; ++i)
+        for (uint32_t r = 0; r < 2 * L; ++r) {
+            uint32_t* ra = bsk.data() + ((static_cast<size_t>(i) * 2 * L + r) * 2) * N;
+            uint32_t* rb = ra + N;
+            for (uint32_t e = 0; e < N; ++e) {
+                ra[e] = static_cast<uint32_t>(rng.next());
+                rb[e] = torus_noise(rng, p.sigma_rlwe);
+            }
+        }
+    {  // b += a * z for every row, in parallel (binary z: shifted additions)
+        const unsigned nth = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+        std::vector<std::thread> pool;
+        const size_t rows = static_cast<size_t>(n) * 2 * L;
+        for (unsigned th = 0; th < nth; ++th)
+            pool.emplace_back([&, th] {
+                for (size_t r = th; r < rows; r += nth) {
+                    uint32_t* ra = bsk.data() + r * 2 * N;
+                    mul_binary_acc(ra, z_out.data(), N, ra + N);
+                }
+            });
+        for (auto& t : pool) t.join();
+    }
+    for (uint32_t i = 0; i < n; ++i)
+        for (uint32_t k = 0; k < L; ++k)
+            for (uint32_t c = 0; c < 2; ++c) {
+                uint32_t* row = bsk.data() + ((static_cast<size_t>(i) * 2 * L + 2 * k + c) * 2 + c) * N;
+                row[0] += static_cast<uint32_t>(s_out[i]) << (32 - (k + 1) * p.bg_bits);
+            }
+    ksk.assign(static_cast<size_t>(N) * p.ks_levels * (base - 1) * (n + 1), 0);
+    for (uint32_t i = 0; i < N; ++i)
+        for (uint32_t l = 0; l < p.ks_levels; ++l)
+            for (uint32_t v = 1; v < base; ++v) {
+                uint32_t* row = ksk.data() + ((static_cast<size_t>(i) * p.ks_levels + l) * (base - 1) + v - 1) * (n + 1);
+                uint32_t b = torus_noise(rng, p.sigma_lwe);
+                for (uint32_t j = 0; j < n; ++j) {
+                    row[j] = static_cast<uint32_t>(rng.next());
+                    if (s_out[j]) b += row[j];
+                }
+                b += (v * static_cast<uint32_t>(z_out[i])) << (32 - (l + 1) * p.ks_base_bits);
+                row[n] = b;
+            }
+}
+
+}  // namespace
+
+extern "C" {
+
+cbs_status cbs_gate_generate_keys_host(const cbs_gate_params* params, uint64_t seed, int32_t* s_lwe, int32_t* z_rlwe,
+                                       uint32_t* bsk, uint32_t* ksk) {
+    CBS_CHECK_ARG(params, "gate_generate_keys_host: null params");
+    if (cbs_status st = validate_gate(*params)) return st;
+    std::vector<int32_t> s, z;
+    std::vector<uint32_t> b, k;
+    gate_keys_host(*params, seed, s, z, b, k);
+    if (s_lwe) std::copy(s.begin(), s.end(), s_lwe);
+    if (z_rlwe) std::copy(z.begin(), z.end(), z_rlwe);
+    if (bsk) std::copy(b.begin(), b.end(), bsk);
+    if (ksk) std::copy(k.begin(), k.end(), ksk);
+    return CBS_OK;
+}
+
+cbs_status cbs_gate_keygen(cbs_gate_context* ctx, uint64_t seed) {
+    CBS_CHECK_ARG(ctx, "gate_keygen: null context");
+    const cbs_gate_params& p = ctx->p;
+    const uint32_t N = p.N;
+    gate_keys_host(p, seed, ctx->s, ctx->z, ctx->bsk, ctx->ksk);
+    std::vector<double2> bskf, tab;
+    if (N == 1024) {
+        torus_keys_to_fft<9>(ctx->bsk.data(), ctx->bsk.size() / N, bskf);
+        cbs::fft_tables_host(N, tab);
+    } else {
+        torus_keys_to_fft<10>(ctx->bsk.data(), ctx->bsk.size() / N, bskf);
+        cbs::fft_tables_host(N, tab);
+    }
+    CBS_CUDA_TRY(ctx->d_bskf.upload(bskf.data(), bskf.size(), nullptr));
+    CBS_CUDA_TRY(ctx->d_tab.upload(tab.data(), tab.size(), nullptr));
+    CBS_CUDA_TRY(ctx->d_ksk.upload(ctx->ksk.data(), ctx->ksk.size(), nullptr));
+    CBS_CUDA_TRY(cudaStreamSynchronize(nullptr));
+    ctx->keys_ready = true;
+    return CBS_OK;
+}
+
+cbs_status cbs_gate_export_keys(const cbs_gate_context* ctx, int32_t* s_lwe, int32_t* z_rlwe, uint32_t* bsk,
+                                uint32_t* ksk) {
+    CBS_CHECK_ARG(ctx, "gate_export_keys: null context");
+    if (!ctx->keys_ready) {
+        set_error("gate_export_keys: no keys (call cbs_gate_keygen first)");
+        return CBS_ERR_NOT_READY;
+    }
+    if (s_lwe) std::copy(ctx->s.begin(), ctx->s.end(), s_lwe);
+    if (z_rlwe) std::copy(ctx->z.begin(), ctx->z.end(), z_rlwe);
+    if (bsk) std::copy(ctx->bsk.begin(), ctx->bsk.end(), bsk);
+    if (ksk) std::copy(ctx->ksk.begin(), ctx->ksk.end(), ksk);
+    return CBS_OK;
+}
+
+cbs_status cbs_gate_encrypt_bits(const cbs_gate_context* ctx, const uint8_t* h_bits, uint32_t count, uint64_t seed,
+                                 uint32_t* h_a, uint32_t* h_b) {
+    CBS_CHECK_ARG(ctx && h_bits && h_a && h_b, "gate_encrypt_bits: null argument");
+    if (!ctx->keys_ready) {
+        set_error("gate_encrypt_bits: no keys (call cbs_gate_keygen first)");
+        return CBS_ERR_NOT_READY;
+    }
+    cbs::Rng rng(seed);
+    const uint32_t n = ctx->p.n;
+    for (uint32_t k = 0; k < count; ++k) {
+        uint32_t b = (h_bits[k] ? (1u << 29) : (0u - (1u << 29))) + torus_noise(rng, ctx->p.sigma_lwe);
+        for (uint32_t j = 0; j < n; ++j) {
+            const uint32_t a = static_cast<uint32_t>(rng.next());
+            h_a[static_cast<size_t>(k) * n + j] = a;
+            if (ctx->s[j]) b += a;
+        }
+        h_b[k] = b;
+    }
+    return CBS_OK;
+}
+
+cbs_status cbs_gate_decrypt_bits(const cbs_gate_context* ctx, const uint32_t* h_a, const uint32_t* h_b,
+                                 uint32_t count, uint8_t* h_bits) {
+    CBS_CHECK_ARG(ctx && h_a && h_b && h_bits, "gate_decrypt_bits: null argument");
+    if (!ctx->keys_ready) {
+        set_error("gate_decrypt_bits: no keys (call cbs_gate_keygen first)");
+        return CBS_ERR_NOT_READY;
+    }
+    const uint32_t n = ctx->p.n;
+    for (uint32_t k = 0; k < count; ++k) {
+        uint32_t ph = h_b[k];
+        for (uint32_t j = 0; j < n; ++j)
+            if (ctx->s[j]) ph -= h_a[static_cast<size_t>(k) * n + j];
+        h_bits[k] = static_cast<int32_t>(ph) > 0 ? 1 : 0;
+    }
+    return CBS_OK;
+}
+
+static cbs_status gate_run(cbs_gate_context* ctx, int gate, const uint32_t* d_a1, const uint32_t* d_b1,
+                           const uint32_t* d_a2, const uint32_t* d_b2, uint32_t count, uint32_t* d_ext,
+                           uint32_t* d_out_a, uint32_t* d_out_b, cudaStream_t s) {
+    if (!ctx->keys_ready) {
+        set_error("gate: no keys (call cbs_gate_keygen first)");
+        return CBS_ERR_NOT_READY;
+    }
+    if (count == 0) return CBS_OK;
+    if (count > ctx->max_batch) {
+        set_error("gate: count above the context's max_batch");
+        return CBS_ERR_SHAPE_MISMATCH;
+    }
+    const cbs_gate_params& p = ctx->p;
+    cbs::GateArgs a{};
+    a.gate = gate;
+    a.a1 = d_a1;
+    a.b1 = d_b1;
+    a.a2 = d_a2;
+    a.b2 = d_b2;
+    a.n = p.n;
+    a.levels = p.levels;
+    a.bg_bits = p.bg_bits;
+    a.bskf = ctx->d_bskf.p;
+    a.tab = ctx->d_tab.p;
+    a.ext = d_ext ? d_ext : ctx->d_ext.p;
+    if (p.N == 1024) CBS_CUDA_TRY(cbs::gate_br_launch<10>(a, count, s));
+    else CBS_CUDA_TRY(cbs::gate_br_launch<11>(a, count, s));
+    if (d_out_a && d_out_b) {
+        const dim3 grid((p.n + 1 + 255) / 256, count);
+        cbs::k_gate_keyswitch<<<grid, 256, (p.N + 1) * sizeof(uint32_t), s>>>(
+            a.ext, ctx->d_ksk.p, p.n, p.N, p.ks_base_bits, p.ks_levels, d_out_a, d_out_b);
+        CBS_LAUNCH_CHECK();
+    }
+    return CBS_OK;
+}
+
+cbs_status cbs_gate_eval_batch_device(cbs_gate_context* ctx, int gate, const uint32_t* d_a1, const uint32_t* d_b1,
+                                      const uint32_t* d_a2, const uint32_t* d_b2, uint32_t count, uint32_t* d_out_a,
+                                      uint32_t* d_out_b, cbs_stream_t stream) {
+    CBS_CHECK_ARG(ctx && d_a1 && d_b1 && d_a2 && d_b2 && d_out_a && d_out_b, "gate_eval_batch: null argument");
+    CBS_CHECK_ARG(gate >= CBS_GATE_OR && gate <= CBS_GATE_XNOR, "gate_eval_batch: unknown gate");
+    return gate_run(ctx, gate, d_a1, d_b1, d_a2, d_b2, count, nullptr, d_out_a, d_out_b, stream);
+}
+
+cbs_status cbs_gate_bootstrap_batch_device(cbs_gate_context* ctx, const uint32_t* d_a, const uint32_t* d_b,
+                                           uint32_t count, uint32_t* d_ext, uint32_t* d_out_a, uint32_t* d_out_b,
+                                           cbs_stream_t stream) {
+    CBS_CHECK_ARG(ctx && d_a && d_b, "gate_bootstrap_batch: null argument");
+    CBS_CHECK_ARG((d_out_a == nullptr) == (d_out_b == nullptr), "gate_bootstrap_batch: give both outputs or neither");
+    CBS_CHECK_ARG(d_ext || d_out_a, "gate_bootstrap_batch: no output requested");
+    return gate_run(ctx, -1, d_a, d_b, nullptr, nullptr, count, d_ext, d_out_a, d_out_b, stream);
+}
+
+}  // extern "C"

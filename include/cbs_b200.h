@@ -249,6 +249,64 @@ cbs_status cbs_circuit_bootstrap_batch_device_noalloc(cbs_context *ctx, const ui
                                                       cbs_stream_t stream);
 
 /* ------------------------------------------------------------------------------------
+ * Gate bootstrapping on the 32-bit torus: binfhe's GINX blind rotation with the FP64 FFT
+ * external product, sample extract and LWE key switch (the reference's
+ * GPUBinFHEContext::BatchGPUEvalBinGate path).  Torus values are uint32 (T = R/Z scaled by
+ * 2^32); a bit is encrypted as +1/8 (1) or -1/8 (0).  LWE ciphertexts: a [count][n],
+ * b [count].  Keys: s (LWE, binary, n), z (RLWE, binary, N); BSK [n][2*levels][2][N]
+ * (RGSW(s_i), row 2k+p adds s_i * 2^(32-(k+1)*bg_bits) to component p of an RLWE(0) under z,
+ * RLWE (a, b) with phase b - a*z); KSK [N][ks_levels][2^ks_base_bits - 1][n+1]
+ * (LWE_s(v * z_i * 2^(32-(l+1)*ks_base_bits))).  The FFT products are exact after rounding
+ * (|products| < 2^50), so results equal exact integer arithmetic.
+ * ------------------------------------------------------------------------------------ */
+typedef struct {
+    uint32_t n;            /* LWE dimension */
+    uint32_t N;            /* ring dimension: 1024 or 2048 */
+    uint32_t bg_bits;      /* gadget base 2^bg_bits */
+    uint32_t levels;       /* gadget digits (bg_bits * levels <= 30) */
+    uint32_t ks_base_bits; /* key-switch base 2^ks_base_bits */
+    uint32_t ks_levels;    /* key-switch digits */
+    double sigma_lwe;      /* LWE and key-switch noise standard deviation on the torus */
+    double sigma_rlwe;     /* bootstrapping-key noise standard deviation on the torus */
+} cbs_gate_params;
+
+/* gate codes (the first values of the reference's BINGATE; XOR / XNOR stand for both its
+ * XOR_FAST / XNOR_FAST and XOR / XNOR, which binfhe-base-scheme-batch.cu:99-110 maps alike) */
+enum { CBS_GATE_OR = 0, CBS_GATE_AND = 1, CBS_GATE_NOR = 2, CBS_GATE_NAND = 3, CBS_GATE_XOR = 4, CBS_GATE_XNOR = 5 };
+
+typedef struct cbs_gate_context cbs_gate_context;
+
+/* n = 636, N = 1024, base 2^7 x 3 digits, key switch base 2^2 x 8 digits, sigma_lwe = 2^-15,
+ * sigma_rlwe = 2^-25 */
+cbs_status cbs_gate_params_default(cbs_gate_params *out);
+/* replaces GPUBinFHEContext construction + BTKeyGen (bitwise/include/binfhecontext.cuh) */
+cbs_status cbs_gate_context_create(const cbs_gate_params *params, uint32_t max_batch, cbs_gate_context **out);
+cbs_status cbs_gate_context_destroy(cbs_gate_context *ctx);
+cbs_status cbs_gate_keygen(cbs_gate_context *ctx, uint64_t seed);
+/* the same keys as cbs_gate_keygen(ctx, seed) on the host only (no device); NULL skips */
+cbs_status cbs_gate_generate_keys_host(const cbs_gate_params *params, uint64_t seed, int32_t *s_lwe, int32_t *z_rlwe,
+                                       uint32_t *bsk, uint32_t *ksk);
+/* host copies of the secrets and keys (any pointer may be NULL) */
+cbs_status cbs_gate_export_keys(const cbs_gate_context *ctx, int32_t *s_lwe, int32_t *z_rlwe, uint32_t *bsk,
+                                uint32_t *ksk);
+/* host-side encryption / decryption of bits under s (test and setup helpers) */
+cbs_status cbs_gate_encrypt_bits(const cbs_gate_context *ctx, const uint8_t *h_bits, uint32_t count, uint64_t seed,
+                                 uint32_t *h_a, uint32_t *h_b);
+cbs_status cbs_gate_decrypt_bits(const cbs_gate_context *ctx, const uint32_t *h_a, const uint32_t *h_b,
+                                 uint32_t count, uint8_t *h_bits);
+/* replaces GPUBinFHEContext::BatchGPUEvalBinGate (bitwise/include/binfhecontext.cuh:53-57;
+ * bitwise/src/binfhe-base-scheme-batch.cu:82-200): out_k = gate(in1_k, in2_k) for k < count */
+cbs_status cbs_gate_eval_batch_device(cbs_gate_context *ctx, int gate, const uint32_t *d_a1, const uint32_t *d_b1,
+                                      const uint32_t *d_a2, const uint32_t *d_b2, uint32_t count, uint32_t *d_out_a,
+                                      uint32_t *d_out_b, cbs_stream_t stream);
+/* the bootstrap alone (sign: +1/8 when the phase is in [0, 1/2), else -1/8), with the
+ * extracted LWE of dimension N ([count][N+1], a then b) written to d_ext when non-NULL
+ * (BatchGPUBootstrapGateCore + sample extract, binfhe-base-scheme-batch.cu:16-140) */
+cbs_status cbs_gate_bootstrap_batch_device(cbs_gate_context *ctx, const uint32_t *d_a, const uint32_t *d_b,
+                                           uint32_t count, uint32_t *d_ext, uint32_t *d_out_a, uint32_t *d_out_b,
+                                           cbs_stream_t stream);
+
+/* ------------------------------------------------------------------------------------
  * RNS (Phantom) core: multi-prime NTT and hybrid key switching, CKKS form.
  * Key modulus chain = the size_q primes of Q followed by the size_p special primes P
  * (every one < 2^60, prime, = 1 mod 2N, distinct); alpha = size_p is the digit width and

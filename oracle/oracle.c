@@ -768,6 +768,125 @@ void orc_keyswitch(uint64_t *ct, const uint64_t *c2, const uint64_t *evk, uint32
 }
 
 /* ------------------------------------------------------------------------------------------ */
+/* gate bootstrap on the 32-bit torus                                                          */
+/* ------------------------------------------------------------------------------------------ */
+
+void orc_gate_combine(int gate, const uint32_t *a1, uint32_t b1, const uint32_t *a2, uint32_t b2, uint32_t n,
+                      uint32_t *a, uint32_t *b) {
+    const uint32_t e8 = 1u << 29, e4 = 1u << 30; /* 1/8, 1/4 */
+    for (uint32_t i = 0; i < n; ++i) {
+        const uint32_t s = a1[i] + a2[i];
+        switch (gate) {
+            case 0: case 1: a[i] = s; break;         /* OR, AND: + c1 + c2 */
+            case 2: case 3: a[i] = 0u - s; break;    /* NOR, NAND: - c1 - c2 */
+            case 4: a[i] = 2u * s; break;            /* XOR: 2 (c1 + c2) */
+            default: a[i] = 0u - 2u * s; break;      /* XNOR: -2 (c1 + c2) */
+        }
+    }
+    const uint32_t s = b1 + b2;
+    switch (gate) {
+        case 0: *b = e8 + s; break;
+        case 1: *b = (0u - e8) + s; break;
+        case 2: *b = (0u - e8) - s; break;
+        case 3: *b = e8 - s; break;
+        case 4: *b = e4 + 2u * s; break;
+        default: *b = (0u - e4) - 2u * s; break;
+    }
+}
+
+/* acc += X^e * src (negacyclic, mod 2^32) */
+static void torus_rot_add(uint32_t *acc, const uint32_t *src, uint32_t e, uint32_t N) {
+    for (uint32_t i = 0; i < N; ++i) {
+        uint32_t t = (i + e) % (2 * N);
+        if (t < N) acc[t] += src[i];
+        else acc[t - N] -= src[i];
+    }
+}
+
+/* out += d * k (negacyclic, d small signed digits, k torus32) */
+static void torus_mac(uint32_t *out, const int32_t *d, const uint32_t *k, uint32_t N) {
+    for (uint32_t i = 0; i < N; ++i) {
+        if (!d[i]) continue;
+        const uint32_t di = (uint32_t)d[i];
+        for (uint32_t j = 0; j < N; ++j) {
+            const uint32_t v = di * k[j];
+            if (i + j < N) out[i + j] += v;
+            else out[i + j - N] -= v;
+        }
+    }
+}
+
+/* signed base-2^bg digits, most significant first, of the top bg*levels bits (rounded) */
+static void torus_decompose(uint32_t x, uint32_t bg_bits, uint32_t levels, int32_t *d) {
+    uint32_t off = 0;
+    for (uint32_t k = 0; k < levels; ++k) off += (1u << (bg_bits - 1)) << (32 - (k + 1) * bg_bits);
+    off += 1u << (32 - levels * bg_bits - 1);
+    const uint32_t w = x + off;
+    for (uint32_t k = 0; k < levels; ++k)
+        d[k] = (int32_t)((w >> (32 - (k + 1) * bg_bits)) & ((1u << bg_bits) - 1)) - (int32_t)(1u << (bg_bits - 1));
+}
+
+void orc_gate_blind_rotate(const orc_gate_params *p, const uint32_t *bsk, const uint32_t *a, uint32_t b,
+                           uint32_t *ext) {
+    const uint32_t N = p->N, L = p->levels, two_n = 2 * N;
+    uint32_t logn2 = 0;
+    while ((1u << logn2) < two_n) ++logn2;
+    const uint32_t sh = 32 - logn2;
+#define MS(x) ((uint32_t)(((x) + (1u << (sh - 1))) >> sh) & (two_n - 1))
+    uint32_t *acc = (uint32_t *)calloc(2 * N, sizeof(uint32_t));
+    uint32_t *prod = (uint32_t *)malloc(2 * N * sizeof(uint32_t));
+    int32_t *dig = (int32_t *)malloc((size_t)2 * L * N * sizeof(int32_t));
+    /* acc = (0, X^-b~ * TV), TV = 1/8 everywhere */
+    const uint32_t bt = MS(b);
+    for (uint32_t i = 0; i < N; ++i) {
+        const uint32_t s = (i + bt) % two_n; /* coefficient i of X^-bt TV = TV[i + bt] (wrapped) */
+        acc[N + i] = (s < N) ? (1u << 29) : (0u - (1u << 29));
+    }
+    for (uint32_t step = 0; step < p->n; ++step) {
+        const uint32_t at = MS(a[step]);
+        if (at == 0) continue;
+        int32_t dd[8];
+        for (uint32_t c = 0; c < 2; ++c)
+            for (uint32_t i = 0; i < N; ++i) {
+                torus_decompose(acc[c * N + i], p->bg_bits, L, dd);
+                for (uint32_t k = 0; k < L; ++k) dig[((size_t)(2 * k + c)) * N + i] = dd[k];
+            }
+        memset(prod, 0, 2 * N * sizeof(uint32_t));
+        const uint32_t *key = bsk + (size_t)step * 2 * L * 2 * N;
+        for (uint32_t r = 0; r < 2 * L; ++r)
+            for (uint32_t c = 0; c < 2; ++c) torus_mac(prod + c * N, dig + (size_t)r * N, key + ((size_t)r * 2 + c) * N, N);
+        for (uint32_t c = 0; c < 2; ++c) {
+            torus_rot_add(acc + c * N, prod + c * N, at, N);
+            for (uint32_t i = 0; i < N; ++i) acc[c * N + i] -= prod[c * N + i];
+        }
+    }
+#undef MS
+    /* sample extract of coefficient 0 */
+    ext[0] = acc[0];
+    for (uint32_t i = 1; i < N; ++i) ext[i] = 0u - acc[N - i];
+    ext[N] = acc[N];
+    free(dig);
+    free(prod);
+    free(acc);
+}
+
+void orc_gate_keyswitch(const orc_gate_params *p, const uint32_t *ksk, const uint32_t *ext, uint32_t *out) {
+    const uint32_t N = p->N, n = p->n, t = p->ks_levels, bb = p->ks_base_bits, base = 1u << bb;
+    const uint32_t round = 1u << (32 - t * bb - 1);
+    for (uint32_t j = 0; j <= n; ++j) out[j] = 0;
+    out[n] = ext[N];
+    for (uint32_t i = 0; i < N; ++i) {
+        const uint32_t x = ext[i] + round;
+        for (uint32_t l = 0; l < t; ++l) {
+            const uint32_t v = (x >> (32 - (l + 1) * bb)) & (base - 1);
+            if (!v) continue;
+            const uint32_t *row = ksk + (((size_t)i * t + l) * (base - 1) + (v - 1)) * (n + 1);
+            for (uint32_t j = 0; j <= n; ++j) out[j] -= row[j];
+        }
+    }
+}
+
+/* ------------------------------------------------------------------------------------------ */
 /* plaintext AES-128 (FIPS-197), restating examples/aes_transcipher/aes128.cuh                 */
 /* ------------------------------------------------------------------------------------------ */
 

@@ -137,6 +137,22 @@ void orc_moddown(const uint64_t *cx, uint64_t *ct, uint32_t log_n, const uint64_
 void orc_keyswitch(uint64_t *ct, const uint64_t *c2, const uint64_t *evk, uint32_t log_n, const uint64_t *q,
                    uint32_t size_ql, uint32_t size_q, const uint64_t *p, uint32_t size_p);
 
+/* ---------------- gate bootstrap on the 32-bit torus (TFHE form of binfhe's GINX) ---------------- */
+typedef struct {
+    uint32_t n, N, bg_bits, levels, ks_base_bits, ks_levels;
+} orc_gate_params;
+/* the linear part of a two-input gate (binfhe-base-scheme-batch.cu:82-110 in torus form):
+ * gate 0 OR, 1 AND, 2 NOR, 3 NAND, 4 XOR, 5 XNOR; messages are +-1/8 */
+void orc_gate_combine(int gate, const uint32_t *a1, uint32_t b1, const uint32_t *a2, uint32_t b2, uint32_t n,
+                      uint32_t *a, uint32_t *b);
+/* blind rotation with test vector 1/8 (binfhe-base-scheme-batch.cu:16-74, rgsw-acc-batch.cu):
+ * bsk [n][2*levels][2][N] torus32 (row 2k+p: digit k of component p), exact integer products;
+ * writes the extracted LWE of dimension N: ext[0..N-1] = a, ext[N] = b */
+void orc_gate_blind_rotate(const orc_gate_params *p, const uint32_t *bsk, const uint32_t *a, uint32_t b,
+                           uint32_t *ext);
+/* LWE key switch N -> n (binfhe-base-scheme-batch.cu:145-185): ksk [N][ks_levels][base-1][n+1] */
+void orc_gate_keyswitch(const orc_gate_params *p, const uint32_t *ksk, const uint32_t *ext, uint32_t *out);
+
 /* ---------------- plaintext AES-128 (examples/aes_transcipher/aes128.cuh) ---------------- */
 void orc_aes128_key_expand(const uint8_t key[16], uint8_t round_keys[11][16]);
 void orc_aes128_encrypt(const uint8_t key[16], const uint8_t in[16], uint8_t out[16]);
