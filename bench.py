@@ -382,13 +382,31 @@ def run_keyswitch(args, rank: int, world: int, local_rank: int) -> None:
     ctx.close()
 
 
+def _ref_phantom_ntt():
+    """The reference's own Phantom NTT kernels rebuilt for sm_100a (oracle/_ref), or None."""
+    so = ROOT / "oracle" / "_ref" / "libref_phantom_ntt.so"
+    if not so.exists():
+        return None
+    lib = ctypes.CDLL(str(so))
+    vp, u32 = ctypes.c_void_p, ctypes.c_uint32
+    lib.ref_gpu_ntt2d_create.argtypes = [u32, u32, vp]
+    lib.ref_gpu_ntt2d_create.restype = vp
+    lib.ref_gpu_ntt2d_forward.argtypes = [vp, vp, u32, u32, vp]
+    lib.ref_gpu_ntt2d_backward.argtypes = [vp, vp, u32, u32, vp]
+    lib.ref_gpu_ntt2d_destroy.argtypes = [vp]
+    return lib
+
+
 def run_rns_ntt(args, rank: int, world: int, local_rank: int) -> None:
-    """Forward + inverse multi-prime NTT over `--batch` ciphertexts x 2 polys x 24 limbs at
-    N = 2^16 (the Phantom-core transform), in place, inputs resident in HBM."""
+    """Forward + inverse multi-prime NTT over `--batch` ciphertexts x 2 polys x `--limbs`
+    limbs at N = 2^`--ntt-logn` (default: the Phantom-core transform, N = 2^16, 24 limbs),
+    in place, inputs resident in HBM; beside it the reference's own 2-D kernels on the same
+    data when they were built (one call per polynomial, the reference's calling convention)."""
     import torch
     torch.cuda.set_device(local_rank)
     pkg = load_pkg()
-    n, size_q = 1 << 16, 24
+    logn, size_q = args.ntt_logn, args.limbs
+    n = 1 << logn
     count = args.batch or 32
     q, p = rns_chain(pkg, n, size_q, 2)
     ctx = pkg.RnsContext(n, q, p)
@@ -407,20 +425,45 @@ def run_rns_ntt(args, rank: int, world: int, local_rank: int) -> None:
     with ClockSampler(local_rank) as clk:
         ms = _timed(torch, stream, fn, args.warmup, args.steps)
     ok = bool(torch.equal(x, ref))  # forward then inverse is the identity
+    ref_gpu = None
+    lib = _ref_phantom_ntt()
+    if lib is not None:
+        chain = np.concatenate([q, p])
+        table = lib.ref_gpu_ntt2d_create(logn, len(chain), chain.ctypes.data)
+        y = ref.clone()
+
+        def rfn():
+            for k in range(polys):
+                ptr = y.data_ptr() + k * size_q * n * 8
+                lib.ref_gpu_ntt2d_forward(table, ptr, size_q, 0, stream.cuda_stream)
+            for k in range(polys):
+                ptr = y.data_ptr() + k * size_q * n * 8
+                lib.ref_gpu_ntt2d_backward(table, ptr, size_q, 0, stream.cuda_stream)
+
+        rms = _timed(torch, stream, rfn, args.warmup, args.steps)
+        same = bool(torch.equal(y, ref))
+        lib.ref_gpu_ntt2d_destroy(table)
+        ref_gpu = {"what": "reference nwt_2d_radix8_forward/backward_inplace (src/ntt/fntt_2d.cu, intt_2d.cu) "
+                           "rebuilt for sm_100a, one call per polynomial", "ms_per_step": rms,
+                   "value": world * polys * size_q / (rms * 1e-3), "roundtrip_identity": same,
+                   "speedup_of_this_build": rms / ms}
     alg = 2 * 2 * polys * size_q * n * 8  # each transform reads and writes every limb once
     peaks = measured_peaks()
     gbs = alg / (ms * 1e-3) / 1e9
-    out = {"metric": "RNS NTT forward+inverse limb-polys/s (N=2^16)", "value": world * polys * size_q / (ms * 1e-3),
+    out = {"metric": f"RNS NTT forward+inverse limb-polys/s (N=2^{logn})",
+           "value": world * polys * size_q / (ms * 1e-3),
            "unit": "limb-polys/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
            "data": "synthetic (seeded uniform residues)",
            "config": {"workload": "rns_ntt", "ciphertexts": count, "polys": polys, "limbs": size_q, "N": n,
-                      "l2": f"{polys * size_q * n * 8 / 1e9:.2f} GB per transform >> 126 MB L2"},
-           "roundtrip_identity": ok, "gpu_launches": args.steps * 4,
-           "roofline": {"kernel": "k_rns_fwd/inv cols+rows", "bound": "hbm", "achieved": gbs, "peak": peaks["hbm_gbs"],
-                        "unit": "GB/s", "frac": gbs / peaks["hbm_gbs"], "peak_src": peaks["src"], "traffic": None,
-                        "algorithmic_bytes_per_step": alg, "note": "two HBM round trips per transform (2-D)"},
-           "clocks": clk.summary()}
+                      "l2": f"{polys * size_q * n * 8 / 1e9:.2f} GB per transform "
+                            f"({'>' if polys * size_q * n * 8 > 126e6 else '<'} 126 MB L2)"},
+           "roundtrip_identity": ok, "gpu_launches": args.steps * (4 if logn >= 13 else 2),
+           "roofline": {"kernel": "k_rns_fwd/inv cols+rows" if logn >= 13 else "k_rns_small_fwd/inv", "bound": "hbm",
+                        "achieved": gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": gbs / peaks["hbm_gbs"],
+                        "peak_src": peaks["src"], "traffic": None, "algorithmic_bytes_per_step": alg,
+                        "note": "two HBM round trips per transform (2-D)" if logn >= 13 else "one round trip"},
+           "reference_gpu": ref_gpu, "clocks": clk.summary()}
     if rank == 0:
         print(json.dumps(out), flush=True)
     ctx.close()
@@ -594,6 +637,8 @@ def main() -> None:
                     help="aes128 is the headline; the others time one kernel family")
     ap.add_argument("--batch", type=int, default=0, help="units per step for the kernel workloads")
     ap.add_argument("--alpha", type=int, default=2, help="special primes (digit width) for --workload keyswitch")
+    ap.add_argument("--ntt-logn", dest="ntt_logn", type=int, default=16, help="log2 N for --workload rns_ntt")
+    ap.add_argument("--limbs", type=int, default=24, help="limbs per polynomial for --workload rns_ntt")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -1,4 +1,4 @@
-// ntt_rns.cu -- multi-prime negacyclic NTT for N = 2^13 .. 2^17 (Phantom's 2-D RNS NTT).
+// ntt_rns.cu -- multi-prime negacyclic NTT for N = 2^10 .. 2^17 (Phantom's RNS NTT).
 //
 // Same transform as src/ntt/fntt_2d.cu / intt_2d.cu (nwt_2d_radix8_forward_inplace and
 // nwt_2d_radix8_backward_inplace): per limb a Cooley-Tukey negacyclic NTT with Phantom's
@@ -312,6 +312,68 @@ __global__ void __launch_bounds__(kGroups * (1 << L1) / 8) k_rns_inv_cols(uint64
         });
 }
 
+// N = 2^10 .. 2^12: one CTA per limb polynomial, the register-blocked single-modulus transform
+// of ntt_core.cuh with the limb's prime tables, plus the same slot maps, out-of-place input,
+// inverse scaling and moddown epilogue as the 2-D kernels
+template <int LOGN, int EPI>
+__global__ void __launch_bounds__(NttPlan<LOGN>::T) k_rns_small_fwd(uint64_t* __restrict__ data, const RnsNttArgs a) {
+    constexpr size_t N = size_t(1) << LOGN;
+    __shared__ uint64_t sm[N];
+    const uint32_t limb_flat = blockIdx.x;
+    const uint32_t poly = limb_flat / a.limbs, limb = limb_flat % a.limbs;
+    const uint32_t prime = a.limb_prime[limb];
+    const uint64_t* tw = a.tw + prime * N;
+    const uint64_t* tws = a.tws + prime * N;
+    const uint64_t q = a.q[prime];
+    uint64_t* dst = limb_ptr(data, a, limb_flat, LOGN);
+    const uint64_t* src = src_ptr(data, a, limb_flat, LOGN);
+    if (EPI == 0) {
+        ntt_forward_cta<LOGN>(
+            sm, threadIdx.x, tw, tws, q, [&](uint32_t i) { return src[i]; },
+            [&](int, uint32_t i, uint64_t v) { dst[i] = v; });
+    } else {
+        const uint64_t* cx = a.epi_cx + poly * a.epi_cx_stride + (static_cast<size_t>(limb) << LOGN);
+        uint64_t* out = a.epi_dst + poly * a.epi_dst_stride + (static_cast<size_t>(limb) << LOGN);
+        const uint64_t f = a.epi_f[limb], fs = a.epi_fs[limb];
+        ntt_forward_cta<LOGN>(
+            sm, threadIdx.x, tw, tws, q, [&](uint32_t i) { return src[i]; },
+            [&](int, uint32_t i, uint64_t v) {
+                uint64_t r = mul_shoup(sub_mod(cx[i], v, q), f, fs, q);
+                if (EPI == 2) r = add_mod(out[i], r, q);
+                out[i] = r;
+            });
+    }
+}
+
+template <int LOGN>
+__global__ void __launch_bounds__(NttPlan<LOGN>::T) k_rns_small_inv(uint64_t* __restrict__ data, const RnsNttArgs a) {
+    constexpr size_t N = size_t(1) << LOGN;
+    __shared__ uint64_t sm[N];
+    const uint32_t limb_flat = blockIdx.x;
+    const uint32_t limb = limb_flat % a.limbs;
+    const uint32_t prime = a.limb_prime[limb];
+    const uint64_t q = a.q[prime];
+    const uint64_t sc = a.scale ? a.scale[limb] : 0, scs = a.scale ? a.scale_s[limb] : 0;
+    uint64_t* dst = limb_ptr(data, a, limb_flat, LOGN);
+    const uint64_t* src = src_ptr(data, a, limb_flat, LOGN);
+    ntt_inverse_cta<LOGN>(
+        sm, threadIdx.x, a.itw + prime * N, a.itws + prime * N, a.n_inv[prime], a.n_inv_s[prime], q,
+        [&](int, uint32_t i) { return src[i]; },
+        [&](uint32_t i, uint64_t v) { dst[i] = sc ? mul_shoup(v, sc, scs, q) : v; });
+}
+
+template <int LOGN>
+static cudaError_t rns_small_launch(uint64_t* data, const RnsNttArgs& a, size_t limb_polys, bool inverse,
+                                    cudaStream_t s) {
+    if (limb_polys > 0x7fffffffu) return cudaErrorInvalidValue;
+    const unsigned blocks = static_cast<unsigned>(limb_polys);
+    if (inverse) k_rns_small_inv<LOGN><<<blocks, NttPlan<LOGN>::T, 0, s>>>(data, a);
+    else if (a.epi == 0) k_rns_small_fwd<LOGN, 0><<<blocks, NttPlan<LOGN>::T, 0, s>>>(data, a);
+    else if (a.epi == 1) k_rns_small_fwd<LOGN, 1><<<blocks, NttPlan<LOGN>::T, 0, s>>>(data, a);
+    else k_rns_small_fwd<LOGN, 2><<<blocks, NttPlan<LOGN>::T, 0, s>>>(data, a);
+    return cudaGetLastError();
+}
+
 template <int L1>
 static cudaError_t rns_launch(uint64_t* data, const RnsNttArgs& a, size_t limb_polys, bool inverse, cudaStream_t s) {
     constexpr uint32_t ROW = 1u << kL2, ROWS = 1u << L1;
@@ -352,6 +414,9 @@ cudaError_t rns_ntt(uint64_t* data, const RnsNttArgs& a, uint32_t log_n, size_t 
     const size_t limb_polys = polys * a.limbs;
     if (limb_polys == 0) return cudaSuccess;
     switch (log_n) {
+        case 10: return rns_small_launch<10>(data, a, limb_polys, inverse, s);
+        case 11: return rns_small_launch<11>(data, a, limb_polys, inverse, s);
+        case 12: return rns_small_launch<12>(data, a, limb_polys, inverse, s);
         case 13: return rns_launch<5>(data, a, limb_polys, inverse, s);
         case 14: return rns_launch<6>(data, a, limb_polys, inverse, s);
         case 15: return rns_launch<7>(data, a, limb_polys, inverse, s);

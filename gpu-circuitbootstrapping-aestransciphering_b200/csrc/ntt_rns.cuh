@@ -1,4 +1,4 @@
-// ntt_rns.cuh -- multi-prime (RNS) negacyclic NTT for N = 2^14 .. 2^17.
+// ntt_rns.cuh -- multi-prime (RNS) negacyclic NTT for N = 2^10 .. 2^17.
 #pragma once
 
 #include <cuda_runtime.h>

@@ -433,8 +433,8 @@ cbs_status cbs_rns_context_create(uint32_t poly_degree, const uint64_t* h_q, uin
     CBS_CHECK_ARG(out && h_q && h_p, "rns_context_create: null argument");
     *out = nullptr;
     const int log_n = cbs::ilog2(poly_degree);
-    CBS_CHECK_ARG(poly_degree == (1u << log_n) && log_n >= 13 && log_n <= 17,
-                  "rns_context_create: poly_degree must be 2^13 .. 2^17");
+    CBS_CHECK_ARG(poly_degree == (1u << log_n) && log_n >= 10 && log_n <= 17,
+                  "rns_context_create: poly_degree must be 2^10 .. 2^17");
     CBS_CHECK_ARG(size_q >= 1 && size_p >= 1 && size_p <= cbs::kMaxAlpha && size_q + size_p <= cbs::kMaxChain,
                   "rns_context_create: need 1 <= size_p <= 16 and size_q + size_p <= 256");
     CBS_CHECK_ARG((size_q + size_p - 1) / size_p <= cbs::kMaxBeta, "rns_context_create: more than 64 digits");

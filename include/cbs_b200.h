@@ -328,7 +328,7 @@ typedef struct {
 } cbs_rns_ntt_tables;
 
 /* replaces PhantomContext(const EncryptionParameters&) for the key-switching path
- * (include/context.cuh:161; src/context.cu): poly_degree 2^13 .. 2^17, 1 <= size_p <= 16,
+ * (include/context.cuh:161; src/context.cu): poly_degree 2^10 .. 2^17, 1 <= size_p <= 16,
  * size_q + size_p <= 256 */
 cbs_status cbs_rns_context_create(uint32_t poly_degree, const uint64_t *h_q, uint32_t size_q, const uint64_t *h_p,
                                   uint32_t size_p, cbs_rns_context **out);

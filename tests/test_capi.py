@@ -78,7 +78,7 @@ def test_rns_context_validation_without_device(lib, oracle):
         return lib.cbs_rns_context_create(deg, q.ctypes.data, len(q), p.ctypes.data, len(p), ctypes.byref(h))
 
     assert create(n // 2 * 3, good[:2], good[2:]) == 1          # not a power of two
-    assert create(1 << 12, good[:2], good[2:]) == 1             # below 2^13
+    assert create(1 << 9, good[:2], good[2:]) == 1              # below 2^10
     assert create(n, good[:2], np.array([], np.uint64)) == 1    # no special prime
     assert create(n, np.array([good[0], good[0]]), good[2:]) == 1  # duplicate
     assert create(n, np.array([good[0] + 2]), good[2:]) == 1   # not prime / not 1 mod 2N

@@ -30,7 +30,7 @@ def rand_limbs(rng, mods, n, lead=()):
     return np.stack([rng.integers(0, int(m), lead + (n,), dtype=np.uint64) for m in mods], axis=len(lead))
 
 
-@pytest.mark.parametrize("logn", [13, 14, 15, 16, 17])
+@pytest.mark.parametrize("logn", [10, 11, 12, 13, 14, 15, 16, 17])
 def test_rns_ntt_bit_exact(env, logn):
     pkg, o, torch = env
     n = 1 << logn
@@ -73,6 +73,8 @@ KS_CASES = [  # (logn, size_q, size_p, size_ql, count)
     (13, 3, 1, 3, 2),   # alpha = 1
     (14, 6, 3, 5, 2),   # alpha = 3, partial digit
     (13, 4, 2, 1, 5),   # level 1: one digit of one limb
+    (12, 3, 2, 3, 2),   # N = 4096: the one-CTA-per-limb transforms
+    (10, 4, 1, 4, 3),
 ]
 
 
