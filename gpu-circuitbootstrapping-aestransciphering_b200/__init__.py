@@ -106,6 +106,8 @@ def _declare(lib: ctypes.CDLL) -> None:
         "cbs_gate_decrypt_bits": (st, [c_vp, c_vp, c_vp, u32, c_vp]),
         "cbs_gate_eval_batch_device": (st, [c_vp, ctypes.c_int, c_vp, c_vp, c_vp, c_vp, u32, c_vp, c_vp, c_vp]),
         "cbs_gate_bootstrap_batch_device": (st, [c_vp, c_vp, c_vp, u32, c_vp, c_vp, c_vp, c_vp]),
+        "cbs_gate_ragged_plan": (st, [c_vp, c_vp, u32, u32]),
+        "cbs_gate_ragged_launch": (st, [c_vp, c_vp]),
         "cbs_rns_context_create": (st, [u32, c_vp, u32, c_vp, u32, c_vp]),
         "cbs_rns_context_destroy": (st, [c_vp]),
         "cbs_rns_context_tables": (st, [c_vp, c_vp]),
@@ -199,6 +201,12 @@ class GateParams(ctypes.Structure):
                 ("sigma_lwe", ctypes.c_double), ("sigma_rlwe", ctypes.c_double)]
 
 
+class GateRequest(ctypes.Structure):
+    """Mirror of cbs_gate_request: one request of a ragged batch (device pointers)."""
+    _fields_ = [("d_a", ctypes.c_void_p), ("d_b", ctypes.c_void_p), ("d_out_a", ctypes.c_void_p),
+                ("d_out_b", ctypes.c_void_p), ("count", ctypes.c_uint32)]
+
+
 def gate_default_params() -> GateParams:
     p = GateParams()
     call("cbs_gate_params_default", ctypes.byref(p))
@@ -252,6 +260,14 @@ class GateContext:
         out = np.zeros(len(b), np.uint8)
         call("cbs_gate_decrypt_bits", self._h, a.ctypes.data, b.ctypes.data, len(b), out.ctypes.data)
         return out
+
+    def ragged_plan(self, requests, grid_ctas: int = 0) -> None:
+        """requests: sequence of (d_a, d_b, d_out_a, d_out_b, count) device pointers."""
+        arr = (GateRequest * max(1, len(requests)))(*[GateRequest(*r) for r in requests])
+        call("cbs_gate_ragged_plan", self._h, arr, len(requests), grid_ctas)
+
+    def ragged_launch(self, stream: int | None = None) -> None:
+        call("cbs_gate_ragged_launch", self._h, stream)
 
     def export_keys(self) -> dict:
         k = gate_key_buffers(self.params)

@@ -29,6 +29,16 @@
 
 namespace cbs {
 
+// one request of a ragged batch: count ciphertexts a [count][n], b [count] in, outputs out_a,
+// out_b; offset = number of ciphertexts in the requests before it
+struct GateReq {
+    const uint32_t* a;
+    const uint32_t* b;
+    uint32_t* out_a;
+    uint32_t* out_b;
+    uint32_t offset, count;
+};
+
 struct GateArgs {
     int gate;              // CBS_GATE_* or -1: bootstrap in1 as is
     const uint32_t* a1;    // [count][n]
@@ -38,8 +48,22 @@ struct GateArgs {
     uint32_t n, levels, bg_bits;
     const double2* bskf;   // [n][2*levels][2][M] key spectra, slot-major rows
     const double2* tab;    // FftTab<log2 M>
-    uint32_t* ext;         // [count][N+1] extracted LWE (a then b)
+    uint32_t* ext;         // [items][N+1] extracted LWE (a then b)
+    const GateReq* reqs;   // ragged mode when non-null: items are the concatenated requests
+    uint32_t num_reqs;
+    uint32_t items;        // ciphertexts in total; CTAs loop over them with stride gridDim.x
 };
+
+// request holding ragged item `item` (binary search over the offsets)
+__device__ __forceinline__ uint32_t gate_req_of(const GateReq* reqs, uint32_t num, uint32_t item) {
+    uint32_t lo = 0, hi = num;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) / 2;
+        if (__ldg(&reqs[mid].offset) <= item) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
 
 __device__ __forceinline__ uint32_t gate_a(int gate, uint32_t x1, uint32_t x2) {
     const uint32_t s = x1 + x2;
@@ -108,10 +132,23 @@ __global__ void __launch_bounds__(GateCfg<LOGN>::T, GateCfg<LOGN>::MIN_BLOCKS) k
     auto ms = [](uint32_t x) { return ((x + (1u << (SH - 1))) >> SH) & (TWO_N - 1); };
 
     for (uint32_t i = tid; i < Tb::size(); i += T) tab[i] = a.tab[i];
-    const uint32_t* a1 = a.a1 + static_cast<size_t>(ct) * a.n;
-    const uint32_t* a2 = a.a2 ? a.a2 + static_cast<size_t>(ct) * a.n : a1;
+    const uint32_t l2 = 2 * levels;
+    for (uint32_t item = ct; item < a.items; item += gridDim.x) {
+    const uint32_t* a1;
+    const uint32_t* a2;
+    uint32_t b;
+    if (a.reqs) {  // ragged: one bootstrap of request r
+        const GateReq& rq = a.reqs[gate_req_of(a.reqs, a.num_reqs, item)];
+        const uint32_t k = item - rq.offset;
+        a1 = rq.a + static_cast<size_t>(k) * a.n;
+        a2 = a1;
+        b = rq.b[k];
+    } else {
+        a1 = a.a1 + static_cast<size_t>(item) * a.n;
+        a2 = a.a2 ? a.a2 + static_cast<size_t>(item) * a.n : a1;
+        b = gate_b(a.gate, a.b1[item], a.b2 ? a.b2[item] : 0u);
+    }
     {
-        const uint32_t b = gate_b(a.gate, a.b1[ct], a.b2 ? a.b2[ct] : 0u);
         const uint32_t bt = ms(b);
         for (uint32_t i = tid; i < N; i += T) {
             acc[i] = 0;
@@ -120,9 +157,8 @@ __global__ void __launch_bounds__(GateCfg<LOGN>::T, GateCfg<LOGN>::MIN_BLOCKS) k
     }
     __syncthreads();
 
-    const uint32_t l2 = 2 * levels;
     for (uint32_t step = 0; step < a.n; ++step) {
-        const uint32_t at = ms(gate_a(a.gate, __ldg(a1 + step), __ldg(a2 + step)));
+        const uint32_t at = ms(a.reqs ? __ldg(a1 + step) : gate_a(a.gate, __ldg(a1 + step), __ldg(a2 + step)));
         if (at == 0) continue;  // X^0 - 1 = 0: the step adds nothing (uniform over the CTA)
         for (uint32_t e = ht; e < M; e += TH) {
             const uint32_t wr = my_acc[e] + off, wi = my_acc[e + M] + off;
@@ -197,13 +233,15 @@ __global__ void __launch_bounds__(GateCfg<LOGN>::T, GateCfg<LOGN>::MIN_BLOCKS) k
     }
     __syncthreads();
     // sample extract of coefficient 0: a'_0 = a_0, a'_i = -a_(N-i), b' = b_0
-    uint32_t* out = a.ext + static_cast<size_t>(ct) * (N + 1);
+    uint32_t* out = a.ext + static_cast<size_t>(item) * (N + 1);
     for (uint32_t i = tid; i <= N; i += T) {
         uint32_t v;
         if (i == N) v = acc[N];
         else if (i == 0) v = acc[0];
         else v = 0u - acc[N - i];
         out[i] = v;
+    }
+    __syncthreads();  // acc is re-initialised by the next item
     }
 }
 
@@ -213,13 +251,14 @@ __global__ void __launch_bounds__(GateCfg<LOGN>::T, GateCfg<LOGN>::MIN_BLOCKS) k
 __global__ void __launch_bounds__(256) k_gate_keyswitch(const uint32_t* __restrict__ ext,
                                                         const uint32_t* __restrict__ ksk, uint32_t n, uint32_t N,
                                                         uint32_t ks_bits, uint32_t ks_levels,
-                                                        uint32_t* __restrict__ out_a, uint32_t* __restrict__ out_b) {
+                                                        uint32_t* __restrict__ out_a, uint32_t* __restrict__ out_b,
+                                                        const GateReq* __restrict__ reqs, uint32_t num_reqs) {
     extern __shared__ uint32_t s_ext[];
-    const uint32_t ct = blockIdx.y;
+    const uint32_t ct = blockIdx.x;  // item
     const uint32_t* src = ext + static_cast<size_t>(ct) * (N + 1);
     for (uint32_t i = threadIdx.x; i <= N; i += blockDim.x) s_ext[i] = src[i];
     __syncthreads();
-    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t j = blockIdx.y * blockDim.x + threadIdx.x;
     if (j > n) return;
     const uint32_t base = 1u << ks_bits, round = 1u << (32 - ks_levels * ks_bits - 1);
     uint32_t accv = (j == n) ? s_ext[N] : 0u;
@@ -231,12 +270,21 @@ __global__ void __launch_bounds__(256) k_gate_keyswitch(const uint32_t* __restri
             if (v) accv -= __ldg(rows + (static_cast<size_t>(l) * (base - 1) + (v - 1)) * (n + 1));
         }
     }
-    if (j < n) out_a[static_cast<size_t>(ct) * n + j] = accv;
-    else out_b[ct] = accv;
+    uint32_t* oa = out_a;
+    uint32_t* ob = out_b;
+    uint32_t k = ct;
+    if (reqs) {
+        const GateReq& rq = reqs[gate_req_of(reqs, num_reqs, ct)];
+        oa = rq.out_a;
+        ob = rq.out_b;
+        k = ct - rq.offset;
+    }
+    if (j < n) oa[static_cast<size_t>(k) * n + j] = accv;
+    else ob[k] = accv;
 }
 
 template <int LOGN>
-static cudaError_t gate_br_launch(const GateArgs& a, uint32_t count, cudaStream_t s) {
+static cudaError_t gate_br_launch(const GateArgs& a, uint32_t grid, cudaStream_t s) {
     constexpr uint32_t N = 1u << LOGN, M = N / 2;
     const size_t smem = (2ull * M + FftTab<LOGN - 1>::size()) * sizeof(double2) + 2ull * N * sizeof(uint32_t) +
                         2ull * a.levels * M * sizeof(uint32_t);
@@ -249,7 +297,7 @@ static cudaError_t gate_br_launch(const GateArgs& a, uint32_t count, cudaStream_
         if (e != cudaSuccess) return e;
         configured[dev] = smem;
     }
-    k_gate_blind_rotate<LOGN><<<count, GateCfg<LOGN>::T, smem, s>>>(a);
+    k_gate_blind_rotate<LOGN><<<grid, GateCfg<LOGN>::T, smem, s>>>(a);
     return cudaGetLastError();
 }
 
@@ -269,6 +317,10 @@ struct cbs_gate_context {
     std::vector<uint32_t> bsk, ksk;  // coefficient form (exported) / device layout
     DevBuf<double2> d_bskf, d_tab;
     DevBuf<uint32_t> d_ksk, d_ext, d_tmp_a, d_tmp_b;
+    // ragged plan (cbs_gate_ragged_plan): request table, its extracted-LWE scratch, grid
+    DevBuf<cbs::GateReq> d_plan;
+    DevBuf<uint32_t> d_plan_ext;
+    uint32_t plan_reqs = 0, plan_items = 0, plan_grid = 0;
 };
 
 namespace {
@@ -568,12 +620,13 @@ static cbs_status gate_run(cbs_gate_context* ctx, int gate, const uint32_t* d_a1
     a.bskf = ctx->d_bskf.p;
     a.tab = ctx->d_tab.p;
     a.ext = d_ext ? d_ext : ctx->d_ext.p;
+    a.items = count;
     if (p.N == 1024) CBS_CUDA_TRY(cbs::gate_br_launch<10>(a, count, s));
     else CBS_CUDA_TRY(cbs::gate_br_launch<11>(a, count, s));
     if (d_out_a && d_out_b) {
-        const dim3 grid((p.n + 1 + 255) / 256, count);
+        const dim3 grid(count, (p.n + 1 + 255) / 256);
         cbs::k_gate_keyswitch<<<grid, 256, (p.N + 1) * sizeof(uint32_t), s>>>(
-            a.ext, ctx->d_ksk.p, p.n, p.N, p.ks_base_bits, p.ks_levels, d_out_a, d_out_b);
+            a.ext, ctx->d_ksk.p, p.n, p.N, p.ks_base_bits, p.ks_levels, d_out_a, d_out_b, nullptr, 0);
         CBS_LAUNCH_CHECK();
     }
     return CBS_OK;
@@ -594,6 +647,57 @@ cbs_status cbs_gate_bootstrap_batch_device(cbs_gate_context* ctx, const uint32_t
     CBS_CHECK_ARG((d_out_a == nullptr) == (d_out_b == nullptr), "gate_bootstrap_batch: give both outputs or neither");
     CBS_CHECK_ARG(d_ext || d_out_a, "gate_bootstrap_batch: no output requested");
     return gate_run(ctx, -1, d_a, d_b, nullptr, nullptr, count, d_ext, d_out_a, d_out_b, stream);
+}
+
+cbs_status cbs_gate_ragged_plan(cbs_gate_context* ctx, const cbs_gate_request* h_reqs, uint32_t num_reqs,
+                                uint32_t grid_ctas) {
+    CBS_CHECK_ARG(ctx && (h_reqs || num_reqs == 0), "gate_ragged_plan: null argument");
+    if (!ctx->keys_ready) {
+        set_error("gate_ragged_plan: no keys (call cbs_gate_keygen first)");
+        return CBS_ERR_NOT_READY;
+    }
+    std::vector<cbs::GateReq> reqs;
+    uint64_t items = 0;
+    for (uint32_t r = 0; r < num_reqs; ++r) {
+        const cbs_gate_request& q = h_reqs[r];
+        if (q.count == 0) continue;
+        CBS_CHECK_ARG(q.d_a && q.d_b && q.d_out_a && q.d_out_b, "gate_ragged_plan: request with a null pointer");
+        reqs.push_back(cbs::GateReq{q.d_a, q.d_b, q.d_out_a, q.d_out_b, static_cast<uint32_t>(items), q.count});
+        items += q.count;
+    }
+    CBS_CHECK_ARG(items < (uint64_t(1) << 31), "gate_ragged_plan: more than 2^31 ciphertexts");
+    ctx->plan_reqs = static_cast<uint32_t>(reqs.size());
+    ctx->plan_items = static_cast<uint32_t>(items);
+    ctx->plan_grid = (grid_ctas == 0 || grid_ctas > items) ? static_cast<uint32_t>(items) : grid_ctas;
+    if (reqs.empty()) return CBS_OK;
+    CBS_CUDA_TRY(ctx->d_plan.alloc(reqs.size()));
+    CBS_CUDA_TRY(cudaMemcpy(ctx->d_plan.p, reqs.data(), reqs.size() * sizeof(cbs::GateReq), cudaMemcpyHostToDevice));
+    CBS_CUDA_TRY(ctx->d_plan_ext.alloc(static_cast<size_t>(items) * (ctx->p.N + 1)));
+    return CBS_OK;
+}
+
+cbs_status cbs_gate_ragged_launch(cbs_gate_context* ctx, cbs_stream_t stream) {
+    CBS_CHECK_ARG(ctx, "gate_ragged_launch: null context");
+    if (ctx->plan_items == 0) return CBS_OK;
+    const cbs_gate_params& p = ctx->p;
+    cbs::GateArgs a{};
+    a.gate = -1;
+    a.n = p.n;
+    a.levels = p.levels;
+    a.bg_bits = p.bg_bits;
+    a.bskf = ctx->d_bskf.p;
+    a.tab = ctx->d_tab.p;
+    a.ext = ctx->d_plan_ext.p;
+    a.reqs = ctx->d_plan.p;
+    a.num_reqs = ctx->plan_reqs;
+    a.items = ctx->plan_items;
+    if (p.N == 1024) CBS_CUDA_TRY(cbs::gate_br_launch<10>(a, ctx->plan_grid, stream));
+    else CBS_CUDA_TRY(cbs::gate_br_launch<11>(a, ctx->plan_grid, stream));
+    const dim3 grid(ctx->plan_items, (p.n + 1 + 255) / 256);
+    cbs::k_gate_keyswitch<<<grid, 256, (p.N + 1) * sizeof(uint32_t), stream>>>(
+        a.ext, ctx->d_ksk.p, p.n, p.N, p.ks_base_bits, p.ks_levels, nullptr, nullptr, a.reqs, a.num_reqs);
+    CBS_LAUNCH_CHECK();
+    return CBS_OK;
 }
 
 }  // extern "C"

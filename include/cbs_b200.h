@@ -306,6 +306,27 @@ cbs_status cbs_gate_bootstrap_batch_device(cbs_gate_context *ctx, const uint32_t
                                            uint32_t count, uint32_t *d_ext, uint32_t *d_out_a, uint32_t *d_out_b,
                                            cbs_stream_t stream);
 
+/* Ragged batching: many bootstrap requests of uneven size (the sign bootstrap of
+ * cbs_gate_bootstrap_batch_device, outputs key-switched to n) in one blind-rotation launch
+ * and one key-switch launch per parameter set, instead of one launch pair per request.  No
+ * reference counterpart (the reference launches per batch).  cbs_gate_ragged_plan uploads
+ * the request table and sizes the context's scratch (synchronous; call it outside any
+ * stream capture); grid_ctas bounds the blind rotation's grid (0: one CTA per ciphertext;
+ * smaller grids make each CTA loop over ciphertexts).  cbs_gate_ragged_launch only launches
+ * kernels, so it can be captured in a CUDA graph and replayed; each replay reruns the plan
+ * on whatever the planned buffers then hold.  Contexts of different parameter sets launch
+ * their plans on separate streams to run side by side. */
+typedef struct {
+    const uint32_t *d_a; /* [count][n] */
+    const uint32_t *d_b; /* [count] */
+    uint32_t *d_out_a;   /* [count][n] */
+    uint32_t *d_out_b;   /* [count] */
+    uint32_t count;
+} cbs_gate_request;
+cbs_status cbs_gate_ragged_plan(cbs_gate_context *ctx, const cbs_gate_request *h_reqs, uint32_t num_reqs,
+                                uint32_t grid_ctas);
+cbs_status cbs_gate_ragged_launch(cbs_gate_context *ctx, cbs_stream_t stream);
+
 /* ------------------------------------------------------------------------------------
  * RNS (Phantom) core: multi-prime NTT and hybrid key switching, CKKS form.
  * Key modulus chain = the size_q primes of Q followed by the size_p special primes P

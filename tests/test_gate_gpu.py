@@ -141,3 +141,58 @@ def test_argument_checks(pkg, gctx):
     st = lib.cbs_gate_bootstrap_batch_device(gctx.handle, da.data_ptr(), db.data_ptr(), 1000, None, out_a.data_ptr(),
                                              out_b.data_ptr(), None)
     assert st == 2  # above max_batch
+
+
+def test_ragged_two_parameter_sets_in_one_graph(pkg):
+    """Requests of uneven size over two parameter sets (N=1024/n=636, N=2048/n=630), planned
+    once and replayed from one captured CUDA graph: outputs equal the per-request launches
+    bit for bit and decrypt to the input bits."""
+    pa = pkg.gate_default_params()
+    pb = pkg.gate_default_params()
+    pb.N, pb.n = 2048, 630
+    ctxs = [pkg.GateContext(pa, max_batch=64), pkg.GateContext(pb, max_batch=64)]
+    for i, c in enumerate(ctxs):
+        c.keygen(40 + i)
+    sizes = [[1, 17, 5], [3, 33]]
+    rng = np.random.default_rng(5)
+    reqs, want = [[], []], []
+    keep = []
+    for i, c in enumerate(ctxs):
+        for cnt in sizes[i]:
+            bits = rng.integers(0, 2, cnt).astype(np.uint8)
+            a, b = c.encrypt(bits, seed=int(rng.integers(1 << 30)))
+            da, db = _dev(a), _dev(b)
+            oa = torch.zeros((cnt, c.params.n), dtype=torch.int32, device="cuda")
+            ob = torch.zeros(cnt, dtype=torch.int32, device="cuda")
+            keep += [da, db, oa, ob]
+            reqs[i].append((da.data_ptr(), db.data_ptr(), oa.data_ptr(), ob.data_ptr(), cnt))
+            # per-request launch for comparison
+            ra = torch.zeros_like(oa)
+            rb = torch.zeros_like(ob)
+            pkg.call("cbs_gate_bootstrap_batch_device", c.handle, da.data_ptr(), db.data_ptr(), cnt, None,
+                     ra.data_ptr(), rb.data_ptr(), None)
+            want.append((i, bits, oa, ob, ra, rb))
+    ctxs[0].ragged_plan(reqs[0], grid_ctas=0)
+    ctxs[1].ragged_plan(reqs[1], grid_ctas=3)  # fewer CTAs than ciphertexts: CTAs loop
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    side = torch.cuda.Stream()
+    with torch.cuda.graph(g):
+        main = torch.cuda.current_stream()
+        side.wait_stream(main)
+        ctxs[0].ragged_launch(main.cuda_stream)
+        with torch.cuda.stream(side):
+            ctxs[1].ragged_launch(side.cuda_stream)
+        main.wait_stream(side)
+    for _ in range(2):
+        for (_, _, oa, ob, _, _) in want:
+            oa.zero_()
+            ob.zero_()
+        g.replay()
+        torch.cuda.synchronize()
+        for (i, bits, oa, ob, ra, rb) in want:
+            assert torch.equal(oa, ra) and torch.equal(ob, rb)
+            assert np.array_equal(ctxs[i].decrypt(_host(oa), _host(ob)), bits)
+    del g
+    for c in ctxs:
+        c.close()
