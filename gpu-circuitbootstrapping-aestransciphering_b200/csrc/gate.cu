@@ -134,114 +134,114 @@ __global__ void __launch_bounds__(GateCfg<LOGN>::T, GateCfg<LOGN>::MIN_BLOCKS) k
     for (uint32_t i = tid; i < Tb::size(); i += T) tab[i] = a.tab[i];
     const uint32_t l2 = 2 * levels;
     for (uint32_t item = ct; item < a.items; item += gridDim.x) {
-    const uint32_t* a1;
-    const uint32_t* a2;
-    uint32_t b;
-    if (a.reqs) {  // ragged: one bootstrap of request r
-        const GateReq& rq = a.reqs[gate_req_of(a.reqs, a.num_reqs, item)];
-        const uint32_t k = item - rq.offset;
-        a1 = rq.a + static_cast<size_t>(k) * a.n;
-        a2 = a1;
-        b = rq.b[k];
-    } else {
-        a1 = a.a1 + static_cast<size_t>(item) * a.n;
-        a2 = a.a2 ? a.a2 + static_cast<size_t>(item) * a.n : a1;
-        b = gate_b(a.gate, a.b1[item], a.b2 ? a.b2[item] : 0u);
-    }
-    {
-        const uint32_t bt = ms(b);
-        for (uint32_t i = tid; i < N; i += T) {
-            acc[i] = 0;
-            acc[N + i] = (((i + bt) & (TWO_N - 1)) < N) ? (1u << 29) : (0u - (1u << 29));
+        const uint32_t* a1;
+        const uint32_t* a2;
+        uint32_t b;
+        if (a.reqs) {  // ragged: one bootstrap of request r
+            const GateReq& rq = a.reqs[gate_req_of(a.reqs, a.num_reqs, item)];
+            const uint32_t k = item - rq.offset;
+            a1 = rq.a + static_cast<size_t>(k) * a.n;
+            a2 = a1;
+            b = rq.b[k];
+        } else {
+            a1 = a.a1 + static_cast<size_t>(item) * a.n;
+            a2 = a.a2 ? a.a2 + static_cast<size_t>(item) * a.n : a1;
+            b = gate_b(a.gate, a.b1[item], a.b2 ? a.b2[item] : 0u);
         }
-    }
-    __syncthreads();
-
-    for (uint32_t step = 0; step < a.n; ++step) {
-        const uint32_t at = ms(a.reqs ? __ldg(a1 + step) : gate_a(a.gate, __ldg(a1 + step), __ldg(a2 + step)));
-        if (at == 0) continue;  // X^0 - 1 = 0: the step adds nothing (uniform over the CTA)
-        for (uint32_t e = ht; e < M; e += TH) {
-            const uint32_t wr = my_acc[e] + off, wi = my_acc[e + M] + off;
-            uint32_t* dst = dig + h * levels * M + e;
-            for (uint32_t k = 0; k < levels; ++k) {
-                const uint32_t s = 32 - (k + 1) * bg, mask = (1u << bg) - 1, half = 1u << (bg - 1);
-                const int32_t dr = static_cast<int32_t>((wr >> s) & mask) - static_cast<int32_t>(half);
-                const int32_t di = static_cast<int32_t>((wi >> s) & mask) - static_cast<int32_t>(half);
-                dst[k * M] = (static_cast<uint32_t>(dr) & 0xffffu) | (static_cast<uint32_t>(di) << 16);
+        {
+            const uint32_t bt = ms(b);
+            for (uint32_t i = tid; i < N; i += T) {
+                acc[i] = 0;
+                acc[N + i] = (((i + bt) & (TWO_N - 1)) < N) ? (1u << 29) : (0u - (1u << 29));
             }
         }
-        half_bar();
-        const double2* ek = a.bskf + static_cast<size_t>(step) * l2 * 2 * M + ht;
-        double2 y0[8], y1[8];
-#pragma unroll
-        for (int j = 0; j < 8; ++j) y0[j] = y1[j] = make_double2(0.0, 0.0);
-        for (uint32_t d = 0; d < levels; ++d) {
-            const uint32_t* dsrc = dig + (h * levels + d) * M;
-            double2 x[8];
-            fft_forward_to_regs<LOGM>(
-                my_fs, ht, tab,
-                [&](int j, uint32_t e) {
-                    const uint32_t v = dsrc[e];
-                    const double re = static_cast<double>(static_cast<int16_t>(v & 0xffffu));
-                    const double im = static_cast<double>(static_cast<int16_t>(v >> 16));
-                    return cmul(make_double2(re, im), gate_twist<LOGM>(tws, j, e));
-                },
-                x, half_bar);
-            const double2* k0 = ek + static_cast<size_t>(2 * d + h) * 2 * M;
-            const double2* k1 = k0 + M;
-#pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                cfma(y0[j], x[j], __ldg(k0 + j * TH));
-                cfma(y1[j], x[j], __ldg(k1 + j * TH));
+        __syncthreads();
+
+        for (uint32_t step = 0; step < a.n; ++step) {
+            const uint32_t at = ms(a.reqs ? __ldg(a1 + step) : gate_a(a.gate, __ldg(a1 + step), __ldg(a2 + step)));
+            if (at == 0) continue;  // X^0 - 1 = 0: the step adds nothing (uniform over the CTA)
+            for (uint32_t e = ht; e < M; e += TH) {
+                const uint32_t wr = my_acc[e] + off, wi = my_acc[e + M] + off;
+                uint32_t* dst = dig + h * levels * M + e;
+                for (uint32_t k = 0; k < levels; ++k) {
+                    const uint32_t s = 32 - (k + 1) * bg, mask = (1u << bg) - 1, half = 1u << (bg - 1);
+                    const int32_t dr = static_cast<int32_t>((wr >> s) & mask) - static_cast<int32_t>(half);
+                    const int32_t di = static_cast<int32_t>((wi >> s) & mask) - static_cast<int32_t>(half);
+                    dst[k * M] = (static_cast<uint32_t>(dr) & 0xffffu) | (static_cast<uint32_t>(di) << 16);
+                }
             }
             half_bar();
+            const double2* ek = a.bskf + static_cast<size_t>(step) * l2 * 2 * M + ht;
+            double2 y0[8], y1[8];
+    #pragma unroll
+            for (int j = 0; j < 8; ++j) y0[j] = y1[j] = make_double2(0.0, 0.0);
+            for (uint32_t d = 0; d < levels; ++d) {
+                const uint32_t* dsrc = dig + (h * levels + d) * M;
+                double2 x[8];
+                fft_forward_to_regs<LOGM>(
+                    my_fs, ht, tab,
+                    [&](int j, uint32_t e) {
+                        const uint32_t v = dsrc[e];
+                        const double re = static_cast<double>(static_cast<int16_t>(v & 0xffffu));
+                        const double im = static_cast<double>(static_cast<int16_t>(v >> 16));
+                        return cmul(make_double2(re, im), gate_twist<LOGM>(tws, j, e));
+                    },
+                    x, half_bar);
+                const double2* k0 = ek + static_cast<size_t>(2 * d + h) * 2 * M;
+                const double2* k1 = k0 + M;
+    #pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    cfma(y0[j], x[j], __ldg(k0 + j * TH));
+                    cfma(y1[j], x[j], __ldg(k1 + j * TH));
+                }
+                half_bar();
+            }
+    #pragma unroll
+            for (int j = 0; j < 8; ++j) my_fs[cswz(8 * ht + j)] = h ? y0[j] : y1[j];
+            __syncthreads();
+            {
+                const double2* take = fs + (1 - h) * M;
+    #pragma unroll
+                for (int j = 0; j < 8; ++j) y0[j] = cadd(h ? y1[j] : y0[j], take[cswz(8 * ht + j)]);
+            }
+            __syncthreads();
+            uint32_t tre[8], tim[8];
+            constexpr double inv_m = 1.0 / M;
+            fft_inverse_from_regs<LOGM>(
+                my_fs, ht, tab, y0,
+                [&](int j, uint32_t e, double2 v) {
+                    const double2 u = cmulc(v, gate_twist<LOGM>(tws, j, e));
+                    tre[j] = static_cast<uint32_t>(static_cast<uint64_t>(__double2ll_rn(u.x * inv_m)));
+                    tim[j] = static_cast<uint32_t>(static_cast<uint64_t>(__double2ll_rn(u.y * inv_m)));
+                },
+                half_bar);
+            half_bar();
+            uint32_t* tsm = reinterpret_cast<uint32_t*>(my_fs);  // N words
+    #pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                tsm[ht + j * TH] = tre[j];
+                tsm[ht + j * TH + M] = tim[j];
+            }
+            half_bar();
+    #pragma unroll 4
+            for (uint32_t k = 0; k < N / TH; ++k) {
+                const uint32_t i = ht + k * TH;
+                const uint32_t s = (i + TWO_N - at) & (TWO_N - 1);
+                const uint32_t v = (s < N) ? tsm[s] : 0u - tsm[s - N];
+                my_acc[i] += v - tsm[i];
+            }
         }
-#pragma unroll
-        for (int j = 0; j < 8; ++j) my_fs[cswz(8 * ht + j)] = h ? y0[j] : y1[j];
         __syncthreads();
-        {
-            const double2* take = fs + (1 - h) * M;
-#pragma unroll
-            for (int j = 0; j < 8; ++j) y0[j] = cadd(h ? y1[j] : y0[j], take[cswz(8 * ht + j)]);
+        // sample extract of coefficient 0: a'_0 = a_0, a'_i = -a_(N-i), b' = b_0
+        uint32_t* out = a.ext + static_cast<size_t>(item) * (N + 1);
+        for (uint32_t i = tid; i <= N; i += T) {
+            uint32_t v;
+            if (i == N) v = acc[N];
+            else if (i == 0) v = acc[0];
+            else v = 0u - acc[N - i];
+            out[i] = v;
         }
-        __syncthreads();
-        uint32_t tre[8], tim[8];
-        constexpr double inv_m = 1.0 / M;
-        fft_inverse_from_regs<LOGM>(
-            my_fs, ht, tab, y0,
-            [&](int j, uint32_t e, double2 v) {
-                const double2 u = cmulc(v, gate_twist<LOGM>(tws, j, e));
-                tre[j] = static_cast<uint32_t>(static_cast<uint64_t>(__double2ll_rn(u.x * inv_m)));
-                tim[j] = static_cast<uint32_t>(static_cast<uint64_t>(__double2ll_rn(u.y * inv_m)));
-            },
-            half_bar);
-        half_bar();
-        uint32_t* tsm = reinterpret_cast<uint32_t*>(my_fs);  // N words
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            tsm[ht + j * TH] = tre[j];
-            tsm[ht + j * TH + M] = tim[j];
-        }
-        half_bar();
-#pragma unroll 4
-        for (uint32_t k = 0; k < N / TH; ++k) {
-            const uint32_t i = ht + k * TH;
-            const uint32_t s = (i + TWO_N - at) & (TWO_N - 1);
-            const uint32_t v = (s < N) ? tsm[s] : 0u - tsm[s - N];
-            my_acc[i] += v - tsm[i];
-        }
-    }
-    __syncthreads();
-    // sample extract of coefficient 0: a'_0 = a_0, a'_i = -a_(N-i), b' = b_0
-    uint32_t* out = a.ext + static_cast<size_t>(item) * (N + 1);
-    for (uint32_t i = tid; i <= N; i += T) {
-        uint32_t v;
-        if (i == N) v = acc[N];
-        else if (i == 0) v = acc[0];
-        else v = 0u - acc[N - i];
-        out[i] = v;
-    }
-    __syncthreads();  // acc is re-initialised by the next item
+        __syncthreads();  // acc is re-initialised by the next item
     }
 }
 
