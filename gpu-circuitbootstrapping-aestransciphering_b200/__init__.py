@@ -106,6 +106,14 @@ def _declare(lib: ctypes.CDLL) -> None:
         "cbs_gate_decrypt_bits": (st, [c_vp, c_vp, c_vp, u32, c_vp]),
         "cbs_gate_eval_batch_device": (st, [c_vp, ctypes.c_int, c_vp, c_vp, c_vp, c_vp, u32, c_vp, c_vp, c_vp]),
         "cbs_gate_bootstrap_batch_device": (st, [c_vp, c_vp, c_vp, u32, c_vp, c_vp, c_vp, c_vp]),
+        "cbs_tcb_params_default": (st, [c_vp]),
+        "cbs_tcb_context_create": (st, [c_vp, u32, c_vp]),
+        "cbs_tcb_context_destroy": (st, [c_vp]),
+        "cbs_tcb_keygen": (st, [c_vp, u64]),
+        "cbs_tcb_generate_keys_host": (st, [c_vp, u64, c_vp, c_vp, c_vp, c_vp, c_vp]),
+        "cbs_tcb_export_keys": (st, [c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
+        "cbs_tcb_encrypt_bits": (st, [c_vp, c_vp, u32, u64, c_vp, c_vp]),
+        "cbs_tcb_circuit_bootstrap_device": (st, [c_vp, c_vp, c_vp, u32, c_vp, c_vp, c_vp]),
         "cbs_gate_ragged_plan": (st, [c_vp, c_vp, u32, u32]),
         "cbs_gate_ragged_launch": (st, [c_vp, c_vp]),
         "cbs_rns_context_create": (st, [u32, c_vp, u32, c_vp, u32, c_vp]),
@@ -278,6 +286,82 @@ class GateContext:
     def close(self) -> None:
         if self._h.value:
             load().cbs_gate_context_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class TcbParams(ctypes.Structure):
+    """Mirror of cbs_tcb_params (include/cbs_b200.h)."""
+    _fields_ = [("n", ctypes.c_uint32), ("N2", ctypes.c_uint32), ("bg2_bits", ctypes.c_uint32),
+                ("l2", ctypes.c_uint32), ("N1", ctypes.c_uint32), ("cb_bits", ctypes.c_uint32),
+                ("cb_levels", ctypes.c_uint32), ("pfks_base_bits", ctypes.c_uint32),
+                ("pfks_levels", ctypes.c_uint32), ("sigma_lwe", ctypes.c_double), ("sigma_lvl2", ctypes.c_double),
+                ("sigma_lvl1", ctypes.c_double)]
+
+
+def tcb_default_params() -> TcbParams:
+    p = TcbParams()
+    call("cbs_tcb_params_default", ctypes.byref(p))
+    return p
+
+
+def tcb_key_buffers(p: TcbParams, with_pfks: bool = True) -> dict:
+    import numpy as np
+    base = 1 << p.pfks_base_bits
+    k = dict(s0=np.zeros(p.n, np.int32), z2=np.zeros(p.N2, np.int32), z1=np.zeros(p.N1, np.int32),
+             bsk2=np.zeros((p.n, 2 * p.l2, 2, p.N2), np.uint64))
+    k["pfks"] = np.zeros((2, p.N2 + 1, p.pfks_levels, base - 1, 2, p.N1), np.uint32) if with_pfks else None
+    return k
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data
+
+
+def tcb_generate_keys_host(p: TcbParams, seed: int, with_pfks: bool = True) -> dict:
+    """Torus circuit-bootstrapping keys on the host only; same keys as TcbContext.keygen(seed)."""
+    k = tcb_key_buffers(p, with_pfks)
+    call("cbs_tcb_generate_keys_host", ctypes.byref(p), seed, *(_ptr(k[x]) for x in ("s0", "z2", "z1", "bsk2", "pfks")))
+    return k
+
+
+class TcbContext:
+    """Owning handle of a cbs_tcb_context (torus circuit bootstrapping with PFKS)."""
+
+    def __init__(self, params: TcbParams | None = None, max_batch: int = 64):
+        self.params = params if params is not None else tcb_default_params()
+        self.max_batch = max_batch
+        self._h = ctypes.c_void_p()
+        call("cbs_tcb_context_create", ctypes.byref(self.params), max_batch, ctypes.byref(self._h))
+
+    @property
+    def handle(self) -> int:
+        return self._h.value
+
+    def keygen(self, seed: int) -> None:
+        call("cbs_tcb_keygen", self._h, seed)
+
+    def encrypt(self, bits, seed: int):
+        import numpy as np
+        bits = np.ascontiguousarray(bits, dtype=np.uint8)
+        a = np.zeros((len(bits), self.params.n), np.uint32)
+        b = np.zeros(len(bits), np.uint32)
+        call("cbs_tcb_encrypt_bits", self._h, bits.ctypes.data, len(bits), seed, a.ctypes.data, b.ctypes.data)
+        return a, b
+
+    def export_keys(self, with_pfks: bool = False) -> dict:
+        k = tcb_key_buffers(self.params, with_pfks)
+        call("cbs_tcb_export_keys", self._h, *(_ptr(k[x]) for x in ("s0", "z2", "z1", "bsk2", "pfks")))
+        return k
+
+    def close(self) -> None:
+        if self._h.value:
+            load().cbs_tcb_context_destroy(self._h)
             self._h = ctypes.c_void_p()
 
     def __del__(self):

@@ -19,6 +19,7 @@
 #include <new>
 #include <string>
 #include <thread>
+#include <type_traits>
 #include <vector>
 
 #include "common.cuh"
@@ -26,33 +27,9 @@
 #include "fft_core.cuh"
 #include "fft_kernels.cuh"
 #include "keygen.h"
+#include "torus.cuh"
 
 namespace cbs {
-
-// one request of a ragged batch: count ciphertexts a [count][n], b [count] in, outputs out_a,
-// out_b; offset = number of ciphertexts in the requests before it
-struct GateReq {
-    const uint32_t* a;
-    const uint32_t* b;
-    uint32_t* out_a;
-    uint32_t* out_b;
-    uint32_t offset, count;
-};
-
-struct GateArgs {
-    int gate;              // CBS_GATE_* or -1: bootstrap in1 as is
-    const uint32_t* a1;    // [count][n]
-    const uint32_t* b1;    // [count]
-    const uint32_t* a2;
-    const uint32_t* b2;
-    uint32_t n, levels, bg_bits;
-    const double2* bskf;   // [n][2*levels][2][M] key spectra, slot-major rows
-    const double2* tab;    // FftTab<log2 M>
-    uint32_t* ext;         // [items][N+1] extracted LWE (a then b)
-    const GateReq* reqs;   // ragged mode when non-null: items are the concatenated requests
-    uint32_t num_reqs;
-    uint32_t items;        // ciphertexts in total; CTAs loop over them with stride gridDim.x
-};
 
 // request holding ragged item `item` (binary search over the offsets)
 __device__ __forceinline__ uint32_t gate_req_of(const GateReq* reqs, uint32_t num, uint32_t item) {
@@ -96,6 +73,22 @@ __device__ __forceinline__ double2 gate_twist(const double2* tws, int j, uint32_
     return make_double2(t.y, t.x);
 }
 
+// the torus value of the FP64 result v of an integer-valued product: exact for 32-bit
+// tori (|v| < 2^52); for 64-bit tori v carries FP64 rounding, reduced mod 2^64 exactly
+template <typename TT>
+__device__ __forceinline__ TT to_torus(double v);
+template <>
+__device__ __forceinline__ uint32_t to_torus<uint32_t>(double v) {
+    return static_cast<uint32_t>(static_cast<uint64_t>(__double2ll_rn(v)));
+}
+template <>
+__device__ __forceinline__ uint64_t to_torus<uint64_t>(double v) {
+    const double k = rint(v * 0x1p-64);
+    double r = fma(-k, 0x1p64, v);  // exact: v - k 2^64, |r| <= 2^63
+    if (r >= 0x1p63) r -= 0x1p64;
+    return static_cast<uint64_t>(__double2ll_rn(r));
+}
+
 template <int LOGN>
 struct GateCfg {
     static constexpr uint32_t T = (1u << LOGN) / 8;
@@ -106,7 +99,7 @@ struct GateCfg {
 // h (0: a, 1: b), all in shared memory.  Same step structure as k_blind_rotate_fft: digits of
 // the own component, forward FFT + products against both key columns per digit, swap of
 // partial sums, inverse FFT, rounding to the torus, rotate-add acc += (X^a - 1) t in place.
-template <int LOGN>
+template <int LOGN, typename TT>
 __global__ void __launch_bounds__(GateCfg<LOGN>::T, GateCfg<LOGN>::MIN_BLOCKS) k_gate_blind_rotate(const GateArgs a) {
     constexpr int LOGM = LOGN - 1;
     constexpr uint32_t N = 1u << LOGN, M = N / 2, TH = M / 8, T = 2 * TH, TWO_N = 2 * N;
@@ -115,16 +108,17 @@ __global__ void __launch_bounds__(GateCfg<LOGN>::T, GateCfg<LOGN>::MIN_BLOCKS) k
     extern __shared__ __align__(16) uint64_t smem[];
     double2* fs = reinterpret_cast<double2*>(smem);                 // [2][M]
     double2* tab = fs + 2 * M;                                      // FftTab<LOGM>
-    uint32_t* acc = reinterpret_cast<uint32_t*>(tab + Tb::size());  // [2][N]
-    uint32_t* dig = acc + 2 * N;                                    // [2][levels][M] packed pairs
+    TT* acc = reinterpret_cast<TT*>(tab + Tb::size());             // [2][N] torus values
+    uint32_t* dig = reinterpret_cast<uint32_t*>(acc + 2 * N);      // [2][levels][M] packed pairs
     const double2* tws = tab + Tb::twist_off();
     const uint32_t ct = blockIdx.x, tid = threadIdx.x;
     const uint32_t h = tid / TH, ht = tid % TH;
-    uint32_t* my_acc = acc + h * N;
+    TT* my_acc = acc + h * N;
     double2* my_fs = fs + h * M;
     const uint32_t levels = a.levels, bg = a.bg_bits;
-    uint32_t off = 1u << (32 - levels * bg - 1);  // rounding of the dropped bits
-    for (uint32_t k = 0; k < levels; ++k) off += (1u << (bg - 1)) << (32 - (k + 1) * bg);
+    constexpr uint32_t W = 8 * sizeof(TT);  // torus width: 32 or 64 bits
+    TT off = TT(1) << (W - levels * bg - 1);  // rounding of the dropped bits
+    for (uint32_t k = 0; k < levels; ++k) off += (TT(1) << (bg - 1)) << (W - (k + 1) * bg);
     auto half_bar = [h]() {
         if (h == 0) asm volatile("bar.sync 1, %0;" ::"n"(TH) : "memory");
         else asm volatile("bar.sync 2, %0;" ::"n"(TH) : "memory");
@@ -144,15 +138,17 @@ __global__ void __launch_bounds__(GateCfg<LOGN>::T, GateCfg<LOGN>::MIN_BLOCKS) k
             a2 = a1;
             b = rq.b[k];
         } else {
-            a1 = a.a1 + static_cast<size_t>(item) * a.n;
-            a2 = a.a2 ? a.a2 + static_cast<size_t>(item) * a.n : a1;
-            b = gate_b(a.gate, a.b1[item], a.b2 ? a.b2[item] : 0u);
+            const uint32_t in = item / a.levels_tv;
+            a1 = a.a1 + static_cast<size_t>(in) * a.n;
+            a2 = a.a2 ? a.a2 + static_cast<size_t>(in) * a.n : a1;
+            b = gate_b(a.gate, a.b1[in], a.b2 ? a.b2[in] : 0u);
         }
+        const TT mu = static_cast<TT>(a.mu[item % a.levels_tv]), b_add = static_cast<TT>(a.b_add[item % a.levels_tv]);
         {
             const uint32_t bt = ms(b);
             for (uint32_t i = tid; i < N; i += T) {
                 acc[i] = 0;
-                acc[N + i] = (((i + bt) & (TWO_N - 1)) < N) ? (1u << 29) : (0u - (1u << 29));
+                acc[N + i] = (((i + bt) & (TWO_N - 1)) < N) ? mu : TT(0) - mu;
             }
         }
         __syncthreads();
@@ -161,10 +157,10 @@ __global__ void __launch_bounds__(GateCfg<LOGN>::T, GateCfg<LOGN>::MIN_BLOCKS) k
             const uint32_t at = ms(a.reqs ? __ldg(a1 + step) : gate_a(a.gate, __ldg(a1 + step), __ldg(a2 + step)));
             if (at == 0) continue;  // X^0 - 1 = 0: the step adds nothing (uniform over the CTA)
             for (uint32_t e = ht; e < M; e += TH) {
-                const uint32_t wr = my_acc[e] + off, wi = my_acc[e + M] + off;
+                const TT wr = my_acc[e] + off, wi = my_acc[e + M] + off;
                 uint32_t* dst = dig + h * levels * M + e;
                 for (uint32_t k = 0; k < levels; ++k) {
-                    const uint32_t s = 32 - (k + 1) * bg, mask = (1u << bg) - 1, half = 1u << (bg - 1);
+                    const uint32_t s = W - (k + 1) * bg, mask = (1u << bg) - 1, half = 1u << (bg - 1);
                     const int32_t dr = static_cast<int32_t>((wr >> s) & mask) - static_cast<int32_t>(half);
                     const int32_t di = static_cast<int32_t>((wi >> s) & mask) - static_cast<int32_t>(half);
                     dst[k * M] = (static_cast<uint32_t>(dr) & 0xffffu) | (static_cast<uint32_t>(di) << 16);
@@ -173,7 +169,7 @@ __global__ void __launch_bounds__(GateCfg<LOGN>::T, GateCfg<LOGN>::MIN_BLOCKS) k
             half_bar();
             const double2* ek = a.bskf + static_cast<size_t>(step) * l2 * 2 * M + ht;
             double2 y0[8], y1[8];
-    #pragma unroll
+#pragma unroll
             for (int j = 0; j < 8; ++j) y0[j] = y1[j] = make_double2(0.0, 0.0);
             for (uint32_t d = 0; d < levels; ++d) {
                 const uint32_t* dsrc = dig + (h * levels + d) * M;
@@ -189,56 +185,56 @@ __global__ void __launch_bounds__(GateCfg<LOGN>::T, GateCfg<LOGN>::MIN_BLOCKS) k
                     x, half_bar);
                 const double2* k0 = ek + static_cast<size_t>(2 * d + h) * 2 * M;
                 const double2* k1 = k0 + M;
-    #pragma unroll
+#pragma unroll
                 for (int j = 0; j < 8; ++j) {
                     cfma(y0[j], x[j], __ldg(k0 + j * TH));
                     cfma(y1[j], x[j], __ldg(k1 + j * TH));
                 }
                 half_bar();
             }
-    #pragma unroll
+#pragma unroll
             for (int j = 0; j < 8; ++j) my_fs[cswz(8 * ht + j)] = h ? y0[j] : y1[j];
             __syncthreads();
             {
                 const double2* take = fs + (1 - h) * M;
-    #pragma unroll
+#pragma unroll
                 for (int j = 0; j < 8; ++j) y0[j] = cadd(h ? y1[j] : y0[j], take[cswz(8 * ht + j)]);
             }
             __syncthreads();
-            uint32_t tre[8], tim[8];
+            TT tre[8], tim[8];
             constexpr double inv_m = 1.0 / M;
             fft_inverse_from_regs<LOGM>(
                 my_fs, ht, tab, y0,
                 [&](int j, uint32_t e, double2 v) {
                     const double2 u = cmulc(v, gate_twist<LOGM>(tws, j, e));
-                    tre[j] = static_cast<uint32_t>(static_cast<uint64_t>(__double2ll_rn(u.x * inv_m)));
-                    tim[j] = static_cast<uint32_t>(static_cast<uint64_t>(__double2ll_rn(u.y * inv_m)));
+                    tre[j] = to_torus<TT>(u.x * inv_m);
+                    tim[j] = to_torus<TT>(u.y * inv_m);
                 },
                 half_bar);
             half_bar();
-            uint32_t* tsm = reinterpret_cast<uint32_t*>(my_fs);  // N words
-    #pragma unroll
+            TT* tsm = reinterpret_cast<TT*>(my_fs);  // N values (the buffer holds 16 M = 8 N bytes)
+#pragma unroll
             for (int j = 0; j < 8; ++j) {
                 tsm[ht + j * TH] = tre[j];
                 tsm[ht + j * TH + M] = tim[j];
             }
             half_bar();
-    #pragma unroll 4
+#pragma unroll 4
             for (uint32_t k = 0; k < N / TH; ++k) {
                 const uint32_t i = ht + k * TH;
                 const uint32_t s = (i + TWO_N - at) & (TWO_N - 1);
-                const uint32_t v = (s < N) ? tsm[s] : 0u - tsm[s - N];
+                const TT v = (s < N) ? tsm[s] : TT(0) - tsm[s - N];
                 my_acc[i] += v - tsm[i];
             }
         }
         __syncthreads();
         // sample extract of coefficient 0: a'_0 = a_0, a'_i = -a_(N-i), b' = b_0
-        uint32_t* out = a.ext + static_cast<size_t>(item) * (N + 1);
+        TT* out = reinterpret_cast<TT*>(a.ext) + static_cast<size_t>(item) * (N + 1);
         for (uint32_t i = tid; i <= N; i += T) {
-            uint32_t v;
-            if (i == N) v = acc[N];
+            TT v;
+            if (i == N) v = acc[N] + b_add;
             else if (i == 0) v = acc[0];
-            else v = 0u - acc[N - i];
+            else v = TT(0) - acc[N - i];
             out[i] = v;
         }
         __syncthreads();  // acc is re-initialised by the next item
@@ -283,21 +279,116 @@ __global__ void __launch_bounds__(256) k_gate_keyswitch(const uint32_t* __restri
     else ob[k] = accv;
 }
 
-template <int LOGN>
+template <int LOGN, typename TT>
 static cudaError_t gate_br_launch(const GateArgs& a, uint32_t grid, cudaStream_t s) {
     constexpr uint32_t N = 1u << LOGN, M = N / 2;
-    const size_t smem = (2ull * M + FftTab<LOGN - 1>::size()) * sizeof(double2) + 2ull * N * sizeof(uint32_t) +
+    const size_t smem = (2ull * M + FftTab<LOGN - 1>::size()) * sizeof(double2) + 2ull * N * sizeof(TT) +
                         2ull * a.levels * M * sizeof(uint32_t);
     static size_t configured[64] = {};
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
     if (configured[dev] < smem) {
-        cudaError_t e = cudaFuncSetAttribute(k_gate_blind_rotate<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             static_cast<int>(smem));
+        cudaError_t e = cudaFuncSetAttribute(k_gate_blind_rotate<LOGN, TT>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
         if (e != cudaSuccess) return e;
         configured[dev] = smem;
     }
-    k_gate_blind_rotate<LOGN><<<grid, GateCfg<LOGN>::T, smem, s>>>(a);
+    k_gate_blind_rotate<LOGN, TT><<<grid, GateCfg<LOGN>::T, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t gate_blind_rotate(const GateArgs& a, uint32_t N, uint32_t grid, cudaStream_t s) {
+    if (N == 1024) return gate_br_launch<10, uint32_t>(a, grid, s);
+    if (N == 2048) return gate_br_launch<11, uint32_t>(a, grid, s);
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t gate_blind_rotate64(const GateArgs& a, uint32_t N, uint32_t grid, cudaStream_t s) {
+    if (N == 1024) return gate_br_launch<10, uint64_t>(a, grid, s);
+    if (N == 2048) return gate_br_launch<11, uint64_t>(a, grid, s);
+    return cudaErrorInvalidValue;
+}
+
+// host helpers shared with the torus circuit bootstrap
+uint32_t torus_from_double(double x) {  // x in torus units (any real), rounded to 2^-32
+    const double f = x - std::floor(x);
+    return static_cast<uint32_t>(static_cast<uint64_t>(std::llround(f * 4294967296.0)));
+}
+
+uint32_t torus_noise(Rng& rng, double sigma) {
+    return static_cast<uint32_t>(static_cast<int64_t>(std::llround(rng.gaussian() * sigma * 4294967296.0)));
+}
+
+// b += a * z (negacyclic, z binary), mod 2^32
+void mul_binary_acc(const uint32_t* a, const int32_t* z, uint32_t N, uint32_t* b) {
+    for (uint32_t j = 0; j < N; ++j) {
+        if (!z[j]) continue;
+        for (uint32_t i = 0; i < N; ++i) {
+            if (i + j < N) b[i + j] += a[i];
+            else b[i + j - N] -= a[i];
+        }
+    }
+}
+
+template <int LOGM, typename KT>
+static void torus_keys_to_fft_t(const KT* keys, size_t count, std::vector<double2>& out) {
+    constexpr uint32_t M = 1u << LOGM, N = 2 * M;
+    using cld = std::complex<long double>;
+    const long double pi = 3.141592653589793238462643383279502884L;
+    std::vector<cld> w(M / 2), twist(M);
+    for (uint32_t e = 0; e < M / 2; ++e) w[e] = std::polar(1.0L, 2.0L * pi * e / M);
+    for (uint32_t e = 0; e < M; ++e) twist[e] = std::polar(1.0L, pi * e / N);
+    out.assign(count * M, make_double2(0, 0));
+    const unsigned nth = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    std::vector<std::thread> pool;
+    for (unsigned th = 0; th < nth; ++th) {
+        pool.emplace_back([&, th] {
+            std::vector<cld> zz(M);
+            for (size_t k = th; k < count; k += nth) {
+                const KT* c = keys + k * N;
+                using ST = typename std::make_signed<KT>::type;  // centred representative
+                for (uint32_t e = 0; e < M; ++e) {
+                    const long double re = static_cast<long double>(static_cast<ST>(c[e]));
+                    const long double im = static_cast<long double>(static_cast<ST>(c[e + M]));
+                    zz[e] = cld(re, im) * twist[e];
+                }
+                // decimation-in-frequency, natural order in, bit-reversed out (fft_core.cuh)
+                for (size_t hh = M / 2; hh >= 1; hh /= 2) {
+                    const size_t stride = M / (2 * hh);
+                    for (size_t s0 = 0; s0 < M; s0 += 2 * hh)
+                        for (size_t j = 0; j < hh; ++j) {
+                            const cld u = zz[s0 + j], v = zz[s0 + j + hh];
+                            zz[s0 + j] = u + v;
+                            zz[s0 + j + hh] = (u - v) * w[j * stride];
+                        }
+                    if (hh == 1) break;
+                }
+                for (uint32_t e = 0; e < M; ++e)
+                    out[k * M + (e % 8) * (M / 8) + e / 8] =
+                        make_double2(static_cast<double>(zz[e].real()), static_cast<double>(zz[e].imag()));
+            }
+        });
+    }
+    for (auto& t : pool) t.join();
+}
+
+void torus_keys_to_fft(uint32_t N, const uint32_t* keys, size_t count, std::vector<double2>& out) {
+    if (N == 1024) torus_keys_to_fft_t<9>(keys, count, out);
+    else if (N == 2048) torus_keys_to_fft_t<10>(keys, count, out);
+    else out.clear();
+}
+
+void torus_keys_to_fft(uint32_t N, const uint64_t* keys, size_t count, std::vector<double2>& out) {
+    if (N == 1024) torus_keys_to_fft_t<9>(keys, count, out);
+    else if (N == 2048) torus_keys_to_fft_t<10>(keys, count, out);
+    else out.clear();
+}
+
+cudaError_t gate_keyswitch(const GateArgs& a, const uint32_t* ksk, uint32_t n, uint32_t N, uint32_t ks_bits,
+                           uint32_t ks_levels, uint32_t* out_a, uint32_t* out_b, cudaStream_t s) {
+    const dim3 grid(a.items, (n + 1 + 255) / 256);
+    k_gate_keyswitch<<<grid, 256, (N + 1) * sizeof(uint32_t), s>>>(static_cast<const uint32_t*>(a.ext), ksk, n, N, ks_bits, ks_levels, out_a, out_b,
+                                                                   a.reqs, a.num_reqs);
     return cudaGetLastError();
 }
 
@@ -325,68 +416,9 @@ struct cbs_gate_context {
 
 namespace {
 
+using cbs::mul_binary_acc;
 using cbs::set_error;
-
-uint32_t torus_from_double(double x) {  // x in torus units (any real), rounded to 2^-32
-    const double f = x - std::floor(x);
-    return static_cast<uint32_t>(static_cast<uint64_t>(std::llround(f * 4294967296.0)));
-}
-
-uint32_t torus_noise(cbs::Rng& rng, double sigma) {
-    return static_cast<uint32_t>(static_cast<int64_t>(std::llround(rng.gaussian() * sigma * 4294967296.0)));
-}
-
-// b += a * z (negacyclic, z binary), mod 2^32
-void mul_binary_acc(const uint32_t* a, const int32_t* z, uint32_t N, uint32_t* b) {
-    for (uint32_t j = 0; j < N; ++j) {
-        if (!z[j]) continue;
-        for (uint32_t i = 0; i < N; ++i) {
-            if (i + j < N) b[i + j] += a[i];
-            else b[i + j - N] -= a[i];
-        }
-    }
-}
-
-template <int LOGM>
-void torus_keys_to_fft(const uint32_t* keys, size_t count, std::vector<double2>& out) {
-    constexpr uint32_t M = 1u << LOGM, N = 2 * M;
-    using cld = std::complex<long double>;
-    const long double pi = 3.141592653589793238462643383279502884L;
-    std::vector<cld> w(M / 2), twist(M);
-    for (uint32_t e = 0; e < M / 2; ++e) w[e] = std::polar(1.0L, 2.0L * pi * e / M);
-    for (uint32_t e = 0; e < M; ++e) twist[e] = std::polar(1.0L, pi * e / N);
-    out.assign(count * M, make_double2(0, 0));
-    const unsigned nth = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
-    std::vector<std::thread> pool;
-    for (unsigned th = 0; th < nth; ++th) {
-        pool.emplace_back([&, th] {
-            std::vector<cld> zz(M);
-            for (size_t k = th; k < count; k += nth) {
-                const uint32_t* c = keys + k * N;
-                for (uint32_t e = 0; e < M; ++e) {
-                    const long double re = static_cast<long double>(static_cast<int32_t>(c[e]));
-                    const long double im = static_cast<long double>(static_cast<int32_t>(c[e + M]));
-                    zz[e] = cld(re, im) * twist[e];
-                }
-                // decimation-in-frequency, natural order in, bit-reversed out (fft_core.cuh)
-                for (size_t hh = M / 2; hh >= 1; hh /= 2) {
-                    const size_t stride = M / (2 * hh);
-                    for (size_t s0 = 0; s0 < M; s0 += 2 * hh)
-                        for (size_t j = 0; j < hh; ++j) {
-                            const cld u = zz[s0 + j], v = zz[s0 + j + hh];
-                            zz[s0 + j] = u + v;
-                            zz[s0 + j + hh] = (u - v) * w[j * stride];
-                        }
-                    if (hh == 1) break;
-                }
-                for (uint32_t e = 0; e < M; ++e)
-                    out[k * M + (e % 8) * (M / 8) + e / 8] =
-                        make_double2(static_cast<double>(zz[e].real()), static_cast<double>(zz[e].imag()));
-            }
-        });
-    }
-    for (auto& t : pool) t.join();
-}
+using cbs::torus_noise;
 
 cbs_status validate_gate(const cbs_gate_params& p) {
     CBS_CHECK_ARG(p.N == 1024 || p.N == 2048, "gate: N must be 1024 or 2048");
@@ -529,10 +561,10 @@ cbs_status cbs_gate_keygen(cbs_gate_context* ctx, uint64_t seed) {
     gate_keys_host(p, seed, ctx->s, ctx->z, ctx->bsk, ctx->ksk);
     std::vector<double2> bskf, tab;
     if (N == 1024) {
-        torus_keys_to_fft<9>(ctx->bsk.data(), ctx->bsk.size() / N, bskf);
+        cbs::torus_keys_to_fft(N, ctx->bsk.data(), ctx->bsk.size() / N, bskf);
         cbs::fft_tables_host(N, tab);
     } else {
-        torus_keys_to_fft<10>(ctx->bsk.data(), ctx->bsk.size() / N, bskf);
+        cbs::torus_keys_to_fft(N, ctx->bsk.data(), ctx->bsk.size() / N, bskf);
         cbs::fft_tables_host(N, tab);
     }
     CBS_CUDA_TRY(ctx->d_bskf.upload(bskf.data(), bskf.size(), nullptr));
@@ -621,12 +653,13 @@ static cbs_status gate_run(cbs_gate_context* ctx, int gate, const uint32_t* d_a1
     a.tab = ctx->d_tab.p;
     a.ext = d_ext ? d_ext : ctx->d_ext.p;
     a.items = count;
-    if (p.N == 1024) CBS_CUDA_TRY(cbs::gate_br_launch<10>(a, count, s));
-    else CBS_CUDA_TRY(cbs::gate_br_launch<11>(a, count, s));
+    a.levels_tv = 1;
+    a.mu[0] = 1u << 29;
+    CBS_CUDA_TRY(cbs::gate_blind_rotate(a, p.N, count, s));
     if (d_out_a && d_out_b) {
         const dim3 grid(count, (p.n + 1 + 255) / 256);
         cbs::k_gate_keyswitch<<<grid, 256, (p.N + 1) * sizeof(uint32_t), s>>>(
-            a.ext, ctx->d_ksk.p, p.n, p.N, p.ks_base_bits, p.ks_levels, d_out_a, d_out_b, nullptr, 0);
+            static_cast<const uint32_t*>(a.ext), ctx->d_ksk.p, p.n, p.N, p.ks_base_bits, p.ks_levels, d_out_a, d_out_b, nullptr, 0);
         CBS_LAUNCH_CHECK();
     }
     return CBS_OK;
@@ -691,11 +724,12 @@ cbs_status cbs_gate_ragged_launch(cbs_gate_context* ctx, cbs_stream_t stream) {
     a.reqs = ctx->d_plan.p;
     a.num_reqs = ctx->plan_reqs;
     a.items = ctx->plan_items;
-    if (p.N == 1024) CBS_CUDA_TRY(cbs::gate_br_launch<10>(a, ctx->plan_grid, stream));
-    else CBS_CUDA_TRY(cbs::gate_br_launch<11>(a, ctx->plan_grid, stream));
+    a.levels_tv = 1;
+    a.mu[0] = 1u << 29;
+    CBS_CUDA_TRY(cbs::gate_blind_rotate(a, p.N, ctx->plan_grid, stream));
     const dim3 grid(ctx->plan_items, (p.n + 1 + 255) / 256);
     cbs::k_gate_keyswitch<<<grid, 256, (p.N + 1) * sizeof(uint32_t), stream>>>(
-        a.ext, ctx->d_ksk.p, p.n, p.N, p.ks_base_bits, p.ks_levels, nullptr, nullptr, a.reqs, a.num_reqs);
+        static_cast<const uint32_t*>(a.ext), ctx->d_ksk.p, p.n, p.N, p.ks_base_bits, p.ks_levels, nullptr, nullptr, a.reqs, a.num_reqs);
     CBS_LAUNCH_CHECK();
     return CBS_OK;
 }

@@ -328,6 +328,51 @@ cbs_status cbs_gate_ragged_plan(cbs_gate_context *ctx, const cbs_gate_request *h
 cbs_status cbs_gate_ragged_launch(cbs_gate_context *ctx, cbs_stream_t stream);
 
 /* ------------------------------------------------------------------------------------
+ * Torus circuit bootstrapping with private functional key switching (PFKS): an LWE bit
+ * (level 0: dimension n, torus32) becomes an RGSW ciphertext under a level-1 RLWE key
+ * (N1, torus32) through cb_levels level-2 blind rotations (ring N2, 64-bit torus, gadget
+ * 2^bg2_bits x l2, FP64 FFT products) with the test vectors g_k / 2, g_k = 2^-(cb_bits (k+1)),
+ * and two PFKS per level (digits of the top 32 bits) into RLWE rows:
+ * row 2k+1 = PFKS_id(m g_k) (component b carries m g_k), row 2k = PFKS_{-z1}(m g_k)
+ * (component a carries m g_k).  No counterpart in the reference, whose circuit bootstrap
+ * uses HomTrace + SchemeSwitch (cbs_circuit_bootstrap_batch_device); this is the PFKS
+ * form the configuration names (base 2^4, 8 digits).  Output RGSW:
+ * [count][cb_levels][2 rows][2 polys][N1] u32, row 2k+c with the message on component c.
+ * Keys: level-2 BSK [n][2*l2][2][N2] uint64; PFKS [2 functions (-z1, id)][N2+1][pfks_levels]
+ * [2^pfks_base_bits - 1][2][N1] uint32.
+ * ------------------------------------------------------------------------------------ */
+typedef struct {
+    uint32_t n;              /* level-0 LWE dimension */
+    uint32_t N2;             /* level-2 ring (blind rotation): 1024 or 2048 on the device */
+    uint32_t bg2_bits, l2;   /* level-2 gadget */
+    uint32_t N1;             /* level-1 ring (output RGSW) */
+    uint32_t cb_bits, cb_levels;          /* output RGSW gadget (cb_levels <= 8) */
+    uint32_t pfks_base_bits, pfks_levels; /* PFKS digits (base_bits * levels = 32) */
+    double sigma_lwe;        /* level-0 noise */
+    double sigma_lvl2;       /* level-2 bootstrapping-key noise */
+    double sigma_lvl1;       /* PFKS key noise */
+} cbs_tcb_params;
+
+typedef struct cbs_tcb_context cbs_tcb_context;
+
+/* n = 630, N2 = 2048, 2^9 x 3, N1 = 1024, output 2^6 x 3, PFKS 2^4 x 8, sigma 2^-15 / 2^-44 / 2^-25 */
+cbs_status cbs_tcb_params_default(cbs_tcb_params *out);
+cbs_status cbs_tcb_context_create(const cbs_tcb_params *params, uint32_t max_batch, cbs_tcb_context **out);
+cbs_status cbs_tcb_context_destroy(cbs_tcb_context *ctx);
+cbs_status cbs_tcb_keygen(cbs_tcb_context *ctx, uint64_t seed);
+/* the same keys on the host only (no device); NULL skips an output */
+cbs_status cbs_tcb_generate_keys_host(const cbs_tcb_params *params, uint64_t seed, int32_t *s0, int32_t *z2,
+                                      int32_t *z1, uint64_t *bsk2, uint32_t *pfks);
+cbs_status cbs_tcb_export_keys(const cbs_tcb_context *ctx, int32_t *s0, int32_t *z2, int32_t *z1, uint64_t *bsk2,
+                               uint32_t *pfks);
+cbs_status cbs_tcb_encrypt_bits(const cbs_tcb_context *ctx, const uint8_t *h_bits, uint32_t count, uint64_t seed,
+                                uint32_t *h_a, uint32_t *h_b);
+/* d_a [count][n], d_b [count] -> d_rgsw [count][cb_levels][2][2][N1]; d_ext (optional,
+ * [count][cb_levels][N2+1] uint64) receives the level-2 LWEs of m g_k that feed the PFKS */
+cbs_status cbs_tcb_circuit_bootstrap_device(cbs_tcb_context *ctx, const uint32_t *d_a, const uint32_t *d_b,
+                                            uint32_t count, uint64_t *d_ext, uint32_t *d_rgsw, cbs_stream_t stream);
+
+/* ------------------------------------------------------------------------------------
  * RNS (Phantom) core: multi-prime NTT and hybrid key switching, CKKS form.
  * Key modulus chain = the size_q primes of Q followed by the size_p special primes P
  * (every one < 2^60, prime, = 1 mod 2N, distinct); alpha = size_p is the digit width and

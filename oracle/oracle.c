@@ -828,6 +828,11 @@ static void torus_decompose(uint32_t x, uint32_t bg_bits, uint32_t levels, int32
 
 void orc_gate_blind_rotate(const orc_gate_params *p, const uint32_t *bsk, const uint32_t *a, uint32_t b,
                            uint32_t *ext) {
+    orc_gate_blind_rotate_tv(p, bsk, a, b, 1u << 29, 0, ext);
+}
+
+void orc_gate_blind_rotate_tv(const orc_gate_params *p, const uint32_t *bsk, const uint32_t *a, uint32_t b,
+                              uint32_t mu, uint32_t b_add, uint32_t *ext) {
     const uint32_t N = p->N, L = p->levels, two_n = 2 * N;
     uint32_t logn2 = 0;
     while ((1u << logn2) < two_n) ++logn2;
@@ -840,7 +845,7 @@ void orc_gate_blind_rotate(const orc_gate_params *p, const uint32_t *bsk, const 
     const uint32_t bt = MS(b);
     for (uint32_t i = 0; i < N; ++i) {
         const uint32_t s = (i + bt) % two_n; /* coefficient i of X^-bt TV = TV[i + bt] (wrapped) */
-        acc[N + i] = (s < N) ? (1u << 29) : (0u - (1u << 29));
+        acc[N + i] = (s < N) ? mu : 0u - mu;
     }
     for (uint32_t step = 0; step < p->n; ++step) {
         const uint32_t at = MS(a[step]);
@@ -864,10 +869,84 @@ void orc_gate_blind_rotate(const orc_gate_params *p, const uint32_t *bsk, const 
     /* sample extract of coefficient 0 */
     ext[0] = acc[0];
     for (uint32_t i = 1; i < N; ++i) ext[i] = 0u - acc[N - i];
-    ext[N] = acc[N];
+    ext[N] = acc[N] + b_add;
     free(dig);
     free(prod);
     free(acc);
+}
+
+/* out += d * k (negacyclic, d small signed digits, k torus64) */
+static void torus64_mac(uint64_t *out, const int32_t *d, const uint64_t *k, uint32_t N) {
+    for (uint32_t i = 0; i < N; ++i) {
+        if (!d[i]) continue;
+        const uint64_t di = (uint64_t)(int64_t)d[i];
+        for (uint32_t j = 0; j < N; ++j) {
+            const uint64_t v = di * k[j];
+            if (i + j < N) out[i + j] += v;
+            else out[i + j - N] -= v;
+        }
+    }
+}
+
+void orc_tcb_blind_rotate64(const orc_gate_params *p, const uint64_t *bsk, const uint32_t *a, uint32_t b,
+                            uint64_t mu, uint64_t b_add, uint64_t *ext) {
+    const uint32_t N = p->N, L = p->levels, two_n = 2 * N, bg = p->bg_bits;
+    uint32_t logn2 = 0;
+    while ((1u << logn2) < two_n) ++logn2;
+    const uint32_t sh = 32 - logn2;
+#define MS(x) ((uint32_t)(((x) + (1u << (sh - 1))) >> sh) & (two_n - 1))
+    uint64_t *acc = (uint64_t *)calloc(2 * N, sizeof(uint64_t));
+    uint64_t *prod = (uint64_t *)malloc(2 * N * sizeof(uint64_t));
+    int32_t *dig = (int32_t *)malloc((size_t)2 * L * N * sizeof(int32_t));
+    uint64_t off = 1ull << (64 - L * bg - 1);
+    for (uint32_t k = 0; k < L; ++k) off += (1ull << (bg - 1)) << (64 - (k + 1) * bg);
+    const uint32_t bt = MS(b);
+    for (uint32_t i = 0; i < N; ++i) acc[N + i] = ((i + bt) % two_n < N) ? mu : 0ull - mu;
+    for (uint32_t step = 0; step < p->n; ++step) {
+        const uint32_t at = MS(a[step]);
+        if (at == 0) continue;
+        for (uint32_t c = 0; c < 2; ++c)
+            for (uint32_t i = 0; i < N; ++i) {
+                const uint64_t w = acc[c * N + i] + off;
+                for (uint32_t k = 0; k < L; ++k)
+                    dig[((size_t)(2 * k + c)) * N + i] =
+                        (int32_t)((w >> (64 - (k + 1) * bg)) & ((1u << bg) - 1)) - (int32_t)(1u << (bg - 1));
+            }
+        memset(prod, 0, 2 * N * sizeof(uint64_t));
+        const uint64_t *key = bsk + (size_t)step * 2 * L * 2 * N;
+        for (uint32_t r = 0; r < 2 * L; ++r)
+            for (uint32_t c = 0; c < 2; ++c) torus64_mac(prod + c * N, dig + (size_t)r * N, key + ((size_t)r * 2 + c) * N, N);
+        for (uint32_t c = 0; c < 2; ++c)
+            for (uint32_t i = 0; i < N; ++i) {
+                const uint32_t t = (i + at) % two_n;
+                if (t < N) acc[c * N + t] += prod[c * N + i];
+                else acc[c * N + t - N] -= prod[c * N + i];
+                acc[c * N + i] -= prod[c * N + i];
+            }
+    }
+#undef MS
+    ext[0] = acc[0];
+    for (uint32_t i = 1; i < N; ++i) ext[i] = 0ull - acc[N - i];
+    ext[N] = acc[N] + b_add;
+    free(dig);
+    free(prod);
+    free(acc);
+}
+
+void orc_tcb_pfks(uint32_t N2, uint32_t N1, uint32_t base_bits, uint32_t levels, const uint32_t *key,
+                  const uint64_t *ext, uint32_t *out) {
+    const uint32_t base = 1u << base_bits;
+    memset(out, 0, 2 * N1 * sizeof(uint32_t));
+    for (uint32_t i = 0; i <= N2; ++i) {
+        const uint64_t x64 = (i < N2) ? 0ull - ext[i] : ext[N2]; /* phase = sum x_i y_i */
+        const uint32_t x = (uint32_t)((x64 + (1ull << 31)) >> 32);  /* top 32 bits, rounded */
+        for (uint32_t j = 0; j < levels; ++j) {
+            const uint32_t v = (x >> (32 - (j + 1) * base_bits)) & (base - 1);
+            if (!v) continue;
+            const uint32_t *row = key + (((size_t)i * levels + j) * (base - 1) + (v - 1)) * 2 * N1;
+            for (uint32_t c = 0; c < 2 * N1; ++c) out[c] += row[c];
+        }
+    }
 }
 
 void orc_gate_keyswitch(const orc_gate_params *p, const uint32_t *ksk, const uint32_t *ext, uint32_t *out) {

@@ -150,6 +150,19 @@ void orc_gate_combine(int gate, const uint32_t *a1, uint32_t b1, const uint32_t 
  * writes the extracted LWE of dimension N: ext[0..N-1] = a, ext[N] = b */
 void orc_gate_blind_rotate(const orc_gate_params *p, const uint32_t *bsk, const uint32_t *a, uint32_t b,
                            uint32_t *ext);
+/* the same with a constant test vector mu (instead of 1/8) and b_add added to the extracted b */
+void orc_gate_blind_rotate_tv(const orc_gate_params *p, const uint32_t *bsk, const uint32_t *a, uint32_t b,
+                              uint32_t mu, uint32_t b_add, uint32_t *ext);
+/* level-2 blind rotation on the 64-bit torus (exact integer products mod 2^64), constant test
+ * vector mu, b_add added to the extracted b: bsk [n][2*levels][2][N] u64, a/b level-0 torus32 */
+void orc_tcb_blind_rotate64(const orc_gate_params *p, const uint64_t *bsk, const uint32_t *a, uint32_t b,
+                            uint64_t mu, uint64_t b_add, uint64_t *ext);
+/* private functional key switch of an extracted torus64 LWE (a[N2], b) into a torus32 RLWE of
+ * dimension N1 (CGGI 2017 Alg. 2): key [N2+1][levels][base-1][2][N1] = RLWE(f(v * y_i *
+ * 2^(32-(j+1)*base_bits))), y_i = key_i (i < N2), y_N2 = 1; digits of the top 32 bits of
+ * (-a, b) rounded */
+void orc_tcb_pfks(uint32_t N2, uint32_t N1, uint32_t base_bits, uint32_t levels, const uint32_t *key,
+                  const uint64_t *ext, uint32_t *out);
 /* LWE key switch N -> n (binfhe-base-scheme-batch.cu:145-185): ksk [N][ks_levels][base-1][n+1] */
 void orc_gate_keyswitch(const orc_gate_params *p, const uint32_t *ksk, const uint32_t *ext, uint32_t *out);
 
