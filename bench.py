@@ -632,6 +632,65 @@ def run_ragged(args, rank: int, world: int, local_rank: int) -> None:
         c.close()
 
 
+def run_tcb(args, rank: int, world: int, local_rank: int) -> None:
+    """Circuit bootstrapping with PFKS (the configuration's parameters): `--batch` LWE bits
+    (default 256, n=630, sigma 2^-15) to RGSW under the level-1 key per step; then the phase
+    error of every produced RGSW row against its exact message and the failure probability
+    of one CMux that uses these rows (Gaussian tail of the measured row error)."""
+    import math
+
+    import torch
+    torch.cuda.set_device(local_rank)
+    pkg = load_pkg()
+    sys.path.insert(0, str(ROOT / "tests"))
+    from tcb_harness import rgsw_row_errors  # noqa: E402  (exact decryption of the rows)
+    count = args.batch or 256
+    ctx = pkg.TcbContext(max_batch=count)
+    ctx.keygen(args.seed)
+    p = ctx.params
+    rng = np.random.default_rng(args.seed + rank)
+    bits = rng.integers(0, 2, count).astype(np.uint8)
+    a, b = ctx.encrypt(bits, seed=args.seed + 3)
+    da = torch.from_numpy(a.view(np.int32)).cuda()
+    db = torch.from_numpy(b.view(np.int32)).cuda()
+    rgsw = torch.zeros((count, p.cb_levels, 2, 2, p.N1), dtype=torch.int32, device="cuda")
+    stream = torch.cuda.Stream()
+    fn = lambda: pkg.call("cbs_tcb_circuit_bootstrap_device", ctx.handle, da.data_ptr(), db.data_ptr(), count,  # noqa: E731
+                          None, rgsw.data_ptr(), stream.cuda_stream)
+    with ClockSampler(local_rank) as clk:
+        ms = _timed(torch, stream, fn, args.warmup, args.steps)
+    keys = ctx.export_keys(with_pfks=False)
+    sample = min(count, 32)
+    rg = rgsw[:sample].cpu().numpy().view(np.uint32)
+    err = rgsw_row_errors(rg, bits[:sample], keys["z1"], p.cb_bits, p.cb_levels).astype(np.float64)
+    sigma_row = float(np.std(err)) / 2 ** 32
+    # one CMux with these rows: error = sum over 2*levels*N1 digit-row products, digits uniform
+    # in [-2^(b-1), 2^(b-1)); a decision at distance 1/8 from the message
+    sigma_digit = (2 ** p.cb_bits) / math.sqrt(12.0)
+    sigma_cmux = math.sqrt(2 * p.cb_levels * p.N1) * sigma_digit * sigma_row
+    z = 0.125 / sigma_cmux
+    log2_pfail = (math.log2(math.erfc(z / math.sqrt(2))) if z < 37 else
+                  -(z * z / 2) / math.log(2) - math.log2(z * math.sqrt(math.pi / 2)))
+    pfks_bytes = 2 * (p.N2 + 1) * p.pfks_levels * ((1 << p.pfks_base_bits) - 1) * 2 * p.N1 * 4
+    out = {"metric": "circuit bootstraps/s with PFKS (n=630 -> RGSW, N2=2048 2^9x3, PFKS 2^4x8, FP64 FFT)",
+           "value": world * count / (ms * 1e-3), "unit": "bits/s", "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64 (64-bit-torus FFT products) + u32/u64 torus",
+           "data": "synthetic (seeded uniform random bits)",
+           "config": {"workload": "tcb_pfks", "bits": count, "n": p.n, "N2": p.N2, "l2": p.l2, "bg2_bits": p.bg2_bits,
+                      "N1": p.N1, "cb": f"2^{p.cb_bits}x{p.cb_levels}", "pfks": f"2^{p.pfks_base_bits}x{p.pfks_levels}",
+                      "l2_cache": f"PFKS keys {pfks_bytes / 1e9:.1f} GB >> 126 MB L2"},
+           "us_per_bit": ms * 1e3 / count, "gpu_launches": args.steps * 2,
+           "phase_error": {"rows_sampled": int(err.size), "sigma_log2": math.log2(sigma_row),
+                           "max_log2": math.log2(float(np.max(np.abs(err))) / 2 ** 32),
+                           "cmux_sigma_log2": math.log2(sigma_cmux), "cmux_pfail_log2": log2_pfail,
+                           "note": "row phases vs exact m*g_k (row 2k+1) and -m*g_k*z1 (row 2k); FP64 path"},
+           "clocks": clk.summary()}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    ctx.close()
+
+
 def compute_rate(backend: str, T: int, p, br_ms: float) -> dict:
     """Algorithmic arithmetic of one blind-rotation launch over T ciphertexts."""
     N, n, l2 = p.N, p.n, 2 * p.digits_g
@@ -728,7 +787,7 @@ def main() -> None:
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--backend", choices=["fft64", "ntt"], default="fft64")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
-    ap.add_argument("--workload", choices=["aes128", "blind_rotate", "keyswitch", "rns_ntt", "gate", "ragged"], default="aes128",
+    ap.add_argument("--workload", choices=["aes128", "blind_rotate", "keyswitch", "rns_ntt", "gate", "ragged", "tcb"], default="aes128",
                     help="aes128 is the headline; the others time one kernel family")
     ap.add_argument("--batch", type=int, default=0, help="units per step for the kernel workloads")
     ap.add_argument("--alpha", type=int, default=2, help="special primes (digit width) for --workload keyswitch")
@@ -750,7 +809,7 @@ def main() -> None:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     runner = {"aes128": run_ours, "blind_rotate": run_blind_rotate, "keyswitch": run_keyswitch,
               "rns_ntt": run_rns_ntt, "gate": run_gate,
-              "ragged": run_ragged}[args.workload]
+              "ragged": run_ragged, "tcb": run_tcb}[args.workload]
     try:
         runner(args, rank, world, local_rank)
     finally:
