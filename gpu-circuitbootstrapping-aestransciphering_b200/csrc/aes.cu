@@ -77,6 +77,21 @@ static cbs_status aes_round(cbs_context* c, uint32_t round, uint32_t chunk, cuda
     const uint32_t N = c->p.N, n = c->p.n, L = c->p.num_lut;
     const uint32_t T = chunk * 128, luts = chunk * 16;
     const bool final_round = (round == 10);
+    if (c->br_backend == CBS_BR_FFT64) {
+        // FFT path: MV RLWEs, LUT ciphertexts and words stay in the coefficient domain; the
+        // RGSW controls are kept as row spectra in the RGSW buffer
+        double2* rgswf = reinterpret_cast<double2*>(c->d_rgsw.p);
+        if (cbs_status st = run_blind_rotate(c, A.st_a.p, A.st_b.p, T, n, c->d_mv.p, s, false)) return st;
+        if (cbs_status st = run_trace_fft(c, c->d_mv.p, T * L, rgswf, s)) return st;
+        if (cbs_status st = run_lut_levels_fft(c, A.tables_coef.p, 256ull * 2 * N, A.lut_sel[final_round ? 1 : 0].p,
+                                               rgswf, static_cast<uint64_t>(L) * 4 * (N / 2), A.ctrl_bits.p, luts,
+                                               A.lut_a.p, A.lut_b.p, A.lut_out.p, s))
+            return st;
+        CBS_CUDA_TRY(launch_assemble_words(A.words.p, A.lut_out.p,
+                                           A.rk_words_coef.p + static_cast<size_t>(round) * 4 * 2 * N, c->p.Q, N,
+                                           chunk, s));
+        return run_extract(c, A.words.p, A.extract_info.p, T, A.st_a.p, A.st_b.p, n, s);
+    }
     if (cbs_status st = run_blind_rotate(c, A.st_a.p, A.st_b.p, T, n, c->d_mv.p, s)) return st;
     if (cbs_status st = run_trace(c, c->d_mv.p, T * L, c->d_rgsw.p, s)) return st;
     if (cbs_status st = run_lut_levels(c, A.tables.p, 256ull * 2 * N, A.lut_sel[final_round ? 1 : 0].p, c->d_rgsw.p,
@@ -183,6 +198,12 @@ cbs_status cbs_aes128_setup(cbs_context* ctx, const uint8_t* key, uint64_t seed)
     CBS_CUDA_TRY(A.rk_words.upload(A.h_rk_words.data(), A.h_rk_words.size(), s));
     CBS_CUDA_TRY(A.rk0_a.upload(A.h_rk0_a.data(), A.h_rk0_a.size(), s));
     CBS_CUDA_TRY(A.rk0_b.upload(A.h_rk0_b.data(), A.h_rk0_b.size(), s));
+    CBS_CUDA_TRY(A.tables_coef.alloc(A.h_tables.size()));
+    CBS_CUDA_TRY(A.rk_words_coef.alloc(A.h_rk_words.size()));
+    CBS_CUDA_TRY(ntt_inverse(A.tables_coef.p, A.tables.p, nullptr, c->d_irp.p, c->d_irps.p, c->d_mod.p, c->d_ninv.p,
+                             c->d_ninv_s.p, N, A.h_tables.size() / N, s));
+    CBS_CUDA_TRY(ntt_inverse(A.rk_words_coef.p, A.rk_words.p, nullptr, c->d_irp.p, c->d_irps.p, c->d_mod.p,
+                             c->d_ninv.p, c->d_ninv_s.p, N, A.h_rk_words.size() / N, s));
     CBS_CUDA_TRY(cudaStreamSynchronize(s));
     A.ready = true;
     return CBS_OK;

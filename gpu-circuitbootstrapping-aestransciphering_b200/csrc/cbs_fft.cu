@@ -20,53 +20,9 @@
 #include "common.cuh"
 #include "fft_core.cuh"
 #include "fft_kernels.cuh"
+#include "fft_ops.cuh"
 
 namespace cbs {
-
-// v mod Q, v the FP64 value of an integer-valued product (|v| < 2^90), computed in FP64:
-// k = rint(v / Q), r = v - k*q_hi - k*q_lo with two fused multiply-adds.  The two roundings of
-// r (|r| < 2Q < 2^55) add at most +-8 to the result, far below the FFT's own rounding error.
-__device__ __forceinline__ uint64_t double_to_mod(double v, const FftKeyArgs& f, uint64_t Q) {
-    const double k = rint(v * f.inv_q);
-    double r = fma(-k, f.q_hi, v);
-    r = fma(-k, f.q_lo, r);
-    int64_t i = __double2ll_rn(r);
-    if (i < 0) i += static_cast<int64_t>(Q);
-    if (i < 0) i += static_cast<int64_t>(Q);
-    if (i >= static_cast<int64_t>(Q)) i -= static_cast<int64_t>(Q);
-    return static_cast<uint64_t>(i);
-}
-
-// Balanced base-2^gbits digits of the prepared value v, all at once: adding
-// O = sum_k 2^(gbits-1) 2^(gbits k) makes every digit field non-negative, so digit k is field
-// k of v + O minus 2^(gbits-1).  This is the unique balanced representation of v modulo
-// 2^(gbits digits) with digits in [-2^(gbits-1), 2^(gbits-1)), i.e. what peel_digit yields
-// with the final carry dropped.
-__device__ __forceinline__ int32_t balanced_digit(int64_t w, int gbits, uint32_t k) {
-    const uint32_t field = static_cast<uint32_t>(static_cast<uint64_t>(w) >> (gbits * k)) & ((1u << gbits) - 1u);
-    return static_cast<int32_t>(field) - (1 << (gbits - 1));
-}
-
-// gadget_prepare(x) + offset for x in [0, Q): centre, round away the ign low bits, add the
-// digit offset.  The sum is non-negative because the offset times 2^ign is at least Q / 2.
-__device__ __forceinline__ int64_t prepared_offset(uint64_t x, uint64_t Q, uint64_t qhalf, uint64_t round_c, int ign) {
-    uint64_t t = x + round_c;
-    if (x >= qhalf) t -= Q;
-    return static_cast<int64_t>(t >> ign);
-}
-
-__device__ __forceinline__ uint32_t pack_digits(int32_t re, int32_t im) {
-    return (static_cast<uint32_t>(re) & 0xffffu) | (static_cast<uint32_t>(im) << 16);
-}
-
-// zeta^e from the half table: register slot j of the first/last pass holds e = tid + j*M/8,
-// so e < M/2 exactly for j < 4; above, zeta^e = i * conj(zeta^(M-e)) = swapped components.
-template <int LOGM>
-__device__ __forceinline__ double2 twist_at(const double2* tws, int j, uint32_t e) {
-    if (j < 4) return tws[e];
-    const double2 t = tws[(1u << LOGM) - e];
-    return make_double2(t.y, t.x);
-}
 
 template <int LOGN>
 struct BrFftCfg {
@@ -257,7 +213,7 @@ static cudaError_t br_fft_launch(const BlindRotateArgs& a, const FftKeyArgs& f, 
 }
 
 cudaError_t launch_blind_rotate_fft(const BlindRotateArgs& a, const FftKeyArgs& f, const cbs_dmodulus* d_mod,
-                                    uint32_t N, uint32_t batch, cudaStream_t s) {
+                                    uint32_t N, uint32_t batch, cudaStream_t s, bool mv_ntt) {
     if (batch == 0) return cudaSuccess;
     cudaError_t e;
     switch (N) {
@@ -266,7 +222,7 @@ cudaError_t launch_blind_rotate_fft(const BlindRotateArgs& a, const FftKeyArgs& 
         case 4096: e = br_fft_launch<12>(a, f, batch, s); break;
         default: return cudaErrorInvalidValue;
     }
-    if (e != cudaSuccess) return e;
+    if (e != cudaSuccess || !mv_ntt) return e;
     return ntt_forward(a.mv_out, a.mv_out, a.t.rp, a.t.rps, d_mod, N, static_cast<size_t>(batch) * a.num_lut * 2, s);
 }
 
@@ -337,36 +293,60 @@ void fft_tables_host(uint32_t N, std::vector<double2>& tab) {
     }
 }
 
-// NTT-domain key polynomials [count][N] (normal form, mod Q) -> FFT spectra [count][M]
-void keys_to_fft_host(const host::NttTables& t, const uint64_t* keys_ntt, size_t count, std::vector<double2>& out) {
+// NTT-domain key polynomials [count][N] (normal form, mod Q) -> FFT spectra.  Each key
+// polynomial k (centred) yields one spectrum, or, when split_bits > 0 and polynomial index
+// i % group == 0 (the first column of each key row), two: k_hi = round(k / 2^split_bits) and
+// k_lo = k - k_hi 2^split_bits, so the output holds count + count / group spectra.  The
+// halves keep products with small digits below 2^48, where the FP64 transform is exact after
+// rounding.
+void keys_to_fft_host(const host::NttTables& t, const uint64_t* keys_ntt, size_t count, std::vector<double2>& out,
+                      uint32_t split_bits, uint32_t group) {
     const uint32_t N = t.n, M = N / 2;
     const uint64_t Q = t.q;
     const long double pi = 3.141592653589793238462643383279502884L;
+    const bool split = split_bits > 0 && group > 0;
     std::vector<cld> w(M / 2), twist(M);
     for (uint32_t e = 0; e < M / 2; ++e) w[e] = std::polar(1.0L, 2.0L * pi * e / M);
     for (uint32_t e = 0; e < M; ++e) twist[e] = std::polar(1.0L, pi * e / N);
-    out.assign(count * M, make_double2(0, 0));
+    // output spectrum index of input polynomial k (and k's lo half at +1 when split)
+    auto out_index = [&](size_t k) { return split ? k + k / group + (k % group ? 1 : 0) : k; };
+    const size_t total = split ? count + count / group : count;
+    out.assign(total * M, make_double2(0, 0));
     const unsigned nth = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
     std::vector<std::thread> pool;
     for (unsigned th = 0; th < nth; ++th) {
         pool.emplace_back([&, th] {
             std::vector<uint64_t> c(N);
+            std::vector<int64_t> v(N), hi(N), lo(N);
             std::vector<cld> z(M);
+            // spectrum of the integer polynomial p, stored slot-major at spectrum index o:
+            // slot s is consumed by thread s / 8 as its register j = s % 8, so it is stored at
+            // j * (M / 8) + s / 8 and each warp load is contiguous
+            auto emit = [&](const std::vector<int64_t>& p, size_t o) {
+                for (uint32_t e = 0; e < M; ++e)
+                    z[e] = cld(static_cast<long double>(p[e]), static_cast<long double>(p[e + M])) * twist[e];
+                host_dif(z, w);
+                for (uint32_t e = 0; e < M; ++e)
+                    out[o * M + (e % 8) * (M / 8) + e / 8] =
+                        make_double2(static_cast<double>(z[e].real()), static_cast<double>(z[e].imag()));
+            };
             for (size_t k = th; k < count; k += nth) {
                 std::copy(keys_ntt + k * N, keys_ntt + (k + 1) * N, c.begin());
                 host::ntt_inverse_host(c.data(), t);
-                for (uint32_t e = 0; e < M; ++e) {
-                    const long double re = c[e] > Q / 2 ? -static_cast<long double>(Q - c[e]) : static_cast<long double>(c[e]);
-                    const long double im =
-                        c[e + M] > Q / 2 ? -static_cast<long double>(Q - c[e + M]) : static_cast<long double>(c[e + M]);
-                    z[e] = cld(re, im) * twist[e];
+                for (uint32_t e = 0; e < N; ++e)
+                    v[e] = c[e] > Q / 2 ? -static_cast<int64_t>(Q - c[e]) : static_cast<int64_t>(c[e]);
+                const size_t o = out_index(k);
+                if (split && k % group == 0) {
+                    const int64_t half = int64_t(1) << (split_bits - 1);
+                    for (uint32_t e = 0; e < N; ++e) {
+                        hi[e] = (v[e] + half) >> split_bits;  // floor division: round to nearest
+                        lo[e] = v[e] - hi[e] * (int64_t(1) << split_bits);
+                    }
+                    emit(hi, o);
+                    emit(lo, o + 1);
+                } else {
+                    emit(v, o);
                 }
-                host_dif(z, w);
-                // spectrum slot s is consumed by thread s / 8 of a half as its register j = s % 8:
-                // store it at j * (M / 8) + s / 8 so each warp load is contiguous
-                for (uint32_t e = 0; e < M; ++e)
-                    out[k * M + (e % 8) * (M / 8) + e / 8] =
-                        make_double2(static_cast<double>(z[e].real()), static_cast<double>(z[e].imag()));
             }
         });
     }

@@ -35,8 +35,10 @@ static cbs_status prepare_fft(cbs_context* c) {
         return CBS_ERR_NOT_READY;
     }
     const size_t polys = c->hk.bsk.size() / c->p.N;
-    std::vector<double2> bskf, ftab;
+    std::vector<double2> bskf, ftab, htf, ssf;
     keys_to_fft_host(c->tab, c->hk.bsk.data(), polys, bskf);
+    keys_to_fft_host(c->tab, c->hk.ht.data(), c->hk.ht.size() / c->p.N, htf, kTraceKeySplitBits, 2);
+    keys_to_fft_host(c->tab, c->hk.ss.data(), c->hk.ss.size() / c->p.N, ssf, kTraceKeySplitBits, 2);
     fft_tables_host(c->p.N, ftab);
     std::vector<uint64_t> p2(64), p2s(64);
     FastMod fm(c->p.Q);
@@ -49,6 +51,8 @@ static cbs_status prepare_fft(cbs_context* c) {
     cudaStream_t s = c->stream;
     CBS_CUDA_TRY(c->d_bskf.upload(bskf.data(), bskf.size(), s));
     CBS_CUDA_TRY(c->d_fft_tab.upload(ftab.data(), ftab.size(), s));
+    CBS_CUDA_TRY(c->d_htf.upload(htf.data(), htf.size(), s));
+    CBS_CUDA_TRY(c->d_ssf.upload(ssf.data(), ssf.size(), s));
     CBS_CUDA_TRY(c->d_pow2.upload(p2.data(), p2.size(), s));
     CBS_CUDA_TRY(c->d_pow2s.upload(p2s.data(), p2s.size(), s));
     CBS_CUDA_TRY(cudaStreamSynchronize(s));
@@ -56,8 +60,22 @@ static cbs_status prepare_fft(cbs_context* c) {
     return CBS_OK;
 }
 
+FftKeyArgs fft_key_args(const cbs_context* c) {
+    FftKeyArgs f{};
+    f.bskf = c->d_bskf.p;
+    f.tab = c->d_fft_tab.p;
+    f.tab_len = static_cast<uint32_t>(c->d_fft_tab.n);
+    f.pow2 = c->d_pow2.p;
+    f.pow2s = c->d_pow2s.p;
+    f.inv_m = 2.0 / static_cast<double>(c->p.N);
+    f.q_hi = static_cast<double>(c->p.Q);
+    f.q_lo = static_cast<double>(static_cast<int64_t>(c->p.Q) - static_cast<int64_t>(f.q_hi));
+    f.inv_q = 1.0 / static_cast<double>(c->p.Q);
+    return f;
+}
+
 cbs_status run_blind_rotate(cbs_context* c, const uint64_t* d_a, const uint64_t* d_b, uint32_t batch,
-                            uint32_t a_stride, uint64_t* d_mv, cudaStream_t s) {
+                            uint32_t a_stride, uint64_t* d_mv, cudaStream_t s, bool mv_ntt) {
     BlindRotateArgs a{};
     a.t = c->ring();
     a.a = d_a;
@@ -73,22 +91,16 @@ cbs_status run_blind_rotate(cbs_context* c, const uint64_t* d_a, const uint64_t*
     a.num_lut = c->p.num_lut;
     a.gadd = c->d_gadd.p;
     a.mv_out = d_mv;
+    if (!mv_ntt && c->br_backend != CBS_BR_FFT64) {
+        set_error("coefficient-domain MV output needs the FFT backend");
+        return CBS_ERR_INVALID_ARG;
+    }
     if (c->br_backend == CBS_BR_FFT64) {
         if (!c->fft_ready) {
             set_error("FFT backend selected but its key material is not prepared");
             return CBS_ERR_NOT_READY;
         }
-        FftKeyArgs f{};
-        f.bskf = c->d_bskf.p;
-        f.tab = c->d_fft_tab.p;
-        f.tab_len = static_cast<uint32_t>(c->d_fft_tab.n);
-        f.pow2 = c->d_pow2.p;
-        f.pow2s = c->d_pow2s.p;
-        f.inv_m = 2.0 / static_cast<double>(c->p.N);
-        f.q_hi = static_cast<double>(c->p.Q);
-        f.q_lo = static_cast<double>(static_cast<int64_t>(c->p.Q) - static_cast<int64_t>(f.q_hi));
-        f.inv_q = 1.0 / static_cast<double>(c->p.Q);
-        CBS_CUDA_TRY(launch_blind_rotate_fft(a, f, c->d_mod.p, c->p.N, batch, s));
+        CBS_CUDA_TRY(launch_blind_rotate_fft(a, fft_key_args(c), c->d_mod.p, c->p.N, batch, s, mv_ntt));
         return CBS_OK;
     }
     CBS_CUDA_TRY(launch_blind_rotate(a, c->p.N, batch, s));
@@ -109,6 +121,91 @@ cbs_status run_trace(cbs_context* c, const uint64_t* d_mv, uint32_t count, uint6
     a.digits_ht = c->p.digits_ht;
     a.digits_ss = c->p.digits_ss;
     CBS_CUDA_TRY(launch_trace_schemeswitch(a, c->p.N, count, s));
+    return CBS_OK;
+}
+
+// inverse of the odd k modulo 2^bits (Newton iteration on 2-adic inverses)
+static uint32_t inv_pow2(uint32_t k, uint32_t bits) {
+    uint32_t x = k;  // k * k = 1 mod 8
+    for (int i = 0; i < 5; ++i) x *= 2u - k * x;
+    return x & ((bits >= 32) ? ~0u : ((1u << bits) - 1u));
+}
+
+cbs_status run_trace_fft(cbs_context* c, const uint64_t* d_mv_coef, uint32_t count, double2* d_rgswf,
+                         cudaStream_t s) {
+    if (!c->fft_ready) {
+        set_error("FFT HomTrace: FFT key material is not prepared");
+        return CBS_ERR_NOT_READY;
+    }
+    TraceFftArgs a{};
+    a.mv = d_mv_coef;
+    a.rgswf = d_rgswf;
+    a.rounds = c->rounds;
+    const uint32_t N = c->p.N, logn = static_cast<uint32_t>(__builtin_ctz(N));
+    for (uint32_t r = 0; r < c->rounds && r < 16; ++r) a.kinv[r] = inv_pow2((N >> r) + 1, logn + 1);
+    a.htf = c->d_htf.p;
+    a.ssf = c->d_ssf.p;
+    {
+        FastMod fm(c->p.Q);
+        uint64_t v = 1 % c->p.Q;
+        for (uint32_t e = 0; e < kTraceKeySplitBits; ++e) v = fm.mul(v, 2);
+        a.split_pow = v;
+        a.split_pow_s = host::shoup(v, c->p.Q);
+    }
+    a.g_ht = make_digit_prep(c->p.Q, c->g_ht, c->p.digits_ht);
+    a.g_ss = make_digit_prep(c->p.Q, c->g_ss, c->p.digits_ss);
+    a.digits_ht = c->p.digits_ht;
+    a.digits_ss = c->p.digits_ss;
+    CBS_CUDA_TRY(launch_trace_ss_fft(a, fft_key_args(c), N, count, s));
+    return CBS_OK;
+}
+
+cbs_status run_cbs(cbs_context* c, const uint64_t* d_a, const uint64_t* d_b, uint32_t batch, uint32_t a_stride,
+                   uint64_t* d_mv, uint64_t* d_rgsw, cudaStream_t s) {
+    const uint32_t count = batch * c->p.num_lut;
+    if (c->br_backend != CBS_BR_FFT64) {
+        if (cbs_status st = run_blind_rotate(c, d_a, d_b, batch, a_stride, d_mv, s)) return st;
+        return run_trace(c, d_mv, count, d_rgsw, s);
+    }
+    // FFT backend: coefficient-domain MV RLWEs, FFT HomTrace into row spectra in the output
+    // buffer, then back to the NTT-domain reference layout in place
+    if (cbs_status st = run_blind_rotate(c, d_a, d_b, batch, a_stride, d_mv, s, false)) return st;
+    return run_trace_fft_ntt_rows(c, d_mv, count, d_rgsw, s);
+}
+
+cbs_status run_trace_fft_ntt_rows(cbs_context* c, const uint64_t* d_mv_coef, uint32_t count, uint64_t* d_rgsw,
+                                  cudaStream_t s) {
+    if (cbs_status st = run_trace_fft(c, d_mv_coef, count, reinterpret_cast<double2*>(d_rgsw), s)) return st;
+    const size_t polys = static_cast<size_t>(count) * 4;
+    CBS_CUDA_TRY(launch_spectra_to_coef(reinterpret_cast<double2*>(d_rgsw), c->p.Q, fft_key_args(c), c->p.N, polys, s));
+    CBS_CUDA_TRY(ntt_forward(d_rgsw, d_rgsw, c->d_rp.p, c->d_rps.p, c->d_mod.p, c->p.N, polys, s));
+    return CBS_OK;
+}
+
+cbs_status run_lut_levels_fft(cbs_context* c, const uint64_t* d_tables, uint64_t table_stride,
+                              const uint32_t* d_lut_sel, const double2* d_rgswf, uint64_t rgsw_stride,
+                              const uint32_t* d_ctrl, uint32_t luts, uint64_t* d_buf_a, uint64_t* d_buf_b,
+                              uint64_t* d_out, cudaStream_t s) {
+    const uint32_t N = c->p.N;
+    const FftKeyArgs f = fft_key_args(c);
+    const uint64_t* in = d_tables;
+    for (uint32_t level = 0; level < 8; ++level) {
+        CmuxFftArgs a{};
+        a.in_count = 256u >> level;
+        a.in = in;
+        a.in_lut_stride = (level == 0) ? table_stride : static_cast<uint64_t>(a.in_count) * 2 * N;
+        a.lut_sel = (level == 0) ? d_lut_sel : nullptr;
+        uint64_t* out = (level == 7) ? d_out : ((level & 1) ? d_buf_b : d_buf_a);
+        a.out = out;
+        a.rgswf = d_rgswf;
+        a.rgsw_stride = rgsw_stride;
+        a.ctrl_bits = d_ctrl;
+        a.level = level;
+        a.g = make_digit_prep(c->p.Q, c->g_cc, c->p.num_lut);
+        a.digits = c->p.num_lut;
+        CBS_CUDA_TRY(launch_cmux_level_fft(a, f, N, luts, s));
+        in = out;
+    }
     return CBS_OK;
 }
 
@@ -420,7 +517,14 @@ cbs_status cbs_trace_schemeswitch_device(cbs_context* ctx, const uint64_t* d_mv,
     if (count == 0) return CBS_OK;
     CBS_CHECK_ARG(d_mv && d_rgsw, "trace: null pointer");
     if (cbs_status st = need_keys(ctx)) return st;
-    return run_trace(ctx, d_mv, count, d_rgsw, reinterpret_cast<cudaStream_t>(stream));
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    if (ctx->br_backend != CBS_BR_FFT64) return run_trace(ctx, d_mv, count, d_rgsw, s);
+    // FFT backend: the MV RLWEs to the coefficient domain (context scratch), FFT HomTrace
+    const size_t N = ctx->p.N, polys = static_cast<size_t>(count) * 2;
+    CBS_CUDA_TRY(ctx->d_mv.alloc(polys * N));
+    CBS_CUDA_TRY(ntt_inverse(ctx->d_mv.p, d_mv, nullptr, ctx->d_irp.p, ctx->d_irps.p, ctx->d_mod.p, ctx->d_ninv.p,
+                             ctx->d_ninv_s.p, N, polys, s));
+    return run_trace_fft_ntt_rows(ctx, ctx->d_mv.p, count, d_rgsw, s);
 }
 
 cbs_status cbs_circuit_bootstrap_batch_device(cbs_context* ctx, const uint64_t* d_a, const uint64_t* d_b,
@@ -437,8 +541,7 @@ cbs_status cbs_circuit_bootstrap_batch_device(cbs_context* ctx, const uint64_t* 
     }
     if (cbs_status st = need_keys(ctx)) return st;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    if (cbs_status st = run_blind_rotate(ctx, d_a, d_b, batch, a_stride, ctx->d_mv.p, s)) return st;
-    if (cbs_status st = run_trace(ctx, ctx->d_mv.p, batch * ctx->p.num_lut, ctx->d_rgsw.p, s)) return st;
+    if (cbs_status st = run_cbs(ctx, d_a, d_b, batch, a_stride, ctx->d_mv.p, ctx->d_rgsw.p, s)) return st;
     *d_rgsw_view = ctx->d_rgsw.p;
     return CBS_OK;
 }

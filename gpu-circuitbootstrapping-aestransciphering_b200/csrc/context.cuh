@@ -24,6 +24,8 @@ struct AesState {
     uint32_t chunk_blocks = 0;            // blocks per device chunk
     DevBuf<uint64_t> tables;              // [8][256][2][N]  Te0..3, Te4_0..3
     DevBuf<uint64_t> rk_words;            // [11][4][2][N]
+    // coefficient-domain copies of tables and rk_words for the FFT CMux path
+    DevBuf<uint64_t> tables_coef, rk_words_coef;
     DevBuf<uint64_t> rk0_a, rk0_b;        // [128][n], [128]
     std::vector<uint64_t> h_tables, h_rk_words, h_rk0_a, h_rk0_b;
     // per-chunk workspace
@@ -63,6 +65,7 @@ struct cbs_context {
     int br_backend = 0;  // CBS_BR_NTT or CBS_BR_FFT64
     bool fft_ready = false;
     cbs::DevBuf<double2> d_bskf, d_fft_tab;
+    cbs::DevBuf<double2> d_htf, d_ssf;  // HomTrace / SchemeSwitch key spectra
     cbs::DevBuf<uint64_t> d_pow2, d_pow2s;
     // scratch
     cbs::DevBuf<uint64_t> d_mv, d_rgsw;
@@ -89,8 +92,25 @@ struct cbs_context {
 
 namespace cbs {
 // shared entry used by the AES driver and the C ABI
+// mv_ntt = false (FFT backend only) leaves the MV RLWEs in the coefficient domain
 cbs_status run_blind_rotate(cbs_context* c, const uint64_t* d_a, const uint64_t* d_b, uint32_t batch,
-                            uint32_t a_stride, uint64_t* d_mv, cudaStream_t s);
+                            uint32_t a_stride, uint64_t* d_mv, cudaStream_t s, bool mv_ntt = true);
+FftKeyArgs fft_key_args(const cbs_context* c);
+// blind rotation + HomTrace/SchemeSwitch of the selected backend: LWE -> RGSW rows in the
+// NTT-domain reference layout [batch][num_lut][2][2][N]; d_mv is [batch][num_lut][2][N] scratch
+// FFT HomTrace + SchemeSwitch with the rows converted to the NTT-domain reference layout
+cbs_status run_trace_fft_ntt_rows(cbs_context* c, const uint64_t* d_mv_coef, uint32_t count, uint64_t* d_rgsw,
+                                  cudaStream_t s);
+cbs_status run_cbs(cbs_context* c, const uint64_t* d_a, const uint64_t* d_b, uint32_t batch, uint32_t a_stride,
+                   uint64_t* d_mv, uint64_t* d_rgsw, cudaStream_t s);
+// FFT HomTrace + SchemeSwitch: coefficient-domain MV RLWEs -> RGSW row spectra [count][2][2][N/2]
+cbs_status run_trace_fft(cbs_context* c, const uint64_t* d_mv_coef, uint32_t count, double2* d_rgswf,
+                         cudaStream_t s);
+// the 8 FFT CMux levels of the LUT trees, coefficient-domain tables in and outputs out
+cbs_status run_lut_levels_fft(cbs_context* c, const uint64_t* d_tables, uint64_t table_stride,
+                              const uint32_t* d_lut_sel, const double2* d_rgswf, uint64_t rgsw_stride,
+                              const uint32_t* d_ctrl, uint32_t luts, uint64_t* d_buf_a, uint64_t* d_buf_b,
+                              uint64_t* d_out, cudaStream_t s);
 cbs_status run_trace(cbs_context* c, const uint64_t* d_mv, uint32_t count, uint64_t* d_rgsw, cudaStream_t s);
 cbs_status run_lut_levels(cbs_context* c, const uint64_t* d_tables, uint64_t table_stride, const uint32_t* d_lut_sel,
                           const uint64_t* d_rgsw_all, uint64_t rgsw_stride, const uint32_t* d_ctrl, uint32_t luts,

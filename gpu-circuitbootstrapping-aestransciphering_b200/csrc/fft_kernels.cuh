@@ -22,10 +22,58 @@ struct FftKeyArgs {
     double inv_q;           // 1 / Q rounded
 };
 
+// Balanced gadget digits by the offset trick: (centred x + round_c) >> ign holds every digit
+// plus 2^(gbits-1) in its bit field k (see prepared_offset in cbs_fft.cu).
+struct DigitPrep {
+    uint64_t q, qhalf;
+    uint64_t round_c;  // 2^(ign-1) + (sum_k 2^(gbits k + gbits - 1)) << ign
+    int ign, gbits;
+};
+
+// HomTrace + SchemeSwitch on coefficient-domain MV RLWEs with FFT key switching.
+struct TraceFftArgs {
+    const uint64_t* mv;     // [count][2][N] coefficient domain (a, b)
+    double2* rgswf;         // [count][2 row types][2 polys][N/2] spectra, slot-major
+    uint32_t rounds;
+    uint32_t kinv[16];      // inverse mod 2N of the automorphism exponent N/2^r + 1 of round r
+    const double2* htf;     // [rounds][digits_ht][3][N/2] key spectra: k0_hi, k0_lo, k1
+    const double2* ssf;     // [digits_ss][3][N/2]
+    uint64_t split_pow, split_pow_s;  // 2^kTraceKeySplitBits mod Q and its Shoup quotient
+    DigitPrep g_ht, g_ss;
+    uint32_t digits_ht, digits_ss;
+};
+
+// One LUT-tree level of FFT CMuxes on coefficient-domain RLWEs.
+struct CmuxFftArgs {
+    const uint64_t* in;           // level input: [sets][in_count][2][N] coefficient domain
+    uint64_t in_lut_stride;       // words between input sets
+    const uint32_t* lut_sel;      // input set of each LUT (level 0: table id); null = the LUT index
+    uint64_t* out;                // [luts][in_count/2][2][N] coefficient domain
+    uint32_t in_count;
+    const double2* rgswf;         // [bits][digits][2][2][N/2] spectra (TraceFftArgs::rgswf)
+    uint64_t rgsw_stride;         // spectra entries per bit
+    const uint32_t* ctrl_bits;    // [luts][8] bit index of the control for each level
+    uint32_t level;
+    DigitPrep g;
+    uint32_t digits;
+};
+
+// mv_ntt: also transform the MV outputs to the NTT domain (the reference layout); false
+// leaves them in the coefficient domain for the FFT HomTrace
 cudaError_t launch_blind_rotate_fft(const BlindRotateArgs& a, const FftKeyArgs& f, const cbs_dmodulus* d_mod,
-                                    uint32_t N, uint32_t batch, cudaStream_t s);
+                                    uint32_t N, uint32_t batch, cudaStream_t s, bool mv_ntt = true);
+cudaError_t launch_trace_ss_fft(const TraceFftArgs& a, const FftKeyArgs& f, uint32_t N, uint32_t count, cudaStream_t s);
+cudaError_t launch_cmux_level_fft(const CmuxFftArgs& a, const FftKeyArgs& f, uint32_t N, uint32_t luts,
+                                  cudaStream_t s);
+// spectra [polys][N/2] (slot-major) -> coefficient-domain polynomials [polys][N] mod Q, in place
+cudaError_t launch_spectra_to_coef(double2* buf, uint64_t Q, const FftKeyArgs& f, uint32_t N, size_t polys,
+                                   cudaStream_t s);
+DigitPrep make_digit_prep(uint64_t q, const Gadget& g, uint32_t digits);
 // the FftTab<log2(N/2)> table (fft_core.cuh) computed in long double
 void fft_tables_host(uint32_t N, std::vector<double2>& tab);
-void keys_to_fft_host(const host::NttTables& t, const uint64_t* keys_ntt, size_t count, std::vector<double2>& out);
+void keys_to_fft_host(const host::NttTables& t, const uint64_t* keys_ntt, size_t count, std::vector<double2>& out,
+                      uint32_t split_bits = 0, uint32_t group = 0);
+// key-column split of the HomTrace / SchemeSwitch key spectra: [row][k0_hi, k0_lo, k1][N/2]
+constexpr uint32_t kTraceKeySplitBits = 27;
 
 }  // namespace cbs

@@ -1,0 +1,65 @@
+// fft_ops.cuh -- element operations shared by the FP64 FFT kernels: reduction of an
+// integer-valued double mod Q, balanced gadget digits by the offset trick, and the twist
+// factors of the folded negacyclic transform.
+#pragma once
+
+#include "fft_core.cuh"
+#include "fft_kernels.cuh"
+
+namespace cbs {
+
+// v mod Q, v the FP64 value of an integer-valued product (|v| < 2^90), computed in FP64:
+// k = rint(v / Q), r = v - k*q_hi - k*q_lo with two fused multiply-adds.  The two roundings of
+// r (|r| < 2Q < 2^55) add at most +-8 to the result, far below the FFT's own rounding error.
+__device__ __forceinline__ uint64_t double_to_mod(double v, const FftKeyArgs& f, uint64_t Q) {
+    const double k = rint(v * f.inv_q);
+    double r = fma(-k, f.q_hi, v);
+    r = fma(-k, f.q_lo, r);
+    int64_t i = __double2ll_rn(r);
+    if (i < 0) i += static_cast<int64_t>(Q);
+    if (i < 0) i += static_cast<int64_t>(Q);
+    if (i >= static_cast<int64_t>(Q)) i -= static_cast<int64_t>(Q);
+    return static_cast<uint64_t>(i);
+}
+
+// Balanced base-2^gbits digits of the prepared value v, all at once: adding
+// O = sum_k 2^(gbits-1) 2^(gbits k) makes every digit field non-negative, so digit k is field
+// k of v + O minus 2^(gbits-1).  This is the unique balanced representation of v modulo
+// 2^(gbits digits) with digits in [-2^(gbits-1), 2^(gbits-1)), i.e. what peel_digit yields
+// with the final carry dropped.
+__device__ __forceinline__ int32_t balanced_digit(int64_t w, int gbits, uint32_t k) {
+    const uint32_t field = static_cast<uint32_t>(static_cast<uint64_t>(w) >> (gbits * k)) & ((1u << gbits) - 1u);
+    return static_cast<int32_t>(field) - (1 << (gbits - 1));
+}
+
+// gadget_prepare(x) + offset for x in [0, Q): centre, round away the ign low bits, add the
+// digit offset.  The sum is non-negative because the offset times 2^ign is at least Q / 2.
+__device__ __forceinline__ int64_t prepared_offset(uint64_t x, uint64_t Q, uint64_t qhalf, uint64_t round_c, int ign) {
+    uint64_t t = x + round_c;
+    if (x >= qhalf) t -= Q;
+    return static_cast<int64_t>(t >> ign);
+}
+
+__device__ __forceinline__ uint32_t pack_digits(int32_t re, int32_t im) {
+    return (static_cast<uint32_t>(re) & 0xffffu) | (static_cast<uint32_t>(im) << 16);
+}
+
+// zeta^e from the half table: register slot j of the first/last pass holds e = tid + j*M/8,
+// so e < M/2 exactly for j < 4; above, zeta^e = i * conj(zeta^(M-e)) = swapped components.
+template <int LOGM>
+__device__ __forceinline__ double2 twist_at(const double2* tws, int j, uint32_t e) {
+    if (j < 4) return tws[e];
+    const double2 t = tws[(1u << LOGM) - e];
+    return make_double2(t.y, t.x);
+}
+
+__device__ __forceinline__ int64_t prepared_offset(uint64_t x, const DigitPrep& g) {
+    return prepared_offset(x, g.q, g.qhalf, g.round_c, g.ign);
+}
+
+// x in [0, Q) as the centred value, in FP64
+__device__ __forceinline__ double centred_double(uint64_t x, uint64_t Q, uint64_t qhalf) {
+    return static_cast<double>(x >= qhalf ? static_cast<int64_t>(x) - static_cast<int64_t>(Q) : static_cast<int64_t>(x));
+}
+
+}  // namespace cbs

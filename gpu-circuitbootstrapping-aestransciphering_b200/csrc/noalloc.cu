@@ -81,8 +81,7 @@ cbs_status cbs_circuit_bootstrap_batch_device_noalloc(cbs_context* ctx, const ui
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     // the blind rotation writes every scratch word it hands to the trace kernel, so stale
     // contents from an earlier call need no clearing
-    if (cbs_status st = run_blind_rotate(ctx, d_a, d_b, batch, a_stride, scratch, s)) return st;
-    return run_trace(ctx, scratch, batch * ctx->p.num_lut, d_rgsw_out, s);
+    return run_cbs(ctx, d_a, d_b, batch, a_stride, scratch, d_rgsw_out, s);
 }
 
 }  // extern "C"

@@ -23,6 +23,8 @@ torch = pytest.importorskip("torch")
 # the per-bit failure probability stays far below 2^-40.
 FFT_PHASE_TOL_LOG2 = 33.0
 RGSW_ROW_TOL = 2 ** 31
+TRACE_ROW_TOL = 2 ** 26
+SS_ROW_TOL = 2 ** 31
 
 
 def _dev(a):
@@ -96,7 +98,39 @@ def test_fft_cbs_rgsw_semantics(pkg, fctx, fkeys, foc):
             # 2^29.4 measured on B200 for these inputs; exact arithmetic gives <= 2^27.5), so
             # the bound is the FFT tolerance scaled to one coefficient, not g_0 / 2
             assert max(abs(int(x)) for x in ph1) < RGSW_ROW_TOL
-            assert max(abs(int(x)) for x in ph0) < g[0] * 2
+            # row 0 carries -s times the FFT HomTrace error (see SS_ROW_TOL)
+            assert max(abs(int(x)) for x in ph0) < SS_ROW_TOL
+
+
+# FFT HomTrace + SchemeSwitch against the exact trace on the same NTT-domain inputs.  The
+# mask column of every trace / scheme-switch key is split into 27-bit halves, so the mask part
+# of each key switch (products < 2^48) rounds to the exact integer; the body column keeps the
+# FP64 error of a 1024-point product of 9-bit digits by 54-bit keys, ~2^16.7 per coefficient
+# over 5 digits, which enters the phase unamplified.  Each later round doubles the variance,
+# so the trace row's phase error is ~2^22 rms; the scheme-switch row carries -s times it
+# (~2^27).  Bounds: 16x above those.
+def test_fft_trace_schemeswitch_phase_error(pkg, fctx, fkeys, foc):
+    p = fctx.params
+    rng = np.random.default_rng(4)
+    count = 3
+    mv = rng.integers(0, p.Q, size=(count, 2, p.N), dtype=np.uint64)
+    out = torch.zeros((count, 2, 2, p.N), dtype=torch.int64, device="cuda")
+    dmv = _dev(mv)
+    pkg.call("cbs_trace_schemeswitch_device", fctx.handle, dmv.data_ptr(), count, out.data_ptr(), None)
+    torch.cuda.synchronize()
+    got = out.cpu().numpy().view(np.uint64).reshape(count, 2, 2, p.N)
+    want = foc.trace_ss(mv).reshape(count, 2, 2, p.N)
+    Q = p.Q
+    worst = [0, 0]
+    for i in range(count):
+        for row in range(2):
+            d = foc.phase_coef(got[i, row]) - foc.phase_coef(want[i, row])
+            e = [((int(x) + Q // 2) % Q) - Q // 2 for x in d]
+            worst[row] = max(worst[row], max(abs(x) for x in e))
+    print(f"FFT trace: max |phase error| trace row 2^{np.log2(worst[1] + 1):.1f}, "
+          f"scheme-switch row 2^{np.log2(worst[0] + 1):.1f}")
+    assert worst[1] < TRACE_ROW_TOL
+    assert worst[0] < SS_ROW_TOL
 
 
 def test_fft_aes128_end_to_end(pkg, fctx, fkeys):
