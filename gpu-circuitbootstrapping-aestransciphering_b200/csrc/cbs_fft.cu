@@ -139,33 +139,25 @@ __global__ void __launch_bounds__(BrFftCfg<LOGN>::T, BrFftCfg<LOGN>::MIN_BLOCKS)
             }
         }
         __syncthreads();
-        uint64_t tre[8], tim[8];
+        // 4. (X^a - 1) t_h in the frequency domain: slot s times psi_s^a - 1, then the inverse
+        //    transform adds the rounded product into the accumulator positions this thread owns
+        //    (the same positions its digit extraction reads: no barrier needed)
+        {
+            const uint32_t mb = mult_base<LOGN>(ht, at);
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const double2 w = zeta_pow<LOGN>(tws, slot_exp<LOGN>(mb, at, j));
+                y0[j] = cmul(y0[j], make_double2(w.x - 1.0, w.y));
+            }
+        }
         fft_inverse_from_regs<LOGM>(
             my_fs, ht, tab, y0,
             [&](int j, uint32_t e, double2 v) {
                 const double2 u = cmulc(v, twist_at<LOGM>(tws, j, e));
-                tre[j] = double_to_mod(u.x * f.inv_m, f, Q);
-                tim[j] = double_to_mod(u.y * f.inv_m, f, Q);
+                my_acc[e] = add_mod(my_acc[e], double_to_mod(u.x * f.inv_m, f, Q), Q);
+                my_acc[e + M] = add_mod(my_acc[e + M], double_to_mod(u.y * f.inv_m, f, Q), Q);
             },
             half_bar);
-        // 4. rotate-add acc_h += (X^a - 1) t_h: t_h goes to this half's (now idle) FFT buffer,
-        //    then each thread updates the positions it owns: acc[i] += t[i - a] - t[i]
-        half_bar();
-        uint64_t* tsm = reinterpret_cast<uint64_t*>(my_fs);  // N words
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            tsm[ht + j * TH] = tre[j];
-            tsm[ht + j * TH + M] = tim[j];
-        }
-        half_bar();
-#pragma unroll 4
-        for (uint32_t k = 0; k < N / TH; ++k) {
-            const uint32_t i = ht + k * TH;
-            const uint32_t s = (i + TWO_N - at) & (TWO_N - 1);  // source index of X^a t in [0, 2N)
-            const uint64_t v = (s < N) ? tsm[s] : tsm[s - N];
-            const uint64_t r = (s < N) ? add_mod(my_acc[i], v, Q) : sub_mod(my_acc[i], v, Q);
-            my_acc[i] = sub_mod(r, tsm[i], Q);
-        }
     }
     __syncthreads();
 

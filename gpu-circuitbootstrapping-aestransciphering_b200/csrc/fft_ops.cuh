@@ -53,6 +53,37 @@ __device__ __forceinline__ double2 twist_at(const double2* tws, int j, uint32_t 
     return make_double2(t.y, t.x);
 }
 
+// zeta^m for zeta = exp(i pi / N), m in [0, 2N), from the half twist table (zeta^r for
+// r <= N/4): m = q N/2 + r gives zeta^m = i^q zeta^r, and for r > N/4,
+// zeta^r = i conj(zeta^(N/2 - r)) (the swapped components of entry N/2 - r).
+template <int LOGN>
+__device__ __forceinline__ double2 zeta_pow(const double2* tws, uint32_t m) {
+    constexpr uint32_t N = 1u << LOGN;
+    const uint32_t q = m >> (LOGN - 1), r = m & (N / 2 - 1);
+    const bool up = r > N / 4;
+    const double2 t = tws[up ? N / 2 - r : r];
+    const double c = up ? t.y : t.x, s = up ? t.x : t.y;
+    const double x = (q & 1) ? s : c, y = (q & 1) ? c : s;
+    return make_double2((q == 1 || q == 2) ? -x : x, (q >= 2) ? -y : y);
+}
+
+// Register slot j of thread t in a forward transform's output (M = N/2 points, M/8 threads,
+// slot s = 8t + j, bit-reversed order) holds the evaluation at psi_s = zeta^(4 rev(s) + 1).
+// rev(s) = rev3(j) M/8 + rev(t) over log2(M/8) bits, so psi_s^a = zeta^(a e_t + a rev3(j) N/4)
+// with e_t = 4 rev(t) + 1: mult_base() gives a e_t mod 2N once per step, slot_exp() the
+// exponent of slot j.
+template <int LOGN>
+__device__ __forceinline__ uint32_t mult_base(uint32_t t, uint32_t a) {
+    constexpr int TB = LOGN - 4;  // log2(M/8)
+    const uint32_t rt = __brev(t) >> (32 - TB);
+    return (a * (4 * rt + 1)) & ((2u << LOGN) - 1);
+}
+template <int LOGN>
+__device__ __forceinline__ uint32_t slot_exp(uint32_t base, uint32_t a, int j) {
+    const uint32_t r3 = ((j & 1) << 2) | (j & 2) | ((j >> 2) & 1);
+    return (base + ((a * r3) & 7u) * ((1u << LOGN) / 4)) & ((2u << LOGN) - 1);
+}
+
 __device__ __forceinline__ int64_t prepared_offset(uint64_t x, const DigitPrep& g) {
     return prepared_offset(x, g.q, g.qhalf, g.round_c, g.ign);
 }
