@@ -54,7 +54,7 @@ __global__ void __launch_bounds__(BrFftCfg<LOGN>::T, BrFftCfg<LOGN>::MIN_BLOCKS)
     const double2* tws = tab + Tb::twist_off();
     const uint32_t ct = blockIdx.x, tid = threadIdx.x;
     const uint32_t h = tid / TH, ht = tid % TH;
-    uint64_t* my_acc = acc + h * N;
+    int64_t* my_acc = reinterpret_cast<int64_t*>(acc) + h * N;
     double2* my_fs = fs + h * M;
     const uint64_t Q = a.t.q;
     const uint32_t digits = a.digits;
@@ -66,15 +66,23 @@ __global__ void __launch_bounds__(BrFftCfg<LOGN>::T, BrFftCfg<LOGN>::MIN_BLOCKS)
     // (x_centred + 2^(ign-1)) >> ign is the balanced rounding of gadget_prepare; adding the
     // digit offset before the shift folds both into one constant
     const uint64_t round_c = (ign ? (uint64_t(1) << (ign - 1)) : 0) + (static_cast<uint64_t>(offset) << ign);
+    // During the steps the accumulator holds y = centre(x) + round_c (an int64 in [lo_b, hi_b),
+    // centre(x) = x - Q for x >= Q/2 as in gadget_prepare), so the prepared digit word is y >> ign
+    // and an update adds a centred residue and corrects once by +-Q.
+    const int64_t hi_b = static_cast<int64_t>(round_c + qhalf), Qs = static_cast<int64_t>(Q), lo_b = hi_b - Qs;
+    auto to_offset = [&](uint64_t x) {
+        return static_cast<int64_t>(x + round_c) - (x >= qhalf ? Qs : 0);
+    };
 
     for (uint32_t i = tid; i < Tb::size(); i += T) tab[i] = f.tab[i];
     {
         const uint32_t bt = special_ms_f(a.b[ct], TWO_N, a.q_lwe, a.bitwidth);
+        int64_t* y = reinterpret_cast<int64_t*>(acc);
         for (uint32_t i = tid; i < N; i += T) {
-            acc[i] = 0;
+            y[i] = to_offset(0);
             const uint32_t s = (i + bt) & (TWO_N - 1);
             const uint64_t v = (s < N) ? a.tv[s] : a.tv[s - N];
-            acc[N + i] = (s < N) ? v : (v ? Q - v : 0);
+            y[N + i] = to_offset((s < N) ? v : (v ? Q - v : 0));
         }
     }
     __syncthreads();
@@ -85,6 +93,7 @@ __global__ void __launch_bounds__(BrFftCfg<LOGN>::T, BrFftCfg<LOGN>::MIN_BLOCKS)
         else asm volatile("bar.sync 2, %0;" ::"n"(TH) : "memory");
     };
     const uint32_t l2 = 2 * digits;
+    const int32_t dbias = 1 << (gbits - 1);
     const uint64_t* arow = a.a + static_cast<size_t>(ct) * a.a_stride;
     for (uint32_t step = 0; step < a.n; ++step) {
         const uint32_t at = special_ms_f(__ldg(arow + step), TWO_N, a.q_lwe, a.bitwidth);
@@ -92,12 +101,15 @@ __global__ void __launch_bounds__(BrFftCfg<LOGN>::T, BrFftCfg<LOGN>::MIN_BLOCKS)
         //    reads) exactly the positions ht + j*TH it owns, so no barrier is needed for dig;
         //    the barrier after this loop orders the previous step's reads of my_fs before
         //    the first transform writes it.
+        const uint32_t fmask = (1u << gbits) - 1u;
         for (uint32_t e = ht; e < M; e += TH) {
-            const int64_t wr = prepared_offset(my_acc[e], Q, qhalf, round_c, ign);
-            const int64_t wi = prepared_offset(my_acc[e + M], Q, qhalf, round_c, ign);
+            const uint64_t wr = static_cast<uint64_t>(my_acc[e]) >> ign;
+            const uint64_t wi = static_cast<uint64_t>(my_acc[e + M]) >> ign;
             uint32_t* dst = dig + h * digits * M + e;
+            // biased digit fields (digit + 2^(gbits-1)), re in the low half-word
             for (uint32_t d = 0; d < digits; ++d)
-                dst[d * M] = pack_digits(balanced_digit(wr, gbits, d), balanced_digit(wi, gbits, d));
+                dst[d * M] = (static_cast<uint32_t>(wr >> (gbits * d)) & fmask) |
+                             ((static_cast<uint32_t>(wi >> (gbits * d)) & fmask) << 16);
         }
         half_bar();
         // 2. forward transforms and products
@@ -112,8 +124,8 @@ __global__ void __launch_bounds__(BrFftCfg<LOGN>::T, BrFftCfg<LOGN>::MIN_BLOCKS)
                 my_fs, ht, tab,
                 [&](int j, uint32_t e) {
                     const uint32_t v = dsrc[e];
-                    const double re = static_cast<double>(static_cast<int16_t>(v & 0xffffu));
-                    const double im = static_cast<double>(static_cast<int16_t>(v >> 16));
+                    const double re = static_cast<double>(static_cast<int32_t>(v & 0xffffu) - dbias);
+                    const double im = static_cast<double>(static_cast<int32_t>(v >> 16) - dbias);
                     return cmul(make_double2(re, im), twist_at<LOGM>(tws, j, e));
                 },
                 x, half_bar);
@@ -154,8 +166,8 @@ __global__ void __launch_bounds__(BrFftCfg<LOGN>::T, BrFftCfg<LOGN>::MIN_BLOCKS)
             my_fs, ht, tab, y0,
             [&](int j, uint32_t e, double2 v) {
                 const double2 u = cmulc(v, twist_at<LOGM>(tws, j, e));
-                my_acc[e] = add_mod(my_acc[e], double_to_mod(u.x * f.inv_m, f, Q), Q);
-                my_acc[e + M] = add_mod(my_acc[e + M], double_to_mod(u.y * f.inv_m, f, Q), Q);
+                my_acc[e] = offset_add(my_acc[e], centred_residue(u.x * f.inv_m, f), lo_b, hi_b, Qs);
+                my_acc[e + M] = offset_add(my_acc[e + M], centred_residue(u.y * f.inv_m, f), lo_b, hi_b, Qs);
             },
             half_bar);
     }
@@ -164,8 +176,13 @@ __global__ void __launch_bounds__(BrFftCfg<LOGN>::T, BrFftCfg<LOGN>::MIN_BLOCKS)
     // finalize (cirbts-batch.cu:2622-2642) and the MV split ct_j = acc * X^-j in the
     // coefficient domain; the caller transforms mv_out to the NTT domain
     for (uint32_t i = tid; i < N; i += T) {
-        acc[i] = mul_shoup(acc[i], a.t.n_inv, a.t.n_inv_s, Q);
-        uint64_t v = mul_shoup(acc[N + i], a.t.n_inv, a.t.n_inv_s, Q);
+        // back from the offset form to [0, Q)
+        const int64_t* y = reinterpret_cast<const int64_t*>(acc);
+        const int64_t c0 = y[i] - static_cast<int64_t>(round_c), c1 = y[N + i] - static_cast<int64_t>(round_c);
+        const uint64_t x0 = static_cast<uint64_t>(c0 < 0 ? c0 + Qs : c0);
+        const uint64_t x1 = static_cast<uint64_t>(c1 < 0 ? c1 + Qs : c1);
+        acc[i] = mul_shoup(x0, a.t.n_inv, a.t.n_inv_s, Q);
+        uint64_t v = mul_shoup(x1, a.t.n_inv, a.t.n_inv_s, Q);
         if (i < a.num_lut) v = add_mod(v, a.gadd[i], Q);
         acc[N + i] = v;
     }

@@ -22,6 +22,23 @@ __device__ __forceinline__ uint64_t double_to_mod(double v, const FftKeyArgs& f,
     return static_cast<uint64_t>(i);
 }
 
+// v - rint(v / Q) Q as an int64, v the FP64 value of an integer-valued product (|v| < 2^90):
+// within Q/2 + 2^37 of zero (the quotient's rounding can be off by one near a half-integer).
+__device__ __forceinline__ int64_t centred_residue(double v, const FftKeyArgs& f) {
+    const double k = rint(v * f.inv_q);
+    double r = fma(-k, f.q_hi, v);
+    r = fma(-k, f.q_lo, r);
+    return __double2ll_rn(r);
+}
+
+// y + t brought back into the window [lo, lo + Q) = [lo, hi), for y in the window and |t| < Q/2
+// + 2^37 (so one correction by +-Q suffices)
+__device__ __forceinline__ int64_t offset_add(int64_t y, int64_t t, int64_t lo, int64_t hi, int64_t Q) {
+    int64_t s = y + t;
+    s = (s < lo) ? s + Q : s;
+    return (s >= hi) ? s - Q : s;
+}
+
 // Balanced base-2^gbits digits of the prepared value v, all at once: adding
 // O = sum_k 2^(gbits-1) 2^(gbits k) makes every digit field non-negative, so digit k is field
 // k of v + O minus 2^(gbits-1).  This is the unique balanced representation of v modulo
