@@ -5,6 +5,9 @@ counter blocks per GPU (default 128; the configuration also names 16 and 1024), 
 128 uniform bits from a seed, full 10-round homomorphic AES via circuit bootstrapping
 (blind rotation + HomTrace + SchemeSwitch), 16 CMux T-table LUTs per block-round and
 sample extract + key switch, every round a captured CUDA graph.  One step = one batch.
+The FP64-FFT backend runs the blind rotation over groups of 2 LWE coefficients by default
+(--multibit 2: the reference's CIRBTS_PBS_MULTIBIT=2 key grouping); --multibit 1 is the
+one-coefficient GINX loop.
 
 value: blocks/s with inputs resident in HBM, CUDA events on the launching stream, max over
 ranks.  e2e: the same metric through the host-buffer C-ABI entry point
@@ -133,6 +136,8 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     ctx = pkg.Context(max_batch=128 * min(blocks, 256))
     ctx.keygen(args.seed)
     pkg.call("cbs_context_set_br_backend", ctx.handle, pkg.BR_FFT64 if args.backend == "fft64" else pkg.BR_NTT)
+    if args.multibit > 1:
+        ctx.set_br_multibit(args.multibit)
     key = np.random.default_rng(args.seed).bytes(16)
     pkg.call("cbs_aes128_setup", ctx.handle, key, args.seed + 1)
     p = ctx.params
@@ -235,6 +240,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
         "config": {"workload": "aes128_ctr_transcipher", "blocks_per_gpu": blocks, "global_blocks": world * blocks,
                    "params": "N=2048 Q=54-bit n=630 q=2^14 BR 2^12x3 RGSW 2^6x4 HT 2^9x5 SS 2^9x5 KS 2^14/2^7",
                    "l2": "per-step working set (keys + RGSW + LUT buffers) >> 126 MB L2",
+                   "br_multibit": args.multibit,
                    "parallelism": f"replicas x{world} (independent blocks per GPU)"},
         "us_per_bootstrap": ms_per_step * 1e3 / (blocks * 128 * ROUNDS),
         "correct_blocks": ok,
@@ -247,7 +253,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
                      "frac": achieved_gbs / peaks["hbm_gbs"], "peak_src": peaks["src"], "traffic": None,
                      "algorithmic_bytes_per_launch": alg_bytes, "launch_ms": br_ms,
                      "note": "compute-bound (integer multiplies for ntt, FP64 pipe for fft64); see compute_rate"},
-        "compute_rate": compute_rate(args.backend, T, p, br_ms),
+        "compute_rate": compute_rate(args.backend, T, p, br_ms, args.multibit),
         "clocks": clk.summary(),
     }
     if rank == 0 and args.cpu_baseline:
@@ -281,6 +287,8 @@ def run_blind_rotate(args, rank: int, world: int, local_rank: int) -> None:
     ctx = pkg.Context(max_batch=T)
     ctx.keygen(args.seed)
     pkg.call("cbs_context_set_br_backend", ctx.handle, pkg.BR_FFT64 if args.backend == "fft64" else pkg.BR_NTT)
+    if args.multibit > 1:
+        ctx.set_br_multibit(args.multibit)
     p = ctx.params
     rng = np.random.default_rng(args.seed + rank)
     a = torch.from_numpy(rng.integers(0, p.q_lwe, size=(T, p.n), dtype=np.int64)).cuda()
@@ -299,13 +307,13 @@ def run_blind_rotate(args, rank: int, world: int, local_rank: int) -> None:
            "unit": "bootstraps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
            "dtype": "f64" if args.backend == "fft64" else "u64", "data": "synthetic (seeded random LWE)",
-           "config": {"workload": "blind_rotate", "batch": T, "backend": args.backend,
+           "config": {"workload": "blind_rotate", "batch": T, "backend": args.backend, "br_multibit": args.multibit,
                       "l2": "BSK read once per launch (124 MB fft64 / 124 MB ntt); no flush between launches"},
            "us_per_bootstrap": ms * 1e3 / T, "gpu_launches": args.steps,
            "roofline": {"kernel": "k_blind_rotate_fft" if args.backend == "fft64" else "k_blind_rotate",
                         "bound": "hbm", "achieved": gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                         "frac": gbs / peaks["hbm_gbs"], "peak_src": peaks["src"], "traffic": None},
-           "compute_rate": compute_rate(args.backend, T, p, ms), "clocks": clk.summary()}
+           "compute_rate": compute_rate(args.backend, T, p, ms, args.multibit), "clocks": clk.summary()}
     if rank == 0:
         print(json.dumps(out), flush=True)
     ctx.close()
@@ -691,14 +699,17 @@ def run_tcb(args, rank: int, world: int, local_rank: int) -> None:
     ctx.close()
 
 
-def compute_rate(backend: str, T: int, p, br_ms: float) -> dict:
-    """Algorithmic arithmetic of one blind-rotation launch over T ciphertexts."""
+def compute_rate(backend: str, T: int, p, br_ms: float, mb: int = 1) -> dict:
+    """Algorithmic arithmetic of one blind-rotation launch over T ciphertexts (mb > 1: groups
+    of mb coefficients, 2^mb - 1 combined keys per spectrum slot and row)."""
     N, n, l2 = p.N, p.n, 2 * p.digits_g
     logn = N.bit_length() - 1
     if backend == "fft64":
         M = N // 2
         fft_flop = 5 * M * (logn - 1)  # radix-2 complex FFT flop count
-        flop = T * n * ((l2 + 2) * fft_flop + 2 * l2 * M * 8)
+        steps = -(-n // mb)
+        keys = (1 << mb) - 1
+        flop = T * steps * ((l2 + 2) * fft_flop + 2 * l2 * M * 8 * (keys + (1 if mb > 1 else 0)))
         return {"kernel": "k_blind_rotate_fft", "fp64_flop_per_launch": flop,
                 "achieved_fp64_tflops": flop / (br_ms * 1e-3) / 1e12}
     modmuls = T * n * (8 * (N // 2) * logn + 2 * l2 * N)
@@ -786,6 +797,9 @@ def main() -> None:
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--backend", choices=["fft64", "ntt"], default="fft64")
+    ap.add_argument("--multibit", type=int, choices=[1, 2, 3], default=None,
+                    help="blind rotation over groups of 1, 2 or 3 LWE coefficients (fft64 backend; "
+                         "default 2 for fft64, 1 for ntt)")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--workload", choices=["aes128", "blind_rotate", "keyswitch", "rns_ntt", "gate", "ragged", "tcb"], default="aes128",
                     help="aes128 is the headline; the others time one kernel family")
@@ -794,6 +808,10 @@ def main() -> None:
     ap.add_argument("--ntt-logn", dest="ntt_logn", type=int, default=16, help="log2 N for --workload rns_ntt")
     ap.add_argument("--limbs", type=int, default=24, help="limbs per polynomial for --workload rns_ntt")
     args = ap.parse_args()
+    if args.multibit is None:
+        args.multibit = 2 if args.backend == "fft64" else 1
+    if args.multibit > 1 and args.backend != "fft64":
+        ap.error("--multibit > 1 needs --backend fft64")
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

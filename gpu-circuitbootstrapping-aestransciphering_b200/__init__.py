@@ -81,6 +81,9 @@ def _declare(lib: ctypes.CDLL) -> None:
         "cbs_context_stream": (st, [c_vp, c_vp]),
         "cbs_keygen": (st, [c_vp, u64]),
         "cbs_context_set_br_backend": (st, [c_vp, ctypes.c_int]),
+        "cbs_context_set_br_multibit": (st, [c_vp, u32]),
+        "cbs_export_mb_bsk": (st, [c_vp, c_vp, c_vp]),
+        "cbs_generate_mb_bsk_host": (st, [c_vp, u64, u32, c_vp, c_vp]),
         "cbs_export_keys": (st, [c_vp] + [c_vp] * 9),
         "cbs_generate_keys_host": (st, [c_vp, u64] + [c_vp] * 9),
         "cbs_context_tables": (st, [c_vp] + [c_vp] * 7),
@@ -165,6 +168,17 @@ def default_params() -> CbsParams:
     return p
 
 
+def generate_mb_bsk_host(params: CbsParams, seed: int, mb: int):
+    """Grouped blind-rotation keys [ceil(n/mb)][2^mb - 1][2*digits_g][2][N] (NTT domain) of the
+    key set cbs_keygen(seed) makes, generated on the host."""
+    import numpy as np
+    words = ctypes.c_size_t()
+    call("cbs_generate_mb_bsk_host", ctypes.byref(params), seed, mb, None, ctypes.byref(words))
+    out = np.zeros(words.value, np.uint64)
+    call("cbs_generate_mb_bsk_host", ctypes.byref(params), seed, mb, out.ctypes.data, ctypes.byref(words))
+    return out
+
+
 class Context:
     """Owning handle of a cbs_context (the GPUCirBTSContext counterpart)."""
 
@@ -196,6 +210,22 @@ class Context:
         """Host copies (numpy) of secrets and key material in the reference layouts."""
         out = key_buffers(self.params)
         call("cbs_export_keys", self._h, *(out[k].ctypes.data for k in KEY_FIELDS))
+        return out
+
+    def set_br_backend(self, backend: int) -> None:
+        call("cbs_context_set_br_backend", self._h, backend)
+
+    def set_br_multibit(self, mb: int) -> None:
+        """Blind rotation over groups of mb = 1, 2 or 3 LWE coefficients (FFT backend)."""
+        call("cbs_context_set_br_multibit", self._h, mb)
+
+    def export_mb_bsk(self):
+        """Grouped blind-rotation keys [ceil(n/mb)][2^mb - 1][2*digits_g][2][N] (NTT domain)."""
+        import numpy as np
+        words = ctypes.c_size_t()
+        call("cbs_export_mb_bsk", self._h, None, ctypes.byref(words))
+        out = np.zeros(words.value, np.uint64)
+        call("cbs_export_mb_bsk", self._h, out.ctypes.data, ctypes.byref(words))
         return out
 
 

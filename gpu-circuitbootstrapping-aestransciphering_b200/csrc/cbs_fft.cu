@@ -199,6 +199,211 @@ __global__ void __launch_bounds__(BrFftCfg<LOGN>::T, BrFftCfg<LOGN>::MIN_BLOCKS)
     }
 }
 
+// Multi-bit blind rotation (the reference's CIRBTS_PBS_MULTIBIT = MB path: key grouping
+// bitwise/src/cirbts/cirbts-init.cu:376-530, MB3 MAC kernel.cu:4585-4771) with FFT products.
+// For binary s_i, prod_{i in G} (1 + (X^{a_i} - 1) s_i) = X^{sum a_i s_i}, so one step per
+// group G of MB coefficients adds sum_S m_S (acc (x) K_S), K_S = RGSW(prod_{i in S} s_i),
+// m_S = prod_{i in S} c_i, c_i = X^{a_i} - 1.  The external product is linear in the key,
+// so per spectrum slot the combined key sum_S m_S(psi) K_S is formed in registers (Horner in
+// the c_i: 2^MB - 1 complex multiply-adds) and multiplied once against the digit spectrum:
+// the digit split, the 6 forward and 2 inverse transforms run once per group instead of
+// once per coefficient, and the rotation needs no separate pass.  c_i(psi_s) comes from one
+// twist-table lookup per group (zeta^(a_i e_t)) times an 8th root of unity per slot.
+// Keys: [groups][2^MB - 1][2*digits][2][N/2] spectra, subsets in the order {0} {1} {2}
+// {0,1} {0,2} {1,2} {0,1,2} (MB = 3) or {0} {1} {0,1} (MB = 2).
+template <int MB>
+__device__ __forceinline__ double2 mb_combined_key(const double2* kp, size_t kstride, const double2 (&c)[MB]) {
+    if constexpr (MB == 2) {
+        // c0 (K0 + c1 K01) + c1 K1
+        double2 t = __ldg(kp);
+        cfma(t, c[1], __ldg(kp + 2 * kstride));
+        double2 r = cmul(c[0], t);
+        cfma(r, c[1], __ldg(kp + kstride));
+        return r;
+    } else {
+        // c0 (K0 + c1 (K01 + c2 K012) + c2 K02) + c1 (K1 + c2 K12) + c2 K2
+        double2 t = __ldg(kp + 3 * kstride);
+        cfma(t, c[2], __ldg(kp + 6 * kstride));
+        double2 t2 = __ldg(kp);
+        cfma(t2, c[1], t);
+        cfma(t2, c[2], __ldg(kp + 4 * kstride));
+        double2 u = __ldg(kp + kstride);
+        cfma(u, c[2], __ldg(kp + 5 * kstride));
+        double2 r = cmul(c[0], t2);
+        cfma(r, c[1], u);
+        cfma(r, c[2], __ldg(kp + 2 * kstride));
+        return r;
+    }
+}
+
+// Residency: the combined-key products keep many key loads in flight.  For MB = 2 one CTA per
+// SM with the whole register file (no spills) is faster than two spilling CTAs (35.9 vs 40.5 us
+// per bootstrap at N = 2048, n = 630); MB = 3 needs the warps of two CTAs to cover its seven
+// key streams (58 vs 97 us).
+template <int LOGN, int MB>
+struct BrFftMbCfg {
+    static constexpr int MIN_BLOCKS = MB == 2 ? 1 : BrFftCfg<LOGN>::MIN_BLOCKS;
+};
+
+template <int LOGN, int MB>
+__global__ void __launch_bounds__(BrFftCfg<LOGN>::T, BrFftMbCfg<LOGN, MB>::MIN_BLOCKS)
+    k_blind_rotate_fft_mb(const BlindRotateArgs a, const FftKeyArgs f) {
+    constexpr int LOGM = LOGN - 1;
+    constexpr uint32_t N = 1u << LOGN, M = N / 2, TH = M / 8, T = 2 * TH, TWO_N = 2 * N;
+    constexpr uint32_t KS = (1u << MB) - 1u;
+    using Tb = FftTab<LOGM>;
+    extern __shared__ __align__(16) uint64_t smem[];
+    uint64_t* acc = smem;                                           // [2][N]
+    double2* fs = reinterpret_cast<double2*>(smem + 2 * N);         // [2][M]
+    double2* tab = fs + 2 * M;                                      // FftTab<LOGM>
+    uint32_t* dig = reinterpret_cast<uint32_t*>(tab + Tb::size());  // [2][digits][M] packed pairs
+    const double2* tws = tab + Tb::twist_off();
+    const uint32_t ct = blockIdx.x, tid = threadIdx.x;
+    const uint32_t h = tid / TH, ht = tid % TH;
+    int64_t* my_acc = reinterpret_cast<int64_t*>(acc) + h * N;
+    double2* my_fs = fs + h * M;
+    const uint64_t Q = a.t.q;
+    const uint32_t digits = a.digits;
+    const int gbits = a.g.gbits;
+    int64_t offset = 0;
+    for (uint32_t k = 0; k < digits; ++k) offset += static_cast<int64_t>(1) << (gbits * k + gbits - 1);
+    const int ign = a.g.ign;
+    const uint64_t qhalf = Q >> 1;
+    const uint64_t round_c = (ign ? (uint64_t(1) << (ign - 1)) : 0) + (static_cast<uint64_t>(offset) << ign);
+    const int64_t hi_b = static_cast<int64_t>(round_c + qhalf), Qs = static_cast<int64_t>(Q), lo_b = hi_b - Qs;
+    auto to_offset = [&](uint64_t x) {
+        return static_cast<int64_t>(x + round_c) - (x >= qhalf ? Qs : 0);
+    };
+
+    for (uint32_t i = tid; i < Tb::size(); i += T) tab[i] = f.tab[i];
+    {
+        const uint32_t bt = special_ms_f(a.b[ct], TWO_N, a.q_lwe, a.bitwidth);
+        int64_t* y = reinterpret_cast<int64_t*>(acc);
+        for (uint32_t i = tid; i < N; i += T) {
+            y[i] = to_offset(0);
+            const uint32_t s = (i + bt) & (TWO_N - 1);
+            const uint64_t v = (s < N) ? a.tv[s] : a.tv[s - N];
+            y[N + i] = to_offset((s < N) ? v : (v ? Q - v : 0));
+        }
+    }
+    __syncthreads();
+
+    auto half_bar = [h]() {
+        if (h == 0) asm volatile("bar.sync 1, %0;" ::"n"(TH) : "memory");
+        else asm volatile("bar.sync 2, %0;" ::"n"(TH) : "memory");
+    };
+    const uint32_t l2 = 2 * digits;
+    const int32_t dbias = 1 << (gbits - 1);
+    const uint64_t* arow = a.a + static_cast<size_t>(ct) * a.a_stride;
+    const uint32_t groups = (a.n + MB - 1) / MB;
+    const size_t kstride = static_cast<size_t>(l2) * 2 * M;  // spectra between subsets of a group
+    for (uint32_t g = 0; g < groups; ++g) {
+        // zeta^(a_i e_t) per coefficient of the group (a_i = 0 past n: c_i = 0)
+        uint32_t at[MB];
+        double2 ub[MB];
+#pragma unroll
+        for (int i = 0; i < MB; ++i) {
+            const uint32_t idx = g * MB + i;
+            at[i] = idx < a.n ? special_ms_f(__ldg(arow + idx), TWO_N, a.q_lwe, a.bitwidth) : 0u;
+            ub[i] = zeta_pow<LOGN>(tws, mult_base<LOGN>(ht, at[i]));
+        }
+        // 1. digits of this half's polynomial (thread-private positions, as in the one-bit form)
+        const uint32_t fmask = (1u << gbits) - 1u;
+        for (uint32_t e = ht; e < M; e += TH) {
+            const uint64_t wr = static_cast<uint64_t>(my_acc[e]) >> ign;
+            const uint64_t wi = static_cast<uint64_t>(my_acc[e + M]) >> ign;
+            uint32_t* dst = dig + h * digits * M + e;
+            for (uint32_t d = 0; d < digits; ++d)
+                dst[d * M] = (static_cast<uint32_t>(wr >> (gbits * d)) & fmask) |
+                             ((static_cast<uint32_t>(wi >> (gbits * d)) & fmask) << 16);
+        }
+        half_bar();
+        // 2. forward transforms; per slot the combined key of row 2d + h, both columns
+        const double2* gk = f.bskf + static_cast<size_t>(g) * KS * kstride + ht;
+        double2 y0[8], y1[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) y0[j] = y1[j] = make_double2(0.0, 0.0);
+        for (uint32_t d = 0; d < digits; ++d) {
+            const uint32_t* dsrc = dig + (h * digits + d) * M;
+            double2 x[8];
+            fft_forward_to_regs<LOGM>(
+                my_fs, ht, tab,
+                [&](int j, uint32_t e) {
+                    const uint32_t v = dsrc[e];
+                    const double re = static_cast<double>(static_cast<int32_t>(v & 0xffffu) - dbias);
+                    const double im = static_cast<double>(static_cast<int32_t>(v >> 16) - dbias);
+                    return cmul(make_double2(re, im), twist_at<LOGM>(tws, j, e));
+                },
+                x, half_bar);
+            const double2* k0 = gk + static_cast<size_t>(2 * d + h) * 2 * M;
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                // c_i(psi_s) = zeta^(a_i e_t) omega8^((a_i rev3(j)) mod 8) - 1; omega8^k is
+                // +-tw[(k mod 4) M/8] of the first-pass table
+                const uint32_t r3 = ((j & 1) << 2) | (j & 2) | ((j >> 2) & 1);
+                double2 c[MB];
+#pragma unroll
+                for (int i = 0; i < MB; ++i) {
+                    const uint32_t k = (at[i] * r3) & 7u;
+                    double2 w = tab[(k & 3u) * (M / 8)];
+                    if (k & 4u) w = make_double2(-w.x, -w.y);
+                    const double2 v = cmul(ub[i], w);
+                    c[i] = make_double2(v.x - 1.0, v.y);
+                }
+                cfma(y0[j], x[j], mb_combined_key<MB>(k0 + j * TH, kstride, c));
+                cfma(y1[j], x[j], mb_combined_key<MB>(k0 + M + j * TH, kstride, c));
+            }
+            half_bar();  // the last pass's reads of my_fs are done before it is written again
+        }
+        // 3. swap partial sums: half 0 keeps output 0, half 1 keeps output 1
+#pragma unroll
+        for (int j = 0; j < 8; ++j) my_fs[cswz(8 * ht + j)] = h ? y0[j] : y1[j];
+        __syncthreads();
+        {
+            const double2* take = fs + (1 - h) * M;
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const double2 t = take[cswz(8 * ht + j)];
+                y0[j] = cadd(h ? y1[j] : y0[j], t);
+            }
+        }
+        __syncthreads();
+        // 4. inverse transform, rounding, accumulate (the monomials are already in the keys)
+        fft_inverse_from_regs<LOGM>(
+            my_fs, ht, tab, y0,
+            [&](int j, uint32_t e, double2 v) {
+                const double2 u = cmulc(v, twist_at<LOGM>(tws, j, e));
+                my_acc[e] = offset_add(my_acc[e], centred_residue(u.x * f.inv_m, f), lo_b, hi_b, Qs);
+                my_acc[e + M] = offset_add(my_acc[e + M], centred_residue(u.y * f.inv_m, f), lo_b, hi_b, Qs);
+            },
+            half_bar);
+    }
+    __syncthreads();
+
+    // finalize (cirbts-batch.cu:2622-2642) and the MV split, as in the one-bit form
+    for (uint32_t i = tid; i < N; i += T) {
+        const int64_t* y = reinterpret_cast<const int64_t*>(acc);
+        const int64_t c0 = y[i] - static_cast<int64_t>(round_c), c1 = y[N + i] - static_cast<int64_t>(round_c);
+        const uint64_t x0 = static_cast<uint64_t>(c0 < 0 ? c0 + Qs : c0);
+        const uint64_t x1 = static_cast<uint64_t>(c1 < 0 ? c1 + Qs : c1);
+        acc[i] = mul_shoup(x0, a.t.n_inv, a.t.n_inv_s, Q);
+        uint64_t v = mul_shoup(x1, a.t.n_inv, a.t.n_inv_s, Q);
+        if (i < a.num_lut) v = add_mod(v, a.gadd[i], Q);
+        acc[N + i] = v;
+    }
+    __syncthreads();
+    for (uint32_t j = 0; j < a.num_lut; ++j) {
+        for (uint32_t p = 0; p < 2; ++p) {
+            const uint64_t* src = acc + p * N;
+            uint64_t* dst = a.mv_out + ((static_cast<size_t>(ct) * a.num_lut + j) * 2 + p) * N;
+            for (uint32_t i = tid; i < N; i += T) {
+                const uint32_t s = i + j;
+                dst[i] = (s < N) ? src[s] : (src[s - N] ? Q - src[s - N] : 0);
+            }
+        }
+    }
+}
+
 cudaError_t ntt_forward(uint64_t* out, const uint64_t* in, const uint64_t* tw, const uint64_t* tws,
                         const cbs_dmodulus* mod, size_t dim, size_t batch, cudaStream_t s);
 
@@ -229,6 +434,40 @@ cudaError_t launch_blind_rotate_fft(const BlindRotateArgs& a, const FftKeyArgs& 
         case 1024: e = br_fft_launch<10>(a, f, batch, s); break;
         case 2048: e = br_fft_launch<11>(a, f, batch, s); break;
         case 4096: e = br_fft_launch<12>(a, f, batch, s); break;
+        default: return cudaErrorInvalidValue;
+    }
+    if (e != cudaSuccess || !mv_ntt) return e;
+    return ntt_forward(a.mv_out, a.mv_out, a.t.rp, a.t.rps, d_mod, N, static_cast<size_t>(batch) * a.num_lut * 2, s);
+}
+
+template <int LOGN, int MB>
+static cudaError_t br_fft_mb_launch(const BlindRotateArgs& a, const FftKeyArgs& f, uint32_t batch, cudaStream_t s) {
+    constexpr uint32_t N = 1u << LOGN, M = N / 2;
+    const size_t smem = 2ull * N * sizeof(uint64_t) + (2ull * M + FftTab<LOGN - 1>::size()) * sizeof(double2) +
+                        2ull * a.digits * M * sizeof(uint32_t);
+    if (f.tab_len != FftTab<LOGN - 1>::size()) return cudaErrorInvalidValue;
+    static size_t configured[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (configured[dev] < smem) {
+        cudaError_t e = cudaFuncSetAttribute(k_blind_rotate_fft_mb<LOGN, MB>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+        if (e != cudaSuccess) return e;
+        configured[dev] = smem;
+    }
+    k_blind_rotate_fft_mb<LOGN, MB><<<batch, BrFftCfg<LOGN>::T, smem, s>>>(a, f);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_blind_rotate_fft_mb(const BlindRotateArgs& a, const FftKeyArgs& f, const cbs_dmodulus* d_mod,
+                                       uint32_t N, uint32_t batch, uint32_t mb, cudaStream_t s, bool mv_ntt) {
+    if (batch == 0) return cudaSuccess;
+    if (mb != 2 && mb != 3) return cudaErrorInvalidValue;
+    cudaError_t e;
+    switch (N) {
+        case 1024: e = mb == 2 ? br_fft_mb_launch<10, 2>(a, f, batch, s) : br_fft_mb_launch<10, 3>(a, f, batch, s); break;
+        case 2048: e = mb == 2 ? br_fft_mb_launch<11, 2>(a, f, batch, s) : br_fft_mb_launch<11, 3>(a, f, batch, s); break;
+        case 4096: e = mb == 2 ? br_fft_mb_launch<12, 2>(a, f, batch, s) : br_fft_mb_launch<12, 3>(a, f, batch, s); break;
         default: return cudaErrorInvalidValue;
     }
     if (e != cudaSuccess || !mv_ntt) return e;

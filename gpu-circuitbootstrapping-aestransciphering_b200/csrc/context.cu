@@ -74,6 +74,31 @@ FftKeyArgs fft_key_args(const cbs_context* c) {
     return f;
 }
 
+// the grouped keys' generator seed is the key seed xor this constant (context and host agree)
+static constexpr uint64_t kMbSeedTweak = 0x6d756c7469626974ull;
+
+// grouped multi-bit keys (generated from the context's secrets, seeded from the key seed)
+// and their spectra
+static cbs_status prepare_mb(cbs_context* c) {
+    if (c->br_mb <= 1 || c->mb_ready) return CBS_OK;
+    if (!c->keys_ready) {
+        set_error("multi-bit blind rotation: no key material (call cbs_keygen first)");
+        return CBS_ERR_NOT_READY;
+    }
+    std::vector<double2> spec;
+    try {
+        generate_mb_bsk(c->p, c->tab, c->hk, c->br_mb, c->key_seed ^ kMbSeedTweak, c->h_mbk);
+        keys_to_fft_host(c->tab, c->h_mbk.data(), c->h_mbk.size() / c->p.N, spec);
+    } catch (const std::exception& e) {
+        set_error(std::string("multi-bit keys: ") + e.what());
+        return CBS_ERR_OOM;
+    }
+    CBS_CUDA_TRY(c->d_bskf_mb.upload(spec.data(), spec.size(), c->stream));
+    CBS_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    c->mb_ready = true;
+    return CBS_OK;
+}
+
 cbs_status run_blind_rotate(cbs_context* c, const uint64_t* d_a, const uint64_t* d_b, uint32_t batch,
                             uint32_t a_stride, uint64_t* d_mv, cudaStream_t s, bool mv_ntt) {
     BlindRotateArgs a{};
@@ -99,6 +124,16 @@ cbs_status run_blind_rotate(cbs_context* c, const uint64_t* d_a, const uint64_t*
         if (!c->fft_ready) {
             set_error("FFT backend selected but its key material is not prepared");
             return CBS_ERR_NOT_READY;
+        }
+        if (c->br_mb > 1) {
+            if (!c->mb_ready) {
+                set_error("multi-bit blind rotation selected but its keys are not prepared");
+                return CBS_ERR_NOT_READY;
+            }
+            FftKeyArgs f = fft_key_args(c);
+            f.bskf = c->d_bskf_mb.p;
+            CBS_CUDA_TRY(launch_blind_rotate_fft_mb(a, f, c->d_mod.p, c->p.N, batch, c->br_mb, s, mv_ntt));
+            return CBS_OK;
         }
         CBS_CUDA_TRY(launch_blind_rotate_fft(a, fft_key_args(c), c->d_mod.p, c->p.N, batch, s, mv_ntt));
         return CBS_OK;
@@ -398,7 +433,48 @@ cbs_status cbs_keygen(cbs_context* ctx, uint64_t seed) {
     c->keys_ready = true;
     c->aes.ready = false;
     c->fft_ready = false;
-    if (c->br_backend == CBS_BR_FFT64) return prepare_fft(c);
+    c->mb_ready = false;
+    c->key_seed = seed;
+    if (c->br_backend == CBS_BR_FFT64) {
+        if (cbs_status st = prepare_fft(c)) return st;
+        return prepare_mb(c);
+    }
+    return CBS_OK;
+}
+
+cbs_status cbs_context_set_br_multibit(cbs_context* ctx, uint32_t mb) {
+    CBS_CHECK_ARG(ctx, "set_br_multibit: null context");
+    CBS_CHECK_ARG(mb >= 1 && mb <= 3, "set_br_multibit: mb must be 1, 2 or 3");
+    if (mb > 1 && ctx->br_backend != CBS_BR_FFT64) {
+        set_error("set_br_multibit: grouped blind rotation is implemented for the FFT64 backend");
+        return CBS_ERR_UNSUPPORTED;
+    }
+    if (mb != ctx->br_mb) {
+        ctx->br_mb = mb;
+        ctx->mb_ready = false;
+        ctx->h_mbk.clear();
+        ctx->d_bskf_mb.reset();
+    }
+    if (mb > 1 && ctx->keys_ready) {
+        if (cbs_status st = prepare_mb(ctx)) return st;
+    }
+    for (auto& g : ctx->aes.graphs)
+        if (g) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+    ctx->aes.graph_chunk = 0;
+    return CBS_OK;
+}
+
+cbs_status cbs_export_mb_bsk(const cbs_context* ctx, uint64_t* out, size_t* words) {
+    CBS_CHECK_ARG(ctx && words, "export_mb_bsk: null argument");
+    if (ctx->br_mb <= 1 || !ctx->mb_ready) {
+        set_error("export_mb_bsk: no grouped keys (select mb > 1 after cbs_keygen)");
+        return CBS_ERR_NOT_READY;
+    }
+    *words = ctx->h_mbk.size();
+    if (out) std::memcpy(out, ctx->h_mbk.data(), ctx->h_mbk.size() * sizeof(uint64_t));
     return CBS_OK;
 }
 
@@ -413,6 +489,12 @@ cbs_status cbs_context_set_br_backend(cbs_context* ctx, int backend) {
         if (cbs_status st = prepare_fft(ctx)) return st;
     }
     ctx->br_backend = backend;
+    if (backend != CBS_BR_FFT64 && ctx->br_mb > 1) {  // grouped keys exist for the FFT form only
+        ctx->br_mb = 1;
+        ctx->mb_ready = false;
+        ctx->h_mbk.clear();
+        ctx->d_bskf_mb.reset();
+    }
     // captured AES round graphs bake in the kernel choice
     for (auto& g : ctx->aes.graphs)
         if (g) {
@@ -420,6 +502,33 @@ cbs_status cbs_context_set_br_backend(cbs_context* ctx, int backend) {
             g = nullptr;
         }
     ctx->aes.graph_chunk = 0;
+    return CBS_OK;
+}
+
+cbs_status cbs_generate_mb_bsk_host(const cbs_params* params, uint64_t seed, uint32_t mb, uint64_t* out,
+                                    size_t* words) {
+    CBS_CHECK_ARG(params && words, "generate_mb_bsk_host: null argument");
+    CBS_CHECK_ARG(mb == 2 || mb == 3, "generate_mb_bsk_host: mb must be 2 or 3");
+    if (cbs_status st = validate(*params)) return st;
+    const size_t need = static_cast<size_t>((params->n + mb - 1) / mb) * mb_subsets(mb) * 2 * params->digits_g * 2 *
+                        params->N;
+    *words = need;
+    if (!out) return CBS_OK;
+    host::NttTables t;
+    if (!host::make_ntt_tables(params->N, params->Q, t)) {
+        set_error("generate_mb_bsk_host: NTT tables failed");
+        return CBS_ERR_INVALID_ARG;
+    }
+    try {
+        HostKeys k;
+        generate_keys(*params, t, seed, k);
+        std::vector<uint64_t> mbk;
+        generate_mb_bsk(*params, t, k, mb, seed ^ kMbSeedTweak, mbk);
+        std::memcpy(out, mbk.data(), mbk.size() * sizeof(uint64_t));
+    } catch (const std::exception& e) {
+        set_error(std::string("generate_mb_bsk_host: ") + e.what());
+        return CBS_ERR_OOM;
+    }
     return CBS_OK;
 }
 

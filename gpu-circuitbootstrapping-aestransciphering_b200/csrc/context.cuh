@@ -66,6 +66,12 @@ struct cbs_context {
     bool fft_ready = false;
     cbs::DevBuf<double2> d_bskf, d_fft_tab;
     cbs::DevBuf<double2> d_htf, d_ssf;  // HomTrace / SchemeSwitch key spectra
+    // multi-bit blind rotation (FFT backend): 1 = one coefficient per step, 2 or 3 = grouped
+    uint32_t br_mb = 1;
+    bool mb_ready = false;
+    uint64_t key_seed = 0;
+    std::vector<uint64_t> h_mbk;         // grouped keys, NTT domain (kept for export)
+    cbs::DevBuf<double2> d_bskf_mb;      // their spectra
     cbs::DevBuf<uint64_t> d_pow2, d_pow2s;
     // scratch
     cbs::DevBuf<uint64_t> d_mv, d_rgsw;

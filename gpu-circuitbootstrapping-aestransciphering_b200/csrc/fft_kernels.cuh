@@ -62,6 +62,10 @@ struct CmuxFftArgs {
 // leaves them in the coefficient domain for the FFT HomTrace
 cudaError_t launch_blind_rotate_fft(const BlindRotateArgs& a, const FftKeyArgs& f, const cbs_dmodulus* d_mod,
                                     uint32_t N, uint32_t batch, cudaStream_t s, bool mv_ntt = true);
+// multi-bit form: groups of mb = 2 or 3 coefficients, f.bskf the grouped key spectra
+// [ceil(n/mb)][2^mb - 1][2*digits][2][N/2]
+cudaError_t launch_blind_rotate_fft_mb(const BlindRotateArgs& a, const FftKeyArgs& f, const cbs_dmodulus* d_mod,
+                                       uint32_t N, uint32_t batch, uint32_t mb, cudaStream_t s, bool mv_ntt = true);
 cudaError_t launch_trace_ss_fft(const TraceFftArgs& a, const FftKeyArgs& f, uint32_t N, uint32_t count, cudaStream_t s);
 cudaError_t launch_cmux_level_fft(const CmuxFftArgs& a, const FftKeyArgs& f, uint32_t N, uint32_t luts,
                                   cudaStream_t s);

@@ -1,9 +1,11 @@
 // keygen.cpp -- see keygen.h.
 #include "keygen.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <stdexcept>
+#include <thread>
 
 namespace cbs {
 
@@ -140,6 +142,60 @@ void rlwe_encrypt(const cbs_params& p, const host::NttTables& t, const HostKeys&
     std::vector<uint64_t> m(msg_coef);
     ntt_fwd_fast(m.data(), t);
     for (uint32_t i = 0; i < p.N; ++i) out_b[i] = fm.add(out_b[i], m[i]);
+}
+
+uint32_t mb_subsets(uint32_t mb) { return (1u << mb) - 1u; }
+
+uint32_t mb_subset_mask(uint32_t mb, uint32_t idx) {
+    // subsets of {0..mb-1} ordered by size, then lexicographically: for mb = 3,
+    // {0} {1} {2} {0,1} {0,2} {1,2} {0,1,2} (the reference's k0 k1 k2 k01 k02 k12 k012,
+    // cirbts-init.cu:499-530); for mb = 2, {0} {1} {0,1} (k0 k1 k01, :485-498)
+    static const uint32_t order2[3] = {0b01, 0b10, 0b11};
+    static const uint32_t order3[7] = {0b001, 0b010, 0b100, 0b011, 0b101, 0b110, 0b111};
+    if (mb == 1) return 1u;
+    if (mb == 2) return order2[idx];
+    return order3[idx];
+}
+
+void generate_mb_bsk(const cbs_params& p, const host::NttTables& t, const HostKeys& k, uint32_t mb, uint64_t seed,
+                     std::vector<uint64_t>& out) {
+    const uint32_t N = p.N, n = p.n, l2 = 2 * p.digits_g, K = mb_subsets(mb);
+    const uint32_t groups = (n + mb - 1) / mb;
+    const uint64_t Q = p.Q;
+    FastMod fm(Q);
+    const auto gbr = gadget_of(Q, p.base_g, p.digits_g);
+    out.assign(static_cast<size_t>(groups) * K * l2 * 2 * N, 0);
+    const unsigned nth = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    std::vector<std::thread> pool;
+    for (unsigned th = 0; th < nth; ++th) {
+        pool.emplace_back([&, th] {
+            std::vector<uint64_t> tmp;
+            for (uint32_t g = th; g < groups; g += nth) {
+                // one generator per group, so the keys do not depend on the thread count
+                Rng rng(seed ^ (0x9e3779b97f4a7c15ull * (g + 1)));
+                for (uint32_t kk = 0; kk < K; ++kk) {
+                    const uint32_t mask = mb_subset_mask(mb, kk);
+                    uint32_t prod = 1;  // the product of the subset's secret bits (0 past n)
+                    for (uint32_t i = 0; i < mb; ++i)
+                        if (mask & (1u << i)) {
+                            const uint32_t idx = g * mb + i;
+                            prod &= (idx < n) ? static_cast<uint32_t>(k.s_lwe[idx]) : 0u;
+                        }
+                    for (uint32_t r = 0; r < l2; ++r) {
+                        uint64_t* a = out.data() + ((static_cast<size_t>(g) * K + kk) * l2 + r) * 2 * N;
+                        uint64_t* b = a + N;
+                        rlwe_zero(p, t, k, fm, rng, a, b, tmp);
+                        if (prod) {
+                            const uint64_t m = gbr[r >> 1];
+                            uint64_t* tgt = (r & 1) ? b : a;
+                            for (uint32_t c = 0; c < N; ++c) tgt[c] = fm.add(tgt[c], m);
+                        }
+                    }
+                }
+            }
+        });
+    }
+    for (auto& th : pool) th.join();
 }
 
 void lwe_encrypt(const cbs_params& p, const HostKeys& k, Rng& rng, uint64_t m, uint64_t* out_a, uint64_t* out_b) {

@@ -142,6 +142,24 @@ cbs_status cbs_keygen(cbs_context *ctx, uint64_t seed);
 enum { CBS_BR_NTT = 0, CBS_BR_FFT64 = 1 };
 cbs_status cbs_context_set_br_backend(cbs_context *ctx, int backend);
 
+/* Multi-bit blind rotation (the reference's CIRBTS_PBS_MULTIBIT grouping,
+ * bitwise/src/cirbts/cirbts-init.cu:376-530 and the MB3 MAC kernel.cu:4585-4771): mb = 1
+ * processes one LWE coefficient per step (default); mb = 2 or 3 groups mb coefficients and
+ * adds sum_S prod_{i in S}(X^{a_i} - 1) * (acc (x) RGSW(prod_{i in S} s_i)) over the
+ * non-empty subsets S, so the accumulator is decomposed and transformed once per group.  The
+ * grouped keys are generated from the context's secrets (2^mb - 1 RGSWs per group) when keys
+ * exist or are next generated.  mb > 1 needs the FFT64 backend (CBS_ERR_UNSUPPORTED
+ * otherwise); selecting the NTT backend resets mb to 1. */
+cbs_status cbs_context_set_br_multibit(cbs_context *ctx, uint32_t mb);
+/* The grouped keys of the current setting, NTT domain, for inspection and tests:
+ * out [ceil(n/mb)][2^mb - 1][2*digits_g][2][N] (null out: only *words is set), subsets in
+ * the order {0} {1} {2} {0,1} {0,2} {1,2} {0,1,2} (mb = 3) or {0} {1} {0,1} (mb = 2). */
+cbs_status cbs_export_mb_bsk(const cbs_context *ctx, uint64_t *out, size_t *words);
+/* Host-only generation of the grouped keys a context keyed with the same seed produces
+ * (for CPU-side checks without a GPU); null out: only *words is set. */
+cbs_status cbs_generate_mb_bsk_host(const cbs_params *params, uint64_t seed, uint32_t mb, uint64_t *out,
+                                    size_t *words);
+
 /* Export for verification (host buffers, NTT-domain normal form, reference layouts):
  * any pointer may be NULL.  s_lwe[n], s_rlwe[N]; bsk[n][2*digits_g][2][N];
  * ht[rounds][digits_ht][2][N]; ss[digits_ss][2][N]; ksk[2][N][base_ks][n+1];

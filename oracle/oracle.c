@@ -378,6 +378,104 @@ void orc_blind_rotate(const orc_cbs_params *p, const orc_cbs_keys *k, const uint
     }
 }
 
+/* Multi-bit blind rotation (the reference's CIRBTS_PBS_MULTIBIT = 2 / 3 path: key grouping
+ * cirbts-init.cu:376-530, MB3 MAC kernel.cu:4585-4771).  For binary s_i,
+ * prod_{i in G} (1 + (X^{a_i} - 1) s_i) = X^{sum a_i s_i}, so one step per group G of mb
+ * coefficients adds sum_S m_S (acc (x) RGSW(prod_{i in S} s_i)) with m_S = prod_{i in S}
+ * (X^{a_i} - 1) over the non-empty subsets S, in the order {0} {1} {2} {0,1} {0,2} {1,2}
+ * {0,1,2} (mb = 3) or {0} {1} {0,1} (mb = 2).  Coefficients past n rotate by 0, so their
+ * subsets vanish.  mbk [groups][2^mb - 1][2*digits_g][2][N] NTT domain. */
+static const uint32_t orc_mb_order2[3] = {1u, 2u, 3u};
+static const uint32_t orc_mb_order3[7] = {1u, 2u, 4u, 3u, 5u, 6u, 7u};
+
+static void blind_rotate_mb_one(const orc_cbs_params *p, const orc_cbs_keys *k, const uint64_t *mbk, uint32_t mb,
+                                const uint64_t *a, uint64_t b, uint64_t *acc, int finalize, uint64_t *work) {
+    const uint32_t N = p->N, l2 = 2 * p->digits_g, K = (1u << mb) - 1u;
+    const uint32_t groups = (p->n + mb - 1) / mb;
+    const uint64_t Q = p->Q;
+    const uint32_t twoN = 2 * N;
+    const uint32_t bw = (p->num_lut <= 1) ? 0 : (uint32_t)(32 - __builtin_clz(p->num_lut - 1));
+    const uint32_t *order = (mb == 2) ? orc_mb_order2 : orc_mb_order3;
+    uint64_t *ct = work;                /* [2][N] */
+    uint64_t *dct = ct + 2 * N;         /* [l2][N] */
+    uint64_t *mono = dct + (size_t)l2 * N; /* [mb][N] */
+    uint64_t *msub = mono + (size_t)mb * N; /* [K][N] */
+    uint64_t dig[64];
+
+    const uint32_t bt = orc_special_ms(b, twoN, p->q_lwe, bw);
+    memset(acc, 0, sizeof(uint64_t) * N);
+    rotate_neg(acc + N, k->tv, bt, N, Q);
+    ntt_fwd_one(acc + N, N, Q, k->rp);
+
+    for (uint32_t g = 0; g < groups; ++g) {
+        memcpy(ct, acc, sizeof(uint64_t) * 2 * N);
+        ntt_inv_one(ct, N, Q, k->irp, k->n_inv);
+        ntt_inv_one(ct + N, N, Q, k->irp, k->n_inv);
+        for (uint32_t poly = 0; poly < 2; ++poly)
+            for (uint32_t c = 0; c < N; ++c) {
+                orc_signed_decompose(ct[poly * N + c], Q, p->base_g, p->digits_g, dig);
+                for (uint32_t j = 0; j < p->digits_g; ++j) dct[(size_t)(2 * j + poly) * N + c] = dig[j];
+            }
+        for (uint32_t d = 0; d < l2; ++d) ntt_fwd_one(dct + (size_t)d * N, N, Q, k->rp);
+        for (uint32_t i = 0; i < mb; ++i) {
+            const uint32_t idx = g * mb + i;
+            const uint32_t at = idx < p->n ? orc_special_ms(a[idx], twoN, p->q_lwe, bw) : 0u;
+            monic_ntt(mono + (size_t)i * N, at, N, Q, k->rp);
+        }
+        for (uint32_t kk = 0; kk < K; ++kk) {
+            uint64_t *m = msub + (size_t)kk * N;
+            for (uint32_t c = 0; c < N; ++c) m[c] = 1;
+            for (uint32_t i = 0; i < mb; ++i)
+                if (order[kk] & (1u << i))
+                    for (uint32_t c = 0; c < N; ++c) m[c] = orc_mulmod(m[c], mono[(size_t)i * N + c], Q);
+        }
+        const uint64_t *gk = mbk + (size_t)g * K * l2 * 2 * N;
+        for (uint32_t c = 0; c < N; ++c) {
+            uint64_t u0 = 0, u1 = 0;
+            for (uint32_t kk = 0; kk < K; ++kk) {
+                const uint64_t *ek = gk + (size_t)kk * l2 * 2 * N;
+                uint64_t t0 = 0, t1 = 0;
+                for (uint32_t d = 0; d < l2; ++d) {
+                    const uint64_t x = dct[(size_t)d * N + c];
+                    t0 = addmod(t0, orc_mulmod(x, ek[(size_t)d * 2 * N + c], Q), Q);
+                    t1 = addmod(t1, orc_mulmod(x, ek[(size_t)d * 2 * N + N + c], Q), Q);
+                }
+                u0 = addmod(u0, orc_mulmod(t0, msub[(size_t)kk * N + c], Q), Q);
+                u1 = addmod(u1, orc_mulmod(t1, msub[(size_t)kk * N + c], Q), Q);
+            }
+            acc[c] = addmod(acc[c], u0, Q);
+            acc[N + c] = addmod(acc[N + c], u1, Q);
+        }
+    }
+
+    if (finalize) {
+        const uint64_t ninv = orc_invmod(N, Q);
+        for (uint32_t c = 0; c < 2 * N; ++c) acc[c] = orc_mulmod(acc[c], ninv, Q);
+        ntt_inv_one(acc, N, Q, k->irp, k->n_inv);
+        ntt_inv_one(acc + N, N, Q, k->irp, k->n_inv);
+        for (uint32_t j = 0; j < p->num_lut; ++j)
+            acc[N + j] = addmod(acc[N + j], orc_mulmod(k->gpow[j] >> 1, ninv, Q), Q);
+        ntt_fwd_one(acc, N, Q, k->rp);
+        ntt_fwd_one(acc + N, N, Q, k->rp);
+    }
+}
+
+void orc_blind_rotate_mb(const orc_cbs_params *p, const orc_cbs_keys *k, const uint64_t *mbk, uint32_t mb,
+                         const uint64_t *a, const uint64_t *b, uint32_t batch, uint32_t a_stride, uint64_t *acc_out,
+                         int finalize) {
+    const uint32_t K = (1u << mb) - 1u;
+    const size_t wsz = (size_t)(2 + 2 * p->digits_g + mb + K) * p->N;
+#pragma omp parallel
+    {
+        uint64_t *work = (uint64_t *)malloc(wsz * sizeof(uint64_t));
+#pragma omp for schedule(dynamic, 1)
+        for (long bi = 0; bi < (long)batch; ++bi)
+            blind_rotate_mb_one(p, k, mbk, mb, a + (size_t)bi * a_stride, b[bi], acc_out + (size_t)bi * 2 * p->N,
+                                finalize, work);
+        free(work);
+    }
+}
+
 /* one HomTrace + SchemeSwitch pipeline for a single MV RLWE (cirbts-batch.cu:1656-1789,
  * kernel.cu:7832-7888 HT update, kernel.cu:8407-8446 SS update, kernel.cu:7776-7789 layout) */
 static void trace_ss_one(const orc_cbs_params *p, const orc_cbs_keys *k, const uint64_t *ct_in, uint64_t *rgsw,

@@ -92,6 +92,12 @@ typedef struct {
  * acc_out [batch][2][N] NTT domain. */
 void orc_blind_rotate(const orc_cbs_params *p, const orc_cbs_keys *k, const uint64_t *a, const uint64_t *b,
                       uint32_t batch, uint32_t a_stride, uint64_t *acc_out, int finalize);
+/* Multi-bit blind rotation, mb = 2 or 3 (cirbts-init.cu:376-530 key grouping, kernel.cu:4585-4771):
+ * mbk [ceil(n/mb)][2^mb - 1][2*digits_g][2][N] NTT domain, subsets ordered {0} {1} {2} {0,1}
+ * {0,2} {1,2} {0,1,2} (mb = 3) or {0} {1} {0,1} (mb = 2). */
+void orc_blind_rotate_mb(const orc_cbs_params *p, const orc_cbs_keys *k, const uint64_t *mbk, uint32_t mb,
+                         const uint64_t *a, const uint64_t *b, uint32_t batch, uint32_t a_stride, uint64_t *acc_out,
+                         int finalize);
 /* BR + finalize + multi-value split (kernel.cu:7498-7536): mv [batch][num_lut][2][N] NTT domain */
 void orc_blind_rotate_mv(const orc_cbs_params *p, const orc_cbs_keys *k, const uint64_t *a, const uint64_t *b,
                          uint32_t batch, uint32_t a_stride, uint64_t *mv);

@@ -28,6 +28,7 @@ def declare_cbs(oracle) -> None:
     u32 = ctypes.c_uint32
     oracle.orc_blind_rotate.argtypes = [vp, vp, vp, vp, u32, u32, vp, ctypes.c_int]
     oracle.orc_blind_rotate_mv.argtypes = [vp, vp, vp, vp, u32, u32, vp]
+    oracle.orc_blind_rotate_mb.argtypes = [vp, vp, vp, u32, vp, vp, u32, u32, vp, ctypes.c_int]
     oracle.orc_circuit_bootstrap.argtypes = [vp, vp, vp, vp, u32, u32, vp]
     oracle.orc_trace_schemeswitch.argtypes = [vp, vp, vp, u32, vp]
     oracle.orc_external_product.argtypes = [vp, vp, vp, u32, ctypes.c_uint64, vp, vp, ctypes.c_uint64, u32, u32]
@@ -50,6 +51,23 @@ class OracleCbs:
                           auto_maps=keys["maps"].ctypes.data, tv=keys["tv"].ctypes.data,
                           gpow=keys["gpow"].ctypes.data, bsk=keys["bsk"].ctypes.data, ht_key=keys["ht"].ctypes.data,
                           ss_key=keys["ss"].ctypes.data)
+
+    def br_acc(self, a: np.ndarray, b: np.ndarray) -> np.ndarray:
+        """Finalized one-bit blind rotation [batch][2][N] (NTT domain)."""
+        batch, stride = a.shape
+        out = np.zeros((batch, 2, self.p.N), np.uint64)
+        self.o.orc_blind_rotate(ctypes.byref(self.op), ctypes.byref(self.ok), a.ctypes.data, b.ctypes.data, batch,
+                                stride, out.ctypes.data, 1)
+        return out
+
+    def br_acc_mb(self, a: np.ndarray, b: np.ndarray, mbk: np.ndarray, mb: int) -> np.ndarray:
+        """Finalized multi-bit blind rotation with grouped keys mbk [batch][2][N] (NTT domain)."""
+        batch, stride = a.shape
+        out = np.zeros((batch, 2, self.p.N), np.uint64)
+        mbk = np.ascontiguousarray(mbk, np.uint64)
+        self.o.orc_blind_rotate_mb(ctypes.byref(self.op), ctypes.byref(self.ok), mbk.ctypes.data, mb, a.ctypes.data,
+                                   b.ctypes.data, batch, stride, out.ctypes.data, 1)
+        return out
 
     def br_mv(self, a: np.ndarray, b: np.ndarray) -> np.ndarray:
         batch, stride = a.shape

@@ -76,6 +76,70 @@ def test_fft_blind_rotate_phase_error_bound(pkg, fctx, fkeys, foc):
     assert log2 < FFT_PHASE_TOL_LOG2
 
 
+@pytest.mark.parametrize("mb", [2, 3])
+def test_fft_multibit_blind_rotate_phase_error(pkg, fctx, fkeys, foc, mb):
+    """Grouped (multi-bit) FFT blind rotation against the oracle's exact grouped rotation with
+    the same keys: the FP64 error of the combined-key products, same tolerance as above."""
+    p = fctx.params
+    fctx.set_br_multibit(mb)
+    try:
+        mbk = fctx.export_mb_bsk()
+        rng = np.random.default_rng(80 + mb)
+        bits = [1, 0, 1]
+        a, b = lwe_encrypt_bits(rng, fkeys["s_lwe"], bits, p.q_lwe)
+        da, db = _dev(a), _dev(b)
+        mv = torch.zeros((len(bits), p.num_lut, 2, p.N), dtype=torch.int64, device="cuda")
+        pkg.call("cbs_blind_rotate_batch_device", fctx.handle, da.data_ptr(), db.data_ptr(), len(bits), p.n,
+                 mv.data_ptr(), None)
+        torch.cuda.synchronize()
+    finally:
+        fctx.set_br_multibit(1)
+    got = mv.cpu().numpy().view(np.uint64).reshape(len(bits), p.num_lut, 2, p.N)
+    want = foc.br_acc_mb(a, b, mbk, mb)
+    Q, N = p.Q, p.N
+    worst = 0
+    for i in range(len(bits)):
+        d = foc.phase_coef(got[i, 0]) - foc.phase_coef(want[i])
+        e = [((int(x) * N + Q // 2) % Q) - Q // 2 for x in d]
+        worst = max(worst, max(abs(x) for x in e))
+    log2 = np.log2(worst + 1)
+    print(f"FFT64 multi-bit (mb={mb}) blind rotation: max |phase error| = 2^{log2:.1f}")
+    assert log2 < FFT_PHASE_TOL_LOG2
+
+
+def test_fft_multibit_aes128_end_to_end(pkg, fctx, fkeys):
+    from cryptography.hazmat.primitives.ciphers import Cipher, algorithms, modes
+    p = fctx.params
+    key = bytes(range(48, 64))
+    fctx.set_br_multibit(3)
+    try:
+        pkg.call("cbs_aes128_setup", fctx.handle, key, 6)
+        blocks = 2
+        rng = np.random.default_rng(10)
+        ctrs = [rng.bytes(16) for _ in range(blocks)]
+        h = np.frombuffer(b"".join(ctrs), np.uint8).copy()
+        oa = np.zeros((blocks * 128, p.n), np.uint64)
+        ob = np.zeros(blocks * 128, np.uint64)
+        pkg.call("cbs_aes128_ctr_transcipher", fctx.handle, h.ctypes.data, blocks, oa.ctypes.data, ob.ctypes.data)
+    finally:
+        fctx.set_br_multibit(1)
+    got_bits, err = lwe_decrypt_bits(fkeys["s_lwe"], oa, ob, p.q_lwe)
+    enc = Cipher(algorithms.AES(key), modes.ECB()).encryptor()
+    for blk in range(blocks):
+        out = bytes(int(sum(int(got_bits[blk * 128 + i * 8 + b]) << b for b in range(8))) for i in range(16))
+        assert out == enc.update(ctrs[blk])
+    assert max(err) < p.q_lwe // 8
+
+
+def test_multibit_needs_fft_backend(pkg):
+    c = pkg.Context(max_batch=4)
+    try:
+        assert pkg.load().cbs_context_set_br_multibit(c.handle, 3) == 6  # CBS_ERR_UNSUPPORTED on the NTT backend
+        assert pkg.load().cbs_context_set_br_multibit(c.handle, 4) == 1
+    finally:
+        c.close()
+
+
 def test_fft_cbs_rgsw_semantics(pkg, fctx, fkeys, foc):
     p = fctx.params
     rng = np.random.default_rng(78)
