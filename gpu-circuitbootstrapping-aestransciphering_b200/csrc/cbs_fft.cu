@@ -242,7 +242,7 @@ __device__ __forceinline__ double2 mb_combined_key(const double2* kp, size_t kst
 // key streams (58 vs 97 us).
 template <int LOGN, int MB>
 struct BrFftMbCfg {
-    static constexpr int MIN_BLOCKS = MB == 2 ? 1 : BrFftCfg<LOGN>::MIN_BLOCKS;
+    static constexpr int MIN_BLOCKS = 1;
 };
 
 template <int LOGN, int MB>
@@ -257,6 +257,7 @@ __global__ void __launch_bounds__(BrFftCfg<LOGN>::T, BrFftMbCfg<LOGN, MB>::MIN_B
     double2* fs = reinterpret_cast<double2*>(smem + 2 * N);         // [2][M]
     double2* tab = fs + 2 * M;                                      // FftTab<LOGM>
     uint32_t* dig = reinterpret_cast<uint32_t*>(tab + Tb::size());  // [2][digits][M] packed pairs
+    double2* cbuf = reinterpret_cast<double2*>(dig + 2 * a.digits * M);  // [MB][8][T] c_i per slot
     const double2* tws = tab + Tb::twist_off();
     const uint32_t ct = blockIdx.x, tid = threadIdx.x;
     const uint32_t h = tid / TH, ht = tid % TH;
@@ -299,13 +300,23 @@ __global__ void __launch_bounds__(BrFftCfg<LOGN>::T, BrFftMbCfg<LOGN, MB>::MIN_B
     const size_t kstride = static_cast<size_t>(l2) * 2 * M;  // spectra between subsets of a group
     for (uint32_t g = 0; g < groups; ++g) {
         // zeta^(a_i e_t) per coefficient of the group (a_i = 0 past n: c_i = 0)
-        uint32_t at[MB];
-        double2 ub[MB];
+        // c_i(psi_s) = zeta^(a_i e_t) omega8^((a_i rev3(j)) mod 8) - 1 for the thread's 8 slots,
+        // kept in shared memory for the group (thread-private entries: no barrier); omega8^k is
+        // +-tw[(k mod 4) M/8] of the first-pass table
 #pragma unroll
         for (int i = 0; i < MB; ++i) {
             const uint32_t idx = g * MB + i;
-            at[i] = idx < a.n ? special_ms_f(__ldg(arow + idx), TWO_N, a.q_lwe, a.bitwidth) : 0u;
-            ub[i] = zeta_pow<LOGN>(tws, mult_base<LOGN>(ht, at[i]));
+            const uint32_t at = idx < a.n ? special_ms_f(__ldg(arow + idx), TWO_N, a.q_lwe, a.bitwidth) : 0u;
+            const double2 ub = zeta_pow<LOGN>(tws, mult_base<LOGN>(ht, at));
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const uint32_t r3 = ((j & 1) << 2) | (j & 2) | ((j >> 2) & 1);
+                const uint32_t k = (at * r3) & 7u;
+                double2 w = tab[(k & 3u) * (M / 8)];
+                if (k & 4u) w = make_double2(-w.x, -w.y);
+                const double2 v = cmul(ub, w);
+                cbuf[(i * 8 + j) * T + tid] = make_double2(v.x - 1.0, v.y);
+            }
         }
         // 1. digits of this half's polynomial (thread-private positions, as in the one-bit form)
         const uint32_t fmask = (1u << gbits) - 1u;
@@ -335,23 +346,44 @@ __global__ void __launch_bounds__(BrFftCfg<LOGN>::T, BrFftMbCfg<LOGN, MB>::MIN_B
                     return cmul(make_double2(re, im), twist_at<LOGM>(tws, j, e));
                 },
                 x, half_bar);
+            // combined keys of row 2d + h, both columns, all 8 slots: subset by subset, the 16
+            // key spectra of one subset are loaded together (16 independent loads in flight)
             const double2* k0 = gk + static_cast<size_t>(2 * d + h) * 2 * M;
+            double2 kc0[8], kc1[8];
+#pragma unroll
+            for (int s = 0; s < static_cast<int>(KS); ++s) {
+                double2 ka[8], kb[8];
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    ka[j] = __ldg(k0 + s * kstride + j * TH);
+                    kb[j] = __ldg(k0 + s * kstride + M + j * TH);
+                }
+                const uint32_t mask = MB == 2 ? (s == 0 ? 1u : (s == 1 ? 2u : 3u))
+                                              : (s < 3 ? (1u << s) : (s == 3 ? 3u : (s == 4 ? 5u : (s == 5 ? 6u : 7u))));
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    double2 m = make_double2(1.0, 0.0);
+                    bool first = true;
+#pragma unroll
+                    for (int i = 0; i < MB; ++i)
+                        if (mask & (1u << i)) {
+                            const double2 c = cbuf[(i * 8 + j) * T + tid];
+                            m = first ? c : cmul(m, c);
+                            first = false;
+                        }
+                    if (s == 0) {
+                        kc0[j] = cmul(m, ka[j]);
+                        kc1[j] = cmul(m, kb[j]);
+                    } else {
+                        cfma(kc0[j], m, ka[j]);
+                        cfma(kc1[j], m, kb[j]);
+                    }
+                }
+            }
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
-                // c_i(psi_s) = zeta^(a_i e_t) omega8^((a_i rev3(j)) mod 8) - 1; omega8^k is
-                // +-tw[(k mod 4) M/8] of the first-pass table
-                const uint32_t r3 = ((j & 1) << 2) | (j & 2) | ((j >> 2) & 1);
-                double2 c[MB];
-#pragma unroll
-                for (int i = 0; i < MB; ++i) {
-                    const uint32_t k = (at[i] * r3) & 7u;
-                    double2 w = tab[(k & 3u) * (M / 8)];
-                    if (k & 4u) w = make_double2(-w.x, -w.y);
-                    const double2 v = cmul(ub[i], w);
-                    c[i] = make_double2(v.x - 1.0, v.y);
-                }
-                cfma(y0[j], x[j], mb_combined_key<MB>(k0 + j * TH, kstride, c));
-                cfma(y1[j], x[j], mb_combined_key<MB>(k0 + M + j * TH, kstride, c));
+                cfma(y0[j], x[j], kc0[j]);
+                cfma(y1[j], x[j], kc1[j]);
             }
             half_bar();  // the last pass's reads of my_fs are done before it is written again
         }
@@ -444,7 +476,7 @@ template <int LOGN, int MB>
 static cudaError_t br_fft_mb_launch(const BlindRotateArgs& a, const FftKeyArgs& f, uint32_t batch, cudaStream_t s) {
     constexpr uint32_t N = 1u << LOGN, M = N / 2;
     const size_t smem = 2ull * N * sizeof(uint64_t) + (2ull * M + FftTab<LOGN - 1>::size()) * sizeof(double2) +
-                        2ull * a.digits * M * sizeof(uint32_t);
+                        2ull * a.digits * M * sizeof(uint32_t) + MB * 8ull * BrFftCfg<LOGN>::T * sizeof(double2);
     if (f.tab_len != FftTab<LOGN - 1>::size()) return cudaErrorInvalidValue;
     static size_t configured[64] = {};
     int dev = 0;
@@ -462,12 +494,11 @@ static cudaError_t br_fft_mb_launch(const BlindRotateArgs& a, const FftKeyArgs& 
 cudaError_t launch_blind_rotate_fft_mb(const BlindRotateArgs& a, const FftKeyArgs& f, const cbs_dmodulus* d_mod,
                                        uint32_t N, uint32_t batch, uint32_t mb, cudaStream_t s, bool mv_ntt) {
     if (batch == 0) return cudaSuccess;
-    if (mb != 2 && mb != 3) return cudaErrorInvalidValue;
+    if (mb != 2 && mb != 3) return cudaErrorInvalidValue;  // N = 4096: the per-slot c_i exceed shared memory
     cudaError_t e;
     switch (N) {
         case 1024: e = mb == 2 ? br_fft_mb_launch<10, 2>(a, f, batch, s) : br_fft_mb_launch<10, 3>(a, f, batch, s); break;
         case 2048: e = mb == 2 ? br_fft_mb_launch<11, 2>(a, f, batch, s) : br_fft_mb_launch<11, 3>(a, f, batch, s); break;
-        case 4096: e = mb == 2 ? br_fft_mb_launch<12, 2>(a, f, batch, s) : br_fft_mb_launch<12, 3>(a, f, batch, s); break;
         default: return cudaErrorInvalidValue;
     }
     if (e != cudaSuccess || !mv_ntt) return e;
