@@ -199,7 +199,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     torch.cuda.synchronize()
     br_ms = e0.elapsed_time(e1) / reps
     N, n, l2, L = p.N, p.n, 2 * p.digits_g, p.num_lut
-    alg_bytes = n * l2 * 2 * N * 8 + T * ((n + 1) * 8 + L * 2 * N * 8)  # key once + LWE in + MV out
+    alg_bytes = br_key_bytes(p, args.multibit) + T * ((n + 1) * 8 + L * 2 * N * 8)  # key once + LWE in + MV out
     peaks = measured_peaks()
     achieved_gbs = alg_bytes / (br_ms * 1e-3) / 1e9
 
@@ -222,7 +222,9 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     e2e_ok = verify(pkg, ctx, key, ctrs, out_ha, out_hb)
 
     chunks = -(-blocks // 256)
-    launches_per_step = chunks * (1 + ROUNDS * 13)
+    # per round: blind rotation, HomTrace+SchemeSwitch, 8 CMux levels, word assembly and
+    # extraction (+ one inverse NTT of the words on the NTT backend); + state init per chunk
+    launches_per_step = chunks * (1 + ROUNDS * (12 if args.backend == "fft64" else 13))
     result = {
         "metric": METRICS[args.backend],
         "value": world * blocks / (ms_per_step * 1e-3),
@@ -247,7 +249,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
         "gpu_launches": launches_per_step * args.steps,
         "e2e": {"value": world * blocks / float(te.item()), "unit": UNIT, "h2d_bytes_per_step": blocks * 128,
                 "d2h_bytes_per_step": blocks * 128 * (p.n + 1) * 8, "correct_blocks": e2e_ok},
-        "roofline": {"kernel": ("k_blind_rotate_fft" if args.backend == "fft64" else "k_blind_rotate")
+        "roofline": {"kernel": br_kernel_name(args)
                      + " (fused GINX blind rotation + finalize + MV split)", "bound": "hbm",
                      "achieved": achieved_gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                      "frac": achieved_gbs / peaks["hbm_gbs"], "peak_src": peaks["src"], "traffic": None,
@@ -300,7 +302,7 @@ def run_blind_rotate(args, rank: int, world: int, local_rank: int) -> None:
     with ClockSampler(local_rank) as clk:
         ms = _timed(torch, stream, fn, args.warmup, args.steps)
     N, n, l2, L = p.N, p.n, 2 * p.digits_g, p.num_lut
-    alg_bytes = n * l2 * 2 * N * 8 + T * ((n + 1) * 8 + L * 2 * N * 8)
+    alg_bytes = br_key_bytes(p, args.multibit) + T * ((n + 1) * 8 + L * 2 * N * 8)
     peaks = measured_peaks()
     gbs = alg_bytes / (ms * 1e-3) / 1e9
     out = {"metric": f"blind rotations/s ({args.backend}, N={N}, n={n})", "value": world * T / (ms * 1e-3),
@@ -310,7 +312,7 @@ def run_blind_rotate(args, rank: int, world: int, local_rank: int) -> None:
            "config": {"workload": "blind_rotate", "batch": T, "backend": args.backend, "br_multibit": args.multibit,
                       "l2": "BSK read once per launch (124 MB fft64 / 124 MB ntt); no flush between launches"},
            "us_per_bootstrap": ms * 1e3 / T, "gpu_launches": args.steps,
-           "roofline": {"kernel": "k_blind_rotate_fft" if args.backend == "fft64" else "k_blind_rotate",
+           "roofline": {"kernel": br_kernel_name(args),
                         "bound": "hbm", "achieved": gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                         "frac": gbs / peaks["hbm_gbs"], "peak_src": peaks["src"], "traffic": None},
            "compute_rate": compute_rate(args.backend, T, p, ms, args.multibit), "clocks": clk.summary()}
@@ -699,6 +701,20 @@ def run_tcb(args, rank: int, world: int, local_rank: int) -> None:
     ctx.close()
 
 
+def br_key_bytes(p, mb: int) -> int:
+    """Blind-rotation key bytes one launch reads (once, shared through L2): n RGSWs, or
+    ceil(n/mb) groups of 2^mb - 1 RGSWs; FFT spectra and NTT words are both 8 bytes per
+    coefficient."""
+    rgsw = 2 * p.digits_g * 2 * p.N * 8
+    return (-(-p.n // mb)) * ((1 << mb) - 1) * rgsw
+
+
+def br_kernel_name(args) -> str:
+    if args.backend != "fft64":
+        return "k_blind_rotate"
+    return "k_blind_rotate_fft" if args.multibit == 1 else f"k_blind_rotate_fft_mb<11,{args.multibit}>"
+
+
 def compute_rate(backend: str, T: int, p, br_ms: float, mb: int = 1) -> dict:
     """Algorithmic arithmetic of one blind-rotation launch over T ciphertexts (mb > 1: groups
     of mb coefficients, 2^mb - 1 combined keys per spectrum slot and row)."""
@@ -710,7 +726,8 @@ def compute_rate(backend: str, T: int, p, br_ms: float, mb: int = 1) -> dict:
         steps = -(-n // mb)
         keys = (1 << mb) - 1
         flop = T * steps * ((l2 + 2) * fft_flop + 2 * l2 * M * 8 * (keys + (1 if mb > 1 else 0)))
-        return {"kernel": "k_blind_rotate_fft", "fp64_flop_per_launch": flop,
+        return {"kernel": "k_blind_rotate_fft" if mb == 1 else f"k_blind_rotate_fft_mb (mb={mb})",
+                "fp64_flop_per_launch": flop,
                 "achieved_fp64_tflops": flop / (br_ms * 1e-3) / 1e12}
     modmuls = T * n * (8 * (N // 2) * logn + 2 * l2 * N)
     return {"kernel": "k_blind_rotate", "modmul_per_launch": modmuls,
