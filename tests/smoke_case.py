@@ -1,5 +1,7 @@
-"""The smoke case run by __graft_entry__.smoke(): a small slice of the hot path on cuda:0
-through the C ABI, checked bit-exactly against the CPU oracle."""
+"""The smoke case run by __graft_entry__.smoke(): small slices of the hot path on cuda:0
+through the C ABI, checked against the CPU oracle: the NTT bit-exactly, the grouped FFT
+blind rotation within its FP64 phase-error bound, the FFT HomTrace / SchemeSwitch rows by
+decryption."""
 from __future__ import annotations
 
 
@@ -33,3 +35,58 @@ def run_smoke(pkg, torch, np) -> None:
     torch.cuda.synchronize()
     assert (x.cpu().numpy().view(np.uint64) == a).all(), "inverse NTT mismatch"
     print("smoke: NTT N=2048 bit-exact vs oracle")
+
+    # the FFT circuit-bootstrapping path on a small ring (N = 1024, n = 64): grouped (mb = 2)
+    # blind rotation against the oracle's exact grouped rotation, then HomTrace +
+    # SchemeSwitch in FFT form through the CBS entry point, rows checked by decryption
+    import ctypes
+
+    from cbs_harness import OracleCbs, lwe_encrypt_bits
+    p = pkg.default_params()
+    p.N, p.n = 1024, 64
+    p.Q = oracle_primes(oracle, 1024, 54, 1)[0]
+    ctx = pkg.Context(p, max_batch=4)
+    try:
+        ctx.keygen(7)
+        ctx.set_br_backend(pkg.BR_FFT64)
+        ctx.set_br_multibit(2)
+        keys = ctx.export_keys()
+        oc = OracleCbs(oracle, p, keys)
+        bits = [1, 0]
+        a, b = lwe_encrypt_bits(np.random.default_rng(1), keys["s_lwe"], bits, p.q_lwe)
+        da, db = dev(a), dev(b)
+        mv = torch.zeros((len(bits), p.num_lut, 2, p.N), dtype=torch.int64, device="cuda")
+        pkg.call("cbs_blind_rotate_batch_device", ctx.handle, da.data_ptr(), db.data_ptr(), len(bits), p.n,
+                 mv.data_ptr(), None)
+        torch.cuda.synchronize()
+        got = mv.cpu().numpy().view(np.uint64)
+        want = oc.br_acc_mb(a, b, ctx.export_mb_bsk(), 2)
+        Q, N = p.Q, p.N
+        worst = 0
+        for i in range(len(bits)):
+            d = oc.phase_coef(got[i, 0]) - oc.phase_coef(want[i])
+            worst = max(worst, max(abs(((int(x) * N + Q // 2) % Q) - Q // 2) for x in d))
+        assert worst < 2 ** 33, f"grouped FFT blind rotation phase error 2^{np.log2(worst + 1):.1f}"
+        print(f"smoke: grouped FFT blind rotation within 2^{np.log2(worst + 1):.1f} of the exact oracle")
+
+        view = ctypes.c_void_p()
+        pkg.call("cbs_circuit_bootstrap_batch_device", ctx.handle, da.data_ptr(), db.data_ptr(), len(bits), p.n,
+                 ctypes.byref(view), None)
+        torch.cuda.synchronize()
+        per = p.num_lut * 4 * p.N
+        rg = np.zeros(len(bits) * per, np.uint64)
+        cudart = ctypes.CDLL("libcudart.so.12")
+        cudart.cudaMemcpy.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int]
+        assert cudart.cudaMemcpy(rg.ctypes.data, view.value, rg.nbytes, 2) == 0  # device to host
+        rg = rg.reshape(len(bits), p.num_lut, 2, 2, p.N)
+        g = [int(x) for x in keys["gpow"]]
+        s = keys["s_rlwe"].astype(object)
+        for i, m in enumerate(bits):
+            for j in range(p.num_lut):
+                ph1 = oc.phase_coef(rg[i, j, 1])
+                ph1[0] -= m * g[j]
+                ph0 = oc.phase_coef(rg[i, j, 0]) + m * g[j] * s
+                assert max(abs(int(x)) for x in ph1) < 2 ** 33 and max(abs(int(x)) for x in ph0) < 2 ** 37
+        print("smoke: FFT HomTrace + SchemeSwitch rows decrypt to m g_j / -m g_j s")
+    finally:
+        ctx.close()
