@@ -63,8 +63,124 @@ __global__ void __launch_bounds__(256) k_tcb_pfks(const uint64_t* __restrict__ e
     for (uint32_t r = 0; r < R; ++r) out[r * 256] = acc[r];
 }
 
+// Tiled PFKS: output rows that share the function read, for each input coefficient i and
+// digit level j, the same 2^b - 1 key rows and differ only in which one their digit selects.
+// A CTA owns 128 output items x 128 output words of one function: per (i, j) it stages that
+// 128-word slice of the key rows in shared memory (row 0 zero, so digit 0 needs no branch)
+// and each thread adds the selected rows for its 4 items x 16 words.  The slices stream
+// through a 4-stage ring filled by per-thread asynchronous copies issued three slices ahead,
+// and the digit words of coefficient i + 1 are loaded while coefficient i is summed, so the
+// loop does not wait on memory latency.  Key traffic falls from one full key stream per
+// output row to one per 128 rows; the sums are the same integers mod 2^32 as the
+// one-row-per-CTA kernel.
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+    const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(smem_dst));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int PENDING>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(PENDING) : "memory");
+}
+
+template <uint32_t BASE_BITS>
+__global__ void __launch_bounds__(256, 2) k_tcb_pfks_tiled(const uint64_t* __restrict__ ext,
+                                                          const uint32_t* __restrict__ key, uint32_t items, uint32_t N2,
+                                                          uint32_t N1, uint32_t levels, uint32_t* __restrict__ rgsw) {
+    constexpr uint32_t B = 1u << BASE_BITS, CT = 128, IT = 128, TPI = 4, CG = 8, STAGES = 4;
+    constexpr uint32_t CHUNKS = (B - 1) * CT / 4, PER_T = (CHUNKS + 255) / 256;
+    __shared__ __align__(16) uint32_t tile[STAGES][B][CT];
+    const uint32_t tid = threadIdx.x, cg = tid % CG, ig = tid / CG;
+    const uint32_t c0 = blockIdx.x * CT, item0 = blockIdx.y * IT + ig * TPI, fn = blockIdx.z;
+    const size_t row_words = 2ull * N1, per_i = static_cast<size_t>(levels) * (B - 1) * row_words;
+    const uint32_t* kf = key + static_cast<size_t>(fn) * (N2 + 1) * per_i + c0;
+    const uint32_t tiles = (N2 + 1) * levels;  // slice t = i * levels + j
+    if (tid < CT)
+#pragma unroll
+        for (uint32_t st = 0; st < STAGES; ++st) tile[st][0][tid] = 0u;
+    // one commit group per slice index, issued or not, so the group count stays uniform
+    auto issue = [&](uint32_t t) {
+        if (t < tiles) {
+            const uint32_t i = t / levels, j = t % levels;
+            const uint32_t* src = kf + i * per_i + static_cast<size_t>(j) * (B - 1) * row_words;
+            uint32_t (*dst)[CT] = tile[t % STAGES];
+#pragma unroll
+            for (uint32_t p = 0; p < PER_T; ++p) {
+                const uint32_t k = tid + 256 * p;
+                if (k < CHUNKS)
+                    cp_async16(&dst[1 + k / (CT / 4)][(k % (CT / 4)) * 4],
+                               src + (k / (CT / 4)) * row_words + (k % (CT / 4)) * 4);
+            }
+        }
+        cp_async_commit();
+    };
+    // top 32 bits (rounded) of -a_i, or of b for i = N2: phase = sum x_i y_i
+    auto load_x = [&](uint32_t i, uint32_t (&x)[TPI]) {
+#pragma unroll
+        for (uint32_t u = 0; u < TPI; ++u) {
+            const uint32_t item = item0 + u;
+            uint64_t x64 = 0;
+            if (item < items && i <= N2) {
+                const uint64_t* in = ext + static_cast<size_t>(item) * (N2 + 1);
+                x64 = (i < N2) ? 0ull - __ldg(in + i) : __ldg(in + N2);
+            }
+            x[u] = static_cast<uint32_t>((x64 + (1ull << 31)) >> 32);
+        }
+    };
+    uint32_t acc[TPI][16];
+#pragma unroll
+    for (uint32_t u = 0; u < TPI; ++u)
+#pragma unroll
+        for (uint32_t w = 0; w < 16; ++w) acc[u][w] = 0u;
+#pragma unroll
+    for (uint32_t t = 0; t < STAGES - 1; ++t) issue(t);
+    uint32_t x[TPI], xn[TPI];
+    load_x(0, x);
+    for (uint32_t i = 0; i <= N2; ++i) {
+        load_x(i + 1, xn);
+        for (uint32_t j = 0; j < levels; ++j) {
+            const uint32_t t = i * levels + j;
+            cp_async_wait<STAGES - 2>();  // this thread's copies of slice t have landed
+            __syncthreads();              // everyone's have; slice t - 1 is no longer read
+            issue(t + STAGES - 1);        // into the stage slice t - 1 used
+            const uint32_t sh = 32 - (j + 1) * BASE_BITS;
+            const uint32_t (*cur)[CT] = tile[t % STAGES];
+#pragma unroll
+            for (uint32_t u = 0; u < TPI; ++u) {
+                const uint32_t* row = cur[(x[u] >> sh) & (B - 1)];
+#pragma unroll
+                for (uint32_t q = 0; q < 4; ++q) {
+                    const uint4 v = *reinterpret_cast<const uint4*>(row + 4 * (cg + CG * q));
+                    acc[u][4 * q] += v.x;
+                    acc[u][4 * q + 1] += v.y;
+                    acc[u][4 * q + 2] += v.z;
+                    acc[u][4 * q + 3] += v.w;
+                }
+            }
+        }
+#pragma unroll
+        for (uint32_t u = 0; u < TPI; ++u) x[u] = xn[u];
+    }
+    cp_async_wait<0>();
+#pragma unroll
+    for (uint32_t u = 0; u < TPI; ++u) {
+        const uint32_t item = item0 + u;
+        if (item >= items) continue;
+        uint32_t* out = rgsw + (static_cast<size_t>(item) * 2 + fn) * row_words + c0;
+#pragma unroll
+        for (uint32_t q = 0; q < 4; ++q)
+            *reinterpret_cast<uint4*>(out + 4 * (cg + CG * q)) =
+                make_uint4(acc[u][4 * q], acc[u][4 * q + 1], acc[u][4 * q + 2], acc[u][4 * q + 3]);
+    }
+}
+
 static cudaError_t tcb_pfks_launch(const uint64_t* ext, const uint32_t* key, uint32_t items, uint32_t N2, uint32_t N1,
                                    uint32_t base_bits, uint32_t levels, uint32_t* rgsw, cudaStream_t s) {
+    if (base_bits == 4 && (2 * N1) % 128 == 0 && levels * base_bits <= 32) {
+        const dim3 grid(2 * N1 / 128, (items + 127) / 128, 2);
+        k_tcb_pfks_tiled<4><<<grid, 256, 0, s>>>(ext, key, items, N2, N1, levels, rgsw);
+        return cudaGetLastError();
+    }
     const unsigned grid = 2 * items;
     switch (N1) {
         case 256: k_tcb_pfks<256><<<grid, 256, 0, s>>>(ext, key, N2, base_bits, levels, rgsw); break;
