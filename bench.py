@@ -488,6 +488,7 @@ def run_gate(args, rank: int, world: int, local_rank: int) -> None:
     count = args.batch or 64
     ctx = pkg.GateContext(max_batch=count)
     ctx.keygen(args.seed)
+    ctx.set_multibit(args.multibit)
     p = ctx.params
     rng = np.random.default_rng(args.seed + rank)
     x = rng.integers(0, 2, count).astype(np.uint8)
@@ -530,7 +531,7 @@ def run_gate(args, rank: int, world: int, local_rank: int) -> None:
            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f64 (FFT products, exact after rounding) + u32 torus",
            "data": "synthetic (seeded uniform random input bits)",
-           "config": {"workload": "gate_nand", "batch": count, "n": p.n, "N": p.N,
+           "config": {"workload": "gate_nand", "batch": count, "n": p.n, "N": p.N, "br_multibit": args.multibit,
                       "gadget": f"2^{p.bg_bits}x{p.levels}", "ks": f"2^{p.ks_base_bits}x{p.ks_levels}",
                       "l2": "keys (62 MB spectra + 62 MB KSK) stay L2/HBM resident; no flush"},
            "us_per_gate": ms * 1e3 / count, "correct_gates": ok, "gpu_launches": args.steps * 2,
@@ -563,6 +564,7 @@ def run_ragged(args, rank: int, world: int, local_rank: int) -> None:
     ctxs = [pkg.GateContext(pa, max_batch=2048), pkg.GateContext(pb, max_batch=2048)]
     for i, c in enumerate(ctxs):
         c.keygen(args.seed + i)
+        c.set_multibit(args.multibit)
     rng = np.random.default_rng(args.seed + 5 + rank)
     reqs, bufs, total = [[], []], [], 0
     while total < total_min:
@@ -628,6 +630,7 @@ def run_ragged(args, rank: int, world: int, local_rank: int) -> None:
            "vs_baseline": None, "dtype": "f64 (FFT products, exact after rounding) + u32 torus",
            "data": "synthetic (seeded request sizes, parameter sets and bits)",
            "config": {"workload": "ragged_bootstrap", "requests": len(bufs), "bootstraps": total,
+                      "br_multibit": args.multibit,
                       "per_set": [sum(r[4] for r in reqs[0]), sum(r[4] for r in reqs[1])],
                       "l2": "keys of both sets (2 x ~125 MB) do not fit L2 together; no flush"},
            "correct": ok, "gpu_launches": args.steps * 4,
@@ -657,6 +660,7 @@ def run_tcb(args, rank: int, world: int, local_rank: int) -> None:
     count = args.batch or 256
     ctx = pkg.TcbContext(max_batch=count)
     ctx.keygen(args.seed)
+    ctx.set_multibit(args.multibit)
     p = ctx.params
     rng = np.random.default_rng(args.seed + rank)
     bits = rng.integers(0, 2, count).astype(np.uint8)
@@ -688,6 +692,7 @@ def run_tcb(args, rank: int, world: int, local_rank: int) -> None:
            "vs_baseline": None, "dtype": "f64 (64-bit-torus FFT products) + u32/u64 torus",
            "data": "synthetic (seeded uniform random bits)",
            "config": {"workload": "tcb_pfks", "bits": count, "n": p.n, "N2": p.N2, "l2": p.l2, "bg2_bits": p.bg2_bits,
+                      "br_multibit": args.multibit,
                       "N1": p.N1, "cb": f"2^{p.cb_bits}x{p.cb_levels}", "pfks": f"2^{p.pfks_base_bits}x{p.pfks_levels}",
                       "l2_cache": f"PFKS keys {pfks_bytes / 1e9:.1f} GB >> 126 MB L2"},
            "us_per_bit": ms * 1e3 / count, "gpu_launches": args.steps * 2,

@@ -103,6 +103,8 @@ def _declare(lib: ctypes.CDLL) -> None:
         "cbs_gate_context_create": (st, [c_vp, u32, c_vp]),
         "cbs_gate_context_destroy": (st, [c_vp]),
         "cbs_gate_keygen": (st, [c_vp, u64]),
+        "cbs_gate_set_multibit": (st, [c_vp, u32]),
+        "cbs_gate_export_mb_bsk": (st, [c_vp, c_vp, c_vp]),
         "cbs_gate_generate_keys_host": (st, [c_vp, u64, c_vp, c_vp, c_vp, c_vp]),
         "cbs_gate_export_keys": (st, [c_vp, c_vp, c_vp, c_vp, c_vp]),
         "cbs_gate_encrypt_bits": (st, [c_vp, c_vp, u32, u64, c_vp, c_vp]),
@@ -113,6 +115,8 @@ def _declare(lib: ctypes.CDLL) -> None:
         "cbs_tcb_context_create": (st, [c_vp, u32, c_vp]),
         "cbs_tcb_context_destroy": (st, [c_vp]),
         "cbs_tcb_keygen": (st, [c_vp, u64]),
+        "cbs_tcb_set_multibit": (st, [c_vp, u32]),
+        "cbs_tcb_export_mb_bsk": (st, [c_vp, c_vp, c_vp]),
         "cbs_tcb_generate_keys_host": (st, [c_vp, u64, c_vp, c_vp, c_vp, c_vp, c_vp]),
         "cbs_tcb_export_keys": (st, [c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
         "cbs_tcb_encrypt_bits": (st, [c_vp, c_vp, u32, u64, c_vp, c_vp]),
@@ -283,6 +287,19 @@ class GateContext:
     def keygen(self, seed: int) -> None:
         call("cbs_gate_keygen", self._h, seed)
 
+    def set_multibit(self, mb: int) -> None:
+        """Blind rotation over groups of mb = 1, 2 or 3 LWE coefficients."""
+        call("cbs_gate_set_multibit", self._h, mb)
+
+    def export_mb_bsk(self):
+        """Grouped keys [ceil(n/mb)][2^mb - 1][2*levels][2][N] (uint32 torus)."""
+        import numpy as np
+        words = ctypes.c_size_t()
+        call("cbs_gate_export_mb_bsk", self._h, None, ctypes.byref(words))
+        out = np.zeros(words.value, np.uint32)
+        call("cbs_gate_export_mb_bsk", self._h, out.ctypes.data, ctypes.byref(words))
+        return out
+
     def encrypt(self, bits, seed: int):
         import numpy as np
         bits = np.ascontiguousarray(bits, dtype=np.uint8)
@@ -375,6 +392,19 @@ class TcbContext:
 
     def keygen(self, seed: int) -> None:
         call("cbs_tcb_keygen", self._h, seed)
+
+    def set_multibit(self, mb: int) -> None:
+        """Level-2 blind rotation over groups of mb = 1, 2 or 3 LWE coefficients."""
+        call("cbs_tcb_set_multibit", self._h, mb)
+
+    def export_mb_bsk(self):
+        """Grouped level-2 keys [ceil(n/mb)][2^mb - 1][2*l2][2][N2] (uint64 torus)."""
+        import numpy as np
+        words = ctypes.c_size_t()
+        call("cbs_tcb_export_mb_bsk", self._h, None, ctypes.byref(words))
+        out = np.zeros(words.value, np.uint64)
+        call("cbs_tcb_export_mb_bsk", self._h, out.ctypes.data, ctypes.byref(words))
+        return out
 
     def encrypt(self, bits, seed: int):
         import numpy as np

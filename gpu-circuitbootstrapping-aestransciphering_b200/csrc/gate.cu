@@ -26,6 +26,7 @@
 #include "devbuf.cuh"
 #include "fft_core.cuh"
 #include "fft_kernels.cuh"
+#include "fft_ops.cuh"
 #include "keygen.h"
 #include "torus.cuh"
 
@@ -241,6 +242,201 @@ __global__ void __launch_bounds__(GateCfg<LOGN>::T, GateCfg<LOGN>::MIN_BLOCKS) k
     }
 }
 
+// Grouped (multi-bit) form of k_gate_blind_rotate, the reference's CIRBTS_PBS_MULTIBIT key
+// grouping (bitwise/src/cirbts/cirbts-init.cu:376-530, kernel.cu:4585-4771) on the torus: per
+// group of MB coefficients acc += sum_S m_S (acc (x) RGSW(prod_{i in S} s_i)), m_S =
+// prod_{i in S} (X^{a_i} - 1), with the combined key sum_S m_S(psi) K_S formed per spectrum
+// slot (the structure of k_blind_rotate_fft_mb: c_i per slot once per group in shared memory,
+// the 16 key spectra of one subset loaded together).  Groups whose rotations are all 0 are
+// skipped.  Keys: [groups][2^MB - 1][2*levels][2][M] spectra.
+template <int LOGN>
+struct GateMbCfg {
+    static constexpr uint32_t T = (1u << LOGN) / 8;
+    static constexpr int MIN_BLOCKS = LOGN <= 10 ? 2 : 1;  // the whole register file per CTA pair / CTA
+};
+
+template <int LOGN, typename TT, int MB>
+__global__ void __launch_bounds__(GateMbCfg<LOGN>::T, GateMbCfg<LOGN>::MIN_BLOCKS)
+    k_gate_blind_rotate_mb(const GateArgs a) {
+    constexpr int LOGM = LOGN - 1;
+    constexpr uint32_t N = 1u << LOGN, M = N / 2, TH = M / 8, T = 2 * TH, TWO_N = 2 * N;
+    constexpr uint32_t SH = 32 - (LOGN + 1);  // torus -> Z_2N
+    constexpr uint32_t KS = (1u << MB) - 1u;
+    using Tb = FftTab<LOGM>;
+    extern __shared__ __align__(16) uint64_t smem[];
+    double2* fs = reinterpret_cast<double2*>(smem);             // [2][M]
+    double2* tab = fs + 2 * M;                                  // FftTab<LOGM>
+    TT* acc = reinterpret_cast<TT*>(tab + Tb::size());         // [2][N] torus values
+    uint32_t* dig = reinterpret_cast<uint32_t*>(acc + 2 * N);  // [2][levels][M] packed pairs
+    double2* cbuf = reinterpret_cast<double2*>(dig + 2 * a.levels * M);  // [MB][8][T]
+    const double2* tws = tab + Tb::twist_off();
+    const uint32_t ct = blockIdx.x, tid = threadIdx.x;
+    const uint32_t h = tid / TH, ht = tid % TH;
+    TT* my_acc = acc + h * N;
+    double2* my_fs = fs + h * M;
+    const uint32_t levels = a.levels, bg = a.bg_bits;
+    constexpr uint32_t W = 8 * sizeof(TT);
+    TT off = TT(1) << (W - levels * bg - 1);
+    for (uint32_t k = 0; k < levels; ++k) off += (TT(1) << (bg - 1)) << (W - (k + 1) * bg);
+    auto half_bar = [h]() {
+        if (h == 0) asm volatile("bar.sync 1, %0;" ::"n"(TH) : "memory");
+        else asm volatile("bar.sync 2, %0;" ::"n"(TH) : "memory");
+    };
+    auto ms = [](uint32_t x) { return ((x + (1u << (SH - 1))) >> SH) & (TWO_N - 1); };
+
+    for (uint32_t i = tid; i < Tb::size(); i += T) tab[i] = a.tab[i];
+    const uint32_t l2 = 2 * levels;
+    const size_t kstride = static_cast<size_t>(l2) * 2 * M;
+    const uint32_t groups = (a.n + MB - 1) / MB;
+    for (uint32_t item = ct; item < a.items; item += gridDim.x) {
+        const uint32_t* a1;
+        const uint32_t* a2;
+        uint32_t b;
+        if (a.reqs) {
+            const GateReq& rq = a.reqs[gate_req_of(a.reqs, a.num_reqs, item)];
+            const uint32_t k = item - rq.offset;
+            a1 = rq.a + static_cast<size_t>(k) * a.n;
+            a2 = a1;
+            b = rq.b[k];
+        } else {
+            const uint32_t in = item / a.levels_tv;
+            a1 = a.a1 + static_cast<size_t>(in) * a.n;
+            a2 = a.a2 ? a.a2 + static_cast<size_t>(in) * a.n : a1;
+            b = gate_b(a.gate, a.b1[in], a.b2 ? a.b2[in] : 0u);
+        }
+        const TT mu = static_cast<TT>(a.mu[item % a.levels_tv]), b_add = static_cast<TT>(a.b_add[item % a.levels_tv]);
+        {
+            const uint32_t bt = ms(b);
+            for (uint32_t i = tid; i < N; i += T) {
+                acc[i] = 0;
+                acc[N + i] = (((i + bt) & (TWO_N - 1)) < N) ? mu : TT(0) - mu;
+            }
+        }
+        __syncthreads();
+
+        for (uint32_t g = 0; g < groups; ++g) {
+            uint32_t at[MB];
+            uint32_t any = 0;
+#pragma unroll
+            for (int i = 0; i < MB; ++i) {
+                const uint32_t idx = g * MB + i;
+                at[i] = idx < a.n ? ms(a.reqs ? __ldg(a1 + idx) : gate_a(a.gate, __ldg(a1 + idx), __ldg(a2 + idx))) : 0u;
+                any |= at[i];
+            }
+            if (any == 0) continue;  // every m_S is 0 (uniform over the CTA)
+#pragma unroll
+            for (int i = 0; i < MB; ++i) {
+                const double2 ub = zeta_pow<LOGN>(tws, mult_base<LOGN>(ht, at[i]));
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    const uint32_t r3 = ((j & 1) << 2) | (j & 2) | ((j >> 2) & 1);
+                    const uint32_t k = (at[i] * r3) & 7u;
+                    double2 w = tab[(k & 3u) * (M / 8)];
+                    if (k & 4u) w = make_double2(-w.x, -w.y);
+                    const double2 v = cmul(ub, w);
+                    cbuf[(i * 8 + j) * T + tid] = make_double2(v.x - 1.0, v.y);
+                }
+            }
+            for (uint32_t e = ht; e < M; e += TH) {
+                const TT wr = my_acc[e] + off, wi = my_acc[e + M] + off;
+                uint32_t* dst = dig + h * levels * M + e;
+                for (uint32_t k = 0; k < levels; ++k) {
+                    const uint32_t sft = W - (k + 1) * bg, mask = (1u << bg) - 1, half = 1u << (bg - 1);
+                    const int32_t dr = static_cast<int32_t>((wr >> sft) & mask) - static_cast<int32_t>(half);
+                    const int32_t di = static_cast<int32_t>((wi >> sft) & mask) - static_cast<int32_t>(half);
+                    dst[k * M] = (static_cast<uint32_t>(dr) & 0xffffu) | (static_cast<uint32_t>(di) << 16);
+                }
+            }
+            half_bar();
+            const double2* gk = a.bskf + static_cast<size_t>(g) * KS * kstride + ht;
+            double2 y0[8], y1[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) y0[j] = y1[j] = make_double2(0.0, 0.0);
+            for (uint32_t d = 0; d < levels; ++d) {
+                const uint32_t* dsrc = dig + (h * levels + d) * M;
+                double2 x[8];
+                fft_forward_to_regs<LOGM>(
+                    my_fs, ht, tab,
+                    [&](int j, uint32_t e) {
+                        const uint32_t v = dsrc[e];
+                        const double re = static_cast<double>(static_cast<int16_t>(v & 0xffffu));
+                        const double im = static_cast<double>(static_cast<int16_t>(v >> 16));
+                        return cmul(make_double2(re, im), gate_twist<LOGM>(tws, j, e));
+                    },
+                    x, half_bar);
+                const double2* k0 = gk + static_cast<size_t>(2 * d + h) * 2 * M;
+                double2 kc0[8], kc1[8];
+#pragma unroll
+                for (int sub = 0; sub < static_cast<int>(KS); ++sub) {
+                    double2 ka[8], kb[8];
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) {
+                        ka[j] = __ldg(k0 + sub * kstride + j * TH);
+                        kb[j] = __ldg(k0 + sub * kstride + M + j * TH);
+                    }
+                    const uint32_t mask = MB == 2 ? (sub == 0 ? 1u : (sub == 1 ? 2u : 3u))
+                                                  : (sub < 3 ? (1u << sub)
+                                                             : (sub == 3 ? 3u : (sub == 4 ? 5u : (sub == 5 ? 6u : 7u))));
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) {
+                        double2 m = make_double2(1.0, 0.0);
+                        bool first = true;
+#pragma unroll
+                        for (int i = 0; i < MB; ++i)
+                            if (mask & (1u << i)) {
+                                const double2 c = cbuf[(i * 8 + j) * T + tid];
+                                m = first ? c : cmul(m, c);
+                                first = false;
+                            }
+                        if (sub == 0) {
+                            kc0[j] = cmul(m, ka[j]);
+                            kc1[j] = cmul(m, kb[j]);
+                        } else {
+                            cfma(kc0[j], m, ka[j]);
+                            cfma(kc1[j], m, kb[j]);
+                        }
+                    }
+                }
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    cfma(y0[j], x[j], kc0[j]);
+                    cfma(y1[j], x[j], kc1[j]);
+                }
+                half_bar();
+            }
+#pragma unroll
+            for (int j = 0; j < 8; ++j) my_fs[cswz(8 * ht + j)] = h ? y0[j] : y1[j];
+            __syncthreads();
+            {
+                const double2* take = fs + (1 - h) * M;
+#pragma unroll
+                for (int j = 0; j < 8; ++j) y0[j] = cadd(h ? y1[j] : y0[j], take[cswz(8 * ht + j)]);
+            }
+            __syncthreads();
+            constexpr double inv_m = 1.0 / M;
+            // the monomials are in the combined keys: add the rounded product in place
+            fft_inverse_from_regs<LOGM>(
+                my_fs, ht, tab, y0,
+                [&](int j, uint32_t e, double2 v) {
+                    const double2 u = cmulc(v, gate_twist<LOGM>(tws, j, e));
+                    my_acc[e] += to_torus<TT>(u.x * inv_m);
+                    my_acc[e + M] += to_torus<TT>(u.y * inv_m);
+                },
+                half_bar);
+        }
+        __syncthreads();
+        TT* out = reinterpret_cast<TT*>(a.ext) + static_cast<size_t>(item) * (N + 1);
+        for (uint32_t i = tid; i <= N; i += T) {
+            TT v;
+            if (i == N) v = acc[N] + b_add;
+            else if (i == 0) v = acc[0];
+            else v = TT(0) - acc[N - i];
+            out[i] = v;
+        }
+        __syncthreads();
+    }
+}
+
 // LWE key switch N -> n of one extracted ciphertext per blockIdx.y; thread j < n + 1 of the
 // grid owns output coefficient j (j = n is b).  The digits of a'_i are the same for every
 // thread, so the inner loop is uniform and each step reads one coalesced key row segment.
@@ -297,16 +493,47 @@ static cudaError_t gate_br_launch(const GateArgs& a, uint32_t grid, cudaStream_t
     return cudaGetLastError();
 }
 
-cudaError_t gate_blind_rotate(const GateArgs& a, uint32_t N, uint32_t grid, cudaStream_t s) {
-    if (N == 1024) return gate_br_launch<10, uint32_t>(a, grid, s);
-    if (N == 2048) return gate_br_launch<11, uint32_t>(a, grid, s);
+template <int LOGN, typename TT, int MB>
+static cudaError_t gate_br_mb_launch(const GateArgs& a, uint32_t grid, cudaStream_t s) {
+    constexpr uint32_t N = 1u << LOGN, M = N / 2;
+    const size_t smem = (2ull * M + FftTab<LOGN - 1>::size()) * sizeof(double2) + 2ull * N * sizeof(TT) +
+                        2ull * a.levels * M * sizeof(uint32_t) + MB * 8ull * GateMbCfg<LOGN>::T * sizeof(double2);
+    static size_t configured[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (configured[dev] < smem) {
+        cudaError_t e = cudaFuncSetAttribute(k_gate_blind_rotate_mb<LOGN, TT, MB>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+        if (e != cudaSuccess) return e;
+        configured[dev] = smem;
+    }
+    k_gate_blind_rotate_mb<LOGN, TT, MB><<<grid, GateMbCfg<LOGN>::T, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <typename TT>
+static cudaError_t gate_br_dispatch(const GateArgs& a, uint32_t N, uint32_t grid, cudaStream_t s) {
+    if (a.mb <= 1) {
+        if (N == 1024) return gate_br_launch<10, TT>(a, grid, s);
+        if (N == 2048) return gate_br_launch<11, TT>(a, grid, s);
+        return cudaErrorInvalidValue;
+    }
+    if (a.mb == 2) {
+        if (N == 1024) return gate_br_mb_launch<10, TT, 2>(a, grid, s);
+        if (N == 2048) return gate_br_mb_launch<11, TT, 2>(a, grid, s);
+    } else if (a.mb == 3) {
+        if (N == 1024) return gate_br_mb_launch<10, TT, 3>(a, grid, s);
+        if (N == 2048) return gate_br_mb_launch<11, TT, 3>(a, grid, s);
+    }
     return cudaErrorInvalidValue;
 }
 
+cudaError_t gate_blind_rotate(const GateArgs& a, uint32_t N, uint32_t grid, cudaStream_t s) {
+    return gate_br_dispatch<uint32_t>(a, N, grid, s);
+}
+
 cudaError_t gate_blind_rotate64(const GateArgs& a, uint32_t N, uint32_t grid, cudaStream_t s) {
-    if (N == 1024) return gate_br_launch<10, uint64_t>(a, grid, s);
-    if (N == 2048) return gate_br_launch<11, uint64_t>(a, grid, s);
-    return cudaErrorInvalidValue;
+    return gate_br_dispatch<uint64_t>(a, N, grid, s);
 }
 
 // host helpers shared with the torus circuit bootstrap
@@ -412,6 +639,12 @@ struct cbs_gate_context {
     DevBuf<cbs::GateReq> d_plan;
     DevBuf<uint32_t> d_plan_ext;
     uint32_t plan_reqs = 0, plan_items = 0, plan_grid = 0;
+    // grouped (multi-bit) blind rotation: mb, its keys (coefficient form) and their spectra
+    uint32_t br_mb = 1;
+    bool mb_ready = false;
+    uint64_t key_seed = 0;
+    std::vector<uint32_t> mbk;
+    DevBuf<double2> d_bskf_mb;
 };
 
 namespace {
@@ -536,9 +769,83 @@ void gate_keys_host(const cbs_gate_params& p, uint64_t seed, std::vector<int32_t
             }
 }
 
+// Grouped keys RGSW_z(prod_{i in S} s_i) for every non-empty subset S of each group of mb
+// LWE coefficients (rows 2k + c add the product times 2^(32 - (k+1) bg) to component c), one
+// generator per row so the keys do not depend on the thread count.
+void gate_mb_keys_host(const cbs_gate_params& p, const std::vector<int32_t>& s, const std::vector<int32_t>& z,
+                       uint32_t mb, uint64_t seed, std::vector<uint32_t>& out) {
+    const uint32_t n = p.n, N = p.N, L = p.levels, K = cbs::mb_subsets(mb), groups = (n + mb - 1) / mb;
+    const size_t rows = static_cast<size_t>(groups) * K * 2 * L;
+    out.assign(rows * 2 * N, 0);
+    const unsigned nth = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    std::vector<std::thread> pool;
+    for (unsigned th = 0; th < nth; ++th)
+        pool.emplace_back([&, th] {
+            for (size_t r = th; r < rows; r += nth) {
+                cbs::Rng rr(seed ^ (0x9e3779b97f4a7c15ull * (r + 1)));
+                uint32_t* ra = out.data() + r * 2 * N;
+                uint32_t* rb = ra + N;
+                for (uint32_t e = 0; e < N; ++e) {
+                    ra[e] = static_cast<uint32_t>(rr.next());
+                    rb[e] = torus_noise(rr, p.sigma_rlwe);
+                }
+                mul_binary_acc(ra, z.data(), N, rb);
+                const uint32_t g = static_cast<uint32_t>(r / (K * 2 * L));
+                const uint32_t kk = static_cast<uint32_t>((r / (2 * L)) % K), row = static_cast<uint32_t>(r % (2 * L));
+                const uint32_t mask = cbs::mb_subset_mask(mb, kk);
+                uint32_t prod = 1;
+                for (uint32_t i = 0; i < mb; ++i)
+                    if (mask & (1u << i)) prod &= (g * mb + i < n) ? static_cast<uint32_t>(s[g * mb + i]) : 0u;
+                (row % 2 ? rb : ra)[0] += prod << (32 - (row / 2 + 1) * p.bg_bits);
+            }
+        });
+    for (auto& t : pool) t.join();
+}
+
+constexpr uint64_t kGateMbSeedTweak = 0x67617465206d6275ull;
+
+cbs_status gate_prepare_mb(cbs_gate_context* ctx) {
+    if (ctx->br_mb <= 1 || ctx->mb_ready || !ctx->keys_ready) return CBS_OK;
+    std::vector<double2> spec;
+    try {
+        gate_mb_keys_host(ctx->p, ctx->s, ctx->z, ctx->br_mb, ctx->key_seed ^ kGateMbSeedTweak, ctx->mbk);
+        cbs::torus_keys_to_fft(ctx->p.N, ctx->mbk.data(), ctx->mbk.size() / ctx->p.N, spec);
+    } catch (const std::exception& e) {
+        set_error(std::string("gate multi-bit keys: ") + e.what());
+        return CBS_ERR_OOM;
+    }
+    CBS_CUDA_TRY(ctx->d_bskf_mb.upload(spec.data(), spec.size(), nullptr));
+    CBS_CUDA_TRY(cudaStreamSynchronize(nullptr));
+    ctx->mb_ready = true;
+    return CBS_OK;
+}
+
 }  // namespace
 
 extern "C" {
+
+cbs_status cbs_gate_set_multibit(cbs_gate_context* ctx, uint32_t mb) {
+    CBS_CHECK_ARG(ctx, "gate_set_multibit: null context");
+    CBS_CHECK_ARG(mb >= 1 && mb <= 3, "gate_set_multibit: mb must be 1, 2 or 3");
+    if (mb != ctx->br_mb) {
+        ctx->br_mb = mb;
+        ctx->mb_ready = false;
+        ctx->mbk.clear();
+        ctx->d_bskf_mb.reset();
+    }
+    return gate_prepare_mb(ctx);
+}
+
+cbs_status cbs_gate_export_mb_bsk(const cbs_gate_context* ctx, uint32_t* out, size_t* words) {
+    CBS_CHECK_ARG(ctx && words, "gate_export_mb_bsk: null argument");
+    if (ctx->br_mb <= 1 || !ctx->mb_ready) {
+        set_error("gate_export_mb_bsk: no grouped keys (select mb > 1 after cbs_gate_keygen)");
+        return CBS_ERR_NOT_READY;
+    }
+    *words = ctx->mbk.size();
+    if (out) std::copy(ctx->mbk.begin(), ctx->mbk.end(), out);
+    return CBS_OK;
+}
 
 cbs_status cbs_gate_generate_keys_host(const cbs_gate_params* params, uint64_t seed, int32_t* s_lwe, int32_t* z_rlwe,
                                        uint32_t* bsk, uint32_t* ksk) {
@@ -572,7 +879,9 @@ cbs_status cbs_gate_keygen(cbs_gate_context* ctx, uint64_t seed) {
     CBS_CUDA_TRY(ctx->d_ksk.upload(ctx->ksk.data(), ctx->ksk.size(), nullptr));
     CBS_CUDA_TRY(cudaStreamSynchronize(nullptr));
     ctx->keys_ready = true;
-    return CBS_OK;
+    ctx->key_seed = seed;
+    ctx->mb_ready = false;
+    return gate_prepare_mb(ctx);
 }
 
 cbs_status cbs_gate_export_keys(const cbs_gate_context* ctx, int32_t* s_lwe, int32_t* z_rlwe, uint32_t* bsk,
@@ -639,6 +948,10 @@ static cbs_status gate_run(cbs_gate_context* ctx, int gate, const uint32_t* d_a1
         set_error("gate: count above the context's max_batch");
         return CBS_ERR_SHAPE_MISMATCH;
     }
+    if (ctx->br_mb > 1 && !ctx->mb_ready) {
+        set_error("gate: grouped keys are not prepared");
+        return CBS_ERR_NOT_READY;
+    }
     const cbs_gate_params& p = ctx->p;
     cbs::GateArgs a{};
     a.gate = gate;
@@ -649,7 +962,8 @@ static cbs_status gate_run(cbs_gate_context* ctx, int gate, const uint32_t* d_a1
     a.n = p.n;
     a.levels = p.levels;
     a.bg_bits = p.bg_bits;
-    a.bskf = ctx->d_bskf.p;
+    a.bskf = ctx->br_mb > 1 ? ctx->d_bskf_mb.p : ctx->d_bskf.p;
+    a.mb = ctx->br_mb;
     a.tab = ctx->d_tab.p;
     a.ext = d_ext ? d_ext : ctx->d_ext.p;
     a.items = count;
@@ -712,13 +1026,18 @@ cbs_status cbs_gate_ragged_plan(cbs_gate_context* ctx, const cbs_gate_request* h
 cbs_status cbs_gate_ragged_launch(cbs_gate_context* ctx, cbs_stream_t stream) {
     CBS_CHECK_ARG(ctx, "gate_ragged_launch: null context");
     if (ctx->plan_items == 0) return CBS_OK;
+    if (ctx->br_mb > 1 && !ctx->mb_ready) {
+        set_error("gate_ragged_launch: grouped keys are not prepared");
+        return CBS_ERR_NOT_READY;
+    }
     const cbs_gate_params& p = ctx->p;
     cbs::GateArgs a{};
     a.gate = -1;
     a.n = p.n;
     a.levels = p.levels;
     a.bg_bits = p.bg_bits;
-    a.bskf = ctx->d_bskf.p;
+    a.bskf = ctx->br_mb > 1 ? ctx->d_bskf_mb.p : ctx->d_bskf.p;
+    a.mb = ctx->br_mb;
     a.tab = ctx->d_tab.p;
     a.ext = ctx->d_plan_ext.p;
     a.reqs = ctx->d_plan.p;

@@ -294,6 +294,12 @@ struct cbs_tcb_context {
     DevBuf<double2> d_bskf, d_tab;
     DevBuf<uint32_t> d_pfks;
     DevBuf<uint64_t> d_ext;
+    // grouped (multi-bit) level-2 blind rotation: mb, its keys (coefficient form), spectra
+    uint32_t br_mb = 1;
+    bool mb_ready = false;
+    uint64_t key_seed = 0;
+    std::vector<uint64_t> mbk2;
+    DevBuf<double2> d_bskf_mb;
 };
 
 namespace {
@@ -399,6 +405,57 @@ void tcb_keys_host(const cbs_tcb_params& p, uint64_t seed, std::vector<int32_t>&
     for (auto& t : pool) t.join();
 }
 
+// Grouped level-2 keys RGSW_z2(prod_{i in S} s0_i) on the 64-bit torus for every non-empty
+// subset S of each group of mb coefficients (row 2k + c adds the product times
+// 2^(64 - (k+1) bg2) to component c); one generator per row.
+void tcb_mb_keys_host(const cbs_tcb_params& p, const std::vector<int32_t>& s0, const std::vector<int32_t>& z2,
+                      uint32_t mb, uint64_t seed, std::vector<uint64_t>& out) {
+    const uint32_t n = p.n, N2 = p.N2, L = p.l2, K = cbs::mb_subsets(mb), groups = (n + mb - 1) / mb;
+    const size_t rows = static_cast<size_t>(groups) * K * 2 * L;
+    out.assign(rows * 2 * N2, 0);
+    cbs::BinaryPolyMul mz2(z2);
+    const unsigned nth = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    std::vector<std::thread> pool;
+    for (unsigned th = 0; th < nth; ++th)
+        pool.emplace_back([&, th] {
+            std::vector<uint64_t> prod(N2);
+            for (size_t r = th; r < rows; r += nth) {
+                cbs::Rng rr(mix(seed * 4 + 3) ^ mix(r));
+                uint64_t* ra = out.data() + r * 2 * N2;
+                uint64_t* rb = ra + N2;
+                for (uint32_t e = 0; e < N2; ++e) ra[e] = rr.next();
+                mz2.mul64(ra, prod.data());
+                for (uint32_t e = 0; e < N2; ++e)
+                    rb[e] = prod[e] + static_cast<uint64_t>(
+                                          std::llround(rr.gaussian() * p.sigma_lvl2 * 18446744073709551616.0));
+                const uint32_t g = static_cast<uint32_t>(r / (K * 2 * L));
+                const uint32_t kk = static_cast<uint32_t>((r / (2 * L)) % K), row = static_cast<uint32_t>(r % (2 * L));
+                const uint32_t mask = cbs::mb_subset_mask(mb, kk);
+                uint64_t prodb = 1;
+                for (uint32_t i = 0; i < mb; ++i)
+                    if (mask & (1u << i)) prodb &= (g * mb + i < n) ? static_cast<uint64_t>(s0[g * mb + i]) : 0u;
+                (row % 2 ? rb : ra)[0] += prodb << (64 - (row / 2 + 1) * p.bg2_bits);
+            }
+        });
+    for (auto& t : pool) t.join();
+}
+
+cbs_status tcb_prepare_mb(cbs_tcb_context* ctx) {
+    if (ctx->br_mb <= 1 || ctx->mb_ready || !ctx->keys_ready) return CBS_OK;
+    std::vector<double2> spec;
+    try {
+        tcb_mb_keys_host(ctx->p, ctx->s0, ctx->z2, ctx->br_mb, ctx->key_seed, ctx->mbk2);
+        cbs::torus_keys_to_fft(ctx->p.N2, ctx->mbk2.data(), ctx->mbk2.size() / ctx->p.N2, spec);
+    } catch (const std::exception& e) {
+        set_error(std::string("tcb multi-bit keys: ") + e.what());
+        return CBS_ERR_OOM;
+    }
+    CBS_CUDA_TRY(ctx->d_bskf_mb.upload(spec.data(), spec.size(), nullptr));
+    CBS_CUDA_TRY(cudaStreamSynchronize(nullptr));
+    ctx->mb_ready = true;
+    return CBS_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -473,6 +530,31 @@ cbs_status cbs_tcb_keygen(cbs_tcb_context* ctx, uint64_t seed) {
     CBS_CUDA_TRY(ctx->d_pfks.upload(ctx->pfks.data(), ctx->pfks.size(), nullptr));
     CBS_CUDA_TRY(cudaStreamSynchronize(nullptr));
     ctx->keys_ready = true;
+    ctx->key_seed = seed;
+    ctx->mb_ready = false;
+    return tcb_prepare_mb(ctx);
+}
+
+cbs_status cbs_tcb_set_multibit(cbs_tcb_context* ctx, uint32_t mb) {
+    CBS_CHECK_ARG(ctx, "tcb_set_multibit: null context");
+    CBS_CHECK_ARG(mb >= 1 && mb <= 3, "tcb_set_multibit: mb must be 1, 2 or 3");
+    if (mb != ctx->br_mb) {
+        ctx->br_mb = mb;
+        ctx->mb_ready = false;
+        ctx->mbk2.clear();
+        ctx->d_bskf_mb.reset();
+    }
+    return tcb_prepare_mb(ctx);
+}
+
+cbs_status cbs_tcb_export_mb_bsk(const cbs_tcb_context* ctx, uint64_t* out, size_t* words) {
+    CBS_CHECK_ARG(ctx && words, "tcb_export_mb_bsk: null argument");
+    if (ctx->br_mb <= 1 || !ctx->mb_ready) {
+        set_error("tcb_export_mb_bsk: no grouped keys (select mb > 1 after cbs_tcb_keygen)");
+        return CBS_ERR_NOT_READY;
+    }
+    *words = ctx->mbk2.size();
+    if (out) std::copy(ctx->mbk2.begin(), ctx->mbk2.end(), out);
     return CBS_OK;
 }
 
@@ -526,6 +608,10 @@ cbs_status cbs_tcb_circuit_bootstrap_device(cbs_tcb_context* ctx, const uint32_t
         return CBS_ERR_SHAPE_MISMATCH;
     }
     const cbs_tcb_params& p = ctx->p;
+    if (ctx->br_mb > 1 && !ctx->mb_ready) {
+        set_error("tcb_circuit_bootstrap: grouped keys are not prepared");
+        return CBS_ERR_NOT_READY;
+    }
     cbs::GateArgs a{};
     a.gate = -1;
     a.a1 = d_a;
@@ -533,7 +619,8 @@ cbs_status cbs_tcb_circuit_bootstrap_device(cbs_tcb_context* ctx, const uint32_t
     a.n = p.n;
     a.levels = p.l2;
     a.bg_bits = p.bg2_bits;
-    a.bskf = ctx->d_bskf.p;
+    a.bskf = ctx->br_mb > 1 ? ctx->d_bskf_mb.p : ctx->d_bskf.p;
+    a.mb = ctx->br_mb;
     a.tab = ctx->d_tab.p;
     a.ext = d_ext ? d_ext : ctx->d_ext.p;
     a.items = count * p.cb_levels;

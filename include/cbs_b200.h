@@ -301,6 +301,13 @@ cbs_status cbs_gate_params_default(cbs_gate_params *out);
 cbs_status cbs_gate_context_create(const cbs_gate_params *params, uint32_t max_batch, cbs_gate_context **out);
 cbs_status cbs_gate_context_destroy(cbs_gate_context *ctx);
 cbs_status cbs_gate_keygen(cbs_gate_context *ctx, uint64_t seed);
+/* Grouped (multi-bit) blind rotation for the gate / ragged paths, the torus form of the
+ * reference's CIRBTS_PBS_MULTIBIT grouping (bitwise/src/cirbts/cirbts-init.cu:376-530): mb = 1
+ * (default) or 2 / 3; the grouped keys RGSW_z(prod_{i in S} s_i) are generated from the
+ * context's secrets (now, or at the next cbs_gate_keygen).  cbs_gate_export_mb_bsk returns them
+ * [ceil(n/mb)][2^mb - 1][2*levels][2][N] (null out: only *words). */
+cbs_status cbs_gate_set_multibit(cbs_gate_context *ctx, uint32_t mb);
+cbs_status cbs_gate_export_mb_bsk(const cbs_gate_context *ctx, uint32_t *out, size_t *words);
 /* the same keys as cbs_gate_keygen(ctx, seed) on the host only (no device); NULL skips */
 cbs_status cbs_gate_generate_keys_host(const cbs_gate_params *params, uint64_t seed, int32_t *s_lwe, int32_t *z_rlwe,
                                        uint32_t *bsk, uint32_t *ksk);
@@ -378,6 +385,10 @@ cbs_status cbs_tcb_params_default(cbs_tcb_params *out);
 cbs_status cbs_tcb_context_create(const cbs_tcb_params *params, uint32_t max_batch, cbs_tcb_context **out);
 cbs_status cbs_tcb_context_destroy(cbs_tcb_context *ctx);
 cbs_status cbs_tcb_keygen(cbs_tcb_context *ctx, uint64_t seed);
+/* Grouped level-2 blind rotation (mb = 1, 2 or 3), as cbs_gate_set_multibit; keys on the
+ * 64-bit torus, [ceil(n/mb)][2^mb - 1][2*l2][2][N2]. */
+cbs_status cbs_tcb_set_multibit(cbs_tcb_context *ctx, uint32_t mb);
+cbs_status cbs_tcb_export_mb_bsk(const cbs_tcb_context *ctx, uint64_t *out, size_t *words);
 /* the same keys on the host only (no device); NULL skips an output */
 cbs_status cbs_tcb_generate_keys_host(const cbs_tcb_params *params, uint64_t seed, int32_t *s0, int32_t *z2,
                                       int32_t *z1, uint64_t *bsk2, uint32_t *pfks);

@@ -1031,6 +1031,133 @@ void orc_tcb_blind_rotate64(const orc_gate_params *p, const uint64_t *bsk, const
     free(acc);
 }
 
+/* Multi-bit (grouped) forms of the two torus blind rotations above, the reference's
+ * CIRBTS_PBS_MULTIBIT grouping (cirbts-init.cu:376-530, kernel.cu:4585-4771) on the torus:
+ * per group of mb coefficients, acc += sum_S m_S (acc (x) RGSW(prod_{i in S} s_i)) with
+ * m_S = prod_{i in S} (X^{a_i} - 1), subsets in the order of orc_mb_order2 / orc_mb_order3.
+ * mbk [ceil(n/mb)][2^mb - 1][2*levels][2][N].  Groups whose rotations are all 0 add nothing
+ * and are skipped. */
+static void torus_mono_minus1(uint32_t *p, uint32_t e, uint32_t N, uint32_t *tmp) {
+    memset(tmp, 0, N * sizeof(uint32_t));
+    torus_rot_add(tmp, p, e, N);
+    for (uint32_t i = 0; i < N; ++i) p[i] = tmp[i] - p[i];
+}
+
+void orc_gate_blind_rotate_tv_mb(const orc_gate_params *p, const uint32_t *mbk, uint32_t mb, const uint32_t *a,
+                                 uint32_t b, uint32_t mu, uint32_t b_add, uint32_t *ext) {
+    const uint32_t N = p->N, L = p->levels, two_n = 2 * N, K = (1u << mb) - 1u;
+    const uint32_t groups = (p->n + mb - 1) / mb;
+    const uint32_t *order = (mb == 2) ? orc_mb_order2 : orc_mb_order3;
+    uint32_t logn2 = 0;
+    while ((1u << logn2) < two_n) ++logn2;
+    const uint32_t sh = 32 - logn2;
+#define MS(x) ((uint32_t)(((x) + (1u << (sh - 1))) >> sh) & (two_n - 1))
+    uint32_t *acc = (uint32_t *)calloc(2 * N, sizeof(uint32_t));
+    uint32_t *prod = (uint32_t *)malloc(2 * N * sizeof(uint32_t));
+    uint32_t *tmp = (uint32_t *)malloc(N * sizeof(uint32_t));
+    int32_t *dig = (int32_t *)malloc((size_t)2 * L * N * sizeof(int32_t));
+    const uint32_t bt = MS(b);
+    for (uint32_t i = 0; i < N; ++i) acc[N + i] = ((i + bt) % two_n < N) ? mu : 0u - mu;
+    for (uint32_t g = 0; g < groups; ++g) {
+        uint32_t at[3] = {0, 0, 0}, any = 0;
+        for (uint32_t i = 0; i < mb; ++i) {
+            const uint32_t idx = g * mb + i;
+            at[i] = idx < p->n ? MS(a[idx]) : 0u;
+            any |= at[i];
+        }
+        if (!any) continue;
+        int32_t dd[8];
+        for (uint32_t c = 0; c < 2; ++c)
+            for (uint32_t i = 0; i < N; ++i) {
+                torus_decompose(acc[c * N + i], p->bg_bits, L, dd);
+                for (uint32_t k = 0; k < L; ++k) dig[((size_t)(2 * k + c)) * N + i] = dd[k];
+            }
+        for (uint32_t kk = 0; kk < K; ++kk) {
+            memset(prod, 0, 2 * N * sizeof(uint32_t));
+            const uint32_t *key = mbk + ((size_t)g * K + kk) * 2 * L * 2 * N;
+            for (uint32_t r = 0; r < 2 * L; ++r)
+                for (uint32_t c = 0; c < 2; ++c)
+                    torus_mac(prod + c * N, dig + (size_t)r * N, key + ((size_t)r * 2 + c) * N, N);
+            for (uint32_t i = 0; i < mb; ++i)
+                if (order[kk] & (1u << i))
+                    for (uint32_t c = 0; c < 2; ++c) torus_mono_minus1(prod + c * N, at[i], N, tmp);
+            for (uint32_t j = 0; j < 2 * N; ++j) acc[j] += prod[j];
+        }
+    }
+#undef MS
+    ext[0] = acc[0];
+    for (uint32_t i = 1; i < N; ++i) ext[i] = 0u - acc[N - i];
+    ext[N] = acc[N] + b_add;
+    free(dig);
+    free(tmp);
+    free(prod);
+    free(acc);
+}
+
+static void torus64_mono_minus1(uint64_t *p, uint32_t e, uint32_t N, uint64_t *tmp) {
+    memset(tmp, 0, N * sizeof(uint64_t));
+    for (uint32_t i = 0; i < N; ++i) {
+        const uint32_t t = (i + e) % (2 * N);
+        if (t < N) tmp[t] += p[i];
+        else tmp[t - N] -= p[i];
+    }
+    for (uint32_t i = 0; i < N; ++i) p[i] = tmp[i] - p[i];
+}
+
+void orc_tcb_blind_rotate64_mb(const orc_gate_params *p, const uint64_t *mbk, uint32_t mb, const uint32_t *a,
+                               uint32_t b, uint64_t mu, uint64_t b_add, uint64_t *ext) {
+    const uint32_t N = p->N, L = p->levels, two_n = 2 * N, bg = p->bg_bits, K = (1u << mb) - 1u;
+    const uint32_t groups = (p->n + mb - 1) / mb;
+    const uint32_t *order = (mb == 2) ? orc_mb_order2 : orc_mb_order3;
+    uint32_t logn2 = 0;
+    while ((1u << logn2) < two_n) ++logn2;
+    const uint32_t sh = 32 - logn2;
+#define MS(x) ((uint32_t)(((x) + (1u << (sh - 1))) >> sh) & (two_n - 1))
+    uint64_t *acc = (uint64_t *)calloc(2 * N, sizeof(uint64_t));
+    uint64_t *prod = (uint64_t *)malloc(2 * N * sizeof(uint64_t));
+    uint64_t *tmp = (uint64_t *)malloc(N * sizeof(uint64_t));
+    int32_t *dig = (int32_t *)malloc((size_t)2 * L * N * sizeof(int32_t));
+    uint64_t off = 1ull << (64 - L * bg - 1);
+    for (uint32_t k = 0; k < L; ++k) off += (1ull << (bg - 1)) << (64 - (k + 1) * bg);
+    const uint32_t bt = MS(b);
+    for (uint32_t i = 0; i < N; ++i) acc[N + i] = ((i + bt) % two_n < N) ? mu : 0ull - mu;
+    for (uint32_t g = 0; g < groups; ++g) {
+        uint32_t at[3] = {0, 0, 0}, any = 0;
+        for (uint32_t i = 0; i < mb; ++i) {
+            const uint32_t idx = g * mb + i;
+            at[i] = idx < p->n ? MS(a[idx]) : 0u;
+            any |= at[i];
+        }
+        if (!any) continue;
+        for (uint32_t c = 0; c < 2; ++c)
+            for (uint32_t i = 0; i < N; ++i) {
+                const uint64_t w = acc[c * N + i] + off;
+                for (uint32_t k = 0; k < L; ++k)
+                    dig[((size_t)(2 * k + c)) * N + i] =
+                        (int32_t)((w >> (64 - (k + 1) * bg)) & ((1u << bg) - 1)) - (int32_t)(1u << (bg - 1));
+            }
+        for (uint32_t kk = 0; kk < K; ++kk) {
+            memset(prod, 0, 2 * N * sizeof(uint64_t));
+            const uint64_t *key = mbk + ((size_t)g * K + kk) * 2 * L * 2 * N;
+            for (uint32_t r = 0; r < 2 * L; ++r)
+                for (uint32_t c = 0; c < 2; ++c)
+                    torus64_mac(prod + c * N, dig + (size_t)r * N, key + ((size_t)r * 2 + c) * N, N);
+            for (uint32_t i = 0; i < mb; ++i)
+                if (order[kk] & (1u << i))
+                    for (uint32_t c = 0; c < 2; ++c) torus64_mono_minus1(prod + c * N, at[i], N, tmp);
+            for (uint32_t j = 0; j < 2 * N; ++j) acc[j] += prod[j];
+        }
+    }
+#undef MS
+    ext[0] = acc[0];
+    for (uint32_t i = 1; i < N; ++i) ext[i] = 0ull - acc[N - i];
+    ext[N] = acc[N] + b_add;
+    free(dig);
+    free(tmp);
+    free(prod);
+    free(acc);
+}
+
 void orc_tcb_pfks(uint32_t N2, uint32_t N1, uint32_t base_bits, uint32_t levels, const uint32_t *key,
                   const uint64_t *ext, uint32_t *out) {
     const uint32_t base = 1u << base_bits;

@@ -163,6 +163,13 @@ void orc_gate_blind_rotate_tv(const orc_gate_params *p, const uint32_t *bsk, con
  * vector mu, b_add added to the extracted b: bsk [n][2*levels][2][N] u64, a/b level-0 torus32 */
 void orc_tcb_blind_rotate64(const orc_gate_params *p, const uint64_t *bsk, const uint32_t *a, uint32_t b,
                             uint64_t mu, uint64_t b_add, uint64_t *ext);
+/* Grouped (multi-bit, mb = 2 or 3) forms of the two torus blind rotations:
+ * mbk [ceil(n/mb)][2^mb - 1][2*levels][2][N], subsets {0} {1} {2} {0,1} {0,2} {1,2} {0,1,2}
+ * (mb = 3) or {0} {1} {0,1} (mb = 2). */
+void orc_gate_blind_rotate_tv_mb(const orc_gate_params *p, const uint32_t *mbk, uint32_t mb, const uint32_t *a,
+                                 uint32_t b, uint32_t mu, uint32_t b_add, uint32_t *ext);
+void orc_tcb_blind_rotate64_mb(const orc_gate_params *p, const uint64_t *mbk, uint32_t mb, const uint32_t *a,
+                               uint32_t b, uint64_t mu, uint64_t b_add, uint64_t *ext);
 /* private functional key switch of an extracted torus64 LWE (a[N2], b) into a torus32 RLWE of
  * dimension N1 (CGGI 2017 Alg. 2): key [N2+1][levels][base-1][2][N1] = RLWE(f(v * y_i *
  * 2^(32-(j+1)*base_bits))), y_i = key_i (i < N2), y_N2 = 1; digits of the top 32 bits of

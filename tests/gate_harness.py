@@ -22,6 +22,7 @@ def declare_gate(o):
     u32 = ctypes.c_uint32
     o.orc_gate_combine.argtypes = [ctypes.c_int, _U32P, u32, _U32P, u32, u32, _U32P, ctypes.POINTER(u32)]
     o.orc_gate_blind_rotate.argtypes = [ctypes.POINTER(OrcGateParams), _U32P, _U32P, u32, _U32P]
+    o.orc_gate_blind_rotate_tv_mb.argtypes = [ctypes.POINTER(OrcGateParams), _U32P, u32, _U32P, u32, u32, u32, _U32P]
     o.orc_gate_keyswitch.argtypes = [ctypes.POINTER(OrcGateParams), _U32P, _U32P, _U32P]
     return o
 
@@ -73,6 +74,20 @@ class OracleGate:
         def one(i):
             ext = np.zeros(N + 1, np.uint32)
             self.o.orc_gate_blind_rotate(ctypes.byref(self.op), bsk, np.ascontiguousarray(a[i]), int(b[i]), ext)
+            return ext
+
+        with ThreadPoolExecutor(self.threads) as ex:
+            return np.stack(list(ex.map(one, range(len(b)))))
+
+    def blind_rotate_mb(self, a, b, mbk, mb):
+        """Grouped (multi-bit) blind rotation with keys mbk, test vector 1/8."""
+        N = self.p.N
+        mbk = np.ascontiguousarray(mbk, np.uint32)
+
+        def one(i):
+            ext = np.zeros(N + 1, np.uint32)
+            self.o.orc_gate_blind_rotate_tv_mb(ctypes.byref(self.op), mbk, mb, np.ascontiguousarray(a[i]), int(b[i]),
+                                               1 << 29, 0, ext)
             return ext
 
         with ThreadPoolExecutor(self.threads) as ex:

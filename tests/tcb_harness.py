@@ -16,6 +16,7 @@ def declare_tcb(o):
     u64 = ctypes.c_uint64
     o.orc_tcb_blind_rotate64.argtypes = [ctypes.POINTER(OrcGateParams), _U64P, _U32P, u32, u64, u64, _U64P]
     o.orc_tcb_pfks.argtypes = [u32, u32, u32, u32, _U32P, _U64P, _U32P]
+    o.orc_tcb_blind_rotate64_mb.argtypes = [ctypes.POINTER(OrcGateParams), _U64P, u32, _U32P, u32, u64, u64, _U64P]
     return o
 
 
@@ -81,6 +82,24 @@ class OracleTcb:
             ext = np.zeros(p.N2 + 1, np.uint64)
             self.o.orc_tcb_blind_rotate64(ctypes.byref(self.op), bsk, np.ascontiguousarray(a[i]), int(b[i]), half,
                                           half, ext)
+            return ext
+
+        with ThreadPoolExecutor(self.threads) as ex:
+            out = list(ex.map(one, jobs))
+        return np.stack(out).reshape(len(b), p.cb_levels, p.N2 + 1)
+
+    def blind_rotate_mb(self, a, b, mbk, mb):
+        """Grouped (multi-bit) level-2 blind rotation with keys mbk: [count][levels][N2+1]."""
+        p = self.p
+        mbk = np.ascontiguousarray(mbk, np.uint64)
+        jobs = [(i, k) for i in range(len(b)) for k in range(p.cb_levels)]
+
+        def one(job):
+            i, k = job
+            half = 1 << (64 - (k + 1) * p.cb_bits - 1)
+            ext = np.zeros(p.N2 + 1, np.uint64)
+            self.o.orc_tcb_blind_rotate64_mb(ctypes.byref(self.op), mbk, mb, np.ascontiguousarray(a[i]), int(b[i]),
+                                             half, half, ext)
             return ext
 
         with ThreadPoolExecutor(self.threads) as ex:

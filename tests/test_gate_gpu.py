@@ -196,3 +196,42 @@ def test_ragged_two_parameter_sets_in_one_graph(pkg):
     del g
     for c in ctxs:
         c.close()
+
+
+@pytest.mark.parametrize("mb", [2, 3])
+def test_multibit_bootstrap_bit_exact(pkg, gctx, gkeys, mb):
+    """Grouped (multi-bit) gate blind rotation against the oracle's exact grouped rotation with
+    the same keys: the products stay below 2^52, so the FP64 result rounds to the exact one."""
+    p = gctx.params
+    gctx.set_multibit(mb)
+    try:
+        mbk = gctx.export_mb_bsk()
+        a, b = gctx.encrypt([1, 0, 1, 1], seed=40 + mb)
+        ext, oa, ob = _bootstrap(pkg, gctx, a, b)
+    finally:
+        gctx.set_multibit(1)
+    og = OracleGate(declare_gate(load_oracle()), p, gkeys)
+    want = og.blind_rotate_mb(a, b, mbk, mb)
+    assert np.array_equal(ext, want)
+    wa, wb = og.keyswitch(want)
+    assert np.array_equal(oa, wa) and np.array_equal(ob, wb)
+
+
+def test_multibit_nand_truth_table(pkg, gctx, gkeys):
+    p = gctx.params
+    rng = np.random.default_rng(12)
+    x = rng.integers(0, 2, 64).astype(np.uint8)
+    y = rng.integers(0, 2, 64).astype(np.uint8)
+    a1, b1 = gctx.encrypt(x, seed=13)
+    a2, b2 = gctx.encrypt(y, seed=14)
+    gctx.set_multibit(2)
+    try:
+        da1, db1, da2, db2 = _dev(a1), _dev(b1), _dev(a2), _dev(b2)
+        oa = torch.zeros((64, p.n), dtype=torch.int32, device="cuda")
+        ob = torch.zeros(64, dtype=torch.int32, device="cuda")
+        pkg.call("cbs_gate_eval_batch_device", gctx.handle, pkg.GATE_NAND, da1.data_ptr(), db1.data_ptr(),
+                 da2.data_ptr(), db2.data_ptr(), 64, oa.data_ptr(), ob.data_ptr(), None)
+        torch.cuda.synchronize()
+    finally:
+        gctx.set_multibit(1)
+    assert np.array_equal(gctx.decrypt(_host(oa), _host(ob)), 1 - (x & y))

@@ -105,3 +105,34 @@ def test_default_rows_and_cmux(pkg):
         ph = rlwe_phase(out, keys["z1"])
         assert abs(int(centered(ph[0] - m * (1 << 30)))) < 1 << 27  # within 1/32 of m/4
     ctx.close()
+
+
+@pytest.mark.parametrize("mb", [2, 3])
+def test_multibit_level2_parity_against_oracle(pkg, mb):
+    """Grouped (multi-bit) level-2 blind rotation against the oracle's exact grouped rotation:
+    the same FP64 digit-boundary argument as the one-bit test, and the PFKS rows it feeds decrypt
+    to m g_k / -m g_k z1."""
+    p = pkg.tcb_default_params()
+    p.n, p.N2, p.N1 = 64, 1024, 256
+    ctx = pkg.TcbContext(p, max_batch=4)
+    try:
+        ctx.keygen(23)
+        ctx.set_multibit(mb)
+        keys = ctx.export_keys(with_pfks=True)
+        mbk = ctx.export_mb_bsk()
+        bits = np.array([1, 0, 1], np.uint8)
+        a, b, ext, rgsw = _run(pkg, ctx, bits, 7)
+    finally:
+        ctx.close()
+    ot = OracleTcb(declare_tcb(load_oracle()), p, keys)
+    want = ot.blind_rotate_mb(a, b, mbk, mb)
+    for i, m in enumerate(int(x) for x in bits):
+        for k in range(p.cb_levels):
+            g = 2.0 ** (32 - (k + 1) * p.cb_bits)
+            ph_gpu = lwe64_phase_top(ext[i, k], keys["z2"])
+            ph_ref = lwe64_phase_top(want[i, k], keys["z2"])
+            assert abs(ph_gpu - ph_ref) < 2 ** 14
+            assert abs(ph_gpu - m * g) < 2 ** 14 and abs(ph_ref - m * g) < 2 ** 14
+    assert np.array_equal(rgsw, ot.pfks(ext))
+    err = rgsw_row_errors(rgsw, bits, keys["z1"], p.cb_bits, p.cb_levels)
+    assert np.max(np.abs(err)) < 2 ** 16
