@@ -276,6 +276,7 @@ cbs_status run_extract(cbs_context* c, const uint64_t* d_words_coef, const uint3
     a.words = d_words_coef;
     a.info = d_info;
     a.ksk = c->d_ksk.p;
+    a.ksk_stride = ksk_row_stride(c->p.n);
     a.out_a = d_out_a;
     a.out_b = d_out_b;
     a.out_stride = out_stride;
@@ -425,7 +426,14 @@ cbs_status cbs_keygen(cbs_context* ctx, uint64_t seed) {
     CBS_CUDA_TRY(c->d_bsk.upload(bsk_m.data(), bsk_m.size(), s));
     CBS_CUDA_TRY(c->d_ht.upload(ht_m.data(), ht_m.size(), s));
     CBS_CUDA_TRY(c->d_ss.upload(ss_m.data(), ss_m.size(), s));
-    CBS_CUDA_TRY(c->d_ksk.upload(c->hk.ksk.data(), c->hk.ksk.size(), s));
+    {
+        // device copy of the key-switching key with rows padded to ksk_row_stride(n) words
+        const size_t rows = c->hk.ksk.size() / (c->p.n + 1), stride = ksk_row_stride(c->p.n);
+        std::vector<uint16_t> padded(rows * stride, 0);
+        for (size_t r = 0; r < rows; ++r)
+            std::memcpy(padded.data() + r * stride, c->hk.ksk.data() + r * (c->p.n + 1), (c->p.n + 1) * sizeof(uint16_t));
+        CBS_CUDA_TRY(c->d_ksk.upload(padded.data(), padded.size(), s));
+    }
     CBS_CUDA_TRY(c->d_tv.upload(c->hk.tv.data(), c->hk.tv.size(), s));
     CBS_CUDA_TRY(c->d_gadd.upload(c->hk.gadd.data(), c->hk.gadd.size(), s));
     CBS_CUDA_TRY(c->d_maps.upload(c->hk.maps.data(), c->hk.maps.size(), s));

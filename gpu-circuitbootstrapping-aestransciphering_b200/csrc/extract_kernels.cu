@@ -5,9 +5,9 @@
 // word w (a'_j = a[idx-j], or -a[N+idx-j]), switch each coefficient Q -> qKS with the same
 // FP64 round-to-nearest expression (aes_gpu_ks.cuh:388-394), key-switch N -> n with two
 // base-2^k digits against the u16 key, and map qKS -> q (exact scale, or round-half-up
-// division when q is not a multiple of qKS, aes_gpu_ks.cuh:431-440).  One CTA per
-// (bit, 256-wide slice of the n+1 outputs); the mod-switched mask is staged through shared
-// memory 256 coefficients at a time; consecutive threads read consecutive key words.
+// division when q is not a multiple of qKS, aes_gpu_ks.cuh:431-440).  One CTA per output
+// bit, 4 outputs per thread; the mod-switched mask is staged in shared memory and
+// consecutive threads read consecutive 8-byte segments of a key row.
 #include "common.cuh"
 #include "extract_kernels.cuh"
 
@@ -23,61 +23,71 @@ __device__ __forceinline__ uint64_t qks_to_q(uint32_t v, uint64_t scale, uint32_
     return static_cast<uint64_t>(x / qks);
 }
 
-__global__ void __launch_bounds__(256) k_extract_keyswitch(const ExtractArgs a) {
-    const uint32_t t = blockIdx.y;
-    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t outlen = a.n + 1;
+// One CTA per output bit: the mod-switched mask (N u16) is staged in shared memory once, and
+// each thread accumulates 4 consecutive outputs from one 8-byte load per key row (rows padded
+// to a multiple of 4 words), unrolled so that 16 independent loads are in flight.
+constexpr uint32_t kExtractThreads = 256;
+
+__global__ void __launch_bounds__(kExtractThreads) k_extract_keyswitch(const ExtractArgs a) {
+    extern __shared__ uint16_t s_a[];  // [N]
+    const uint32_t t = blockIdx.x;
+    const uint32_t outlen = a.n + 1, stride = a.ksk_stride;
     const uint32_t info = __ldg(a.info + t);
     const uint32_t word = info >> 16, idx = info & 0xFFFFu;
     const uint64_t* aw = a.words + static_cast<size_t>(word) * 2 * a.N;
     const uint64_t* bw = aw + a.N;
-    const bool active = k < outlen;
-    uint32_t acc = 0;
-    if (active && k == a.n) acc = ms_pow2(bw[idx], a.q_over_Q, a.mask);
-
-    const uint32_t bmask = a.base_ks - 1;
-    const size_t stride_i = static_cast<size_t>(a.base_ks) * outlen;
-    const size_t stride_j = static_cast<size_t>(a.N) * stride_i;
-    __shared__ uint16_t s_a[256];
-    for (uint32_t tile = 0; tile < a.N; tile += 256) {
-        const uint32_t c = tile + threadIdx.x;
-        if (c < a.N) {
-            uint64_t v;
-            if (c <= idx) {
-                v = aw[idx - c];
-            } else {
-                const uint64_t x = aw[a.N + idx - c];
-                v = x ? a.Q - x : 0;
-            }
-            s_a[threadIdx.x] = static_cast<uint16_t>(ms_pow2(v, a.q_over_Q, a.mask));
+    for (uint32_t c = threadIdx.x; c < a.N; c += blockDim.x) {
+        uint64_t v;
+        if (c <= idx) {
+            v = aw[idx - c];
+        } else {
+            const uint64_t x = aw[a.N + idx - c];
+            v = x ? a.Q - x : 0;
         }
-        __syncthreads();
-        if (active) {
-            const uint32_t cnt = min(256u, a.N - tile);
-            const uint16_t* k0 = a.ksk + static_cast<size_t>(tile) * stride_i + k;
-            const uint16_t* k1 = k0 + stride_j;
-#pragma unroll 4
-            for (uint32_t j = 0; j < cnt; ++j) {
-                const uint32_t ai = s_a[j];
-                const uint32_t d0 = ai & bmask, d1 = (ai >> a.base_log2) & bmask;
-                acc -= static_cast<uint32_t>(__ldg(k0 + d0 * outlen)) + static_cast<uint32_t>(__ldg(k1 + d1 * outlen));
-                k0 += stride_i;
-                k1 += stride_i;
-            }
-        }
-        __syncthreads();
+        s_a[c] = static_cast<uint16_t>(ms_pow2(v, a.q_over_Q, a.mask));
     }
-    if (active) {
-        const uint64_t val = qks_to_q(acc & a.mask, a.scale, a.qks, a.q_lwe);
-        if (k == a.n) a.out_b[t] = val;
-        else a.out_a[static_cast<size_t>(t) * a.out_stride + k] = val;
+    __syncthreads();
+    const uint32_t bmask = a.base_ks - 1;
+    const size_t stride_i = static_cast<size_t>(a.base_ks) * stride;
+    const size_t stride_j = static_cast<size_t>(a.N) * stride_i;
+    for (uint32_t q = threadIdx.x; 4 * q < outlen; q += blockDim.x) {
+        uint32_t acc0 = 0, acc1 = 0, acc2 = 0, acc3 = 0;
+        const uint16_t* k0 = a.ksk + 4 * q;
+        const uint16_t* k1 = k0 + stride_j;
+#pragma unroll 8
+        for (uint32_t j = 0; j < a.N; ++j) {
+            const uint32_t ai = s_a[j];
+            const uint32_t d0 = ai & bmask, d1 = (ai >> a.base_log2) & bmask;
+            const uint2 u = __ldg(reinterpret_cast<const uint2*>(k0 + d0 * stride));
+            const uint2 v = __ldg(reinterpret_cast<const uint2*>(k1 + d1 * stride));
+            acc0 -= (u.x & 0xffffu) + (v.x & 0xffffu);
+            acc1 -= (u.x >> 16) + (v.x >> 16);
+            acc2 -= (u.y & 0xffffu) + (v.y & 0xffffu);
+            acc3 -= (u.y >> 16) + (v.y >> 16);
+            k0 += stride_i;
+            k1 += stride_i;
+        }
+        const uint32_t accs[4] = {acc0, acc1, acc2, acc3};
+#pragma unroll
+        for (uint32_t w = 0; w < 4; ++w) {
+            const uint32_t k = 4 * q + w;
+            if (k > a.n) break;
+            uint32_t accv = accs[w];
+            if (k == a.n) accv += ms_pow2(bw[idx], a.q_over_Q, a.mask);
+            const uint64_t val = qks_to_q(accv & a.mask, a.scale, a.qks, a.q_lwe);
+            if (k == a.n) a.out_b[t] = val;
+            else a.out_a[static_cast<size_t>(t) * a.out_stride + k] = val;
+        }
     }
 }
 
 cudaError_t launch_extract_keyswitch(const ExtractArgs& a, uint32_t count, cudaStream_t s) {
     if (count == 0) return cudaSuccess;
-    dim3 grid((a.n + 1 + 255) / 256, count);
-    k_extract_keyswitch<<<grid, 256, 0, s>>>(a);
+    if (a.ksk_stride % 4 != 0 || a.ksk_stride < a.n + 1) return cudaErrorInvalidValue;
+    // one thread per 4 outputs (158 at n = 630), rounded to whole warps
+    const uint32_t quads = a.ksk_stride / 4;
+    const uint32_t threads = quads >= kExtractThreads ? kExtractThreads : ((quads + 31) / 32) * 32;
+    k_extract_keyswitch<<<count, threads, a.N * sizeof(uint16_t), s>>>(a);
     return cudaGetLastError();
 }
 

@@ -10,7 +10,8 @@ namespace cbs {
 struct ExtractArgs {
     const uint64_t* words;  // [words][2][N] coefficient domain
     const uint32_t* info;   // [count] (word << 16) | coefficient
-    const uint16_t* ksk;    // [2][N][base_ks][n+1]
+    const uint16_t* ksk;    // [2][N][base_ks][ksk_stride] (rows of n + 1 words padded to a multiple of 4)
+    uint32_t ksk_stride;
     uint64_t* out_a;        // [count][out_stride]
     uint64_t* out_b;        // [count]
     uint32_t out_stride;
@@ -24,6 +25,8 @@ struct ExtractArgs {
 };
 
 cudaError_t launch_extract_keyswitch(const ExtractArgs& a, uint32_t count, cudaStream_t s);
+// row stride of the device key-switching key: n + 1 rounded up to a multiple of 4 words
+inline uint32_t ksk_row_stride(uint32_t n) { return (n + 1 + 3) & ~3u; }
 cudaError_t launch_init_state(uint64_t* out_a, uint64_t* out_b, const uint64_t* rk_a, const uint64_t* rk_b,
                               const uint8_t* bits, uint64_t half, uint64_t q, uint32_t n, uint32_t total,
                               cudaStream_t s);
