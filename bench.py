@@ -479,6 +479,19 @@ def run_rns_ntt(args, rank: int, world: int, local_rank: int) -> None:
     ctx.close()
 
 
+# external-product arithmetic of the torus-32 gate path (cbs_gate_set_fft_mode): key limbs
+# per key polynomial, bytes per spectrum value, and how the JSON line names it
+FFT_MODE_INFO = {
+    "fp64": {"limbs": 1, "bytes": 16, "fp": "fp64", "name": "FP64 FFT", "kernel": "k_gate_blind_rotate",
+             "dtype": "f64 (FFT products, exact after rounding) + u32 torus"},
+    "fp32-split": {"limbs": 2, "bytes": 8, "fp": "fp32", "name": "split-FP32 FFT",
+                   "kernel": "k_gate_blind_rotate_f32<LIMBS=2>",
+                   "dtype": "f32 (FFT products; keys split into a 24/25-bit and an exact 8/7-bit limb) + u32 torus"},
+    "fp32": {"limbs": 1, "bytes": 8, "fp": "fp32", "name": "FP32 FFT", "kernel": "k_gate_blind_rotate_f32<LIMBS=1>",
+             "dtype": "f32 (FFT products on whole keys, approximate) + u32 torus"},
+}
+
+
 def run_gate(args, rank: int, world: int, local_rank: int) -> None:
     """Plain gate bootstrapping (torus-32, n=636, N=1024, base 2^7 x 3, FP64 FFT): `--batch`
     NAND gates per step (default 64, the configuration's batch), inputs resident in HBM."""
@@ -489,6 +502,7 @@ def run_gate(args, rank: int, world: int, local_rank: int) -> None:
     ctx = pkg.GateContext(max_batch=count)
     ctx.keygen(args.seed)
     ctx.set_multibit(args.multibit)
+    ctx.set_fft_mode(args.fft_mode)
     p = ctx.params
     rng = np.random.default_rng(args.seed + rank)
     x = rng.integers(0, 2, count).astype(np.uint8)
@@ -522,26 +536,31 @@ def run_gate(args, rank: int, world: int, local_rank: int) -> None:
     e2e_ms = _timed(torch, stream, e2e, 1, max(1, args.steps))
     M = p.N // 2
     logm = M.bit_length() - 1
-    flop = count * p.n * ((2 * p.levels + 2) * 5 * M * logm + 2 * 2 * p.levels * M * 8)
-    key_bytes = p.n * 2 * p.levels * 2 * M * 16 + p.N * p.ks_levels * ((1 << p.ks_base_bits) - 1) * (p.n + 1) * 4
+    fm = FFT_MODE_INFO[args.fft_mode]
+    limbs, esize = fm["limbs"], fm["bytes"]
+    flop = count * p.n * ((2 * p.levels + 2 * limbs) * 5 * M * logm + 2 * 2 * p.levels * limbs * M * 8)
+    key_bytes = (p.n * 2 * p.levels * 2 * limbs * M * esize +
+                 p.N * p.ks_levels * ((1 << p.ks_base_bits) - 1) * (p.n + 1) * 4)
     peaks = measured_peaks()
     gbs = key_bytes / (ms * 1e-3) / 1e9
-    out = {"metric": f"NAND gate bootstraps/s (torus32, n={p.n}, N={p.N}, FP64 FFT)",
+    out = {"metric": f"NAND gate bootstraps/s (torus32, n={p.n}, N={p.N}, {fm['name']})",
            "value": world * count / (ms * 1e-3), "unit": "gates/s", "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-           "vs_baseline": None, "dtype": "f64 (FFT products, exact after rounding) + u32 torus",
+           "vs_baseline": None, "dtype": fm["dtype"],
            "data": "synthetic (seeded uniform random input bits)",
            "config": {"workload": "gate_nand", "batch": count, "n": p.n, "N": p.N, "br_multibit": args.multibit,
+                      "fft_mode": args.fft_mode,
                       "gadget": f"2^{p.bg_bits}x{p.levels}", "ks": f"2^{p.ks_base_bits}x{p.ks_levels}",
                       "l2": "keys (62 MB spectra + 62 MB KSK) stay L2/HBM resident; no flush"},
            "us_per_gate": ms * 1e3 / count, "correct_gates": ok, "gpu_launches": args.steps * 2,
            "e2e": {"value": world * count / (e2e_ms * 1e-3), "unit": "gates/s",
                    "h2d_bytes_per_step": 2 * count * (p.n + 1) * 4, "d2h_bytes_per_step": count * (p.n + 1) * 4},
-           "roofline": {"kernel": "k_gate_blind_rotate + k_gate_keyswitch", "bound": "hbm", "achieved": gbs,
+           "roofline": {"kernel": f"{fm['kernel']} + k_gate_keyswitch", "bound": "hbm", "achieved": gbs,
                         "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": gbs / peaks["hbm_gbs"],
                         "peak_src": peaks["src"], "traffic": None,
-                        "note": "key bytes once per step; the blind rotation is FP64-bound, see compute_rate"},
-           "compute_rate": {"fp64_flop_per_step": flop, "achieved_fp64_tflops": flop / (ms * 1e-3) / 1e12},
+                        "note": "key bytes once per step; the blind rotation is FP-pipe-bound, see compute_rate"},
+           "compute_rate": {f"{fm['fp']}_flop_per_step": flop,
+                            f"achieved_{fm['fp']}_tflops": flop / (ms * 1e-3) / 1e12},
            "clocks": clk.summary()}
     if rank == 0:
         print(json.dumps(out), flush=True)
@@ -565,6 +584,7 @@ def run_ragged(args, rank: int, world: int, local_rank: int) -> None:
     for i, c in enumerate(ctxs):
         c.keygen(args.seed + i)
         c.set_multibit(args.multibit)
+        c.set_fft_mode(args.fft_mode)
     rng = np.random.default_rng(args.seed + 5 + rank)
     reqs, bufs, total = [[], []], [], 0
     while total < total_min:
@@ -627,10 +647,10 @@ def run_ragged(args, rank: int, world: int, local_rank: int) -> None:
     out = {"metric": "ragged sign-bootstrap throughput (bootstraps/s, mixed N=1024/n=636 and N=2048/n=630)",
            "value": world * total / (ms * 1e-3), "unit": "bootstraps/s", "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-           "vs_baseline": None, "dtype": "f64 (FFT products, exact after rounding) + u32 torus",
+           "vs_baseline": None, "dtype": FFT_MODE_INFO[args.fft_mode]["dtype"],
            "data": "synthetic (seeded request sizes, parameter sets and bits)",
            "config": {"workload": "ragged_bootstrap", "requests": len(bufs), "bootstraps": total,
-                      "br_multibit": args.multibit,
+                      "br_multibit": args.multibit, "fft_mode": args.fft_mode,
                       "per_set": [sum(r[4] for r in reqs[0]), sum(r[4] for r in reqs[1])],
                       "l2": "keys of both sets (2 x ~125 MB) do not fit L2 together; no flush"},
            "correct": ok, "gpu_launches": args.steps * 4,
@@ -822,6 +842,10 @@ def main() -> None:
     ap.add_argument("--multibit", type=int, choices=[1, 2, 3], default=None,
                     help="blind rotation over groups of 1, 2 or 3 LWE coefficients (fft64 backend; "
                          "default 2 for fft64, 1 for ntt)")
+    ap.add_argument("--fft-mode", dest="fft_mode", choices=["fp64", "fp32-split", "fp32"], default="fp64",
+                    help="external-product arithmetic of --workload gate / ragged (torus-32): exact FP64, "
+                         "split FP32 (24/25-bit + exact top key limb), or FP32 on whole keys; FP32 modes use "
+                         "--multibit 1")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--workload", choices=["aes128", "blind_rotate", "keyswitch", "rns_ntt", "gate", "ragged", "tcb"], default="aes128",
                     help="aes128 is the headline; the others time one kernel family")
@@ -830,6 +854,12 @@ def main() -> None:
     ap.add_argument("--ntt-logn", dest="ntt_logn", type=int, default=16, help="log2 N for --workload rns_ntt")
     ap.add_argument("--limbs", type=int, default=24, help="limbs per polynomial for --workload rns_ntt")
     args = ap.parse_args()
+    if args.fft_mode != "fp64":
+        if args.workload not in ("gate", "ragged"):
+            ap.error("--fft-mode applies to --workload gate / ragged")
+        if args.multibit not in (None, 1):
+            ap.error("--fft-mode fp32* runs one coefficient per step (--multibit 1)")
+        args.multibit = 1
     if args.multibit is None:
         args.multibit = 2 if args.backend == "fft64" else 1
     if args.multibit > 1 and args.backend != "fft64":

@@ -104,6 +104,7 @@ def _declare(lib: ctypes.CDLL) -> None:
         "cbs_gate_context_destroy": (st, [c_vp]),
         "cbs_gate_keygen": (st, [c_vp, u64]),
         "cbs_gate_set_multibit": (st, [c_vp, u32]),
+        "cbs_gate_set_fft_mode": (st, [c_vp, u32]),
         "cbs_gate_export_mb_bsk": (st, [c_vp, c_vp, c_vp]),
         "cbs_gate_generate_keys_host": (st, [c_vp, u64, c_vp, c_vp, c_vp, c_vp]),
         "cbs_gate_export_keys": (st, [c_vp, c_vp, c_vp, c_vp, c_vp]),
@@ -290,6 +291,13 @@ class GateContext:
     def set_multibit(self, mb: int) -> None:
         """Blind rotation over groups of mb = 1, 2 or 3 LWE coefficients."""
         call("cbs_gate_set_multibit", self._h, mb)
+
+    FFT_MODES = {"fp64": 0, "fp32-split": 1, "fp32": 2}
+
+    def set_fft_mode(self, mode: str) -> None:
+        """External-product arithmetic: "fp64" (exact, default), "fp32-split" (FP32 transforms,
+        keys split into a 24-bit and an exact 8-bit limb) or "fp32" (FP32, whole keys)."""
+        call("cbs_gate_set_fft_mode", self._h, self.FFT_MODES[mode])
 
     def export_mb_bsk(self):
         """Grouped keys [ceil(n/mb)][2^mb - 1][2*levels][2][N] (uint32 torus)."""

@@ -33,24 +33,50 @@ __device__ __forceinline__ void cfma(double2& acc, double2 a, double2 b) {
     acc.x = fma(a.x, b.x, fma(-a.y, b.y, acc.x));
     acc.y = fma(a.x, b.y, fma(a.y, b.x, acc.y));
 }
+__device__ __forceinline__ double2 mul_i(double2 v) { return make_double2(-v.y, v.x); }
+__device__ __forceinline__ double2 mul_negi(double2 v) { return make_double2(v.y, -v.x); }
 
+// the same operations in FP32 (the split-FP32 external product of the 32-bit torus)
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csubd(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+    return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+}
+__device__ __forceinline__ float2 cmulc(float2 a, float2 b) {
+    return make_float2(fmaf(a.x, b.x, a.y * b.y), fmaf(a.y, b.x, -a.x * b.y));
+}
+__device__ __forceinline__ void cfma(float2& acc, float2 a, float2 b) {
+    acc.x = fmaf(a.x, b.x, fmaf(-a.y, b.y, acc.x));
+    acc.y = fmaf(a.x, b.y, fmaf(a.y, b.x, acc.y));
+}
+__device__ __forceinline__ float2 mul_i(float2 v) { return make_float2(-v.y, v.x); }
+__device__ __forceinline__ float2 mul_negi(float2 v) { return make_float2(v.y, -v.x); }
+
+// Shared-memory swizzles of the transform buffers.  16-byte elements: e ^ ((e >> 3) & 7)
+// makes every pass free of bank conflicts for M = 512 and 1024; 8-byte elements need the
+// four-bit form e ^ ((e >> 3) & 15) (both permute the low four bits only, so they stay
+// inside [0, M) and inside every aligned block of 16).
 __device__ __forceinline__ uint32_t cswz(uint32_t e) { return e ^ ((e >> 3) & 7u); }
+template <class C>
+__device__ __forceinline__ uint32_t cswz_of(uint32_t e) {
+    if constexpr (sizeof(C) == 8) return e ^ ((e >> 3) & 15u);
+    else return cswz(e);
+}
 
 // DIF butterfly: (u, v) -> (u + v, (u - v) * w)
-__device__ __forceinline__ void dif_bf(double2& u, double2& v, double2 w) {
-    const double2 s = cadd(u, v);
+template <class C>
+__device__ __forceinline__ void dif_bf(C& u, C& v, C w) {
+    const C s = cadd(u, v);
     v = cmul(csubd(u, v), w);
     u = s;
 }
 // DIT butterfly (inverse of the above up to a factor 2): (p, s) -> (p + s*conj(w), p - s*conj(w))
-__device__ __forceinline__ void dit_bf(double2& p, double2& s, double2 w) {
-    const double2 t = cmulc(s, w);
+template <class C>
+__device__ __forceinline__ void dit_bf(C& p, C& s, C w) {
+    const C t = cmulc(s, w);
     s = csubd(p, t);
     p = cadd(p, t);
 }
-
-__device__ __forceinline__ double2 mul_i(double2 v) { return make_double2(-v.y, v.x); }
-__device__ __forceinline__ double2 mul_negi(double2 v) { return make_double2(v.y, -v.x); }
 
 // Twiddle tables of one transform length, kept in shared memory by the kernels:
 //   [0, M/2)            tw[e] = exp(2*pi*i*e/M), read directly by the first pass (its index
@@ -82,21 +108,21 @@ struct FftTab {
 // DIF pass over R stages starting at DFT half-size h = M / (2m).  COMPACT: tb is the pass's
 // [k][j0] table; otherwise tb is tw, indexed directly.  Twiddles known to be 1 or i are
 // applied without multiplications.
-template <int LOGM, int R, bool COMPACT>
-__device__ __forceinline__ void dif_pass(double2 (&x)[8], uint32_t m, uint32_t tid, const double2* tb) {
+template <int LOGM, int R, bool COMPACT, class C>
+__device__ __forceinline__ void dif_pass(C (&x)[8], uint32_t m, uint32_t tid, const C* tb) {
     constexpr uint32_t M = 1u << LOGM;
     const uint32_t h = M / (2 * m);
     if (R == 3) {
         const uint32_t q = h / 4, j0 = tid % q;
         if (COMPACT && q == 1) {  // h = 4: stage 1 twiddles 1, w8, i, w8^3; stage 2 1, i; stage 3 1
             {
-                const double2 t = csubd(x[0], x[4]);
+                const C t = csubd(x[0], x[4]);
                 x[0] = cadd(x[0], x[4]);
                 x[4] = t;
             }
             dif_bf(x[1], x[5], tb[1]);
             {
-                const double2 t = mul_i(csubd(x[2], x[6]));
+                const C t = mul_i(csubd(x[2], x[6]));
                 x[2] = cadd(x[2], x[6]);
                 x[6] = t;
             }
@@ -104,7 +130,7 @@ __device__ __forceinline__ void dif_pass(double2 (&x)[8], uint32_t m, uint32_t t
             // stage 2: twiddle 1 on the slot pairs (0,2), (4,6) and i on (1,3), (5,7)
 #pragma unroll
             for (int g = 0; g < 8; g += 4) {
-                double2 t = csubd(x[g], x[g + 2]);
+                C t = csubd(x[g], x[g + 2]);
                 x[g] = cadd(x[g], x[g + 2]);
                 x[g + 2] = t;
                 t = mul_i(csubd(x[g + 1], x[g + 3]));
@@ -113,7 +139,7 @@ __device__ __forceinline__ void dif_pass(double2 (&x)[8], uint32_t m, uint32_t t
             }
 #pragma unroll
             for (int r = 0; r < 8; r += 2) {
-                const double2 t = csubd(x[r], x[r + 1]);
+                const C t = csubd(x[r], x[r + 1]);
                 x[r] = cadd(x[r], x[r + 1]);
                 x[r + 1] = t;
             }
@@ -123,19 +149,19 @@ __device__ __forceinline__ void dif_pass(double2 (&x)[8], uint32_t m, uint32_t t
         for (int r = 0; r < 4; ++r) dif_bf(x[r], x[r + 4], COMPACT ? tb[r * q + j0] : tb[(j0 + r * q) * m]);
 #pragma unroll
         for (int r = 0; r < 2; ++r) {
-            const double2 w = COMPACT ? tb[4 * q + r * q + j0] : tb[(j0 + r * q) * 2 * m];
+            const C w = COMPACT ? tb[4 * q + r * q + j0] : tb[(j0 + r * q) * 2 * m];
             dif_bf(x[r], x[r + 2], w);
             dif_bf(x[r + 4], x[r + 6], w);
         }
         if (COMPACT && q == 2) {  // h = 8: the last stage's twiddle is i^j0
 #pragma unroll
             for (int r = 0; r < 8; r += 2) {
-                const double2 t = csubd(x[r], x[r + 1]);
+                const C t = csubd(x[r], x[r + 1]);
                 x[r] = cadd(x[r], x[r + 1]);
                 x[r + 1] = j0 ? mul_i(t) : t;
             }
         } else {
-            const double2 w = COMPACT ? tb[6 * q + j0] : tb[j0 * 4 * m];
+            const C w = COMPACT ? tb[6 * q + j0] : tb[j0 * 4 * m];
 #pragma unroll
             for (int r = 0; r < 8; r += 2) dif_bf(x[r], x[r + 1], w);
         }
@@ -144,9 +170,9 @@ __device__ __forceinline__ void dif_pass(double2 (&x)[8], uint32_t m, uint32_t t
 #pragma unroll
         for (int hh = 0; hh < 2; ++hh) {
             const uint32_t j0 = (2 * tid + hh) % q;
-            double2* v = x + 4 * hh;
+            C* v = x + 4 * hh;
             if (COMPACT && q == 1) {  // twiddles 1, i, 1
-                double2 t = csubd(v[0], v[2]);
+                C t = csubd(v[0], v[2]);
                 v[0] = cadd(v[0], v[2]);
                 v[2] = t;
                 t = mul_i(csubd(v[1], v[3]));
@@ -161,7 +187,7 @@ __device__ __forceinline__ void dif_pass(double2 (&x)[8], uint32_t m, uint32_t t
             } else {
                 dif_bf(v[0], v[2], COMPACT ? tb[j0] : tb[j0 * m]);
                 dif_bf(v[1], v[3], COMPACT ? tb[q + j0] : tb[(j0 + q) * m]);
-                const double2 w = COMPACT ? tb[2 * q + j0] : tb[j0 * 2 * m];
+                const C w = COMPACT ? tb[2 * q + j0] : tb[j0 * 2 * m];
                 dif_bf(v[0], v[1], w);
                 dif_bf(v[2], v[3], w);
             }
@@ -170,7 +196,7 @@ __device__ __forceinline__ void dif_pass(double2 (&x)[8], uint32_t m, uint32_t t
 #pragma unroll
         for (int hh = 0; hh < 4; ++hh) {
             if (COMPACT && h == 1) {  // twiddle 1
-                const double2 t = csubd(x[2 * hh], x[2 * hh + 1]);
+                const C t = csubd(x[2 * hh], x[2 * hh + 1]);
                 x[2 * hh] = cadd(x[2 * hh], x[2 * hh + 1]);
                 x[2 * hh + 1] = t;
             } else {
@@ -181,8 +207,8 @@ __device__ __forceinline__ void dif_pass(double2 (&x)[8], uint32_t m, uint32_t t
     }
 }
 
-template <int LOGM, int R, bool COMPACT>
-__device__ __forceinline__ void dit_pass(double2 (&x)[8], uint32_t m, uint32_t tid, const double2* tb) {
+template <int LOGM, int R, bool COMPACT, class C>
+__device__ __forceinline__ void dit_pass(C (&x)[8], uint32_t m, uint32_t tid, const C* tb) {
     constexpr uint32_t M = 1u << LOGM;
     const uint32_t h = M / (2 * m);
     if (R == 3) {
@@ -190,13 +216,13 @@ __device__ __forceinline__ void dit_pass(double2 (&x)[8], uint32_t m, uint32_t t
         if (COMPACT && q == 1) {
 #pragma unroll
             for (int r = 0; r < 8; r += 2) {
-                const double2 t = x[r + 1];
+                const C t = x[r + 1];
                 x[r + 1] = csubd(x[r], t);
                 x[r] = cadd(x[r], t);
             }
 #pragma unroll
             for (int g = 0; g < 8; g += 4) {  // twiddle 1 on (0,2), (4,6); i (conjugated) on (1,3), (5,7)
-                double2 t = x[g + 2];
+                C t = x[g + 2];
                 x[g + 2] = csubd(x[g], t);
                 x[g] = cadd(x[g], t);
                 t = mul_negi(x[g + 3]);
@@ -204,13 +230,13 @@ __device__ __forceinline__ void dit_pass(double2 (&x)[8], uint32_t m, uint32_t t
                 x[g + 1] = cadd(x[g + 1], t);
             }
             {
-                const double2 t = x[4];
+                const C t = x[4];
                 x[4] = csubd(x[0], t);
                 x[0] = cadd(x[0], t);
             }
             dit_bf(x[1], x[5], tb[1]);
             {
-                const double2 t = mul_negi(x[6]);
+                const C t = mul_negi(x[6]);
                 x[6] = csubd(x[2], t);
                 x[2] = cadd(x[2], t);
             }
@@ -220,18 +246,18 @@ __device__ __forceinline__ void dit_pass(double2 (&x)[8], uint32_t m, uint32_t t
         if (COMPACT && q == 2) {
 #pragma unroll
             for (int r = 0; r < 8; r += 2) {
-                const double2 t = j0 ? mul_negi(x[r + 1]) : x[r + 1];
+                const C t = j0 ? mul_negi(x[r + 1]) : x[r + 1];
                 x[r + 1] = csubd(x[r], t);
                 x[r] = cadd(x[r], t);
             }
         } else {
-            const double2 w = COMPACT ? tb[6 * q + j0] : tb[j0 * 4 * m];
+            const C w = COMPACT ? tb[6 * q + j0] : tb[j0 * 4 * m];
 #pragma unroll
             for (int r = 0; r < 8; r += 2) dit_bf(x[r], x[r + 1], w);
         }
 #pragma unroll
         for (int r = 0; r < 2; ++r) {
-            const double2 w = COMPACT ? tb[4 * q + r * q + j0] : tb[(j0 + r * q) * 2 * m];
+            const C w = COMPACT ? tb[4 * q + r * q + j0] : tb[(j0 + r * q) * 2 * m];
             dit_bf(x[r], x[r + 2], w);
             dit_bf(x[r + 4], x[r + 6], w);
         }
@@ -242,9 +268,9 @@ __device__ __forceinline__ void dit_pass(double2 (&x)[8], uint32_t m, uint32_t t
 #pragma unroll
         for (int hh = 0; hh < 2; ++hh) {
             const uint32_t j0 = (2 * tid + hh) % q;
-            double2* v = x + 4 * hh;
+            C* v = x + 4 * hh;
             if (COMPACT && q == 1) {
-                double2 t = v[1];
+                C t = v[1];
                 v[1] = csubd(v[0], t);
                 v[0] = cadd(v[0], t);
                 t = v[3];
@@ -257,7 +283,7 @@ __device__ __forceinline__ void dit_pass(double2 (&x)[8], uint32_t m, uint32_t t
                 v[3] = csubd(v[1], t);
                 v[1] = cadd(v[1], t);
             } else {
-                const double2 w = COMPACT ? tb[2 * q + j0] : tb[j0 * 2 * m];
+                const C w = COMPACT ? tb[2 * q + j0] : tb[j0 * 2 * m];
                 dit_bf(v[0], v[1], w);
                 dit_bf(v[2], v[3], w);
                 dit_bf(v[0], v[2], COMPACT ? tb[j0] : tb[j0 * m]);
@@ -268,7 +294,7 @@ __device__ __forceinline__ void dit_pass(double2 (&x)[8], uint32_t m, uint32_t t
 #pragma unroll
         for (int hh = 0; hh < 4; ++hh) {
             if (COMPACT && h == 1) {
-                const double2 t = x[2 * hh + 1];
+                const C t = x[2 * hh + 1];
                 x[2 * hh + 1] = csubd(x[2 * hh], t);
                 x[2 * hh] = cadd(x[2 * hh], t);
             } else {
@@ -297,12 +323,11 @@ constexpr bool inv_exchange_in_warp(int p) {
 
 // Forward FFT of one folded, twisted polynomial by M/8 threads.  tab: the FftTab layout (in
 // shared memory); load(j, e) returns z_e for register slot j (e < M); on return x[j] holds
-// spectrum slot 8*tid + j.  sm: M double2 of shared memory, which the caller must not let
+// spectrum slot 8*tid + j.  sm: M elements of shared memory, which the caller must not let
 // other threads of the group still be reading when this is entered; bar() synchronises the
 // M/8 threads of the transform.
-template <int LOGM, class Load, class Bar>
-__device__ __forceinline__ void fft_forward_to_regs(double2* sm, uint32_t tid, const double2* tab, Load load,
-                                                    double2 (&x)[8], Bar bar) {
+template <int LOGM, class Load, class Bar, class C>
+__device__ __forceinline__ void fft_forward_to_regs(C* sm, uint32_t tid, const C* tab, Load load, C (&x)[8], Bar bar) {
     using Pl = NttPlan<LOGM>;
     using Tb = FftTab<LOGM>;
     static_assert(Pl::P >= 2, "fft needs M >= 64");
@@ -312,17 +337,17 @@ __device__ __forceinline__ void fft_forward_to_regs(double2* sm, uint32_t tid, c
 #pragma unroll
     for (int p = 1; p < Pl::P; ++p) {
 #pragma unroll
-        for (int j = 0; j < 8; ++j) sm[cswz(pass_index<LOGM, 3>(1u << (3 * (p - 1)), tid, j))] = x[j];
+        for (int j = 0; j < 8; ++j) sm[cswz_of<C>(pass_index<LOGM, 3>(1u << (3 * (p - 1)), tid, j))] = x[j];
         if (fwd_exchange_in_warp<LOGM>(p)) __syncwarp();
         else bar();
         const uint32_t m = 1u << (3 * p);
         if (p < Pl::P - 1) {
 #pragma unroll
-            for (int j = 0; j < 8; ++j) x[j] = sm[cswz(pass_index<LOGM, 3>(m, tid, j))];
+            for (int j = 0; j < 8; ++j) x[j] = sm[cswz_of<C>(pass_index<LOGM, 3>(m, tid, j))];
             dif_pass<LOGM, 3, true>(x, m, tid, tab + Tb::pass_off(p));
         } else {
 #pragma unroll
-            for (int j = 0; j < 8; ++j) x[j] = sm[cswz(pass_index<LOGM, Pl::tail_r>(m, tid, j))];
+            for (int j = 0; j < 8; ++j) x[j] = sm[cswz_of<C>(pass_index<LOGM, Pl::tail_r>(m, tid, j))];
             dif_pass<LOGM, Pl::tail_r, true>(x, m, tid, tab + Tb::pass_off(p));
         }
     }
@@ -333,29 +358,29 @@ __device__ __forceinline__ void fft_forward_to_regs(double2* sm, uint32_t tid, c
 // constant after unrolling, so callers can keep per-slot results in registers).  Same
 // shared-memory contract and barrier as the forward transform; on return other threads of
 // the group may still be reading sm.
-template <int LOGM, class Store, class Bar>
-__device__ __forceinline__ void fft_inverse_from_regs(double2* sm, uint32_t tid, const double2* tab, double2 (&x)[8],
-                                                      Store store, Bar bar) {
+template <int LOGM, class Store, class Bar, class C>
+__device__ __forceinline__ void fft_inverse_from_regs(C* sm, uint32_t tid, const C* tab, C (&x)[8], Store store,
+                                                      Bar bar) {
     using Pl = NttPlan<LOGM>;
     using Tb = FftTab<LOGM>;
     constexpr uint32_t mt = 1u << (3 * (Pl::P - 1));
     dit_pass<LOGM, Pl::tail_r, true>(x, mt, tid, tab + Tb::pass_off(Pl::P - 1));
 #pragma unroll
-    for (int j = 0; j < 8; ++j) sm[cswz(pass_index<LOGM, Pl::tail_r>(mt, tid, j))] = x[j];
+    for (int j = 0; j < 8; ++j) sm[cswz_of<C>(pass_index<LOGM, Pl::tail_r>(mt, tid, j))] = x[j];
     if (inv_exchange_in_warp<LOGM>(Pl::P - 2)) __syncwarp();
     else bar();
 #pragma unroll
     for (int p = Pl::P - 2; p >= 0; --p) {
         const uint32_t m = 1u << (3 * p);
 #pragma unroll
-        for (int j = 0; j < 8; ++j) x[j] = sm[cswz(pass_index<LOGM, 3>(m, tid, j))];
+        for (int j = 0; j < 8; ++j) x[j] = sm[cswz_of<C>(pass_index<LOGM, 3>(m, tid, j))];
         if (p == 0) dit_pass<LOGM, 3, false>(x, m, tid, tab);
         else dit_pass<LOGM, 3, true>(x, m, tid, tab + Tb::pass_off(p));
         if (p > 0) {
             // each pass reads and writes its own per-thread set and the sets partition [0, M), so
             // the write needs no barrier; the read of pass p - 1 does
 #pragma unroll
-            for (int j = 0; j < 8; ++j) sm[cswz(pass_index<LOGM, 3>(m, tid, j))] = x[j];
+            for (int j = 0; j < 8; ++j) sm[cswz_of<C>(pass_index<LOGM, 3>(m, tid, j))] = x[j];
             if (inv_exchange_in_warp<LOGM>(p - 1)) __syncwarp();
             else bar();
         }

@@ -67,11 +67,14 @@ __device__ __forceinline__ uint32_t gate_b(int gate, uint32_t x1, uint32_t x2) {
     }
 }
 
-template <int LOGM>
-__device__ __forceinline__ double2 gate_twist(const double2* tws, int j, uint32_t e) {
+template <int LOGM, class C>
+__device__ __forceinline__ C gate_twist(const C* tws, int j, uint32_t e) {
     if (j < 4) return tws[e];
-    const double2 t = tws[(1u << LOGM) - e];
-    return make_double2(t.y, t.x);
+    const C t = tws[(1u << LOGM) - e];
+    C r;
+    r.x = t.y;
+    r.y = t.x;
+    return r;
 }
 
 // the torus value of the FP64 result v of an integer-valued product: exact for 32-bit
@@ -236,6 +239,190 @@ __global__ void __launch_bounds__(GateCfg<LOGN>::T, GateCfg<LOGN>::MIN_BLOCKS) k
             if (i == N) v = acc[N] + b_add;
             else if (i == 0) v = acc[0];
             else v = TT(0) - acc[N - i];
+            out[i] = v;
+        }
+        __syncthreads();  // acc is re-initialised by the next item
+    }
+}
+
+// inputs of item `item` of a blind-rotation launch: the LWE rows a1 and a2 (a2 = a1 outside
+// gate mode) and the combined b
+__device__ __forceinline__ void gate_item_inputs(const GateArgs& a, uint32_t item, const uint32_t*& a1,
+                                                 const uint32_t*& a2, uint32_t& b) {
+    if (a.reqs) {  // ragged: one bootstrap of request r
+        const GateReq& rq = a.reqs[gate_req_of(a.reqs, a.num_reqs, item)];
+        const uint32_t k = item - rq.offset;
+        a1 = rq.a + static_cast<size_t>(k) * a.n;
+        a2 = a1;
+        b = rq.b[k];
+    } else {
+        const uint32_t in = item / a.levels_tv;
+        a1 = a.a1 + static_cast<size_t>(in) * a.n;
+        a2 = a.a2 ? a.a2 + static_cast<size_t>(in) * a.n : a1;
+        b = gate_b(a.gate, a.b1[in], a.b2 ? a.b2[in] : 0u);
+    }
+}
+
+// Split-FP32 form of k_gate_blind_rotate on the 32-bit torus (one coefficient per step).  The
+// transforms run in FP32.  Each key polynomial k is held as LIMBS FP32 spectra: LIMBS = 2
+// splits k = lo + 2^S hi (mod 2^32), S = log2 N + 14 (24 at N = 1024, 25 at N = 2048), into
+// its signed S-bit residue lo and the signed (32 - S)-bit hi; LIMBS = 1 keeps the centred k.
+// The three digit spectra of a half serve every limb; per limb the partial sums of the own
+// column are exchanged between the halves as in the FP64 kernel, inverse-transformed,
+// rounded to integers, and the limbs are recombined in 32-bit integers (lo + (hi << S)).
+// With digits |d| <= 2^6 the hi limb's sums stay near 2^18 in magnitude, far inside FP32's
+// 24-bit mantissa (FP32 error ~0.05 rms against the 0.5 that rounding tolerates), so they
+// round to the exact integers and the result differs from the exact product by the FP32
+// error of the lo limb alone (about 2^11 rms of the 2^32 torus per external product; about
+// 2^19 with LIMBS = 1).  This is the limb split of the reference's split-FFT backend
+// (bitwise/src/cirbts/cirbts-init.cu:1084-1140, FP64 limbs recombined with base powers mod
+// Q) carried to FP32 on the torus, where only the top limb has to be exact.
+template <int LOGN, int LIMBS>
+__global__ void __launch_bounds__(GateCfg<LOGN>::T, GateCfg<LOGN>::MIN_BLOCKS)
+    k_gate_blind_rotate_f32(const GateArgs a) {
+    constexpr int LOGM = LOGN - 1;
+    constexpr uint32_t N = 1u << LOGN, M = N / 2, TH = M / 8, T = 2 * TH, TWO_N = 2 * N;
+    constexpr uint32_t SH = 32 - (LOGN + 1);  // torus -> Z_2N
+    constexpr uint32_t SPLIT = LOGN + 14;     // lo limb bits
+    using Tb = FftTab<LOGM>;
+    extern __shared__ __align__(16) uint64_t smem[];
+    float2* fs = reinterpret_cast<float2*>(smem);                   // [2][LIMBS][M]
+    float2* tab = fs + 2 * LIMBS * M;                               // FftTab<LOGM> in FP32
+    uint32_t* acc = reinterpret_cast<uint32_t*>(tab + Tb::size());  // [2][N] torus values
+    uint32_t* dig = acc + 2 * N;                                    // [2][levels][M] packed pairs
+    const float2* tws = tab + Tb::twist_off();
+    const uint32_t tid = threadIdx.x, h = tid / TH, ht = tid % TH;
+    uint32_t* my_acc = acc + h * N;
+    float2* my_fs = fs + h * LIMBS * M;
+    const uint32_t levels = a.levels, bg = a.bg_bits, l2 = 2 * levels;
+    uint32_t off = 1u << (32 - levels * bg - 1);  // rounding of the dropped bits
+    for (uint32_t k = 0; k < levels; ++k) off += (1u << (bg - 1)) << (32 - (k + 1) * bg);
+    auto half_bar = [h]() {
+        if (h == 0) asm volatile("bar.sync 1, %0;" ::"n"(TH) : "memory");
+        else asm volatile("bar.sync 2, %0;" ::"n"(TH) : "memory");
+    };
+    auto ms = [](uint32_t x) { return ((x + (1u << (SH - 1))) >> SH) & (TWO_N - 1); };
+
+    for (uint32_t i = tid; i < Tb::size(); i += T) tab[i] = a.tab32[i];
+    for (uint32_t item = blockIdx.x; item < a.items; item += gridDim.x) {
+        const uint32_t* a1;
+        const uint32_t* a2;
+        uint32_t b;
+        gate_item_inputs(a, item, a1, a2, b);
+        const uint32_t mu = static_cast<uint32_t>(a.mu[item % a.levels_tv]);
+        const uint32_t b_add = static_cast<uint32_t>(a.b_add[item % a.levels_tv]);
+        {
+            const uint32_t bt = ms(b);
+            for (uint32_t i = tid; i < N; i += T) {
+                acc[i] = 0;
+                acc[N + i] = (((i + bt) & (TWO_N - 1)) < N) ? mu : 0u - mu;
+            }
+        }
+        __syncthreads();
+
+        for (uint32_t step = 0; step < a.n; ++step) {
+            const uint32_t at = ms(a.reqs ? __ldg(a1 + step) : gate_a(a.gate, __ldg(a1 + step), __ldg(a2 + step)));
+            if (at == 0) continue;  // X^0 - 1 = 0: the step adds nothing (uniform over the CTA)
+            for (uint32_t e = ht; e < M; e += TH) {
+                const uint32_t wr = my_acc[e] + off, wi = my_acc[e + M] + off;
+                uint32_t* dst = dig + h * levels * M + e;
+                for (uint32_t k = 0; k < levels; ++k) {
+                    const uint32_t s = 32 - (k + 1) * bg, mask = (1u << bg) - 1, half = 1u << (bg - 1);
+                    const int32_t dr = static_cast<int32_t>((wr >> s) & mask) - static_cast<int32_t>(half);
+                    const int32_t di = static_cast<int32_t>((wi >> s) & mask) - static_cast<int32_t>(half);
+                    dst[k * M] = (static_cast<uint32_t>(dr) & 0xffffu) | (static_cast<uint32_t>(di) << 16);
+                }
+            }
+            half_bar();
+            const float2* ek = a.bskf32 + static_cast<size_t>(step) * l2 * 2 * LIMBS * M + ht;
+            float2 y[2][LIMBS][8];
+#pragma unroll
+            for (int c = 0; c < 2; ++c)
+#pragma unroll
+                for (int l = 0; l < LIMBS; ++l)
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) y[c][l][j] = make_float2(0.f, 0.f);
+            for (uint32_t d = 0; d < levels; ++d) {
+                const uint32_t* dsrc = dig + (h * levels + d) * M;
+                float2 x[8];
+                fft_forward_to_regs<LOGM>(
+                    my_fs, ht, tab,
+                    [&](int j, uint32_t e) {
+                        const uint32_t v = dsrc[e];
+                        const float re = static_cast<float>(static_cast<int16_t>(v & 0xffffu));
+                        const float im = static_cast<float>(static_cast<int16_t>(v >> 16));
+                        return cmul(make_float2(re, im), gate_twist<LOGM>(tws, j, e));
+                    },
+                    x, half_bar);
+                const float2* kr = ek + static_cast<size_t>(2 * d + h) * 2 * LIMBS * M;  // [column][limb][M]
+#pragma unroll
+                for (int c = 0; c < 2; ++c)
+#pragma unroll
+                    for (int l = 0; l < LIMBS; ++l)
+#pragma unroll
+                        for (int j = 0; j < 8; ++j) cfma(y[c][l][j], x[j], __ldg(kr + (c * LIMBS + l) * M + j * TH));
+                half_bar();
+            }
+            // column 1 - h of every limb goes to the other half, column h stays
+#pragma unroll
+            for (int l = 0; l < LIMBS; ++l)
+#pragma unroll
+                for (int j = 0; j < 8; ++j) my_fs[l * M + cswz_of<float2>(8 * ht + j)] = h ? y[0][l][j] : y[1][l][j];
+            __syncthreads();
+            float2 z[LIMBS][8];
+            {
+                const float2* take = fs + (1 - h) * LIMBS * M;
+#pragma unroll
+                for (int l = 0; l < LIMBS; ++l)
+#pragma unroll
+                    for (int j = 0; j < 8; ++j)
+                        z[l][j] = cadd(h ? y[1][l][j] : y[0][l][j], take[l * M + cswz_of<float2>(8 * ht + j)]);
+            }
+            __syncthreads();
+            uint32_t tre[8], tim[8];
+            constexpr float inv_m = 1.0f / M;
+#pragma unroll
+            for (int l = 0; l < LIMBS; ++l) {
+                fft_inverse_from_regs<LOGM>(
+                    my_fs, ht, tab, z[l],
+                    [&](int j, uint32_t e, float2 v) {
+                        const float2 u = cmulc(v, gate_twist<LOGM>(tws, j, e));
+                        const uint32_t re = static_cast<uint32_t>(__float2ll_rn(u.x * inv_m));
+                        const uint32_t im = static_cast<uint32_t>(__float2ll_rn(u.y * inv_m));
+                        if (l == 0) {
+                            tre[j] = re;
+                            tim[j] = im;
+                        } else {
+                            tre[j] += re << SPLIT;
+                            tim[j] += im << SPLIT;
+                        }
+                    },
+                    half_bar);
+                half_bar();
+            }
+            uint32_t* tsm = reinterpret_cast<uint32_t*>(my_fs);  // N words (the buffer holds LIMBS * 8 M bytes)
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                tsm[ht + j * TH] = tre[j];
+                tsm[ht + j * TH + M] = tim[j];
+            }
+            half_bar();
+#pragma unroll 4
+            for (uint32_t k = 0; k < N / TH; ++k) {
+                const uint32_t i = ht + k * TH;
+                const uint32_t s = (i + TWO_N - at) & (TWO_N - 1);
+                const uint32_t v = (s < N) ? tsm[s] : 0u - tsm[s - N];
+                my_acc[i] += v - tsm[i];
+            }
+        }
+        __syncthreads();
+        // sample extract of coefficient 0: a'_0 = a_0, a'_i = -a_(N-i), b' = b_0
+        uint32_t* out = reinterpret_cast<uint32_t*>(a.ext) + static_cast<size_t>(item) * (N + 1);
+        for (uint32_t i = tid; i <= N; i += T) {
+            uint32_t v;
+            if (i == N) v = acc[N] + b_add;
+            else if (i == 0) v = acc[0];
+            else v = 0u - acc[N - i];
             out[i] = v;
         }
         __syncthreads();  // acc is re-initialised by the next item
@@ -511,8 +698,39 @@ static cudaError_t gate_br_mb_launch(const GateArgs& a, uint32_t grid, cudaStrea
     return cudaGetLastError();
 }
 
+template <int LOGN, int LIMBS>
+static cudaError_t gate_br_f32_launch(const GateArgs& a, uint32_t grid, cudaStream_t s) {
+    constexpr uint32_t N = 1u << LOGN, M = N / 2;
+    const size_t smem = (2ull * LIMBS * M + FftTab<LOGN - 1>::size()) * sizeof(float2) + 2ull * N * sizeof(uint32_t) +
+                        2ull * a.levels * M * sizeof(uint32_t);
+    static size_t configured[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (configured[dev] < smem) {
+        cudaError_t e = cudaFuncSetAttribute(k_gate_blind_rotate_f32<LOGN, LIMBS>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+        if (e != cudaSuccess) return e;
+        configured[dev] = smem;
+    }
+    k_gate_blind_rotate_f32<LOGN, LIMBS><<<grid, GateCfg<LOGN>::T, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
 template <typename TT>
 static cudaError_t gate_br_dispatch(const GateArgs& a, uint32_t N, uint32_t grid, cudaStream_t s) {
+    if (a.fft_mode != 0) {  // FP32 external products: 32-bit torus, one coefficient per step
+        if constexpr (std::is_same<TT, uint32_t>::value) {
+            if (a.mb > 1 || !a.bskf32 || !a.tab32) return cudaErrorInvalidValue;
+            if (a.fft_mode == 1) {
+                if (N == 1024) return gate_br_f32_launch<10, 2>(a, grid, s);
+                if (N == 2048) return gate_br_f32_launch<11, 2>(a, grid, s);
+            } else if (a.fft_mode == 2) {
+                if (N == 1024) return gate_br_f32_launch<10, 1>(a, grid, s);
+                if (N == 2048) return gate_br_f32_launch<11, 1>(a, grid, s);
+            }
+        }
+        return cudaErrorInvalidValue;
+    }
     if (a.mb <= 1) {
         if (N == 1024) return gate_br_launch<10, TT>(a, grid, s);
         if (N == 2048) return gate_br_launch<11, TT>(a, grid, s);
@@ -557,46 +775,97 @@ void mul_binary_acc(const uint32_t* a, const int32_t* z, uint32_t N, uint32_t* b
     }
 }
 
+using cld = std::complex<long double>;
+
+// tables of the host transform: w[e] = exp(2 pi i e / M) (e < M/2), twist[e] = exp(i pi e / N)
+template <int LOGM>
+static void host_fft_tables_ld(std::vector<cld>& w, std::vector<cld>& twist) {
+    constexpr uint32_t M = 1u << LOGM, N = 2 * M;
+    const long double pi = 3.141592653589793238462643383279502884L;
+    w.resize(M / 2);
+    twist.resize(M);
+    for (uint32_t e = 0; e < M / 2; ++e) w[e] = std::polar(1.0L, 2.0L * pi * e / M);
+    for (uint32_t e = 0; e < M; ++e) twist[e] = std::polar(1.0L, pi * e / N);
+}
+
+// folded transform of one real polynomial given by coef(e), e < N: zz[e] = (c_e + i c_(e+M))
+// zeta^e, then decimation in frequency (natural order in, bit-reversed out, the order of
+// fft_core.cuh's spectra before their slot-major placement (e % 8) * (M / 8) + e / 8)
+template <int LOGM, class Coef>
+static void host_fold_fft_ld(Coef coef, const std::vector<cld>& w, const std::vector<cld>& twist,
+                             std::vector<cld>& zz) {
+    constexpr uint32_t M = 1u << LOGM;
+    zz.resize(M);
+    for (uint32_t e = 0; e < M; ++e) zz[e] = cld(coef(e), coef(e + M)) * twist[e];
+    for (size_t hh = M / 2; hh >= 1; hh /= 2) {
+        const size_t stride = M / (2 * hh);
+        for (size_t s0 = 0; s0 < M; s0 += 2 * hh)
+            for (size_t j = 0; j < hh; ++j) {
+                const cld u = zz[s0 + j], v = zz[s0 + j + hh];
+                zz[s0 + j] = u + v;
+                zz[s0 + j + hh] = (u - v) * w[j * stride];
+            }
+        if (hh == 1) break;
+    }
+}
+
+template <class F>
+static void host_parallel_for(size_t count, F f) {
+    const unsigned nth = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    std::vector<std::thread> pool;
+    for (unsigned th = 0; th < nth; ++th)
+        pool.emplace_back([&, th] {
+            for (size_t k = th; k < count; k += nth) f(k);
+        });
+    for (auto& t : pool) t.join();
+}
+
 template <int LOGM, typename KT>
 static void torus_keys_to_fft_t(const KT* keys, size_t count, std::vector<double2>& out) {
     constexpr uint32_t M = 1u << LOGM, N = 2 * M;
-    using cld = std::complex<long double>;
-    const long double pi = 3.141592653589793238462643383279502884L;
-    std::vector<cld> w(M / 2), twist(M);
-    for (uint32_t e = 0; e < M / 2; ++e) w[e] = std::polar(1.0L, 2.0L * pi * e / M);
-    for (uint32_t e = 0; e < M; ++e) twist[e] = std::polar(1.0L, pi * e / N);
+    std::vector<cld> w, twist;
+    host_fft_tables_ld<LOGM>(w, twist);
     out.assign(count * M, make_double2(0, 0));
-    const unsigned nth = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
-    std::vector<std::thread> pool;
-    for (unsigned th = 0; th < nth; ++th) {
-        pool.emplace_back([&, th] {
-            std::vector<cld> zz(M);
-            for (size_t k = th; k < count; k += nth) {
-                const KT* c = keys + k * N;
-                using ST = typename std::make_signed<KT>::type;  // centred representative
-                for (uint32_t e = 0; e < M; ++e) {
-                    const long double re = static_cast<long double>(static_cast<ST>(c[e]));
-                    const long double im = static_cast<long double>(static_cast<ST>(c[e + M]));
-                    zz[e] = cld(re, im) * twist[e];
-                }
-                // decimation-in-frequency, natural order in, bit-reversed out (fft_core.cuh)
-                for (size_t hh = M / 2; hh >= 1; hh /= 2) {
-                    const size_t stride = M / (2 * hh);
-                    for (size_t s0 = 0; s0 < M; s0 += 2 * hh)
-                        for (size_t j = 0; j < hh; ++j) {
-                            const cld u = zz[s0 + j], v = zz[s0 + j + hh];
-                            zz[s0 + j] = u + v;
-                            zz[s0 + j + hh] = (u - v) * w[j * stride];
-                        }
-                    if (hh == 1) break;
-                }
-                for (uint32_t e = 0; e < M; ++e)
-                    out[k * M + (e % 8) * (M / 8) + e / 8] =
-                        make_double2(static_cast<double>(zz[e].real()), static_cast<double>(zz[e].imag()));
-            }
-        });
-    }
-    for (auto& t : pool) t.join();
+    using ST = typename std::make_signed<KT>::type;  // centred representative
+    host_parallel_for(count, [&](size_t k) {
+        thread_local std::vector<cld> zz;
+        const KT* c = keys + k * N;
+        host_fold_fft_ld<LOGM>([c](uint32_t e) { return static_cast<long double>(static_cast<ST>(c[e])); }, w, twist,
+                               zz);
+        for (uint32_t e = 0; e < M; ++e)
+            out[k * M + (e % 8) * (M / 8) + e / 8] =
+                make_double2(static_cast<double>(zz[e].real()), static_cast<double>(zz[e].imag()));
+    });
+}
+
+template <int LOGM>
+static void torus_keys_to_fft32_t(const uint32_t* keys, size_t count, uint32_t limbs, std::vector<float2>& out) {
+    constexpr uint32_t M = 1u << LOGM, N = 2 * M;
+    std::vector<cld> w, twist;
+    host_fft_tables_ld<LOGM>(w, twist);
+    out.assign(count * limbs * M, make_float2(0, 0));
+    constexpr uint32_t split = LOGM + 15;  // lo limb bits, log2 N + 14 (k_gate_blind_rotate_f32)
+    host_parallel_for(count * limbs, [&](size_t kl) {
+        thread_local std::vector<cld> zz;
+        const uint32_t* c = keys + (kl / limbs) * N;
+        const uint32_t l = static_cast<uint32_t>(kl % limbs);
+        auto coef = [c, l, limbs](uint32_t e) -> long double {
+            if (limbs == 1) return static_cast<long double>(static_cast<int32_t>(c[e]));
+            const int32_t lo = static_cast<int32_t>(c[e] << (32 - split)) >> (32 - split);  // signed residue
+            if (l == 0) return static_cast<long double>(lo);
+            return static_cast<long double>(static_cast<int32_t>(c[e] - static_cast<uint32_t>(lo)) >> split);
+        };
+        host_fold_fft_ld<LOGM>(coef, w, twist, zz);
+        for (uint32_t e = 0; e < M; ++e)
+            out[kl * M + (e % 8) * (M / 8) + e / 8] =
+                make_float2(static_cast<float>(zz[e].real()), static_cast<float>(zz[e].imag()));
+    });
+}
+
+void torus_keys_to_fft32(uint32_t N, const uint32_t* keys, size_t count, uint32_t limbs, std::vector<float2>& out) {
+    if (N == 1024) torus_keys_to_fft32_t<9>(keys, count, limbs, out);
+    else if (N == 2048) torus_keys_to_fft32_t<10>(keys, count, limbs, out);
+    else out.clear();
 }
 
 void torus_keys_to_fft(uint32_t N, const uint32_t* keys, size_t count, std::vector<double2>& out) {
@@ -645,6 +914,11 @@ struct cbs_gate_context {
     uint64_t key_seed = 0;
     std::vector<uint32_t> mbk;
     DevBuf<double2> d_bskf_mb;
+    // external-product arithmetic (CBS_FFT_*) and, for the FP32 modes, the key-limb spectra and
+    // the FP32 transform table
+    uint32_t fft_mode = CBS_FFT_FP64;
+    bool f32_ready = false;
+    DevBuf<float2> d_bskf32, d_tab32;
 };
 
 namespace {
@@ -804,6 +1078,49 @@ void gate_mb_keys_host(const cbs_gate_params& p, const std::vector<int32_t>& s, 
 
 constexpr uint64_t kGateMbSeedTweak = 0x67617465206d6275ull;
 
+// FP32 key-limb spectra of the one-bit keys and the FP32 copy of the transform table
+cbs_status gate_prepare_f32(cbs_gate_context* ctx) {
+    if (ctx->fft_mode == CBS_FFT_FP64 || ctx->f32_ready || !ctx->keys_ready) return CBS_OK;
+    const uint32_t limbs = ctx->fft_mode == CBS_FFT_FP32_SPLIT ? 2 : 1;
+    std::vector<float2> spec, tab32;
+    std::vector<double2> tab;
+    try {
+        cbs::torus_keys_to_fft32(ctx->p.N, ctx->bsk.data(), ctx->bsk.size() / ctx->p.N, limbs, spec);
+        cbs::fft_tables_host(ctx->p.N, tab);
+        tab32.resize(tab.size());
+        for (size_t i = 0; i < tab.size(); ++i)
+            tab32[i] = make_float2(static_cast<float>(tab[i].x), static_cast<float>(tab[i].y));
+    } catch (const std::exception& e) {
+        set_error(std::string("gate FP32 keys: ") + e.what());
+        return CBS_ERR_OOM;
+    }
+    CBS_CUDA_TRY(ctx->d_bskf32.upload(spec.data(), spec.size(), nullptr));
+    CBS_CUDA_TRY(ctx->d_tab32.upload(tab32.data(), tab32.size(), nullptr));
+    CBS_CUDA_TRY(cudaStreamSynchronize(nullptr));
+    ctx->f32_ready = true;
+    return CBS_OK;
+}
+
+// the arithmetic fields of the launch arguments; CBS_ERR_NOT_READY when the selected keys are
+// not prepared
+cbs_status gate_fill_keys(const cbs_gate_context* ctx, cbs::GateArgs& a) {
+    if (ctx->br_mb > 1 && !ctx->mb_ready) {
+        set_error("gate: grouped keys are not prepared");
+        return CBS_ERR_NOT_READY;
+    }
+    if (ctx->fft_mode != CBS_FFT_FP64 && !ctx->f32_ready) {
+        set_error("gate: FP32 key spectra are not prepared");
+        return CBS_ERR_NOT_READY;
+    }
+    a.bskf = ctx->br_mb > 1 ? ctx->d_bskf_mb.p : ctx->d_bskf.p;
+    a.mb = ctx->br_mb;
+    a.tab = ctx->d_tab.p;
+    a.fft_mode = ctx->fft_mode;
+    a.bskf32 = ctx->d_bskf32.p;
+    a.tab32 = ctx->d_tab32.p;
+    return CBS_OK;
+}
+
 cbs_status gate_prepare_mb(cbs_gate_context* ctx) {
     if (ctx->br_mb <= 1 || ctx->mb_ready || !ctx->keys_ready) return CBS_OK;
     std::vector<double2> spec;
@@ -827,6 +1144,8 @@ extern "C" {
 cbs_status cbs_gate_set_multibit(cbs_gate_context* ctx, uint32_t mb) {
     CBS_CHECK_ARG(ctx, "gate_set_multibit: null context");
     CBS_CHECK_ARG(mb >= 1 && mb <= 3, "gate_set_multibit: mb must be 1, 2 or 3");
+    CBS_CHECK_ARG(mb == 1 || ctx->fft_mode == CBS_FFT_FP64,
+                  "gate_set_multibit: the FP32 external products run one coefficient per step (mb = 1)");
     if (mb != ctx->br_mb) {
         ctx->br_mb = mb;
         ctx->mb_ready = false;
@@ -834,6 +1153,25 @@ cbs_status cbs_gate_set_multibit(cbs_gate_context* ctx, uint32_t mb) {
         ctx->d_bskf_mb.reset();
     }
     return gate_prepare_mb(ctx);
+}
+
+cbs_status cbs_gate_set_fft_mode(cbs_gate_context* ctx, uint32_t mode) {
+    CBS_CHECK_ARG(ctx, "gate_set_fft_mode: null context");
+    CBS_CHECK_ARG(mode == CBS_FFT_FP64 || mode == CBS_FFT_FP32_SPLIT || mode == CBS_FFT_FP32,
+                  "gate_set_fft_mode: mode must be CBS_FFT_FP64, CBS_FFT_FP32_SPLIT or CBS_FFT_FP32");
+    CBS_CHECK_ARG(mode == CBS_FFT_FP64 || ctx->br_mb <= 1,
+                  "gate_set_fft_mode: the FP32 external products run one coefficient per step (mb = 1)");
+    // the split's top limb times a digit, summed over N terms, must stay far inside the 24-bit
+    // FP32 mantissa for its rounding to be exact: digits of at most 7 bits
+    CBS_CHECK_ARG(mode != CBS_FFT_FP32_SPLIT || ctx->p.bg_bits <= 7,
+                  "gate_set_fft_mode: split FP32 needs bg_bits <= 7");
+    if (mode != ctx->fft_mode) {
+        ctx->fft_mode = mode;
+        ctx->f32_ready = false;
+        ctx->d_bskf32.reset();
+        ctx->d_tab32.reset();
+    }
+    return gate_prepare_f32(ctx);
 }
 
 cbs_status cbs_gate_export_mb_bsk(const cbs_gate_context* ctx, uint32_t* out, size_t* words) {
@@ -881,6 +1219,8 @@ cbs_status cbs_gate_keygen(cbs_gate_context* ctx, uint64_t seed) {
     ctx->keys_ready = true;
     ctx->key_seed = seed;
     ctx->mb_ready = false;
+    ctx->f32_ready = false;
+    if (cbs_status st = gate_prepare_f32(ctx)) return st;
     return gate_prepare_mb(ctx);
 }
 
@@ -948,12 +1288,9 @@ static cbs_status gate_run(cbs_gate_context* ctx, int gate, const uint32_t* d_a1
         set_error("gate: count above the context's max_batch");
         return CBS_ERR_SHAPE_MISMATCH;
     }
-    if (ctx->br_mb > 1 && !ctx->mb_ready) {
-        set_error("gate: grouped keys are not prepared");
-        return CBS_ERR_NOT_READY;
-    }
     const cbs_gate_params& p = ctx->p;
     cbs::GateArgs a{};
+    if (cbs_status st = gate_fill_keys(ctx, a)) return st;
     a.gate = gate;
     a.a1 = d_a1;
     a.b1 = d_b1;
@@ -962,9 +1299,6 @@ static cbs_status gate_run(cbs_gate_context* ctx, int gate, const uint32_t* d_a1
     a.n = p.n;
     a.levels = p.levels;
     a.bg_bits = p.bg_bits;
-    a.bskf = ctx->br_mb > 1 ? ctx->d_bskf_mb.p : ctx->d_bskf.p;
-    a.mb = ctx->br_mb;
-    a.tab = ctx->d_tab.p;
     a.ext = d_ext ? d_ext : ctx->d_ext.p;
     a.items = count;
     a.levels_tv = 1;
@@ -1026,19 +1360,13 @@ cbs_status cbs_gate_ragged_plan(cbs_gate_context* ctx, const cbs_gate_request* h
 cbs_status cbs_gate_ragged_launch(cbs_gate_context* ctx, cbs_stream_t stream) {
     CBS_CHECK_ARG(ctx, "gate_ragged_launch: null context");
     if (ctx->plan_items == 0) return CBS_OK;
-    if (ctx->br_mb > 1 && !ctx->mb_ready) {
-        set_error("gate_ragged_launch: grouped keys are not prepared");
-        return CBS_ERR_NOT_READY;
-    }
     const cbs_gate_params& p = ctx->p;
     cbs::GateArgs a{};
+    if (cbs_status st = gate_fill_keys(ctx, a)) return st;
     a.gate = -1;
     a.n = p.n;
     a.levels = p.levels;
     a.bg_bits = p.bg_bits;
-    a.bskf = ctx->br_mb > 1 ? ctx->d_bskf_mb.p : ctx->d_bskf.p;
-    a.mb = ctx->br_mb;
-    a.tab = ctx->d_tab.p;
     a.ext = ctx->d_plan_ext.p;
     a.reqs = ctx->d_plan.p;
     a.num_reqs = ctx->plan_reqs;

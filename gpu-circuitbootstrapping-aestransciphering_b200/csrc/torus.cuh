@@ -44,6 +44,11 @@ struct GateArgs {
     // 0 or 1: one coefficient per step (bskf [n][2*levels][2][M]); 2 or 3: groups of mb
     // coefficients (bskf [ceil(n/mb)][2^mb - 1][2*levels][2][M], the grouped kernel)
     uint32_t mb;
+    // external-product arithmetic (CBS_FFT_*): 0 FP64 (bskf, tab); 1 split FP32, 2 FP32 (32-bit
+    // torus, mb <= 1): bskf32 [n][2*levels][2][limbs][M] key-limb spectra, tab32 the FP32 table
+    uint32_t fft_mode;
+    const float2* bskf32;
+    const float2* tab32;
 };
 
 cudaError_t gate_blind_rotate(const GateArgs& a, uint32_t N, uint32_t grid, cudaStream_t s);    // 32-bit torus
@@ -59,5 +64,9 @@ void mul_binary_acc(const uint32_t* a, const int32_t* z, uint32_t N, uint32_t* b
 // the blind-rotation kernels
 void torus_keys_to_fft(uint32_t N, const uint32_t* keys, size_t count, std::vector<double2>& out);
 void torus_keys_to_fft(uint32_t N, const uint64_t* keys, size_t count, std::vector<double2>& out);
+// FP32 form: each torus32 polynomial as `limbs` spectra [count][limbs][N/2]; limbs = 2 splits
+// k = lo + 2^S hi, S = log2 N + 14, with lo the signed S-bit residue and hi the signed
+// (32 - S)-bit rest; limbs = 1 keeps the centred k
+void torus_keys_to_fft32(uint32_t N, const uint32_t* keys, size_t count, uint32_t limbs, std::vector<float2>& out);
 
 }  // namespace cbs

@@ -308,6 +308,19 @@ cbs_status cbs_gate_keygen(cbs_gate_context *ctx, uint64_t seed);
  * [ceil(n/mb)][2^mb - 1][2*levels][2][N] (null out: only *words). */
 cbs_status cbs_gate_set_multibit(cbs_gate_context *ctx, uint32_t mb);
 cbs_status cbs_gate_export_mb_bsk(const cbs_gate_context *ctx, uint32_t *out, size_t *words);
+/* Arithmetic of the external product in the gate / ragged blind rotation:
+ *   CBS_FFT_FP64        FP64 transforms; every product rounds to the exact integer (default);
+ *   CBS_FFT_FP32_SPLIT  FP32 transforms, keys split k = lo + 2^S hi (S = log2 N + 14: a 24- or
+ *                       25-bit lo and a 7- or 8-bit hi limb), recombined in integers; the hi
+ *                       limb is exact, the lo limb leaves ~2^11 rms of FP32 error per product
+ *                       on the 2^32 torus;
+ *   CBS_FFT_FP32        FP32 transforms on the whole key (~2^19 rms per product; the phase
+ *                       error of a bootstrap then reaches the gate margin: comparison only).
+ * The FP32 modes need mb = 1; split FP32 needs bg_bits <= 7.
+ * This is the limb split of the reference's split-FFT backend (bitwise/src/cirbts/
+ * cirbts-init.cu:1084-1140, FP64 there) in FP32 on the 32-bit torus. */
+enum { CBS_FFT_FP64 = 0, CBS_FFT_FP32_SPLIT = 1, CBS_FFT_FP32 = 2 };
+cbs_status cbs_gate_set_fft_mode(cbs_gate_context *ctx, uint32_t mode);
 /* the same keys as cbs_gate_keygen(ctx, seed) on the host only (no device); NULL skips */
 cbs_status cbs_gate_generate_keys_host(const cbs_gate_params *params, uint64_t seed, int32_t *s_lwe, int32_t *z_rlwe,
                                        uint32_t *bsk, uint32_t *ksk);
