@@ -85,6 +85,8 @@ def _declare(lib: ctypes.CDLL) -> None:
         "cbs_export_mb_bsk": (st, [c_vp, c_vp, c_vp]),
         "cbs_generate_mb_bsk_host": (st, [c_vp, u64, u32, c_vp, c_vp]),
         "cbs_export_keys": (st, [c_vp] + [c_vp] * 9),
+        "cbs_import_keys": (st, [c_vp] + [c_vp] * 6),
+        "cbs_import_mb_bsk": (st, [c_vp, u32, c_vp, sz]),
         "cbs_generate_keys_host": (st, [c_vp, u64] + [c_vp] * 9),
         "cbs_context_tables": (st, [c_vp] + [c_vp] * 7),
         "cbs_blind_rotate_batch_device": (st, [c_vp, c_vp, c_vp, u32, u32, c_vp, c_vp]),
@@ -94,6 +96,7 @@ def _declare(lib: ctypes.CDLL) -> None:
         "cbs_extract_keyswitch_device": (st, [c_vp, c_vp, u32, c_vp, u32, c_vp, c_vp, u32, c_vp]),
         "cbs_aes128_setup": (st, [c_vp, c_vp, u64]),
         "cbs_aes128_export_material": (st, [c_vp, c_vp, c_vp, c_vp, c_vp]),
+        "cbs_aes128_import_material": (st, [c_vp, c_vp, c_vp, c_vp, c_vp]),
         "cbs_aes128_ctr_transcipher_device": (st, [c_vp, c_vp, u32, c_vp, c_vp, ctypes.c_int, c_vp]),
         "cbs_aes128_ctr_transcipher": (st, [c_vp, c_vp, u32, c_vp, c_vp]),
         "cbs_lwe_decrypt_bits": (st, [c_vp, c_vp, c_vp, u32, u32, c_vp]),
@@ -216,6 +219,38 @@ class Context:
         out = key_buffers(self.params)
         call("cbs_export_keys", self._h, *(out[k].ctypes.data for k in KEY_FIELDS))
         return out
+
+    def import_keys(self, keys: dict, with_secrets: bool = True) -> None:
+        """Load evaluation keys (the dict of export_keys / generate_keys_host) instead of
+        keygen; with_secrets=False leaves the context without s_lwe / s_rlwe."""
+        import numpy as np
+        arr = {k: np.ascontiguousarray(keys[k]) for k in ("bsk", "ht", "ss", "ksk")}
+        sec = [None, None]
+        if with_secrets:
+            sec = [np.ascontiguousarray(keys["s_lwe"], np.int32), np.ascontiguousarray(keys["s_rlwe"], np.int32)]
+        call("cbs_import_keys", self._h, *(None if v is None else v.ctypes.data for v in sec),
+             *(arr[k].ctypes.data for k in ("bsk", "ht", "ss", "ksk")))
+
+    def import_mb_bsk(self, mb: int, keys) -> None:
+        """Grouped keys in the layout of export_mb_bsk (selects mb)."""
+        import numpy as np
+        keys = np.ascontiguousarray(keys, np.uint64)
+        call("cbs_import_mb_bsk", self._h, mb, keys.ctypes.data, keys.size)
+
+    def aes_export_material(self) -> dict:
+        """Encrypted AES material of cbs_aes128_setup: tables, rk_words, rk0_a, rk0_b."""
+        import numpy as np
+        p = self.params
+        out = {"tables": np.zeros(8 * 256 * 2 * p.N, np.uint64), "rk_words": np.zeros(11 * 4 * 2 * p.N, np.uint64),
+               "rk0_a": np.zeros(128 * p.n, np.uint64), "rk0_b": np.zeros(128, np.uint64)}
+        call("cbs_aes128_export_material", self._h, *(out[k].ctypes.data for k in ("tables", "rk_words", "rk0_a",
+                                                                                   "rk0_b")))
+        return out
+
+    def aes_import_material(self, m: dict) -> None:
+        import numpy as np
+        arr = [np.ascontiguousarray(m[k], np.uint64) for k in ("tables", "rk_words", "rk0_a", "rk0_b")]
+        call("cbs_aes128_import_material", self._h, *(a.ctypes.data for a in arr))
 
     def set_br_backend(self, backend: int) -> None:
         call("cbs_context_set_br_backend", self._h, backend)

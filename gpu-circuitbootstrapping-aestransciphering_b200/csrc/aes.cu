@@ -27,12 +27,7 @@ static constexpr uint32_t kAesMaxChunkBlocks = 256;
 static cbs_status aes_prepare_chunk(cbs_context* c, uint32_t chunk) {
     AesState& A = c->aes;
     if (A.chunk_blocks >= chunk && A.ctr_bits.p) return CBS_OK;
-    for (auto& g : A.graphs)
-        if (g) {
-            cudaGraphExecDestroy(g);
-            g = nullptr;
-        }
-    A.graph_chunk = 0;
+    A.drop_graphs();
     const size_t N = c->p.N, n = c->p.n, L = c->p.num_lut;
     const size_t T = static_cast<size_t>(chunk) * 128, luts = static_cast<size_t>(chunk) * 16;
     CBS_CUDA_TRY(A.ctr_bits.alloc(T));
@@ -113,11 +108,7 @@ static cbs_status aes_run_rounds(cbs_context* c, uint32_t chunk, cudaStream_t s,
         return CBS_OK;
     }
     if (A.graph_chunk != chunk) {
-        for (auto& g : A.graphs)
-            if (g) {
-                cudaGraphExecDestroy(g);
-                g = nullptr;
-            }
+        A.drop_graphs();
         // this call runs eagerly (which also configures every kernel outside a capture);
         // the captured graphs serve the following calls
         for (uint32_t r = 1; r <= 10; ++r)
@@ -149,10 +140,36 @@ using namespace cbs;
 
 extern "C" {
 
+// upload the host AES material of A (tables, round-key words, round-0 key bits) and derive
+// the coefficient-domain copies of the FFT path
+static cbs_status aes_upload_material(cbs_context* c) {
+    AesState& A = c->aes;
+    const uint32_t N = c->p.N;
+    cudaStream_t s = c->stream;
+    CBS_CUDA_TRY(A.tables.upload(A.h_tables.data(), A.h_tables.size(), s));
+    CBS_CUDA_TRY(A.rk_words.upload(A.h_rk_words.data(), A.h_rk_words.size(), s));
+    CBS_CUDA_TRY(A.rk0_a.upload(A.h_rk0_a.data(), A.h_rk0_a.size(), s));
+    CBS_CUDA_TRY(A.rk0_b.upload(A.h_rk0_b.data(), A.h_rk0_b.size(), s));
+    CBS_CUDA_TRY(A.tables_coef.alloc(A.h_tables.size()));
+    CBS_CUDA_TRY(A.rk_words_coef.alloc(A.h_rk_words.size()));
+    CBS_CUDA_TRY(ntt_inverse(A.tables_coef.p, A.tables.p, nullptr, c->d_irp.p, c->d_irps.p, c->d_mod.p, c->d_ninv.p,
+                             c->d_ninv_s.p, N, A.h_tables.size() / N, s));
+    CBS_CUDA_TRY(ntt_inverse(A.rk_words_coef.p, A.rk_words.p, nullptr, c->d_irp.p, c->d_irps.p, c->d_mod.p,
+                             c->d_ninv.p, c->d_ninv_s.p, N, A.h_rk_words.size() / N, s));
+    CBS_CUDA_TRY(cudaStreamSynchronize(s));
+    A.ready = true;
+    return CBS_OK;
+}
+
 cbs_status cbs_aes128_setup(cbs_context* ctx, const uint8_t* key, uint64_t seed) {
     CBS_CHECK_ARG(ctx && key, "aes_setup: null argument");
     if (!ctx->keys_ready) {
         set_error("aes_setup: no key material (call cbs_keygen first)");
+        return CBS_ERR_NOT_READY;
+    }
+    if (!ctx->has_secret) {
+        set_error("aes_setup: encrypting the AES material needs the secret key; the key owner's "
+                  "cbs_aes128_export_material output loads with cbs_aes128_import_material");
         return CBS_ERR_NOT_READY;
     }
     cbs_context* c = ctx;
@@ -193,20 +210,38 @@ cbs_status cbs_aes128_setup(cbs_context* ctx, const uint8_t* key, uint64_t seed)
         lwe_encrypt(c->p, c->hk, rng, bit ? (c->p.q_lwe >> 1) : 0, A.h_rk0_a.data() + static_cast<size_t>(t) * n,
                     A.h_rk0_b.data() + t);
     }
-    cudaStream_t s = c->stream;
-    CBS_CUDA_TRY(A.tables.upload(A.h_tables.data(), A.h_tables.size(), s));
-    CBS_CUDA_TRY(A.rk_words.upload(A.h_rk_words.data(), A.h_rk_words.size(), s));
-    CBS_CUDA_TRY(A.rk0_a.upload(A.h_rk0_a.data(), A.h_rk0_a.size(), s));
-    CBS_CUDA_TRY(A.rk0_b.upload(A.h_rk0_b.data(), A.h_rk0_b.size(), s));
-    CBS_CUDA_TRY(A.tables_coef.alloc(A.h_tables.size()));
-    CBS_CUDA_TRY(A.rk_words_coef.alloc(A.h_rk_words.size()));
-    CBS_CUDA_TRY(ntt_inverse(A.tables_coef.p, A.tables.p, nullptr, c->d_irp.p, c->d_irps.p, c->d_mod.p, c->d_ninv.p,
-                             c->d_ninv_s.p, N, A.h_tables.size() / N, s));
-    CBS_CUDA_TRY(ntt_inverse(A.rk_words_coef.p, A.rk_words.p, nullptr, c->d_irp.p, c->d_irps.p, c->d_mod.p,
-                             c->d_ninv.p, c->d_ninv_s.p, N, A.h_rk_words.size() / N, s));
-    CBS_CUDA_TRY(cudaStreamSynchronize(s));
-    A.ready = true;
-    return CBS_OK;
+    return aes_upload_material(c);
+}
+
+cbs_status cbs_aes128_import_material(cbs_context* ctx, const uint64_t* h_tables, const uint64_t* h_rk_words,
+                                      const uint64_t* h_rk0_a, const uint64_t* h_rk0_b) {
+    CBS_CHECK_ARG(ctx && h_tables && h_rk_words && h_rk0_a && h_rk0_b, "aes_import: null argument");
+    if (!ctx->keys_ready) {
+        set_error("aes_import: import or generate the evaluation keys first");
+        return CBS_ERR_NOT_READY;
+    }
+    cbs_context* c = ctx;
+    AesState& A = c->aes;
+    const uint32_t N = c->p.N, n = c->p.n;
+    const uint64_t Q = c->p.Q, q = c->p.q_lwe;
+    const size_t n_tab = static_cast<size_t>(8) * 256 * 2 * N, n_rk = static_cast<size_t>(11) * 4 * 2 * N;
+    for (size_t i = 0; i < n_tab; ++i) CBS_CHECK_ARG(h_tables[i] < Q, "aes_import: table words must be below Q");
+    for (size_t i = 0; i < n_rk; ++i) CBS_CHECK_ARG(h_rk_words[i] < Q, "aes_import: round-key words must be below Q");
+    for (size_t i = 0; i < static_cast<size_t>(128) * n; ++i)
+        CBS_CHECK_ARG(h_rk0_a[i] < q, "aes_import: round-0 LWE entries must be below q");
+    for (size_t i = 0; i < 128; ++i) CBS_CHECK_ARG(h_rk0_b[i] < q, "aes_import: round-0 LWE entries must be below q");
+    try {
+        A.h_tables.assign(h_tables, h_tables + n_tab);
+        A.h_rk_words.assign(h_rk_words, h_rk_words + n_rk);
+        A.h_rk0_a.assign(h_rk0_a, h_rk0_a + static_cast<size_t>(128) * n);
+        A.h_rk0_b.assign(h_rk0_b, h_rk0_b + 128);
+    } catch (const std::exception& e) {
+        set_error(std::string("aes_import: ") + e.what());
+        return CBS_ERR_OOM;
+    }
+    std::memset(A.key, 0, sizeof(A.key));  // the AES key stays with its owner
+    A.ready = false;
+    return aes_upload_material(c);
 }
 
 cbs_status cbs_aes128_export_material(const cbs_context* ctx, uint64_t* h_tables, uint64_t* h_rk_words,
@@ -284,8 +319,8 @@ cbs_status cbs_aes128_ctr_transcipher(cbs_context* ctx, const uint8_t* h_counter
 cbs_status cbs_lwe_decrypt_bits(const cbs_context* ctx, const uint64_t* h_a, const uint64_t* h_b, uint32_t count,
                                 uint32_t a_stride, uint8_t* h_bits) {
     CBS_CHECK_ARG(ctx && (count == 0 || (h_a && h_b && h_bits)), "lwe_decrypt: null argument");
-    if (!ctx->keys_ready) {
-        set_error("lwe_decrypt: no key material");
+    if (!ctx->keys_ready || !ctx->has_secret) {
+        set_error("lwe_decrypt: no secret key in this context");
         return CBS_ERR_NOT_READY;
     }
     CBS_CHECK_ARG(a_stride >= ctx->p.n, "lwe_decrypt: a_stride < n");

@@ -79,15 +79,10 @@ static constexpr uint64_t kMbSeedTweak = 0x6d756c7469626974ull;
 
 // grouped multi-bit keys (generated from the context's secrets, seeded from the key seed)
 // and their spectra
-static cbs_status prepare_mb(cbs_context* c) {
-    if (c->br_mb <= 1 || c->mb_ready) return CBS_OK;
-    if (!c->keys_ready) {
-        set_error("multi-bit blind rotation: no key material (call cbs_keygen first)");
-        return CBS_ERR_NOT_READY;
-    }
+// spectra of the grouped keys in c->h_mbk, uploaded
+static cbs_status upload_mb_spectra(cbs_context* c) {
     std::vector<double2> spec;
     try {
-        generate_mb_bsk(c->p, c->tab, c->hk, c->br_mb, c->key_seed ^ kMbSeedTweak, c->h_mbk);
         keys_to_fft_host(c->tab, c->h_mbk.data(), c->h_mbk.size() / c->p.N, spec);
     } catch (const std::exception& e) {
         set_error(std::string("multi-bit keys: ") + e.what());
@@ -97,6 +92,26 @@ static cbs_status prepare_mb(cbs_context* c) {
     CBS_CUDA_TRY(cudaStreamSynchronize(c->stream));
     c->mb_ready = true;
     return CBS_OK;
+}
+
+static cbs_status prepare_mb(cbs_context* c) {
+    if (c->br_mb <= 1 || c->mb_ready) return CBS_OK;
+    if (!c->keys_ready) {
+        set_error("multi-bit blind rotation: no key material (call cbs_keygen first)");
+        return CBS_ERR_NOT_READY;
+    }
+    if (!c->has_secret) {
+        set_error("multi-bit blind rotation: generating grouped keys needs the secret key; "
+                  "import them with cbs_import_mb_bsk");
+        return CBS_ERR_NOT_READY;
+    }
+    try {
+        generate_mb_bsk(c->p, c->tab, c->hk, c->br_mb, c->key_seed ^ kMbSeedTweak, c->h_mbk);
+    } catch (const std::exception& e) {
+        set_error(std::string("multi-bit keys: ") + e.what());
+        return CBS_ERR_OOM;
+    }
+    return upload_mb_spectra(c);
 }
 
 cbs_status run_blind_rotate(cbs_context* c, const uint64_t* d_a, const uint64_t* d_b, uint32_t batch,
@@ -395,8 +410,7 @@ cbs_status cbs_context_create(const cbs_params* params, uint32_t max_batch, cbs_
 
 cbs_status cbs_context_destroy(cbs_context* ctx) {
     if (!ctx) return CBS_OK;
-    for (auto& g : ctx->aes.graphs)
-        if (g) cudaGraphExecDestroy(g);
+    ctx->aes.drop_graphs();
     cudaStream_t s = ctx->stream;
     delete ctx;
     if (s) cudaStreamDestroy(s);
@@ -409,15 +423,9 @@ cbs_status cbs_context_stream(const cbs_context* ctx, cbs_stream_t* out) {
     return CBS_OK;
 }
 
-cbs_status cbs_keygen(cbs_context* ctx, uint64_t seed) {
-    CBS_CHECK_ARG(ctx, "keygen: null context");
-    cbs_context* c = ctx;
-    try {
-        generate_keys(c->p, c->tab, seed, c->hk);
-    } catch (const std::exception& e) {
-        set_error(std::string("keygen: ") + e.what());
-        return CBS_ERR_OOM;
-    }
+// upload the evaluation keys of c->hk (bsk / ht / ss to Montgomery form, the KSK with padded
+// rows, the derived tables) and rebuild what depends on them
+static cbs_status upload_host_keys(cbs_context* c) {
     FastMod fm(c->p.Q);
     cudaStream_t s = c->stream;
     const auto bsk_m = to_mont(c->hk.bsk, fm, c->mont_r);
@@ -442,12 +450,107 @@ cbs_status cbs_keygen(cbs_context* ctx, uint64_t seed) {
     c->aes.ready = false;
     c->fft_ready = false;
     c->mb_ready = false;
-    c->key_seed = seed;
+    c->h_mbk.clear();
+    c->d_bskf_mb.reset();
+    c->aes.drop_graphs();
     if (c->br_backend == CBS_BR_FFT64) {
         if (cbs_status st = prepare_fft(c)) return st;
         return prepare_mb(c);
     }
     return CBS_OK;
+}
+
+cbs_status cbs_keygen(cbs_context* ctx, uint64_t seed) {
+    CBS_CHECK_ARG(ctx, "keygen: null context");
+    cbs_context* c = ctx;
+    try {
+        generate_keys(c->p, c->tab, seed, c->hk);
+    } catch (const std::exception& e) {
+        set_error(std::string("keygen: ") + e.what());
+        return CBS_ERR_OOM;
+    }
+    c->has_secret = true;
+    c->key_seed = seed;
+    return upload_host_keys(c);
+}
+
+cbs_status cbs_import_keys(cbs_context* ctx, const int32_t* s_lwe, const int32_t* s_rlwe, const uint64_t* bsk,
+                           const uint64_t* ht, const uint64_t* ss, const uint16_t* ksk) {
+    CBS_CHECK_ARG(ctx && bsk && ht && ss && ksk, "import_keys: null argument (bsk, ht, ss and ksk are required)");
+    CBS_CHECK_ARG((s_lwe == nullptr) == (s_rlwe == nullptr), "import_keys: give both secrets or neither");
+    cbs_context* c = ctx;
+    const cbs_params& p = c->p;
+    const uint32_t N = p.N, n = p.n;
+    const uint64_t Q = p.Q;
+    const size_t n_bsk = static_cast<size_t>(n) * 2 * p.digits_g * 2 * N;
+    const size_t n_ht = static_cast<size_t>(c->rounds) * p.digits_ht * 2 * N;
+    const size_t n_ss = static_cast<size_t>(p.digits_ss) * 2 * N;
+    const size_t n_ksk = static_cast<size_t>(2) * N * p.base_ks * (n + 1);
+    auto below_q = [Q](const uint64_t* v, size_t len) {
+        for (size_t i = 0; i < len; ++i)
+            if (v[i] >= Q) return false;
+        return true;
+    };
+    CBS_CHECK_ARG(below_q(bsk, n_bsk) && below_q(ht, n_ht) && below_q(ss, n_ss),
+                  "import_keys: key words must be residues mod Q (NTT domain, the layouts of cbs_export_keys)");
+    for (size_t i = 0; i < n_ksk; ++i)
+        CBS_CHECK_ARG(ksk[i] < p.qks, "import_keys: key-switching key entries must be below qks");
+    if (s_lwe) {
+        for (uint32_t i = 0; i < n; ++i) CBS_CHECK_ARG(s_lwe[i] == 0 || s_lwe[i] == 1, "import_keys: s_lwe must be binary");
+        for (uint32_t i = 0; i < N; ++i)
+            CBS_CHECK_ARG(s_rlwe[i] >= -1 && s_rlwe[i] <= 1, "import_keys: s_rlwe must be ternary");
+    }
+    HostKeys& k = c->hk;
+    try {
+        k.bsk.assign(bsk, bsk + n_bsk);
+        k.ht.assign(ht, ht + n_ht);
+        k.ss.assign(ss, ss + n_ss);
+        k.ksk.assign(ksk, ksk + n_ksk);
+        derive_key_tables(p, k);
+        if (s_lwe) {
+            set_secrets(p, c->tab, s_lwe, s_rlwe, k);
+        } else {
+            k.s_lwe.clear();
+            k.s_rlwe.clear();
+            k.s_ntt.clear();
+        }
+    } catch (const std::exception& e) {
+        set_error(std::string("import_keys: ") + e.what());
+        return CBS_ERR_OOM;
+    }
+    c->has_secret = s_lwe != nullptr;
+    c->key_seed = 0;
+    return upload_host_keys(c);
+}
+
+cbs_status cbs_import_mb_bsk(cbs_context* ctx, uint32_t mb, const uint64_t* keys, size_t words) {
+    CBS_CHECK_ARG(ctx && keys, "import_mb_bsk: null argument");
+    CBS_CHECK_ARG(mb == 2 || mb == 3, "import_mb_bsk: mb must be 2 or 3");
+    if (ctx->br_backend != CBS_BR_FFT64) {
+        set_error("import_mb_bsk: grouped blind rotation is implemented for the FFT64 backend");
+        return CBS_ERR_UNSUPPORTED;
+    }
+    if (!ctx->keys_ready) {
+        set_error("import_mb_bsk: import or generate the keys first");
+        return CBS_ERR_NOT_READY;
+    }
+    const cbs_params& p = ctx->p;
+    const size_t want = static_cast<size_t>((p.n + mb - 1) / mb) * mb_subsets(mb) * 2 * p.digits_g * 2 * p.N;
+    if (words != want) {
+        set_error("import_mb_bsk: words must be ceil(n/mb) * (2^mb - 1) * 2 digits_g * 2 N");
+        return CBS_ERR_SHAPE_MISMATCH;
+    }
+    for (size_t i = 0; i < words; ++i) CBS_CHECK_ARG(keys[i] < p.Q, "import_mb_bsk: key words must be residues mod Q");
+    try {
+        ctx->h_mbk.assign(keys, keys + words);
+    } catch (const std::exception& e) {
+        set_error(std::string("import_mb_bsk: ") + e.what());
+        return CBS_ERR_OOM;
+    }
+    ctx->br_mb = mb;
+    ctx->mb_ready = false;
+    ctx->aes.drop_graphs();
+    return upload_mb_spectra(ctx);
 }
 
 cbs_status cbs_context_set_br_multibit(cbs_context* ctx, uint32_t mb) {
@@ -466,12 +569,7 @@ cbs_status cbs_context_set_br_multibit(cbs_context* ctx, uint32_t mb) {
     if (mb > 1 && ctx->keys_ready) {
         if (cbs_status st = prepare_mb(ctx)) return st;
     }
-    for (auto& g : ctx->aes.graphs)
-        if (g) {
-            cudaGraphExecDestroy(g);
-            g = nullptr;
-        }
-    ctx->aes.graph_chunk = 0;
+    ctx->aes.drop_graphs();
     return CBS_OK;
 }
 
@@ -504,12 +602,7 @@ cbs_status cbs_context_set_br_backend(cbs_context* ctx, int backend) {
         ctx->d_bskf_mb.reset();
     }
     // captured AES round graphs bake in the kernel choice
-    for (auto& g : ctx->aes.graphs)
-        if (g) {
-            cudaGraphExecDestroy(g);
-            g = nullptr;
-        }
-    ctx->aes.graph_chunk = 0;
+    ctx->aes.drop_graphs();
     return CBS_OK;
 }
 

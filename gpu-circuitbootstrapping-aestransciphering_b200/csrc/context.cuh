@@ -39,6 +39,15 @@ struct AesState {
     DevBuf<uint32_t> extract_info;        // [chunk*128]
     std::array<cudaGraphExec_t, 10> graphs{};
     uint32_t graph_chunk = 0;
+    // the captured round graphs hold device pointers of the keys; dropped when keys change
+    void drop_graphs() {
+        for (auto& g : graphs)
+            if (g) {
+                cudaGraphExecDestroy(g);
+                g = nullptr;
+            }
+        graph_chunk = 0;
+    }
 };
 
 }  // namespace cbs
@@ -56,8 +65,10 @@ struct cbs_context {
     cbs::DevBuf<uint64_t> d_rp, d_rps, d_irp, d_irps, d_ninv, d_ninv_s;
     cbs::DevBuf<cbs_dmodulus> d_mod;
     cbs::DevBuf<uint32_t> d_maps;
-    // keys
+    // keys (has_secret: hk holds s_lwe / s_rlwe, i.e. the keys came from cbs_keygen or were
+    // imported with their secrets; without them the context evaluates only)
     bool keys_ready = false;
+    bool has_secret = false;
     cbs::HostKeys hk;
     cbs::DevBuf<uint64_t> d_tv, d_gadd, d_bsk, d_ht, d_ss;
     cbs::DevBuf<uint16_t> d_ksk;

@@ -213,6 +213,51 @@ void lwe_encrypt(const cbs_params& p, const HostKeys& k, Rng& rng, uint64_t m, u
     *out_b = static_cast<uint64_t>(bm);
 }
 
+// The material a context derives from the parameters alone: the gadget powers, the
+// multi-value test vector, the finalize constants and the NTT-domain automorphism maps.
+void derive_key_tables(const cbs_params& p, HostKeys& k) {
+    const uint32_t N = p.N;
+    const uint64_t Q = p.Q;
+    FastMod fm(Q);
+    const uint32_t logn = static_cast<uint32_t>(__builtin_ctz(N));
+    const uint32_t rounds = logn - p.trace_shift;
+    // test vector: slot j of each 2^bw block holds -+g_j/2 (negative on the first half)
+    k.gpow = cbs_gadget_powers(p);
+    uint32_t bw = 0;
+    while ((1u << bw) < p.num_lut) ++bw;
+    k.tv.assign(N, 0);
+    for (uint32_t i = 0; i < N; ++i) {
+        const uint32_t slot = i & ((1u << bw) - 1);
+        if (slot >= p.num_lut) continue;
+        const uint64_t half = (k.gpow[slot] >> 1) % Q;
+        k.tv[i] = (i < N / 2) ? (half ? Q - half : 0) : half;
+    }
+    const uint64_t ninv = host::invmod(N, Q);
+    k.gadd.resize(p.num_lut);
+    for (uint32_t j = 0; j < p.num_lut; ++j) k.gadd[j] = fm.mul((k.gpow[j] >> 1) % Q, ninv);
+
+    // NTT-domain automorphism maps (kernel.cu:7554-7571)
+    k.maps.assign(static_cast<size_t>(rounds) * N, 0);
+    for (uint32_t lv = 0; lv < rounds; ++lv) {
+        const uint64_t kk = (static_cast<uint64_t>(N) >> lv) + 1;
+        for (uint32_t tid = 0; tid < N; ++tid) {
+            const uint32_t j = host::bit_reverse(tid, static_cast<int>(logn));
+            const uint32_t idx = static_cast<uint32_t>((((2ull * j + 1) * kk) & (2ull * N - 1)) >> 1);
+            k.maps[static_cast<size_t>(lv) * N + tid] = host::bit_reverse(idx, static_cast<int>(logn));
+        }
+    }
+}
+
+void set_secrets(const cbs_params& p, const host::NttTables& t, const int32_t* s_lwe, const int32_t* s_rlwe,
+                 HostKeys& k) {
+    FastMod fm(p.Q);
+    k.s_lwe.assign(s_lwe, s_lwe + p.n);
+    k.s_rlwe.assign(s_rlwe, s_rlwe + p.N);
+    k.s_ntt.resize(p.N);
+    for (uint32_t i = 0; i < p.N; ++i) k.s_ntt[i] = fm.from_signed(k.s_rlwe[i]);
+    ntt_fwd_fast(k.s_ntt.data(), t);
+}
+
 void generate_keys(const cbs_params& p, const host::NttTables& t, uint64_t seed, HostKeys& k) {
     const uint32_t N = p.N, n = p.n;
     const uint64_t Q = p.Q;
@@ -280,31 +325,7 @@ void generate_keys(const cbs_params& p, const host::NttTables& t, uint64_t seed,
         for (uint32_t c = 0; c < N; ++c) b[c] = fm.add(b[c], fm.mul(fm.mul(k.s_ntt[c], k.s_ntt[c]), gss[j]));
     }
 
-    // test vector: slot j of each 2^bw block holds -+g_j/2 (negative on the first half)
-    k.gpow = cbs_gadget_powers(p);
-    uint32_t bw = 0;
-    while ((1u << bw) < p.num_lut) ++bw;
-    k.tv.assign(N, 0);
-    for (uint32_t i = 0; i < N; ++i) {
-        const uint32_t slot = i & ((1u << bw) - 1);
-        if (slot >= p.num_lut) continue;
-        const uint64_t half = (k.gpow[slot] >> 1) % Q;
-        k.tv[i] = (i < N / 2) ? (half ? Q - half : 0) : half;
-    }
-    const uint64_t ninv = host::invmod(N, Q);
-    k.gadd.resize(p.num_lut);
-    for (uint32_t j = 0; j < p.num_lut; ++j) k.gadd[j] = fm.mul((k.gpow[j] >> 1) % Q, ninv);
-
-    // NTT-domain automorphism maps (kernel.cu:7554-7571)
-    k.maps.assign(static_cast<size_t>(rounds) * N, 0);
-    for (uint32_t lv = 0; lv < rounds; ++lv) {
-        const uint64_t kk = (static_cast<uint64_t>(N) >> lv) + 1;
-        for (uint32_t tid = 0; tid < N; ++tid) {
-            const uint32_t j = host::bit_reverse(tid, static_cast<int>(logn));
-            const uint32_t idx = static_cast<uint32_t>((((2ull * j + 1) * kk) & (2ull * N - 1)) >> 1);
-            k.maps[static_cast<size_t>(lv) * N + tid] = host::bit_reverse(idx, static_cast<int>(logn));
-        }
-    }
+    derive_key_tables(p, k);
 
     // extraction key switch N -> n: LWE_s(v * s'_i * B^j) mod qks, u16 packed
     const uint32_t qks = p.qks, bks = p.base_ks, outlen = n + 1;

@@ -51,6 +51,12 @@ struct HostKeys {
 std::vector<uint64_t> cbs_gadget_powers(const cbs_params& p);
 
 void generate_keys(const cbs_params& p, const host::NttTables& t, uint64_t seed, HostKeys& k);
+// gpow, tv, gadd and maps of k from the parameters (part of generate_keys; used alone when
+// the evaluation keys come from the caller)
+void derive_key_tables(const cbs_params& p, HostKeys& k);
+// s_lwe (n), s_rlwe (N) and NTT(s_rlwe) of k from caller buffers
+void set_secrets(const cbs_params& p, const host::NttTables& t, const int32_t* s_lwe, const int32_t* s_rlwe,
+                 HostKeys& k);
 
 // RLWE encryption of a coefficient-domain message (mod Q) into NTT-domain (a, b)
 void rlwe_encrypt(const cbs_params& p, const host::NttTables& t, const HostKeys& k, Rng& rng,

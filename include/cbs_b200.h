@@ -167,6 +167,22 @@ cbs_status cbs_generate_mb_bsk_host(const cbs_params *params, uint64_t seed, uin
 cbs_status cbs_export_keys(const cbs_context *ctx, int32_t *s_lwe, int32_t *s_rlwe, uint64_t *bsk, uint64_t *ht,
                            uint64_t *ss, uint16_t *ksk, uint64_t *tv, uint64_t *gpow, uint32_t *maps);
 
+/* Load evaluation keys made elsewhere (by the key owner's cbs_generate_keys_host, or
+ * cbs_export_keys of another context with the same parameters) instead of cbs_keygen: the
+ * key upload of GPUCirBTSContext(const CirBTSContext&, maxBatch) (cirbts.cuh:420,
+ * gpu_init_cirbsk cirbts-init.cu:200-865) for keys the caller owns.  bsk, ht, ss and ksk are
+ * required, in the layouts of cbs_export_keys (every word checked: residues mod Q, KSK
+ * entries below qks); the test vector, gadget powers and automorphism maps are derived from
+ * the parameters.  The secrets are optional: with s_lwe = s_rlwe = NULL the context holds
+ * evaluation keys only, and what needs a secret (generating grouped keys, cbs_aes128_setup,
+ * cbs_lwe_decrypt_bits) returns CBS_ERR_NOT_READY; cbs_import_mb_bsk and
+ * cbs_aes128_import_material then supply that material. */
+cbs_status cbs_import_keys(cbs_context *ctx, const int32_t *s_lwe, const int32_t *s_rlwe, const uint64_t *bsk,
+                           const uint64_t *ht, const uint64_t *ss, const uint16_t *ksk);
+/* Grouped keys for mb = 2 or 3 in the layout of cbs_export_mb_bsk (words must match);
+ * selects mb like cbs_context_set_br_multibit.  FFT64 backend. */
+cbs_status cbs_import_mb_bsk(cbs_context *ctx, uint32_t mb, const uint64_t *keys, size_t words);
+
 /* The same key generation without a device (host buffers as in cbs_export_keys); the keys
  * of cbs_keygen(ctx, seed) equal those of cbs_generate_keys_host(params, seed). */
 cbs_status cbs_generate_keys_host(const cbs_params *params, uint64_t seed, int32_t *s_lwe, int32_t *s_rlwe,
@@ -232,6 +248,11 @@ cbs_status cbs_aes128_setup(cbs_context *ctx, const uint8_t *key, uint64_t seed)
  * (NTT domain), rk0_a [128][n], rk0_b [128]; any pointer may be NULL. */
 cbs_status cbs_aes128_export_material(const cbs_context *ctx, uint64_t *h_tables, uint64_t *h_rk_words,
                                       uint64_t *h_rk0_a, uint64_t *h_rk0_b);
+/* Load encrypted material in the layouts above (made by the key owner's cbs_aes128_setup and
+ * exported) instead of cbs_aes128_setup: a context holding evaluation keys only can then
+ * transcipher; the AES key itself never reaches it.  Words checked (below Q / below q). */
+cbs_status cbs_aes128_import_material(cbs_context *ctx, const uint64_t *h_tables, const uint64_t *h_rk_words,
+                                      const uint64_t *h_rk0_a, const uint64_t *h_rk0_b);
 /* Device variant: d_counter_bits [blocks*128] (0/1, bit t = byte*8 + b of each counter
  * block); d_out_a [blocks*128][n], d_out_b [blocks*128].  use_graphs != 0 replays one
  * captured CUDA graph per round (captured on the first call for a chunk size). */

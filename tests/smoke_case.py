@@ -90,3 +90,39 @@ def run_smoke(pkg, torch, np) -> None:
         print("smoke: FFT HomTrace + SchemeSwitch rows decrypt to m g_j / -m g_j s")
     finally:
         ctx.close()
+
+    # split-FP32 gate bootstrap (torus 32, N = 1024, n = 64): FP32 transforms with the keys
+    # split into a 24-bit and an exact 8-bit limb; the extracted LWE's noise stays within the
+    # FP32 bound of the exact FP64 path's, and every bit decrypts
+    gp = pkg.gate_default_params()
+    gp.n = 64
+    g = pkg.GateContext(gp, max_batch=8)
+    try:
+        g.keygen(5)
+        gk = g.export_keys()
+        gbits = np.array([1, 0, 0, 1, 1, 0, 1, 0], np.uint8)
+        ga, gb = g.encrypt(gbits, seed=6)
+        z = gk["z_rlwe"].astype(np.int64)
+        want = np.where(gbits == 1, 1 << 29, -(1 << 29))
+        noise = {}
+        for mode in ("fp64", "fp32-split"):
+            g.set_fft_mode(mode)
+            dga = torch.from_numpy(ga.view(np.int32)).cuda()
+            dgb = torch.from_numpy(gb.view(np.int32)).cuda()
+            ext = torch.zeros((len(gbits), gp.N + 1), dtype=torch.int32, device="cuda")
+            oa = torch.zeros((len(gbits), gp.n), dtype=torch.int32, device="cuda")
+            ob = torch.zeros(len(gbits), dtype=torch.int32, device="cuda")
+            pkg.call("cbs_gate_bootstrap_batch_device", g.handle, dga.data_ptr(), dgb.data_ptr(), len(gbits),
+                     ext.data_ptr(), oa.data_ptr(), ob.data_ptr(), None)
+            torch.cuda.synchronize()
+            e = ext.cpu().numpy().view(np.uint32).astype(np.int64)
+            ph = (e[:, gp.N] - e[:, : gp.N] @ z - want) % (1 << 32)
+            noise[mode] = int(np.abs(np.where(ph >= 1 << 31, ph - (1 << 32), ph)).max())
+            got = g.decrypt(oa.cpu().numpy().view(np.uint32), ob.cpu().numpy().view(np.uint32))
+            assert np.array_equal(got, gbits), f"{mode} gate bootstrap decrypts wrong"
+        g.set_fft_mode("fp64")
+        assert noise["fp32-split"] < 2 ** 27, f"split-FP32 output noise 2^{np.log2(noise['fp32-split']):.1f}"
+        print(f"smoke: split-FP32 gate bootstrap decrypts; output noise max 2^{np.log2(noise['fp32-split']):.1f} "
+              f"(FP64 2^{np.log2(noise['fp64']):.1f})")
+    finally:
+        g.close()
