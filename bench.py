@@ -252,7 +252,8 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
         "roofline": {"kernel": br_kernel_name(args)
                      + " (fused GINX blind rotation + finalize + MV split)", "bound": "hbm",
                      "achieved": achieved_gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                     "frac": achieved_gbs / peaks["hbm_gbs"], "peak_src": peaks["src"], "traffic": None,
+                     "frac": achieved_gbs / peaks["hbm_gbs"], "peak_src": peaks["src"],
+                     "traffic": BR_TRAFFIC.get((args.backend, args.multibit, T)),
                      "algorithmic_bytes_per_launch": alg_bytes, "launch_ms": br_ms,
                      "note": "compute-bound (integer multiplies for ntt, FP64 pipe for fft64); see compute_rate"},
         "compute_rate": compute_rate(args.backend, T, p, br_ms, args.multibit),
@@ -732,6 +733,13 @@ def br_key_bytes(p, mb: int) -> int:
     coefficient."""
     rgsw = 2 * p.digits_g * 2 * p.N * 8
     return (-(-p.n // mb)) * ((1 << mb) - 1) * rgsw
+
+
+# DRAM bytes (read + write) of one blind-rotation launch, measured with ncu
+# (dram__bytes_read.sum + dram__bytes_write.sum, one pass) on the launch this bench times:
+# (backend, mb, ciphertexts per launch) -> bytes.  16384 = 128 blocks x 128 bits; the grouped
+# key (186 MB) does not fit L2 and is re-read by each wave of 148 ciphertexts.
+BR_TRAFFIC = {("fft64", 2, 16384): 20810.3e6 + 2151.6e6}
 
 
 def br_kernel_name(args) -> str:
