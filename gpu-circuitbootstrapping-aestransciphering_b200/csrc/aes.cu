@@ -80,7 +80,7 @@ static cbs_status aes_round(cbs_context* c, uint32_t round, uint32_t chunk, cuda
         if (cbs_status st = run_trace_fft(c, c->d_mv.p, T * L, rgswf, s)) return st;
         if (cbs_status st = run_lut_levels_fft(c, A.tables_coef.p, 256ull * 2 * N, A.lut_sel[final_round ? 1 : 0].p,
                                                rgswf, static_cast<uint64_t>(L) * 4 * (N / 2), A.ctrl_bits.p, luts,
-                                               A.lut_a.p, A.lut_b.p, A.lut_out.p, s))
+                                               A.lut_a.p, A.lut_b.p, A.lut_out.p, s, A.tables_spec.p))
             return st;
         CBS_CUDA_TRY(launch_assemble_words(A.words.p, A.lut_out.p,
                                            A.rk_words_coef.p + static_cast<size_t>(round) * 4 * 2 * N, c->p.Q, N,
@@ -158,6 +158,21 @@ static cbs_status aes_upload_material(cbs_context* c) {
                              c->d_ninv.p, c->d_ninv_s.p, N, A.h_rk_words.size() / N, s));
     CBS_CUDA_TRY(cudaStreamSynchronize(s));
     A.ready = true;
+    A.spec_ready = false;
+    return CBS_OK;
+}
+
+// level-0 table spectra of the FFT path (once per material; outside any capture)
+static cbs_status aes_prepare_spectra(cbs_context* c, cudaStream_t s) {
+    AesState& A = c->aes;
+    if (c->br_backend != CBS_BR_FFT64 || A.spec_ready) return CBS_OK;
+    const size_t M = c->p.N / 2, len = static_cast<size_t>(8) * 128 * 2 * c->p.num_lut * M;
+    const double2* old = A.tables_spec.p;
+    CBS_CUDA_TRY(A.tables_spec.alloc(len));
+    if (A.tables_spec.p != old) A.drop_graphs();  // captured rounds hold the old pointer
+    if (cbs_status st = build_table_spectra(c, A.tables_coef.p, 256ull * 2 * c->p.N, 8, A.tables_spec.p, s)) return st;
+    CBS_CUDA_TRY(cudaStreamSynchronize(s));
+    A.spec_ready = true;
     return CBS_OK;
 }
 
@@ -276,6 +291,7 @@ cbs_status cbs_aes128_ctr_transcipher_device(cbs_context* ctx, const uint8_t* d_
     const uint32_t max_chunk = std::max(1u, std::min(kAesMaxChunkBlocks, c->max_batch / 128u));
     const uint32_t chunk = std::min(blocks, max_chunk);
     if (cbs_status st = aes_prepare_chunk(c, chunk)) return st;
+    if (cbs_status st = aes_prepare_spectra(c, s)) return st;
     for (uint32_t off = 0; off < blocks; off += chunk) {
         const uint32_t cur = std::min(chunk, blocks - off);
         const uint32_t T = cur * 128;

@@ -226,10 +226,68 @@ __global__ void __launch_bounds__(LutFftCfg<LOGN>::T, LutFftCfg<LOGN>::TRACE_BLO
     store_spectrum<T>(out + M, tid, x);
 }
 
+// prepared digit words (re, im) of component p of in1 - in0 into ws[M]
+template <uint32_t N, uint32_t T>
+__device__ __forceinline__ void cmux_diff_words(uint2* ws, const uint64_t* in0, const uint64_t* in1, uint32_t p,
+                                                const DigitPrep& g, uint32_t tid) {
+    constexpr uint32_t M = N / 2;
+    for (uint32_t e = tid; e < M; e += T) {
+        const uint32_t lo = p * N + e, hi = lo + M;
+        const uint64_t dr = sub_mod(__ldg(in1 + lo), __ldg(in0 + lo), g.q);
+        const uint64_t di = sub_mod(__ldg(in1 + hi), __ldg(in0 + hi), g.q);
+        ws[e] = make_uint2(static_cast<uint32_t>(prepared_offset(dr, g)), static_cast<uint32_t>(prepared_offset(di, g)));
+    }
+}
+
+// forward transform of digit d of the prepared words src into x
+template <int LOGM, class Bar>
+__device__ __forceinline__ void cmux_digit_fft(double2* fs, uint32_t tid, const double2* tab, const uint2* src,
+                                               int gbits, uint32_t d, double2 (&x)[8], Bar bar) {
+    const double2* tws = tab + FftTab<LOGM>::twist_off();
+    fft_forward_to_regs<LOGM>(
+        fs, tid, tab,
+        [&](int j, uint32_t e) {
+            const uint2 w = src[e];
+            return cmul(make_double2(static_cast<double>(balanced_digit(w.x, gbits, d)),
+                                     static_cast<double>(balanced_digit(w.y, gbits, d))),
+                        twist_at<LOGM>(tws, j, e));
+        },
+        x, bar);
+}
+
+// Digit spectra of the level-0 pair differences of fixed LUT tables, computed once: CTA
+// (i, set, r) writes transform r = 2d + p of in[2i+1] - in[2i] (set `set`) to
+// out[((set * pairs + i) * 2 digits + r) * M], slot-major as the CMux reads it.
+template <int LOGN>
+__global__ void __launch_bounds__(LutFftCfg<LOGN>::T) k_cmux_pair_spectra(const CmuxFftArgs a, const FftKeyArgs f,
+                                                                            double2* out) {
+    constexpr int LOGM = LOGN - 1;
+    constexpr uint32_t N = 1u << LOGN, M = N / 2, T = M / 8;
+    using Tb = FftTab<LOGM>;
+    extern __shared__ __align__(16) uint64_t smem[];
+    uint2* ws = reinterpret_cast<uint2*>(smem);            // [M]
+    double2* fs = reinterpret_cast<double2*>(ws + 2 * M);  // [M]
+    double2* tab = fs + M;
+    const uint32_t i = blockIdx.x, set = blockIdx.y, r = blockIdx.z, tid = threadIdx.x;
+    for (uint32_t k = tid; k < Tb::size(); k += T) tab[k] = f.tab[k];
+    const uint64_t* in0 = a.in + set * a.in_lut_stride + static_cast<size_t>(2 * i) * 2 * N;
+    cmux_diff_words<N, T>(ws, in0, in0 + 2 * N, r & 1, a.g, tid);
+    __syncthreads();
+    double2 x[8];
+    cmux_digit_fft<LOGM>(fs, tid, tab, ws, a.g.gbits, r >> 1, x, []() { __syncthreads(); });
+    double2* dst = out + ((static_cast<size_t>(set) * gridDim.x + i) * gridDim.z + r) * M + tid;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) dst[j * T] = x[j];
+}
+
 // One CMux of a LUT-tree level per CTA: ct0 = input 2i, ct1 = input 2i + 1 of the LUT's set,
 // control = RGSW of bit ctrl_bits[lut][level].  The prepared digit words of both difference
 // polynomials are computed once into shared memory (digits * gbits <= 32 bits per word);
-// transform r = 2d + p takes digit d of polynomial p and multiplies it against row r.
+// transform r = 2d + p takes digit d of polynomial p and multiplies it against row r.  With
+// a.in_spec (level 0 over fixed tables) the digit spectra are read from k_cmux_pair_spectra's
+// output instead (no decomposition, no forward transforms).  CTAs run pair-major within a
+// LUT: the 128 CTAs of a LUT share its control's row spectra through L2, and the few tables
+// of a round (4 x 16.7 MB of spectra at N = 2048) stay L2-resident across the LUTs.
 template <int LOGN>
 __global__ void __launch_bounds__(LutFftCfg<LOGN>::T, LutFftCfg<LOGN>::CMUX_BLOCKS)
     k_cmux_level_fft(const CmuxFftArgs a, const FftKeyArgs f) {
@@ -241,6 +299,7 @@ __global__ void __launch_bounds__(LutFftCfg<LOGN>::T, LutFftCfg<LOGN>::CMUX_BLOC
     double2* fs = reinterpret_cast<double2*>(ws + 2 * M);  // [M]
     double2* tab = fs + M;
     const double2* tws = tab + Tb::twist_off();
+    const bool pre = a.in_spec != nullptr;
     const uint32_t i = blockIdx.x, lut = blockIdx.y, tid = threadIdx.x;
     const uint64_t Q = a.g.q;
     auto bar = []() { __syncthreads(); };
@@ -249,36 +308,28 @@ __global__ void __launch_bounds__(LutFftCfg<LOGN>::T, LutFftCfg<LOGN>::CMUX_BLOC
     const uint32_t set = a.lut_sel ? __ldg(a.lut_sel + lut) : lut;
     const uint64_t* in0 = a.in + set * a.in_lut_stride + static_cast<size_t>(2 * i) * 2 * N;
     const uint64_t* in1 = in0 + 2 * N;
+    const double2* spec = nullptr;
+    if (pre) {
+        spec = a.in_spec + (static_cast<size_t>(set) * (a.in_count / 2) + i) * 2 * a.digits * M + tid;
+    } else {
 #pragma unroll
-    for (uint32_t p = 0; p < 2; ++p)
-        for (uint32_t e = tid; e < M; e += T) {
-            const uint32_t lo = p * N + e, hi = lo + M;
-            const uint64_t dr = sub_mod(__ldg(in1 + lo), __ldg(in0 + lo), Q);
-            const uint64_t di = sub_mod(__ldg(in1 + hi), __ldg(in0 + hi), Q);
-            ws[p * M + e] = make_uint2(static_cast<uint32_t>(prepared_offset(dr, a.g)),
-                                       static_cast<uint32_t>(prepared_offset(di, a.g)));
-        }
+        for (uint32_t p = 0; p < 2; ++p) cmux_diff_words<N, T>(ws + p * M, in0, in1, p, a.g, tid);
+    }
     __syncthreads();
 
     const uint32_t bit = __ldg(a.ctrl_bits + static_cast<size_t>(lut) * 8 + a.level);
     const double2* G = a.rgswf + static_cast<size_t>(bit) * a.rgsw_stride + tid;
-    const int gbits = a.g.gbits;
     double2 y0[8], y1[8];
 #pragma unroll
     for (int j = 0; j < 8; ++j) y0[j] = y1[j] = make_double2(0.0, 0.0);
     for (uint32_t r = 0; r < 2 * a.digits; ++r) {
-        const uint2* src = ws + (r & 1) * M;
-        const uint32_t d = r >> 1;
         double2 x[8];
-        fft_forward_to_regs<LOGM>(
-            fs, tid, tab,
-            [&](int j, uint32_t e) {
-                const uint2 w = src[e];
-                return cmul(make_double2(static_cast<double>(balanced_digit(w.x, gbits, d)),
-                                         static_cast<double>(balanced_digit(w.y, gbits, d))),
-                            twist_at<LOGM>(tws, j, e));
-            },
-            x, bar);
+        if (pre) {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) x[j] = __ldg(spec + static_cast<size_t>(r) * M + j * T);
+        } else {
+            cmux_digit_fft<LOGM>(fs, tid, tab, ws + (r & 1) * M, a.g.gbits, r >> 1, x, bar);
+        }
         const double2* k0 = G + static_cast<size_t>(r) * 2 * M;
         const double2* k1 = k0 + M;
 #pragma unroll
@@ -286,7 +337,7 @@ __global__ void __launch_bounds__(LutFftCfg<LOGN>::T, LutFftCfg<LOGN>::CMUX_BLOC
             cfma(y0[j], x[j], __ldg(k0 + j * T));
             cfma(y1[j], x[j], __ldg(k1 + j * T));
         }
-        __syncthreads();
+        if (!pre) __syncthreads();
     }
     uint64_t* out = a.out + (static_cast<size_t>(lut) * (a.in_count / 2) + i) * 2 * N;
     fft_inverse_from_regs<LOGM>(
@@ -376,6 +427,32 @@ static cudaError_t cmux_fft_launch(const CmuxFftArgs& a, const FftKeyArgs& f, ui
 }
 
 template <int LOGN>
+static cudaError_t pair_spectra_launch(const CmuxFftArgs& a, const FftKeyArgs& f, uint32_t sets, double2* out,
+                                       cudaStream_t s) {
+    constexpr uint32_t N = 1u << LOGN, M = N / 2;
+    if (f.tab_len != FftTab<LOGN - 1>::size()) return cudaErrorInvalidValue;
+    const size_t smem = 2ull * M * sizeof(uint2) + (M + FftTab<LOGN - 1>::size()) * sizeof(double2);
+    static size_t configured[64] = {};
+    cudaError_t e = opt_in_smem(k_cmux_pair_spectra<LOGN>, smem, configured);
+    if (e != cudaSuccess) return e;
+    const dim3 grid(a.in_count / 2, sets, 2 * a.digits);
+    k_cmux_pair_spectra<LOGN><<<grid, LutFftCfg<LOGN>::T, smem, s>>>(a, f, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cmux_pair_spectra(const CmuxFftArgs& a, const FftKeyArgs& f, uint32_t N, uint32_t sets,
+                                     double2* out, cudaStream_t s) {
+    if (sets == 0 || a.in_count < 2) return cudaSuccess;
+    if (sets > 65535 || 2 * a.digits > 64 || a.in_count / 2 > 0x7fffffffu) return cudaErrorInvalidValue;
+    switch (N) {
+        case 1024: return pair_spectra_launch<10>(a, f, sets, out, s);
+        case 2048: return pair_spectra_launch<11>(a, f, sets, out, s);
+        case 4096: return pair_spectra_launch<12>(a, f, sets, out, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+template <int LOGN>
 static cudaError_t spectra_launch(double2* buf, uint64_t Q, const FftKeyArgs& f, size_t polys, cudaStream_t s) {
     constexpr uint32_t M = 1u << (LOGN - 1);
     if (f.tab_len != FftTab<LOGN - 1>::size()) return cudaErrorInvalidValue;
@@ -415,6 +492,7 @@ cudaError_t launch_cmux_level_fft(const CmuxFftArgs& a, const FftKeyArgs& f, uin
                                   cudaStream_t s) {
     if (luts == 0) return cudaSuccess;
     if (a.in_count < 2 || a.digits == 0 || a.digits * static_cast<uint32_t>(a.g.gbits) > 32) return cudaErrorInvalidValue;
+    if (luts > 65535 || (a.in_spec && a.level != 0)) return cudaErrorInvalidValue;
     switch (N) {
         case 1024: return cmux_fft_launch<10>(a, f, luts, s);
         case 2048: return cmux_fft_launch<11>(a, f, luts, s);

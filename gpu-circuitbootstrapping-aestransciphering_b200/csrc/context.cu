@@ -232,10 +232,22 @@ cbs_status run_trace_fft_ntt_rows(cbs_context* c, const uint64_t* d_mv_coef, uin
     return CBS_OK;
 }
 
+cbs_status build_table_spectra(cbs_context* c, const uint64_t* d_tables, uint64_t table_stride, uint32_t sets,
+                               double2* out, cudaStream_t s) {
+    CmuxFftArgs a{};
+    a.in = d_tables;
+    a.in_lut_stride = table_stride;
+    a.in_count = 256;
+    a.g = make_digit_prep(c->p.Q, c->g_cc, c->p.num_lut);
+    a.digits = c->p.num_lut;
+    CBS_CUDA_TRY(launch_cmux_pair_spectra(a, fft_key_args(c), c->p.N, sets, out, s));
+    return CBS_OK;
+}
+
 cbs_status run_lut_levels_fft(cbs_context* c, const uint64_t* d_tables, uint64_t table_stride,
                               const uint32_t* d_lut_sel, const double2* d_rgswf, uint64_t rgsw_stride,
                               const uint32_t* d_ctrl, uint32_t luts, uint64_t* d_buf_a, uint64_t* d_buf_b,
-                              uint64_t* d_out, cudaStream_t s) {
+                              uint64_t* d_out, cudaStream_t s, const double2* d_table_spec) {
     const uint32_t N = c->p.N;
     const FftKeyArgs f = fft_key_args(c);
     const uint64_t* in = d_tables;
@@ -253,6 +265,7 @@ cbs_status run_lut_levels_fft(cbs_context* c, const uint64_t* d_tables, uint64_t
         a.level = level;
         a.g = make_digit_prep(c->p.Q, c->g_cc, c->p.num_lut);
         a.digits = c->p.num_lut;
+        a.in_spec = (level == 0) ? d_table_spec : nullptr;
         CBS_CUDA_TRY(launch_cmux_level_fft(a, f, N, luts, s));
         in = out;
     }

@@ -24,8 +24,11 @@ struct AesState {
     uint32_t chunk_blocks = 0;            // blocks per device chunk
     DevBuf<uint64_t> tables;              // [8][256][2][N]  Te0..3, Te4_0..3
     DevBuf<uint64_t> rk_words;            // [11][4][2][N]
-    // coefficient-domain copies of tables and rk_words for the FFT CMux path
+    // coefficient-domain copies of tables and rk_words for the FFT CMux path, and the level-0
+    // digit spectra of the table pairs ([8][128][2*num_lut][N/2], built on first FFT use)
     DevBuf<uint64_t> tables_coef, rk_words_coef;
+    DevBuf<double2> tables_spec;
+    bool spec_ready = false;
     DevBuf<uint64_t> rk0_a, rk0_b;        // [128][n], [128]
     std::vector<uint64_t> h_tables, h_rk_words, h_rk0_a, h_rk0_b;
     // per-chunk workspace
@@ -124,10 +127,15 @@ cbs_status run_cbs(cbs_context* c, const uint64_t* d_a, const uint64_t* d_b, uin
 cbs_status run_trace_fft(cbs_context* c, const uint64_t* d_mv_coef, uint32_t count, double2* d_rgswf,
                          cudaStream_t s);
 // the 8 FFT CMux levels of the LUT trees, coefficient-domain tables in and outputs out
+// d_table_spec (optional): the level-0 pair spectra of d_tables (build_table_spectra)
 cbs_status run_lut_levels_fft(cbs_context* c, const uint64_t* d_tables, uint64_t table_stride,
                               const uint32_t* d_lut_sel, const double2* d_rgswf, uint64_t rgsw_stride,
                               const uint32_t* d_ctrl, uint32_t luts, uint64_t* d_buf_a, uint64_t* d_buf_b,
-                              uint64_t* d_out, cudaStream_t s);
+                              uint64_t* d_out, cudaStream_t s, const double2* d_table_spec = nullptr);
+// level-0 digit spectra of `sets` fixed 256-entry tables (coefficient domain) into out
+// [sets][128][2*num_lut][N/2]
+cbs_status build_table_spectra(cbs_context* c, const uint64_t* d_tables, uint64_t table_stride, uint32_t sets,
+                               double2* out, cudaStream_t s);
 cbs_status run_trace(cbs_context* c, const uint64_t* d_mv, uint32_t count, uint64_t* d_rgsw, cudaStream_t s);
 cbs_status run_lut_levels(cbs_context* c, const uint64_t* d_tables, uint64_t table_stride, const uint32_t* d_lut_sel,
                           const uint64_t* d_rgsw_all, uint64_t rgsw_stride, const uint32_t* d_ctrl, uint32_t luts,

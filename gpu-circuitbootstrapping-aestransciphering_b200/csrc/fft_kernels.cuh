@@ -56,6 +56,9 @@ struct CmuxFftArgs {
     uint32_t level;
     DigitPrep g;
     uint32_t digits;
+    // level 0 over fixed tables: [sets][in_count/2][2*digits][N/2] digit spectra of
+    // in[2i+1] - in[2i] from launch_cmux_pair_spectra (null: computed in the CMux)
+    const double2* in_spec;
 };
 
 // mv_ntt: also transform the MV outputs to the NTT domain (the reference layout); false
@@ -67,6 +70,10 @@ cudaError_t launch_blind_rotate_fft(const BlindRotateArgs& a, const FftKeyArgs& 
 cudaError_t launch_blind_rotate_fft_mb(const BlindRotateArgs& a, const FftKeyArgs& f, const cbs_dmodulus* d_mod,
                                        uint32_t N, uint32_t batch, uint32_t mb, cudaStream_t s, bool mv_ntt = true);
 cudaError_t launch_trace_ss_fft(const TraceFftArgs& a, const FftKeyArgs& f, uint32_t N, uint32_t count, cudaStream_t s);
+// digit spectra of the pair differences of `sets` fixed level-0 input sets (a.in, a.in_lut_stride,
+// a.in_count, a.g, a.digits) into out [sets][in_count/2][2*digits][N/2]
+cudaError_t launch_cmux_pair_spectra(const CmuxFftArgs& a, const FftKeyArgs& f, uint32_t N, uint32_t sets,
+                                     double2* out, cudaStream_t s);
 cudaError_t launch_cmux_level_fft(const CmuxFftArgs& a, const FftKeyArgs& f, uint32_t N, uint32_t luts,
                                   cudaStream_t s);
 // spectra [polys][N/2] (slot-major) -> coefficient-domain polynomials [polys][N] mod Q, in place
