@@ -49,6 +49,14 @@ def load_pkg():
     return mod
 
 
+def load_replicas():
+    """The package's multi-GPU plumbing (replicas.py: CTR-stream sharding, max over ranks)."""
+    spec = importlib.util.spec_from_file_location("cbs_b200_replicas", PKG_DIR / "replicas.py")
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
 def measured_peaks() -> dict:
     f = ROOT / "MEASURED_PEAKS.json"
     if f.exists():
@@ -128,7 +136,6 @@ def verify(pkg, ctx, key: bytes, ctrs: np.ndarray, ha: np.ndarray, hb: np.ndarra
 
 def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     import torch
-    import torch.distributed as dist
 
     torch.cuda.set_device(local_rank)
     pkg = load_pkg()
@@ -141,8 +148,8 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     key = np.random.default_rng(args.seed).bytes(16)
     pkg.call("cbs_aes128_setup", ctx.handle, key, args.seed + 1)
     p = ctx.params
-    rng = np.random.default_rng(args.seed + 100 + rank)
-    ctrs = rng.integers(0, 256, size=(blocks, 16), dtype=np.uint8)
+    rep = load_replicas()
+    ctrs = rep.rank_counters(args.seed, rank, world, blocks)  # this rank's share of one CTR stream
     d_bits = torch.from_numpy(counter_bits(ctrs)).cuda()
     out_a = torch.empty((blocks * 128, p.n), dtype=torch.int64, device="cuda")
     out_b = torch.empty(blocks * 128, dtype=torch.int64, device="cuda")
@@ -157,8 +164,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
+    rep.barrier(world)
     torch.cuda.synchronize()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local_rank) as clk:
@@ -167,13 +173,8 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
             step()
         ev1.record(stream)
         torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    ms = ev0.elapsed_time(ev1)
-    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
+    rep.barrier(world)
+    ms_max = rep.max_over_ranks(ev0.elapsed_time(ev1), world, device="cuda")
     ms_per_step = ms_max / args.steps
 
     # correctness of the last step's output
@@ -209,16 +210,12 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     e2e_steps = max(1, min(args.steps, 2))
     pkg.call("cbs_aes128_ctr_transcipher", ctx.handle, ctrs.ctypes.data, blocks, out_ha.ctypes.data,
              out_hb.ctypes.data)
-    if world > 1:
-        dist.barrier()
-    t0 = time.perf_counter()
+    rep.barrier(world)
+    t0 = time.perf_counter()  # the host API call is synchronous: copies and kernels inside
     for _ in range(e2e_steps):
         pkg.call("cbs_aes128_ctr_transcipher", ctx.handle, ctrs.ctypes.data, blocks, out_ha.ctypes.data,
                  out_hb.ctypes.data)
-    e2e_s = (time.perf_counter() - t0) / e2e_steps
-    te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_ms = rep.max_over_ranks((time.perf_counter() - t0) / e2e_steps * 1e3, world, device="cuda")
     e2e_ok = verify(pkg, ctx, key, ctrs, out_ha, out_hb)
 
     chunks = -(-blocks // 256)
@@ -227,7 +224,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     launches_per_step = chunks * (1 + ROUNDS * (12 if args.backend == "fft64" else 13))
     result = {
         "metric": METRICS[args.backend],
-        "value": world * blocks / (ms_per_step * 1e-3),
+        "value": rep.whole_job_rate(world, blocks, ms_per_step),
         "unit": UNIT,
         "n_gpus": world,
         "steps": args.steps,
@@ -238,7 +235,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
         "vs_baseline": None,
         "dtype": "f64 (blind-rotation FFT products) + u64 (exact mod-Q NTT elsewhere)" if args.backend == "fft64"
                  else "u64 (exact mod-Q NTT arithmetic)",
-        "data": "synthetic (seeded random counters and key)",
+        "data": "synthetic (seeded AES key; counters: one seeded CTR stream, rank r takes blocks [r B, (r+1) B))",
         "config": {"workload": "aes128_ctr_transcipher", "blocks_per_gpu": blocks, "global_blocks": world * blocks,
                    "params": "N=2048 Q=54-bit n=630 q=2^14 BR 2^12x3 RGSW 2^6x4 HT 2^9x5 SS 2^9x5 KS 2^14/2^7",
                    "l2": "per-step working set (keys + RGSW + LUT buffers) >> 126 MB L2",
@@ -247,7 +244,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
         "us_per_bootstrap": ms_per_step * 1e3 / (blocks * 128 * ROUNDS),
         "correct_blocks": ok,
         "gpu_launches": launches_per_step * args.steps,
-        "e2e": {"value": world * blocks / float(te.item()), "unit": UNIT, "h2d_bytes_per_step": blocks * 128,
+        "e2e": {"value": rep.whole_job_rate(world, blocks, e2e_ms), "unit": UNIT, "h2d_bytes_per_step": blocks * 128,
                 "d2h_bytes_per_step": blocks * 128 * (p.n + 1) * 8, "correct_blocks": e2e_ok},
         "roofline": {"kernel": br_kernel_name(args)
                      + " (fused GINX blind rotation + finalize + MV split)", "bound": "hbm",
@@ -884,7 +881,8 @@ def main() -> None:
         import torch
         import torch.distributed as dist
         torch.cuda.set_device(local_rank)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        # short timeout: a rank that dies or hangs ends the others' next collective with an error
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     runner = {"aes128": run_ours, "blind_rotate": run_blind_rotate, "keyswitch": run_keyswitch,
               "rns_ntt": run_rns_ntt, "gate": run_gate,
               "ragged": run_ragged, "tcb": run_tcb}[args.workload]
