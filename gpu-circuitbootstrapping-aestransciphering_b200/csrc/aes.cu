@@ -211,7 +211,8 @@ cbs_status cbs_aes128_setup(cbs_context* ctx, const uint8_t* key, uint64_t seed)
     A.h_rk_words.assign(static_cast<size_t>(11) * 4 * 2 * N, 0);
     for (uint32_t r = 0; r <= 10; ++r)
         for (uint32_t col = 0; col < 4; ++col) {
-            const uint32_t w = aes::pack_be(rk[r][col * 4 + 0], rk[r][col * 4 + 1], rk[r][col * 4 + 2], rk[r][col * 4 + 3]);
+            const uint32_t w =
+                aes::pack_be(rk[r][col * 4 + 0], rk[r][col * 4 + 1], rk[r][col * 4 + 2], rk[r][col * 4 + 3]);
             std::fill(msg.begin(), msg.end(), 0);
             for (uint32_t b = 0; b < 32; ++b) msg[b] = ((w >> b) & 1u) ? delta : 0;
             uint64_t* ct = A.h_rk_words.data() + (static_cast<size_t>(r) * 4 + col) * 2 * N;
@@ -295,13 +296,15 @@ cbs_status cbs_aes128_ctr_transcipher_device(cbs_context* ctx, const uint8_t* d_
     for (uint32_t off = 0; off < blocks; off += chunk) {
         const uint32_t cur = std::min(chunk, blocks - off);
         const uint32_t T = cur * 128;
-        CBS_CUDA_TRY(launch_init_state(A.st_a.p, A.st_b.p, A.rk0_a.p, A.rk0_b.p, d_counter_bits + static_cast<size_t>(off) * 128,
+        CBS_CUDA_TRY(launch_init_state(A.st_a.p, A.st_b.p, A.rk0_a.p, A.rk0_b.p,
+                                       d_counter_bits + static_cast<size_t>(off) * 128,
                                        c->p.q_lwe >> 1, c->p.q_lwe, n, T, s));
         // graphs are built for full chunks; a ragged tail runs eagerly
         if (cbs_status st = aes_run_rounds(c, cur, s, use_graphs && cur == chunk)) return st;
         CBS_CUDA_TRY(cudaMemcpyAsync(d_out_a + static_cast<size_t>(off) * 128 * n, A.st_a.p,
                                      static_cast<size_t>(T) * n * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s));
-        CBS_CUDA_TRY(cudaMemcpyAsync(d_out_b + static_cast<size_t>(off) * 128, A.st_b.p, static_cast<size_t>(T) * sizeof(uint64_t),
+        CBS_CUDA_TRY(cudaMemcpyAsync(d_out_b + static_cast<size_t>(off) * 128, A.st_b.p,
+                                     static_cast<size_t>(T) * sizeof(uint64_t),
                                      cudaMemcpyDeviceToDevice, s));
     }
     return CBS_OK;

@@ -358,8 +358,7 @@ __global__ void __launch_bounds__(BrFftCfg<LOGN>::T, BrFftMbCfg<LOGN, MB>::MIN_B
                     ka[j] = __ldg(k0 + s * kstride + j * TH);
                     kb[j] = __ldg(k0 + s * kstride + M + j * TH);
                 }
-                const uint32_t mask = MB == 2 ? (s == 0 ? 1u : (s == 1 ? 2u : 3u))
-                                              : (s < 3 ? (1u << s) : (s == 3 ? 3u : (s == 4 ? 5u : (s == 5 ? 6u : 7u))));
+                const uint32_t mask = mb_key_mask(MB, s);
 #pragma unroll
                 for (int j = 0; j < 8; ++j) {
                     double2 m = make_double2(1.0, 0.0);
@@ -497,8 +496,12 @@ cudaError_t launch_blind_rotate_fft_mb(const BlindRotateArgs& a, const FftKeyArg
     if (mb != 2 && mb != 3) return cudaErrorInvalidValue;  // N = 4096: the per-slot c_i exceed shared memory
     cudaError_t e;
     switch (N) {
-        case 1024: e = mb == 2 ? br_fft_mb_launch<10, 2>(a, f, batch, s) : br_fft_mb_launch<10, 3>(a, f, batch, s); break;
-        case 2048: e = mb == 2 ? br_fft_mb_launch<11, 2>(a, f, batch, s) : br_fft_mb_launch<11, 3>(a, f, batch, s); break;
+        case 1024:
+            e = mb == 2 ? br_fft_mb_launch<10, 2>(a, f, batch, s) : br_fft_mb_launch<10, 3>(a, f, batch, s);
+            break;
+        case 2048:
+            e = mb == 2 ? br_fft_mb_launch<11, 2>(a, f, batch, s) : br_fft_mb_launch<11, 3>(a, f, batch, s);
+            break;
         default: return cudaErrorInvalidValue;
     }
     if (e != cudaSuccess || !mv_ntt) return e;

@@ -235,7 +235,8 @@ __device__ __forceinline__ void cmux_diff_words(uint2* ws, const uint64_t* in0, 
         const uint32_t lo = p * N + e, hi = lo + M;
         const uint64_t dr = sub_mod(__ldg(in1 + lo), __ldg(in0 + lo), g.q);
         const uint64_t di = sub_mod(__ldg(in1 + hi), __ldg(in0 + hi), g.q);
-        ws[e] = make_uint2(static_cast<uint32_t>(prepared_offset(dr, g)), static_cast<uint32_t>(prepared_offset(di, g)));
+        ws[e] = make_uint2(static_cast<uint32_t>(prepared_offset(dr, g)),
+                           static_cast<uint32_t>(prepared_offset(di, g)));
     }
 }
 
@@ -491,7 +492,8 @@ cudaError_t launch_trace_ss_fft(const TraceFftArgs& a, const FftKeyArgs& f, uint
 cudaError_t launch_cmux_level_fft(const CmuxFftArgs& a, const FftKeyArgs& f, uint32_t N, uint32_t luts,
                                   cudaStream_t s) {
     if (luts == 0) return cudaSuccess;
-    if (a.in_count < 2 || a.digits == 0 || a.digits * static_cast<uint32_t>(a.g.gbits) > 32) return cudaErrorInvalidValue;
+    if (a.in_count < 2 || a.digits == 0 || a.digits * static_cast<uint32_t>(a.g.gbits) > 32)
+        return cudaErrorInvalidValue;
     if (luts > 65535 || (a.in_spec && a.level != 0)) return cudaErrorInvalidValue;
     switch (N) {
         case 1024: return cmux_fft_launch<10>(a, f, luts, s);

@@ -56,7 +56,8 @@ __device__ __forceinline__ void rotate_add(uint64_t* acc, const uint64_t* t, uin
 }
 
 template <int LOGN>
-__global__ void __launch_bounds__(NttPlan<LOGN>::T, 256 / NttPlan<LOGN>::T + (NttPlan<LOGN>::T < 512)) k_blind_rotate(const BlindRotateArgs a) {
+__global__ void __launch_bounds__(NttPlan<LOGN>::T, 256 / NttPlan<LOGN>::T + (NttPlan<LOGN>::T < 512))
+    k_blind_rotate(const BlindRotateArgs a) {
     constexpr uint32_t N = 1u << LOGN, T = NttPlan<LOGN>::T, TWO_N = 2 * N;
     extern __shared__ uint64_t smem[];
     uint64_t* acc0 = smem;
@@ -92,7 +93,8 @@ __global__ void __launch_bounds__(NttPlan<LOGN>::T, 256 / NttPlan<LOGN>::T + (Nt
             ntt_forward_to_regs<LOGN>(
                 scr, tid, t.rp, t.rps, Q, [&](uint32_t i) { return digit_mod(src[i], a.g, d); }, x);
             const ulonglong2* k0 = reinterpret_cast<const ulonglong2*>(ek + static_cast<size_t>(r) * 2 * N + 8 * tid);
-            const ulonglong2* k1 = reinterpret_cast<const ulonglong2*>(ek + static_cast<size_t>(r) * 2 * N + N + 8 * tid);
+            const ulonglong2* k1 =
+                reinterpret_cast<const ulonglong2*>(ek + static_cast<size_t>(r) * 2 * N + N + 8 * tid);
 #pragma unroll
             for (int h = 0; h < 4; ++h) {
                 const ulonglong2 v0 = __ldg(k0 + h), v1 = __ldg(k1 + h);
@@ -143,7 +145,8 @@ __global__ void __launch_bounds__(NttPlan<LOGN>::T, 256 / NttPlan<LOGN>::T + (Nt
 }
 
 template <int LOGN>
-__global__ void __launch_bounds__(NttPlan<LOGN>::T, 256 / NttPlan<LOGN>::T + (NttPlan<LOGN>::T < 512)) k_trace_ss(const TraceArgs a) {
+__global__ void __launch_bounds__(NttPlan<LOGN>::T, 256 / NttPlan<LOGN>::T + (NttPlan<LOGN>::T < 512))
+    k_trace_ss(const TraceArgs a) {
     constexpr uint32_t N = 1u << LOGN, T = NttPlan<LOGN>::T;
     extern __shared__ uint64_t smem[];
     uint64_t* c0 = smem;
@@ -226,7 +229,8 @@ __global__ void __launch_bounds__(NttPlan<LOGN>::T, 256 / NttPlan<LOGN>::T + (Nt
 }
 
 template <int LOGN>
-__global__ void __launch_bounds__(NttPlan<LOGN>::T, 256 / NttPlan<LOGN>::T + (NttPlan<LOGN>::T < 512)) k_cmux_level(const CmuxLevelArgs a) {
+__global__ void __launch_bounds__(NttPlan<LOGN>::T, 256 / NttPlan<LOGN>::T + (NttPlan<LOGN>::T < 512))
+    k_cmux_level(const CmuxLevelArgs a) {
     constexpr uint32_t N = 1u << LOGN, T = NttPlan<LOGN>::T;
     (void)T;
     extern __shared__ uint64_t smem[];
@@ -245,7 +249,8 @@ __global__ void __launch_bounds__(NttPlan<LOGN>::T, 256 / NttPlan<LOGN>::T + (Nt
     __syncthreads();
     ntt_inverse_cta<LOGN>(
         scr, tid, t.irp, t.irps, t.n_inv, t.n_inv_s, Q,
-        [&](int, uint32_t k) { return sub_mod(in1[N + k], in0[N + k], Q); }, [&](uint32_t k, uint64_t v) { d1[k] = v; });
+        [&](int, uint32_t k) { return sub_mod(in1[N + k], in0[N + k], Q); },
+        [&](uint32_t k, uint64_t v) { d1[k] = v; });
     __syncthreads();
 
     const uint32_t bit = __ldg(a.ctrl_bits + static_cast<size_t>(lut) * 8 + a.level);

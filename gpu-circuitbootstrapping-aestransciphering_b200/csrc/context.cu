@@ -452,7 +452,8 @@ static cbs_status upload_host_keys(cbs_context* c) {
         const size_t rows = c->hk.ksk.size() / (c->p.n + 1), stride = ksk_row_stride(c->p.n);
         std::vector<uint16_t> padded(rows * stride, 0);
         for (size_t r = 0; r < rows; ++r)
-            std::memcpy(padded.data() + r * stride, c->hk.ksk.data() + r * (c->p.n + 1), (c->p.n + 1) * sizeof(uint16_t));
+            std::memcpy(padded.data() + r * stride, c->hk.ksk.data() + r * (c->p.n + 1),
+                        (c->p.n + 1) * sizeof(uint16_t));
         CBS_CUDA_TRY(c->d_ksk.upload(padded.data(), padded.size(), s));
     }
     CBS_CUDA_TRY(c->d_tv.upload(c->hk.tv.data(), c->hk.tv.size(), s));
@@ -509,7 +510,8 @@ cbs_status cbs_import_keys(cbs_context* ctx, const int32_t* s_lwe, const int32_t
     for (size_t i = 0; i < n_ksk; ++i)
         CBS_CHECK_ARG(ksk[i] < p.qks, "import_keys: key-switching key entries must be below qks");
     if (s_lwe) {
-        for (uint32_t i = 0; i < n; ++i) CBS_CHECK_ARG(s_lwe[i] == 0 || s_lwe[i] == 1, "import_keys: s_lwe must be binary");
+        for (uint32_t i = 0; i < n; ++i)
+            CBS_CHECK_ARG(s_lwe[i] == 0 || s_lwe[i] == 1, "import_keys: s_lwe must be binary");
         for (uint32_t i = 0; i < N; ++i)
             CBS_CHECK_ARG(s_rlwe[i] >= -1 && s_rlwe[i] <= 1, "import_keys: s_rlwe must be ternary");
     }
@@ -647,8 +649,8 @@ cbs_status cbs_generate_mb_bsk_host(const cbs_params* params, uint64_t seed, uin
 }
 
 cbs_status cbs_generate_keys_host(const cbs_params* params, uint64_t seed, int32_t* s_lwe, int32_t* s_rlwe,
-                                  uint64_t* bsk, uint64_t* ht, uint64_t* ss, uint16_t* ksk, uint64_t* tv, uint64_t* gpow,
-                                  uint32_t* maps) {
+                                  uint64_t* bsk, uint64_t* ht, uint64_t* ss, uint16_t* ksk, uint64_t* tv,
+                                  uint64_t* gpow, uint32_t* maps) {
     CBS_CHECK_ARG(params, "generate_keys_host: null params");
     if (cbs_status st = validate(*params)) return st;
     host::NttTables t;
@@ -780,7 +782,8 @@ cbs_status cbs_lut8x32_batch_device(cbs_context* ctx, const uint64_t* d_tables, 
     CBS_CHECK_ARG(rgsw_stride >= static_cast<uint64_t>(ctx->p.num_lut) * 4 * ctx->p.N, "lut: rgsw_stride too small");
     for (uint32_t u = 0; u < luts; ++u) {
         CBS_CHECK_ARG(h_table_of_lut[u] < num_tables, "lut: table index out of range");
-        for (uint32_t k = 0; k < 8; ++k) CBS_CHECK_ARG(h_ctrl_bits[u * 8 + k] < num_bits, "lut: control bit out of range");
+        for (uint32_t k = 0; k < 8; ++k)
+            CBS_CHECK_ARG(h_ctrl_bits[u * 8 + k] < num_bits, "lut: control bit out of range");
     }
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const size_t N = ctx->p.N;

@@ -8,6 +8,13 @@
 
 namespace cbs {
 
+// bit mask of the LWE coefficients in grouped key kk of a group of mb (the subset order of the
+// grouped keys: mb = 2: {0} {1} {0,1}; mb = 3: {0} {1} {2} {0,1} {0,2} {1,2} {0,1,2})
+__host__ __device__ constexpr uint32_t mb_key_mask(int mb, uint32_t kk) {
+    if (mb == 2) return kk == 0 ? 1u : (kk == 1 ? 2u : 3u);
+    return kk < 3 ? (1u << kk) : (kk == 3 ? 3u : (kk == 4 ? 5u : (kk == 5 ? 6u : 7u)));
+}
+
 // v mod Q, v the FP64 value of an integer-valued product (|v| < 2^90), computed in FP64:
 // k = rint(v / Q), r = v - k*q_hi - k*q_lo with two fused multiply-adds.  The two roundings of
 // r (|r| < 2Q < 2^55) add at most +-8 to the result, far below the FFT's own rounding error.
@@ -107,7 +114,8 @@ __device__ __forceinline__ int64_t prepared_offset(uint64_t x, const DigitPrep& 
 
 // x in [0, Q) as the centred value, in FP64
 __device__ __forceinline__ double centred_double(uint64_t x, uint64_t Q, uint64_t qhalf) {
-    return static_cast<double>(x >= qhalf ? static_cast<int64_t>(x) - static_cast<int64_t>(Q) : static_cast<int64_t>(x));
+    return static_cast<double>(x >= qhalf ? static_cast<int64_t>(x) - static_cast<int64_t>(Q)
+                                          : static_cast<int64_t>(x));
 }
 
 }  // namespace cbs

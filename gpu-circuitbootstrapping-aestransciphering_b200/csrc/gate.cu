@@ -507,7 +507,8 @@ __global__ void __launch_bounds__(GateMbCfg<LOGN>::T, GateMbCfg<LOGN>::MIN_BLOCK
 #pragma unroll
             for (int i = 0; i < MB; ++i) {
                 const uint32_t idx = g * MB + i;
-                at[i] = idx < a.n ? ms(a.reqs ? __ldg(a1 + idx) : gate_a(a.gate, __ldg(a1 + idx), __ldg(a2 + idx))) : 0u;
+                at[i] = idx < a.n ? ms(a.reqs ? __ldg(a1 + idx) : gate_a(a.gate, __ldg(a1 + idx), __ldg(a2 + idx)))
+                                  : 0u;
                 any |= at[i];
             }
             if (any == 0) continue;  // every m_S is 0 (uniform over the CTA)
@@ -561,9 +562,7 @@ __global__ void __launch_bounds__(GateMbCfg<LOGN>::T, GateMbCfg<LOGN>::MIN_BLOCK
                         ka[j] = __ldg(k0 + sub * kstride + j * TH);
                         kb[j] = __ldg(k0 + sub * kstride + M + j * TH);
                     }
-                    const uint32_t mask = MB == 2 ? (sub == 0 ? 1u : (sub == 1 ? 2u : 3u))
-                                                  : (sub < 3 ? (1u << sub)
-                                                             : (sub == 3 ? 3u : (sub == 4 ? 5u : (sub == 5 ? 6u : 7u))));
+                    const uint32_t mask = mb_key_mask(MB, sub);
 #pragma unroll
                     for (int j = 0; j < 8; ++j) {
                         double2 m = make_double2(1.0, 0.0);
@@ -883,7 +882,8 @@ void torus_keys_to_fft(uint32_t N, const uint64_t* keys, size_t count, std::vect
 cudaError_t gate_keyswitch(const GateArgs& a, const uint32_t* ksk, uint32_t n, uint32_t N, uint32_t ks_bits,
                            uint32_t ks_levels, uint32_t* out_a, uint32_t* out_b, cudaStream_t s) {
     const dim3 grid(a.items, (n + 1 + 255) / 256);
-    k_gate_keyswitch<<<grid, 256, (N + 1) * sizeof(uint32_t), s>>>(static_cast<const uint32_t*>(a.ext), ksk, n, N, ks_bits, ks_levels, out_a, out_b,
+    k_gate_keyswitch<<<grid, 256, (N + 1) * sizeof(uint32_t), s>>>(static_cast<const uint32_t*>(a.ext), ksk, n, N,
+                                                                   ks_bits, ks_levels, out_a, out_b,
                                                                    a.reqs, a.num_reqs);
     return cudaGetLastError();
 }
@@ -1032,7 +1032,8 @@ void gate_keys_host(const cbs_gate_params& p, uint64_t seed, std::vector<int32_t
     for (uint32_t i = 0; i < N; ++i)
         for (uint32_t l = 0; l < p.ks_levels; ++l)
             for (uint32_t v = 1; v < base; ++v) {
-                uint32_t* row = ksk.data() + ((static_cast<size_t>(i) * p.ks_levels + l) * (base - 1) + v - 1) * (n + 1);
+                uint32_t* row =
+                    ksk.data() + ((static_cast<size_t>(i) * p.ks_levels + l) * (base - 1) + v - 1) * (n + 1);
                 uint32_t b = torus_noise(rng, p.sigma_lwe);
                 for (uint32_t j = 0; j < n; ++j) {
                     row[j] = static_cast<uint32_t>(rng.next());
@@ -1307,7 +1308,8 @@ static cbs_status gate_run(cbs_gate_context* ctx, int gate, const uint32_t* d_a1
     if (d_out_a && d_out_b) {
         const dim3 grid(count, (p.n + 1 + 255) / 256);
         cbs::k_gate_keyswitch<<<grid, 256, (p.N + 1) * sizeof(uint32_t), s>>>(
-            static_cast<const uint32_t*>(a.ext), ctx->d_ksk.p, p.n, p.N, p.ks_base_bits, p.ks_levels, d_out_a, d_out_b, nullptr, 0);
+            static_cast<const uint32_t*>(a.ext), ctx->d_ksk.p, p.n, p.N, p.ks_base_bits, p.ks_levels, d_out_a, d_out_b,
+            nullptr, 0);
         CBS_LAUNCH_CHECK();
     }
     return CBS_OK;
@@ -1376,7 +1378,8 @@ cbs_status cbs_gate_ragged_launch(cbs_gate_context* ctx, cbs_stream_t stream) {
     CBS_CUDA_TRY(cbs::gate_blind_rotate(a, p.N, ctx->plan_grid, stream));
     const dim3 grid(ctx->plan_items, (p.n + 1 + 255) / 256);
     cbs::k_gate_keyswitch<<<grid, 256, (p.N + 1) * sizeof(uint32_t), stream>>>(
-        static_cast<const uint32_t*>(a.ext), ctx->d_ksk.p, p.n, p.N, p.ks_base_bits, p.ks_levels, nullptr, nullptr, a.reqs, a.num_reqs);
+        static_cast<const uint32_t*>(a.ext), ctx->d_ksk.p, p.n, p.N, p.ks_base_bits, p.ks_levels, nullptr, nullptr,
+        a.reqs, a.num_reqs);
     CBS_LAUNCH_CHECK();
     return CBS_OK;
 }

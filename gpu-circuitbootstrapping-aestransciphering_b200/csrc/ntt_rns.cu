@@ -303,7 +303,8 @@ __global__ void __launch_bounds__(kGroups * (1 << L1) / 8) k_rns_inv_cols(uint64
     const uint64_t scs = a.scale ? a.scale_s[limb_flat % a.limbs] : 0;
     uint64_t* poly = limb_ptr(data, a, limb_flat, L1 + kL2) + colblk * kGroups + g;
     sub_inv<L1>(
-        sm + g * col_stride<L1>(), gt, itw, itws, q, [](uint32_t m) { return m; }, [&](uint32_t e) { return poly[e * ROW]; },
+        sm + g * col_stride<L1>(), gt, itw, itws, q, [](uint32_t m) { return m; },
+        [&](uint32_t e) { return poly[e * ROW]; },
         [&](uint32_t e, uint64_t v, int j) {
             v = csub(v, q);
             if (j < 4) v = mul_shoup(v, ninv, ninvs, q);  // x-half of the m = 1 stage

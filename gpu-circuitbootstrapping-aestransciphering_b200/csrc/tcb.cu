@@ -481,7 +481,8 @@ cbs_status cbs_tcb_context_create(const cbs_tcb_params* params, uint32_t max_bat
     CBS_CHECK_ARG(params && out, "tcb_context_create: null argument");
     *out = nullptr;
     if (cbs_status st = validate_tcb(*params)) return st;
-    CBS_CHECK_ARG(params->N2 == 1024 || params->N2 == 2048, "tcb_context_create: the device blind rotation needs N2 of 1024 or 2048");
+    CBS_CHECK_ARG(params->N2 == 1024 || params->N2 == 2048,
+                  "tcb_context_create: the device blind rotation needs N2 of 1024 or 2048");
     CBS_CHECK_ARG(params->N1 >= 256, "tcb_context_create: the device PFKS needs N1 >= 256");
     CBS_CHECK_ARG(max_batch >= 1 && max_batch <= (1u << 20), "tcb_context_create: max_batch out of range");
     auto* c = new (std::nothrow) cbs_tcb_context();

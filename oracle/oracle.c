@@ -836,7 +836,8 @@ void orc_moddown(const uint64_t *cx, uint64_t *ct, uint32_t log_n, const uint64_
         for (uint32_t k = 0; k < size_p; ++k) P = orc_mulmod(P, p[k] % q[i], q[i]);
         const uint64_t pinv = orc_invmod(P, q[i]);
         for (uint32_t c = 0; c < n; ++c)
-            ct[(size_t)i * n + c] = orc_mulmod(submod(cx[(size_t)i * n + c], delta[(size_t)i * n + c], q[i]), pinv, q[i]);
+            ct[(size_t)i * n + c] =
+                orc_mulmod(submod(cx[(size_t)i * n + c], delta[(size_t)i * n + c], q[i]), pinv, q[i]);
     }
     free(dst);
     free(delta);
@@ -957,7 +958,8 @@ void orc_gate_blind_rotate_tv(const orc_gate_params *p, const uint32_t *bsk, con
         memset(prod, 0, 2 * N * sizeof(uint32_t));
         const uint32_t *key = bsk + (size_t)step * 2 * L * 2 * N;
         for (uint32_t r = 0; r < 2 * L; ++r)
-            for (uint32_t c = 0; c < 2; ++c) torus_mac(prod + c * N, dig + (size_t)r * N, key + ((size_t)r * 2 + c) * N, N);
+            for (uint32_t c = 0; c < 2; ++c)
+                torus_mac(prod + c * N, dig + (size_t)r * N, key + ((size_t)r * 2 + c) * N, N);
         for (uint32_t c = 0; c < 2; ++c) {
             torus_rot_add(acc + c * N, prod + c * N, at, N);
             for (uint32_t i = 0; i < N; ++i) acc[c * N + i] -= prod[c * N + i];
@@ -1013,7 +1015,8 @@ void orc_tcb_blind_rotate64(const orc_gate_params *p, const uint64_t *bsk, const
         memset(prod, 0, 2 * N * sizeof(uint64_t));
         const uint64_t *key = bsk + (size_t)step * 2 * L * 2 * N;
         for (uint32_t r = 0; r < 2 * L; ++r)
-            for (uint32_t c = 0; c < 2; ++c) torus64_mac(prod + c * N, dig + (size_t)r * N, key + ((size_t)r * 2 + c) * N, N);
+            for (uint32_t c = 0; c < 2; ++c)
+                torus64_mac(prod + c * N, dig + (size_t)r * N, key + ((size_t)r * 2 + c) * N, N);
         for (uint32_t c = 0; c < 2; ++c)
             for (uint32_t i = 0; i < N; ++i) {
                 const uint32_t t = (i + at) % two_n;

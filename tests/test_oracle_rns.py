@@ -12,7 +12,8 @@ import numpy as np
 import pytest
 
 from conftest import oracle_tables
-from rns_harness import crt_centered, declare_rns, make_switch_key, mulmod, ntt, rns_primes, small_to_rns, submod, addmod
+from rns_harness import (addmod, crt_centered, declare_rns, make_switch_key, mulmod, ntt, rns_primes, small_to_rns,
+                         submod)
 
 
 @pytest.fixture(scope="module")

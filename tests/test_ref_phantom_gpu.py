@@ -51,7 +51,8 @@ def test_1d_batched_matches_reference_kernel(ref):
     dm = pkg.DModulus()
     pkg.call("cbs_ntt_tables_host", n, q, *(t.ctypes.data for t in tabs), ninv.ctypes.data, ctypes.addressof(dm))
     d_tabs = [_dev(t) for t in tabs]
-    d_mod = torch.from_numpy(np.array([dm.value, dm.const_ratio[0], dm.const_ratio[1]], np.uint64).view(np.int64)).cuda()
+    dmod = np.array([dm.value, dm.const_ratio[0], dm.const_ratio[1]], np.uint64)
+    d_mod = torch.from_numpy(dmod.view(np.int64)).cuda()
     d_ninv = _dev(ninv)
     rng = np.random.default_rng(4)
     x = rng.integers(0, q, size=(37, n), dtype=np.uint64)

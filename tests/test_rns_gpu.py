@@ -6,7 +6,8 @@ import numpy as np
 import pytest
 
 from conftest import load_pkg, load_oracle
-from rns_harness import declare_rns, make_switch_key, mulmod, ntt, rns_primes, small_to_rns, submod, addmod, crt_centered
+from rns_harness import (addmod, crt_centered, declare_rns, make_switch_key, mulmod, ntt, rns_primes, small_to_rns,
+                         submod)
 
 pytestmark = pytest.mark.gpu
 
