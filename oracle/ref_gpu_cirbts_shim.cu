@@ -6,6 +6,7 @@
 // binary MAC with the AoS key).  Test infrastructure only: the GPU tests compare the
 // accumulator it produces with the oracle's, which the product's NTT path matches bit for bit.
 #include <cstdint>
+#include <utility>
 #include <vector>
 
 #include "cirbts/kernel.cuh"
@@ -58,6 +59,64 @@ int ref_cirbts_blind_rotate_steps(uint64_t* acc, const uint64_t* d_a, uint32_t a
     cudaFree(ct);
     cudaFree(dct);
     cudaFree(index_pos);
+    return static_cast<int>(e);
+}
+
+// HomTrace + SchemeSwitch of count MV RLWEs in the reference's default (unfused) launch
+// sequence (bitwise/src/cirbts/cirbts-batch.cu:1656-1789): per round k the permuting INTT of
+// c0, kernel_Fused_Permute_Decompose, the NTT of the digits and
+// kernel_MultAddUpdate_HT_PermuteC1; kernel_SaveToRGSW of the trace (row 1); then INTT,
+// decomposition, NTT and kernel_MultAddUpdate_SS against the s^2 key, saved as row 0.
+// c0 / c1 [count][N] NTT domain (the MV RLWEs' two components), keys [rounds][digits_ht][2][N]
+// and [digits_ss][2][N] with their Shoup tables, maps_out [rounds][N] receives the
+// automorphism maps from the reference's kernel_GenerateCoefficientAutoMaps, rgsw_out
+// [count][2 rows][2][N].  Returns the CUDA error code.
+int ref_cirbts_trace_schemeswitch(const uint64_t* c0_in, const uint64_t* c1_in, uint32_t count, const uint64_t* ht_key,
+                                  const uint64_t* ht_key_shoup, const uint64_t* ss_key, const uint64_t* ss_key_shoup,
+                                  uint32_t rounds, uint32_t base_ht, uint32_t digits_ht, uint32_t base_ss,
+                                  uint32_t digits_ss, uint32_t* maps_out, const void* d_mod, const uint64_t* tw,
+                                  const uint64_t* tws, const uint64_t* itw, const uint64_t* itws, const uint64_t* ninv,
+                                  const uint64_t* ninv_s, uint32_t N, uint64_t Q, uint64_t* rgsw_out, void* stream) {
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const DModulus* mod = static_cast<const DModulus*>(d_mod);
+    uint32_t logn = 0;
+    while ((1u << logn) < N) ++logn;
+    const size_t plane = static_cast<size_t>(count) * N;
+    const uint32_t dmax = digits_ht > digits_ss ? digits_ht : digits_ss;
+    uint64_t *c0 = nullptr, *c1 = nullptr, *n0 = nullptr, *n1 = nullptr, *perm = nullptr, *dig = nullptr, *s0 = nullptr,
+             *s1 = nullptr;
+    cudaError_t e = cudaSuccess;
+    for (uint64_t** b : {&c0, &c1, &n0, &n1, &perm, &s0, &s1})
+        if (e == cudaSuccess) e = cudaMalloc(b, sizeof(uint64_t) * plane);
+    if (e == cudaSuccess) e = cudaMalloc(&dig, sizeof(uint64_t) * plane * dmax);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(c0, c0_in, sizeof(uint64_t) * plane, cudaMemcpyDeviceToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(c1, c1_in, sizeof(uint64_t) * plane, cudaMemcpyDeviceToDevice, s);
+    if (e == cudaSuccess) {
+        const dim3 block(256), grid((N + 255) / 256, count);
+        kernel_GenerateCoefficientAutoMaps<<<dim3((N + 255) / 256, rounds), block, 0, s>>>(maps_out, N, logn, 2 * N - 1,
+                                                                                            rounds);
+        for (uint32_t k = 0; k < rounds; ++k) {
+            const uint32_t* map = maps_out + static_cast<size_t>(k) * N;
+            inwt_1d_opt_permute_batched(perm, c0, map, itw, itws, mod, ninv, ninv_s, N, count, s);
+            kernel_Fused_Permute_Decompose<<<grid, block, 0, s>>>(dig, perm, Q, base_ht, digits_ht, N, count);
+            fnwt_1d_opt_batched(dig, tw, tws, mod, N, static_cast<size_t>(count) * digits_ht, s);
+            const size_t kofs = static_cast<size_t>(k) * digits_ht * 2 * N;
+            kernel_MultAddUpdate_HT_PermuteC1<<<grid, block, 0, s>>>(n0, n1, dig, ht_key + kofs, ht_key_shoup + kofs, c0,
+                                                                      c1, map, mod, digits_ht, N, count, plane);
+            std::swap(c0, n0);
+            std::swap(c1, n1);
+        }
+        kernel_SaveToRGSW<<<grid, block, 0, s>>>(rgsw_out, c0, c1, 1, N, count);
+        inwt_1d_opt_batched(c0, itw, itws, mod, ninv, ninv_s, N, count, s);
+        kernel_Fused_Permute_Decompose<<<grid, block, 0, s>>>(dig, c0, Q, base_ss, digits_ss, N, count);
+        fnwt_1d_opt_batched(dig, tw, tws, mod, N, static_cast<size_t>(count) * digits_ss, s);
+        kernel_MultAddUpdate_SS<<<grid, block, 0, s>>>(s0, s1, dig, ss_key, ss_key_shoup, c1, mod, digits_ss, N, count,
+                                                        plane);
+        kernel_SaveToRGSW<<<grid, block, 0, s>>>(rgsw_out, s0, s1, 0, N, count);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    }
+    for (uint64_t* b : {c0, c1, n0, n1, perm, dig, s0, s1}) cudaFree(b);
     return static_cast<int>(e);
 }
 

@@ -1,13 +1,17 @@
-"""The oracle's one-bit GINX blind rotation against the reference's own CirBTS kernels
-(bitwise/src/cirbts/kernel.cu: kernel_SpecialMS_IndexPos_Batch, kernel_SignedDigitDecompose2_
-FusedFNWT_Batch, kernel_EvalAccCore_Binary_Batch; Phantom's inwt_1d_opt_outofplace_batched),
-rebuilt for sm_100a by `make -C oracle ref_gpu_cirbts` and launched in the reference's
-per-step sequence (ref_gpu_cirbts_shim.cu).  From the same initial accumulator, with the
-product's keys (its [n][2 digits][2][N] NTT-domain layout is the reference's AoS RF key),
-n = 630 steps of the reference kernels give the oracle's accumulator word for word.  The
-product's exact-NTT blind rotation is bit-identical to the oracle (test_cbs_gpu.py), so this
-pins a9's arithmetic -- modulus switch, signed gadget decomposition, key products, monomial
-multiplication -- against the reference itself."""
+"""The oracle's blind rotation (a9) and HomTrace + SchemeSwitch (a10) against the reference's
+own CirBTS kernels (bitwise/src/cirbts/kernel.cu) and Phantom's 1-D NTT (src/ntt/ntt_1d.cu),
+rebuilt for sm_100a by `make -C oracle ref_gpu_cirbts` and launched in the reference's launch
+sequences (ref_gpu_cirbts_shim.cu):
+* blind rotation: kernel_SpecialMS_IndexPos_Batch, then per step inwt_1d_opt_outofplace_batched,
+  kernel_SignedDigitDecompose2_FusedFNWT_Batch and kernel_EvalAccCore_Binary_Batch with the
+  product's keys (its [n][2 digits][2][N] NTT-domain layout is the reference's AoS RF key):
+  from the same initial accumulator, n = 630 steps give the oracle's accumulator word for word;
+* HomTrace + SchemeSwitch: kernel_GenerateCoefficientAutoMaps, per round the permuting INTT,
+  kernel_Fused_Permute_Decompose, the NTT and kernel_MultAddUpdate_HT_PermuteC1, then
+  kernel_MultAddUpdate_SS and kernel_SaveToRGSW: the oracle's RGSW rows word for word, and the
+  product's automorphism maps.
+The product's exact-NTT kernels are bit-identical to the oracle (test_cbs_gpu.py), so these pin
+a9 and a10 against the reference itself."""
 from __future__ import annotations
 
 import ctypes
@@ -95,3 +99,48 @@ def test_blind_rotation_matches_reference_kernels(pkg, oracle, ref):
     got = dev["acc"].cpu().numpy().view(np.uint64).reshape(batch, 2, N)
     assert not np.array_equal(got, init)
     assert np.array_equal(got, want)
+
+
+def test_trace_schemeswitch_matches_reference_kernels(pkg, oracle, ref):
+    """HomTrace + SchemeSwitch (a10) in the reference's default launch sequence on the same
+    MV RLWEs and keys give the oracle's RGSW rows word for word, and the reference's own
+    automorphism-map kernel gives the product's maps."""
+    vp, u32, u64 = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64
+    ref.ref_cirbts_trace_schemeswitch.argtypes = [vp, vp, u32, vp, vp, vp, vp, u32, u32, u32, u32, u32, vp, vp, vp,
+                                                  vp, vp, vp, vp, vp, u32, u64, vp, vp]
+    ref.ref_cirbts_trace_schemeswitch.restype = ctypes.c_int
+    oracle.orc_trace_schemeswitch.argtypes = [vp, vp, vp, u32, vp]
+    p = pkg.default_params()
+    N, Q = p.N, p.Q
+    rounds = N.bit_length() - 1 - p.trace_shift
+    keys = pkg.generate_keys_host(p, 29)
+    oc = OracleCbs(oracle, p, keys)
+    count = 4
+    ct = np.random.default_rng(10).integers(0, Q, size=(count, 2, N), dtype=np.uint64)
+    want = np.zeros((count, 2, 2, N), np.uint64)
+    oracle.orc_trace_schemeswitch(ctypes.byref(oc.op), ctypes.byref(oc.ok), ct.ctypes.data, count, want.ctypes.data)
+
+    tabs = [np.zeros(N, np.uint64) for _ in range(4)]
+    ninv = np.zeros(2, np.uint64)
+    dm = pkg.DModulus()
+    pkg.call("cbs_ntt_tables_host", N, Q, *(t.ctypes.data for t in tabs), ninv.ctypes.data, ctypes.addressof(dm))
+    ht = np.ascontiguousarray(keys["ht"]).reshape(-1)
+    ss = np.ascontiguousarray(keys["ss"]).reshape(-1)
+    hts, sss = np.zeros_like(ht), np.zeros_like(ss)
+    ref.ref_cirbts_shoup(ht.ctypes.data, hts.ctypes.data, ht.size, Q)
+    ref.ref_cirbts_shoup(ss.ctypes.data, sss.ctypes.data, ss.size, Q)
+    dmod = np.array([dm.value, dm.const_ratio[0], dm.const_ratio[1]], np.uint64)
+    dev = {name: _dev(v) for name, v in [("c0", ct[:, 0, :]), ("c1", ct[:, 1, :]), ("ht", ht), ("hts", hts),
+                                         ("ss", ss), ("sss", sss), ("mod", dmod), ("tw", tabs[0]), ("tws", tabs[1]),
+                                         ("itw", tabs[2]), ("itws", tabs[3]), ("ninv", ninv)]}
+    maps = torch.zeros((rounds, N), dtype=torch.int32, device="cuda")
+    rows = torch.zeros((count, 2, 2, N), dtype=torch.int64, device="cuda")
+    st = ref.ref_cirbts_trace_schemeswitch(
+        dev["c0"].data_ptr(), dev["c1"].data_ptr(), count, dev["ht"].data_ptr(), dev["hts"].data_ptr(),
+        dev["ss"].data_ptr(), dev["sss"].data_ptr(), rounds, p.base_ht, p.digits_ht, p.base_ss, p.digits_ss,
+        maps.data_ptr(), dev["mod"].data_ptr(), dev["tw"].data_ptr(), dev["tws"].data_ptr(), dev["itw"].data_ptr(),
+        dev["itws"].data_ptr(), dev["ninv"].data_ptr(), dev["ninv"].data_ptr() + 8, N, Q, rows.data_ptr(), None)
+    torch.cuda.synchronize()
+    assert st == 0
+    assert np.array_equal(maps.cpu().numpy().view(np.uint32), np.asarray(keys["maps"]).reshape(rounds, N))
+    assert np.array_equal(rows.cpu().numpy().view(np.uint64), want)
