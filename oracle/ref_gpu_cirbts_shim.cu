@@ -62,6 +62,54 @@ int ref_cirbts_blind_rotate_steps(uint64_t* acc, const uint64_t* d_a, uint32_t a
     return static_cast<int>(e);
 }
 
+// Grouped (mb = 2) blind rotation in the reference's CIRBTS_PBS_MULTIBIT=2 launch sequence
+// (bitwise/src/cirbts/cirbts-batch.cu:4402-4470): per group the INTT and fused
+// decomposition/NTT, then kernel_EvalAccCore_Binary_MB2_Grouped_Batch (or the one-key grouped
+// kernel for an odd tail coefficient).  ek / ek_shoup: the reference's grouped RF key
+// [3 subsets {0} {1} {0,1}][ceil(n/2)][2 digits][2][N] and its Shoup table; the rest as
+// ref_cirbts_blind_rotate_steps.
+int ref_cirbts_blind_rotate_mb2(uint64_t* acc, const uint64_t* d_a, uint32_t a_stride, uint32_t n, uint32_t batch,
+                                const uint64_t* ek, const uint64_t* ek_shoup, const uint64_t* monic, const void* d_mod,
+                                const uint64_t* tw, const uint64_t* tws, const uint64_t* itw, const uint64_t* itws,
+                                const uint64_t* ninv, const uint64_t* ninv_s, uint32_t N, uint64_t Q, uint32_t base_g,
+                                uint32_t digits_g, uint64_t q_lwe, uint32_t bitwidth, void* stream) {
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const DModulus* mod = static_cast<const DModulus*>(d_mod);
+    const uint32_t digitsG2 = 2 * digits_g, twoN = 2 * N, groups = (n + 1) / 2;
+    const size_t key_block = static_cast<size_t>(groups) * digitsG2 * 2 * N;
+    uint64_t *ct = nullptr, *dct = nullptr;
+    uint32_t* index_pos = nullptr;
+    cudaError_t e = cudaMalloc(&ct, sizeof(uint64_t) * 2 * N * batch);
+    if (e == cudaSuccess) e = cudaMalloc(&dct, sizeof(uint64_t) * digitsG2 * N * batch);
+    if (e == cudaSuccess) e = cudaMalloc(&index_pos, sizeof(uint32_t) * n * batch);
+    if (e == cudaSuccess) {
+        kernel_SpecialMS_IndexPos_Batch<<<dim3((n + 255) / 256, batch), 256, 0, s>>>(d_a, index_pos, n, batch, a_stride,
+                                                                                     twoN, q_lwe, bitwidth);
+        const uint32_t tpb = N / 2 < 256 ? N / 2 : 256;
+        const dim3 eb(256), eg((N + 255) / 256, batch);
+        for (uint32_t g = 0; g < groups && e == cudaSuccess; ++g) {
+            const uint32_t idx0 = 2 * g, idx1 = idx0 + 1;
+            inwt_1d_opt_outofplace_batched(ct, acc, itw, itws, mod, ninv, ninv_s, N, static_cast<size_t>(2) * batch,
+                                           s);
+            kernel_SignedDigitDecompose2_FusedFNWT_Batch<<<digitsG2 * batch, tpb, N * sizeof(uint64_t), s>>>(
+                dct, ct, Q, base_g, digits_g, N, batch, tw, tws, mod);
+            if (idx1 < n)
+                kernel_EvalAccCore_Binary_MB2_Grouped_Batch<<<eg, eb, 0, s>>>(
+                    acc, dct, ek, ek_shoup, ek + key_block, ek_shoup + key_block, ek + 2 * key_block,
+                    ek_shoup + 2 * key_block, monic, N, mod, digitsG2, g, idx0, idx1, index_pos, n);
+            else
+                kernel_EvalAccCore_Binary_Grouped_Batch<<<eg, eb, 0, s>>>(acc, dct, ek, ek_shoup, monic, N, mod, digitsG2,
+                                                                          g, idx0, index_pos, n);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    }
+    cudaFree(ct);
+    cudaFree(dct);
+    cudaFree(index_pos);
+    return static_cast<int>(e);
+}
+
 // HomTrace + SchemeSwitch of count MV RLWEs in the reference's default (unfused) launch
 // sequence (bitwise/src/cirbts/cirbts-batch.cu:1656-1789): per round k the permuting INTT of
 // c0, kernel_Fused_Permute_Decompose, the NTT of the digits and

@@ -6,6 +6,8 @@ sequences (ref_gpu_cirbts_shim.cu):
   kernel_SignedDigitDecompose2_FusedFNWT_Batch and kernel_EvalAccCore_Binary_Batch with the
   product's keys (its [n][2 digits][2][N] NTT-domain layout is the reference's AoS RF key):
   from the same initial accumulator, n = 630 steps give the oracle's accumulator word for word;
+  likewise the grouped mb = 2 sequence (kernel_EvalAccCore_Binary_MB2_Grouped_Batch) against
+  the oracle's exact grouped rotation;
 * HomTrace + SchemeSwitch: kernel_GenerateCoefficientAutoMaps, per round the permuting INTT,
   kernel_Fused_Permute_Decompose, the NTT and kernel_MultAddUpdate_HT_PermuteC1, then
   kernel_MultAddUpdate_SS and kernel_SaveToRGSW: the oracle's RGSW rows word for word, and the
@@ -44,32 +46,17 @@ def _dev(a):
     return torch.from_numpy(np.ascontiguousarray(a).view(np.int64)).cuda()
 
 
-def test_blind_rotation_matches_reference_kernels(pkg, oracle, ref):
-    p = pkg.default_params()
-    N, n, Q = p.N, p.n, p.Q
-    keys = pkg.generate_keys_host(p, 23)
-    oc = OracleCbs(oracle, p, keys)
-    batch = 2
-    rng = np.random.default_rng(9)
-    a = rng.integers(0, p.q_lwe, size=(batch, n), dtype=np.uint64)
-    b = rng.integers(0, p.q_lwe, batch, dtype=np.uint64)
-
-    def orc_acc(steps):
-        op = type(oc.op).from_buffer_copy(oc.op)
-        op.n = steps
-        out = np.zeros((batch, 2, N), np.uint64)
-        oracle.orc_blind_rotate(ctypes.byref(op), ctypes.byref(oc.ok), a.ctypes.data, b.ctypes.data, batch, n,
-                                out.ctypes.data, 0)
-        return out
-
-    init, want = orc_acc(0), orc_acc(n)
-
-    # Phantom tables of Q (pinned to the reference's host code elsewhere) and the monomial
-    # table NTT(X^k - 1), k < 2N, with X^(N+j) = -X^j (cirbts-init.cu:991-1010)
+def _tables(pkg, N, Q):
+    """Phantom tables of Q (pinned to the reference's host code elsewhere) and the DModulus."""
     tabs = [np.zeros(N, np.uint64) for _ in range(4)]
     ninv = np.zeros(2, np.uint64)
     dm = pkg.DModulus()
     pkg.call("cbs_ntt_tables_host", N, Q, *(t.ctypes.data for t in tabs), ninv.ctypes.data, ctypes.addressof(dm))
+    return tabs, ninv, np.array([dm.value, dm.const_ratio[0], dm.const_ratio[1]], np.uint64)
+
+
+def _monic(oracle, oc, N, Q):
+    """NTT(X^k - 1) for k < 2N with X^(N+j) = -X^j (cirbts-init.cu:991-1010)."""
     monic = np.zeros((2 * N, N), np.uint64)
     k = np.arange(1, N)
     monic[k, k] = 1
@@ -80,11 +67,41 @@ def test_blind_rotation_matches_reference_kernels(pkg, oracle, ref):
     oracle.orc_ntt_forward.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_uint32, ctypes.c_uint64,
                                        ctypes.c_void_p]
     oracle.orc_ntt_forward(monic.ctypes.data, 2 * N, N, Q, oc.rp.ctypes.data)
+    return monic
+
+
+def _orc_acc(oracle, oc, a, b, steps, mbk=None, mb=1):
+    """The oracle's accumulator after `steps` LWE coefficients, not finalized (NTT domain)."""
+    op = type(oc.op).from_buffer_copy(oc.op)
+    op.n = steps
+    batch, stride = a.shape
+    out = np.zeros((batch, 2, oc.p.N), np.uint64)
+    if mbk is None:
+        oracle.orc_blind_rotate(ctypes.byref(op), ctypes.byref(oc.ok), a.ctypes.data, b.ctypes.data, batch, stride,
+                                out.ctypes.data, 0)
+    else:
+        oracle.orc_blind_rotate_mb(ctypes.byref(op), ctypes.byref(oc.ok), mbk.ctypes.data, mb, a.ctypes.data,
+                                   b.ctypes.data, batch, stride, out.ctypes.data, 0)
+    return out
+
+
+def test_blind_rotation_matches_reference_kernels(pkg, oracle, ref):
+    p = pkg.default_params()
+    N, n, Q = p.N, p.n, p.Q
+    keys = pkg.generate_keys_host(p, 23)
+    oc = OracleCbs(oracle, p, keys)
+    batch = 2
+    rng = np.random.default_rng(9)
+    a = rng.integers(0, p.q_lwe, size=(batch, n), dtype=np.uint64)
+    b = rng.integers(0, p.q_lwe, batch, dtype=np.uint64)
+
+    init, want = _orc_acc(oracle, oc, a, b, 0), _orc_acc(oracle, oc, a, b, n)
+    tabs, ninv, dmod = _tables(pkg, N, Q)
+    monic = _monic(oracle, oc, N, Q)
 
     ek = np.ascontiguousarray(keys["bsk"]).reshape(-1)
     eks = np.zeros_like(ek)
     ref.ref_cirbts_shoup(ek.ctypes.data, eks.ctypes.data, ek.size, Q)
-    dmod = np.array([dm.value, dm.const_ratio[0], dm.const_ratio[1]], np.uint64)
     bitwidth = max(0, (p.num_lut - 1).bit_length())
     dev = {name: _dev(v) for name, v in [("acc", init), ("a", a), ("ek", ek), ("eks", eks), ("monic", monic),
                                          ("mod", dmod), ("tw", tabs[0]), ("tws", tabs[1]), ("itw", tabs[2]),
@@ -120,16 +137,12 @@ def test_trace_schemeswitch_matches_reference_kernels(pkg, oracle, ref):
     want = np.zeros((count, 2, 2, N), np.uint64)
     oracle.orc_trace_schemeswitch(ctypes.byref(oc.op), ctypes.byref(oc.ok), ct.ctypes.data, count, want.ctypes.data)
 
-    tabs = [np.zeros(N, np.uint64) for _ in range(4)]
-    ninv = np.zeros(2, np.uint64)
-    dm = pkg.DModulus()
-    pkg.call("cbs_ntt_tables_host", N, Q, *(t.ctypes.data for t in tabs), ninv.ctypes.data, ctypes.addressof(dm))
+    tabs, ninv, dmod = _tables(pkg, N, Q)
     ht = np.ascontiguousarray(keys["ht"]).reshape(-1)
     ss = np.ascontiguousarray(keys["ss"]).reshape(-1)
     hts, sss = np.zeros_like(ht), np.zeros_like(ss)
     ref.ref_cirbts_shoup(ht.ctypes.data, hts.ctypes.data, ht.size, Q)
     ref.ref_cirbts_shoup(ss.ctypes.data, sss.ctypes.data, ss.size, Q)
-    dmod = np.array([dm.value, dm.const_ratio[0], dm.const_ratio[1]], np.uint64)
     dev = {name: _dev(v) for name, v in [("c0", ct[:, 0, :]), ("c1", ct[:, 1, :]), ("ht", ht), ("hts", hts),
                                          ("ss", ss), ("sss", sss), ("mod", dmod), ("tw", tabs[0]), ("tws", tabs[1]),
                                          ("itw", tabs[2]), ("itws", tabs[3]), ("ninv", ninv)]}
@@ -144,3 +157,47 @@ def test_trace_schemeswitch_matches_reference_kernels(pkg, oracle, ref):
     assert st == 0
     assert np.array_equal(maps.cpu().numpy().view(np.uint32), np.asarray(keys["maps"]).reshape(rounds, N))
     assert np.array_equal(rows.cpu().numpy().view(np.uint64), want)
+
+
+def test_grouped_blind_rotation_matches_reference_kernels(pkg, oracle, ref):
+    """The grouped (mb = 2, CIRBTS_PBS_MULTIBIT=2) blind rotation: the reference's
+    kernel_EvalAccCore_Binary_MB2_Grouped_Batch sequence with the product's grouped keys
+    (re-laid [subset][group] as the reference's RF key) reproduces the oracle's exact grouped
+    accumulator word for word; the product's FFT form is checked against that oracle within
+    its phase-error bound (test_cbs_fft_gpu.py)."""
+    vp, u32, u64 = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64
+    ref.ref_cirbts_blind_rotate_mb2.argtypes = [vp, vp, u32, u32, u32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, u32,
+                                                u64, u32, u32, u64, u32, vp]
+    ref.ref_cirbts_blind_rotate_mb2.restype = ctypes.c_int
+    oracle.orc_blind_rotate_mb.argtypes = [vp, vp, vp, u32, vp, vp, u32, u32, vp, ctypes.c_int]
+    p = pkg.default_params()
+    N, n, Q = p.N, p.n, p.Q
+    keys = pkg.generate_keys_host(p, 31)
+    mbk = np.ascontiguousarray(pkg.generate_mb_bsk_host(p, 31, 2))
+    oc = OracleCbs(oracle, p, keys)
+    batch = 2
+    rng = np.random.default_rng(12)
+    a = rng.integers(0, p.q_lwe, size=(batch, n), dtype=np.uint64)
+    b = rng.integers(0, p.q_lwe, batch, dtype=np.uint64)
+    init = _orc_acc(oracle, oc, a, b, 0)
+    want = _orc_acc(oracle, oc, a, b, n, mbk=mbk, mb=2)
+    tabs, ninv, dmod = _tables(pkg, N, Q)
+    monic = _monic(oracle, oc, N, Q)
+    groups = (n + 1) // 2
+    ek = np.ascontiguousarray(mbk.reshape(groups, 3, -1).transpose(1, 0, 2)).reshape(-1)  # [subset][group][...]
+    eks = np.zeros_like(ek)
+    ref.ref_cirbts_shoup(ek.ctypes.data, eks.ctypes.data, ek.size, Q)
+    bitwidth = max(0, (p.num_lut - 1).bit_length())
+    dev = {name: _dev(v) for name, v in [("acc", init), ("a", a), ("ek", ek), ("eks", eks), ("monic", monic),
+                                         ("mod", dmod), ("tw", tabs[0]), ("tws", tabs[1]), ("itw", tabs[2]),
+                                         ("itws", tabs[3]), ("ninv", ninv)]}
+    st = ref.ref_cirbts_blind_rotate_mb2(
+        dev["acc"].data_ptr(), dev["a"].data_ptr(), n, n, batch, dev["ek"].data_ptr(), dev["eks"].data_ptr(),
+        dev["monic"].data_ptr(), dev["mod"].data_ptr(), dev["tw"].data_ptr(), dev["tws"].data_ptr(),
+        dev["itw"].data_ptr(), dev["itws"].data_ptr(), dev["ninv"].data_ptr(), dev["ninv"].data_ptr() + 8, N, Q,
+        p.base_g, p.digits_g, p.q_lwe, bitwidth, None)
+    torch.cuda.synchronize()
+    assert st == 0
+    got = dev["acc"].cpu().numpy().view(np.uint64).reshape(batch, 2, N)
+    assert not np.array_equal(got, init)
+    assert np.array_equal(got, want)
