@@ -1,0 +1,122 @@
+"""Timing beside the reference's own GPU kernels on the same B200: the reference's one-bit and
+grouped (mb = 2) blind rotations (bitwise/src/cirbts/kernel.cu + Phantom's ntt_1d.cu, rebuilt
+for sm_100a by `make -C oracle ref_gpu_cirbts`, launched in the reference's per-step sequences by
+ref_gpu_cirbts_shim.cu) against the product's blind rotation (cbs_blind_rotate_batch_device,
+exact-NTT and FP64-FFT backends, one-bit and grouped) at the same batch, N = 2048, n = 630.
+Prints microseconds per bootstrap; asserts only that every run completes.  The reference's
+timed region covers its kernels only (no finalize / MV split, which the product's includes).
+
+    python -m pytest tests/test_ref_timing_gpu.py -m gpu -s
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import pytest
+
+from conftest import ORACLE_DIR
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+REF_SO = ORACLE_DIR / "_ref" / "libref_cirbts.so"
+BATCH = 1184  # 8 waves of the one-CTA-per-SM grouped kernel
+
+
+def _dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a).view(np.int64)).cuda()
+
+
+def _time_ms(fn, reps=2):
+    fn()
+    torch.cuda.synchronize()
+    best = float("inf")
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn()
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    return best
+
+
+def test_blind_rotation_timing_beside_reference_kernels(pkg):
+    if not REF_SO.exists():
+        pytest.skip("reference CirBTS kernels not built (make -C oracle ref_gpu_cirbts)")
+    ref = ctypes.CDLL(str(REF_SO))
+    vp, u32, u64, sz = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_size_t
+    argt = [vp, vp, u32, u32, u32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, u32, u64, u32, u32, u64, u32, vp]
+    for f in (ref.ref_cirbts_blind_rotate_steps, ref.ref_cirbts_blind_rotate_mb2):
+        f.argtypes = argt
+        f.restype = ctypes.c_int
+    ref.ref_cirbts_shoup.argtypes = [vp, vp, sz, u64]
+
+    ctx = pkg.Context(max_batch=BATCH)
+    ctx.keygen(41)
+    p = ctx.params
+    N, n, Q = p.N, p.n, p.Q
+    keys = ctx.export_keys()
+    rng = np.random.default_rng(3)
+    a = rng.integers(0, p.q_lwe, size=(BATCH, n), dtype=np.uint64)
+    b = rng.integers(0, p.q_lwe, BATCH, dtype=np.uint64)
+    da, db = _dev(a), _dev(b)
+    mv = torch.empty((BATCH, p.num_lut, 2, N), dtype=torch.int64, device="cuda")
+    results = {}
+
+    def ours():
+        pkg.call("cbs_blind_rotate_batch_device", ctx.handle, da.data_ptr(), db.data_ptr(), BATCH, n, mv.data_ptr(),
+                 None)
+
+    for name, backend, mb in [("product exact NTT, one-bit", pkg.BR_NTT, 1),
+                              ("product FP64 FFT, one-bit", pkg.BR_FFT64, 1),
+                              ("product FP64 FFT, mb = 2", pkg.BR_FFT64, 2)]:
+        ctx.set_br_backend(backend)
+        ctx.set_br_multibit(mb)
+        results[name] = _time_ms(ours)
+    mbk = ctx.export_mb_bsk()
+    ctx.set_br_backend(pkg.BR_NTT)
+
+    # the reference's kernels: tables, monomials NTT(X^k - 1), keys with Shoup tables
+    tabs = [np.zeros(N, np.uint64) for _ in range(4)]
+    ninv = np.zeros(2, np.uint64)
+    dm = pkg.DModulus()
+    pkg.call("cbs_ntt_tables_host", N, Q, *(t.ctypes.data for t in tabs), ninv.ctypes.data, ctypes.addressof(dm))
+    monic = np.zeros((2 * N, N), np.uint64)
+    k = np.arange(1, N)
+    monic[k, k] = 1
+    monic[1:N, 0] = Q - 1
+    monic[N, 0] = Q - 2
+    monic[N + k, k] = Q - 1
+    monic[N + k, 0] = Q - 1
+    d_monic = _dev(monic)
+    pkg.call("cbs_fnwt_1d_opt_batched", d_monic.data_ptr(), _dev(tabs[0]).data_ptr(), _dev(tabs[1]).data_ptr(),
+             _dev(np.array([dm.value, dm.const_ratio[0], dm.const_ratio[1]], np.uint64)).data_ptr(), N, 2 * N, None)
+    dev = {nm: _dev(v) for nm, v in [("tw", tabs[0]), ("tws", tabs[1]), ("itw", tabs[2]), ("itws", tabs[3]),
+                                     ("ninv", ninv),
+                                     ("mod", np.array([dm.value, dm.const_ratio[0], dm.const_ratio[1]], np.uint64))]}
+    bitwidth = max(0, (p.num_lut - 1).bit_length())
+    acc = torch.from_numpy(rng.integers(0, Q, size=(BATCH, 2, N), dtype=np.uint64).view(np.int64)).cuda()
+    groups = (n + 1) // 2
+    for name, fn, key in [("reference kernels, one-bit", ref.ref_cirbts_blind_rotate_steps,
+                           np.ascontiguousarray(keys["bsk"]).reshape(-1)),
+                          ("reference kernels, mb = 2", ref.ref_cirbts_blind_rotate_mb2,
+                           np.ascontiguousarray(mbk.reshape(groups, 3, -1).transpose(1, 0, 2)).reshape(-1))]:
+        ks = np.zeros_like(key)
+        ref.ref_cirbts_shoup(key.ctypes.data, ks.ctypes.data, key.size, Q)
+        d_k, d_ks = _dev(key), _dev(ks)
+
+        def run():
+            st = fn(acc.data_ptr(), da.data_ptr(), n, n, BATCH, d_k.data_ptr(), d_ks.data_ptr(), d_monic.data_ptr(),
+                    dev["mod"].data_ptr(), dev["tw"].data_ptr(), dev["tws"].data_ptr(), dev["itw"].data_ptr(),
+                    dev["itws"].data_ptr(), dev["ninv"].data_ptr(), dev["ninv"].data_ptr() + 8, N, Q, p.base_g,
+                    p.digits_g, p.q_lwe, bitwidth, None)
+            assert st == 0
+
+        results[name] = _time_ms(run, reps=1)
+        del d_k, d_ks
+    ctx.close()
+    print(f"\nblind rotation, N = {N}, n = {n}, batch {BATCH}, one B200 (us per bootstrap):")
+    for name, ms in results.items():
+        print(f"  {name:32s} {ms * 1e3 / BATCH:9.1f}")
+    assert all(v > 0 for v in results.values())
