@@ -396,26 +396,11 @@ def run_keyswitch(args, rank: int, world: int, local_rank: int) -> None:
     ctx.close()
 
 
-def _ref_phantom_ntt():
-    """The reference's own Phantom NTT kernels rebuilt for sm_100a (oracle/_ref), or None."""
-    so = ROOT / "oracle" / "_ref" / "libref_phantom_ntt.so"
-    if not so.exists():
-        return None
-    lib = ctypes.CDLL(str(so))
-    vp, u32 = ctypes.c_void_p, ctypes.c_uint32
-    lib.ref_gpu_ntt2d_create.argtypes = [u32, u32, vp]
-    lib.ref_gpu_ntt2d_create.restype = vp
-    lib.ref_gpu_ntt2d_forward.argtypes = [vp, vp, u32, u32, vp]
-    lib.ref_gpu_ntt2d_backward.argtypes = [vp, vp, u32, u32, vp]
-    lib.ref_gpu_ntt2d_destroy.argtypes = [vp]
-    return lib
-
-
 def run_rns_ntt(args, rank: int, world: int, local_rank: int) -> None:
     """Forward + inverse multi-prime NTT over `--batch` ciphertexts x 2 polys x `--limbs`
     limbs at N = 2^`--ntt-logn` (default: the Phantom-core transform, N = 2^16, 24 limbs),
-    in place, inputs resident in HBM; beside it the reference's own 2-D kernels on the same
-    data when they were built (one call per polynomial, the reference's calling convention)."""
+    in place, inputs resident in HBM.  (The reference's own 2-D kernels on the same data are
+    timed beside it by tests/test_ref_timing_gpu.py.)"""
     import torch
     torch.cuda.set_device(local_rank)
     pkg = load_pkg()
@@ -439,28 +424,6 @@ def run_rns_ntt(args, rank: int, world: int, local_rank: int) -> None:
     with ClockSampler(local_rank) as clk:
         ms = _timed(torch, stream, fn, args.warmup, args.steps)
     ok = bool(torch.equal(x, ref))  # forward then inverse is the identity
-    ref_gpu = None
-    lib = _ref_phantom_ntt()
-    if lib is not None:
-        chain = np.concatenate([q, p])
-        table = lib.ref_gpu_ntt2d_create(logn, len(chain), chain.ctypes.data)
-        y = ref.clone()
-
-        def rfn():
-            for k in range(polys):
-                ptr = y.data_ptr() + k * size_q * n * 8
-                lib.ref_gpu_ntt2d_forward(table, ptr, size_q, 0, stream.cuda_stream)
-            for k in range(polys):
-                ptr = y.data_ptr() + k * size_q * n * 8
-                lib.ref_gpu_ntt2d_backward(table, ptr, size_q, 0, stream.cuda_stream)
-
-        rms = _timed(torch, stream, rfn, args.warmup, args.steps)
-        same = bool(torch.equal(y, ref))
-        lib.ref_gpu_ntt2d_destroy(table)
-        ref_gpu = {"what": "reference nwt_2d_radix8_forward/backward_inplace (src/ntt/fntt_2d.cu, intt_2d.cu) "
-                           "rebuilt for sm_100a, one call per polynomial", "ms_per_step": rms,
-                   "value": world * polys * size_q / (rms * 1e-3), "roundtrip_identity": same,
-                   "speedup_of_this_build": rms / ms}
     alg = 2 * 2 * polys * size_q * n * 8  # each transform reads and writes every limb once
     peaks = measured_peaks()
     gbs = alg / (ms * 1e-3) / 1e9
@@ -477,7 +440,7 @@ def run_rns_ntt(args, rank: int, world: int, local_rank: int) -> None:
                         "achieved": gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": gbs / peaks["hbm_gbs"],
                         "peak_src": peaks["src"], "traffic": None, "algorithmic_bytes_per_step": alg,
                         "note": "two HBM round trips per transform (2-D)" if logn >= 13 else "one round trip"},
-           "reference_gpu": ref_gpu, "clocks": clk.summary()}
+           "clocks": clk.summary()}
     if rank == 0:
         print(json.dumps(out), flush=True)
     ctx.close()

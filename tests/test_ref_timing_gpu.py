@@ -120,3 +120,48 @@ def test_blind_rotation_timing_beside_reference_kernels(pkg):
     for name, ms in results.items():
         print(f"  {name:32s} {ms * 1e3 / BATCH:9.1f}")
     assert all(v > 0 for v in results.values())
+
+
+def test_rns_ntt_timing_beside_reference_kernels(pkg):
+    """The Phantom-core 2-D NTT (N = 2^16, 32 ciphertexts x 2 polys x 24 limbs, forward +
+    inverse, in place) against the reference's nwt_2d_radix8_forward/backward_inplace
+    (src/ntt/fntt_2d.cu, intt_2d.cu, rebuilt by `make -C oracle ref_gpu`, one call per
+    polynomial as the reference's API takes them); both round trips must give the input back."""
+    so = ORACLE_DIR / "_ref" / "libref_phantom_ntt.so"
+    if not so.exists():
+        pytest.skip("reference Phantom NTT library not built (make -C oracle ref_gpu)")
+    lib = ctypes.CDLL(str(so))
+    vp, u32 = ctypes.c_void_p, ctypes.c_uint32
+    lib.ref_gpu_ntt2d_create.argtypes = [u32, u32, vp]
+    lib.ref_gpu_ntt2d_create.restype = vp
+    lib.ref_gpu_ntt2d_forward.argtypes = [vp, vp, u32, u32, vp]
+    lib.ref_gpu_ntt2d_backward.argtypes = [vp, vp, u32, u32, vp]
+    lib.ref_gpu_ntt2d_destroy.argtypes = [vp]
+    logn, size_q, polys = 16, 24, 64
+    n = 1 << logn
+    q = np.zeros(size_q + 2, np.uint64)
+    pkg.call("cbs_get_primes", n, 50, size_q + 2, q.ctypes.data)  # as bench.py rns_chain
+    ctx = pkg.RnsContext(n, q[:size_q], q[size_q:])
+    x = torch.remainder(torch.randint(0, 2 ** 62, (polys, size_q, n), dtype=torch.int64, device="cuda"),
+                        torch.from_numpy(q[:size_q].view(np.int64)).cuda().view(1, -1, 1)).contiguous()
+    orig = x.clone()
+    y = x.clone()
+
+    def ours():
+        pkg.call("cbs_rns_ntt_batched", ctx.handle, x.data_ptr(), polys, size_q * n, size_q, 0, 0, None)
+        pkg.call("cbs_rns_ntt_batched", ctx.handle, x.data_ptr(), polys, size_q * n, size_q, 0, 1, None)
+
+    table = lib.ref_gpu_ntt2d_create(logn, len(q), q.ctypes.data)
+
+    def theirs():
+        for k in range(polys):
+            lib.ref_gpu_ntt2d_forward(table, y.data_ptr() + k * size_q * n * 8, size_q, 0, None)
+        for k in range(polys):
+            lib.ref_gpu_ntt2d_backward(table, y.data_ptr() + k * size_q * n * 8, size_q, 0, None)
+
+    t_ours, t_ref = _time_ms(ours, reps=3), _time_ms(theirs, reps=3)
+    lib.ref_gpu_ntt2d_destroy(table)
+    ctx.close()
+    print(f"\n2-D NTT N = 2^16, {polys} polys x {size_q} limbs, forward + inverse: product {t_ours:.2f} ms, "
+          f"reference kernels {t_ref:.2f} ms ({t_ref / t_ours:.2f}x)")
+    assert torch.equal(x, orig) and torch.equal(y, orig)
