@@ -3,8 +3,10 @@ grouped (mb = 2) blind rotations (bitwise/src/cirbts/kernel.cu + Phantom's ntt_1
 for sm_100a by `make -C oracle ref_gpu_cirbts`, launched in the reference's per-step sequences by
 ref_gpu_cirbts_shim.cu) against the product's blind rotation (cbs_blind_rotate_batch_device,
 exact-NTT and FP64-FFT backends, one-bit and grouped) at the same batch, N = 2048, n = 630.
-Prints microseconds per bootstrap; asserts only that every run completes.  The reference's
-timed region covers its kernels only (no finalize / MV split, which the product's includes).
+Also the 2-D NTT and the sample extract + key switch beside the reference's kernels.  Prints
+the times; asserts only that the runs complete (and, where both write comparable outputs, that
+they agree).  The reference's blind-rotation timing covers its kernels only (no finalize / MV
+split, which the product's includes).
 
     python -m pytest tests/test_ref_timing_gpu.py -m gpu -s
 """
@@ -165,3 +167,51 @@ def test_rns_ntt_timing_beside_reference_kernels(pkg):
     print(f"\n2-D NTT N = 2^16, {polys} polys x {size_q} limbs, forward + inverse: product {t_ours:.2f} ms, "
           f"reference kernels {t_ref:.2f} ms ({t_ref / t_ours:.2f}x)")
     assert torch.equal(x, orig) and torch.equal(y, orig)
+
+
+def test_extraction_timing_beside_reference_kernel(pkg):
+    """Sample extract + LWE key switch of one AES round's 16384 bits (128 blocks) from 512
+    coefficient-domain words: the product's k_extract_keyswitch against the reference's
+    kernel_SampleExtractKeySwitchToLWE (aes_gpu_ks.cuh, `make -C oracle ref_gpu_extract`).  The
+    reference's timed call includes its workspace allocation, as its helper makes it."""
+    so = ORACLE_DIR / "_ref" / "libref_extract.so"
+    if not so.exists():
+        pytest.skip("reference extraction kernel not built (make -C oracle ref_gpu_extract)")
+    lib = ctypes.CDLL(str(so))
+    vp, u32, u64 = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64
+    lib.ref_gpu_extract_keyswitch.argtypes = [vp, u32, u32, u32, u32, vp, vp, vp, u32, u64, u64, vp, vp, u32,
+                                              ctypes.c_int]
+    lib.ref_gpu_extract_keyswitch.restype = ctypes.c_int
+    ctx = pkg.Context(max_batch=16384)
+    ctx.keygen(43)
+    p = ctx.params
+    N, n = p.N, p.n
+    ksk = np.ascontiguousarray(ctx.export_keys()["ksk"]).reshape(-1)
+    rng = np.random.default_rng(5)
+    W, count = 512, 16384
+    words = rng.integers(0, p.Q, size=(W, 2, N), dtype=np.uint64)
+    info = ((np.arange(count, dtype=np.uint32) // 32) << 16 | rng.integers(0, 32, count, dtype=np.uint32))
+    info = info.astype(np.uint32)
+    d_words = _dev(words)
+    oa = torch.zeros((count, n), dtype=torch.int64, device="cuda")
+    ob = torch.zeros(count, dtype=torch.int64, device="cuda")
+    d_ksk = torch.from_numpy(ksk.view(np.int16)).cuda()
+    d_a, d_b = _dev(words[:, 0, :]), _dev(words[:, 1, :])
+    d_info = torch.from_numpy(info.view(np.int32)).cuda()
+    ra = torch.zeros_like(oa)
+    rb = torch.zeros_like(ob)
+
+    def ours():
+        pkg.call("cbs_extract_keyswitch_device", ctx.handle, d_words.data_ptr(), W, info.ctypes.data, count,
+                 oa.data_ptr(), ob.data_ptr(), n, None)
+
+    def theirs():
+        assert lib.ref_gpu_extract_keyswitch(d_ksk.data_ptr(), n, N, p.base_ks, p.qks, d_a.data_ptr(), d_b.data_ptr(),
+                                             d_info.data_ptr(), count, p.Q, p.q_lwe, ra.data_ptr(), rb.data_ptr(), n,
+                                             0) == 0
+
+    t_ours, t_ref = _time_ms(ours, reps=3), _time_ms(theirs, reps=3)
+    ctx.close()
+    print(f"\nextract + key switch, {count} bits, N = {N}, n = {n}: product {t_ours:.2f} ms, "
+          f"reference kernel {t_ref:.2f} ms ({t_ref / t_ours:.2f}x)")
+    assert torch.equal(oa, ra) and torch.equal(ob, rb)
