@@ -215,3 +215,63 @@ def test_extraction_timing_beside_reference_kernel(pkg):
     print(f"\nextract + key switch, {count} bits, N = {N}, n = {n}: product {t_ours:.2f} ms, "
           f"reference kernel {t_ref:.2f} ms ({t_ref / t_ours:.2f}x)")
     assert torch.equal(oa, ra) and torch.equal(ob, rb)
+
+
+def test_trace_schemeswitch_timing_beside_reference_kernels(pkg):
+    """HomTrace + SchemeSwitch of 2048 MV RLWEs (N = 2048, 11 rounds, HT 2^9 x 5, SS 2^9 x 5):
+    the product's exact-NTT and FFT forms (cbs_trace_schemeswitch_device) against the
+    reference's default launch sequence (ref_gpu_cirbts_shim.cu; its call includes its buffer
+    allocation).  The exact form and the reference must agree word for word."""
+    if not REF_SO.exists():
+        pytest.skip("reference CirBTS kernels not built (make -C oracle ref_gpu_cirbts)")
+    ref = ctypes.CDLL(str(REF_SO))
+    vp, u32, u64, sz = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_size_t
+    ref.ref_cirbts_trace_schemeswitch.argtypes = [vp, vp, u32, vp, vp, vp, vp, u32, u32, u32, u32, u32, vp, vp, vp,
+                                                  vp, vp, vp, vp, vp, u32, u64, vp, vp]
+    ref.ref_cirbts_trace_schemeswitch.restype = ctypes.c_int
+    ref.ref_cirbts_shoup.argtypes = [vp, vp, sz, u64]
+    count = 2048
+    ctx = pkg.Context(max_batch=count)
+    ctx.keygen(47)
+    p = ctx.params
+    N, Q = p.N, p.Q
+    rounds = N.bit_length() - 1 - p.trace_shift
+    keys = ctx.export_keys()
+    mv = np.random.default_rng(6).integers(0, Q, size=(count, 2, N), dtype=np.uint64)
+    d_mv = _dev(mv)
+    rows = {name: torch.zeros((count, 2, 2, N), dtype=torch.int64, device="cuda") for name in ("ntt", "fft", "ref")}
+    times = {}
+    for name, backend in (("ntt", pkg.BR_NTT), ("fft", pkg.BR_FFT64)):
+        ctx.set_br_backend(backend)
+        times[name] = _time_ms(lambda: pkg.call("cbs_trace_schemeswitch_device", ctx.handle, d_mv.data_ptr(), count,
+                                                rows[name].data_ptr(), None), reps=3)
+    ctx.set_br_backend(pkg.BR_NTT)
+    tabs = [np.zeros(N, np.uint64) for _ in range(4)]
+    ninv = np.zeros(2, np.uint64)
+    dm = pkg.DModulus()
+    pkg.call("cbs_ntt_tables_host", N, Q, *(t.ctypes.data for t in tabs), ninv.ctypes.data, ctypes.addressof(dm))
+    ht = np.ascontiguousarray(keys["ht"]).reshape(-1)
+    ss = np.ascontiguousarray(keys["ss"]).reshape(-1)
+    hts, sss = np.zeros_like(ht), np.zeros_like(ss)
+    ref.ref_cirbts_shoup(ht.ctypes.data, hts.ctypes.data, ht.size, Q)
+    ref.ref_cirbts_shoup(ss.ctypes.data, sss.ctypes.data, ss.size, Q)
+    dev = {nm: _dev(v) for nm, v in [("c0", mv[:, 0, :]), ("c1", mv[:, 1, :]), ("ht", ht), ("hts", hts), ("ss", ss),
+                                     ("sss", sss), ("tw", tabs[0]), ("tws", tabs[1]), ("itw", tabs[2]),
+                                     ("itws", tabs[3]), ("ninv", ninv),
+                                     ("mod", np.array([dm.value, dm.const_ratio[0], dm.const_ratio[1]], np.uint64))]}
+    maps = torch.zeros((rounds, N), dtype=torch.int32, device="cuda")
+
+    def theirs():
+        assert ref.ref_cirbts_trace_schemeswitch(
+            dev["c0"].data_ptr(), dev["c1"].data_ptr(), count, dev["ht"].data_ptr(), dev["hts"].data_ptr(),
+            dev["ss"].data_ptr(), dev["sss"].data_ptr(), rounds, p.base_ht, p.digits_ht, p.base_ss, p.digits_ss,
+            maps.data_ptr(), dev["mod"].data_ptr(), dev["tw"].data_ptr(), dev["tws"].data_ptr(), dev["itw"].data_ptr(),
+            dev["itws"].data_ptr(), dev["ninv"].data_ptr(), dev["ninv"].data_ptr() + 8, N, Q, rows["ref"].data_ptr(),
+            None) == 0
+
+    times["ref"] = _time_ms(theirs, reps=3)
+    ctx.close()
+    print(f"\nHomTrace + SchemeSwitch, {count} MV RLWEs, N = {N} (us per RLWE): product exact NTT "
+          f"{times['ntt'] * 1e3 / count:.2f}, product FP64 FFT {times['fft'] * 1e3 / count:.2f}, "
+          f"reference kernels {times['ref'] * 1e3 / count:.2f}")
+    assert torch.equal(rows["ntt"], rows["ref"])
