@@ -10,9 +10,11 @@ The FP64-FFT backend runs the blind rotation over groups of 2 LWE coefficients b
 one-coefficient GINX loop.
 
 value: blocks/s with inputs resident in HBM, CUDA events on the launching stream, max over
-ranks.  e2e: the same metric through the host-buffer C-ABI entry point
-(cbs_aes128_ctr_transcipher: counters in host memory, LWE outputs copied back).  Every
-output block is decrypted and compared with AES-128 from OpenSSL after the timed region.
+ranks.  e2e: the same metric through the host-buffer C-ABI entry point of the whole
+transciphering job (cbs_aes128_ctr_transcipher_ciphertext: counters and a public AES-CTR
+ciphertext in host memory, LWE encryptions of the plaintext bits copied back).  Every output
+block is decrypted and compared after the timed region: the keystream with AES-128 from
+OpenSSL, the e2e output with the plaintext.
 
 --impl reference: the CPU restatement of the same path (oracle/, all host threads) on a
 bounded sample of the same workload; rank 0 only.
@@ -122,15 +124,22 @@ def counter_bits(ctrs: np.ndarray) -> np.ndarray:
     return np.unpackbits(ctrs, axis=1, bitorder="little").reshape(-1).astype(np.uint8)
 
 
-def verify(pkg, ctx, key: bytes, ctrs: np.ndarray, ha: np.ndarray, hb: np.ndarray) -> int:
+def aes_ecb(key: bytes, blocks: np.ndarray) -> np.ndarray:
+    """AES-128 of each 16-byte row (OpenSSL through `cryptography`)."""
     from cryptography.hazmat.primitives.ciphers import Cipher, algorithms, modes
+    enc = Cipher(algorithms.AES(key), modes.ECB()).encryptor()
+    return np.frombuffer(enc.update(blocks.tobytes()), np.uint8).reshape(blocks.shape[0], 16)
+
+
+def verify(pkg, ctx, key: bytes, ctrs: np.ndarray, ha: np.ndarray, hb: np.ndarray,
+           plain: np.ndarray | None = None) -> int:
+    """Blocks whose decrypted LWE bits equal AES_K(counter), or `plain` when given."""
     n = ctx.params.n
     blocks = ctrs.shape[0]
     dec = np.zeros(blocks * 128, np.uint8)
     pkg.call("cbs_lwe_decrypt_bits", ctx.handle, ha.ctypes.data, hb.ctypes.data, blocks * 128, n, dec.ctypes.data)
     got = np.packbits(dec.reshape(blocks, 128), axis=1, bitorder="little")
-    enc = Cipher(algorithms.AES(key), modes.ECB()).encryptor()
-    want = np.frombuffer(enc.update(ctrs.tobytes()), np.uint8).reshape(blocks, 16)
+    want = aes_ecb(key, ctrs) if plain is None else plain
     return int((got == want).all(axis=1).sum())
 
 
@@ -207,19 +216,25 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     peaks = measured_peaks()
     achieved_gbs = alg_bytes / (br_ms * 1e-3) / 1e9
 
-    # e2e through the host-buffer C-ABI entry point
+    # e2e through the host-buffer C-ABI entry point of the whole job: a public AES-CTR
+    # ciphertext of seeded random plaintext in, LWE encryptions of the plaintext bits out
+    plain = np.random.default_rng(args.seed + 1 + rank).integers(0, 256, (blocks, 16), dtype=np.uint8)
+    cipher = np.ascontiguousarray(plain ^ aes_ecb(key, ctrs))
     out_ha = np.empty((blocks * 128, p.n), np.uint64)
     out_hb = np.empty(blocks * 128, np.uint64)
     e2e_steps = max(1, min(args.steps, 2))
-    pkg.call("cbs_aes128_ctr_transcipher", ctx.handle, ctrs.ctypes.data, blocks, out_ha.ctypes.data,
-             out_hb.ctypes.data)
+
+    def e2e_call():
+        pkg.call("cbs_aes128_ctr_transcipher_ciphertext", ctx.handle, ctrs.ctypes.data, cipher.ctypes.data, blocks,
+                 out_ha.ctypes.data, out_hb.ctypes.data)
+
+    e2e_call()
     rep.barrier(world)
     t0 = time.perf_counter()  # the host API call is synchronous: copies and kernels inside
     for _ in range(e2e_steps):
-        pkg.call("cbs_aes128_ctr_transcipher", ctx.handle, ctrs.ctypes.data, blocks, out_ha.ctypes.data,
-                 out_hb.ctypes.data)
+        e2e_call()
     e2e_ms = rep.max_over_ranks((time.perf_counter() - t0) / e2e_steps * 1e3, world, device="cuda")
-    e2e_ok = verify(pkg, ctx, key, ctrs, out_ha, out_hb)
+    e2e_ok = verify(pkg, ctx, key, ctrs, out_ha, out_hb, plain)
 
     chunks = -(-blocks // 256)
     # per round: blind rotation, HomTrace+SchemeSwitch, 8 CMux levels, word assembly and
@@ -247,7 +262,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
         "us_per_bootstrap": ms_per_step * 1e3 / (blocks * 128 * ROUNDS),
         "correct_blocks": ok,
         "gpu_launches": launches_per_step * args.steps,
-        "e2e": {"value": rep.whole_job_rate(world, blocks, e2e_ms), "unit": UNIT, "h2d_bytes_per_step": blocks * 128,
+        "e2e": {"value": rep.whole_job_rate(world, blocks, e2e_ms), "unit": UNIT, "h2d_bytes_per_step": blocks * (128 + 16),
                 "d2h_bytes_per_step": blocks * 128 * (p.n + 1) * 8, "correct_blocks": e2e_ok},
         "roofline": {"kernel": br_kernel_name(args)
                      + " (fused GINX blind rotation + finalize + MV split)", "bound": "hbm",

@@ -99,6 +99,8 @@ def _declare(lib: ctypes.CDLL) -> None:
         "cbs_aes128_import_material": (st, [c_vp, c_vp, c_vp, c_vp, c_vp]),
         "cbs_aes128_ctr_transcipher_device": (st, [c_vp, c_vp, u32, c_vp, c_vp, ctypes.c_int, c_vp]),
         "cbs_aes128_ctr_transcipher": (st, [c_vp, c_vp, u32, c_vp, c_vp]),
+        "cbs_aes128_ctr_add_ciphertext_device": (st, [c_vp, c_vp, u32, c_vp, c_vp]),
+        "cbs_aes128_ctr_transcipher_ciphertext": (st, [c_vp, c_vp, c_vp, u32, c_vp, c_vp]),
         "cbs_lwe_decrypt_bits": (st, [c_vp, c_vp, c_vp, u32, u32, c_vp]),
         "cbs_circuit_bootstrap_noalloc_capacity_words": (sz, []),
         "cbs_circuit_bootstrap_batch_device_noalloc": (st, [c_vp, c_vp, c_vp, u32, u32, c_vp, c_vp]),

@@ -310,11 +310,21 @@ cbs_status cbs_aes128_ctr_transcipher_device(cbs_context* ctx, const uint8_t* d_
     return CBS_OK;
 }
 
-cbs_status cbs_aes128_ctr_transcipher(cbs_context* ctx, const uint8_t* h_counters, uint32_t blocks, uint64_t* h_out_a,
-                                      uint64_t* h_out_b) {
-    CBS_CHECK_ARG(ctx, "aes_transcipher: null context");
+cbs_status cbs_aes128_ctr_add_ciphertext_device(cbs_context* ctx, const uint8_t* d_cipher, uint32_t blocks,
+                                               uint64_t* d_b, cbs_stream_t stream) {
+    CBS_CHECK_ARG(ctx, "aes_add_ciphertext: null context");
     if (blocks == 0) return CBS_OK;
-    CBS_CHECK_ARG(h_counters && h_out_a && h_out_b, "aes_transcipher: null pointer");
+    CBS_CHECK_ARG(d_cipher && d_b, "aes_add_ciphertext: null pointer");
+    CBS_CHECK_ARG(blocks <= (1u << 24), "aes_add_ciphertext: at most 2^24 blocks per call");
+    cudaStream_t s = stream ? reinterpret_cast<cudaStream_t>(stream) : ctx->stream;
+    CBS_CUDA_TRY(launch_add_public_bits(d_b, d_cipher, ctx->p.q_lwe >> 1, ctx->p.q_lwe, blocks * 128u, s));
+    return CBS_OK;
+}
+
+// host transciphering: keystream LWEs of AES_K(counter), plus the public ciphertext bits
+// when h_cipher is given (then LWEs of the plaintext bits)
+static cbs_status aes_ctr_host(cbs_context* ctx, const uint8_t* h_counters, const uint8_t* h_cipher,
+                               uint32_t blocks, uint64_t* h_out_a, uint64_t* h_out_b) {
     cbs_context* c = ctx;
     cudaStream_t s = c->stream;
     const size_t T = static_cast<size_t>(blocks) * 128, n = c->p.n;
@@ -329,10 +339,34 @@ cbs_status cbs_aes128_ctr_transcipher(cbs_context* ctx, const uint8_t* h_counter
     if (cbs_status st = cbs_aes128_ctr_transcipher_device(c, d_bits.p, blocks, d_a.p, d_b.p, 1,
                                                           reinterpret_cast<cbs_stream_t>(s)))
         return st;
+    DevBuf<uint8_t> d_cipher;
+    if (h_cipher) {
+        CBS_CUDA_TRY(d_cipher.upload(h_cipher, static_cast<size_t>(blocks) * 16, s));
+        if (cbs_status st = cbs_aes128_ctr_add_ciphertext_device(c, d_cipher.p, blocks, d_b.p,
+                                                                 reinterpret_cast<cbs_stream_t>(s)))
+            return st;
+    }
     CBS_CUDA_TRY(cudaMemcpyAsync(h_out_a, d_a.p, T * n * sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
     CBS_CUDA_TRY(cudaMemcpyAsync(h_out_b, d_b.p, T * sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
     CBS_CUDA_TRY(cudaStreamSynchronize(s));
     return CBS_OK;
+}
+
+cbs_status cbs_aes128_ctr_transcipher(cbs_context* ctx, const uint8_t* h_counters, uint32_t blocks, uint64_t* h_out_a,
+                                      uint64_t* h_out_b) {
+    CBS_CHECK_ARG(ctx, "aes_transcipher: null context");
+    if (blocks == 0) return CBS_OK;
+    CBS_CHECK_ARG(h_counters && h_out_a && h_out_b, "aes_transcipher: null pointer");
+    return aes_ctr_host(ctx, h_counters, nullptr, blocks, h_out_a, h_out_b);
+}
+
+cbs_status cbs_aes128_ctr_transcipher_ciphertext(cbs_context* ctx, const uint8_t* h_counters,
+                                                 const uint8_t* h_cipher, uint32_t blocks, uint64_t* h_out_a,
+                                                 uint64_t* h_out_b) {
+    CBS_CHECK_ARG(ctx, "aes_transcipher: null context");
+    if (blocks == 0) return CBS_OK;
+    CBS_CHECK_ARG(h_counters && h_cipher && h_out_a && h_out_b, "aes_transcipher: null pointer");
+    return aes_ctr_host(ctx, h_counters, h_cipher, blocks, h_out_a, h_out_b);
 }
 
 cbs_status cbs_lwe_decrypt_bits(const cbs_context* ctx, const uint64_t* h_a, const uint64_t* h_b, uint32_t count,

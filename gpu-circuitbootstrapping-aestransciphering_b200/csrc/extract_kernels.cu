@@ -123,6 +123,26 @@ cudaError_t launch_init_state(uint64_t* out_a, uint64_t* out_b, const uint64_t* 
     return cudaGetLastError();
 }
 
+// transciphering proper (main.cu:1569-1582, EvalAddConstEq(ct, q/2) per set bit): the
+// keystream LWE of bit t gains q/2 where bit t of the public AES-CTR ciphertext is 1, so b
+// then encrypts the plaintext bit.  bytes [total / 8], bit t = byte t/8, bit t%8 (LSB first).
+__global__ void k_add_public_bits(uint64_t* b, const uint8_t* bytes, uint64_t half, uint64_t q, uint32_t total) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= total) return;
+    if ((bytes[t >> 3] >> (t & 7u)) & 1u) {
+        uint64_t v = b[t] + half;
+        if (v >= q) v -= q;
+        b[t] = v;
+    }
+}
+
+cudaError_t launch_add_public_bits(uint64_t* b, const uint8_t* bytes, uint64_t half, uint64_t q, uint32_t total,
+                                   cudaStream_t s) {
+    if (!total) return cudaSuccess;
+    k_add_public_bits<<<(total + 255) / 256, 256, 0, s>>>(b, bytes, half, q, total);
+    return cudaGetLastError();
+}
+
 // AES word assembly: out column c of block b = sum over rows of the LUT of byte (row, c+row)
 // plus the round-key word (the reference's fused final add, gpu_lut.cuh:1305-1370, and
 // kernel_RLWE_AddWords4Inplace_Blocks, main.cu:1516-1523).  lut_out [blocks][16][2][N] with

@@ -30,6 +30,9 @@ inline uint32_t ksk_row_stride(uint32_t n) { return (n + 1 + 3) & ~3u; }
 cudaError_t launch_init_state(uint64_t* out_a, uint64_t* out_b, const uint64_t* rk_a, const uint64_t* rk_b,
                               const uint8_t* bits, uint64_t half, uint64_t q, uint32_t n, uint32_t total,
                               cudaStream_t s);
+// b[t] += q/2 (mod q) where bit t of bytes is set (bit t = byte t/8, bit t%8)
+cudaError_t launch_add_public_bits(uint64_t* b, const uint8_t* bytes, uint64_t half, uint64_t q, uint32_t total,
+                                   cudaStream_t s);
 cudaError_t launch_assemble_words(uint64_t* words, const uint64_t* lut_out, const uint64_t* rk, uint64_t Q, uint32_t N,
                                   uint32_t blocks, cudaStream_t s);
 

@@ -262,6 +262,18 @@ cbs_status cbs_aes128_ctr_transcipher_device(cbs_context *ctx, const uint8_t *d_
 /* Host-buffer entry point: h_counters [blocks][16] -> h_out_a [blocks*128][n], h_out_b. */
 cbs_status cbs_aes128_ctr_transcipher(cbs_context *ctx, const uint8_t *h_counters, uint32_t blocks,
                                       uint64_t *h_out_a, uint64_t *h_out_b);
+/* Transciphering proper (replaces the per-bit EvalAddConstEq(ct, q/2) on the host after the
+ * download, examples/aes_transcipher/main.cu:1569-1582): plaintext = keystream XOR public
+ * AES-CTR ciphertext, so add q_lwe/2 (mod q_lwe) to d_b[t] wherever bit t of d_cipher
+ * ([blocks][16] bytes, bit t = byte*8 + b, LSB first) is 1.  In place, on the device; d_b
+ * (the keystream b words of cbs_aes128_ctr_transcipher_device) then encrypts the plaintext. */
+cbs_status cbs_aes128_ctr_add_ciphertext_device(cbs_context *ctx, const uint8_t *d_cipher, uint32_t blocks,
+                                                uint64_t *d_b, cbs_stream_t stream);
+/* Host-buffer transciphering of a public AES-CTR ciphertext: h_counters and h_cipher
+ * [blocks][16] -> h_out_a [blocks*128][n], h_out_b: LWE encryptions of the plaintext bits. */
+cbs_status cbs_aes128_ctr_transcipher_ciphertext(cbs_context *ctx, const uint8_t *h_counters,
+                                                 const uint8_t *h_cipher, uint32_t blocks, uint64_t *h_out_a,
+                                                 uint64_t *h_out_b);
 /* Client-side helper (uses the secret key): decrypt LWE bits (mod q_lwe) to 0/1. */
 cbs_status cbs_lwe_decrypt_bits(const cbs_context *ctx, const uint64_t *h_a, const uint64_t *h_b, uint32_t count,
                                 uint32_t a_stride, uint8_t *h_bits);

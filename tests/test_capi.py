@@ -62,6 +62,9 @@ def test_argument_validation_without_device(lib):
     p = ctypes.addressof(buf)
     assert lib.cbs_inwt_1d_opt_permute_batched(p, p, p, p, p, p, p, p, 2048, 1, None) == 1
     assert b"in-place" in lib.cbs_last_error()
+    # AES ciphertext add: null context / pointers rejected, empty input accepted
+    assert lib.cbs_aes128_ctr_add_ciphertext_device(None, p, 1, p, None) == 1
+    assert lib.cbs_aes128_ctr_transcipher_ciphertext(None, p, p, 1, p, p) == 1
     # not enough NTT-friendly primes of 13 bits for N=2048
     assert lib.cbs_get_primes(2048, 13, 5, np.zeros(5, np.uint64).ctypes.data) == 1
 

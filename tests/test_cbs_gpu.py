@@ -281,3 +281,55 @@ def test_aes128_ctr_transcipher_host_api(pkg, ctx, keys, aes_ctx):
     for blk in range(2):
         out = bytes(int(sum(int(dec[blk * 128 + i * 8 + b]) << b for b in range(8))) for i in range(16))
         assert out == want[blk]
+
+
+@pytest.mark.parametrize("blocks", [1, 3, 1000])
+def test_aes128_ctr_add_ciphertext_device_bit_exact(pkg, ctx, blocks):
+    """b[t] + q/2 mod q exactly where bit t of the public ciphertext is set (main.cu:1569-1582),
+    nothing else touched; 1000 blocks leave a partial last CTA."""
+    p = ctx.params
+    rng = np.random.default_rng(70 + blocks)
+    T = blocks * 128
+    b = rng.integers(0, p.q_lwe, T, dtype=np.uint64)
+    b[:3] = [0, p.q_lwe // 2, p.q_lwe - 1]  # wrap edges
+    cipher = rng.integers(0, 256, blocks * 16, dtype=np.uint8)
+    cipher[0] = 0x07
+    db = dev(b)
+    pkg.call("cbs_aes128_ctr_add_ciphertext_device", ctx.handle, dev(cipher).data_ptr(), blocks, db.data_ptr(),
+             None)
+    torch.cuda.synchronize()
+    bits = np.unpackbits(cipher, bitorder="little").astype(np.uint64)
+    want = (b + bits * (p.q_lwe // 2)) % p.q_lwe
+    assert np.array_equal(host(db), want)
+    assert pkg.load().cbs_aes128_ctr_add_ciphertext_device(ctx.handle, None, 0, None, None) == 0  # empty
+
+
+def test_aes128_ctr_transcipher_ciphertext_decrypts_to_plaintext(pkg, ctx, keys, aes_ctx):
+    """Counters + a public AES-CTR ciphertext in, LWE encryptions of the plaintext bits out:
+    the reference's download -> EvalAddConstEq -> Decrypt sequence with the add on the GPU."""
+    p = ctx.params
+    key, _, _ = aes_ctx
+    rng = np.random.default_rng(77)
+    blocks = 2
+    ctrs = [rng.bytes(16) for _ in range(blocks)]
+    plain = [rng.bytes(16) for _ in range(blocks)]
+    ks = _aes_ecb(key, ctrs)
+    cipher = [bytes(x ^ y for x, y in zip(pt, k)) for pt, k in zip(plain, ks)]
+    hc = np.frombuffer(b"".join(ctrs), np.uint8).copy()
+    hx = np.frombuffer(b"".join(cipher), np.uint8).copy()
+    oa = np.zeros((blocks * 128, p.n), np.uint64)
+    ob = np.zeros(blocks * 128, np.uint64)
+    pkg.call("cbs_aes128_ctr_transcipher_ciphertext", ctx.handle, hc.ctypes.data, hx.ctypes.data, blocks,
+             oa.ctypes.data, ob.ctypes.data)
+    dec = np.zeros(blocks * 128, np.uint8)
+    pkg.call("cbs_lwe_decrypt_bits", ctx.handle, oa.ctypes.data, ob.ctypes.data, blocks * 128, p.n, dec.ctypes.data)
+    for blk in range(blocks):
+        out = bytes(int(sum(int(dec[blk * 128 + i * 8 + b]) << b for b in range(8))) for i in range(16))
+        assert out == plain[blk]
+    # the keystream path on the same counters: same a, b differing by q/2 exactly where the
+    # ciphertext bit is set
+    ka = np.zeros_like(oa)
+    kb = np.zeros_like(ob)
+    pkg.call("cbs_aes128_ctr_transcipher", ctx.handle, hc.ctypes.data, blocks, ka.ctypes.data, kb.ctypes.data)
+    bits = np.unpackbits(hx, bitorder="little").astype(np.uint64)
+    assert np.array_equal((kb + bits * (p.q_lwe // 2)) % p.q_lwe, ob)
