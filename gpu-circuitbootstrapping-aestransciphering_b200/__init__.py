@@ -95,6 +95,8 @@ def _declare(lib: ctypes.CDLL) -> None:
         "cbs_lut8x32_batch_device": (st, [c_vp, c_vp, u32, c_vp, c_vp, u32, u64, c_vp, u32, c_vp, c_vp]),
         "cbs_extract_keyswitch_device": (st, [c_vp, c_vp, u32, c_vp, u32, c_vp, c_vp, u32, c_vp]),
         "cbs_aes128_setup": (st, [c_vp, c_vp, u64]),
+        "cbs_aes128_setup_device": (st, [c_vp, c_vp, c_vp]),
+        "cbs_cdt_table_host": (st, [ctypes.c_double, c_vp, u32, c_vp]),
         "cbs_aes128_export_material": (st, [c_vp, c_vp, c_vp, c_vp, c_vp]),
         "cbs_aes128_import_material": (st, [c_vp, c_vp, c_vp, c_vp, c_vp]),
         "cbs_aes128_ctr_transcipher_device": (st, [c_vp, c_vp, u32, c_vp, c_vp, ctypes.c_int, c_vp]),

@@ -15,6 +15,7 @@
 #include "aes_host.h"
 #include "common.cuh"
 #include "context.cuh"
+#include "encrypt.cuh"
 
 namespace cbs {
 
@@ -140,6 +141,8 @@ using namespace cbs;
 
 extern "C" {
 
+static cbs_status aes_derive_material(cbs_context* c);
+
 // upload the host AES material of A (tables, round-key words, round-0 key bits) and derive
 // the coefficient-domain copies of the FFT path
 static cbs_status aes_upload_material(cbs_context* c) {
@@ -150,6 +153,14 @@ static cbs_status aes_upload_material(cbs_context* c) {
     CBS_CUDA_TRY(A.rk_words.upload(A.h_rk_words.data(), A.h_rk_words.size(), s));
     CBS_CUDA_TRY(A.rk0_a.upload(A.h_rk0_a.data(), A.h_rk0_a.size(), s));
     CBS_CUDA_TRY(A.rk0_b.upload(A.h_rk0_b.data(), A.h_rk0_b.size(), s));
+    return aes_derive_material(c);
+}
+
+// coefficient-domain copies of the device tables / round-key words (FFT path), then ready
+static cbs_status aes_derive_material(cbs_context* c) {
+    AesState& A = c->aes;
+    const uint32_t N = c->p.N;
+    cudaStream_t s = c->stream;
     CBS_CUDA_TRY(A.tables_coef.alloc(A.h_tables.size()));
     CBS_CUDA_TRY(A.rk_words_coef.alloc(A.h_rk_words.size()));
     CBS_CUDA_TRY(ntt_inverse(A.tables_coef.p, A.tables.p, nullptr, c->d_irp.p, c->d_irps.p, c->d_mod.p, c->d_ninv.p,
@@ -227,6 +238,119 @@ cbs_status cbs_aes128_setup(cbs_context* ctx, const uint8_t* key, uint64_t seed)
                     A.h_rk0_b.data() + t);
     }
     return aes_upload_material(c);
+}
+
+// the plaintext words of the material: T-tables [8][256] then round-key words [11][4]
+// (key_material.cuh:30-36), and the round-0 key bits [128]
+static void aes_material_words(const uint8_t* key, std::vector<uint32_t>& words, std::vector<uint8_t>& bits) {
+    aes::Block k{};
+    std::memcpy(k.data(), key, 16);
+    const auto rk = aes::key_expand(k);
+    const auto te = aes::enc_tables();
+    words.clear();
+    for (uint32_t tb = 0; tb < 8; ++tb)
+        for (uint32_t x = 0; x < 256; ++x) words.push_back(te[tb][x]);
+    for (uint32_t r = 0; r <= 10; ++r)
+        for (uint32_t col = 0; col < 4; ++col)
+            words.push_back(aes::pack_be(rk[r][col * 4 + 0], rk[r][col * 4 + 1], rk[r][col * 4 + 2], rk[r][col * 4 + 3]));
+    bits.resize(128);
+    for (uint32_t t = 0; t < 128; ++t) bits[t] = (rk[0][t / 8] >> (t % 8)) & 1u;
+}
+
+cbs_status cbs_aes128_setup_device(cbs_context* ctx, const uint8_t* key, const uint8_t* rng_key) {
+    CBS_CHECK_ARG(ctx && key && rng_key, "aes_setup_device: null argument");
+    if (!ctx->keys_ready || !ctx->has_secret) {
+        set_error("aes_setup_device: encrypting the AES material needs the secret key (cbs_keygen or "
+                  "cbs_import_keys with secrets)");
+        return CBS_ERR_NOT_READY;
+    }
+    cbs_context* c = ctx;
+    AesState& A = c->aes;
+    const uint32_t N = c->p.N, n = c->p.n;
+    cudaStream_t s = c->stream;
+    std::memcpy(A.key, key, 16);
+    std::vector<uint32_t> words;
+    std::vector<uint8_t> bits;
+    aes_material_words(key, words, bits);
+    const uint32_t n_tab = 8 * 256, n_rk = 11 * 4;
+    ChachaKey ck{};
+    std::memcpy(ck.w, rng_key, 32);
+    const auto cdt_r = cdt_table(c->p.sigma_rlwe), cdt_l = cdt_table(c->p.sigma_lwe);
+    DevBuf<uint32_t> d_words;
+    DevBuf<uint64_t> d_tmp, d_s_ntt, d_cdt_r, d_cdt_l;
+    DevBuf<int32_t> d_s;
+    DevBuf<uint8_t> d_bits;
+    CBS_CUDA_TRY(d_words.upload(words.data(), words.size(), s));
+    CBS_CUDA_TRY(d_s_ntt.upload(c->hk.s_ntt.data(), N, s));
+    CBS_CUDA_TRY(d_s.upload(c->hk.s_lwe.data(), n, s));
+    CBS_CUDA_TRY(d_bits.upload(bits.data(), 128, s));
+    if (!cdt_r.empty()) CBS_CUDA_TRY(d_cdt_r.upload(cdt_r.data(), cdt_r.size(), s));
+    if (!cdt_l.empty()) CBS_CUDA_TRY(d_cdt_l.upload(cdt_l.data(), cdt_l.size(), s));
+    CBS_CUDA_TRY(d_tmp.alloc(static_cast<size_t>(n_tab) * N));
+    CBS_CUDA_TRY(A.tables.alloc(static_cast<size_t>(n_tab) * 2 * N));
+    CBS_CUDA_TRY(A.rk_words.alloc(static_cast<size_t>(n_rk) * 2 * N));
+    CBS_CUDA_TRY(A.rk0_a.alloc(static_cast<size_t>(128) * n));
+    CBS_CUDA_TRY(A.rk0_b.alloc(128));
+    EncryptRlweArgs ra{};
+    ra.key = ck;
+    ra.tmp = d_tmp.p;
+    ra.s_ntt = d_s_ntt.p;
+    ra.cdt = d_cdt_r.p;
+    ra.cdt_len = static_cast<uint32_t>(cdt_r.size());
+    ra.N = N;
+    ra.Q = c->p.Q;
+    ra.delta = c->p.Q >> 1;
+    ra.ratio0 = c->tab.ratio0;
+    ra.ratio1 = c->tab.ratio1;
+    ra.words = d_words.p;
+    ra.ct = A.tables.p;
+    ra.first = 0;
+    CBS_CUDA_TRY(launch_encrypt_rlwe_words(ra, n_tab, c->d_rp.p, c->d_rps.p, c->d_mod.p, s));
+    ra.words = d_words.p + n_tab;
+    ra.ct = A.rk_words.p;
+    ra.first = n_tab;
+    CBS_CUDA_TRY(launch_encrypt_rlwe_words(ra, n_rk, c->d_rp.p, c->d_rps.p, c->d_mod.p, s));
+    EncryptLweArgs la{};
+    la.key = ck;
+    la.bits = d_bits.p;
+    la.s = d_s.p;
+    la.cdt = d_cdt_l.p;
+    la.cdt_len = static_cast<uint32_t>(cdt_l.size());
+    la.n = n;
+    la.a_stride = n;
+    la.q = c->p.q_lwe;
+    la.out_a = A.rk0_a.p;
+    la.out_b = A.rk0_b.p;
+    CBS_CUDA_TRY(launch_encrypt_lwe_bits(la, 128, s));
+    // host copies for cbs_aes128_export_material
+    try {
+        A.h_tables.resize(static_cast<size_t>(n_tab) * 2 * N);
+        A.h_rk_words.resize(static_cast<size_t>(n_rk) * 2 * N);
+        A.h_rk0_a.resize(static_cast<size_t>(128) * n);
+        A.h_rk0_b.resize(128);
+    } catch (const std::exception& e) {
+        set_error(std::string("aes_setup_device: ") + e.what());
+        return CBS_ERR_OOM;
+    }
+    CBS_CUDA_TRY(cudaMemcpyAsync(A.h_tables.data(), A.tables.p, A.h_tables.size() * 8, cudaMemcpyDeviceToHost, s));
+    CBS_CUDA_TRY(cudaMemcpyAsync(A.h_rk_words.data(), A.rk_words.p, A.h_rk_words.size() * 8, cudaMemcpyDeviceToHost,
+                                 s));
+    CBS_CUDA_TRY(cudaMemcpyAsync(A.h_rk0_a.data(), A.rk0_a.p, A.h_rk0_a.size() * 8, cudaMemcpyDeviceToHost, s));
+    CBS_CUDA_TRY(cudaMemcpyAsync(A.h_rk0_b.data(), A.rk0_b.p, A.h_rk0_b.size() * 8, cudaMemcpyDeviceToHost, s));
+    CBS_CUDA_TRY(cudaStreamSynchronize(s));  // before the scratch buffers above are freed
+    return aes_derive_material(c);
+}
+
+cbs_status cbs_cdt_table_host(double sigma, uint64_t* out, uint32_t cap, uint32_t* len) {
+    CBS_CHECK_ARG(len, "cdt_table: null len");
+    CBS_CHECK_ARG(sigma >= 0 && sigma < 1e6, "cdt_table: sigma out of range");
+    const auto T = cdt_table(sigma);
+    *len = static_cast<uint32_t>(T.size());
+    if (out) {
+        CBS_CHECK_ARG(cap >= T.size(), "cdt_table: cap below the table length");
+        std::memcpy(out, T.data(), T.size() * sizeof(uint64_t));
+    }
+    return CBS_OK;
 }
 
 cbs_status cbs_aes128_import_material(cbs_context* ctx, const uint64_t* h_tables, const uint64_t* h_rk_words,

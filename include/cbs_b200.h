@@ -244,6 +244,16 @@ cbs_status cbs_extract_keyswitch_device(cbs_context *ctx, const uint64_t *d_word
 /* Encrypt the AES material for key[16] under the context's keys (tables Te0..3/Te4_*, the
  * 11 round-key words, the round-0 key bits). */
 cbs_status cbs_aes128_setup(cbs_context *ctx, const uint8_t *key, uint64_t seed);
+/* The same material encrypted on the device (the reference encrypts it on the host, one
+ * sample at a time: EncryptWord32RLWE / BuildTableRLWE, rlwe_tables.cuh:5-24;
+ * BuildEncryptedKeyMaterial, key_material.cuh:12-46).  Randomness from ChaCha20 (RFC 8439)
+ * under rng_key[32]: one block per coefficient, counter = coefficient index, nonce = (sample
+ * index, 1 for RLWE / 2 for LWE, 0); masks floor(x q / 2^128) from words 0-3, noise from the
+ * discrete Gaussian table of cbs_cdt_table_host with words 4-5.  Needs the secret key. */
+cbs_status cbs_aes128_setup_device(cbs_context *ctx, const uint8_t *key, const uint8_t *rng_key);
+/* T[k] = floor(2^63 P(|X| <= k)) of the discrete Gaussian exp(-x^2 / 2 sigma^2), k = 0.. while
+ * below 2^63; *len = its length; out (cap words) may be NULL to query the length. */
+cbs_status cbs_cdt_table_host(double sigma, uint64_t *out, uint32_t cap, uint32_t *len);
 /* Host copies of the encrypted material: tables [8][256][2][N], rk_words [11][4][2][N]
  * (NTT domain), rk0_a [128][n], rk0_b [128]; any pointer may be NULL. */
 cbs_status cbs_aes128_export_material(const cbs_context *ctx, uint64_t *h_tables, uint64_t *h_rk_words,

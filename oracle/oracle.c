@@ -1302,3 +1302,111 @@ void orc_aes_enc_tables(uint32_t te[8][256]) {
         te[7][x] = pack_be(0, 0, 0, s);
     }
 }
+
+
+/* ---------------- encryption of the AES material ---------------- */
+
+static uint32_t orc_rotl32(uint32_t x, int r) { return (x << r) | (x >> (32 - r)); }
+
+static void orc_chacha_qr(uint32_t *x, int a, int b, int c, int d) {
+    x[a] += x[b]; x[d] = orc_rotl32(x[d] ^ x[a], 16);
+    x[c] += x[d]; x[b] = orc_rotl32(x[b] ^ x[c], 12);
+    x[a] += x[b]; x[d] = orc_rotl32(x[d] ^ x[a], 8);
+    x[c] += x[d]; x[b] = orc_rotl32(x[b] ^ x[c], 7);
+}
+
+void orc_chacha20_block(const uint32_t key[8], uint32_t counter, const uint32_t nonce[3], uint32_t out[16]) {
+    uint32_t in[16] = {0x61707865u, 0x3320646eu, 0x79622d32u, 0x6b206574u};
+    for (int i = 0; i < 8; ++i) in[4 + i] = key[i];
+    in[12] = counter;
+    in[13] = nonce[0];
+    in[14] = nonce[1];
+    in[15] = nonce[2];
+    uint32_t x[16];
+    memcpy(x, in, sizeof(x));
+    for (int r = 0; r < 10; ++r) {
+        orc_chacha_qr(x, 0, 4, 8, 12);
+        orc_chacha_qr(x, 1, 5, 9, 13);
+        orc_chacha_qr(x, 2, 6, 10, 14);
+        orc_chacha_qr(x, 3, 7, 11, 15);
+        orc_chacha_qr(x, 0, 5, 10, 15);
+        orc_chacha_qr(x, 1, 6, 11, 12);
+        orc_chacha_qr(x, 2, 7, 8, 13);
+        orc_chacha_qr(x, 3, 4, 9, 14);
+    }
+    for (int i = 0; i < 16; ++i) out[i] = x[i] + in[i];
+}
+
+uint64_t orc_uniform_mod(const uint32_t w[4], uint64_t q) {
+    const u128 x = (u128)w[0] | ((u128)w[1] << 32) | ((u128)w[2] << 64) | ((u128)w[3] << 96);
+    /* floor(x q / 2^128) = floor((hi q + floor(lo q / 2^64)) / 2^64) */
+    const uint64_t lo = (uint64_t)x, hi = (uint64_t)(x >> 64);
+    const u128 t = (u128)hi * q + (uint64_t)(((u128)lo * q) >> 64);
+    return (uint64_t)(t >> 64);
+}
+
+uint32_t orc_cdt_table(double sigma, uint64_t *T, uint32_t cap) {
+    if (!(sigma > 0)) return 0;
+    const long double s2 = 2.0L * (long double)sigma * (long double)sigma;
+    const int X = (int)ceil(14.0 * sigma) + 1;
+    long double S = 1.0L;
+    for (int x = 1; x <= X; ++x) S += 2.0L * expl(-(long double)x * x / s2);
+    const long double two63 = 9223372036854775808.0L;
+    long double cum = 1.0L;
+    uint32_t len = 0;
+    for (int k = 0; k <= X; ++k) {
+        if (k > 0) cum += 2.0L * expl(-(long double)k * k / s2);
+        const long double t = floorl(two63 * (cum / S));
+        if (t >= two63) break;
+        if (len < cap) T[len] = (uint64_t)t;
+        ++len;
+    }
+    return len;
+}
+
+int64_t orc_cdt_sample(uint64_t u, const uint64_t *T, uint32_t len) {
+    const uint64_t v = u & 0x7fffffffffffffffull;
+    int64_t mag = 0;
+    for (uint32_t k = 0; k < len; ++k) mag += v >= T[k];
+    return (u >> 63) ? -mag : mag;
+}
+
+void orc_encrypt_words_rlwe(const uint32_t key[8], const uint32_t *words, uint32_t count, uint32_t first, uint32_t N,
+                            uint64_t Q, const uint64_t *rp, const uint64_t *s_ntt, const uint64_t *T, uint32_t tlen,
+                            uint64_t *out) {
+    uint64_t *tmp = (uint64_t *)malloc((size_t)N * sizeof(uint64_t));
+    for (uint32_t r = 0; r < count; ++r) {
+        uint64_t *a = out + (size_t)r * 2 * N, *b = a + N;
+        const uint32_t nonce[3] = {first + r, 1u, 0u};
+        for (uint32_t i = 0; i < N; ++i) {
+            uint32_t blk[16];
+            orc_chacha20_block(key, i, nonce, blk);
+            a[i] = orc_uniform_mod(blk, Q);
+            const int64_t e = orc_cdt_sample((uint64_t)blk[4] | ((uint64_t)blk[5] << 32), T, tlen);
+            uint64_t v = e < 0 ? Q - (uint64_t)(-e) : (uint64_t)e;
+            if (i < 32 && ((words[r] >> i) & 1u)) v = (v + (Q >> 1)) % Q;
+            tmp[i] = v;
+        }
+        orc_ntt_forward(tmp, 1, N, Q, rp);
+        for (uint32_t i = 0; i < N; ++i) b[i] = (orc_mulmod(a[i], s_ntt[i], Q) + tmp[i]) % Q;
+    }
+    free(tmp);
+}
+
+void orc_encrypt_bits_lwe(const uint32_t key[8], const uint8_t *bits, uint32_t count, uint32_t n, uint64_t q,
+                          const int32_t *s, const uint64_t *T, uint32_t tlen, uint64_t *a, uint64_t *b) {
+    for (uint32_t t = 0; t < count; ++t) {
+        const uint32_t nonce[3] = {t, 2u, 0u};
+        u128 acc = 0;
+        uint32_t blk[16];
+        for (uint32_t i = 0; i < n; ++i) {
+            orc_chacha20_block(key, i, nonce, blk);
+            a[(size_t)t * n + i] = orc_uniform_mod(blk, q);
+            if (s[i]) acc += a[(size_t)t * n + i];
+        }
+        orc_chacha20_block(key, n, nonce, blk);
+        const int64_t e = orc_cdt_sample((uint64_t)blk[4] | ((uint64_t)blk[5] << 32), T, tlen);
+        const uint64_t eq = e < 0 ? q - (uint64_t)(-e) % q : (uint64_t)e % q;
+        b[t] = (uint64_t)((acc % q + (bits[t] ? q >> 1 : 0) + eq) % q);
+    }
+}

@@ -188,6 +188,28 @@ void orc_aes_enc_tables(uint32_t te[8][256]);
 /* OpenMP thread count used by the batched routines */
 int orc_num_threads(void);
 
+/* ---------------- encryption of the AES material (rlwe_tables.cuh:5-24,
+ * key_material.cuh:12-46; the reference encrypts on the host through OpenFHE, whose
+ * sampler is absent, so this restates the device design: ChaCha20 per coefficient,
+ * floor(x q / 2^128) masks, discrete-Gaussian noise by cumulative table) ---------------- */
+
+/* RFC 8439 s2.3 block function: state = constants, key[8], counter, nonce[3]; out[16] */
+void orc_chacha20_block(const uint32_t key[8], uint32_t counter, const uint32_t nonce[3], uint32_t out[16]);
+/* floor(x q / 2^128), x = w[0] + w[1] 2^32 + w[2] 2^64 + w[3] 2^96 */
+uint64_t orc_uniform_mod(const uint32_t w[4], uint64_t q);
+/* T[k] = floor(2^63 P(|X| <= k)) of exp(-x^2 / 2 sigma^2) while below 2^63; returns the length */
+uint32_t orc_cdt_table(double sigma, uint64_t *T, uint32_t cap);
+/* sign = bit 63 of u, magnitude = #{k : (u mod 2^63) >= T[k]} */
+int64_t orc_cdt_sample(uint64_t u, const uint64_t *T, uint32_t len);
+/* RLWE (NTT domain) of count words, sample indices first.., bit j of a word -> floor(Q/2)
+ * on coefficient j; out [count][2][N] */
+void orc_encrypt_words_rlwe(const uint32_t key[8], const uint32_t *words, uint32_t count, uint32_t first, uint32_t N,
+                            uint64_t Q, const uint64_t *rp, const uint64_t *s_ntt, const uint64_t *T, uint32_t tlen,
+                            uint64_t *out);
+/* LWE of count bits (floor(q/2) scaling) under the binary s[n]; a [count][n], b [count] */
+void orc_encrypt_bits_lwe(const uint32_t key[8], const uint8_t *bits, uint32_t count, uint32_t n, uint64_t q,
+                          const int32_t *s, const uint64_t *T, uint32_t tlen, uint64_t *a, uint64_t *b);
+
 #ifdef __cplusplus
 }
 #endif
