@@ -344,6 +344,49 @@ def rns_chain(pkg, n: int, size_q: int, size_p: int, bits: int = 50):
     return out[:size_q].copy(), out[size_q:].copy()
 
 
+def run_aes_setup(args, rank: int, world: int, local_rank: int) -> None:
+    """Encryption of the AES material (8 x 256 T-table words and 44 round-key words as RLWE,
+    the 128 round-0 key bits as LWE): cbs_aes128_setup_device (ChaCha20, NTT and products on
+    the GPU, host copies downloaded) per step, beside the host encryption cbs_aes128_setup
+    (the reference's shape: one sample at a time on one host thread).  Both end with the
+    material resident and its coefficient-domain copies derived."""
+    import torch
+    torch.cuda.set_device(local_rank)
+    pkg = load_pkg()
+    ctx = pkg.Context(max_batch=128)
+    ctx.keygen(args.seed)
+    key, rng_key = bytes(range(16)), bytes(range(32, 64))
+    for _ in range(max(1, args.warmup)):
+        pkg.call("cbs_aes128_setup_device", ctx.handle, key, rng_key)
+    torch.cuda.synchronize()
+    rep = load_replicas()
+    with ClockSampler(local_rank) as clk:
+        rep.barrier(world)
+        t0 = time.perf_counter()  # each call is synchronous (it ends with the host copies)
+        for _ in range(args.steps):
+            pkg.call("cbs_aes128_setup_device", ctx.handle, key, rng_key)
+        dev_ms = rep.max_over_ranks((time.perf_counter() - t0) / args.steps * 1e3, world, device="cuda")
+    t0 = time.perf_counter()
+    pkg.call("cbs_aes128_setup", ctx.handle, key, 7)
+    host_ms = (time.perf_counter() - t0) * 1e3
+    samples = 8 * 256 + 44
+    out = {"metric": "AES material encryptions/s (2092 RLWE + 128 LWE samples each)",
+           "value": world * 1e3 / dev_ms, "unit": "setups/s", "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": dev_ms, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "u32 (ChaCha20) + u64 (mod-Q NTT)", "data": "synthetic (seeded keys)",
+           "config": {"workload": "aes_setup", "rlwe_samples": samples, "lwe_samples": 128, "N": ctx.params.N},
+           "gpu_launches": args.steps * (2 * 3 + 1 + 2),
+           "e2e": {"value": world * 1e3 / dev_ms, "unit": "setups/s", "h2d_bytes_per_step": samples * 4 + 128,
+                   "d2h_bytes_per_step": (samples * 2 * ctx.params.N + 128 * (ctx.params.n + 1)) * 8},
+           "roofline": None,
+           "cpu_baseline": {"value": 1e3 / host_ms, "unit": "setups/s", "cores": 1, "kind": "port",
+                            "sample": "one cbs_aes128_setup: the same samples encrypted on the host, "
+                                      "one at a time (xoshiro + Box-Muller noise, host NTT)"},
+           "clocks": clk.summary()}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
 def run_keyswitch(args, rank: int, world: int, local_rank: int) -> None:
     """Phantom RNS core: hybrid key switching of `--batch` ciphertexts (N = 2^16, 24 primes of
     50 bits + alpha special primes) per step, inputs resident in HBM."""
@@ -864,7 +907,8 @@ def main() -> None:
                          "split FP32 (24/25-bit + exact top key limb), or FP32 on whole keys; FP32 modes use "
                          "--multibit 1")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
-    ap.add_argument("--workload", choices=["aes128", "blind_rotate", "keyswitch", "rns_ntt", "gate", "ragged", "tcb"],
+    ap.add_argument("--workload", choices=["aes128", "blind_rotate", "keyswitch", "rns_ntt", "gate", "ragged", "tcb",
+                                           "aes_setup"],
                     default="aes128",
                     help="aes128 is the headline; the others time one kernel family")
     ap.add_argument("--batch", type=int, default=0, help="units per step for the kernel workloads")
@@ -898,7 +942,7 @@ def main() -> None:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     runner = {"aes128": run_ours, "blind_rotate": run_blind_rotate, "keyswitch": run_keyswitch,
               "rns_ntt": run_rns_ntt, "gate": run_gate,
-              "ragged": run_ragged, "tcb": run_tcb}[args.workload]
+              "ragged": run_ragged, "tcb": run_tcb, "aes_setup": run_aes_setup}[args.workload]
     try:
         runner(args, rank, world, local_rank)
     finally:
