@@ -347,7 +347,7 @@ def rns_chain(pkg, n: int, size_q: int, size_p: int, bits: int = 50):
 def run_aes_setup(args, rank: int, world: int, local_rank: int) -> None:
     """Encryption of the AES material (8 x 256 T-table words and 44 round-key words as RLWE,
     the 128 round-0 key bits as LWE): cbs_aes128_setup_device (ChaCha20, NTT and products on
-    the GPU, host copies downloaded) per step, beside the host encryption cbs_aes128_setup
+    the GPU; the host copies stay on the device until exported) per step, beside the host encryption cbs_aes128_setup
     (the reference's shape: one sample at a time on one host thread).  Both end with the
     material resident and its coefficient-domain copies derived."""
     import torch
@@ -377,7 +377,7 @@ def run_aes_setup(args, rank: int, world: int, local_rank: int) -> None:
            "config": {"workload": "aes_setup", "rlwe_samples": samples, "lwe_samples": 128, "N": ctx.params.N},
            "gpu_launches": args.steps * (2 * 3 + 1 + 2),
            "e2e": {"value": world * 1e3 / dev_ms, "unit": "setups/s", "h2d_bytes_per_step": samples * 4 + 128,
-                   "d2h_bytes_per_step": (samples * 2 * ctx.params.N + 128 * (ctx.params.n + 1)) * 8},
+                   "d2h_bytes_per_step": 0},
            "roofline": None,
            "cpu_baseline": {"value": 1e3 / host_ms, "unit": "setups/s", "cores": 1, "kind": "port",
                             "sample": "one cbs_aes128_setup: the same samples encrypted on the host, "

@@ -153,6 +153,7 @@ static cbs_status aes_upload_material(cbs_context* c) {
     CBS_CUDA_TRY(A.rk_words.upload(A.h_rk_words.data(), A.h_rk_words.size(), s));
     CBS_CUDA_TRY(A.rk0_a.upload(A.h_rk0_a.data(), A.h_rk0_a.size(), s));
     CBS_CUDA_TRY(A.rk0_b.upload(A.h_rk0_b.data(), A.h_rk0_b.size(), s));
+    A.host_stale = false;
     return aes_derive_material(c);
 }
 
@@ -161,12 +162,13 @@ static cbs_status aes_derive_material(cbs_context* c) {
     AesState& A = c->aes;
     const uint32_t N = c->p.N;
     cudaStream_t s = c->stream;
-    CBS_CUDA_TRY(A.tables_coef.alloc(A.h_tables.size()));
-    CBS_CUDA_TRY(A.rk_words_coef.alloc(A.h_rk_words.size()));
+    const size_t tab_words = static_cast<size_t>(8) * 256 * 2 * N, rk_words = static_cast<size_t>(11) * 4 * 2 * N;
+    CBS_CUDA_TRY(A.tables_coef.alloc(tab_words));
+    CBS_CUDA_TRY(A.rk_words_coef.alloc(rk_words));
     CBS_CUDA_TRY(ntt_inverse(A.tables_coef.p, A.tables.p, nullptr, c->d_irp.p, c->d_irps.p, c->d_mod.p, c->d_ninv.p,
-                             c->d_ninv_s.p, N, A.h_tables.size() / N, s));
+                             c->d_ninv_s.p, N, tab_words / N, s));
     CBS_CUDA_TRY(ntt_inverse(A.rk_words_coef.p, A.rk_words.p, nullptr, c->d_irp.p, c->d_irps.p, c->d_mod.p,
-                             c->d_ninv.p, c->d_ninv_s.p, N, A.h_rk_words.size() / N, s));
+                             c->d_ninv.p, c->d_ninv_s.p, N, rk_words / N, s));
     CBS_CUDA_TRY(cudaStreamSynchronize(s));
     A.ready = true;
     A.spec_ready = false;
@@ -322,23 +324,13 @@ cbs_status cbs_aes128_setup_device(cbs_context* ctx, const uint8_t* key, const u
     la.out_a = A.rk0_a.p;
     la.out_b = A.rk0_b.p;
     CBS_CUDA_TRY(launch_encrypt_lwe_bits(la, 128, s));
-    // host copies for cbs_aes128_export_material
-    try {
-        A.h_tables.resize(static_cast<size_t>(n_tab) * 2 * N);
-        A.h_rk_words.resize(static_cast<size_t>(n_rk) * 2 * N);
-        A.h_rk0_a.resize(static_cast<size_t>(128) * n);
-        A.h_rk0_b.resize(128);
-    } catch (const std::exception& e) {
-        set_error(std::string("aes_setup_device: ") + e.what());
-        return CBS_ERR_OOM;
-    }
-    CBS_CUDA_TRY(cudaMemcpyAsync(A.h_tables.data(), A.tables.p, A.h_tables.size() * 8, cudaMemcpyDeviceToHost, s));
-    CBS_CUDA_TRY(cudaMemcpyAsync(A.h_rk_words.data(), A.rk_words.p, A.h_rk_words.size() * 8, cudaMemcpyDeviceToHost,
-                                 s));
-    CBS_CUDA_TRY(cudaMemcpyAsync(A.h_rk0_a.data(), A.rk0_a.p, A.h_rk0_a.size() * 8, cudaMemcpyDeviceToHost, s));
-    CBS_CUDA_TRY(cudaMemcpyAsync(A.h_rk0_b.data(), A.rk0_b.p, A.h_rk0_b.size() * 8, cudaMemcpyDeviceToHost, s));
-    CBS_CUDA_TRY(cudaStreamSynchronize(s));  // before the scratch buffers above are freed
-    return aes_derive_material(c);
+    // no host copies: cbs_aes128_export_material reads the device buffers
+    A.h_tables.clear();
+    A.h_rk_words.clear();
+    A.h_rk0_a.clear();
+    A.h_rk0_b.clear();
+    A.host_stale = true;
+    return aes_derive_material(c);  // synchronizes before the scratch buffers above are freed
 }
 
 cbs_status cbs_cdt_table_host(double sigma, uint64_t* out, uint32_t cap, uint32_t* len) {
@@ -392,6 +384,18 @@ cbs_status cbs_aes128_export_material(const cbs_context* ctx, uint64_t* h_tables
         return CBS_ERR_NOT_READY;
     }
     const AesState& A = ctx->aes;
+    if (A.host_stale) {  // encrypted on the device
+        const size_t N = ctx->p.N, n = ctx->p.n;
+        cudaStream_t s = ctx->stream;
+        if (h_tables)
+            CBS_CUDA_TRY(cudaMemcpyAsync(h_tables, A.tables.p, 8ull * 256 * 2 * N * 8, cudaMemcpyDeviceToHost, s));
+        if (h_rk_words)
+            CBS_CUDA_TRY(cudaMemcpyAsync(h_rk_words, A.rk_words.p, 11ull * 4 * 2 * N * 8, cudaMemcpyDeviceToHost, s));
+        if (h_rk0_a) CBS_CUDA_TRY(cudaMemcpyAsync(h_rk0_a, A.rk0_a.p, 128ull * n * 8, cudaMemcpyDeviceToHost, s));
+        if (h_rk0_b) CBS_CUDA_TRY(cudaMemcpyAsync(h_rk0_b, A.rk0_b.p, 128ull * 8, cudaMemcpyDeviceToHost, s));
+        CBS_CUDA_TRY(cudaStreamSynchronize(s));
+        return CBS_OK;
+    }
     if (h_tables) std::memcpy(h_tables, A.h_tables.data(), A.h_tables.size() * 8);
     if (h_rk_words) std::memcpy(h_rk_words, A.h_rk_words.data(), A.h_rk_words.size() * 8);
     if (h_rk0_a) std::memcpy(h_rk0_a, A.h_rk0_a.data(), A.h_rk0_a.size() * 8);

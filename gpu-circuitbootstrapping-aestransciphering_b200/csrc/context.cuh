@@ -20,6 +20,7 @@ namespace cbs {
 
 struct AesState {
     bool ready = false;
+    bool host_stale = false;              // material encrypted on the device: no h_* copies
     uint8_t key[16];
     uint32_t chunk_blocks = 0;            // blocks per device chunk
     DevBuf<uint64_t> tables;              // [8][256][2][N]  Te0..3, Te4_0..3
