@@ -8,6 +8,9 @@
 // the encrypted round-key word (column c gathers byte (row, c+row): ShiftRows), and
 // extracts + key-switches the 128 state bits back to LWE (extract.cuh:283-366).  The
 // per-round sequence of launches is captured once per chunk size into a CUDA graph.
+#include <sys/random.h>
+
+#include <cerrno>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -204,6 +207,7 @@ cbs_status cbs_aes128_setup(cbs_context* ctx, const uint8_t* key, uint64_t seed)
     AesState& A = c->aes;
     const uint32_t N = c->p.N, n = c->p.n;
     const uint64_t Q = c->p.Q, delta = Q >> 1;
+    A.ready = false;  // set again once the new material is uploaded and derived
     aes::Block k{};
     std::memcpy(k.data(), key, 16);
     std::memcpy(A.key, key, 16);
@@ -259,8 +263,22 @@ static void aes_material_words(const uint8_t* key, std::vector<uint32_t>& words,
     for (uint32_t t = 0; t < 128; ++t) bits[t] = (rk[0][t / 8] >> (t % 8)) & 1u;
 }
 
+// 32 bytes from the operating system's CSPRNG (getrandom(2), retried on EINTR / short reads)
+static bool os_random_bytes(uint8_t* out, size_t len) {
+    size_t got = 0;
+    while (got < len) {
+        const ssize_t r = getrandom(out + got, len - got, 0);
+        if (r < 0) {
+            if (errno == EINTR) continue;
+            return false;
+        }
+        got += static_cast<size_t>(r);
+    }
+    return true;
+}
+
 cbs_status cbs_aes128_setup_device(cbs_context* ctx, const uint8_t* key, const uint8_t* rng_key) {
-    CBS_CHECK_ARG(ctx && key && rng_key, "aes_setup_device: null argument");
+    CBS_CHECK_ARG(ctx && key, "aes_setup_device: null argument");
     if (!ctx->keys_ready || !ctx->has_secret) {
         set_error("aes_setup_device: encrypting the AES material needs the secret key (cbs_keygen or "
                   "cbs_import_keys with secrets)");
@@ -270,13 +288,23 @@ cbs_status cbs_aes128_setup_device(cbs_context* ctx, const uint8_t* key, const u
     AesState& A = c->aes;
     const uint32_t N = c->p.N, n = c->p.n;
     cudaStream_t s = c->stream;
+    ChachaKey ck{};
+    if (rng_key) {
+        std::memcpy(ck.w, rng_key, 32);
+    } else if (!os_random_bytes(reinterpret_cast<uint8_t*>(ck.w), 32)) {
+        set_error(std::string("aes_setup_device: getrandom failed: ") + std::strerror(errno));
+        return CBS_ERR_UNSUPPORTED;
+    }
+    // the buffers below are overwritten in place: until derive succeeds the context holds no
+    // usable material (a failure midway leaves it not ready rather than half old, half new)
+    A.ready = false;
+    A.spec_ready = false;
+    A.drop_graphs();
     std::memcpy(A.key, key, 16);
     std::vector<uint32_t> words;
     std::vector<uint8_t> bits;
     aes_material_words(key, words, bits);
     const uint32_t n_tab = 8 * 256, n_rk = 11 * 4;
-    ChachaKey ck{};
-    std::memcpy(ck.w, rng_key, 32);
     const auto cdt_r = cdt_table(c->p.sigma_rlwe), cdt_l = cdt_table(c->p.sigma_lwe);
     DevBuf<uint32_t> d_words;
     DevBuf<uint64_t> d_tmp, d_s_ntt, d_cdt_r, d_cdt_l;
@@ -330,7 +358,10 @@ cbs_status cbs_aes128_setup_device(cbs_context* ctx, const uint8_t* key, const u
     A.h_rk0_a.clear();
     A.h_rk0_b.clear();
     A.host_stale = true;
-    return aes_derive_material(c);  // synchronizes before the scratch buffers above are freed
+    const cbs_status st = aes_derive_material(c);  // synchronizes before the scratch buffers are freed
+    volatile uint32_t* wipe = ck.w;
+    for (int i = 0; i < 8; ++i) wipe[i] = 0;
+    return st;
 }
 
 cbs_status cbs_cdt_table_host(double sigma, uint64_t* out, uint32_t cap, uint32_t* len) {

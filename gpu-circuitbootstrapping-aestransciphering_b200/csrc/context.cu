@@ -324,6 +324,8 @@ cbs_status run_extract(cbs_context* c, const uint64_t* d_words_coef, const uint3
 
 static bool pow2(uint64_t x) { return x && !(x & (x - 1)); }
 
+static constexpr double kMaxSigma = 1000.0;
+
 static cbs_status validate(const cbs_params& p) {
     CBS_CHECK_ARG(p.N == 1024 || p.N == 2048 || p.N == 4096, "params: N must be 1024, 2048 or 4096");
     CBS_CHECK_ARG(p.Q > 2 && p.Q < (1ull << 62) && (p.Q - 1) % (2ull * p.N) == 0, "params: Q must be 1 mod 2N, < 2^62");
@@ -338,6 +340,9 @@ static cbs_status validate(const cbs_params& p) {
     CBS_CHECK_ARG(pow2(p.qks) && p.qks <= 65536 && pow2(p.base_ks), "params: qks/base_ks must be powers of two");
     CBS_CHECK_ARG(static_cast<uint64_t>(p.base_ks) * p.base_ks >= p.qks && p.base_ks < p.qks,
                   "params: extraction key switch needs exactly two digits");
+    // the discrete-Gaussian samplers tabulate about 14 sigma entries and scan them per sample
+    CBS_CHECK_ARG(p.sigma_lwe >= 0 && p.sigma_lwe < kMaxSigma && p.sigma_rlwe >= 0 && p.sigma_rlwe < kMaxSigma,
+                  "params: sigma_lwe and sigma_rlwe must lie in [0, 1000)");
     return CBS_OK;
 }
 

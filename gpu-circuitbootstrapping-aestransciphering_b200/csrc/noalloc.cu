@@ -76,6 +76,15 @@ cbs_status cbs_circuit_bootstrap_batch_device_noalloc(cbs_context* ctx, const ui
         set_error("circuit_bootstrap_noalloc: no key material (call cbs_keygen first)");
         return CBS_ERR_NOT_READY;
     }
+    // the scratch address is per device: the current device must hold this context's keys
+    int dev = -1;
+    CBS_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev != ctx->device) {
+        set_error("circuit_bootstrap_noalloc: the current device (" + std::to_string(dev) +
+                  ") is not the context's device (" + std::to_string(ctx->device) +
+                  "); call cudaSetDevice first");
+        return CBS_ERR_INVALID_ARG;
+    }
     uint64_t* scratch = nullptr;
     if (cbs_status st = scratch_address(&scratch)) return st;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);

@@ -110,8 +110,8 @@ typedef struct {
     uint32_t trace_shift;/* log2 N - trace rounds; 0 = full trace */
     uint32_t qks;        /* extraction key-switch modulus (power of two, <= 2^16) */
     uint32_t base_ks;    /* extraction key-switch base (power of two, two digits cover qks) */
-    double sigma_lwe;    /* noise of fresh LWE samples and of the key-switching key */
-    double sigma_rlwe;   /* noise of RLWE / RGSW key material */
+    double sigma_lwe;    /* noise of fresh LWE samples and of the key-switching key, [0, 1000) */
+    double sigma_rlwe;   /* noise of RLWE / RGSW key material, [0, 1000) */
 } cbs_params;
 
 typedef struct cbs_context cbs_context;
@@ -249,7 +249,14 @@ cbs_status cbs_aes128_setup(cbs_context *ctx, const uint8_t *key, uint64_t seed)
  * BuildEncryptedKeyMaterial, key_material.cuh:12-46).  Randomness from ChaCha20 (RFC 8439)
  * under rng_key[32]: one block per coefficient, counter = coefficient index, nonce = (sample
  * index, 1 for RLWE / 2 for LWE, 0); masks floor(x q / 2^128) from words 0-3, noise from the
- * discrete Gaussian table of cbs_cdt_table_host with words 4-5.  Needs the secret key. */
+ * discrete Gaussian table of cbs_cdt_table_host with words 4-5.  Needs the secret key.
+ * rng_key determines every mask and noise value, so it is as sensitive as the secret key:
+ * whoever knows it recomputes (a, e) and solves b - e - m = a s for s, and two setups under
+ * the same rng_key (another AES key, or another context sharing s) reveal the difference of
+ * their messages.  It must come from a CSPRNG, stay secret and never be reused.  Pass
+ * rng_key = NULL to have the call draw a fresh one from the operating system (getrandom);
+ * a fixed rng_key is for reproducible tests only.  On any failure the context holds no AES
+ * material (CBS_ERR_NOT_READY from the transcipher calls) until a setup succeeds. */
 cbs_status cbs_aes128_setup_device(cbs_context *ctx, const uint8_t *key, const uint8_t *rng_key);
 /* T[k] = floor(2^63 P(|X| <= k)) of the discrete Gaussian exp(-x^2 / 2 sigma^2), k = 0.. while
  * below 2^63; *len = its length; out (cap words) may be NULL to query the length. */
@@ -305,6 +312,8 @@ cbs_status cbs_lwe_decrypt_bits(const cbs_context *ctx, const uint64_t *h_a, con
  * streams or contexts in flight at once) race; serialize them.  The context itself must
  * already exist with its keys (cbs_context_create / cbs_keygen allocate). */
 size_t cbs_circuit_bootstrap_noalloc_capacity_words(void);
+/* The calling thread's current device must be the one the context was created on
+ * (CBS_ERR_INVALID_ARG otherwise): the keys live there, and so does the array the call uses. */
 cbs_status cbs_circuit_bootstrap_batch_device_noalloc(cbs_context *ctx, const uint64_t *d_a, const uint64_t *d_b,
                                                       uint32_t batch, uint32_t a_stride, uint64_t *d_rgsw_out,
                                                       cbs_stream_t stream);

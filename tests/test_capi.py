@@ -109,3 +109,19 @@ def test_cpp_facade_compiles(tmp_path):
     r = subprocess.run([gxx, "-std=c++17", "-fsyntax-only", "-I", str(ROOT / "include"), "-I",
                         "/usr/local/cuda/include", str(src)], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+@pytest.mark.parametrize("field,value", [("sigma_lwe", 1e3), ("sigma_rlwe", 5e4), ("sigma_lwe", -1.0),
+                                         ("sigma_rlwe", float("nan"))])
+def test_params_reject_sigma_out_of_range(pkg, lib, field, value):
+    """The discrete-Gaussian samplers tabulate ~14 sigma entries: sigma is bounded to [0, 1000)
+    by every parameter check (context creation and the host key generation alike)."""
+    p = pkg.default_params()
+    setattr(p, field, value)
+    h = ctypes.c_void_p()
+    assert lib.cbs_context_create(ctypes.byref(p), 8, ctypes.byref(h)) == 1
+    assert b"sigma" in lib.cbs_last_error()
+    assert h.value is None
+    words = ctypes.c_size_t()
+    assert lib.cbs_generate_mb_bsk_host(ctypes.byref(p), 1, 2, None, ctypes.byref(words)) == 1
+    assert b"sigma" in lib.cbs_last_error()

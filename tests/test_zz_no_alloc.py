@@ -29,10 +29,16 @@ def _copy_view(view: int, words: int):
     return out
 
 
-def test_noalloc_matches_allocating_entry_point(pkg):
+@pytest.mark.parametrize("backend", ["ntt", "fft64"])
+def test_noalloc_matches_allocating_entry_point(pkg, backend):
+    """Both blind-rotation backends: the exact NTT one hands NTT-domain RLWEs to the trace; the
+    FFT one hands coefficient-domain RLWEs to the FFT trace, whose row spectra are written into
+    the caller's output buffer and converted there to the NTT-domain rows."""
     lib = pkg.load()
     ctx = pkg.Context(max_batch=32)
     ctx.keygen(5)
+    if backend == "fft64":
+        ctx.set_br_backend(1)
     p = ctx.params
     keys = ctx.export_keys()
     per = p.num_lut * 4 * p.N
