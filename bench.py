@@ -149,7 +149,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     torch.cuda.set_device(local_rank)
     pkg = load_pkg()
     blocks = args.blocks
-    ctx = pkg.Context(max_batch=128 * min(blocks, 256))
+    ctx = pkg.Context(params=pkg.preset_params(args.params), max_batch=128 * min(blocks, 256))
     ctx.keygen(args.seed)
     pkg.call("cbs_context_set_br_backend", ctx.handle, pkg.BR_FFT64 if args.backend == "fft64" else pkg.BR_NTT)
     if args.multibit > 1:
@@ -255,7 +255,9 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
                  else "u64 (exact mod-Q NTT arithmetic)",
         "data": "synthetic (seeded AES key; counters: one seeded CTR stream, rank r takes blocks [r B, (r+1) B))",
         "config": {"workload": "aes128_ctr_transcipher", "blocks_per_gpu": blocks, "global_blocks": world * blocks,
-                   "params": "N=2048 Q=54-bit n=630 q=2^14 BR 2^12x3 RGSW 2^6x4 HT 2^9x5 SS 2^9x5 KS 2^14/2^7",
+                   "params": f"N=2048 Q=54-bit n=630 q=2^14 BR 2^{p.base_g.bit_length() - 1}x{p.digits_g} RGSW 2^6x4 "
+                             f"HT 2^9x5 SS 2^9x5 KS 2^14/2^7",
+                   "param_set": args.params,
                    "l2": "per-step working set (keys + RGSW + LUT buffers) >> 126 MB L2",
                    "br_multibit": args.multibit,
                    "parallelism": f"replicas x{world} (independent blocks per GPU)"},
@@ -302,7 +304,7 @@ def run_blind_rotate(args, rank: int, world: int, local_rank: int) -> None:
     torch.cuda.set_device(local_rank)
     pkg = load_pkg()
     T = args.batch or 2368
-    ctx = pkg.Context(max_batch=T)
+    ctx = pkg.Context(params=pkg.preset_params(args.params), max_batch=T)
     ctx.keygen(args.seed)
     pkg.call("cbs_context_set_br_backend", ctx.handle, pkg.BR_FFT64 if args.backend == "fft64" else pkg.BR_NTT)
     if args.multibit > 1:
@@ -326,6 +328,7 @@ def run_blind_rotate(args, rank: int, world: int, local_rank: int) -> None:
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
            "dtype": "f64" if args.backend == "fft64" else "u64", "data": "synthetic (seeded random LWE)",
            "config": {"workload": "blind_rotate", "batch": T, "backend": args.backend, "br_multibit": args.multibit,
+                      "param_set": args.params, "br_gadget": f"2^{p.base_g.bit_length() - 1}x{p.digits_g}",
                       "l2": "BSK read once per launch (124 MB fft64 / 124 MB ntt); no flush between launches"},
            "us_per_bootstrap": ms * 1e3 / T, "gpu_launches": args.steps,
            "roofline": {"kernel": br_kernel_name(args),
@@ -906,6 +909,9 @@ def main() -> None:
                     help="external-product arithmetic of --workload gate / ragged (torus-32): exact FP64, "
                          "split FP32 (24/25-bit + exact top key limb), or FP32 on whole keys; FP32 modes use "
                          "--multibit 1")
+    ap.add_argument("--params", choices=["3x12", "2x18"], default="3x12",
+                    help="parameter set of the aes128 / blind_rotate workloads: blind-rotation gadget 2^12 x 3 "
+                         "(cbs_params_default) or 2^18 x 2")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--workload", choices=["aes128", "blind_rotate", "keyswitch", "rns_ntt", "gate", "ragged", "tcb",
                                            "aes_setup"],

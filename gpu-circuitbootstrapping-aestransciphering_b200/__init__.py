@@ -76,6 +76,7 @@ def _declare(lib: ctypes.CDLL) -> None:
         "cbs_ntt_tables_host": (st, [u32, u64, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
         "cbs_get_primes": (st, [u32, ctypes.c_int, u32, c_vp]),
         "cbs_params_default": (st, [c_vp]),
+        "cbs_params_preset": (st, [ctypes.c_int, c_vp]),
         "cbs_context_create": (st, [c_vp, u32, c_vp]),
         "cbs_context_destroy": (st, [c_vp]),
         "cbs_context_stream": (st, [c_vp, c_vp]),
@@ -93,6 +94,7 @@ def _declare(lib: ctypes.CDLL) -> None:
         "cbs_trace_schemeswitch_device": (st, [c_vp, c_vp, u32, c_vp, c_vp]),
         "cbs_circuit_bootstrap_batch_device": (st, [c_vp, c_vp, c_vp, u32, u32, c_vp, c_vp]),
         "cbs_lut8x32_batch_device": (st, [c_vp, c_vp, u32, c_vp, c_vp, u32, u64, c_vp, u32, c_vp, c_vp]),
+        "cbs_cmux_batch_device": (st, [c_vp, c_vp, c_vp, c_vp, u64, u32, c_vp, c_vp]),
         "cbs_extract_keyswitch_device": (st, [c_vp, c_vp, u32, c_vp, u32, c_vp, c_vp, u32, c_vp]),
         "cbs_aes128_setup": (st, [c_vp, c_vp, u64]),
         "cbs_aes128_setup_device": (st, [c_vp, c_vp, c_vp]),
@@ -177,6 +179,30 @@ def call(name: str, *args) -> None:
 def default_params() -> CbsParams:
     p = CbsParams()
     call("cbs_params_default", ctypes.byref(p))
+    return p
+
+
+def log2_pfail_gaussian(sigma: float, margin: float) -> float:
+    """log2 P(|X| >= margin) for X ~ N(0, sigma^2), i.e. log2 erfc(margin / (sqrt(2) sigma));
+    past erfc's underflow, the leading term of its asymptotic expansion."""
+    import math
+    if sigma <= 0:
+        return float("-inf")
+    z = margin / sigma
+    if z < 37:
+        return math.log2(math.erfc(z / math.sqrt(2)))
+    return -(z * z / 2) / math.log(2) - math.log2(z * math.sqrt(math.pi / 2))
+
+
+PARAMS_AES_3X12, PARAMS_AES_2X18 = 0, 1
+PRESETS = {"3x12": PARAMS_AES_3X12, "2x18": PARAMS_AES_2X18}
+
+
+def preset_params(name: str) -> CbsParams:
+    """A named parameter set: "3x12" (cbs_params_default) or "2x18" (blind-rotation gadget
+    2^18 x 2)."""
+    p = CbsParams()
+    call("cbs_params_preset", PRESETS[name], ctypes.byref(p))
     return p
 
 

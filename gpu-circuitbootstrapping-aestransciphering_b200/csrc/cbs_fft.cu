@@ -24,6 +24,31 @@
 
 namespace cbs {
 
+// The biased digit fields (digit + 2^(gbits-1)) of one folded pair (a_e, a_(e+M)): packed in
+// one 32-bit word for digits of up to 15 bits (re in the low half-word), two words for wider
+// digits (the 2 x 18-bit gadget).
+template <bool WIDE>
+struct DigitPair {
+    using T = uint32_t;
+    __device__ static __forceinline__ T pack(uint32_t re, uint32_t im) { return re | (im << 16); }
+    __device__ static __forceinline__ double2 unpack(T v, int32_t bias) {
+        return make_double2(static_cast<double>(static_cast<int32_t>(v & 0xffffu) - bias),
+                            static_cast<double>(static_cast<int32_t>(v >> 16) - bias));
+    }
+};
+template <>
+struct DigitPair<true> {
+    using T = uint2;
+    __device__ static __forceinline__ T pack(uint32_t re, uint32_t im) { return make_uint2(re, im); }
+    __device__ static __forceinline__ double2 unpack(T v, int32_t bias) {
+        return make_double2(static_cast<double>(static_cast<int32_t>(v.x) - bias),
+                            static_cast<double>(static_cast<int32_t>(v.y) - bias));
+    }
+};
+
+// gadget digits wider than the packed 16-bit fields take the two-word form
+__host__ __device__ constexpr bool wide_digits(int gbits) { return gbits > 15; }
+
 template <int LOGN>
 struct BrFftCfg {
     static constexpr uint32_t T = (1u << LOGN) / 8;
@@ -40,17 +65,18 @@ struct BrFftCfg {
 //     holds the full spectrum of output h and inverse-transforms it into registers;
 //  4. output h is staged in this half's FFT buffer and each thread updates the accumulator
 //     positions it owns: acc_h[i] += t_h[i - a] (negacyclic wrap) - t_h[i].
-template <int LOGN>
+template <int LOGN, bool WIDE>
 __global__ void __launch_bounds__(BrFftCfg<LOGN>::T, BrFftCfg<LOGN>::MIN_BLOCKS)
     k_blind_rotate_fft(const BlindRotateArgs a, const FftKeyArgs f) {
     constexpr int LOGM = LOGN - 1;
     constexpr uint32_t N = 1u << LOGN, M = N / 2, TH = M / 8, T = 2 * TH, TWO_N = 2 * N;
     using Tb = FftTab<LOGM>;
+    using DigT = typename DigitPair<WIDE>::T;
     extern __shared__ __align__(16) uint64_t smem[];
     uint64_t* acc = smem;                                           // [2][N]
     double2* fs = reinterpret_cast<double2*>(smem + 2 * N);         // [2][M]
     double2* tab = fs + 2 * M;                                      // FftTab<LOGM>
-    uint32_t* dig = reinterpret_cast<uint32_t*>(tab + Tb::size());  // [2][digits][M] packed pairs
+    DigT* dig = reinterpret_cast<DigT*>(tab + Tb::size());          // [2][digits][M] digit pairs
     const double2* tws = tab + Tb::twist_off();
     const uint32_t ct = blockIdx.x, tid = threadIdx.x;
     const uint32_t h = tid / TH, ht = tid % TH;
@@ -105,11 +131,11 @@ __global__ void __launch_bounds__(BrFftCfg<LOGN>::T, BrFftCfg<LOGN>::MIN_BLOCKS)
         for (uint32_t e = ht; e < M; e += TH) {
             const uint64_t wr = static_cast<uint64_t>(my_acc[e]) >> ign;
             const uint64_t wi = static_cast<uint64_t>(my_acc[e + M]) >> ign;
-            uint32_t* dst = dig + h * digits * M + e;
-            // biased digit fields (digit + 2^(gbits-1)), re in the low half-word
+            DigT* dst = dig + h * digits * M + e;
+            // biased digit fields (digit + 2^(gbits-1))
             for (uint32_t d = 0; d < digits; ++d)
-                dst[d * M] = (static_cast<uint32_t>(wr >> (gbits * d)) & fmask) |
-                             ((static_cast<uint32_t>(wi >> (gbits * d)) & fmask) << 16);
+                dst[d * M] = DigitPair<WIDE>::pack(static_cast<uint32_t>(wr >> (gbits * d)) & fmask,
+                                                   static_cast<uint32_t>(wi >> (gbits * d)) & fmask);
         }
         half_bar();
         // 2. forward transforms and products
@@ -118,15 +144,12 @@ __global__ void __launch_bounds__(BrFftCfg<LOGN>::T, BrFftCfg<LOGN>::MIN_BLOCKS)
 #pragma unroll
         for (int j = 0; j < 8; ++j) y0[j] = y1[j] = make_double2(0.0, 0.0);
         for (uint32_t d = 0; d < digits; ++d) {
-            const uint32_t* dsrc = dig + (h * digits + d) * M;
+            const DigT* dsrc = dig + (h * digits + d) * M;
             double2 x[8];
             fft_forward_to_regs<LOGM>(
                 my_fs, ht, tab,
                 [&](int j, uint32_t e) {
-                    const uint32_t v = dsrc[e];
-                    const double re = static_cast<double>(static_cast<int32_t>(v & 0xffffu) - dbias);
-                    const double im = static_cast<double>(static_cast<int32_t>(v >> 16) - dbias);
-                    return cmul(make_double2(re, im), twist_at<LOGM>(tws, j, e));
+                    return cmul(DigitPair<WIDE>::unpack(dsrc[e], dbias), twist_at<LOGM>(tws, j, e));
                 },
                 x, half_bar);
             const double2* k0 = ek + static_cast<size_t>(2 * d + h) * 2 * M;  // key row 2d + h, slot-major
@@ -245,18 +268,19 @@ struct BrFftMbCfg {
     static constexpr int MIN_BLOCKS = 1;
 };
 
-template <int LOGN, int MB>
+template <int LOGN, int MB, bool WIDE>
 __global__ void __launch_bounds__(BrFftCfg<LOGN>::T, BrFftMbCfg<LOGN, MB>::MIN_BLOCKS)
     k_blind_rotate_fft_mb(const BlindRotateArgs a, const FftKeyArgs f) {
     constexpr int LOGM = LOGN - 1;
     constexpr uint32_t N = 1u << LOGN, M = N / 2, TH = M / 8, T = 2 * TH, TWO_N = 2 * N;
     constexpr uint32_t KS = (1u << MB) - 1u;
     using Tb = FftTab<LOGM>;
+    using DigT = typename DigitPair<WIDE>::T;
     extern __shared__ __align__(16) uint64_t smem[];
     uint64_t* acc = smem;                                           // [2][N]
     double2* fs = reinterpret_cast<double2*>(smem + 2 * N);         // [2][M]
     double2* tab = fs + 2 * M;                                      // FftTab<LOGM>
-    uint32_t* dig = reinterpret_cast<uint32_t*>(tab + Tb::size());  // [2][digits][M] packed pairs
+    DigT* dig = reinterpret_cast<DigT*>(tab + Tb::size());          // [2][digits][M] digit pairs
     double2* cbuf = reinterpret_cast<double2*>(dig + 2 * a.digits * M);  // [MB][8][T] c_i per slot
     const double2* tws = tab + Tb::twist_off();
     const uint32_t ct = blockIdx.x, tid = threadIdx.x;
@@ -323,10 +347,10 @@ __global__ void __launch_bounds__(BrFftCfg<LOGN>::T, BrFftMbCfg<LOGN, MB>::MIN_B
         for (uint32_t e = ht; e < M; e += TH) {
             const uint64_t wr = static_cast<uint64_t>(my_acc[e]) >> ign;
             const uint64_t wi = static_cast<uint64_t>(my_acc[e + M]) >> ign;
-            uint32_t* dst = dig + h * digits * M + e;
+            DigT* dst = dig + h * digits * M + e;
             for (uint32_t d = 0; d < digits; ++d)
-                dst[d * M] = (static_cast<uint32_t>(wr >> (gbits * d)) & fmask) |
-                             ((static_cast<uint32_t>(wi >> (gbits * d)) & fmask) << 16);
+                dst[d * M] = DigitPair<WIDE>::pack(static_cast<uint32_t>(wr >> (gbits * d)) & fmask,
+                                                   static_cast<uint32_t>(wi >> (gbits * d)) & fmask);
         }
         half_bar();
         // 2. forward transforms; per slot the combined key of row 2d + h, both columns
@@ -335,15 +359,12 @@ __global__ void __launch_bounds__(BrFftCfg<LOGN>::T, BrFftMbCfg<LOGN, MB>::MIN_B
 #pragma unroll
         for (int j = 0; j < 8; ++j) y0[j] = y1[j] = make_double2(0.0, 0.0);
         for (uint32_t d = 0; d < digits; ++d) {
-            const uint32_t* dsrc = dig + (h * digits + d) * M;
+            const DigT* dsrc = dig + (h * digits + d) * M;
             double2 x[8];
             fft_forward_to_regs<LOGM>(
                 my_fs, ht, tab,
                 [&](int j, uint32_t e) {
-                    const uint32_t v = dsrc[e];
-                    const double re = static_cast<double>(static_cast<int32_t>(v & 0xffffu) - dbias);
-                    const double im = static_cast<double>(static_cast<int32_t>(v >> 16) - dbias);
-                    return cmul(make_double2(re, im), twist_at<LOGM>(tws, j, e));
+                    return cmul(DigitPair<WIDE>::unpack(dsrc[e], dbias), twist_at<LOGM>(tws, j, e));
                 },
                 x, half_bar);
             // combined keys of row 2d + h, both columns, all 8 slots: subset by subset, the 16
@@ -438,28 +459,35 @@ __global__ void __launch_bounds__(BrFftCfg<LOGN>::T, BrFftMbCfg<LOGN, MB>::MIN_B
 cudaError_t ntt_forward(uint64_t* out, const uint64_t* in, const uint64_t* tw, const uint64_t* tws,
                         const cbs_dmodulus* mod, size_t dim, size_t batch, cudaStream_t s);
 
-template <int LOGN>
+template <int LOGN, bool WIDE>
 static cudaError_t br_fft_launch(const BlindRotateArgs& a, const FftKeyArgs& f, uint32_t batch, cudaStream_t s) {
     constexpr uint32_t N = 1u << LOGN, M = N / 2;
     const size_t smem = 2ull * N * sizeof(uint64_t) + (2ull * M + FftTab<LOGN - 1>::size()) * sizeof(double2) +
-                        2ull * a.digits * M * sizeof(uint32_t);
+                        2ull * a.digits * M * sizeof(typename DigitPair<WIDE>::T);
     if (f.tab_len != FftTab<LOGN - 1>::size()) return cudaErrorInvalidValue;
     static size_t configured[64] = {};  // per device
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
     if (configured[dev] < smem) {
-        cudaError_t e = cudaFuncSetAttribute(k_blind_rotate_fft<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             static_cast<int>(smem));
+        cudaError_t e = cudaFuncSetAttribute(k_blind_rotate_fft<LOGN, WIDE>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
         if (e != cudaSuccess) return e;
         configured[dev] = smem;
     }
-    k_blind_rotate_fft<LOGN><<<batch, BrFftCfg<LOGN>::T, smem, s>>>(a, f);
+    k_blind_rotate_fft<LOGN, WIDE><<<batch, BrFftCfg<LOGN>::T, smem, s>>>(a, f);
     return cudaGetLastError();
+}
+
+template <int LOGN>
+static cudaError_t br_fft_launch(const BlindRotateArgs& a, const FftKeyArgs& f, uint32_t batch, cudaStream_t s) {
+    return wide_digits(a.g.gbits) ? br_fft_launch<LOGN, true>(a, f, batch, s)
+                                  : br_fft_launch<LOGN, false>(a, f, batch, s);
 }
 
 cudaError_t launch_blind_rotate_fft(const BlindRotateArgs& a, const FftKeyArgs& f, const cbs_dmodulus* d_mod,
                                     uint32_t N, uint32_t batch, cudaStream_t s, bool mv_ntt) {
     if (batch == 0) return cudaSuccess;
+    if (a.g.gbits < 1 || a.g.gbits > 24 || a.digits < 1 || a.digits > 4) return cudaErrorInvalidValue;
     cudaError_t e;
     switch (N) {
         case 1024: e = br_fft_launch<10>(a, f, batch, s); break;
@@ -471,29 +499,37 @@ cudaError_t launch_blind_rotate_fft(const BlindRotateArgs& a, const FftKeyArgs& 
     return ntt_forward(a.mv_out, a.mv_out, a.t.rp, a.t.rps, d_mod, N, static_cast<size_t>(batch) * a.num_lut * 2, s);
 }
 
-template <int LOGN, int MB>
+template <int LOGN, int MB, bool WIDE>
 static cudaError_t br_fft_mb_launch(const BlindRotateArgs& a, const FftKeyArgs& f, uint32_t batch, cudaStream_t s) {
     constexpr uint32_t N = 1u << LOGN, M = N / 2;
     const size_t smem = 2ull * N * sizeof(uint64_t) + (2ull * M + FftTab<LOGN - 1>::size()) * sizeof(double2) +
-                        2ull * a.digits * M * sizeof(uint32_t) + MB * 8ull * BrFftCfg<LOGN>::T * sizeof(double2);
+                        2ull * a.digits * M * sizeof(typename DigitPair<WIDE>::T) +
+                        MB * 8ull * BrFftCfg<LOGN>::T * sizeof(double2);
     if (f.tab_len != FftTab<LOGN - 1>::size()) return cudaErrorInvalidValue;
     static size_t configured[64] = {};
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
     if (configured[dev] < smem) {
-        cudaError_t e = cudaFuncSetAttribute(k_blind_rotate_fft_mb<LOGN, MB>,
+        cudaError_t e = cudaFuncSetAttribute(k_blind_rotate_fft_mb<LOGN, MB, WIDE>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
         if (e != cudaSuccess) return e;
         configured[dev] = smem;
     }
-    k_blind_rotate_fft_mb<LOGN, MB><<<batch, BrFftCfg<LOGN>::T, smem, s>>>(a, f);
+    k_blind_rotate_fft_mb<LOGN, MB, WIDE><<<batch, BrFftCfg<LOGN>::T, smem, s>>>(a, f);
     return cudaGetLastError();
+}
+
+template <int LOGN, int MB>
+static cudaError_t br_fft_mb_launch(const BlindRotateArgs& a, const FftKeyArgs& f, uint32_t batch, cudaStream_t s) {
+    return wide_digits(a.g.gbits) ? br_fft_mb_launch<LOGN, MB, true>(a, f, batch, s)
+                                  : br_fft_mb_launch<LOGN, MB, false>(a, f, batch, s);
 }
 
 cudaError_t launch_blind_rotate_fft_mb(const BlindRotateArgs& a, const FftKeyArgs& f, const cbs_dmodulus* d_mod,
                                        uint32_t N, uint32_t batch, uint32_t mb, cudaStream_t s, bool mv_ntt) {
     if (batch == 0) return cudaSuccess;
     if (mb != 2 && mb != 3) return cudaErrorInvalidValue;  // N = 4096: the per-slot c_i exceed shared memory
+    if (a.g.gbits < 1 || a.g.gbits > 24 || a.digits < 1 || a.digits > 4) return cudaErrorInvalidValue;
     cudaError_t e;
     switch (N) {
         case 1024:

@@ -392,6 +392,26 @@ __global__ void __launch_bounds__(LutFftCfg<LOGN>::T) k_spectra_to_coef(double2*
     (void)N;
 }
 
+// Coefficient-domain polynomials mod Q -> spectra (the row-spectrum form the FFT CMux reads):
+// CTA k forward-transforms the centred polynomial coef[k] and stores its spectrum slot-major at
+// out[k].  Out of place (the transform reads every coefficient of its polynomial).
+template <int LOGN>
+__global__ void __launch_bounds__(LutFftCfg<LOGN>::T) k_coef_to_spectra(const uint64_t* coef, double2* out,
+                                                                          uint64_t Q, const FftKeyArgs f) {
+    constexpr int LOGM = LOGN - 1;
+    constexpr uint32_t N = 1u << LOGN, M = N / 2, T = M / 8;
+    using Tb = FftTab<LOGM>;
+    extern __shared__ __align__(16) uint64_t smem[];
+    double2* fs = reinterpret_cast<double2*>(smem);
+    double2* tab = fs + M;
+    const uint32_t tid = threadIdx.x;
+    for (uint32_t k = tid; k < Tb::size(); k += T) tab[k] = f.tab[k];
+    __syncthreads();
+    double2 x[8];
+    fft_of_poly<LOGM>(fs, tid, tab, coef + static_cast<size_t>(blockIdx.x) * N, Q, x, []() { __syncthreads(); });
+    store_spectrum<T>(out + static_cast<size_t>(blockIdx.x) * M, tid, x);
+}
+
 template <class K>
 static cudaError_t opt_in_smem(K kernel, size_t bytes, size_t (&configured)[64]) {
     int dev = 0;
@@ -473,6 +493,31 @@ cudaError_t launch_spectra_to_coef(double2* buf, uint64_t Q, const FftKeyArgs& f
         case 1024: return spectra_launch<10>(buf, Q, f, polys, s);
         case 2048: return spectra_launch<11>(buf, Q, f, polys, s);
         case 4096: return spectra_launch<12>(buf, Q, f, polys, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+template <int LOGN>
+static cudaError_t coef_spectra_launch(const uint64_t* coef, double2* out, uint64_t Q, const FftKeyArgs& f,
+                                       size_t polys, cudaStream_t s) {
+    constexpr uint32_t M = 1u << (LOGN - 1);
+    if (f.tab_len != FftTab<LOGN - 1>::size()) return cudaErrorInvalidValue;
+    const size_t smem = (M + FftTab<LOGN - 1>::size()) * sizeof(double2);
+    static size_t configured[64] = {};
+    cudaError_t e = opt_in_smem(k_coef_to_spectra<LOGN>, smem, configured);
+    if (e != cudaSuccess) return e;
+    k_coef_to_spectra<LOGN><<<static_cast<unsigned>(polys), LutFftCfg<LOGN>::T, smem, s>>>(coef, out, Q, f);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_coef_to_spectra(const uint64_t* coef, double2* out, uint64_t Q, const FftKeyArgs& f, uint32_t N,
+                                   size_t polys, cudaStream_t s) {
+    if (polys == 0) return cudaSuccess;
+    if (polys > 0x7fffffffull) return cudaErrorInvalidValue;
+    switch (N) {
+        case 1024: return coef_spectra_launch<10>(coef, out, Q, f, polys, s);
+        case 2048: return coef_spectra_launch<11>(coef, out, Q, f, polys, s);
+        case 4096: return coef_spectra_launch<12>(coef, out, Q, f, polys, s);
         default: return cudaErrorInvalidValue;
     }
 }

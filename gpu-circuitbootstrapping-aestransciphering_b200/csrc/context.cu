@@ -378,6 +378,17 @@ cbs_status cbs_params_default(cbs_params* out) {
     return CBS_OK;
 }
 
+cbs_status cbs_params_preset(int which, cbs_params* out) {
+    CBS_CHECK_ARG(out, "params_preset: null output");
+    CBS_CHECK_ARG(which == CBS_PARAMS_AES_3X12 || which == CBS_PARAMS_AES_2X18, "params_preset: unknown preset");
+    if (cbs_status st = cbs_params_default(out)) return st;
+    if (which == CBS_PARAMS_AES_2X18) {
+        out->base_g = 1u << 18;
+        out->digits_g = 2;
+    }
+    return CBS_OK;
+}
+
 cbs_status cbs_context_create(const cbs_params* params, uint32_t max_batch, cbs_context** out) {
     CBS_CHECK_ARG(params && out, "context_create: null argument");
     CBS_CHECK_ARG(max_batch >= 1 && max_batch <= (1u << 22), "context_create: max_batch out of range");
@@ -607,8 +618,8 @@ cbs_status cbs_export_mb_bsk(const cbs_context* ctx, uint64_t* out, size_t* word
 cbs_status cbs_context_set_br_backend(cbs_context* ctx, int backend) {
     CBS_CHECK_ARG(ctx, "set_br_backend: null context");
     CBS_CHECK_ARG(backend == CBS_BR_NTT || backend == CBS_BR_FFT64, "set_br_backend: unknown backend");
-    if (backend == CBS_BR_FFT64 && (ctx->p.digits_g > 4 || ctx->p.base_g > (1u << 15))) {
-        set_error("set_br_backend: the FFT64 backend supports at most 4 gadget digits of at most 15 bits");
+    if (backend == CBS_BR_FFT64 && (ctx->p.digits_g > 4 || ctx->p.base_g > (1u << 24))) {
+        set_error("set_br_backend: the FFT64 backend supports at most 4 gadget digits of at most 24 bits");
         return CBS_ERR_UNSUPPORTED;
     }
     if (backend == CBS_BR_FFT64 && ctx->keys_ready) {
@@ -802,6 +813,81 @@ cbs_status cbs_lut8x32_batch_device(cbs_context* ctx, const uint64_t* d_tables, 
                                  cudaMemcpyHostToDevice, s));
     return run_lut_levels(ctx, d_tables, 256ull * 2 * N, ctx->d_lut_sel_scratch.p, d_rgsw_all, rgsw_stride,
                           ctx->d_ctrl_scratch.p, luts, ctx->d_lut_a.p, ctx->d_lut_b.p, d_out, s);
+}
+
+cbs_status cbs_cmux_batch_device(cbs_context* ctx, const uint64_t* d_ct0, const uint64_t* d_ct1,
+                                 const uint64_t* d_rgsw, uint64_t rgsw_stride, uint32_t count, uint64_t* d_out,
+                                 cbs_stream_t stream) {
+    CBS_CHECK_ARG(ctx, "cmux: null context");
+    if (count == 0) return CBS_OK;
+    CBS_CHECK_ARG(d_ct0 && d_ct1 && d_rgsw && d_out, "cmux: null pointer");
+    CBS_CHECK_ARG(count <= 65535, "cmux: at most 65535 CMuxes per call");
+    const size_t N = ctx->p.N, L = ctx->p.num_lut, M = N / 2;
+    CBS_CHECK_ARG(rgsw_stride == 0 || rgsw_stride >= L * 4 * N, "cmux: rgsw_stride below num_lut * 4 * N");
+    const uint32_t n_rgsw = rgsw_stride == 0 ? 1u : count;  // stride 0: one control for every item
+    if (ctx->br_backend == CBS_BR_FFT64 && !ctx->fft_ready) {
+        set_error("cmux: FFT backend selected but its key material is not prepared");
+        return CBS_ERR_NOT_READY;
+    }
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    // pairs [count][ct0, ct1][2][N] (the level-input layout of the LUT kernels), control u = bit u
+    CBS_CUDA_TRY(ctx->d_lut_a.alloc(static_cast<size_t>(count) * 6 * N));
+    uint64_t* pairs = ctx->d_lut_a.p;
+    uint64_t* out_coef = pairs + static_cast<size_t>(count) * 4 * N;
+    CBS_CUDA_TRY(cudaMemcpy2DAsync(pairs, 4 * N * 8, d_ct0, 2 * N * 8, 2 * N * 8, count, cudaMemcpyDeviceToDevice, s));
+    CBS_CUDA_TRY(cudaMemcpy2DAsync(pairs + 2 * N, 4 * N * 8, d_ct1, 2 * N * 8, 2 * N * 8, count,
+                                   cudaMemcpyDeviceToDevice, s));
+    std::vector<uint32_t> ctrl(static_cast<size_t>(count) * 8, 0);
+    for (uint32_t u = 0; u < count; ++u) ctrl[static_cast<size_t>(u) * 8] = u;
+    CBS_CUDA_TRY(ctx->d_ctrl_scratch.upload(ctrl.data(), ctrl.size(), s));
+    if (ctx->br_backend != CBS_BR_FFT64) {
+        CmuxLevelArgs a{};
+        a.t = ctx->ring();
+        a.in_count = 2;
+        a.in = pairs;
+        a.in_lut_stride = 4 * N;
+        a.lut_sel = nullptr;
+        a.out = d_out;
+        a.rgsw_all = d_rgsw;
+        a.rgsw_stride = rgsw_stride;
+        a.ctrl_bits = ctx->d_ctrl_scratch.p;
+        a.level = 0;
+        a.g = ctx->g_cc;
+        a.digits = ctx->p.num_lut;
+        CBS_CUDA_TRY(launch_cmux_level(a, ctx->p.N, count, s));
+        return CBS_OK;
+    }
+    // FFT backend: inputs to the coefficient domain, control rows to spectra, the FFT CMux,
+    // the output back to the NTT domain
+    const size_t rows = static_cast<size_t>(n_rgsw) * L * 4;
+    CBS_CUDA_TRY(ctx->d_lut_b.alloc(2 * rows * N));
+    uint64_t* rgsw_coef = ctx->d_lut_b.p;
+    double2* rgsw_spec = reinterpret_cast<double2*>(ctx->d_lut_b.p + rows * N);
+    CBS_CUDA_TRY(ntt_inverse(pairs, pairs, nullptr, ctx->d_irp.p, ctx->d_irps.p, ctx->d_mod.p, ctx->d_ninv.p,
+                             ctx->d_ninv_s.p, N, static_cast<size_t>(count) * 4, s));
+    CBS_CUDA_TRY(cudaMemcpy2DAsync(rgsw_coef, L * 4 * N * 8, d_rgsw, (rgsw_stride ? rgsw_stride : L * 4 * N) * 8,
+                                   L * 4 * N * 8, n_rgsw, cudaMemcpyDeviceToDevice, s));
+    CBS_CUDA_TRY(ntt_inverse(rgsw_coef, rgsw_coef, nullptr, ctx->d_irp.p, ctx->d_irps.p, ctx->d_mod.p, ctx->d_ninv.p,
+                             ctx->d_ninv_s.p, N, rows, s));
+    const FftKeyArgs f = fft_key_args(ctx);
+    CBS_CUDA_TRY(launch_coef_to_spectra(rgsw_coef, rgsw_spec, ctx->p.Q, f, ctx->p.N, rows, s));
+    CmuxFftArgs a{};
+    a.in = pairs;
+    a.in_lut_stride = 4 * N;
+    a.lut_sel = nullptr;
+    a.out = out_coef;
+    a.in_count = 2;
+    a.rgswf = rgsw_spec;
+    a.rgsw_stride = rgsw_stride ? L * 4 * M : 0;
+    a.ctrl_bits = ctx->d_ctrl_scratch.p;
+    a.level = 0;
+    a.g = make_digit_prep(ctx->p.Q, ctx->g_cc, ctx->p.num_lut);
+    a.digits = ctx->p.num_lut;
+    a.in_spec = nullptr;
+    CBS_CUDA_TRY(launch_cmux_level_fft(a, f, ctx->p.N, count, s));
+    CBS_CUDA_TRY(ntt_forward(d_out, out_coef, ctx->d_rp.p, ctx->d_rps.p, ctx->d_mod.p, N,
+                             static_cast<size_t>(count) * 2, s));
+    return CBS_OK;
 }
 
 cbs_status cbs_extract_keyswitch_device(cbs_context* ctx, const uint64_t* d_words_coef, uint32_t words,

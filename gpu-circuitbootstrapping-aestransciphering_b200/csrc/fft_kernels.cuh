@@ -79,6 +79,9 @@ cudaError_t launch_cmux_level_fft(const CmuxFftArgs& a, const FftKeyArgs& f, uin
 // spectra [polys][N/2] (slot-major) -> coefficient-domain polynomials [polys][N] mod Q, in place
 cudaError_t launch_spectra_to_coef(double2* buf, uint64_t Q, const FftKeyArgs& f, uint32_t N, size_t polys,
                                    cudaStream_t s);
+// coefficient-domain polynomials [polys][N] mod Q -> spectra [polys][N/2] (slot-major), out of place
+cudaError_t launch_coef_to_spectra(const uint64_t* coef, double2* out, uint64_t Q, const FftKeyArgs& f, uint32_t N,
+                                   size_t polys, cudaStream_t s);
 DigitPrep make_digit_prep(uint64_t q, const Gadget& g, uint32_t digits);
 // the FftTab<log2(N/2)> table (fft_core.cuh) computed in long double
 void fft_tables_host(uint32_t N, std::vector<double2>& tab);

@@ -120,6 +120,15 @@ typedef struct cbs_context cbs_context;
  * BR gadget 2^12 x 3, RGSW out 2^6 x 4 (4 LUT levels), HomTrace 2^9 x 5, SchemeSwitch 2^9 x 5,
  * extraction KS qKS=2^14, base 2^7 (two digits). */
 cbs_status cbs_params_default(cbs_params *out);
+/* Named parameter sets.  CBS_PARAMS_AES_3X12 is cbs_params_default.  CBS_PARAMS_AES_2X18 is
+ * the same set with the blind-rotation gadget 2^18 x 2 (18 low bits of Q still dropped): two
+ * thirds of the external-product work and key bytes per blind-rotation step, for a larger
+ * but still negligible decryption-failure probability (the noise budget of every other stage
+ * is unchanged; the blind-rotation error reaches the RGSW rows only through the one
+ * coefficient the trace keeps).  No reference counterpart: the reference's own sets live in
+ * its absent OpenFHE fork (examples/aes_transcipher/main.cu:188-222). */
+enum { CBS_PARAMS_AES_3X12 = 0, CBS_PARAMS_AES_2X18 = 1 };
+cbs_status cbs_params_preset(int which, cbs_params *out);
 
 /* replaces GPUCirBTSContext(const CirBTSContext&, uint32_t maxBatchSize) (cirbts.cuh:420)
  * plus gpu_init_ntt (cirbts-init.cu:867-1302): tables on the current device, scratch for
@@ -223,6 +232,18 @@ cbs_status cbs_lut8x32_batch_device(cbs_context *ctx, const uint64_t *d_tables, 
                                     const uint32_t *h_table_of_lut, const uint64_t *d_rgsw_all, uint32_t num_bits,
                                     uint64_t rgsw_stride, const uint32_t *h_ctrl_bits, uint32_t luts, uint64_t *d_out,
                                     cbs_stream_t stream);
+
+/* One CMux per item (replaces one tree level of the reference's LUT, kernel_LUT_CMUX_Delta +
+ * kernel_LUT_CMUX_ExternalProduct, examples/aes_transcipher/gpu_lut.cuh:521-595):
+ * d_out[u] = d_ct0[u] + RGSW_u (x) (d_ct1[u] - d_ct0[u]) for u < count, RGSW_u the CBS output
+ * rows of bit u at d_rgsw + u * rgsw_stride ([num_lut][2][2][N]; rgsw_stride = 0: one control for
+ * every item, as at one level of a LUT tree); ciphertexts [count][2][N],
+ * all NTT domain.  The context's backend picks the arithmetic: exact NTT products (CBS_BR_NTT)
+ * or the FP64 FFT CMux of the AES path (CBS_BR_FFT64; inputs converted to the coefficient
+ * domain and the rows to spectra inside the call, output back to the NTT domain). */
+cbs_status cbs_cmux_batch_device(cbs_context *ctx, const uint64_t *d_ct0, const uint64_t *d_ct1,
+                                 const uint64_t *d_rgsw, uint64_t rgsw_stride, uint32_t count, uint64_t *d_out,
+                                 cbs_stream_t stream);
 
 /* Sample extract + LWE key switch N->n + modulus switch qKS->q (replaces
  * ExtractStateBytesToLWEDeviceBatch, examples/aes_transcipher/extract.cuh:283-366, and

@@ -33,7 +33,7 @@ def _dev(a):
 
 @pytest.fixture(scope="module")
 def fctx(pkg):
-    c = pkg.Context(max_batch=64)
+    c = pkg.Context(max_batch=2048)  # 16 AES blocks in one chunk
     c.keygen(23)
     pkg.call("cbs_context_set_br_backend", c.handle, pkg.BR_FFT64)
     yield c
@@ -215,6 +215,42 @@ def test_fft_aes128_end_to_end(pkg, fctx, fkeys):
         out = bytes(int(sum(int(got_bits[blk * 128 + i * 8 + b]) << b for b in range(8))) for i in range(16))
         assert out == enc.update(ctrs[blk])
     assert max(err) < p.q_lwe // 8
+
+
+def test_fft_aes128_16_blocks_grouped(pkg, fctx, fkeys):
+    """Config 4 at 16 blocks on the headline configuration (FFT backend, grouped mb = 2 blind
+    rotation, graphs replayed): a key of 16 seeded random bytes, 16 seeded random counters,
+    every keystream block equal to OpenSSL AES-128 and every bit's decryption error reported."""
+    from cryptography.hazmat.primitives.ciphers import Cipher, algorithms, modes
+    p = fctx.params
+    rng = np.random.default_rng(1616)
+    key = rng.bytes(16)
+    blocks = 16
+    pkg.call("cbs_context_set_br_multibit", fctx.handle, 2)
+    try:
+        pkg.call("cbs_aes128_setup_device", fctx.handle, key, rng.bytes(32))
+        ctrs = [rng.bytes(16) for _ in range(blocks)]
+        bits = np.array([[(c[t // 8] >> (t % 8)) & 1 for t in range(128)] for c in ctrs], np.uint8).reshape(-1)
+        dbits = torch.from_numpy(bits).cuda()
+        oa = torch.zeros((blocks * 128, p.n), dtype=torch.int64, device="cuda")
+        ob = torch.zeros(blocks * 128, dtype=torch.int64, device="cuda")
+        enc = Cipher(algorithms.AES(key), modes.ECB()).encryptor()
+        want = [enc.update(c) for c in ctrs]
+        for rep in range(2):  # capture, then replay the round graphs
+            oa.zero_()
+            ob.zero_()
+            pkg.call("cbs_aes128_ctr_transcipher_device", fctx.handle, dbits.data_ptr(), blocks, oa.data_ptr(),
+                     ob.data_ptr(), 1, None)
+            torch.cuda.synchronize()
+            got_bits, err = lwe_decrypt_bits(fkeys["s_lwe"], oa.cpu().numpy().view(np.uint64),
+                                             ob.cpu().numpy().view(np.uint64), p.q_lwe)
+            for blk in range(blocks):
+                out = bytes(int(sum(int(got_bits[blk * 128 + i * 8 + b]) << b for b in range(8))) for i in range(16))
+                assert out == want[blk], f"block {blk} rep {rep}"
+            print(f"AES 16 blocks (mb = 2): max |error| {max(err)} of margin {p.q_lwe // 4}")
+            assert max(err) < p.q_lwe // 8
+    finally:
+        pkg.call("cbs_context_set_br_multibit", fctx.handle, 1)
 
 
 def test_backend_switch_validates(pkg, fctx):

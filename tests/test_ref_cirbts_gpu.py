@@ -85,8 +85,10 @@ def _orc_acc(oracle, oc, a, b, steps, mbk=None, mb=1):
     return out
 
 
-def test_blind_rotation_matches_reference_kernels(pkg, oracle, ref):
-    p = pkg.default_params()
+@pytest.mark.parametrize("preset", ["3x12", "2x18"])
+def test_blind_rotation_matches_reference_kernels(pkg, oracle, ref, preset):
+    """Both blind-rotation gadgets (2^12 x 3, the default set, and 2^18 x 2)."""
+    p = pkg.preset_params(preset)
     N, n, Q = p.N, p.n, p.Q
     keys = pkg.generate_keys_host(p, 23)
     oc = OracleCbs(oracle, p, keys)
@@ -159,7 +161,8 @@ def test_trace_schemeswitch_matches_reference_kernels(pkg, oracle, ref):
     assert np.array_equal(rows.cpu().numpy().view(np.uint64), want)
 
 
-def test_grouped_blind_rotation_matches_reference_kernels(pkg, oracle, ref):
+@pytest.mark.parametrize("preset", ["3x12", "2x18"])
+def test_grouped_blind_rotation_matches_reference_kernels(pkg, oracle, ref, preset):
     """The grouped (mb = 2, CIRBTS_PBS_MULTIBIT=2) blind rotation: the reference's
     kernel_EvalAccCore_Binary_MB2_Grouped_Batch sequence with the product's grouped keys
     (re-laid [subset][group] as the reference's RF key) reproduces the oracle's exact grouped
@@ -170,7 +173,7 @@ def test_grouped_blind_rotation_matches_reference_kernels(pkg, oracle, ref):
                                                 u64, u32, u32, u64, u32, vp]
     ref.ref_cirbts_blind_rotate_mb2.restype = ctypes.c_int
     oracle.orc_blind_rotate_mb.argtypes = [vp, vp, vp, u32, vp, vp, u32, u32, vp, ctypes.c_int]
-    p = pkg.default_params()
+    p = pkg.preset_params(preset)
     N, n, Q = p.N, p.n, p.Q
     keys = pkg.generate_keys_host(p, 31)
     mbk = np.ascontiguousarray(pkg.generate_mb_bsk_host(p, 31, 2))

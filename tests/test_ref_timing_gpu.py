@@ -92,11 +92,11 @@ def test_blind_rotation_timing_beside_reference_kernels(pkg):
     monic[N + k, k] = Q - 1
     monic[N + k, 0] = Q - 1
     d_monic = _dev(monic)
-    pkg.call("cbs_fnwt_1d_opt_batched", d_monic.data_ptr(), _dev(tabs[0]).data_ptr(), _dev(tabs[1]).data_ptr(),
-             _dev(np.array([dm.value, dm.const_ratio[0], dm.const_ratio[1]], np.uint64)).data_ptr(), N, 2 * N, None)
     dev = {nm: _dev(v) for nm, v in [("tw", tabs[0]), ("tws", tabs[1]), ("itw", tabs[2]), ("itws", tabs[3]),
                                      ("ninv", ninv),
                                      ("mod", np.array([dm.value, dm.const_ratio[0], dm.const_ratio[1]], np.uint64))]}
+    pkg.call("cbs_fnwt_1d_opt_batched", d_monic.data_ptr(), dev["tw"].data_ptr(), dev["tws"].data_ptr(),
+             dev["mod"].data_ptr(), N, 2 * N, None)
     bitwidth = max(0, (p.num_lut - 1).bit_length())
     acc = torch.from_numpy(rng.integers(0, Q, size=(BATCH, 2, N), dtype=np.uint64).view(np.int64)).cuda()
     groups = (n + 1) // 2

@@ -203,3 +203,29 @@ def test_keyswitch_phantom_core_size(env, alpha):
                         alpha)
         assert np.array_equal(ct_gpu[k], one)
     ctx.close()
+
+
+def test_keyswitch_phantom_core_batch32(env):
+    """Config 2 at its full batch: 32 ciphertexts of N = 2^16 over 24 primes of 50 bits + 2
+    special primes (beta = 12) key-switched in one call, every one bit-exact against the
+    oracle (the oracle's per-ciphertext cost, a few seconds on the host, sets the time of this
+    test)."""
+    pkg, o, torch = env
+    n, logn, size_q, alpha, count = 1 << 16, 16, 24, 2, 32
+    q, p = rns_primes(o, n, size_q, alpha)
+    rng = np.random.default_rng(3232)
+    ctx = pkg.RnsContext(n, q, p)
+    c2, ct, evk = _ks_inputs(o, rng, n, q, p, size_q, count)
+    d_c2, d_ct = dev(torch, c2), dev(torch, ct)
+    d_evk = [dev(torch, evk[b]) for b in range(evk.shape[0])]
+    ptrs = pkg.RnsContext.evk_array([t.data_ptr() for t in d_evk])
+    pkg.call("cbs_rns_keyswitch_inplace", ctx.handle, d_ct.data_ptr(), d_c2.data_ptr(), ptrs, size_q, count, None)
+    torch.cuda.synchronize()
+    ct_gpu = host(d_ct).reshape(ct.shape)
+    del d_c2, d_ct, d_evk
+    evk = np.ascontiguousarray(evk)
+    for k in range(count):
+        one = np.ascontiguousarray(ct[k]).copy()
+        o.orc_keyswitch(one, np.ascontiguousarray(c2[k]), evk, logn, q, size_q, size_q, p, alpha)
+        assert np.array_equal(ct_gpu[k], one), k
+    ctx.close()
