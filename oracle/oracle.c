@@ -1410,3 +1410,242 @@ void orc_encrypt_bits_lwe(const uint32_t key[8], const uint8_t *bits, uint32_t c
         b[t] = (uint64_t)((acc % q + (bits[t] ? q >> 1 : 0) + eq) % q);
     }
 }
+
+/* ------------------------------------------------------------------------------------------ */
+/* key generation for the CPU legs (restates the CUDA path's seeded host key generation)       */
+/* ------------------------------------------------------------------------------------------ */
+
+typedef struct {
+    uint64_t s[4];
+} orc_rng;
+
+static uint64_t rng_splitmix(uint64_t *x) {
+    uint64_t z = (*x += 0x9e3779b97f4a7c15ull);
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    return z ^ (z >> 31);
+}
+
+static void rng_seed(orc_rng *r, uint64_t seed) {
+    uint64_t x = seed;
+    for (int i = 0; i < 4; ++i) r->s[i] = rng_splitmix(&x);
+}
+
+/* xoshiro256** */
+static uint64_t rng_next(orc_rng *r) {
+    uint64_t *s = r->s;
+    const uint64_t m = s[1] * 5;
+    const uint64_t out = ((m << 7) | (m >> 57)) * 9;
+    const uint64_t t = s[1] << 17;
+    s[2] ^= s[0];
+    s[3] ^= s[1];
+    s[1] ^= s[2];
+    s[0] ^= s[3];
+    s[2] ^= t;
+    s[3] = (s[3] << 45) | (s[3] >> 19);
+    return out;
+}
+
+/* uniform below bound: rejection on the smallest covering bit mask */
+static uint64_t rng_uniform(orc_rng *r, uint64_t bound) {
+    int bits = 0;
+    while (bits < 64 && ((bound - 1) >> bits)) ++bits;
+    const uint64_t mask = bits >= 64 ? ~0ull : ((1ull << bits) - 1);
+    for (;;) {
+        const uint64_t v = rng_next(r) & mask;
+        if (v < bound) return v;
+    }
+}
+
+static int64_t rng_rounded_gaussian(orc_rng *r, double sigma) {
+    const double u1 = ((double)(rng_next(r) >> 11) + 1.0) * 0x1.0p-53;
+    const double u2 = (double)(rng_next(r) >> 11) * 0x1.0p-53;
+    const double g = sqrt(-2.0 * log(u1)) * cos(2.0 * M_PI * u2);
+    return (int64_t)llround(g * sigma);
+}
+
+static uint64_t mod_signed(int64_t v, uint64_t q) {
+    const int64_t m = v % (int64_t)q;
+    return m < 0 ? (uint64_t)(m + (int64_t)q) : (uint64_t)m;
+}
+
+/* gadget g_j = 2^(ign + j gbits), ign = log2 Q - digits gbits (kernel.cu:37-68) */
+static void gadget_powers(uint64_t Q, uint32_t base, uint32_t digits, uint64_t *g) {
+    const int gb = __builtin_ctz(base);
+    const int logq = 64 - __builtin_clzll(Q);
+    int ign = logq - (int)digits * gb;
+    if (ign < 0) ign = 0;
+    for (uint32_t j = 0; j < digits; ++j) g[j] = (1ull << (ign + (int)j * gb)) % Q;
+}
+
+/* a uniform (NTT domain), b = a s + NTT(e) */
+static void keygen_rlwe_zero(orc_rng *r, uint32_t N, uint64_t Q, double sigma, const uint64_t *rp,
+                             const uint64_t *s_ntt, uint64_t *a, uint64_t *b, uint64_t *tmp) {
+    for (uint32_t i = 0; i < N; ++i) a[i] = rng_uniform(r, Q);
+    for (uint32_t i = 0; i < N; ++i) tmp[i] = mod_signed(rng_rounded_gaussian(r, sigma), Q);
+    ntt_fwd_one(tmp, N, Q, rp);
+    for (uint32_t i = 0; i < N; ++i) b[i] = addmod(orc_mulmod(a[i], s_ntt[i], Q), tmp[i], Q);
+}
+
+int orc_cbs_keygen(const orc_cbs_params *p, double sigma_lwe, double sigma_rlwe, uint32_t qks, uint32_t base_ks,
+                   uint64_t seed, int32_t *s_lwe_out, int32_t *s_rlwe_out, uint64_t *bsk_out, uint64_t *ht_out,
+                   uint64_t *ss_out, uint16_t *ksk_out, uint64_t *tv_out, uint64_t *gpow_out, uint32_t *maps_out) {
+    const uint32_t N = p->N, n = p->n, log_n = p->log_n, l2 = 2 * p->digits_g, rounds = p->trace_rounds;
+    const uint64_t Q = p->Q;
+    uint64_t *rp = (uint64_t *)malloc(sizeof(uint64_t) * N), *irp = (uint64_t *)malloc(sizeof(uint64_t) * N);
+    uint64_t ninv[2];
+    if (orc_ntt_tables(log_n, Q, rp, NULL, irp, NULL, ninv) != 0) {
+        free(rp);
+        free(irp);
+        return -1;
+    }
+    orc_rng r;
+    rng_seed(&r, seed);
+    int32_t *s_lwe = (int32_t *)malloc(sizeof(int32_t) * n), *s_rlwe = (int32_t *)malloc(sizeof(int32_t) * N);
+    uint64_t *s_ntt = (uint64_t *)malloc(sizeof(uint64_t) * N), *tmp = (uint64_t *)malloc(sizeof(uint64_t) * N);
+    uint64_t *a_scr = (uint64_t *)malloc(sizeof(uint64_t) * 2 * N);
+    for (uint32_t i = 0; i < n; ++i) s_lwe[i] = (int32_t)(rng_next(&r) & 1);
+    for (uint32_t i = 0; i < N; ++i) s_rlwe[i] = (int32_t)rng_uniform(&r, 3) - 1;
+    for (uint32_t i = 0; i < N; ++i) s_ntt[i] = mod_signed(s_rlwe[i], Q);
+    ntt_fwd_one(s_ntt, N, Q, rp);
+
+    /* BSK: rows r = 2j + poly carry s_i g_j on component poly */
+    uint64_t gbr[64], ght[64], gss[64];
+    gadget_powers(Q, p->base_g, p->digits_g, gbr);
+    for (uint32_t i = 0; i < n; ++i)
+        for (uint32_t row = 0; row < l2; ++row) {
+            uint64_t *a = bsk_out ? bsk_out + ((size_t)i * l2 + row) * 2 * N : a_scr;
+            uint64_t *b = a + N;
+            keygen_rlwe_zero(&r, N, Q, sigma_rlwe, rp, s_ntt, a, b, tmp);
+            if (s_lwe[i]) {
+                uint64_t *tgt = (row & 1) ? b : a;
+                for (uint32_t c = 0; c < N; ++c) tgt[c] = addmod(tgt[c], gbr[row >> 1], Q);
+            }
+        }
+
+    /* HomTrace keys: automorphism X -> X^(N/2^r + 1) of s */
+    gadget_powers(Q, p->base_ht, p->digits_ht, ght);
+    uint64_t *sig = (uint64_t *)malloc(sizeof(uint64_t) * N);
+    for (uint32_t rd = 0; rd < rounds; ++rd) {
+        const uint64_t kk = ((uint64_t)N >> rd) + 1;
+        memset(sig, 0, sizeof(uint64_t) * N);
+        for (uint32_t i = 0; i < N; ++i) {
+            const uint64_t e = ((uint64_t)i * kk) % (2ull * N);
+            if (e < N) sig[e] = addmod(sig[e], mod_signed(s_rlwe[i], Q), Q);
+            else sig[e - N] = addmod(sig[e - N], mod_signed(-(int64_t)s_rlwe[i], Q), Q);
+        }
+        ntt_fwd_one(sig, N, Q, rp);
+        for (uint32_t j = 0; j < p->digits_ht; ++j) {
+            uint64_t *a = ht_out ? ht_out + ((size_t)rd * p->digits_ht + j) * 2 * N : a_scr;
+            uint64_t *b = a + N;
+            keygen_rlwe_zero(&r, N, Q, sigma_rlwe, rp, s_ntt, a, b, tmp);
+            for (uint32_t c = 0; c < N; ++c) b[c] = submod(b[c], orc_mulmod(sig[c], ght[j], Q), Q);
+        }
+    }
+    free(sig);
+
+    /* SchemeSwitch key: s^2 g_j */
+    gadget_powers(Q, p->base_ss, p->digits_ss, gss);
+    for (uint32_t j = 0; j < p->digits_ss; ++j) {
+        uint64_t *a = ss_out ? ss_out + (size_t)j * 2 * N : a_scr;
+        uint64_t *b = a + N;
+        keygen_rlwe_zero(&r, N, Q, sigma_rlwe, rp, s_ntt, a, b, tmp);
+        for (uint32_t c = 0; c < N; ++c)
+            b[c] = addmod(b[c], orc_mulmod(orc_mulmod(s_ntt[c], s_ntt[c], Q), gss[j], Q), Q);
+    }
+
+    /* derived tables: gadget powers of the RGSW output, the multi-value test vector (slot j of
+     * every 2^bw block holds -+g_j/2, negative on the first half), the automorphism maps */
+    uint64_t gcc[64];
+    gadget_powers(Q, p->base_cc, p->num_lut, gcc);
+    if (gpow_out) memcpy(gpow_out, gcc, sizeof(uint64_t) * p->num_lut);
+    if (tv_out) {
+        uint32_t bw = 0;
+        while ((1u << bw) < p->num_lut) ++bw;
+        for (uint32_t i = 0; i < N; ++i) {
+            const uint32_t slot = i & ((1u << bw) - 1);
+            tv_out[i] = 0;
+            if (slot >= p->num_lut) continue;
+            const uint64_t half = (gcc[slot] >> 1) % Q;
+            tv_out[i] = (i < N / 2) ? (half ? Q - half : 0) : half;
+        }
+    }
+    if (maps_out) orc_auto_maps(maps_out, N, rounds);
+
+    /* extraction key switch N -> n: LWE_s(v s'_i B^j) mod qks, u16 */
+    const uint32_t outlen = n + 1, mask = qks - 1;
+    uint16_t *row_scr = (uint16_t *)malloc(sizeof(uint16_t) * outlen);
+    for (uint32_t j = 0; j < 2; ++j) {
+        const uint32_t bj = (j == 0) ? 1u : base_ks;
+        for (uint32_t i = 0; i < N; ++i) {
+            const uint32_t si = (uint32_t)(s_rlwe[i] + (int32_t)qks) & mask;
+            for (uint32_t v = 0; v < base_ks; ++v) {
+                uint16_t *row = ksk_out ? ksk_out + (((size_t)j * N + i) * base_ks + v) * outlen : row_scr;
+                uint32_t acc = 0;
+                for (uint32_t c = 0; c < n; ++c) {
+                    const uint32_t a = (uint32_t)(rng_next(&r) & mask);
+                    row[c] = (uint16_t)a;
+                    if (s_lwe[c]) acc += a;
+                }
+                const int64_t e = rng_rounded_gaussian(&r, sigma_lwe);
+                const uint32_t m = (v * si * bj) & mask;
+                row[n] = (uint16_t)((acc + m + (uint32_t)e) & mask);
+            }
+        }
+    }
+    free(row_scr);
+    if (s_lwe_out) memcpy(s_lwe_out, s_lwe, sizeof(int32_t) * n);
+    if (s_rlwe_out) memcpy(s_rlwe_out, s_rlwe, sizeof(int32_t) * N);
+    free(a_scr);
+    free(tmp);
+    free(s_ntt);
+    free(s_rlwe);
+    free(s_lwe);
+    free(irp);
+    free(rp);
+    return 0;
+}
+
+void orc_cbs_keygen_mb(const orc_cbs_params *p, double sigma_rlwe, const int32_t *s_lwe, const int32_t *s_rlwe,
+                       uint32_t mb, uint64_t seed, uint64_t *mbk) {
+    static const uint32_t order2[3] = {1u, 2u, 3u};
+    static const uint32_t order3[7] = {1u, 2u, 4u, 3u, 5u, 6u, 7u};
+    const uint32_t N = p->N, n = p->n, l2 = 2 * p->digits_g, K = (1u << mb) - 1u, groups = (n + mb - 1) / mb;
+    const uint64_t Q = p->Q;
+    uint64_t *rp = (uint64_t *)malloc(sizeof(uint64_t) * N), *irp = (uint64_t *)malloc(sizeof(uint64_t) * N);
+    uint64_t ninv[2];
+    orc_ntt_tables(p->log_n, Q, rp, NULL, irp, NULL, ninv);
+    uint64_t *s_ntt = (uint64_t *)malloc(sizeof(uint64_t) * N);
+    for (uint32_t i = 0; i < N; ++i) s_ntt[i] = mod_signed(s_rlwe[i], Q);
+    ntt_fwd_one(s_ntt, N, Q, rp);
+    uint64_t gbr[64];
+    gadget_powers(Q, p->base_g, p->digits_g, gbr);
+#pragma omp parallel for schedule(dynamic)
+    for (long g = 0; g < (long)groups; ++g) {
+        uint64_t *tmp = (uint64_t *)malloc(sizeof(uint64_t) * N);
+        orc_rng r;
+        rng_seed(&r, seed ^ (0x9e3779b97f4a7c15ull * (uint64_t)(g + 1)));
+        for (uint32_t kk = 0; kk < K; ++kk) {
+            const uint32_t mask = mb == 2 ? order2[kk] : order3[kk];
+            uint32_t prod = 1;
+            for (uint32_t i = 0; i < mb; ++i)
+                if (mask & (1u << i)) {
+                    const uint32_t idx = (uint32_t)g * mb + i;
+                    prod &= idx < n ? (uint32_t)s_lwe[idx] : 0u;
+                }
+            for (uint32_t row = 0; row < l2; ++row) {
+                uint64_t *a = mbk + (((size_t)g * K + kk) * l2 + row) * 2 * N;
+                uint64_t *b = a + N;
+                keygen_rlwe_zero(&r, N, Q, sigma_rlwe, rp, s_ntt, a, b, tmp);
+                if (prod) {
+                    uint64_t *tgt = (row & 1) ? b : a;
+                    for (uint32_t c = 0; c < N; ++c) tgt[c] = addmod(tgt[c], gbr[row >> 1], Q);
+                }
+            }
+        }
+        free(tmp);
+    }
+    free(s_ntt);
+    free(irp);
+    free(rp);
+}

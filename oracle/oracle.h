@@ -210,6 +210,25 @@ void orc_encrypt_words_rlwe(const uint32_t key[8], const uint32_t *words, uint32
 void orc_encrypt_bits_lwe(const uint32_t key[8], const uint8_t *bits, uint32_t count, uint32_t n, uint64_t q,
                           const int32_t *s, const uint64_t *T, uint32_t tlen, uint64_t *a, uint64_t *b);
 
+/* ---------------- key generation for the CPU legs (the reference generates its keys in the
+ * absent OpenFHE fork: CirBTKeyGen / KeySwitchGen, examples/aes_transcipher/main.cu:232-252).
+ * Restates the seeded host key generation of the CUDA path's host side, generator included
+ * (xoshiro256** seeded through splitmix64, Box-Muller Gaussians rounded to integers), so the
+ * same seed gives the same keys word for word: binary LWE secret, ternary RLWE secret, BSK
+ * RGSW(s_i) [n][2 digits_g][2][N], HomTrace keys (k1 - k0 s = -sigma_r(s) g_j + e)
+ * [rounds][digits_ht][2][N], SchemeSwitch key (k1 - k0 s = s^2 g_j + e) [digits_ss][2][N], all
+ * NTT domain, the extraction KSK [2][N][base_ks][n+1] u16 mod qks, and the derived test vector
+ * tv[N], gadget powers gpow[num_lut] and automorphism maps [rounds][N].  Any output may be
+ * NULL.  Returns 0, or -1 for parameters without NTT tables. ---------------- */
+int orc_cbs_keygen(const orc_cbs_params *p, double sigma_lwe, double sigma_rlwe, uint32_t qks, uint32_t base_ks,
+                   uint64_t seed, int32_t *s_lwe, int32_t *s_rlwe, uint64_t *bsk, uint64_t *ht, uint64_t *ss,
+                   uint16_t *ksk, uint64_t *tv, uint64_t *gpow, uint32_t *maps);
+/* the grouped (mb = 2 or 3) keys of the same key set: RGSW(prod_{i in S} s_i) per group and
+ * non-empty subset S, [ceil(n/mb)][2^mb - 1][2 digits_g][2][N]; one generator per group seeded
+ * with seed ^ (0x9e3779b97f4a7c15 (g + 1)) */
+void orc_cbs_keygen_mb(const orc_cbs_params *p, double sigma_rlwe, const int32_t *s_lwe, const int32_t *s_rlwe,
+                       uint32_t mb, uint64_t seed, uint64_t *mbk);
+
 #ifdef __cplusplus
 }
 #endif

@@ -3,10 +3,11 @@ secret keys exported by the product) and small utilities shared by the CBS tests
 from __future__ import annotations
 
 import ctypes
+from types import SimpleNamespace
 
 import numpy as np
 
-from conftest import _U16P, _U32P, _U64P, oracle_tables
+from conftest import _U16P, _U32P, _U64P, oracle_primes, oracle_tables
 
 
 class OrcParams(ctypes.Structure):
@@ -138,3 +139,62 @@ def lwe_decrypt_bits(s_lwe: np.ndarray, a: np.ndarray, b: np.ndarray, q: int):
     bits = np.array([((2 * x + q // 2) // q) & 1 for x in ph], dtype=np.uint8)
     err = [min(abs(x - (q // 2) * int(bt)), q - abs(x - (q // 2) * int(bt))) for x, bt in zip(ph, bits)]
     return bits, err
+
+
+def orc_params(p) -> OrcParams:
+    """The oracle's parameter record of a parameter set (any object with the cbs_params fields)."""
+    N = p.N
+    return OrcParams(N=N, log_n=N.bit_length() - 1, Q=p.Q, n=p.n, q_lwe=p.q_lwe, base_g=p.base_g,
+                     digits_g=p.digits_g, num_lut=p.num_lut, base_cc=p.base_cc, base_ht=p.base_ht,
+                     digits_ht=p.digits_ht, base_ss=p.base_ss, digits_ss=p.digits_ss,
+                     trace_rounds=N.bit_length() - 1 - p.trace_shift)
+
+
+def oracle_keys(oracle, p, seed: int) -> dict:
+    """The key set of seed from the oracle's key generation (same layouts as the product's
+    export_keys)."""
+    vp = ctypes.c_void_p
+    oracle.orc_cbs_keygen.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_uint32, ctypes.c_uint32,
+                                      ctypes.c_uint64] + [vp] * 9
+    oracle.orc_cbs_keygen.restype = ctypes.c_int
+    N, n, rounds = p.N, p.n, p.N.bit_length() - 1 - p.trace_shift
+    k = {"s_lwe": np.zeros(n, np.int32), "s_rlwe": np.zeros(N, np.int32),
+         "bsk": np.zeros((n, 2 * p.digits_g, 2, N), np.uint64),
+         "ht": np.zeros((rounds, p.digits_ht, 2, N), np.uint64), "ss": np.zeros((p.digits_ss, 2, N), np.uint64),
+         "ksk": np.zeros((2, N, p.base_ks, n + 1), np.uint16), "tv": np.zeros(N, np.uint64),
+         "gpow": np.zeros(p.num_lut, np.uint64), "maps": np.zeros((rounds, N), np.uint32)}
+    op = orc_params(p)
+    st = oracle.orc_cbs_keygen(ctypes.byref(op), p.sigma_lwe, p.sigma_rlwe, p.qks, p.base_ks, seed,
+                               *(k[f].ctypes.data for f in ("s_lwe", "s_rlwe", "bsk", "ht", "ss", "ksk", "tv", "gpow",
+                                                            "maps")))
+    assert st == 0
+    return k
+
+
+def oracle_params(oracle, preset: str = "3x12") -> SimpleNamespace:
+    """The parameter sets of cbs_params_preset restated for the CPU legs, which load nothing from
+    the product library (test_oracle_keygen.py pins the values to the product's)."""
+    base_g, digits_g = {"3x12": (1 << 12, 3), "2x18": (1 << 18, 2)}[preset]
+    return SimpleNamespace(N=2048, Q=oracle_primes(oracle, 2048, 54, 1)[0], n=630, q_lwe=1 << 14, base_g=base_g,
+                           digits_g=digits_g, num_lut=4, base_cc=1 << 6, base_ht=1 << 9, digits_ht=5,
+                           base_ss=1 << 9, digits_ss=5, trace_shift=0, qks=1 << 14, base_ks=1 << 7, sigma_lwe=0.5,
+                           sigma_rlwe=3.19)
+
+
+# the product seeds a context's grouped keys with the key seed xor this tweak
+MB_SEED_TWEAK = 0x6d756c7469626974
+
+
+def oracle_keys_mb(oracle, p, keys: dict, mb: int, seed: int) -> np.ndarray:
+    """Grouped keys [ceil(n/mb)][2^mb - 1][2 digits_g][2][N] of a key set from the oracle, seeded
+    as a context keyed with `seed` seeds them."""
+    vp = ctypes.c_void_p
+    oracle.orc_cbs_keygen_mb.argtypes = [vp, ctypes.c_double, vp, vp, ctypes.c_uint32, ctypes.c_uint64, vp]
+    groups = -(-p.n // mb)
+    out = np.zeros((groups, (1 << mb) - 1, 2 * p.digits_g, 2, p.N), np.uint64)
+    op = orc_params(p)
+    s_lwe = np.ascontiguousarray(keys["s_lwe"], np.int32)
+    s_rlwe = np.ascontiguousarray(keys["s_rlwe"], np.int32)
+    oracle.orc_cbs_keygen_mb(ctypes.byref(op), p.sigma_rlwe, s_lwe.ctypes.data, s_rlwe.ctypes.data, mb,
+                             seed ^ MB_SEED_TWEAK, out.ctypes.data)
+    return out
