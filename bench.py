@@ -143,6 +143,59 @@ def verify(pkg, ctx, key: bytes, ctrs: np.ndarray, ha: np.ndarray, hb: np.ndarra
     return int((got == want).all(axis=1).sum())
 
 
+def output_noise(pkg, ctx, key: bytes, ctrs: np.ndarray, ha: np.ndarray, hb: np.ndarray) -> dict:
+    """Phase error of the transciphered keystream bits (secret key exported for the measurement
+    only): e = b - <a, s> - m q/2 (mod q, centred) against the true AES bit m; its rms sigma and the
+    Gaussian tail at the decision margin q/4 give the failure probability of one bit decision
+    (every extraction of every round has this noise: 1280 decisions per block)."""
+    p = ctx.params
+    s = np.zeros(p.n, np.int32)
+    pkg.call("cbs_export_keys", ctx.handle, s.ctypes.data, None, None, None, None, None, None, None, None)
+    q = int(p.q_lwe)
+    dot = (ha[:, : p.n].astype(np.int64) @ s.astype(np.int64)) % q
+    m = np.unpackbits(aes_ecb(key, ctrs), axis=1, bitorder="little").reshape(-1).astype(np.int64)
+    e = (hb.astype(np.int64) - dot - m * (q // 2) + q // 2) % q - q // 2
+    sigma = float(np.sqrt(np.mean(e.astype(np.float64) ** 2)))
+    lp = pkg.log2_pfail_gaussian(sigma, q / 4)
+    return {"bits": int(e.size), "sigma": sigma, "max_abs": int(np.abs(e).max()), "margin": q // 4,
+            "p_fail_log2_per_bit": lp, "p_fail_log2_per_block": lp + float(np.log2(128 * ROUNDS)),
+            "target_log2": -40.0,
+            "method": "sigma = rms of the measured output-bit phase errors (keystream bits of the last step); "
+                      "p = erfc(margin / (sqrt(2) sigma)) per bit decision, x 1280 decisions per block"}
+
+
+def gate_split_pair(pkg, torch, count: int = 1184, steps: int = 3) -> dict:
+    """The split-FP32 external product where it is built (torus-32 gate path, n = 636, N = 1024):
+    NAND gates/s with split FP32 (one-bit) beside FP64 (grouped mb = 2, the FP64 default), same
+    inputs, timed with CUDA events; every output gate checked."""
+    ctx = pkg.GateContext(max_batch=count)
+    ctx.keygen(7)
+    p = ctx.params
+    rng = np.random.default_rng(7)
+    x = rng.integers(0, 2, count).astype(np.uint8)
+    y = rng.integers(0, 2, count).astype(np.uint8)
+    a1, b1 = ctx.encrypt(x, seed=8)
+    a2, b2 = ctx.encrypt(y, seed=9)
+    d = [torch.from_numpy(np.ascontiguousarray(v).view(np.int32)).cuda() for v in (a1, b1, a2, b2)]
+    oa = torch.zeros((count, p.n), dtype=torch.int32, device="cuda")
+    ob = torch.zeros(count, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.Stream()
+    res = {}
+    for name, mb, mode in (("fp64_mb2", 2, "fp64"), ("split_fp32", 1, "fp32-split")):
+        ctx.set_fft_mode("fp64")
+        ctx.set_multibit(mb)
+        ctx.set_fft_mode(mode)
+        fn = lambda: pkg.call("cbs_gate_eval_batch_device", ctx.handle, pkg.GATE_NAND,  # noqa: E731
+                              *(t.data_ptr() for t in d), count, oa.data_ptr(), ob.data_ptr(), stream.cuda_stream)
+        ms = _timed(torch, stream, fn, 2, steps)
+        ok = int((ctx.decrypt(oa.cpu().numpy().view(np.uint32), ob.cpu().numpy().view(np.uint32))
+                  == 1 - (x & y)).sum())
+        res[name] = {"gates_per_s": count / (ms * 1e-3), "correct": ok, "of": count}
+    ctx.close()
+    res["ratio_split_over_fp64"] = res["split_fp32"]["gates_per_s"] / res["fp64_mb2"]["gates_per_s"]
+    return res
+
+
 def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     import torch
 
@@ -186,10 +239,11 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     ms_max = rep.max_over_ranks(ev0.elapsed_time(ev1), world, device="cuda")
     ms_per_step = ms_max / args.steps
 
-    # correctness of the last step's output
+    # correctness of the last step's output and its noise
     ha = out_a.cpu().numpy().view(np.uint64).copy()
     hb = out_b.cpu().numpy().view(np.uint64).copy()
     ok = verify(pkg, ctx, key, ctrs, ha, hb)
+    noise = output_noise(pkg, ctx, key, ctrs, ha, hb)
 
     # dominant kernel: the fused blind rotation over the whole batch, timed alone
     T = min(blocks, 256) * 128
@@ -213,8 +267,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     br_ms = e0.elapsed_time(e1) / reps
     N, n, l2, L = p.N, p.n, 2 * p.digits_g, p.num_lut
     alg_bytes = br_key_bytes(p, args.multibit) + T * ((n + 1) * 8 + L * 2 * N * 8)  # key once + LWE in + MV out
-    peaks = measured_peaks()
-    achieved_gbs = alg_bytes / (br_ms * 1e-3) / 1e9
+    traffic = BR_TRAFFIC.get((args.backend, args.params, args.multibit, T))
 
     # e2e through the host-buffer C-ABI entry point of the whole job: a public AES-CTR
     # ciphertext of seeded random plaintext in, LWE encryptions of the plaintext bits out
@@ -266,18 +319,19 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
         "gpu_launches": launches_per_step * args.steps,
         "e2e": {"value": rep.whole_job_rate(world, blocks, e2e_ms), "unit": UNIT, "h2d_bytes_per_step": blocks * (128 + 16),
                 "d2h_bytes_per_step": blocks * 128 * (p.n + 1) * 8, "correct_blocks": e2e_ok},
-        "roofline": {"kernel": br_kernel_name(args)
-                     + " (fused GINX blind rotation + finalize + MV split)", "bound": "hbm",
-                     "achieved": achieved_gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                     "frac": achieved_gbs / peaks["hbm_gbs"], "peak_src": peaks["src"],
-                     "traffic": BR_TRAFFIC.get((args.backend, args.multibit, T)),
-                     "algorithmic_bytes_per_launch": alg_bytes, "launch_ms": br_ms,
-                     "note": "compute-bound (integer multiplies for ntt, FP64 pipe for fft64); see compute_rate"},
-        "compute_rate": compute_rate(args.backend, T, p, br_ms, args.multibit),
+        "roofline": br_roofline(args, p, T, br_ms, alg_bytes, traffic),
+        "p_fail": noise,
         "clocks": clk.summary(),
     }
+    if args.backend == "fft64":
+        result["split_fp32"] = {
+            "aes_path": "not built: an exact FP32 limb of the 54-bit-Q external product holds at most 3 bits "
+                        "under 12-bit digits (6 under 9-bit) at N = 2048, i.e. 18+ limbs with an inverse "
+                        "transform and key spectra each against one FP64 product, and a whole-key FP32 product "
+                        "misses by ~2^-7 of Q (tests/test_fp32_split_analysis.py)",
+            "gate_path_measured": gate_split_pair(pkg, torch)}
     if rank == 0 and args.cpu_baseline:
-        result["cpu_baseline"] = cpu_baseline(args, pkg)
+        result["cpu_baseline"] = cpu_baseline(args)
     if rank == 0:
         print(json.dumps(result), flush=True)
     ctx.close()
@@ -321,8 +375,6 @@ def run_blind_rotate(args, rank: int, world: int, local_rank: int) -> None:
         ms = _timed(torch, stream, fn, args.warmup, args.steps)
     N, n, l2, L = p.N, p.n, 2 * p.digits_g, p.num_lut
     alg_bytes = br_key_bytes(p, args.multibit) + T * ((n + 1) * 8 + L * 2 * N * 8)
-    peaks = measured_peaks()
-    gbs = alg_bytes / (ms * 1e-3) / 1e9
     out = {"metric": f"blind rotations/s ({args.backend}, N={N}, n={n})", "value": world * T / (ms * 1e-3),
            "unit": "bootstraps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -331,10 +383,9 @@ def run_blind_rotate(args, rank: int, world: int, local_rank: int) -> None:
                       "param_set": args.params, "br_gadget": f"2^{p.base_g.bit_length() - 1}x{p.digits_g}",
                       "l2": "BSK read once per launch (124 MB fft64 / 124 MB ntt); no flush between launches"},
            "us_per_bootstrap": ms * 1e3 / T, "gpu_launches": args.steps,
-           "roofline": {"kernel": br_kernel_name(args),
-                        "bound": "hbm", "achieved": gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                        "frac": gbs / peaks["hbm_gbs"], "peak_src": peaks["src"], "traffic": None},
-           "compute_rate": compute_rate(args.backend, T, p, ms, args.multibit), "clocks": clk.summary()}
+           "roofline": br_roofline(args, p, T, ms, alg_bytes, BR_TRAFFIC.get((args.backend, args.params,
+                                                                              args.multibit, T))),
+           "clocks": clk.summary()}
     if rank == 0:
         print(json.dumps(out), flush=True)
     ctx.close()
@@ -768,9 +819,31 @@ def br_key_bytes(p, mb: int) -> int:
 
 # DRAM bytes (read + write) of one blind-rotation launch, measured with ncu
 # (dram__bytes_read.sum + dram__bytes_write.sum, one pass) on the launch this bench times:
-# (backend, mb, ciphertexts per launch) -> bytes.  16384 = 128 blocks x 128 bits; the grouped
-# key (186 MB) does not fit L2 and is re-read by each wave of 148 ciphertexts.
-BR_TRAFFIC = {("fft64", 2, 16384): 20810.3e6 + 2151.6e6}
+# (backend, parameter set, mb, ciphertexts per launch) -> bytes.  16384 = 128 blocks x 128 bits;
+# the 3x12 grouped key (186 MB) does not fit L2 and is re-read by each wave of 148 ciphertexts.
+BR_TRAFFIC = {("fft64", "3x12", 2, 16384): 20810.3e6 + 2151.6e6}
+
+
+def br_roofline(args, p, T: int, br_ms: float, alg_bytes: int, traffic) -> dict:
+    """Roofline of the dominant kernel, the fused blind rotation: on the FFT backend its bound is
+    the FP64 pipe (algorithmic flops per launch over the launch time against the recorded FP64
+    peak); the exact-NTT backend is bounded by 64-bit integer multiplies and reports HBM."""
+    name = br_kernel_name(args) + " (fused GINX blind rotation + finalize + MV split)"
+    extra = {"algorithmic_bytes_per_launch": alg_bytes, "launch_ms": br_ms, "traffic": traffic,
+             "traffic_over_algorithmic": (traffic / alg_bytes) if traffic else None,
+             "traffic_src": "ncu dram__bytes_read.sum + dram__bytes_write.sum of this launch (one pass), recorded"}
+    if args.backend == "fft64":
+        flop = fp64_flop_per_launch(p, T, args.multibit)
+        achieved = flop / (br_ms * 1e-3) / 1e12
+        return {"kernel": name, "bound": "fp64", "achieved": achieved, "peak": FP64_PEAK["tflops"],
+                "unit": "TFLOP/s", "frac": achieved / FP64_PEAK["tflops"], "peak_src": FP64_PEAK["src"],
+                "fp64_flop_per_launch": flop, **extra}
+    peaks = measured_peaks()
+    gbs = alg_bytes / (br_ms * 1e-3) / 1e9
+    return {"kernel": name, "bound": "hbm", "achieved": gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+            "frac": gbs / peaks["hbm_gbs"], "peak_src": peaks["src"],
+            "note": "integer-multiply bound; compute_rate gives the modular products per second",
+            "compute_rate": compute_rate(args.backend, T, p, br_ms, args.multibit), **extra}
 
 
 def br_kernel_name(args) -> str:
@@ -779,42 +852,61 @@ def br_kernel_name(args) -> str:
     return "k_blind_rotate_fft" if args.multibit == 1 else f"k_blind_rotate_fft_mb<11,{args.multibit}>"
 
 
-def fp64_peak_tflops() -> float:
-    """Measured FP64 peak of this GPU: cuBLAS DGEMM (torch.matmul, float64, 4096^3, 2 n^3
-    flop), best of 5 after a warm-up, CUDA events on the current stream."""
+# FP64 peak of this pool's B200, measured once (not driver-written): cuBLAS DGEMM through
+# torch.matmul, float64 4096^3 (2 n^3 flop), best of 5 after a warm-up, CUDA events; three runs
+# on separate boxes gave 35.43, 35.36 and 35.40 TFLOP/s at 1965 MHz (profiles/fp64_peak_b200.md).
+FP64_PEAK = {"tflops": 35.4, "src": "recorded: cuBLAS DGEMM 4096^3 (torch.matmul float64), best of 5, "
+                                    "median of three B200 runs (profiles/fp64_peak_b200.md); not driver-written"}
+
+
+def run_fp64_peak(args, rank: int, world: int, local_rank: int) -> None:
+    """The FP64 peak the blind rotation's roofline is quoted against: cuBLAS DGEMM through
+    torch.matmul, float64 n^3 (n = 4096, 2 n^3 flop), best of 5 after a warm-up, CUDA events."""
     import torch
+    torch.cuda.set_device(local_rank)
     n = 4096
     a = torch.randn((n, n), dtype=torch.float64, device="cuda")
     b = torch.randn((n, n), dtype=torch.float64, device="cuda")
     torch.matmul(a, b)
     best = float("inf")
-    for _ in range(5):
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        torch.matmul(a, b)
-        e1.record()
-        torch.cuda.synchronize()
-        best = min(best, e0.elapsed_time(e1))
-    return 2 * n ** 3 / (best * 1e-3) / 1e12
+    with ClockSampler(local_rank) as clk:
+        for _ in range(5):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            torch.matmul(a, b)
+            e1.record()
+            torch.cuda.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+    if rank == 0:
+        print(json.dumps({"metric": "FP64 DGEMM TFLOP/s (cuBLAS through torch.matmul, 4096^3)",
+                          "value": 2 * n ** 3 / (best * 1e-3) / 1e12, "unit": "TFLOP/s", "ms": best,
+                          "clocks": clk.summary()}), flush=True)
+
+
+def fp64_flop_per_launch(p, T: int, mb: int) -> int:
+    """Algorithmic FP64 flops of one FFT blind-rotation launch over T ciphertexts: per step (mb = 1)
+    or group, 2 digits_g forward and 2 inverse M-point complex transforms (5 M log2 M each), and
+    per spectrum slot and key row 8 flops per complex multiply-add with the 2^mb - 1 combined keys
+    plus the product with the digit spectrum (mb > 1)."""
+    N, n, l2 = p.N, p.n, 2 * p.digits_g
+    M = N // 2
+    fft_flop = 5 * M * (M.bit_length() - 1)
+    steps = -(-n // mb)
+    keys = (1 << mb) - 1
+    return T * steps * ((l2 + 2) * fft_flop + 2 * l2 * M * 8 * (keys + (1 if mb > 1 else 0)))
 
 
 def compute_rate(backend: str, T: int, p, br_ms: float, mb: int = 1) -> dict:
-    """Algorithmic arithmetic of one blind-rotation launch over T ciphertexts (mb > 1: groups
-    of mb coefficients, 2^mb - 1 combined keys per spectrum slot and row)."""
+    """Algorithmic arithmetic rate of one blind-rotation launch over T ciphertexts."""
     N, n, l2 = p.N, p.n, 2 * p.digits_g
     logn = N.bit_length() - 1
     if backend == "fft64":
-        M = N // 2
-        fft_flop = 5 * M * (logn - 1)  # radix-2 complex FFT flop count
-        steps = -(-n // mb)
-        keys = (1 << mb) - 1
-        flop = T * steps * ((l2 + 2) * fft_flop + 2 * l2 * M * 8 * (keys + (1 if mb > 1 else 0)))
+        flop = fp64_flop_per_launch(p, T, mb)
         achieved = flop / (br_ms * 1e-3) / 1e12
-        peak = fp64_peak_tflops()
         return {"kernel": "k_blind_rotate_fft" if mb == 1 else f"k_blind_rotate_fft_mb (mb={mb})",
                 "fp64_flop_per_launch": flop, "achieved_fp64_tflops": achieved,
-                "fp64_peak_tflops": peak, "frac": achieved / peak,
-                "peak_src": "measured in this run: cuBLAS DGEMM (torch.matmul float64 4096^3), best of 5",
+                "fp64_peak_tflops": FP64_PEAK["tflops"], "frac": achieved / FP64_PEAK["tflops"],
+                "peak_src": FP64_PEAK["src"],
                 "note": "algorithmic flops (5 M log2 M per M-point complex transform, 8 per complex "
                         "multiply-add); ncu counts ~12 % more executed FP64 flops"}
     modmuls = T * n * (8 * (N // 2) * logn + 2 * l2 * N)
@@ -822,71 +914,92 @@ def compute_rate(backend: str, T: int, p, br_ms: float, mb: int = 1) -> dict:
             "achieved_gmodmul_s": modmuls / (br_ms * 1e-3) / 1e9}
 
 
-def cpu_sample(args, pkg) -> dict:
-    """Time the CPU oracle on a bounded sample: `threads` circuit bootstraps in parallel, one
-    LUT per thread, 128 extractions; compose per-block time from the per-unit throughputs."""
+def cpu_sample(args) -> dict:
+    """Time the CPU oracle on a bounded sample of the AES workload, with the bench's parameter
+    set and blind-rotation grouping: two circuit bootstraps per host thread in parallel (blind
+    rotation over groups of args.multibit coefficients + HomTrace + SchemeSwitch of its num_lut
+    multi-value RLWEs), two 8->32 CMux LUTs per thread, 128 extract + key switches; blocks/s is
+    composed as 10 rounds x (128 CBS + 16 LUT + 128 extractions) from the per-unit times.  Keys
+    and parameters come from the oracle itself: nothing of the product library is loaded."""
     sys.path.insert(0, str(ROOT / "tests"))
-    from cbs_harness import OracleCbs, lwe_encrypt_bits  # noqa: E402
+    from cbs_harness import OracleCbs, lwe_encrypt_bits, oracle_keys, oracle_keys_mb, oracle_params  # noqa: E402
     from conftest import load_oracle  # noqa: E402
     from concurrent.futures import ThreadPoolExecutor
 
     o = load_oracle()
     threads = int(o.orc_num_threads())
-    p = pkg.default_params()
-    keys = pkg.generate_keys_host(p, args.seed)
+    p = oracle_params(o, args.params)
+    keys = oracle_keys(o, p, args.seed)
+    mb = args.multibit
+    mbk = oracle_keys_mb(o, p, keys, mb, args.seed) if mb > 1 else None
     oc = OracleCbs(o, p, keys)
     rng = np.random.default_rng(1)
-    nb = threads
+    nb = 2 * threads  # two per thread: a few seconds of host work per sample
     a, b = lwe_encrypt_bits(rng, keys["s_lwe"], rng.integers(0, 2, nb), p.q_lwe)
+    w0 = time.perf_counter()
     t0 = time.perf_counter()
-    mv = oc.br_mv(a, b)
+    if mbk is None:
+        oc.br_acc(a, b)
+    else:
+        oc.br_acc_mb(a, b, mbk, mb)
+    t_br = (time.perf_counter() - t0) / nb
+    mv = rng.integers(0, p.Q, size=(nb * p.num_lut, 2, p.N), dtype=np.uint64)
+    t0 = time.perf_counter()
     rg = oc.trace_ss(mv)
-    t_cbs = (time.perf_counter() - t0) / nb
-    rg = rg.reshape(nb, -1)
+    t_trace = (time.perf_counter() - t0) / nb
+    t_cbs = t_br + t_trace
+    rg = rg.reshape(nb, -1)[:, : p.num_lut * 4 * p.N]
     table = rng.integers(0, p.Q, size=(256, 2, p.N), dtype=np.uint64)
     ctrls = [np.ascontiguousarray(rg[k % nb]) for k in range(8)]
     t0 = time.perf_counter()
     with ThreadPoolExecutor(threads) as ex:
-        list(ex.map(lambda _: oc.lut(table, ctrls), range(threads)))
-    t_lut = (time.perf_counter() - t0) / threads
+        list(ex.map(lambda _: oc.lut(table, ctrls), range(2 * threads)))
+    t_lut = (time.perf_counter() - t0) / (2 * threads)
     words = rng.integers(0, p.Q, size=(4, 2, p.N), dtype=np.uint64)
     info = np.array([((t // 32) << 16) | (t % 32) for t in range(128)], np.uint32)
     t0 = time.perf_counter()
     oc.extract(words, info)
     t_ext = (time.perf_counter() - t0) / 128
+    wall = time.perf_counter() - w0
     per_block = ROUNDS * (128 * t_cbs + 16 * t_lut + 128 * t_ext)
     return {"value": 1.0 / per_block, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{nb} circuit bootstraps (BR n={p.n} + HomTrace + SchemeSwitch) in parallel, {threads} "
-                      f"8->32 CMux LUTs, 128 extract+KS; blocks/s composed as 10 rounds x (128 CBS + 16 LUT + "
+            "sample": f"{nb} circuit bootstraps (blind rotation n={p.n}, mb={mb}, gadget 2^{p.base_g.bit_length() - 1}"
+                      f"x{p.digits_g}; HomTrace + SchemeSwitch of {p.num_lut} RLWEs each) on {threads} threads, "
+                      f"{2 * threads} 8->32 CMux LUTs, 128 extract+KS; blocks/s composed as 10 rounds x (128 CBS + 16 LUT + "
                       f"128 extract) from the per-unit times",
-            "per_unit_s": {"cbs": t_cbs, "lut": t_lut, "extract": t_ext}}
+            "sample_wall_s": wall, "params": args.params,
+            "per_unit_s": {"cbs": t_cbs, "blind_rotation": t_br, "trace": t_trace, "lut": t_lut, "extract": t_ext},
+            "mulmod": "exact 128/64-bit hardware division (measured on the build host: 8.1 ns per dependent "
+                      "modular product against 10.5 ns for a Barrett reduction, so kept)"}
 
 
-def cpu_baseline(args, pkg) -> dict:
-    return cpu_sample(args, pkg)
+def cpu_baseline(args) -> dict:
+    return cpu_sample(args)
 
 
 def run_reference(args, rank: int) -> None:
     if rank != 0:
         return
-    pkg = load_pkg()
-    vals = []
+    vals, walls = [], []
     last = None
     for i in range(args.warmup + args.steps):
-        r = cpu_sample(args, pkg)
+        r = cpu_sample(args)
         if i >= args.warmup:
             vals.append(r["value"])
+            walls.append(r["sample_wall_s"])
             last = r
     value = statistics.median(vals)
     last["value"] = value
     out = {
         "impl": "reference", "metric": METRICS[args.backend], "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "u64 (exact mod-Q arithmetic, CPU)",
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(walls),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64 (exact mod-Q arithmetic, CPU)",
         "data": "synthetic (seeded)",
-        "config": {"workload": "aes128_ctr_transcipher", "blocks_per_gpu": args.blocks,
+        "config": {"workload": "aes128_ctr_transcipher", "blocks_per_gpu": args.blocks, "param_set": args.params,
+                   "br_multibit": args.multibit,
                    "note": "the reference's CPU path (OpenFHE fork) is absent; CPU restatement of the same "
-                           "algorithm (oracle/) on all host threads, bounded sample per step"},
+                           "algorithm (oracle/) on all host threads; each step is one bounded sample (its wall "
+                           "time is ms_per_step) from which blocks/s is composed"},
         "cpu_baseline": last,
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -909,12 +1022,12 @@ def main() -> None:
                     help="external-product arithmetic of --workload gate / ragged (torus-32): exact FP64, "
                          "split FP32 (24/25-bit + exact top key limb), or FP32 on whole keys; FP32 modes use "
                          "--multibit 1")
-    ap.add_argument("--params", choices=["3x12", "2x18"], default="3x12",
+    ap.add_argument("--params", choices=["3x12", "2x18"], default="2x18",
                     help="parameter set of the aes128 / blind_rotate workloads: blind-rotation gadget 2^12 x 3 "
                          "(cbs_params_default) or 2^18 x 2")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--workload", choices=["aes128", "blind_rotate", "keyswitch", "rns_ntt", "gate", "ragged", "tcb",
-                                           "aes_setup"],
+                                           "aes_setup", "fp64_peak"],
                     default="aes128",
                     help="aes128 is the headline; the others time one kernel family")
     ap.add_argument("--batch", type=int, default=0, help="units per step for the kernel workloads")
@@ -948,7 +1061,8 @@ def main() -> None:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     runner = {"aes128": run_ours, "blind_rotate": run_blind_rotate, "keyswitch": run_keyswitch,
               "rns_ntt": run_rns_ntt, "gate": run_gate,
-              "ragged": run_ragged, "tcb": run_tcb, "aes_setup": run_aes_setup}[args.workload]
+              "ragged": run_ragged, "tcb": run_tcb, "aes_setup": run_aes_setup,
+              "fp64_peak": run_fp64_peak}[args.workload]
     try:
         runner(args, rank, world, local_rank)
     finally:
