@@ -95,6 +95,10 @@ def _declare(lib: ctypes.CDLL) -> None:
         "cbs_circuit_bootstrap_batch_device": (st, [c_vp, c_vp, c_vp, u32, u32, c_vp, c_vp]),
         "cbs_lut8x32_batch_device": (st, [c_vp, c_vp, u32, c_vp, c_vp, u32, u64, c_vp, u32, c_vp, c_vp]),
         "cbs_cmux_batch_device": (st, [c_vp, c_vp, c_vp, c_vp, u64, u32, c_vp, c_vp]),
+        "cbs_circuit_bootstrap_batch": (st, [c_vp, c_vp, c_vp, u32, u32, c_vp]),
+        "cbs_context_set_br_schedule": (st, [c_vp, u32]),
+        "cbs_autotune_blind_rotation": (st, [c_vp, u32, ctypes.c_char_p, c_vp]),
+        "cbs_context_tuned": (st, [c_vp, c_vp]),
         "cbs_extract_keyswitch_device": (st, [c_vp, c_vp, u32, c_vp, u32, c_vp, c_vp, u32, c_vp]),
         "cbs_aes128_setup": (st, [c_vp, c_vp, u64]),
         "cbs_aes128_setup_device": (st, [c_vp, c_vp, c_vp]),
@@ -194,6 +198,17 @@ def log2_pfail_gaussian(sigma: float, margin: float) -> float:
     return -(z * z / 2) / math.log(2) - math.log2(z * math.sqrt(math.pi / 2))
 
 
+class TuneChoice(ctypes.Structure):
+    """cbs_tune_choice: the blind rotation's tuned grouping and schedule."""
+    _fields_ = [("mb", ctypes.c_uint32), ("schedule", ctypes.c_uint32), ("us_per_bootstrap", ctypes.c_double),
+                ("batch", ctypes.c_uint32), ("candidates", ctypes.c_uint32)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+BR_SCHEDULE_AUTO, BR_SCHEDULE_DIGITWISE, BR_SCHEDULE_LOCKSTEP = 0, 1, 2
+
 PARAMS_AES_3X12, PARAMS_AES_2X18 = 0, 1
 PRESETS = {"3x12": PARAMS_AES_3X12, "2x18": PARAMS_AES_2X18}
 
@@ -284,6 +299,18 @@ class Context:
 
     def set_br_backend(self, backend: int) -> None:
         call("cbs_context_set_br_backend", self._h, backend)
+
+    def autotune(self, batch: int, cache_path: str | None = None) -> dict:
+        """Time the blind rotation's groupings / schedules at `batch`, apply and cache the fastest."""
+        c = TuneChoice()
+        call("cbs_autotune_blind_rotation", self._h, batch, cache_path.encode() if cache_path else None,
+             ctypes.byref(c))
+        return c.as_dict()
+
+    def tuned(self) -> dict | None:
+        """The tuned choice this context holds (from the cache or the last autotune), or None."""
+        c = TuneChoice()
+        return c.as_dict() if load().cbs_context_tuned(self._h, ctypes.byref(c)) == 0 else None
 
     def set_br_multibit(self, mb: int) -> None:
         """Blind rotation over groups of mb = 1, 2 or 3 LWE coefficients (FFT backend)."""

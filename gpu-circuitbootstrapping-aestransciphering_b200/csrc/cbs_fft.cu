@@ -456,6 +456,183 @@ __global__ void __launch_bounds__(BrFftCfg<LOGN>::T, BrFftMbCfg<LOGN, MB>::MIN_B
     }
 }
 
+// Two-digit form of the grouped blind rotation (the 2^18 x 2 gadget).  Each half transforms both
+// digits of its polynomial in lockstep (fft_forward2_to_regs: interleaved butterflies, one set
+// of barriers, an exchange buffer per digit), then, per digit and subset S, multiplies the digit
+// spectrum by m_S(psi) and accumulates it against the subset's key spectra of row 2d + h:
+// y_c += (x_d m_S) K_S[2d + h][c].  Same arithmetic count as forming the combined key first; the
+// two live digit spectra take the registers the combined-key accumulators held.
+template <int LOGN, int MB, bool WIDE>
+__global__ void __launch_bounds__(BrFftCfg<LOGN>::T, 1)
+    k_blind_rotate_fft_mb_d2(const BlindRotateArgs a, const FftKeyArgs f) {
+    constexpr int LOGM = LOGN - 1;
+    constexpr uint32_t N = 1u << LOGN, M = N / 2, TH = M / 8, T = 2 * TH, TWO_N = 2 * N;
+    constexpr uint32_t KS = (1u << MB) - 1u;
+    constexpr uint32_t DIGITS = 2;
+    using Tb = FftTab<LOGM>;
+    using DigT = typename DigitPair<WIDE>::T;
+    extern __shared__ __align__(16) uint64_t smem[];
+    uint64_t* acc = smem;                                           // [2][N]
+    double2* fs = reinterpret_cast<double2*>(smem + 2 * N);         // [2 halves][2 digits][M]
+    double2* tab = fs + 4 * M;                                      // FftTab<LOGM>
+    DigT* dig = reinterpret_cast<DigT*>(tab + Tb::size());          // [2][2][M] digit pairs
+    double2* cbuf = reinterpret_cast<double2*>(dig + 2 * DIGITS * M);  // [MB][8][T] c_i per slot
+    const double2* tws = tab + Tb::twist_off();
+    const uint32_t ct = blockIdx.x, tid = threadIdx.x;
+    const uint32_t h = tid / TH, ht = tid % TH;
+    int64_t* my_acc = reinterpret_cast<int64_t*>(acc) + h * N;
+    double2* my_fs0 = fs + (2 * h) * M;
+    double2* my_fs1 = my_fs0 + M;
+    const uint64_t Q = a.t.q;
+    const int gbits = a.g.gbits;
+    int64_t offset = 0;
+    for (uint32_t k = 0; k < DIGITS; ++k) offset += static_cast<int64_t>(1) << (gbits * k + gbits - 1);
+    const int ign = a.g.ign;
+    const uint64_t qhalf = Q >> 1;
+    const uint64_t round_c = (ign ? (uint64_t(1) << (ign - 1)) : 0) + (static_cast<uint64_t>(offset) << ign);
+    const int64_t hi_b = static_cast<int64_t>(round_c + qhalf), Qs = static_cast<int64_t>(Q), lo_b = hi_b - Qs;
+    auto to_offset = [&](uint64_t x) {
+        return static_cast<int64_t>(x + round_c) - (x >= qhalf ? Qs : 0);
+    };
+
+    for (uint32_t i = tid; i < Tb::size(); i += T) tab[i] = f.tab[i];
+    {
+        const uint32_t bt = special_ms_f(a.b[ct], TWO_N, a.q_lwe, a.bitwidth);
+        int64_t* y = reinterpret_cast<int64_t*>(acc);
+        for (uint32_t i = tid; i < N; i += T) {
+            y[i] = to_offset(0);
+            const uint32_t s = (i + bt) & (TWO_N - 1);
+            const uint64_t v = (s < N) ? a.tv[s] : a.tv[s - N];
+            y[N + i] = to_offset((s < N) ? v : (v ? Q - v : 0));
+        }
+    }
+    __syncthreads();
+
+    auto half_bar = [h]() {
+        if (h == 0) asm volatile("bar.sync 1, %0;" ::"n"(TH) : "memory");
+        else asm volatile("bar.sync 2, %0;" ::"n"(TH) : "memory");
+    };
+    constexpr uint32_t l2 = 2 * DIGITS;
+    const int32_t dbias = 1 << (gbits - 1);
+    const uint64_t* arow = a.a + static_cast<size_t>(ct) * a.a_stride;
+    const uint32_t groups = (a.n + MB - 1) / MB;
+    constexpr size_t kstride = static_cast<size_t>(l2) * 2 * M;  // spectra between subsets of a group
+    const uint32_t fmask = (1u << gbits) - 1u;
+    for (uint32_t g = 0; g < groups; ++g) {
+        // c_i(psi_s) for the thread's 8 slots, as in k_blind_rotate_fft_mb
+#pragma unroll
+        for (int i = 0; i < MB; ++i) {
+            const uint32_t idx = g * MB + i;
+            const uint32_t at = idx < a.n ? special_ms_f(__ldg(arow + idx), TWO_N, a.q_lwe, a.bitwidth) : 0u;
+            const double2 ub = zeta_pow<LOGN>(tws, mult_base<LOGN>(ht, at));
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const uint32_t r3 = ((j & 1) << 2) | (j & 2) | ((j >> 2) & 1);
+                const uint32_t k = (at * r3) & 7u;
+                double2 w = tab[(k & 3u) * (M / 8)];
+                if (k & 4u) w = make_double2(-w.x, -w.y);
+                const double2 v = cmul(ub, w);
+                cbuf[(i * 8 + j) * T + tid] = make_double2(v.x - 1.0, v.y);
+            }
+        }
+        // 1. both digits of this half's polynomial (thread-private positions)
+        for (uint32_t e = ht; e < M; e += TH) {
+            const uint64_t wr = static_cast<uint64_t>(my_acc[e]) >> ign;
+            const uint64_t wi = static_cast<uint64_t>(my_acc[e + M]) >> ign;
+            DigT* dst = dig + h * DIGITS * M + e;
+#pragma unroll
+            for (uint32_t d = 0; d < DIGITS; ++d)
+                dst[d * M] = DigitPair<WIDE>::pack(static_cast<uint32_t>(wr >> (gbits * d)) & fmask,
+                                                   static_cast<uint32_t>(wi >> (gbits * d)) & fmask);
+        }
+        half_bar();
+        // 2. the two forward transforms in lockstep
+        const DigT* d0 = dig + (h * DIGITS) * M;
+        const DigT* d1 = d0 + M;
+        double2 x0[8], x1[8];
+        fft_forward2_to_regs<LOGM>(
+            my_fs0, my_fs1, ht, tab,
+            [&](int j, uint32_t e) { return cmul(DigitPair<WIDE>::unpack(d0[e], dbias), twist_at<LOGM>(tws, j, e)); },
+            [&](int j, uint32_t e) { return cmul(DigitPair<WIDE>::unpack(d1[e], dbias), twist_at<LOGM>(tws, j, e)); },
+            x0, x1, half_bar);
+        // 3. products with the subsets' keys, row 2d + h, both columns
+        const double2* gk = f.bskf + static_cast<size_t>(g) * KS * kstride + ht;
+        double2 y0[8], y1[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) y0[j] = y1[j] = make_double2(0.0, 0.0);
+#pragma unroll
+        for (uint32_t d = 0; d < DIGITS; ++d) {
+            const double2* k0 = gk + static_cast<size_t>(2 * d + h) * 2 * M;
+#pragma unroll
+            for (int s = 0; s < static_cast<int>(KS); ++s) {
+                double2 ka[8], kb[8];
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    ka[j] = __ldg(k0 + s * kstride + j * TH);
+                    kb[j] = __ldg(k0 + s * kstride + M + j * TH);
+                }
+                const uint32_t mask = mb_key_mask(MB, s);
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    double2 t = d ? x1[j] : x0[j];
+#pragma unroll
+                    for (int i = 0; i < MB; ++i)
+                        if (mask & (1u << i)) t = cmul(t, cbuf[(i * 8 + j) * T + tid]);
+                    cfma(y0[j], t, ka[j]);
+                    cfma(y1[j], t, kb[j]);
+                }
+            }
+        }
+        half_bar();  // the transforms' last reads of my_fs0 / my_fs1 are done before the swap writes
+        // 4. swap partial sums: half 0 keeps output 0, half 1 keeps output 1
+#pragma unroll
+        for (int j = 0; j < 8; ++j) my_fs0[cswz(8 * ht + j)] = h ? y0[j] : y1[j];
+        __syncthreads();
+        {
+            const double2* take = fs + (2 * (1 - h)) * M;
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const double2 t = take[cswz(8 * ht + j)];
+                y0[j] = cadd(h ? y1[j] : y0[j], t);
+            }
+        }
+        __syncthreads();
+        // 5. inverse transform, rounding, accumulate
+        fft_inverse_from_regs<LOGM>(
+            my_fs0, ht, tab, y0,
+            [&](int j, uint32_t e, double2 v) {
+                const double2 u = cmulc(v, twist_at<LOGM>(tws, j, e));
+                my_acc[e] = offset_add(my_acc[e], centred_residue(u.x * f.inv_m, f), lo_b, hi_b, Qs);
+                my_acc[e + M] = offset_add(my_acc[e + M], centred_residue(u.y * f.inv_m, f), lo_b, hi_b, Qs);
+            },
+            half_bar);
+    }
+    __syncthreads();
+
+    // finalize and the MV split, as in the one-bit form
+    for (uint32_t i = tid; i < N; i += T) {
+        const int64_t* y = reinterpret_cast<const int64_t*>(acc);
+        const int64_t c0 = y[i] - static_cast<int64_t>(round_c), c1 = y[N + i] - static_cast<int64_t>(round_c);
+        const uint64_t x0 = static_cast<uint64_t>(c0 < 0 ? c0 + Qs : c0);
+        const uint64_t x1 = static_cast<uint64_t>(c1 < 0 ? c1 + Qs : c1);
+        acc[i] = mul_shoup(x0, a.t.n_inv, a.t.n_inv_s, Q);
+        uint64_t v = mul_shoup(x1, a.t.n_inv, a.t.n_inv_s, Q);
+        if (i < a.num_lut) v = add_mod(v, a.gadd[i], Q);
+        acc[N + i] = v;
+    }
+    __syncthreads();
+    for (uint32_t j = 0; j < a.num_lut; ++j) {
+        for (uint32_t p = 0; p < 2; ++p) {
+            const uint64_t* src = acc + p * N;
+            uint64_t* dst = a.mv_out + ((static_cast<size_t>(ct) * a.num_lut + j) * 2 + p) * N;
+            for (uint32_t i = tid; i < N; i += T) {
+                const uint32_t s = i + j;
+                dst[i] = (s < N) ? src[s] : (src[s - N] ? Q - src[s - N] : 0);
+            }
+        }
+    }
+}
+
 cudaError_t ntt_forward(uint64_t* out, const uint64_t* in, const uint64_t* tw, const uint64_t* tws,
                         const cbs_dmodulus* mod, size_t dim, size_t batch, cudaStream_t s);
 
@@ -519,8 +696,35 @@ static cudaError_t br_fft_mb_launch(const BlindRotateArgs& a, const FftKeyArgs& 
     return cudaGetLastError();
 }
 
+template <int LOGN, int MB, bool WIDE>
+static cudaError_t br_fft_mb_d2_launch(const BlindRotateArgs& a, const FftKeyArgs& f, uint32_t batch,
+                                       cudaStream_t s) {
+    constexpr uint32_t N = 1u << LOGN, M = N / 2;
+    const size_t smem = 2ull * N * sizeof(uint64_t) + (4ull * M + FftTab<LOGN - 1>::size()) * sizeof(double2) +
+                        4ull * M * sizeof(typename DigitPair<WIDE>::T) + MB * 8ull * BrFftCfg<LOGN>::T * sizeof(double2);
+    if (f.tab_len != FftTab<LOGN - 1>::size()) return cudaErrorInvalidValue;
+    static size_t configured[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (configured[dev] < smem) {
+        cudaError_t e = cudaFuncSetAttribute(k_blind_rotate_fft_mb_d2<LOGN, MB, WIDE>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+        if (e != cudaSuccess) return e;
+        configured[dev] = smem;
+    }
+    k_blind_rotate_fft_mb_d2<LOGN, MB, WIDE><<<batch, BrFftCfg<LOGN>::T, smem, s>>>(a, f);
+    return cudaGetLastError();
+}
+
 template <int LOGN, int MB>
 static cudaError_t br_fft_mb_launch(const BlindRotateArgs& a, const FftKeyArgs& f, uint32_t batch, cudaStream_t s) {
+    if constexpr (MB == 2) {
+        // the two-digit gadget: both digit transforms in lockstep unless the digit-by-digit
+        // schedule was chosen
+        if (a.digits == 2 && a.schedule != CBS_BR_SCHEDULE_DIGITWISE)
+            return wide_digits(a.g.gbits) ? br_fft_mb_d2_launch<LOGN, MB, true>(a, f, batch, s)
+                                          : br_fft_mb_d2_launch<LOGN, MB, false>(a, f, batch, s);
+    }
     return wide_digits(a.g.gbits) ? br_fft_mb_launch<LOGN, MB, true>(a, f, batch, s)
                                   : br_fft_mb_launch<LOGN, MB, false>(a, f, batch, s);
 }

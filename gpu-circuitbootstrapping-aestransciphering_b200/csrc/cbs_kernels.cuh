@@ -37,6 +37,7 @@ struct BlindRotateArgs {
     uint32_t num_lut;
     const uint64_t* gadd;    // [num_lut] (gpow[j] >> 1) * N^-1 mod Q
     uint64_t* mv_out;        // [batch][num_lut][2][N] NTT domain (MV RLWEs after finalize)
+    uint32_t schedule;       // FFT grouped form: CBS_BR_SCHEDULE_* (0 = the tuned / default choice)
 };
 
 struct TraceArgs {

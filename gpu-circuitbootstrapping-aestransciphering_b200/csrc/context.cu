@@ -114,6 +114,21 @@ static cbs_status prepare_mb(cbs_context* c) {
     return upload_mb_spectra(c);
 }
 
+cbs_status apply_tuned_multibit(cbs_context* c) {
+    // the cached grouping applies when the caller chose none and the grouped keys can be made
+    if (!c->has_tuned || c->mb_explicit || c->tuned.mb == c->br_mb || c->br_backend != CBS_BR_FFT64) return CBS_OK;
+    if (c->tuned.mb > 1 && c->keys_ready && !c->has_secret) return CBS_OK;
+    c->br_mb = c->tuned.mb;
+    c->mb_ready = false;
+    c->h_mbk.clear();
+    c->d_bskf_mb.reset();
+    if (c->br_mb > 1 && c->keys_ready) {
+        if (cbs_status st = prepare_mb(c)) return st;
+    }
+    c->aes.drop_graphs();
+    return CBS_OK;
+}
+
 cbs_status run_blind_rotate(cbs_context* c, const uint64_t* d_a, const uint64_t* d_b, uint32_t batch,
                             uint32_t a_stride, uint64_t* d_mv, cudaStream_t s, bool mv_ntt) {
     BlindRotateArgs a{};
@@ -131,6 +146,8 @@ cbs_status run_blind_rotate(cbs_context* c, const uint64_t* d_a, const uint64_t*
     a.num_lut = c->p.num_lut;
     a.gadd = c->d_gadd.p;
     a.mv_out = d_mv;
+    a.schedule = c->br_schedule != CBS_BR_SCHEDULE_AUTO ? c->br_schedule
+                                                          : (c->has_tuned ? c->tuned.schedule : CBS_BR_SCHEDULE_AUTO);
     if (!mv_ntt && c->br_backend != CBS_BR_FFT64) {
         set_error("coefficient-domain MV output needs the FFT backend");
         return CBS_ERR_INVALID_ARG;
@@ -433,6 +450,7 @@ cbs_status cbs_context_create(const cbs_params* params, uint32_t max_batch, cbs_
     CBS_CUDA_TRY(c->d_mv.alloc(static_cast<size_t>(max_batch) * L * 2 * N));
     CBS_CUDA_TRY(c->d_rgsw.alloc(static_cast<size_t>(max_batch) * L * 4 * N));
     CBS_CUDA_TRY(cudaStreamSynchronize(s));
+    c->has_tuned = tune_cache_lookup(c, nullptr, &c->tuned);
     *out = guard.release();
     return CBS_OK;
 }
@@ -557,6 +575,7 @@ cbs_status cbs_import_keys(cbs_context* ctx, const int32_t* s_lwe, const int32_t
 cbs_status cbs_import_mb_bsk(cbs_context* ctx, uint32_t mb, const uint64_t* keys, size_t words) {
     CBS_CHECK_ARG(ctx && keys, "import_mb_bsk: null argument");
     CBS_CHECK_ARG(mb == 2 || mb == 3, "import_mb_bsk: mb must be 2 or 3");
+    ctx->mb_explicit = true;
     if (ctx->br_backend != CBS_BR_FFT64) {
         set_error("import_mb_bsk: grouped blind rotation is implemented for the FFT64 backend");
         return CBS_ERR_UNSUPPORTED;
@@ -584,9 +603,28 @@ cbs_status cbs_import_mb_bsk(cbs_context* ctx, uint32_t mb, const uint64_t* keys
     return upload_mb_spectra(ctx);
 }
 
+cbs_status cbs_context_set_br_schedule(cbs_context* ctx, uint32_t schedule) {
+    CBS_CHECK_ARG(ctx, "set_br_schedule: null context");
+    CBS_CHECK_ARG(schedule <= CBS_BR_SCHEDULE_LOCKSTEP, "set_br_schedule: unknown schedule");
+    ctx->br_schedule = schedule;
+    ctx->aes.drop_graphs();  // captured rounds bake in the kernel choice
+    return CBS_OK;
+}
+
+cbs_status cbs_context_tuned(const cbs_context* ctx, cbs_tune_choice* out) {
+    CBS_CHECK_ARG(ctx && out, "context_tuned: null argument");
+    if (!ctx->has_tuned) {
+        set_error("context_tuned: no tuning-cache entry for this GPU and parameter set");
+        return CBS_ERR_NOT_READY;
+    }
+    *out = ctx->tuned;
+    return CBS_OK;
+}
+
 cbs_status cbs_context_set_br_multibit(cbs_context* ctx, uint32_t mb) {
     CBS_CHECK_ARG(ctx, "set_br_multibit: null context");
     CBS_CHECK_ARG(mb >= 1 && mb <= 3, "set_br_multibit: mb must be 1, 2 or 3");
+    ctx->mb_explicit = true;
     if (mb > 1 && ctx->br_backend != CBS_BR_FFT64) {
         set_error("set_br_multibit: grouped blind rotation is implemented for the FFT64 backend");
         return CBS_ERR_UNSUPPORTED;
@@ -626,6 +664,9 @@ cbs_status cbs_context_set_br_backend(cbs_context* ctx, int backend) {
         if (cbs_status st = prepare_fft(ctx)) return st;
     }
     ctx->br_backend = backend;
+    if (backend == CBS_BR_FFT64) {
+        if (cbs_status st = apply_tuned_multibit(ctx)) return st;
+    }
     if (backend != CBS_BR_FFT64 && ctx->br_mb > 1) {  // grouped keys exist for the FFT form only
         ctx->br_mb = 1;
         ctx->mb_ready = false;
@@ -784,6 +825,34 @@ cbs_status cbs_circuit_bootstrap_batch_device(cbs_context* ctx, const uint64_t* 
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     if (cbs_status st = run_cbs(ctx, d_a, d_b, batch, a_stride, ctx->d_mv.p, ctx->d_rgsw.p, s)) return st;
     *d_rgsw_view = ctx->d_rgsw.p;
+    return CBS_OK;
+}
+
+cbs_status cbs_circuit_bootstrap_batch(cbs_context* ctx, const uint64_t* h_a, const uint64_t* h_b, uint32_t batch,
+                                       uint32_t a_stride, uint64_t* h_rgsw_out) {
+    CBS_CHECK_ARG(ctx, "cbs_host: null context");
+    if (batch == 0) return CBS_OK;
+    CBS_CHECK_ARG(h_a && h_b && h_rgsw_out, "cbs_host: null pointer");
+    CBS_CHECK_ARG(a_stride >= ctx->p.n, "cbs_host: a_stride < n");
+    if (batch > ctx->max_batch) {
+        set_error("cbs_host: batch exceeds the context's max_batch (recreate the context)");
+        return CBS_ERR_SHAPE_MISMATCH;
+    }
+    const uint64_t q = ctx->p.q_lwe;
+    for (size_t i = 0; i < static_cast<size_t>(batch); ++i) {
+        CBS_CHECK_ARG(h_b[i] < q, "cbs_host: LWE b entries must be below q_lwe");
+        for (uint32_t j = 0; j < ctx->p.n; ++j)
+            CBS_CHECK_ARG(h_a[i * a_stride + j] < q, "cbs_host: LWE a entries must be below q_lwe");
+    }
+    if (cbs_status st = need_keys(ctx)) return st;
+    cudaStream_t s = ctx->stream;
+    DevBuf<uint64_t> d_a, d_b;
+    CBS_CUDA_TRY(d_a.upload(h_a, static_cast<size_t>(batch) * a_stride, s));
+    CBS_CUDA_TRY(d_b.upload(h_b, batch, s));
+    if (cbs_status st = run_cbs(ctx, d_a.p, d_b.p, batch, a_stride, ctx->d_mv.p, ctx->d_rgsw.p, s)) return st;
+    const size_t words = static_cast<size_t>(batch) * ctx->p.num_lut * 4 * ctx->p.N;
+    CBS_CUDA_TRY(cudaMemcpyAsync(h_rgsw_out, ctx->d_rgsw.p, words * sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+    CBS_CUDA_TRY(cudaStreamSynchronize(s));
     return CBS_OK;
 }
 

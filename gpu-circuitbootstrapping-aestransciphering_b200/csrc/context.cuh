@@ -83,6 +83,10 @@ struct cbs_context {
     cbs::DevBuf<double2> d_htf, d_ssf;  // HomTrace / SchemeSwitch key spectra
     // multi-bit blind rotation (FFT backend): 1 = one coefficient per step, 2 or 3 = grouped
     uint32_t br_mb = 1;
+    bool mb_explicit = false;            // mb chosen by the caller (not by the tuning cache)
+    uint32_t br_schedule = 0;            // CBS_BR_SCHEDULE_*
+    bool has_tuned = false;              // a tuning-cache entry for this GPU and parameter set
+    cbs_tune_choice tuned{};
     bool mb_ready = false;
     uint64_t key_seed = 0;
     std::vector<uint64_t> h_mbk;         // grouped keys, NTT domain (kept for export)
@@ -117,6 +121,11 @@ namespace cbs {
 cbs_status run_blind_rotate(cbs_context* c, const uint64_t* d_a, const uint64_t* d_b, uint32_t batch,
                             uint32_t a_stride, uint64_t* d_mv, cudaStream_t s, bool mv_ntt = true);
 FftKeyArgs fft_key_args(const cbs_context* c);
+// the tuning cache (tune.cu): the entry for this context's GPU and parameter set, if any
+bool tune_cache_lookup(const cbs_context* c, const char* path, cbs_tune_choice* out);
+// on the FFT64 backend, switch to the tuning cache's grouping unless the caller chose one (grouped
+// keys are generated from the secret key; without it the grouping stays as it is)
+cbs_status apply_tuned_multibit(cbs_context* c);
 // blind rotation + HomTrace/SchemeSwitch of the selected backend: LWE -> RGSW rows in the
 // NTT-domain reference layout [batch][num_lut][2][2][N]; d_mv is [batch][num_lut][2][N] scratch
 // FFT HomTrace + SchemeSwitch with the rows converted to the NTT-domain reference layout

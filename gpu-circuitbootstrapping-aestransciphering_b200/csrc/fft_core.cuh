@@ -353,6 +353,56 @@ __device__ __forceinline__ void fft_forward_to_regs(C* sm, uint32_t tid, const C
     }
 }
 
+// Two independent forward FFTs in lockstep (the same M/8 threads, separate exchange buffers
+// sm0 / sm1): each pass's butterflies of both transforms interleave, which doubles the
+// independent FP64 work between exchanges, and the two transforms share every barrier.
+template <int LOGM, class Load0, class Load1, class Bar, class C>
+__device__ __forceinline__ void fft_forward2_to_regs(C* sm0, C* sm1, uint32_t tid, const C* tab, Load0 load0,
+                                                     Load1 load1, C (&x0)[8], C (&x1)[8], Bar bar) {
+    using Pl = NttPlan<LOGM>;
+    using Tb = FftTab<LOGM>;
+    static_assert(Pl::P >= 2, "fft needs M >= 64");
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        const uint32_t e = pass_index<LOGM, 3>(1u, tid, j);
+        x0[j] = load0(j, e);
+        x1[j] = load1(j, e);
+    }
+    dif_pass<LOGM, 3, false>(x0, 1u, tid, tab);
+    dif_pass<LOGM, 3, false>(x1, 1u, tid, tab);
+#pragma unroll
+    for (int p = 1; p < Pl::P; ++p) {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const uint32_t e = cswz_of<C>(pass_index<LOGM, 3>(1u << (3 * (p - 1)), tid, j));
+            sm0[e] = x0[j];
+            sm1[e] = x1[j];
+        }
+        if (fwd_exchange_in_warp<LOGM>(p)) __syncwarp();
+        else bar();
+        const uint32_t m = 1u << (3 * p);
+        if (p < Pl::P - 1) {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const uint32_t e = cswz_of<C>(pass_index<LOGM, 3>(m, tid, j));
+                x0[j] = sm0[e];
+                x1[j] = sm1[e];
+            }
+            dif_pass<LOGM, 3, true>(x0, m, tid, tab + Tb::pass_off(p));
+            dif_pass<LOGM, 3, true>(x1, m, tid, tab + Tb::pass_off(p));
+        } else {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const uint32_t e = cswz_of<C>(pass_index<LOGM, Pl::tail_r>(m, tid, j));
+                x0[j] = sm0[e];
+                x1[j] = sm1[e];
+            }
+            dif_pass<LOGM, Pl::tail_r, true>(x0, m, tid, tab + Tb::pass_off(p));
+            dif_pass<LOGM, Pl::tail_r, true>(x1, m, tid, tab + Tb::pass_off(p));
+        }
+    }
+}
+
 // Inverse FFT (without the 1/M factor) from the thread's spectrum slots 8*tid + j in x;
 // store(j, e, v) receives element e < M in natural order (register slot j, a compile-time
 // constant after unrolling, so callers can keep per-slot results in registers).  Same

@@ -160,6 +160,38 @@ cbs_status cbs_context_set_br_backend(cbs_context *ctx, int backend);
  * exist or are next generated.  mb > 1 needs the FFT64 backend (CBS_ERR_UNSUPPORTED
  * otherwise); selecting the NTT backend resets mb to 1. */
 cbs_status cbs_context_set_br_multibit(cbs_context *ctx, uint32_t mb);
+/* Schedule of the grouped FFT blind rotation with a two-digit gadget: CBS_BR_SCHEDULE_LOCKSTEP
+ * transforms both digits of a polynomial together (interleaved butterflies, shared barriers),
+ * CBS_BR_SCHEDULE_DIGITWISE one after the other; CBS_BR_SCHEDULE_AUTO (default) takes the
+ * autotuner's cached choice for this GPU and parameter set, else lockstep.  Results differ only
+ * by FP64 rounding (both within the phase-error bound).  No reference counterpart. */
+enum { CBS_BR_SCHEDULE_AUTO = 0, CBS_BR_SCHEDULE_DIGITWISE = 1, CBS_BR_SCHEDULE_LOCKSTEP = 2 };
+cbs_status cbs_context_set_br_schedule(cbs_context *ctx, uint32_t schedule);
+
+/* Autotuner of the blind rotation (no reference counterpart: the reference exposes ~70
+ * environment knobs, examples/aes_transcipher/main.cu:107-136, and times three block sizes
+ * inline, bitwise/src/cirbts/cirbts-batch.cu:2410-2460).  On the FFT64 backend it times the
+ * blind rotation of `batch` synthetic LWE ciphertexts (CUDA events on the context's stream, one
+ * warm-up and two timed launches per candidate) for every grouping mb in {1, 2, 3} and, where
+ * it applies, both schedules; grouped keys need the secret key (without it only the current mb
+ * is timed).  The fastest is applied to the context and stored in the tuning cache under (GPU
+ * name, parameter set, batch rounded up to a power of two): cache_path, or NULL for
+ * $CBS_TUNE_CACHE, else $XDG_CACHE_HOME/cbs_b200/tune.json, else $HOME/.cache/cbs_b200/tune.json.
+ * cbs_context_create reads the cache: a context whose mb was not set explicitly takes the
+ * cached grouping when the FFT64 backend is selected, and its schedule at launch.
+ * Synchronous; allocates; not for use inside a stream capture. */
+typedef struct {
+    uint32_t mb;             /* grouping of the blind rotation (1, 2 or 3) */
+    uint32_t schedule;       /* CBS_BR_SCHEDULE_DIGITWISE or CBS_BR_SCHEDULE_LOCKSTEP */
+    double us_per_bootstrap; /* measured at the tuned batch */
+    uint32_t batch;          /* the batch the choice was measured at */
+    uint32_t candidates;     /* configurations timed */
+} cbs_tune_choice;
+cbs_status cbs_autotune_blind_rotation(cbs_context *ctx, uint32_t batch, const char *cache_path, cbs_tune_choice *out);
+/* The choice the context holds (from its cache read at creation or the last autotune);
+ * CBS_ERR_NOT_READY when there is none. */
+cbs_status cbs_context_tuned(const cbs_context *ctx, cbs_tune_choice *out);
+
 /* The grouped keys of the current setting, NTT domain, for inspection and tests:
  * out [ceil(n/mb)][2^mb - 1][2*digits_g][2][N] (null out: only *words is set), subsets in
  * the order {0} {1} {2} {0,1} {0,2} {1,2} {0,1,2} (mb = 3) or {0} {1} {0,1} (mb = 2). */
@@ -223,6 +255,14 @@ cbs_status cbs_trace_schemeswitch_device(cbs_context *ctx, const uint64_t *d_mv,
 cbs_status cbs_circuit_bootstrap_batch_device(cbs_context *ctx, const uint64_t *d_a, const uint64_t *d_b,
                                               uint32_t batch, uint32_t a_stride, const uint64_t **d_rgsw_view,
                                               cbs_stream_t stream);
+
+/* Host-buffer circuit bootstrapping (replaces gpu_CircuitBootstrappingBatch, cirbts-batch.cu:81,
+ * and gpu_CircuitBootstrapping, cirbts-bootstrap.cu:89, whose OpenFHE LWECiphertext vectors
+ * become plain arrays): h_a [batch][a_stride], h_b [batch] mod q_lwe (checked) ->
+ * h_rgsw_out [batch][num_lut][2][2][N] (the layout of the device view), on the context's stream,
+ * synchronous. */
+cbs_status cbs_circuit_bootstrap_batch(cbs_context *ctx, const uint64_t *h_a, const uint64_t *h_b, uint32_t batch,
+                                       uint32_t a_stride, uint64_t *h_rgsw_out);
 
 /* Batched 8->32 CMux LUT (replaces EvalLUT8x32_RLWE_GPU_DeviceCtrl_Batch,
  * examples/aes_transcipher/gpu_lut.cuh:1783-2214): d_tables [tables][256][2][N] NTT domain,

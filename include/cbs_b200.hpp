@@ -6,16 +6,21 @@
 //   * GPUCirBTSContext (bitwise/include/cirbts/cirbts.cuh:420-498): construction from
 //     parameters + max batch, the device-LWE circuit-bootstrapping entry point returning a
 //     non-owning DeviceRGSWBatchView, the NTT-table accessors and stream();
-//   * the example's LUT and extraction helpers (gpu_lut.cuh:1783, extract.cuh:283).
+//   * the host-input CBS entry points (cirbts.cuh:454-462) on plain LWE / RGSW structs;
+//   * Phantom's key-switching types (EncryptionParameters, PhantomContext, PhantomCiphertext,
+//     PhantomRelinKey) and keyswitch_inplace (src/eval_key_switch.cu:94), CKKS form;
+//   * GPUBinFHEContext::BatchGPUEvalBinGate (bitwise/include/binfhecontext.cuh:53-57).
 // Errors surface as exceptions on this side (like OPENFHE_THROW / PHANTOM_CHECK_CUDA in the
 // reference); the C ABI underneath never throws.
 #pragma once
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <stdexcept>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "cbs_b200.h"
@@ -69,6 +74,56 @@ inline void inwt_1d_opt_permute_batched(uint64_t* out, const uint64_t* in, const
                                           batch, as_stream(stream)),
           "inwt_1d_opt_permute_batched");
 }
+
+inline void check_cuda(cudaError_t e, const char* where) {
+    if (e != cudaSuccess) throw std::runtime_error(std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+// Owning device array (the role of phantom::util::cuda_auto_ptr, include/cuda_wrapper.cuh:90):
+// grows on resize, contents not preserved.
+template <class T>
+class DeviceArray {
+   public:
+    DeviceArray() = default;
+    explicit DeviceArray(size_t n) { resize(n); }
+    DeviceArray(const DeviceArray&) = delete;
+    DeviceArray& operator=(const DeviceArray&) = delete;
+    DeviceArray(DeviceArray&& o) noexcept : p_(o.p_), n_(o.n_) { o.p_ = nullptr, o.n_ = 0; }
+    DeviceArray& operator=(DeviceArray&& o) noexcept {
+        std::swap(p_, o.p_);
+        std::swap(n_, o.n_);
+        return *this;
+    }
+    ~DeviceArray() { cudaFree(p_); }
+    void resize(size_t n) {
+        if (n <= n_) return;
+        cudaFree(p_);
+        p_ = nullptr;
+        n_ = 0;
+        check_cuda(cudaMalloc(reinterpret_cast<void**>(&p_), n * sizeof(T)), "DeviceArray");
+        n_ = n;
+    }
+    [[nodiscard]] T* data() const { return p_; }
+    [[nodiscard]] size_t size() const { return n_; }
+
+   private:
+    T* p_ = nullptr;
+    size_t n_ = 0;
+};
+
+// The OpenFHE ciphertext types of the reference's CBS and gate interfaces as plain structs:
+// an LWE ciphertext (a[n], b mod q; lbcrypto::LWECiphertextImpl) and the host copy of one
+// bit's RGSW rows [digitsCC * 2 rows][2 polys][N] (NTT domain; RGSWCiphertext of cirbts.cuh).
+struct LWECiphertext {
+    std::vector<uint64_t> a;
+    uint64_t b = 0;
+    uint64_t q = 0;
+};
+struct RGSWCiphertext {
+    std::vector<uint64_t> data;
+    uint32_t digitsCC = 0;
+    uint32_t N = 0;
+};
 
 // ---- GPUCirBTSContext (bitwise/include/cirbts/cirbts.cuh:31-500) ----
 class GPUCirBTSContext {
@@ -127,10 +182,59 @@ class GPUCirBTSContext {
         return v;
     }
 
+    // cirbts.cuh:462 gpu_CircuitBootstrappingBatchToDevice(params, ek, vector<LWECiphertext>): host
+    // LWE ciphertexts staged to the device, then the device-LWE entry point
+    [[nodiscard]] DeviceRGSWBatchView gpu_CircuitBootstrappingBatchToDevice(const std::vector<LWECiphertext>& cts) {
+        if (cts.empty()) return {};
+        const uint32_t n = params_.n, batch = static_cast<uint32_t>(cts.size());
+        std::vector<uint64_t> a, b;
+        pack(cts, a, b);
+        stage_.resize(a.size() + b.size());
+        const cudaStream_t s = stream();
+        check_cuda(cudaMemcpyAsync(stage_.data(), a.data(), a.size() * 8, cudaMemcpyHostToDevice, s), "stage a");
+        check_cuda(cudaMemcpyAsync(stage_.data() + a.size(), b.data(), b.size() * 8, cudaMemcpyHostToDevice, s),
+                   "stage b");
+        return gpu_CircuitBootstrappingBatchToDeviceFromDeviceLWE(stage_.data(), stage_.data() + a.size(), batch, n);
+    }
+    // cirbts.cuh:458 gpu_CircuitBootstrappingBatch(params, ek, vector<LWECiphertext>): host RGSWs out
+    [[nodiscard]] std::vector<RGSWCiphertext> gpu_CircuitBootstrappingBatch(const std::vector<LWECiphertext>& cts) {
+        std::vector<RGSWCiphertext> out;
+        if (cts.empty()) return out;
+        std::vector<uint64_t> a, b;
+        pack(cts, a, b);
+        const size_t per = static_cast<size_t>(params_.num_lut) * 4 * params_.N;
+        std::vector<uint64_t> rg(per * cts.size());
+        check(cbs_circuit_bootstrap_batch(ctx_, a.data(), b.data(), static_cast<uint32_t>(cts.size()), params_.n,
+                                          rg.data()),
+              "gpu_CircuitBootstrappingBatch");
+        out.resize(cts.size());
+        for (size_t i = 0; i < cts.size(); ++i) {
+            out[i].digitsCC = params_.num_lut;
+            out[i].N = params_.N;
+            out[i].data.assign(rg.begin() + i * per, rg.begin() + (i + 1) * per);
+        }
+        return out;
+    }
+    // cirbts.cuh:454 gpu_CircuitBootstrapping(params, ek, ct)
+    [[nodiscard]] RGSWCiphertext gpu_CircuitBootstrapping(const LWECiphertext& ct) {
+        return gpu_CircuitBootstrappingBatch(std::vector<LWECiphertext>{ct}).front();
+    }
+
     [[nodiscard]] cbs_context* handle() const { return ctx_; }
     [[nodiscard]] const cbs_params& params() const { return params_; }
 
    private:
+    void pack(const std::vector<LWECiphertext>& cts, std::vector<uint64_t>& a, std::vector<uint64_t>& b) const {
+        const uint32_t n = params_.n;
+        a.assign(cts.size() * n, 0);
+        b.assign(cts.size(), 0);
+        for (size_t i = 0; i < cts.size(); ++i) {
+            if (cts[i].a.size() != n || cts[i].q != params_.q_lwe)
+                throw Error(CBS_ERR_SHAPE_MISMATCH, "LWECiphertext: dimension or modulus differs from the context's");
+            std::copy(cts[i].a.begin(), cts[i].a.end(), a.begin() + i * n);
+            b[i] = cts[i].b;
+        }
+    }
     const cbs_dmodulus* table(int) const {
         const cbs_dmodulus* m = nullptr;
         check(cbs_context_tables(ctx_, &m, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr), "tables");
@@ -144,6 +248,7 @@ class GPUCirBTSContext {
     cbs_params params_;
     uint32_t max_batch_;
     cbs_context* ctx_ = nullptr;
+    DeviceArray<uint64_t> stage_;
 };
 
 // ---- Phantom RNS core (include/context.cuh:161, include/ntt.cuh:232-262,
@@ -189,6 +294,216 @@ class RnsContext {
    private:
     uint32_t size_q_, size_p_;
     cbs_rns_context* ctx_ = nullptr;
+};
+
+// ---- Phantom's C++ types for the key-switching path (include/host/encryptionparams.h:37,
+//      include/context.cuh:161, include/ciphertext.cuh:8, include/secretkey.h:101,
+//      src/eval_key_switch.cu:94) ----
+namespace phantom {
+// scheme_type of include/host/encryptionparams.h:14 (the key-switching path here is the CKKS form)
+enum class scheme_type : std::uint8_t { scheme_none = 0x0, bfv = 0x1, ckks = 0x2, bgv = 0x3 };
+
+// The parameters PhantomContext is built from: ring degree, the key modulus chain (the primes of
+// Q followed by the special primes P, as Phantom's coeff_modulus holds them) and the number of
+// special primes.  arith::Modulus becomes its value.
+class EncryptionParameters {
+   public:
+    explicit EncryptionParameters(scheme_type scheme = scheme_type::scheme_none) : scheme_(scheme) {}
+    void set_poly_modulus_degree(std::size_t n) { poly_modulus_degree_ = n; }
+    void set_coeff_modulus(const std::vector<uint64_t>& coeff_modulus) { coeff_modulus_ = coeff_modulus; }
+    void set_special_modulus_size(std::size_t size_p) { special_modulus_size_ = size_p; }
+    [[nodiscard]] scheme_type scheme() const noexcept { return scheme_; }
+    [[nodiscard]] std::size_t poly_modulus_degree() const noexcept { return poly_modulus_degree_; }
+    [[nodiscard]] const std::vector<uint64_t>& coeff_modulus() const noexcept { return coeff_modulus_; }
+    [[nodiscard]] std::size_t special_modulus_size() const noexcept { return special_modulus_size_; }
+
+   private:
+    scheme_type scheme_;
+    std::size_t poly_modulus_degree_ = 0;
+    std::vector<uint64_t> coeff_modulus_;
+    std::size_t special_modulus_size_ = 1;
+};
+}  // namespace phantom
+
+// PhantomContext: the chain's device tables and the modup / moddown constants.  Chain index c
+// (c >= 1) is the level with size_Q - (c - 1) primes of Q, as in Phantom (index 0 = the key level).
+class PhantomContext {
+   public:
+    explicit PhantomContext(const phantom::EncryptionParameters& params)
+        : scheme_(params.scheme()), poly_degree_(params.poly_modulus_degree()) {
+        if (scheme_ != phantom::scheme_type::ckks)
+            throw Error(CBS_ERR_UNSUPPORTED, "PhantomContext: the key-switching path is built for CKKS");
+        const auto& chain = params.coeff_modulus();
+        const size_t size_p = params.special_modulus_size();
+        if (size_p == 0 || chain.size() <= size_p) throw Error(CBS_ERR_INVALID_ARG, "PhantomContext: bad chain");
+        q_.assign(chain.begin(), chain.end() - static_cast<std::ptrdiff_t>(size_p));
+        p_.assign(chain.end() - static_cast<std::ptrdiff_t>(size_p), chain.end());
+        check(cbs_rns_context_create(static_cast<uint32_t>(poly_degree_), q_.data(), static_cast<uint32_t>(q_.size()),
+                                     p_.data(), static_cast<uint32_t>(p_.size()), &ctx_),
+              "PhantomContext");
+        coeff_mod_size_ = chain.size();
+    }
+    PhantomContext(const PhantomContext&) = delete;
+    void operator=(const PhantomContext&) = delete;
+    ~PhantomContext() { cbs_rns_context_destroy(ctx_); }
+
+    [[nodiscard]] cbs_rns_ntt_tables gpu_rns_tables() const {
+        cbs_rns_ntt_tables t{};
+        check(cbs_rns_context_tables(ctx_, &t), "gpu_rns_tables");
+        return t;
+    }
+    // limbs of Q at chain index c
+    [[nodiscard]] size_t coeff_modulus_size(size_t chain_index) const {
+        if (chain_index < 1 || chain_index > q_.size())
+            throw Error(CBS_ERR_INVALID_ARG, "PhantomContext: chain index out of range");
+        return q_.size() - (chain_index - 1);
+    }
+    [[nodiscard]] phantom::scheme_type scheme() const { return scheme_; }
+    [[nodiscard]] size_t poly_degree() const { return poly_degree_; }
+    [[nodiscard]] size_t coeff_mod_size() const { return coeff_mod_size_; }
+    [[nodiscard]] size_t special_modulus_size() const { return p_.size(); }
+    [[nodiscard]] cbs_rns_context* handle() const { return ctx_; }
+
+   private:
+    phantom::scheme_type scheme_;
+    size_t poly_degree_ = 0, coeff_mod_size_ = 0;
+    std::vector<uint64_t> q_, p_;
+    cbs_rns_context* ctx_ = nullptr;
+};
+
+// PhantomCiphertext: size polynomials of coeff_modulus_size limbs, NTT form, device resident
+// ([size][coeff_modulus_size][N] words).
+class PhantomCiphertext {
+   public:
+    PhantomCiphertext() = default;
+    void resize(const PhantomContext& context, size_t chain_index, size_t size, const cudaStream_t&) {
+        chain_index_ = chain_index;
+        size_ = size;
+        coeff_modulus_size_ = context.coeff_modulus_size(chain_index);
+        poly_modulus_degree_ = context.poly_degree();
+        data_.resize(size_ * coeff_modulus_size_ * poly_modulus_degree_);
+    }
+    [[nodiscard]] uint64_t* data() const { return data_.data(); }
+    [[nodiscard]] size_t size() const { return size_; }
+    [[nodiscard]] size_t chain_index() const { return chain_index_; }
+    [[nodiscard]] size_t coeff_modulus_size() const { return coeff_modulus_size_; }
+    [[nodiscard]] size_t poly_modulus_degree() const { return poly_modulus_degree_; }
+    [[nodiscard]] bool is_ntt_form() const { return is_ntt_form_; }
+
+   private:
+    size_t size_ = 0, chain_index_ = 0, coeff_modulus_size_ = 0, poly_modulus_degree_ = 0;
+    bool is_ntt_form_ = true;
+    DeviceArray<uint64_t> data_;
+};
+
+// PhantomRelinKey: beta switching keys, one per digit, each [2][size_Q + size_P][N] on the device;
+// public_keys_ptr() lists them (host array of device pointers here, a device array in Phantom).
+class PhantomRelinKey {
+   public:
+    PhantomRelinKey() = default;
+    // host keys [beta][2][size_Q + size_P][N], uploaded
+    PhantomRelinKey(const PhantomContext& context, const std::vector<uint64_t>& keys, size_t beta) {
+        const size_t per = 2 * context.coeff_mod_size() * context.poly_degree();
+        if (keys.size() != beta * per) throw Error(CBS_ERR_SHAPE_MISMATCH, "PhantomRelinKey: key size");
+        data_.resize(keys.size());
+        check_cuda(cudaMemcpy(data_.data(), keys.data(), keys.size() * 8, cudaMemcpyHostToDevice), "PhantomRelinKey");
+        for (size_t b = 0; b < beta; ++b) ptrs_.push_back(data_.data() + b * per);
+    }
+    PhantomRelinKey(const PhantomRelinKey&) = delete;
+    PhantomRelinKey& operator=(const PhantomRelinKey&) = delete;
+    PhantomRelinKey(PhantomRelinKey&&) = default;
+    PhantomRelinKey& operator=(PhantomRelinKey&&) = default;
+    [[nodiscard]] const uint64_t* const* public_keys_ptr() const { return ptrs_.data(); }
+    [[nodiscard]] size_t dnum() const { return ptrs_.size(); }
+
+   private:
+    DeviceArray<uint64_t> data_;
+    std::vector<const uint64_t*> ptrs_;
+};
+
+// keyswitch_inplace (src/eval_key_switch.cu:94-181), CKKS: encrypted (size >= 2 polys at chain
+// index c, size_Ql = its coeff_modulus_size limbs) += keyswitch(c2 [size_Ql][N]) with the relin
+// keys' digits; is_relin only changes the reference's BFV level choice and is accepted for shape.
+inline void keyswitch_inplace(const PhantomContext& context, PhantomCiphertext& encrypted, uint64_t* c2,
+                              const PhantomRelinKey& relin_keys, bool is_relin, const cudaStream_t& stream) {
+    (void)is_relin;
+    if (context.scheme() != phantom::scheme_type::ckks)
+        throw Error(CBS_ERR_UNSUPPORTED, "keyswitch_inplace: unsupported scheme in keyswitch_inplace");
+    const uint32_t size_ql = static_cast<uint32_t>(encrypted.coeff_modulus_size());
+    check(cbs_rns_keyswitch_inplace(context.handle(), encrypted.data(), c2, relin_keys.public_keys_ptr(), size_ql, 1,
+                                    as_stream(stream)),
+          "keyswitch_inplace");
+}
+
+// ---- GPUBinFHEContext (bitwise/include/binfhecontext.cuh:8-118): gate bootstrapping on the
+//      32-bit torus (LWECiphertext::q = 2^32) ----
+enum BINGATE { OR = CBS_GATE_OR, AND = CBS_GATE_AND, NOR = CBS_GATE_NOR, NAND = CBS_GATE_NAND, XOR = CBS_GATE_XOR,
+               XNOR = CBS_GATE_XNOR };
+
+class GPUBinFHEContext {
+   public:
+    explicit GPUBinFHEContext(const cbs_gate_params& params, uint32_t max_batch = 1024)
+        : params_(params), max_batch_(max_batch) {
+        check(cbs_gate_context_create(&params_, max_batch_, &ctx_), "GPUBinFHEContext");
+    }
+    GPUBinFHEContext(const GPUBinFHEContext&) = delete;
+    GPUBinFHEContext& operator=(const GPUBinFHEContext&) = delete;
+    ~GPUBinFHEContext() { cbs_gate_context_destroy(ctx_); }
+
+    // GPUBTKeyGen (binfhecontext.cuh:38), from a seed
+    void GPUBTKeyGen(uint64_t seed) { check(cbs_gate_keygen(ctx_, seed), "GPUBTKeyGen"); }
+
+    // binfhecontext.cuh:53-57
+    [[nodiscard]] std::vector<LWECiphertext> BatchGPUEvalBinGate(BINGATE gate, const std::vector<LWECiphertext>& v_ct1,
+                                                                 const std::vector<LWECiphertext>& v_ct2,
+                                                                 const cudaStream_t& stream = nullptr) {
+        if (v_ct1.size() != v_ct2.size()) throw Error(CBS_ERR_SHAPE_MISMATCH, "BatchGPUEvalBinGate: batch sizes");
+        const size_t count = v_ct1.size(), n = params_.n;
+        std::vector<LWECiphertext> out(count);
+        if (!count) return out;
+        if (count > max_batch_) throw Error(CBS_ERR_SHAPE_MISMATCH, "BatchGPUEvalBinGate: batch above max_batch");
+        std::vector<uint32_t> a1(count * n), b1(count), a2(count * n), b2(count);
+        auto put = [&](const std::vector<LWECiphertext>& v, std::vector<uint32_t>& a, std::vector<uint32_t>& b) {
+            for (size_t i = 0; i < count; ++i) {
+                if (v[i].a.size() != n || v[i].q != (uint64_t(1) << 32))
+                    throw Error(CBS_ERR_SHAPE_MISMATCH, "BatchGPUEvalBinGate: dimension or modulus");
+                for (size_t j = 0; j < n; ++j) a[i * n + j] = static_cast<uint32_t>(v[i].a[j]);
+                b[i] = static_cast<uint32_t>(v[i].b);
+            }
+        };
+        put(v_ct1, a1, b1);
+        put(v_ct2, a2, b2);
+        const size_t words = 3 * (count * n + count);  // in1, in2, out
+        dev_.resize(words);
+        uint32_t* d = dev_.data();
+        uint32_t *da1 = d, *db1 = da1 + count * n, *da2 = db1 + count, *db2 = da2 + count * n, *doa = db2 + count,
+                 *dob = doa + count * n;
+        check_cuda(cudaMemcpyAsync(da1, a1.data(), a1.size() * 4, cudaMemcpyHostToDevice, stream), "in1 a");
+        check_cuda(cudaMemcpyAsync(db1, b1.data(), b1.size() * 4, cudaMemcpyHostToDevice, stream), "in1 b");
+        check_cuda(cudaMemcpyAsync(da2, a2.data(), a2.size() * 4, cudaMemcpyHostToDevice, stream), "in2 a");
+        check_cuda(cudaMemcpyAsync(db2, b2.data(), b2.size() * 4, cudaMemcpyHostToDevice, stream), "in2 b");
+        check(cbs_gate_eval_batch_device(ctx_, static_cast<int>(gate), da1, db1, da2, db2, static_cast<uint32_t>(count),
+                                         doa, dob, as_stream(stream)),
+              "BatchGPUEvalBinGate");
+        std::vector<uint32_t> oa(count * n), ob(count);
+        check_cuda(cudaMemcpyAsync(oa.data(), doa, oa.size() * 4, cudaMemcpyDeviceToHost, stream), "out a");
+        check_cuda(cudaMemcpyAsync(ob.data(), dob, ob.size() * 4, cudaMemcpyDeviceToHost, stream), "out b");
+        check_cuda(cudaStreamSynchronize(stream), "BatchGPUEvalBinGate");
+        for (size_t i = 0; i < count; ++i) {
+            out[i].a.assign(oa.begin() + i * n, oa.begin() + (i + 1) * n);
+            out[i].b = ob[i];
+            out[i].q = uint64_t(1) << 32;
+        }
+        return out;
+    }
+    [[nodiscard]] cbs_gate_context* handle() const { return ctx_; }
+    [[nodiscard]] const cbs_gate_params& params() const { return params_; }
+
+   private:
+    cbs_gate_params params_;
+    uint32_t max_batch_;
+    cbs_gate_context* ctx_ = nullptr;
+    DeviceArray<uint32_t> dev_;
 };
 
 }  // namespace cbs_b200

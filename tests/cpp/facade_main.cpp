@@ -1,0 +1,158 @@
+// A C++ caller of the reference-shaped facade (include/cbs_b200.hpp) linked against
+// libcbs_b200.so: the program a Phantom / CirBTS user would write, run by
+// tests/test_cpp_facade_gpu.py, which supplies the inputs and checks the outputs against the
+// oracle.  Modes (argv[1]), files in the directory argv[2]:
+//   ks    keyswitch_inplace through EncryptionParameters / PhantomContext / PhantomCiphertext /
+//         PhantomRelinKey: ks_dims (N size_q size_p chain_index beta), ks_chain, ks_c2, ks_ct,
+//         ks_evk -> ks_out
+//   cbs   GPUCirBTSContext: KeyGen(seed), gpu_CircuitBootstrappingBatch, gpu_CircuitBootstrapping and
+//         gpu_CircuitBootstrappingBatchToDevice on host LWE ciphertexts: cbs_dims (seed batch),
+//         cbs_a, cbs_b -> cbs_out (the batch's RGSW rows)
+//   gate  GPUBinFHEContext::BatchGPUEvalBinGate(NAND): exit status 0 when every gate decrypts to
+//         the truth table
+#include <cstdio>
+#include <fstream>
+#include <iostream>
+#include <string>
+#include <vector>
+
+#include "cbs_b200.hpp"
+
+using namespace cbs_b200;
+
+template <class T>
+static std::vector<T> read_raw(const std::string& path) {
+    std::ifstream f(path, std::ios::binary | std::ios::ate);
+    if (!f) throw std::runtime_error("cannot open " + path);
+    const std::streamsize bytes = f.tellg();
+    f.seekg(0);
+    std::vector<T> v(static_cast<size_t>(bytes) / sizeof(T));
+    f.read(reinterpret_cast<char*>(v.data()), bytes);
+    return v;
+}
+
+template <class T>
+static void write_raw(const std::string& path, const std::vector<T>& v) {
+    std::ofstream f(path, std::ios::binary);
+    f.write(reinterpret_cast<const char*>(v.data()), static_cast<std::streamsize>(v.size() * sizeof(T)));
+}
+
+static int run_ks(const std::string& dir) {
+    const auto dims = read_raw<uint64_t>(dir + "/ks_dims");
+    const size_t N = dims[0], size_q = dims[1], size_p = dims[2], chain_index = dims[3], beta = dims[4];
+    const auto chain = read_raw<uint64_t>(dir + "/ks_chain");
+    phantom::EncryptionParameters parms(phantom::scheme_type::ckks);
+    parms.set_poly_modulus_degree(N);
+    parms.set_coeff_modulus(chain);
+    parms.set_special_modulus_size(size_p);
+    PhantomContext context(parms);
+    cudaStream_t stream = nullptr;
+    check_cuda(cudaStreamCreate(&stream), "stream");
+    PhantomCiphertext ct;
+    ct.resize(context, chain_index, 2, stream);
+    const size_t size_ql = ct.coeff_modulus_size();
+    if (size_ql != size_q - (chain_index - 1)) return 3;
+    const auto h_ct = read_raw<uint64_t>(dir + "/ks_ct");
+    const auto h_c2 = read_raw<uint64_t>(dir + "/ks_c2");
+    if (h_ct.size() != 2 * size_ql * N || h_c2.size() != size_ql * N) return 4;
+    check_cuda(cudaMemcpy(ct.data(), h_ct.data(), h_ct.size() * 8, cudaMemcpyHostToDevice), "ct in");
+    DeviceArray<uint64_t> c2(h_c2.size());
+    check_cuda(cudaMemcpy(c2.data(), h_c2.data(), h_c2.size() * 8, cudaMemcpyHostToDevice), "c2 in");
+    PhantomRelinKey relin(context, read_raw<uint64_t>(dir + "/ks_evk"), beta);
+    keyswitch_inplace(context, ct, c2.data(), relin, false, stream);
+    std::vector<uint64_t> out(h_ct.size());
+    check_cuda(cudaStreamSynchronize(stream), "sync");
+    check_cuda(cudaMemcpy(out.data(), ct.data(), out.size() * 8, cudaMemcpyDeviceToHost), "ct out");
+    write_raw(dir + "/ks_out", out);
+    cudaStreamDestroy(stream);
+    return 0;
+}
+
+static int run_cbs(const std::string& dir) {
+    const auto dims = read_raw<uint64_t>(dir + "/cbs_dims");
+    const uint64_t seed = dims[0];
+    const uint32_t batch = static_cast<uint32_t>(dims[1]);
+    cbs_params params{};
+    check(cbs_params_default(&params), "params");
+    GPUCirBTSContext cc(params, batch);
+    cc.KeyGen(seed);
+    const auto a = read_raw<uint64_t>(dir + "/cbs_a");
+    const auto b = read_raw<uint64_t>(dir + "/cbs_b");
+    std::vector<LWECiphertext> cts(batch);
+    for (uint32_t i = 0; i < batch; ++i) {
+        cts[i].a.assign(a.begin() + static_cast<size_t>(i) * params.n, a.begin() + static_cast<size_t>(i + 1) * params.n);
+        cts[i].b = b[i];
+        cts[i].q = params.q_lwe;
+    }
+    const auto rgsw = cc.gpu_CircuitBootstrappingBatch(cts);
+    std::vector<uint64_t> out;
+    for (const auto& r : rgsw) out.insert(out.end(), r.data.begin(), r.data.end());
+    write_raw(dir + "/cbs_out", out);
+    // the single-ciphertext and device-view forms agree with the batch
+    const auto one = cc.gpu_CircuitBootstrapping(cts[batch - 1]);
+    if (one.data != rgsw[batch - 1].data) return 5;
+    const auto view = cc.gpu_CircuitBootstrappingBatchToDevice(cts);
+    std::vector<uint64_t> back(view.per_ciphertext_elems * view.batch);
+    check_cuda(cudaStreamSynchronize(view.stream), "sync");
+    check_cuda(cudaMemcpy(back.data(), view.d_rgsw, back.size() * 8, cudaMemcpyDeviceToHost), "view");
+    if (back != out) return 6;
+    // a ciphertext of another modulus is rejected with an exception
+    try {
+        LWECiphertext bad = cts[0];
+        bad.q = params.q_lwe * 2;
+        (void)cc.gpu_CircuitBootstrapping(bad);
+        return 7;
+    } catch (const Error&) {
+    }
+    return 0;
+}
+
+static int run_gate(const std::string&) {
+    cbs_gate_params gp{};
+    check(cbs_gate_params_default(&gp), "gate params");
+    GPUBinFHEContext cc(gp, 64);
+    cc.GPUBTKeyGen(17);
+    const uint32_t count = 16;
+    std::vector<uint8_t> x(count), y(count);
+    for (uint32_t i = 0; i < count; ++i) x[i] = i & 1, y[i] = (i >> 1) & 1;
+    std::vector<uint32_t> a1(count * gp.n), b1(count), a2(count * gp.n), b2(count);
+    check(cbs_gate_encrypt_bits(cc.handle(), x.data(), count, 1, a1.data(), b1.data()), "encrypt");
+    check(cbs_gate_encrypt_bits(cc.handle(), y.data(), count, 2, a2.data(), b2.data()), "encrypt");
+    auto wrap = [&](const std::vector<uint32_t>& a, const std::vector<uint32_t>& b) {
+        std::vector<LWECiphertext> v(count);
+        for (uint32_t i = 0; i < count; ++i) {
+            v[i].a.assign(a.begin() + static_cast<size_t>(i) * gp.n, a.begin() + static_cast<size_t>(i + 1) * gp.n);
+            v[i].b = b[i];
+            v[i].q = uint64_t(1) << 32;
+        }
+        return v;
+    };
+    const auto out = cc.BatchGPUEvalBinGate(NAND, wrap(a1, b1), wrap(a2, b2));
+    std::vector<uint32_t> oa(count * gp.n), ob(count);
+    for (uint32_t i = 0; i < count; ++i) {
+        for (uint32_t j = 0; j < gp.n; ++j) oa[static_cast<size_t>(i) * gp.n + j] = static_cast<uint32_t>(out[i].a[j]);
+        ob[i] = static_cast<uint32_t>(out[i].b);
+    }
+    std::vector<uint8_t> dec(count);
+    check(cbs_gate_decrypt_bits(cc.handle(), oa.data(), ob.data(), count, dec.data()), "decrypt");
+    for (uint32_t i = 0; i < count; ++i)
+        if (dec[i] != static_cast<uint8_t>(1 - (x[i] & y[i]))) return 8;
+    return 0;
+}
+
+int main(int argc, char** argv) {
+    if (argc < 3) {
+        std::fprintf(stderr, "usage: %s ks|cbs|gate <dir>\n", argv[0]);
+        return 2;
+    }
+    try {
+        const std::string mode = argv[1], dir = argv[2];
+        if (mode == "ks") return run_ks(dir);
+        if (mode == "cbs") return run_cbs(dir);
+        if (mode == "gate") return run_gate(dir);
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "error: %s\n", e.what());
+        return 1;
+    }
+    return 2;
+}

@@ -1,0 +1,89 @@
+"""A C++ program written against the reference-shaped facade (include/cbs_b200.hpp), compiled
+and linked against libcbs_b200.so, run on the GPU (tests/cpp/facade_main.cpp):
+* keyswitch_inplace(PhantomContext, PhantomCiphertext, c2, PhantomRelinKey, is_relin, stream)
+  (src/eval_key_switch.cu:94) on a level-2 ciphertext, bit-exact against the oracle;
+* GPUCirBTSContext::gpu_CircuitBootstrappingBatch / gpu_CircuitBootstrapping /
+  gpu_CircuitBootstrappingBatchToDevice on host LWE ciphertexts (cirbts.cuh:454-462), the RGSW
+  rows bit-exact against the oracle's circuit bootstrap;
+* GPUBinFHEContext::BatchGPUEvalBinGate(NAND, ...) (binfhecontext.cuh:53-57), every gate
+  decrypting to the truth table."""
+from __future__ import annotations
+
+import ctypes
+import shutil
+import subprocess
+
+import numpy as np
+import pytest
+
+from cbs_harness import OracleCbs, lwe_encrypt_bits
+from conftest import PKG_DIR, ROOT
+from rns_harness import declare_rns, rns_primes
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def facade_bin(tmp_path_factory, lib):
+    gxx = shutil.which("g++")
+    if gxx is None:
+        pytest.skip("no C++ compiler")
+    out = tmp_path_factory.mktemp("facade") / "facade_main"
+    cmd = [gxx, "-std=c++17", "-O1", "-I", str(ROOT / "include"), "-I", "/usr/local/cuda/include",
+           str(ROOT / "tests" / "cpp" / "facade_main.cpp"), "-o", str(out), "-L", str(PKG_DIR), "-lcbs_b200",
+           "-L/usr/local/cuda/lib64", "-lcudart", f"-Wl,-rpath,{PKG_DIR}"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    return out
+
+
+def _run(binary, mode, d):
+    r = subprocess.run([str(binary), mode, str(d)], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, f"{mode}: exit {r.returncode}: {r.stderr}"
+
+
+def test_facade_keyswitch_inplace(facade_bin, tmp_path, oracle):
+    o = declare_rns(oracle)
+    n, logn, size_q, size_p, chain_index = 1 << 12, 12, 6, 2, 2
+    size_ql = size_q - (chain_index - 1)
+    q, p = rns_primes(o, n, size_q, size_p)
+    chain = np.concatenate([q, p]).astype(np.uint64)
+    beta = -(-size_q // size_p)
+    rng = np.random.default_rng(404)
+    ql = q[:size_ql]
+    c2 = np.stack([rng.integers(0, int(m), n, dtype=np.uint64) for m in ql])
+    ct = np.stack([np.stack([rng.integers(0, int(m), n, dtype=np.uint64) for m in ql]) for _ in range(2)])
+    evk = np.stack([np.stack([np.stack([rng.integers(0, int(m), n, dtype=np.uint64) for m in chain])
+                              for _ in range(2)]) for _ in range(beta)])
+    np.array([n, size_q, size_p, chain_index, beta], np.uint64).tofile(tmp_path / "ks_dims")
+    chain.tofile(tmp_path / "ks_chain")
+    c2.tofile(tmp_path / "ks_c2")
+    ct.tofile(tmp_path / "ks_ct")
+    evk.tofile(tmp_path / "ks_evk")
+    _run(facade_bin, "ks", tmp_path)
+    got = np.fromfile(tmp_path / "ks_out", np.uint64).reshape(ct.shape)
+    want = np.ascontiguousarray(ct).copy()
+    o.orc_keyswitch(want, np.ascontiguousarray(c2), np.ascontiguousarray(evk), logn, q, size_ql, size_q, p, size_p)
+    assert np.array_equal(got, want)
+
+
+def test_facade_circuit_bootstrap_host_lwe(facade_bin, tmp_path, pkg, oracle):
+    p = pkg.default_params()
+    seed, batch = 21, 3
+    keys = pkg.generate_keys_host(p, seed)
+    rng = np.random.default_rng(5)
+    a, b = lwe_encrypt_bits(rng, keys["s_lwe"], [1, 0, 1], p.q_lwe)
+    np.array([seed, batch], np.uint64).tofile(tmp_path / "cbs_dims")
+    a.astype(np.uint64).tofile(tmp_path / "cbs_a")
+    b.astype(np.uint64).tofile(tmp_path / "cbs_b")
+    _run(facade_bin, "cbs", tmp_path)
+    got = np.fromfile(tmp_path / "cbs_out", np.uint64).reshape(batch, p.num_lut, 2, 2, p.N)
+    oc = OracleCbs(oracle, p, keys)
+    want = np.zeros((batch, p.num_lut, 2, 2, p.N), np.uint64)
+    oracle.orc_circuit_bootstrap(ctypes.byref(oc.op), ctypes.byref(oc.ok), a.ctypes.data, b.ctypes.data, batch, p.n,
+                                 want.ctypes.data)
+    assert np.array_equal(got, want)
+
+
+def test_facade_batch_gate(facade_bin, tmp_path):
+    _run(facade_bin, "gate", tmp_path)
