@@ -205,7 +205,12 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     ctx = pkg.Context(params=pkg.preset_params(args.params), max_batch=128 * min(blocks, 256))
     ctx.keygen(args.seed)
     pkg.call("cbs_context_set_br_backend", ctx.handle, pkg.BR_FFT64 if args.backend == "fft64" else pkg.BR_NTT)
-    if args.multibit > 1:
+    tuned = None
+    if args.backend == "fft64" and args.tune:
+        # the product's autotuner picks the grouping and schedule (16 waves of 148 ciphertexts)
+        tuned = ctx.autotune(min(16 * 148, 128 * min(blocks, 256)))
+        args.multibit, args.schedule = tuned["mb"], tuned["schedule"]
+    elif args.multibit > 1:
         ctx.set_br_multibit(args.multibit)
     key = np.random.default_rng(args.seed).bytes(16)
     pkg.call("cbs_aes128_setup", ctx.handle, key, args.seed + 1)
@@ -313,6 +318,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
                    "param_set": args.params,
                    "l2": "per-step working set (keys + RGSW + LUT buffers) >> 126 MB L2",
                    "br_multibit": args.multibit,
+                   "br_tuned": tuned,
                    "parallelism": f"replicas x{world} (independent blocks per GPU)"},
         "us_per_bootstrap": ms_per_step * 1e3 / (blocks * 128 * ROUNDS),
         "correct_blocks": ok,
@@ -830,7 +836,7 @@ def br_roofline(args, p, T: int, br_ms: float, alg_bytes: int, traffic) -> dict:
     """Roofline of the dominant kernel, the fused blind rotation: on the FFT backend its bound is
     the FP64 pipe (algorithmic flops per launch over the launch time against the recorded FP64
     peak); the exact-NTT backend is bounded by 64-bit integer multiplies and reports HBM."""
-    name = br_kernel_name(args) + " (fused GINX blind rotation + finalize + MV split)"
+    name = br_kernel_name(args, p) + " (fused GINX blind rotation + finalize + MV split)"
     extra = {"algorithmic_bytes_per_launch": alg_bytes, "launch_ms": br_ms, "traffic": traffic,
              "traffic_over_algorithmic": (traffic / alg_bytes) if traffic else None,
              "traffic_src": "ncu dram__bytes_read.sum + dram__bytes_write.sum of this launch (one pass), recorded"}
@@ -848,10 +854,14 @@ def br_roofline(args, p, T: int, br_ms: float, alg_bytes: int, traffic) -> dict:
             "compute_rate": compute_rate(args.backend, T, p, br_ms, args.multibit), **extra}
 
 
-def br_kernel_name(args) -> str:
+def br_kernel_name(args, p=None) -> str:
     if args.backend != "fft64":
         return "k_blind_rotate"
-    return "k_blind_rotate_fft" if args.multibit == 1 else f"k_blind_rotate_fft_mb<11,{args.multibit}>"
+    if args.multibit == 1:
+        return "k_blind_rotate_fft"
+    if args.multibit == 2 and p is not None and p.digits_g == 2 and getattr(args, "schedule", 0) != 1:
+        return "k_blind_rotate_fft_mb_d2<11,2> (two digit transforms in lockstep)"
+    return f"k_blind_rotate_fft_mb<11,{args.multibit}>"
 
 
 # FP64 peak of this pool's B200, measured once (not driver-written): cuBLAS DGEMM through
@@ -1027,6 +1037,8 @@ def main() -> None:
     ap.add_argument("--params", choices=["3x12", "2x18"], default="2x18",
                     help="parameter set of the aes128 / blind_rotate workloads: blind-rotation gadget 2^12 x 3 "
                          "(cbs_params_default) or 2^18 x 2")
+    ap.add_argument("--no-tune", dest="tune", action="store_false",
+                    help="aes128 on fft64: use --multibit instead of the product's autotuned grouping")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--workload", choices=["aes128", "blind_rotate", "keyswitch", "rns_ntt", "gate", "ragged", "tcb",
                                            "aes_setup", "fp64_peak"],
@@ -1043,6 +1055,8 @@ def main() -> None:
         if args.multibit not in (None, 1):
             ap.error("--fft-mode fp32* runs one coefficient per step (--multibit 1)")
         args.multibit = 1
+    if args.multibit is not None:
+        args.tune = False  # an explicit grouping is measured as given
     if args.multibit is None:
         args.multibit = 2 if args.backend == "fft64" else 1
     if args.multibit > 1 and args.backend != "fft64":

@@ -3,6 +3,8 @@ from __future__ import annotations
 
 import ctypes
 import importlib.util
+import os
+import tempfile
 import subprocess
 import sys
 from pathlib import Path
@@ -11,6 +13,10 @@ import numpy as np
 import pytest
 
 ROOT = Path(__file__).resolve().parents[1]
+
+# the tests never read a tuning cache of the machine (a cached blind-rotation grouping would
+# change what selecting the FFT64 backend does): every session gets an empty one of its own
+os.environ["CBS_TUNE_CACHE"] = os.path.join(tempfile.mkdtemp(prefix="cbs_tune_"), "tune.json")
 PKG_DIR = ROOT / "gpu-circuitbootstrapping-aestransciphering_b200"
 ORACLE_DIR = ROOT / "oracle"
 GOLDEN = Path(__file__).resolve().parent / "golden"
