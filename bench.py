@@ -871,6 +871,41 @@ FP64_PEAK = {"tflops": 35.4, "src": "recorded: cuBLAS DGEMM 4096^3 (torch.matmul
                                     "median of three B200 runs (profiles/fp64_peak_b200.md); not driver-written"}
 
 
+def run_keygen(args, rank: int, world: int, local_rank: int) -> None:
+    """Key generation of the headline parameter set: the seeded host generation (cbs_keygen, the
+    role of the reference's OpenFHE CirBTKeyGen + gpu_init_cirbsk) against the device generation
+    (cbs_keygen_device, ChaCha20 per coefficient), each followed by the FFT key spectra and the
+    grouped (mb = 2) keys the AES path needs; wall time of the synchronous calls."""
+    import torch
+    torch.cuda.set_device(local_rank)
+    pkg = load_pkg()
+    p = pkg.preset_params(args.params)
+    res = {}
+    for name in ("host", "device"):
+        ctx = pkg.Context(params=p, max_batch=128)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        if name == "host":
+            ctx.keygen(args.seed)
+        else:
+            ctx.keygen_device(bytes(range(32)))
+        t1 = time.perf_counter()
+        pkg.call("cbs_context_set_br_backend", ctx.handle, pkg.BR_FFT64)
+        ctx.set_br_multibit(2)
+        t2 = time.perf_counter()
+        res[name] = {"keygen_s": t1 - t0, "fft_and_grouped_keys_s": t2 - t1, "total_s": t2 - t0}
+        ctx.close()
+    if rank == 0:
+        print(json.dumps({"metric": f"key generation, {args.params} parameter set (seconds, lower is better)",
+                          "value": res["device"]["keygen_s"], "unit": "s", "n_gpus": 1, "steps": 1, "warmup": 0,
+                          "higher_is_better": False, "data": "synthetic (fixed ChaCha20 key / seed)",
+                          "config": {"workload": "keygen", "param_set": args.params,
+                                     "keys": "secrets, BSK, HomTrace, SchemeSwitch, extraction KSK; then FFT "
+                                             "spectra and mb = 2 grouped keys"},
+                          "host": res["host"], "device": res["device"],
+                          "speedup_keygen": res["host"]["keygen_s"] / res["device"]["keygen_s"]}), flush=True)
+
+
 def run_fp64_peak(args, rank: int, world: int, local_rank: int) -> None:
     """The FP64 peak the blind rotation's roofline is quoted against: cuBLAS DGEMM through
     torch.matmul, float64 n^3 (n = 4096, 2 n^3 flop), best of 5 after a warm-up, CUDA events."""
@@ -1041,7 +1076,7 @@ def main() -> None:
                     help="aes128 on fft64: use --multibit instead of the product's autotuned grouping")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--workload", choices=["aes128", "blind_rotate", "keyswitch", "rns_ntt", "gate", "ragged", "tcb",
-                                           "aes_setup", "fp64_peak"],
+                                           "aes_setup", "fp64_peak", "keygen"],
                     default="aes128",
                     help="aes128 is the headline; the others time one kernel family")
     ap.add_argument("--batch", type=int, default=0, help="units per step for the kernel workloads")
@@ -1078,7 +1113,7 @@ def main() -> None:
     runner = {"aes128": run_ours, "blind_rotate": run_blind_rotate, "keyswitch": run_keyswitch,
               "rns_ntt": run_rns_ntt, "gate": run_gate,
               "ragged": run_ragged, "tcb": run_tcb, "aes_setup": run_aes_setup,
-              "fp64_peak": run_fp64_peak}[args.workload]
+              "fp64_peak": run_fp64_peak, "keygen": run_keygen}[args.workload]
     try:
         runner(args, rank, world, local_rank)
     finally:

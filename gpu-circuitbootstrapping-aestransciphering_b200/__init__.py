@@ -97,6 +97,7 @@ def _declare(lib: ctypes.CDLL) -> None:
         "cbs_cmux_batch_device": (st, [c_vp, c_vp, c_vp, c_vp, u64, u32, c_vp, c_vp]),
         "cbs_circuit_bootstrap_batch": (st, [c_vp, c_vp, c_vp, u32, u32, c_vp]),
         "cbs_context_set_br_schedule": (st, [c_vp, u32]),
+        "cbs_keygen_device": (st, [c_vp, c_vp]),
         "cbs_autotune_blind_rotation": (st, [c_vp, u32, ctypes.c_char_p, c_vp]),
         "cbs_context_tuned": (st, [c_vp, c_vp]),
         "cbs_extract_keyswitch_device": (st, [c_vp, c_vp, u32, c_vp, u32, c_vp, c_vp, u32, c_vp]),
@@ -244,6 +245,11 @@ class Context:
     @property
     def handle(self) -> int:
         return self._h.value
+
+    def keygen_device(self, rng_key: bytes | None = None) -> None:
+        """Generate every key on the device from ChaCha20 under rng_key (32 bytes; None draws one
+        from the operating system)."""
+        call("cbs_keygen_device", self._h, rng_key)
 
     def keygen(self, seed: int) -> None:
         call("cbs_keygen", self._h, seed)

@@ -105,6 +105,11 @@ static cbs_status prepare_mb(cbs_context* c) {
                   "import them with cbs_import_mb_bsk");
         return CBS_ERR_NOT_READY;
     }
+    if (c->device_keyed) {
+        // keys drawn on the device (cbs_keygen_device): the grouped keys from the same stream
+        if (cbs_status st = device_grouped_keys(c, c->br_mb)) return st;
+        return upload_mb_spectra(c);
+    }
     try {
         generate_mb_bsk(c->p, c->tab, c->hk, c->br_mb, c->key_seed ^ kMbSeedTweak, c->h_mbk);
     } catch (const std::exception& e) {
@@ -363,6 +368,42 @@ static cbs_status validate(const cbs_params& p) {
     return CBS_OK;
 }
 
+cbs_status upload_host_keys(cbs_context* c) {
+    FastMod fm(c->p.Q);
+    cudaStream_t s = c->stream;
+    const auto bsk_m = to_mont(c->hk.bsk, fm, c->mont_r);
+    const auto ht_m = to_mont(c->hk.ht, fm, c->mont_r);
+    const auto ss_m = to_mont(c->hk.ss, fm, c->mont_r);
+    CBS_CUDA_TRY(c->d_bsk.upload(bsk_m.data(), bsk_m.size(), s));
+    CBS_CUDA_TRY(c->d_ht.upload(ht_m.data(), ht_m.size(), s));
+    CBS_CUDA_TRY(c->d_ss.upload(ss_m.data(), ss_m.size(), s));
+    {
+        // device copy of the key-switching key with rows padded to ksk_row_stride(n) words
+        const size_t rows = c->hk.ksk.size() / (c->p.n + 1), stride = ksk_row_stride(c->p.n);
+        std::vector<uint16_t> padded(rows * stride, 0);
+        for (size_t r = 0; r < rows; ++r)
+            std::memcpy(padded.data() + r * stride, c->hk.ksk.data() + r * (c->p.n + 1),
+                        (c->p.n + 1) * sizeof(uint16_t));
+        CBS_CUDA_TRY(c->d_ksk.upload(padded.data(), padded.size(), s));
+    }
+    CBS_CUDA_TRY(c->d_tv.upload(c->hk.tv.data(), c->hk.tv.size(), s));
+    CBS_CUDA_TRY(c->d_gadd.upload(c->hk.gadd.data(), c->hk.gadd.size(), s));
+    CBS_CUDA_TRY(c->d_maps.upload(c->hk.maps.data(), c->hk.maps.size(), s));
+    CBS_CUDA_TRY(cudaStreamSynchronize(s));
+    c->keys_ready = true;
+    c->aes.ready = false;
+    c->fft_ready = false;
+    c->mb_ready = false;
+    c->h_mbk.clear();
+    c->d_bskf_mb.reset();
+    c->aes.drop_graphs();
+    if (c->br_backend == CBS_BR_FFT64) {
+        if (cbs_status st = prepare_fft(c)) return st;
+        return prepare_mb(c);
+    }
+    return CBS_OK;
+}
+
 }  // namespace cbs
 
 using namespace cbs;
@@ -458,6 +499,8 @@ cbs_status cbs_context_create(const cbs_params* params, uint32_t max_batch, cbs_
 cbs_status cbs_context_destroy(cbs_context* ctx) {
     if (!ctx) return CBS_OK;
     ctx->aes.drop_graphs();
+    volatile uint32_t* wipe = ctx->keygen_key.w;  // the key the device key set was drawn with
+    for (int i = 0; i < 8; ++i) wipe[i] = 0;
     cudaStream_t s = ctx->stream;
     delete ctx;
     if (s) cudaStreamDestroy(s);
@@ -472,41 +515,6 @@ cbs_status cbs_context_stream(const cbs_context* ctx, cbs_stream_t* out) {
 
 // upload the evaluation keys of c->hk (bsk / ht / ss to Montgomery form, the KSK with padded
 // rows, the derived tables) and rebuild what depends on them
-static cbs_status upload_host_keys(cbs_context* c) {
-    FastMod fm(c->p.Q);
-    cudaStream_t s = c->stream;
-    const auto bsk_m = to_mont(c->hk.bsk, fm, c->mont_r);
-    const auto ht_m = to_mont(c->hk.ht, fm, c->mont_r);
-    const auto ss_m = to_mont(c->hk.ss, fm, c->mont_r);
-    CBS_CUDA_TRY(c->d_bsk.upload(bsk_m.data(), bsk_m.size(), s));
-    CBS_CUDA_TRY(c->d_ht.upload(ht_m.data(), ht_m.size(), s));
-    CBS_CUDA_TRY(c->d_ss.upload(ss_m.data(), ss_m.size(), s));
-    {
-        // device copy of the key-switching key with rows padded to ksk_row_stride(n) words
-        const size_t rows = c->hk.ksk.size() / (c->p.n + 1), stride = ksk_row_stride(c->p.n);
-        std::vector<uint16_t> padded(rows * stride, 0);
-        for (size_t r = 0; r < rows; ++r)
-            std::memcpy(padded.data() + r * stride, c->hk.ksk.data() + r * (c->p.n + 1),
-                        (c->p.n + 1) * sizeof(uint16_t));
-        CBS_CUDA_TRY(c->d_ksk.upload(padded.data(), padded.size(), s));
-    }
-    CBS_CUDA_TRY(c->d_tv.upload(c->hk.tv.data(), c->hk.tv.size(), s));
-    CBS_CUDA_TRY(c->d_gadd.upload(c->hk.gadd.data(), c->hk.gadd.size(), s));
-    CBS_CUDA_TRY(c->d_maps.upload(c->hk.maps.data(), c->hk.maps.size(), s));
-    CBS_CUDA_TRY(cudaStreamSynchronize(s));
-    c->keys_ready = true;
-    c->aes.ready = false;
-    c->fft_ready = false;
-    c->mb_ready = false;
-    c->h_mbk.clear();
-    c->d_bskf_mb.reset();
-    c->aes.drop_graphs();
-    if (c->br_backend == CBS_BR_FFT64) {
-        if (cbs_status st = prepare_fft(c)) return st;
-        return prepare_mb(c);
-    }
-    return CBS_OK;
-}
 
 cbs_status cbs_keygen(cbs_context* ctx, uint64_t seed) {
     CBS_CHECK_ARG(ctx, "keygen: null context");
@@ -519,6 +527,7 @@ cbs_status cbs_keygen(cbs_context* ctx, uint64_t seed) {
     }
     c->has_secret = true;
     c->key_seed = seed;
+    c->device_keyed = false;
     return upload_host_keys(c);
 }
 

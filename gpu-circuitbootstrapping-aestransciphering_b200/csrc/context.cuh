@@ -11,6 +11,7 @@
 #include "../../include/cbs_b200.h"
 #include "cbs_kernels.cuh"
 #include "devbuf.cuh"
+#include "encrypt.cuh"
 #include "extract_kernels.cuh"
 #include "fft_kernels.cuh"
 #include "host_math.h"
@@ -89,6 +90,8 @@ struct cbs_context {
     cbs_tune_choice tuned{};
     bool mb_ready = false;
     uint64_t key_seed = 0;
+    bool device_keyed = false;           // keys drawn on the device (cbs_keygen_device) under keygen_key
+    cbs::ChachaKey keygen_key{};
     std::vector<uint64_t> h_mbk;         // grouped keys, NTT domain (kept for export)
     cbs::DevBuf<double2> d_bskf_mb;      // their spectra
     cbs::DevBuf<uint64_t> d_pow2, d_pow2s;
@@ -126,6 +129,10 @@ bool tune_cache_lookup(const cbs_context* c, const char* path, cbs_tune_choice* 
 // on the FFT64 backend, switch to the tuning cache's grouping unless the caller chose one (grouped
 // keys are generated from the secret key; without it the grouping stays as it is)
 cbs_status apply_tuned_multibit(cbs_context* c);
+// host key copies (c->hk) -> device keys, derived tables; resets the FFT / grouped state
+cbs_status upload_host_keys(cbs_context* c);
+// the grouped keys of a device-generated key set into c->h_mbk (keygen_device.cu)
+cbs_status device_grouped_keys(cbs_context* c, uint32_t mb);
 // blind rotation + HomTrace/SchemeSwitch of the selected backend: LWE -> RGSW rows in the
 // NTT-domain reference layout [batch][num_lut][2][2][N]; d_mv is [batch][num_lut][2][N] scratch
 // FFT HomTrace + SchemeSwitch with the rows converted to the NTT-domain reference layout

@@ -17,7 +17,7 @@ struct ChachaKey {
 
 struct EncryptRlweArgs {
     ChachaKey key;
-    const uint32_t* words;  // [count] plaintext words (bit j -> coefficient j)
+    const uint32_t* words;  // [count] plaintext words (bit j -> coefficient j); null = encryptions of 0
     uint64_t* ct;           // [count][2][N] out: (a, b), NTT domain
     uint64_t* tmp;          // [count][N] scratch
     const uint64_t* s_ntt;  // [N] NTT(s), normal form
@@ -26,6 +26,7 @@ struct EncryptRlweArgs {
     uint32_t N;
     uint32_t first;         // sample index of words[0] (the ChaCha20 nonce)
     uint64_t Q, delta, ratio0, ratio1;
+    uint32_t domain;        // second nonce word: 1 = AES material; key generation uses 4-9
 };
 
 struct EncryptLweArgs {

@@ -143,6 +143,20 @@ cbs_status cbs_context_stream(const cbs_context *ctx, cbs_stream_t *out);
  * gpu_init_cirbsk, cirbts-init.cu:200-865). */
 cbs_status cbs_keygen(cbs_context *ctx, uint64_t seed);
 
+/* All key material generated on the device (no reference counterpart on the device: the
+ * reference's KeyGen / CirBTKeyGen / KeySwitchGen run in its OpenFHE fork on the host,
+ * examples/aes_transcipher/main.cu:232-252, and gpu_init_cirbsk re-lays the keys for the device
+ * in host loops, bitwise/src/cirbts/cirbts-init.cu:367-864).  Every word comes from ChaCha20
+ * (RFC 8439) under rng_key[32], one block per coefficient addressed by (counter, sample,
+ * domain): secrets (domain 3), bootstrapping key (4), HomTrace keys (5), SchemeSwitch key (6),
+ * extraction key-switching key (7), grouped keys when mb > 1 is selected (8 / 9); RLWE masks
+ * in the NTT domain from words 0-3, noise from the discrete-Gaussian table of
+ * cbs_cdt_table_host with words 4-5.  The same secrecy rules as cbs_aes128_setup_device apply:
+ * rng_key decides the secret key, so it must come from a CSPRNG, stay secret and never be
+ * reused; NULL draws a fresh key from the operating system (getrandom).  The context keeps
+ * host copies (cbs_export_keys) and wipes its copy of rng_key on destroy. */
+cbs_status cbs_keygen_device(cbs_context *ctx, const uint8_t *rng_key);
+
 /* Blind-rotation external-product backend.  CBS_BR_NTT: exact 64-bit NTT arithmetic mod Q
  * (bit-identical to the reference's kernels).  CBS_BR_FFT64: FP64 FFT products (the
  * reference's gate-bootstrap / split-FFT form, bitwise/src/fft.cu:3614-3755); the key

@@ -1649,3 +1649,181 @@ void orc_cbs_keygen_mb(const orc_cbs_params *p, double sigma_rlwe, const int32_t
     free(irp);
     free(rp);
 }
+
+/* ------------------------------------------------------------------------------------------ */
+/* key generation on the device, restated (ChaCha20-addressed words)                           */
+/* ------------------------------------------------------------------------------------------ */
+
+/* RLWE(0) sample (sample, domain): a = NTT-domain mask, b = a s + NTT(e) */
+static void chacha_rlwe_zero(const uint32_t key[8], uint32_t sample, uint32_t domain, uint32_t N, uint64_t Q,
+                             const uint64_t *rp, const uint64_t *s_ntt, const uint64_t *T, uint32_t tlen, uint64_t *a,
+                             uint64_t *b, uint64_t *tmp) {
+    const uint32_t nonce[3] = {sample, domain, 0u};
+    for (uint32_t i = 0; i < N; ++i) {
+        uint32_t blk[16];
+        orc_chacha20_block(key, i, nonce, blk);
+        a[i] = orc_uniform_mod(blk, Q);
+        const int64_t e = orc_cdt_sample((uint64_t)blk[4] | ((uint64_t)blk[5] << 32), T, tlen);
+        tmp[i] = e < 0 ? Q - (uint64_t)(-e) : (uint64_t)e;
+    }
+    ntt_fwd_one(tmp, N, Q, rp);
+    for (uint32_t i = 0; i < N; ++i) b[i] = addmod(orc_mulmod(a[i], s_ntt[i], Q), tmp[i], Q);
+}
+
+static void chacha_secrets(const uint32_t key[8], uint32_t n, uint32_t N, int32_t *s_lwe, int32_t *s_rlwe) {
+    for (uint32_t i = 0; i < n; ++i) {
+        uint32_t blk[16];
+        const uint32_t nonce[3] = {0u, 3u, 0u};
+        orc_chacha20_block(key, i, nonce, blk);
+        s_lwe[i] = (int32_t)(blk[0] & 1u);
+    }
+    for (uint32_t i = 0; i < N; ++i) {
+        uint32_t blk[16];
+        const uint32_t nonce[3] = {1u, 3u, 0u};
+        orc_chacha20_block(key, i, nonce, blk);
+        s_rlwe[i] = (int32_t)orc_uniform_mod(blk, 3) - 1;
+    }
+}
+
+int orc_cbs_keygen_chacha(const orc_cbs_params *p, double sigma_lwe, double sigma_rlwe, uint32_t qks,
+                          uint32_t base_ks, const uint32_t key[8], int32_t *s_lwe_out, int32_t *s_rlwe_out,
+                          uint64_t *bsk_out, uint64_t *ht_out, uint64_t *ss_out, uint16_t *ksk_out) {
+    const uint32_t N = p->N, n = p->n, l2 = 2 * p->digits_g, rounds = p->trace_rounds;
+    const uint64_t Q = p->Q;
+    uint64_t *rp = (uint64_t *)malloc(sizeof(uint64_t) * N), *irp = (uint64_t *)malloc(sizeof(uint64_t) * N);
+    uint64_t ninv[2];
+    if (orc_ntt_tables(p->log_n, Q, rp, NULL, irp, NULL, ninv) != 0) {
+        free(rp);
+        free(irp);
+        return -1;
+    }
+    uint64_t TR[4096], TL[4096];
+    const uint32_t lr = orc_cdt_table(sigma_rlwe, TR, 4096), ll = orc_cdt_table(sigma_lwe, TL, 4096);
+    int32_t *s_lwe = (int32_t *)malloc(sizeof(int32_t) * n), *s_rlwe = (int32_t *)malloc(sizeof(int32_t) * N);
+    chacha_secrets(key, n, N, s_lwe, s_rlwe);
+    uint64_t *s_ntt = (uint64_t *)malloc(sizeof(uint64_t) * N);
+    for (uint32_t i = 0; i < N; ++i) s_ntt[i] = s_rlwe[i] < 0 ? Q - 1 : (uint64_t)s_rlwe[i];
+    ntt_fwd_one(s_ntt, N, Q, rp);
+    uint64_t gbr[64], ght[64], gss[64];
+    gadget_powers(Q, p->base_g, p->digits_g, gbr);
+    gadget_powers(Q, p->base_ht, p->digits_ht, ght);
+    gadget_powers(Q, p->base_ss, p->digits_ss, gss);
+
+    if (bsk_out) {
+#pragma omp parallel for schedule(dynamic)
+        for (long smp = 0; smp < (long)n * l2; ++smp) {
+            uint64_t *tmp = (uint64_t *)malloc(sizeof(uint64_t) * N);
+            const uint32_t i = (uint32_t)(smp / l2), row = (uint32_t)(smp % l2);
+            uint64_t *a = bsk_out + (size_t)smp * 2 * N, *b = a + N;
+            chacha_rlwe_zero(key, (uint32_t)smp, 4u, N, Q, rp, s_ntt, TR, lr, a, b, tmp);
+            if (s_lwe[i]) {
+                uint64_t *tgt = (row & 1) ? b : a;
+                for (uint32_t c = 0; c < N; ++c) tgt[c] = addmod(tgt[c], gbr[row >> 1], Q);
+            }
+            free(tmp);
+        }
+    }
+    if (ht_out) {
+        uint64_t *sig = (uint64_t *)malloc(sizeof(uint64_t) * (size_t)rounds * N);
+        for (uint32_t rd = 0; rd < rounds; ++rd) {
+            const uint64_t kk = ((uint64_t)N >> rd) + 1;
+            uint64_t *sg = sig + (size_t)rd * N;
+            for (uint32_t i = 0; i < N; ++i) {
+                const uint64_t e = ((uint64_t)i * kk) % (2ull * N);
+                const int32_t v = e < N ? s_rlwe[i] : -s_rlwe[i];
+                sg[e % N] = v < 0 ? Q - (uint64_t)(-v) : (uint64_t)v;
+            }
+            ntt_fwd_one(sg, N, Q, rp);
+        }
+#pragma omp parallel for schedule(dynamic)
+        for (long smp = 0; smp < (long)rounds * p->digits_ht; ++smp) {
+            uint64_t *tmp = (uint64_t *)malloc(sizeof(uint64_t) * N);
+            const uint32_t rd = (uint32_t)(smp / p->digits_ht), j = (uint32_t)(smp % p->digits_ht);
+            uint64_t *a = ht_out + (size_t)smp * 2 * N, *b = a + N;
+            chacha_rlwe_zero(key, (uint32_t)smp, 5u, N, Q, rp, s_ntt, TR, lr, a, b, tmp);
+            for (uint32_t c = 0; c < N; ++c) b[c] = submod(b[c], orc_mulmod(sig[(size_t)rd * N + c], ght[j], Q), Q);
+            free(tmp);
+        }
+        free(sig);
+    }
+    if (ss_out) {
+        uint64_t *tmp = (uint64_t *)malloc(sizeof(uint64_t) * N);
+        for (uint32_t j = 0; j < p->digits_ss; ++j) {
+            uint64_t *a = ss_out + (size_t)j * 2 * N, *b = a + N;
+            chacha_rlwe_zero(key, j, 6u, N, Q, rp, s_ntt, TR, lr, a, b, tmp);
+            for (uint32_t c = 0; c < N; ++c)
+                b[c] = addmod(b[c], orc_mulmod(orc_mulmod(s_ntt[c], s_ntt[c], Q), gss[j], Q), Q);
+        }
+        free(tmp);
+    }
+    if (ksk_out) {
+        const uint32_t mask = qks - 1, outlen = n + 1;
+#pragma omp parallel for schedule(static)
+        for (long t = 0; t < (long)2 * N * base_ks; ++t) {
+            const uint32_t v = (uint32_t)(t % base_ks), i = (uint32_t)((t / base_ks) % N), j = (uint32_t)(t / ((long)base_ks * N));
+            uint16_t *row = ksk_out + (size_t)t * outlen;
+            const uint32_t nonce[3] = {(uint32_t)t, 7u, 0u};
+            uint32_t acc = 0, blk[16];
+            for (uint32_t c = 0; c < n; ++c) {
+                orc_chacha20_block(key, c, nonce, blk);
+                const uint32_t a = (uint32_t)orc_uniform_mod(blk, qks);
+                row[c] = (uint16_t)a;
+                if (s_lwe[c]) acc += a;
+            }
+            orc_chacha20_block(key, n, nonce, blk);
+            const int64_t e = orc_cdt_sample((uint64_t)blk[4] | ((uint64_t)blk[5] << 32), TL, ll);
+            const uint32_t si = (uint32_t)(s_rlwe[i] + (int32_t)qks) & mask;
+            const uint32_t bj = j == 0 ? 1u : base_ks;
+            const uint32_t m = (v * si * bj) & mask;
+            row[n] = (uint16_t)((acc + m + (uint32_t)(int32_t)e) & mask);
+        }
+    }
+    if (s_lwe_out) memcpy(s_lwe_out, s_lwe, sizeof(int32_t) * n);
+    if (s_rlwe_out) memcpy(s_rlwe_out, s_rlwe, sizeof(int32_t) * N);
+    free(s_ntt);
+    free(s_rlwe);
+    free(s_lwe);
+    free(irp);
+    free(rp);
+    return 0;
+}
+
+void orc_cbs_keygen_chacha_mb(const orc_cbs_params *p, double sigma_rlwe, const uint32_t key[8],
+                              const int32_t *s_lwe, const int32_t *s_rlwe, uint32_t mb, uint64_t *mbk) {
+    static const uint32_t order2[3] = {1u, 2u, 3u};
+    static const uint32_t order3[7] = {1u, 2u, 4u, 3u, 5u, 6u, 7u};
+    const uint32_t N = p->N, n = p->n, l2 = 2 * p->digits_g, K = (1u << mb) - 1u, groups = (n + mb - 1) / mb;
+    const uint64_t Q = p->Q;
+    uint64_t *rp = (uint64_t *)malloc(sizeof(uint64_t) * N), *irp = (uint64_t *)malloc(sizeof(uint64_t) * N);
+    uint64_t ninv[2];
+    orc_ntt_tables(p->log_n, Q, rp, NULL, irp, NULL, ninv);
+    uint64_t TR[4096];
+    const uint32_t lr = orc_cdt_table(sigma_rlwe, TR, 4096);
+    uint64_t *s_ntt = (uint64_t *)malloc(sizeof(uint64_t) * N);
+    for (uint32_t i = 0; i < N; ++i) s_ntt[i] = s_rlwe[i] < 0 ? Q - 1 : (uint64_t)s_rlwe[i];
+    ntt_fwd_one(s_ntt, N, Q, rp);
+    uint64_t gbr[64];
+    gadget_powers(Q, p->base_g, p->digits_g, gbr);
+#pragma omp parallel for schedule(dynamic)
+    for (long smp = 0; smp < (long)groups * K * l2; ++smp) {
+        uint64_t *tmp = (uint64_t *)malloc(sizeof(uint64_t) * N);
+        const uint32_t row = (uint32_t)(smp % l2), kk = (uint32_t)((smp / l2) % K), g = (uint32_t)(smp / ((long)l2 * K));
+        const uint32_t mask = mb == 2 ? order2[kk] : order3[kk];
+        uint32_t prod = 1;
+        for (uint32_t i = 0; i < mb; ++i)
+            if (mask & (1u << i)) {
+                const uint32_t idx = g * mb + i;
+                prod &= idx < n ? (uint32_t)s_lwe[idx] : 0u;
+            }
+        uint64_t *a = mbk + (size_t)smp * 2 * N, *b = a + N;
+        chacha_rlwe_zero(key, (uint32_t)smp, mb == 2 ? 8u : 9u, N, Q, rp, s_ntt, TR, lr, a, b, tmp);
+        if (prod) {
+            uint64_t *tgt = (row & 1) ? b : a;
+            for (uint32_t c = 0; c < N; ++c) tgt[c] = addmod(tgt[c], gbr[row >> 1], Q);
+        }
+        free(tmp);
+    }
+    free(s_ntt);
+    free(irp);
+    free(rp);
+}

@@ -229,6 +229,22 @@ int orc_cbs_keygen(const orc_cbs_params *p, double sigma_lwe, double sigma_rlwe,
 void orc_cbs_keygen_mb(const orc_cbs_params *p, double sigma_rlwe, const int32_t *s_lwe, const int32_t *s_rlwe,
                        uint32_t mb, uint64_t seed, uint64_t *mbk);
 
+/* ---------------- key generation on the device (cbs_keygen_device; no reference counterpart on
+ * the device, the reference's keys come from its absent OpenFHE fork): every word from ChaCha20
+ * under key[8], block (counter, nonce = (sample, domain, 0)): secrets domain 3 (s_lwe[i] = bit 0
+ * of block (i, 0); s_rlwe[i] = floor(3 x / 2^128) - 1 of block (i, 1)), BSK domain 4 (sample
+ * i 2 digits_g + row), HomTrace domain 5 (sample round digits_ht + j), SchemeSwitch domain 6,
+ * KSK domain 7 (sample (j N + i) base_ks + v, mask words floor(qks x / 2^128) from block
+ * (c, sample), noise from block (n, sample)), grouped keys domain 8 (mb = 2) / 9 (mb = 3).
+ * RLWE samples: NTT-domain mask floor(Q x / 2^128) of words 0-3, noise of words 4-5 by the
+ * table of orc_cdt_table, b = a s + NTT(e); then the message as the seeded key generation adds
+ * it.  Layouts as orc_cbs_keygen; any output may be NULL; returns 0 or -1 (no NTT tables). */
+int orc_cbs_keygen_chacha(const orc_cbs_params *p, double sigma_lwe, double sigma_rlwe, uint32_t qks,
+                          uint32_t base_ks, const uint32_t key[8], int32_t *s_lwe, int32_t *s_rlwe, uint64_t *bsk,
+                          uint64_t *ht, uint64_t *ss, uint16_t *ksk);
+void orc_cbs_keygen_chacha_mb(const orc_cbs_params *p, double sigma_rlwe, const uint32_t key[8],
+                              const int32_t *s_lwe, const int32_t *s_rlwe, uint32_t mb, uint64_t *mbk);
+
 #ifdef __cplusplus
 }
 #endif

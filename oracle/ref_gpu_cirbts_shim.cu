@@ -110,6 +110,54 @@ int ref_cirbts_blind_rotate_mb2(uint64_t* acc, const uint64_t* d_a, uint32_t a_s
     return static_cast<int>(e);
 }
 
+// N-major index positions [n][batch] of the LWE masks (kernel_SpecialMS_IndexPos_Batch_NMajor,
+// the layout CIRBTS_BATCH_INDEX_NMAJOR=1 selects), into caller memory.
+int ref_cirbts_index_nmajor(const uint64_t* d_a, uint32_t a_stride, uint32_t n, uint32_t batch, uint32_t N,
+                            uint64_t q_lwe, uint32_t bitwidth, uint32_t* index_out, void* stream) {
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    kernel_SpecialMS_IndexPos_Batch_NMajor<<<dim3((n + 255) / 256, batch), 256, 0, s>>>(d_a, index_out, n, batch, a_stride,
+                                                                                        2 * N, q_lwe, bitwidth);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    return static_cast<int>(e);
+}
+
+// Grouped (mb = 3) blind rotation in the configuration the reference's AES example selects by
+// default for batched circuit bootstrapping (examples/aes_transcipher/main.cu:123-136:
+// CIRBTS_PBS_MULTIBIT=3, CIRBTS_EVALACC_SOA=1, CIRBTS_BATCH_INDEX_NMAJOR=1, EvalAcc block X 128;
+// fused-NTT threads per block from CIRBTS_FUSED_NTT_TPB, 384 in the AES fast defaults
+// :107-121), launch sequence of bitwise/src/cirbts/cirbts-batch.cu:2640-2700: per group the INTT,
+// kernel_SignedDigitDecompose2_FusedFNWT_Batch and kernel_EvalAccCore_Binary_MB3_Grouped_Batch_
+// SoA_NMajor.  ek_soa / ek_shoup_soa: host arrays of the 7 subset keys ({0} {1} {2} {0,1} {0,2}
+// {1,2} {0,1,2}), each in the SoA layout [groups][N/32 tiles][2 digits][2][32 lanes] with its
+// Shoup table; index_nmajor from ref_cirbts_index_nmajor; ct [2 batch][N] and dct
+// [2 digits batch][N] are caller scratch (nothing is allocated here, so a timed call measures
+// the kernels only).  n must be a multiple of 3 (no tail group).
+int ref_cirbts_blind_rotate_mb3_soa(uint64_t* acc, uint32_t n, uint32_t batch, const uint64_t* const* ek_soa,
+                                    const uint64_t* const* ek_shoup_soa, const uint64_t* monic, const void* d_mod,
+                                    const uint64_t* tw, const uint64_t* tws, const uint64_t* itw, const uint64_t* itws,
+                                    const uint64_t* ninv, const uint64_t* ninv_s, uint32_t N, uint64_t Q,
+                                    uint32_t base_g, uint32_t digits_g, const uint32_t* index_nmajor, uint32_t tpb,
+                                    uint32_t block_x, uint64_t* ct, uint64_t* dct, void* stream) {
+    if (n % 3 != 0 || tpb == 0 || block_x == 0) return static_cast<int>(cudaErrorInvalidValue);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const DModulus* mod = static_cast<const DModulus*>(d_mod);
+    const uint32_t digitsG2 = 2 * digits_g, groups = n / 3, tiles = N / 32;
+    const dim3 eb(block_x), eg((N + block_x - 1) / block_x, batch);
+    cudaError_t e = cudaSuccess;
+    for (uint32_t g = 0; g < groups && e == cudaSuccess; ++g) {
+        inwt_1d_opt_outofplace_batched(ct, acc, itw, itws, mod, ninv, ninv_s, N, static_cast<size_t>(2) * batch, s);
+        kernel_SignedDigitDecompose2_FusedFNWT_Batch<<<digitsG2 * batch, tpb, N * sizeof(uint64_t), s>>>(
+            dct, ct, Q, base_g, digits_g, N, batch, tw, tws, mod);
+        kernel_EvalAccCore_Binary_MB3_Grouped_Batch_SoA_NMajor<<<eg, eb, 0, s>>>(
+            acc, dct, ek_soa[0], ek_shoup_soa[0], ek_soa[1], ek_shoup_soa[1], ek_soa[2], ek_shoup_soa[2], ek_soa[3],
+            ek_shoup_soa[3], ek_soa[4], ek_shoup_soa[4], ek_soa[5], ek_shoup_soa[5], ek_soa[6], ek_shoup_soa[6], monic, N,
+            tiles, mod, digitsG2, g, 3 * g, 3 * g + 1, 3 * g + 2, index_nmajor, batch);
+        e = cudaGetLastError();
+    }
+    return static_cast<int>(e);
+}
+
 // HomTrace + SchemeSwitch of count MV RLWEs in the reference's default (unfused) launch
 // sequence (bitwise/src/cirbts/cirbts-batch.cu:1656-1789): per round k the permuting INTT of
 // c0, kernel_Fused_Permute_Decompose, the NTT of the digits and

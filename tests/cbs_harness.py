@@ -198,3 +198,27 @@ def oracle_keys_mb(oracle, p, keys: dict, mb: int, seed: int) -> np.ndarray:
     oracle.orc_cbs_keygen_mb(ctypes.byref(op), p.sigma_rlwe, s_lwe.ctypes.data, s_rlwe.ctypes.data, mb,
                              seed ^ MB_SEED_TWEAK, out.ctypes.data)
     return out
+
+
+# a fixed ChaCha20 key for reproducible key-generation tests
+RNG_KEY = bytes(range(100, 132))
+
+
+def oracle_chacha_keys(oracle, p, key: bytes) -> dict:
+    """The key set the device key generation draws under the ChaCha20 key `key`, restated by
+    the oracle (orc_cbs_keygen_chacha)."""
+    vp = ctypes.c_void_p
+    oracle.orc_cbs_keygen_chacha.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_uint32, ctypes.c_uint32,
+                                             vp, vp, vp, vp, vp, vp, vp]
+    oracle.orc_cbs_keygen_chacha.restype = ctypes.c_int
+    N, n, rounds = p.N, p.n, p.N.bit_length() - 1 - p.trace_shift
+    k = {"s_lwe": np.zeros(n, np.int32), "s_rlwe": np.zeros(N, np.int32),
+         "bsk": np.zeros((n, 2 * p.digits_g, 2, N), np.uint64),
+         "ht": np.zeros((rounds, p.digits_ht, 2, N), np.uint64), "ss": np.zeros((p.digits_ss, 2, N), np.uint64),
+         "ksk": np.zeros((2, N, p.base_ks, n + 1), np.uint16)}
+    kw = np.frombuffer(key, np.uint32).copy()
+    op = orc_params(p)
+    st = oracle.orc_cbs_keygen_chacha(ctypes.byref(op), p.sigma_lwe, p.sigma_rlwe, p.qks, p.base_ks, kw.ctypes.data,
+                                      *(k[f].ctypes.data for f in ("s_lwe", "s_rlwe", "bsk", "ht", "ss", "ksk")))
+    assert st == 0
+    return k

@@ -204,3 +204,69 @@ def test_grouped_blind_rotation_matches_reference_kernels(pkg, oracle, ref, pres
     got = dev["acc"].cpu().numpy().view(np.uint64).reshape(batch, 2, N)
     assert not np.array_equal(got, init)
     assert np.array_equal(got, want)
+
+
+def _mb3_soa_keys(mbk, p):
+    """The grouped mb = 3 keys [groups][7][2 digits][2][N] re-laid as the reference's 7 SoA subset
+    keys [groups][N/32 tiles][2 digits][2][32 lanes] (kernel_SwizzleRFKey, kernel.cu:2383-2404)."""
+    groups = -(-p.n // 3)
+    l2 = 2 * p.digits_g
+    k = np.asarray(mbk).reshape(groups, 7, l2, 2, p.N // 32, 32)
+    return [np.ascontiguousarray(k[:, s].transpose(0, 3, 1, 2, 4)).reshape(-1) for s in range(7)]
+
+
+@pytest.mark.parametrize("preset", ["3x12", "2x18"])
+def test_grouped_mb3_soa_matches_reference_kernels(pkg, oracle, ref, preset):
+    """The reference's AES-default grouping (CIRBTS_PBS_MULTIBIT=3 with SoA keys and N-major
+    index positions: kernel_EvalAccCore_Binary_MB3_Grouped_Batch_SoA_NMajor, kernel.cu:4585-4771,
+    fused-NTT threads per block 384, EvalAcc block X 128) with the product's grouped mb = 3 keys
+    reproduces the oracle's exact grouped accumulator word for word; the product's FFT mb = 3
+    rotation is checked against that oracle within its phase-error bound (test_cbs_fft_gpu.py)."""
+    vp, u32, u64 = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64
+    ref.ref_cirbts_index_nmajor.argtypes = [vp, u32, u32, u32, u32, u64, u32, vp, vp]
+    ref.ref_cirbts_index_nmajor.restype = ctypes.c_int
+    ref.ref_cirbts_blind_rotate_mb3_soa.argtypes = [vp, u32, u32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, u32, u64,
+                                                    u32, u32, vp, u32, u32, vp, vp, vp]
+    ref.ref_cirbts_blind_rotate_mb3_soa.restype = ctypes.c_int
+    oracle.orc_blind_rotate_mb.argtypes = [vp, vp, vp, u32, vp, vp, u32, u32, vp, ctypes.c_int]
+    p = pkg.preset_params(preset)
+    N, n, Q = p.N, p.n, p.Q
+    keys = pkg.generate_keys_host(p, 37)
+    mbk = np.ascontiguousarray(pkg.generate_mb_bsk_host(p, 37, 3))
+    oc = OracleCbs(oracle, p, keys)
+    batch = 2
+    rng = np.random.default_rng(14)
+    a = rng.integers(0, p.q_lwe, size=(batch, n), dtype=np.uint64)
+    b = rng.integers(0, p.q_lwe, batch, dtype=np.uint64)
+    init = _orc_acc(oracle, oc, a, b, 0)
+    want = _orc_acc(oracle, oc, a, b, n, mbk=mbk, mb=3)
+    tabs, ninv, dmod = _tables(pkg, N, Q)
+    monic = _monic(oracle, oc, N, Q)
+    soa = _mb3_soa_keys(mbk, p)
+    shoups = []
+    for k in soa:
+        ks = np.zeros_like(k)
+        ref.ref_cirbts_shoup(k.ctypes.data, ks.ctypes.data, k.size, Q)
+        shoups.append(ks)
+    d_keys = [_dev(k) for k in soa]
+    d_shoups = [_dev(k) for k in shoups]
+    kp = (ctypes.c_void_p * 7)(*[t.data_ptr() for t in d_keys])
+    ksp = (ctypes.c_void_p * 7)(*[t.data_ptr() for t in d_shoups])
+    bitwidth = max(0, (p.num_lut - 1).bit_length())
+    dev = {name: _dev(v) for name, v in [("acc", init), ("a", a), ("monic", monic), ("mod", dmod), ("tw", tabs[0]),
+                                         ("tws", tabs[1]), ("itw", tabs[2]), ("itws", tabs[3]), ("ninv", ninv)]}
+    idx = torch.zeros(n * batch, dtype=torch.int32, device="cuda")
+    ct = torch.zeros(2 * batch * N, dtype=torch.int64, device="cuda")
+    dct = torch.zeros(2 * p.digits_g * batch * N, dtype=torch.int64, device="cuda")
+    assert ref.ref_cirbts_index_nmajor(dev["a"].data_ptr(), n, n, batch, N, p.q_lwe, bitwidth, idx.data_ptr(),
+                                       None) == 0
+    st = ref.ref_cirbts_blind_rotate_mb3_soa(
+        dev["acc"].data_ptr(), n, batch, kp, ksp, dev["monic"].data_ptr(), dev["mod"].data_ptr(), dev["tw"].data_ptr(),
+        dev["tws"].data_ptr(), dev["itw"].data_ptr(), dev["itws"].data_ptr(), dev["ninv"].data_ptr(),
+        dev["ninv"].data_ptr() + 8, N, Q, p.base_g, p.digits_g, idx.data_ptr(), 384, 128, ct.data_ptr(),
+        dct.data_ptr(), None)
+    torch.cuda.synchronize()
+    assert st == 0
+    got = dev["acc"].cpu().numpy().view(np.uint64).reshape(batch, 2, N)
+    assert not np.array_equal(got, init)
+    assert np.array_equal(got, want)

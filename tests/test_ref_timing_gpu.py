@@ -275,3 +275,96 @@ def test_trace_schemeswitch_timing_beside_reference_kernels(pkg):
           f"{times['ntt'] * 1e3 / count:.2f}, product FP64 FFT {times['fft'] * 1e3 / count:.2f}, "
           f"reference kernels {times['ref'] * 1e3 / count:.2f}")
     assert torch.equal(rows["ntt"], rows["ref"])
+
+
+@pytest.mark.parametrize("preset", ["3x12", "2x18"])
+def test_blind_rotation_timing_beside_reference_aes_default(pkg, preset):
+    """The reference's fastest shipped blind-rotation configuration for its AES example
+    (examples/aes_transcipher/main.cu:107-136: CIRBTS_PBS_MULTIBIT=3, SoA keys, N-major index
+    positions, EvalAcc block X 128, fused-NTT threads per block 384;
+    kernel_EvalAccCore_Binary_MB3_Grouped_Batch_SoA_NMajor, kernel.cu:4585) beside the product's
+    blind rotation (FP64 FFT, mb = 2, the tuned default schedule, and mb = 3) on the same
+    parameter set and batch.  The reference's scratch and index positions are prepared outside
+    the timed region (its own driver allocates inside every call); best of 3 repeats each.  The
+    fused INTT + decomposition kernel for one-digit gadgets (kernel.cu:561, AES2048_D1) does not
+    apply to these two- and three-digit gadgets."""
+    if not REF_SO.exists():
+        pytest.skip("reference CirBTS kernels not built (make -C oracle ref_gpu_cirbts)")
+    from test_ref_cirbts_gpu import _mb3_soa_keys
+    ref = ctypes.CDLL(str(REF_SO))
+    vp, u32, u64, sz = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_size_t
+    ref.ref_cirbts_shoup.argtypes = [vp, vp, sz, u64]
+    ref.ref_cirbts_index_nmajor.argtypes = [vp, u32, u32, u32, u32, u64, u32, vp, vp]
+    ref.ref_cirbts_index_nmajor.restype = ctypes.c_int
+    ref.ref_cirbts_blind_rotate_mb3_soa.argtypes = [vp, u32, u32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, u32, u64,
+                                                    u32, u32, vp, u32, u32, vp, vp, vp]
+    ref.ref_cirbts_blind_rotate_mb3_soa.restype = ctypes.c_int
+
+    p = pkg.preset_params(preset)
+    ctx = pkg.Context(params=p, max_batch=BATCH)
+    ctx.keygen(43)
+    N, n, Q = p.N, p.n, p.Q
+    rng = np.random.default_rng(5)
+    a = rng.integers(0, p.q_lwe, size=(BATCH, n), dtype=np.uint64)
+    b = rng.integers(0, p.q_lwe, BATCH, dtype=np.uint64)
+    da, db = _dev(a), _dev(b)
+    mv = torch.empty((BATCH, p.num_lut, 2, N), dtype=torch.int64, device="cuda")
+    results = {}
+
+    def ours():
+        pkg.call("cbs_blind_rotate_batch_device", ctx.handle, da.data_ptr(), db.data_ptr(), BATCH, n, mv.data_ptr(),
+                 None)
+
+    ctx.set_br_backend(pkg.BR_FFT64)
+    for name, mb in [("product FP64 FFT, mb = 2", 2), ("product FP64 FFT, mb = 3", 3)]:
+        ctx.set_br_multibit(mb)
+        results[name] = _time_ms(ours, reps=3)
+    mbk = ctx.export_mb_bsk()  # mb = 3 keys
+    soa = _mb3_soa_keys(mbk, p)
+    del mbk
+    d_keys, d_shoups = [], []
+    for k in soa:
+        ks = np.zeros_like(k)
+        ref.ref_cirbts_shoup(k.ctypes.data, ks.ctypes.data, k.size, Q)
+        d_keys.append(_dev(k))
+        d_shoups.append(_dev(ks))
+    kp = (ctypes.c_void_p * 7)(*[t.data_ptr() for t in d_keys])
+    ksp = (ctypes.c_void_p * 7)(*[t.data_ptr() for t in d_shoups])
+    tabs = [np.zeros(N, np.uint64) for _ in range(4)]
+    ninv = np.zeros(2, np.uint64)
+    dm = pkg.DModulus()
+    pkg.call("cbs_ntt_tables_host", N, Q, *(t.ctypes.data for t in tabs), ninv.ctypes.data, ctypes.addressof(dm))
+    monic = np.zeros((2 * N, N), np.uint64)
+    k = np.arange(1, N)
+    monic[k, k] = 1
+    monic[1:N, 0] = Q - 1
+    monic[N, 0] = Q - 2
+    monic[N + k, k] = Q - 1
+    monic[N + k, 0] = Q - 1
+    d_monic = _dev(monic)
+    dev = {nm: _dev(v) for nm, v in [("tw", tabs[0]), ("tws", tabs[1]), ("itw", tabs[2]), ("itws", tabs[3]),
+                                     ("ninv", ninv),
+                                     ("mod", np.array([dm.value, dm.const_ratio[0], dm.const_ratio[1]], np.uint64))]}
+    pkg.call("cbs_fnwt_1d_opt_batched", d_monic.data_ptr(), dev["tw"].data_ptr(), dev["tws"].data_ptr(),
+             dev["mod"].data_ptr(), N, 2 * N, None)
+    bitwidth = max(0, (p.num_lut - 1).bit_length())
+    acc = torch.from_numpy(rng.integers(0, Q, size=(BATCH, 2, N), dtype=np.uint64).view(np.int64)).cuda()
+    idx = torch.zeros(n * BATCH, dtype=torch.int32, device="cuda")
+    ct = torch.zeros(2 * BATCH * N, dtype=torch.int64, device="cuda")
+    dct = torch.zeros(2 * p.digits_g * BATCH * N, dtype=torch.int64, device="cuda")
+    assert ref.ref_cirbts_index_nmajor(da.data_ptr(), n, n, BATCH, N, p.q_lwe, bitwidth, idx.data_ptr(), None) == 0
+
+    def theirs():
+        st = ref.ref_cirbts_blind_rotate_mb3_soa(
+            acc.data_ptr(), n, BATCH, kp, ksp, d_monic.data_ptr(), dev["mod"].data_ptr(), dev["tw"].data_ptr(),
+            dev["tws"].data_ptr(), dev["itw"].data_ptr(), dev["itws"].data_ptr(), dev["ninv"].data_ptr(),
+            dev["ninv"].data_ptr() + 8, N, Q, p.base_g, p.digits_g, idx.data_ptr(), 384, 128, ct.data_ptr(),
+            dct.data_ptr(), None)
+        assert st == 0
+
+    results["reference AES default (MB3 SoA N-major)"] = _time_ms(theirs, reps=3)
+    ctx.close()
+    print(f"\nblind rotation, {preset} gadget, N = {N}, n = {n}, batch {BATCH}, one B200 (us per bootstrap):")
+    for name, ms in results.items():
+        print(f"  {name:42s} {ms * 1e3 / BATCH:9.1f}")
+    assert all(v > 0 for v in results.values())
