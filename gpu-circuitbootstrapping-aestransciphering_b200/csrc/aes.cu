@@ -490,15 +490,17 @@ static cbs_status aes_ctr_host(cbs_context* ctx, const uint8_t* h_counters, cons
     std::vector<uint8_t> bits(T);
     for (size_t blk = 0; blk < blocks; ++blk)
         for (uint32_t t = 0; t < 128; ++t) bits[blk * 128 + t] = (h_counters[blk * 16 + t / 8] >> (t % 8)) & 1u;
-    DevBuf<uint8_t> d_bits;
-    DevBuf<uint64_t> d_a, d_b;
+    // staging buffers kept by the context across calls (grown on demand)
+    AesState& A = c->aes;
+    DevBuf<uint8_t>& d_bits = A.host_bits;
+    DevBuf<uint64_t>&d_a = A.host_a, &d_b = A.host_b;
     CBS_CUDA_TRY(d_bits.upload(bits.data(), T, s));
     CBS_CUDA_TRY(d_a.alloc(T * n));
     CBS_CUDA_TRY(d_b.alloc(T));
     if (cbs_status st = cbs_aes128_ctr_transcipher_device(c, d_bits.p, blocks, d_a.p, d_b.p, 1,
                                                           reinterpret_cast<cbs_stream_t>(s)))
         return st;
-    DevBuf<uint8_t> d_cipher;
+    DevBuf<uint8_t>& d_cipher = A.host_cipher;
     if (h_cipher) {
         CBS_CUDA_TRY(d_cipher.upload(h_cipher, static_cast<size_t>(blocks) * 16, s));
         if (cbs_status st = cbs_aes128_ctr_add_ciphertext_device(c, d_cipher.p, blocks, d_b.p,

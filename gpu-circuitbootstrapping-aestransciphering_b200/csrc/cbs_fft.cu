@@ -563,24 +563,21 @@ __global__ void __launch_bounds__(BrFftCfg<LOGN>::T, 1)
 #pragma unroll
         for (uint32_t d = 0; d < DIGITS; ++d) {
             const double2* k0 = gk + static_cast<size_t>(2 * d + h) * 2 * M;
-            // subsets in the order {0}, {0, 1}, {1} (key blocks 0, 2, 1): x c_0 is formed once and
-            // reused for (x c_0) c_1
-            double2 xc0[8];
 #pragma unroll
-            for (int o = 0; o < static_cast<int>(KS); ++o) {
-                const int s = o == 0 ? 0 : (o == 1 ? 2 : 1);
+            for (int s = 0; s < static_cast<int>(KS); ++s) {
                 double2 ka[8], kb[8];
 #pragma unroll
                 for (int j = 0; j < 8; ++j) {
                     ka[j] = __ldg(k0 + s * kstride + j * TH);
                     kb[j] = __ldg(k0 + s * kstride + M + j * TH);
                 }
+                const uint32_t mask = mb_key_mask(MB, s);
 #pragma unroll
                 for (int j = 0; j < 8; ++j) {
-                    double2 t;
-                    if (s == 0) t = xc0[j] = cmul(d ? x1[j] : x0[j], cbuf[j * T + tid]);
-                    else if (s == 2) t = cmul(xc0[j], cbuf[(8 + j) * T + tid]);
-                    else t = cmul(d ? x1[j] : x0[j], cbuf[(8 + j) * T + tid]);
+                    double2 t = d ? x1[j] : x0[j];
+#pragma unroll
+                    for (int i = 0; i < MB; ++i)
+                        if (mask & (1u << i)) t = cmul(t, cbuf[(i * 8 + j) * T + tid]);
                     cfma(y0[j], t, ka[j]);
                     cfma(y1[j], t, kb[j]);
                 }

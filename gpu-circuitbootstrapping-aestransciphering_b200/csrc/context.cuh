@@ -42,6 +42,9 @@ struct AesState {
     DevBuf<uint32_t> lut_sel[2];          // table id per LUT (normal rounds, final round)
     DevBuf<uint32_t> ctrl_bits;           // [chunk*16][8]
     DevBuf<uint32_t> extract_info;        // [chunk*128]
+    // staging of the host-buffer entry points (counter bits, outputs, public ciphertext)
+    DevBuf<uint8_t> host_bits, host_cipher;
+    DevBuf<uint64_t> host_a, host_b;
     std::array<cudaGraphExec_t, 10> graphs{};
     uint32_t graph_chunk = 0;
     // the captured round graphs hold device pointers of the keys; dropped when keys change
