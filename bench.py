@@ -706,22 +706,22 @@ def run_ragged(args, rank: int, world: int, local_rank: int) -> None:
             cur.wait_stream(s_side)
         return g
 
-    # tile schedule: persistent grid size per parameter set, chosen by timing one replay of
-    # each candidate (0 = one CTA per ciphertext)
+    # tile schedule: the product's autotuner picks each parameter set's persistent grid on its plan
     sms = torch.cuda.get_device_properties(local_rank).multi_processor_count
-    cands = [(0, 0), (4 * sms, 2 * sms), (8 * sms, 4 * sms), (2 * sms, sms)]
     tune = []
+    best = []
+    for i, c in enumerate(ctxs):
+        c.ragged_plan(reqs[i], grid_ctas=0)
+        grid, t_ms = c.ragged_autotune()
+        best.append(grid)
+        tune.append({"set": i, "grid_ctas": grid, "ctas_per_sm": grid / sms, "ms": t_ms})
+
     def replay_on(graph):
         def run():
             with torch.cuda.stream(s_main):  # replay on the stream the events are recorded on
                 graph.replay()
         return run
 
-    for cand in cands:
-        g = capture(cand)
-        tune.append((_timed(torch, s_main, replay_on(g), 1, 1), cand))
-        del g
-    best_ms, best = min(tune)
     g = capture(best)
     with ClockSampler(local_rank) as clk:
         ms = _timed(torch, s_main, replay_on(g), args.warmup, args.steps)
@@ -742,7 +742,8 @@ def run_ragged(args, rank: int, world: int, local_rank: int) -> None:
            "correct": ok, "gpu_launches": args.steps * 4,
            "per_request_launches": {"ms_per_step": per_ms, "value": world * total / (per_ms * 1e-3),
                                     "launches_per_step": 2 * len(bufs), "ragged_speedup": per_ms / ms},
-           "autotune": {"chosen_grid_ctas": list(best), "tried": [{"grid_ctas": list(c), "ms": t} for t, c in tune]},
+           "autotune": {"chosen_grid_ctas": list(best), "per_set": tune,
+                        "note": "cbs_gate_ragged_autotune: one timed launch per candidate grid and set"},
            "clocks": clk.summary()}
     if rank == 0:
         print(json.dumps(out), flush=True)

@@ -98,6 +98,7 @@ def _declare(lib: ctypes.CDLL) -> None:
         "cbs_circuit_bootstrap_batch": (st, [c_vp, c_vp, c_vp, u32, u32, c_vp]),
         "cbs_context_set_br_schedule": (st, [c_vp, u32]),
         "cbs_keygen_device": (st, [c_vp, c_vp]),
+        "cbs_gate_ragged_autotune": (st, [c_vp, c_vp, c_vp]),
         "cbs_autotune_blind_rotation": (st, [c_vp, u32, ctypes.c_char_p, c_vp]),
         "cbs_context_tuned": (st, [c_vp, c_vp]),
         "cbs_extract_keyswitch_device": (st, [c_vp, c_vp, u32, c_vp, u32, c_vp, c_vp, u32, c_vp]),
@@ -426,6 +427,13 @@ class GateContext:
         """requests: sequence of (d_a, d_b, d_out_a, d_out_b, count) device pointers."""
         arr = (GateRequest * max(1, len(requests)))(*[GateRequest(*r) for r in requests])
         call("cbs_gate_ragged_plan", self._h, arr, len(requests), grid_ctas)
+
+    def ragged_autotune(self) -> tuple[int, float]:
+        """Time the current plan at each candidate persistent grid, keep the fastest; returns
+        (grid CTAs, ms)."""
+        g, ms = ctypes.c_uint32(), ctypes.c_double()
+        call("cbs_gate_ragged_autotune", self._h, ctypes.byref(g), ctypes.byref(ms))
+        return g.value, ms.value
 
     def ragged_launch(self, stream: int | None = None) -> None:
         call("cbs_gate_ragged_launch", self._h, stream)

@@ -1359,6 +1359,55 @@ cbs_status cbs_gate_ragged_plan(cbs_gate_context* ctx, const cbs_gate_request* h
     return CBS_OK;
 }
 
+cbs_status cbs_gate_ragged_autotune(cbs_gate_context* ctx, uint32_t* chosen_grid, double* ms_out) {
+    CBS_CHECK_ARG(ctx, "gate_ragged_autotune: null context");
+    if (ctx->plan_items == 0) {
+        set_error("gate_ragged_autotune: no plan (call cbs_gate_ragged_plan first)");
+        return CBS_ERR_NOT_READY;
+    }
+    int dev = 0, sms = 0;
+    CBS_CUDA_TRY(cudaGetDevice(&dev));
+    CBS_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const uint32_t items = ctx->plan_items, keep = ctx->plan_grid;
+    const uint32_t su = static_cast<uint32_t>(sms);
+    const uint32_t cands[] = {items, 2 * su, 4 * su, 8 * su};
+    cudaStream_t s = nullptr;
+    CBS_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaError_t ce = cudaEventCreate(&e0);
+    if (ce == cudaSuccess) ce = cudaEventCreate(&e1);
+    double best_ms = 1e300;
+    uint32_t best = keep;
+    cbs_status st = CBS_OK;
+    for (uint32_t g : cands) {
+        if (ce != cudaSuccess || st != CBS_OK) break;
+        ctx->plan_grid = g > items ? items : g;
+        if ((st = cbs_gate_ragged_launch(ctx, reinterpret_cast<cbs_stream_t>(s)))) break;  // warm-up
+        ce = cudaEventRecord(e0, s);
+        if (ce == cudaSuccess && (st = cbs_gate_ragged_launch(ctx, reinterpret_cast<cbs_stream_t>(s)))) break;
+        if (ce == cudaSuccess) ce = cudaEventRecord(e1, s);
+        if (ce == cudaSuccess) ce = cudaEventSynchronize(e1);
+        float ms = 0;
+        if (ce == cudaSuccess) ce = cudaEventElapsedTime(&ms, e0, e1);
+        if (ce == cudaSuccess && ms < best_ms) {
+            best_ms = ms;
+            best = ctx->plan_grid;
+        }
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaStreamDestroy(s);
+    ctx->plan_grid = (st == CBS_OK && ce == cudaSuccess) ? best : keep;
+    if (st != CBS_OK) return st;
+    if (ce != cudaSuccess) {
+        set_error(std::string("gate_ragged_autotune: ") + cudaGetErrorString(ce));
+        return CBS_ERR_CUDA;
+    }
+    if (chosen_grid) *chosen_grid = best;
+    if (ms_out) *ms_out = best_ms;
+    return CBS_OK;
+}
+
 cbs_status cbs_gate_ragged_launch(cbs_gate_context* ctx, cbs_stream_t stream) {
     CBS_CHECK_ARG(ctx, "gate_ragged_launch: null context");
     if (ctx->plan_items == 0) return CBS_OK;

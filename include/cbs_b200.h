@@ -491,6 +491,12 @@ typedef struct {
 cbs_status cbs_gate_ragged_plan(cbs_gate_context *ctx, const cbs_gate_request *h_reqs, uint32_t num_reqs,
                                 uint32_t grid_ctas);
 cbs_status cbs_gate_ragged_launch(cbs_gate_context *ctx, cbs_stream_t stream);
+/* Picks the persistent grid of the current plan (the ragged launch's tile schedule): times one
+ * ragged launch per candidate (one CTA per ciphertext, 2, 4 and 8 CTAs per SM) with CUDA
+ * events, keeps the fastest in the plan and returns it (and its time in ms; either pointer may
+ * be NULL).  Runs the plan's launches, so the planned outputs are overwritten; synchronous, not
+ * for use inside a stream capture.  No reference counterpart. */
+cbs_status cbs_gate_ragged_autotune(cbs_gate_context *ctx, uint32_t *chosen_grid, double *ms);
 
 /* ------------------------------------------------------------------------------------
  * Torus circuit bootstrapping with private functional key switching (PFKS): an LWE bit

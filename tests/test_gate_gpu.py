@@ -173,6 +173,8 @@ def test_ragged_two_parameter_sets_in_one_graph(pkg):
                      ra.data_ptr(), rb.data_ptr(), None)
             want.append((i, bits, oa, ob, ra, rb))
     ctxs[0].ragged_plan(reqs[0], grid_ctas=0)
+    grid, ms = ctxs[0].ragged_autotune()  # the product's tile choice for set 0's plan
+    assert grid >= 1 and ms > 0
     ctxs[1].ragged_plan(reqs[1], grid_ctas=3)  # fewer CTAs than ciphertexts: CTAs loop
     torch.cuda.synchronize()
     g = torch.cuda.CUDAGraph()
