@@ -210,8 +210,10 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
         # the product's autotuner picks the grouping and schedule (16 waves of 148 ciphertexts)
         tuned = ctx.autotune(min(16 * 148, 128 * min(blocks, 256)))
         args.multibit, args.schedule = tuned["mb"], tuned["schedule"]
-    elif args.multibit > 1:
-        ctx.set_br_multibit(args.multibit)
+    else:
+        if args.multibit > 1:
+            ctx.set_br_multibit(args.multibit)
+        ctx.set_br_schedule(args.schedule)
     key = np.random.default_rng(args.seed).bytes(16)
     pkg.call("cbs_aes128_setup", ctx.handle, key, args.seed + 1)
     p = ctx.params
@@ -318,6 +320,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
                    "param_set": args.params,
                    "l2": "per-step working set (keys + RGSW + LUT buffers) >> 126 MB L2",
                    "br_multibit": args.multibit,
+                   "br_schedule": args.schedule,
                    "br_tuned": tuned,
                    "parallelism": f"replicas x{world} (independent blocks per GPU)"},
         "us_per_bootstrap": ms_per_step * 1e3 / (blocks * 128 * ROUNDS),
@@ -369,6 +372,7 @@ def run_blind_rotate(args, rank: int, world: int, local_rank: int) -> None:
     pkg.call("cbs_context_set_br_backend", ctx.handle, pkg.BR_FFT64 if args.backend == "fft64" else pkg.BR_NTT)
     if args.multibit > 1:
         ctx.set_br_multibit(args.multibit)
+    ctx.set_br_schedule(args.schedule)
     p = ctx.params
     rng = np.random.default_rng(args.seed + rank)
     a = torch.from_numpy(rng.integers(0, p.q_lwe, size=(T, p.n), dtype=np.int64)).cuda()
@@ -386,6 +390,7 @@ def run_blind_rotate(args, rank: int, world: int, local_rank: int) -> None:
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
            "dtype": "f64" if args.backend == "fft64" else "u64", "data": "synthetic (seeded random LWE)",
            "config": {"workload": "blind_rotate", "batch": T, "backend": args.backend, "br_multibit": args.multibit,
+                      "br_schedule": args.schedule,
                       "param_set": args.params, "br_gadget": f"2^{p.base_g.bit_length() - 1}x{p.digits_g}",
                       "l2": "BSK read once per launch (124 MB fft64 / 124 MB ntt); no flush between launches"},
            "us_per_bootstrap": ms * 1e3 / T, "gpu_launches": args.steps,
@@ -860,7 +865,10 @@ def br_kernel_name(args, p=None) -> str:
         return "k_blind_rotate"
     if args.multibit == 1:
         return "k_blind_rotate_fft"
-    if args.multibit == 2 and p is not None and p.digits_g == 2 and getattr(args, "schedule", 0) != 1:
+    sched = getattr(args, "schedule", 0)
+    if args.multibit == 2 and p is not None and p.digits_g == 2 and sched == 3 and p.N == 2048:
+        return "k_blind_rotate_fft_mb2_x2<11> (two ciphertexts per CTA, digit transforms in lockstep)"
+    if args.multibit == 2 and p is not None and p.digits_g == 2 and sched != 1:
         return "k_blind_rotate_fft_mb_d2<11,2> (two digit transforms in lockstep)"
     return f"k_blind_rotate_fft_mb<11,{args.multibit}>"
 
@@ -1075,6 +1083,9 @@ def main() -> None:
                          "(cbs_params_default) or 2^18 x 2")
     ap.add_argument("--no-tune", dest="tune", action="store_false",
                     help="aes128 on fft64: use --multibit instead of the product's autotuned grouping")
+    ap.add_argument("--schedule", choices=["auto", "digitwise", "lockstep", "paired"], default="auto",
+                    help="two-digit grouped blind-rotation schedule (aes128 with --no-tune / --multibit, "
+                         "blind_rotate); auto = the context's tuned choice")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--workload", choices=["aes128", "blind_rotate", "keyswitch", "rns_ntt", "gate", "ragged", "tcb",
                                            "aes_setup", "fp64_peak", "keygen"],
@@ -1091,8 +1102,9 @@ def main() -> None:
         if args.multibit not in (None, 1):
             ap.error("--fft-mode fp32* runs one coefficient per step (--multibit 1)")
         args.multibit = 1
-    if args.multibit is not None:
-        args.tune = False  # an explicit grouping is measured as given
+    args.schedule = {"auto": 0, "digitwise": 1, "lockstep": 2, "paired": 3}[args.schedule]
+    if args.multibit is not None or args.schedule:
+        args.tune = False  # an explicit grouping or schedule is measured as given
     if args.multibit is None:
         args.multibit = 2 if args.backend == "fft64" else 1
     if args.multibit > 1 and args.backend != "fft64":

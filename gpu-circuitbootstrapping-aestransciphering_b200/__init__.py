@@ -209,7 +209,7 @@ class TuneChoice(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
-BR_SCHEDULE_AUTO, BR_SCHEDULE_DIGITWISE, BR_SCHEDULE_LOCKSTEP = 0, 1, 2
+BR_SCHEDULE_AUTO, BR_SCHEDULE_DIGITWISE, BR_SCHEDULE_LOCKSTEP, BR_SCHEDULE_PAIRED = 0, 1, 2, 3
 
 PARAMS_AES_3X12, PARAMS_AES_2X18 = 0, 1
 PRESETS = {"3x12": PARAMS_AES_3X12, "2x18": PARAMS_AES_2X18}
@@ -322,6 +322,10 @@ class Context:
     def set_br_multibit(self, mb: int) -> None:
         """Blind rotation over groups of mb = 1, 2 or 3 LWE coefficients (FFT backend)."""
         call("cbs_context_set_br_multibit", self._h, mb)
+
+    def set_br_schedule(self, schedule: int) -> None:
+        """Two-digit grouped blind-rotation schedule (BR_SCHEDULE_*; AUTO = the tuned one)."""
+        call("cbs_context_set_br_schedule", self._h, schedule)
 
     def export_mb_bsk(self):
         """Grouped blind-rotation keys [ceil(n/mb)][2^mb - 1][2*digits_g][2][N] (NTT domain)."""

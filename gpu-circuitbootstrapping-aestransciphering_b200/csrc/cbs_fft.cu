@@ -633,6 +633,184 @@ __global__ void __launch_bounds__(BrFftCfg<LOGN>::T, 1)
     }
 }
 
+// Paired form of the two-digit grouped blind rotation (mb = 2, 2^18 x 2 gadget): two
+// ciphertexts per CTA of 512 threads, so an SM holds 16 warps instead of 8.  To fit 128
+// registers and the shared memory of two ciphertexts, the work per group is split by output
+// column instead of by input polynomial:
+//  1. each half (128 threads) transforms the two digits of its polynomial in lockstep, with the
+//     digits read straight from the accumulator (no digit buffer), and stores both spectra;
+//  2. after a barrier of the ciphertext's 256 threads, half h forms output column h for its 8
+//     slots from all four digit spectra: y_h += (x_row m_S(psi)) K_S[row][h] over the rows and
+//     subsets, with c_i(psi) = zeta^(a_i e_t) omega8^k - 1 recomputed per slot (no c buffer);
+//  3. after a second barrier (every spectrum read), half h inverse-transforms y_h in its own
+//     spectrum buffer and adds the rounded result into the accumulator positions it owns.
+// Shared memory per CTA: the FFT tables once, then per ciphertext the accumulator [2][N] and
+// the spectra [2 halves][2 digits][N/2] (210 KB at N = 2048).  An odd batch's last CTA runs its
+// second ciphertext as a copy of the first and writes nothing for it.
+template <int LOGN, bool WIDE>
+__global__ void __launch_bounds__(4 * ((1u << LOGN) / 16), 1)
+    k_blind_rotate_fft_mb2_x2(const BlindRotateArgs a, const FftKeyArgs f, uint32_t batch) {
+    constexpr int LOGM = LOGN - 1;
+    constexpr uint32_t N = 1u << LOGN, M = N / 2, TH = M / 8, TWO_N = 2 * N;
+    constexpr uint32_t KS = 3, DIGITS = 2, L2 = 2 * DIGITS;
+    using Tb = FftTab<LOGM>;
+    extern __shared__ __align__(16) uint64_t smem[];
+    double2* tab = reinterpret_cast<double2*>(smem);                 // FftTab<LOGM>, shared
+    const uint32_t tid = threadIdx.x, c2 = tid / (2 * TH), h = (tid / TH) & 1u, ht = tid % TH;
+    const uint32_t lt = tid % (2 * TH);                               // thread within the ciphertext
+    const uint32_t ct_raw = 2 * blockIdx.x + c2;
+    const bool live = ct_raw < batch;
+    const uint32_t ct = live ? ct_raw : batch - 1;
+    // per-ciphertext region after the tables: acc [2][N] u64, spec [2][2][M] double2
+    constexpr size_t tab_words = (Tb::size() * sizeof(double2) + 15) / 16 * 2;  // 16-byte aligned, in u64
+    constexpr size_t ct_words = 2 * N + 4 * M * 2;
+    uint64_t* acc = smem + tab_words + c2 * ct_words;
+    double2* spec = reinterpret_cast<double2*>(acc + 2 * N);           // [p][d][M]
+    const double2* tws = tab + Tb::twist_off();
+    int64_t* my_acc = reinterpret_cast<int64_t*>(acc) + h * N;
+    double2* my_s0 = spec + (2 * h) * M;
+    double2* my_s1 = my_s0 + M;
+    const uint64_t Q = a.t.q;
+    const int gbits = a.g.gbits;
+    int64_t offset = 0;
+    for (uint32_t k = 0; k < DIGITS; ++k) offset += static_cast<int64_t>(1) << (gbits * k + gbits - 1);
+    const int ign = a.g.ign;
+    const uint64_t qhalf = Q >> 1;
+    const uint64_t round_c = (ign ? (uint64_t(1) << (ign - 1)) : 0) + (static_cast<uint64_t>(offset) << ign);
+    const int64_t hi_b = static_cast<int64_t>(round_c + qhalf), Qs = static_cast<int64_t>(Q), lo_b = hi_b - Qs;
+    auto to_offset = [&](uint64_t x) {
+        return static_cast<int64_t>(x + round_c) - (x >= qhalf ? Qs : 0);
+    };
+
+    for (uint32_t i = tid; i < Tb::size(); i += blockDim.x) tab[i] = f.tab[i];
+    {
+        const uint32_t bt = special_ms_f(a.b[ct], TWO_N, a.q_lwe, a.bitwidth);
+        int64_t* y = reinterpret_cast<int64_t*>(acc);
+        for (uint32_t i = lt; i < N; i += 2 * TH) {
+            y[i] = to_offset(0);
+            const uint32_t s = (i + bt) & (TWO_N - 1);
+            const uint64_t v = (s < N) ? a.tv[s] : a.tv[s - N];
+            y[N + i] = to_offset((s < N) ? v : (v ? Q - v : 0));
+        }
+    }
+    __syncthreads();
+
+    // named barriers: 1 + c2 over the ciphertext's 256 threads, 3 + 2 c2 + h over a half
+    const uint32_t ct_bar = 1 + c2, half_id = 3 + 2 * c2 + h;
+    auto ct_sync = [ct_bar]() { asm volatile("bar.sync %0, %1;" ::"r"(ct_bar), "n"(2 * TH) : "memory"); };
+    auto half_bar = [half_id]() { asm volatile("bar.sync %0, %1;" ::"r"(half_id), "n"(TH) : "memory"); };
+    const int32_t dbias = 1 << (gbits - 1);
+    const uint32_t fmask = (1u << gbits) - 1u;
+    const uint64_t* arow = a.a + static_cast<size_t>(ct) * a.a_stride;
+    const uint32_t groups = (a.n + 1) / 2;
+    constexpr size_t kstride = static_cast<size_t>(L2) * 2 * M;  // spectra between subsets of a group
+    for (uint32_t g = 0; g < groups; ++g) {
+        // 1. the two digit transforms of polynomial h, digits read from the accumulator
+        double2 x0[8], x1[8];
+        fft_forward2_to_regs<LOGM>(
+            my_s0, my_s1, ht, tab,
+            [&](int j, uint32_t e) {
+                const uint64_t wr = static_cast<uint64_t>(my_acc[e]) >> ign;
+                const uint64_t wi = static_cast<uint64_t>(my_acc[e + M]) >> ign;
+                return cmul(DigitPair<true>::unpack(make_uint2(static_cast<uint32_t>(wr) & fmask,
+                                                               static_cast<uint32_t>(wi) & fmask),
+                                                    dbias),
+                            twist_at<LOGM>(tws, j, e));
+            },
+            [&](int j, uint32_t e) {
+                const uint64_t wr = static_cast<uint64_t>(my_acc[e]) >> ign;
+                const uint64_t wi = static_cast<uint64_t>(my_acc[e + M]) >> ign;
+                return cmul(DigitPair<true>::unpack(make_uint2(static_cast<uint32_t>(wr >> gbits) & fmask,
+                                                               static_cast<uint32_t>(wi >> gbits) & fmask),
+                                                    dbias),
+                            twist_at<LOGM>(tws, j, e));
+            },
+            x0, x1, half_bar);
+        half_bar();  // the transforms' last reads of my_s0 / my_s1 are done
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            my_s0[cswz(8 * ht + j)] = x0[j];
+            my_s1[cswz(8 * ht + j)] = x1[j];
+        }
+        // the group's rotations (read before the barrier, their latency hidden by it)
+        const uint32_t idx0 = 2 * g, idx1 = idx0 + 1;
+        const uint32_t at0 = special_ms_f(__ldg(arow + idx0), TWO_N, a.q_lwe, a.bitwidth);
+        const uint32_t at1 = idx1 < a.n ? special_ms_f(__ldg(arow + idx1), TWO_N, a.q_lwe, a.bitwidth) : 0u;
+        const double2 ub0 = zeta_pow<LOGN>(tws, mult_base<LOGN>(ht, at0));
+        const double2 ub1 = zeta_pow<LOGN>(tws, mult_base<LOGN>(ht, at1));
+        ct_sync();
+        // 2. output column h from the four digit spectra
+        const double2* gk = f.bskf + static_cast<size_t>(g) * KS * kstride + static_cast<size_t>(h) * M + ht;
+        double2 y[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const uint32_t r3 = ((j & 1) << 2) | (j & 2) | ((j >> 2) & 1);
+            double2 c0, c1;
+            {
+                const uint32_t k = (at0 * r3) & 7u;
+                double2 w = tab[(k & 3u) * (M / 8)];
+                if (k & 4u) w = make_double2(-w.x, -w.y);
+                c0 = cmul(ub0, w);
+                c0.x -= 1.0;
+            }
+            {
+                const uint32_t k = (at1 * r3) & 7u;
+                double2 w = tab[(k & 3u) * (M / 8)];
+                if (k & 4u) w = make_double2(-w.x, -w.y);
+                c1 = cmul(ub1, w);
+                c1.x -= 1.0;
+            }
+            const double2 c01 = cmul(c0, c1);
+            double2 acc_j = make_double2(0.0, 0.0);
+#pragma unroll
+            for (uint32_t row = 0; row < L2; ++row) {
+                // row 2d + p: digit d of polynomial p, spectrum buffer p, d
+                const double2 x = spec[((row & 1u) * 2 + (row >> 1)) * M + cswz(8 * ht + j)];
+                const double2* kr = gk + static_cast<size_t>(row) * 2 * M + j * TH;
+                cfma(acc_j, cmul(x, c0), __ldg(kr));
+                cfma(acc_j, cmul(x, c1), __ldg(kr + kstride));
+                cfma(acc_j, cmul(x, c01), __ldg(kr + 2 * kstride));
+            }
+            y[j] = acc_j;
+        }
+        ct_sync();  // every spectrum read is done before the inverse transforms reuse the buffers
+        // 3. inverse transform, rounding, accumulate
+        fft_inverse_from_regs<LOGM>(
+            my_s0, ht, tab, y,
+            [&](int j, uint32_t e, double2 v) {
+                const double2 u = cmulc(v, twist_at<LOGM>(tws, j, e));
+                my_acc[e] = offset_add(my_acc[e], centred_residue(u.x * f.inv_m, f), lo_b, hi_b, Qs);
+                my_acc[e + M] = offset_add(my_acc[e + M], centred_residue(u.y * f.inv_m, f), lo_b, hi_b, Qs);
+            },
+            half_bar);
+    }
+    ct_sync();
+
+    // finalize and the MV split, as in the one-bit form
+    for (uint32_t i = lt; i < N; i += 2 * TH) {
+        const int64_t* y = reinterpret_cast<const int64_t*>(acc);
+        const int64_t v0 = y[i] - static_cast<int64_t>(round_c), v1 = y[N + i] - static_cast<int64_t>(round_c);
+        const uint64_t x0 = static_cast<uint64_t>(v0 < 0 ? v0 + Qs : v0);
+        const uint64_t x1 = static_cast<uint64_t>(v1 < 0 ? v1 + Qs : v1);
+        acc[i] = mul_shoup(x0, a.t.n_inv, a.t.n_inv_s, Q);
+        uint64_t v = mul_shoup(x1, a.t.n_inv, a.t.n_inv_s, Q);
+        if (i < a.num_lut) v = add_mod(v, a.gadd[i], Q);
+        acc[N + i] = v;
+    }
+    ct_sync();
+    if (!live) return;
+    for (uint32_t j = 0; j < a.num_lut; ++j) {
+        for (uint32_t p = 0; p < 2; ++p) {
+            const uint64_t* src = acc + p * N;
+            uint64_t* dst = a.mv_out + ((static_cast<size_t>(ct) * a.num_lut + j) * 2 + p) * N;
+            for (uint32_t i = lt; i < N; i += 2 * TH) {
+                const uint32_t s = i + j;
+                dst[i] = (s < N) ? src[s] : (src[s - N] ? Q - src[s - N] : 0);
+            }
+        }
+    }
+}
+
 cudaError_t ntt_forward(uint64_t* out, const uint64_t* in, const uint64_t* tw, const uint64_t* tws,
                         const cbs_dmodulus* mod, size_t dim, size_t batch, cudaStream_t s);
 
@@ -716,8 +894,32 @@ static cudaError_t br_fft_mb_d2_launch(const BlindRotateArgs& a, const FftKeyArg
     return cudaGetLastError();
 }
 
+template <int LOGN>
+static cudaError_t br_fft_mb2_x2_launch(const BlindRotateArgs& a, const FftKeyArgs& f, uint32_t batch,
+                                        cudaStream_t s) {
+    constexpr uint32_t N = 1u << LOGN, M = N / 2;
+    constexpr size_t tab_bytes = (FftTab<LOGN - 1>::size() * sizeof(double2) + 15) / 16 * 16;
+    const size_t smem = tab_bytes + 2 * (2ull * N * sizeof(uint64_t) + 4ull * M * sizeof(double2));
+    if (f.tab_len != FftTab<LOGN - 1>::size()) return cudaErrorInvalidValue;
+    static size_t configured[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (configured[dev] < smem) {
+        cudaError_t e = cudaFuncSetAttribute(k_blind_rotate_fft_mb2_x2<LOGN, true>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+        if (e != cudaSuccess) return e;
+        configured[dev] = smem;
+    }
+    k_blind_rotate_fft_mb2_x2<LOGN, true><<<(batch + 1) / 2, 4 * (N / 16), smem, s>>>(a, f, batch);
+    return cudaGetLastError();
+}
+
 template <int LOGN, int MB>
 static cudaError_t br_fft_mb_launch(const BlindRotateArgs& a, const FftKeyArgs& f, uint32_t batch, cudaStream_t s) {
+    if constexpr (MB == 2 && LOGN == 11) {
+        // two ciphertexts per CTA (digits read from the accumulator: any digit width up to 24 bits)
+        if (a.digits == 2 && a.schedule == CBS_BR_SCHEDULE_PAIRED) return br_fft_mb2_x2_launch<LOGN>(a, f, batch, s);
+    }
     if constexpr (MB == 2) {
         // the two-digit gadget: both digit transforms in lockstep unless the digit-by-digit
         // schedule was chosen

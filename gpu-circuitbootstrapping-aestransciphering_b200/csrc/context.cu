@@ -614,7 +614,7 @@ cbs_status cbs_import_mb_bsk(cbs_context* ctx, uint32_t mb, const uint64_t* keys
 
 cbs_status cbs_context_set_br_schedule(cbs_context* ctx, uint32_t schedule) {
     CBS_CHECK_ARG(ctx, "set_br_schedule: null context");
-    CBS_CHECK_ARG(schedule <= CBS_BR_SCHEDULE_LOCKSTEP, "set_br_schedule: unknown schedule");
+    CBS_CHECK_ARG(schedule <= CBS_BR_SCHEDULE_PAIRED, "set_br_schedule: unknown schedule");
     ctx->br_schedule = schedule;
     ctx->aes.drop_graphs();  // captured rounds bake in the kernel choice
     return CBS_OK;

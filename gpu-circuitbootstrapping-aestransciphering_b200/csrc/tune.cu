@@ -2,7 +2,8 @@
 //
 // The blind rotation has two launch-form knobs on the FFT64 backend: the grouping mb (1, 2 or 3
 // LWE coefficients per step, with 2^mb - 1 grouped keys) and, for a two-digit gadget with mb = 2,
-// the schedule of the two digit transforms (lockstep or one after the other).  The tuner times
+// the schedule (the two digit transforms one after the other, in lockstep, or in lockstep with
+// two ciphertexts per CTA at N = 2048).  The tuner times
 // every candidate on a synthetic batch with CUDA events and keeps the fastest; the choice is
 // stored per (GPU name, parameter set, batch bucket) in a small JSON file that every context
 // reads at creation.  (The reference has no tuner of its own: ~70 environment knobs,
@@ -100,7 +101,7 @@ static std::vector<CacheEntry> read_cache(const std::string& file) {
             continue;
         field_num(line, "batch", &batch);
         field_num(line, "candidates", &cand);
-        if (mb < 1 || mb > 3 || sch < 0 || sch > CBS_BR_SCHEDULE_LOCKSTEP) continue;
+        if (mb < 1 || mb > 3 || sch < 0 || sch > CBS_BR_SCHEDULE_PAIRED) continue;
         e.bucket = static_cast<uint32_t>(bucket);
         e.choice.mb = static_cast<uint32_t>(mb);
         e.choice.schedule = static_cast<uint32_t>(sch);
@@ -214,6 +215,7 @@ cbs_status cbs_autotune_blind_rotation(cbs_context* ctx, uint32_t batch, const c
         if (cbs_status st = cbs_context_set_br_multibit(c, mb)) return st;
         std::vector<uint32_t> schedules = {CBS_BR_SCHEDULE_DIGITWISE};
         if (mb == 2 && c->p.digits_g == 2) schedules.push_back(CBS_BR_SCHEDULE_LOCKSTEP);
+        if (mb == 2 && c->p.digits_g == 2 && c->p.N == 2048 && batch >= 2) schedules.push_back(CBS_BR_SCHEDULE_PAIRED);
         for (uint32_t sch : schedules) {
             c->br_schedule = sch;
             if (cbs_status st = run_blind_rotate(c, d_a.p, d_b.p, batch, c->p.n, c->d_mv.p, s, false)) return st;

@@ -176,10 +176,13 @@ cbs_status cbs_context_set_br_backend(cbs_context *ctx, int backend);
 cbs_status cbs_context_set_br_multibit(cbs_context *ctx, uint32_t mb);
 /* Schedule of the grouped FFT blind rotation with a two-digit gadget: CBS_BR_SCHEDULE_LOCKSTEP
  * transforms both digits of a polynomial together (interleaved butterflies, shared barriers),
- * CBS_BR_SCHEDULE_DIGITWISE one after the other; CBS_BR_SCHEDULE_AUTO (default) takes the
- * autotuner's cached choice for this GPU and parameter set, else lockstep.  Results differ only
- * by FP64 rounding (both within the phase-error bound).  No reference counterpart. */
-enum { CBS_BR_SCHEDULE_AUTO = 0, CBS_BR_SCHEDULE_DIGITWISE = 1, CBS_BR_SCHEDULE_LOCKSTEP = 2 };
+ * CBS_BR_SCHEDULE_DIGITWISE one after the other, CBS_BR_SCHEDULE_PAIRED runs two ciphertexts per
+ * CTA (mb = 2, N = 2048; 16 warps per SM, work split by output column);
+ * CBS_BR_SCHEDULE_AUTO (default) takes the autotuner's cached choice for this GPU and parameter
+ * set, else lockstep.  Results differ only by FP64 rounding (all within the phase-error bound).
+ * No reference counterpart. */
+enum { CBS_BR_SCHEDULE_AUTO = 0, CBS_BR_SCHEDULE_DIGITWISE = 1, CBS_BR_SCHEDULE_LOCKSTEP = 2,
+       CBS_BR_SCHEDULE_PAIRED = 3 };
 cbs_status cbs_context_set_br_schedule(cbs_context *ctx, uint32_t schedule);
 
 /* Autotuner of the blind rotation (no reference counterpart: the reference exposes ~70
@@ -196,7 +199,7 @@ cbs_status cbs_context_set_br_schedule(cbs_context *ctx, uint32_t schedule);
  * Synchronous; allocates; not for use inside a stream capture. */
 typedef struct {
     uint32_t mb;             /* grouping of the blind rotation (1, 2 or 3) */
-    uint32_t schedule;       /* CBS_BR_SCHEDULE_DIGITWISE or CBS_BR_SCHEDULE_LOCKSTEP */
+    uint32_t schedule;       /* CBS_BR_SCHEDULE_DIGITWISE, _LOCKSTEP or _PAIRED */
     double us_per_bootstrap; /* measured at the tuned batch */
     uint32_t batch;          /* the batch the choice was measured at */
     uint32_t candidates;     /* configurations timed */

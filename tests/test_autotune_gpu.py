@@ -1,5 +1,5 @@
-"""The blind-rotation autotuner: it times every grouping (mb = 1, 2, 3) and both schedules of the
-two-digit gadget, applies the fastest, writes it to the tuning cache, and a context created
+"""The blind-rotation autotuner: it times every grouping (mb = 1, 2, 3) and the three schedules of
+the two-digit gadget at mb = 2, applies the fastest, writes it to the tuning cache, and a context created
 afterwards reads the cache and takes the cached grouping when the FFT64 backend is selected
 (unless the caller sets mb)."""
 from __future__ import annotations
@@ -22,8 +22,8 @@ def test_autotune_caches_and_applies(pkg, tmp_path, monkeypatch):
         c.keygen(3)
         c.set_br_backend(pkg.BR_FFT64)
         choice = c.autotune(296)
-        assert choice["mb"] in (1, 2, 3) and choice["candidates"] == 4 and choice["us_per_bootstrap"] > 0
-        assert choice["schedule"] in (pkg.BR_SCHEDULE_DIGITWISE, pkg.BR_SCHEDULE_LOCKSTEP)
+        assert choice["mb"] in (1, 2, 3) and choice["candidates"] == 5 and choice["us_per_bootstrap"] > 0
+        assert choice["schedule"] in (pkg.BR_SCHEDULE_DIGITWISE, pkg.BR_SCHEDULE_LOCKSTEP, pkg.BR_SCHEDULE_PAIRED)
         print(f"tuned: {choice}")
         entries = json.loads(cache.read_text())
         assert len(entries) == 1 and entries[0]["mb"] == choice["mb"] and entries[0]["bucket"] == 512

@@ -72,33 +72,45 @@ def test_exact_blind_rotate_bit_exact(pkg, wctx, wkeys, woc):
     assert np.array_equal(mv.cpu().numpy().view(np.uint64).reshape(want.shape), want)
 
 
-def test_grouped_fft_blind_rotate_phase_error(pkg, wctx, wkeys, woc):
+@pytest.mark.parametrize("schedule,bits", [("digitwise", [0, 1, 1]), ("lockstep", [0, 1, 1]),
+                                           ("paired", [0, 1, 1]), ("paired", [1, 0, 1, 1])])
+def test_grouped_fft_blind_rotate_phase_error(pkg, wctx, wkeys, woc, schedule, bits):
+    """Every schedule of the two-digit grouped rotation; the paired one (two ciphertexts per CTA)
+    on an odd batch (its last CTA runs a copy of the last ciphertext and writes nothing for it)
+    and an even one."""
     p = wctx.params
+    sched = {"digitwise": pkg.BR_SCHEDULE_DIGITWISE, "lockstep": pkg.BR_SCHEDULE_LOCKSTEP,
+             "paired": pkg.BR_SCHEDULE_PAIRED}[schedule]
+    B = len(bits)
     pkg.call("cbs_context_set_br_backend", wctx.handle, pkg.BR_FFT64)
     wctx.set_br_multibit(2)
+    wctx.set_br_schedule(sched)
     try:
         mbk = wctx.export_mb_bsk()
         rng = np.random.default_rng(6)
-        a, b = lwe_encrypt_bits(rng, wkeys["s_lwe"], [0, 1, 1], p.q_lwe)
-        mv = torch.zeros((3, p.num_lut, 2, p.N), dtype=torch.int64, device="cuda")
+        a, b = lwe_encrypt_bits(rng, wkeys["s_lwe"], bits, p.q_lwe)
+        mv = torch.full((B + 1, p.num_lut, 2, p.N), 7, dtype=torch.int64, device="cuda")
         da, db = _dev(a), _dev(b)
-        pkg.call("cbs_blind_rotate_batch_device", wctx.handle, da.data_ptr(), db.data_ptr(), 3, p.n, mv.data_ptr(),
+        pkg.call("cbs_blind_rotate_batch_device", wctx.handle, da.data_ptr(), db.data_ptr(), B, p.n, mv.data_ptr(),
                  None)
         torch.cuda.synchronize()
     finally:
+        wctx.set_br_schedule(pkg.BR_SCHEDULE_AUTO)
         pkg.call("cbs_context_set_br_backend", wctx.handle, pkg.BR_NTT)
-    got = mv.cpu().numpy().view(np.uint64).reshape(3, p.num_lut, 2, p.N)
+    allv = mv.cpu().numpy().view(np.uint64)
+    assert (allv[B] == 7).all()  # nothing written past the batch
+    got = allv[:B].reshape(B, p.num_lut, 2, p.N)
     want = woc.br_acc_mb(a, b, mbk, 2)
     Q, N = p.Q, p.N
     worst, sq, cnt = 0, 0.0, 0
-    for i in range(3):
+    for i in range(B):
         d = woc.phase_coef(got[i, 0]) - woc.phase_coef(want[i])
         e = [((int(x) * N + Q // 2) % Q) - Q // 2 for x in d]
         worst = max(worst, max(abs(x) for x in e))
         sq += sum(float(x) * float(x) for x in e)
         cnt += len(e)
     log2 = np.log2(worst + 1)
-    print(f"2x18 grouped FFT blind rotation: phase error rms 2^{0.5 * np.log2(sq / cnt):.1f}, max 2^{log2:.1f}")
+    print(f"2x18 grouped FFT blind rotation ({schedule}, batch {B}): phase error rms 2^{0.5 * np.log2(sq / cnt):.1f}, max 2^{log2:.1f}")
     assert log2 < FFT_PHASE_TOL_LOG2_2X18
 
 

@@ -368,3 +368,74 @@ def test_blind_rotation_timing_beside_reference_aes_default(pkg, preset):
     for name, ms in results.items():
         print(f"  {name:42s} {ms * 1e3 / BATCH:9.1f}")
     assert all(v > 0 for v in results.values())
+
+
+def test_modup_moddown_timing_beside_reference_rns_tool(pkg):
+    """The product's modup and moddown_from_NTT (cbs_rns_modup, cbs_rns_moddown_from_ntt) against
+    the reference's DRNSTool::modup / moddown_from_NTT (include/rns.cuh:156-164, rebuilt by
+    `make -C oracle ref_gpu_rns`, one call per ciphertext as the reference's key switch makes
+    them) on the key-switching configuration N = 2^16, 24 + 2 primes, 32 ciphertexts; the
+    outputs must agree word for word."""
+    so = ORACLE_DIR / "_ref" / "libref_rns.so"
+    if not so.exists():
+        pytest.skip("reference Phantom RNS tool not built (make -C oracle ref_gpu_rns)")
+    lib = ctypes.CDLL(str(so))
+    vp, u32 = ctypes.c_void_p, ctypes.c_uint32
+    lib.ref_rns_create.argtypes = [u32, vp, u32, u32]
+    lib.ref_rns_create.restype = vp
+    lib.ref_rns_destroy.argtypes = [vp]
+    lib.ref_rns_modup.argtypes = [vp, u32, vp, vp, u32, vp]
+    lib.ref_rns_moddown_from_ntt.argtypes = [vp, u32, vp, vp, u32, vp]
+    logn, size_q, size_p, count = 16, 24, 2, 32
+    n = 1 << logn
+    chain = np.zeros(size_q + size_p, np.uint64)
+    pkg.call("cbs_get_primes", n, 50, size_q + size_p, chain.ctypes.data)
+    q, p = chain[:size_q].copy(), chain[size_q:].copy()
+    ctx = pkg.RnsContext(n, q, p)
+    rctx = lib.ref_rns_create(logn, chain.ctypes.data, size_q, size_p)
+    assert rctx
+    try:
+        beta, qlp = ctx.beta(size_q), size_q + size_p
+        mods_q = torch.from_numpy(q.view(np.int64)).cuda().view(1, -1, 1)
+        c2 = torch.remainder(torch.randint(0, 2 ** 62, (count, size_q, n), dtype=torch.int64, device="cuda"), mods_q)
+        mine = torch.zeros((count, beta, qlp, n), dtype=torch.int64, device="cuda")
+        theirs = torch.zeros_like(mine)
+        t_up = _time_ms(lambda: pkg.call("cbs_rns_modup", ctx.handle, mine.data_ptr(), c2.data_ptr(), size_q, count,
+                                         None), reps=3)
+        r_up = _time_ms(lambda: lib.ref_rns_modup(rctx, size_q, theirs.data_ptr(), c2.data_ptr(), count, None), reps=3)
+        assert torch.equal(mine, theirs)
+        del mine, theirs
+        polys = 2 * count
+        mods_qp = torch.from_numpy(chain.view(np.int64)).cuda().view(1, -1, 1)
+        cx = torch.remainder(torch.randint(0, 2 ** 62, (polys, qlp, n), dtype=torch.int64, device="cuda"), mods_qp)
+        work = torch.empty_like(cx)
+        out_m = torch.zeros((polys, size_q, n), dtype=torch.int64, device="cuda")
+        out_t = torch.zeros_like(out_m)
+
+        def fresh_ms(run, out):
+            # both sides transform the P limbs of cx in place: each repeat starts from a fresh
+            # copy (the copy and the clearing of the output are not timed)
+            best = float("inf")
+            for _ in range(4):
+                work.copy_(cx)
+                out.zero_()
+                torch.cuda.synchronize()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                run()
+                e1.record()
+                torch.cuda.synchronize()
+                best = min(best, e0.elapsed_time(e1))
+            return best
+
+        t_dn = fresh_ms(lambda: pkg.call("cbs_rns_moddown_from_ntt", ctx.handle, out_m.data_ptr(), work.data_ptr(),
+                                         size_q, polys, 0, None), out_m)
+        r_dn = fresh_ms(lambda: lib.ref_rns_moddown_from_ntt(rctx, size_q, out_t.data_ptr(), work.data_ptr(), polys,
+                                                             None), out_t)
+        assert torch.equal(out_m, out_t)
+    finally:
+        lib.ref_rns_destroy(rctx)
+        ctx.close()
+    print(f"\nN = 2^16, {size_q} + {size_p} primes, {count} ciphertexts (modup) / {polys} polynomials (moddown):\n"
+          f"  modup            product {t_up:7.2f} ms, reference DRNSTool {r_up:7.2f} ms ({r_up / t_up:.2f}x)\n"
+          f"  moddown_from_NTT product {t_dn:7.2f} ms, reference DRNSTool {r_dn:7.2f} ms ({r_dn / t_dn:.2f}x)")
