@@ -639,11 +639,13 @@ __global__ void __launch_bounds__(BrFftCfg<LOGN>::T, 1)
 // column instead of by input polynomial:
 //  1. each half (128 threads) transforms the two digits of its polynomial in lockstep, with the
 //     digits read straight from the accumulator (no digit buffer), and stores both spectra;
-//  2. after a barrier of the ciphertext's 256 threads, half h forms output column h for its 8
-//     slots from all four digit spectra: y_h += (x_row m_S(psi)) K_S[row][h] over the rows and
-//     subsets, with c_i(psi) = zeta^(a_i e_t) omega8^k - 1 recomputed per slot (no c buffer);
-//  3. after a second barrier (every spectrum read), half h inverse-transforms y_h in its own
-//     spectrum buffer and adds the rounded result into the accumulator positions it owns.
+//  2. after a CTA barrier, the 512 threads split by output column, slot half and position: each
+//     forms its 4 slots of output column mh for BOTH ciphertexts from all four digit spectra of
+//     each, y_mh += x_row (sum_S m_S(psi) K_S[row][mh]) over the rows, so every key word loaded
+//     feeds two ciphertexts; c_i(psi) = zeta^(a_i e_t) omega8^k - 1 is recomputed per slot;
+//  3. after a second barrier (every spectrum read) the outputs go to the [mh][0] spectrum
+//     buffers, and after a third, half h of each ciphertext inverse-transforms its column and
+//     adds the rounded result into the accumulator positions it owns.
 // Shared memory per CTA: the FFT tables once, then per ciphertext the accumulator [2][N] and
 // the spectra [2 halves][2 digits][N/2] (210 KB at N = 2048).  An odd batch's last CTA runs its
 // second ciphertext as a copy of the first and writes nothing for it.
@@ -701,7 +703,17 @@ __global__ void __launch_bounds__(4 * ((1u << LOGN) / 16), 1)
     auto half_bar = [half_id]() { asm volatile("bar.sync %0, %1;" ::"r"(half_id), "n"(TH) : "memory"); };
     const int32_t dbias = 1 << (gbits - 1);
     const uint32_t fmask = (1u << gbits) - 1u;
-    const uint64_t* arow = a.a + static_cast<size_t>(ct) * a.a_stride;
+    const uint64_t* arow[2];
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+        const uint32_t cr = 2 * blockIdx.x + c;
+        arow[c] = a.a + static_cast<size_t>(cr < batch ? cr : batch - 1) * a.a_stride;
+    }
+    // the product phase's split of the 512 threads: output column mh, slot half sh, position mt
+    const uint32_t mh = tid / (2 * TH), sh = (tid / TH) & 1u, mt = tid % TH;
+    auto spec_of = [&](int c) {
+        return reinterpret_cast<double2*>(smem + tab_words + c * ct_words + 2 * N);
+    };
     const uint32_t groups = (a.n + 1) / 2;
     constexpr size_t kstride = static_cast<size_t>(L2) * 2 * M;  // spectra between subsets of a group
     for (uint32_t g = 0; g < groups; ++g) {
@@ -732,51 +744,69 @@ __global__ void __launch_bounds__(4 * ((1u << LOGN) / 16), 1)
             my_s0[cswz(8 * ht + j)] = x0[j];
             my_s1[cswz(8 * ht + j)] = x1[j];
         }
-        // the group's rotations (read before the barrier, their latency hidden by it)
+        // the group's rotations of both ciphertexts (read before the barrier)
         const uint32_t idx0 = 2 * g, idx1 = idx0 + 1;
-        const uint32_t at0 = special_ms_f(__ldg(arow + idx0), TWO_N, a.q_lwe, a.bitwidth);
-        const uint32_t at1 = idx1 < a.n ? special_ms_f(__ldg(arow + idx1), TWO_N, a.q_lwe, a.bitwidth) : 0u;
-        const double2 ub0 = zeta_pow<LOGN>(tws, mult_base<LOGN>(ht, at0));
-        const double2 ub1 = zeta_pow<LOGN>(tws, mult_base<LOGN>(ht, at1));
-        ct_sync();
-        // 2. output column h from the four digit spectra
-        const double2* gk = f.bskf + static_cast<size_t>(g) * KS * kstride + static_cast<size_t>(h) * M + ht;
-        double2 y[8];
+        uint32_t at[2][2];
+        double2 ub[2][2];
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
+        for (int c = 0; c < 2; ++c) {
+            at[c][0] = special_ms_f(__ldg(arow[c] + idx0), TWO_N, a.q_lwe, a.bitwidth);
+            at[c][1] = idx1 < a.n ? special_ms_f(__ldg(arow[c] + idx1), TWO_N, a.q_lwe, a.bitwidth) : 0u;
+            ub[c][0] = zeta_pow<LOGN>(tws, mult_base<LOGN>(mt, at[c][0]));
+            ub[c][1] = zeta_pow<LOGN>(tws, mult_base<LOGN>(mt, at[c][1]));
+        }
+        __syncthreads();
+        // 2. output column mh, slots 4 sh .. 4 sh + 3, of both ciphertexts: each key word feeds
+        // both, through the combined key sum_S m_S(psi) K_S[row][mh] of each
+        const double2* gk = f.bskf + static_cast<size_t>(g) * KS * kstride + static_cast<size_t>(mh) * M + mt;
+        double2 y[2][4];
+#pragma unroll
+        for (int jj = 0; jj < 4; ++jj) {
+            const uint32_t j = 4 * sh + jj;
             const uint32_t r3 = ((j & 1) << 2) | (j & 2) | ((j >> 2) & 1);
-            double2 c0, c1;
-            {
-                const uint32_t k = (at0 * r3) & 7u;
-                double2 w = tab[(k & 3u) * (M / 8)];
-                if (k & 4u) w = make_double2(-w.x, -w.y);
-                c0 = cmul(ub0, w);
-                c0.x -= 1.0;
+            double2 cc[2][3];
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+#pragma unroll
+                for (int i = 0; i < 2; ++i) {
+                    const uint32_t k = (at[c][i] * r3) & 7u;
+                    double2 w = tab[(k & 3u) * (M / 8)];
+                    if (k & 4u) w = make_double2(-w.x, -w.y);
+                    cc[c][i] = cmul(ub[c][i], w);
+                    cc[c][i].x -= 1.0;
+                }
+                cc[c][2] = cmul(cc[c][0], cc[c][1]);
+                y[c][jj] = make_double2(0.0, 0.0);
             }
-            {
-                const uint32_t k = (at1 * r3) & 7u;
-                double2 w = tab[(k & 3u) * (M / 8)];
-                if (k & 4u) w = make_double2(-w.x, -w.y);
-                c1 = cmul(ub1, w);
-                c1.x -= 1.0;
-            }
-            const double2 c01 = cmul(c0, c1);
-            double2 acc_j = make_double2(0.0, 0.0);
+            const uint32_t xs = cswz(8 * mt + j);
 #pragma unroll
             for (uint32_t row = 0; row < L2; ++row) {
-                // row 2d + p: digit d of polynomial p, spectrum buffer p, d
-                const double2 x = spec[((row & 1u) * 2 + (row >> 1)) * M + cswz(8 * ht + j)];
+                // row 2d + p: digit d of polynomial p, spectrum buffer [p][d]
                 const double2* kr = gk + static_cast<size_t>(row) * 2 * M + j * TH;
-                cfma(acc_j, cmul(x, c0), __ldg(kr));
-                cfma(acc_j, cmul(x, c1), __ldg(kr + kstride));
-                cfma(acc_j, cmul(x, c01), __ldg(kr + 2 * kstride));
+                const double2 k0 = __ldg(kr), k1 = __ldg(kr + kstride), k2 = __ldg(kr + 2 * kstride);
+                const uint32_t xo = ((row & 1u) * 2 + (row >> 1)) * M + xs;
+#pragma unroll
+                for (int c = 0; c < 2; ++c) {
+                    double2 kc = cmul(cc[c][0], k0);
+                    cfma(kc, cc[c][1], k1);
+                    cfma(kc, cc[c][2], k2);
+                    cfma(y[c][jj], spec_of(c)[xo], kc);
+                }
             }
-            y[j] = acc_j;
         }
-        ct_sync();  // every spectrum read is done before the inverse transforms reuse the buffers
+        __syncthreads();  // every spectrum read is done: the outputs take the [mh][0] buffers
+#pragma unroll
+        for (int c = 0; c < 2; ++c)
+#pragma unroll
+            for (int jj = 0; jj < 4; ++jj) spec_of(c)[(2 * mh) * M + cswz(8 * mt + 4 * sh + jj)] = y[c][jj];
+        __syncthreads();
+        double2 yv[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) yv[j] = my_s0[cswz(8 * ht + j)];
+        half_bar();  // every output slot is in registers before the transform reuses the buffer
         // 3. inverse transform, rounding, accumulate
         fft_inverse_from_regs<LOGM>(
-            my_s0, ht, tab, y,
+            my_s0, ht, tab, yv,
             [&](int j, uint32_t e, double2 v) {
                 const double2 u = cmulc(v, twist_at<LOGM>(tws, j, e));
                 my_acc[e] = offset_add(my_acc[e], centred_residue(u.x * f.inv_m, f), lo_b, hi_b, Qs);
