@@ -716,6 +716,8 @@ __global__ void __launch_bounds__(4 * ((1u << LOGN) / 16), 1)
     };
     const uint32_t groups = (a.n + 1) / 2;
     constexpr size_t kstride = static_cast<size_t>(L2) * 2 * M;  // spectra between subsets of a group
+    // omega8 = tab[M/8] = (w8r, w8s w8r) and omega8^2 = tab[M/4] = (0, w8s)
+    const double w8r = tab[M / 8].x, w8s = tab[2 * (M / 8)].y;
     for (uint32_t g = 0; g < groups; ++g) {
         // 1. the two digit transforms of polynomial h, digits read from the accumulator
         double2 x0[8], x1[8];
@@ -769,8 +771,11 @@ __global__ void __launch_bounds__(4 * ((1u << LOGN) / 16), 1)
             for (int c = 0; c < 2; ++c) {
 #pragma unroll
                 for (int i = 0; i < 2; ++i) {
-                    const uint32_t k = (at[c][i] * r3) & 7u;
-                    double2 w = tab[(k & 3u) * (M / 8)];
+                    // omega8^k from its two distinct magnitudes (no table read)
+                    const uint32_t k = (at[c][i] * r3) & 7u, k3 = k & 3u;
+                    double2 w;
+                    w.x = k3 == 0 ? 1.0 : (k3 == 2 ? 0.0 : (k3 == 1 ? w8r : -w8r));
+                    w.y = k3 == 0 ? 0.0 : (k3 == 2 ? w8s : w8s * w8r);
                     if (k & 4u) w = make_double2(-w.x, -w.y);
                     cc[c][i] = cmul(ub[c][i], w);
                     cc[c][i].x -= 1.0;
