@@ -21,6 +21,7 @@
 #include "fft_core.cuh"
 #include "fft_kernels.cuh"
 #include "fft_ops.cuh"
+#include "tmem.cuh"
 
 namespace cbs {
 
@@ -646,15 +647,21 @@ __global__ void __launch_bounds__(BrFftCfg<LOGN>::T, 1)
 //  3. after a second barrier (every spectrum read) the outputs go to the [mh][0] spectrum
 //     buffers, and after a third, half h of each ciphertext inverse-transforms its column and
 //     adds the rounded result into the accumulator positions it owns.
-// Shared memory per CTA: the FFT tables once, then per ciphertext the accumulator [2][N] and
-// the spectra [2 halves][2 digits][N/2] (210 KB at N = 2048).  An odd batch's last CTA runs its
-// second ciphertext as a copy of the first and writes nothing for it.
+// The accumulator lives in tensor memory: a thread's transform reads and writes the same 16
+// coefficients every group (positions e, e + M of its 8 slots), so they stay in its TMEM lane
+// (ht, the same lane its warp quadrant reaches), 32 columns per half and ciphertext, 128 in all.
+// Shared memory: the FFT tables once, then per ciphertext the spectra [2 halves][2 digits][N/2]
+// (146 KB at N = 2048); the final accumulator passes through the spectra area for the MV
+// split.  An odd batch's last CTA runs its second ciphertext as a copy of the first and writes
+// nothing for it.
 template <int LOGN, bool WIDE>
 __global__ void __launch_bounds__(4 * ((1u << LOGN) / 16), 1)
     k_blind_rotate_fft_mb2_x2(const BlindRotateArgs a, const FftKeyArgs f, uint32_t batch) {
     constexpr int LOGM = LOGN - 1;
     constexpr uint32_t N = 1u << LOGN, M = N / 2, TH = M / 8, TWO_N = 2 * N;
     constexpr uint32_t KS = 3, DIGITS = 2, L2 = 2 * DIGITS;
+    constexpr uint32_t TMEM_COLS = 128;  // 4 (ciphertext, half) pairs x 32 columns
+    static_assert(TH == 128, "one TMEM lane per transform thread");
     using Tb = FftTab<LOGM>;
     extern __shared__ __align__(16) uint64_t smem[];
     double2* tab = reinterpret_cast<double2*>(smem);                 // FftTab<LOGM>, shared
@@ -663,13 +670,12 @@ __global__ void __launch_bounds__(4 * ((1u << LOGN) / 16), 1)
     const uint32_t ct_raw = 2 * blockIdx.x + c2;
     const bool live = ct_raw < batch;
     const uint32_t ct = live ? ct_raw : batch - 1;
-    // per-ciphertext region after the tables: acc [2][N] u64, spec [2][2][M] double2
+    // after the tables: the TMEM base address (16 bytes), then per ciphertext spec [2][2][M]
     constexpr size_t tab_words = (Tb::size() * sizeof(double2) + 15) / 16 * 2;  // 16-byte aligned, in u64
-    constexpr size_t ct_words = 2 * N + 4 * M * 2;
-    uint64_t* acc = smem + tab_words + c2 * ct_words;
-    double2* spec = reinterpret_cast<double2*>(acc + 2 * N);           // [p][d][M]
+    constexpr size_t ct_words = 4 * M * 2;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + tab_words);
+    double2* spec = reinterpret_cast<double2*>(smem + tab_words + 2 + c2 * ct_words);  // [p][d][M]
     const double2* tws = tab + Tb::twist_off();
-    int64_t* my_acc = reinterpret_cast<int64_t*>(acc) + h * N;
     double2* my_s0 = spec + (2 * h) * M;
     double2* my_s1 = my_s0 + M;
     const uint64_t Q = a.t.q;
@@ -684,16 +690,43 @@ __global__ void __launch_bounds__(4 * ((1u << LOGN) / 16), 1)
         return static_cast<int64_t>(x + round_c) - (x >= qhalf ? Qs : 0);
     };
 
+    if (tid < 32) tmem_alloc(tmem_slot, TMEM_COLS);
     for (uint32_t i = tid; i < Tb::size(); i += blockDim.x) tab[i] = f.tab[i];
+    tmem_fence_before();
+    __syncthreads();
+    tmem_fence_after();
+    const uint32_t tmem_base = *tmem_slot;
+    // this thread's 32 columns: word 4j + {0, 1} = coefficient e_j (lo, hi), {2, 3} = e_j + M,
+    // e_j = the transform's position of slot j; two 16-column halves (slots 0-3, 4-7)
+    const uint32_t tacc = tmem_quadrant_addr(tmem_base, (2 * c2 + h) * 32);
+    auto pack = [](uint32_t (&w)[16], int q, int64_t v) {
+        w[q] = static_cast<uint32_t>(static_cast<uint64_t>(v));
+        w[q + 1] = static_cast<uint32_t>(static_cast<uint64_t>(v) >> 32);
+    };
+    auto unpack = [](const uint32_t (&w)[16], int q) {
+        return static_cast<int64_t>(static_cast<uint64_t>(w[q]) | (static_cast<uint64_t>(w[q + 1]) << 32));
+    };
     {
+        // polynomial 0 = 0, polynomial 1 = X^b times the test vector, in offset form
         const uint32_t bt = special_ms_f(a.b[ct], TWO_N, a.q_lwe, a.bitwidth);
-        int64_t* y = reinterpret_cast<int64_t*>(acc);
-        for (uint32_t i = lt; i < N; i += 2 * TH) {
-            y[i] = to_offset(0);
+        auto init = [&](uint32_t i) -> int64_t {
+            if (h == 0) return to_offset(0);
             const uint32_t s = (i + bt) & (TWO_N - 1);
             const uint64_t v = (s < N) ? a.tv[s] : a.tv[s - N];
-            y[N + i] = to_offset((s < N) ? v : (v ? Q - v : 0));
+            return to_offset((s < N) ? v : (v ? Q - v : 0));
+        };
+#pragma unroll
+        for (int half = 0; half < 2; ++half) {
+            uint32_t w[16];
+#pragma unroll
+            for (int jj = 0; jj < 4; ++jj) {
+                const uint32_t e = pass_index<LOGM, 3>(1u, ht, 4 * half + jj);
+                pack(w, 4 * jj, init(e));
+                pack(w, 4 * jj + 2, init(e + M));
+            }
+            tmem_store16(tacc + 16 * half, w);
         }
+        tmem_wait_store();
     }
     __syncthreads();
 
@@ -712,7 +745,7 @@ __global__ void __launch_bounds__(4 * ((1u << LOGN) / 16), 1)
     // the product phase's split of the 512 threads: output column mh, slot half sh, position mt
     const uint32_t mh = tid / (2 * TH), sh = (tid / TH) & 1u, mt = tid % TH;
     auto spec_of = [&](int c) {
-        return reinterpret_cast<double2*>(smem + tab_words + c * ct_words + 2 * N);
+        return reinterpret_cast<double2*>(smem + tab_words + 2 + c * ct_words);
     };
     const uint32_t groups = (a.n + 1) / 2;
     constexpr size_t kstride = static_cast<size_t>(L2) * 2 * M;  // spectra between subsets of a group
@@ -721,25 +754,23 @@ __global__ void __launch_bounds__(4 * ((1u << LOGN) / 16), 1)
     for (uint32_t g = 0; g < groups; ++g) {
         // 1. the two digit transforms of polynomial h, digits read from the accumulator
         double2 x0[8], x1[8];
-        fft_forward2_to_regs<LOGM>(
-            my_s0, my_s1, ht, tab,
-            [&](int j, uint32_t e) {
-                const uint64_t wr = static_cast<uint64_t>(my_acc[e]) >> ign;
-                const uint64_t wi = static_cast<uint64_t>(my_acc[e + M]) >> ign;
+        {
+            uint32_t wa[16], wb[16];
+            tmem_load16(tacc, wa);
+            tmem_load16(tacc + 16, wb);
+            auto digit_pair = [&](int j, uint32_t e, int shift) {
+                const uint32_t(&w)[16] = j < 4 ? wa : wb;
+                const uint64_t wr = static_cast<uint64_t>(unpack(w, 4 * (j & 3))) >> (ign + shift);
+                const uint64_t wi = static_cast<uint64_t>(unpack(w, 4 * (j & 3) + 2)) >> (ign + shift);
                 return cmul(DigitPair<true>::unpack(make_uint2(static_cast<uint32_t>(wr) & fmask,
                                                                static_cast<uint32_t>(wi) & fmask),
                                                     dbias),
                             twist_at<LOGM>(tws, j, e));
-            },
-            [&](int j, uint32_t e) {
-                const uint64_t wr = static_cast<uint64_t>(my_acc[e]) >> ign;
-                const uint64_t wi = static_cast<uint64_t>(my_acc[e + M]) >> ign;
-                return cmul(DigitPair<true>::unpack(make_uint2(static_cast<uint32_t>(wr >> gbits) & fmask,
-                                                               static_cast<uint32_t>(wi >> gbits) & fmask),
-                                                    dbias),
-                            twist_at<LOGM>(tws, j, e));
-            },
-            x0, x1, half_bar);
+            };
+            fft_forward2_to_regs<LOGM>(
+                my_s0, my_s1, ht, tab, [&](int j, uint32_t e) { return digit_pair(j, e, 0); },
+                [&](int j, uint32_t e) { return digit_pair(j, e, gbits); }, x0, x1, half_bar);
+        }
         half_bar();  // the transforms' last reads of my_s0 / my_s1 are done
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
@@ -809,17 +840,42 @@ __global__ void __launch_bounds__(4 * ((1u << LOGN) / 16), 1)
 #pragma unroll
         for (int j = 0; j < 8; ++j) yv[j] = my_s0[cswz(8 * ht + j)];
         half_bar();  // every output slot is in registers before the transform reuses the buffer
-        // 3. inverse transform, rounding, accumulate
+        // 3. inverse transform, rounding, accumulate into the TMEM accumulator (each 16-column
+        // half read when its first slot arrives, written back after its last)
+        uint32_t wacc[16];
         fft_inverse_from_regs<LOGM>(
             my_s0, ht, tab, yv,
             [&](int j, uint32_t e, double2 v) {
+                if ((j & 3) == 0) tmem_load16(tacc + 16 * (j >> 2), wacc);
                 const double2 u = cmulc(v, twist_at<LOGM>(tws, j, e));
-                my_acc[e] = offset_add(my_acc[e], centred_residue(u.x * f.inv_m, f), lo_b, hi_b, Qs);
-                my_acc[e + M] = offset_add(my_acc[e + M], centred_residue(u.y * f.inv_m, f), lo_b, hi_b, Qs);
+                const int q = 4 * (j & 3);
+                pack(wacc, q, offset_add(unpack(wacc, q), centred_residue(u.x * f.inv_m, f), lo_b, hi_b, Qs));
+                pack(wacc, q + 2, offset_add(unpack(wacc, q + 2), centred_residue(u.y * f.inv_m, f), lo_b, hi_b, Qs));
+                if ((j & 3) == 3) tmem_store16(tacc + 16 * (j >> 2), wacc);
             },
             half_bar);
+        tmem_wait_store();
     }
-    ct_sync();
+
+    // the accumulator to shared memory ([2][N], natural order, in this ciphertext's spectra
+    // area), then TMEM is released
+    uint64_t* acc = reinterpret_cast<uint64_t*>(spec);
+    ct_sync();  // the last inverse transforms' reads of the spectra area are done
+#pragma unroll
+    for (int half = 0; half < 2; ++half) {
+        uint32_t w[16];
+        tmem_load16(tacc + 16 * half, w);
+#pragma unroll
+        for (int jj = 0; jj < 4; ++jj) {
+            const uint32_t e = pass_index<LOGM, 3>(1u, ht, 4 * half + jj);
+            acc[h * N + e] = static_cast<uint64_t>(unpack(w, 4 * jj));
+            acc[h * N + e + M] = static_cast<uint64_t>(unpack(w, 4 * jj + 2));
+        }
+    }
+    tmem_fence_before();
+    __syncthreads();
+    tmem_fence_after();
+    if (tid < 32) tmem_dealloc(tmem_base, TMEM_COLS);
 
     // finalize and the MV split, as in the one-bit form
     for (uint32_t i = lt; i < N; i += 2 * TH) {
@@ -934,7 +990,7 @@ static cudaError_t br_fft_mb2_x2_launch(const BlindRotateArgs& a, const FftKeyAr
                                         cudaStream_t s) {
     constexpr uint32_t N = 1u << LOGN, M = N / 2;
     constexpr size_t tab_bytes = (FftTab<LOGN - 1>::size() * sizeof(double2) + 15) / 16 * 16;
-    const size_t smem = tab_bytes + 2 * (2ull * N * sizeof(uint64_t) + 4ull * M * sizeof(double2));
+    const size_t smem = tab_bytes + 16 + 2 * (4ull * M * sizeof(double2));
     if (f.tab_len != FftTab<LOGN - 1>::size()) return cudaErrorInvalidValue;
     static size_t configured[64] = {};
     int dev = 0;
