@@ -1008,8 +1008,10 @@ static cudaError_t br_fft_mb2_x2_launch(const BlindRotateArgs& a, const FftKeyAr
 template <int LOGN, int MB>
 static cudaError_t br_fft_mb_launch(const BlindRotateArgs& a, const FftKeyArgs& f, uint32_t batch, cudaStream_t s) {
     if constexpr (MB == 2 && LOGN == 11) {
-        // two ciphertexts per CTA (digits read from the accumulator: any digit width up to 24 bits)
-        if (a.digits == 2 && a.schedule == CBS_BR_SCHEDULE_PAIRED) return br_fft_mb2_x2_launch<LOGN>(a, f, batch, s);
+        // two ciphertexts per CTA (digits read from the accumulator: any digit width up to 24
+        // bits); also the default when no schedule was chosen or tuned (the fastest form on B200)
+        if (a.digits == 2 && (a.schedule == CBS_BR_SCHEDULE_PAIRED || a.schedule == CBS_BR_SCHEDULE_AUTO))
+            return br_fft_mb2_x2_launch<LOGN>(a, f, batch, s);
     }
     if constexpr (MB == 2) {
         // the two-digit gadget: both digit transforms in lockstep unless the digit-by-digit

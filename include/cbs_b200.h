@@ -179,8 +179,8 @@ cbs_status cbs_context_set_br_multibit(cbs_context *ctx, uint32_t mb);
  * CBS_BR_SCHEDULE_DIGITWISE one after the other, CBS_BR_SCHEDULE_PAIRED runs two ciphertexts per
  * CTA (mb = 2, N = 2048; 16 warps per SM, work split by output column);
  * CBS_BR_SCHEDULE_AUTO (default) takes the autotuner's cached choice for this GPU and parameter
- * set, else lockstep.  Results differ only by FP64 rounding (all within the phase-error bound).
- * No reference counterpart. */
+ * set, else paired where it applies (mb = 2, N = 2048), else lockstep.  Results differ only by
+ * FP64 rounding (all within the phase-error bound).  No reference counterpart. */
 enum { CBS_BR_SCHEDULE_AUTO = 0, CBS_BR_SCHEDULE_DIGITWISE = 1, CBS_BR_SCHEDULE_LOCKSTEP = 2,
        CBS_BR_SCHEDULE_PAIRED = 3 };
 cbs_status cbs_context_set_br_schedule(cbs_context *ctx, uint32_t schedule);
