@@ -14,7 +14,8 @@
 // so a limb crosses HBM twice per transform.  Columns: a CTA takes 16 adjacent columns and
 // its threads interleave columns so every global access is a 128-byte run; rows: 16 rows of
 // 256 contiguous words per CTA.  Intermediate values stay lazy (< 4q forward, < 2q
-// inverse); the second kernel reduces fully.
+// inverse); the second kernel reduces fully.  When every prime of the chain is below 2^50
+// the same kernels run on the FP64 pipe (exact products in doubles, see below).
 #include <atomic>
 
 #include "common.cuh"
@@ -175,6 +176,201 @@ __device__ __forceinline__ void sub_inv(uint64_t* sm, uint32_t gt, const uint64_
     for (int j = 0; j < 8; ++j) store(pass_index<LOGS, 3>(1u, gt, j), x[j], j);
 }
 
+
+// ---------------------------------------------------------------------------------------------
+// FP64-pipe form (primes below 2^50).  The 64-bit Shoup products above are emulated with 32-bit
+// integer multiplies and bound the integer pipe while the FP64 pipe idles.  For q < 2^50 every
+// residue, lazy value and twiddle is an integer below 2^53, held exactly in a double, and the
+// modular product is computed exactly on the FP64 pipe:
+//   h = fl(v w), l = fma(v, w, -h)          (error-free product, Ogita-Rump-Oishi TwoProduct:
+//                                            v w = h + l exactly)
+//   k = rint(h / q)   (as h * fl(1/q))      (quotient estimate, within +-2 of v w / q)
+//   r = fma(-k, q, h) + l                    (= v w - k q exactly)
+// fma(-k, q, h) is exact because its true value h - k q = r - l is an integer of magnitude
+// below 2q + 2^49 < 2^53; r itself lies in (-2q, 2q) and is congruent to v w.  This is the
+// floating-point quotient estimate of Shoup's MulMod (NTL) carried out entirely in doubles.
+// Values are signed and lazy: each radix-8 pass first reduces its 8 inputs to |x| <= q/2 + 1
+// (x - rint(x/q) q, one FMA), after which three forward stages grow them to at most 2q + 4 and
+// three inverse stages to at most 4q + 8, far inside the exact range.  The twiddles are the
+// same tables converted to doubles; results are the integer path's residues, bit for bit.
+struct DMod {
+    double q, qinv;
+};
+
+__device__ __forceinline__ DMod dmod_of(uint64_t q) { return {static_cast<double>(q), 1.0 / static_cast<double>(q)}; }
+
+// v w mod q, in (-2q, 2q), exact for |v| < 2^52 and 0 <= w < q < 2^50
+__device__ __forceinline__ double dmulmod(double v, double w, const DMod& m) {
+    const double h = __dmul_rn(v, w);
+    const double l = __fma_rn(v, w, -h);
+    const double k = rint(__dmul_rn(h, m.qinv));
+    return __dadd_rn(__fma_rn(-k, m.q, h), l);
+}
+
+// x mod q in [-q/2 - 1, q/2 + 1] for |x| < 2^52
+__device__ __forceinline__ double dreduce(double x, const DMod& m) {
+    return __fma_rn(-rint(__dmul_rn(x, m.qinv)), m.q, x);
+}
+
+// [0, q) from |x| < 2^52
+__device__ __forceinline__ uint64_t dto_residue(double x, const DMod& m) {
+    double r = dreduce(x, m);
+    if (r < 0.0) r = __dadd_rn(r, m.q);
+    return __double2ull_rn(r);
+}
+
+__device__ __forceinline__ void ct_bf_d(double& x, double& y, double w, const DMod& m) {
+    const double t = dmulmod(y, w, m);
+    y = __dsub_rn(x, t);
+    x = __dadd_rn(x, t);
+}
+
+__device__ __forceinline__ void gs_bf_d(double& x, double& y, double w, const DMod& m) {
+    const double t = __dsub_rn(x, y);
+    x = __dadd_rn(x, y);
+    y = dmulmod(t, w, m);
+}
+
+// the passes of fwd_pass_b / inv_pass_b with double values and twiddles; inputs reduced first
+template <int LOGS, int R>
+__device__ __forceinline__ void fwd_pass_d(double (&x)[8], uint32_t m, uint32_t base, uint32_t tid,
+                                           const double* __restrict__ tw, const DMod& md) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) x[j] = dreduce(x[j], md);
+    if (R == 3) {
+        const uint32_t i1 = base + pass_group<LOGS, 3>(m, tid, 0);
+        {
+            const double w = __ldg(tw + i1);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) ct_bf_d(x[j], x[j + 4], w, md);
+        }
+        {
+            const double w0 = __ldg(tw + 2 * i1), w1 = __ldg(tw + 2 * i1 + 1);
+            ct_bf_d(x[0], x[2], w0, md);
+            ct_bf_d(x[1], x[3], w0, md);
+            ct_bf_d(x[4], x[6], w1, md);
+            ct_bf_d(x[5], x[7], w1, md);
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) ct_bf_d(x[2 * j], x[2 * j + 1], __ldg(tw + 4 * i1 + j), md);
+    } else if (R == 2) {
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const uint32_t i1 = base + pass_group<LOGS, 2>(m, tid, h);
+            const double w = __ldg(tw + i1);
+            double* v = x + 4 * h;
+            ct_bf_d(v[0], v[2], w, md);
+            ct_bf_d(v[1], v[3], w, md);
+            ct_bf_d(v[0], v[1], __ldg(tw + 2 * i1), md);
+            ct_bf_d(v[2], v[3], __ldg(tw + 2 * i1 + 1), md);
+        }
+    } else {
+#pragma unroll
+        for (int h = 0; h < 4; ++h) {
+            const uint32_t i1 = base + pass_group<LOGS, 1>(m, tid, h);
+            ct_bf_d(x[2 * h], x[2 * h + 1], __ldg(tw + i1), md);
+        }
+    }
+}
+
+template <int LOGS, int R>
+__device__ __forceinline__ void inv_pass_d(double (&x)[8], uint32_t m, uint32_t base, uint32_t tid,
+                                           const double* __restrict__ tw, const DMod& md) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) x[j] = dreduce(x[j], md);
+    if (R == 3) {
+        const uint32_t i1 = base + pass_group<LOGS, 3>(m, tid, 0);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) gs_bf_d(x[2 * j], x[2 * j + 1], __ldg(tw + 4 * i1 + j), md);
+        {
+            const double w0 = __ldg(tw + 2 * i1), w1 = __ldg(tw + 2 * i1 + 1);
+            gs_bf_d(x[0], x[2], w0, md);
+            gs_bf_d(x[1], x[3], w0, md);
+            gs_bf_d(x[4], x[6], w1, md);
+            gs_bf_d(x[5], x[7], w1, md);
+        }
+        {
+            const double w = __ldg(tw + i1);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) gs_bf_d(x[j], x[j + 4], w, md);
+        }
+    } else if (R == 2) {
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const uint32_t i1 = base + pass_group<LOGS, 2>(m, tid, h);
+            double* v = x + 4 * h;
+            gs_bf_d(v[0], v[1], __ldg(tw + 2 * i1), md);
+            gs_bf_d(v[2], v[3], __ldg(tw + 2 * i1 + 1), md);
+            const double w = __ldg(tw + i1);
+            gs_bf_d(v[0], v[2], w, md);
+            gs_bf_d(v[1], v[3], w, md);
+        }
+    } else {
+#pragma unroll
+        for (int h = 0; h < 4; ++h) {
+            const uint32_t i1 = base + pass_group<LOGS, 1>(m, tid, h);
+            gs_bf_d(x[2 * h], x[2 * h + 1], __ldg(tw + i1), md);
+        }
+    }
+}
+
+template <int LOGS, class TwB, class Load, class Store>
+__device__ __forceinline__ void sub_fwd_d(double* sm, uint32_t gt, const double* __restrict__ tw, const DMod& md,
+                                          TwB twb, Load load, Store store) {
+    using Pl = NttPlan<LOGS>;
+    double x[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) x[j] = load(pass_index<LOGS, 3>(1u, gt, j));
+    fwd_pass_d<LOGS, 3>(x, 1u, twb(1u), gt, tw, md);
+#pragma unroll
+    for (int p = 1; p < Pl::P; ++p) {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) sm[swz(pass_index<LOGS, 3>(1u << (3 * (p - 1)), gt, j))] = x[j];
+        __syncthreads();
+        const uint32_t m = 1u << (3 * p);
+        if (p < Pl::P - 1) {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) x[j] = sm[swz(pass_index<LOGS, 3>(m, gt, j))];
+            fwd_pass_d<LOGS, 3>(x, m, twb(m), gt, tw, md);
+        } else {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) x[j] = sm[swz(pass_index<LOGS, Pl::tail_r>(m, gt, j))];
+            fwd_pass_d<LOGS, Pl::tail_r>(x, m, twb(m), gt, tw, md);
+        }
+    }
+    constexpr uint32_t mt = 1u << (3 * (Pl::P - 1));
+#pragma unroll
+    for (int j = 0; j < 8; ++j) store(pass_index<LOGS, Pl::tail_r>(mt, gt, j), x[j]);
+}
+
+template <int LOGS, class TwB, class Load, class Store>
+__device__ __forceinline__ void sub_inv_d(double* sm, uint32_t gt, const double* __restrict__ tw, const DMod& md,
+                                          TwB twb, Load load, Store store) {
+    using Pl = NttPlan<LOGS>;
+    constexpr uint32_t mt = 1u << (3 * (Pl::P - 1));
+    double x[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) x[j] = load(pass_index<LOGS, Pl::tail_r>(mt, gt, j));
+    inv_pass_d<LOGS, Pl::tail_r>(x, mt, twb(mt), gt, tw, md);
+#pragma unroll
+    for (int j = 0; j < 8; ++j) sm[swz(pass_index<LOGS, Pl::tail_r>(mt, gt, j))] = x[j];
+    __syncthreads();
+#pragma unroll
+    for (int p = Pl::P - 2; p >= 0; --p) {
+        const uint32_t m = 1u << (3 * p);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) x[j] = sm[swz(pass_index<LOGS, 3>(m, gt, j))];
+        inv_pass_d<LOGS, 3>(x, m, twb(m), gt, tw, md);
+        if (p > 0) {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) sm[swz(pass_index<LOGS, 3>(m, gt, j))] = x[j];
+            __syncthreads();
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < 8; ++j) store(pass_index<LOGS, 3>(1u, gt, j), x[j], j);
+}
+
 constexpr int kL2 = 8;            // row stages (rows of 256 words)
 constexpr uint32_t kGroups = 16;  // sub-transforms per CTA
 
@@ -201,8 +397,9 @@ __device__ __forceinline__ const uint64_t* src_ptr(uint64_t* data, const RnsNttA
     return a.in + static_cast<size_t>(poly) * a.in_poly_stride + (static_cast<size_t>(slot) << log_n);
 }
 
-// forward phase 1: columns (2^L1 points each, stride 2^L2), lazy output
-template <int L1>
+// forward phase 1: columns (2^L1 points each, stride 2^L2), lazy output (FP: signed lazy
+// doubles written in place, read back by the row phase)
+template <int L1, bool FP>
 __global__ void __launch_bounds__(kGroups * (1 << L1) / 8) k_rns_fwd_cols(uint64_t* __restrict__ data,
                                                                          const RnsNttArgs a) {
     constexpr uint32_t ROW = 1u << kL2;
@@ -218,13 +415,21 @@ __global__ void __launch_bounds__(kGroups * (1 << L1) / 8) k_rns_fwd_cols(uint64
     const uint64_t q = a.q[prime];
     uint64_t* poly = limb_ptr(data, a, limb_flat, L1 + kL2) + colblk * kGroups + g;
     const uint64_t* src = src_ptr(data, a, limb_flat, L1 + kL2) + colblk * kGroups + g;
-    sub_fwd<L1>(
-        sm + g * col_stride<L1>(), gt, tw, tws, q, [](uint32_t m) { return m; },
-        [&](uint32_t e) { return src[e * ROW]; }, [&](uint32_t e, uint64_t v) { poly[e * ROW] = v; });
+    if constexpr (FP) {
+        double* dpoly = reinterpret_cast<double*>(poly);
+        sub_fwd_d<L1>(
+            reinterpret_cast<double*>(sm) + g * col_stride<L1>(), gt, a.twd + prime * N, dmod_of(q),
+            [](uint32_t m) { return m; }, [&](uint32_t e) { return __ull2double_rn(src[e * ROW]); },
+            [&](uint32_t e, double v) { dpoly[e * ROW] = v; });
+    } else {
+        sub_fwd<L1>(
+            sm + g * col_stride<L1>(), gt, tw, tws, q, [](uint32_t m) { return m; },
+            [&](uint32_t e) { return src[e * ROW]; }, [&](uint32_t e, uint64_t v) { poly[e * ROW] = v; });
+    }
 }
 
 // forward phase 2: rows (256 contiguous words), full reduction, optional moddown epilogue
-template <int L1, int EPI>
+template <int L1, int EPI, bool FP>
 __global__ void __launch_bounds__(kGroups * 32) k_rns_fwd_rows(uint64_t* __restrict__ data, const RnsNttArgs a) {
     constexpr uint32_t ROW = 1u << kL2, ROWS = 1u << L1;
     extern __shared__ uint64_t sm[];
@@ -239,6 +444,32 @@ __global__ void __launch_bounds__(kGroups * 32) k_rns_fwd_rows(uint64_t* __restr
     const uint64_t q = a.q[prime], q2 = q << 1;
     const uint32_t R = rowblk * kGroups + g;
     uint64_t* row = limb_ptr(data, a, limb_flat, L1 + kL2) + static_cast<size_t>(R) * ROW;
+    if constexpr (FP) {
+        const DMod md = dmod_of(q);
+        const double* drow = reinterpret_cast<const double*>(row);
+        double* dsm = reinterpret_cast<double*>(sm) + g * ROW;
+        const double* twd = a.twd + prime * N;
+        if (EPI == 0) {
+            sub_fwd_d<kL2>(
+                dsm, gt, twd, md, [&](uint32_t m) { return m * (ROWS + R); }, [&](uint32_t e) { return drow[e]; },
+                [&](uint32_t e, double v) { row[e] = dto_residue(v, md); });
+        } else {
+            const uint32_t poly = limb_flat / a.limbs, limb = limb_flat % a.limbs;
+            const size_t off = (static_cast<size_t>(limb) << (L1 + kL2)) + static_cast<size_t>(R) * ROW;
+            const uint64_t* cx = a.epi_cx + poly * a.epi_cx_stride + off;
+            uint64_t* dst = a.epi_dst + poly * a.epi_dst_stride + off;
+            const uint64_t f = a.epi_f[limb], fs = a.epi_fs[limb];
+            sub_fwd_d<kL2>(
+                dsm, gt, twd, md, [&](uint32_t m) { return m * (ROWS + R); }, [&](uint32_t e) { return drow[e]; },
+                [&](uint32_t e, double dv) {
+                    const uint64_t v = dto_residue(dv, md);
+                    uint64_t r = mul_shoup(sub_mod(cx[e], v, q), f, fs, q);
+                    if (EPI == 2) r = add_mod(dst[e], r, q);
+                    dst[e] = r;
+                });
+        }
+        return;
+    }
     if (EPI == 0) {
         sub_fwd<kL2>(
             sm + g * ROW, gt, tw, tws, q, [&](uint32_t m) { return m * (ROWS + R); },
@@ -261,8 +492,8 @@ __global__ void __launch_bounds__(kGroups * 32) k_rns_fwd_rows(uint64_t* __restr
     }
 }
 
-// inverse phase A: rows (lazy output < 2q)
-template <int L1>
+// inverse phase A: rows (lazy output < 2q; FP: signed lazy doubles in place)
+template <int L1, bool FP>
 __global__ void __launch_bounds__(kGroups * 32) k_rns_inv_rows(uint64_t* __restrict__ data, const RnsNttArgs a) {
     constexpr uint32_t ROW = 1u << kL2, ROWS = 1u << L1;
     extern __shared__ uint64_t sm[];
@@ -278,13 +509,21 @@ __global__ void __launch_bounds__(kGroups * 32) k_rns_inv_rows(uint64_t* __restr
     const uint32_t R = rowblk * kGroups + g;
     uint64_t* row = limb_ptr(data, a, limb_flat, L1 + kL2) + static_cast<size_t>(R) * ROW;
     const uint64_t* src = src_ptr(data, a, limb_flat, L1 + kL2) + static_cast<size_t>(R) * ROW;
-    sub_inv<kL2>(
-        sm + g * ROW, gt, itw, itws, q, [&](uint32_t m) { return m * (ROWS + R); }, [&](uint32_t e) { return src[e]; },
-        [&](uint32_t e, uint64_t v, int) { row[e] = v; });
+    if constexpr (FP) {
+        double* drow = reinterpret_cast<double*>(row);
+        sub_inv_d<kL2>(
+            reinterpret_cast<double*>(sm) + g * ROW, gt, a.itwd + prime * N, dmod_of(q),
+            [&](uint32_t m) { return m * (ROWS + R); }, [&](uint32_t e) { return __ull2double_rn(src[e]); },
+            [&](uint32_t e, double v, int) { drow[e] = v; });
+    } else {
+        sub_inv<kL2>(
+            sm + g * ROW, gt, itw, itws, q, [&](uint32_t m) { return m * (ROWS + R); },
+            [&](uint32_t e) { return src[e]; }, [&](uint32_t e, uint64_t v, int) { row[e] = v; });
+    }
 }
 
 // inverse phase B: columns, n^-1 on the x-half of the last stage, full reduction
-template <int L1>
+template <int L1, bool FP>
 __global__ void __launch_bounds__(kGroups * (1 << L1) / 8) k_rns_inv_cols(uint64_t* __restrict__ data,
                                                                          const RnsNttArgs a) {
     constexpr uint32_t ROW = 1u << kL2;
@@ -302,6 +541,20 @@ __global__ void __launch_bounds__(kGroups * (1 << L1) / 8) k_rns_inv_cols(uint64
     const uint64_t sc = a.scale ? a.scale[limb_flat % a.limbs] : 0;
     const uint64_t scs = a.scale ? a.scale_s[limb_flat % a.limbs] : 0;
     uint64_t* poly = limb_ptr(data, a, limb_flat, L1 + kL2) + colblk * kGroups + g;
+    if constexpr (FP) {
+        const DMod md = dmod_of(q);
+        const double ninv_d = static_cast<double>(ninv), sc_d = static_cast<double>(sc);
+        const double* dpoly = reinterpret_cast<const double*>(poly);
+        sub_inv_d<L1>(
+            reinterpret_cast<double*>(sm) + g * col_stride<L1>(), gt, a.itwd + prime * N, md,
+            [](uint32_t m) { return m; }, [&](uint32_t e) { return dpoly[e * ROW]; },
+            [&](uint32_t e, double v, int j) {
+                if (j < 4) v = dmulmod(v, ninv_d, md);  // x-half of the m = 1 stage
+                if (sc) v = dmulmod(v, sc_d, md);
+                poly[e * ROW] = dto_residue(v, md);
+            });
+        return;
+    }
     sub_inv<L1>(
         sm + g * col_stride<L1>(), gt, itw, itws, q, [](uint32_t m) { return m; },
         [&](uint32_t e) { return poly[e * ROW]; },
@@ -385,28 +638,42 @@ static cudaError_t rns_launch(uint64_t* data, const RnsNttArgs& a, size_t limb_p
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
     if (!(attr_set.load() >> dev & 1)) {
-        cudaError_t e = cudaFuncSetAttribute(k_rns_fwd_cols<L1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             static_cast<int>(col_smem));
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(k_rns_inv_cols<L1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     static_cast<int>(col_smem));
-        if (e != cudaSuccess) return e;
+        const void* fns[] = {reinterpret_cast<const void*>(k_rns_fwd_cols<L1, false>),
+                             reinterpret_cast<const void*>(k_rns_inv_cols<L1, false>),
+                             reinterpret_cast<const void*>(k_rns_fwd_cols<L1, true>),
+                             reinterpret_cast<const void*>(k_rns_inv_cols<L1, true>)};
+        for (const void* fn : fns) {
+            cudaError_t e =
+                cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(col_smem));
+            if (e != cudaSuccess) return e;
+        }
         attr_set.fetch_or(uint64_t(1) << dev);
     }
     const size_t col_blocks = limb_polys * (ROW / kGroups), row_blocks = limb_polys * (ROWS / kGroups);
     if (col_blocks > 0x7fffffffu || row_blocks > 0x7fffffffu) return cudaErrorInvalidValue;
     const uint32_t col_threads = kGroups * (1u << L1) / 8, row_threads = kGroups * 32;
+    const unsigned cb = static_cast<unsigned>(col_blocks), rb = static_cast<unsigned>(row_blocks);
+    if (a.twd && a.itwd) {
+        // every prime of the chain is below 2^50: the FP64-pipe form
+        if (!inverse) {
+            k_rns_fwd_cols<L1, true><<<cb, col_threads, col_smem, s>>>(data, a);
+            if (a.epi == 0) k_rns_fwd_rows<L1, 0, true><<<rb, row_threads, row_smem, s>>>(data, a);
+            else if (a.epi == 1) k_rns_fwd_rows<L1, 1, true><<<rb, row_threads, row_smem, s>>>(data, a);
+            else k_rns_fwd_rows<L1, 2, true><<<rb, row_threads, row_smem, s>>>(data, a);
+        } else {
+            k_rns_inv_rows<L1, true><<<rb, row_threads, row_smem, s>>>(data, a);
+            k_rns_inv_cols<L1, true><<<cb, col_threads, col_smem, s>>>(data, a);
+        }
+        return cudaGetLastError();
+    }
     if (!inverse) {
-        k_rns_fwd_cols<L1><<<static_cast<unsigned>(col_blocks), col_threads, col_smem, s>>>(data, a);
-        if (a.epi == 0)
-            k_rns_fwd_rows<L1, 0><<<static_cast<unsigned>(row_blocks), row_threads, row_smem, s>>>(data, a);
-        else if (a.epi == 1)
-            k_rns_fwd_rows<L1, 1><<<static_cast<unsigned>(row_blocks), row_threads, row_smem, s>>>(data, a);
-        else
-            k_rns_fwd_rows<L1, 2><<<static_cast<unsigned>(row_blocks), row_threads, row_smem, s>>>(data, a);
+        k_rns_fwd_cols<L1, false><<<cb, col_threads, col_smem, s>>>(data, a);
+        if (a.epi == 0) k_rns_fwd_rows<L1, 0, false><<<rb, row_threads, row_smem, s>>>(data, a);
+        else if (a.epi == 1) k_rns_fwd_rows<L1, 1, false><<<rb, row_threads, row_smem, s>>>(data, a);
+        else k_rns_fwd_rows<L1, 2, false><<<rb, row_threads, row_smem, s>>>(data, a);
     } else {
-        k_rns_inv_rows<L1><<<static_cast<unsigned>(row_blocks), row_threads, row_smem, s>>>(data, a);
-        k_rns_inv_cols<L1><<<static_cast<unsigned>(col_blocks), col_threads, col_smem, s>>>(data, a);
+        k_rns_inv_rows<L1, false><<<rb, row_threads, row_smem, s>>>(data, a);
+        k_rns_inv_cols<L1, false><<<cb, col_threads, col_smem, s>>>(data, a);
     }
     return cudaGetLastError();
 }

@@ -20,6 +20,10 @@ struct RnsNttArgs {
     const uint64_t* q = nullptr;
     const uint64_t* n_inv = nullptr;
     const uint64_t* n_inv_s = nullptr;
+    // the tw / itw tables as doubles, set only when every prime is below 2^50: the 2-D
+    // transforms (N >= 2^13) then run on the FP64 pipe, with the same results
+    const double* twd = nullptr;
+    const double* itwd = nullptr;
     const uint32_t* limb_prime = nullptr;  // device [limbs]: table row of launch limb l
     const uint32_t* limb_slot = nullptr;   // device [limbs]: limb position in the polynomial (null: l)
     uint32_t limbs = 0;

@@ -211,6 +211,7 @@ struct cbs_rns_context {
     std::vector<uint64_t> primes;  // Q chain then P
     std::vector<cbs::host::NttTables> tabs;
     DevBuf<uint64_t> d_tw, d_tws, d_itw, d_itws, d_q, d_ninv, d_ninv_s, d_r0, d_r1;
+    DevBuf<double> d_twd, d_itwd;  // tw / itw as doubles when every prime is below 2^50
     DevBuf<cbs_dmodulus> d_mod;
     DevBuf<uint32_t> d_ident;  // 0 .. size_qp - 1
     std::map<uint32_t, std::unique_ptr<cbs::RnsLevel>> levels;
@@ -225,6 +226,8 @@ struct cbs_rns_context {
         a.q = d_q.p;
         a.n_inv = d_ninv.p;
         a.n_inv_s = d_ninv_s.p;
+        a.twd = d_twd.p;
+        a.itwd = d_itwd.p;
         return a;
     }
 };
@@ -489,6 +492,12 @@ cbs_status cbs_rns_context_create(uint32_t poly_degree, const uint64_t* h_q, uin
     if (c->red_k == 0) c->red_k = 1;
     CBS_CUDA_TRY(upload_sync(c->d_tw, tw));
     CBS_CUDA_TRY(upload_sync(c->d_tws, tws));
+    if (qmax < (uint64_t(1) << 50)) {
+        // exact doubles of the twiddles for the FP64-pipe transforms
+        std::vector<double> twd(tw.begin(), tw.end()), itwd(itw.begin(), itw.end());
+        CBS_CUDA_TRY(upload_sync(c->d_twd, twd));
+        CBS_CUDA_TRY(upload_sync(c->d_itwd, itwd));
+    }
     CBS_CUDA_TRY(upload_sync(c->d_itw, itw));
     CBS_CUDA_TRY(upload_sync(c->d_itws, itws));
     CBS_CUDA_TRY(upload_sync(c->d_q, qv));

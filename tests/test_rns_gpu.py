@@ -31,11 +31,14 @@ def rand_limbs(rng, mods, n, lead=()):
     return np.stack([rng.integers(0, int(m), lead + (n,), dtype=np.uint64) for m in mods], axis=len(lead))
 
 
-@pytest.mark.parametrize("logn", [10, 11, 12, 13, 14, 15, 16, 17])
-def test_rns_ntt_bit_exact(env, logn):
+@pytest.mark.parametrize("logn,bits", [(10, 50), (11, 50), (12, 50), (13, 50), (14, 50), (15, 50), (16, 50),
+                                       (17, 50), (13, 59), (16, 59)])
+def test_rns_ntt_bit_exact(env, logn, bits):
+    """50-bit primes take the FP64-pipe 2-D transforms (N >= 2^13), 59-bit primes the integer
+    ones; both bit-exact."""
     pkg, o, torch = env
     n = 1 << logn
-    q, p = rns_primes(o, n, 3, 2)
+    q, p = rns_primes(o, n, 3, 2, bits)
     chain = np.concatenate([q, p])
     ctx = pkg.RnsContext(n, q, p)
     rng = np.random.default_rng(logn)
