@@ -141,6 +141,7 @@ def _declare(lib: ctypes.CDLL) -> None:
         "cbs_gate_ragged_launch": (st, [c_vp, c_vp]),
         "cbs_rns_context_create": (st, [u32, c_vp, u32, c_vp, u32, c_vp]),
         "cbs_rns_context_destroy": (st, [c_vp]),
+        "cbs_rns_device_fault": (st, [c_vp, c_vp, ctypes.c_int]),
         "cbs_rns_context_tables": (st, [c_vp, c_vp]),
         "cbs_rns_prepare_level": (st, [c_vp, u32]),
         "cbs_nwt_2d_radix8_forward_inplace": (st, [c_vp, c_vp, u32, u32, c_vp]),
@@ -566,6 +567,12 @@ class RnsContext:
     @property
     def handle(self) -> int:
         return self._h.value
+
+    def device_fault(self, clear: bool = False) -> int:
+        """The RNS context's device fault word (0 after correct runs)."""
+        v = ctypes.c_uint32()
+        call("cbs_rns_device_fault", self._h, ctypes.byref(v), int(clear))
+        return v.value
 
     def beta(self, size_ql: int) -> int:
         return -(-size_ql // self.size_p)

@@ -18,6 +18,7 @@
 // the same kernels run on the FP64 pipe (exact products in doubles, see below).
 #include <atomic>
 
+#include "async_copy.cuh"
 #include "common.cuh"
 #include "ntt_core.cuh"
 #include "ntt_rns.cuh"
@@ -566,6 +567,109 @@ __global__ void __launch_bounds__(kGroups * (1 << L1) / 8) k_rns_inv_cols(uint64
         });
 }
 
+// Row phases of the FP64 form with bulk copies: a CTA's 16 rows are 32 KB of one limb,
+// contiguous in memory, so one thread moves them between global and shared memory with a
+// single cp.async.bulk each way (completion on an mbarrier for the load, a bulk group for the
+// store) instead of 8-byte loads and stores from every thread, which keep the load/store
+// queues full (lg_throttle) at a fraction of HBM bandwidth.  Shared memory: the exchange
+// buffer, the 32 KB staging block and the mbarrier.  A load whose wait expires sets bit 1 of
+// *a.fault and the CTA finishes on whatever the staging block holds.
+constexpr long long kBulkWaitLimit = 1ll << 31;  // SM clocks, about a second
+
+__device__ __forceinline__ bool rows_bulk_load(double* stage, const void* src, uint64_t* bar, uint32_t* fault) {
+    constexpr uint32_t bytes = kGroups * (1u << kL2) * sizeof(uint64_t);
+    if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        mbar_init_fence();
+        mbar_arrive_expect_tx(bar, bytes);
+        bulk_load(stage, src, bytes, bar);
+    }
+    __syncthreads();
+    const bool ok = mbar_wait_bounded(bar, 0, kBulkWaitLimit);
+    if (!ok && fault) atomicOr(fault, 1u);
+    return ok;
+}
+
+__device__ __forceinline__ void rows_bulk_store(void* dst, const double* stage) {
+    constexpr uint32_t bytes = kGroups * (1u << kL2) * sizeof(uint64_t);
+    fence_proxy_async_smem();  // this thread's staging writes, before the copy engine reads them
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        bulk_store(dst, stage, bytes);
+        bulk_store_commit_and_drain();
+    }
+}
+
+template <int L1, int EPI>
+__global__ void __launch_bounds__(kGroups * 32) k_rns_fwd_rows_bulk(uint64_t* __restrict__ data, const RnsNttArgs a) {
+    constexpr uint32_t ROW = 1u << kL2, ROWS = 1u << L1;
+    extern __shared__ __align__(16) uint64_t sm[];
+    double* xsm = reinterpret_cast<double*>(sm);               // exchange [kGroups][ROW]
+    double* stage = xsm + kGroups * ROW;                       // staging [kGroups][ROW]
+    uint64_t* bar = sm + 2 * kGroups * ROW;
+    const uint32_t tid = threadIdx.x;
+    const uint32_t g = tid / 32, gt = tid % 32;
+    const uint32_t rowblk = blockIdx.x % (ROWS / kGroups);
+    const uint32_t limb_flat = blockIdx.x / (ROWS / kGroups);
+    const uint32_t prime = a.limb_prime[limb_flat % a.limbs];
+    const size_t N = size_t(1) << (L1 + kL2);
+    const uint64_t q = a.q[prime];
+    const DMod md = dmod_of(q);
+    const uint32_t R = rowblk * kGroups + g;
+    uint64_t* blk = limb_ptr(data, a, limb_flat, L1 + kL2) + static_cast<size_t>(rowblk) * kGroups * ROW;
+    rows_bulk_load(stage, blk, bar, a.fault);
+    double* my = stage + g * ROW;
+    uint64_t* myu = reinterpret_cast<uint64_t*>(my);
+    const double* twd = a.twd + prime * N;
+    if (EPI == 0) {
+        sub_fwd_d<kL2>(
+            xsm + g * ROW, gt, twd, md, [&](uint32_t m) { return m * (ROWS + R); }, [&](uint32_t e) { return my[e]; },
+            [&](uint32_t e, double v) { myu[e] = dto_residue(v, md); });
+        rows_bulk_store(blk, stage);
+    } else {
+        const uint32_t poly = limb_flat / a.limbs, limb = limb_flat % a.limbs;
+        const size_t off = (static_cast<size_t>(limb) << (L1 + kL2)) + static_cast<size_t>(R) * ROW;
+        const uint64_t* cx = a.epi_cx + poly * a.epi_cx_stride + off;
+        uint64_t* dst = a.epi_dst + poly * a.epi_dst_stride + off;
+        const uint64_t f = a.epi_f[limb], fs = a.epi_fs[limb];
+        sub_fwd_d<kL2>(
+            xsm + g * ROW, gt, twd, md, [&](uint32_t m) { return m * (ROWS + R); }, [&](uint32_t e) { return my[e]; },
+            [&](uint32_t e, double dv) {
+                const uint64_t v = dto_residue(dv, md);
+                uint64_t r = mul_shoup(sub_mod(cx[e], v, q), f, fs, q);
+                if (EPI == 2) r = add_mod(dst[e], r, q);
+                dst[e] = r;
+            });
+    }
+}
+
+template <int L1>
+__global__ void __launch_bounds__(kGroups * 32) k_rns_inv_rows_bulk(uint64_t* __restrict__ data, const RnsNttArgs a) {
+    constexpr uint32_t ROW = 1u << kL2, ROWS = 1u << L1;
+    extern __shared__ __align__(16) uint64_t sm[];
+    double* xsm = reinterpret_cast<double*>(sm);
+    double* stage = xsm + kGroups * ROW;
+    uint64_t* bar = sm + 2 * kGroups * ROW;
+    const uint32_t tid = threadIdx.x;
+    const uint32_t g = tid / 32, gt = tid % 32;
+    const uint32_t rowblk = blockIdx.x % (ROWS / kGroups);
+    const uint32_t limb_flat = blockIdx.x / (ROWS / kGroups);
+    const uint32_t prime = a.limb_prime[limb_flat % a.limbs];
+    const size_t N = size_t(1) << (L1 + kL2);
+    const uint64_t q = a.q[prime];
+    const uint32_t R = rowblk * kGroups + g;
+    const size_t blk_off = static_cast<size_t>(rowblk) * kGroups * ROW;
+    uint64_t* blk = limb_ptr(data, a, limb_flat, L1 + kL2) + blk_off;
+    const uint64_t* src = src_ptr(data, a, limb_flat, L1 + kL2) + blk_off;
+    rows_bulk_load(stage, src, bar, a.fault);
+    double* my = stage + g * ROW;
+    const uint64_t* myu = reinterpret_cast<const uint64_t*>(my);
+    sub_inv_d<kL2>(
+        xsm + g * ROW, gt, a.itwd + prime * N, dmod_of(q), [&](uint32_t m) { return m * (ROWS + R); },
+        [&](uint32_t e) { return __ull2double_rn(myu[e]); }, [&](uint32_t e, double v, int) { my[e] = v; });
+    rows_bulk_store(blk, stage);
+}
+
 // N = 2^10 .. 2^12: one CTA per limb polynomial, the register-blocked single-modulus transform
 // of ntt_core.cuh with the limb's prime tables, plus the same slot maps, out-of-place input,
 // inverse scaling and moddown epilogue as the 2-D kernels
@@ -654,14 +758,36 @@ static cudaError_t rns_launch(uint64_t* data, const RnsNttArgs& a, size_t limb_p
     const uint32_t col_threads = kGroups * (1u << L1) / 8, row_threads = kGroups * 32;
     const unsigned cb = static_cast<unsigned>(col_blocks), rb = static_cast<unsigned>(row_blocks);
     if (a.twd && a.itwd) {
-        // every prime of the chain is below 2^50: the FP64-pipe form
+        // every prime of the chain is below 2^50: the FP64-pipe form; its row phases move each
+        // CTA's 32 KB block with bulk copies when every block address is 16-byte aligned
+        const auto a16 = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; };
+        const bool bulk = a16(data) && (a.poly_stride & 1u) == 0 && (!a.in || (a16(a.in) && (a.in_poly_stride & 1u) == 0));
+        constexpr size_t bulk_smem = 2 * row_smem + 16;
+        static std::atomic<uint64_t> bulk_attr{0};
+        if (bulk && !(bulk_attr.load() >> dev & 1)) {
+            const void* fns[] = {reinterpret_cast<const void*>(k_rns_fwd_rows_bulk<L1, 0>),
+                                 reinterpret_cast<const void*>(k_rns_fwd_rows_bulk<L1, 1>),
+                                 reinterpret_cast<const void*>(k_rns_fwd_rows_bulk<L1, 2>),
+                                 reinterpret_cast<const void*>(k_rns_inv_rows_bulk<L1>)};
+            for (const void* fn : fns) {
+                cudaError_t e =
+                    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bulk_smem));
+                if (e != cudaSuccess) return e;
+            }
+            bulk_attr.fetch_or(uint64_t(1) << dev);
+        }
         if (!inverse) {
             k_rns_fwd_cols<L1, true><<<cb, col_threads, col_smem, s>>>(data, a);
-            if (a.epi == 0) k_rns_fwd_rows<L1, 0, true><<<rb, row_threads, row_smem, s>>>(data, a);
+            if (bulk) {
+                if (a.epi == 0) k_rns_fwd_rows_bulk<L1, 0><<<rb, row_threads, bulk_smem, s>>>(data, a);
+                else if (a.epi == 1) k_rns_fwd_rows_bulk<L1, 1><<<rb, row_threads, bulk_smem, s>>>(data, a);
+                else k_rns_fwd_rows_bulk<L1, 2><<<rb, row_threads, bulk_smem, s>>>(data, a);
+            } else if (a.epi == 0) k_rns_fwd_rows<L1, 0, true><<<rb, row_threads, row_smem, s>>>(data, a);
             else if (a.epi == 1) k_rns_fwd_rows<L1, 1, true><<<rb, row_threads, row_smem, s>>>(data, a);
             else k_rns_fwd_rows<L1, 2, true><<<rb, row_threads, row_smem, s>>>(data, a);
         } else {
-            k_rns_inv_rows<L1, true><<<rb, row_threads, row_smem, s>>>(data, a);
+            if (bulk) k_rns_inv_rows_bulk<L1><<<rb, row_threads, bulk_smem, s>>>(data, a);
+            else k_rns_inv_rows<L1, true><<<rb, row_threads, row_smem, s>>>(data, a);
             k_rns_inv_cols<L1, true><<<cb, col_threads, col_smem, s>>>(data, a);
         }
         return cudaGetLastError();

@@ -24,6 +24,7 @@ struct RnsNttArgs {
     // transforms (N >= 2^13) then run on the FP64 pipe, with the same results
     const double* twd = nullptr;
     const double* itwd = nullptr;
+    uint32_t* fault = nullptr;  // device word: bit 1 set if a bulk copy's bounded wait expired
     const uint32_t* limb_prime = nullptr;  // device [limbs]: table row of launch limb l
     const uint32_t* limb_slot = nullptr;   // device [limbs]: limb position in the polynomial (null: l)
     uint32_t limbs = 0;

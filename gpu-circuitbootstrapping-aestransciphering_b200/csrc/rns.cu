@@ -212,6 +212,7 @@ struct cbs_rns_context {
     std::vector<cbs::host::NttTables> tabs;
     DevBuf<uint64_t> d_tw, d_tws, d_itw, d_itws, d_q, d_ninv, d_ninv_s, d_r0, d_r1;
     DevBuf<double> d_twd, d_itwd;  // tw / itw as doubles when every prime is below 2^50
+    DevBuf<uint32_t> d_fault;      // device fault word (CBS_FAULT_* bits)
     DevBuf<cbs_dmodulus> d_mod;
     DevBuf<uint32_t> d_ident;  // 0 .. size_qp - 1
     std::map<uint32_t, std::unique_ptr<cbs::RnsLevel>> levels;
@@ -228,6 +229,7 @@ struct cbs_rns_context {
         a.n_inv_s = d_ninv_s.p;
         a.twd = d_twd.p;
         a.itwd = d_itwd.p;
+        a.fault = d_fault.p;
         return a;
     }
 };
@@ -492,6 +494,8 @@ cbs_status cbs_rns_context_create(uint32_t poly_degree, const uint64_t* h_q, uin
     if (c->red_k == 0) c->red_k = 1;
     CBS_CUDA_TRY(upload_sync(c->d_tw, tw));
     CBS_CUDA_TRY(upload_sync(c->d_tws, tws));
+    CBS_CUDA_TRY(c->d_fault.alloc(1));
+    CBS_CUDA_TRY(cudaMemset(c->d_fault.p, 0, sizeof(uint32_t)));
     if (qmax < (uint64_t(1) << 50)) {
         // exact doubles of the twiddles for the FP64-pipe transforms
         std::vector<double> twd(tw.begin(), tw.end()), itwd(itw.begin(), itw.end());
@@ -513,6 +517,15 @@ cbs_status cbs_rns_context_create(uint32_t poly_degree, const uint64_t* h_q, uin
 
 cbs_status cbs_rns_context_destroy(cbs_rns_context* ctx) {
     delete ctx;
+    return CBS_OK;
+}
+
+cbs_status cbs_rns_device_fault(cbs_rns_context* ctx, uint32_t* out, int clear) {
+    CBS_CHECK_ARG(ctx && out, "rns_device_fault: null argument");
+    CBS_CUDA_TRY(cudaSetDevice(ctx->device));
+    CBS_CUDA_TRY(cudaDeviceSynchronize());
+    CBS_CUDA_TRY(cudaMemcpy(out, ctx->d_fault.p, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    if (clear && *out) CBS_CUDA_TRY(cudaMemset(ctx->d_fault.p, 0, sizeof(uint32_t)));
     return CBS_OK;
 }
 

@@ -577,6 +577,12 @@ typedef struct {
 cbs_status cbs_rns_context_create(uint32_t poly_degree, const uint64_t *h_q, uint32_t size_q, const uint64_t *h_p,
                                   uint32_t size_p, cbs_rns_context **out);
 cbs_status cbs_rns_context_destroy(cbs_rns_context *ctx);
+/* Device fault word of the RNS context: bit CBS_RNS_FAULT_BULK_COPY is set when a bulk copy of
+ * the FP64-pipe transforms did not complete within its bounded wait (about a second); the
+ * launch then finishes with unreliable outputs instead of hanging.  Synchronizes the device;
+ * clear != 0 resets the word.  0 after every correct run.  No reference counterpart. */
+enum { CBS_RNS_FAULT_BULK_COPY = 1 };
+cbs_status cbs_rns_device_fault(cbs_rns_context *ctx, uint32_t *out, int clear);
 /* replaces PhantomContext::gpu_rns_tables() (include/context.cuh) */
 cbs_status cbs_rns_context_tables(const cbs_rns_context *ctx, cbs_rns_ntt_tables *out);
 /* Builds (once) the modup / moddown constants of level size_ql; the other calls build them on

@@ -54,6 +54,7 @@ def test_rns_ntt_bit_exact(env, logn, bits):
     want = ntt(o, x, chain[1:4])
     assert np.array_equal(got[:, :3], want)
     assert np.array_equal(got[:, 3], np.zeros((2, n), np.uint64))  # the gap is untouched
+    assert ctx.device_fault() == 0
     pkg.call("cbs_rns_ntt_batched", ctx.handle, d.data_ptr(), 2, stride, 3, 1, 1, None)
     torch.cuda.synchronize()
     assert np.array_equal(host(d).reshape(2, 4, n)[:, :3], x)
