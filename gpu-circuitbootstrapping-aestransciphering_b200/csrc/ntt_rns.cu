@@ -20,6 +20,7 @@
 
 #include "async_copy.cuh"
 #include "common.cuh"
+#include "fp64_mod.cuh"
 #include "ntt_core.cuh"
 #include "ntt_rns.cuh"
 
@@ -179,47 +180,11 @@ __device__ __forceinline__ void sub_inv(uint64_t* sm, uint32_t gt, const uint64_
 
 
 // ---------------------------------------------------------------------------------------------
-// FP64-pipe form (primes below 2^50).  The 64-bit Shoup products above are emulated with 32-bit
-// integer multiplies and bound the integer pipe while the FP64 pipe idles.  For q < 2^50 every
-// residue, lazy value and twiddle is an integer below 2^53, held exactly in a double, and the
-// modular product is computed exactly on the FP64 pipe:
-//   h = fl(v w), l = fma(v, w, -h)          (error-free product, Ogita-Rump-Oishi TwoProduct:
-//                                            v w = h + l exactly)
-//   k = rint(h / q)   (as h * fl(1/q))      (quotient estimate, within +-2 of v w / q)
-//   r = fma(-k, q, h) + l                    (= v w - k q exactly)
-// fma(-k, q, h) is exact because its true value h - k q = r - l is an integer of magnitude
-// below 2q + 2^49 < 2^53; r itself lies in (-2q, 2q) and is congruent to v w.  This is the
-// floating-point quotient estimate of Shoup's MulMod (NTL) carried out entirely in doubles.
-// Values are signed and lazy: each radix-8 pass first reduces its 8 inputs to |x| <= q/2 + 1
-// (x - rint(x/q) q, one FMA), after which three forward stages grow them to at most 2q + 4 and
-// three inverse stages to at most 4q + 8, far inside the exact range.  The twiddles are the
-// same tables converted to doubles; results are the integer path's residues, bit for bit.
-struct DMod {
-    double q, qinv;
-};
-
-__device__ __forceinline__ DMod dmod_of(uint64_t q) { return {static_cast<double>(q), 1.0 / static_cast<double>(q)}; }
-
-// v w mod q, in (-2q, 2q), exact for |v| < 2^52 and 0 <= w < q < 2^50
-__device__ __forceinline__ double dmulmod(double v, double w, const DMod& m) {
-    const double h = __dmul_rn(v, w);
-    const double l = __fma_rn(v, w, -h);
-    const double k = rint(__dmul_rn(h, m.qinv));
-    return __dadd_rn(__fma_rn(-k, m.q, h), l);
-}
-
-// x mod q in [-q/2 - 1, q/2 + 1] for |x| < 2^52
-__device__ __forceinline__ double dreduce(double x, const DMod& m) {
-    return __fma_rn(-rint(__dmul_rn(x, m.qinv)), m.q, x);
-}
-
-// [0, q) from |x| < 2^52
-__device__ __forceinline__ uint64_t dto_residue(double x, const DMod& m) {
-    double r = dreduce(x, m);
-    if (r < 0.0) r = __dadd_rn(r, m.q);
-    return __double2ull_rn(r);
-}
-
+// FP64-pipe form (primes below 2^50): the exact modular products of fp64_mod.cuh.  Values are
+// signed and lazy: each radix-8 pass first reduces its 8 inputs to |x| <= q/2 + 1, after which
+// three forward stages grow them to at most 2q + 4 and three inverse stages to at most
+// 4q + 8, far inside the exact range.  The twiddles are the same tables converted to doubles;
+// results are the integer path's residues, bit for bit.
 __device__ __forceinline__ void ct_bf_d(double& x, double& y, double w, const DMod& m) {
     const double t = dmulmod(y, w, m);
     y = __dsub_rn(x, t);

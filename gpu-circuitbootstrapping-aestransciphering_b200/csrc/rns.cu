@@ -26,6 +26,7 @@
 #include "arith.cuh"
 #include "common.cuh"
 #include "devbuf.cuh"
+#include "fp64_mod.cuh"
 #include "host_math.h"
 #include "ntt_rns.cuh"
 
@@ -58,6 +59,7 @@ struct ModupArgs {
     const uint64_t* r0;
     const uint64_t* r1;
     uint32_t log_n, ql, qlp, alpha, beta;
+    const double* qinv;  // fl(1 / q) per prime, when every prime is below 2^50 (null otherwise)
 };
 
 struct EvkPtrs {
@@ -78,6 +80,7 @@ struct ModdownArgs {
     const uint64_t* r0;
     const uint64_t* r1;
     uint32_t log_n, ql, qlp, alpha;
+    const double* qinv;  // fl(1 / q) per prime, when every prime is below 2^50 (null otherwise)
 };
 
 __device__ __forceinline__ uint64_t barrett(u128 x, const uint64_t* q, const uint64_t* r0, const uint64_t* r1,
@@ -121,6 +124,50 @@ __global__ void __launch_bounds__(kThreads) k_modup_bconv(const uint64_t* __rest
         for (uint32_t i = 0; i < kMaxAlpha; ++i)
             if (i < cnt) add_wide(acc, mul_wide(y[i], w[i]));
         tb[static_cast<size_t>(__ldg(slot + k)) * N] = barrett(acc, a.q, a.r0, a.r1, __ldg(prime + k));
+    }
+}
+
+// the same base conversion on the FP64 pipe (every prime below 2^50, fp64_mod.cuh): products
+// reduced exactly to |r| <= 0.875 q, partial sums folded every 8 terms; same residues
+__global__ void __launch_bounds__(kThreads) k_modup_bconv_d(const uint64_t* __restrict__ coef,
+                                                            const uint64_t* __restrict__ c2, uint64_t* __restrict__ t,
+                                                            const ModupArgs a) {
+    extern __shared__ uint64_t s_qhat[];
+    const uint32_t b = blockIdx.y, ct = blockIdx.z;
+    const uint32_t start = a.alpha * b;
+    const uint32_t cnt = (b == a.beta - 1) ? a.ql - a.alpha * (a.beta - 1) : a.alpha;
+    const uint32_t ncompl = a.qlp - cnt;
+    const uint64_t* qh = a.qhat + static_cast<size_t>(b) * a.qlp * a.alpha;
+    for (uint32_t i = threadIdx.x; i < ncompl * a.alpha; i += blockDim.x) s_qhat[i] = qh[i];
+    __syncthreads();
+    const size_t N = size_t(1) << a.log_n;
+    const size_t c = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const uint64_t* ci = coef + static_cast<size_t>(ct) * a.ql * N + start * N + c;
+    const uint64_t* c2i = c2 + static_cast<size_t>(ct) * a.ql * N + start * N + c;
+    uint64_t* tb = t + (static_cast<size_t>(ct) * a.beta + b) * a.qlp * N + c;
+    double y[kMaxAlpha];
+#pragma unroll
+    for (uint32_t i = 0; i < kMaxAlpha; ++i) {
+        if (i < cnt) {
+            y[i] = __ull2double_rn(ci[i * N]);
+            tb[(start + i) * N] = c2i[i * N];
+        }
+    }
+    const uint32_t* slot = a.out_slot + static_cast<size_t>(b) * a.qlp;
+    const uint32_t* prime = a.out_prime + static_cast<size_t>(b) * a.qlp;
+    for (uint32_t k = 0; k < ncompl; ++k) {
+        const uint32_t pk = __ldg(prime + k);
+        const DMod md{static_cast<double>(__ldg(a.q + pk)), __ldg(a.qinv + pk)};
+        const uint64_t* w = s_qhat + k * a.alpha;
+        double acc = 0.0;
+#pragma unroll
+        for (uint32_t i = 0; i < kMaxAlpha; ++i) {
+            if (i < cnt) {
+                if (i && (i & 7u) == 0) acc = dreduce(acc, md);
+                acc = __dadd_rn(acc, dmulmod(y[i], __ull2double_rn(w[i]), md));
+            }
+        }
+        tb[static_cast<size_t>(__ldg(slot + k)) * N] = dto_residue(acc, md);
     }
 }
 
@@ -174,6 +221,56 @@ __global__ void __launch_bounds__(kThreads) k_ks_inner(const uint64_t* __restric
     }
 }
 
+// the same inner product on the FP64 pipe (every prime below 2^50, fp64_mod.cuh): each product
+// is reduced exactly to |r| <= 0.875 q, sums of up to 8 of them are folded back to |x| <= q/2 + 1,
+// so every partial sum stays an exact integer below 2^53; same residues as k_ks_inner
+template <int CT>
+__global__ void __launch_bounds__(kThreads) k_ks_inner_d(const uint64_t* __restrict__ t, const EvkPtrs evk,
+                                                         uint64_t* __restrict__ cx, const InnerArgs a) {
+    const size_t N = size_t(1) << a.log_n;
+    const size_t idx = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;  // l * N + c
+    const uint32_t l = static_cast<uint32_t>(idx >> a.log_n);
+    const size_t c = idx & (N - 1);
+    const uint32_t pr = __ldg(a.prime + l);
+    const uint32_t ct0 = blockIdx.y * CT;
+    double acc0[CT], acc1[CT];
+#pragma unroll
+    for (int j = 0; j < CT; ++j) acc0[j] = acc1[j] = 0.0;
+    const size_t tstride = static_cast<size_t>(a.beta) * a.qlp * N;  // per ciphertext
+    const DMod md = dmod_of(__ldg(a.q + pr));
+    uint32_t since = 0;
+    for (uint32_t b = 0; b < a.beta; ++b) {
+        const double e0 = __ull2double_rn(__ldg(evk.p[b] + static_cast<size_t>(pr) * N + c));
+        const double e1 = __ull2double_rn(__ldg(evk.p[b] + (static_cast<size_t>(a.qp) + pr) * N + c));
+        const uint64_t* tb = t + (static_cast<size_t>(b) * a.qlp + l) * N + c;
+        if (since == 8) {
+#pragma unroll
+            for (int j = 0; j < CT; ++j) {
+                acc0[j] = dreduce(acc0[j], md);
+                acc1[j] = dreduce(acc1[j], md);
+            }
+            since = 0;
+        }
+#pragma unroll
+        for (int j = 0; j < CT; ++j) {
+            if (ct0 + j < a.count) {
+                const double x = __ull2double_rn(tb[(ct0 + j) * tstride]);
+                acc0[j] = __dadd_rn(acc0[j], dmulmod(x, e0, md));
+                acc1[j] = __dadd_rn(acc1[j], dmulmod(x, e1, md));
+            }
+        }
+        ++since;
+    }
+#pragma unroll
+    for (int j = 0; j < CT; ++j) {
+        if (ct0 + j < a.count) {
+            uint64_t* o = cx + (static_cast<size_t>(ct0 + j) * 2 * a.qlp + l) * N + c;
+            o[0] = dto_residue(acc0[j], md);
+            o[static_cast<size_t>(a.qlp) * N] = dto_residue(acc1[j], md);
+        }
+    }
+}
+
 // moddown, step 2: delta[poly][i] = sum_j y_j * Phat_j (mod q_i) from the scaled P residues
 // (src/rns_bconv.cu:798-801, bConv_BEHZ base_P_to_Ql)
 __global__ void __launch_bounds__(kThreads) k_moddown_bconv(const uint64_t* __restrict__ cx,
@@ -200,6 +297,36 @@ __global__ void __launch_bounds__(kThreads) k_moddown_bconv(const uint64_t* __re
     }
 }
 
+// the same on the FP64 pipe (every prime below 2^50, fp64_mod.cuh); same residues
+__global__ void __launch_bounds__(kThreads) k_moddown_bconv_d(const uint64_t* __restrict__ cx,
+                                                              uint64_t* __restrict__ delta, const ModdownArgs a) {
+    extern __shared__ uint64_t s_phat[];
+    for (uint32_t i = threadIdx.x; i < a.ql * a.alpha; i += blockDim.x) s_phat[i] = a.phat[i];
+    __syncthreads();
+    const size_t N = size_t(1) << a.log_n;
+    const size_t c = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const uint32_t poly = blockIdx.y;
+    const uint64_t* src = cx + (static_cast<size_t>(poly) * a.qlp + a.ql) * N + c;
+    double y[kMaxAlpha];
+#pragma unroll
+    for (uint32_t j = 0; j < kMaxAlpha; ++j)
+        if (j < a.alpha) y[j] = __ull2double_rn(src[j * N]);
+    uint64_t* dst = delta + static_cast<size_t>(poly) * a.ql * N + c;
+    for (uint32_t i = 0; i < a.ql; ++i) {
+        const DMod md{static_cast<double>(__ldg(a.q + i)), __ldg(a.qinv + i)};
+        const uint64_t* w = s_phat + i * a.alpha;
+        double acc = 0.0;
+#pragma unroll
+        for (uint32_t j = 0; j < kMaxAlpha; ++j) {
+            if (j < a.alpha) {
+                if (j && (j & 7u) == 0) acc = dreduce(acc, md);
+                acc = __dadd_rn(acc, dmulmod(y[j], __ull2double_rn(w[j]), md));
+            }
+        }
+        dst[i * N] = dto_residue(acc, md);
+    }
+}
+
 }  // namespace cbs
 
 using cbs::DevBuf;
@@ -212,6 +339,7 @@ struct cbs_rns_context {
     std::vector<cbs::host::NttTables> tabs;
     DevBuf<uint64_t> d_tw, d_tws, d_itw, d_itws, d_q, d_ninv, d_ninv_s, d_r0, d_r1;
     DevBuf<double> d_twd, d_itwd;  // tw / itw as doubles when every prime is below 2^50
+    DevBuf<double> d_qinv;         // fl(1 / q) per prime, likewise
     DevBuf<uint32_t> d_fault;      // device fault word (CBS_FAULT_* bits)
     DevBuf<cbs_dmodulus> d_mod;
     DevBuf<uint32_t> d_ident;  // 0 .. size_qp - 1
@@ -364,7 +492,12 @@ cbs_status run_modup(cbs_rns_context* c, cbs::RnsLevel* lv, uint64_t* d_t, const
                      c->log_n, lv->ql, lv->qlp, lv->alpha, lv->beta};
     const dim3 grid(static_cast<unsigned>(N / cbs::kThreads), lv->beta, count);
     const size_t smem = static_cast<size_t>(lv->qlp) * lv->alpha * sizeof(uint64_t);
-    cbs::k_modup_bconv<<<grid, cbs::kThreads, smem, s>>>(c->s_coef.p, d_c2, d_t, m);
+    if (c->d_qinv.p) {
+        m.qinv = c->d_qinv.p;
+        cbs::k_modup_bconv_d<<<grid, cbs::kThreads, smem, s>>>(c->s_coef.p, d_c2, d_t, m);
+    } else {
+        cbs::k_modup_bconv<<<grid, cbs::kThreads, smem, s>>>(c->s_coef.p, d_c2, d_t, m);
+    }
     CBS_LAUNCH_CHECK();
     // 3. forward NTT of every converted limb (the digit's own limbs are already NTT domain)
     cbs::RnsNttArgs f = c->ntt_args();
@@ -387,7 +520,8 @@ cbs_status run_inner(cbs_rns_context* c, cbs::RnsLevel* lv, uint64_t* d_cx, cons
     cbs::InnerArgs a{lv->ip_prime.p, c->d_q.p, c->d_r0.p, c->d_r1.p, c->log_n, lv->qlp, c->size_qp,
                      lv->beta, count, c->red_k};
     const dim3 grid(static_cast<unsigned>(static_cast<size_t>(lv->qlp) * c->n / cbs::kThreads), (count + CT - 1) / CT);
-    cbs::k_ks_inner<CT><<<grid, cbs::kThreads, 0, s>>>(d_t, e, d_cx, a);
+    if (c->d_twd.p) cbs::k_ks_inner_d<CT><<<grid, cbs::kThreads, 0, s>>>(d_t, e, d_cx, a);
+    else cbs::k_ks_inner<CT><<<grid, cbs::kThreads, 0, s>>>(d_t, e, d_cx, a);
     CBS_LAUNCH_CHECK();
     return CBS_OK;
 }
@@ -410,8 +544,13 @@ cbs_status run_moddown(cbs_rns_context* c, cbs::RnsLevel* lv, uint64_t* d_ct, ui
     // 2. base conversion P -> Ql
     cbs::ModdownArgs m{lv->md_phat.p, c->d_q.p, c->d_r0.p, c->d_r1.p, c->log_n, lv->ql, lv->qlp, lv->alpha};
     const dim3 grid(static_cast<unsigned>(N / cbs::kThreads), polys);
-    cbs::k_moddown_bconv<<<grid, cbs::kThreads, static_cast<size_t>(lv->ql) * lv->alpha * sizeof(uint64_t), s>>>(
-        d_cx, c->s_delta.p, m);
+    const size_t md_smem = static_cast<size_t>(lv->ql) * lv->alpha * sizeof(uint64_t);
+    if (c->d_qinv.p) {
+        m.qinv = c->d_qinv.p;
+        cbs::k_moddown_bconv_d<<<grid, cbs::kThreads, md_smem, s>>>(d_cx, c->s_delta.p, m);
+    } else {
+        cbs::k_moddown_bconv<<<grid, cbs::kThreads, md_smem, s>>>(d_cx, c->s_delta.p, m);
+    }
     CBS_LAUNCH_CHECK();
     // 3. forward NTT of delta with the fused (cx - delta) * P^-1 epilogue
     cbs::RnsNttArgs f = c->ntt_args();
@@ -498,9 +637,11 @@ cbs_status cbs_rns_context_create(uint32_t poly_degree, const uint64_t* h_q, uin
     CBS_CUDA_TRY(cudaMemset(c->d_fault.p, 0, sizeof(uint32_t)));
     if (qmax < (uint64_t(1) << 50)) {
         // exact doubles of the twiddles for the FP64-pipe transforms
-        std::vector<double> twd(tw.begin(), tw.end()), itwd(itw.begin(), itw.end());
+        std::vector<double> twd(tw.begin(), tw.end()), itwd(itw.begin(), itw.end()), qinv(L);
+        for (size_t i = 0; i < L; ++i) qinv[i] = 1.0 / static_cast<double>(primes[i]);
         CBS_CUDA_TRY(upload_sync(c->d_twd, twd));
         CBS_CUDA_TRY(upload_sync(c->d_itwd, itwd));
+        CBS_CUDA_TRY(upload_sync(c->d_qinv, qinv));
     }
     CBS_CUDA_TRY(upload_sync(c->d_itw, itw));
     CBS_CUDA_TRY(upload_sync(c->d_itws, itws));
