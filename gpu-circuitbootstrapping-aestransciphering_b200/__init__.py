@@ -142,6 +142,18 @@ def _declare(lib: ctypes.CDLL) -> None:
         "cbs_rns_context_create": (st, [u32, c_vp, u32, c_vp, u32, c_vp]),
         "cbs_rns_context_destroy": (st, [c_vp]),
         "cbs_rns_device_fault": (st, [c_vp, c_vp, ctypes.c_int]),
+        "cbs_ckks_add_inplace": (st, [c_vp, c_vp, c_vp, u32, u32, c_vp]),
+        "cbs_ckks_sub_inplace": (st, [c_vp, c_vp, c_vp, u32, u32, ctypes.c_int, c_vp]),
+        "cbs_ckks_negate_inplace": (st, [c_vp, c_vp, u32, u32, c_vp]),
+        "cbs_ckks_multiply_plain_inplace": (st, [c_vp, c_vp, c_vp, u32, u32, c_vp]),
+        "cbs_ckks_multiply_inplace": (st, [c_vp, c_vp, c_vp, u32, c_vp]),
+        "cbs_ckks_relinearize_inplace": (st, [c_vp, c_vp, c_vp, u32, c_vp]),
+        "cbs_ckks_multiply_and_relin_inplace": (st, [c_vp, c_vp, c_vp, c_vp, u32, c_vp]),
+        "cbs_ckks_rescale_to_next": (st, [c_vp, c_vp, c_vp, u32, u32, c_vp]),
+        "cbs_ckks_mod_switch_to_next": (st, [c_vp, c_vp, c_vp, u32, u32, c_vp]),
+        "cbs_ckks_galois_elt_from_step": (u32, [ctypes.c_int, u32]),
+        "cbs_ckks_apply_galois_inplace": (st, [c_vp, c_vp, u32, c_vp, u32, c_vp]),
+        "cbs_ckks_rotate_inplace": (st, [c_vp, c_vp, ctypes.c_int, c_vp, u32, c_vp]),
         "cbs_rns_context_tables": (st, [c_vp, c_vp]),
         "cbs_rns_prepare_level": (st, [c_vp, u32]),
         "cbs_nwt_2d_radix8_forward_inplace": (st, [c_vp, c_vp, u32, u32, c_vp]),

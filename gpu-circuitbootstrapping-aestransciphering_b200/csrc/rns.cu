@@ -29,6 +29,7 @@
 #include "fp64_mod.cuh"
 #include "host_math.h"
 #include "ntt_rns.cuh"
+#include "rns_context.cuh"
 
 namespace cbs {
 
@@ -37,19 +38,6 @@ constexpr uint32_t kMaxChain = 256;  // primes in Q + P
 constexpr uint32_t kMaxBeta = 64;    // digits
 constexpr uint32_t kThreads = 256;
 
-// per-level constants of modup / moddown (built on first use of a level)
-struct RnsLevel {
-    uint32_t ql = 0, qlp = 0, alpha = 0, beta = 0, ntt_limbs = 0;
-    DevBuf<uint64_t> mu_scale, mu_scale_s;       // [ql] partQlHatInv_mod_Ql (rns.cu:120-200)
-    DevBuf<uint32_t> mu_out_slot, mu_out_prime;  // [beta][qlp] complement limbs of each digit
-    DevBuf<uint64_t> mu_qhat;                    // [beta][qlp][alpha] qhat_i mod m_out
-    DevBuf<uint32_t> mu_ntt_slot, mu_ntt_prime;  // [ntt_limbs] limbs transformed after bconv
-    DevBuf<uint32_t> ip_prime;                   // [qlp] key-chain index of limb l of QlP
-    DevBuf<uint32_t> md_slot, md_prime;          // [alpha] P limbs inside a QlP poly
-    DevBuf<uint64_t> md_scale, md_scale_s;       // [alpha] Phat_j^-1 mod p_j
-    DevBuf<uint64_t> md_phat;                    // [ql][alpha] Phat_j mod q_i
-    DevBuf<uint64_t> md_pinv, md_pinv_s;         // [ql] P^-1 mod q_i
-};
 
 struct ModupArgs {
     const uint32_t* out_slot;
@@ -331,36 +319,6 @@ __global__ void __launch_bounds__(kThreads) k_moddown_bconv_d(const uint64_t* __
 
 using cbs::DevBuf;
 
-struct cbs_rns_context {
-    uint32_t log_n = 0, n = 0, size_q = 0, size_p = 0, size_qp = 0;
-    uint32_t red_k = 1;
-    int device = 0;
-    std::vector<uint64_t> primes;  // Q chain then P
-    std::vector<cbs::host::NttTables> tabs;
-    DevBuf<uint64_t> d_tw, d_tws, d_itw, d_itws, d_q, d_ninv, d_ninv_s, d_r0, d_r1;
-    DevBuf<double> d_twd, d_itwd;  // tw / itw as doubles when every prime is below 2^50
-    DevBuf<double> d_qinv;         // fl(1 / q) per prime, likewise
-    DevBuf<uint32_t> d_fault;      // device fault word (CBS_FAULT_* bits)
-    DevBuf<cbs_dmodulus> d_mod;
-    DevBuf<uint32_t> d_ident;  // 0 .. size_qp - 1
-    std::map<uint32_t, std::unique_ptr<cbs::RnsLevel>> levels;
-    DevBuf<uint64_t> s_coef, s_t, s_cx, s_delta;  // scratch, grown on demand
-
-    cbs::RnsNttArgs ntt_args() const {
-        cbs::RnsNttArgs a;
-        a.tw = d_tw.p;
-        a.tws = d_tws.p;
-        a.itw = d_itw.p;
-        a.itws = d_itws.p;
-        a.q = d_q.p;
-        a.n_inv = d_ninv.p;
-        a.n_inv_s = d_ninv_s.p;
-        a.twd = d_twd.p;
-        a.itwd = d_itwd.p;
-        a.fault = d_fault.p;
-        return a;
-    }
-};
 
 namespace {
 
@@ -379,6 +337,10 @@ uint64_t prod_mod(const std::vector<uint64_t>& ms, size_t skip, uint64_t m) {
         if (k != skip) r = cbs::host::mulmod(r, ms[k] % m, m);
     return r;
 }
+
+}  // namespace
+
+namespace cbs {
 
 // constants of level ql (host restatement of src/rns.cu:120-200 and the BEHZ tables of
 // src/rns_base.cu for the part/complement and P/Ql bases)
@@ -470,6 +432,14 @@ cbs_status grow(DevBuf<uint64_t>& b, size_t words) {
     CBS_CUDA_TRY(b.alloc(words));
     return CBS_OK;
 }
+
+}  // namespace cbs
+
+namespace {
+
+using cbs::build_level;
+using cbs::check_level;
+using cbs::grow;
 
 // modup of count ciphertexts' c2 [count][ql][N] into t [count][beta][qlp][N]
 cbs_status run_modup(cbs_rns_context* c, cbs::RnsLevel* lv, uint64_t* d_t, const uint64_t* d_c2, uint32_t count,
@@ -569,6 +539,31 @@ cbs_status run_moddown(cbs_rns_context* c, cbs::RnsLevel* lv, uint64_t* d_ct, ui
 }
 
 }  // namespace
+
+namespace cbs {
+
+cbs_status run_keyswitch(cbs_rns_context* ctx, uint64_t* d_ct, const uint64_t* d_c2, const uint64_t* const* h_evks,
+                         uint32_t size_ql, uint32_t count, cudaStream_t stream) {
+    cbs_status st = check_level(ctx, size_ql);
+    if (st != CBS_OK) return st;
+    CBS_CHECK_ARG(count <= 32767, "rns_keyswitch_inplace: count above 32767");
+    if (count == 0) return CBS_OK;
+    RnsLevel* lv = nullptr;
+    st = build_level(ctx, size_ql, &lv);
+    if (st != CBS_OK) return st;
+    const size_t N = ctx->n;
+    st = grow(ctx->s_t, static_cast<size_t>(count) * lv->beta * lv->qlp * N);
+    if (st != CBS_OK) return st;
+    st = grow(ctx->s_cx, static_cast<size_t>(count) * 2 * lv->qlp * N);
+    if (st != CBS_OK) return st;
+    st = run_modup(ctx, lv, ctx->s_t.p, d_c2, count, stream);
+    if (st != CBS_OK) return st;
+    st = run_inner(ctx, lv, ctx->s_cx.p, ctx->s_t.p, h_evks, count, stream);
+    if (st != CBS_OK) return st;
+    return run_moddown(ctx, lv, d_ct, ctx->s_cx.p, 2 * count, true, stream);
+}
+
+}  // namespace cbs
 
 extern "C" {
 
@@ -765,24 +760,8 @@ cbs_status cbs_rns_moddown_from_ntt(cbs_rns_context* ctx, uint64_t* d_ct, uint64
 cbs_status cbs_rns_keyswitch_inplace(cbs_rns_context* ctx, uint64_t* d_ct, const uint64_t* d_c2,
                                      const uint64_t* const* h_evks, uint32_t size_ql, uint32_t count,
                                      cbs_stream_t stream) {
-    cbs_status st = check_level(ctx, size_ql);
-    if (st != CBS_OK) return st;
     CBS_CHECK_ARG(d_ct && d_c2 && h_evks, "rns_keyswitch_inplace: null argument");
-    CBS_CHECK_ARG(count <= 32767, "rns_keyswitch_inplace: count above 32767");
-    if (count == 0) return CBS_OK;
-    cbs::RnsLevel* lv = nullptr;
-    st = build_level(ctx, size_ql, &lv);
-    if (st != CBS_OK) return st;
-    const size_t N = ctx->n;
-    st = grow(ctx->s_t, static_cast<size_t>(count) * lv->beta * lv->qlp * N);
-    if (st != CBS_OK) return st;
-    st = grow(ctx->s_cx, static_cast<size_t>(count) * 2 * lv->qlp * N);
-    if (st != CBS_OK) return st;
-    st = run_modup(ctx, lv, ctx->s_t.p, d_c2, count, stream);
-    if (st != CBS_OK) return st;
-    st = run_inner(ctx, lv, ctx->s_cx.p, ctx->s_t.p, h_evks, count, stream);
-    if (st != CBS_OK) return st;
-    return run_moddown(ctx, lv, d_ct, ctx->s_cx.p, 2 * count, true, stream);
+    return cbs::run_keyswitch(ctx, d_ct, d_c2, h_evks, size_ql, count, stream);
 }
 
 }  // extern "C"

@@ -626,6 +626,57 @@ cbs_status cbs_rns_keyswitch_inplace(cbs_rns_context *ctx, uint64_t *d_ct, const
                                      const uint64_t *const *h_evks, uint32_t size_ql, uint32_t count,
                                      cbs_stream_t stream);
 
+/* ---- CKKS evaluator on the RNS context (src/evaluate.cu; csrc/ckks.cu) ----
+ * Ciphertexts are NTT-domain polynomials over the first size_ql primes of the chain,
+ * [size][size_ql][N] (PhantomCiphertext::data(): size 2, or 3 after a multiplication); all
+ * outputs fully reduced.  Key arrays are host arrays of beta device pointers, as for
+ * cbs_rns_keyswitch_inplace. */
+/* replaces add_inplace (include/evaluate.cuh:46): ct1 += ct2 over size polynomials */
+cbs_status cbs_ckks_add_inplace(cbs_rns_context *ctx, uint64_t *d_ct1, const uint64_t *d_ct2, uint32_t size,
+                                uint32_t size_ql, cbs_stream_t stream);
+/* replaces sub_inplace (include/evaluate.cuh:61): ct1 = ct1 - ct2, or ct2 - ct1 when negate */
+cbs_status cbs_ckks_sub_inplace(cbs_rns_context *ctx, uint64_t *d_ct1, const uint64_t *d_ct2, uint32_t size,
+                                uint32_t size_ql, int negate, cbs_stream_t stream);
+/* replaces negate_inplace (include/evaluate.cuh:37) */
+cbs_status cbs_ckks_negate_inplace(cbs_rns_context *ctx, uint64_t *d_ct, uint32_t size, uint32_t size_ql,
+                                   cbs_stream_t stream);
+/* replaces multiply_plain_inplace (include/evaluate.cuh:94), CKKS: every polynomial times the
+ * NTT-domain plaintext d_plain [size_ql][N] */
+cbs_status cbs_ckks_multiply_plain_inplace(cbs_rns_context *ctx, uint64_t *d_ct, const uint64_t *d_plain,
+                                           uint32_t size, uint32_t size_ql, cbs_stream_t stream);
+/* replaces multiply_inplace (include/evaluate.cuh:105; bgv_ckks_multiply, src/evaluate.cu:345):
+ * d_ct1 [3][size_ql][N] holds (a0, a1) on entry and (a0 b0, a0 b1 + a1 b0, a1 b1) on return;
+ * d_ct2 = (b0, b1), or d_ct1 itself to square; other overlaps are rejected */
+cbs_status cbs_ckks_multiply_inplace(cbs_rns_context *ctx, uint64_t *d_ct1, const uint64_t *d_ct2, uint32_t size_ql,
+                                     cbs_stream_t stream);
+/* replaces relinearize_inplace (include/evaluate.cuh:125; src/evaluate.cu:1345): d_ct
+ * [3][size_ql][N] -> its first two polynomials += keyswitch(c2) with the relinearisation key */
+cbs_status cbs_ckks_relinearize_inplace(cbs_rns_context *ctx, uint64_t *d_ct, const uint64_t *const *h_relin_keys,
+                                        uint32_t size_ql, cbs_stream_t stream);
+/* replaces multiply_and_relin_inplace (include/evaluate.cuh:115) */
+cbs_status cbs_ckks_multiply_and_relin_inplace(cbs_rns_context *ctx, uint64_t *d_ct1, const uint64_t *d_ct2,
+                                               const uint64_t *const *h_relin_keys, uint32_t size_ql,
+                                               cbs_stream_t stream);
+/* replaces rescale_to_next (include/evaluate.cuh:137; DRNSTool::divide_and_round_q_last_ntt,
+ * src/rns.cu:1183-1208): d_src [size][size_ql][N] -> d_dst [size][size_ql - 1][N]; d_src is
+ * left unchanged (the reference works on a copy) */
+cbs_status cbs_ckks_rescale_to_next(cbs_rns_context *ctx, uint64_t *d_dst, const uint64_t *d_src, uint32_t size,
+                                    uint32_t size_ql, cbs_stream_t stream);
+/* replaces mod_switch_to_next (include/evaluate.cuh:146), CKKS: drop the last limb */
+cbs_status cbs_ckks_mod_switch_to_next(cbs_rns_context *ctx, uint64_t *d_dst, const uint64_t *d_src, uint32_t size,
+                                       uint32_t size_ql, cbs_stream_t stream);
+/* replaces phantom::util::get_elt_from_step (include/galois.cuh:17): the Galois element of a
+ * rotation by step slots (0 = conjugation); 0 when |step| >= N/2 */
+uint32_t cbs_ckks_galois_elt_from_step(int step, uint32_t poly_degree);
+/* replaces apply_galois_inplace (include/evaluate.cuh:215; src/evaluate.cu:1571), CKKS: the
+ * NTT-slot permutation of the element on both polynomials, then c1 wiped and
+ * (c0, 0) += keyswitch(sigma(c1)) with the element's Galois key.  d_ct [2][size_ql][N]. */
+cbs_status cbs_ckks_apply_galois_inplace(cbs_rns_context *ctx, uint64_t *d_ct, uint32_t galois_elt,
+                                         const uint64_t *const *h_galois_keys, uint32_t size_ql, cbs_stream_t stream);
+/* replaces rotate_inplace (include/evaluate.cuh:229) */
+cbs_status cbs_ckks_rotate_inplace(cbs_rns_context *ctx, uint64_t *d_ct, int step, const uint64_t *const *h_galois_keys,
+                                   uint32_t size_ql, cbs_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -72,4 +72,22 @@ int ref_rns_moddown_from_ntt(void* ctx, uint32_t size_ql, uint64_t* ct, uint64_t
     }
 }
 
+// divide_and_round_q_last_ntt (CKKS rescale_to_next, src/rns.cu:1183-1208) of `size`
+// polynomials at the level with size_ql primes: src [size][size_ql][N] (its last limb is
+// transformed in place, as in the reference) -> dst [size][size_ql - 1][N]
+int ref_rns_rescale(void* ctx, uint32_t size_ql, uint64_t* dst, uint64_t* src, uint32_t size, void* stream) {
+    try {
+        auto* c = static_cast<PhantomContext*>(ctx);
+        const auto& key = c->get_context_data(0);
+        const size_t size_q = key.parms().coeff_modulus().size() - key.parms().special_modulus_size();
+        const size_t idx = 1 + (size_q - size_ql);
+        const auto& rns = c->get_context_data_rns_tool(idx);
+        const cudaStream_t s = static_cast<cudaStream_t>(stream);
+        rns.divide_and_round_q_last_ntt(dst, src, size, c->gpu_rns_tables(), s);
+        return static_cast<int>(cudaStreamSynchronize(s));
+    } catch (...) {
+        return -1;
+    }
+}
+
 }  // extern "C"

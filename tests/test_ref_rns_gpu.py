@@ -38,6 +38,7 @@ def ref():
     lib.ref_rns_destroy.argtypes = [vp]
     lib.ref_rns_modup.argtypes = [vp, u32, vp, vp, u32, vp]
     lib.ref_rns_moddown_from_ntt.argtypes = [vp, u32, vp, vp, u32, vp]
+    lib.ref_rns_rescale.argtypes = [vp, u32, vp, vp, u32, vp]
     return lib
 
 
@@ -87,6 +88,32 @@ def test_modup_moddown_match_reference_rns_tool(pkg, ref, logn, size_q, size_p, 
         out_t = torch.zeros_like(out_m)
         pkg.call("cbs_rns_moddown_from_ntt", ctx.handle, out_m.data_ptr(), d_cx_m.data_ptr(), size_ql, polys, 0, None)
         assert ref.ref_rns_moddown_from_ntt(rctx, size_ql, out_t.data_ptr(), d_cx_t.data_ptr(), polys, None) == 0
+        torch.cuda.synchronize()
+        assert np.array_equal(_host(out_m, out_m.shape), _host(out_t, out_t.shape))
+    finally:
+        ref.ref_rns_destroy(rctx)
+        ctx.close()
+
+
+@pytest.mark.parametrize("logn,size_q,size_ql", [(13, 5, 5), (14, 6, 4), (16, 24, 24)])
+def test_rescale_matches_reference_rns_tool(pkg, ref, logn, size_q, size_ql):
+    """cbs_ckks_rescale_to_next against the reference's DRNSTool::divide_and_round_q_last_ntt
+    (src/rns.cu:1183-1208) on the same NTT-domain ciphertext: the same words."""
+    n, size_p, size = 1 << logn, 2, 2
+    chain = np.zeros(size_q + size_p, np.uint64)
+    pkg.call("cbs_get_primes", n, 50, size_q + size_p, chain.ctypes.data)
+    q, p = chain[:size_q].copy(), chain[size_q:].copy()
+    ctx = pkg.RnsContext(n, q, p)
+    rctx = ref.ref_rns_create(logn, chain.ctypes.data, size_q, size_p)
+    assert rctx
+    try:
+        rng = np.random.default_rng(logn * 31 + size_ql)
+        src = _limbs(rng, q[:size_ql], n, (size,))
+        d_src_m, d_src_t = _dev(src), _dev(src)
+        out_m = torch.zeros((size, size_ql - 1, n), dtype=torch.int64, device="cuda")
+        out_t = torch.zeros_like(out_m)
+        pkg.call("cbs_ckks_rescale_to_next", ctx.handle, out_m.data_ptr(), d_src_m.data_ptr(), size, size_ql, None)
+        assert ref.ref_rns_rescale(rctx, size_ql, out_t.data_ptr(), d_src_t.data_ptr(), size, None) == 0
         torch.cuda.synchronize()
         assert np.array_equal(_host(out_m, out_m.shape), _host(out_t, out_t.shape))
     finally:
