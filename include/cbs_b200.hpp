@@ -21,6 +21,7 @@
 #include <stdexcept>
 #include <string>
 #include <utility>
+#include <map>
 #include <vector>
 
 #include "cbs_b200.h"
@@ -389,10 +390,50 @@ class PhantomCiphertext {
     [[nodiscard]] size_t coeff_modulus_size() const { return coeff_modulus_size_; }
     [[nodiscard]] size_t poly_modulus_degree() const { return poly_modulus_degree_; }
     [[nodiscard]] bool is_ntt_form() const { return is_ntt_form_; }
+    // CKKS scale bookkeeping (PhantomCiphertext::GetScalingFactor / SetScalingFactor)
+    [[nodiscard]] double GetScalingFactor() const { return scale_; }
+    void SetScalingFactor(double scale) { scale_ = scale; }
+    // keep the first min(size, new_size) polynomials, grow or shrink to new_size (device copy)
+    void resize_keep(size_t new_size, const cudaStream_t& stream) {
+        const size_t per = coeff_modulus_size_ * poly_modulus_degree_;
+        if (new_size > size_) {
+            DeviceArray<uint64_t> bigger(new_size * per);
+            check_cuda(cudaMemcpyAsync(bigger.data(), data_.data(), size_ * per * 8, cudaMemcpyDeviceToDevice, stream),
+                       "PhantomCiphertext");
+            data_ = std::move(bigger);
+        }
+        size_ = new_size;
+    }
+    // the storage of a ciphertext one level down (chain index + 1), same size
+    void reset_level(const PhantomContext& context, size_t chain_index, DeviceArray<uint64_t>&& data) {
+        chain_index_ = chain_index;
+        coeff_modulus_size_ = context.coeff_modulus_size(chain_index);
+        data_ = std::move(data);
+    }
 
    private:
     size_t size_ = 0, chain_index_ = 0, coeff_modulus_size_ = 0, poly_modulus_degree_ = 0;
     bool is_ntt_form_ = true;
+    double scale_ = 1.0;
+    DeviceArray<uint64_t> data_;
+};
+
+// PhantomPlaintext: one NTT-form polynomial of coeff_modulus_size limbs on the device
+// ([coeff_modulus_size][N] words) at chain index c.
+class PhantomPlaintext {
+   public:
+    PhantomPlaintext() = default;
+    void resize(const PhantomContext& context, size_t chain_index) {
+        chain_index_ = chain_index;
+        coeff_modulus_size_ = context.coeff_modulus_size(chain_index);
+        data_.resize(coeff_modulus_size_ * context.poly_degree());
+    }
+    [[nodiscard]] uint64_t* data() const { return data_.data(); }
+    [[nodiscard]] size_t chain_index() const { return chain_index_; }
+    [[nodiscard]] size_t coeff_modulus_size() const { return coeff_modulus_size_; }
+
+   private:
+    size_t chain_index_ = 0, coeff_modulus_size_ = 0;
     DeviceArray<uint64_t> data_;
 };
 
@@ -433,6 +474,128 @@ inline void keyswitch_inplace(const PhantomContext& context, PhantomCiphertext& 
     check(cbs_rns_keyswitch_inplace(context.handle(), encrypted.data(), c2, relin_keys.public_keys_ptr(), size_ql, 1,
                                     as_stream(stream)),
           "keyswitch_inplace");
+}
+
+// ---- CKKS evaluator (include/evaluate.cuh; csrc/ckks.cu), NTT-form ciphertexts ----
+inline uint32_t level_limbs(const PhantomCiphertext& ct) { return static_cast<uint32_t>(ct.coeff_modulus_size()); }
+inline void same_level(const PhantomCiphertext& a, const PhantomCiphertext& b, const char* what) {
+    if (a.chain_index() != b.chain_index()) throw Error(CBS_ERR_SHAPE_MISMATCH, std::string(what) + ": level mismatch");
+}
+
+// add_inplace (include/evaluate.cuh:46)
+inline void add_inplace(const PhantomContext& context, PhantomCiphertext& encrypted1,
+                        const PhantomCiphertext& encrypted2) {
+    same_level(encrypted1, encrypted2, "add_inplace");
+    if (encrypted1.size() != encrypted2.size()) throw Error(CBS_ERR_SHAPE_MISMATCH, "add_inplace: size mismatch");
+    check(cbs_ckks_add_inplace(context.handle(), encrypted1.data(), encrypted2.data(),
+                               static_cast<uint32_t>(encrypted1.size()), level_limbs(encrypted1), nullptr),
+          "add_inplace");
+}
+// sub_inplace (include/evaluate.cuh:61): encrypted1 -= encrypted2, or encrypted2 - encrypted1
+inline void sub_inplace(const PhantomContext& context, PhantomCiphertext& encrypted1,
+                        const PhantomCiphertext& encrypted2, bool negate = false) {
+    same_level(encrypted1, encrypted2, "sub_inplace");
+    if (encrypted1.size() != encrypted2.size()) throw Error(CBS_ERR_SHAPE_MISMATCH, "sub_inplace: size mismatch");
+    check(cbs_ckks_sub_inplace(context.handle(), encrypted1.data(), encrypted2.data(),
+                               static_cast<uint32_t>(encrypted1.size()), level_limbs(encrypted1), negate ? 1 : 0,
+                               nullptr),
+          "sub_inplace");
+}
+// negate_inplace (include/evaluate.cuh:37)
+inline void negate_inplace(const PhantomContext& context, PhantomCiphertext& encrypted) {
+    check(cbs_ckks_negate_inplace(context.handle(), encrypted.data(), static_cast<uint32_t>(encrypted.size()),
+                                  level_limbs(encrypted), nullptr),
+          "negate_inplace");
+}
+// multiply_plain_inplace (include/evaluate.cuh:94)
+inline void multiply_plain_inplace(const PhantomContext& context, PhantomCiphertext& encrypted,
+                                   const PhantomPlaintext& plain) {
+    if (plain.chain_index() != encrypted.chain_index())
+        throw Error(CBS_ERR_SHAPE_MISMATCH, "multiply_plain_inplace: level mismatch");
+    check(cbs_ckks_multiply_plain_inplace(context.handle(), encrypted.data(), plain.data(),
+                                          static_cast<uint32_t>(encrypted.size()), level_limbs(encrypted), nullptr),
+          "multiply_plain_inplace");
+}
+// multiply_inplace (include/evaluate.cuh:105): size-2 operands, encrypted1 becomes size 3;
+// CKKS scales multiply
+inline void multiply_inplace(const PhantomContext& context, PhantomCiphertext& encrypted1,
+                             const PhantomCiphertext& encrypted2) {
+    same_level(encrypted1, encrypted2, "multiply_inplace");
+    if (encrypted1.size() != 2 || encrypted2.size() != 2)
+        throw Error(CBS_ERR_UNSUPPORTED, "multiply_inplace: size-2 ciphertexts");
+    const bool square = &encrypted1 == &encrypted2;
+    encrypted1.resize_keep(3, cudaStream_t{});
+    check(cbs_ckks_multiply_inplace(context.handle(), encrypted1.data(), square ? encrypted1.data() : encrypted2.data(),
+                                    level_limbs(encrypted1), nullptr),
+          "multiply_inplace");
+    encrypted1.SetScalingFactor(encrypted1.GetScalingFactor() * encrypted2.GetScalingFactor());
+}
+// relinearize_inplace (include/evaluate.cuh:125)
+inline void relinearize_inplace(const PhantomContext& context, PhantomCiphertext& encrypted,
+                                const PhantomRelinKey& relin_keys) {
+    if (encrypted.size() != 3) throw Error(CBS_ERR_UNSUPPORTED, "relinearize_inplace: destination_size must be 3");
+    check(cbs_ckks_relinearize_inplace(context.handle(), encrypted.data(), relin_keys.public_keys_ptr(),
+                                       level_limbs(encrypted), nullptr),
+          "relinearize_inplace");
+    encrypted.resize_keep(2, cudaStream_t{});
+}
+// multiply_and_relin_inplace (include/evaluate.cuh:115)
+inline void multiply_and_relin_inplace(const PhantomContext& context, PhantomCiphertext& encrypted1,
+                                       const PhantomCiphertext& encrypted2, const PhantomRelinKey& relin_keys) {
+    multiply_inplace(context, encrypted1, encrypted2);
+    relinearize_inplace(context, encrypted1, relin_keys);
+}
+// rescale_to_next_inplace (include/evaluate.cuh:140): one level down, the scale divided by the
+// dropped prime
+inline void rescale_to_next_inplace(const PhantomContext& context, PhantomCiphertext& encrypted, double q_last) {
+    const size_t next = encrypted.chain_index() + 1;
+    const uint32_t limbs = level_limbs(encrypted);
+    DeviceArray<uint64_t> out(encrypted.size() * (limbs - 1) * context.poly_degree());
+    check(cbs_ckks_rescale_to_next(context.handle(), out.data(), encrypted.data(),
+                                   static_cast<uint32_t>(encrypted.size()), limbs, nullptr),
+          "rescale_to_next");
+    encrypted.reset_level(context, next, std::move(out));
+    encrypted.SetScalingFactor(encrypted.GetScalingFactor() / q_last);
+}
+// mod_switch_to_next_inplace (include/evaluate.cuh:149), CKKS: the last limb dropped
+inline void mod_switch_to_next_inplace(const PhantomContext& context, PhantomCiphertext& encrypted) {
+    const size_t next = encrypted.chain_index() + 1;
+    const uint32_t limbs = level_limbs(encrypted);
+    DeviceArray<uint64_t> out(encrypted.size() * (limbs - 1) * context.poly_degree());
+    check(cbs_ckks_mod_switch_to_next(context.handle(), out.data(), encrypted.data(),
+                                      static_cast<uint32_t>(encrypted.size()), limbs, nullptr),
+          "mod_switch_to_next");
+    encrypted.reset_level(context, next, std::move(out));
+}
+
+// PhantomGaloisKey: one switching key (PhantomRelinKey shape) per Galois element
+class PhantomGaloisKey {
+   public:
+    void insert(uint32_t galois_elt, PhantomRelinKey&& key) { keys_[galois_elt] = std::move(key); }
+    [[nodiscard]] const PhantomRelinKey& get_relin_keys(uint32_t galois_elt) const {
+        auto it = keys_.find(galois_elt);
+        if (it == keys_.end()) throw Error(CBS_ERR_INVALID_ARG, "PhantomGaloisKey: no key for this Galois element");
+        return it->second;
+    }
+
+   private:
+    std::map<uint32_t, PhantomRelinKey> keys_;
+};
+
+// apply_galois_inplace (include/evaluate.cuh:215) and rotate_inplace (:229), CKKS
+inline void apply_galois_inplace(const PhantomContext& context, PhantomCiphertext& encrypted, uint32_t galois_elt,
+                                 const PhantomGaloisKey& galois_keys) {
+    if (encrypted.size() != 2) throw Error(CBS_ERR_UNSUPPORTED, "apply_galois_inplace: encrypted size must be 2");
+    check(cbs_ckks_apply_galois_inplace(context.handle(), encrypted.data(), galois_elt,
+                                        galois_keys.get_relin_keys(galois_elt).public_keys_ptr(),
+                                        level_limbs(encrypted), nullptr),
+          "apply_galois_inplace");
+}
+inline void rotate_inplace(const PhantomContext& context, PhantomCiphertext& encrypted, int step,
+                           const PhantomGaloisKey& galois_keys) {
+    const uint32_t elt = cbs_ckks_galois_elt_from_step(step, static_cast<uint32_t>(context.poly_degree()));
+    if (!elt) throw Error(CBS_ERR_INVALID_ARG, "rotate_inplace: step count too large");
+    apply_galois_inplace(context, encrypted, elt, galois_keys);
 }
 
 // ---- GPUBinFHEContext (bitwise/include/binfhecontext.cuh:8-118): gate bootstrapping on the

@@ -10,6 +10,9 @@
 //         cbs_a, cbs_b -> cbs_out (the batch's RGSW rows)
 //   gate  GPUBinFHEContext::BatchGPUEvalBinGate(NAND): exit status 0 when every gate decrypts to
 //         the truth table
+//   ckks  the CKKS evaluator: multiply_and_relin_inplace then rescale_to_next_inplace of ct1 by
+//         ct2, and rotate_inplace of ct1 by one step: ck_dims (N size_q size_p chain_index beta
+//         galois_elt), ck_chain, ck_ct1, ck_ct2, ck_rk, ck_gk -> ck_mr, ck_rot
 #include <cstdio>
 #include <fstream>
 #include <iostream>
@@ -140,9 +143,48 @@ static int run_gate(const std::string&) {
     return 0;
 }
 
+static int run_ckks(const std::string& dir) {
+    const auto dims = read_raw<uint64_t>(dir + "/ck_dims");
+    const size_t N = dims[0], size_p = dims[2], chain_index = dims[3], beta = dims[4];
+    const uint32_t elt = static_cast<uint32_t>(dims[5]);
+    phantom::EncryptionParameters parms(phantom::scheme_type::ckks);
+    parms.set_poly_modulus_degree(N);
+    parms.set_coeff_modulus(read_raw<uint64_t>(dir + "/ck_chain"));
+    parms.set_special_modulus_size(size_p);
+    PhantomContext context(parms);
+    const cudaStream_t stream = nullptr;
+    auto load_ct = [&](const std::string& name, PhantomCiphertext& ct) {
+        ct.resize(context, chain_index, 2, stream);
+        const auto h = read_raw<uint64_t>(dir + "/" + name);
+        if (h.size() != 2 * ct.coeff_modulus_size() * N) throw std::runtime_error("ciphertext size");
+        check_cuda(cudaMemcpy(ct.data(), h.data(), h.size() * 8, cudaMemcpyHostToDevice), "ct in");
+    };
+    auto save_ct = [&](const std::string& name, const PhantomCiphertext& ct) {
+        std::vector<uint64_t> h(ct.size() * ct.coeff_modulus_size() * N);
+        check_cuda(cudaDeviceSynchronize(), "sync");
+        check_cuda(cudaMemcpy(h.data(), ct.data(), h.size() * 8, cudaMemcpyDeviceToHost), "ct out");
+        write_raw(dir + "/" + name, h);
+    };
+    PhantomCiphertext ct1, ct2, ct3;
+    load_ct("ck_ct1", ct1);
+    load_ct("ck_ct2", ct2);
+    load_ct("ck_ct1", ct3);
+    PhantomRelinKey relin(context, read_raw<uint64_t>(dir + "/ck_rk"), beta);
+    PhantomGaloisKey galois;
+    galois.insert(elt, PhantomRelinKey(context, read_raw<uint64_t>(dir + "/ck_gk"), beta));
+    multiply_and_relin_inplace(context, ct1, ct2, relin);
+    const size_t limbs = ct1.coeff_modulus_size();
+    rescale_to_next_inplace(context, ct1, static_cast<double>(read_raw<uint64_t>(dir + "/ck_chain")[limbs - 1]));
+    if (ct1.chain_index() != chain_index + 1 || ct1.size() != 2) return 5;
+    save_ct("ck_mr", ct1);
+    rotate_inplace(context, ct3, 1, galois);
+    save_ct("ck_rot", ct3);
+    return 0;
+}
+
 int main(int argc, char** argv) {
     if (argc < 3) {
-        std::fprintf(stderr, "usage: %s ks|cbs|gate <dir>\n", argv[0]);
+        std::fprintf(stderr, "usage: %s ks|cbs|gate|ckks <dir>\n", argv[0]);
         return 2;
     }
     try {
@@ -150,6 +192,7 @@ int main(int argc, char** argv) {
         if (mode == "ks") return run_ks(dir);
         if (mode == "cbs") return run_cbs(dir);
         if (mode == "gate") return run_gate(dir);
+        if (mode == "ckks") return run_ckks(dir);
     } catch (const std::exception& e) {
         std::fprintf(stderr, "error: %s\n", e.what());
         return 1;

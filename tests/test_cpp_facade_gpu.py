@@ -6,7 +6,10 @@ and linked against libcbs_b200.so, run on the GPU (tests/cpp/facade_main.cpp):
   gpu_CircuitBootstrappingBatchToDevice on host LWE ciphertexts (cirbts.cuh:454-462), the RGSW
   rows bit-exact against the oracle's circuit bootstrap;
 * GPUBinFHEContext::BatchGPUEvalBinGate(NAND, ...) (binfhecontext.cuh:53-57), every gate
-  decrypting to the truth table."""
+  decrypting to the truth table;
+* the CKKS evaluator (include/evaluate.cuh): multiply_and_relin_inplace + rescale_to_next_inplace
+  and rotate_inplace, bit-exact against the oracle's keyswitch with the restated tensor
+  product, rescale and Galois permutation."""
 from __future__ import annotations
 
 import ctypes
@@ -87,3 +90,51 @@ def test_facade_circuit_bootstrap_host_lwe(facade_bin, tmp_path, pkg, oracle):
 
 def test_facade_batch_gate(facade_bin, tmp_path):
     _run(facade_bin, "gate", tmp_path)
+
+
+def test_facade_ckks_evaluator(facade_bin, tmp_path, oracle):
+    from rns_harness import addmod, mulmod, ntt
+    from test_ckks_gpu import galois_perm, rescale_oracle
+    o = declare_rns(oracle)
+    n, logn, size_q, size_p, chain_index = 1 << 12, 12, 5, 2, 1
+    size_ql = size_q - (chain_index - 1)
+    q, p = rns_primes(o, n, size_q, size_p)
+    chain = np.concatenate([q, p]).astype(np.uint64)
+    beta = -(-size_q // size_p)
+    rng = np.random.default_rng(606)
+    ql = q[:size_ql]
+    colq = ql.reshape(-1, 1)
+
+    def rnd(shape_lead):
+        return np.stack([np.stack([rng.integers(0, int(m), n, dtype=np.uint64) for m in ql])
+                         for _ in range(shape_lead)])
+
+    ct1, ct2 = rnd(2), rnd(2)
+    rk = np.stack([np.stack([np.stack([rng.integers(0, int(m), n, dtype=np.uint64) for m in chain])
+                             for _ in range(2)]) for _ in range(beta)])
+    gk = np.stack([np.stack([np.stack([rng.integers(0, int(m), n, dtype=np.uint64) for m in chain])
+                             for _ in range(2)]) for _ in range(beta)])
+    elt = 5  # rotation by one step
+    np.array([n, size_q, size_p, chain_index, beta, elt], np.uint64).tofile(tmp_path / "ck_dims")
+    chain.tofile(tmp_path / "ck_chain")
+    ct1.tofile(tmp_path / "ck_ct1")
+    ct2.tofile(tmp_path / "ck_ct2")
+    rk.tofile(tmp_path / "ck_rk")
+    gk.tofile(tmp_path / "ck_gk")
+    _run(facade_bin, "ckks", tmp_path)
+    # multiply + relinearize + rescale
+    d0 = mulmod(ct1[0], ct2[0], colq)
+    d1 = addmod(mulmod(ct1[0], ct2[1], colq), mulmod(ct1[1], ct2[0], colq), colq)
+    d2 = mulmod(ct1[1], ct2[1], colq)
+    want = np.ascontiguousarray(np.stack([d0, d1]))
+    o.orc_keyswitch(want, np.ascontiguousarray(d2), np.ascontiguousarray(rk), logn, q, size_ql, size_q, p, size_p)
+    want = rescale_oracle(o, want, ql)
+    got = np.fromfile(tmp_path / "ck_mr", np.uint64).reshape(want.shape)
+    assert np.array_equal(got, want)
+    # rotate by one step
+    perm = galois_perm(elt, logn)
+    want = np.ascontiguousarray(np.stack([ct1[0][:, perm], np.zeros_like(ct1[1])]))
+    o.orc_keyswitch(want, np.ascontiguousarray(ct1[1][:, perm]), np.ascontiguousarray(gk), logn, q, size_ql, size_q,
+                    p, size_p)
+    got = np.fromfile(tmp_path / "ck_rot", np.uint64).reshape(want.shape)
+    assert np.array_equal(got, want)
