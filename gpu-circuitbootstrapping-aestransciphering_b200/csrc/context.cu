@@ -386,6 +386,12 @@ cbs_status upload_host_keys(cbs_context* c) {
                         (c->p.n + 1) * sizeof(uint16_t));
         CBS_CUDA_TRY(c->d_ksk.upload(padded.data(), padded.size(), s));
     }
+    c->ksk_device_only = false;
+    return finish_key_upload(c);
+}
+
+cbs_status finish_key_upload(cbs_context* c) {
+    cudaStream_t s = c->stream;
     CBS_CUDA_TRY(c->d_tv.upload(c->hk.tv.data(), c->hk.tv.size(), s));
     CBS_CUDA_TRY(c->d_gadd.upload(c->hk.gadd.data(), c->hk.gadd.size(), s));
     CBS_CUDA_TRY(c->d_maps.upload(c->hk.maps.data(), c->hk.maps.size(), s));
@@ -762,7 +768,16 @@ cbs_status cbs_export_keys(const cbs_context* ctx, int32_t* s_lwe, int32_t* s_rl
     cp(bsk, k.bsk);
     cp(ht, k.ht);
     cp(ss, k.ss);
-    cp(ksk, k.ksk);
+    if (ksk && ctx->ksk_device_only) {
+        // a device-generated key-switching key lives on the device only: unpad its rows
+        const size_t row = (ctx->p.n + 1) * sizeof(uint16_t), stride = ksk_row_stride(ctx->p.n);
+        CBS_CUDA_TRY(cudaSetDevice(ctx->device));
+        CBS_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        CBS_CUDA_TRY(cudaMemcpy2D(ksk, row, ctx->d_ksk.p, stride * sizeof(uint16_t), row, ctx->d_ksk.n / stride,
+                                  cudaMemcpyDeviceToHost));
+    } else {
+        cp(ksk, k.ksk);
+    }
     cp(tv, k.tv);
     cp(gpow, k.gpow);
     cp(maps, k.maps);

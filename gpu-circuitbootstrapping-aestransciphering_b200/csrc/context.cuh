@@ -94,6 +94,7 @@ struct cbs_context {
     bool mb_ready = false;
     uint64_t key_seed = 0;
     bool device_keyed = false;           // keys drawn on the device (cbs_keygen_device) under keygen_key
+    bool ksk_device_only = false;        // the key-switching key exists only in d_ksk (hk.ksk empty)
     cbs::ChachaKey keygen_key{};
     std::vector<uint64_t> h_mbk;         // grouped keys, NTT domain (kept for export)
     cbs::DevBuf<double2> d_bskf_mb;      // their spectra
@@ -134,6 +135,9 @@ bool tune_cache_lookup(const cbs_context* c, const char* path, cbs_tune_choice* 
 cbs_status apply_tuned_multibit(cbs_context* c);
 // host key copies (c->hk) -> device keys, derived tables; resets the FFT / grouped state
 cbs_status upload_host_keys(cbs_context* c);
+// the derived tables (tv, gadd, maps) of c->hk to the device and the key state reset, after the
+// key material itself is on the device (upload_host_keys or the device keygen)
+cbs_status finish_key_upload(cbs_context* c);
 // the grouped keys of a device-generated key set into c->h_mbk (keygen_device.cu)
 cbs_status device_grouped_keys(cbs_context* c, uint32_t mb);
 // blind rotation + HomTrace/SchemeSwitch of the selected backend: LWE -> RGSW rows in the

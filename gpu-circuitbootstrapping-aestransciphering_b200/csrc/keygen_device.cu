@@ -96,12 +96,15 @@ __global__ void k_keygen_square(const uint64_t* s_ntt, uint64_t* out, uint32_t N
 }
 
 // extraction key switch N -> n, one CTA per LWE sample, block-reduced <a, s> (u16 words, qks <= 2^16)
+// rows written row_stride words apart (the extraction kernel's padded layout, pad words zero)
 __global__ void k_keygen_ksk(ChachaKey k, const int32_t* s_lwe, const int32_t* s_rlwe, uint16_t* ksk, uint32_t n,
-                             uint32_t N, uint32_t base, uint32_t qks, const uint64_t* cdt, uint32_t cdt_len) {
+                             uint32_t N, uint32_t base, uint32_t qks, const uint64_t* cdt, uint32_t cdt_len,
+                             uint32_t row_stride) {
     __shared__ uint32_t part[32];
     const uint32_t t = blockIdx.x;
     const uint32_t v = t % base, i = (t / base) % N, j = t / (base * N);
-    uint16_t* row = ksk + static_cast<size_t>(t) * (n + 1);
+    uint16_t* row = ksk + static_cast<size_t>(t) * row_stride;
+    for (uint32_t c = n + 1 + threadIdx.x; c < row_stride; c += blockDim.x) row[c] = 0;
     uint32_t acc = 0;
     for (uint32_t c = threadIdx.x; c < n; c += blockDim.x) {
         uint32_t blk[6];
@@ -126,6 +129,23 @@ __global__ void k_keygen_ksk(ChachaKey k, const int32_t* s_lwe, const int32_t* s
         const uint32_t m = (v * si * bj) & mask;
         row[n] = static_cast<uint16_t>((sum + m + static_cast<uint32_t>(static_cast<int32_t>(e))) & mask);
     }
+}
+
+// NTT-domain key words to the Montgomery form the exact kernels read: x 2^64 mod Q
+__global__ void k_keygen_to_mont(uint64_t* out, const uint64_t* in, size_t count, uint64_t r, uint64_t rs, uint64_t Q) {
+    for (size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < count;
+         i += static_cast<size_t>(gridDim.x) * blockDim.x)
+        out[i] = mul_shoup(in[i], r, rs, Q);
+}
+
+static cudaError_t to_mont_device(const cbs_context* c, DevBuf<uint64_t>& out, const uint64_t* in, size_t count,
+                                  cudaStream_t s) {
+    cudaError_t e = out.alloc(count);
+    if (e != cudaSuccess) return e;
+    const unsigned blocks = static_cast<unsigned>(std::min<size_t>((count + 255) / 256, 148u * 32u));
+    k_keygen_to_mont<<<blocks ? blocks : 1, 256, 0, s>>>(out.p, in, count, c->mont_r, host::shoup(c->mont_r, c->p.Q),
+                                                         c->p.Q);
+    return cudaGetLastError();
 }
 
 static cudaError_t rlwe_zero_batch(const cbs_context* c, const ChachaKey& k, uint32_t domain, uint32_t count,
@@ -284,6 +304,7 @@ cbs_status cbs_keygen_device(cbs_context* ctx, const uint8_t* rng_key) {
         CBS_CUDA_TRY(cudaGetLastError());
         hk.bsk.resize(bsk_samples * 2 * N);
         CBS_CUDA_TRY(cudaMemcpyAsync(hk.bsk.data(), d_keys.p, hk.bsk.size() * 8, cudaMemcpyDeviceToHost, s));
+        CBS_CUDA_TRY(to_mont_device(c, c->d_bsk, d_keys.p, hk.bsk.size(), s));
         CBS_CUDA_TRY(cudaStreamSynchronize(s));
     }
 
@@ -303,6 +324,7 @@ cbs_status cbs_keygen_device(cbs_context* ctx, const uint8_t* rng_key) {
         CBS_CUDA_TRY(cudaGetLastError());
         hk.ht.resize(static_cast<size_t>(cnt) * 2 * N);
         CBS_CUDA_TRY(cudaMemcpyAsync(hk.ht.data(), d_keys.p, hk.ht.size() * 8, cudaMemcpyDeviceToHost, s));
+        CBS_CUDA_TRY(to_mont_device(c, c->d_ht, d_keys.p, hk.ht.size(), s));
         CBS_CUDA_TRY(cudaStreamSynchronize(s));
     }
 
@@ -321,20 +343,21 @@ cbs_status cbs_keygen_device(cbs_context* ctx, const uint8_t* rng_key) {
         CBS_CUDA_TRY(cudaGetLastError());
         hk.ss.resize(static_cast<size_t>(cnt) * 2 * N);
         CBS_CUDA_TRY(cudaMemcpyAsync(hk.ss.data(), d_keys.p, hk.ss.size() * 8, cudaMemcpyDeviceToHost, s));
+        CBS_CUDA_TRY(to_mont_device(c, c->d_ss, d_keys.p, hk.ss.size(), s));
         CBS_CUDA_TRY(cudaStreamSynchronize(s));
     }
 
     // extraction key switch
     {
         const size_t samples = static_cast<size_t>(2) * N * p.base_ks;
-        DevBuf<uint16_t> d_ksk;
-        CBS_CUDA_TRY(d_ksk.alloc(samples * (n + 1)));
-        k_keygen_ksk<<<static_cast<unsigned>(samples), 128, 0, s>>>(k, d_s_lwe.p, d_s_rlwe.p, d_ksk.p, n, N, p.base_ks,
-                                                                     p.qks, d_cdt_l.p, ll);
+        // written straight into the context's padded device key; exported on demand
+        const uint32_t stride = ksk_row_stride(n);
+        CBS_CUDA_TRY(c->d_ksk.alloc(samples * stride));
+        k_keygen_ksk<<<static_cast<unsigned>(samples), 128, 0, s>>>(k, d_s_lwe.p, d_s_rlwe.p, c->d_ksk.p, n, N,
+                                                                     p.base_ks, p.qks, d_cdt_l.p, ll, stride);
         CBS_CUDA_TRY(cudaGetLastError());
-        hk.ksk.resize(samples * (n + 1));
-        CBS_CUDA_TRY(cudaMemcpyAsync(hk.ksk.data(), d_ksk.p, hk.ksk.size() * 2, cudaMemcpyDeviceToHost, s));
         CBS_CUDA_TRY(cudaStreamSynchronize(s));
+        c->ksk_device_only = true;
     }
     derive_key_tables(p, hk);
     c->keygen_key = k;
@@ -343,7 +366,7 @@ cbs_status cbs_keygen_device(cbs_context* ctx, const uint8_t* rng_key) {
     c->key_seed = 0;
     volatile uint32_t* wipe = k.w;
     for (int i = 0; i < 8; ++i) wipe[i] = 0;
-    return upload_host_keys(c);
+    return finish_key_upload(c);
 }
 
 }  // extern "C"
