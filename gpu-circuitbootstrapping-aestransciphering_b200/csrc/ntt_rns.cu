@@ -280,9 +280,12 @@ __device__ __forceinline__ void inv_pass_d(double (&x)[8], uint32_t m, uint32_t 
     }
 }
 
-template <int LOGS, class TwB, class Load, class Store>
-__device__ __forceinline__ void sub_fwd_d(double* sm, uint32_t gt, const double* __restrict__ tw, const DMod& md,
-                                          TwB twb, Load load, Store store) {
+// sub_fwd_d with two hooks: after_loads() runs after the first CTA barrier (every initial load
+// of every thread has completed), before_store() just before the outputs are stored
+template <int LOGS, class TwB, class Load, class Store, class AfterLoads, class BeforeStore>
+__device__ __forceinline__ void sub_fwd_d_hooked(double* sm, uint32_t gt, const double* __restrict__ tw,
+                                                 const DMod& md, TwB twb, Load load, Store store,
+                                                 AfterLoads after_loads, BeforeStore before_store) {
     using Pl = NttPlan<LOGS>;
     double x[8];
 #pragma unroll
@@ -293,6 +296,7 @@ __device__ __forceinline__ void sub_fwd_d(double* sm, uint32_t gt, const double*
 #pragma unroll
         for (int j = 0; j < 8; ++j) sm[swz(pass_index<LOGS, 3>(1u << (3 * (p - 1)), gt, j))] = x[j];
         __syncthreads();
+        if (p == 1) after_loads();
         const uint32_t m = 1u << (3 * p);
         if (p < Pl::P - 1) {
 #pragma unroll
@@ -305,8 +309,15 @@ __device__ __forceinline__ void sub_fwd_d(double* sm, uint32_t gt, const double*
         }
     }
     constexpr uint32_t mt = 1u << (3 * (Pl::P - 1));
+    before_store();
 #pragma unroll
     for (int j = 0; j < 8; ++j) store(pass_index<LOGS, Pl::tail_r>(mt, gt, j), x[j]);
+}
+
+template <int LOGS, class TwB, class Load, class Store>
+__device__ __forceinline__ void sub_fwd_d(double* sm, uint32_t gt, const double* __restrict__ tw, const DMod& md,
+                                          TwB twb, Load load, Store store) {
+    sub_fwd_d_hooked<LOGS>(sm, gt, tw, md, twb, load, store, []() {}, []() {});
 }
 
 template <int LOGS, class TwB, class Load, class Store>
@@ -571,7 +582,7 @@ __global__ void __launch_bounds__(kGroups * 32) k_rns_fwd_rows_bulk(uint64_t* __
     extern __shared__ __align__(16) uint64_t sm[];
     double* xsm = reinterpret_cast<double*>(sm);               // exchange [kGroups][ROW]
     double* stage = xsm + kGroups * ROW;                       // staging [kGroups][ROW]
-    uint64_t* bar = sm + 2 * kGroups * ROW;
+    uint64_t* bar = sm + (EPI ? 3 : 2) * kGroups * ROW;  // after the staging blocks
     const uint32_t tid = threadIdx.x;
     const uint32_t g = tid / 32, gt = tid % 32;
     const uint32_t rowblk = blockIdx.x % (ROWS / kGroups);
@@ -592,19 +603,48 @@ __global__ void __launch_bounds__(kGroups * 32) k_rns_fwd_rows_bulk(uint64_t* __
             [&](uint32_t e, double v) { myu[e] = dto_residue(v, md); });
         rows_bulk_store(blk, stage);
     } else {
+        // the epilogue's cx block (and for EPI 2 the dst block, into the data stage once every
+        // thread has read its inputs) stream in by bulk copies while the transform runs; the
+        // results go out with one bulk store
         const uint32_t poly = limb_flat / a.limbs, limb = limb_flat % a.limbs;
-        const size_t off = (static_cast<size_t>(limb) << (L1 + kL2)) + static_cast<size_t>(R) * ROW;
-        const uint64_t* cx = a.epi_cx + poly * a.epi_cx_stride + off;
-        uint64_t* dst = a.epi_dst + poly * a.epi_dst_stride + off;
+        const size_t blk_off = (static_cast<size_t>(limb) << (L1 + kL2)) + static_cast<size_t>(rowblk) * kGroups * ROW;
+        const uint64_t* cx_blk = a.epi_cx + poly * a.epi_cx_stride + blk_off;
+        uint64_t* dst_blk = a.epi_dst + poly * a.epi_dst_stride + blk_off;
+        uint64_t* cxs = reinterpret_cast<uint64_t*>(stage + kGroups * ROW);  // [kGroups][ROW]
+        uint64_t* bar2 = bar + 1;
+        constexpr uint32_t bytes = kGroups * ROW * sizeof(uint64_t);
+        if (tid == 0) {
+            mbar_init(bar2, 1);
+            mbar_init_fence();
+            mbar_arrive_expect_tx(bar2, EPI == 2 ? 2 * bytes : bytes);
+            bulk_load(cxs, cx_blk, bytes, bar2);
+        }
         const uint64_t f = a.epi_f[limb], fs = a.epi_fs[limb];
-        sub_fwd_d<kL2>(
+        uint64_t* my_cx = cxs + g * ROW;
+        const uint64_t* my_dst = reinterpret_cast<const uint64_t*>(my);
+        sub_fwd_d_hooked<kL2>(
             xsm + g * ROW, gt, twd, md, [&](uint32_t m) { return m * (ROWS + R); }, [&](uint32_t e) { return my[e]; },
             [&](uint32_t e, double dv) {
                 const uint64_t v = dto_residue(dv, md);
-                uint64_t r = mul_shoup(sub_mod(cx[e], v, q), f, fs, q);
-                if (EPI == 2) r = add_mod(dst[e], r, q);
-                dst[e] = r;
+                uint64_t r = mul_shoup(sub_mod(my_cx[e], v, q), f, fs, q);
+                if (EPI == 2) r = add_mod(my_dst[e], r, q);
+                my_cx[e] = r;
+            },
+            [&]() {
+                if (EPI == 2 && tid == 0) {
+                    fence_proxy_async_smem();  // the data stage was read by the generic proxy
+                    bulk_load(stage, dst_blk, bytes, bar2);
+                }
+            },
+            [&]() {
+                if (!mbar_wait_bounded(bar2, 0, kBulkWaitLimit) && a.fault) atomicOr(a.fault, 1u);
             });
+        fence_proxy_async_smem();
+        __syncthreads();
+        if (tid == 0) {
+            bulk_store(dst_blk, cxs, bytes);
+            bulk_store_commit_and_drain();
+        }
     }
 }
 
@@ -726,8 +766,10 @@ static cudaError_t rns_launch(uint64_t* data, const RnsNttArgs& a, size_t limb_p
         // every prime of the chain is below 2^50: the FP64-pipe form; its row phases move each
         // CTA's 32 KB block with bulk copies when every block address is 16-byte aligned
         const auto a16 = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; };
-        const bool bulk = a16(data) && (a.poly_stride & 1u) == 0 && (!a.in || (a16(a.in) && (a.in_poly_stride & 1u) == 0));
-        constexpr size_t bulk_smem = 2 * row_smem + 16;
+        const bool bulk = a16(data) && (a.poly_stride & 1u) == 0 && (!a.in || (a16(a.in) && (a.in_poly_stride & 1u) == 0)) &&
+                          (a.epi == 0 || (a16(a.epi_cx) && a16(a.epi_dst) && (a.epi_cx_stride & 1u) == 0 &&
+                                          (a.epi_dst_stride & 1u) == 0));
+        constexpr size_t bulk_smem = 2 * row_smem + 16, bulk_epi_smem = 3 * row_smem + 16;
         static std::atomic<uint64_t> bulk_attr{0};
         if (bulk && !(bulk_attr.load() >> dev & 1)) {
             const void* fns[] = {reinterpret_cast<const void*>(k_rns_fwd_rows_bulk<L1, 0>),
@@ -735,8 +777,8 @@ static cudaError_t rns_launch(uint64_t* data, const RnsNttArgs& a, size_t limb_p
                                  reinterpret_cast<const void*>(k_rns_fwd_rows_bulk<L1, 2>),
                                  reinterpret_cast<const void*>(k_rns_inv_rows_bulk<L1>)};
             for (const void* fn : fns) {
-                cudaError_t e =
-                    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bulk_smem));
+                cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                     static_cast<int>(bulk_epi_smem));
                 if (e != cudaSuccess) return e;
             }
             bulk_attr.fetch_or(uint64_t(1) << dev);
@@ -745,8 +787,8 @@ static cudaError_t rns_launch(uint64_t* data, const RnsNttArgs& a, size_t limb_p
             k_rns_fwd_cols<L1, true><<<cb, col_threads, col_smem, s>>>(data, a);
             if (bulk) {
                 if (a.epi == 0) k_rns_fwd_rows_bulk<L1, 0><<<rb, row_threads, bulk_smem, s>>>(data, a);
-                else if (a.epi == 1) k_rns_fwd_rows_bulk<L1, 1><<<rb, row_threads, bulk_smem, s>>>(data, a);
-                else k_rns_fwd_rows_bulk<L1, 2><<<rb, row_threads, bulk_smem, s>>>(data, a);
+                else if (a.epi == 1) k_rns_fwd_rows_bulk<L1, 1><<<rb, row_threads, bulk_epi_smem, s>>>(data, a);
+                else k_rns_fwd_rows_bulk<L1, 2><<<rb, row_threads, bulk_epi_smem, s>>>(data, a);
             } else if (a.epi == 0) k_rns_fwd_rows<L1, 0, true><<<rb, row_threads, row_smem, s>>>(data, a);
             else if (a.epi == 1) k_rns_fwd_rows<L1, 1, true><<<rb, row_threads, row_smem, s>>>(data, a);
             else k_rns_fwd_rows<L1, 2, true><<<rb, row_threads, row_smem, s>>>(data, a);
