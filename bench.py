@@ -821,12 +821,17 @@ def run_tcb(args, rank: int, world: int, local_rank: int) -> None:
     ctx.close()
 
 
+def mb_keys(mb: int) -> int:
+    """Grouped keys per group: 2^mb - 1 subsets, 8 for the staged mb = 4 (3 + 1)."""
+    return 8 if mb == 4 else (1 << mb) - 1
+
+
 def br_key_bytes(p, mb: int) -> int:
     """Blind-rotation key bytes one launch reads (once, shared through L2): n RGSWs, or
-    ceil(n/mb) groups of 2^mb - 1 RGSWs; FFT spectra and NTT words are both 8 bytes per
+    ceil(n/mb) groups of mb_keys(mb) RGSWs; FFT spectra and NTT words are both 8 bytes per
     coefficient."""
     rgsw = 2 * p.digits_g * 2 * p.N * 8
-    return (-(-p.n // mb)) * ((1 << mb) - 1) * rgsw
+    return (-(-p.n // mb)) * mb_keys(mb) * rgsw
 
 
 # DRAM bytes (read + write) of one blind-rotation launch, measured with ncu
@@ -943,10 +948,14 @@ def fp64_flop_per_launch(p, T: int, mb: int) -> int:
     """Algorithmic FP64 flops of one FFT blind-rotation launch over T ciphertexts: per step (mb = 1)
     or group, 2 digits_g forward and 2 inverse M-point complex transforms (5 M log2 M each), and
     per spectrum slot and key row 8 flops per complex multiply-add with the 2^mb - 1 combined keys
-    plus the product with the digit spectrum (mb > 1)."""
+    plus the product with the digit spectrum (mb > 1).  The staged mb = 4 runs per group an mb = 3
+    step and a one-bit step (the latter skipped for a group without a fourth coefficient)."""
     N, n, l2 = p.N, p.n, 2 * p.digits_g
     M = N // 2
     fft_flop = 5 * M * (M.bit_length() - 1)
+    if mb == 4:
+        return T * (
+            (-(-n // 4)) * ((l2 + 2) * fft_flop + 2 * l2 * M * 8 * 8) + (n // 4) * ((l2 + 2) * fft_flop + 2 * l2 * M * 8))
     steps = -(-n // mb)
     keys = (1 << mb) - 1
     return T * steps * ((l2 + 2) * fft_flop + 2 * l2 * M * 8 * (keys + (1 if mb > 1 else 0)))
@@ -1071,9 +1080,9 @@ def main() -> None:
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--backend", choices=["fft64", "ntt"], default="fft64")
-    ap.add_argument("--multibit", type=int, choices=[1, 2, 3], default=None,
-                    help="blind rotation over groups of 1, 2 or 3 LWE coefficients (fft64 backend; "
-                         "default 2 for fft64, 1 for ntt)")
+    ap.add_argument("--multibit", type=int, choices=[1, 2, 3, 4], default=None,
+                    help="blind rotation over groups of 1, 2, 3 or 4 (staged 3 + 1) LWE coefficients "
+                         "(fft64 backend; default 2 for fft64, 1 for ntt)")
     ap.add_argument("--fft-mode", dest="fft_mode", choices=["fp64", "fp32-split", "fp32"], default="fp64",
                     help="external-product arithmetic of --workload gate / ragged (torus-32): exact FP64, "
                          "split FP32 (24/25-bit + exact top key limb), or FP32 on whole keys; FP32 modes use "

@@ -237,7 +237,8 @@ def preset_params(name: str) -> CbsParams:
 
 
 def generate_mb_bsk_host(params: CbsParams, seed: int, mb: int):
-    """Grouped blind-rotation keys [ceil(n/mb)][2^mb - 1][2*digits_g][2][N] (NTT domain) of the
+    """Grouped blind-rotation keys [ceil(n/mb)][keys][2*digits_g][2][N] (NTT domain; keys = 3, 7, 8
+    for mb = 2, 3, 4) of the
     key set cbs_keygen(seed) makes, generated on the host."""
     import numpy as np
     words = ctypes.c_size_t()
@@ -333,7 +334,8 @@ class Context:
         return c.as_dict() if load().cbs_context_tuned(self._h, ctypes.byref(c)) == 0 else None
 
     def set_br_multibit(self, mb: int) -> None:
-        """Blind rotation over groups of mb = 1, 2 or 3 LWE coefficients (FFT backend)."""
+        """Blind rotation over groups of mb = 1, 2, 3 or 4 LWE coefficients (FFT backend; mb = 4 is
+        the staged grouping: an mb = 3 step, then a one-bit step)."""
         call("cbs_context_set_br_multibit", self._h, mb)
 
     def set_br_schedule(self, schedule: int) -> None:
@@ -341,7 +343,8 @@ class Context:
         call("cbs_context_set_br_schedule", self._h, schedule)
 
     def export_mb_bsk(self):
-        """Grouped blind-rotation keys [ceil(n/mb)][2^mb - 1][2*digits_g][2][N] (NTT domain)."""
+        """Grouped blind-rotation keys [ceil(n/mb)][keys][2*digits_g][2][N] (NTT domain; keys = 3, 7,
+        8 for mb = 2, 3, 4)."""
         import numpy as np
         words = ctypes.c_size_t()
         call("cbs_export_mb_bsk", self._h, None, ctypes.byref(words))

@@ -14,6 +14,7 @@
 #include <cmath>
 #include <complex>
 #include <thread>
+#include <type_traits>
 #include <vector>
 
 #include "cbs_kernels.cuh"
@@ -233,8 +234,11 @@ __global__ void __launch_bounds__(BrFftCfg<LOGN>::T, BrFftCfg<LOGN>::MIN_BLOCKS)
 // the digit split, the 6 forward and 2 inverse transforms run once per group instead of
 // once per coefficient, and the rotation needs no separate pass.  c_i(psi_s) comes from one
 // twist-table lookup per group (zeta^(a_i e_t)) times an 8th root of unity per slot.
-// Keys: [groups][2^MB - 1][2*digits][2][N/2] spectra, subsets in the order {0} {1} {2}
-// {0,1} {0,2} {1,2} {0,1,2} (MB = 3) or {0} {1} {0,1} (MB = 2).
+// Keys: [groups][keys][2*digits][2][N/2] spectra, subsets in the order {0} {1} {2}
+// {0,1} {0,2} {1,2} {0,1,2} (MB = 3) or {0} {1} {0,1} (MB = 2).  MB = 4 is the reference's
+// staged grouping (cirbts-init.cu:536-565 keys, cirbts-batch.cu:2767-2923 sequence): 8 keys
+// {0} {1} {2} {3} {0,1} {0,2} {1,2} {0,1,2} per group of 4, applied as the MB = 3 step of
+// coefficients 0-2 and then a one-bit step of coefficient 3 on a fresh digit split.
 template <int MB>
 __device__ __forceinline__ double2 mb_combined_key(const double2* kp, size_t kstride, const double2 (&c)[MB]) {
     if constexpr (MB == 2) {
@@ -274,7 +278,7 @@ __global__ void __launch_bounds__(BrFftCfg<LOGN>::T, BrFftMbCfg<LOGN, MB>::MIN_B
     k_blind_rotate_fft_mb(const BlindRotateArgs a, const FftKeyArgs f) {
     constexpr int LOGM = LOGN - 1;
     constexpr uint32_t N = 1u << LOGN, M = N / 2, TH = M / 8, T = 2 * TH, TWO_N = 2 * N;
-    constexpr uint32_t KS = (1u << MB) - 1u;
+    constexpr uint32_t KS = mb_group_keys(MB);
     using Tb = FftTab<LOGM>;
     using DigT = typename DigitPair<WIDE>::T;
     extern __shared__ __align__(16) uint64_t smem[];
@@ -282,7 +286,7 @@ __global__ void __launch_bounds__(BrFftCfg<LOGN>::T, BrFftMbCfg<LOGN, MB>::MIN_B
     double2* fs = reinterpret_cast<double2*>(smem + 2 * N);         // [2][M]
     double2* tab = fs + 2 * M;                                      // FftTab<LOGM>
     DigT* dig = reinterpret_cast<DigT*>(tab + Tb::size());          // [2][digits][M] digit pairs
-    double2* cbuf = reinterpret_cast<double2*>(dig + 2 * a.digits * M);  // [MB][8][T] c_i per slot
+    double2* cbuf = reinterpret_cast<double2*>(dig + 2 * a.digits * M);  // [step coefs][8][T] c_i per slot
     const double2* tws = tab + Tb::twist_off();
     const uint32_t ct = blockIdx.x, tid = threadIdx.x;
     const uint32_t h = tid / TH, ht = tid % TH;
@@ -323,14 +327,18 @@ __global__ void __launch_bounds__(BrFftCfg<LOGN>::T, BrFftMbCfg<LOGN, MB>::MIN_B
     const uint64_t* arow = a.a + static_cast<size_t>(ct) * a.a_stride;
     const uint32_t groups = (a.n + MB - 1) / MB;
     const size_t kstride = static_cast<size_t>(l2) * 2 * M;  // spectra between subsets of a group
-    for (uint32_t g = 0; g < groups; ++g) {
-        // zeta^(a_i e_t) per coefficient of the group (a_i = 0 past n: c_i = 0)
+    // one step: SMB coefficients idx0 .. idx0 + SMB - 1 against the group's keys slot(s) for
+    // the subsets s of mb_key_mask(SMB, s)
+    auto step = [&](auto smb_tag, uint32_t idx0, const double2* gkey, auto slot) {
+        constexpr int SMB = decltype(smb_tag)::value;
+        constexpr uint32_t SKS = (1u << SMB) - 1u;
+        // zeta^(a_i e_t) per coefficient of the step (a_i = 0 past n: c_i = 0)
         // c_i(psi_s) = zeta^(a_i e_t) omega8^((a_i rev3(j)) mod 8) - 1 for the thread's 8 slots,
-        // kept in shared memory for the group (thread-private entries: no barrier); omega8^k is
+        // kept in shared memory for the step (thread-private entries: no barrier); omega8^k is
         // +-tw[(k mod 4) M/8] of the first-pass table
 #pragma unroll
-        for (int i = 0; i < MB; ++i) {
-            const uint32_t idx = g * MB + i;
+        for (int i = 0; i < SMB; ++i) {
+            const uint32_t idx = idx0 + i;
             const uint32_t at = idx < a.n ? special_ms_f(__ldg(arow + idx), TWO_N, a.q_lwe, a.bitwidth) : 0u;
             const double2 ub = zeta_pow<LOGN>(tws, mult_base<LOGN>(ht, at));
 #pragma unroll
@@ -355,7 +363,7 @@ __global__ void __launch_bounds__(BrFftCfg<LOGN>::T, BrFftMbCfg<LOGN, MB>::MIN_B
         }
         half_bar();
         // 2. forward transforms; per slot the combined key of row 2d + h, both columns
-        const double2* gk = f.bskf + static_cast<size_t>(g) * KS * kstride + ht;
+        const double2* gk = gkey + ht;
         double2 y0[8], y1[8];
 #pragma unroll
         for (int j = 0; j < 8; ++j) y0[j] = y1[j] = make_double2(0.0, 0.0);
@@ -373,20 +381,21 @@ __global__ void __launch_bounds__(BrFftCfg<LOGN>::T, BrFftMbCfg<LOGN, MB>::MIN_B
             const double2* k0 = gk + static_cast<size_t>(2 * d + h) * 2 * M;
             double2 kc0[8], kc1[8];
 #pragma unroll
-            for (int s = 0; s < static_cast<int>(KS); ++s) {
+            for (int s = 0; s < static_cast<int>(SKS); ++s) {
                 double2 ka[8], kb[8];
+                const double2* ks = k0 + static_cast<size_t>(slot(s)) * kstride;
 #pragma unroll
                 for (int j = 0; j < 8; ++j) {
-                    ka[j] = __ldg(k0 + s * kstride + j * TH);
-                    kb[j] = __ldg(k0 + s * kstride + M + j * TH);
+                    ka[j] = __ldg(ks + j * TH);
+                    kb[j] = __ldg(ks + M + j * TH);
                 }
-                const uint32_t mask = mb_key_mask(MB, s);
+                const uint32_t mask = mb_key_mask(SMB, s);
 #pragma unroll
                 for (int j = 0; j < 8; ++j) {
                     double2 m = make_double2(1.0, 0.0);
                     bool first = true;
 #pragma unroll
-                    for (int i = 0; i < MB; ++i)
+                    for (int i = 0; i < SMB; ++i)
                         if (mask & (1u << i)) {
                             const double2 c = cbuf[(i * 8 + j) * T + tid];
                             m = first ? c : cmul(m, c);
@@ -430,6 +439,17 @@ __global__ void __launch_bounds__(BrFftCfg<LOGN>::T, BrFftMbCfg<LOGN, MB>::MIN_B
                 my_acc[e + M] = offset_add(my_acc[e + M], centred_residue(u.y * f.inv_m, f), lo_b, hi_b, Qs);
             },
             half_bar);
+    };
+    for (uint32_t g = 0; g < groups; ++g) {
+        const double2* gk = f.bskf + static_cast<size_t>(g) * KS * kstride;
+        if constexpr (MB == 4) {
+            // the staged grouping: the mb = 3 step of coefficients 0-2 (keys 0 1 2 4 5 6 7), then a
+            // one-bit step of coefficient 3 (key 3) on the updated accumulator
+            step(std::integral_constant<int, 3>{}, 4 * g, gk, [](int s) { return s < 3 ? s : s + 1; });
+            if (4 * g + 3 < a.n) step(std::integral_constant<int, 1>{}, 4 * g + 3, gk, [](int) { return 3; });
+        } else {
+            step(std::integral_constant<int, MB>{}, g * MB, gk, [](int s) { return s; });
+        }
     }
     __syncthreads();
 
@@ -950,7 +970,7 @@ static cudaError_t br_fft_mb_launch(const BlindRotateArgs& a, const FftKeyArgs& 
     constexpr uint32_t N = 1u << LOGN, M = N / 2;
     const size_t smem = 2ull * N * sizeof(uint64_t) + (2ull * M + FftTab<LOGN - 1>::size()) * sizeof(double2) +
                         2ull * a.digits * M * sizeof(typename DigitPair<WIDE>::T) +
-                        MB * 8ull * BrFftCfg<LOGN>::T * sizeof(double2);
+                        mb_step_coefs(MB) * 8ull * BrFftCfg<LOGN>::T * sizeof(double2);
     if (f.tab_len != FftTab<LOGN - 1>::size()) return cudaErrorInvalidValue;
     static size_t configured[64] = {};
     int dev = 0;
@@ -1027,15 +1047,17 @@ static cudaError_t br_fft_mb_launch(const BlindRotateArgs& a, const FftKeyArgs& 
 cudaError_t launch_blind_rotate_fft_mb(const BlindRotateArgs& a, const FftKeyArgs& f, const cbs_dmodulus* d_mod,
                                        uint32_t N, uint32_t batch, uint32_t mb, cudaStream_t s, bool mv_ntt) {
     if (batch == 0) return cudaSuccess;
-    if (mb != 2 && mb != 3) return cudaErrorInvalidValue;  // N = 4096: the per-slot c_i exceed shared memory
+    if (mb < 2 || mb > 4) return cudaErrorInvalidValue;  // N = 4096: the per-slot c_i exceed shared memory
     if (a.g.gbits < 1 || a.g.gbits > 24 || a.digits < 1 || a.digits > 4) return cudaErrorInvalidValue;
     cudaError_t e;
     switch (N) {
         case 1024:
-            e = mb == 2 ? br_fft_mb_launch<10, 2>(a, f, batch, s) : br_fft_mb_launch<10, 3>(a, f, batch, s);
+            e = mb == 2 ? br_fft_mb_launch<10, 2>(a, f, batch, s)
+                        : (mb == 3 ? br_fft_mb_launch<10, 3>(a, f, batch, s) : br_fft_mb_launch<10, 4>(a, f, batch, s));
             break;
         case 2048:
-            e = mb == 2 ? br_fft_mb_launch<11, 2>(a, f, batch, s) : br_fft_mb_launch<11, 3>(a, f, batch, s);
+            e = mb == 2 ? br_fft_mb_launch<11, 2>(a, f, batch, s)
+                        : (mb == 3 ? br_fft_mb_launch<11, 3>(a, f, batch, s) : br_fft_mb_launch<11, 4>(a, f, batch, s));
             break;
         default: return cudaErrorInvalidValue;
     }

@@ -589,7 +589,7 @@ cbs_status cbs_import_keys(cbs_context* ctx, const int32_t* s_lwe, const int32_t
 
 cbs_status cbs_import_mb_bsk(cbs_context* ctx, uint32_t mb, const uint64_t* keys, size_t words) {
     CBS_CHECK_ARG(ctx && keys, "import_mb_bsk: null argument");
-    CBS_CHECK_ARG(mb == 2 || mb == 3, "import_mb_bsk: mb must be 2 or 3");
+    CBS_CHECK_ARG(mb >= 2 && mb <= 4, "import_mb_bsk: mb must be 2, 3 or 4");
     ctx->mb_explicit = true;
     if (ctx->br_backend != CBS_BR_FFT64) {
         set_error("import_mb_bsk: grouped blind rotation is implemented for the FFT64 backend");
@@ -602,7 +602,7 @@ cbs_status cbs_import_mb_bsk(cbs_context* ctx, uint32_t mb, const uint64_t* keys
     const cbs_params& p = ctx->p;
     const size_t want = static_cast<size_t>((p.n + mb - 1) / mb) * mb_subsets(mb) * 2 * p.digits_g * 2 * p.N;
     if (words != want) {
-        set_error("import_mb_bsk: words must be ceil(n/mb) * (2^mb - 1) * 2 digits_g * 2 N");
+        set_error("import_mb_bsk: words must be ceil(n/mb) * keys(mb) * 2 digits_g * 2 N (keys 3, 7, 8)");
         return CBS_ERR_SHAPE_MISMATCH;
     }
     for (size_t i = 0; i < words; ++i) CBS_CHECK_ARG(keys[i] < p.Q, "import_mb_bsk: key words must be residues mod Q");
@@ -638,7 +638,7 @@ cbs_status cbs_context_tuned(const cbs_context* ctx, cbs_tune_choice* out) {
 
 cbs_status cbs_context_set_br_multibit(cbs_context* ctx, uint32_t mb) {
     CBS_CHECK_ARG(ctx, "set_br_multibit: null context");
-    CBS_CHECK_ARG(mb >= 1 && mb <= 3, "set_br_multibit: mb must be 1, 2 or 3");
+    CBS_CHECK_ARG(mb >= 1 && mb <= 4, "set_br_multibit: mb must be 1, 2, 3 or 4");
     ctx->mb_explicit = true;
     if (mb > 1 && ctx->br_backend != CBS_BR_FFT64) {
         set_error("set_br_multibit: grouped blind rotation is implemented for the FFT64 backend");
@@ -696,7 +696,7 @@ cbs_status cbs_context_set_br_backend(cbs_context* ctx, int backend) {
 cbs_status cbs_generate_mb_bsk_host(const cbs_params* params, uint64_t seed, uint32_t mb, uint64_t* out,
                                     size_t* words) {
     CBS_CHECK_ARG(params && words, "generate_mb_bsk_host: null argument");
-    CBS_CHECK_ARG(mb == 2 || mb == 3, "generate_mb_bsk_host: mb must be 2 or 3");
+    CBS_CHECK_ARG(mb >= 2 && mb <= 4, "generate_mb_bsk_host: mb must be 2, 3 or 4");
     if (cbs_status st = validate(*params)) return st;
     const size_t need = static_cast<size_t>((params->n + mb - 1) / mb) * mb_subsets(mb) * 2 * params->digits_g * 2 *
                         params->N;

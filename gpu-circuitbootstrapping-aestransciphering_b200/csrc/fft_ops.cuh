@@ -9,11 +9,19 @@
 namespace cbs {
 
 // bit mask of the LWE coefficients in grouped key kk of a group of mb (the subset order of the
-// grouped keys: mb = 2: {0} {1} {0,1}; mb = 3: {0} {1} {2} {0,1} {0,2} {1,2} {0,1,2})
+// grouped keys: mb = 2: {0} {1} {0,1}; mb = 3: {0} {1} {2} {0,1} {0,2} {1,2} {0,1,2}; mb = 4,
+// the staged grouping: {0} {1} {2} {3} {0,1} {0,2} {1,2} {0,1,2})
 __host__ __device__ constexpr uint32_t mb_key_mask(int mb, uint32_t kk) {
     if (mb == 2) return kk == 0 ? 1u : (kk == 1 ? 2u : 3u);
+    if (mb == 4) return kk < 4 ? (1u << kk) : (kk == 4 ? 3u : (kk == 5 ? 5u : (kk == 6 ? 6u : 7u)));
     return kk < 3 ? (1u << kk) : (kk == 3 ? 3u : (kk == 4 ? 5u : (kk == 5 ? 6u : 7u)));
 }
+
+// grouped keys per group of mb coefficients: 2^mb - 1 subsets (mb = 2, 3); 8 for the staged mb = 4
+__host__ __device__ constexpr uint32_t mb_group_keys(int mb) { return mb == 4 ? 8u : (1u << mb) - 1u; }
+
+// LWE coefficients per step of a group (the staged mb = 4 runs steps of 3 and 1)
+__host__ __device__ constexpr int mb_step_coefs(int mb) { return mb == 4 ? 3 : mb; }
 
 // v mod Q, v the FP64 value of an integer-valued product (|v| < 2^90), computed in FP64:
 // k = rint(v / Q), r = v - k*q_hi - k*q_lo with two fused multiply-adds.  The two roundings of

@@ -144,16 +144,20 @@ void rlwe_encrypt(const cbs_params& p, const host::NttTables& t, const HostKeys&
     for (uint32_t i = 0; i < p.N; ++i) out_b[i] = fm.add(out_b[i], m[i]);
 }
 
-uint32_t mb_subsets(uint32_t mb) { return (1u << mb) - 1u; }
+uint32_t mb_subsets(uint32_t mb) { return mb == 4 ? 8u : (1u << mb) - 1u; }
 
 uint32_t mb_subset_mask(uint32_t mb, uint32_t idx) {
     // subsets of {0..mb-1} ordered by size, then lexicographically: for mb = 3,
     // {0} {1} {2} {0,1} {0,2} {1,2} {0,1,2} (the reference's k0 k1 k2 k01 k02 k12 k012,
-    // cirbts-init.cu:499-530); for mb = 2, {0} {1} {0,1} (k0 k1 k01, :485-498)
+    // cirbts-init.cu:499-530); for mb = 2, {0} {1} {0,1} (k0 k1 k01, :485-498).  mb = 4 is the
+    // reference's staged grouping (:536-565): k0 k1 k2 k3 k01 k02 k12 k012, the mb = 3 keys of
+    // coefficients 0-2 and the one-bit key of coefficient 3.
     static const uint32_t order2[3] = {0b01, 0b10, 0b11};
     static const uint32_t order3[7] = {0b001, 0b010, 0b100, 0b011, 0b101, 0b110, 0b111};
+    static const uint32_t order4[8] = {0b0001, 0b0010, 0b0100, 0b1000, 0b0011, 0b0101, 0b0110, 0b0111};
     if (mb == 1) return 1u;
     if (mb == 2) return order2[idx];
+    if (mb == 4) return order4[idx];
     return order3[idx];
 }
 

@@ -61,10 +61,11 @@ void set_secrets(const cbs_params& p, const host::NttTables& t, const int32_t* s
 // RLWE encryption of a coefficient-domain message (mod Q) into NTT-domain (a, b)
 void rlwe_encrypt(const cbs_params& p, const host::NttTables& t, const HostKeys& k, Rng& rng,
                   const std::vector<uint64_t>& msg_coef, uint64_t* out_a_ntt, uint64_t* out_b_ntt);
-// Multi-bit blind-rotation keys (the reference's CIRBTS_PBS_MULTIBIT = 2 / 3 grouping,
-// bitwise/src/cirbts/cirbts-init.cu:376-530): LWE coefficients in groups of mb, and for every
-// non-empty subset S of a group an RGSW of prod_{i in S} s_i (0 for indices >= n), in the
-// order of mb_subset_mask: out [ceil(n/mb)][2^mb - 1][2*digits_g][2][N], NTT domain.
+// Multi-bit blind-rotation keys (the reference's CIRBTS_PBS_MULTIBIT = 2 / 3 / 4 grouping,
+// bitwise/src/cirbts/cirbts-init.cu:376-565): LWE coefficients in groups of mb, and for every
+// key subset S of a group (mb = 2, 3: every non-empty subset; mb = 4: the seven of
+// coefficients 0-2 and {3}) an RGSW of prod_{i in S} s_i (0 for indices >= n), in the order of
+// mb_subset_mask: out [ceil(n/mb)][mb_subsets(mb)][2*digits_g][2][N], NTT domain.
 uint32_t mb_subsets(uint32_t mb);
 uint32_t mb_subset_mask(uint32_t mb, uint32_t idx);
 void generate_mb_bsk(const cbs_params& p, const host::NttTables& t, const HostKeys& k, uint32_t mb, uint64_t seed,

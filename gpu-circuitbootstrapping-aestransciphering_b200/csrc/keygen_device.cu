@@ -16,7 +16,7 @@
 //   domain 7  extraction KSK, sample ((j N + i) base_ks + v): a[c] = floor(qks x / 2^128) from
 //             ChaCha20(c, (t, 7)), noise from ChaCha20(n, (t, 7)) words 4-5, b = <a, s> +
 //             v s'_i base_ks^j + e mod qks
-//   domain 8 / 9  grouped keys for mb = 2 / 3, sample (group * (2^mb - 1) + subset) * 2 digits
+//   domain 8 / 9 / 10  grouped keys for mb = 2 / 3 / 4, sample (group * keys + subset) * 2 digits
 //             + row: RLWE(0), g_j added as for the BSK when prod_{i in subset} s_i = 1
 // RLWE(0) samples are those of the AES-material encryption (encrypt.cu): NTT-domain mask from
 // words 0-3, discrete-Gaussian noise from words 4-5, b = a s + NTT(e).
@@ -195,9 +195,9 @@ static bool os_random_key(ChachaKey& k) {
     return true;
 }
 
-// the grouped keys of the device-generated key set (domain 8 / 9) into c->h_mbk
+// the grouped keys of the device-generated key set (domain 8 / 9 / 10) into c->h_mbk
 cbs_status device_grouped_keys(cbs_context* c, uint32_t mb) {
-    const uint32_t N = c->p.N, n = c->p.n, l2 = 2 * c->p.digits_g, K = (1u << mb) - 1u, groups = (n + mb - 1) / mb;
+    const uint32_t N = c->p.N, n = c->p.n, l2 = 2 * c->p.digits_g, K = mb_subsets(mb), groups = (n + mb - 1) / mb;
     cudaStream_t s = c->stream;
     const auto cdt_r = cdt_table(c->p.sigma_rlwe);
     DevBuf<uint64_t> d_cdt, d_s_ntt, d_g, d_keys, d_tmp;
@@ -222,7 +222,7 @@ cbs_status device_grouped_keys(cbs_context* c, uint32_t mb) {
     const size_t samples = bits.size() * l2;
     CBS_CUDA_TRY(d_keys.alloc(samples * 2 * N));
     CBS_CUDA_TRY(d_tmp.alloc(samples * N));
-    CBS_CUDA_TRY(rlwe_zero_batch(c, c->keygen_key, mb == 2 ? 8u : 9u, static_cast<uint32_t>(samples), d_keys.p,
+    CBS_CUDA_TRY(rlwe_zero_batch(c, c->keygen_key, mb == 2 ? 8u : (mb == 3 ? 9u : 10u), static_cast<uint32_t>(samples), d_keys.p,
                                  d_tmp.p, d_s_ntt.p, d_cdt, static_cast<uint32_t>(cdt_r.size()), s));
     const size_t work = samples * N;
     k_keygen_rgsw_message<<<static_cast<unsigned>((work + 255) / 256), 256, 0, s>>>(

@@ -1,7 +1,8 @@
 // tune.cu -- autotuner of the blind rotation and its on-disk cache.
 //
 // The blind rotation has two launch-form knobs on the FFT64 backend: the grouping mb (1, 2 or 3
-// LWE coefficients per step, with 2^mb - 1 grouped keys) and, for a two-digit gadget with mb = 2,
+// LWE coefficients per step, with 2^mb - 1 grouped keys, or the staged 4 = 3 + 1 with 8 keys)
+// and, for a two-digit gadget with mb = 2,
 // the schedule (the two digit transforms one after the other, in lockstep, or in lockstep with
 // two ciphertexts per CTA at N = 2048).  The tuner times
 // every candidate on a synthetic batch with CUDA events and keeps the fastest; the choice is
@@ -101,7 +102,7 @@ static std::vector<CacheEntry> read_cache(const std::string& file) {
             continue;
         field_num(line, "batch", &batch);
         field_num(line, "candidates", &cand);
-        if (mb < 1 || mb > 3 || sch < 0 || sch > CBS_BR_SCHEDULE_PAIRED) continue;
+        if (mb < 1 || mb > 4 || sch < 0 || sch > CBS_BR_SCHEDULE_PAIRED) continue;
         e.bucket = static_cast<uint32_t>(bucket);
         e.choice.mb = static_cast<uint32_t>(mb);
         e.choice.schedule = static_cast<uint32_t>(sch);
@@ -206,7 +207,7 @@ cbs_status cbs_autotune_blind_rotation(cbs_context* ctx, uint32_t batch, const c
     // candidates: every grouping the context can form keys for, and both schedules where they differ
     const uint32_t keep_mb = c->br_mb, keep_schedule = c->br_schedule;
     std::vector<uint32_t> mbs;
-    if (c->has_secret) mbs = {1, 2, 3};
+    if (c->has_secret) mbs = {1, 2, 3, 4};
     else mbs = {keep_mb};
     cbs_tune_choice best{};
     best.us_per_bootstrap = 1e300;

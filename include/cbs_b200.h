@@ -149,7 +149,7 @@ cbs_status cbs_keygen(cbs_context *ctx, uint64_t seed);
  * in host loops, bitwise/src/cirbts/cirbts-init.cu:367-864).  Every word comes from ChaCha20
  * (RFC 8439) under rng_key[32], one block per coefficient addressed by (counter, sample,
  * domain): secrets (domain 3), bootstrapping key (4), HomTrace keys (5), SchemeSwitch key (6),
- * extraction key-switching key (7), grouped keys when mb > 1 is selected (8 / 9); RLWE masks
+ * extraction key-switching key (7), grouped keys when mb > 1 is selected (8 / 9 / 10); RLWE masks
  * in the NTT domain from words 0-3, noise from the discrete-Gaussian table of
  * cbs_cdt_table_host with words 4-5.  The same secrecy rules as cbs_aes128_setup_device apply:
  * rng_key decides the secret key, so it must come from a CSPRNG, stay secret and never be
@@ -166,13 +166,16 @@ enum { CBS_BR_NTT = 0, CBS_BR_FFT64 = 1 };
 cbs_status cbs_context_set_br_backend(cbs_context *ctx, int backend);
 
 /* Multi-bit blind rotation (the reference's CIRBTS_PBS_MULTIBIT grouping,
- * bitwise/src/cirbts/cirbts-init.cu:376-530 and the MB3 MAC kernel.cu:4585-4771): mb = 1
+ * bitwise/src/cirbts/cirbts-init.cu:376-565 and the MB3 MAC kernel.cu:4585-4771): mb = 1
  * processes one LWE coefficient per step (default); mb = 2 or 3 groups mb coefficients and
  * adds sum_S prod_{i in S}(X^{a_i} - 1) * (acc (x) RGSW(prod_{i in S} s_i)) over the
- * non-empty subsets S, so the accumulator is decomposed and transformed once per group.  The
- * grouped keys are generated from the context's secrets (2^mb - 1 RGSWs per group) when keys
- * exist or are next generated.  mb > 1 needs the FFT64 backend (CBS_ERR_UNSUPPORTED
- * otherwise); selecting the NTT backend resets mb to 1. */
+ * non-empty subsets S, so the accumulator is decomposed and transformed once per group.
+ * mb = 4 is the reference's staged grouping (cirbts-batch.cu:2767-2923): groups of 4 with 8
+ * keys ({0} {1} {2} {3} {0,1} {0,2} {1,2} {0,1,2}), applied as the mb = 3 step of coefficients
+ * 0-2 and then a one-bit step of coefficient 3 on a fresh decomposition.  The grouped keys are
+ * generated from the context's secrets (3, 7 or 8 RGSWs per group) when keys exist or are next
+ * generated.  mb > 1 needs the FFT64 backend (CBS_ERR_UNSUPPORTED otherwise); selecting the
+ * NTT backend resets mb to 1. */
 cbs_status cbs_context_set_br_multibit(cbs_context *ctx, uint32_t mb);
 /* Schedule of the grouped FFT blind rotation with a two-digit gadget: CBS_BR_SCHEDULE_LOCKSTEP
  * transforms both digits of a polynomial together (interleaved butterflies, shared barriers),
@@ -189,7 +192,7 @@ cbs_status cbs_context_set_br_schedule(cbs_context *ctx, uint32_t schedule);
  * environment knobs, examples/aes_transcipher/main.cu:107-136, and times three block sizes
  * inline, bitwise/src/cirbts/cirbts-batch.cu:2410-2460).  On the FFT64 backend it times the
  * blind rotation of `batch` synthetic LWE ciphertexts (CUDA events on the context's stream, one
- * warm-up and two timed launches per candidate) for every grouping mb in {1, 2, 3} and, where
+ * warm-up and two timed launches per candidate) for every grouping mb in {1, 2, 3, 4} and, where
  * it applies, both schedules; grouped keys need the secret key (without it only the current mb
  * is timed).  The fastest is applied to the context and stored in the tuning cache under (GPU
  * name, parameter set, batch rounded up to a power of two): cache_path, or NULL for
@@ -198,7 +201,7 @@ cbs_status cbs_context_set_br_schedule(cbs_context *ctx, uint32_t schedule);
  * cached grouping when the FFT64 backend is selected, and its schedule at launch.
  * Synchronous; allocates; not for use inside a stream capture. */
 typedef struct {
-    uint32_t mb;             /* grouping of the blind rotation (1, 2 or 3) */
+    uint32_t mb;             /* grouping of the blind rotation (1, 2, 3 or 4) */
     uint32_t schedule;       /* CBS_BR_SCHEDULE_DIGITWISE, _LOCKSTEP or _PAIRED */
     double us_per_bootstrap; /* measured at the tuned batch */
     uint32_t batch;          /* the batch the choice was measured at */
@@ -210,8 +213,9 @@ cbs_status cbs_autotune_blind_rotation(cbs_context *ctx, uint32_t batch, const c
 cbs_status cbs_context_tuned(const cbs_context *ctx, cbs_tune_choice *out);
 
 /* The grouped keys of the current setting, NTT domain, for inspection and tests:
- * out [ceil(n/mb)][2^mb - 1][2*digits_g][2][N] (null out: only *words is set), subsets in
- * the order {0} {1} {2} {0,1} {0,2} {1,2} {0,1,2} (mb = 3) or {0} {1} {0,1} (mb = 2). */
+ * out [ceil(n/mb)][keys][2*digits_g][2][N] (null out: only *words is set; keys = 3, 7, 8 for
+ * mb = 2, 3, 4), subsets in the order {0} {1} {2} {0,1} {0,2} {1,2} {0,1,2} (mb = 3),
+ * {0} {1} {0,1} (mb = 2) or {0} {1} {2} {3} {0,1} {0,2} {1,2} {0,1,2} (mb = 4). */
 cbs_status cbs_export_mb_bsk(const cbs_context *ctx, uint64_t *out, size_t *words);
 /* Host-only generation of the grouped keys a context keyed with the same seed produces
  * (for CPU-side checks without a GPU); null out: only *words is set. */
@@ -237,7 +241,7 @@ cbs_status cbs_export_keys(const cbs_context *ctx, int32_t *s_lwe, int32_t *s_rl
  * cbs_aes128_import_material then supply that material. */
 cbs_status cbs_import_keys(cbs_context *ctx, const int32_t *s_lwe, const int32_t *s_rlwe, const uint64_t *bsk,
                            const uint64_t *ht, const uint64_t *ss, const uint16_t *ksk);
-/* Grouped keys for mb = 2 or 3 in the layout of cbs_export_mb_bsk (words must match);
+/* Grouped keys for mb = 2, 3 or 4 in the layout of cbs_export_mb_bsk (words must match);
  * selects mb like cbs_context_set_br_multibit.  FFT64 backend. */
 cbs_status cbs_import_mb_bsk(cbs_context *ctx, uint32_t mb, const uint64_t *keys, size_t words);
 

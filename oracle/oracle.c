@@ -378,29 +378,88 @@ void orc_blind_rotate(const orc_cbs_params *p, const orc_cbs_keys *k, const uint
     }
 }
 
-/* Multi-bit blind rotation (the reference's CIRBTS_PBS_MULTIBIT = 2 / 3 path: key grouping
- * cirbts-init.cu:376-530, MB3 MAC kernel.cu:4585-4771).  For binary s_i,
- * prod_{i in G} (1 + (X^{a_i} - 1) s_i) = X^{sum a_i s_i}, so one step per group G of mb
- * coefficients adds sum_S m_S (acc (x) RGSW(prod_{i in S} s_i)) with m_S = prod_{i in S}
- * (X^{a_i} - 1) over the non-empty subsets S, in the order {0} {1} {2} {0,1} {0,2} {1,2}
- * {0,1,2} (mb = 3) or {0} {1} {0,1} (mb = 2).  Coefficients past n rotate by 0, so their
- * subsets vanish.  mbk [groups][2^mb - 1][2*digits_g][2][N] NTT domain. */
+/* Multi-bit blind rotation (the reference's CIRBTS_PBS_MULTIBIT = 2 / 3 / 4 path: key grouping
+ * cirbts-init.cu:376-565, MB3 MAC kernel.cu:4585-4771, MB4 staging cirbts-batch.cu:2767-2923).
+ * For binary s_i, prod_{i in G} (1 + (X^{a_i} - 1) s_i) = X^{sum a_i s_i}, so one step per
+ * group G of mb coefficients adds sum_S m_S (acc (x) RGSW(prod_{i in S} s_i)) with m_S =
+ * prod_{i in S} (X^{a_i} - 1) over the non-empty subsets S, in the order {0} {1} {2} {0,1}
+ * {0,2} {1,2} {0,1,2} (mb = 3) or {0} {1} {0,1} (mb = 2).  mb = 4 is the reference's staged
+ * grouping: 8 keys per group of 4, {0} {1} {2} {3} {0,1} {0,2} {1,2} {0,1,2}; the group adds
+ * the mb = 3 step of coefficients 0-2 (keys 0 1 2 4 5 6 7), then a one-bit step of
+ * coefficient 3 (key 3) on a fresh decomposition of the updated accumulator.  Coefficients
+ * past n rotate by 0, so their subsets vanish.  mbk [groups][keys][2*digits_g][2][N] NTT domain. */
 static const uint32_t orc_mb_order2[3] = {1u, 2u, 3u};
 static const uint32_t orc_mb_order3[7] = {1u, 2u, 4u, 3u, 5u, 6u, 7u};
+static const uint32_t orc_mb_order4[8] = {1u, 2u, 4u, 8u, 3u, 5u, 6u, 7u};
+
+uint32_t orc_mb_keys(uint32_t mb) { return mb == 4 ? 8u : (1u << mb) - 1u; }
+
+uint32_t orc_mb_mask(uint32_t mb, uint32_t kk) {
+    return mb == 2 ? orc_mb_order2[kk] : (mb == 3 ? orc_mb_order3[kk] : (mb == 4 ? orc_mb_order4[kk] : 1u));
+}
+
+/* one step: decompose acc, then acc += sum over the step's keys of m_mask (acc (x) key), the
+ * monomials of the nc coefficients idx0 .. idx0 + nc - 1 */
+static void mb_step(const orc_cbs_params *p, const orc_cbs_keys *k, const uint64_t *a, uint32_t idx0, uint32_t nc,
+                    const uint64_t *gk, const uint32_t *slots, const uint32_t *masks, uint32_t nkeys, uint64_t *acc,
+                    uint64_t *work) {
+    const uint32_t N = p->N, l2 = 2 * p->digits_g, twoN = 2 * N;
+    const uint64_t Q = p->Q;
+    const uint32_t bw = (p->num_lut <= 1) ? 0 : (uint32_t)(32 - __builtin_clz(p->num_lut - 1));
+    uint64_t *ct = work;                    /* [2][N] */
+    uint64_t *dct = ct + 2 * N;             /* [l2][N] */
+    uint64_t *mono = dct + (size_t)l2 * N;  /* [nc][N] */
+    uint64_t *msub = mono + (size_t)3 * N;  /* [nkeys][N] */
+    uint64_t dig[64];
+    memcpy(ct, acc, sizeof(uint64_t) * 2 * N);
+    ntt_inv_one(ct, N, Q, k->irp, k->n_inv);
+    ntt_inv_one(ct + N, N, Q, k->irp, k->n_inv);
+    for (uint32_t poly = 0; poly < 2; ++poly)
+        for (uint32_t c = 0; c < N; ++c) {
+            orc_signed_decompose(ct[poly * N + c], Q, p->base_g, p->digits_g, dig);
+            for (uint32_t j = 0; j < p->digits_g; ++j) dct[(size_t)(2 * j + poly) * N + c] = dig[j];
+        }
+    for (uint32_t d = 0; d < l2; ++d) ntt_fwd_one(dct + (size_t)d * N, N, Q, k->rp);
+    for (uint32_t i = 0; i < nc; ++i) {
+        const uint32_t idx = idx0 + i;
+        const uint32_t at = idx < p->n ? orc_special_ms(a[idx], twoN, p->q_lwe, bw) : 0u;
+        monic_ntt(mono + (size_t)i * N, at, N, Q, k->rp);
+    }
+    for (uint32_t kk = 0; kk < nkeys; ++kk) {
+        uint64_t *m = msub + (size_t)kk * N;
+        for (uint32_t c = 0; c < N; ++c) m[c] = 1;
+        for (uint32_t i = 0; i < nc; ++i)
+            if (masks[kk] & (1u << i))
+                for (uint32_t c = 0; c < N; ++c) m[c] = orc_mulmod(m[c], mono[(size_t)i * N + c], Q);
+    }
+    for (uint32_t c = 0; c < N; ++c) {
+        uint64_t u0 = 0, u1 = 0;
+        for (uint32_t kk = 0; kk < nkeys; ++kk) {
+            const uint64_t *ek = gk + (size_t)slots[kk] * l2 * 2 * N;
+            uint64_t t0 = 0, t1 = 0;
+            for (uint32_t d = 0; d < l2; ++d) {
+                const uint64_t x = dct[(size_t)d * N + c];
+                t0 = addmod(t0, orc_mulmod(x, ek[(size_t)d * 2 * N + c], Q), Q);
+                t1 = addmod(t1, orc_mulmod(x, ek[(size_t)d * 2 * N + N + c], Q), Q);
+            }
+            u0 = addmod(u0, orc_mulmod(t0, msub[(size_t)kk * N + c], Q), Q);
+            u1 = addmod(u1, orc_mulmod(t1, msub[(size_t)kk * N + c], Q), Q);
+        }
+        acc[c] = addmod(acc[c], u0, Q);
+        acc[N + c] = addmod(acc[N + c], u1, Q);
+    }
+}
 
 static void blind_rotate_mb_one(const orc_cbs_params *p, const orc_cbs_keys *k, const uint64_t *mbk, uint32_t mb,
                                 const uint64_t *a, uint64_t b, uint64_t *acc, int finalize, uint64_t *work) {
-    const uint32_t N = p->N, l2 = 2 * p->digits_g, K = (1u << mb) - 1u;
+    static const uint32_t id_slots[7] = {0u, 1u, 2u, 3u, 4u, 5u, 6u};
+    static const uint32_t mb4_slots_a[7] = {0u, 1u, 2u, 4u, 5u, 6u, 7u};
+    static const uint32_t mb4_slot_b[1] = {3u}, one_mask[1] = {1u};
+    const uint32_t N = p->N, l2 = 2 * p->digits_g, K = orc_mb_keys(mb);
     const uint32_t groups = (p->n + mb - 1) / mb;
     const uint64_t Q = p->Q;
     const uint32_t twoN = 2 * N;
     const uint32_t bw = (p->num_lut <= 1) ? 0 : (uint32_t)(32 - __builtin_clz(p->num_lut - 1));
-    const uint32_t *order = (mb == 2) ? orc_mb_order2 : orc_mb_order3;
-    uint64_t *ct = work;                /* [2][N] */
-    uint64_t *dct = ct + 2 * N;         /* [l2][N] */
-    uint64_t *mono = dct + (size_t)l2 * N; /* [mb][N] */
-    uint64_t *msub = mono + (size_t)mb * N; /* [K][N] */
-    uint64_t dig[64];
 
     const uint32_t bt = orc_special_ms(b, twoN, p->q_lwe, bw);
     memset(acc, 0, sizeof(uint64_t) * N);
@@ -408,43 +467,12 @@ static void blind_rotate_mb_one(const orc_cbs_params *p, const orc_cbs_keys *k, 
     ntt_fwd_one(acc + N, N, Q, k->rp);
 
     for (uint32_t g = 0; g < groups; ++g) {
-        memcpy(ct, acc, sizeof(uint64_t) * 2 * N);
-        ntt_inv_one(ct, N, Q, k->irp, k->n_inv);
-        ntt_inv_one(ct + N, N, Q, k->irp, k->n_inv);
-        for (uint32_t poly = 0; poly < 2; ++poly)
-            for (uint32_t c = 0; c < N; ++c) {
-                orc_signed_decompose(ct[poly * N + c], Q, p->base_g, p->digits_g, dig);
-                for (uint32_t j = 0; j < p->digits_g; ++j) dct[(size_t)(2 * j + poly) * N + c] = dig[j];
-            }
-        for (uint32_t d = 0; d < l2; ++d) ntt_fwd_one(dct + (size_t)d * N, N, Q, k->rp);
-        for (uint32_t i = 0; i < mb; ++i) {
-            const uint32_t idx = g * mb + i;
-            const uint32_t at = idx < p->n ? orc_special_ms(a[idx], twoN, p->q_lwe, bw) : 0u;
-            monic_ntt(mono + (size_t)i * N, at, N, Q, k->rp);
-        }
-        for (uint32_t kk = 0; kk < K; ++kk) {
-            uint64_t *m = msub + (size_t)kk * N;
-            for (uint32_t c = 0; c < N; ++c) m[c] = 1;
-            for (uint32_t i = 0; i < mb; ++i)
-                if (order[kk] & (1u << i))
-                    for (uint32_t c = 0; c < N; ++c) m[c] = orc_mulmod(m[c], mono[(size_t)i * N + c], Q);
-        }
         const uint64_t *gk = mbk + (size_t)g * K * l2 * 2 * N;
-        for (uint32_t c = 0; c < N; ++c) {
-            uint64_t u0 = 0, u1 = 0;
-            for (uint32_t kk = 0; kk < K; ++kk) {
-                const uint64_t *ek = gk + (size_t)kk * l2 * 2 * N;
-                uint64_t t0 = 0, t1 = 0;
-                for (uint32_t d = 0; d < l2; ++d) {
-                    const uint64_t x = dct[(size_t)d * N + c];
-                    t0 = addmod(t0, orc_mulmod(x, ek[(size_t)d * 2 * N + c], Q), Q);
-                    t1 = addmod(t1, orc_mulmod(x, ek[(size_t)d * 2 * N + N + c], Q), Q);
-                }
-                u0 = addmod(u0, orc_mulmod(t0, msub[(size_t)kk * N + c], Q), Q);
-                u1 = addmod(u1, orc_mulmod(t1, msub[(size_t)kk * N + c], Q), Q);
-            }
-            acc[c] = addmod(acc[c], u0, Q);
-            acc[N + c] = addmod(acc[N + c], u1, Q);
+        if (mb == 4) {
+            mb_step(p, k, a, 4 * g, 3, gk, mb4_slots_a, orc_mb_order3, 7, acc, work);
+            if (4 * g + 3 < p->n) mb_step(p, k, a, 4 * g + 3, 1, gk, mb4_slot_b, one_mask, 1, acc, work);
+        } else {
+            mb_step(p, k, a, g * mb, mb, gk, id_slots, mb == 2 ? orc_mb_order2 : orc_mb_order3, K, acc, work);
         }
     }
 
@@ -463,8 +491,7 @@ static void blind_rotate_mb_one(const orc_cbs_params *p, const orc_cbs_keys *k, 
 void orc_blind_rotate_mb(const orc_cbs_params *p, const orc_cbs_keys *k, const uint64_t *mbk, uint32_t mb,
                          const uint64_t *a, const uint64_t *b, uint32_t batch, uint32_t a_stride, uint64_t *acc_out,
                          int finalize) {
-    const uint32_t K = (1u << mb) - 1u;
-    const size_t wsz = (size_t)(2 + 2 * p->digits_g + mb + K) * p->N;
+    const size_t wsz = (size_t)(2 + 2 * p->digits_g + 3 + orc_mb_keys(mb)) * p->N;
 #pragma omp parallel
     {
         uint64_t *work = (uint64_t *)malloc(wsz * sizeof(uint64_t));
@@ -1608,9 +1635,7 @@ int orc_cbs_keygen(const orc_cbs_params *p, double sigma_lwe, double sigma_rlwe,
 
 void orc_cbs_keygen_mb(const orc_cbs_params *p, double sigma_rlwe, const int32_t *s_lwe, const int32_t *s_rlwe,
                        uint32_t mb, uint64_t seed, uint64_t *mbk) {
-    static const uint32_t order2[3] = {1u, 2u, 3u};
-    static const uint32_t order3[7] = {1u, 2u, 4u, 3u, 5u, 6u, 7u};
-    const uint32_t N = p->N, n = p->n, l2 = 2 * p->digits_g, K = (1u << mb) - 1u, groups = (n + mb - 1) / mb;
+    const uint32_t N = p->N, n = p->n, l2 = 2 * p->digits_g, K = orc_mb_keys(mb), groups = (n + mb - 1) / mb;
     const uint64_t Q = p->Q;
     uint64_t *rp = (uint64_t *)malloc(sizeof(uint64_t) * N), *irp = (uint64_t *)malloc(sizeof(uint64_t) * N);
     uint64_t ninv[2];
@@ -1626,7 +1651,7 @@ void orc_cbs_keygen_mb(const orc_cbs_params *p, double sigma_rlwe, const int32_t
         orc_rng r;
         rng_seed(&r, seed ^ (0x9e3779b97f4a7c15ull * (uint64_t)(g + 1)));
         for (uint32_t kk = 0; kk < K; ++kk) {
-            const uint32_t mask = mb == 2 ? order2[kk] : order3[kk];
+            const uint32_t mask = orc_mb_mask(mb, kk);
             uint32_t prod = 1;
             for (uint32_t i = 0; i < mb; ++i)
                 if (mask & (1u << i)) {
@@ -1790,9 +1815,7 @@ int orc_cbs_keygen_chacha(const orc_cbs_params *p, double sigma_lwe, double sigm
 
 void orc_cbs_keygen_chacha_mb(const orc_cbs_params *p, double sigma_rlwe, const uint32_t key[8],
                               const int32_t *s_lwe, const int32_t *s_rlwe, uint32_t mb, uint64_t *mbk) {
-    static const uint32_t order2[3] = {1u, 2u, 3u};
-    static const uint32_t order3[7] = {1u, 2u, 4u, 3u, 5u, 6u, 7u};
-    const uint32_t N = p->N, n = p->n, l2 = 2 * p->digits_g, K = (1u << mb) - 1u, groups = (n + mb - 1) / mb;
+    const uint32_t N = p->N, n = p->n, l2 = 2 * p->digits_g, K = orc_mb_keys(mb), groups = (n + mb - 1) / mb;
     const uint64_t Q = p->Q;
     uint64_t *rp = (uint64_t *)malloc(sizeof(uint64_t) * N), *irp = (uint64_t *)malloc(sizeof(uint64_t) * N);
     uint64_t ninv[2];
@@ -1808,7 +1831,7 @@ void orc_cbs_keygen_chacha_mb(const orc_cbs_params *p, double sigma_rlwe, const 
     for (long smp = 0; smp < (long)groups * K * l2; ++smp) {
         uint64_t *tmp = (uint64_t *)malloc(sizeof(uint64_t) * N);
         const uint32_t row = (uint32_t)(smp % l2), kk = (uint32_t)((smp / l2) % K), g = (uint32_t)(smp / ((long)l2 * K));
-        const uint32_t mask = mb == 2 ? order2[kk] : order3[kk];
+        const uint32_t mask = orc_mb_mask(mb, kk);
         uint32_t prod = 1;
         for (uint32_t i = 0; i < mb; ++i)
             if (mask & (1u << i)) {
@@ -1816,7 +1839,7 @@ void orc_cbs_keygen_chacha_mb(const orc_cbs_params *p, double sigma_rlwe, const 
                 prod &= idx < n ? (uint32_t)s_lwe[idx] : 0u;
             }
         uint64_t *a = mbk + (size_t)smp * 2 * N, *b = a + N;
-        chacha_rlwe_zero(key, (uint32_t)smp, mb == 2 ? 8u : 9u, N, Q, rp, s_ntt, TR, lr, a, b, tmp);
+        chacha_rlwe_zero(key, (uint32_t)smp, mb == 2 ? 8u : (mb == 3 ? 9u : 10u), N, Q, rp, s_ntt, TR, lr, a, b, tmp);
         if (prod) {
             uint64_t *tgt = (row & 1) ? b : a;
             for (uint32_t c = 0; c < N; ++c) tgt[c] = addmod(tgt[c], gbr[row >> 1], Q);

@@ -92,9 +92,13 @@ typedef struct {
  * acc_out [batch][2][N] NTT domain. */
 void orc_blind_rotate(const orc_cbs_params *p, const orc_cbs_keys *k, const uint64_t *a, const uint64_t *b,
                       uint32_t batch, uint32_t a_stride, uint64_t *acc_out, int finalize);
-/* Multi-bit blind rotation, mb = 2 or 3 (cirbts-init.cu:376-530 key grouping, kernel.cu:4585-4771):
- * mbk [ceil(n/mb)][2^mb - 1][2*digits_g][2][N] NTT domain, subsets ordered {0} {1} {2} {0,1}
- * {0,2} {1,2} {0,1,2} (mb = 3) or {0} {1} {0,1} (mb = 2). */
+/* Multi-bit blind rotation, mb = 2, 3 or 4 (cirbts-init.cu:376-565 key grouping,
+ * kernel.cu:4585-4771, MB4 staging cirbts-batch.cu:2767-2923): mbk [ceil(n/mb)][keys][2*digits_g]
+ * [2][N] NTT domain, keys = orc_mb_keys(mb), subsets in the order of orc_mb_mask: {0} {1} {2}
+ * {0,1} {0,2} {1,2} {0,1,2} (mb = 3), {0} {1} {0,1} (mb = 2), {0} {1} {2} {3} {0,1} {0,2} {1,2}
+ * {0,1,2} (mb = 4: the mb = 3 step of coefficients 0-2, then a one-bit step of coefficient 3). */
+uint32_t orc_mb_keys(uint32_t mb);
+uint32_t orc_mb_mask(uint32_t mb, uint32_t kk);
 void orc_blind_rotate_mb(const orc_cbs_params *p, const orc_cbs_keys *k, const uint64_t *mbk, uint32_t mb,
                          const uint64_t *a, const uint64_t *b, uint32_t batch, uint32_t a_stride, uint64_t *acc_out,
                          int finalize);
@@ -223,8 +227,8 @@ void orc_encrypt_bits_lwe(const uint32_t key[8], const uint8_t *bits, uint32_t c
 int orc_cbs_keygen(const orc_cbs_params *p, double sigma_lwe, double sigma_rlwe, uint32_t qks, uint32_t base_ks,
                    uint64_t seed, int32_t *s_lwe, int32_t *s_rlwe, uint64_t *bsk, uint64_t *ht, uint64_t *ss,
                    uint16_t *ksk, uint64_t *tv, uint64_t *gpow, uint32_t *maps);
-/* the grouped (mb = 2 or 3) keys of the same key set: RGSW(prod_{i in S} s_i) per group and
- * non-empty subset S, [ceil(n/mb)][2^mb - 1][2 digits_g][2][N]; one generator per group seeded
+/* the grouped (mb = 2, 3 or 4) keys of the same key set: RGSW(prod_{i in S} s_i) per group and
+ * key subset S (orc_mb_mask), [ceil(n/mb)][orc_mb_keys(mb)][2 digits_g][2][N]; one generator per group seeded
  * with seed ^ (0x9e3779b97f4a7c15 (g + 1)) */
 void orc_cbs_keygen_mb(const orc_cbs_params *p, double sigma_rlwe, const int32_t *s_lwe, const int32_t *s_rlwe,
                        uint32_t mb, uint64_t seed, uint64_t *mbk);
@@ -235,7 +239,7 @@ void orc_cbs_keygen_mb(const orc_cbs_params *p, double sigma_rlwe, const int32_t
  * of block (i, 0); s_rlwe[i] = floor(3 x / 2^128) - 1 of block (i, 1)), BSK domain 4 (sample
  * i 2 digits_g + row), HomTrace domain 5 (sample round digits_ht + j), SchemeSwitch domain 6,
  * KSK domain 7 (sample (j N + i) base_ks + v, mask words floor(qks x / 2^128) from block
- * (c, sample), noise from block (n, sample)), grouped keys domain 8 (mb = 2) / 9 (mb = 3).
+ * (c, sample), noise from block (n, sample)), grouped keys domain 8 / 9 / 10 (mb = 2 / 3 / 4).
  * RLWE samples: NTT-domain mask floor(Q x / 2^128) of words 0-3, noise of words 4-5 by the
  * table of orc_cdt_table, b = a s + NTT(e); then the message as the seeded key generation adds
  * it.  Layouts as orc_cbs_keygen; any output may be NULL; returns 0 or -1 (no NTT tables). */

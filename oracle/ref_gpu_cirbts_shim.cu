@@ -110,6 +110,74 @@ int ref_cirbts_blind_rotate_mb2(uint64_t* acc, const uint64_t* d_a, uint32_t a_s
     return static_cast<int>(e);
 }
 
+// Staged grouped (mb = 4, CIRBTS_PBS_MULTIBIT=4) blind rotation in the reference's launch
+// sequence (bitwise/src/cirbts/cirbts-batch.cu:2767-2923, AoS keys): per group of 4, the INTT
+// and fused decomposition/NTT, then kernel_EvalAccCore_Binary_MB3_Grouped_Batch on coefficients
+// 0-2 (the MB2 grouped or one-key kernel for a shorter tail); then, when the group has a fourth
+// coefficient, a fresh INTT and decomposition/NTT and the one-key kernel with key 3.
+// ek / ek_shoup: the reference's 8-slot grouped RF key [8 {0} {1} {2} {3} {0,1} {0,2} {1,2}
+// {0,1,2}][ceil(n/4)][2 digits][2][N] (cirbts-init.cu:536-565) and its Shoup table; the rest as
+// ref_cirbts_blind_rotate_steps.
+int ref_cirbts_blind_rotate_mb4(uint64_t* acc, const uint64_t* d_a, uint32_t a_stride, uint32_t n, uint32_t batch,
+                                const uint64_t* ek, const uint64_t* ek_shoup, const uint64_t* monic, const void* d_mod,
+                                const uint64_t* tw, const uint64_t* tws, const uint64_t* itw, const uint64_t* itws,
+                                const uint64_t* ninv, const uint64_t* ninv_s, uint32_t N, uint64_t Q, uint32_t base_g,
+                                uint32_t digits_g, uint64_t q_lwe, uint32_t bitwidth, void* stream) {
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const DModulus* mod = static_cast<const DModulus*>(d_mod);
+    const uint32_t digitsG2 = 2 * digits_g, twoN = 2 * N, groups = (n + 3) / 4;
+    const size_t key_block = static_cast<size_t>(groups) * digitsG2 * 2 * N;
+    const uint64_t* k[8];
+    const uint64_t* ks[8];
+    for (int i = 0; i < 8; ++i) {
+        k[i] = ek + i * key_block;
+        ks[i] = ek_shoup + i * key_block;
+    }
+    uint64_t *ct = nullptr, *dct = nullptr;
+    uint32_t* index_pos = nullptr;
+    cudaError_t e = cudaMalloc(&ct, sizeof(uint64_t) * 2 * N * batch);
+    if (e == cudaSuccess) e = cudaMalloc(&dct, sizeof(uint64_t) * digitsG2 * N * batch);
+    if (e == cudaSuccess) e = cudaMalloc(&index_pos, sizeof(uint32_t) * n * batch);
+    if (e == cudaSuccess) {
+        kernel_SpecialMS_IndexPos_Batch<<<dim3((n + 255) / 256, batch), 256, 0, s>>>(d_a, index_pos, n, batch, a_stride,
+                                                                                     twoN, q_lwe, bitwidth);
+        const uint32_t tpb = N / 2 < 256 ? N / 2 : 256;
+        const dim3 eb(128), eg((N + 127) / 128, batch);
+        auto decompose = [&]() {
+            inwt_1d_opt_outofplace_batched(ct, acc, itw, itws, mod, ninv, ninv_s, N, static_cast<size_t>(2) * batch,
+                                           s);
+            kernel_SignedDigitDecompose2_FusedFNWT_Batch<<<digitsG2 * batch, tpb, N * sizeof(uint64_t), s>>>(
+                dct, ct, Q, base_g, digits_g, N, batch, tw, tws, mod);
+        };
+        for (uint32_t g = 0; g < groups && e == cudaSuccess; ++g) {
+            const uint32_t idx0 = 4 * g, idx1 = idx0 + 1, idx2 = idx0 + 2, idx3 = idx0 + 3;
+            decompose();
+            if (idx2 < n)
+                kernel_EvalAccCore_Binary_MB3_Grouped_Batch<<<eg, eb, 0, s>>>(
+                    acc, dct, k[0], ks[0], k[1], ks[1], k[2], ks[2], k[4], ks[4], k[5], ks[5], k[6], ks[6], k[7], ks[7],
+                    monic, N, mod, digitsG2, g, idx0, idx1, idx2, index_pos, n);
+            else if (idx1 < n)
+                kernel_EvalAccCore_Binary_MB2_Grouped_Batch<<<eg, eb, 0, s>>>(acc, dct, k[0], ks[0], k[1], ks[1], k[4],
+                                                                              ks[4], monic, N, mod, digitsG2, g, idx0,
+                                                                              idx1, index_pos, n);
+            else
+                kernel_EvalAccCore_Binary_Grouped_Batch<<<eg, eb, 0, s>>>(acc, dct, k[0], ks[0], monic, N, mod,
+                                                                          digitsG2, g, idx0, index_pos, n);
+            if (idx3 < n) {
+                decompose();
+                kernel_EvalAccCore_Binary_Grouped_Batch<<<eg, eb, 0, s>>>(acc, dct, k[3], ks[3], monic, N, mod,
+                                                                          digitsG2, g, idx3, index_pos, n);
+            }
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    }
+    cudaFree(ct);
+    cudaFree(dct);
+    cudaFree(index_pos);
+    return static_cast<int>(e);
+}
+
 // N-major index positions [n][batch] of the LWE masks (kernel_SpecialMS_IndexPos_Batch_NMajor,
 // the layout CIRBTS_BATCH_INDEX_NMAJOR=1 selects), into caller memory.
 int ref_cirbts_index_nmajor(const uint64_t* d_a, uint32_t a_stride, uint32_t n, uint32_t batch, uint32_t N,

@@ -10,6 +10,11 @@ import numpy as np
 from conftest import _U16P, _U32P, _U64P, oracle_primes, oracle_tables
 
 
+def mb_keys(mb: int) -> int:
+    """Grouped keys per group: every non-empty subset (mb = 2, 3), 8 for the staged mb = 4."""
+    return 8 if mb == 4 else (1 << mb) - 1
+
+
 class OrcParams(ctypes.Structure):
     _fields_ = [("N", ctypes.c_uint32), ("log_n", ctypes.c_uint32), ("Q", ctypes.c_uint64), ("n", ctypes.c_uint32),
                 ("q_lwe", ctypes.c_uint64), ("base_g", ctypes.c_uint32), ("digits_g", ctypes.c_uint32),
@@ -186,12 +191,12 @@ MB_SEED_TWEAK = 0x6d756c7469626974
 
 
 def oracle_keys_mb(oracle, p, keys: dict, mb: int, seed: int) -> np.ndarray:
-    """Grouped keys [ceil(n/mb)][2^mb - 1][2 digits_g][2][N] of a key set from the oracle, seeded
-    as a context keyed with `seed` seeds them."""
+    """Grouped keys [ceil(n/mb)][keys][2 digits_g][2][N] of a key set from the oracle (keys = 3, 7, 8
+    for mb = 2, 3, 4), seeded as a context keyed with `seed` seeds them."""
     vp = ctypes.c_void_p
     oracle.orc_cbs_keygen_mb.argtypes = [vp, ctypes.c_double, vp, vp, ctypes.c_uint32, ctypes.c_uint64, vp]
     groups = -(-p.n // mb)
-    out = np.zeros((groups, (1 << mb) - 1, 2 * p.digits_g, 2, p.N), np.uint64)
+    out = np.zeros((groups, mb_keys(mb), 2 * p.digits_g, 2, p.N), np.uint64)
     op = orc_params(p)
     s_lwe = np.ascontiguousarray(keys["s_lwe"], np.int32)
     s_rlwe = np.ascontiguousarray(keys["s_rlwe"], np.int32)

@@ -1,4 +1,4 @@
-"""The blind-rotation autotuner: it times every grouping (mb = 1, 2, 3) and the three schedules of
+"""The blind-rotation autotuner: it times every grouping (mb = 1, 2, 3, staged 4) and the three schedules of
 the two-digit gadget at mb = 2, applies the fastest, writes it to the tuning cache, and a context created
 afterwards reads the cache and takes the cached grouping when the FFT64 backend is selected
 (unless the caller sets mb)."""
@@ -22,7 +22,7 @@ def test_autotune_caches_and_applies(pkg, tmp_path, monkeypatch):
         c.keygen(3)
         c.set_br_backend(pkg.BR_FFT64)
         choice = c.autotune(296)
-        assert choice["mb"] in (1, 2, 3) and choice["candidates"] == 5 and choice["us_per_bootstrap"] > 0
+        assert choice["mb"] in (1, 2, 3, 4) and choice["candidates"] == 6 and choice["us_per_bootstrap"] > 0
         assert choice["schedule"] in (pkg.BR_SCHEDULE_DIGITWISE, pkg.BR_SCHEDULE_LOCKSTEP, pkg.BR_SCHEDULE_PAIRED)
         print(f"tuned: {choice}")
         entries = json.loads(cache.read_text())
@@ -40,7 +40,8 @@ def test_autotune_caches_and_applies(pkg, tmp_path, monkeypatch):
         if choice["mb"] > 1:  # the cached grouping is in effect: its grouped keys exist
             mbk = c2.export_mb_bsk()
             groups = -(-p.n // choice["mb"])
-            assert np.asarray(mbk).size == groups * ((1 << choice["mb"]) - 1) * 2 * p.digits_g * 2 * p.N
+            keys = 8 if choice["mb"] == 4 else (1 << choice["mb"]) - 1
+            assert np.asarray(mbk).size == groups * keys * 2 * p.digits_g * 2 * p.N
         c2.set_br_multibit(1)  # an explicit choice overrides the cache
         assert pkg.load().cbs_export_mb_bsk(c2.handle, None, pkg.ctypes.byref(pkg.ctypes.c_size_t())) == 7
     finally:

@@ -76,10 +76,11 @@ def test_fft_blind_rotate_phase_error_bound(pkg, fctx, fkeys, foc):
     assert log2 < FFT_PHASE_TOL_LOG2
 
 
-@pytest.mark.parametrize("mb", [2, 3])
+@pytest.mark.parametrize("mb", [2, 3, 4])
 def test_fft_multibit_blind_rotate_phase_error(pkg, fctx, fkeys, foc, mb):
     """Grouped (multi-bit) FFT blind rotation against the oracle's exact grouped rotation with
-    the same keys: the FP64 error of the combined-key products, same tolerance as above."""
+    the same keys: the FP64 error of the combined-key products, same tolerance as above.  mb = 4
+    is the staged grouping (an mb = 3 step and a one-bit step per group of 4)."""
     p = fctx.params
     fctx.set_br_multibit(mb)
     try:
@@ -135,7 +136,8 @@ def test_multibit_needs_fft_backend(pkg):
     c = pkg.Context(max_batch=4)
     try:
         assert pkg.load().cbs_context_set_br_multibit(c.handle, 3) == 6  # CBS_ERR_UNSUPPORTED on the NTT backend
-        assert pkg.load().cbs_context_set_br_multibit(c.handle, 4) == 1
+        assert pkg.load().cbs_context_set_br_multibit(c.handle, 4) == 6
+        assert pkg.load().cbs_context_set_br_multibit(c.handle, 5) == 1  # CBS_ERR_INVALID_ARG
     finally:
         c.close()
 

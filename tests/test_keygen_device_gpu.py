@@ -25,18 +25,19 @@ def test_device_keygen_matches_oracle_word_for_word(pkg, oracle):
         for f in ("s_lwe", "s_rlwe", "bsk", "ht", "ss", "ksk"):
             assert np.array_equal(np.asarray(got[f]).reshape(-1), want[f].reshape(-1).astype(np.asarray(got[f]).dtype)), f
         assert set(np.unique(want["s_rlwe"])) <= {-1, 0, 1} and 0 < want["s_lwe"].sum() < p.n
-        # grouped keys from the same stream
+        # grouped keys from the same stream (mb = 2: domain 8; the staged mb = 4: domain 10)
         c.set_br_backend(pkg.BR_FFT64)
-        c.set_br_multibit(2)
-        mbk = c.export_mb_bsk()
         vp = ctypes.c_void_p
         oracle.orc_cbs_keygen_chacha_mb.argtypes = [vp, ctypes.c_double, vp, vp, vp, ctypes.c_uint32, vp]
-        wm = np.zeros_like(mbk)
         kw = np.frombuffer(RNG_KEY, np.uint32).copy()
         op = orc_params(p)
-        oracle.orc_cbs_keygen_chacha_mb(ctypes.byref(op), p.sigma_rlwe, kw.ctypes.data, want["s_lwe"].ctypes.data,
-                                        want["s_rlwe"].ctypes.data, 2, wm.ctypes.data)
-        assert np.array_equal(mbk, wm)
+        for mb in (2, 4):
+            c.set_br_multibit(mb)
+            mbk = c.export_mb_bsk()
+            wm = np.zeros_like(mbk)
+            oracle.orc_cbs_keygen_chacha_mb(ctypes.byref(op), p.sigma_rlwe, kw.ctypes.data, want["s_lwe"].ctypes.data,
+                                            want["s_rlwe"].ctypes.data, mb, wm.ctypes.data)
+            assert np.array_equal(mbk, wm), mb
     finally:
         c.close()
 

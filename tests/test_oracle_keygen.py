@@ -1,7 +1,7 @@
 """The oracle's key generation (the CPU legs' keys, so the CPU baseline needs nothing from the
 product library) against the product's seeded host key generation: the same seed gives the
 same secrets, bootstrapping, HomTrace, SchemeSwitch and extraction keys, test vector, gadget
-powers and automorphism maps word for word, and the same grouped (mb = 2) keys."""
+powers and automorphism maps word for word, and the same grouped (mb = 2, 4) keys."""
 from __future__ import annotations
 
 import ctypes
@@ -21,11 +21,12 @@ def test_oracle_keygen_matches_host_keygen(pkg, oracle, preset):
         assert np.array_equal(np.asarray(got[f]).reshape(-1), np.asarray(want[f]).reshape(-1).astype(got[f].dtype)), f
 
 
-def test_oracle_grouped_keygen_matches_host(pkg, oracle):
+@pytest.mark.parametrize("mb", [2, 4])
+def test_oracle_grouped_keygen_matches_host(pkg, oracle, mb):
     p = pkg.default_params()
     keys = pkg.generate_keys_host(p, 13)
-    want = np.asarray(pkg.generate_mb_bsk_host(p, 13, 2)).reshape(-1)
-    got = oracle_keys_mb(oracle, p, keys, 2, 13).reshape(-1)
+    want = np.asarray(pkg.generate_mb_bsk_host(p, 13, mb)).reshape(-1)
+    got = oracle_keys_mb(oracle, p, keys, mb, 13).reshape(-1)
     assert np.array_equal(got, want)
 
 

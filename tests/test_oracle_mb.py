@@ -1,5 +1,5 @@
-"""CPU checks of the multi-bit blind rotation (the reference's CIRBTS_PBS_MULTIBIT = 2 / 3
-grouping): the host-generated grouped keys are RGSW encryptions of the subset products of
+"""CPU checks of the multi-bit blind rotation (the reference's CIRBTS_PBS_MULTIBIT = 2 / 3 / 4
+grouping; 4 is the staged 3 + 1 grouping with 8 keys per group): the host-generated grouped keys are RGSW encryptions of the subset products of
 the secret bits, and the oracle's exact grouped blind rotation decrypts to the same
 accumulator as the one-bit blind rotation on the same inputs, within the key noise (tail
 groups included: n = 13 leaves one coefficient in the last group)."""
@@ -12,7 +12,8 @@ import pytest
 
 from cbs_harness import OracleCbs, lwe_encrypt_bits
 
-SUBSETS = {2: [0b01, 0b10, 0b11], 3: [0b001, 0b010, 0b100, 0b011, 0b101, 0b110, 0b111]}
+SUBSETS = {2: [0b01, 0b10, 0b11], 3: [0b001, 0b010, 0b100, 0b011, 0b101, 0b110, 0b111],
+           4: [0b0001, 0b0010, 0b0100, 0b1000, 0b0011, 0b0101, 0b0110, 0b0111]}
 
 
 @pytest.fixture(scope="module")
@@ -27,11 +28,11 @@ def small(pkg, oracle):
     return p, keys, OracleCbs(oracle, p, keys)
 
 
-@pytest.mark.parametrize("mb", [2, 3])
+@pytest.mark.parametrize("mb", [2, 3, 4])
 def test_grouped_keys_encrypt_subset_products(pkg, small, mb):
     p, keys, oc = small
     mbk = pkg.generate_mb_bsk_host(p, 31, mb)
-    K, l2, N = (1 << mb) - 1, 2 * p.digits_g, p.N
+    K, l2, N = len(SUBSETS[mb]), 2 * p.digits_g, p.N
     groups = (p.n + mb - 1) // mb
     mbk = mbk.reshape(groups, K, l2, 2, N)
     s = keys["s_lwe"]
@@ -49,7 +50,7 @@ def test_grouped_keys_encrypt_subset_products(pkg, small, mb):
             assert max(abs(int(x)) for x in ph) < 2 ** 20
 
 
-@pytest.mark.parametrize("mb", [2, 3])
+@pytest.mark.parametrize("mb", [2, 3, 4])
 def test_grouped_blind_rotation_matches_one_bit(pkg, small, mb):
     p, keys, oc = small
     mbk = pkg.generate_mb_bsk_host(p, 31, mb)

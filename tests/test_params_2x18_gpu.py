@@ -72,6 +72,40 @@ def test_exact_blind_rotate_bit_exact(pkg, wctx, wkeys, woc):
     assert np.array_equal(mv.cpu().numpy().view(np.uint64).reshape(want.shape), want)
 
 
+@pytest.mark.parametrize("mb", [3, 4])
+def test_grouped_fft_blind_rotate_phase_error_mb3_mb4(pkg, wctx, wkeys, woc, mb):
+    """The generic grouped kernel on the two-digit gadget: mb = 3 and the staged mb = 4 (an mb = 3
+    step and a one-bit step per group of 4) against the oracle's exact grouped rotation."""
+    p = wctx.params
+    bits = [1, 0, 1]
+    B = len(bits)
+    pkg.call("cbs_context_set_br_backend", wctx.handle, pkg.BR_FFT64)
+    wctx.set_br_multibit(mb)
+    try:
+        mbk = wctx.export_mb_bsk()
+        rng = np.random.default_rng(60 + mb)
+        a, b = lwe_encrypt_bits(rng, wkeys["s_lwe"], bits, p.q_lwe)
+        mv = torch.zeros((B, p.num_lut, 2, p.N), dtype=torch.int64, device="cuda")
+        da, db = _dev(a), _dev(b)
+        pkg.call("cbs_blind_rotate_batch_device", wctx.handle, da.data_ptr(), db.data_ptr(), B, p.n, mv.data_ptr(),
+                 None)
+        torch.cuda.synchronize()
+    finally:
+        wctx.set_br_multibit(2)
+        pkg.call("cbs_context_set_br_backend", wctx.handle, pkg.BR_NTT)
+    got = mv.cpu().numpy().view(np.uint64).reshape(B, p.num_lut, 2, p.N)
+    want = woc.br_acc_mb(a, b, mbk, mb)
+    Q, N = p.Q, p.N
+    worst = 0
+    for i in range(B):
+        d = woc.phase_coef(got[i, 0]) - woc.phase_coef(want[i])
+        e = [((int(x) * N + Q // 2) % Q) - Q // 2 for x in d]
+        worst = max(worst, max(abs(x) for x in e))
+    log2 = np.log2(worst + 1)
+    print(f"2x18 grouped FFT blind rotation (mb = {mb}): max |phase error| 2^{log2:.1f}")
+    assert log2 < FFT_PHASE_TOL_LOG2_2X18
+
+
 @pytest.mark.parametrize("schedule,bits", [("digitwise", [0, 1, 1]), ("lockstep", [0, 1, 1]),
                                            ("paired", [0, 1, 1]), ("paired", [1, 0, 1, 1])])
 def test_grouped_fft_blind_rotate_phase_error(pkg, wctx, wkeys, woc, schedule, bits):

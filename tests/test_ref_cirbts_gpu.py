@@ -6,8 +6,9 @@ sequences (ref_gpu_cirbts_shim.cu):
   kernel_SignedDigitDecompose2_FusedFNWT_Batch and kernel_EvalAccCore_Binary_Batch with the
   product's keys (its [n][2 digits][2][N] NTT-domain layout is the reference's AoS RF key):
   from the same initial accumulator, n = 630 steps give the oracle's accumulator word for word;
-  likewise the grouped mb = 2 sequence (kernel_EvalAccCore_Binary_MB2_Grouped_Batch) against
-  the oracle's exact grouped rotation;
+  likewise the grouped mb = 2 sequence (kernel_EvalAccCore_Binary_MB2_Grouped_Batch), the staged
+  mb = 4 sequence (MB3 grouped kernel, then a one-key step) and the AES example's mb = 3 SoA
+  sequence against the oracle's exact grouped rotation;
 * HomTrace + SchemeSwitch: kernel_GenerateCoefficientAutoMaps, per round the permuting INTT,
   kernel_Fused_Permute_Decompose, the NTT and kernel_MultAddUpdate_HT_PermuteC1, then
   kernel_MultAddUpdate_SS and kernel_SaveToRGSW: the oracle's RGSW rows word for word, and the
@@ -161,44 +162,49 @@ def test_trace_schemeswitch_matches_reference_kernels(pkg, oracle, ref):
     assert np.array_equal(rows.cpu().numpy().view(np.uint64), want)
 
 
-@pytest.mark.parametrize("preset", ["3x12", "2x18"])
-def test_grouped_blind_rotation_matches_reference_kernels(pkg, oracle, ref, preset):
-    """The grouped (mb = 2, CIRBTS_PBS_MULTIBIT=2) blind rotation: the reference's
-    kernel_EvalAccCore_Binary_MB2_Grouped_Batch sequence with the product's grouped keys
-    (re-laid [subset][group] as the reference's RF key) reproduces the oracle's exact grouped
-    accumulator word for word; the product's FFT form is checked against that oracle within
-    its phase-error bound (test_cbs_fft_gpu.py)."""
+@pytest.mark.parametrize("preset,mb,steps", [("3x12", 2, 630), ("2x18", 2, 630), ("3x12", 4, 630),
+                                              ("2x18", 4, 629), ("2x18", 4, 627)])
+def test_grouped_blind_rotation_matches_reference_kernels(pkg, oracle, ref, preset, mb, steps):
+    """The grouped blind rotation: mb = 2 (CIRBTS_PBS_MULTIBIT=2), the reference's
+    kernel_EvalAccCore_Binary_MB2_Grouped_Batch sequence, and the staged mb = 4
+    (CIRBTS_PBS_MULTIBIT=4: kernel_EvalAccCore_Binary_MB3_Grouped_Batch on coefficients 0-2 of a
+    group, then a fresh decomposition and the one-key kernel with key 3), with the product's
+    grouped keys re-laid [subset][group] as the reference's RF key, reproduce the oracle's exact
+    grouped accumulator word for word.  The mb = 4 cases end on a group of 2 (the reference's
+    MB2 tail), 1 (its one-key tail) and 3 coefficients (no one-bit step).  The product's FFT form
+    is checked against that oracle within its phase-error bound (test_cbs_fft_gpu.py)."""
     vp, u32, u64 = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64
-    ref.ref_cirbts_blind_rotate_mb2.argtypes = [vp, vp, u32, u32, u32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, u32,
-                                                u64, u32, u32, u64, u32, vp]
-    ref.ref_cirbts_blind_rotate_mb2.restype = ctypes.c_int
+    fn = ref.ref_cirbts_blind_rotate_mb2 if mb == 2 else ref.ref_cirbts_blind_rotate_mb4
+    fn.argtypes = [vp, vp, u32, u32, u32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, u32, u64, u32, u32, u64, u32, vp]
+    fn.restype = ctypes.c_int
     oracle.orc_blind_rotate_mb.argtypes = [vp, vp, vp, u32, vp, vp, u32, u32, vp, ctypes.c_int]
     p = pkg.preset_params(preset)
     N, n, Q = p.N, p.n, p.Q
     keys = pkg.generate_keys_host(p, 31)
-    mbk = np.ascontiguousarray(pkg.generate_mb_bsk_host(p, 31, 2))
+    K = 3 if mb == 2 else 8
+    groups = -(-steps // mb)
+    mbk = np.asarray(pkg.generate_mb_bsk_host(p, 31, mb)).reshape(-1, K, 2 * p.digits_g * 2 * N)[:groups]
+    mbk = np.ascontiguousarray(mbk)
     oc = OracleCbs(oracle, p, keys)
     batch = 2
-    rng = np.random.default_rng(12)
+    rng = np.random.default_rng(12 + mb)
     a = rng.integers(0, p.q_lwe, size=(batch, n), dtype=np.uint64)
     b = rng.integers(0, p.q_lwe, batch, dtype=np.uint64)
     init = _orc_acc(oracle, oc, a, b, 0)
-    want = _orc_acc(oracle, oc, a, b, n, mbk=mbk, mb=2)
+    want = _orc_acc(oracle, oc, a, b, steps, mbk=mbk, mb=mb)
     tabs, ninv, dmod = _tables(pkg, N, Q)
     monic = _monic(oracle, oc, N, Q)
-    groups = (n + 1) // 2
-    ek = np.ascontiguousarray(mbk.reshape(groups, 3, -1).transpose(1, 0, 2)).reshape(-1)  # [subset][group][...]
+    ek = np.ascontiguousarray(mbk.transpose(1, 0, 2)).reshape(-1)  # [subset][group][...]
     eks = np.zeros_like(ek)
     ref.ref_cirbts_shoup(ek.ctypes.data, eks.ctypes.data, ek.size, Q)
     bitwidth = max(0, (p.num_lut - 1).bit_length())
     dev = {name: _dev(v) for name, v in [("acc", init), ("a", a), ("ek", ek), ("eks", eks), ("monic", monic),
                                          ("mod", dmod), ("tw", tabs[0]), ("tws", tabs[1]), ("itw", tabs[2]),
                                          ("itws", tabs[3]), ("ninv", ninv)]}
-    st = ref.ref_cirbts_blind_rotate_mb2(
-        dev["acc"].data_ptr(), dev["a"].data_ptr(), n, n, batch, dev["ek"].data_ptr(), dev["eks"].data_ptr(),
-        dev["monic"].data_ptr(), dev["mod"].data_ptr(), dev["tw"].data_ptr(), dev["tws"].data_ptr(),
-        dev["itw"].data_ptr(), dev["itws"].data_ptr(), dev["ninv"].data_ptr(), dev["ninv"].data_ptr() + 8, N, Q,
-        p.base_g, p.digits_g, p.q_lwe, bitwidth, None)
+    st = fn(dev["acc"].data_ptr(), dev["a"].data_ptr(), n, steps, batch, dev["ek"].data_ptr(), dev["eks"].data_ptr(),
+            dev["monic"].data_ptr(), dev["mod"].data_ptr(), dev["tw"].data_ptr(), dev["tws"].data_ptr(),
+            dev["itw"].data_ptr(), dev["itws"].data_ptr(), dev["ninv"].data_ptr(), dev["ninv"].data_ptr() + 8, N, Q,
+            p.base_g, p.digits_g, p.q_lwe, bitwidth, None)
     torch.cuda.synchronize()
     assert st == 0
     got = dev["acc"].cpu().numpy().view(np.uint64).reshape(batch, 2, N)

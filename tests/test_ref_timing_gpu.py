@@ -316,7 +316,8 @@ def test_blind_rotation_timing_beside_reference_aes_default(pkg, preset):
                  None)
 
     ctx.set_br_backend(pkg.BR_FFT64)
-    for name, mb in [("product FP64 FFT, mb = 2", 2), ("product FP64 FFT, mb = 3", 3)]:
+    for name, mb in [("product FP64 FFT, mb = 2", 2), ("product FP64 FFT, mb = 4 (staged)", 4),
+                     ("product FP64 FFT, mb = 3", 3)]:
         ctx.set_br_multibit(mb)
         results[name] = _time_ms(ours, reps=3)
     mbk = ctx.export_mb_bsk()  # mb = 3 keys
