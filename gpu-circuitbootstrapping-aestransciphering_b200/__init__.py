@@ -23,6 +23,7 @@ c_u32p = ctypes.POINTER(ctypes.c_uint32)
 c_vp = ctypes.c_void_p
 
 BR_NTT, BR_FFT64 = 0, 1
+BR_GINX, BR_LMKCDEY = 0, 1
 
 CBS_STATUS = {
     0: "CBS_OK", 1: "CBS_ERR_INVALID_ARG", 2: "CBS_ERR_SHAPE_MISMATCH", 3: "CBS_ERR_OOM",
@@ -83,6 +84,12 @@ def _declare(lib: ctypes.CDLL) -> None:
         "cbs_keygen": (st, [c_vp, u64]),
         "cbs_context_set_br_backend": (st, [c_vp, ctypes.c_int]),
         "cbs_context_set_br_multibit": (st, [c_vp, u32]),
+        "cbs_context_set_br_method": (st, [c_vp, ctypes.c_int, u32]),
+        "cbs_export_lmkcdey_keys": (st, [c_vp, c_vp, c_vp, c_vp, c_vp]),
+        "cbs_import_lmkcdey_keys": (st, [c_vp, u32, c_vp, sz, c_vp, sz]),
+        "cbs_generate_lmkcdey_keys_host": (st, [c_vp, u64, u32, c_vp, c_vp, c_vp, c_vp]),
+        "cbs_lmkcdey_auto_maps_host": (st, [u32, u32, c_vp]),
+        "cbs_lmkcdey_eval_acc_batch_device": (st, [c_vp, c_vp, u32, c_vp, u32, c_vp]),
         "cbs_export_mb_bsk": (st, [c_vp, c_vp, c_vp]),
         "cbs_generate_mb_bsk_host": (st, [c_vp, u64, u32, c_vp, c_vp]),
         "cbs_export_keys": (st, [c_vp] + [c_vp] * 9),
@@ -236,6 +243,27 @@ def preset_params(name: str) -> CbsParams:
     return p
 
 
+def generate_lmkcdey_keys_host(params: CbsParams, seed: int, num_auto_keys: int):
+    """LMKCDEY keys (eval [n][2*digits_g][2][N], auto [1 + num_auto_keys][digits_g][2][N], NTT domain)
+    of the key set cbs_keygen(seed) makes, generated on the host."""
+    import numpy as np
+    ew, aw = ctypes.c_size_t(), ctypes.c_size_t()
+    call("cbs_generate_lmkcdey_keys_host", ctypes.byref(params), seed, num_auto_keys, None, None, ctypes.byref(ew),
+         ctypes.byref(aw))
+    ev, au = np.zeros(ew.value, np.uint64), np.zeros(aw.value, np.uint64)
+    call("cbs_generate_lmkcdey_keys_host", ctypes.byref(params), seed, num_auto_keys, ev.ctypes.data, au.ctypes.data,
+         ctypes.byref(ew), ctypes.byref(aw))
+    return ev.reshape(params.n, 2 * params.digits_g, 2, params.N), au.reshape(-1, params.digits_g, 2, params.N)
+
+
+def lmkcdey_auto_maps_host(N: int, num_auto_keys: int):
+    """NTT-domain automorphism maps [1 + num_auto_keys][N] of the LMKCDEY key set."""
+    import numpy as np
+    out = np.zeros((1 + num_auto_keys, N), np.uint32)
+    call("cbs_lmkcdey_auto_maps_host", N, num_auto_keys, out.ctypes.data)
+    return out
+
+
 def generate_mb_bsk_host(params: CbsParams, seed: int, mb: int):
     """Grouped blind-rotation keys [ceil(n/mb)][keys][2*digits_g][2][N] (NTT domain; keys = 3, 7, 8
     for mb = 2, 3, 4) of the
@@ -341,6 +369,28 @@ class Context:
     def set_br_schedule(self, schedule: int) -> None:
         """Two-digit grouped blind-rotation schedule (BR_SCHEDULE_*; AUTO = the tuned one)."""
         call("cbs_context_set_br_schedule", self._h, schedule)
+
+    def set_br_method(self, method: int, num_auto_keys: int = 10) -> None:
+        """Blind-rotation method: BR_GINX (default) or BR_LMKCDEY with automorphism keys for 2N - 5
+        and 5^1 .. 5^num_auto_keys (NTT backend, num_lut = 1, g (digits_g + 1) >= log2 Q)."""
+        call("cbs_context_set_br_method", self._h, method, num_auto_keys)
+
+    def export_lmkcdey_keys(self):
+        """LMKCDEY keys (NTT domain): eval [n][2*digits_g][2][N], auto [1 + num_auto_keys][digits_g][2][N]."""
+        import numpy as np
+        ew, aw = ctypes.c_size_t(), ctypes.c_size_t()
+        call("cbs_export_lmkcdey_keys", self._h, None, None, ctypes.byref(ew), ctypes.byref(aw))
+        ev, au = np.zeros(ew.value, np.uint64), np.zeros(aw.value, np.uint64)
+        call("cbs_export_lmkcdey_keys", self._h, ev.ctypes.data, au.ctypes.data, ctypes.byref(ew), ctypes.byref(aw))
+        p = self.params
+        return ev.reshape(p.n, 2 * p.digits_g, 2, p.N), au.reshape(-1, p.digits_g, 2, p.N)
+
+    def import_lmkcdey_keys(self, num_auto_keys: int, eval_keys, auto_keys) -> None:
+        """LMKCDEY keys in the layout of export_lmkcdey_keys (selects the method)."""
+        import numpy as np
+        ev = np.ascontiguousarray(eval_keys, np.uint64).reshape(-1)
+        au = np.ascontiguousarray(auto_keys, np.uint64).reshape(-1)
+        call("cbs_import_lmkcdey_keys", self._h, num_auto_keys, ev.ctypes.data, ev.size, au.ctypes.data, au.size)
 
     def export_mb_bsk(self):
         """Grouped blind-rotation keys [ceil(n/mb)][keys][2*digits_g][2][N] (NTT domain; keys = 3, 7,

@@ -34,14 +34,6 @@ __device__ __forceinline__ uint64_t digit_mod(uint64_t x, const Gadget& g, uint3
     return signed_to_mod(r, g.q);
 }
 
-// coefficient i of X^{-e} p (e in [0, 2N))
-template <uint32_t N>
-__device__ __forceinline__ uint64_t rot_neg(const uint64_t* p, uint32_t e, uint32_t i, uint64_t q) {
-    const uint32_t s = (i + e) & (2 * N - 1);
-    const uint64_t v = (s < N) ? p[s] : p[s - N];
-    return (s < N) ? v : (v ? q - v : 0);
-}
-
 // acc += X^{e} t - t (coefficient domain)
 template <uint32_t N, uint32_t T>
 __device__ __forceinline__ void rotate_add(uint64_t* acc, const uint64_t* t, uint32_t e, uint32_t tid, uint64_t q) {

@@ -78,6 +78,14 @@ __device__ __forceinline__ uint32_t special_ms_f(uint64_t v, uint32_t two_n, uin
     return static_cast<uint32_t>((r * shift) & (static_cast<uint64_t>(two_n) - 1ull));
 }
 
+// coefficient i of X^{-e} p (e in [0, 2N))
+template <uint32_t N>
+__device__ __forceinline__ uint64_t rot_neg(const uint64_t* p, uint32_t e, uint32_t i, uint64_t q) {
+    const uint32_t s = (i + e) & (2 * N - 1);
+    const uint64_t v = (s < N) ? p[s] : p[s - N];
+    return (s < N) ? v : (v ? q - v : 0);
+}
+
 cudaError_t launch_blind_rotate(const BlindRotateArgs& a, uint32_t N, uint32_t batch, cudaStream_t s);
 cudaError_t launch_trace_schemeswitch(const TraceArgs& a, uint32_t N, uint32_t count, cudaStream_t s);
 cudaError_t launch_cmux_level(const CmuxLevelArgs& a, uint32_t N, uint32_t luts, cudaStream_t s);

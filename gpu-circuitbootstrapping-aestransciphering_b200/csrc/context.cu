@@ -175,6 +175,7 @@ cbs_status run_blind_rotate(cbs_context* c, const uint64_t* d_a, const uint64_t*
         CBS_CUDA_TRY(launch_blind_rotate_fft(a, fft_key_args(c), c->d_mod.p, c->p.N, batch, s, mv_ntt));
         return CBS_OK;
     }
+    if (c->br_method == CBS_BR_LMKCDEY) return run_blind_rotate_lmkcdey(c, d_a, d_b, batch, a_stride, d_mv, s);
     CBS_CUDA_TRY(launch_blind_rotate(a, c->p.N, batch, s));
     return CBS_OK;
 }
@@ -402,13 +403,20 @@ cbs_status finish_key_upload(cbs_context* c) {
     c->mb_ready = false;
     c->h_mbk.clear();
     c->d_bskf_mb.reset();
+    c->lmk_ready = false;
+    c->h_lmk_eval.clear();
+    c->h_lmk_auto.clear();
     c->aes.drop_graphs();
     if (c->br_backend == CBS_BR_FFT64) {
         if (cbs_status st = prepare_fft(c)) return st;
         return prepare_mb(c);
     }
+    // LMKCDEY keys follow from the secrets of a seeded key set (otherwise they are imported)
+    if (c->br_method == CBS_BR_LMKCDEY && c->has_secret && !c->device_keyed) return prepare_lmkcdey(c);
     return CBS_OK;
 }
+
+cbs_status validate_params(const cbs_params& p) { return validate(p); }
 
 }  // namespace cbs
 
@@ -687,6 +695,12 @@ cbs_status cbs_context_set_br_backend(cbs_context* ctx, int backend) {
         ctx->mb_ready = false;
         ctx->h_mbk.clear();
         ctx->d_bskf_mb.reset();
+    }
+    if (backend != CBS_BR_NTT && ctx->br_method == CBS_BR_LMKCDEY) {  // LMKCDEY exists for the NTT form only
+        ctx->br_method = CBS_BR_GINX;
+        ctx->lmk_ready = false;
+        ctx->h_lmk_eval.clear();
+        ctx->h_lmk_auto.clear();
     }
     // captured AES round graphs bake in the kernel choice
     ctx->aes.drop_graphs();

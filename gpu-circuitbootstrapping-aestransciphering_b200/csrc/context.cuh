@@ -98,6 +98,15 @@ struct cbs_context {
     cbs::ChachaKey keygen_key{};
     std::vector<uint64_t> h_mbk;         // grouped keys, NTT domain (kept for export)
     cbs::DevBuf<double2> d_bskf_mb;      // their spectra
+    // LMKCDEY blind rotation (NTT backend): the keys in the NTT domain (kept for export), their
+    // Montgomery-form device copies, the automorphism maps and the discrete-log table
+    int br_method = 0;                   // CBS_BR_GINX or CBS_BR_LMKCDEY
+    uint32_t lmk_num_auto = 0;
+    bool lmk_ready = false;
+    std::vector<uint64_t> h_lmk_eval, h_lmk_auto;
+    cbs::DevBuf<uint64_t> d_lmk_eval, d_lmk_auto;
+    cbs::DevBuf<uint32_t> d_lmk_maps;
+    cbs::DevBuf<int32_t> d_lmk_log;
     cbs::DevBuf<uint64_t> d_pow2, d_pow2s;
     // scratch
     cbs::DevBuf<uint64_t> d_mv, d_rgsw;
@@ -140,6 +149,13 @@ cbs_status upload_host_keys(cbs_context* c);
 cbs_status finish_key_upload(cbs_context* c);
 // the grouped keys of a device-generated key set into c->h_mbk (keygen_device.cu)
 cbs_status device_grouped_keys(cbs_context* c, uint32_t mb);
+// parameter checks of cbs_context_create
+cbs_status validate_params(const cbs_params& p);
+// LMKCDEY (lmkcdey.cu): its keys from the context's secrets when the method is selected and keys
+// exist; the blind rotation into the MV layout of run_blind_rotate (NTT domain)
+cbs_status prepare_lmkcdey(cbs_context* c);
+cbs_status run_blind_rotate_lmkcdey(cbs_context* c, const uint64_t* d_a, const uint64_t* d_b, uint32_t batch,
+                                    uint32_t a_stride, uint64_t* d_mv, cudaStream_t s);
 // blind rotation + HomTrace/SchemeSwitch of the selected backend: LWE -> RGSW rows in the
 // NTT-domain reference layout [batch][num_lut][2][2][N]; d_mv is [batch][num_lut][2][N] scratch
 // FFT HomTrace + SchemeSwitch with the rows converted to the NTT-domain reference layout

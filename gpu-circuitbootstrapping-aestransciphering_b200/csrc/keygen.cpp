@@ -202,6 +202,85 @@ void generate_mb_bsk(const cbs_params& p, const host::NttTables& t, const HostKe
     for (auto& th : pool) th.join();
 }
 
+std::vector<uint32_t> lmkcdey_auto_pows(uint32_t N, uint32_t num_auto_keys) {
+    const uint32_t M = 2 * N;
+    std::vector<uint32_t> pows(1 + num_auto_keys);
+    pows[0] = M - 5;
+    uint64_t v = 1;
+    for (uint32_t i = 1; i <= num_auto_keys; ++i) {
+        v = (v * 5) % M;
+        pows[i] = static_cast<uint32_t>(v);
+    }
+    return pows;
+}
+
+void lmkcdey_auto_maps(uint32_t N, uint32_t num_auto_keys, std::vector<uint32_t>& maps) {
+    uint32_t logn = 0;
+    while ((1u << logn) < N) ++logn;
+    auto brev = [logn](uint32_t x) {
+        uint32_t r = 0;
+        for (uint32_t i = 0; i < logn; ++i) r |= ((x >> i) & 1u) << (logn - 1 - i);
+        return r;
+    };
+    const auto pows = lmkcdey_auto_pows(N, num_auto_keys);
+    maps.assign(pows.size() * N, 0);
+    // slot t holds the evaluation at zeta^(2 brev(t) + 1); psi_k reads the slot of its k-th power
+    for (size_t k = 0; k < pows.size(); ++k)
+        for (uint32_t t = 0; t < N; ++t) {
+            const uint64_t e = 2ull * brev(t) + 1;
+            maps[k * N + t] = brev(static_cast<uint32_t>(((e * pows[k]) & (2ull * N - 1)) >> 1));
+        }
+}
+
+void generate_lmkcdey_keys(const cbs_params& p, const host::NttTables& t, const HostKeys& k, uint32_t num_auto_keys,
+                           uint64_t seed, std::vector<uint64_t>& eval, std::vector<uint64_t>& autok) {
+    const uint32_t N = p.N, n = p.n, dg = p.digits_g, M = 2 * N;
+    int g = 0;
+    while ((1u << g) < p.base_g) ++g;
+    const uint64_t Q = p.Q;
+    FastMod fm(Q);
+    std::vector<uint64_t> gp(dg);
+    for (uint32_t j = 0; j < dg; ++j) gp[j] = (1ull << (g * (j + 1))) % Q;
+    std::vector<uint32_t> maps;
+    lmkcdey_auto_maps(N, num_auto_keys, maps);
+    const uint32_t count = 1 + num_auto_keys;
+    eval.assign(static_cast<size_t>(n) * 2 * dg * 2 * N, 0);
+    autok.assign(static_cast<size_t>(count) * dg * 2 * N, 0);
+    const unsigned nth = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    std::vector<std::thread> pool;
+    for (unsigned th = 0; th < nth; ++th) {
+        pool.emplace_back([&, th] {
+            std::vector<uint64_t> tmp, mono(N);
+            for (uint32_t i = th; i < n; i += nth) {
+                Rng rng(seed ^ (0x9e3779b97f4a7c15ull * (i + 1)));
+                const int64_t e = ((static_cast<int64_t>(k.s_lwe[i]) % M) + M) % M;
+                std::fill(mono.begin(), mono.end(), 0);
+                if (e < N) mono[e] = 1 % Q;
+                else mono[e - N] = Q - 1;
+                ntt_fwd_fast(mono.data(), t);
+                for (uint32_t r = 0; r < 2 * dg; ++r) {
+                    uint64_t* a = eval.data() + (static_cast<size_t>(i) * 2 * dg + r) * 2 * N;
+                    uint64_t* b = a + N;
+                    rlwe_zero(p, t, k, fm, rng, a, b, tmp);
+                    uint64_t* tgt = (r & 1) ? b : a;
+                    for (uint32_t c = 0; c < N; ++c) tgt[c] = fm.add(tgt[c], fm.mul(mono[c], gp[r >> 1]));
+                }
+            }
+            for (uint32_t kk = th; kk < count; kk += nth) {
+                Rng rng(seed ^ 0x6c6d6b6364657921ull ^ (0x9e3779b97f4a7c15ull * (kk + 1)));
+                const uint32_t* map = maps.data() + static_cast<size_t>(kk) * N;
+                for (uint32_t j = 0; j < dg; ++j) {
+                    uint64_t* a = autok.data() + (static_cast<size_t>(kk) * dg + j) * 2 * N;
+                    uint64_t* b = a + N;
+                    rlwe_zero(p, t, k, fm, rng, a, b, tmp);
+                    for (uint32_t c = 0; c < N; ++c) b[c] = fm.sub(b[c], fm.mul(k.s_ntt[map[c]], gp[j]));
+                }
+            }
+        });
+    }
+    for (auto& th : pool) th.join();
+}
+
 void lwe_encrypt(const cbs_params& p, const HostKeys& k, Rng& rng, uint64_t m, uint64_t* out_a, uint64_t* out_b) {
     const uint64_t q = p.q_lwe;
     u128 acc = 0;

@@ -1850,3 +1850,314 @@ void orc_cbs_keygen_chacha_mb(const orc_cbs_params *p, double sigma_rlwe, const 
     free(irp);
     free(rp);
 }
+
+/* ------------------------------------------------------------------------------------------ */
+/* LMKCDEY blind rotation (bitwise/src/cirbts/cirbts-lmkcdey.cu, keys cirbts-init.cu:630-726)   */
+/* ------------------------------------------------------------------------------------------ */
+
+/* automorphism powers of the non-windowed key set (cirbts-lmkcdey.cu:66-103 with window 0):
+ * pows[0] = 2N - 5, pows[i] = 5^i mod 2N for i = 1 .. num_auto_keys; returns the count */
+uint32_t orc_lmkcdey_auto_pows(uint32_t N, uint32_t num_auto_keys, uint32_t *pows) {
+    const uint32_t M = 2 * N;
+    pows[0] = M - 5;
+    uint64_t v = 1;
+    for (uint32_t i = 1; i <= num_auto_keys; ++i) {
+        v = (v * 5) % M;
+        pows[i] = (uint32_t)v;
+    }
+    return 1 + num_auto_keys;
+}
+
+/* NTT-domain permutation of X -> X^k for every power: slot t holds the evaluation at
+ * zeta^(2 brev(t) + 1), so psi_k(p) at slot t is p at the slot of zeta^((2 brev(t) + 1) k);
+ * maps [count][N], out[t] = in[map[t]] as kernel_Permute_Only reads it (kernel.cu:7588) */
+void orc_lmkcdey_auto_maps(uint32_t N, uint32_t num_auto_keys, uint32_t *maps) {
+    uint32_t log_n = 0;
+    while ((1u << log_n) < N) ++log_n;
+    uint32_t *pows = (uint32_t *)malloc(sizeof(uint32_t) * (num_auto_keys + 1));
+    const uint32_t count = orc_lmkcdey_auto_pows(N, num_auto_keys, pows);
+    for (uint32_t k = 0; k < count; ++k)
+        for (uint32_t t = 0; t < N; ++t) {
+            const uint64_t e = 2ull * brev(t, log_n) + 1;
+            const uint32_t idx = (uint32_t)(((e * pows[k]) & (2ull * N - 1)) >> 1);
+            maps[(size_t)k * N + t] = brev(idx, log_n);
+        }
+    free(pows);
+}
+
+/* approximate signed digit idx of x (kernel.cu:887-915): the centred value split into signed
+ * g-bit digits from the least significant end, the first digit dropped */
+static uint64_t lmk_digit(uint64_t x, uint64_t Q, int g, uint32_t idx) {
+    int64_t d = x < (Q >> 1) ? (int64_t)x : (int64_t)x - (int64_t)Q;
+    int64_t r = (int64_t)((uint64_t)d << (64 - g)) >> (64 - g);
+    d = (d - r) >> g;
+    for (uint32_t k = 0; k <= idx; ++k) {
+        r = (int64_t)((uint64_t)d << (64 - g)) >> (64 - g);
+        d = (d - r) >> g;
+    }
+    return r < 0 ? (uint64_t)(r + (int64_t)Q) : (uint64_t)r;
+}
+
+/* LMKCDEY keys from the secrets: eval [n][2 digits_g][2][N] = RGSW(X^{s_i}) with gadget
+ * powers 2^{g (j + 1)} (row 2j carries the message on component a, row 2j + 1 on b);
+ * autok [count][digits_g][2][N] = RLWE(0) with b -= 2^{g (j + 1)} psi_k(s) for every power k
+ * of orc_lmkcdey_auto_pows.  One generator per key: eval key i seeded with
+ * seed ^ (0x9e3779b97f4a7c15 (i + 1)), automorphism key k with
+ * seed ^ 0x6c6d6b6364657921 ^ (0x9e3779b97f4a7c15 (k + 1)). */
+void orc_lmkcdey_keygen(const orc_cbs_params *p, double sigma_rlwe, const int32_t *s_lwe, const int32_t *s_rlwe,
+                        uint32_t num_auto_keys, uint64_t seed, uint64_t *eval, uint64_t *autok) {
+    const uint32_t N = p->N, n = p->n, dg = p->digits_g, M = 2 * N;
+    const int g = __builtin_ctz(p->base_g);
+    const uint64_t Q = p->Q;
+    uint64_t *rp = (uint64_t *)malloc(sizeof(uint64_t) * N), *irp = (uint64_t *)malloc(sizeof(uint64_t) * N);
+    uint64_t ninv[2];
+    orc_ntt_tables(p->log_n, Q, rp, NULL, irp, NULL, ninv);
+    uint64_t *s_ntt = (uint64_t *)malloc(sizeof(uint64_t) * N);
+    for (uint32_t i = 0; i < N; ++i) s_ntt[i] = mod_signed(s_rlwe[i], Q);
+    ntt_fwd_one(s_ntt, N, Q, rp);
+    uint64_t gp[64];
+    for (uint32_t j = 0; j < dg; ++j) {
+        uint64_t v = 1 % Q;
+        for (int e = 0; e < g * (int)(j + 1); ++e) v = addmod(v, v, Q);
+        gp[j] = v;
+    }
+#pragma omp parallel for schedule(dynamic)
+    for (long i = 0; i < (long)n; ++i) {
+        uint64_t *tmp = (uint64_t *)malloc(sizeof(uint64_t) * N), *mono = (uint64_t *)malloc(sizeof(uint64_t) * N);
+        orc_rng r;
+        rng_seed(&r, seed ^ (0x9e3779b97f4a7c15ull * (uint64_t)(i + 1)));
+        const uint32_t e = (uint32_t)(((int64_t)s_lwe[i] % (int64_t)M + (int64_t)M) % (int64_t)M);
+        memset(mono, 0, sizeof(uint64_t) * N);
+        if (e < N) mono[e] = 1 % Q;
+        else mono[e - N] = Q - 1;
+        ntt_fwd_one(mono, N, Q, rp);
+        for (uint32_t row = 0; row < 2 * dg; ++row) {
+            uint64_t *a = eval + ((size_t)i * 2 * dg + row) * 2 * N, *b = a + N;
+            keygen_rlwe_zero(&r, N, Q, sigma_rlwe, rp, s_ntt, a, b, tmp);
+            uint64_t *tgt = (row & 1) ? b : a;
+            for (uint32_t c = 0; c < N; ++c) tgt[c] = addmod(tgt[c], orc_mulmod(mono[c], gp[row >> 1], Q), Q);
+        }
+        free(mono);
+        free(tmp);
+    }
+    const uint32_t count = 1 + num_auto_keys;
+    uint32_t *maps = (uint32_t *)malloc(sizeof(uint32_t) * count * N);
+    orc_lmkcdey_auto_maps(N, num_auto_keys, maps);
+#pragma omp parallel for schedule(dynamic)
+    for (long k = 0; k < (long)count; ++k) {
+        uint64_t *tmp = (uint64_t *)malloc(sizeof(uint64_t) * N);
+        orc_rng r;
+        rng_seed(&r, seed ^ 0x6c6d6b6364657921ull ^ (0x9e3779b97f4a7c15ull * (uint64_t)(k + 1)));
+        const uint32_t *map = maps + (size_t)k * N;
+        for (uint32_t j = 0; j < dg; ++j) {
+            uint64_t *a = autok + ((size_t)k * dg + j) * 2 * N, *b = a + N;
+            keygen_rlwe_zero(&r, N, Q, sigma_rlwe, rp, s_ntt, a, b, tmp);
+            for (uint32_t c = 0; c < N; ++c) b[c] = submod(b[c], orc_mulmod(s_ntt[map[c]], gp[j], Q), Q);
+        }
+        free(tmp);
+    }
+    free(maps);
+    free(s_ntt);
+    free(irp);
+    free(rp);
+}
+
+/* discrete log of odd x in Z_2N to base 5 with sign: w for x = 5^w, -w for x = -5^w (w >= 1),
+ * 2N for x = -1 (the reference's logGen, cirbts-lmkcdey.cu:143-176) */
+static void lmk_log_table(uint32_t N, int32_t *log_tab /* [N], index x >> 1 */) {
+    const uint32_t M = 2 * N, Nh = N / 2;
+    uint64_t v = 1;
+    for (uint32_t w = 0; w < Nh; ++w) {
+        log_tab[v >> 1] = (int32_t)w;
+        const uint32_t neg = (uint32_t)(M - v);
+        log_tab[neg >> 1] = w == 0 ? (int32_t)M : -(int32_t)w;
+        v = (v * 5) % M;
+    }
+}
+
+typedef struct {
+    const orc_cbs_params *p;
+    const uint64_t *eval, *autok;
+    const uint32_t *maps;
+    uint64_t *ct, *dct, *perm0, *perm1, *tmp;
+    const uint64_t *rp, *irp;
+    uint64_t n_inv;
+} lmk_ctx;
+
+/* AddToAccLMKCDEY_GPU (cirbts-lmkcdey.cu:239-259): acc <- acc (x) RGSW(X^{s_j}) */
+static void lmk_add(lmk_ctx *c, uint64_t *acc, uint32_t j) {
+    const orc_cbs_params *p = c->p;
+    const uint32_t N = p->N, dg = p->digits_g;
+    const int g = __builtin_ctz(p->base_g);
+    const uint64_t Q = p->Q;
+    const uint64_t *key = c->eval + (size_t)j * 2 * dg * 2 * N;
+    memcpy(c->ct, acc, sizeof(uint64_t) * 2 * N);
+    ntt_inv_one(c->ct, N, Q, c->irp, c->n_inv);
+    ntt_inv_one(c->ct + N, N, Q, c->irp, c->n_inv);
+    for (uint32_t d = 0; d < dg; ++d)
+        for (uint32_t poly = 0; poly < 2; ++poly) {
+            uint64_t *row = c->dct + (size_t)(2 * d + poly) * N;
+            for (uint32_t i = 0; i < N; ++i) row[i] = lmk_digit(c->ct[poly * N + i], Q, g, d);
+            ntt_fwd_one(row, N, Q, c->rp);
+        }
+    for (uint32_t i = 0; i < N; ++i) {
+        uint64_t s0 = 0, s1 = 0;
+        for (uint32_t r = 0; r < 2 * dg; ++r) {
+            const uint64_t x = c->dct[(size_t)r * N + i];
+            s0 = addmod(s0, orc_mulmod(x, key[(size_t)r * 2 * N + i], Q), Q);
+            s1 = addmod(s1, orc_mulmod(x, key[(size_t)r * 2 * N + N + i], Q), Q);
+        }
+        acc[i] = s0;
+        acc[N + i] = s1;
+    }
+}
+
+/* AutomorphismLMKCDEY_GPU (cirbts-lmkcdey.cu:261-292): acc <- key switch of psi_k(acc) */
+static void lmk_auto(lmk_ctx *c, uint64_t *acc, uint32_t k) {
+    const orc_cbs_params *p = c->p;
+    const uint32_t N = p->N, dg = p->digits_g;
+    const int g = __builtin_ctz(p->base_g);
+    const uint64_t Q = p->Q;
+    const uint32_t *map = c->maps + (size_t)k * N;
+    const uint64_t *key = c->autok + (size_t)k * dg * 2 * N;
+    for (uint32_t i = 0; i < N; ++i) {
+        c->perm1[i] = acc[N + map[i]];
+        c->perm0[i] = acc[map[i]];
+    }
+    ntt_inv_one(c->perm0, N, Q, c->irp, c->n_inv);
+    for (uint32_t d = 0; d < dg; ++d) {
+        uint64_t *row = c->dct + (size_t)d * N;
+        for (uint32_t i = 0; i < N; ++i) row[i] = lmk_digit(c->perm0[i], Q, g, d);
+        ntt_fwd_one(row, N, Q, c->rp);
+    }
+    for (uint32_t i = 0; i < N; ++i) {
+        uint64_t s0 = 0, s1 = 0;
+        for (uint32_t d = 0; d < dg; ++d) {
+            const uint64_t x = c->dct[(size_t)d * N + i];
+            s0 = addmod(s0, orc_mulmod(x, key[(size_t)d * 2 * N + i], Q), Q);
+            s1 = addmod(s1, orc_mulmod(x, key[(size_t)d * 2 * N + N + i], Q), Q);
+        }
+        acc[i] = s0;
+        acc[N + i] = addmod(c->perm1[i], s1, Q);
+    }
+}
+
+/* LMKCDEY_EvalAcc (cirbts-lmkcdey.cu:105-407, window 0) on acc [2][N] (NTT domain, in place):
+ * a_neg [n] the masks mod 2N as the reference's EvalAcc receives them (negated by the caller,
+ * cirbts-bootstrap.cu:681-689).  The LWE coefficients are bucketed by the signed base-5
+ * logarithm of the odd residue (-a_neg) | 1, then processed bucket by bucket with
+ * automorphisms between them. */
+void orc_lmkcdey_eval_acc(const orc_cbs_params *p, const uint64_t *eval, const uint64_t *autok, const uint32_t *maps,
+                          uint32_t num_auto_keys, const uint32_t *a_neg, uint32_t n, uint64_t *acc) {
+    const uint32_t N = p->N, Nh = N / 2, M = 2 * N, mask = M - 1, buckets = 2 * Nh, dg = p->digits_g;
+    uint64_t *rp = (uint64_t *)malloc(sizeof(uint64_t) * N), *irp = (uint64_t *)malloc(sizeof(uint64_t) * N);
+    uint64_t ninv[2];
+    orc_ntt_tables(p->log_n, p->Q, rp, NULL, irp, NULL, ninv);
+    int32_t *log_tab = (int32_t *)malloc(sizeof(int32_t) * N);
+    lmk_log_table(N, log_tab);
+    uint32_t *bucket = (uint32_t *)malloc(sizeof(uint32_t) * (n ? n : 1));
+    uint32_t *offs = (uint32_t *)calloc(buckets + 1, sizeof(uint32_t));
+    uint32_t *cur = (uint32_t *)malloc(sizeof(uint32_t) * (buckets + 1));
+    uint32_t *items = (uint32_t *)malloc(sizeof(uint32_t) * (n ? n : 1));
+    for (uint32_t i = 0; i < n; ++i) {
+        const uint32_t odd = ((0u - a_neg[i]) & mask) | 1u;
+        const int32_t idx = log_tab[odd >> 1];
+        bucket[i] = idx == (int32_t)M ? buckets - 1 : (uint32_t)(idx + (int32_t)(Nh - 1));
+        ++offs[bucket[i] + 1];
+    }
+    for (uint32_t b = 0; b < buckets; ++b) offs[b + 1] += offs[b];
+    memcpy(cur, offs, sizeof(uint32_t) * (buckets + 1));
+    for (uint32_t i = 0; i < n; ++i) items[cur[bucket[i]]++] = i;
+
+    lmk_ctx c;
+    c.p = p;
+    c.eval = eval;
+    c.autok = autok;
+    c.maps = maps;
+    c.rp = rp;
+    c.irp = irp;
+    c.n_inv = ninv[0];
+    c.ct = (uint64_t *)malloc(sizeof(uint64_t) * 2 * N);
+    c.dct = (uint64_t *)malloc(sizeof(uint64_t) * 2 * dg * N);
+    c.perm0 = (uint64_t *)malloc(sizeof(uint64_t) * N);
+    c.perm1 = (uint64_t *)malloc(sizeof(uint64_t) * N);
+    c.tmp = NULL;
+
+    /* acc1 = psi_{2N-5}(acc1) without key switching (the mask is 0) */
+    for (uint32_t i = 0; i < N; ++i) c.perm1[i] = acc[N + maps[i]];
+    memcpy(acc + N, c.perm1, sizeof(uint64_t) * N);
+    for (int half = 0; half < 2; ++half) {
+        /* half 0: a = -5^i (buckets 0 .. Nh-2), half 1: a = 5^i (buckets 2Nh-2 .. Nh) */
+        uint32_t skips = 0;
+        for (uint32_t i = Nh - 1; i > 0; --i) {
+            const uint32_t b = half == 0 ? (Nh - 1) - i : (Nh - 1) + i;
+            if (offs[b] != offs[b + 1]) {
+                if (skips != 0) {
+                    lmk_auto(&c, acc, skips);
+                    skips = 0;
+                }
+                for (uint32_t pos = offs[b]; pos < offs[b + 1]; ++pos) lmk_add(&c, acc, items[pos]);
+            }
+            ++skips;
+            if (skips == num_auto_keys || i == 1) {
+                lmk_auto(&c, acc, skips);
+                skips = 0;
+            }
+        }
+        if (half == 0) {
+            /* a = -1, then psi_{2N-5} */
+            for (uint32_t pos = offs[buckets - 1]; pos < offs[buckets]; ++pos) lmk_add(&c, acc, items[pos]);
+            lmk_auto(&c, acc, 0);
+        } else {
+            /* a = 1 */
+            for (uint32_t pos = offs[Nh - 1]; pos < offs[Nh]; ++pos) lmk_add(&c, acc, items[pos]);
+        }
+    }
+    free(c.ct);
+    free(c.dct);
+    free(c.perm0);
+    free(c.perm1);
+    free(items);
+    free(cur);
+    free(offs);
+    free(bucket);
+    free(log_tab);
+    free(irp);
+    free(rp);
+}
+
+/* the circuit-bootstrapping blind rotation with the LMKCDEY accumulator
+ * (cirbts-bootstrap.cu:600-720 with method LMKCDEY): acc = (0, X^{-b~} TV) with the special
+ * mod switch of b, the masks rounded to Z_2N (the reference passes them unswitched, which is
+ * the same when q_lwe = 2N) and negated, LMKCDEY_EvalAcc (which rounds them to odd), then the
+ * finalize of the GINX form.  acc_out [batch][2][N] NTT domain. */
+void orc_blind_rotate_lmkcdey(const orc_cbs_params *p, const orc_cbs_keys *k, const uint64_t *eval,
+                              const uint64_t *autok, const uint32_t *maps, uint32_t num_auto_keys, const uint64_t *a,
+                              const uint64_t *b, uint32_t batch, uint32_t a_stride, uint64_t *acc_out, int finalize) {
+    const uint32_t N = p->N, twoN = 2 * N;
+    const uint64_t Q = p->Q;
+    const uint32_t bw = (p->num_lut <= 1) ? 0 : (uint32_t)(32 - __builtin_clz(p->num_lut - 1));
+#pragma omp parallel for schedule(dynamic, 1)
+    for (long bi = 0; bi < (long)batch; ++bi) {
+        uint64_t *acc = acc_out + (size_t)bi * 2 * N;
+        const uint64_t *arow = a + (size_t)bi * a_stride;
+        uint32_t *a_neg = (uint32_t *)malloc(sizeof(uint32_t) * (p->n ? p->n : 1));
+        for (uint32_t i = 0; i < p->n; ++i) a_neg[i] = (twoN - orc_special_ms(arow[i], twoN, p->q_lwe, 0)) & (twoN - 1);
+        const uint32_t bt = orc_special_ms(b[bi], twoN, p->q_lwe, bw);
+        memset(acc, 0, sizeof(uint64_t) * N);
+        rotate_neg(acc + N, k->tv, bt, N, Q);
+        ntt_fwd_one(acc + N, N, Q, k->rp);
+        orc_lmkcdey_eval_acc(p, eval, autok, maps, num_auto_keys, a_neg, p->n, acc);
+        free(a_neg);
+        if (finalize) {
+            const uint64_t ninv = orc_invmod(N, Q);
+            for (uint32_t c = 0; c < 2 * N; ++c) acc[c] = orc_mulmod(acc[c], ninv, Q);
+            ntt_inv_one(acc, N, Q, k->irp, k->n_inv);
+            ntt_inv_one(acc + N, N, Q, k->irp, k->n_inv);
+            for (uint32_t j = 0; j < p->num_lut; ++j)
+                acc[N + j] = addmod(acc[N + j], orc_mulmod(k->gpow[j] >> 1, ninv, Q), Q);
+            ntt_fwd_one(acc, N, Q, k->rp);
+            ntt_fwd_one(acc + N, N, Q, k->rp);
+        }
+    }
+}

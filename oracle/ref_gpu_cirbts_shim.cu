@@ -178,6 +178,104 @@ int ref_cirbts_blind_rotate_mb4(uint64_t* acc, const uint64_t* d_a, uint32_t a_s
     return static_cast<int>(e);
 }
 
+// LMKCDEY_EvalAcc (bitwise/src/cirbts/cirbts-lmkcdey.cu:105-407, window 0) of one ciphertext
+// in the reference's launch sequence, over the reference's own kernels: the bucket CSR built
+// on the host from the signed base-5 logarithms of (-a) | 1, kernel_Permute_Only for the
+// automorphisms, inwt/fnwt_1d_opt_batched, kernel_SignedDigitDecomposeLMKCDEY_Ciphertext /
+// _Poly (first digit dropped), kernel_MultAdd and kernel_AddInPlace.  acc [2][N] device, NTT
+// domain, updated in place; h_a [n] host, the masks mod 2N as EvalAcc receives them; eval
+// [n][2 digits][2][N], autok [1 + num_auto_keys][digits][2][N] (NTT domain), maps
+// [1 + num_auto_keys][N] device; digits is the reference's digitsG - 1.  Scratch is
+// allocated once per call; returns the CUDA error code.
+int ref_cirbts_lmkcdey_eval_acc(uint64_t* acc, const uint32_t* h_a, uint32_t n, const uint64_t* eval,
+                                const uint64_t* autok, const uint32_t* maps, uint32_t num_auto_keys, const void* d_mod,
+                                const uint64_t* tw, const uint64_t* tws, const uint64_t* itw, const uint64_t* itws,
+                                const uint64_t* ninv, const uint64_t* ninv_s, uint32_t N, uint64_t Q, uint32_t base_g,
+                                uint32_t digits, void* stream) {
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const DModulus* mod = static_cast<const DModulus*>(d_mod);
+    const uint32_t Nh = N / 2, M = 2 * N, mask = M - 1, buckets = 2 * Nh, digits2 = 2 * digits;
+    // signed base-5 logarithms of the odd residues (the reference's logGen)
+    std::vector<int32_t> log_gen(M, 0);
+    {
+        uint64_t v = 1;
+        for (uint32_t w = 0; w < Nh; ++w) {
+            log_gen[v] = static_cast<int32_t>(w);
+            log_gen[M - v] = w == 0 ? static_cast<int32_t>(M) : -static_cast<int32_t>(w);
+            v = (v * 5) % M;
+        }
+    }
+    std::vector<uint32_t> bucket_of(n), offsets(buckets + 1, 0), items(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        const uint32_t odd = ((0u - (h_a[i] & mask)) & mask) | 1u;
+        const int32_t index = log_gen[odd];
+        bucket_of[i] = index == static_cast<int32_t>(M) ? buckets - 1 : static_cast<uint32_t>(index + (int32_t)(Nh - 1));
+        ++offsets[bucket_of[i] + 1];
+    }
+    for (uint32_t b = 0; b < buckets; ++b) offsets[b + 1] += offsets[b];
+    {
+        std::vector<uint32_t> cursor(offsets);
+        for (uint32_t i = 0; i < n; ++i) items[cursor[bucket_of[i]]++] = i;
+    }
+    uint64_t *ct = nullptr, *dct = nullptr, *pc0 = nullptr, *pc1 = nullptr, *dcta = nullptr, *ks0 = nullptr,
+             *ks1 = nullptr;
+    cudaError_t e = cudaSuccess;
+    for (auto bp : {std::make_pair(&ct, 2 * N), std::make_pair(&dct, digits2 * N), std::make_pair(&pc0, N),
+                    std::make_pair(&pc1, N), std::make_pair(&dcta, digits * N), std::make_pair(&ks0, N),
+                    std::make_pair(&ks1, N)})
+        if (e == cudaSuccess) e = cudaMalloc(bp.first, sizeof(uint64_t) * bp.second);
+    const dim3 block(256), grid((N + 255) / 256);
+    const size_t eval_stride = static_cast<size_t>(digits2) * 2 * N, auto_stride = static_cast<size_t>(digits) * 2 * N;
+    auto add_to_acc = [&](uint32_t j) {
+        cudaMemcpyAsync(ct, acc, 2 * N * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s);
+        inwt_1d_opt_batched(ct, itw, itws, mod, ninv, ninv_s, N, 2, s);
+        kernel_SignedDigitDecomposeLMKCDEY_Ciphertext<<<grid, block, 0, s>>>(dct, ct, Q, base_g, digits2, N);
+        fnwt_1d_opt_batched(dct, tw, tws, mod, N, digits2, s);
+        kernel_MultAdd<<<grid, block, 0, s>>>(acc, acc + N, dct, eval + j * eval_stride, mod, digits2, N, 1);
+    };
+    auto automorphism = [&](uint32_t k) {
+        const uint32_t* map = maps + static_cast<size_t>(k) * N;
+        kernel_Permute_Only<<<grid, block, 0, s>>>(pc1, acc + N, map, N, 1, Q);
+        kernel_Permute_Only<<<grid, block, 0, s>>>(pc0, acc, map, N, 1, Q);
+        cudaMemcpyAsync(acc + N, pc1, N * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s);
+        inwt_1d_opt_batched(pc0, itw, itws, mod, ninv, ninv_s, N, 1, s);
+        kernel_SignedDigitDecomposeLMKCDEY_Poly<<<grid, block, 0, s>>>(dcta, pc0, Q, base_g, digits, N);
+        fnwt_1d_opt_batched(dcta, tw, tws, mod, N, digits, s);
+        kernel_MultAdd<<<grid, block, 0, s>>>(ks0, ks1, dcta, autok + k * auto_stride, mod, digits, N, 1);
+        cudaMemcpyAsync(acc, ks0, N * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s);
+        kernel_AddInPlace<<<grid, block, 0, s>>>(acc + N, ks1, mod, N);
+    };
+    if (e == cudaSuccess) {
+        kernel_Permute_Only<<<grid, block, 0, s>>>(pc1, acc + N, maps, N, 1, Q);
+        cudaMemcpyAsync(acc + N, pc1, N * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s);
+        for (int half = 0; half < 2; ++half) {
+            uint32_t skips = 0;
+            for (uint32_t i = Nh - 1; i > 0; --i) {
+                const uint32_t b = half == 0 ? (Nh - 1) - i : (Nh - 1) + i;
+                if (offsets[b] != offsets[b + 1]) {
+                    if (skips != 0) {
+                        automorphism(skips);
+                        skips = 0;
+                    }
+                    for (uint32_t pos = offsets[b]; pos < offsets[b + 1]; ++pos) add_to_acc(items[pos]);
+                }
+                ++skips;
+                if (skips == num_auto_keys || i == 1) {
+                    automorphism(skips);
+                    skips = 0;
+                }
+            }
+            const uint32_t sb = half == 0 ? buckets - 1 : Nh - 1;
+            for (uint32_t pos = offsets[sb]; pos < offsets[sb + 1]; ++pos) add_to_acc(items[pos]);
+            if (half == 0) automorphism(0);
+        }
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    }
+    for (uint64_t* b : {ct, dct, pc0, pc1, dcta, ks0, ks1}) cudaFree(b);
+    return static_cast<int>(e);
+}
+
 // N-major index positions [n][batch] of the LWE masks (kernel_SpecialMS_IndexPos_Batch_NMajor,
 // the layout CIRBTS_BATCH_INDEX_NMAJOR=1 selects), into caller memory.
 int ref_cirbts_index_nmajor(const uint64_t* d_a, uint32_t a_stride, uint32_t n, uint32_t batch, uint32_t N,

@@ -75,6 +75,20 @@ class OracleCbs:
                                    b.ctypes.data, batch, stride, out.ctypes.data, 1)
         return out
 
+    def br_acc_lmkcdey(self, a: np.ndarray, b: np.ndarray, lmk: dict, finalize: bool = True) -> np.ndarray:
+        """LMKCDEY blind rotation [batch][2][N] (NTT domain) with the keys and maps of
+        oracle_lmkcdey_keys."""
+        vp, u32 = ctypes.c_void_p, ctypes.c_uint32
+        self.o.orc_blind_rotate_lmkcdey.argtypes = [vp, vp, vp, vp, vp, u32, vp, vp, u32, u32, vp, ctypes.c_int]
+        batch, stride = a.shape
+        a = np.ascontiguousarray(a, np.uint64)
+        b = np.ascontiguousarray(b, np.uint64)
+        out = np.zeros((batch, 2, self.p.N), np.uint64)
+        self.o.orc_blind_rotate_lmkcdey(ctypes.byref(self.op), ctypes.byref(self.ok), lmk["eval"].ctypes.data,
+                                        lmk["auto"].ctypes.data, lmk["maps"].ctypes.data, lmk["num_auto_keys"],
+                                        a.ctypes.data, b.ctypes.data, batch, stride, out.ctypes.data, int(finalize))
+        return out
+
     def br_mv(self, a: np.ndarray, b: np.ndarray) -> np.ndarray:
         batch, stride = a.shape
         out = np.zeros((batch, self.p.num_lut, 2, self.p.N), np.uint64)
@@ -203,6 +217,29 @@ def oracle_keys_mb(oracle, p, keys: dict, mb: int, seed: int) -> np.ndarray:
     oracle.orc_cbs_keygen_mb(ctypes.byref(op), p.sigma_rlwe, s_lwe.ctypes.data, s_rlwe.ctypes.data, mb,
                              seed ^ MB_SEED_TWEAK, out.ctypes.data)
     return out
+
+
+LMK_SEED_TWEAK = 0x6C6D6B6365797331  # the LMKCDEY keys' generator seed is the key seed xor this
+
+
+def oracle_lmkcdey_keys(oracle, p, keys: dict, num_auto_keys: int, seed: int) -> dict:
+    """LMKCDEY keys of a key set from the oracle, seeded as a context keyed with `seed` seeds
+    them: eval [n][2 digits_g][2][N], auto [1 + num_auto_keys][digits_g][2][N] (NTT domain), and
+    the NTT-domain automorphism maps [1 + num_auto_keys][N]."""
+    vp, u32 = ctypes.c_void_p, ctypes.c_uint32
+    oracle.orc_lmkcdey_keygen.argtypes = [vp, ctypes.c_double, vp, vp, u32, ctypes.c_uint64, vp, vp]
+    oracle.orc_lmkcdey_auto_maps.argtypes = [u32, u32, vp]
+    count = 1 + num_auto_keys
+    ev = np.zeros((p.n, 2 * p.digits_g, 2, p.N), np.uint64)
+    au = np.zeros((count, p.digits_g, 2, p.N), np.uint64)
+    maps = np.zeros((count, p.N), np.uint32)
+    op = orc_params(p)
+    s_lwe = np.ascontiguousarray(keys["s_lwe"], np.int32)
+    s_rlwe = np.ascontiguousarray(keys["s_rlwe"], np.int32)
+    oracle.orc_lmkcdey_keygen(ctypes.byref(op), p.sigma_rlwe, s_lwe.ctypes.data, s_rlwe.ctypes.data, num_auto_keys,
+                              seed ^ LMK_SEED_TWEAK, ev.ctypes.data, au.ctypes.data)
+    oracle.orc_lmkcdey_auto_maps(p.N, num_auto_keys, maps.ctypes.data)
+    return {"eval": ev, "auto": au, "maps": maps, "num_auto_keys": num_auto_keys}
 
 
 # a fixed ChaCha20 key for reproducible key-generation tests

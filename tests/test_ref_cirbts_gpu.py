@@ -8,7 +8,9 @@ sequences (ref_gpu_cirbts_shim.cu):
   from the same initial accumulator, n = 630 steps give the oracle's accumulator word for word;
   likewise the grouped mb = 2 sequence (kernel_EvalAccCore_Binary_MB2_Grouped_Batch), the staged
   mb = 4 sequence (MB3 grouped kernel, then a one-key step) and the AES example's mb = 3 SoA
-  sequence against the oracle's exact grouped rotation;
+  sequence against the oracle's exact grouped rotation; and LMKCDEY_EvalAcc
+  (cirbts-lmkcdey.cu:105-407: host buckets, kernel_Permute_Only, the LMKCDEY decompositions,
+  kernel_MultAdd, kernel_AddInPlace) against the oracle's LMKCDEY accumulator;
 * HomTrace + SchemeSwitch: kernel_GenerateCoefficientAutoMaps, per round the permuting INTT,
   kernel_Fused_Permute_Decompose, the NTT and kernel_MultAddUpdate_HT_PermuteC1, then
   kernel_MultAddUpdate_SS and kernel_SaveToRGSW: the oracle's RGSW rows word for word, and the
@@ -276,3 +278,45 @@ def test_grouped_mb3_soa_matches_reference_kernels(pkg, oracle, ref, preset):
     got = dev["acc"].cpu().numpy().view(np.uint64).reshape(batch, 2, N)
     assert not np.array_equal(got, init)
     assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("num_auto", [10, 1])
+def test_lmkcdey_eval_acc_matches_reference_kernels(pkg, oracle, ref, num_auto):
+    """LMKCDEY_EvalAcc in the reference's launch sequence over its own kernels, with the
+    product's LMKCDEY keys and maps, reproduces the oracle's accumulator word for word (the
+    product's kernel equals the oracle: tests/test_lmkcdey_gpu.py)."""
+    from cbs_harness import oracle_lmkcdey_keys
+    vp, u32, u64 = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64
+    ref.ref_cirbts_lmkcdey_eval_acc.argtypes = [vp, vp, u32, vp, vp, vp, u32, vp, vp, vp, vp, vp, vp, vp, u32, u64,
+                                                u32, u32, vp]
+    ref.ref_cirbts_lmkcdey_eval_acc.restype = ctypes.c_int
+    oracle.orc_lmkcdey_eval_acc.argtypes = [vp, vp, vp, vp, u32, vp, u32, vp]
+    p = pkg.preset_params("2x18")
+    p.num_lut = 1
+    N, n, Q = p.N, p.n, p.Q
+    keys = pkg.generate_keys_host(p, 61)
+    lmk = oracle_lmkcdey_keys(oracle, p, keys, num_auto, 61)
+    oc = OracleCbs(oracle, p, keys)
+    tabs, ninv, dmod = _tables(pkg, N, Q)
+    rng = np.random.default_rng(num_auto + 5)
+    dev = {name: _dev(v) for name, v in [("eval", lmk["eval"]), ("auto", lmk["auto"]), ("mod", dmod),
+                                         ("tw", tabs[0]), ("tws", tabs[1]), ("itw", tabs[2]), ("itws", tabs[3]),
+                                         ("ninv", ninv)]}
+    d_maps = torch.from_numpy(lmk["maps"].view(np.int32)).cuda()
+    for trial in range(2):
+        acc = rng.integers(0, Q, size=(2, N), dtype=np.uint64)
+        a_neg = np.ascontiguousarray(rng.integers(0, 2 * N, size=n, dtype=np.uint32))
+        want = acc.copy()
+        oracle.orc_lmkcdey_eval_acc(ctypes.byref(oc.op), lmk["eval"].ctypes.data, lmk["auto"].ctypes.data,
+                                    lmk["maps"].ctypes.data, num_auto, a_neg.ctypes.data, n, want.ctypes.data)
+        d_acc = _dev(acc)
+        st = ref.ref_cirbts_lmkcdey_eval_acc(
+            d_acc.data_ptr(), a_neg.ctypes.data, n, dev["eval"].data_ptr(), dev["auto"].data_ptr(), d_maps.data_ptr(),
+            num_auto, dev["mod"].data_ptr(), dev["tw"].data_ptr(), dev["tws"].data_ptr(), dev["itw"].data_ptr(),
+            dev["itws"].data_ptr(), dev["ninv"].data_ptr(), dev["ninv"].data_ptr() + 8, N, Q, p.base_g, p.digits_g,
+            None)
+        torch.cuda.synchronize()
+        assert st == 0
+        got = d_acc.cpu().numpy().view(np.uint64).reshape(2, N)
+        assert not np.array_equal(got, acc)
+        assert np.array_equal(got, want), trial

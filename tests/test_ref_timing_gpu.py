@@ -13,6 +13,7 @@ split, which the product's includes).
 from __future__ import annotations
 
 import ctypes
+import time
 
 import numpy as np
 import pytest
@@ -440,3 +441,89 @@ def test_modup_moddown_timing_beside_reference_rns_tool(pkg):
     print(f"\nN = 2^16, {size_q} + {size_p} primes, {count} ciphertexts (modup) / {polys} polynomials (moddown):\n"
           f"  modup            product {t_up:7.2f} ms, reference DRNSTool {r_up:7.2f} ms ({r_up / t_up:.2f}x)\n"
           f"  moddown_from_NTT product {t_dn:7.2f} ms, reference DRNSTool {r_dn:7.2f} ms ({r_dn / t_dn:.2f}x)")
+
+
+def test_lmkcdey_timing_beside_reference_kernels(pkg):
+    """The LMKCDEY accumulator (EvalAcc; N = 2048, n = 630, 2^18 x 2 gadget with the first digit
+    dropped, 10 automorphism keys): the product's k_lmkcdey, one CTA per ciphertext over a batch,
+    against the reference's LMKCDEY_EvalAcc sequence over its own kernels, one ciphertext per call
+    as the reference runs it (ref_gpu_cirbts_shim.cu; its call allocates its scratch and builds the
+    buckets on the host).  Both start from the same accumulator and masks and must agree."""
+    if not REF_SO.exists():
+        pytest.skip("reference CirBTS kernels not built (make -C oracle ref_gpu_cirbts)")
+    ref = ctypes.CDLL(str(REF_SO))
+    vp, u32, u64 = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64
+    ref.ref_cirbts_lmkcdey_eval_acc.argtypes = [vp, vp, u32, vp, vp, vp, u32, vp, vp, vp, vp, vp, vp, vp, u32, u64,
+                                                u32, u32, vp]
+    ref.ref_cirbts_lmkcdey_eval_acc.restype = ctypes.c_int
+    num_auto, batch = 10, 1184
+    p = pkg.preset_params("2x18")
+    p.num_lut = 1
+    N, n, Q = p.N, p.n, p.Q
+    ctx = pkg.Context(params=p, max_batch=batch)
+    try:
+        ctx.keygen(71)
+        ctx.set_br_method(pkg.BR_LMKCDEY, num_auto)
+        ev, au = ctx.export_lmkcdey_keys()
+        rng = np.random.default_rng(8)
+        acc = rng.integers(0, Q, size=(batch, 2, N), dtype=np.uint64)
+        a_neg = rng.integers(0, 2 * N, size=(batch, n), dtype=np.uint32)
+        d_acc0 = _dev(acc)
+        d_acc = d_acc0.clone()
+        d_a = torch.from_numpy(a_neg.view(np.int32)).cuda()
+
+        def ours():
+            d_acc.copy_(d_acc0)
+            pkg.call("cbs_lmkcdey_eval_acc_batch_device", ctx.handle, d_a.data_ptr(), n, d_acc.data_ptr(), batch, None)
+
+        ms_ours = _time_ms(ours, reps=2)
+        got = d_acc.cpu().numpy().view(np.uint64).reshape(batch, 2, N)
+        # the whole bootstrapping rotation (bootstrap form, finalize and MV output), LMKCDEY and
+        # the exact GINX one-bit form on the same parameters
+        la = rng.integers(0, p.q_lwe, size=(batch, n), dtype=np.uint64)
+        lb = rng.integers(0, p.q_lwe, batch, dtype=np.uint64)
+        dla, dlb = _dev(la), _dev(lb)
+        mv = torch.empty((batch, p.num_lut, 2, N), dtype=torch.int64, device="cuda")
+
+        def rotate():
+            pkg.call("cbs_blind_rotate_batch_device", ctx.handle, dla.data_ptr(), dlb.data_ptr(), batch, n,
+                     mv.data_ptr(), None)
+
+        ms_br_lmk = _time_ms(rotate, reps=2)
+        ctx.set_br_method(pkg.BR_GINX, 0)
+        ms_br_ginx = _time_ms(rotate, reps=2)
+        ctx.set_br_method(pkg.BR_LMKCDEY, num_auto)
+
+        tabs = [np.zeros(N, np.uint64) for _ in range(4)]
+        ninv = np.zeros(2, np.uint64)
+        dm = pkg.DModulus()
+        pkg.call("cbs_ntt_tables_host", N, Q, *(t.ctypes.data for t in tabs), ninv.ctypes.data, ctypes.addressof(dm))
+        dmod = np.array([dm.value, dm.const_ratio[0], dm.const_ratio[1]], np.uint64)
+        maps = pkg.lmkcdey_auto_maps_host(N, num_auto)
+        dv = {nm: _dev(v) for nm, v in [("ev", ev), ("au", au), ("mod", dmod), ("tw", tabs[0]), ("tws", tabs[1]),
+                                        ("itw", tabs[2]), ("itws", tabs[3]), ("ninv", ninv)]}
+        d_maps = torch.from_numpy(maps.view(np.int32)).cuda()
+        reps = 2
+        r_acc = [_dev(acc[i]) for i in range(reps)]
+        rows = [np.ascontiguousarray(a_neg[i]) for i in range(reps)]
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for i in range(reps):
+            st = ref.ref_cirbts_lmkcdey_eval_acc(
+                r_acc[i].data_ptr(), rows[i].ctypes.data, n, dv["ev"].data_ptr(), dv["au"].data_ptr(),
+                d_maps.data_ptr(), num_auto, dv["mod"].data_ptr(), dv["tw"].data_ptr(), dv["tws"].data_ptr(),
+                dv["itw"].data_ptr(), dv["itws"].data_ptr(), dv["ninv"].data_ptr(), dv["ninv"].data_ptr() + 8, N, Q,
+                p.base_g, p.digits_g, None)
+            assert st == 0
+        torch.cuda.synchronize()
+        ms_ref = (time.perf_counter() - t0) * 1e3 / reps
+        for i in range(reps):
+            assert np.array_equal(r_acc[i].cpu().numpy().view(np.uint64).reshape(2, N), got[i]), i
+    finally:
+        ctx.close()
+    print(f"\nLMKCDEY EvalAcc, 2x18, N = 2048, n = 630, 10 automorphism keys, one B200 (us per ciphertext):")
+    print(f"  product k_lmkcdey, batch {batch:5d}          {ms_ours * 1e3 / batch:9.1f}")
+    print(f"  reference kernels, one per call          {ms_ref * 1e3:9.1f}")
+    print(f"whole blind rotation (finalize, MV output), same parameters, batch {batch} (us per ciphertext):")
+    print(f"  product LMKCDEY                          {ms_br_lmk * 1e3 / batch:9.1f}")
+    print(f"  product exact NTT GINX, one-bit          {ms_br_ginx * 1e3 / batch:9.1f}")
