@@ -150,6 +150,25 @@ class GPUCirBTSContext {
     // KeyGen + RLWEKeyGen + CirBTKeyGen + KeySwitchGen of the example, from a seed
     void KeyGen(uint64_t seed) { check(cbs_keygen(ctx_, seed), "KeyGen"); }
 
+    // The context's BINFHE_METHOD (GenerateCirBTSContext(paramset, GINX | LMKCDEY),
+    // cirbts-init.cu:630-726): CBS_BR_GINX or CBS_BR_LMKCDEY with automorphism keys for 2N - 5 and
+    // 5^1 .. 5^numAutoKeys; the LMKCDEY keys follow the context's secrets
+    void SetMethod(int method, uint32_t numAutoKeys = 10) {
+        check(cbs_context_set_br_method(ctx_, method, numAutoKeys), "SetMethod");
+    }
+    // cirbts.cuh:491 LMKCDEY_EvalAcc(params, a, d_acc): a [n] on the host, the masks mod 2N as the
+    // bootstrap passes them (negated), d_acc [2][N] on the device (NTT domain), updated in place
+    void LMKCDEY_EvalAcc(const std::vector<uint32_t>& a, uint64_t* d_acc) {
+        if (a.size() != params_.n)
+            throw Error(CBS_ERR_SHAPE_MISMATCH, "LMKCDEY_EvalAcc: a must hold n masks");
+        stage_a_.resize(a.size());
+        const cudaStream_t s = stream();
+        check_cuda(cudaMemcpyAsync(stage_a_.data(), a.data(), a.size() * 4, cudaMemcpyHostToDevice, s), "stage a");
+        check(cbs_lmkcdey_eval_acc_batch_device(ctx_, stage_a_.data(), params_.n, d_acc, 1, as_stream(s)),
+              "LMKCDEY_EvalAcc");
+        check_cuda(cudaStreamSynchronize(s), "LMKCDEY_EvalAcc");  // the staged masks are reused
+    }
+
     [[nodiscard]] const cbs_dmodulus* d_modulus() const { return table(0); }
     [[nodiscard]] const uint64_t* d_twiddles() const { return tab64(1); }
     [[nodiscard]] const uint64_t* d_twiddles_shoup() const { return tab64(2); }
@@ -250,6 +269,7 @@ class GPUCirBTSContext {
     uint32_t max_batch_;
     cbs_context* ctx_ = nullptr;
     DeviceArray<uint64_t> stage_;
+    DeviceArray<uint32_t> stage_a_;
 };
 
 // ---- Phantom RNS core (include/context.cuh:161, include/ntt.cuh:232-262,

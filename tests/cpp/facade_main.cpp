@@ -10,6 +10,9 @@
 //         cbs_a, cbs_b -> cbs_out (the batch's RGSW rows)
 //   gate  GPUBinFHEContext::BatchGPUEvalBinGate(NAND): exit status 0 when every gate decrypts to
 //         the truth table
+//   lmk   GPUCirBTSContext with SetMethod(LMKCDEY): gpu_CircuitBootstrappingBatch on the 2^18 x 2
+//         preset with one LUT slot, and LMKCDEY_EvalAcc on a given accumulator: lmk_dims (seed
+//         batch num_auto_keys), lmk_a, lmk_b, lmk_acc, lmk_masks -> lmk_cbs_out, lmk_acc_out
 //   ckks  the CKKS evaluator: multiply_and_relin_inplace then rescale_to_next_inplace of ct1 by
 //         ct2, and rotate_inplace of ct1 by one step: ck_dims (N size_q size_p chain_index beta
 //         galois_elt), ck_chain, ck_ct1, ck_ct2, ck_rk, ck_gk -> ck_mr, ck_rot
@@ -110,6 +113,40 @@ static int run_cbs(const std::string& dir) {
     return 0;
 }
 
+static int run_lmk(const std::string& dir) {
+    const auto dims = read_raw<uint64_t>(dir + "/lmk_dims");
+    const uint64_t seed = dims[0];
+    const uint32_t batch = static_cast<uint32_t>(dims[1]), num_auto = static_cast<uint32_t>(dims[2]);
+    cbs_params params{};
+    check(cbs_params_preset(CBS_PARAMS_AES_2X18, &params), "params");
+    params.num_lut = 1;
+    GPUCirBTSContext cc(params, batch);
+    cc.SetMethod(CBS_BR_LMKCDEY, num_auto);
+    cc.KeyGen(seed);
+    const auto a = read_raw<uint64_t>(dir + "/lmk_a");
+    const auto b = read_raw<uint64_t>(dir + "/lmk_b");
+    std::vector<LWECiphertext> cts(batch);
+    for (uint32_t i = 0; i < batch; ++i) {
+        cts[i].a.assign(a.begin() + static_cast<size_t>(i) * params.n, a.begin() + static_cast<size_t>(i + 1) * params.n);
+        cts[i].b = b[i];
+        cts[i].q = params.q_lwe;
+    }
+    const auto rgsw = cc.gpu_CircuitBootstrappingBatch(cts);
+    std::vector<uint64_t> out;
+    for (const auto& r : rgsw) out.insert(out.end(), r.data.begin(), r.data.end());
+    write_raw(dir + "/lmk_cbs_out", out);
+    // EvalAcc on a given accumulator and masks
+    const auto acc = read_raw<uint64_t>(dir + "/lmk_acc");
+    const auto masks = read_raw<uint32_t>(dir + "/lmk_masks");
+    DeviceArray<uint64_t> d_acc(acc.size());
+    check_cuda(cudaMemcpy(d_acc.data(), acc.data(), acc.size() * 8, cudaMemcpyHostToDevice), "acc in");
+    cc.LMKCDEY_EvalAcc(masks, d_acc.data());
+    std::vector<uint64_t> acc_out(acc.size());
+    check_cuda(cudaMemcpy(acc_out.data(), d_acc.data(), acc.size() * 8, cudaMemcpyDeviceToHost), "acc out");
+    write_raw(dir + "/lmk_acc_out", acc_out);
+    return 0;
+}
+
 static int run_gate(const std::string&) {
     cbs_gate_params gp{};
     check(cbs_gate_params_default(&gp), "gate params");
@@ -184,7 +221,7 @@ static int run_ckks(const std::string& dir) {
 
 int main(int argc, char** argv) {
     if (argc < 3) {
-        std::fprintf(stderr, "usage: %s ks|cbs|gate|ckks <dir>\n", argv[0]);
+        std::fprintf(stderr, "usage: %s ks|cbs|gate|ckks|lmk <dir>\n", argv[0]);
         return 2;
     }
     try {
@@ -193,6 +230,7 @@ int main(int argc, char** argv) {
         if (mode == "cbs") return run_cbs(dir);
         if (mode == "gate") return run_gate(dir);
         if (mode == "ckks") return run_ckks(dir);
+        if (mode == "lmk") return run_lmk(dir);
     } catch (const std::exception& e) {
         std::fprintf(stderr, "error: %s\n", e.what());
         return 1;

@@ -7,6 +7,8 @@ and linked against libcbs_b200.so, run on the GPU (tests/cpp/facade_main.cpp):
   rows bit-exact against the oracle's circuit bootstrap;
 * GPUBinFHEContext::BatchGPUEvalBinGate(NAND, ...) (binfhecontext.cuh:53-57), every gate
   decrypting to the truth table;
+* GPUCirBTSContext with the LMKCDEY method (SetMethod, LMKCDEY_EvalAcc, cirbts.cuh:491), CBS rows
+  and EvalAcc bit-exact against the oracle;
 * the CKKS evaluator (include/evaluate.cuh): multiply_and_relin_inplace + rescale_to_next_inplace
   and rotate_inplace, bit-exact against the oracle's keyswitch with the restated tensor
   product, rescale and Galois permutation."""
@@ -86,6 +88,36 @@ def test_facade_circuit_bootstrap_host_lwe(facade_bin, tmp_path, pkg, oracle):
     oracle.orc_circuit_bootstrap(ctypes.byref(oc.op), ctypes.byref(oc.ok), a.ctypes.data, b.ctypes.data, batch, p.n,
                                  want.ctypes.data)
     assert np.array_equal(got, want)
+
+
+def test_facade_lmkcdey(facade_bin, tmp_path, pkg, oracle):
+    """SetMethod(LMKCDEY) and LMKCDEY_EvalAcc through the facade: the CBS rows equal the oracle's
+    HomTrace + SchemeSwitch of its LMKCDEY accumulator, and EvalAcc the oracle's, word for word."""
+    from cbs_harness import oracle_lmkcdey_keys
+    p = pkg.preset_params("2x18")
+    p.num_lut = 1
+    seed, batch, num_auto = 23, 2, 10
+    keys = pkg.generate_keys_host(p, seed)
+    rng = np.random.default_rng(6)
+    a, b = lwe_encrypt_bits(rng, keys["s_lwe"], [1, 0], p.q_lwe)
+    acc = rng.integers(0, p.Q, size=(2, p.N), dtype=np.uint64)
+    masks = rng.integers(0, 2 * p.N, size=p.n, dtype=np.uint32)
+    np.array([seed, batch, num_auto], np.uint64).tofile(tmp_path / "lmk_dims")
+    a.astype(np.uint64).tofile(tmp_path / "lmk_a")
+    b.astype(np.uint64).tofile(tmp_path / "lmk_b")
+    acc.tofile(tmp_path / "lmk_acc")
+    masks.tofile(tmp_path / "lmk_masks")
+    _run(facade_bin, "lmk", tmp_path)
+    oc = OracleCbs(oracle, p, keys)
+    lmk = oracle_lmkcdey_keys(oracle, p, keys, num_auto, seed)
+    got = np.fromfile(tmp_path / "lmk_cbs_out", np.uint64).reshape(batch, 2, 2, p.N)
+    assert np.array_equal(got, oc.trace_ss(oc.br_acc_lmkcdey(a, b, lmk)))
+    vp, u32 = ctypes.c_void_p, ctypes.c_uint32
+    oracle.orc_lmkcdey_eval_acc.argtypes = [vp, vp, vp, vp, u32, vp, u32, vp]
+    want = acc.copy()
+    oracle.orc_lmkcdey_eval_acc(ctypes.byref(oc.op), lmk["eval"].ctypes.data, lmk["auto"].ctypes.data,
+                                lmk["maps"].ctypes.data, num_auto, masks.ctypes.data, p.n, want.ctypes.data)
+    assert np.array_equal(np.fromfile(tmp_path / "lmk_acc_out", np.uint64).reshape(2, p.N), want)
 
 
 def test_facade_batch_gate(facade_bin, tmp_path):
