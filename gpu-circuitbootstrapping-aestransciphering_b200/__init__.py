@@ -134,6 +134,12 @@ def _declare(lib: ctypes.CDLL) -> None:
         "cbs_gate_decrypt_bits": (st, [c_vp, c_vp, c_vp, u32, c_vp]),
         "cbs_gate_eval_batch_device": (st, [c_vp, ctypes.c_int, c_vp, c_vp, c_vp, c_vp, u32, c_vp, c_vp, c_vp]),
         "cbs_gate_bootstrap_batch_device": (st, [c_vp, c_vp, c_vp, u32, c_vp, c_vp, c_vp, c_vp]),
+        "cbs_gate_bootstrap_func_batch_device": (st, [c_vp, c_vp, c_vp, u32, u32, c_vp, u64, c_vp, c_vp, c_vp]),
+        "cbs_gate_eval_func_batch_device": (st, [c_vp, c_vp, c_vp, u32, u32, c_vp, u32, c_vp, c_vp, c_vp]),
+        "cbs_gate_eval_floor_batch_device": (st, [c_vp, c_vp, c_vp, u32, u64, u32, u32, u32, c_vp, c_vp, c_vp]),
+        "cbs_gate_eval_sign_batch_device": (st, [c_vp, c_vp, c_vp, u32, u64, u32, u32, ctypes.c_int, c_vp, c_vp,
+                                                 c_vp]),
+        "cbs_gate_eval_decomp_batch_device": (st, [c_vp, c_vp, c_vp, u32, u64, u32, u32, c_vp, c_vp, c_vp, c_vp]),
         "cbs_tcb_params_default": (st, [c_vp]),
         "cbs_tcb_context_create": (st, [c_vp, u32, c_vp]),
         "cbs_tcb_context_destroy": (st, [c_vp]),

@@ -152,7 +152,9 @@ __global__ void __launch_bounds__(GateCfg<LOGN>::T, GateCfg<LOGN>::MIN_BLOCKS) k
             const uint32_t bt = ms(b);
             for (uint32_t i = tid; i < N; i += T) {
                 acc[i] = 0;
-                acc[N + i] = (((i + bt) & (TWO_N - 1)) < N) ? mu : TT(0) - mu;
+                const uint32_t sp = (i + bt) & (TWO_N - 1);
+                const TT tv = a.tv ? static_cast<TT>(__ldg(a.tv + (sp & (N - 1)))) : mu;
+                acc[N + i] = sp < N ? tv : TT(0) - tv;
             }
         }
         __syncthreads();
@@ -315,7 +317,9 @@ __global__ void __launch_bounds__(GateCfg<LOGN>::T, GateCfg<LOGN>::MIN_BLOCKS)
             const uint32_t bt = ms(b);
             for (uint32_t i = tid; i < N; i += T) {
                 acc[i] = 0;
-                acc[N + i] = (((i + bt) & (TWO_N - 1)) < N) ? mu : 0u - mu;
+                const uint32_t sp = (i + bt) & (TWO_N - 1);
+                const uint32_t tv = a.tv ? __ldg(a.tv + (sp & (N - 1))) : mu;
+                acc[N + i] = sp < N ? tv : 0u - tv;
             }
         }
         __syncthreads();
@@ -496,7 +500,9 @@ __global__ void __launch_bounds__(GateMbCfg<LOGN>::T, GateMbCfg<LOGN>::MIN_BLOCK
             const uint32_t bt = ms(b);
             for (uint32_t i = tid; i < N; i += T) {
                 acc[i] = 0;
-                acc[N + i] = (((i + bt) & (TWO_N - 1)) < N) ? mu : TT(0) - mu;
+                const uint32_t sp = (i + bt) & (TWO_N - 1);
+                const TT tv = a.tv ? static_cast<TT>(__ldg(a.tv + (sp & (N - 1)))) : mu;
+                acc[N + i] = sp < N ? tv : TT(0) - tv;
             }
         }
         __syncthreads();
@@ -896,30 +902,29 @@ cudaError_t gate_keyswitch(const GateArgs& a, const uint32_t* ksk, uint32_t n, u
 
 using cbs::DevBuf;
 
-struct cbs_gate_context {
-    cbs_gate_params p{};
-    uint32_t max_batch = 0;
-    bool keys_ready = false;
-    std::vector<int32_t> s, z;      // LWE key (n), RLWE key (N), binary
-    std::vector<uint32_t> bsk, ksk;  // coefficient form (exported) / device layout
-    DevBuf<double2> d_bskf, d_tab;
-    DevBuf<uint32_t> d_ksk, d_ext, d_tmp_a, d_tmp_b;
-    // ragged plan (cbs_gate_ragged_plan): request table, its extracted-LWE scratch, grid
-    DevBuf<cbs::GateReq> d_plan;
-    DevBuf<uint32_t> d_plan_ext;
-    uint32_t plan_reqs = 0, plan_items = 0, plan_grid = 0;
-    // grouped (multi-bit) blind rotation: mb, its keys (coefficient form) and their spectra
-    uint32_t br_mb = 1;
-    bool mb_ready = false;
-    uint64_t key_seed = 0;
-    std::vector<uint32_t> mbk;
-    DevBuf<double2> d_bskf_mb;
-    // external-product arithmetic (CBS_FFT_*) and, for the FP32 modes, the key-limb spectra and
-    // the FP32 transform table
-    uint32_t fft_mode = CBS_FFT_FP64;
-    bool f32_ready = false;
-    DevBuf<float2> d_bskf32, d_tab32;
-};
+#include "gate_context.cuh"
+
+namespace cbs {
+
+cbs_status gate_fill_keys(const cbs_gate_context* ctx, GateArgs& a) {
+    if (ctx->br_mb > 1 && !ctx->mb_ready) {
+        set_error("gate: grouped keys are not prepared");
+        return CBS_ERR_NOT_READY;
+    }
+    if (ctx->fft_mode != CBS_FFT_FP64 && !ctx->f32_ready) {
+        set_error("gate: FP32 key spectra are not prepared");
+        return CBS_ERR_NOT_READY;
+    }
+    a.bskf = ctx->br_mb > 1 ? ctx->d_bskf_mb.p : ctx->d_bskf.p;
+    a.mb = ctx->br_mb;
+    a.tab = ctx->d_tab.p;
+    a.fft_mode = ctx->fft_mode;
+    a.bskf32 = ctx->d_bskf32.p;
+    a.tab32 = ctx->d_tab32.p;
+    return CBS_OK;
+}
+
+}  // namespace cbs
 
 namespace {
 
@@ -1104,23 +1109,6 @@ cbs_status gate_prepare_f32(cbs_gate_context* ctx) {
 
 // the arithmetic fields of the launch arguments; CBS_ERR_NOT_READY when the selected keys are
 // not prepared
-cbs_status gate_fill_keys(const cbs_gate_context* ctx, cbs::GateArgs& a) {
-    if (ctx->br_mb > 1 && !ctx->mb_ready) {
-        set_error("gate: grouped keys are not prepared");
-        return CBS_ERR_NOT_READY;
-    }
-    if (ctx->fft_mode != CBS_FFT_FP64 && !ctx->f32_ready) {
-        set_error("gate: FP32 key spectra are not prepared");
-        return CBS_ERR_NOT_READY;
-    }
-    a.bskf = ctx->br_mb > 1 ? ctx->d_bskf_mb.p : ctx->d_bskf.p;
-    a.mb = ctx->br_mb;
-    a.tab = ctx->d_tab.p;
-    a.fft_mode = ctx->fft_mode;
-    a.bskf32 = ctx->d_bskf32.p;
-    a.tab32 = ctx->d_tab32.p;
-    return CBS_OK;
-}
 
 cbs_status gate_prepare_mb(cbs_gate_context* ctx) {
     if (ctx->br_mb <= 1 || ctx->mb_ready || !ctx->keys_ready) return CBS_OK;

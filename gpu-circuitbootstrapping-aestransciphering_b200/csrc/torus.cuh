@@ -41,6 +41,9 @@ struct GateArgs {
     uint32_t levels_tv;
     uint64_t mu[8];        // in the kernel's torus width
     uint64_t b_add[8];
+    // 32-bit torus only: a test vector [N] (coefficient domain) in place of the constant mu
+    // (functional bootstrapping; levels_tv = 1)
+    const uint32_t* tv;
     // 0 or 1: one coefficient per step (bskf [n][2*levels][2][M]); 2 or 3: groups of mb
     // coefficients (bskf [ceil(n/mb)][2^mb - 1][2*levels][2][M], the grouped kernel)
     uint32_t mb;

@@ -518,6 +518,51 @@ cbs_status cbs_gate_bootstrap_batch_device(cbs_gate_context *ctx, const uint32_t
                                            uint32_t count, uint32_t *d_ext, uint32_t *d_out_a, uint32_t *d_out_b,
                                            cbs_stream_t stream);
 
+/* Functional bootstrapping on the gate context (the reference's large-precision evaluators,
+ * https://eprint.iacr.org/2021/1337, as bitwise/src/binfhe-base-scheme-batch.cu:215-712 batches
+ * them behind GPUBinFHEContext::BatchGPUEvalFunc / Floor / Sign / Decomp,
+ * bitwise/include/binfhecontext.cuh:60-118).  Ciphertexts here are LWE vectors under the
+ * context's key s with an explicit power-of-two modulus, as the reference's LWECiphertext
+ * carries one: a [count][n], b [count], uint32 words holding residues mod that modulus (device
+ * pointers).  The bootstraps need the FP64 external product (cbs_gate_set_fft_mode) and allocate
+ * the context's scratch on first use.  beta is the reference's GetBeta() (OpenFHE's error bound,
+ * 128 in its parameter sets), q its LWE modulus Getq() (a power of two dividing 2N).
+ *
+ * cbs_gate_bootstrap_func_batch_device: BatchGPUBootstrapFunc (:215-364): input mod q_in
+ * (power of two, 4 <= q_in <= 2N), f given on [0, q_in/2) by h_lut [q_in/2] (host, values in
+ * [0, fmod)); the output (mod fmod, a power of two <= 2^32) encrypts f(phase) for phases in
+ * [0, q_in/2) and -f(phase - q_in/2) above (the negacyclic extension every caller relies on). */
+cbs_status cbs_gate_bootstrap_func_batch_device(cbs_gate_context *ctx, const uint32_t *d_a, const uint32_t *d_b,
+                                                uint32_t count, uint32_t q_in, const uint64_t *h_lut, uint64_t fmod,
+                                                uint32_t *d_out_a, uint32_t *d_out_b, cbs_stream_t stream);
+/* BatchGPUEvalFunc (:366-479): ciphertexts mod q (power of two <= 2N), h_lut [q] (host, values
+ * mod q) the function on Z_q; negacyclic tables take one bootstrap, periodic ones two, any
+ * other table (q <= N) two at modulus 2q.  Output mod q. */
+cbs_status cbs_gate_eval_func_batch_device(cbs_gate_context *ctx, const uint32_t *d_a, const uint32_t *d_b,
+                                           uint32_t count, uint32_t q, const uint32_t *h_lut, uint32_t beta,
+                                           uint32_t *d_out_a, uint32_t *d_out_b, cbs_stream_t stream);
+/* BatchGPUEvalFloor (:481-543): ciphertexts mod `mod` (power of two <= 2^32); clears the low
+ * bits of the phase below q (roundbits = 0) or below beta 2^(roundbits+1); output mod `mod`. */
+cbs_status cbs_gate_eval_floor_batch_device(cbs_gate_context *ctx, const uint32_t *d_a, const uint32_t *d_b,
+                                            uint32_t count, uint64_t mod, uint32_t q, uint32_t roundbits,
+                                            uint32_t beta, uint32_t *d_out_a, uint32_t *d_out_b, cbs_stream_t stream);
+/* BatchGPUEvalSign (:545-631): ciphertexts mod `mod` > q; floors and switches the modulus down
+ * by q / (2 beta) until it is at most q, then bootstraps the sign: output mod q encrypting 0
+ * for phases below mod/2 and q/2 above (scheme_switch: -q/4 and q/4, the reference's encoding
+ * for scheme switching).  Its single bootstrapping key serves every round (the reference's GPU
+ * context holds one, so its base-switching branch never runs). */
+cbs_status cbs_gate_eval_sign_batch_device(cbs_gate_context *ctx, const uint32_t *d_a, const uint32_t *d_b,
+                                           uint32_t count, uint64_t mod, uint32_t q, uint32_t beta, int scheme_switch,
+                                           uint32_t *d_out_a, uint32_t *d_out_b, cbs_stream_t stream);
+/* BatchGPUEvalDecomp (:633-712): ciphertexts mod `mod` > q into digits, least significant first:
+ * digit k [k][count][n] / [k][count] is the phase mod q before the k-th floor, the last the
+ * remainder at the final modulus.  *digits: in, the capacity of the outputs; out, the digits
+ * made (also when the capacity is too small, CBS_ERR_INVALID_ARG). */
+cbs_status cbs_gate_eval_decomp_batch_device(cbs_gate_context *ctx, const uint32_t *d_a, const uint32_t *d_b,
+                                             uint32_t count, uint64_t mod, uint32_t q, uint32_t beta,
+                                             uint32_t *d_out_a, uint32_t *d_out_b, uint32_t *digits,
+                                             cbs_stream_t stream);
+
 /* Ragged batching: many bootstrap requests of uneven size (the sign bootstrap of
  * cbs_gate_bootstrap_batch_device, outputs key-switched to n) in one blind-rotation launch
  * and one key-switch launch per parameter set, instead of one launch pair per request.  No

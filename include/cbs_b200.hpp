@@ -679,14 +679,163 @@ class GPUBinFHEContext {
         }
         return out;
     }
+
+    // The functional evaluators (binfhecontext.cuh:60-118; binfhe-base-scheme-batch.cu:366-712).
+    // Their LWECiphertexts carry a power-of-two modulus q; the parameter set's LWE modulus and the
+    // error bound beta (the reference's Getq() and GetBeta()) are set here (defaults N and 128).
+    void SetFunctionalParams(uint32_t lweModulus, uint32_t beta) {
+        lwe_q_ = lweModulus;
+        beta_ = beta;
+    }
+    // GPUEvalFunc / BatchGPUEvalFunc: LUT [q] over Z_q, q the ciphertexts' modulus
+    [[nodiscard]] std::vector<LWECiphertext> BatchGPUEvalFunc(const std::vector<LWECiphertext>& v_ct,
+                                                              const std::vector<uint64_t>& LUT,
+                                                              const cudaStream_t& stream = nullptr) {
+        const uint64_t q = common_modulus(v_ct, "BatchGPUEvalFunc");
+        if (LUT.size() != q) throw Error(CBS_ERR_SHAPE_MISMATCH, "BatchGPUEvalFunc: the LUT must have q entries");
+        std::vector<uint32_t> lut(LUT.begin(), LUT.end());
+        return unary(v_ct, q, stream, [&](const uint32_t* a, const uint32_t* b, uint32_t count, uint32_t* oa,
+                                          uint32_t* ob, cbs_stream_t s) {
+            return cbs_gate_eval_func_batch_device(ctx_, a, b, count, static_cast<uint32_t>(q), lut.data(), beta_, oa,
+                                                   ob, s);
+        });
+    }
+    [[nodiscard]] LWECiphertext GPUEvalFunc(const LWECiphertext& ct, const std::vector<uint64_t>& LUT,
+                                            const cudaStream_t& stream = nullptr) {
+        return BatchGPUEvalFunc(std::vector<LWECiphertext>{ct}, LUT, stream).front();
+    }
+    // GPUEvalFloor / BatchGPUEvalFloor
+    [[nodiscard]] std::vector<LWECiphertext> BatchGPUEvalFloor(const std::vector<LWECiphertext>& v_ct,
+                                                               uint32_t roundbits = 0,
+                                                               const cudaStream_t& stream = nullptr) {
+        const uint64_t mod = common_modulus(v_ct, "BatchGPUEvalFloor");
+        return unary(v_ct, mod, stream, [&](const uint32_t* a, const uint32_t* b, uint32_t count, uint32_t* oa,
+                                            uint32_t* ob, cbs_stream_t s) {
+            return cbs_gate_eval_floor_batch_device(ctx_, a, b, count, mod, lwe_q(), roundbits, beta_, oa, ob, s);
+        });
+    }
+    [[nodiscard]] LWECiphertext GPUEvalFloor(const LWECiphertext& ct, uint32_t roundbits = 0,
+                                             const cudaStream_t& stream = nullptr) {
+        return BatchGPUEvalFloor(std::vector<LWECiphertext>{ct}, roundbits, stream).front();
+    }
+    // GPUEvalSign / BatchGPUEvalSign: outputs modulo the LWE modulus
+    [[nodiscard]] std::vector<LWECiphertext> BatchGPUEvalSign(const std::vector<LWECiphertext>& v_ct,
+                                                              bool schemeSwitch = false,
+                                                              const cudaStream_t& stream = nullptr) {
+        const uint64_t mod = common_modulus(v_ct, "BatchGPUEvalSign");
+        return unary(v_ct, lwe_q(), stream, [&](const uint32_t* a, const uint32_t* b, uint32_t count, uint32_t* oa,
+                                                uint32_t* ob, cbs_stream_t s) {
+            return cbs_gate_eval_sign_batch_device(ctx_, a, b, count, mod, lwe_q(), beta_, schemeSwitch ? 1 : 0, oa, ob,
+                                                   s);
+        });
+    }
+    [[nodiscard]] LWECiphertext GPUEvalSign(const LWECiphertext& ct, bool schemeSwitch = false,
+                                            const cudaStream_t& stream = nullptr) {
+        return BatchGPUEvalSign(std::vector<LWECiphertext>{ct}, schemeSwitch, stream).front();
+    }
+    // GPUEvalDecomp / BatchGPUEvalDecomp: per ciphertext its digits, least significant first
+    [[nodiscard]] std::vector<std::vector<LWECiphertext>> BatchGPUEvalDecomp(const std::vector<LWECiphertext>& v_ct,
+                                                                             const cudaStream_t& stream = nullptr) {
+        const uint64_t mod = common_modulus(v_ct, "BatchGPUEvalDecomp");
+        const size_t count = v_ct.size(), n = params_.n;
+        std::vector<std::vector<LWECiphertext>> out(count);
+        if (!count) return out;
+        uint32_t digits = 0;  // ask for the digit count first
+        const uint32_t q = lwe_q();
+        (void)cbs_gate_eval_decomp_batch_device(ctx_, nullptr, nullptr, 0, mod, q, beta_, nullptr, nullptr, &digits,
+                                                nullptr);
+        if (digits == 0) throw Error(CBS_ERR_INVALID_ARG, std::string("BatchGPUEvalDecomp: ") + cbs_last_error());
+        upload(v_ct, stream);
+        uint32_t* d = dev_.data();
+        const size_t in_words = count * n + count;
+        dev_out_.resize(digits * in_words);
+        uint32_t *oa = dev_out_.data(), *ob = oa + digits * count * n;
+        uint32_t cap = digits;
+        check(cbs_gate_eval_decomp_batch_device(ctx_, d, d + count * n, static_cast<uint32_t>(count), mod, q, beta_,
+                                                oa, ob, &cap, as_stream(stream)),
+              "BatchGPUEvalDecomp");
+        std::vector<uint32_t> ha(digits * count * n), hb(digits * count);
+        check_cuda(cudaMemcpyAsync(ha.data(), oa, ha.size() * 4, cudaMemcpyDeviceToHost, stream), "digits a");
+        check_cuda(cudaMemcpyAsync(hb.data(), ob, hb.size() * 4, cudaMemcpyDeviceToHost, stream), "digits b");
+        check_cuda(cudaStreamSynchronize(stream), "BatchGPUEvalDecomp");
+        // digit moduli: q for every floor, the final modulus for the last
+        const int qb = log2_of(q), bb = log2_of(beta_);
+        int mb = log2_of(mod);
+        std::vector<uint64_t> mods;
+        while (mb > qb) {
+            mods.push_back(q);
+            mb = mb - qb + 1 + bb;
+        }
+        mods.push_back(uint64_t(1) << mb);
+        for (size_t i = 0; i < count; ++i)
+            for (uint32_t k = 0; k < digits; ++k) {
+                LWECiphertext c;
+                c.a.assign(ha.begin() + (k * count + i) * n, ha.begin() + (k * count + i + 1) * n);
+                c.b = hb[k * count + i];
+                c.q = mods[k];
+                out[i].push_back(std::move(c));
+            }
+        return out;
+    }
+    [[nodiscard]] std::vector<LWECiphertext> GPUEvalDecomp(const LWECiphertext& ct, const cudaStream_t& stream = nullptr) {
+        return BatchGPUEvalDecomp(std::vector<LWECiphertext>{ct}, stream).front();
+    }
+
     [[nodiscard]] cbs_gate_context* handle() const { return ctx_; }
     [[nodiscard]] const cbs_gate_params& params() const { return params_; }
 
    private:
+    static int log2_of(uint64_t v) {
+        int b = 0;
+        while ((uint64_t(1) << b) < v) ++b;
+        return b;
+    }
+    uint32_t lwe_q() const { return lwe_q_ ? lwe_q_ : params_.N; }
+    uint64_t common_modulus(const std::vector<LWECiphertext>& v, const char* who) const {
+        if (v.empty()) return lwe_q();
+        const uint64_t q = v[0].q;
+        for (const auto& c : v)
+            if (c.q != q || c.a.size() != params_.n)
+                throw Error(CBS_ERR_SHAPE_MISMATCH, std::string(who) + ": ciphertexts of one modulus and dimension n");
+        if (v.size() > max_batch_) throw Error(CBS_ERR_SHAPE_MISMATCH, std::string(who) + ": batch above max_batch");
+        return q;
+    }
+    void upload(const std::vector<LWECiphertext>& v, const cudaStream_t& stream) {
+        const size_t count = v.size(), n = params_.n;
+        std::vector<uint32_t> h(count * n + count);
+        for (size_t i = 0; i < count; ++i) {
+            for (size_t j = 0; j < n; ++j) h[i * n + j] = static_cast<uint32_t>(v[i].a[j]);
+            h[count * n + i] = static_cast<uint32_t>(v[i].b);
+        }
+        dev_.resize(h.size());
+        check_cuda(cudaMemcpyAsync(dev_.data(), h.data(), h.size() * 4, cudaMemcpyHostToDevice, stream), "upload");
+        check_cuda(cudaStreamSynchronize(stream), "upload");  // h is a temporary
+    }
+    template <class F>
+    std::vector<LWECiphertext> unary(const std::vector<LWECiphertext>& v, uint64_t out_q, const cudaStream_t& stream,
+                                     F fn) {
+        const size_t count = v.size(), n = params_.n;
+        std::vector<LWECiphertext> out(count);
+        if (!count) return out;
+        upload(v, stream);
+        dev_out_.resize(count * n + count);
+        uint32_t *d = dev_.data(), *o = dev_out_.data();
+        check(fn(d, d + count * n, static_cast<uint32_t>(count), o, o + count * n, as_stream(stream)), "evaluator");
+        std::vector<uint32_t> h(count * n + count);
+        check_cuda(cudaMemcpyAsync(h.data(), o, h.size() * 4, cudaMemcpyDeviceToHost, stream), "download");
+        check_cuda(cudaStreamSynchronize(stream), "evaluator");
+        for (size_t i = 0; i < count; ++i) {
+            out[i].a.assign(h.begin() + i * n, h.begin() + (i + 1) * n);
+            out[i].b = h[count * n + i];
+            out[i].q = out_q;
+        }
+        return out;
+    }
     cbs_gate_params params_;
     uint32_t max_batch_;
     cbs_gate_context* ctx_ = nullptr;
-    DeviceArray<uint32_t> dev_;
+    DeviceArray<uint32_t> dev_, dev_out_;
+    uint32_t lwe_q_ = 0, beta_ = 128;
 };
 
 }  // namespace cbs_b200

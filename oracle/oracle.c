@@ -959,6 +959,12 @@ void orc_gate_blind_rotate(const orc_gate_params *p, const uint32_t *bsk, const 
 
 void orc_gate_blind_rotate_tv(const orc_gate_params *p, const uint32_t *bsk, const uint32_t *a, uint32_t b,
                               uint32_t mu, uint32_t b_add, uint32_t *ext) {
+    orc_gate_blind_rotate_lut(p, bsk, a, b, NULL, mu, b_add, ext);
+}
+
+/* the same rotation of an arbitrary test vector tv [N] (coefficient domain; NULL: the constant mu) */
+void orc_gate_blind_rotate_lut(const orc_gate_params *p, const uint32_t *bsk, const uint32_t *a, uint32_t b,
+                               const uint32_t *tv, uint32_t mu, uint32_t b_add, uint32_t *ext) {
     const uint32_t N = p->N, L = p->levels, two_n = 2 * N;
     uint32_t logn2 = 0;
     while ((1u << logn2) < two_n) ++logn2;
@@ -971,7 +977,8 @@ void orc_gate_blind_rotate_tv(const orc_gate_params *p, const uint32_t *bsk, con
     const uint32_t bt = MS(b);
     for (uint32_t i = 0; i < N; ++i) {
         const uint32_t s = (i + bt) % two_n; /* coefficient i of X^-bt TV = TV[i + bt] (wrapped) */
-        acc[N + i] = (s < N) ? mu : 0u - mu;
+        const uint32_t v = tv ? tv[s % N] : mu;
+        acc[N + i] = (s < N) ? v : 0u - v;
     }
     for (uint32_t step = 0; step < p->n; ++step) {
         const uint32_t at = MS(a[step]);
@@ -1218,6 +1225,30 @@ void orc_gate_keyswitch(const orc_gate_params *p, const uint32_t *ksk, const uin
             for (uint32_t j = 0; j <= n; ++j) out[j] -= row[j];
         }
     }
+}
+
+/* the programmable bootstrap of the functional evaluators (binfhe-base-scheme-batch.cu:215-364):
+ * a [n], b mod 2^in_bits lifted to the torus, the test vector (2^32 / 2^f_bits) lut[j] at
+ * coefficient j 2N / 2^in_bits (j < 2^in_bits / 2), rotation, extraction, key switch to n, and the
+ * rounding to Z_(2^f_bits).  out [n + 1] (a then b). */
+void orc_gate_bootstrap_func(const orc_gate_params *p, const uint32_t *bsk, const uint32_t *ksk, const uint32_t *a,
+                             uint32_t b, uint32_t in_bits, const uint64_t *lut, uint32_t f_bits, uint32_t *out) {
+    const uint32_t N = p->N, n = p->n, q_in = 1u << in_bits, factor = 2 * N / q_in;
+    uint32_t *tv = (uint32_t *)calloc(N, sizeof(uint32_t));
+    uint32_t *at = (uint32_t *)malloc(sizeof(uint32_t) * n);
+    uint32_t *ext = (uint32_t *)malloc(sizeof(uint32_t) * (N + 1));
+    for (uint32_t j = 0; j < q_in / 2; ++j) tv[j * factor] = (uint32_t)(lut[j] << (32 - f_bits));
+    for (uint32_t i = 0; i < n; ++i) at[i] = a[i] << (32 - in_bits);
+    orc_gate_blind_rotate_lut(p, bsk, at, b << (32 - in_bits), tv, 0, 0, ext);
+    orc_gate_keyswitch(p, ksk, ext, out);
+    const uint32_t sh = 32 - f_bits, mask = f_bits >= 32 ? ~0u : ((1u << f_bits) - 1u);
+    for (uint32_t i = 0; i <= n; ++i) {
+        const uint64_t x = out[i];
+        out[i] = (uint32_t)(sh ? (x + (1ull << (sh - 1))) >> sh : x) & mask;
+    }
+    free(ext);
+    free(at);
+    free(tv);
 }
 
 /* ------------------------------------------------------------------------------------------ */

@@ -182,6 +182,14 @@ void orc_tcb_pfks(uint32_t N2, uint32_t N1, uint32_t base_bits, uint32_t levels,
                   const uint64_t *ext, uint32_t *out);
 /* LWE key switch N -> n (binfhe-base-scheme-batch.cu:145-185): ksk [N][ks_levels][base-1][n+1] */
 void orc_gate_keyswitch(const orc_gate_params *p, const uint32_t *ksk, const uint32_t *ext, uint32_t *out);
+/* the rotation of an arbitrary test vector tv [N] (NULL: the constant mu) */
+void orc_gate_blind_rotate_lut(const orc_gate_params *p, const uint32_t *bsk, const uint32_t *a, uint32_t b,
+                               const uint32_t *tv, uint32_t mu, uint32_t b_add, uint32_t *ext);
+/* the programmable bootstrap (binfhe-base-scheme-batch.cu:215-364): a [n], b mod 2^in_bits, lut
+ * [2^in_bits / 2] values mod 2^f_bits; out [n + 1] mod 2^f_bits encrypting lut[phase] (negacyclic
+ * above half) */
+void orc_gate_bootstrap_func(const orc_gate_params *p, const uint32_t *bsk, const uint32_t *ksk, const uint32_t *a,
+                             uint32_t b, uint32_t in_bits, const uint64_t *lut, uint32_t f_bits, uint32_t *out);
 
 /* ---------------- plaintext AES-128 (examples/aes_transcipher/aes128.cuh) ---------------- */
 void orc_aes128_key_expand(const uint8_t key[16], uint8_t round_keys[11][16]);

@@ -10,12 +10,15 @@
 //         cbs_a, cbs_b -> cbs_out (the batch's RGSW rows)
 //   gate  GPUBinFHEContext::BatchGPUEvalBinGate(NAND): exit status 0 when every gate decrypts to
 //         the truth table
+//   gfunc GPUBinFHEContext's functional evaluators (BatchGPUEvalFunc, GPUEvalFunc, BatchGPUEvalSign,
+//         BatchGPUEvalFloor, BatchGPUEvalDecomp): exit status 0 when every result decrypts right
 //   lmk   GPUCirBTSContext with SetMethod(LMKCDEY): gpu_CircuitBootstrappingBatch on the 2^18 x 2
 //         preset with one LUT slot, and LMKCDEY_EvalAcc on a given accumulator: lmk_dims (seed
 //         batch num_auto_keys), lmk_a, lmk_b, lmk_acc, lmk_masks -> lmk_cbs_out, lmk_acc_out
 //   ckks  the CKKS evaluator: multiply_and_relin_inplace then rescale_to_next_inplace of ct1 by
 //         ct2, and rotate_inplace of ct1 by one step: ck_dims (N size_q size_p chain_index beta
 //         galois_elt), ck_chain, ck_ct1, ck_ct2, ck_rk, ck_gk -> ck_mr, ck_rot
+#include <algorithm>
 #include <cstdio>
 #include <fstream>
 #include <iostream>
@@ -180,6 +183,74 @@ static int run_gate(const std::string&) {
     return 0;
 }
 
+// LWE encryption of phases mod q under s (test helper: the facade's user holds s)
+static std::vector<LWECiphertext> encrypt_mod(const std::vector<int32_t>& s, const std::vector<uint64_t>& phases,
+                                              uint64_t q, uint64_t seed) {
+    uint64_t x = seed;
+    auto next = [&]() {  // splitmix64
+        uint64_t z = (x += 0x9e3779b97f4a7c15ull);
+        z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+        z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+        return z ^ (z >> 31);
+    };
+    std::vector<LWECiphertext> v(phases.size());
+    for (size_t i = 0; i < phases.size(); ++i) {
+        v[i].a.resize(s.size());
+        uint64_t dot = 0;
+        for (size_t j = 0; j < s.size(); ++j) {
+            v[i].a[j] = next() & (q - 1);
+            dot += v[i].a[j] * static_cast<uint64_t>(s[j]);
+        }
+        v[i].b = (dot + phases[i] + (next() % 3) - 1) & (q - 1);  // noise in {-1, 0, 1}
+        v[i].q = q;
+    }
+    return v;
+}
+
+static uint64_t phase_of(const std::vector<int32_t>& s, const LWECiphertext& c) {
+    uint64_t dot = 0;
+    for (size_t j = 0; j < s.size(); ++j) dot += c.a[j] * static_cast<uint64_t>(s[j]);
+    return (c.b - dot) & (c.q - 1);
+}
+
+static int run_gfunc(const std::string&) {
+    cbs_gate_params gp{};
+    check(cbs_gate_params_default(&gp), "gate params");
+    GPUBinFHEContext cc(gp, 16);
+    cc.GPUBTKeyGen(23);
+    cc.SetFunctionalParams(1024, 128);
+    std::vector<int32_t> s(gp.n);
+    check(cbs_gate_export_keys(cc.handle(), s.data(), nullptr, nullptr, nullptr), "keys");
+    // EvalFunc of x -> 3x mod 4 (an arbitrary table) on q = 1024
+    const uint64_t q = 1024, P = 4;
+    std::vector<uint64_t> lut(q);
+    for (uint64_t x = 0; x < q; ++x) lut[x] = (q / P) * ((3 * ((x * P) / q)) % P);
+    std::vector<uint64_t> ms = {0, 1, 2, 3}, ph;
+    for (auto m : ms) ph.push_back(m * (q / P));
+    const auto fo = cc.BatchGPUEvalFunc(encrypt_mod(s, ph, q, 1), lut);
+    for (size_t i = 0; i < ms.size(); ++i)
+        if (((phase_of(s, fo[i]) + q / (2 * P)) / (q / P)) % P != (3 * ms[i]) % P) return 20;
+    if (cc.GPUEvalFunc(encrypt_mod(s, {ph[1]}, q, 2)[0], lut).q != q) return 21;
+    // EvalSign of 14-bit values: output mod q, 0 below 2^13 and q/2 above
+    const uint64_t mod = uint64_t(1) << 14;
+    const std::vector<uint64_t> xs = {1000, 7000, 9000, 15000};
+    const auto sg = cc.BatchGPUEvalSign(encrypt_mod(s, xs, mod, 3));
+    for (size_t i = 0; i < xs.size(); ++i) {
+        const uint64_t p = phase_of(s, sg[i]), want = xs[i] >= mod / 2 ? q / 2 : 0;
+        const uint64_t d = (p - want) & (q - 1);
+        if (std::min(d, q - d) >= q / 8) return 22;
+    }
+    // EvalFloor keeps the modulus; EvalDecomp gives three digits for 14 bits at q = 2^10, beta = 2^7
+    if (cc.BatchGPUEvalFloor(encrypt_mod(s, xs, mod, 4))[0].q != mod) return 23;
+    const auto dg = cc.BatchGPUEvalDecomp(encrypt_mod(s, xs, mod, 5));
+    if (dg.size() != xs.size() || dg[0].size() != 3) return 24;
+    for (size_t i = 0; i < xs.size(); ++i) {
+        const uint64_t d = (phase_of(s, dg[i][0]) - xs[i]) & (q - 1);
+        if (std::min(d, q - d) >= 32) return 25;
+    }
+    return 0;
+}
+
 static int run_ckks(const std::string& dir) {
     const auto dims = read_raw<uint64_t>(dir + "/ck_dims");
     const size_t N = dims[0], size_p = dims[2], chain_index = dims[3], beta = dims[4];
@@ -221,7 +292,7 @@ static int run_ckks(const std::string& dir) {
 
 int main(int argc, char** argv) {
     if (argc < 3) {
-        std::fprintf(stderr, "usage: %s ks|cbs|gate|ckks|lmk <dir>\n", argv[0]);
+        std::fprintf(stderr, "usage: %s ks|cbs|gate|ckks|lmk|gfunc <dir>\n", argv[0]);
         return 2;
     }
     try {
@@ -231,6 +302,7 @@ int main(int argc, char** argv) {
         if (mode == "gate") return run_gate(dir);
         if (mode == "ckks") return run_ckks(dir);
         if (mode == "lmk") return run_lmk(dir);
+        if (mode == "gfunc") return run_gfunc(dir);
     } catch (const std::exception& e) {
         std::fprintf(stderr, "error: %s\n", e.what());
         return 1;

@@ -294,9 +294,8 @@ def test_aes128_ctr_add_ciphertext_device_bit_exact(pkg, ctx, blocks):
     b[:3] = [0, p.q_lwe // 2, p.q_lwe - 1]  # wrap edges
     cipher = rng.integers(0, 256, blocks * 16, dtype=np.uint8)
     cipher[0] = 0x07
-    db = dev(b)
-    pkg.call("cbs_aes128_ctr_add_ciphertext_device", ctx.handle, dev(cipher).data_ptr(), blocks, db.data_ptr(),
-             None)
+    db, dc = dev(b), dev(cipher)  # both held until the kernel has run
+    pkg.call("cbs_aes128_ctr_add_ciphertext_device", ctx.handle, dc.data_ptr(), blocks, db.data_ptr(), None)
     torch.cuda.synchronize()
     bits = np.unpackbits(cipher, bitorder="little").astype(np.uint64)
     want = (b + bits * (p.q_lwe // 2)) % p.q_lwe

@@ -6,7 +6,8 @@ and linked against libcbs_b200.so, run on the GPU (tests/cpp/facade_main.cpp):
   gpu_CircuitBootstrappingBatchToDevice on host LWE ciphertexts (cirbts.cuh:454-462), the RGSW
   rows bit-exact against the oracle's circuit bootstrap;
 * GPUBinFHEContext::BatchGPUEvalBinGate(NAND, ...) (binfhecontext.cuh:53-57), every gate
-  decrypting to the truth table;
+  decrypting to the truth table, and its functional evaluators (EvalFunc / Floor / Sign / Decomp,
+  :60-118), every result decrypting right;
 * GPUCirBTSContext with the LMKCDEY method (SetMethod, LMKCDEY_EvalAcc, cirbts.cuh:491), CBS rows
   and EvalAcc bit-exact against the oracle;
 * the CKKS evaluator (include/evaluate.cuh): multiply_and_relin_inplace + rescale_to_next_inplace
@@ -122,6 +123,13 @@ def test_facade_lmkcdey(facade_bin, tmp_path, pkg, oracle):
 
 def test_facade_batch_gate(facade_bin, tmp_path):
     _run(facade_bin, "gate", tmp_path)
+
+
+def test_facade_functional_evaluators(facade_bin, tmp_path):
+    """GPUBinFHEContext::BatchGPUEvalFunc / GPUEvalFunc / BatchGPUEvalSign / BatchGPUEvalFloor /
+    BatchGPUEvalDecomp (binfhecontext.cuh:60-118) at the default gate parameters: every result
+    decrypts to what it computes."""
+    _run(facade_bin, "gfunc", tmp_path)
 
 
 def test_facade_ckks_evaluator(facade_bin, tmp_path, oracle):
