@@ -84,11 +84,11 @@ def _declare(lib: ctypes.CDLL) -> None:
         "cbs_keygen": (st, [c_vp, u64]),
         "cbs_context_set_br_backend": (st, [c_vp, ctypes.c_int]),
         "cbs_context_set_br_multibit": (st, [c_vp, u32]),
-        "cbs_context_set_br_method": (st, [c_vp, ctypes.c_int, u32]),
+        "cbs_context_set_br_method": (st, [c_vp, ctypes.c_int, u32, u32]),
         "cbs_export_lmkcdey_keys": (st, [c_vp, c_vp, c_vp, c_vp, c_vp]),
-        "cbs_import_lmkcdey_keys": (st, [c_vp, u32, c_vp, sz, c_vp, sz]),
-        "cbs_generate_lmkcdey_keys_host": (st, [c_vp, u64, u32, c_vp, c_vp, c_vp, c_vp]),
-        "cbs_lmkcdey_auto_maps_host": (st, [u32, u32, c_vp]),
+        "cbs_import_lmkcdey_keys": (st, [c_vp, u32, u32, c_vp, sz, c_vp, sz]),
+        "cbs_generate_lmkcdey_keys_host": (st, [c_vp, u64, u32, u32, c_vp, c_vp, c_vp, c_vp]),
+        "cbs_lmkcdey_auto_maps_host": (st, [u32, u32, u32, c_vp, c_vp]),
         "cbs_lmkcdey_eval_acc_batch_device": (st, [c_vp, c_vp, u32, c_vp, u32, c_vp]),
         "cbs_export_mb_bsk": (st, [c_vp, c_vp, c_vp]),
         "cbs_generate_mb_bsk_host": (st, [c_vp, u64, u32, c_vp, c_vp]),
@@ -249,24 +249,26 @@ def preset_params(name: str) -> CbsParams:
     return p
 
 
-def generate_lmkcdey_keys_host(params: CbsParams, seed: int, num_auto_keys: int):
-    """LMKCDEY keys (eval [n][2*digits_g][2][N], auto [1 + num_auto_keys][digits_g][2][N], NTT domain)
-    of the key set cbs_keygen(seed) makes, generated on the host."""
+def generate_lmkcdey_keys_host(params: CbsParams, seed: int, num_auto_keys: int, window: int = 0):
+    """LMKCDEY keys (eval [n][2*digits_g][2][N], auto [keys][digits_g][2][N], NTT domain) of the key set
+    cbs_keygen(seed) makes, generated on the host."""
     import numpy as np
     ew, aw = ctypes.c_size_t(), ctypes.c_size_t()
-    call("cbs_generate_lmkcdey_keys_host", ctypes.byref(params), seed, num_auto_keys, None, None, ctypes.byref(ew),
-         ctypes.byref(aw))
-    ev, au = np.zeros(ew.value, np.uint64), np.zeros(aw.value, np.uint64)
-    call("cbs_generate_lmkcdey_keys_host", ctypes.byref(params), seed, num_auto_keys, ev.ctypes.data, au.ctypes.data,
+    call("cbs_generate_lmkcdey_keys_host", ctypes.byref(params), seed, num_auto_keys, window, None, None,
          ctypes.byref(ew), ctypes.byref(aw))
+    ev, au = np.zeros(ew.value, np.uint64), np.zeros(aw.value, np.uint64)
+    call("cbs_generate_lmkcdey_keys_host", ctypes.byref(params), seed, num_auto_keys, window, ev.ctypes.data,
+         au.ctypes.data, ctypes.byref(ew), ctypes.byref(aw))
     return ev.reshape(params.n, 2 * params.digits_g, 2, params.N), au.reshape(-1, params.digits_g, 2, params.N)
 
 
-def lmkcdey_auto_maps_host(N: int, num_auto_keys: int):
-    """NTT-domain automorphism maps [1 + num_auto_keys][N] of the LMKCDEY key set."""
+def lmkcdey_auto_maps_host(N: int, num_auto_keys: int, window: int = 0):
+    """NTT-domain automorphism maps [keys][N] of the LMKCDEY key set."""
     import numpy as np
-    out = np.zeros((1 + num_auto_keys, N), np.uint32)
-    call("cbs_lmkcdey_auto_maps_host", N, num_auto_keys, out.ctypes.data)
+    count = ctypes.c_uint32()
+    call("cbs_lmkcdey_auto_maps_host", N, num_auto_keys, window, None, ctypes.byref(count))
+    out = np.zeros((count.value, N), np.uint32)
+    call("cbs_lmkcdey_auto_maps_host", N, num_auto_keys, window, out.ctypes.data, None)
     return out
 
 
@@ -376,10 +378,11 @@ class Context:
         """Two-digit grouped blind-rotation schedule (BR_SCHEDULE_*; AUTO = the tuned one)."""
         call("cbs_context_set_br_schedule", self._h, schedule)
 
-    def set_br_method(self, method: int, num_auto_keys: int = 10) -> None:
+    def set_br_method(self, method: int, num_auto_keys: int = 10, window: int = 0) -> None:
         """Blind-rotation method: BR_GINX (default) or BR_LMKCDEY with automorphism keys for 2N - 5
-        and 5^1 .. 5^num_auto_keys (NTT backend, num_lut = 1, g (digits_g + 1) >= log2 Q)."""
-        call("cbs_context_set_br_method", self._h, method, num_auto_keys)
+        and 5^1 .. 5^num_auto_keys, or with window > 1 the windowed key set (NTT backend,
+        num_lut = 1, g (digits_g + 1) >= log2 Q)."""
+        call("cbs_context_set_br_method", self._h, method, num_auto_keys, window)
 
     def export_lmkcdey_keys(self):
         """LMKCDEY keys (NTT domain): eval [n][2*digits_g][2][N], auto [1 + num_auto_keys][digits_g][2][N]."""
@@ -391,12 +394,13 @@ class Context:
         p = self.params
         return ev.reshape(p.n, 2 * p.digits_g, 2, p.N), au.reshape(-1, p.digits_g, 2, p.N)
 
-    def import_lmkcdey_keys(self, num_auto_keys: int, eval_keys, auto_keys) -> None:
+    def import_lmkcdey_keys(self, num_auto_keys: int, eval_keys, auto_keys, window: int = 0) -> None:
         """LMKCDEY keys in the layout of export_lmkcdey_keys (selects the method)."""
         import numpy as np
         ev = np.ascontiguousarray(eval_keys, np.uint64).reshape(-1)
         au = np.ascontiguousarray(auto_keys, np.uint64).reshape(-1)
-        call("cbs_import_lmkcdey_keys", self._h, num_auto_keys, ev.ctypes.data, ev.size, au.ctypes.data, au.size)
+        call("cbs_import_lmkcdey_keys", self._h, num_auto_keys, window, ev.ctypes.data, ev.size, au.ctypes.data,
+             au.size)
 
     def export_mb_bsk(self):
         """Grouped blind-rotation keys [ceil(n/mb)][keys][2*digits_g][2][N] (NTT domain; keys = 3, 7,

@@ -102,6 +102,7 @@ struct cbs_context {
     // Montgomery-form device copies, the automorphism maps and the discrete-log table
     int br_method = 0;                   // CBS_BR_GINX or CBS_BR_LMKCDEY
     uint32_t lmk_num_auto = 0;
+    uint32_t lmk_window = 0;             // > 1: the windowed key set (5^1 .. 5^w, 5^2w, 5^3w, ...)
     bool lmk_ready = false;
     std::vector<uint64_t> h_lmk_eval, h_lmk_auto;
     cbs::DevBuf<uint64_t> d_lmk_eval, d_lmk_auto;

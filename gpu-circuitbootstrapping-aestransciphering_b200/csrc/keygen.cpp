@@ -202,19 +202,24 @@ void generate_mb_bsk(const cbs_params& p, const host::NttTables& t, const HostKe
     for (auto& th : pool) th.join();
 }
 
-std::vector<uint32_t> lmkcdey_auto_pows(uint32_t N, uint32_t num_auto_keys) {
+std::vector<uint32_t> lmkcdey_auto_pows(uint32_t N, uint32_t num_auto_keys, uint32_t window) {
     const uint32_t M = 2 * N;
-    std::vector<uint32_t> pows(1 + num_auto_keys);
-    pows[0] = M - 5;
-    uint64_t v = 1;
-    for (uint32_t i = 1; i <= num_auto_keys; ++i) {
-        v = (v * 5) % M;
-        pows[i] = static_cast<uint32_t>(v);
+    auto pow5 = [M](uint32_t k) {
+        uint64_t v = 1;
+        for (uint32_t i = 0; i < k; ++i) v = (v * 5) % M;
+        return static_cast<uint32_t>(v);
+    };
+    std::vector<uint32_t> pows{M - 5};
+    if (window > 1) {
+        for (uint32_t k = 1; k <= window; ++k) pows.push_back(pow5(k));
+        for (uint32_t k = 2 * window; k <= N / 2 - 1; k += window) pows.push_back(pow5(k));
+    } else {
+        for (uint32_t k = 1; k <= num_auto_keys; ++k) pows.push_back(pow5(k));
     }
     return pows;
 }
 
-void lmkcdey_auto_maps(uint32_t N, uint32_t num_auto_keys, std::vector<uint32_t>& maps) {
+void lmkcdey_auto_maps(uint32_t N, uint32_t num_auto_keys, uint32_t window, std::vector<uint32_t>& maps) {
     uint32_t logn = 0;
     while ((1u << logn) < N) ++logn;
     auto brev = [logn](uint32_t x) {
@@ -222,7 +227,7 @@ void lmkcdey_auto_maps(uint32_t N, uint32_t num_auto_keys, std::vector<uint32_t>
         for (uint32_t i = 0; i < logn; ++i) r |= ((x >> i) & 1u) << (logn - 1 - i);
         return r;
     };
-    const auto pows = lmkcdey_auto_pows(N, num_auto_keys);
+    const auto pows = lmkcdey_auto_pows(N, num_auto_keys, window);
     maps.assign(pows.size() * N, 0);
     // slot t holds the evaluation at zeta^(2 brev(t) + 1); psi_k reads the slot of its k-th power
     for (size_t k = 0; k < pows.size(); ++k)
@@ -233,7 +238,7 @@ void lmkcdey_auto_maps(uint32_t N, uint32_t num_auto_keys, std::vector<uint32_t>
 }
 
 void generate_lmkcdey_keys(const cbs_params& p, const host::NttTables& t, const HostKeys& k, uint32_t num_auto_keys,
-                           uint64_t seed, std::vector<uint64_t>& eval, std::vector<uint64_t>& autok) {
+                           uint32_t window, uint64_t seed, std::vector<uint64_t>& eval, std::vector<uint64_t>& autok) {
     const uint32_t N = p.N, n = p.n, dg = p.digits_g, M = 2 * N;
     int g = 0;
     while ((1u << g) < p.base_g) ++g;
@@ -242,8 +247,8 @@ void generate_lmkcdey_keys(const cbs_params& p, const host::NttTables& t, const 
     std::vector<uint64_t> gp(dg);
     for (uint32_t j = 0; j < dg; ++j) gp[j] = (1ull << (g * (j + 1))) % Q;
     std::vector<uint32_t> maps;
-    lmkcdey_auto_maps(N, num_auto_keys, maps);
-    const uint32_t count = 1 + num_auto_keys;
+    lmkcdey_auto_maps(N, num_auto_keys, window, maps);
+    const uint32_t count = static_cast<uint32_t>(maps.size() / N);
     eval.assign(static_cast<size_t>(n) * 2 * dg * 2 * N, 0);
     autok.assign(static_cast<size_t>(count) * dg * 2 * N, 0);
     const unsigned nth = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));

@@ -71,17 +71,18 @@ uint32_t mb_subset_mask(uint32_t mb, uint32_t idx);
 void generate_mb_bsk(const cbs_params& p, const host::NttTables& t, const HostKeys& k, uint32_t mb, uint64_t seed,
                      std::vector<uint64_t>& out);
 // LMKCDEY keys (the reference's method = LMKCDEY, bitwise/src/cirbts/cirbts-init.cu:630-726;
-// non-windowed key set of cirbts-lmkcdey.cu:66-103): automorphism powers pows[0] = 2N - 5,
-// pows[i] = 5^i mod 2N (i = 1 .. num_auto_keys); maps [count][N] the NTT-domain permutations
-// out[t] = in[map[t]] of X -> X^k; eval [n][2*digits_g][2][N] = RGSW(X^{s_i}) and autok
-// [count][digits_g][2][N] = RLWE(0) with b -= 2^{g (j+1)} psi_k(s), NTT domain, gadget powers
-// 2^{g (j+1)} (the approximate decomposition drops the first g-bit digit).  One generator
-// per key, seeded seed ^ (0x9e3779b97f4a7c15 (i + 1)) for eval key i and
+// key set of cirbts-lmkcdey.cu:66-103): automorphism powers pows[0] = 2N - 5, then 5^i mod 2N
+// (i = 1 .. num_auto_keys), or for window > 1 5^1 .. 5^window and 5^(2 window), 5^(3 window),
+// ... below 5^(N/2); maps [count][N] the NTT-domain permutations out[t] = in[map[t]] of X -> X^k;
+// eval [n][2*digits_g][2][N] = RGSW(X^{s_i}) and autok [count][digits_g][2][N] = RLWE(0) with
+// b -= 2^{g (j+1)} psi_k(s), NTT domain, gadget powers 2^{g (j+1)} (the approximate
+// decomposition drops the first g-bit digit).  One generator per key, seeded
+// seed ^ (0x9e3779b97f4a7c15 (i + 1)) for eval key i and
 // seed ^ 0x6c6d6b6364657921 ^ (0x9e3779b97f4a7c15 (k + 1)) for automorphism key k.
-std::vector<uint32_t> lmkcdey_auto_pows(uint32_t N, uint32_t num_auto_keys);
-void lmkcdey_auto_maps(uint32_t N, uint32_t num_auto_keys, std::vector<uint32_t>& maps);
+std::vector<uint32_t> lmkcdey_auto_pows(uint32_t N, uint32_t num_auto_keys, uint32_t window);
+void lmkcdey_auto_maps(uint32_t N, uint32_t num_auto_keys, uint32_t window, std::vector<uint32_t>& maps);
 void generate_lmkcdey_keys(const cbs_params& p, const host::NttTables& t, const HostKeys& k, uint32_t num_auto_keys,
-                           uint64_t seed, std::vector<uint64_t>& eval, std::vector<uint64_t>& autok);
+                           uint32_t window, uint64_t seed, std::vector<uint64_t>& eval, std::vector<uint64_t>& autok);
 
 // LWE encryption of m (already scaled) mod q under s_lwe
 void lwe_encrypt(const cbs_params& p, const HostKeys& k, Rng& rng, uint64_t m, uint64_t* out_a, uint64_t* out_b);

@@ -53,6 +53,7 @@ struct LmkArgs {
     const uint32_t* maps;     // [count][N] NTT-domain permutations out[t] = in[map[t]]
     const int32_t* log_tab;   // [N] signed base-5 logarithm of the odd residue 2i + 1
     uint32_t num_auto_keys;
+    uint32_t window;          // > 1: windowed key set, a skip closes with 5^(q window) then 5^r
     uint32_t digits;
     int gbits;
 };
@@ -239,9 +240,32 @@ __global__ void __launch_bounds__(NttPlan<LOGN>::T, 256 / NttPlan<LOGN>::T + (Nt
         for (int j = 0; j < 8; ++j) acc1[8 * tid + j] = v[j];
         __syncthreads();
     }
-    uint32_t half = 0, i = NH - 1, pos = 0, hi = 0, skips = 0, stage = 0;
+    uint32_t half = 0, i = NH - 1, pos = 0, hi = 0, skips = 0, stage = 0, pend = 0;
+    bool has_pend = false;
+    const uint32_t W = a.window;
+    // the automorphisms closing a run of sk steps (apply_skip, cirbts-lmkcdey.cu:311-325): the key
+    // of 5^sk, or with a window those of 5^(q W) and 5^r (sk = q W + r); the second is left pending
+    auto key_of = [W](uint32_t k) { return (W > 1 && k > W) ? W + k / W - 1 : k; };
+    auto skip_ops = [&](uint32_t sk, uint32_t& arg) {
+        if (W <= 1) {
+            arg = sk;
+            return;
+        }
+        const uint32_t q = sk / W, r = sk % W;
+        arg = q ? key_of(q * W) : key_of(r);
+        if (q && r) {
+            pend = key_of(r);
+            has_pend = true;
+        }
+    };
     // the next operation: is_auto and its key (automorphism power index or coefficient)
     auto next = [&](bool& is_auto, uint32_t& arg) -> bool {
+        if (has_pend) {
+            has_pend = false;
+            is_auto = true;
+            arg = pend;
+            return true;
+        }
         for (;;) {
             if (stage == 0) {  // enter the step of logarithm i (i = 0: the special bucket)
                 if (i > 0) {
@@ -251,7 +275,7 @@ __global__ void __launch_bounds__(NttPlan<LOGN>::T, 256 / NttPlan<LOGN>::T + (Nt
                     stage = 1;
                     if (pos != hi && skips != 0) {
                         is_auto = true;
-                        arg = skips;
+                        skip_ops(skips, arg);
                         skips = 0;
                         return true;
                     }
@@ -269,9 +293,9 @@ __global__ void __launch_bounds__(NttPlan<LOGN>::T, 256 / NttPlan<LOGN>::T + (Nt
                 }
                 ++skips;
                 stage = 2;
-                if (skips == a.num_auto_keys || i == 1) {
+                if ((W <= 1 && skips == a.num_auto_keys) || i == 1) {
                     is_auto = true;
-                    arg = skips;
+                    skip_ops(skips, arg);
                     skips = 0;
                     return true;
                 }
@@ -393,8 +417,8 @@ static bool lmk_gadget_ok(const cbs_params& p) {
 }
 
 static size_t lmk_eval_words(const cbs_params& p) { return static_cast<size_t>(p.n) * 2 * p.digits_g * 2 * p.N; }
-static size_t lmk_auto_words(const cbs_params& p, uint32_t num_auto) {
-    return (1ull + num_auto) * p.digits_g * 2 * p.N;
+static size_t lmk_auto_words(const cbs_params& p, uint32_t num_auto, uint32_t window) {
+    return lmkcdey_auto_pows(p.N, num_auto, window).size() * p.digits_g * 2 * p.N;
 }
 
 // host keys (c->h_lmk_eval / h_lmk_auto, NTT domain) -> Montgomery-form device keys, maps, log table
@@ -404,7 +428,7 @@ static cbs_status upload_lmkcdey(cbs_context* c) {
     for (size_t i = 0; i < ev.size(); ++i) ev[i] = fm.mul(c->h_lmk_eval[i], c->mont_r);
     for (size_t i = 0; i < au.size(); ++i) au[i] = fm.mul(c->h_lmk_auto[i], c->mont_r);
     std::vector<uint32_t> maps;
-    lmkcdey_auto_maps(c->p.N, c->lmk_num_auto, maps);
+    lmkcdey_auto_maps(c->p.N, c->lmk_num_auto, c->lmk_window, maps);
     const auto log_tab = lmk_log_table(c->p.N);
     cudaStream_t s = c->stream;
     CBS_CUDA_TRY(c->d_lmk_eval.upload(ev.data(), ev.size(), s));
@@ -430,7 +454,8 @@ cbs_status prepare_lmkcdey(cbs_context* c) {
         return CBS_ERR_UNSUPPORTED;
     }
     try {
-        generate_lmkcdey_keys(c->p, c->tab, c->hk, c->lmk_num_auto, c->key_seed ^ kLmkSeedTweak, c->h_lmk_eval,
+        generate_lmkcdey_keys(c->p, c->tab, c->hk, c->lmk_num_auto, c->lmk_window, c->key_seed ^ kLmkSeedTweak,
+                              c->h_lmk_eval,
                               c->h_lmk_auto);
     } catch (const std::exception& e) {
         set_error(std::string("LMKCDEY keys: ") + e.what());
@@ -453,6 +478,7 @@ static LmkArgs lmk_args(const cbs_context* c) {
     a.maps = c->d_lmk_maps.p;
     a.log_tab = c->d_lmk_log.p;
     a.num_auto_keys = c->lmk_num_auto;
+    a.window = c->lmk_window > 1 ? c->lmk_window : 0;
     a.digits = c->p.digits_g;
     int g = 0;
     while ((1u << g) < c->p.base_g) ++g;
@@ -481,7 +507,7 @@ using namespace cbs;
 
 extern "C" {
 
-cbs_status cbs_context_set_br_method(cbs_context* ctx, int method, uint32_t num_auto_keys) {
+cbs_status cbs_context_set_br_method(cbs_context* ctx, int method, uint32_t num_auto_keys, uint32_t window) {
     CBS_CHECK_ARG(ctx, "set_br_method: null context");
     CBS_CHECK_ARG(method == CBS_BR_GINX || method == CBS_BR_LMKCDEY, "set_br_method: unknown method");
     if (method == CBS_BR_GINX) {
@@ -491,6 +517,7 @@ cbs_status cbs_context_set_br_method(cbs_context* ctx, int method, uint32_t num_
     }
     const cbs_params& p = ctx->p;
     CBS_CHECK_ARG(num_auto_keys >= 1 && num_auto_keys < p.N / 2, "set_br_method: num_auto_keys must lie in [1, N/2)");
+    CBS_CHECK_ARG(window < p.N / 2, "set_br_method: window must lie in [0, N/2)");
     if (ctx->br_backend != CBS_BR_NTT) {
         set_error("set_br_method: the LMKCDEY blind rotation is implemented for the NTT backend");
         return CBS_ERR_UNSUPPORTED;
@@ -506,13 +533,15 @@ cbs_status cbs_context_set_br_method(cbs_context* ctx, int method, uint32_t num_
         return CBS_ERR_UNSUPPORTED;
     }
     CBS_CHECK_ARG(p.n < 65536 && p.n <= 2 * p.N, "set_br_method: LWE dimension too large for the LMKCDEY kernel");
-    if (ctx->br_method != CBS_BR_LMKCDEY || ctx->lmk_num_auto != num_auto_keys) {
+    if (window == 1) window = 0;  // a window of 1 is the plain key set
+    if (ctx->br_method != CBS_BR_LMKCDEY || ctx->lmk_num_auto != num_auto_keys || ctx->lmk_window != window) {
         ctx->lmk_ready = false;
         ctx->h_lmk_eval.clear();
         ctx->h_lmk_auto.clear();
     }
     ctx->br_method = CBS_BR_LMKCDEY;
     ctx->lmk_num_auto = num_auto_keys;
+    ctx->lmk_window = window;
     ctx->aes.drop_graphs();
     return prepare_lmkcdey(ctx);
 }
@@ -531,18 +560,19 @@ cbs_status cbs_export_lmkcdey_keys(const cbs_context* ctx, uint64_t* eval, uint6
     return CBS_OK;
 }
 
-cbs_status cbs_import_lmkcdey_keys(cbs_context* ctx, uint32_t num_auto_keys, const uint64_t* eval, size_t eval_words,
-                                   const uint64_t* autok, size_t auto_words) {
+cbs_status cbs_import_lmkcdey_keys(cbs_context* ctx, uint32_t num_auto_keys, uint32_t window, const uint64_t* eval,
+                                   size_t eval_words, const uint64_t* autok, size_t auto_words) {
     CBS_CHECK_ARG(ctx && eval && autok, "import_lmkcdey_keys: null argument");
     if (!ctx->keys_ready) {
         set_error("import_lmkcdey_keys: import or generate the keys first");
         return CBS_ERR_NOT_READY;
     }
     const cbs_params& p = ctx->p;
-    CBS_CHECK_ARG(num_auto_keys >= 1 && num_auto_keys < p.N / 2,
-                  "import_lmkcdey_keys: num_auto_keys must lie in [1, N/2)");
-    if (eval_words != lmk_eval_words(p) || auto_words != lmk_auto_words(p, num_auto_keys)) {
-        set_error("import_lmkcdey_keys: words must be n * 2 digits_g * 2 N and (1 + num_auto_keys) digits_g * 2 N");
+    CBS_CHECK_ARG(num_auto_keys >= 1 && num_auto_keys < p.N / 2 && window < p.N / 2,
+                  "import_lmkcdey_keys: num_auto_keys must lie in [1, N/2), window in [0, N/2)");
+    if (eval_words != lmk_eval_words(p) || auto_words != lmk_auto_words(p, num_auto_keys, window)) {
+        set_error("import_lmkcdey_keys: words must be n * 2 digits_g * 2 N and keys * digits_g * 2 N (keys: 1 + "
+                  "num_auto_keys, or with a window 1 + window + floor((N/2 - 1) / window) - 1)");
         return CBS_ERR_SHAPE_MISMATCH;
     }
     for (size_t i = 0; i < eval_words; ++i) CBS_CHECK_ARG(eval[i] < p.Q, "import_lmkcdey_keys: words must be residues");
@@ -552,7 +582,7 @@ cbs_status cbs_import_lmkcdey_keys(cbs_context* ctx, uint32_t num_auto_keys, con
     ctx->has_secret = false;
     ctx->br_method = CBS_BR_GINX;
     ctx->lmk_ready = false;
-    cbs_status st = cbs_context_set_br_method(ctx, CBS_BR_LMKCDEY, num_auto_keys);
+    cbs_status st = cbs_context_set_br_method(ctx, CBS_BR_LMKCDEY, num_auto_keys, window);
     ctx->has_secret = had_secret;
     if (st != CBS_OK && st != CBS_ERR_NOT_READY) {
         ctx->br_method = CBS_BR_GINX;
@@ -569,13 +599,14 @@ cbs_status cbs_import_lmkcdey_keys(cbs_context* ctx, uint32_t num_auto_keys, con
 }
 
 cbs_status cbs_generate_lmkcdey_keys_host(const cbs_params* params, uint64_t seed, uint32_t num_auto_keys,
-                                          uint64_t* eval, uint64_t* autok, size_t* eval_words, size_t* auto_words) {
+                                          uint32_t window, uint64_t* eval, uint64_t* autok, size_t* eval_words,
+                                          size_t* auto_words) {
     CBS_CHECK_ARG(params && eval_words && auto_words, "generate_lmkcdey_keys_host: null argument");
     if (cbs_status st = validate_params(*params)) return st;
-    CBS_CHECK_ARG(num_auto_keys >= 1 && num_auto_keys < params->N / 2,
-                  "generate_lmkcdey_keys_host: num_auto_keys must lie in [1, N/2)");
+    CBS_CHECK_ARG(num_auto_keys >= 1 && num_auto_keys < params->N / 2 && window < params->N / 2,
+                  "generate_lmkcdey_keys_host: num_auto_keys must lie in [1, N/2), window in [0, N/2)");
     *eval_words = lmk_eval_words(*params);
-    *auto_words = lmk_auto_words(*params, num_auto_keys);
+    *auto_words = lmk_auto_words(*params, num_auto_keys, window);
     if (!eval || !autok) return CBS_OK;
     host::NttTables t;
     if (!host::make_ntt_tables(params->N, params->Q, t)) {
@@ -586,7 +617,7 @@ cbs_status cbs_generate_lmkcdey_keys_host(const cbs_params* params, uint64_t see
         HostKeys k;
         generate_keys(*params, t, seed, k);
         std::vector<uint64_t> ev, au;
-        generate_lmkcdey_keys(*params, t, k, num_auto_keys, seed ^ kLmkSeedTweak, ev, au);
+        generate_lmkcdey_keys(*params, t, k, num_auto_keys, window, seed ^ kLmkSeedTweak, ev, au);
         std::memcpy(eval, ev.data(), ev.size() * sizeof(uint64_t));
         std::memcpy(autok, au.data(), au.size() * sizeof(uint64_t));
     } catch (const std::exception& e) {
@@ -596,11 +627,14 @@ cbs_status cbs_generate_lmkcdey_keys_host(const cbs_params* params, uint64_t see
     return CBS_OK;
 }
 
-cbs_status cbs_lmkcdey_auto_maps_host(uint32_t N, uint32_t num_auto_keys, uint32_t* maps) {
-    CBS_CHECK_ARG(maps && N >= 64 && (N & (N - 1)) == 0 && num_auto_keys >= 1 && num_auto_keys < N / 2,
+cbs_status cbs_lmkcdey_auto_maps_host(uint32_t N, uint32_t num_auto_keys, uint32_t window, uint32_t* maps,
+                                      uint32_t* count) {
+    CBS_CHECK_ARG(N >= 64 && (N & (N - 1)) == 0 && num_auto_keys >= 1 && num_auto_keys < N / 2 && window < N / 2,
                   "lmkcdey_auto_maps_host: bad arguments");
     std::vector<uint32_t> m;
-    lmkcdey_auto_maps(N, num_auto_keys, m);
+    lmkcdey_auto_maps(N, num_auto_keys, window, m);
+    if (count) *count = static_cast<uint32_t>(m.size() / N);
+    if (!maps) return CBS_OK;
     std::memcpy(maps, m.data(), m.size() * sizeof(uint32_t));
     return CBS_OK;
 }

@@ -183,8 +183,11 @@ cbs_status cbs_context_set_br_multibit(cbs_context *ctx, uint32_t mb);
  * the bootstrap cirbts-bootstrap.cu:600-720).  CBS_BR_LMKCDEY multiplies the accumulator by
  * RGSW(X^{s_i}) per coefficient with automorphisms X -> X^{5^k} (key switches) between
  * coefficients of different base-5 logarithm of their odd mask; num_auto_keys is the largest
- * power k with a key (the reference's numAutoKeys; keys for 2N - 5 and 5^1 .. 5^num_auto_keys,
- * non-windowed).  Its keys (RGSW(X^{s_i}) and the automorphism keys, approximate gadget with
+ * power k with a key (the reference's numAutoKeys; keys for 2N - 5 and 5^1 .. 5^num_auto_keys).
+ * window > 1 selects the reference's windowed key set (CIRBTS_LMK_AUTOKEYS_WINDOW,
+ * cirbts-lmkcdey.cu:49-103, 311-325): keys for 2N - 5, 5^1 .. 5^window and 5^(2 window),
+ * 5^(3 window), ... below 5^(N/2), a run of s steps closing with 5^(q window) then 5^r
+ * (s = q window + r); window 0 or 1: non-windowed.  Its keys (RGSW(X^{s_i}) and the automorphism keys, approximate gadget with
  * powers 2^{g (j+1)}: the first g-bit digit is dropped, as the reference decomposes) are
  * generated from the context's secrets when keys exist or are next generated (seeded host
  * generator; for device-generated keys import them).  Preconditions, else CBS_ERR_UNSUPPORTED:
@@ -194,23 +197,26 @@ cbs_status cbs_context_set_br_multibit(cbs_context *ctx, uint32_t mb);
  * absorb (the reference's LMKCDEY path passes the masks unswitched and has the same limit).
  * The masks are rounded to Z_2N and forced odd (identical to the reference when q_lwe = 2N). */
 enum { CBS_BR_GINX = 0, CBS_BR_LMKCDEY = 1 };
-cbs_status cbs_context_set_br_method(cbs_context *ctx, int method, uint32_t num_auto_keys);
+cbs_status cbs_context_set_br_method(cbs_context *ctx, int method, uint32_t num_auto_keys, uint32_t window);
 /* The LMKCDEY keys, NTT domain: eval [n][2*digits_g][2][N] (RGSW(X^{s_i}); row 2j carries
- * 2^{g(j+1)} X^{s_i} on component a, row 2j+1 on b), autok [1 + num_auto_keys][digits_g][2][N]
- * (RLWE(0) with b -= 2^{g(j+1)} psi_k(s) for k = 2N - 5, 5^1, 5^2, ...).  Null outputs: only
- * the word counts are set. */
+ * 2^{g(j+1)} X^{s_i} on component a, row 2j+1 on b), autok [keys][digits_g][2][N] (RLWE(0) with
+ * b -= 2^{g(j+1)} psi_k(s) for the key set's powers k in order: 2N - 5, 5^1, 5^2, ...).  Null
+ * outputs: only the word counts are set. */
 cbs_status cbs_export_lmkcdey_keys(const cbs_context *ctx, uint64_t *eval, uint64_t *autok, size_t *eval_words,
                                    size_t *auto_words);
 /* Keys in the layout of cbs_export_lmkcdey_keys (a server without secrets); selects LMKCDEY
  * like cbs_context_set_br_method. */
-cbs_status cbs_import_lmkcdey_keys(cbs_context *ctx, uint32_t num_auto_keys, const uint64_t *eval, size_t eval_words,
-                                   const uint64_t *autok, size_t auto_words);
+cbs_status cbs_import_lmkcdey_keys(cbs_context *ctx, uint32_t num_auto_keys, uint32_t window, const uint64_t *eval,
+                                   size_t eval_words, const uint64_t *autok, size_t auto_words);
 /* Host-only generation of the LMKCDEY keys a context keyed with the same seed produces. */
 cbs_status cbs_generate_lmkcdey_keys_host(const cbs_params *params, uint64_t seed, uint32_t num_auto_keys,
-                                          uint64_t *eval, uint64_t *autok, size_t *eval_words, size_t *auto_words);
-/* NTT-domain automorphism maps [1 + num_auto_keys][N] of the key set (out[t] = in[map[t]] is
- * X -> X^k in the NTT domain; OpenFHE's PrecomputeAutoMap for this transform's slot order). */
-cbs_status cbs_lmkcdey_auto_maps_host(uint32_t N, uint32_t num_auto_keys, uint32_t *maps);
+                                          uint32_t window, uint64_t *eval, uint64_t *autok, size_t *eval_words,
+                                          size_t *auto_words);
+/* NTT-domain automorphism maps [keys][N] of the key set (out[t] = in[map[t]] is X -> X^k in the
+ * NTT domain; OpenFHE's PrecomputeAutoMap for this transform's slot order); *count (optional)
+ * receives the number of keys; maps may be NULL. */
+cbs_status cbs_lmkcdey_auto_maps_host(uint32_t N, uint32_t num_auto_keys, uint32_t window, uint32_t *maps,
+                                      uint32_t *count);
 /* LMKCDEY_EvalAcc (cirbts-lmkcdey.cu:105-407) on a batch, device pointers: a_neg [batch][a_stride]
  * the masks mod 2N as the reference's EvalAcc receives them (already negated by the caller,
  * cirbts-bootstrap.cu:681-689), acc [batch][2][N] NTT domain, updated in place.  One CTA per

@@ -152,9 +152,10 @@ class GPUCirBTSContext {
 
     // The context's BINFHE_METHOD (GenerateCirBTSContext(paramset, GINX | LMKCDEY),
     // cirbts-init.cu:630-726): CBS_BR_GINX or CBS_BR_LMKCDEY with automorphism keys for 2N - 5 and
-    // 5^1 .. 5^numAutoKeys; the LMKCDEY keys follow the context's secrets
-    void SetMethod(int method, uint32_t numAutoKeys = 10) {
-        check(cbs_context_set_br_method(ctx_, method, numAutoKeys), "SetMethod");
+    // 5^1 .. 5^numAutoKeys, or the windowed key set (CIRBTS_LMK_AUTOKEYS_WINDOW) when
+    // autoKeysWindow > 1; the LMKCDEY keys follow the context's secrets
+    void SetMethod(int method, uint32_t numAutoKeys = 10, uint32_t autoKeysWindow = 0) {
+        check(cbs_context_set_br_method(ctx_, method, numAutoKeys, autoKeysWindow), "SetMethod");
     }
     // cirbts.cuh:491 LMKCDEY_EvalAcc(params, a, d_acc): a [n] on the host, the masks mod 2N as the
     // bootstrap passes them (negated), d_acc [2][N] on the device (NTT domain), updated in place

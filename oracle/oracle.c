@@ -1886,27 +1886,48 @@ void orc_cbs_keygen_chacha_mb(const orc_cbs_params *p, double sigma_rlwe, const 
 /* LMKCDEY blind rotation (bitwise/src/cirbts/cirbts-lmkcdey.cu, keys cirbts-init.cu:630-726)   */
 /* ------------------------------------------------------------------------------------------ */
 
-/* automorphism powers of the non-windowed key set (cirbts-lmkcdey.cu:66-103 with window 0):
- * pows[0] = 2N - 5, pows[i] = 5^i mod 2N for i = 1 .. num_auto_keys; returns the count */
-uint32_t orc_lmkcdey_auto_pows(uint32_t N, uint32_t num_auto_keys, uint32_t *pows) {
-    const uint32_t M = 2 * N;
-    pows[0] = M - 5;
+static uint64_t lmk_pow5(uint32_t k, uint32_t M) {
     uint64_t v = 1;
-    for (uint32_t i = 1; i <= num_auto_keys; ++i) {
-        v = (v * 5) % M;
-        pows[i] = (uint32_t)v;
+    for (uint32_t i = 0; i < k; ++i) v = (v * 5) % M;
+    return v;
+}
+
+/* automorphism powers of the key set (cirbts-lmkcdey.cu:66-103): pows[0] = 2N - 5, then
+ * 5^i mod 2N for i = 1 .. num_auto_keys (window <= 1), or for window > 1 the powers 5^1 .. 5^window
+ * followed by 5^(2 window), 5^(3 window), ... up to N/2 - 1 (5^window is not repeated);
+ * returns the count.  pows may be NULL (count only). */
+uint32_t orc_lmkcdey_auto_pows(uint32_t N, uint32_t num_auto_keys, uint32_t window, uint32_t *pows) {
+    const uint32_t M = 2 * N, Nh = N / 2;
+    uint32_t c = 0;
+    if (pows) pows[c] = M - 5;
+    ++c;
+    if (window > 1) {
+        for (uint32_t k = 1; k <= window; ++k) {
+            if (pows) pows[c] = (uint32_t)lmk_pow5(k, M);
+            ++c;
+        }
+        for (uint32_t k = 2 * window; k <= Nh - 1; k += window) {
+            if (pows) pows[c] = (uint32_t)lmk_pow5(k, M);
+            ++c;
+        }
+    } else {
+        for (uint32_t k = 1; k <= num_auto_keys; ++k) {
+            if (pows) pows[c] = (uint32_t)lmk_pow5(k, M);
+            ++c;
+        }
     }
-    return 1 + num_auto_keys;
+    return c;
 }
 
 /* NTT-domain permutation of X -> X^k for every power: slot t holds the evaluation at
  * zeta^(2 brev(t) + 1), so psi_k(p) at slot t is p at the slot of zeta^((2 brev(t) + 1) k);
  * maps [count][N], out[t] = in[map[t]] as kernel_Permute_Only reads it (kernel.cu:7588) */
-void orc_lmkcdey_auto_maps(uint32_t N, uint32_t num_auto_keys, uint32_t *maps) {
+void orc_lmkcdey_auto_maps(uint32_t N, uint32_t num_auto_keys, uint32_t window, uint32_t *maps) {
     uint32_t log_n = 0;
     while ((1u << log_n) < N) ++log_n;
-    uint32_t *pows = (uint32_t *)malloc(sizeof(uint32_t) * (num_auto_keys + 1));
-    const uint32_t count = orc_lmkcdey_auto_pows(N, num_auto_keys, pows);
+    const uint32_t count = orc_lmkcdey_auto_pows(N, num_auto_keys, window, NULL);
+    uint32_t *pows = (uint32_t *)malloc(sizeof(uint32_t) * count);
+    orc_lmkcdey_auto_pows(N, num_auto_keys, window, pows);
     for (uint32_t k = 0; k < count; ++k)
         for (uint32_t t = 0; t < N; ++t) {
             const uint64_t e = 2ull * brev(t, log_n) + 1;
@@ -1936,7 +1957,7 @@ static uint64_t lmk_digit(uint64_t x, uint64_t Q, int g, uint32_t idx) {
  * seed ^ (0x9e3779b97f4a7c15 (i + 1)), automorphism key k with
  * seed ^ 0x6c6d6b6364657921 ^ (0x9e3779b97f4a7c15 (k + 1)). */
 void orc_lmkcdey_keygen(const orc_cbs_params *p, double sigma_rlwe, const int32_t *s_lwe, const int32_t *s_rlwe,
-                        uint32_t num_auto_keys, uint64_t seed, uint64_t *eval, uint64_t *autok) {
+                        uint32_t num_auto_keys, uint32_t window, uint64_t seed, uint64_t *eval, uint64_t *autok) {
     const uint32_t N = p->N, n = p->n, dg = p->digits_g, M = 2 * N;
     const int g = __builtin_ctz(p->base_g);
     const uint64_t Q = p->Q;
@@ -1971,9 +1992,9 @@ void orc_lmkcdey_keygen(const orc_cbs_params *p, double sigma_rlwe, const int32_
         free(mono);
         free(tmp);
     }
-    const uint32_t count = 1 + num_auto_keys;
+    const uint32_t count = orc_lmkcdey_auto_pows(N, num_auto_keys, window, NULL);
     uint32_t *maps = (uint32_t *)malloc(sizeof(uint32_t) * count * N);
-    orc_lmkcdey_auto_maps(N, num_auto_keys, maps);
+    orc_lmkcdey_auto_maps(N, num_auto_keys, window, maps);
 #pragma omp parallel for schedule(dynamic)
     for (long k = 0; k < (long)count; ++k) {
         uint64_t *tmp = (uint64_t *)malloc(sizeof(uint64_t) * N);
@@ -2078,8 +2099,25 @@ static void lmk_auto(lmk_ctx *c, uint64_t *acc, uint32_t k) {
  * cirbts-bootstrap.cu:681-689).  The LWE coefficients are bucketed by the signed base-5
  * logarithm of the odd residue (-a_neg) | 1, then processed bucket by bucket with
  * automorphisms between them. */
+/* key index of the power 5^k in the key set of orc_lmkcdey_auto_pows */
+static uint32_t lmk_key_index(uint32_t k, uint32_t window) {
+    return (window > 1 && k > window) ? window + k / window - 1 : k;
+}
+
+/* the automorphisms closing a run of `skips` steps: 5^skips (non-windowed), or 5^(q window)
+ * then 5^r for skips = q window + r (apply_skip, cirbts-lmkcdey.cu:311-325) */
+static void lmk_skip(lmk_ctx *c, uint64_t *acc, uint32_t skips, uint32_t window) {
+    if (window <= 1) {
+        lmk_auto(c, acc, skips);
+        return;
+    }
+    const uint32_t q = skips / window, r = skips % window;
+    if (q) lmk_auto(c, acc, lmk_key_index(q * window, window));
+    if (r) lmk_auto(c, acc, lmk_key_index(r, window));
+}
+
 void orc_lmkcdey_eval_acc(const orc_cbs_params *p, const uint64_t *eval, const uint64_t *autok, const uint32_t *maps,
-                          uint32_t num_auto_keys, const uint32_t *a_neg, uint32_t n, uint64_t *acc) {
+                          uint32_t num_auto_keys, uint32_t window, const uint32_t *a_neg, uint32_t n, uint64_t *acc) {
     const uint32_t N = p->N, Nh = N / 2, M = 2 * N, mask = M - 1, buckets = 2 * Nh, dg = p->digits_g;
     uint64_t *rp = (uint64_t *)malloc(sizeof(uint64_t) * N), *irp = (uint64_t *)malloc(sizeof(uint64_t) * N);
     uint64_t ninv[2];
@@ -2124,14 +2162,14 @@ void orc_lmkcdey_eval_acc(const orc_cbs_params *p, const uint64_t *eval, const u
             const uint32_t b = half == 0 ? (Nh - 1) - i : (Nh - 1) + i;
             if (offs[b] != offs[b + 1]) {
                 if (skips != 0) {
-                    lmk_auto(&c, acc, skips);
+                    lmk_skip(&c, acc, skips, window);
                     skips = 0;
                 }
                 for (uint32_t pos = offs[b]; pos < offs[b + 1]; ++pos) lmk_add(&c, acc, items[pos]);
             }
             ++skips;
-            if (skips == num_auto_keys || i == 1) {
-                lmk_auto(&c, acc, skips);
+            if ((window <= 1 && skips == num_auto_keys) || i == 1) {
+                lmk_skip(&c, acc, skips, window);
                 skips = 0;
             }
         }
@@ -2163,7 +2201,8 @@ void orc_lmkcdey_eval_acc(const orc_cbs_params *p, const uint64_t *eval, const u
  * the same when q_lwe = 2N) and negated, LMKCDEY_EvalAcc (which rounds them to odd), then the
  * finalize of the GINX form.  acc_out [batch][2][N] NTT domain. */
 void orc_blind_rotate_lmkcdey(const orc_cbs_params *p, const orc_cbs_keys *k, const uint64_t *eval,
-                              const uint64_t *autok, const uint32_t *maps, uint32_t num_auto_keys, const uint64_t *a,
+                              const uint64_t *autok, const uint32_t *maps, uint32_t num_auto_keys, uint32_t window,
+                              const uint64_t *a,
                               const uint64_t *b, uint32_t batch, uint32_t a_stride, uint64_t *acc_out, int finalize) {
     const uint32_t N = p->N, twoN = 2 * N;
     const uint64_t Q = p->Q;
@@ -2178,7 +2217,7 @@ void orc_blind_rotate_lmkcdey(const orc_cbs_params *p, const orc_cbs_keys *k, co
         memset(acc, 0, sizeof(uint64_t) * N);
         rotate_neg(acc + N, k->tv, bt, N, Q);
         ntt_fwd_one(acc + N, N, Q, k->rp);
-        orc_lmkcdey_eval_acc(p, eval, autok, maps, num_auto_keys, a_neg, p->n, acc);
+        orc_lmkcdey_eval_acc(p, eval, autok, maps, num_auto_keys, window, a_neg, p->n, acc);
         free(a_neg);
         if (finalize) {
             const uint64_t ninv = orc_invmod(N, Q);

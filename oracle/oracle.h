@@ -258,22 +258,24 @@ void orc_cbs_keygen_chacha_mb(const orc_cbs_params *p, double sigma_rlwe, const 
                               const int32_t *s_lwe, const int32_t *s_rlwe, uint32_t mb, uint64_t *mbk);
 
 /* ---------------- LMKCDEY blind rotation (bitwise/src/cirbts/cirbts-lmkcdey.cu; keys
- * cirbts-init.cu:630-726), the non-windowed key set.  Powers: [0] = 2N - 5, [i] = 5^i
- * (i = 1 .. num_auto_keys); maps [count][N] NTT-domain permutations out[t] = in[map[t]].
+ * cirbts-init.cu:630-726).  Powers: [0] = 2N - 5, then 5^i (i = 1 .. num_auto_keys), or for
+ * window > 1 (the reference's CIRBTS_LMK_AUTOKEYS_WINDOW) 5^1 .. 5^window and 5^(2 window),
+ * 5^(3 window), ... below 5^(N/2); maps [count][N] NTT-domain permutations out[t] = in[map[t]].
  * Keys: eval [n][2 digits_g][2][N] = RGSW(X^{s_i}), autok [count][digits_g][2][N] = RLWE(0)
  * with b -= 2^{g (j+1)} psi_k(s), both NTT domain, gadget powers 2^{g (j+1)} (the first
  * digit of the approximate decomposition is dropped).  orc_lmkcdey_eval_acc restates
  * LMKCDEY_EvalAcc on acc [2][N] in place for the negated masks a_neg mod 2N;
  * orc_blind_rotate_lmkcdey is the whole bootstrapping rotation (init, EvalAcc, finalize). */
-uint32_t orc_lmkcdey_auto_pows(uint32_t N, uint32_t num_auto_keys, uint32_t *pows);
-void orc_lmkcdey_auto_maps(uint32_t N, uint32_t num_auto_keys, uint32_t *maps);
+uint32_t orc_lmkcdey_auto_pows(uint32_t N, uint32_t num_auto_keys, uint32_t window, uint32_t *pows);
+void orc_lmkcdey_auto_maps(uint32_t N, uint32_t num_auto_keys, uint32_t window, uint32_t *maps);
 void orc_lmkcdey_keygen(const orc_cbs_params *p, double sigma_rlwe, const int32_t *s_lwe, const int32_t *s_rlwe,
-                        uint32_t num_auto_keys, uint64_t seed, uint64_t *eval, uint64_t *autok);
+                        uint32_t num_auto_keys, uint32_t window, uint64_t seed, uint64_t *eval, uint64_t *autok);
 void orc_lmkcdey_eval_acc(const orc_cbs_params *p, const uint64_t *eval, const uint64_t *autok, const uint32_t *maps,
-                          uint32_t num_auto_keys, const uint32_t *a_neg, uint32_t n, uint64_t *acc);
+                          uint32_t num_auto_keys, uint32_t window, const uint32_t *a_neg, uint32_t n, uint64_t *acc);
 void orc_blind_rotate_lmkcdey(const orc_cbs_params *p, const orc_cbs_keys *k, const uint64_t *eval,
-                              const uint64_t *autok, const uint32_t *maps, uint32_t num_auto_keys, const uint64_t *a,
-                              const uint64_t *b, uint32_t batch, uint32_t a_stride, uint64_t *acc_out, int finalize);
+                              const uint64_t *autok, const uint32_t *maps, uint32_t num_auto_keys, uint32_t window,
+                              const uint64_t *a, const uint64_t *b, uint32_t batch, uint32_t a_stride,
+                              uint64_t *acc_out, int finalize);
 
 #ifdef __cplusplus
 }

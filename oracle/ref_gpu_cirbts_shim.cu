@@ -178,7 +178,8 @@ int ref_cirbts_blind_rotate_mb4(uint64_t* acc, const uint64_t* d_a, uint32_t a_s
     return static_cast<int>(e);
 }
 
-// LMKCDEY_EvalAcc (bitwise/src/cirbts/cirbts-lmkcdey.cu:105-407, window 0) of one ciphertext
+// LMKCDEY_EvalAcc (bitwise/src/cirbts/cirbts-lmkcdey.cu:105-407; window > 1 is its
+// CIRBTS_LMK_AUTOKEYS_WINDOW key set, :49-103, and apply_skip, :302-325) of one ciphertext
 // in the reference's launch sequence, over the reference's own kernels: the bucket CSR built
 // on the host from the signed base-5 logarithms of (-a) | 1, kernel_Permute_Only for the
 // automorphisms, inwt/fnwt_1d_opt_batched, kernel_SignedDigitDecomposeLMKCDEY_Ciphertext /
@@ -188,7 +189,8 @@ int ref_cirbts_blind_rotate_mb4(uint64_t* acc, const uint64_t* d_a, uint32_t a_s
 // [1 + num_auto_keys][N] device; digits is the reference's digitsG - 1.  Scratch is
 // allocated once per call; returns the CUDA error code.
 int ref_cirbts_lmkcdey_eval_acc(uint64_t* acc, const uint32_t* h_a, uint32_t n, const uint64_t* eval,
-                                const uint64_t* autok, const uint32_t* maps, uint32_t num_auto_keys, const void* d_mod,
+                                const uint64_t* autok, const uint32_t* maps, uint32_t num_auto_keys, uint32_t window,
+                                const void* d_mod,
                                 const uint64_t* tw, const uint64_t* tws, const uint64_t* itw, const uint64_t* itws,
                                 const uint64_t* ninv, const uint64_t* ninv_s, uint32_t N, uint64_t Q, uint32_t base_g,
                                 uint32_t digits, void* stream) {
@@ -245,6 +247,43 @@ int ref_cirbts_lmkcdey_eval_acc(uint64_t* acc, const uint32_t* h_a, uint32_t n, 
         cudaMemcpyAsync(acc, ks0, N * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s);
         kernel_AddInPlace<<<grid, block, 0, s>>>(acc + N, ks1, mod, N);
     };
+    // the key set's powers and their indices (build_lmk_auto_pows: 2N - 5, then 5^1 .. 5^numAutoKeys,
+    // or 5^1 .. 5^window and every window-th power below 5^(N/2), repeats skipped)
+    const bool use_window = window > 1;
+    std::vector<uint64_t> pows{M - 5};
+    auto pow5 = [M](uint32_t k) {
+        uint64_t v = 1;
+        for (uint32_t i = 0; i < k; ++i) v = (v * 5) % M;
+        return v;
+    };
+    auto push = [&](uint32_t k) {
+        const uint64_t v = pow5(k);
+        for (uint64_t w : pows)
+            if (w == v) return;
+        pows.push_back(v);
+    };
+    if (use_window) {
+        for (uint32_t k = 1; k <= window; ++k) push(k);
+        for (uint32_t k = window; k <= Nh - 1; k += window) push(k);
+    } else {
+        for (uint32_t k = 1; k <= num_auto_keys; ++k) push(k);
+    }
+    auto key_index_for_step = [&](uint32_t step) {
+        const uint64_t v = pow5(step);
+        for (uint32_t i = 0; i < pows.size(); ++i)
+            if (pows[i] == v) return i;
+        return 0u;
+    };
+    auto apply_skip = [&](uint32_t skip) {
+        if (skip == 0) return;
+        if (!use_window) {
+            automorphism(key_index_for_step(skip));
+            return;
+        }
+        const uint32_t q = skip / window, r = skip % window;
+        if (q) automorphism(key_index_for_step(q * window));
+        if (r) automorphism(key_index_for_step(r));
+    };
     if (e == cudaSuccess) {
         kernel_Permute_Only<<<grid, block, 0, s>>>(pc1, acc + N, maps, N, 1, Q);
         cudaMemcpyAsync(acc + N, pc1, N * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s);
@@ -254,13 +293,19 @@ int ref_cirbts_lmkcdey_eval_acc(uint64_t* acc, const uint32_t* h_a, uint32_t n, 
                 const uint32_t b = half == 0 ? (Nh - 1) - i : (Nh - 1) + i;
                 if (offsets[b] != offsets[b + 1]) {
                     if (skips != 0) {
-                        automorphism(skips);
+                        if (use_window) apply_skip(skips);
+                        else automorphism(skips);
                         skips = 0;
                     }
                     for (uint32_t pos = offsets[b]; pos < offsets[b + 1]; ++pos) add_to_acc(items[pos]);
                 }
                 ++skips;
-                if (skips == num_auto_keys || i == 1) {
+                if (use_window) {
+                    if (i == 1) {
+                        apply_skip(skips);
+                        skips = 0;
+                    }
+                } else if (skips == num_auto_keys || i == 1) {
                     automorphism(skips);
                     skips = 0;
                 }

@@ -79,14 +79,15 @@ class OracleCbs:
         """LMKCDEY blind rotation [batch][2][N] (NTT domain) with the keys and maps of
         oracle_lmkcdey_keys."""
         vp, u32 = ctypes.c_void_p, ctypes.c_uint32
-        self.o.orc_blind_rotate_lmkcdey.argtypes = [vp, vp, vp, vp, vp, u32, vp, vp, u32, u32, vp, ctypes.c_int]
+        self.o.orc_blind_rotate_lmkcdey.argtypes = [vp, vp, vp, vp, vp, u32, u32, vp, vp, u32, u32, vp, ctypes.c_int]
         batch, stride = a.shape
         a = np.ascontiguousarray(a, np.uint64)
         b = np.ascontiguousarray(b, np.uint64)
         out = np.zeros((batch, 2, self.p.N), np.uint64)
         self.o.orc_blind_rotate_lmkcdey(ctypes.byref(self.op), ctypes.byref(self.ok), lmk["eval"].ctypes.data,
                                         lmk["auto"].ctypes.data, lmk["maps"].ctypes.data, lmk["num_auto_keys"],
-                                        a.ctypes.data, b.ctypes.data, batch, stride, out.ctypes.data, int(finalize))
+                                        lmk.get("window", 0), a.ctypes.data, b.ctypes.data, batch, stride,
+                                        out.ctypes.data, int(finalize))
         return out
 
     def br_mv(self, a: np.ndarray, b: np.ndarray) -> np.ndarray:
@@ -222,14 +223,16 @@ def oracle_keys_mb(oracle, p, keys: dict, mb: int, seed: int) -> np.ndarray:
 LMK_SEED_TWEAK = 0x6C6D6B6365797331  # the LMKCDEY keys' generator seed is the key seed xor this
 
 
-def oracle_lmkcdey_keys(oracle, p, keys: dict, num_auto_keys: int, seed: int) -> dict:
+def oracle_lmkcdey_keys(oracle, p, keys: dict, num_auto_keys: int, seed: int, window: int = 0) -> dict:
     """LMKCDEY keys of a key set from the oracle, seeded as a context keyed with `seed` seeds
-    them: eval [n][2 digits_g][2][N], auto [1 + num_auto_keys][digits_g][2][N] (NTT domain), and
-    the NTT-domain automorphism maps [1 + num_auto_keys][N]."""
+    them: eval [n][2 digits_g][2][N], auto [keys][digits_g][2][N] (NTT domain), and the NTT-domain
+    automorphism maps [keys][N] (keys: 1 + num_auto_keys, or the windowed set)."""
     vp, u32 = ctypes.c_void_p, ctypes.c_uint32
-    oracle.orc_lmkcdey_keygen.argtypes = [vp, ctypes.c_double, vp, vp, u32, ctypes.c_uint64, vp, vp]
-    oracle.orc_lmkcdey_auto_maps.argtypes = [u32, u32, vp]
-    count = 1 + num_auto_keys
+    oracle.orc_lmkcdey_keygen.argtypes = [vp, ctypes.c_double, vp, vp, u32, u32, ctypes.c_uint64, vp, vp]
+    oracle.orc_lmkcdey_auto_maps.argtypes = [u32, u32, u32, vp]
+    oracle.orc_lmkcdey_auto_pows.argtypes = [u32, u32, u32, vp]
+    oracle.orc_lmkcdey_auto_pows.restype = u32
+    count = oracle.orc_lmkcdey_auto_pows(p.N, num_auto_keys, window, None)
     ev = np.zeros((p.n, 2 * p.digits_g, 2, p.N), np.uint64)
     au = np.zeros((count, p.digits_g, 2, p.N), np.uint64)
     maps = np.zeros((count, p.N), np.uint32)
@@ -237,9 +240,9 @@ def oracle_lmkcdey_keys(oracle, p, keys: dict, num_auto_keys: int, seed: int) ->
     s_lwe = np.ascontiguousarray(keys["s_lwe"], np.int32)
     s_rlwe = np.ascontiguousarray(keys["s_rlwe"], np.int32)
     oracle.orc_lmkcdey_keygen(ctypes.byref(op), p.sigma_rlwe, s_lwe.ctypes.data, s_rlwe.ctypes.data, num_auto_keys,
-                              seed ^ LMK_SEED_TWEAK, ev.ctypes.data, au.ctypes.data)
-    oracle.orc_lmkcdey_auto_maps(p.N, num_auto_keys, maps.ctypes.data)
-    return {"eval": ev, "auto": au, "maps": maps, "num_auto_keys": num_auto_keys}
+                              window, seed ^ LMK_SEED_TWEAK, ev.ctypes.data, au.ctypes.data)
+    oracle.orc_lmkcdey_auto_maps(p.N, num_auto_keys, window, maps.ctypes.data)
+    return {"eval": ev, "auto": au, "maps": maps, "num_auto_keys": num_auto_keys, "window": window}
 
 
 # a fixed ChaCha20 key for reproducible key-generation tests

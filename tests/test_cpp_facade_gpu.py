@@ -114,10 +114,10 @@ def test_facade_lmkcdey(facade_bin, tmp_path, pkg, oracle):
     got = np.fromfile(tmp_path / "lmk_cbs_out", np.uint64).reshape(batch, 2, 2, p.N)
     assert np.array_equal(got, oc.trace_ss(oc.br_acc_lmkcdey(a, b, lmk)))
     vp, u32 = ctypes.c_void_p, ctypes.c_uint32
-    oracle.orc_lmkcdey_eval_acc.argtypes = [vp, vp, vp, vp, u32, vp, u32, vp]
+    oracle.orc_lmkcdey_eval_acc.argtypes = [vp, vp, vp, vp, u32, u32, vp, u32, vp]
     want = acc.copy()
     oracle.orc_lmkcdey_eval_acc(ctypes.byref(oc.op), lmk["eval"].ctypes.data, lmk["auto"].ctypes.data,
-                                lmk["maps"].ctypes.data, num_auto, masks.ctypes.data, p.n, want.ctypes.data)
+                                lmk["maps"].ctypes.data, num_auto, 0, masks.ctypes.data, p.n, want.ctypes.data)
     assert np.array_equal(np.fromfile(tmp_path / "lmk_acc_out", np.uint64).reshape(2, p.N), want)
 
 

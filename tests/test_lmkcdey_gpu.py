@@ -83,16 +83,18 @@ def test_lmkcdey_blind_rotation_matches_oracle(pkg, lctx, lkeys, loc, lmk):
     assert np.array_equal(_host(mv, (len(bits), 2, p.N)), want)
 
 
-@pytest.mark.parametrize("num_auto", [1, NUM_AUTO, 200])
-def test_lmkcdey_eval_acc_matches_oracle(pkg, oracle, lctx, lkeys, num_auto):
+@pytest.mark.parametrize("num_auto,window", [(1, 0), (NUM_AUTO, 0), (200, 0), (NUM_AUTO, 32), (NUM_AUTO, 5)])
+def test_lmkcdey_eval_acc_matches_oracle(pkg, oracle, lctx, lkeys, num_auto, window):
     """EvalAcc on random NTT-domain accumulators and random masks: every automorphism-key count
-    changes where the walk places its automorphisms (1: one per step; 200: only at buckets)."""
+    changes where the walk places its automorphisms (1: one per step; 200: only at buckets), and
+    the windowed key sets close long runs with two automorphisms (5^(q w), then 5^r)."""
     p = lctx.params
     N, Q, n = p.N, p.Q, p.n
-    if num_auto != NUM_AUTO:
-        lctx.set_br_method(pkg.BR_LMKCDEY, num_auto)
+    changed = (num_auto, window) != (NUM_AUTO, 0)
+    if changed:
+        lctx.set_br_method(pkg.BR_LMKCDEY, num_auto, window)
     try:
-        keys = oracle_lmkcdey_keys(oracle, p, lkeys, num_auto, SEED)
+        keys = oracle_lmkcdey_keys(oracle, p, lkeys, num_auto, SEED, window)
         rng = np.random.default_rng(num_auto)
         batch, stride = 2, n + 3
         acc = rng.integers(0, Q, size=(batch, 2, N), dtype=np.uint64)
@@ -104,16 +106,17 @@ def test_lmkcdey_eval_acc_matches_oracle(pkg, oracle, lctx, lkeys, num_auto):
         torch.cuda.synchronize()
         got = _host(d_acc, (batch, 2, N))
         vp, u32 = ctypes.c_void_p, ctypes.c_uint32
-        oracle.orc_lmkcdey_eval_acc.argtypes = [vp, vp, vp, vp, u32, vp, u32, vp]
+        oracle.orc_lmkcdey_eval_acc.argtypes = [vp, vp, vp, vp, u32, u32, vp, u32, vp]
         op = OracleCbs(oracle, p, lkeys).op
         for i in range(batch):
             want = np.ascontiguousarray(acc[i])
             row = np.ascontiguousarray(a_neg[i, :n])
             oracle.orc_lmkcdey_eval_acc(ctypes.byref(op), keys["eval"].ctypes.data, keys["auto"].ctypes.data,
-                                        keys["maps"].ctypes.data, num_auto, row.ctypes.data, n, want.ctypes.data)
+                                        keys["maps"].ctypes.data, num_auto, window, row.ctypes.data, n,
+                                        want.ctypes.data)
             assert np.array_equal(got[i], want), i
     finally:
-        if num_auto != NUM_AUTO:
+        if changed:
             lctx.set_br_method(pkg.BR_LMKCDEY, NUM_AUTO)
 
 
@@ -155,7 +158,7 @@ def test_lmkcdey_import_on_a_server_without_secrets(pkg, lctx, lkeys):
     try:
         pkg.call("cbs_import_keys", srv.handle, None, None, *(np.ascontiguousarray(lkeys[k]).ctypes.data
                                                                for k in ("bsk", "ht", "ss", "ksk")))
-        assert pkg.load().cbs_context_set_br_method(srv.handle, pkg.BR_LMKCDEY, NUM_AUTO) == 7  # no secret
+        assert pkg.load().cbs_context_set_br_method(srv.handle, pkg.BR_LMKCDEY, NUM_AUTO, 0) == 7  # no secret
         srv.import_lmkcdey_keys(NUM_AUTO, ev, au)
         a, b = lwe_encrypt_bits(np.random.default_rng(2), lkeys["s_lwe"], [1, 1], p.q_lwe)
         outs = []
@@ -175,7 +178,7 @@ def test_lmkcdey_preconditions(pkg):
     lib = pkg.load()
     c = pkg.Context(params=pkg.preset_params("2x18"), max_batch=4)  # num_lut = 4
     try:
-        assert lib.cbs_context_set_br_method(c.handle, pkg.BR_LMKCDEY, NUM_AUTO) == 6
+        assert lib.cbs_context_set_br_method(c.handle, pkg.BR_LMKCDEY, NUM_AUTO, 0) == 6
         assert b"num_lut" in lib.cbs_last_error()
     finally:
         c.close()
@@ -183,16 +186,17 @@ def test_lmkcdey_preconditions(pkg):
     p.num_lut = 1
     c = pkg.Context(params=p, max_batch=4)
     try:
-        assert lib.cbs_context_set_br_method(c.handle, pkg.BR_LMKCDEY, NUM_AUTO) == 6
+        assert lib.cbs_context_set_br_method(c.handle, pkg.BR_LMKCDEY, NUM_AUTO, 0) == 6
         assert b"log2 Q" in lib.cbs_last_error()
     finally:
         c.close()
     c = pkg.Context(params=_params(pkg), max_batch=4)
     try:
-        assert lib.cbs_context_set_br_method(c.handle, pkg.BR_LMKCDEY, 0) == 1
-        assert lib.cbs_context_set_br_method(c.handle, 7, NUM_AUTO) == 1
+        assert lib.cbs_context_set_br_method(c.handle, pkg.BR_LMKCDEY, 0, 0) == 1
+        assert lib.cbs_context_set_br_method(c.handle, 7, NUM_AUTO, 0) == 1
+        assert lib.cbs_context_set_br_method(c.handle, pkg.BR_LMKCDEY, NUM_AUTO, c.params.N // 2) == 1
         c.set_br_backend(pkg.BR_FFT64)
-        assert lib.cbs_context_set_br_method(c.handle, pkg.BR_LMKCDEY, NUM_AUTO) == 6
+        assert lib.cbs_context_set_br_method(c.handle, pkg.BR_LMKCDEY, NUM_AUTO, 0) == 6
         c.set_br_backend(pkg.BR_NTT)
         c.set_br_method(pkg.BR_LMKCDEY, NUM_AUTO)  # keys follow at keygen
         c.keygen(3)

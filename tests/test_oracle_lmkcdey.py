@@ -89,8 +89,11 @@ def test_keys_encrypt_their_messages(small):
             assert max(abs(x) for x in err) < 2 ** 20
 
 
-def test_lmkcdey_rotation_matches_one_bit_phase(pkg, oracle, small):
+@pytest.mark.parametrize("window", [0, 8])
+def test_lmkcdey_rotation_matches_one_bit_phase(pkg, oracle, small, window):
     p, keys, oc, lmk = small
+    if window:
+        lmk = oracle_lmkcdey_keys(oracle, p, keys, NUM_AUTO, 41, window)
     N, Q = p.N, p.Q
     oracle.orc_special_ms.restype = ctypes.c_uint32
     bw = max(0, (p.num_lut - 1).bit_length())
@@ -114,15 +117,18 @@ def test_lmkcdey_rotation_matches_one_bit_phase(pkg, oracle, small):
     assert worst < 2 ** 32
 
 
-@pytest.mark.parametrize("preset,num_auto", [("2x18", 10), ("2x18", 1)])
-def test_oracle_lmkcdey_keygen_matches_host(pkg, oracle, preset, num_auto):
+@pytest.mark.parametrize("preset,num_auto,window", [("2x18", 10, 0), ("2x18", 1, 0), ("2x18", 10, 32)])
+def test_oracle_lmkcdey_keygen_matches_host(pkg, oracle, preset, num_auto, window):
     """The product's seeded host generation of the LMKCDEY keys and maps against the oracle's,
-    word for word (the oracle's keys are the ones the GPU parity tests compare against)."""
+    word for word (the oracle's keys are the ones the GPU parity tests compare against); the
+    windowed set (window 32 at N = 2048) holds 2N - 5, 5^1 .. 5^32 and 5^64 .. 5^992."""
     p = pkg.preset_params(preset)
     p.num_lut = 1
     keys = pkg.generate_keys_host(p, 7)
-    want = oracle_lmkcdey_keys(oracle, p, keys, num_auto, 7)
-    ev, au = pkg.generate_lmkcdey_keys_host(p, 7, num_auto)
+    want = oracle_lmkcdey_keys(oracle, p, keys, num_auto, 7, window)
+    ev, au = pkg.generate_lmkcdey_keys_host(p, 7, num_auto, window)
     assert np.array_equal(ev, want["eval"])
     assert np.array_equal(au, want["auto"])
-    assert np.array_equal(pkg.lmkcdey_auto_maps_host(p.N, num_auto), want["maps"])
+    assert np.array_equal(pkg.lmkcdey_auto_maps_host(p.N, num_auto, window), want["maps"])
+    if window:
+        assert au.shape[0] == 1 + window + (p.N // 2 - 1) // window - 1

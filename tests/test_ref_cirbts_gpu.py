@@ -280,22 +280,22 @@ def test_grouped_mb3_soa_matches_reference_kernels(pkg, oracle, ref, preset):
     assert np.array_equal(got, want)
 
 
-@pytest.mark.parametrize("num_auto", [10, 1])
-def test_lmkcdey_eval_acc_matches_reference_kernels(pkg, oracle, ref, num_auto):
+@pytest.mark.parametrize("num_auto,window", [(10, 0), (1, 0), (10, 32)])
+def test_lmkcdey_eval_acc_matches_reference_kernels(pkg, oracle, ref, num_auto, window):
     """LMKCDEY_EvalAcc in the reference's launch sequence over its own kernels, with the
     product's LMKCDEY keys and maps, reproduces the oracle's accumulator word for word (the
     product's kernel equals the oracle: tests/test_lmkcdey_gpu.py)."""
     from cbs_harness import oracle_lmkcdey_keys
     vp, u32, u64 = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64
-    ref.ref_cirbts_lmkcdey_eval_acc.argtypes = [vp, vp, u32, vp, vp, vp, u32, vp, vp, vp, vp, vp, vp, vp, u32, u64,
-                                                u32, u32, vp]
+    ref.ref_cirbts_lmkcdey_eval_acc.argtypes = [vp, vp, u32, vp, vp, vp, u32, u32, vp, vp, vp, vp, vp, vp, vp, u32,
+                                                u64, u32, u32, vp]
     ref.ref_cirbts_lmkcdey_eval_acc.restype = ctypes.c_int
-    oracle.orc_lmkcdey_eval_acc.argtypes = [vp, vp, vp, vp, u32, vp, u32, vp]
+    oracle.orc_lmkcdey_eval_acc.argtypes = [vp, vp, vp, vp, u32, u32, vp, u32, vp]
     p = pkg.preset_params("2x18")
     p.num_lut = 1
     N, n, Q = p.N, p.n, p.Q
     keys = pkg.generate_keys_host(p, 61)
-    lmk = oracle_lmkcdey_keys(oracle, p, keys, num_auto, 61)
+    lmk = oracle_lmkcdey_keys(oracle, p, keys, num_auto, 61, window)
     oc = OracleCbs(oracle, p, keys)
     tabs, ninv, dmod = _tables(pkg, N, Q)
     rng = np.random.default_rng(num_auto + 5)
@@ -308,11 +308,12 @@ def test_lmkcdey_eval_acc_matches_reference_kernels(pkg, oracle, ref, num_auto):
         a_neg = np.ascontiguousarray(rng.integers(0, 2 * N, size=n, dtype=np.uint32))
         want = acc.copy()
         oracle.orc_lmkcdey_eval_acc(ctypes.byref(oc.op), lmk["eval"].ctypes.data, lmk["auto"].ctypes.data,
-                                    lmk["maps"].ctypes.data, num_auto, a_neg.ctypes.data, n, want.ctypes.data)
+                                    lmk["maps"].ctypes.data, num_auto, window, a_neg.ctypes.data, n,
+                                    want.ctypes.data)
         d_acc = _dev(acc)
         st = ref.ref_cirbts_lmkcdey_eval_acc(
             d_acc.data_ptr(), a_neg.ctypes.data, n, dev["eval"].data_ptr(), dev["auto"].data_ptr(), d_maps.data_ptr(),
-            num_auto, dev["mod"].data_ptr(), dev["tw"].data_ptr(), dev["tws"].data_ptr(), dev["itw"].data_ptr(),
+            num_auto, window, dev["mod"].data_ptr(), dev["tw"].data_ptr(), dev["tws"].data_ptr(), dev["itw"].data_ptr(),
             dev["itws"].data_ptr(), dev["ninv"].data_ptr(), dev["ninv"].data_ptr() + 8, N, Q, p.base_g, p.digits_g,
             None)
         torch.cuda.synchronize()

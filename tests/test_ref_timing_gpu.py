@@ -453,8 +453,8 @@ def test_lmkcdey_timing_beside_reference_kernels(pkg):
         pytest.skip("reference CirBTS kernels not built (make -C oracle ref_gpu_cirbts)")
     ref = ctypes.CDLL(str(REF_SO))
     vp, u32, u64 = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64
-    ref.ref_cirbts_lmkcdey_eval_acc.argtypes = [vp, vp, u32, vp, vp, vp, u32, vp, vp, vp, vp, vp, vp, vp, u32, u64,
-                                                u32, u32, vp]
+    ref.ref_cirbts_lmkcdey_eval_acc.argtypes = [vp, vp, u32, vp, vp, vp, u32, u32, vp, vp, vp, vp, vp, vp, vp, u32,
+                                                u64, u32, u32, vp]
     ref.ref_cirbts_lmkcdey_eval_acc.restype = ctypes.c_int
     num_auto, batch = 10, 1184
     p = pkg.preset_params("2x18")
@@ -490,7 +490,7 @@ def test_lmkcdey_timing_beside_reference_kernels(pkg):
                      mv.data_ptr(), None)
 
         ms_br_lmk = _time_ms(rotate, reps=2)
-        ctx.set_br_method(pkg.BR_GINX, 0)
+        ctx.set_br_method(pkg.BR_GINX, 0, 0)
         ms_br_ginx = _time_ms(rotate, reps=2)
         ctx.set_br_method(pkg.BR_LMKCDEY, num_auto)
 
@@ -511,7 +511,7 @@ def test_lmkcdey_timing_beside_reference_kernels(pkg):
         for i in range(reps):
             st = ref.ref_cirbts_lmkcdey_eval_acc(
                 r_acc[i].data_ptr(), rows[i].ctypes.data, n, dv["ev"].data_ptr(), dv["au"].data_ptr(),
-                d_maps.data_ptr(), num_auto, dv["mod"].data_ptr(), dv["tw"].data_ptr(), dv["tws"].data_ptr(),
+                d_maps.data_ptr(), num_auto, 0, dv["mod"].data_ptr(), dv["tw"].data_ptr(), dv["tws"].data_ptr(),
                 dv["itw"].data_ptr(), dv["itws"].data_ptr(), dv["ninv"].data_ptr(), dv["ninv"].data_ptr() + 8, N, Q,
                 p.base_g, p.digits_g, None)
             assert st == 0
