@@ -367,12 +367,19 @@ def run_blind_rotate(args, rank: int, world: int, local_rank: int) -> None:
     torch.cuda.set_device(local_rank)
     pkg = load_pkg()
     T = args.batch or 2368
-    ctx = pkg.Context(params=pkg.preset_params(args.params), max_batch=T)
+    params = pkg.preset_params(args.params)
+    lmk = args.method == "lmkcdey"
+    if lmk:  # one test-vector slot (LMKCDEY's odd masks), the exact NTT form
+        params.num_lut = 1
+        args.backend, args.multibit = "ntt", 1
+    ctx = pkg.Context(params=params, max_batch=T)
     ctx.keygen(args.seed)
     pkg.call("cbs_context_set_br_backend", ctx.handle, pkg.BR_FFT64 if args.backend == "fft64" else pkg.BR_NTT)
     if args.multibit > 1:
         ctx.set_br_multibit(args.multibit)
     ctx.set_br_schedule(args.schedule)
+    if lmk:
+        ctx.set_br_method(pkg.BR_LMKCDEY, 10, 0)
     p = ctx.params
     rng = np.random.default_rng(args.seed + rank)
     a = torch.from_numpy(rng.integers(0, p.q_lwe, size=(T, p.n), dtype=np.int64)).cuda()
@@ -385,12 +392,13 @@ def run_blind_rotate(args, rank: int, world: int, local_rank: int) -> None:
         ms = _timed(torch, stream, fn, args.warmup, args.steps)
     N, n, l2, L = p.N, p.n, 2 * p.digits_g, p.num_lut
     alg_bytes = br_key_bytes(p, args.multibit) + T * ((n + 1) * 8 + L * 2 * N * 8)
-    out = {"metric": f"blind rotations/s ({args.backend}, N={N}, n={n})", "value": world * T / (ms * 1e-3),
+    out = {"metric": f"blind rotations/s ({'lmkcdey, ' if lmk else ''}{args.backend}, N={N}, n={n})",
+           "value": world * T / (ms * 1e-3),
            "unit": "bootstraps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
            "dtype": "f64" if args.backend == "fft64" else "u64", "data": "synthetic (seeded random LWE)",
            "config": {"workload": "blind_rotate", "batch": T, "backend": args.backend, "br_multibit": args.multibit,
-                      "br_schedule": args.schedule,
+                      "br_schedule": args.schedule, "br_method": args.method,
                       "param_set": args.params, "br_gadget": f"2^{p.base_g.bit_length() - 1}x{p.digits_g}",
                       "l2": "BSK read once per launch (124 MB fft64 / 124 MB ntt); no flush between launches"},
            "us_per_bootstrap": ms * 1e3 / T, "gpu_launches": args.steps,
@@ -847,7 +855,8 @@ def br_roofline(args, p, T: int, br_ms: float, alg_bytes: int, traffic) -> dict:
     """Roofline of the dominant kernel, the fused blind rotation: on the FFT backend its bound is
     the FP64 pipe (algorithmic flops per launch over the launch time against the recorded FP64
     peak); the exact-NTT backend is bounded by 64-bit integer multiplies and reports HBM."""
-    name = br_kernel_name(args, p) + " (fused GINX blind rotation + finalize + MV split)"
+    method = "LMKCDEY" if getattr(args, "method", "ginx") == "lmkcdey" else "GINX"
+    name = br_kernel_name(args, p) + f" (fused {method} blind rotation + finalize + MV split)"
     extra = {"algorithmic_bytes_per_launch": alg_bytes, "launch_ms": br_ms, "traffic": traffic,
              "traffic_over_algorithmic": (traffic / alg_bytes) if traffic else None,
              "traffic_src": "ncu dram__bytes_read.sum + dram__bytes_write.sum of this launch (one pass), recorded"}
@@ -866,6 +875,8 @@ def br_roofline(args, p, T: int, br_ms: float, alg_bytes: int, traffic) -> dict:
 
 
 def br_kernel_name(args, p=None) -> str:
+    if getattr(args, "method", "ginx") == "lmkcdey":
+        return "k_lmkcdey"
     if args.backend != "fft64":
         return "k_blind_rotate"
     if args.multibit == 1:
@@ -1101,6 +1112,9 @@ def main() -> None:
                     default="aes128",
                     help="aes128 is the headline; the others time one kernel family")
     ap.add_argument("--batch", type=int, default=0, help="units per step for the kernel workloads")
+    ap.add_argument("--method", choices=["ginx", "lmkcdey"], default="ginx",
+                    help="blind-rotation method of --workload blind_rotate (lmkcdey: exact NTT form, one LUT slot, "
+                         "10 automorphism keys; needs --params 2x18)")
     ap.add_argument("--alpha", type=int, default=2, help="special primes (digit width) for --workload keyswitch")
     ap.add_argument("--ntt-logn", dest="ntt_logn", type=int, default=16, help="log2 N for --workload rns_ntt")
     ap.add_argument("--limbs", type=int, default=24, help="limbs per polynomial for --workload rns_ntt")
