@@ -871,7 +871,8 @@ def br_roofline(args, p, T: int, br_ms: float, alg_bytes: int, traffic) -> dict:
     return {"kernel": name, "bound": "hbm", "achieved": gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
             "frac": gbs / peaks["hbm_gbs"], "peak_src": peaks["src"],
             "note": "integer-multiply bound; compute_rate gives the modular products per second",
-            "compute_rate": compute_rate(args.backend, T, p, br_ms, args.multibit), **extra}
+            "compute_rate": None if method == "LMKCDEY" else compute_rate(args.backend, T, p, br_ms, args.multibit),
+            **extra}
 
 
 def br_kernel_name(args, p=None) -> str:
