@@ -22,7 +22,7 @@ c_u64p = ctypes.POINTER(ctypes.c_uint64)
 c_u32p = ctypes.POINTER(ctypes.c_uint32)
 c_vp = ctypes.c_void_p
 
-BR_NTT, BR_FFT64 = 0, 1
+BR_NTT, BR_FFT64, BR_FFT64_SPLIT = 0, 1, 2
 BR_GINX, BR_LMKCDEY = 0, 1
 
 CBS_STATUS = {
@@ -92,6 +92,7 @@ def _declare(lib: ctypes.CDLL) -> None:
         "cbs_lmkcdey_eval_acc_batch_device": (st, [c_vp, c_vp, u32, c_vp, u32, c_vp]),
         "cbs_export_mb_bsk": (st, [c_vp, c_vp, c_vp]),
         "cbs_generate_mb_bsk_host": (st, [c_vp, u64, u32, c_vp, c_vp]),
+        "cbs_split_fft_plan": (st, [c_vp, c_vp, c_vp, c_vp]),
         "cbs_export_keys": (st, [c_vp] + [c_vp] * 9),
         "cbs_import_keys": (st, [c_vp] + [c_vp] * 6),
         "cbs_import_mb_bsk": (st, [c_vp, u32, c_vp, sz]),
@@ -270,6 +271,13 @@ def lmkcdey_auto_maps_host(N: int, num_auto_keys: int, window: int = 0):
     out = np.zeros((count.value, N), np.uint32)
     call("cbs_lmkcdey_auto_maps_host", N, num_auto_keys, window, out.ctypes.data, None)
     return out
+
+
+def split_fft_plan(params: CbsParams):
+    """(limbs, limb_bits, bound_bits) of the exact split-FFT blind rotation (BR_FFT64_SPLIT)."""
+    limbs, lb, bound = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
+    call("cbs_split_fft_plan", ctypes.byref(params), ctypes.byref(limbs), ctypes.byref(lb), ctypes.byref(bound))
+    return limbs.value, lb.value, bound.value
 
 
 def generate_mb_bsk_host(params: CbsParams, seed: int, mb: int):

@@ -74,6 +74,45 @@ FftKeyArgs fft_key_args(const cbs_context* c) {
     return f;
 }
 
+// limb spectra of the bootstrapping key and the FFT tables for the exact split-FFT backend
+static cbs_status prepare_split(cbs_context* c) {
+    if (c->split_ready) return CBS_OK;
+    if (!c->keys_ready) {
+        set_error("split FFT backend: no key material (call cbs_keygen first)");
+        return CBS_ERR_NOT_READY;
+    }
+    std::vector<double2> bskx, ftab;
+    try {
+        keys_to_fft_limbs_host(c->tab, c->hk.bsk.data(), c->hk.bsk.size() / c->p.N, 4 * c->p.digits_g, c->split,
+                               bskx);
+    } catch (const std::exception& e) {
+        set_error(std::string("split FFT keys: ") + e.what());
+        return CBS_ERR_OOM;
+    }
+    fft_tables_host(c->p.N, ftab);
+    cudaStream_t s = c->stream;
+    CBS_CUDA_TRY(c->d_bskx.upload(bskx.data(), bskx.size(), s));
+    CBS_CUDA_TRY(c->d_fft_tab.upload(ftab.data(), ftab.size(), s));
+    CBS_CUDA_TRY(cudaStreamSynchronize(s));
+    c->split_ready = true;
+    return CBS_OK;
+}
+
+static SplitKeyArgs split_key_args(const cbs_context* c) {
+    SplitKeyArgs k{};
+    k.bskx = c->d_bskx.p;
+    k.limbs = c->split.limbs;
+    FastMod fm(c->p.Q);
+    const uint64_t base = (uint64_t(1) << c->split.limb_bits) % c->p.Q;  // limb_bits <= 50
+    uint64_t v = 1 % c->p.Q;
+    for (uint32_t l = 0; l < kMaxSplitLimbs; ++l) {
+        k.pw[l] = v;
+        k.pws[l] = host::shoup(v, c->p.Q);
+        v = fm.mul(v, base);
+    }
+    return k;
+}
+
 // the grouped keys' generator seed is the key seed xor this constant (context and host agree)
 static constexpr uint64_t kMbSeedTweak = 0x6d756c7469626974ull;
 
@@ -173,6 +212,14 @@ cbs_status run_blind_rotate(cbs_context* c, const uint64_t* d_a, const uint64_t*
             return CBS_OK;
         }
         CBS_CUDA_TRY(launch_blind_rotate_fft(a, fft_key_args(c), c->d_mod.p, c->p.N, batch, s, mv_ntt));
+        return CBS_OK;
+    }
+    if (c->br_backend == CBS_BR_FFT64_SPLIT) {
+        if (!c->split_ready) {
+            set_error("split FFT backend selected but its key material is not prepared");
+            return CBS_ERR_NOT_READY;
+        }
+        CBS_CUDA_TRY(launch_blind_rotate_fft_split(a, fft_key_args(c), split_key_args(c), c->d_mod.p, c->p.N, batch, s));
         return CBS_OK;
     }
     if (c->br_method == CBS_BR_LMKCDEY) return run_blind_rotate_lmkcdey(c, d_a, d_b, batch, a_stride, d_mv, s);
@@ -400,6 +447,8 @@ cbs_status finish_key_upload(cbs_context* c) {
     c->keys_ready = true;
     c->aes.ready = false;
     c->fft_ready = false;
+    c->split_ready = false;
+    c->d_bskx.reset();
     c->mb_ready = false;
     c->h_mbk.clear();
     c->d_bskf_mb.reset();
@@ -411,6 +460,7 @@ cbs_status finish_key_upload(cbs_context* c) {
         if (cbs_status st = prepare_fft(c)) return st;
         return prepare_mb(c);
     }
+    if (c->br_backend == CBS_BR_FFT64_SPLIT) return prepare_split(c);
     // LMKCDEY keys follow from the secrets of a seeded key set (otherwise they are imported)
     if (c->br_method == CBS_BR_LMKCDEY && c->has_secret && !c->device_keyed) return prepare_lmkcdey(c);
     return CBS_OK;
@@ -678,10 +728,32 @@ cbs_status cbs_export_mb_bsk(const cbs_context* ctx, uint64_t* out, size_t* word
 
 cbs_status cbs_context_set_br_backend(cbs_context* ctx, int backend) {
     CBS_CHECK_ARG(ctx, "set_br_backend: null context");
-    CBS_CHECK_ARG(backend == CBS_BR_NTT || backend == CBS_BR_FFT64, "set_br_backend: unknown backend");
+    CBS_CHECK_ARG(backend == CBS_BR_NTT || backend == CBS_BR_FFT64 || backend == CBS_BR_FFT64_SPLIT,
+                  "set_br_backend: unknown backend");
     if (backend == CBS_BR_FFT64 && (ctx->p.digits_g > 4 || ctx->p.base_g > (1u << 24))) {
         set_error("set_br_backend: the FFT64 backend supports at most 4 gadget digits of at most 24 bits");
         return CBS_ERR_UNSUPPORTED;
+    }
+    if (backend == CBS_BR_FFT64_SPLIT) {
+        SplitPlan plan;
+        const int gbits = __builtin_ctz(ctx->p.base_g);
+        if ((ctx->p.N != 1024 && ctx->p.N != 2048) || ctx->p.digits_g < 2 || ctx->p.digits_g > 4 ||
+            ctx->p.base_g > (1u << 24) || !split_plan(ctx->p.N, ctx->p.Q, gbits, ctx->p.digits_g, plan)) {
+            set_error("set_br_backend: the split FFT backend needs N = 1024 or 2048, 2-4 gadget digits of at "
+                      "most 24 bits, and a limb split (at most 4 limbs) whose products stay below 2^50 and Q/2");
+            return CBS_ERR_UNSUPPORTED;
+        }
+        if (ctx->br_backend != CBS_BR_FFT64_SPLIT || ctx->split.limbs != plan.limbs) {
+            ctx->split_ready = false;
+            ctx->d_bskx.reset();
+        }
+        ctx->split = plan;
+        if (ctx->keys_ready) {
+            if (cbs_status st = prepare_split(ctx)) return st;
+        }
+    } else if (ctx->split_ready) {  // the limb spectra are needed by the split backend only
+        ctx->split_ready = false;
+        ctx->d_bskx.reset();
     }
     if (backend == CBS_BR_FFT64 && ctx->keys_ready) {
         if (cbs_status st = prepare_fft(ctx)) return st;
@@ -704,6 +776,20 @@ cbs_status cbs_context_set_br_backend(cbs_context* ctx, int backend) {
     }
     // captured AES round graphs bake in the kernel choice
     ctx->aes.drop_graphs();
+    return CBS_OK;
+}
+
+cbs_status cbs_split_fft_plan(const cbs_params* params, uint32_t* limbs, uint32_t* limb_bits, uint32_t* bound_bits) {
+    CBS_CHECK_ARG(params && limbs && limb_bits && bound_bits, "split_fft_plan: null argument");
+    if (cbs_status st = validate(*params)) return st;
+    SplitPlan plan;
+    if (!split_plan(params->N, params->Q, __builtin_ctz(params->base_g), params->digits_g, plan)) {
+        set_error("split_fft_plan: no split of at most 4 limbs keeps the products below 2^50 and Q/2");
+        return CBS_ERR_UNSUPPORTED;
+    }
+    *limbs = plan.limbs;
+    *limb_bits = plan.limb_bits;
+    *bound_bits = plan.bound_bits;
     return CBS_OK;
 }
 

@@ -81,10 +81,14 @@ struct cbs_context {
     cbs::DevBuf<uint64_t> d_tv, d_gadd, d_bsk, d_ht, d_ss;
     cbs::DevBuf<uint16_t> d_ksk;
     // FP64 FFT blind-rotation backend (built on demand from the keys)
-    int br_backend = 0;  // CBS_BR_NTT or CBS_BR_FFT64
+    int br_backend = 0;  // CBS_BR_NTT, CBS_BR_FFT64 or CBS_BR_FFT64_SPLIT
     bool fft_ready = false;
     cbs::DevBuf<double2> d_bskf, d_fft_tab;
     cbs::DevBuf<double2> d_htf, d_ssf;  // HomTrace / SchemeSwitch key spectra
+    // exact split-FFT blind rotation (CBS_BR_FFT64_SPLIT): key limb spectra and the limb plan
+    bool split_ready = false;
+    cbs::SplitPlan split{};
+    cbs::DevBuf<double2> d_bskx;
     // multi-bit blind rotation (FFT backend): 1 = one coefficient per step, 2 or 3 = grouped
     uint32_t br_mb = 1;
     bool mb_explicit = false;            // mb chosen by the caller (not by the tuning cache)

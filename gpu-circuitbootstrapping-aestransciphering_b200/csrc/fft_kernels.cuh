@@ -61,6 +61,32 @@ struct CmuxFftArgs {
     const double2* in_spec;
 };
 
+// Exact blind rotation over FP64 products of key limbs: each key polynomial k (centred) is
+// cut into `limbs` balanced limbs of `limb_bits` bits, k = sum_l 2^(limb_bits l) k_l, and the
+// limb spectra of one step are stored [limbs][2*digits][2][N/2] (slot-major, as bskf).
+constexpr uint32_t kMaxSplitLimbs = 4;
+struct SplitPlan {
+    uint32_t limbs = 0, limb_bits = 0;
+    uint32_t bound_bits = 0;  // log2 of the bound on every rounded limb-product coefficient
+};
+struct SplitKeyArgs {
+    const double2* bskx;                 // [n][limbs][2*digits][2][N/2] limb spectra
+    uint32_t limbs;
+    uint64_t pw[kMaxSplitLimbs];         // 2^(limb_bits l) mod Q
+    uint64_t pws[kMaxSplitLimbs];        // their Shoup quotients
+};
+// the limb split for ring N, modulus Q and a gadget of `digits` digits of gbits bits: false
+// when no split of at most kMaxSplitLimbs limbs keeps the products below 2^50 and Q / 2
+bool split_plan(uint32_t N, uint64_t Q, int gbits, uint32_t digits, SplitPlan& out);
+// key polynomials [count][N] (NTT domain, mod Q), per_step consecutive polynomials to a step,
+// to limb spectra [count / per_step][limbs][per_step][N/2]
+void keys_to_fft_limbs_host(const host::NttTables& t, const uint64_t* keys_ntt, size_t count, uint32_t per_step,
+                            const SplitPlan& plan, std::vector<double2>& out);
+// one-bit GINX blind rotation with exact limb products (N = 1024 or 2048, 2-4 digits); the MV
+// outputs are bit-identical to launch_blind_rotate's and left in the NTT domain
+cudaError_t launch_blind_rotate_fft_split(const BlindRotateArgs& a, const FftKeyArgs& f, const SplitKeyArgs& k,
+                                          const cbs_dmodulus* d_mod, uint32_t N, uint32_t batch, cudaStream_t s);
+
 // mv_ntt: also transform the MV outputs to the NTT domain (the reference layout); false
 // leaves them in the coefficient domain for the FFT HomTrace
 cudaError_t launch_blind_rotate_fft(const BlindRotateArgs& a, const FftKeyArgs& f, const cbs_dmodulus* d_mod,

@@ -126,4 +126,35 @@ __device__ __forceinline__ double centred_double(uint64_t x, uint64_t Q, uint64_
                                           : static_cast<int64_t>(x));
 }
 
+// The biased digit fields (digit + 2^(gbits-1)) of one folded pair (a_e, a_(e+M)): packed in
+// one 32-bit word for digits of up to 15 bits (re in the low half-word), two words for wider
+// digits (the 2 x 18-bit gadget).
+template <bool WIDE>
+struct DigitPair {
+    using T = uint32_t;
+    __device__ static __forceinline__ T pack(uint32_t re, uint32_t im) { return re | (im << 16); }
+    __device__ static __forceinline__ double2 unpack(T v, int32_t bias) {
+        return make_double2(static_cast<double>(static_cast<int32_t>(v & 0xffffu) - bias),
+                            static_cast<double>(static_cast<int32_t>(v >> 16) - bias));
+    }
+};
+template <>
+struct DigitPair<true> {
+    using T = uint2;
+    __device__ static __forceinline__ T pack(uint32_t re, uint32_t im) { return make_uint2(re, im); }
+    __device__ static __forceinline__ double2 unpack(T v, int32_t bias) {
+        return make_double2(static_cast<double>(static_cast<int32_t>(v.x) - bias),
+                            static_cast<double>(static_cast<int32_t>(v.y) - bias));
+    }
+};
+
+// gadget digits wider than the packed 16-bit fields take the two-word form
+__host__ __device__ constexpr bool wide_digits(int gbits) { return gbits > 15; }
+
+template <int LOGN>
+struct BrFftCfg {
+    static constexpr uint32_t T = (1u << LOGN) / 8;
+    static constexpr int MIN_BLOCKS = LOGN <= 10 ? 4 : (LOGN == 11 ? 2 : 1);
+};
+
 }  // namespace cbs

@@ -161,9 +161,24 @@ cbs_status cbs_keygen_device(cbs_context *ctx, const uint8_t *rng_key);
  * (bit-identical to the reference's kernels).  CBS_BR_FFT64: FP64 FFT products (the
  * reference's gate-bootstrap / split-FFT form, bitwise/src/fft.cu:3614-3755); the key
  * spectra are precomputed from the keys, each product carries a bounded FP64 rounding error
- * that adds to the blind-rotation noise (the test suite states and checks the bound). */
-enum { CBS_BR_NTT = 0, CBS_BR_FFT64 = 1 };
+ * that adds to the blind-rotation noise (the test suite states and checks the bound).
+ * CBS_BR_FFT64_SPLIT: the reference's split-FFT CBS backend (CIRBTS_USE_SPLIT_FFT,
+ * bitwise/src/cirbts/cirbts-init.cu:1084-1140, cirbts-bootstrap.cu:939-1085): the key is cut
+ * into balanced limbs small enough that every FP64 digit x limb product rounds to its exact
+ * integer, so the blind rotation -- and every output -- is bit-identical to CBS_BR_NTT's;
+ * HomTrace, SchemeSwitch and the CMux run in their exact NTT forms.  One-bit GINX only (mb 1),
+ * N = 1024 or 2048, 2-4 gadget digits; CBS_ERR_UNSUPPORTED when no split of at most 4 limbs
+ * keeps the products below 2^50 (cbs_split_fft_plan reports the split). */
+enum { CBS_BR_NTT = 0, CBS_BR_FFT64 = 1, CBS_BR_FFT64_SPLIT = 2 };
 cbs_status cbs_context_set_br_backend(cbs_context *ctx, int backend);
+
+/* The limb split CBS_BR_FFT64_SPLIT uses for these parameters: *limbs limbs of *limb_bits
+ * bits, every rounded limb-product coefficient below 2^*bound_bits (<= 50).  The reference's
+ * sizing is limb_bits = 50 - (log2 Bg + log2 N + log2 digitsG2) unsigned limbs
+ * (cirbts-init.cu:1097-1120); here the limbs are balanced and equalised.  CBS_ERR_UNSUPPORTED
+ * when no split of at most 4 limbs exists. */
+cbs_status cbs_split_fft_plan(const cbs_params *params, uint32_t *limbs, uint32_t *limb_bits,
+                              uint32_t *bound_bits);
 
 /* Multi-bit blind rotation (the reference's CIRBTS_PBS_MULTIBIT grouping,
  * bitwise/src/cirbts/cirbts-init.cu:376-565 and the MB3 MAC kernel.cu:4585-4771): mb = 1

@@ -29,16 +29,17 @@ def _copy_view(view: int, words: int):
     return out
 
 
-@pytest.mark.parametrize("backend", ["ntt", "fft64"])
+@pytest.mark.parametrize("backend", ["ntt", "fft64", "fft64_split"])
 def test_noalloc_matches_allocating_entry_point(pkg, backend):
-    """Both blind-rotation backends: the exact NTT one hands NTT-domain RLWEs to the trace; the
+    """Every blind-rotation backend: the exact NTT one hands NTT-domain RLWEs to the trace; the
     FFT one hands coefficient-domain RLWEs to the FFT trace, whose row spectra are written into
-    the caller's output buffer and converted there to the NTT-domain rows."""
+    the caller's output buffer and converted there to the NTT-domain rows; the exact split-FFT
+    one hands NTT-domain RLWEs to the exact trace."""
     lib = pkg.load()
     ctx = pkg.Context(max_batch=32)
     ctx.keygen(5)
-    if backend == "fft64":
-        ctx.set_br_backend(1)
+    if backend != "ntt":
+        ctx.set_br_backend(pkg.BR_FFT64 if backend == "fft64" else pkg.BR_FFT64_SPLIT)
     p = ctx.params
     keys = ctx.export_keys()
     per = p.num_lut * 4 * p.N
