@@ -38,7 +38,12 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 PKG_DIR = ROOT / "gpu-circuitbootstrapping-aestransciphering_b200"
 METRICS = {"fft64": "AES-128 CTR transciphering blocks/s (1 B200, FP64-FFT circuit bootstrapping)",
-           "ntt": "AES-128 CTR transciphering blocks/s (1 B200, exact-NTT circuit bootstrapping)"}
+           "ntt": "AES-128 CTR transciphering blocks/s (1 B200, exact-NTT circuit bootstrapping)",
+           "fft64-split": "AES-128 CTR transciphering blocks/s (1 B200, exact split-FFT circuit bootstrapping)"}
+
+
+def backend_id(pkg, name: str) -> int:
+    return {"fft64": pkg.BR_FFT64, "ntt": pkg.BR_NTT, "fft64-split": pkg.BR_FFT64_SPLIT}[name]
 UNIT = "blocks/s"
 ROUNDS = 10
 
@@ -204,7 +209,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     blocks = args.blocks
     ctx = pkg.Context(params=pkg.preset_params(args.params), max_batch=128 * min(blocks, 256))
     ctx.keygen(args.seed)
-    pkg.call("cbs_context_set_br_backend", ctx.handle, pkg.BR_FFT64 if args.backend == "fft64" else pkg.BR_NTT)
+    pkg.call("cbs_context_set_br_backend", ctx.handle, backend_id(pkg, args.backend))
     tuned = None
     if args.backend == "fft64" and args.tune:
         # the product's autotuner picks the grouping and schedule (16 waves of 148 ciphertexts)
@@ -299,7 +304,8 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     chunks = -(-blocks // 256)
     # per round: blind rotation, HomTrace+SchemeSwitch, 8 CMux levels, word assembly and
     # extraction (+ one inverse NTT of the words on the NTT backend); + state init per chunk
-    launches_per_step = chunks * (1 + ROUNDS * (12 if args.backend == "fft64" else 13))
+    # (the split backend adds one forward NTT of the MV outputs after its blind rotation)
+    launches_per_step = chunks * (1 + ROUNDS * {"fft64": 12, "ntt": 13, "fft64-split": 14}[args.backend])
     result = {
         "metric": METRICS[args.backend],
         "value": rep.whole_job_rate(world, blocks, ms_per_step),
@@ -312,6 +318,8 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f64 (blind-rotation FFT products) + u64 (exact mod-Q NTT elsewhere)" if args.backend == "fft64"
+                 else "f64 (exact blind-rotation key-limb products) + u64 (exact mod-Q NTT elsewhere)"
+                 if args.backend == "fft64-split"
                  else "u64 (exact mod-Q NTT arithmetic)",
         "data": "synthetic (seeded AES key; counters: one seeded CTR stream, rank r takes blocks [r B, (r+1) B))",
         "config": {"workload": "aes128_ctr_transcipher", "blocks_per_gpu": blocks, "global_blocks": world * blocks,
@@ -374,7 +382,7 @@ def run_blind_rotate(args, rank: int, world: int, local_rank: int) -> None:
         args.backend, args.multibit = "ntt", 1
     ctx = pkg.Context(params=params, max_batch=T)
     ctx.keygen(args.seed)
-    pkg.call("cbs_context_set_br_backend", ctx.handle, pkg.BR_FFT64 if args.backend == "fft64" else pkg.BR_NTT)
+    pkg.call("cbs_context_set_br_backend", ctx.handle, backend_id(pkg, args.backend))
     if args.multibit > 1:
         ctx.set_br_multibit(args.multibit)
     ctx.set_br_schedule(args.schedule)
@@ -396,7 +404,7 @@ def run_blind_rotate(args, rank: int, world: int, local_rank: int) -> None:
            "value": world * T / (ms * 1e-3),
            "unit": "bootstraps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-           "dtype": "f64" if args.backend == "fft64" else "u64", "data": "synthetic (seeded random LWE)",
+           "dtype": "u64" if args.backend == "ntt" else "f64", "data": "synthetic (seeded random LWE)",
            "config": {"workload": "blind_rotate", "batch": T, "backend": args.backend, "br_multibit": args.multibit,
                       "br_schedule": args.schedule, "br_method": args.method,
                       "param_set": args.params, "br_gadget": f"2^{p.base_g.bit_length() - 1}x{p.digits_g}",
@@ -860,8 +868,9 @@ def br_roofline(args, p, T: int, br_ms: float, alg_bytes: int, traffic) -> dict:
     extra = {"algorithmic_bytes_per_launch": alg_bytes, "launch_ms": br_ms, "traffic": traffic,
              "traffic_over_algorithmic": (traffic / alg_bytes) if traffic else None,
              "traffic_src": "ncu dram__bytes_read.sum + dram__bytes_write.sum of this launch (one pass), recorded"}
-    if args.backend == "fft64":
-        flop = fp64_flop_per_launch(p, T, args.multibit)
+    if args.backend in ("fft64", "fft64-split"):
+        flop = (fp64_flop_per_launch(p, T, args.multibit) if args.backend == "fft64"
+                else split_fp64_flop_per_launch(p, T, args.multibit))
         achieved = flop / (br_ms * 1e-3) / 1e12
         return {"kernel": name, "bound": "fp64", "achieved": achieved, "peak": FP64_PEAK["tflops"],
                 "unit": "TFLOP/s", "frac": achieved / FP64_PEAK["tflops"], "peak_src": FP64_PEAK["src"],
@@ -878,6 +887,8 @@ def br_roofline(args, p, T: int, br_ms: float, alg_bytes: int, traffic) -> dict:
 def br_kernel_name(args, p=None) -> str:
     if getattr(args, "method", "ginx") == "lmkcdey":
         return "k_lmkcdey"
+    if args.backend == "fft64-split":
+        return f"k_blind_rotate_fft_split<11,·,{p.digits_g if p is not None else '·'},{args.multibit}>"
     if args.backend != "fft64":
         return "k_blind_rotate"
     if args.multibit == 1:
@@ -971,6 +982,18 @@ def fp64_flop_per_launch(p, T: int, mb: int) -> int:
     steps = -(-n // mb)
     keys = (1 << mb) - 1
     return T * steps * ((l2 + 2) * fft_flop + 2 * l2 * M * 8 * (keys + (1 if mb > 1 else 0)))
+
+
+def split_fp64_flop_per_launch(p, T: int, mb: int) -> int:
+    """Algorithmic FP64 flops of the exact split-FFT blind rotation: per step 2 digits forward
+    and 2 limbs inverse M-point transforms, and per limb the digit x key-limb products of both
+    columns (mb = 2: the combined key c0 (K0 + c1 K01) + c1 K1 adds three complex multiply-adds
+    per product).  Limbs from the plan the backend uses (cbs_split_fft_plan)."""
+    M, n, l2 = p.N // 2, p.n, 2 * p.digits_g
+    limbs = 3  # both parameter sets, mb 1 and 2: 3 balanced limbs of 18 bits
+    fft_flop = 5 * M * (M.bit_length() - 1)
+    steps = -(-n // mb)
+    return T * steps * ((l2 + 2 * limbs) * fft_flop + limbs * 2 * l2 * M * 8 * (1 if mb == 1 else 4))
 
 
 def compute_rate(backend: str, T: int, p, br_ms: float, mb: int = 1) -> dict:
@@ -1091,10 +1114,12 @@ def main() -> None:
     ap.add_argument("--blocks", type=int, default=128)
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--backend", choices=["fft64", "ntt"], default="fft64")
+    ap.add_argument("--backend", choices=["fft64", "ntt", "fft64-split"], default="fft64",
+                    help="blind-rotation arithmetic: FP64 FFT (approximate, the headline), exact 64-bit NTT, or "
+                         "the exact split FFT (FP64 products of key limbs, bit-identical to ntt)")
     ap.add_argument("--multibit", type=int, choices=[1, 2, 3, 4], default=None,
                     help="blind rotation over groups of 1, 2, 3 or 4 (staged 3 + 1) LWE coefficients "
-                         "(fft64 backend; default 2 for fft64, 1 for ntt)")
+                         "(fft64 backend; fft64-split takes 1 or 2; default 2 for fft64, 1 otherwise)")
     ap.add_argument("--fft-mode", dest="fft_mode", choices=["fp64", "fp32-split", "fp32"], default="fp64",
                     help="external-product arithmetic of --workload gate / ragged (torus-32): exact FP64, "
                          "split FP32 (24/25-bit + exact top key limb), or FP32 on whole keys; FP32 modes use "
@@ -1131,8 +1156,8 @@ def main() -> None:
         args.tune = False  # an explicit grouping or schedule is measured as given
     if args.multibit is None:
         args.multibit = 2 if args.backend == "fft64" else 1
-    if args.multibit > 1 and args.backend != "fft64":
-        ap.error("--multibit > 1 needs --backend fft64")
+    if args.multibit > 1 and args.backend != "fft64" and not (args.backend == "fft64-split" and args.multibit == 2):
+        ap.error("--multibit > 1 needs --backend fft64 (or 2 with fft64-split)")
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

@@ -92,7 +92,7 @@ def _declare(lib: ctypes.CDLL) -> None:
         "cbs_lmkcdey_eval_acc_batch_device": (st, [c_vp, c_vp, u32, c_vp, u32, c_vp]),
         "cbs_export_mb_bsk": (st, [c_vp, c_vp, c_vp]),
         "cbs_generate_mb_bsk_host": (st, [c_vp, u64, u32, c_vp, c_vp]),
-        "cbs_split_fft_plan": (st, [c_vp, c_vp, c_vp, c_vp]),
+        "cbs_split_fft_plan": (st, [c_vp, u32, c_vp, c_vp, c_vp]),
         "cbs_export_keys": (st, [c_vp] + [c_vp] * 9),
         "cbs_import_keys": (st, [c_vp] + [c_vp] * 6),
         "cbs_import_mb_bsk": (st, [c_vp, u32, c_vp, sz]),
@@ -273,10 +273,11 @@ def lmkcdey_auto_maps_host(N: int, num_auto_keys: int, window: int = 0):
     return out
 
 
-def split_fft_plan(params: CbsParams):
-    """(limbs, limb_bits, bound_bits) of the exact split-FFT blind rotation (BR_FFT64_SPLIT)."""
+def split_fft_plan(params: CbsParams, mb: int = 1):
+    """(limbs, limb_bits, bound_bits) of the exact split-FFT blind rotation (BR_FFT64_SPLIT) for
+    grouping mb (1 or 2)."""
     limbs, lb, bound = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
-    call("cbs_split_fft_plan", ctypes.byref(params), ctypes.byref(limbs), ctypes.byref(lb), ctypes.byref(bound))
+    call("cbs_split_fft_plan", ctypes.byref(params), mb, ctypes.byref(limbs), ctypes.byref(lb), ctypes.byref(bound))
     return limbs.value, lb.value, bound.value
 
 

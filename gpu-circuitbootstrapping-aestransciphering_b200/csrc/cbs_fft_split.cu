@@ -43,7 +43,7 @@ struct BrSplitCfg {
 //     halves swap partial sums so half h holds output h; times psi^a - 1; inverse transform;
 //     each coefficient rounds to the exact integer limb product, is scaled by 2^(lb l) mod Q and
 //     added to the accumulator position this thread owns.
-template <int LOGN, bool WIDE, int DIG>
+template <int LOGN, bool WIDE, int DIG, int MB>
 __global__ void __launch_bounds__(BrSplitCfg<LOGN>::T, BrSplitCfg<LOGN>::MIN_BLOCKS)
     k_blind_rotate_fft_split(const BlindRotateArgs a, const FftKeyArgs f, const SplitKeyArgs sk) {
     constexpr int LOGM = LOGN - 1;
@@ -55,6 +55,7 @@ __global__ void __launch_bounds__(BrSplitCfg<LOGN>::T, BrSplitCfg<LOGN>::MIN_BLO
     double2* fs = reinterpret_cast<double2*>(smem + 2 * N);         // [2][M]
     double2* tab = fs + 2 * M;                                      // FftTab<LOGM>
     DigT* dig = reinterpret_cast<DigT*>(tab + Tb::size());          // [2][DIG][M] digit pairs
+    double2* cbuf = reinterpret_cast<double2*>(dig + 2 * DIG * M);  // MB = 2: [2][8][T] c_i per slot
     const double2* tws = tab + Tb::twist_off();
     const uint32_t ct = blockIdx.x, tid = threadIdx.x;
     const uint32_t h = tid / TH, ht = tid % TH;
@@ -104,9 +105,30 @@ __global__ void __launch_bounds__(BrSplitCfg<LOGN>::T, BrSplitCfg<LOGN>::MIN_BLO
     const int32_t dbias = 1 << (gbits - 1);
     const uint32_t fmask = (1u << gbits) - 1u;
     const uint64_t* arow = a.a + static_cast<size_t>(ct) * a.a_stride;
-    constexpr uint32_t PER_STEP = 4 * DIG;  // key polynomials per step and limb: [2*DIG rows][2 columns]
-    for (uint32_t step = 0; step < a.n; ++step) {
-        const uint32_t at = special_ms_f(__ldg(arow + step), TWO_N, a.q_lwe, a.bitwidth);
+    // key polynomials per step and limb: [subsets][2*DIG rows][2 columns]
+    constexpr uint32_t PER_STEP = (MB == 1 ? 1 : 3) * 4 * DIG;
+    const uint32_t steps = (a.n + MB - 1) / MB;
+    for (uint32_t step = 0; step < steps; ++step) {
+        // mask exponents of the step's coefficients (0 past n: X^0 - 1 = 0 drops the term)
+        uint32_t at[MB];
+#pragma unroll
+        for (int i = 0; i < MB; ++i) {
+            const uint32_t idx = step * MB + i;
+            at[i] = idx < a.n ? special_ms_f(__ldg(arow + idx), TWO_N, a.q_lwe, a.bitwidth) : 0u;
+        }
+        if constexpr (MB == 2) {
+            // c_i(psi_s) = psi_s^(a_i) - 1 for the thread's 8 slots, thread-private in shared
+            // memory for the step (the combined key c0 (K0 + c1 K01) + c1 K1 needs them per limb)
+#pragma unroll
+            for (int i = 0; i < 2; ++i) {
+                const uint32_t mb_i = mult_base<LOGN>(ht, at[i]);
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    const double2 w = zeta_pow<LOGN>(tws, slot_exp<LOGN>(mb_i, at[i], j));
+                    cbuf[(i * 8 + j) * T + tid] = make_double2(w.x - 1.0, w.y);
+                }
+            }
+        }
         // 1. digits of this half's polynomial (positions ht + j*TH, owned by this thread)
         for (uint32_t e = ht; e < M; e += TH) {
             const uint64_t wr = static_cast<uint64_t>(my_acc[e]) >> ign;
@@ -131,7 +153,7 @@ __global__ void __launch_bounds__(BrSplitCfg<LOGN>::T, BrSplitCfg<LOGN>::MIN_BLO
                 x[d], half_bar);
             half_bar();
         }
-        const uint32_t mbase = mult_base<LOGN>(ht, at);
+        const uint32_t mbase = mult_base<LOGN>(ht, at[0]);
         const double2* ek = sk.bskx + static_cast<size_t>(step) * limbs * PER_STEP * M + ht;
         // 3. one product, swap and inverse transform per limb
 #pragma unroll 1
@@ -148,10 +170,27 @@ __global__ void __launch_bounds__(BrSplitCfg<LOGN>::T, BrSplitCfg<LOGN>::MIN_BLO
             for (int d = 0; d < DIG; ++d) {
                 const double2* k0 = el + static_cast<size_t>(2 * d + h) * 2 * M;  // row 2d + h, column 0
                 const double2* k1 = k0 + M;
+                if constexpr (MB == 1) {
 #pragma unroll
-                for (int j = 0; j < 8; ++j) {
-                    cfma(y0[j], x[d][j], __ldg(k0 + j * TH));
-                    cfma(y1[j], x[d][j], __ldg(k1 + j * TH));
+                    for (int j = 0; j < 8; ++j) {
+                        cfma(y0[j], x[d][j], __ldg(k0 + j * TH));
+                        cfma(y1[j], x[d][j], __ldg(k1 + j * TH));
+                    }
+                } else {
+                    // subsets {0} {1} {0,1} at spectrum offsets 0, 4 DIG M, 8 DIG M
+                    constexpr size_t KS = static_cast<size_t>(4) * DIG * M;
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) {
+                        const double2 c0 = cbuf[j * T + tid], c1 = cbuf[(8 + j) * T + tid];
+                        double2 ta = __ldg(k0 + j * TH), tb = __ldg(k1 + j * TH);
+                        cfma(ta, c1, __ldg(k0 + 2 * KS + j * TH));
+                        cfma(tb, c1, __ldg(k1 + 2 * KS + j * TH));
+                        double2 ra = cmul(c0, ta), rb = cmul(c0, tb);
+                        cfma(ra, c1, __ldg(k0 + KS + j * TH));
+                        cfma(rb, c1, __ldg(k1 + KS + j * TH));
+                        cfma(y0[j], x[d][j], ra);
+                        cfma(y1[j], x[d][j], rb);
+                    }
                 }
             }
             // the previous limb's inverse transform (or the forward passes) no longer reads fs
@@ -168,10 +207,12 @@ __global__ void __launch_bounds__(BrSplitCfg<LOGN>::T, BrSplitCfg<LOGN>::MIN_BLO
                 }
             }
             __syncthreads();
+            if constexpr (MB == 1) {
 #pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                const double2 w = zeta_pow<LOGN>(tws, slot_exp<LOGN>(mbase, at, j));
-                y0[j] = cmul(y0[j], make_double2(w.x - 1.0, w.y));
+                for (int j = 0; j < 8; ++j) {
+                    const double2 w = zeta_pow<LOGN>(tws, slot_exp<LOGN>(mbase, at[0], j));
+                    y0[j] = cmul(y0[j], make_double2(w.x - 1.0, w.y));
+                }
             }
             fft_inverse_from_regs<LOGM>(
                 my_fs, ht, tab, y0,
@@ -213,47 +254,61 @@ __global__ void __launch_bounds__(BrSplitCfg<LOGN>::T, BrSplitCfg<LOGN>::MIN_BLO
 cudaError_t ntt_forward(uint64_t* out, const uint64_t* in, const uint64_t* tw, const uint64_t* tws,
                         const cbs_dmodulus* mod, size_t dim, size_t batch, cudaStream_t s);
 
-template <int LOGN, bool WIDE, int DIG>
+template <int LOGN, bool WIDE, int DIG, int MB>
 static cudaError_t br_split_launch(const BlindRotateArgs& a, const FftKeyArgs& f, const SplitKeyArgs& k,
                                    uint32_t batch, cudaStream_t s) {
-    constexpr uint32_t N = 1u << LOGN, M = N / 2;
+    constexpr uint32_t N = 1u << LOGN, M = N / 2, T = BrSplitCfg<LOGN>::T;
     const size_t smem = 2ull * N * sizeof(uint64_t) + (2ull * M + FftTab<LOGN - 1>::size()) * sizeof(double2) +
-                        2ull * DIG * M * sizeof(typename DigitPair<WIDE>::T);
+                        2ull * DIG * M * sizeof(typename DigitPair<WIDE>::T) +
+                        (MB == 2 ? 2ull * 8 * T * sizeof(double2) : 0);
     static size_t configured[64] = {};  // per device
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
     if (configured[dev] < smem) {
-        cudaError_t e = cudaFuncSetAttribute(k_blind_rotate_fft_split<LOGN, WIDE, DIG>,
+        cudaError_t e = cudaFuncSetAttribute(k_blind_rotate_fft_split<LOGN, WIDE, DIG, MB>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
         if (e != cudaSuccess) return e;
         configured[dev] = smem;
     }
-    k_blind_rotate_fft_split<LOGN, WIDE, DIG><<<batch, BrSplitCfg<LOGN>::T, smem, s>>>(a, f, k);
+    k_blind_rotate_fft_split<LOGN, WIDE, DIG, MB><<<batch, T, smem, s>>>(a, f, k);
     return cudaGetLastError();
 }
 
 template <int LOGN, bool WIDE>
 static cudaError_t br_split_launch(const BlindRotateArgs& a, const FftKeyArgs& f, const SplitKeyArgs& k,
-                                   uint32_t batch, cudaStream_t s) {
+                                   uint32_t batch, uint32_t mb, cudaStream_t s) {
+    if (mb == 2) {
+        switch (a.digits) {
+            case 2: return br_split_launch<LOGN, WIDE, 2, 2>(a, f, k, batch, s);
+            case 3: return br_split_launch<LOGN, WIDE, 3, 2>(a, f, k, batch, s);
+            default: return cudaErrorInvalidValue;
+        }
+    }
     switch (a.digits) {
-        case 2: return br_split_launch<LOGN, WIDE, 2>(a, f, k, batch, s);
-        case 3: return br_split_launch<LOGN, WIDE, 3>(a, f, k, batch, s);
-        case 4: return br_split_launch<LOGN, WIDE, 4>(a, f, k, batch, s);
+        case 2: return br_split_launch<LOGN, WIDE, 2, 1>(a, f, k, batch, s);
+        case 3: return br_split_launch<LOGN, WIDE, 3, 1>(a, f, k, batch, s);
+        case 4: return br_split_launch<LOGN, WIDE, 4, 1>(a, f, k, batch, s);
         default: return cudaErrorInvalidValue;
     }
 }
 
 cudaError_t launch_blind_rotate_fft_split(const BlindRotateArgs& a, const FftKeyArgs& f, const SplitKeyArgs& k,
-                                          const cbs_dmodulus* d_mod, uint32_t N, uint32_t batch, cudaStream_t s) {
+                                          const cbs_dmodulus* d_mod, uint32_t N, uint32_t batch, uint32_t mb,
+                                          cudaStream_t s) {
     if (batch == 0) return cudaSuccess;
-    if (a.g.gbits < 1 || a.g.gbits > 24 || a.digits < 2 || a.digits > 4) return cudaErrorInvalidValue;
+    if (a.g.gbits < 1 || a.g.gbits > 24 || a.digits < 2 || a.digits > (mb == 2 ? 3u : 4u)) return cudaErrorInvalidValue;
+    if (mb != 1 && mb != 2) return cudaErrorInvalidValue;
     if (k.limbs < 1 || k.limbs > kMaxSplitLimbs || k.bskx == nullptr) return cudaErrorInvalidValue;
     if (f.tab_len != (N == 1024 ? FftTab<9>::size() : FftTab<10>::size())) return cudaErrorInvalidValue;
     const bool wide = wide_digits(a.g.gbits);
     cudaError_t e;
     switch (N) {
-        case 1024: e = wide ? br_split_launch<10, true>(a, f, k, batch, s) : br_split_launch<10, false>(a, f, k, batch, s); break;
-        case 2048: e = wide ? br_split_launch<11, true>(a, f, k, batch, s) : br_split_launch<11, false>(a, f, k, batch, s); break;
+        case 1024:
+            e = wide ? br_split_launch<10, true>(a, f, k, batch, mb, s) : br_split_launch<10, false>(a, f, k, batch, mb, s);
+            break;
+        case 2048:
+            e = wide ? br_split_launch<11, true>(a, f, k, batch, mb, s) : br_split_launch<11, false>(a, f, k, batch, mb, s);
+            break;
         default: return cudaErrorInvalidValue;
     }
     if (e != cudaSuccess) return e;
@@ -268,18 +323,21 @@ static uint32_t bit_length(uint64_t v) {
     return b;
 }
 
-bool split_plan(uint32_t N, uint64_t Q, int gbits, uint32_t digits, SplitPlan& out) {
-    if (N < 2 || (N & (N - 1)) || Q < 3 || gbits < 1 || digits < 1) return false;
+bool split_plan(uint32_t N, uint64_t Q, int gbits, uint32_t digits, uint32_t mb, SplitPlan& out) {
+    if (N < 2 || (N & (N - 1)) || Q < 3 || gbits < 1 || digits < 1 || mb < 1 || mb > 2) return false;
     const uint32_t logn = bit_length(N) - 1, logq = bit_length(Q);
     const uint32_t log_rows = bit_length(2 * digits - 1);  // ceil(log2(2 digits))
-    // |limb| <= 2^(lb-1), |digit| <= 2^(g-1), N * 2 digits terms, x2 for X^a - 1:
-    // bound_bits = lb + g - 1 + log2 N + ceil(log2(2 digits)), kept <= 50 (the reference's margin)
-    const int lb_max = 51 - gbits - static_cast<int>(logn) - static_cast<int>(log_rows);
+    // |limb| <= 2^(lb-1), |digit| <= 2^(g-1), N * 2 digits terms, times the monomial factor: X^a - 1
+    // (L1 norm 2, one bit) for mb = 1, c0 + c1 + c0 c1 (L1 norm 2 + 2 + 4, three bits) for mb = 2:
+    // bound_bits = lb + g - 2 + log2 N + ceil(log2(2 digits)) + mono_bits, kept <= 50 (the
+    // reference's margin)
+    const uint32_t mono_bits = mb == 1 ? 1 : 3;
+    const int lb_max = 52 - gbits - static_cast<int>(logn) - static_cast<int>(log_rows) - static_cast<int>(mono_bits);
     if (lb_max < 2) return false;
     const uint32_t limbs = (logq + static_cast<uint32_t>(lb_max) - 1) / static_cast<uint32_t>(lb_max);
     if (limbs < 1 || limbs > kMaxSplitLimbs) return false;
     const uint32_t lb = (logq + limbs - 1) / limbs;
-    const uint32_t bound = lb + static_cast<uint32_t>(gbits) - 1 + logn + log_rows;
+    const uint32_t bound = lb + static_cast<uint32_t>(gbits) - 2 + logn + log_rows + mono_bits;
     // the rounded limb product must also sit below Q/2 (it is added as a centred residue):
     // 2^bound <= 2^(logq - 2) <= Q/2
     if (bound > 50 || bound + 2 > logq) return false;

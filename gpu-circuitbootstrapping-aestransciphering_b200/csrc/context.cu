@@ -74,17 +74,25 @@ FftKeyArgs fft_key_args(const cbs_context* c) {
     return f;
 }
 
-// limb spectra of the bootstrapping key and the FFT tables for the exact split-FFT backend
+static cbs_status make_grouped_keys(cbs_context* c);
+
+// limb spectra of the bootstrapping key (mb = 1) or of the grouped keys (mb = 2, generated here
+// unless imported) and the FFT tables for the exact split-FFT backend
 static cbs_status prepare_split(cbs_context* c) {
     if (c->split_ready) return CBS_OK;
     if (!c->keys_ready) {
         set_error("split FFT backend: no key material (call cbs_keygen first)");
         return CBS_ERR_NOT_READY;
     }
+    const bool grouped = c->br_mb > 1;
+    if (grouped && c->h_mbk.empty()) {
+        if (cbs_status st = make_grouped_keys(c)) return st;
+    }
+    const std::vector<uint64_t>& src = grouped ? c->h_mbk : c->hk.bsk;
+    const uint32_t per_step = (grouped ? mb_subsets(c->br_mb) : 1u) * 4 * c->p.digits_g;
     std::vector<double2> bskx, ftab;
     try {
-        keys_to_fft_limbs_host(c->tab, c->hk.bsk.data(), c->hk.bsk.size() / c->p.N, 4 * c->p.digits_g, c->split,
-                               bskx);
+        keys_to_fft_limbs_host(c->tab, src.data(), src.size() / c->p.N, per_step, c->split, bskx);
     } catch (const std::exception& e) {
         set_error(std::string("split FFT keys: ") + e.what());
         return CBS_ERR_OOM;
@@ -95,7 +103,26 @@ static cbs_status prepare_split(cbs_context* c) {
     CBS_CUDA_TRY(c->d_fft_tab.upload(ftab.data(), ftab.size(), s));
     CBS_CUDA_TRY(cudaStreamSynchronize(s));
     c->split_ready = true;
+    if (grouped) c->mb_ready = true;
     return CBS_OK;
+}
+
+// the limb split of the split-FFT backend for grouping mb, or CBS_ERR_UNSUPPORTED
+static cbs_status split_plan_for(const cbs_context* c, uint32_t mb, SplitPlan& plan, const char* who) {
+    const int gbits = __builtin_ctz(c->p.base_g);
+    if ((c->p.N != 1024 && c->p.N != 2048) || c->p.digits_g < 2 || c->p.digits_g > (mb == 2 ? 3u : 4u) ||
+        c->p.base_g > (1u << 24) || !split_plan(c->p.N, c->p.Q, gbits, c->p.digits_g, mb, plan)) {
+        set_error(std::string(who) +
+                  ": the split FFT backend needs N = 1024 or 2048, 2-4 gadget digits (2-3 for mb = 2) of at most 24 "
+                  "bits, mb 1 or 2, and a limb split (at most 4 limbs) whose products stay below 2^50 and Q/2");
+        return CBS_ERR_UNSUPPORTED;
+    }
+    return CBS_OK;
+}
+
+static void reset_split(cbs_context* c) {
+    c->split_ready = false;
+    c->d_bskx.reset();
 }
 
 static SplitKeyArgs split_key_args(const cbs_context* c) {
@@ -133,8 +160,8 @@ static cbs_status upload_mb_spectra(cbs_context* c) {
     return CBS_OK;
 }
 
-static cbs_status prepare_mb(cbs_context* c) {
-    if (c->br_mb <= 1 || c->mb_ready) return CBS_OK;
+// grouped keys of the context's secrets into c->h_mbk
+static cbs_status make_grouped_keys(cbs_context* c) {
     if (!c->keys_ready) {
         set_error("multi-bit blind rotation: no key material (call cbs_keygen first)");
         return CBS_ERR_NOT_READY;
@@ -144,17 +171,21 @@ static cbs_status prepare_mb(cbs_context* c) {
                   "import them with cbs_import_mb_bsk");
         return CBS_ERR_NOT_READY;
     }
-    if (c->device_keyed) {
-        // keys drawn on the device (cbs_keygen_device): the grouped keys from the same stream
-        if (cbs_status st = device_grouped_keys(c, c->br_mb)) return st;
-        return upload_mb_spectra(c);
-    }
+    // keys drawn on the device (cbs_keygen_device): the grouped keys from the same stream
+    if (c->device_keyed) return device_grouped_keys(c, c->br_mb);
     try {
         generate_mb_bsk(c->p, c->tab, c->hk, c->br_mb, c->key_seed ^ kMbSeedTweak, c->h_mbk);
     } catch (const std::exception& e) {
         set_error(std::string("multi-bit keys: ") + e.what());
         return CBS_ERR_OOM;
     }
+    return CBS_OK;
+}
+
+static cbs_status prepare_mb(cbs_context* c) {
+    if (c->br_mb <= 1 || c->mb_ready) return CBS_OK;
+    if (c->br_backend == CBS_BR_FFT64_SPLIT) return prepare_split(c);
+    if (cbs_status st = make_grouped_keys(c)) return st;
     return upload_mb_spectra(c);
 }
 
@@ -219,7 +250,8 @@ cbs_status run_blind_rotate(cbs_context* c, const uint64_t* d_a, const uint64_t*
             set_error("split FFT backend selected but its key material is not prepared");
             return CBS_ERR_NOT_READY;
         }
-        CBS_CUDA_TRY(launch_blind_rotate_fft_split(a, fft_key_args(c), split_key_args(c), c->d_mod.p, c->p.N, batch, s));
+        CBS_CUDA_TRY(launch_blind_rotate_fft_split(a, fft_key_args(c), split_key_args(c), c->d_mod.p, c->p.N, batch,
+                                                   c->br_mb, s));
         return CBS_OK;
     }
     if (c->br_method == CBS_BR_LMKCDEY) return run_blind_rotate_lmkcdey(c, d_a, d_b, batch, a_stride, d_mv, s);
@@ -649,9 +681,15 @@ cbs_status cbs_import_mb_bsk(cbs_context* ctx, uint32_t mb, const uint64_t* keys
     CBS_CHECK_ARG(ctx && keys, "import_mb_bsk: null argument");
     CBS_CHECK_ARG(mb >= 2 && mb <= 4, "import_mb_bsk: mb must be 2, 3 or 4");
     ctx->mb_explicit = true;
-    if (ctx->br_backend != CBS_BR_FFT64) {
-        set_error("import_mb_bsk: grouped blind rotation is implemented for the FFT64 backend");
+    const bool split = ctx->br_backend == CBS_BR_FFT64_SPLIT;
+    if (ctx->br_backend != CBS_BR_FFT64 && !(split && mb == 2)) {
+        set_error("import_mb_bsk: grouped blind rotation is implemented for the FFT64 backend (mb 2-4) and the "
+                  "split FFT backend (mb 2)");
         return CBS_ERR_UNSUPPORTED;
+    }
+    SplitPlan plan;
+    if (split) {
+        if (cbs_status st = split_plan_for(ctx, mb, plan, "import_mb_bsk")) return st;
     }
     if (!ctx->keys_ready) {
         set_error("import_mb_bsk: import or generate the keys first");
@@ -673,6 +711,11 @@ cbs_status cbs_import_mb_bsk(cbs_context* ctx, uint32_t mb, const uint64_t* keys
     ctx->br_mb = mb;
     ctx->mb_ready = false;
     ctx->aes.drop_graphs();
+    if (split) {
+        ctx->split = plan;
+        reset_split(ctx);
+        return prepare_split(ctx);
+    }
     return upload_mb_spectra(ctx);
 }
 
@@ -698,17 +741,27 @@ cbs_status cbs_context_set_br_multibit(cbs_context* ctx, uint32_t mb) {
     CBS_CHECK_ARG(ctx, "set_br_multibit: null context");
     CBS_CHECK_ARG(mb >= 1 && mb <= 4, "set_br_multibit: mb must be 1, 2, 3 or 4");
     ctx->mb_explicit = true;
-    if (mb > 1 && ctx->br_backend != CBS_BR_FFT64) {
-        set_error("set_br_multibit: grouped blind rotation is implemented for the FFT64 backend");
+    const bool split = ctx->br_backend == CBS_BR_FFT64_SPLIT;
+    if (mb > 1 && ctx->br_backend != CBS_BR_FFT64 && !(split && mb == 2)) {
+        set_error("set_br_multibit: grouped blind rotation is implemented for the FFT64 backend (mb 2-4) and the "
+                  "split FFT backend (mb 2)");
         return CBS_ERR_UNSUPPORTED;
+    }
+    SplitPlan plan;
+    if (split) {
+        if (cbs_status st = split_plan_for(ctx, mb, plan, "set_br_multibit")) return st;
     }
     if (mb != ctx->br_mb) {
         ctx->br_mb = mb;
         ctx->mb_ready = false;
         ctx->h_mbk.clear();
         ctx->d_bskf_mb.reset();
+        reset_split(ctx);
     }
-    if (mb > 1 && ctx->keys_ready) {
+    if (split) ctx->split = plan;
+    if (split && ctx->keys_ready) {  // limb spectra of the BSK (mb = 1) or of the grouped keys
+        if (cbs_status st = prepare_split(ctx)) return st;
+    } else if (mb > 1 && ctx->keys_ready) {
         if (cbs_status st = prepare_mb(ctx)) return st;
     }
     ctx->aes.drop_graphs();
@@ -734,26 +787,28 @@ cbs_status cbs_context_set_br_backend(cbs_context* ctx, int backend) {
         set_error("set_br_backend: the FFT64 backend supports at most 4 gadget digits of at most 24 bits");
         return CBS_ERR_UNSUPPORTED;
     }
+    const int prev = ctx->br_backend;
+    SplitPlan plan;
     if (backend == CBS_BR_FFT64_SPLIT) {
-        SplitPlan plan;
-        const int gbits = __builtin_ctz(ctx->p.base_g);
-        if ((ctx->p.N != 1024 && ctx->p.N != 2048) || ctx->p.digits_g < 2 || ctx->p.digits_g > 4 ||
-            ctx->p.base_g > (1u << 24) || !split_plan(ctx->p.N, ctx->p.Q, gbits, ctx->p.digits_g, plan)) {
-            set_error("set_br_backend: the split FFT backend needs N = 1024 or 2048, 2-4 gadget digits of at "
-                      "most 24 bits, and a limb split (at most 4 limbs) whose products stay below 2^50 and Q/2");
-            return CBS_ERR_UNSUPPORTED;
-        }
-        if (ctx->br_backend != CBS_BR_FFT64_SPLIT || ctx->split.limbs != plan.limbs) {
-            ctx->split_ready = false;
-            ctx->d_bskx.reset();
-        }
+        // the grouping survives only a re-selection of the same backend
+        if (cbs_status st = split_plan_for(ctx, prev == backend ? ctx->br_mb : 1, plan, "set_br_backend")) return st;
+    }
+    if (backend != prev && ctx->br_mb > 1) {  // grouped keys belong to the backend that made them
+        ctx->br_mb = 1;
+        ctx->mb_ready = false;
+        ctx->h_mbk.clear();
+        ctx->d_bskf_mb.reset();
+        reset_split(ctx);
+    }
+    if (backend == CBS_BR_FFT64_SPLIT) {
+        if (prev != backend || ctx->split.limbs != plan.limbs || ctx->split.limb_bits != plan.limb_bits)
+            reset_split(ctx);
         ctx->split = plan;
         if (ctx->keys_ready) {
             if (cbs_status st = prepare_split(ctx)) return st;
         }
     } else if (ctx->split_ready) {  // the limb spectra are needed by the split backend only
-        ctx->split_ready = false;
-        ctx->d_bskx.reset();
+        reset_split(ctx);
     }
     if (backend == CBS_BR_FFT64 && ctx->keys_ready) {
         if (cbs_status st = prepare_fft(ctx)) return st;
@@ -761,12 +816,6 @@ cbs_status cbs_context_set_br_backend(cbs_context* ctx, int backend) {
     ctx->br_backend = backend;
     if (backend == CBS_BR_FFT64) {
         if (cbs_status st = apply_tuned_multibit(ctx)) return st;
-    }
-    if (backend != CBS_BR_FFT64 && ctx->br_mb > 1) {  // grouped keys exist for the FFT form only
-        ctx->br_mb = 1;
-        ctx->mb_ready = false;
-        ctx->h_mbk.clear();
-        ctx->d_bskf_mb.reset();
     }
     if (backend != CBS_BR_NTT && ctx->br_method == CBS_BR_LMKCDEY) {  // LMKCDEY exists for the NTT form only
         ctx->br_method = CBS_BR_GINX;
@@ -779,11 +828,13 @@ cbs_status cbs_context_set_br_backend(cbs_context* ctx, int backend) {
     return CBS_OK;
 }
 
-cbs_status cbs_split_fft_plan(const cbs_params* params, uint32_t* limbs, uint32_t* limb_bits, uint32_t* bound_bits) {
+cbs_status cbs_split_fft_plan(const cbs_params* params, uint32_t mb, uint32_t* limbs, uint32_t* limb_bits,
+                              uint32_t* bound_bits) {
     CBS_CHECK_ARG(params && limbs && limb_bits && bound_bits, "split_fft_plan: null argument");
+    CBS_CHECK_ARG(mb == 1 || mb == 2, "split_fft_plan: mb must be 1 or 2");
     if (cbs_status st = validate(*params)) return st;
     SplitPlan plan;
-    if (!split_plan(params->N, params->Q, __builtin_ctz(params->base_g), params->digits_g, plan)) {
+    if (!split_plan(params->N, params->Q, __builtin_ctz(params->base_g), params->digits_g, mb, plan)) {
         set_error("split_fft_plan: no split of at most 4 limbs keeps the products below 2^50 and Q/2");
         return CBS_ERR_UNSUPPORTED;
     }

@@ -75,17 +75,21 @@ struct SplitKeyArgs {
     uint64_t pw[kMaxSplitLimbs];         // 2^(limb_bits l) mod Q
     uint64_t pws[kMaxSplitLimbs];        // their Shoup quotients
 };
-// the limb split for ring N, modulus Q and a gadget of `digits` digits of gbits bits: false
-// when no split of at most kMaxSplitLimbs limbs keeps the products below 2^50 and Q / 2
-bool split_plan(uint32_t N, uint64_t Q, int gbits, uint32_t digits, SplitPlan& out);
+// the limb split for ring N, modulus Q, a gadget of `digits` digits of gbits bits and the
+// grouping mb (1 or 2): false when no split of at most kMaxSplitLimbs limbs keeps the products
+// below 2^50 and Q / 2
+bool split_plan(uint32_t N, uint64_t Q, int gbits, uint32_t digits, uint32_t mb, SplitPlan& out);
 // key polynomials [count][N] (NTT domain, mod Q), per_step consecutive polynomials to a step,
 // to limb spectra [count / per_step][limbs][per_step][N/2]
 void keys_to_fft_limbs_host(const host::NttTables& t, const uint64_t* keys_ntt, size_t count, uint32_t per_step,
                             const SplitPlan& plan, std::vector<double2>& out);
-// one-bit GINX blind rotation with exact limb products (N = 1024 or 2048, 2-4 digits); the MV
-// outputs are bit-identical to launch_blind_rotate's and left in the NTT domain
+// GINX blind rotation with exact limb products (N = 1024 or 2048): one-bit (mb = 1, 2-4 digits,
+// k.bskx the limbs of the BSK) or grouped mb = 2 (2-3 digits, k.bskx the limbs of the grouped
+// keys [groups][limbs][3 subsets][2*digits][2][N/2]); the MV outputs are bit-identical to
+// launch_blind_rotate's and left in the NTT domain
 cudaError_t launch_blind_rotate_fft_split(const BlindRotateArgs& a, const FftKeyArgs& f, const SplitKeyArgs& k,
-                                          const cbs_dmodulus* d_mod, uint32_t N, uint32_t batch, cudaStream_t s);
+                                          const cbs_dmodulus* d_mod, uint32_t N, uint32_t batch, uint32_t mb,
+                                          cudaStream_t s);
 
 // mv_ntt: also transform the MV outputs to the NTT domain (the reference layout); false
 // leaves them in the coefficient domain for the FFT HomTrace

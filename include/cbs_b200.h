@@ -166,18 +166,21 @@ cbs_status cbs_keygen_device(cbs_context *ctx, const uint8_t *rng_key);
  * bitwise/src/cirbts/cirbts-init.cu:1084-1140, cirbts-bootstrap.cu:939-1085): the key is cut
  * into balanced limbs small enough that every FP64 digit x limb product rounds to its exact
  * integer, so the blind rotation -- and every output -- is bit-identical to CBS_BR_NTT's;
- * HomTrace, SchemeSwitch and the CMux run in their exact NTT forms.  One-bit GINX only (mb 1),
- * N = 1024 or 2048, 2-4 gadget digits; CBS_ERR_UNSUPPORTED when no split of at most 4 limbs
- * keeps the products below 2^50 (cbs_split_fft_plan reports the split). */
+ * HomTrace, SchemeSwitch and the CMux run in their exact NTT forms.  GINX one-bit (2-4 gadget
+ * digits) or grouped mb = 2 (2-3 digits, cbs_context_set_br_multibit after selecting the
+ * backend), N = 1024 or 2048; CBS_ERR_UNSUPPORTED when no split of at most 4 limbs keeps the
+ * products below 2^50 (cbs_split_fft_plan reports the split).  Selecting another backend resets
+ * the grouping to mb = 1. */
 enum { CBS_BR_NTT = 0, CBS_BR_FFT64 = 1, CBS_BR_FFT64_SPLIT = 2 };
 cbs_status cbs_context_set_br_backend(cbs_context *ctx, int backend);
 
-/* The limb split CBS_BR_FFT64_SPLIT uses for these parameters: *limbs limbs of *limb_bits
- * bits, every rounded limb-product coefficient below 2^*bound_bits (<= 50).  The reference's
- * sizing is limb_bits = 50 - (log2 Bg + log2 N + log2 digitsG2) unsigned limbs
- * (cirbts-init.cu:1097-1120); here the limbs are balanced and equalised.  CBS_ERR_UNSUPPORTED
- * when no split of at most 4 limbs exists. */
-cbs_status cbs_split_fft_plan(const cbs_params *params, uint32_t *limbs, uint32_t *limb_bits,
+/* The limb split CBS_BR_FFT64_SPLIT uses for these parameters and grouping mb (1 or 2):
+ * *limbs limbs of *limb_bits bits, every rounded limb-product coefficient below 2^*bound_bits
+ * (<= 50).  The reference's sizing is limb_bits = 50 - (log2 Bg + log2 N + log2 digitsG2)
+ * unsigned limbs (cirbts-init.cu:1097-1120); here the limbs are balanced and equalised, and
+ * mb = 2 adds two bits for the monomial factor c0 + c1 + c0 c1.  CBS_ERR_UNSUPPORTED when no
+ * split of at most 4 limbs exists. */
+cbs_status cbs_split_fft_plan(const cbs_params *params, uint32_t mb, uint32_t *limbs, uint32_t *limb_bits,
                               uint32_t *bound_bits);
 
 /* Multi-bit blind rotation (the reference's CIRBTS_PBS_MULTIBIT grouping,
@@ -189,8 +192,8 @@ cbs_status cbs_split_fft_plan(const cbs_params *params, uint32_t *limbs, uint32_
  * keys ({0} {1} {2} {3} {0,1} {0,2} {1,2} {0,1,2}), applied as the mb = 3 step of coefficients
  * 0-2 and then a one-bit step of coefficient 3 on a fresh decomposition.  The grouped keys are
  * generated from the context's secrets (3, 7 or 8 RGSWs per group) when keys exist or are next
- * generated.  mb > 1 needs the FFT64 backend (CBS_ERR_UNSUPPORTED otherwise); selecting the
- * NTT backend resets mb to 1. */
+ * generated.  mb > 1 needs the FFT64 backend, or mb = 2 the split FFT backend
+ * (CBS_ERR_UNSUPPORTED otherwise); selecting another backend resets mb to 1. */
 cbs_status cbs_context_set_br_multibit(cbs_context *ctx, uint32_t mb);
 
 /* Blind-rotation method (the reference's BINFHE_METHOD of the CirBTS context: GINX, or

@@ -79,6 +79,53 @@ def test_split_blind_rotate_equals_ntt_kernel_at_296(pkg, sctx):
     assert diff == 0, f"{diff} of {got.size} words differ"
 
 
+def test_split_grouped_blind_rotate_equals_oracle(pkg, oracle, sctx):
+    """Grouped mb = 2 on the split backend (keys for {0} {1} {0,1}, combined per spectrum slot as
+    c0 (K0 + c1 K01) + c1 K1): bit-identical to the oracle's exact grouped rotation
+    (orc_blind_rotate_mb) with the same grouped keys, for encryptions and for uniform masks."""
+    p = sctx.params
+    limbs, lb, bound = pkg.split_fft_plan(p, 2)
+    print(f"{sctx.preset} mb = 2: {limbs} limbs of {lb} bits, limb products below 2^{bound}")
+    assert bound <= 50
+    keys = sctx.export_keys()
+    oc = OracleCbs(oracle, p, keys)
+    sctx.set_br_multibit(2)
+    try:
+        mbk = sctx.export_mb_bsk()
+        rng = np.random.default_rng(17)
+        a1, b1 = lwe_encrypt_bits(rng, keys["s_lwe"], [1, 0, 1], p.q_lwe)
+        a2 = rng.integers(0, p.q_lwe, size=(3, p.n), dtype=np.uint64)
+        b2 = rng.integers(0, p.q_lwe, size=3, dtype=np.uint64)
+        a, b = np.vstack([a1, a2]), np.concatenate([b1, b2])
+        got = _blind_rotate(pkg, sctx, a, b)
+    finally:
+        sctx.set_br_multibit(1)
+    want = oc.br_acc_mb(a, b, mbk, 2)
+    assert np.array_equal(got[:, 0], want)
+
+
+def test_split_grouped_aes128(pkg, sctx):
+    """AES-128 CTR with the grouped split blind rotation: keystream equal to OpenSSL's."""
+    from cryptography.hazmat.primitives.ciphers import Cipher, algorithms, modes
+    p = sctx.params
+    key = bytes(range(96, 112))
+    rng = np.random.default_rng(23)
+    ctr = rng.bytes(16)
+    h = np.frombuffer(ctr, np.uint8).copy()
+    sctx.set_br_multibit(2)
+    try:
+        pkg.call("cbs_aes128_setup", sctx.handle, key, 5)
+        oa = np.zeros((128, p.n), np.uint64)
+        ob = np.zeros(128, np.uint64)
+        pkg.call("cbs_aes128_ctr_transcipher", sctx.handle, h.ctypes.data, 1, oa.ctypes.data, ob.ctypes.data)
+    finally:
+        sctx.set_br_multibit(1)
+    got_bits, err = lwe_decrypt_bits(sctx.export_keys()["s_lwe"], oa, ob, p.q_lwe)
+    out = bytes(int(sum(int(got_bits[i * 8 + k]) << k for k in range(8))) for i in range(16))
+    assert out == Cipher(algorithms.AES(key), modes.ECB()).encryptor().update(ctr)
+    assert max(err) < p.q_lwe // 8
+
+
 def test_split_aes128_equals_ntt_backend(pkg, sctx):
     """AES-128 CTR on the split backend: the keystream equals OpenSSL's and every output LWE word
     equals the exact NTT backend's on the same keys and counters."""
@@ -138,11 +185,14 @@ def test_split_blind_rotate_timing(pkg, sctx):
     t0 = time.time()
     try:
         split_us = time_backend(pkg.BR_FFT64_SPLIT)
+        sctx.set_br_multibit(2)
+        split2_us = time_backend(pkg.BR_FFT64_SPLIT)
         ntt_us = time_backend(pkg.BR_NTT)
         fft_us = time_backend(pkg.BR_FFT64)
     finally:
         pkg.call("cbs_context_set_br_backend", sctx.handle, pkg.BR_FFT64_SPLIT)
-    print(f"{sctx.preset} blind rotation, {batch} cts: split FFT (exact) {split_us:.1f} us, exact NTT "
-          f"{ntt_us:.1f} us, FP64 FFT one-bit (approximate) {fft_us:.1f} us per bootstrap "
-          f"({time.time() - t0:.1f} s)")
-    assert split_us > 0 and ntt_us > 0
+        sctx.set_br_multibit(1)
+    print(f"{sctx.preset} blind rotation, {batch} cts: split FFT (exact) one-bit {split_us:.1f} us, mb = 2 "
+          f"{split2_us:.1f} us, exact NTT {ntt_us:.1f} us, FP64 FFT one-bit (approximate) {fft_us:.1f} us per "
+          f"bootstrap ({time.time() - t0:.1f} s)")
+    assert split_us > 0 and split2_us > 0 and ntt_us > 0

@@ -29,6 +29,12 @@ def test_split_plan_presets(pkg, preset, want):
     assert math.ceil(int(p.Q).bit_length() / ref_bits) == limbs
 
 
+@pytest.mark.parametrize("preset,want", [("3x12", (3, 18, 45)), ("2x18", (3, 18, 50))])
+def test_split_plan_grouped(pkg, preset, want):
+    """mb = 2: the monomial factor c0 + c1 + c0 c1 has L1 norm 8, two bits above X^a - 1."""
+    assert pkg.split_fft_plan(pkg.preset_params(preset), 2) == want
+
+
 def test_split_plan_wide_gadgets(pkg):
     p = pkg.preset_params("3x12")
     p.base_g, p.digits_g = 1 << 24, 2  # 24-bit digits: limbs of at most 14 bits, 4 of them
