@@ -150,6 +150,13 @@ class GPUCirBTSContext {
     // KeyGen + RLWEKeyGen + CirBTKeyGen + KeySwitchGen of the example, from a seed
     void KeyGen(uint64_t seed) { check(cbs_keygen(ctx_, seed), "KeyGen"); }
 
+    // The context's CBS backend (the reference reads CIRBTS_BACKEND=ntt|split_fft or
+    // CIRBTS_USE_SPLIT_FFT at construction, cirbts-backend.cu:14-38, cirbts-init.cu:333-337):
+    // CBS_BR_NTT, CBS_BR_FFT64 or CBS_BR_FFT64_SPLIT (exact, the reference's split_fft)
+    void SetBackend(int backend) { check(cbs_context_set_br_backend(ctx_, backend), "SetBackend"); }
+    // CIRBTS_PBS_MULTIBIT (cirbts-init.cu:376-386): 1, or 2 / 3 / 4 grouped coefficients per step
+    void SetMultibit(uint32_t mb) { check(cbs_context_set_br_multibit(ctx_, mb), "SetMultibit"); }
+
     // The context's BINFHE_METHOD (GenerateCirBTSContext(paramset, GINX | LMKCDEY),
     // cirbts-init.cu:630-726): CBS_BR_GINX or CBS_BR_LMKCDEY with automorphism keys for 2N - 5 and
     // 5^1 .. 5^numAutoKeys, or the windowed key set (CIRBTS_LMK_AUTOKEYS_WINDOW) when

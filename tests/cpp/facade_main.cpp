@@ -6,8 +6,8 @@
 //         PhantomRelinKey: ks_dims (N size_q size_p chain_index beta), ks_chain, ks_c2, ks_ct,
 //         ks_evk -> ks_out
 //   cbs   GPUCirBTSContext: KeyGen(seed), gpu_CircuitBootstrappingBatch, gpu_CircuitBootstrapping and
-//         gpu_CircuitBootstrappingBatchToDevice on host LWE ciphertexts: cbs_dims (seed batch),
-//         cbs_a, cbs_b -> cbs_out (the batch's RGSW rows)
+//         gpu_CircuitBootstrappingBatchToDevice on host LWE ciphertexts: cbs_dims (seed batch
+//         [backend]), cbs_a, cbs_b -> cbs_out (the batch's RGSW rows)
 //   gate  GPUBinFHEContext::BatchGPUEvalBinGate(NAND): exit status 0 when every gate decrypts to
 //         the truth table
 //   gfunc GPUBinFHEContext's functional evaluators (BatchGPUEvalFunc, GPUEvalFunc, BatchGPUEvalSign,
@@ -84,6 +84,7 @@ static int run_cbs(const std::string& dir) {
     cbs_params params{};
     check(cbs_params_default(&params), "params");
     GPUCirBTSContext cc(params, batch);
+    if (dims.size() > 2) cc.SetBackend(static_cast<int>(dims[2]));  // default: the context's (NTT)
     cc.KeyGen(seed);
     const auto a = read_raw<uint64_t>(dir + "/cbs_a");
     const auto b = read_raw<uint64_t>(dir + "/cbs_b");

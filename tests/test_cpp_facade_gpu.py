@@ -73,13 +73,17 @@ def test_facade_keyswitch_inplace(facade_bin, tmp_path, oracle):
     assert np.array_equal(got, want)
 
 
-def test_facade_circuit_bootstrap_host_lwe(facade_bin, tmp_path, pkg, oracle):
+@pytest.mark.parametrize("backend", ["ntt", "split"])
+def test_facade_circuit_bootstrap_host_lwe(facade_bin, tmp_path, pkg, oracle, backend):
+    """The exact backends through the facade (SetBackend): NTT and the split FFT (the
+    reference's CIRBTS_BACKEND=split_fft), both bit-identical to the oracle's CBS."""
     p = pkg.default_params()
     seed, batch = 21, 3
     keys = pkg.generate_keys_host(p, seed)
     rng = np.random.default_rng(5)
     a, b = lwe_encrypt_bits(rng, keys["s_lwe"], [1, 0, 1], p.q_lwe)
-    np.array([seed, batch], np.uint64).tofile(tmp_path / "cbs_dims")
+    be = pkg.BR_NTT if backend == "ntt" else pkg.BR_FFT64_SPLIT
+    np.array([seed, batch, be], np.uint64).tofile(tmp_path / "cbs_dims")
     a.astype(np.uint64).tofile(tmp_path / "cbs_a")
     b.astype(np.uint64).tofile(tmp_path / "cbs_b")
     _run(facade_bin, "cbs", tmp_path)
