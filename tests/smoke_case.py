@@ -88,6 +88,23 @@ def run_smoke(pkg, torch, np) -> None:
                 ph0 = oc.phase_coef(rg[i, j, 0]) + m * g[j] * s
                 assert max(abs(int(x)) for x in ph1) < 2 ** 33 and max(abs(int(x)) for x in ph0) < 2 ** 37
         print("smoke: FFT HomTrace + SchemeSwitch rows decrypt to m g_j / -m g_j s")
+
+        # the exact split-FFT blind rotation (key limbs whose FP64 products round exactly):
+        # one-bit and grouped mb = 2, each equal word for word to the oracle's exact rotation
+        ctx.set_br_backend(pkg.BR_FFT64_SPLIT)
+        for mb in (1, 2):
+            ctx.set_br_multibit(mb)
+            mv.zero_()
+            pkg.call("cbs_blind_rotate_batch_device", ctx.handle, da.data_ptr(), db.data_ptr(), len(bits), p.n,
+                     mv.data_ptr(), None)
+            torch.cuda.synchronize()
+            got = mv.cpu().numpy().view(np.uint64)
+            if mb == 1:
+                assert np.array_equal(got, oc.br_mv(a, b)), "split FFT blind rotation differs from the oracle"
+            else:
+                want = oc.br_acc_mb(a, b, ctx.export_mb_bsk(), 2)
+                assert np.array_equal(got[:, 0], want), "grouped split FFT blind rotation differs from the oracle"
+        print("smoke: exact split-FFT blind rotation (one-bit and mb = 2) equal to the oracle word for word")
     finally:
         ctx.close()
 
