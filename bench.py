@@ -169,6 +169,31 @@ def output_noise(pkg, ctx, key: bytes, ctrs: np.ndarray, ha: np.ndarray, hb: np.
                       "p = erfc(margin / (sqrt(2) sigma)) per bit decision, x 1280 decisions per block"}
 
 
+def split_fft64_pair(pkg, torch, ctx, count: int = 2368, steps: int = 2) -> dict:
+    """The exact split-FFT blind rotation (CBS_BR_FFT64_SPLIT: FP64 products of 18-bit key limbs,
+    bit-identical to the exact NTT kernel) beside the approximate FP64 kernel on the AES
+    context's keys, grouped mb = 2, `count` seeded random LWE ciphertexts, CUDA events; the
+    context is left on the split backend (called after the AES legs)."""
+    p = ctx.params
+    rng = np.random.default_rng(11)
+    a = torch.from_numpy(rng.integers(0, p.q_lwe, size=(count, p.n), dtype=np.int64)).cuda()
+    b = torch.from_numpy(rng.integers(0, p.q_lwe, size=count, dtype=np.int64)).cuda()
+    mv = torch.empty((count, p.num_lut, 2, p.N), dtype=torch.int64, device="cuda")
+    stream = torch.cuda.Stream()
+    fn = lambda: pkg.call("cbs_blind_rotate_batch_device", ctx.handle, a.data_ptr(), b.data_ptr(), count,  # noqa: E731
+                          p.n, mv.data_ptr(), stream.cuda_stream)
+    res = {"batch": count, "br_multibit": 2}
+    for name, backend in (("fp64_approximate", pkg.BR_FFT64), ("split_exact", pkg.BR_FFT64_SPLIT)):
+        pkg.call("cbs_context_set_br_backend", ctx.handle, backend)
+        ctx.set_br_multibit(2)
+        res[name] = {"us_per_bootstrap": _timed(torch, stream, fn, 1, steps) * 1e3 / count}
+    res["limbs"] = dict(zip(("limbs", "limb_bits", "bound_bits"), pkg.split_fft_plan(p, 2)))
+    res["ratio_split_over_fp64_time"] = res["split_exact"]["us_per_bootstrap"] / res["fp64_approximate"]["us_per_bootstrap"]
+    res["note"] = ("AES on the exact split backend: bench.py --backend fft64-split --multibit 2 "
+                   "(every output word equal to the exact NTT path's)")
+    return res
+
+
 def gate_split_pair(pkg, torch, count: int = 1184, steps: int = 3) -> dict:
     """The split-FP32 external product where it is built (torus-32 gate path, n = 636, N = 1024):
     NAND gates/s with split FP32 (one-bit) beside FP64 (grouped mb = 2, the FP64 default), same
@@ -347,6 +372,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
                         "transform and key spectra each against one FP64 product, and a whole-key FP32 product "
                         "misses by ~2^-7 of Q (tests/test_fp32_split_analysis.py)",
             "gate_path_measured": gate_split_pair(pkg, torch)}
+        result["split_fft64"] = split_fft64_pair(pkg, torch, ctx)
     if rank == 0 and args.cpu_baseline:
         result["cpu_baseline"] = cpu_baseline(args)
     if rank == 0:
