@@ -1036,9 +1036,7 @@ cudaError_t launch_blind_rotate_fft_mb(const BlindRotateArgs& a, const FftKeyArg
 
 // ---- host side: FFT-domain key material ----
 
-using cld = std::complex<long double>;
-
-static void host_dif(std::vector<cld>& a, const std::vector<cld>& w) {
+void host_dif(std::vector<cld>& a, const std::vector<cld>& w) {
     const size_t M = a.size();
     for (size_t h = M / 2; h >= 1; h /= 2) {
         const size_t stride = M / (2 * h);

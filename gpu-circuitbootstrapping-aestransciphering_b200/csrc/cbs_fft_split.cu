@@ -347,8 +347,6 @@ bool split_plan(uint32_t N, uint64_t Q, int gbits, uint32_t digits, uint32_t mb,
     return true;
 }
 
-using cld = std::complex<long double>;
-
 void keys_to_fft_limbs_host(const host::NttTables& t, const uint64_t* keys_ntt, size_t count, uint32_t per_step,
                             const SplitPlan& plan, std::vector<double2>& out) {
     const uint32_t N = t.n, M = N / 2, L = plan.limbs, lb = plan.limb_bits;
@@ -386,18 +384,9 @@ void keys_to_fft_limbs_host(const host::NttTables& t, const uint64_t* keys_ntt, 
                     for (uint32_t e = 0; e < M; ++e)
                         z[e] = cld(static_cast<long double>(limb[e]), static_cast<long double>(limb[e + M])) *
                                twist[e];
-                    // forward DIF transform, slot s stored at (s % 8) * (M / 8) + s / 8 (the
-                    // register order of the thread that consumes it, as keys_to_fft_host)
-                    for (size_t hh = M / 2; hh >= 1; hh /= 2) {
-                        const size_t stride = M / (2 * hh);
-                        for (size_t s0 = 0; s0 < M; s0 += 2 * hh)
-                            for (size_t j = 0; j < hh; ++j) {
-                                const cld u = z[s0 + j], q = z[s0 + j + hh];
-                                z[s0 + j] = u + q;
-                                z[s0 + j + hh] = (u - q) * w[j * stride];
-                            }
-                        if (hh == 1) break;
-                    }
+                    // slot s stored at (s % 8) * (M / 8) + s / 8 (the register order of the
+                    // thread that consumes it, as keys_to_fft_host)
+                    host_dif(z, w);
                     const size_t o = (step * L + l) * per_step + within;
                     for (uint32_t e = 0; e < M; ++e)
                         out[o * M + (e % 8) * (M / 8) + e / 8] =

@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <complex>
 #include <cstdint>
 #include <vector>
 
@@ -115,6 +116,10 @@ cudaError_t launch_coef_to_spectra(const uint64_t* coef, double2* out, uint64_t 
 DigitPrep make_digit_prep(uint64_t q, const Gadget& g, uint32_t digits);
 // the FftTab<log2(N/2)> table (fft_core.cuh) computed in long double
 void fft_tables_host(uint32_t N, std::vector<double2>& tab);
+// in-place forward DIF transform of a (size M, twiddles w[e] = exp(2 pi i e / M), e < M/2) in
+// long double: the host side of the key spectra
+using cld = std::complex<long double>;
+void host_dif(std::vector<cld>& a, const std::vector<cld>& w);
 void keys_to_fft_host(const host::NttTables& t, const uint64_t* keys_ntt, size_t count, std::vector<double2>& out,
                       uint32_t split_bits = 0, uint32_t group = 0);
 // key-column split of the HomTrace / SchemeSwitch key spectra: [row][k0_hi, k0_lo, k1][N/2]
