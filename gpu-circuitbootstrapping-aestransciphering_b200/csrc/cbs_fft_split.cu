@@ -158,53 +158,69 @@ __global__ void __launch_bounds__(BrSplitCfg<LOGN>::T, BrSplitCfg<LOGN>::MIN_BLO
         // 3. one product, swap and inverse transform per limb
 #pragma unroll 1
         for (uint32_t l = 0; l < limbs; ++l) {
-            double2 y0[8], y1[8];
-#pragma unroll
-            for (int j = 0; j < 8; ++j) y0[j] = y1[j] = make_double2(0.0, 0.0);
             const double2* el = ek + static_cast<size_t>(l) * PER_STEP * M;
             // 2^(lb l) mod Q by selects on the uniform l (an indexed kernel-parameter array
             // would be copied to local memory)
             const uint64_t pw = l == 1 ? sk.pw[1] : (l == 2 ? sk.pw[2] : sk.pw[3]);
             const uint64_t pws = l == 1 ? sk.pws[1] : (l == 2 ? sk.pws[2] : sk.pws[3]);
+            // mb = 2, column c of this half's partial product: sum over d of the digit spectrum
+            // times the combined key c0 (K0 + c1 K01) + c1 K1 of row 2d + h, column c (subsets
+            // {0} {1} {0,1} at spectrum offsets 0, 4 DIG M, 8 DIG M)
+            auto column = [&](uint32_t c, double2 (&y)[8]) {
+                constexpr size_t KS = static_cast<size_t>(4) * DIG * M;
 #pragma unroll
-            for (int d = 0; d < DIG; ++d) {
-                const double2* k0 = el + static_cast<size_t>(2 * d + h) * 2 * M;  // row 2d + h, column 0
-                const double2* k1 = k0 + M;
-                if constexpr (MB == 1) {
+                for (int j = 0; j < 8; ++j) y[j] = make_double2(0.0, 0.0);
 #pragma unroll
-                    for (int j = 0; j < 8; ++j) {
-                        cfma(y0[j], x[d][j], __ldg(k0 + j * TH));
-                        cfma(y1[j], x[d][j], __ldg(k1 + j * TH));
-                    }
-                } else {
-                    // subsets {0} {1} {0,1} at spectrum offsets 0, 4 DIG M, 8 DIG M
-                    constexpr size_t KS = static_cast<size_t>(4) * DIG * M;
+                for (int d = 0; d < DIG; ++d) {
+                    const double2* kc = el + (static_cast<size_t>(2 * d + h) * 2 + c) * M;
 #pragma unroll
                     for (int j = 0; j < 8; ++j) {
                         const double2 c0 = cbuf[j * T + tid], c1 = cbuf[(8 + j) * T + tid];
-                        double2 ta = __ldg(k0 + j * TH), tb = __ldg(k1 + j * TH);
-                        cfma(ta, c1, __ldg(k0 + 2 * KS + j * TH));
-                        cfma(tb, c1, __ldg(k1 + 2 * KS + j * TH));
-                        double2 ra = cmul(c0, ta), rb = cmul(c0, tb);
-                        cfma(ra, c1, __ldg(k0 + KS + j * TH));
-                        cfma(rb, c1, __ldg(k1 + KS + j * TH));
-                        cfma(y0[j], x[d][j], ra);
-                        cfma(y1[j], x[d][j], rb);
+                        double2 t = __ldg(kc + j * TH);
+                        cfma(t, c1, __ldg(kc + 2 * KS + j * TH));
+                        double2 r = cmul(c0, t);
+                        cfma(r, c1, __ldg(kc + KS + j * TH));
+                        cfma(y[j], x[d][j], r);
                     }
                 }
-            }
-            // the previous limb's inverse transform (or the forward passes) no longer reads fs
-            __syncthreads();
+            };
+            double2 y0[8];
+            if constexpr (MB == 1) {
+                // both columns together: twice the key loads in flight (faster one-bit, where the
+                // registers allow it)
+                double2 y1[8];
 #pragma unroll
-            for (int j = 0; j < 8; ++j) my_fs[cswz(8 * ht + j)] = h ? y0[j] : y1[j];
-            __syncthreads();
-            {
+                for (int j = 0; j < 8; ++j) y0[j] = y1[j] = make_double2(0.0, 0.0);
+#pragma unroll
+                for (int d = 0; d < DIG; ++d) {
+                    const double2* k0 = el + static_cast<size_t>(2 * d + h) * 2 * M;  // row 2d + h
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) {
+                        cfma(y0[j], x[d][j], __ldg(k0 + j * TH));
+                        cfma(y1[j], x[d][j], __ldg(k0 + M + j * TH));
+                    }
+                }
+                // the previous limb's inverse transform (or the forward passes) no longer reads fs
+                __syncthreads();
+#pragma unroll
+                for (int j = 0; j < 8; ++j) my_fs[cswz(8 * ht + j)] = h ? y0[j] : y1[j];
+                __syncthreads();
                 const double2* take = fs + (1 - h) * M;
 #pragma unroll
-                for (int j = 0; j < 8; ++j) {
-                    const double2 t = take[cswz(8 * ht + j)];
-                    y0[j] = cadd(h ? y1[j] : y0[j], t);
-                }
+                for (int j = 0; j < 8; ++j) y0[j] = cadd(h ? y1[j] : y0[j], take[cswz(8 * ht + j)]);
+            } else {
+                // the other half's output column first (its key loads overlap the barrier), then
+                // this half's own column while the other half's partial sums land: one column of
+                // accumulators is live at a time (the combined keys need the registers)
+                column(1 - h, y0);
+                __syncthreads();  // the previous limb's inverse transform no longer reads fs
+#pragma unroll
+                for (int j = 0; j < 8; ++j) my_fs[cswz(8 * ht + j)] = y0[j];
+                column(h, y0);
+                __syncthreads();
+                const double2* take = fs + (1 - h) * M;
+#pragma unroll
+                for (int j = 0; j < 8; ++j) y0[j] = cadd(y0[j], take[cswz(8 * ht + j)]);
             }
             __syncthreads();
             if constexpr (MB == 1) {
