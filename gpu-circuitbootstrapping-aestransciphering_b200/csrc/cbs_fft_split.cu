@@ -36,11 +36,13 @@ struct BrSplitCfg {
     static constexpr int MIN_BLOCKS = LOGN <= 10 ? 2 : 1;
 };
 
-// Two halves of M/8 threads per CTA (k_blind_rotate_fft's organisation).  Per step:
+// Two halves of M/8 threads per CTA (k_blind_rotate_fft's organisation).  Per step (MB = 1) or
+// group of two coefficients (MB = 2):
 //  1. digits of each half's accumulator polynomial, packed biased pairs in shared memory;
 //  2. half h forward-transforms its DIG digit polynomials into registers;
-//  3. per limb l: both key columns of rows 2d + h, limb l, against the digit spectra; the
-//     halves swap partial sums so half h holds output h; times psi^a - 1; inverse transform;
+//  3. per limb l: both key columns of rows 2d + h, limb l (MB = 2: the combined keys
+//     c0 (K0 + c1 K01) + c1 K1, one column at a time), against the digit spectra; the halves
+//     swap partial sums so half h holds output h; MB = 1: times psi^a - 1; inverse transform;
 //     each coefficient rounds to the exact integer limb product, is scaled by 2^(lb l) mod Q and
 //     added to the accumulator position this thread owns.
 template <int LOGN, bool WIDE, int DIG, int MB>
