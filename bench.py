@@ -1145,7 +1145,7 @@ def main() -> None:
                          "the exact split FFT (FP64 products of key limbs, bit-identical to ntt)")
     ap.add_argument("--multibit", type=int, choices=[1, 2, 3, 4], default=None,
                     help="blind rotation over groups of 1, 2, 3 or 4 (staged 3 + 1) LWE coefficients "
-                         "(fft64 backend; fft64-split takes 1 or 2; default 2 for fft64, 1 otherwise)")
+                         "(fft64 backend; fft64-split takes 1 or 2; default 2 for fft64 and fft64-split, 1 for ntt)")
     ap.add_argument("--fft-mode", dest="fft_mode", choices=["fp64", "fp32-split", "fp32"], default="fp64",
                     help="external-product arithmetic of --workload gate / ragged (torus-32): exact FP64, "
                          "split FP32 (24/25-bit + exact top key limb), or FP32 on whole keys; FP32 modes use "
@@ -1181,7 +1181,7 @@ def main() -> None:
     if args.multibit is not None or args.schedule:
         args.tune = False  # an explicit grouping or schedule is measured as given
     if args.multibit is None:
-        args.multibit = 2 if args.backend == "fft64" else 1
+        args.multibit = 2 if args.backend in ("fft64", "fft64-split") else 1
     if args.multibit > 1 and args.backend != "fft64" and not (args.backend == "fft64-split" and args.multibit == 2):
         ap.error("--multibit > 1 needs --backend fft64 (or 2 with fft64-split)")
     world = int(os.environ.get("WORLD_SIZE", "1"))
