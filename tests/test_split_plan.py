@@ -36,6 +36,14 @@ def test_split_plan_grouped(pkg, preset, want):
     assert pkg.split_fft_plan(pkg.preset_params(preset), 2) == want
 
 
+def test_split_plan_small_ring(pkg):
+    """N = 1024 (the smoke case's ring): one bit less of N, the same 3 limbs, a bit more margin."""
+    p = pkg.preset_params("3x12")
+    p.N = 1024
+    assert pkg.split_fft_plan(p, 1) == (3, 18, 42)
+    assert pkg.split_fft_plan(p, 2) == (3, 18, 44)
+
+
 def test_split_plan_wide_gadgets(pkg):
     p = pkg.preset_params("3x12")
     p.base_g, p.digits_g = 1 << 24, 2  # 24-bit digits: limbs of at most 14 bits, 4 of them
